@@ -1,0 +1,482 @@
+// SPDX-License-Identifier: GPL-3.0-or-later
+// Host-side inputs of a domain (cw_case) and the seeded synthetic case generators.
+//
+// Straka density current: a restatement of CPPWRF's ideal-case set-up for "straka" -- the dry sounding
+// (cases::Sounding, src/cases/cases.cpp:17-86), the uniform_z eta levels (:194-201), the level
+// coefficients (BaseState::set_levels, src/dyn/state.cpp:86-116), the hydrostatic initial state
+// (cases::initialize, cases.cpp:224-287) and the 1-D base profiles (src/cases/model.cpp:149-177) -- with
+// the same operation order, so the reference's regression goldens can be reproduced from it.
+//
+// Limited-area case: a from-scratch generator (see cw_gen_lam below) for a 3-D domain with terrain,
+// the hybrid sigma-pressure coordinate, moist species and specified lateral boundaries.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <numbers>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "cw_fields.hpp"
+
+namespace cw {
+namespace cst {
+constexpr double g = 9.81;
+constexpr double r_d = 287.0;
+constexpr double cp = 7.0 * r_d / 2.0;
+constexpr double cv = cp - r_d;
+constexpr double cvpm = -cv / cp;
+constexpr double rcp = r_d / cp;
+constexpr double p1000mb = 100000.0;
+constexpr double t0 = 300.0;
+constexpr double r_v = 461.6;
+constexpr double rvovrd = r_v / r_d;
+constexpr double ep_2 = r_d / r_v;
+}  // namespace cst
+}  // namespace cw
+
+struct cw_case {
+  cw_grid g{};
+  cw_options o{};
+  std::vector<std::vector<double>> f;   // CW_U_1 .. CW_COSA
+  std::vector<std::vector<double>> q1, q2, qtf;
+  std::vector<cw_layout> L;
+  cw_layout Lq{};
+  // vertical arrays
+  std::vector<double> znu, znw, dnw, dn, rdnw, rdn, fnm, fnp, c1h, c2h, c3h, c4h, c1f, c2f, c3f, c4f, u_base, v_base,
+      t_base, qv_base_1d, z_base;
+  double cf1 = 0, cf2 = 0, cf3 = 0, cfn = 0, cfn1 = 0, rdx = 0, rdy = 0, p_top = 0;
+  // boundary slabs: [var][side] values / tends; scalars [n][side]
+  std::vector<double> lv[5][4], lt[5][4];
+  std::vector<std::vector<double>> qv[4], qt[4];
+  std::vector<char> q_have;
+  double dtbc = 0;
+
+  double& at(int id, int i, int j, int k) {
+    const cw_layout& l = L[id];
+    return f[id][size_t(l.offset + i * l.si + j * l.sj + k * l.sk)];
+  }
+  size_t idx(const cw_layout& l, int i, int j, int k) const { return size_t(l.offset + i * l.si + j * l.sj + k * l.sk); }
+};
+
+namespace {
+
+// HaloLine (src/core/halo.cpp:52-88) on a host array: x pass over the rows, y pass over the full x extent
+void host_fill_halo(const cw_grid& g, const cw_layout& L, double* base, bool odd_x, bool odd_y) {
+  if (L.uniform) return;
+  double* p = base + L.offset;
+  auto line = [&](double* q, int64_t sn, int n, bool face, bool periodic, bool odd, bool flat, int lo, int hi, int a) {
+    const int nl = face ? 4 : 3;
+    const int i = a < nl ? (face ? -a : -1 - a) : n + (a - nl);
+    if (i < lo || i >= hi) return;
+    int src;
+    if (flat) {
+      const int last = face ? n : n - 1;
+      src = i < 0 ? 0 : (i > last ? last : i);
+    } else if (periodic) {
+      src = ((i % n) + n) % n;
+    } else if (face) {
+      src = i <= 0 ? -i : 2 * n - i;
+    } else {
+      src = i < 0 ? -1 - i : 2 * n - 1 - i;
+    }
+    double v = q[src * sn];
+    if (!periodic && !flat && src == i) return;
+    if (!periodic && !flat && odd) v = -v;
+    q[i * sn] = v;
+  };
+  const bool ux = L.stagger == 'U', vy = L.stagger == 'V';
+  for (int k = 0; k < L.nz; ++k)
+    for (int a = 0; a < (ux ? 8 : 6); ++a)
+      for (int j = 0; j < L.ny; ++j)
+        line(p + j * L.sj + k * L.sk, 1, g.nx, ux, g.bc_x == CW_BC_PERIODIC, odd_x, cw::flat_x(g), L.wi0, L.wi1, a);
+  if (cw::two_d(g)) return;
+  for (int k = 0; k < L.nz; ++k)
+    for (int i = L.wi0; i < L.wi1; ++i)
+      for (int a = 0; a < (vy ? 8 : 6); ++a)
+        line(p + i + k * L.sk, L.sj, g.ny, vy, g.bc_y == CW_BC_PERIODIC, odd_y, cw::flat_y(g), L.wj0, L.wj1, a);
+}
+
+void fill_default_halo(cw_case* c, int id) {
+  const cw_layout& L = c->L[id];
+  const bool three = L.rank == 3;
+  host_fill_halo(c->g, L, c->f[id].data(), three && L.stagger == 'U', three && L.stagger == 'V');
+}
+
+// cases::Sounding (src/cases/cases.cpp:17-86), dry or moist
+struct Sounding {
+  std::vector<double> pi_, w_;
+  double dz_;
+  double (*th_)(double, const void*);
+  double (*qv_)(double, const void*);
+  const void* ctx;
+  double theta(double z) const { return th_(z, ctx); }
+  double qv(double z) const { return qv_ ? qv_(z, ctx) : 0.0; }
+  double theta_rho(double z) const {
+    if (!qv_) return theta(z);
+    const double q = qv(z);
+    return theta(z) * (1.0 + cw::cst::rvovrd * q) / (1.0 + q);
+  }
+  Sounding(double (*th_fn)(double, const void*), double (*qv_fn)(double, const void*), const void* c, double p_surf,
+           double zmax, double dz)
+      : dz_(dz), th_(th_fn), qv_(qv_fn), ctx(c) {
+    using namespace cw::cst;
+    const int n = int(std::ceil(zmax / dz)) + 2;
+    pi_.resize(n);
+    pi_[0] = std::pow(p_surf / p1000mb, rcp);
+    for (int m = 1; m < n; ++m) {
+      const double z0 = (m - 1) * dz, z1 = m * dz;
+      const double f = (1.0 / theta_rho(z0) + 4.0 / theta_rho(0.5 * (z0 + z1)) + 1.0 / theta_rho(z1)) / 6.0;
+      pi_[m] = pi_[m - 1] - g / cp * f * dz;
+    }
+    if (qv_) {
+      auto rq = [&](int m) {
+        const double z = m * dz, pi = pi_[m], pp = p1000mb * std::pow(pi, 1.0 / rcp);
+        return pp / (r_d * theta(z) * (1.0 + rvovrd * qv(z)) * pi) * qv(z);
+      };
+      w_.assign(n, 0.0);
+      for (int m = n - 2; m >= 0; --m) w_[m] = w_[m + 1] + 0.5 * g * dz * (rq(m) + rq(m + 1));
+    }
+  }
+  double p(double z) const {
+    using namespace cw::cst;
+    const double s = z / dz_;
+    const int m = int(std::floor(s));
+    if (m < 0 || m + 1 >= int(pi_.size())) throw std::runtime_error("Sounding::p out of range");
+    const double z0 = m * dz_, h = z - z0;
+    const double f = (1.0 / theta_rho(z0) + 4.0 / theta_rho(z0 + 0.5 * h) + 1.0 / theta_rho(z)) / 6.0;
+    const double pi = pi_[m] - g / cp * f * h;
+    return p1000mb * std::pow(pi, 1.0 / rcp);
+  }
+  double z_of_p(double pp) const {
+    double lo = 0, hi = (pi_.size() - 2) * dz_;
+    if (pp > p(lo) || pp < p(hi)) throw std::runtime_error("Sounding::z_of_p out of range");
+    for (int it = 0; it < 200 && hi - lo > 1e-9; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      (p(mid) > pp ? lo : hi) = mid;
+    }
+    return 0.5 * (lo + hi);
+  }
+};
+
+// BaseState::set_levels, hybrid_opt = 0 (src/dyn/state.cpp:86-116)
+void set_levels(cw_case* c, const std::vector<double>& e) {
+  const int nz = c->g.nz;
+  if (int(e.size()) != nz + 1) throw std::runtime_error("set_levels: need nz+1 eta levels");
+  for (int k = 0; k <= nz; ++k) c->znw[k] = e[k];
+  for (int k = 0; k < nz; ++k) {
+    c->dnw[k] = c->znw[k + 1] - c->znw[k];
+    c->rdnw[k] = 1.0 / c->dnw[k];
+    c->znu[k] = 0.5 * (c->znw[k + 1] + c->znw[k]);
+  }
+  for (int k = 1; k < nz; ++k) {
+    c->dn[k] = 0.5 * (c->dnw[k] + c->dnw[k - 1]);
+    c->rdn[k] = 1.0 / c->dn[k];
+    c->fnp[k] = 0.5 * c->dnw[k] / c->dn[k];
+    c->fnm[k] = 0.5 * c->dnw[k - 1] / c->dn[k];
+  }
+  const double cof1 = (2. * c->dn[1] + c->dn[2]) / (c->dn[1] + c->dn[2]) * c->dnw[0] / c->dn[1];
+  const double cof2 = c->dn[1] / (c->dn[1] + c->dn[2]) * c->dnw[0] / c->dn[2];
+  c->cf1 = c->fnp[1] + cof1;
+  c->cf2 = c->fnm[1] - cof1 - cof2;
+  c->cf3 = cof2;
+  c->cfn = (0.5 * c->dnw[nz - 1] + c->dn[nz - 1]) / c->dn[nz - 1];
+  c->cfn1 = -0.5 * c->dnw[nz - 1] / c->dn[nz - 1];
+  for (int k = 0; k < nz; ++k) { c->c1h[k] = 1; c->c2h[k] = 0; c->c3h[k] = c->znu[k]; c->c4h[k] = 0; }
+  for (int k = 0; k <= nz; ++k) { c->c1f[k] = 1; c->c2f[k] = 0; c->c3f[k] = c->znw[k]; c->c4f[k] = 0; }
+}
+
+
+}  // namespace
+
+extern "C" {
+
+int cw_default_options(cw_options* o) {
+  if (!o) return -1;
+  std::memset(o, 0, sizeof *o);
+  o->khdif = 0; o->kvdif = 0; o->pr_inv = 3.0;
+  o->top_lid = 0; o->h_adv_order = 5; o->v_adv_order = 3; o->w_damping = 0; o->w_crit_cfl = 1.0;
+  o->epssm = 0.1; o->smdiv = 0.1; o->emdiv = 0.01;
+  o->damp_opt = 0; o->hypsometric_opt = 1; o->zdamp = 5000.0; o->dampcoef = 0.2;
+  o->time_step_sound = 0;
+  o->moist_adv_opt = 1; o->scalar_adv_opt = 1; o->tke_adv_opt = 1;
+  o->diff_opt = 0; o->km_opt = 1;
+  o->flat = 1; o->n_moist = 0; o->n_scalars = 0; o->lbc = 0; o->precision = CW_FP64;
+  return 0;
+}
+
+int cw_layout_of(const cw_grid* g, const cw_options* o, int field, cw_layout* out) {
+  if (!g || !o || !out) return -1;
+  try {
+    if (field >= 0 && field < CW_Q_1) *out = cw::field_layout(*g, *o, field);
+    else if (field >= CW_Q_1 && field <= CW_Q_TENDF) *out = cw::layout_make(*g, 'M', 3, false);
+    else return -1;
+  } catch (...) {
+    return -1;
+  }
+  return 0;
+}
+
+int cw_case_create(const cw_grid* g, const cw_options* o, cw_case** out) {
+  if (!g || !o || !out) return -1;
+  if (cw::unsupported(*g, *o)) return -2;
+  try {
+    cw_case* c = new cw_case;
+    c->g = *g;
+    c->o = *o;
+    c->f.resize(CW_Q_1);
+    c->L.resize(CW_Q_1);
+    for (int id = 0; id < CW_Q_1; ++id) {
+      c->L[id] = cw::field_layout(*g, *o, id);
+      c->f[id].assign(size_t(c->L[id].total), 0.0);
+    }
+    for (int id : {CW_MSFTX, CW_MSFTY, CW_MSFUX, CW_MSFUY, CW_MSFVX, CW_MSFVY, CW_MSFVX_INV, CW_COSA})
+      std::fill(c->f[id].begin(), c->f[id].end(), 1.0);
+    c->Lq = cw::layout_make(*g, 'M', 3, false);
+    c->q1.assign(o->n_scalars, std::vector<double>(size_t(c->Lq.total), 0.0));
+    c->q2 = c->q1;
+    c->qtf = c->q1;
+    const int nz = g->nz;
+    for (auto* a : {&c->znu, &c->dnw, &c->rdnw, &c->c1h, &c->c2h, &c->c3h, &c->c4h, &c->u_base, &c->v_base, &c->t_base,
+                    &c->qv_base_1d, &c->z_base})
+      a->assign(nz, 0.0);
+    for (auto* a : {&c->znw, &c->dn, &c->rdn, &c->fnm, &c->fnp, &c->c1f, &c->c2f, &c->c3f, &c->c4f}) a->assign(nz + 1, 0.0);
+    c->rdx = 1.0 / g->dx;
+    c->rdy = cw::two_d(*g) ? 0.0 : 1.0 / g->dy;
+    c->p_top = g->p_top;
+    if (o->lbc) {
+      for (int v = 0; v < 5; ++v)
+        for (int s = 0; s < 4; ++s) {
+          const size_t n = size_t(cw::lbc_npos(*g, v, s)) * cw::lbc_nk(*g, v) * cw::kLbcWidth;
+          c->lv[v][s].assign(n, 0.0);
+          c->lt[v][s].assign(n, 0.0);
+        }
+      for (int s = 0; s < 4; ++s) {
+        const size_t n = size_t(s < 2 ? g->ny : g->nx) * nz * cw::kLbcWidth;
+        c->qv[s].assign(o->n_scalars, std::vector<double>(n, 0.0));
+        c->qt[s].assign(o->n_scalars, std::vector<double>(n, 0.0));
+      }
+      c->q_have.assign(o->n_scalars, 0);
+    }
+    *out = c;
+  } catch (...) {
+    return -3;
+  }
+  return 0;
+}
+
+int cw_case_destroy(cw_case* c) {
+  delete c;
+  return 0;
+}
+
+int cw_case_field(cw_case* c, int field, int n, double** data, cw_layout* layout) {
+  if (!c) return -1;
+  if (field >= 0 && field < CW_Q_1) {
+    if (data) *data = c->f[field].data();
+    if (layout) *layout = c->L[field];
+    return 0;
+  }
+  if (n < 0 || n >= c->o.n_scalars) return -1;
+  std::vector<double>* v = field == CW_Q_1 ? &c->q1[n] : field == CW_Q_2 ? &c->q2[n] : field == CW_Q_TENDF ? &c->qtf[n] : nullptr;
+  if (!v) return -1;
+  if (data) *data = v->data();
+  if (layout) *layout = c->Lq;
+  return 0;
+}
+
+int cw_case_vertical(cw_case* c, cw_vertical* v) {
+  if (!c || !v) return -1;
+  *v = cw_vertical{c->znu.data(), c->dnw.data(), c->rdnw.data(), c->c1h.data(), c->c2h.data(), c->c3h.data(),
+                   c->c4h.data(), c->znw.data(), c->dn.data(), c->rdn.data(), c->fnm.data(), c->fnp.data(),
+                   c->c1f.data(), c->c2f.data(), c->c3f.data(), c->c4f.data(), c->u_base.data(), c->v_base.data(),
+                   c->t_base.data(), c->qv_base_1d.data(), c->z_base.data(), c->cf1, c->cf2, c->cf3, c->cfn, c->cfn1,
+                   c->rdx, c->rdy, c->p_top, cw::cst::t0};
+  return 0;
+}
+
+int cw_case_lbc(cw_case* c, int is_scalar, int var, int side, double** values, double** tends, size_t* count) {
+  if (!c || !c->o.lbc || side < 0 || side > 3) return -1;
+  if (!is_scalar) {
+    if (var < 0 || var > 4) return -1;
+    if (values) *values = c->lv[var][side].data();
+    if (tends) *tends = c->lt[var][side].data();
+    if (count) *count = c->lv[var][side].size();
+    return 0;
+  }
+  if (var < 0 || var >= c->o.n_scalars) return -1;
+  if (!c->q_have[var]) {
+    if (count) *count = 0;
+    return 1;  // no boundary data for this scalar (flow_dep_bdy)
+  }
+  if (values) *values = c->qv[side][var].data();
+  if (tends) *tends = c->qt[side][var].data();
+  if (count) *count = c->qv[side][var].size();
+  return 0;
+}
+
+int cw_case_lbc_time(cw_case* c, double* dtbc) {
+  if (!c || !dtbc) return -1;
+  *dtbc = c->dtbc;
+  return 0;
+}
+
+int cw_default_ideal_params(cw_ideal_params* p, int kind) {
+  if (!p || kind < 0 || kind > 3) return -1;
+  p->kind = kind;
+  p->theta0 = p->n_bv = p->u0 = p->xc = p->zc = p->xr = p->zr = p->amplitude = p->radius = p->a = CW_DEFAULT;
+  p->p_surf = 1.0e5;
+  return 0;
+}
+
+namespace {
+struct IdealCtx {
+  int kind;
+  double theta0, n_bv, u0;
+};
+double ideal_theta(double z, const void* v) {
+  const IdealCtx* c = static_cast<const IdealCtx*>(v);
+  if (c->kind == CW_IDEAL_REST_STATE || c->kind == CW_IDEAL_IGW) return c->theta0 * std::exp(c->n_bv * c->n_bv * z / cw::cst::g);
+  return 300.0;
+}
+double or_default(double v, double d) { return v < -1e299 ? d : v; }
+}  // namespace
+
+// cases::make_case + init_ideal + cases::initialize for the dry ideal cases (no moisture, flat terrain).
+// The grid's p_top becomes the sounding's pressure at ztop (src/cases/model.cpp:96-99).
+int cw_gen_ideal(cw_case* c, const cw_ideal_params* pp) {
+  if (!c || !pp) return -1;
+  using namespace cw::cst;
+  try {
+    cw_grid& G = c->g;
+    if (!c->o.flat || c->o.n_scalars != 0 || c->o.lbc) return -2;
+    const int kind = pp->kind;
+    const double pi = std::numbers::pi;
+    const double xcenter = 0.5 * G.nx * G.dx;
+    IdealCtx ctx{kind, 300.0, 0.01, 0.0};
+    double xc = 0, zc = 0, xr = 0, zr = 0, amp = 0, rad = 0, aa = 0, u_env = 0;
+    switch (kind) {
+      case CW_IDEAL_REST_STATE:
+        ctx.theta0 = or_default(pp->theta0, 300.0);
+        ctx.n_bv = or_default(pp->n_bv, 0.01);
+        u_env = or_default(pp->u0, 0.0);
+        break;
+      case CW_IDEAL_STRAKA:
+        xc = or_default(pp->xc, xcenter); zc = or_default(pp->zc, 3000.0);
+        xr = or_default(pp->xr, 4000.0); zr = or_default(pp->zr, 2000.0);
+        amp = or_default(pp->amplitude, -15.0);
+        break;
+      case CW_IDEAL_WARM_BUBBLE:
+        xc = or_default(pp->xc, xcenter); zc = or_default(pp->zc, 2000.0);
+        rad = or_default(pp->radius, 2000.0); amp = or_default(pp->amplitude, 2.0);
+        break;
+      case CW_IDEAL_IGW:
+        ctx.theta0 = 300.0;
+        ctx.n_bv = or_default(pp->n_bv, 0.01);
+        u_env = or_default(pp->u0, 20.0);
+        amp = or_default(pp->amplitude, 0.01);
+        aa = or_default(pp->a, 5000.0);
+        xc = or_default(pp->xc, 100000.0);
+        break;
+      default: return -1;
+    }
+    const double Hz = G.ztop;
+    // theta'(x, y, z, exner) of make_case (cases.cpp:103-134); libm::pow(v, 2) is v * v (gcc's fold)
+    auto theta_pert = [&](double x, double z, double exner) -> double {
+      switch (kind) {
+        case CW_IDEAL_STRAKA: {
+          const double a = (x - xc) / xr, b = (z - zc) / zr;
+          const double L = std::sqrt(a * a + b * b);
+          return L <= 1.0 ? amp * 0.5 * (std::cos(pi * L) + 1.0) / exner : 0.0;
+        }
+        case CW_IDEAL_WARM_BUBBLE: {
+          const double a = (x - xc) / rad, b = (z - zc) / rad;
+          const double L = std::sqrt(a * a + b * b);
+          if (!(L <= 1.0)) return 0.0;
+          const double cl = std::cos(0.5 * pi * L);
+          return amp * (cl * cl);
+        }
+        case CW_IDEAL_IGW: {
+          const double t = (x - xc) / aa;
+          return amp * std::sin(pi * z / Hz) / (1.0 + t * t);
+        }
+        default: return 0.0;
+      }
+    };
+    Sounding snd(ideal_theta, nullptr, &ctx, pp->p_surf, G.ztop * 1.2 + 1000.0, 0.5);
+    G.p_top = snd.p(G.ztop);
+    c->p_top = G.p_top;
+    const int nz = G.nz;
+    std::vector<double> eta(nz + 1);  // make_eta_levels, uniform_z
+    {
+      const double ps = snd.p(0.0), pt = snd.p(G.ztop);
+      for (int k = 0; k <= nz; ++k) eta[k] = (snd.p(G.ztop * k / nz) - pt) / (ps - pt);
+      eta[0] = 1.0;
+      eta[nz] = 0.0;
+    }
+    set_levels(c, eta);
+    const double mub = pp->p_surf - G.p_top;
+    std::vector<double> pb(nz), tb(nz), alb(nz), phb(nz + 1), zm(nz), exn(nz);
+    for (int k = 0; k < nz; ++k) {
+      pb[k] = c->c3h[k] * mub + c->c4h[k] + G.p_top;
+      tb[k] = snd.theta(snd.z_of_p(pb[k]));
+      alb[k] = (r_d / p1000mb) * tb[k] * std::pow(pb[k] / p1000mb, cvpm);
+      exn[k] = std::pow(pb[k] / p1000mb, rcp);
+    }
+    phb[0] = 0.0;
+    for (int k = 0; k < nz; ++k) phb[k + 1] = phb[k] - c->dnw[k] * (c->c1h[k] * mub + c->c2h[k]) * alb[k];
+    for (int k = 0; k < nz; ++k) zm[k] = 0.5 * (phb[k] + phb[k + 1]) / g;
+    c->f[CW_MUB][0] = mub;
+    for (int k = 0; k < nz; ++k) {
+      c->f[CW_PB][k] = pb[k];
+      c->f[CW_ALB][k] = alb[k];
+      c->f[CW_T_INIT][k] = tb[k] - t0;
+    }
+    for (int k = 0; k <= nz; ++k) c->f[CW_PHB][k] = phb[k];
+    const int nx = G.nx, ny = G.ny;
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+          const double x = (i + 0.5) * G.dx;
+          const double t = tb[k] + theta_pert(x, zm[k], exn[k]);
+          const double alt = (r_d / p1000mb) * t * std::pow(pb[k] / p1000mb, cvpm);
+          const double al = alt - alb[k];
+          c->at(CW_T_2, i, j, k) = t - t0;
+          c->at(CW_AL, i, j, k) = al;
+          c->at(CW_ALT, i, j, k) = alt;
+        }
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        double ph = 0.0;
+        c->at(CW_PH_2, i, j, 0) = 0.0;
+        for (int k = 0; k < nz; ++k) {
+          ph -= c->dnw[k] * ((c->c1h[k] * mub + c->c2h[k]) * c->at(CW_AL, i, j, k));
+          c->at(CW_PH_2, i, j, k + 1) = ph;
+        }
+      }
+    const cw_layout& Lu = c->L[CW_U_2];
+    for (int k = 0; k < Lu.nz; ++k)
+      for (int j = 0; j < Lu.ny; ++j)
+        for (int i = 0; i < Lu.nx; ++i)
+          c->at(CW_U_2, i, j, k) = (G.bc_x == CW_BC_SYMMETRIC && (i == 0 || i == G.nx)) ? 0.0 : u_env;
+    for (int id : {CW_T_2, CW_AL, CW_ALT, CW_PH_2, CW_U_2, CW_V_2, CW_W_2, CW_P, CW_MU_2}) fill_default_halo(c, id);
+    c->f[CW_U_1] = c->f[CW_U_2];
+    c->f[CW_V_1] = c->f[CW_V_2];
+    c->f[CW_W_1] = c->f[CW_W_2];
+    c->f[CW_T_1] = c->f[CW_T_2];
+    c->f[CW_PH_1] = c->f[CW_PH_2];
+    c->f[CW_MU_1] = c->f[CW_MU_2];
+    for (int k = 0; k < nz; ++k) {  // model.cpp:149-177: the column (0, 0)
+      c->u_base[k] = c->at(CW_U_2, 0, 0, k);
+      c->v_base[k] = c->at(CW_V_2, 0, 0, k);
+      c->t_base[k] = c->f[CW_T_INIT][k];
+      c->qv_base_1d[k] = 0.0;
+      c->z_base[k] = 0.5 * (phb[k] + phb[k + 1]) / g;
+    }
+  } catch (const std::exception&) {
+    return -3;
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,191 @@
+/* SPDX-License-Identifier: GPL-3.0-or-later
+ *
+ * cw_dycore.h -- C ABI of the B200-native WRF-ARW RK3 split-explicit dynamical core.
+ *
+ * This is the drop-in boundary for CPPWRF's dynamics step. Every entry point below replaces one
+ * reference interface; the citation after each declaration names it (file:line in CPPWRF).
+ * Conventions (all entry points):
+ *   - plain C types, no C++ or torch types; every function returns int: 0 = ok, < 0 = error
+ *     (the message is kept per handle, cw_last_error), > 0 = a WRF fatal code raised on the device;
+ *   - no exceptions cross the ABI; a handle is used by one host thread at a time (as RK3 is,
+ *     src/dyn/rk3.hpp:34, one host thread per domain, src/core/backend.cpp:73-81);
+ *   - field memory uses CPPWRF's Layout (src/core/halo.cpp:12-48): structure of arrays, i fastest,
+ *     k slowest, halo 3 in x (and y when ny > 1), row pitch a multiple of 32 elements, element
+ *     (0,0,0) at offset 8 + hy*pitch; horizontally uniform base fields are stored 1D (one value
+ *     per level, src/core/field.hpp:145-191). cw_field_layout reports it for every field.
+ */
+#ifndef CW_DYCORE_H
+#define CW_DYCORE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Lateral boundary kinds, cppwrf::BC (src/core/grid.hpp:19). */
+enum cw_bc { CW_BC_PERIODIC = 0, CW_BC_SYMMETRIC = 1, CW_BC_SPECIFIED = 2, CW_BC_OPEN = 3 };
+
+/* Arithmetic of a handle: CW_FP64 is the plain form, bit-identical to the reference CPU FP64 build;
+ * CW_MIXED keeps the bulk stencils in FP32 and the column solves / sums in FP64. */
+enum cw_precision { CW_FP64 = 0, CW_MIXED = 1 };
+
+/* cppwrf::Grid (src/core/grid.hpp:21-55): mass points nx, ny, nz (ny = 1: 2-D x-z). */
+typedef struct cw_grid {
+  int nx, ny, nz;
+  double dx, dy, dt, ztop, p_top;
+  int bc_x, bc_y; /* enum cw_bc */
+} cw_grid;
+
+/* Namelist options of the dynamics step, as cases::Model::build maps them (src/cases/model.cpp:255-345). */
+typedef struct cw_options {
+  /* LargeStepParams (src/dyn/large_step.hpp:14-22) */
+  double khdif, kvdif, pr_inv;
+  int top_lid, h_adv_order, v_adv_order, w_damping;
+  double w_crit_cfl;
+  /* AcousticParams (src/dyn/rk3.hpp:19-25) */
+  double epssm, smdiv, emdiv;
+  int damp_opt, hypsometric_opt;
+  double zdamp, dampcoef;
+  int time_step_sound; /* 0: RK3::auto_sound_steps (src/dyn/rk3.cpp:149-152) */
+  /* ScalarParams (src/dyn/scalars.hpp:14-19) */
+  int moist_adv_opt, scalar_adv_opt, tke_adv_opt;
+  /* DiffusionConfig (src/dyn/diffusion_driver.hpp:24-51): diff_opt 0 or 1 with km_opt 1 */
+  int diff_opt, km_opt;
+  /* State / BaseState shape: flat = horizontally uniform base state (1-D storage, BaseState::flat) */
+  int flat;
+  int n_moist;   /* moist species (they come first among the scalars, State::add_scalar) */
+  int n_scalars; /* moist species + passive tracers */
+  int lbc;       /* 1: a LateralBC is attached (RK3::set_lateral_bc, width 5 / spec 1 / relax 4) */
+  int precision; /* enum cw_precision */
+} cw_options;
+
+/* Fills o with the reference defaults (the values Model::build takes when a key is absent). */
+int cw_default_options(cw_options* o);
+
+/* Vertical coordinate: BaseState's 1-D arrays and scalars (src/dyn/state.hpp:108-115), sizes
+ * nz (mass levels) or nz + 1 (w levels) as noted. The caller computes them (BaseState::set_levels,
+ * src/dyn/state.cpp:86-116, or cw_levels_from_eta below). */
+typedef struct cw_vertical {
+  const double *znu, *dnw, *rdnw, *c1h, *c2h, *c3h, *c4h;          /* nz */
+  const double *znw, *dn, *rdn, *fnm, *fnp, *c1f, *c2f, *c3f, *c4f; /* nz + 1 */
+  const double *u_base, *v_base, *t_base, *qv_base_1d, *z_base;    /* nz (may be NULL: zero) */
+  double cf1, cf2, cf3, cfn, cfn1, rdx, rdy, p_top, t0;
+} cw_vertical;
+
+/* Field identifiers: State (src/dyn/state.hpp:30-78), Tendencies (:80-90), BaseState (:92-119).
+ * Scalars take an index n (0 .. n_scalars-1). */
+enum cw_field {
+  CW_U_1 = 0, CW_U_2, CW_V_1, CW_V_2, CW_W_1, CW_W_2, CW_T_1, CW_T_2, CW_PH_1, CW_PH_2, CW_MU_1, CW_MU_2,
+  CW_P, CW_AL, CW_ALT, CW_PHP, CW_WW, CW_MUT, CW_MUU, CW_MUV, CW_MUTS, CW_MUUS, CW_MUVS, CW_RU, CW_RV, CW_RW,
+  CW_RU_M, CW_RV_M, CW_WW_M, CW_CQU, CW_CQV, CW_CQW, CW_H_DIABATIC,
+  CW_RU_TEND, CW_RV_TEND, CW_RW_TEND, CW_T_TEND, CW_PH_TEND, CW_MU_TEND,
+  CW_RU_TENDF, CW_RV_TENDF, CW_RW_TENDF, CW_T_TENDF, CW_PH_TENDF,
+  CW_MUB, CW_PB, CW_ALB, CW_T_INIT, CW_QV_BASE, CW_PHB, CW_HT,
+  CW_MSFTX, CW_MSFTY, CW_MSFUX, CW_MSFUY, CW_MSFVX, CW_MSFVY, CW_MSFVX_INV, CW_F, CW_E, CW_SINA, CW_COSA,
+  CW_Q_1, CW_Q_2, CW_Q_TENDF, /* with index n */
+  CW_NFIELDS
+};
+
+/* A field's storage, cppwrf::Layout (src/core/field.hpp:46-64). Element (i,j,k) is at
+ * offset + i*si + j*sj + k*sk of an allocation of total elements. stagger: 'M','U','V','W'. */
+typedef struct cw_layout {
+  int nx, ny, nz, rank, uniform;
+  char stagger;
+  int64_t si, sj, sk, offset, total;
+  int wi0, wi1, wj0, wj1;
+} cw_layout;
+
+/* Lateral boundary slabs, LateralBC::Var / Side (src/dyn/lateral_bc.hpp:30-31). */
+enum cw_lbc_var { CW_LBC_U = 0, CW_LBC_V, CW_LBC_T, CW_LBC_PH, CW_LBC_MU };
+enum cw_lbc_side { CW_XS = 0, CW_XE, CW_YS, CW_YE };
+
+typedef struct cw_handle cw_handle;
+
+/* Layout of a field of a grid without a handle: Layout::make (src/core/halo.cpp:12-48). */
+int cw_layout_of(const cw_grid* g, const cw_options* o, int field, cw_layout* out);
+
+/* RK3 ctor (src/dyn/rk3.hpp:36-37, rk3.cpp:128-136) together with the State, Tendencies and BaseState
+ * allocation of cases::Model (src/cases/model.hpp:28-50): device-resident, zero-filled. */
+int cw_create(const cw_grid* g, const cw_options* o, cw_handle** out);
+/* ~RK3 and the Model's fields. */
+int cw_destroy(cw_handle* h);
+/* BaseState::set_levels + upload_levels (src/dyn/state.cpp:86-124): the 1-D vertical arrays. */
+int cw_set_vertical(cw_handle* h, const cw_vertical* v);
+/* FieldT::fill_host / download (src/core/field.hpp:119-129): copies a field's whole allocation
+ * (halo included, Layout order) from / to host memory; count = layout.total. */
+int cw_upload(cw_handle* h, int field, int n, const double* host, size_t count);
+int cw_download(cw_handle* h, int field, int n, double* host, size_t count);
+/* The field's layout (FieldT::layout, src/core/field.hpp:107). */
+int cw_field_layout(cw_handle* h, int field, int n, cw_layout* out);
+/* The device address of element (0,0,0) of a field (FieldT::data, src/core/field.hpp:108). */
+int cw_field_device_ptr(cw_handle* h, int field, int n, void** out);
+/* LateralBC::set / set_scalar (src/dyn/lateral_bc.hpp:42-44): values and tendencies of one
+ * variable and side, (pos, k, b) with pos fastest, b = 0 the outermost row. */
+int cw_set_lbc(cw_handle* h, int var, int side, const double* values, const double* tends, size_t count);
+int cw_set_lbc_scalar(cw_handle* h, int n, int side, const double* values, const double* tends, size_t count);
+/* LateralBC::dtbc (src/dyn/lateral_bc.hpp:57): seconds since the start of the boundary interval. */
+int cw_set_lbc_time(cw_handle* h, double dtbc);
+/* RK3::step (src/dyn/rk3.hpp:52, rk3.cpp:166-250), nsteps times in a row on the handle's stream. */
+int cw_step(cw_handle* h, int nsteps);
+/* RK3::set_dt (src/dyn/rk3.hpp:45, rk3.cpp:159-164). */
+int cw_set_dt(cw_handle* h, double dt, int n_sound);
+/* RK3::n_sound (src/dyn/rk3.hpp:43). */
+int cw_n_sound(cw_handle* h, int* out);
+/* The stream the handle launches on (cuda_stream_raw, src/core/backend.cpp:73-81); NULL = its own. */
+int cw_set_stream(cw_handle* h, void* cuda_stream);
+/* dev_sync + fatal_check (src/core/backend.hpp:745-769): waits for the handle's work and reports a
+ * device-side error status. */
+int cw_sync(cw_handle* h);
+/* The last error message of h (or of the last failed cw_create when h is NULL). */
+const char* cw_last_error(cw_handle* h);
+/* Kernel launches of the last cw_step call (the count this library issued). */
+int cw_launch_count(cw_handle* h, long long* out);
+
+/* ---- host-side inputs ----
+ * A cw_case holds one domain's complete input in host memory, in the same layouts as the handle's
+ * fields: State, BaseState, the vertical arrays and the boundary slabs. The generators fill it from a
+ * seed; cw_upload_case copies it into a handle (the Model set-up, src/cases/model.cpp:71-179). It
+ * needs no GPU. */
+typedef struct cw_case cw_case;
+int cw_case_create(const cw_grid* g, const cw_options* o, cw_case** out);
+int cw_case_destroy(cw_case* c);
+/* host array of a field (the whole allocation) and its layout */
+int cw_case_field(cw_case* c, int field, int n, double** data, cw_layout* layout);
+int cw_case_vertical(cw_case* c, cw_vertical* out);
+/* boundary slabs of a variable (is_scalar = 0, var = enum cw_lbc_var) or scalar n (is_scalar = 1) */
+int cw_case_lbc(cw_case* c, int is_scalar, int var, int side, double** values, double** tends, size_t* count);
+int cw_case_lbc_time(cw_case* c, double* dtbc);
+int cw_upload_case(cw_handle* h, cw_case* c);
+
+/* Idealized cases of CPPWRF (cases::make_case, src/cases/cases.cpp:90-192, and cases::initialize,
+ * :224-287, with make_eta_levels "uniform_z", :194-201, and the base profiles of model.cpp:149-177).
+ * kind: CW_IDEAL_REST_STATE (theta0 exp(N^2 z / g), uniform u0), CW_IDEAL_STRAKA (cold bubble),
+ * CW_IDEAL_WARM_BUBBLE (Bryan-Fritsch thermal), CW_IDEAL_IGW (Skamarock-Klemp gravity wave).
+ * Parameters left at CW_DEFAULT take the reference's defaults for the kind. */
+enum cw_ideal_kind { CW_IDEAL_REST_STATE = 0, CW_IDEAL_STRAKA = 1, CW_IDEAL_WARM_BUBBLE = 2, CW_IDEAL_IGW = 3 };
+#define CW_DEFAULT (-1.0e300)
+typedef struct cw_ideal_params {
+  int kind;
+  double theta0, n_bv, u0, xc, zc, xr, zr, amplitude, radius, a, p_surf;
+} cw_ideal_params;
+int cw_default_ideal_params(cw_ideal_params* p, int kind);
+int cw_gen_ideal(cw_case* c, const cw_ideal_params* p);
+
+/* Limited-area case: terrain, hybrid sigma-pressure coordinate, moist species, specified boundaries
+ * relaxed toward the initial state; all randomness from seed. */
+typedef struct cw_lam_params {
+  uint64_t seed;
+  double t_surf, lapse, t_strat, p_surf, hill_height, hill_halfwidth, orog_max, u_mean, u_pert, rh_mean, rh_pert,
+      q_patch_max, theta_pert, wind_pert, etac;
+  int hybrid_opt;
+} cw_lam_params;
+int cw_default_lam_params(cw_lam_params* p);
+int cw_gen_lam(cw_case* c, const cw_lam_params* p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CW_DYCORE_H */
