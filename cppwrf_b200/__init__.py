@@ -1,0 +1,94 @@
+# SPDX-License-Identifier: GPL-3.0-or-later
+"""B200-native WRF-ARW RK3 split-explicit dynamical core (CPPWRF's dyn::RK3 step) -- Python host mirror.
+
+The dynamics run in libcw_dycore.so (sm_100a CUDA kernels + C++20 host runtime, include/cw_dycore.h).
+This module mirrors the reference's step interface for Python callers:
+
+    dom = Domain(grid, options)          # RK3(grid, LargeStepParams, AcousticParams, time_step_sound, ScalarParams)
+    dom.upload_case(case)                # cases::Model set-up: State, BaseState, vertical arrays, boundaries
+    dom.step(n)                          # RK3::step(State&, Tendencies&, const BaseState&), n times
+    dom.field("U_2")                     # FieldT::download (whole allocation, CPPWRF layout)
+
+There is no CPU path: a missing library or device raises.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+from .capi import (DEFAULT, FIELDS, FP64, IGW, MIXED, PERIODIC, REST_STATE, SPECIFIED, STRAKA, SYMMETRIC,
+                   WARM_BUBBLE, Case, F, Grid, Layout, Options, default_options, grid, interior)
+
+__all__ = ["Domain", "Batch", "Case", "Grid", "Options", "Layout", "grid", "default_options", "interior", "capi",
+           "FIELDS", "F", "PERIODIC", "SYMMETRIC", "SPECIFIED", "FP64", "MIXED", "REST_STATE", "STRAKA",
+           "WARM_BUBBLE", "IGW", "DEFAULT"]
+
+
+class CwError(RuntimeError):
+    pass
+
+
+def _check(lib, h, rc, what):
+    if rc != 0:
+        msg = lib.cw_last_error(h)
+        raise CwError(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+
+class Domain:
+    """One domain on the device (a handle of the C ABI)."""
+
+    def __init__(self, g, o, lib=None):
+        self.lib = lib or capi.load()
+        self.g, self.o = g, o
+        self.h = C.c_void_p()
+        rc = self.lib.cw_create(C.byref(g), C.byref(o), C.byref(self.h))
+        _check(self.lib, None, rc, "cw_create")
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.lib.cw_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def upload_case(self, case):
+        _check(self.lib, self.h, self.lib.cw_upload_case(self.h, case.h), "cw_upload_case")
+        return self
+
+    def step(self, n=1):
+        _check(self.lib, self.h, self.lib.cw_step(self.h, n), "cw_step")
+        return self
+
+    def sync(self):
+        _check(self.lib, self.h, self.lib.cw_sync(self.h), "cw_sync")
+
+    def n_sound(self):
+        v = C.c_int()
+        self.lib.cw_n_sound(self.h, C.byref(v))
+        return v.value
+
+    def launches(self):
+        v = C.c_longlong()
+        self.lib.cw_launch_count(self.h, C.byref(v))
+        return v.value
+
+    def layout(self, name, n=0):
+        L = Layout()
+        _check(self.lib, self.h, self.lib.cw_field_layout(self.h, F[name], n, C.byref(L)), "cw_field_layout")
+        return L
+
+    def field(self, name, n=0):
+        L = self.layout(name, n)
+        out = np.empty(L.total, dtype=np.float64)
+        rc = self.lib.cw_download(self.h, F[name], n, out.ctypes.data_as(C.POINTER(C.c_double)), out.size)
+        _check(self.lib, self.h, rc, "cw_download")
+        return out
+
+    def upload(self, name, arr, n=0):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        rc = self.lib.cw_upload(self.h, F[name], n, a.ctypes.data_as(C.POINTER(C.c_double)), a.size)
+        _check(self.lib, self.h, rc, "cw_upload")
+
+    def set_graph(self, on):
+        self.lib.cw_set_graph(self.h, 1 if on else 0)

@@ -479,4 +479,358 @@ int cw_gen_ideal(cw_case* c, const cw_ideal_params* pp) {
   return 0;
 }
 
+int cw_default_lam_params(cw_lam_params* p) {
+  if (!p) return -1;
+  p->seed = 1;
+  p->t_surf = 290.0;
+  p->lapse = 0.0065;
+  p->t_strat = 216.65;
+  p->p_surf = 1.0e5;
+  p->hill_height = 1500.0;
+  p->hill_halfwidth = -1.0;  // < 0: a tenth of the domain's width
+  p->orog_max = 800.0;
+  p->u_mean = 10.0;
+  p->u_pert = 2.0;
+  p->rh_mean = 0.70;
+  p->rh_pert = 0.15;
+  p->q_patch_max = 1.0e-3;
+  p->theta_pert = 0.0;
+  p->wind_pert = 0.0;
+  p->etac = 0.2;
+  p->hybrid_opt = 2;
+  return 0;
+}
+
+namespace {
+// splitmix64: the generator's only source of randomness
+struct Rng {
+  uint64_t s;
+  uint64_t next() {
+    uint64_t z = (s += 0x9e3779b97f4a7c15ULL);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+  }
+  double uniform() { return double(next() >> 11) * 0x1.0p-53; }  // [0, 1)
+};
+// a smooth random field in [-1, 1]: a few Fourier modes with random phases, amplitudes ~ |k|^-slope
+struct Noise {
+  struct Mode { double kx, ky, kz, ph, a; };
+  std::vector<Mode> m;
+  double norm = 1;
+  Noise(Rng& r, double Lx, double Ly, double Lz, int nmodes, double slope, int kmax) {
+    const double pi = std::numbers::pi;
+    double sum = 0;
+    for (int n = 0; n < nmodes; ++n) {
+      const int ix = 1 + int(r.uniform() * kmax), iy = int(r.uniform() * (kmax + 1)), iz = int(r.uniform() * 3);
+      const double kk = std::sqrt(double(ix * ix + iy * iy));
+      Mode md{2 * pi * ix / Lx * (r.uniform() < 0.5 ? -1 : 1), Ly > 0 ? 2 * pi * iy / Ly : 0.0, Lz > 0 ? pi * iz / Lz : 0.0,
+              2 * pi * r.uniform(), std::pow(kk, -slope)};
+      sum += md.a;
+      m.push_back(md);
+    }
+    norm = sum > 0 ? 1.0 / sum : 1.0;
+  }
+  double operator()(double x, double y, double z) const {
+    double v = 0;
+    for (const Mode& md : m) v += md.a * std::cos(md.kx * x + md.ky * y + md.kz * z + md.ph);
+    return v * norm;
+  }
+};
+}  // namespace
+
+// A limited-area domain with terrain, the hybrid sigma-pressure coordinate, moisture and specified boundaries.
+//   Vertical: stretched eta levels; hybrid_opt 2 coefficients with etac as WRF computes them (the formula of
+//   CPPWRF's src/cases/wrf_ideal.cpp:275-306). Base state: a dry T(z) profile, T_surf - lapse z up to the
+//   isothermal t_strat, in hydrostatic balance; the base fields at each column's hybrid pressure levels as
+//   WRF's real-data base state is formed (pb from c3h, c4h and mub; t_init, alb from T(pb); phb integrated
+//   from g ht, the discrete relation of src/cases/real_case.cpp:269-280). Terrain: a Gaussian hill in the
+//   middle plus seeded spectral orography (power ~ k^-3), 0 .. orog_max. State: theta_m from the base
+//   theta and qv = RH qsat (RH = rh_mean +- rh_pert, seeded); p' = 0, mu' = 0, al and ph' from the
+//   equation of state and the discrete hydrostatic relation (as cases::initialize); u = u_mean + noise,
+//   v = noise (+- u_pert); w from the kinematic surface condition, filled up with znw^2 (start_em);
+//   species 1.. of the moist set (qc, qr, qi, qs) and tracers: seeded patches up to q_patch_max.
+//   Boundaries: slabs of the initial state, coupled as WRF's boundary file holds them (u, v with the face
+//   column masses, t, ph, qv with the column mass), tendencies 0; qv has boundary data, the other
+//   scalars take flow_dep_bdy.
+int cw_gen_lam(cw_case* c, const cw_lam_params* pp) {
+  if (!c || !pp) return -1;
+  using namespace cw::cst;
+  try {
+    cw_grid& G = c->g;
+    const cw_options& o = c->o;
+    if (o.flat || cw::two_d(G)) return -2;
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    const double p_top = G.p_top > 0 ? G.p_top : 5000.0;
+    G.p_top = p_top;
+    c->p_top = p_top;
+    Rng rng{pp->seed * 0x2545f4914f6cdd1dULL + 12345};
+    // ---- dry reference profile T(z), p(z) and its inverse T(p)
+    const double Ts = pp->t_surf, lap = pp->lapse, Tst = pp->t_strat, ps0 = pp->p_surf;
+    const double z_tr = (Ts - Tst) / lap, ex = g / (r_d * lap);
+    const double p_tr = ps0 * std::pow(Tst / Ts, ex);
+    auto p_of_z = [&](double z) {
+      return z < z_tr ? ps0 * std::pow((Ts - lap * z) / Ts, ex) : p_tr * std::exp(-g * (z - z_tr) / (r_d * Tst));
+    };
+    auto T_of_p = [&](double p) { return p >= p_tr ? Ts * std::pow(p / ps0, 1.0 / ex) : Tst; };
+    // ---- eta levels (stretched) and the coefficients of set_levels
+    std::vector<double> eta(nz + 1);
+    {
+      const double zs = 0.4, den = 1.0 - std::exp(-1.0 / zs);
+      for (int k = 0; k <= nz; ++k) eta[k] = (std::exp(-double(k) / nz / zs) - std::exp(-1.0 / zs)) / den;
+      eta[0] = 1.0;
+      eta[nz] = 0.0;
+    }
+    set_levels(c, eta);
+    // ---- hybrid coefficients (hybrid_opt 2; 0 keeps set_levels' terrain-following values)
+    if (pp->hybrid_opt == 2) {
+      const double etac = pp->etac;
+      const double B1 = 2. * (etac * etac) * (1. - etac);
+      const double B2 = -etac * (4. - 3. * etac - etac * etac * etac);
+      const double B3 = 2. * (1. - etac * etac * etac);
+      const double B4 = -(1. - etac * etac);
+      const double B5 = (1. - etac) * (1. - etac) * ((1. - etac) * (1. - etac));
+      std::vector<double>& znw = c->znw;
+      for (int k = 0; k <= nz; ++k) {
+        double v = (B1 + B2 * znw[k] + B3 * (znw[k] * znw[k]) + B4 * (znw[k] * znw[k] * znw[k])) / B5;
+        if (znw[k] < etac) v = 0.;
+        if (k == 0) v = 1.;
+        else if (k == nz) v = 0.;
+        c->c3f[k] = v;
+      }
+      for (int k = 0; k <= nz; ++k) c->c4f[k] = (znw[k] - c->c3f[k]) * (p1000mb - p_top);
+      for (int k = 0; k < nz; ++k) {
+        c->c3h[k] = (c->c3f[k + 1] + c->c3f[k]) * 0.5;
+        c->c4h[k] = (c->znu[k] - c->c3h[k]) * (p1000mb - p_top);
+      }
+      for (int k = 1; k < nz; ++k) c->c1f[k] = (c->c3h[k] - c->c3h[k - 1]) / (c->znu[k] - c->znu[k - 1]);
+      c->c1f[0] = 1.;
+      c->c1f[nz] = 0.;
+      for (int k = 0; k <= nz; ++k) c->c2f[k] = (1. - c->c1f[k]) * (p1000mb - p_top);
+      for (int k = 0; k < nz; ++k) {
+        c->c1h[k] = (c->c3f[k + 1] - c->c3f[k]) / (znw[k + 1] - znw[k]);
+        c->c2h[k] = (1. - c->c1h[k]) * (p1000mb - p_top);
+      }
+    } else {
+      for (int k = 0; k < nz; ++k) c->c4h[k] = 0.0;
+    }
+    // ---- terrain
+    const double Lx = nx * G.dx, Ly = ny * G.dy;
+    const double hw = pp->hill_halfwidth > 0 ? pp->hill_halfwidth : 0.1 * std::min(Lx, Ly);
+    Noise orog(rng, Lx, Ly, 0.0, 24, 1.5, 6);
+    std::vector<double> oro(size_t(nx) * ny);
+    double omin = 1e300, omax = -1e300;
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const double v = orog((i + 0.5) * G.dx, (j + 0.5) * G.dy, 0.0);
+        oro[size_t(j) * nx + i] = v;
+        omin = std::min(omin, v);
+        omax = std::max(omax, v);
+      }
+    auto ht_at = [&](int i, int j) {
+      const double x = (i + 0.5) * G.dx - 0.5 * Lx, y = (j + 0.5) * G.dy - 0.5 * Ly;
+      const double hill = pp->hill_height * std::exp(-(x * x + y * y) / (hw * hw));
+      const double o2 = pp->orog_max * (oro[size_t(j) * nx + i] - omin) / std::max(omax - omin, 1e-30);
+      return hill + o2;
+    };
+    // ---- base state
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const double ht = ht_at(i, j);
+        c->at(CW_HT, i, j, 0) = ht;
+        const double p_surf = p_of_z(ht);
+        const double mub = p_surf - p_top;
+        c->at(CW_MUB, i, j, 0) = mub;
+        double phb = g * ht;
+        c->at(CW_PHB, i, j, 0) = phb;
+        for (int k = 0; k < nz; ++k) {
+          const double pb = c->c3h[k] * mub + c->c4h[k] + p_top;
+          const double temp = T_of_p(pb);
+          const double t_init = temp * std::pow(p1000mb / pb, r_d / cp) - t0;
+          const double alb = (r_d / p1000mb) * (t_init + t0) * std::pow(pb / p1000mb, cvpm);
+          c->at(CW_PB, i, j, k) = pb;
+          c->at(CW_T_INIT, i, j, k) = t_init;
+          c->at(CW_ALB, i, j, k) = alb;
+          phb = phb - c->dnw[k] * (c->c1h[k] * mub + c->c2h[k]) * alb;
+          c->at(CW_PHB, i, j, k + 1) = phb;
+        }
+      }
+    // ---- state
+    Noise nrh(rng, Lx, Ly, G.ztop > 0 ? G.ztop : 20000.0, 16, 1.0, 5);
+    Noise nu(rng, Lx, Ly, 15000.0, 16, 1.0, 4), nv(rng, Lx, Ly, 15000.0, 16, 1.0, 4), nth(rng, Lx, Ly, 15000.0, 16, 1.0, 4);
+    std::vector<double> qv(size_t(nx) * ny * nz, 0.0);
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+          const double pb = c->at(CW_PB, i, j, k), th = c->at(CW_T_INIT, i, j, k) + t0;
+          const double z = 0.5 * (c->at(CW_PHB, i, j, k) + c->at(CW_PHB, i, j, k + 1)) / g;
+          const double T = th * std::pow(pb / p1000mb, r_d / cp);
+          double rh = pp->rh_mean + pp->rh_pert * nrh((i + 0.5) * G.dx, (j + 0.5) * G.dy, z);
+          rh = std::min(1.0, std::max(0.0, rh));
+          const double es = 611.2 * std::exp(17.67 * (T - 273.15) / (T - 29.65));
+          const double q = o.n_moist > 0 ? std::max(0.0, rh * ep_2 * es / std::max(pb - es, 1.0)) : 0.0;
+          qv[(size_t(k) * ny + j) * nx + i] = q;
+          const double thp = pp->theta_pert * nth((i + 0.5) * G.dx, (j + 0.5) * G.dy, z);
+          const double thm = (th + thp) * (1.0 + rvovrd * q);
+          const double alt = (r_d / p1000mb) * thm * std::pow(pb / p1000mb, cvpm);
+          c->at(CW_T_2, i, j, k) = thm - t0;
+          c->at(CW_ALT, i, j, k) = alt;
+          c->at(CW_AL, i, j, k) = alt - c->at(CW_ALB, i, j, k);
+        }
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const double mub = c->at(CW_MUB, i, j, 0);
+        double ph = 0.0;
+        c->at(CW_PH_2, i, j, 0) = 0.0;
+        for (int k = 0; k < nz; ++k) {
+          ph -= c->dnw[k] * ((c->c1h[k] * mub + c->c2h[k]) * c->at(CW_AL, i, j, k));
+          c->at(CW_PH_2, i, j, k + 1) = ph;
+        }
+      }
+    const double up = pp->u_pert + pp->wind_pert;
+    const cw_layout& Lu = c->L[CW_U_2];
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < Lu.ny; ++j)
+        for (int i = 0; i < Lu.nx; ++i)
+          c->at(CW_U_2, i, j, k) = pp->u_mean + up * nu(i * G.dx, (j + 0.5) * G.dy, (k + 0.5) * 300.0);
+    const cw_layout& Lv = c->L[CW_V_2];
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < Lv.ny; ++j)
+        for (int i = 0; i < Lv.nx; ++i) c->at(CW_V_2, i, j, k) = up * nv((i + 0.5) * G.dx, j * G.dy, (k + 0.5) * 300.0);
+    // moist species and tracers
+    const int ns = o.n_scalars;
+    for (int n = 0; n < ns; ++n) {
+      std::vector<double>& q2 = c->q2[n];
+      const cw_layout& L = c->Lq;
+      if (n == 0 && o.n_moist > 0) {
+        for (int k = 0; k < nz; ++k)
+          for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) q2[c->idx(L, i, j, k)] = qv[(size_t(k) * ny + j) * nx + i];
+        continue;
+      }
+      // patches: Gaussian blobs, cloud species in the lower / ice species in the upper troposphere
+      const int nb = 4;
+      struct Blob { double x, y, z, r, rz, a; };
+      std::vector<Blob> blobs;
+      const bool ice = n == 3 || n == 4;
+      for (int b = 0; b < nb; ++b)
+        blobs.push_back(Blob{Lx * (0.15 + 0.7 * rng.uniform()), Ly * (0.15 + 0.7 * rng.uniform()),
+                             (ice ? 6000.0 : 1500.0) + 3000.0 * rng.uniform(), (3 + 5 * rng.uniform()) * G.dx,
+                             800.0 + 1200.0 * rng.uniform(), pp->q_patch_max * (0.2 + 0.8 * rng.uniform())});
+      for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+          for (int i = 0; i < nx; ++i) {
+            const double x = (i + 0.5) * G.dx, y = (j + 0.5) * G.dy;
+            const double z = 0.5 * (c->at(CW_PHB, i, j, k) + c->at(CW_PHB, i, j, k + 1)) / g;
+            double v = 0;
+            for (const Blob& b : blobs) {
+              const double d2 = ((x - b.x) * (x - b.x) + (y - b.y) * (y - b.y)) / (b.r * b.r) + (z - b.z) * (z - b.z) / (b.rz * b.rz);
+              v += b.a * std::exp(-d2);
+            }
+            q2[c->idx(L, i, j, k)] = std::min(v, pp->q_patch_max);
+          }
+    }
+    // qv_base (3-D): the base state is dry
+    // w: the kinematic surface condition from u, v and the terrain, znw^2 upward (start_em, rk3.cpp:173-200)
+    for (int id : {CW_U_2, CW_V_2, CW_T_2, CW_AL, CW_ALT, CW_PH_2, CW_W_2, CW_P, CW_MU_2, CW_MUB, CW_PB, CW_ALB, CW_T_INIT,
+                   CW_PHB, CW_HT, CW_QV_BASE})
+      fill_default_halo(c, id);
+    for (int n = 0; n < ns; ++n) host_fill_halo(G, c->Lq, c->q2[n].data(), false, false);
+    // cf1..cf3 of set_levels (hybrid coefficients do not change them)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        auto ht = [&](int ii, int jj) { return c->at(CW_HT, ii, jj, 0); };
+        auto U = [&](int ii, int jj, int kk) { return c->at(CW_U_2, ii, jj, kk); };
+        auto V = [&](int ii, int jj, int kk) { return c->at(CW_V_2, ii, jj, kk); };
+        const double cf1 = c->cf1, cf2 = c->cf2, cf3 = c->cf3;
+        const double ws =
+            c->at(CW_MSFTY, i, j, 0) * 0.5 * c->rdy *
+                ((ht(i, j + 1) - ht(i, j)) * (cf1 * V(i, j + 1, 0) + cf2 * V(i, j + 1, 1) + cf3 * V(i, j + 1, 2)) +
+                 (ht(i, j) - ht(i, j - 1)) * (cf1 * V(i, j, 0) + cf2 * V(i, j, 1) + cf3 * V(i, j, 2))) +
+            c->at(CW_MSFTX, i, j, 0) * 0.5 * c->rdx *
+                ((ht(i + 1, j) - ht(i, j)) * (cf1 * U(i + 1, j, 0) + cf2 * U(i + 1, j, 1) + cf3 * U(i + 1, j, 2)) +
+                 (ht(i, j) - ht(i - 1, j)) * (cf1 * U(i, j, 0) + cf2 * U(i, j, 1) + cf3 * U(i, j, 2)));
+        c->at(CW_W_2, i, j, 0) = ws;
+        for (int k = 1; k <= nz; ++k) c->at(CW_W_2, i, j, k) = ws * c->znw[k] * c->znw[k];
+      }
+    fill_default_halo(c, CW_W_2);
+    c->f[CW_U_1] = c->f[CW_U_2];
+    c->f[CW_V_1] = c->f[CW_V_2];
+    c->f[CW_W_1] = c->f[CW_W_2];
+    c->f[CW_T_1] = c->f[CW_T_2];
+    c->f[CW_PH_1] = c->f[CW_PH_2];
+    c->f[CW_MU_1] = c->f[CW_MU_2];
+    for (int n = 0; n < ns; ++n) c->q1[n] = c->q2[n];
+    for (int k = 0; k < nz; ++k) {
+      c->u_base[k] = c->at(CW_U_2, 0, 0, k);
+      c->v_base[k] = c->at(CW_V_2, 0, 0, k);
+      c->t_base[k] = c->at(CW_T_INIT, 0, 0, k);
+      c->qv_base_1d[k] = 0.0;
+      c->z_base[k] = 0.5 * (c->at(CW_PHB, 0, 0, k) + c->at(CW_PHB, 0, 0, k + 1)) / g;
+    }
+    // ---- boundary slabs (pos, k, b) of the coupled initial state; tendencies 0
+    if (o.lbc) {
+      auto mub = [&](int i, int j) { return c->at(CW_MUB, i, j, 0); };
+      auto mut = [&](int i, int j) { return c->at(CW_MU_2, i, j, 0) + mub(i, j); };
+      auto muu = [&](int i, int j) {  // KMu with the doubled edge column
+        const int a = i == 0 ? 0 : i - 1, b = i == nx ? nx - 1 : i;
+        return 0.5 * (c->at(CW_MU_2, b, j, 0) + c->at(CW_MU_2, a, j, 0) + mub(b, j) + mub(a, j));
+      };
+      auto muv = [&](int i, int j) {
+        const int a = j == 0 ? 0 : j - 1, b = j == ny ? ny - 1 : j;
+        return 0.5 * (c->at(CW_MU_2, i, b, 0) + c->at(CW_MU_2, i, a, 0) + mub(i, b) + mub(i, a));
+      };
+      for (int var = 0; var < 5; ++var)
+        for (int side = 0; side < 4; ++side) {
+          std::vector<double>& vals = c->lv[var][side];
+          const int npos = cw::lbc_npos(G, var, side), nk = cw::lbc_nk(G, var);
+          const int ibe = var == CW_LBC_U ? nx : nx - 1, jbe = var == CW_LBC_V ? ny : ny - 1;
+          for (int b = 0; b < cw::kLbcWidth; ++b)
+            for (int k = 0; k < nk; ++k)
+              for (int pos = 0; pos < npos; ++pos) {
+                int i, j;
+                switch (side) {
+                  case CW_XS: i = b; j = pos; break;
+                  case CW_XE: i = ibe - b; j = pos; break;
+                  case CW_YS: i = pos; j = b; break;
+                  default: i = pos; j = jbe - b; break;
+                }
+                double v = 0;
+                switch (var) {
+                  case CW_LBC_U: v = c->at(CW_U_2, i, j, k) * (c->c1h[k] * muu(i, j) + c->c2h[k]); break;
+                  case CW_LBC_V: v = c->at(CW_V_2, i, j, k) * (c->c1h[k] * muv(i, j) + c->c2h[k]); break;
+                  case CW_LBC_T: v = c->at(CW_T_2, i, j, k) * (c->c1h[k] * mut(i, j) + c->c2h[k]); break;
+                  case CW_LBC_PH: v = c->at(CW_PH_2, i, j, k) * (c->c1f[k] * mut(i, j) + c->c2f[k]); break;
+                  default: v = c->at(CW_MU_2, i, j, 0); break;
+                }
+                vals[pos + size_t(k) * npos + size_t(b) * npos * nk] = v;
+              }
+        }
+      if (o.n_moist > 0) {  // qv
+        c->q_have[0] = 1;
+        for (int side = 0; side < 4; ++side) {
+          std::vector<double>& vals = c->qv[side][0];
+          const int npos = side < 2 ? ny : nx;
+          for (int b = 0; b < cw::kLbcWidth; ++b)
+            for (int k = 0; k < nz; ++k)
+              for (int pos = 0; pos < npos; ++pos) {
+                int i, j;
+                switch (side) {
+                  case CW_XS: i = b; j = pos; break;
+                  case CW_XE: i = nx - 1 - b; j = pos; break;
+                  case CW_YS: i = pos; j = b; break;
+                  default: i = pos; j = ny - 1 - b; break;
+                }
+                vals[pos + size_t(k) * npos + size_t(b) * npos * nz] =
+                    c->q2[0][c->idx(c->Lq, i, j, k)] * (c->c1h[k] * mut(i, j) + c->c2h[k]);
+              }
+        }
+      }
+    }
+  } catch (const std::exception&) {
+    return -3;
+  }
+  return 0;
+}
+
 }  // extern "C"

@@ -1,0 +1,1028 @@
+// SPDX-License-Identifier: GPL-3.0-or-later
+// Host runtime of the dycore: handles (one or many domains), the device arena, the per-domain Dom
+// tables, the halo refresh sets, the RK3 step as a sequence of batched launches (captured once into a
+// CUDA graph and replayed), and the C ABI of include/cw_dycore.h.
+//
+// The step order is CPPWRF's RK3::step (src/dyn/rk3.cpp:166-250): copy of the time-t state, then per RK
+// stage rk_step_prep, rk_tendency (+ stage-1 diffusion and boundary relaxation), the acoustic loop,
+// small_step_finish, scalar transport and calc_p_rho_phi; spec_bdy_final and set_w_surface at the end.
+// Halos are refreshed where the reference refreshes them; refreshes with no kernel in between that
+// reads the refreshed cells are merged into one launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <utility>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "cw_fields.hpp"
+#include "kernels_ac.cuh"
+
+namespace cw {
+
+#define CW_CUDA(x)                                                                          \
+  do {                                                                                      \
+    cudaError_t e_ = (x);                                                                   \
+    if (e_ != cudaSuccess) throw std::runtime_error(std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
+
+// the work fields of one domain beyond State / Tendencies / BaseState (SmallStep's fields)
+enum Work { W_U_SAVE, W_V_SAVE, W_W_SAVE, W_T_SAVE, W_PH_SAVE, W_WW1, W_C2A, W_PM1, W_T_2SAVE, W_A, W_ALPHA, W_GAMMA,
+            W_MU_SAVE, W_MUDF, W_MUAVE, W_W_RHS, W_T2A, W_N };
+inline FieldKind work_kind(int w) {
+  switch (w) {
+    case W_U_SAVE: return {'U', 3, false};
+    case W_V_SAVE: return {'V', 3, false};
+    case W_W_SAVE: case W_PH_SAVE: case W_WW1: case W_A: case W_ALPHA: case W_GAMMA: case W_W_RHS: return {'W', 3, false};
+    case W_MU_SAVE: case W_MUDF: case W_MUAVE: return {'M', 2, false};
+    default: return {'M', 3, false};
+  }
+}
+
+struct Member {
+  cw_grid g{};
+  cw_options o{};
+  int n_sound = 0;
+  int esz = 8;  // element size of the fields (8: FP64 form, 4: mixed form)
+  std::vector<cw_layout> L;         // CW_U_1 .. CW_COSA
+  std::vector<char*> base;          // allocation of each field
+  std::vector<cw_layout> LW;
+  std::vector<char*> wbase;
+  cw_layout Lq{};
+  std::vector<char*> q1, qa, qb, qtf, qsc;  // scalar allocations; q_2 is qa or qb by the parity
+  double* vert = nullptr;           // device 1-D arrays (double)
+  size_t vert_off[24]{};
+  char* slab[5] = {};               // LBC slabs per variable (values 4 sides, tendencies 4 sides)
+  size_t slab_off[5][8]{};
+  std::vector<char*> qslab;
+  std::vector<std::array<size_t, 8>> qslab_off;
+  std::vector<char> q_have;
+  double dtbc = 0;
+  int q_parity = 0;
+  double cf1 = 0, cf2 = 0, cf3 = 0, cfn = 0, cfn1 = 0, rdx = 0, rdy = 0;
+};
+
+template <class R>
+struct DevTables {  // device copies of the Dom array and the scalar tables
+  Dom<R>* doms = nullptr;
+  V3<R>* qtab = nullptr;  // per member: q1, q2, qn, qtf, qscale (5 x n_scalars)
+  Slabs<R>* lbcq = nullptr;
+};
+
+struct HaloSetHost {
+  std::vector<HaloField> f;
+  HaloField* fd = nullptr;
+  long long* startd = nullptr;
+  HaloSet set{};
+};
+
+}  // namespace cw
+
+using namespace cw;
+
+struct cw_handle {
+  int precision = CW_FP64;
+  std::vector<Member> m;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  char* arena = nullptr;
+  size_t arena_bytes = 0;
+  DevTables<double> t64;
+  DevTables<float> t32;
+  BlockMap bmap[6]{};
+  int total_blocks[6]{};
+  // halo sets of the fill points
+  enum { H_MU1, H_PREP0, H_PREP1, H_SS0, H_UV, H_AC, H_POST, H_FIN, H_Q1PD, H_SCPD, H_Q2, H_END_P, H_WS0, H_WS1, H_N };
+  HaloSetHost hs[H_N];
+  std::vector<CopyDesc> copies;
+  CopyDesc* copies_d = nullptr;
+  long long* copies_start_d = nullptr;
+  long long copies_total = 0;
+  std::vector<CopyDesc> zeros;  // mudf reset
+  CopyDesc* zeros_d = nullptr;
+  long long* zeros_start_d = nullptr;
+  long long zeros_total = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  bool graph_ok = false;
+  bool use_graph = true;
+  long long launches_step = 0;   // launches of one step
+  long long launches_last = 0;   // launches of the last cw_step call
+  std::string err;
+  std::vector<void*> extra;      // other device allocations
+};
+
+namespace {
+thread_local std::string g_create_err;
+
+template <class F>
+int guarded(cw_handle* h, F f) {
+  try {
+    return f();
+  } catch (const std::exception& e) {
+    if (h) h->err = e.what();
+    else g_create_err = e.what();
+    return -1;
+  }
+}
+
+size_t field_bytes(const cw_layout& L, int esz) { return size_t(L.total) * esz; }
+
+template <class R>
+V3<R> view3(char* base, const cw_layout& L) {
+  return V3<R>{reinterpret_cast<R*>(base) + L.offset, int(L.sj), int(L.sk)};
+}
+template <class R>
+VB<R> viewb(char* base, const cw_layout& L) {
+  return VB<R>{reinterpret_cast<const R*>(base) + L.offset, int(L.si), int(L.sj), int(L.sk)};
+}
+
+// the device arena: every field of every member, vertical arrays, slabs
+void allocate(cw_handle* h) {
+  size_t total = 0;
+  auto take = [&](size_t bytes) {
+    const size_t off = total;
+    total += align_up(bytes);
+    return off;
+  };
+  struct Plan {
+    std::vector<size_t> f, w, q1, qa, qb, qtf, qsc, qslab;
+    size_t vert;
+    size_t slab[5];
+  };
+  std::vector<Plan> plan(h->m.size());
+  for (size_t mi = 0; mi < h->m.size(); ++mi) {
+    Member& M = h->m[mi];
+    Plan& P = plan[mi];
+    M.L.resize(CW_Q_1);
+    for (int id = 0; id < CW_Q_1; ++id) {
+      M.L[id] = field_layout(M.g, M.o, id);
+      P.f.push_back(take(field_bytes(M.L[id], M.esz)));
+    }
+    M.LW.resize(W_N);
+    for (int w = 0; w < W_N; ++w) {
+      const FieldKind k = work_kind(w);
+      M.LW[w] = layout_make(M.g, k.stagger, k.rank, false);
+      P.w.push_back(take(field_bytes(M.LW[w], M.esz)));
+    }
+    M.Lq = layout_make(M.g, 'M', 3, false);
+    for (int n = 0; n < M.o.n_scalars; ++n) {
+      P.q1.push_back(take(field_bytes(M.Lq, M.esz)));
+      P.qa.push_back(take(field_bytes(M.Lq, M.esz)));
+      P.qb.push_back(take(field_bytes(M.Lq, M.esz)));
+      P.qtf.push_back(take(field_bytes(M.Lq, M.esz)));
+      P.qsc.push_back(take(field_bytes(M.Lq, M.esz)));
+    }
+    P.vert = take(24 * size_t(M.g.nz + 2) * sizeof(double));
+    for (int v = 0; v < 5; ++v) {
+      size_t n = 0;
+      if (M.o.lbc)
+        for (int half = 0; half < 2; ++half)
+          for (int s = 0; s < 4; ++s) {
+            M.slab_off[v][half * 4 + s] = n;
+            n += size_t(lbc_npos(M.g, v, s)) * lbc_nk(M.g, v) * kLbcWidth;
+          }
+      P.slab[v] = M.o.lbc ? take(n * M.esz) : 0;
+    }
+    M.qslab_off.assign(M.o.n_scalars, {});
+    M.q_have.assign(M.o.n_scalars, 0);
+    for (int n = 0; n < M.o.n_scalars; ++n) {
+      size_t cnt = 0;
+      if (M.o.lbc)
+        for (int half = 0; half < 2; ++half)
+          for (int s = 0; s < 4; ++s) {
+            M.qslab_off[n][half * 4 + s] = cnt;
+            cnt += size_t(s < 2 ? M.g.ny : M.g.nx) * M.g.nz * kLbcWidth;
+          }
+      P.qslab.push_back(M.o.lbc ? take(cnt * M.esz) : 0);
+    }
+  }
+  CW_CUDA(cudaMalloc(&h->arena, total));
+  CW_CUDA(cudaMemsetAsync(h->arena, 0, total, h->stream));
+  h->arena_bytes = total;
+  for (size_t mi = 0; mi < h->m.size(); ++mi) {
+    Member& M = h->m[mi];
+    Plan& P = plan[mi];
+    for (int id = 0; id < CW_Q_1; ++id) M.base.push_back(h->arena + P.f[id]);
+    for (int w = 0; w < W_N; ++w) M.wbase.push_back(h->arena + P.w[w]);
+    for (int n = 0; n < M.o.n_scalars; ++n) {
+      M.q1.push_back(h->arena + P.q1[n]);
+      M.qa.push_back(h->arena + P.qa[n]);
+      M.qb.push_back(h->arena + P.qb[n]);
+      M.qtf.push_back(h->arena + P.qtf[n]);
+      M.qsc.push_back(h->arena + P.qsc[n]);
+      M.qslab.push_back(M.o.lbc ? h->arena + P.qslab[n] : nullptr);
+    }
+    M.vert = reinterpret_cast<double*>(h->arena + P.vert);
+    for (int a = 0; a < 24; ++a) M.vert_off[a] = size_t(a) * (M.g.nz + 2);
+    for (int v = 0; v < 5; ++v) M.slab[v] = M.o.lbc ? h->arena + P.slab[v] : nullptr;
+  }
+  // BaseState defaults: map factors and cosa = 1 (src/dyn/state.cpp:80-83)
+  for (Member& M : h->m)
+    for (int id : {CW_MSFTX, CW_MSFTY, CW_MSFUX, CW_MSFUY, CW_MSFVX, CW_MSFVY, CW_MSFVX_INV, CW_COSA}) {
+      const size_t n = size_t(M.L[id].total);
+      if (M.esz == 8) {
+        std::vector<double> one(n, 1.0);
+        CW_CUDA(cudaMemcpyAsync(M.base[id], one.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
+        CW_CUDA(cudaStreamSynchronize(h->stream));
+      } else {
+        std::vector<float> one(n, 1.0f);
+        CW_CUDA(cudaMemcpyAsync(M.base[id], one.data(), n * 4, cudaMemcpyHostToDevice, h->stream));
+        CW_CUDA(cudaStreamSynchronize(h->stream));
+      }
+    }
+}
+
+// vertical array slots in Member::vert
+enum { VA_ZNU, VA_ZNW, VA_DNW, VA_DN, VA_RDNW, VA_RDN, VA_FNM, VA_FNP, VA_C1H, VA_C2H, VA_C1F, VA_C2F, VA_UB, VA_VB,
+       VA_FCX, VA_GCX };
+
+template <class R>
+Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
+  Member& M = h->m[mi];
+  Dom<R> D{};
+  const cw_grid& g = M.g;
+  const cw_options& o = M.o;
+  D.nx = g.nx; D.ny = g.ny; D.nz = g.nz; D.nyv = nys(g, 'V'); D.two_d = two_d(g); D.do_y = !two_d(g);
+  D.bc_x = g.bc_x; D.bc_y = g.bc_y;
+  D.spec_x = flat_x(g); D.spec_y = flat_y(g) && !two_d(g);
+  D.lbc = o.lbc; D.flat = o.flat; D.n_moist = o.n_moist; D.n_scalars = o.n_scalars;
+  D.diff_on = o.diff_opt == 1; D.top_lid = o.top_lid; D.w_damping = o.w_damping; D.n_sound = M.n_sound;
+  D.moist_adv_opt = o.moist_adv_opt; D.scalar_adv_opt = o.scalar_adv_opt;
+  D.dt = g.dt; D.epssm = o.epssm; D.smdiv = o.smdiv; D.emdiv = o.emdiv; D.khdif = o.khdif; D.kvdif = o.kvdif;
+  D.prandtl = 1.0 / o.pr_inv;
+  D.hup = o.h_adv_order == 5 ? 1.0 : 0.0;
+  D.vup = o.v_adv_order == 3 ? 1.0 : 0.0;
+  D.w_crit_cfl = o.w_crit_cfl;
+  D.dtbc = M.dtbc;
+  D.cf1 = M.cf1; D.cf2 = M.cf2; D.cf3 = M.cf3; D.cfn = M.cfn; D.cfn1 = M.cfn1; D.rdx = M.rdx; D.rdy = M.rdy;
+  const double* v = M.vert;
+  auto va = [&](int a) { return v + M.vert_off[a]; };
+  D.znu = va(VA_ZNU); D.znw = va(VA_ZNW); D.dnw = va(VA_DNW); D.dn = va(VA_DN); D.rdnw = va(VA_RDNW); D.rdn = va(VA_RDN);
+  D.fnm = va(VA_FNM); D.fnp = va(VA_FNP); D.c1h = va(VA_C1H); D.c2h = va(VA_C2H); D.c1f = va(VA_C1F); D.c2f = va(VA_C2F);
+  D.u_base = va(VA_UB); D.v_base = va(VA_VB); D.fcx = va(VA_FCX); D.gcx = va(VA_GCX);
+  auto f3 = [&](int id) { return view3<R>(M.base[id], M.L[id]); };
+  auto fb = [&](int id) { return viewb<R>(M.base[id], M.L[id]); };
+  auto w3 = [&](int w) { return view3<R>(M.wbase[w], M.LW[w]); };
+  D.u1 = f3(CW_U_1); D.u2 = f3(CW_U_2); D.v1 = f3(CW_V_1); D.v2 = f3(CW_V_2); D.w1 = f3(CW_W_1); D.w2 = f3(CW_W_2);
+  D.t1 = f3(CW_T_1); D.t2 = f3(CW_T_2); D.ph1 = f3(CW_PH_1); D.ph2 = f3(CW_PH_2); D.mu1 = f3(CW_MU_1); D.mu2 = f3(CW_MU_2);
+  D.p = f3(CW_P); D.al = f3(CW_AL); D.alt = f3(CW_ALT); D.php = f3(CW_PHP); D.ww = f3(CW_WW); D.mut = f3(CW_MUT);
+  D.muu = f3(CW_MUU); D.muv = f3(CW_MUV); D.muts = f3(CW_MUTS); D.muus = f3(CW_MUUS); D.muvs = f3(CW_MUVS);
+  D.ru = f3(CW_RU); D.rv = f3(CW_RV); D.rw = f3(CW_RW); D.ru_m = f3(CW_RU_M); D.rv_m = f3(CW_RV_M); D.ww_m = f3(CW_WW_M);
+  D.cqu = f3(CW_CQU); D.cqv = f3(CW_CQV); D.cqw = f3(CW_CQW); D.hd = f3(CW_H_DIABATIC);
+  D.ru_tend = f3(CW_RU_TEND); D.rv_tend = f3(CW_RV_TEND); D.rw_tend = f3(CW_RW_TEND); D.t_tend = f3(CW_T_TEND);
+  D.ph_tend = f3(CW_PH_TEND); D.mu_tend = f3(CW_MU_TEND); D.ru_tendf = f3(CW_RU_TENDF); D.rv_tendf = f3(CW_RV_TENDF);
+  D.rw_tendf = f3(CW_RW_TENDF); D.t_tendf = f3(CW_T_TENDF); D.ph_tendf = f3(CW_PH_TENDF);
+  D.mub = fb(CW_MUB); D.pb = fb(CW_PB); D.alb = fb(CW_ALB); D.t_init = fb(CW_T_INIT); D.qv_base = fb(CW_QV_BASE);
+  D.phb = fb(CW_PHB); D.ht = fb(CW_HT); D.msftx = fb(CW_MSFTX); D.msfty = fb(CW_MSFTY); D.msfux = fb(CW_MSFUX);
+  D.msfuy = fb(CW_MSFUY); D.msfvx = fb(CW_MSFVX); D.msfvy = fb(CW_MSFVY); D.msfvx_inv = fb(CW_MSFVX_INV);
+  D.u_save = w3(W_U_SAVE); D.v_save = w3(W_V_SAVE); D.w_save = w3(W_W_SAVE); D.t_save = w3(W_T_SAVE);
+  D.ph_save = w3(W_PH_SAVE); D.ww1 = w3(W_WW1); D.c2a = w3(W_C2A); D.pm1 = w3(W_PM1); D.t_2save = w3(W_T_2SAVE);
+  D.a = w3(W_A); D.alpha = w3(W_ALPHA); D.gamma = w3(W_GAMMA); D.mu_save = w3(W_MU_SAVE); D.mudf = w3(W_MUDF);
+  D.muave = w3(W_MUAVE); D.w_rhs = w3(W_W_RHS); D.t2a = w3(W_T2A);
+  const int ns = o.n_scalars;
+  D.q1 = qtab_d; D.q2 = qtab_d + ns; D.qn = qtab_d + 2 * ns; D.qtf = qtab_d + 3 * ns; D.qscale = qtab_d + 4 * ns;
+  for (int var = 0; var < 5; ++var) {
+    Slabs<R>& s = D.lbc_var[var];
+    s.nk = lbc_nk(g, var);
+    s.have = o.lbc;
+    for (int sd = 0; sd < 4; ++sd) {
+      s.npos[sd] = lbc_npos(g, var, sd);
+      s.v[sd] = M.slab[var] ? reinterpret_cast<const R*>(M.slab[var]) + M.slab_off[var][sd] : nullptr;
+      s.t[sd] = M.slab[var] ? reinterpret_cast<const R*>(M.slab[var]) + M.slab_off[var][4 + sd] : nullptr;
+    }
+  }
+  D.lbc_q = lbcq_d;
+  return D;
+}
+
+template <class R>
+void upload_tables(cw_handle* h, DevTables<R>& T) {
+  const size_t nm = h->m.size();
+  if (!T.doms) CW_CUDA(cudaMalloc(&T.doms, nm * sizeof(Dom<R>)));
+  size_t nq = 0;
+  for (const Member& M : h->m) nq += size_t(M.o.n_scalars);
+  if (!T.qtab && nq) CW_CUDA(cudaMalloc(&T.qtab, 5 * nq * sizeof(V3<R>)));
+  if (!T.lbcq && nq) CW_CUDA(cudaMalloc(&T.lbcq, nq * sizeof(Slabs<R>)));
+  std::vector<Dom<R>> doms(nm);
+  std::vector<V3<R>> qtab(5 * nq);
+  std::vector<Slabs<R>> lbcq(nq);
+  size_t q0 = 0;
+  for (size_t mi = 0; mi < nm; ++mi) {
+    Member& M = h->m[mi];
+    const int ns = M.o.n_scalars;
+    doms[mi] = make_dom<R>(h, mi, T.qtab ? T.qtab + 5 * q0 : nullptr, T.lbcq ? T.lbcq + q0 : nullptr);
+    for (int n = 0; n < ns; ++n) {
+      char* q2 = M.q_parity ? M.qb[n] : M.qa[n];
+      char* qn = M.q_parity ? M.qa[n] : M.qb[n];
+      qtab[5 * q0 + n] = view3<R>(M.q1[n], M.Lq);
+      qtab[5 * q0 + ns + n] = view3<R>(q2, M.Lq);
+      qtab[5 * q0 + 2 * ns + n] = view3<R>(qn, M.Lq);
+      qtab[5 * q0 + 3 * ns + n] = view3<R>(M.qtf[n], M.Lq);
+      qtab[5 * q0 + 4 * ns + n] = view3<R>(M.qsc[n], M.Lq);
+      Slabs<R>& s = lbcq[q0 + n];
+      s.nk = M.g.nz;
+      s.have = M.o.lbc && M.q_have[n];
+      for (int sd = 0; sd < 4; ++sd) {
+        s.npos[sd] = sd < 2 ? M.g.ny : M.g.nx;
+        s.v[sd] = M.qslab[n] ? reinterpret_cast<const R*>(M.qslab[n]) + M.qslab_off[n][sd] : nullptr;
+        s.t[sd] = M.qslab[n] ? reinterpret_cast<const R*>(M.qslab[n]) + M.qslab_off[n][4 + sd] : nullptr;
+      }
+    }
+    q0 += size_t(ns);
+  }
+  CW_CUDA(cudaMemcpyAsync(T.doms, doms.data(), nm * sizeof(Dom<R>), cudaMemcpyHostToDevice, h->stream));
+  if (nq) {
+    CW_CUDA(cudaMemcpyAsync(T.qtab, qtab.data(), qtab.size() * sizeof(V3<R>), cudaMemcpyHostToDevice, h->stream));
+    CW_CUDA(cudaMemcpyAsync(T.lbcq, lbcq.data(), lbcq.size() * sizeof(Slabs<R>), cudaMemcpyHostToDevice, h->stream));
+  }
+  CW_CUDA(cudaStreamSynchronize(h->stream));
+}
+
+void upload_tables(cw_handle* h) {
+  if (h->precision == CW_FP64) upload_tables<double>(h, h->t64);
+  else upload_tables<float>(h, h->t32);
+}
+
+void build_blockmaps(cw_handle* h) {
+  for (int kind = 0; kind < 6; ++kind) {
+    BlockMap& bm = h->bmap[kind];
+    bm.n = int(h->m.size());
+    int s = 0;
+    for (size_t mi = 0; mi < h->m.size(); ++mi) {
+      bm.start[mi] = s;
+      const Member& M = h->m[mi];
+      s += blocks_of(kind, M.g.nx, M.g.ny, M.g.nz, nys(M.g, 'V'));
+    }
+    bm.start[h->m.size()] = s;
+    h->total_blocks[kind] = s;
+  }
+}
+
+// ---- halo sets
+enum HaloParity { HP_DEFAULT, HP_EVEN, HP_ODDFACE_X, HP_ODD_Y };
+struct HaloItem {
+  char* base;        // allocation (nullptr: indirect)
+  void* ind;         // indirect view address
+  cw_layout L;
+  int parity;
+};
+
+HaloField halo_field(const Member& M, const HaloItem& it) {
+  HaloField f{};
+  const cw_layout& L = it.L;
+  f.p = it.base ? it.base + size_t(L.offset) * M.esz : nullptr;
+  f.ind = it.ind;
+  f.sj = int(L.sj);
+  f.sk = int(L.sk);
+  f.lnx = L.nx;
+  f.lny = L.ny;
+  f.nk = L.nz;
+  f.wi0 = L.wi0; f.wi1 = L.wi1; f.wj0 = L.wj0; f.wj1 = L.wj1;
+  f.gnx = M.g.nx;
+  f.gny = M.g.ny;
+  f.periodic_x = M.g.bc_x == CW_BC_PERIODIC;
+  f.periodic_y = M.g.bc_y == CW_BC_PERIODIC;
+  f.flat_x = flat_x(M.g);
+  f.flat_y = flat_y(M.g);
+  f.two_d = two_d(M.g);
+  f.face_x = L.stagger == 'U';
+  f.face_y = L.stagger == 'V';
+  const bool three = L.rank == 3;
+  switch (it.parity) {
+    case HP_DEFAULT: f.odd_x = three && L.stagger == 'U'; f.odd_y = three && L.stagger == 'V'; break;
+    case HP_ODDFACE_X: f.odd_x = 1; f.oddface_x = 1; break;
+    case HP_ODD_Y: f.odd_y = 1; break;
+    default: break;
+  }
+  f.is_float = M.esz == 4;
+  f.ncell_x = (long long)(f.face_x ? 8 : 6) * L.ny * L.nz;
+  f.ncell = f.ncell_x + (f.two_d ? 0 : (long long)(f.face_y ? 8 : 6) * (L.wi1 - L.wi0) * L.nz);
+  return f;
+}
+
+void finish_haloset(cw_handle* h, HaloSetHost& s) {
+  const int nf = int(s.f.size());
+  std::vector<long long> start(nf + 1, 0);
+  int odd = 0;
+  for (int n = 0; n < nf; ++n) {
+    start[n + 1] = start[n] + s.f[n].ncell;
+    odd |= s.f[n].oddface_x;
+  }
+  if (nf) {
+    CW_CUDA(cudaMalloc(&s.fd, nf * sizeof(HaloField)));
+    CW_CUDA(cudaMalloc(&s.startd, (nf + 1) * sizeof(long long)));
+    CW_CUDA(cudaMemcpy(s.fd, s.f.data(), nf * sizeof(HaloField), cudaMemcpyHostToDevice));
+    CW_CUDA(cudaMemcpy(s.startd, start.data(), (nf + 1) * sizeof(long long), cudaMemcpyHostToDevice));
+  }
+  s.set = HaloSet{s.fd, s.startd, nf, start[nf], odd};
+}
+
+template <class R>
+void build_halosets_t(cw_handle* h, DevTables<R>& T) {
+  size_t q0 = 0;
+  for (size_t mi = 0; mi < h->m.size(); ++mi) {
+    Member& M = h->m[mi];
+    const int ns = M.o.n_scalars;
+    auto F = [&](int id, int par = HP_DEFAULT) { return HaloItem{M.base[id], nullptr, M.L[id], par}; };
+    auto W = [&](int w, int par = HP_DEFAULT) { return HaloItem{M.wbase[w], nullptr, M.LW[w], par}; };
+    auto add = [&](int set, std::initializer_list<HaloItem> items) {
+      for (const HaloItem& it : items) h->hs[set].f.push_back(halo_field(M, it));
+    };
+    const bool spec = specified(M.g);
+    add(cw_handle::H_MU1, {F(CW_MU_1)});
+    add(cw_handle::H_PREP0, {F(CW_U_2), F(CW_V_2), F(CW_W_2), F(CW_T_2), F(CW_PH_2), F(CW_P), F(CW_AL)});
+    if (!spec) add(cw_handle::H_PREP0, {F(CW_MU_2)});
+    add(cw_handle::H_PREP1, {F(CW_MUT), F(CW_RU), F(CW_RV), F(CW_RW), F(CW_ALT), F(CW_PHP), F(CW_MUU, HP_ODDFACE_X),
+                             F(CW_MUV, HP_ODD_Y), F(CW_WW)});
+    add(cw_handle::H_SS0, {F(CW_U_2), F(CW_V_2), F(CW_PH_2), W(W_T_SAVE), W(W_U_SAVE), W(W_V_SAVE), F(CW_MU_2),
+                           F(CW_MUTS), F(CW_P), F(CW_AL)});
+    add(cw_handle::H_UV, {F(CW_U_2)});
+    if (!two_d(M.g)) add(cw_handle::H_UV, {F(CW_V_2)});
+    add(cw_handle::H_AC, {F(CW_MU_2), W(W_MUDF), F(CW_MUTS), F(CW_PH_2), F(CW_P), F(CW_AL)});
+    add(cw_handle::H_POST, {F(CW_MUTS), F(CW_RU_M), F(CW_RV_M), F(CW_WW_M)});
+    add(cw_handle::H_FIN, {F(CW_U_2), F(CW_V_2), F(CW_W_2), F(CW_T_2), F(CW_PH_2), F(CW_WW), F(CW_MU_2), F(CW_P), F(CW_AL)});
+    for (int n = 0; n < ns; ++n) {
+      add(cw_handle::H_Q1PD, {HaloItem{M.q1[n], nullptr, M.Lq, HP_DEFAULT}});
+      add(cw_handle::H_SCPD, {HaloItem{M.qsc[n], nullptr, M.Lq, HP_DEFAULT}});
+      add(cw_handle::H_Q2, {HaloItem{nullptr, T.qtab + 5 * q0 + ns + n, M.Lq, HP_DEFAULT}});
+    }
+    add(cw_handle::H_END_P, {F(CW_P), F(CW_AL)});
+    add(cw_handle::H_WS0, {F(CW_U_2), F(CW_V_2)});
+    add(cw_handle::H_WS1, {F(CW_W_2)});
+    q0 += size_t(ns);
+  }
+  for (int s = 0; s < cw_handle::H_N; ++s) finish_haloset(h, h->hs[s]);
+}
+
+void build_copies(cw_handle* h) {
+  // step start: u_1 = u_2, ... (whole allocations, src/dyn/rk3.cpp:175-178); q_1 = q_2 read through the table
+  size_t q0 = 0;
+  for (Member& M : h->m) {
+    const int pairs[6][2] = {{CW_U_1, CW_U_2}, {CW_V_1, CW_V_2}, {CW_W_1, CW_W_2}, {CW_T_1, CW_T_2}, {CW_PH_1, CW_PH_2}, {CW_MU_1, CW_MU_2}};
+    for (auto& p : pairs)
+      h->copies.push_back(CopyDesc{M.base[p[0]], M.base[p[1]], nullptr, M.L[p[0]].total, M.esz == 4, 0});
+    const int ns = M.o.n_scalars;
+    for (int n = 0; n < ns; ++n) {
+      // src through the device table entry q2[n].p (the element (0,0,0) pointer): offset back to the allocation
+      const void* const* ind = nullptr;
+      if (h->precision == CW_FP64) ind = reinterpret_cast<const void* const*>(&(h->t64.qtab + 5 * q0 + ns + n)->p);
+      else ind = reinterpret_cast<const void* const*>(&(h->t32.qtab + 5 * q0 + ns + n)->p);
+      CopyDesc c{M.q1[n], nullptr, ind, M.Lq.total, M.esz == 4, M.Lq.offset};
+      h->copies.push_back(c);
+    }
+    h->zeros.push_back(CopyDesc{M.wbase[W_MUDF], nullptr, nullptr, M.LW[W_MUDF].total, M.esz == 4, 0});
+    q0 += size_t(ns);
+  }
+  auto up = [&](std::vector<CopyDesc>& v, CopyDesc*& d, long long*& sd, long long& total) {
+    std::vector<long long> st(v.size() + 1, 0);
+    for (size_t n = 0; n < v.size(); ++n) st[n + 1] = st[n] + v[n].n;
+    total = st.back();
+    CW_CUDA(cudaMalloc(&d, v.size() * sizeof(CopyDesc)));
+    CW_CUDA(cudaMalloc(&sd, st.size() * sizeof(long long)));
+    CW_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(CopyDesc), cudaMemcpyHostToDevice));
+    CW_CUDA(cudaMemcpy(sd, st.data(), st.size() * sizeof(long long), cudaMemcpyHostToDevice));
+  };
+  up(h->copies, h->copies_d, h->copies_start_d, h->copies_total);
+  up(h->zeros, h->zeros_d, h->zeros_start_d, h->zeros_total);
+}
+
+// ---- the step
+struct Launcher {
+  cw_handle* h;
+  long long count = 0;
+  void check() {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw std::runtime_error(std::string("kernel launch: ") + cudaGetErrorString(e));
+    ++count;
+  }
+  void halo(int set) {
+    const HaloSet& s = h->hs[set].set;
+    if (s.total == 0) return;
+    const int bs = 256;
+    const unsigned nb = unsigned((s.total + bs - 1) / bs);
+    k_halo<<<nb, bs, 0, h->stream>>>(s, 0);
+    check();
+    if (s.has_oddface) {
+      k_halo<<<nb, bs, 0, h->stream>>>(s, 1);
+      check();
+    }
+  }
+  void copy_list(CopyDesc* d, long long* sd, size_t n, long long total) {
+    if (!total) return;
+    const int bs = 256;
+    k_copy<<<unsigned((total + bs - 1) / bs), bs, 0, h->stream>>>(d, int(n), sd);
+    check();
+  }
+  template <class R, class K, class... Args>
+  void run(int kind, K kern, const Dom<R>* doms, Args... args) {
+    const int nb = h->total_blocks[kind];
+    if (nb == 0) return;
+    const int bs = is_column(kind) ? CX : PX;
+    kern<<<nb, bs, 0, h->stream>>>(doms, h->bmap[kind], args...);
+    check();
+  }
+};
+
+template <class R>
+void enqueue_step(cw_handle* h, Launcher& L, DevTables<R>& T) {
+  const Dom<R>* d = T.doms;
+  const Member& M0 = h->m[0];
+  bool lbc = false, terrain = false, scalars = false, any_pd = false;
+  for (const Member& M : h->m) {
+    lbc |= M.o.lbc != 0;
+    terrain |= !M.o.flat;
+    scalars |= M.o.n_scalars > 0;
+    for (int n = 0; n < M.o.n_scalars; ++n)
+      any_pd |= (n < M.o.n_moist ? M.o.moist_adv_opt : M.o.scalar_adv_opt) == 1;
+  }
+  const int n_sound = M0.n_sound;
+  if (lbc) {
+    k_advance_time<R><<<unsigned(h->m.size()), 1, 0, h->stream>>>(T.doms, int(h->m.size()));
+    L.check();
+  }
+  L.copy_list(h->copies_d, h->copies_start_d, h->copies.size(), h->copies_total);
+  L.halo(cw_handle::H_MU1);
+  for (int rk = 1; rk <= 3; ++rk) {
+    const int ns = rk == 1 ? 1 : (rk == 2 ? n_sound / 2 : n_sound);
+    L.halo(cw_handle::H_PREP0);
+    L.run(RG_COLS_STAG, k_ls_prep<R>, d);
+    L.halo(cw_handle::H_PREP1);
+    if (rk == 1) L.run(RG_STAG, k_tendf_rk1<R>, d);
+    if (rk == 1 && lbc) L.run(RG_RING, k_ring<R>, d, int(RO_RELAX_DRY), rk);
+    L.run(RG_STAG, k_tend<R>, d, rk);
+    if (lbc) L.run(RG_RING, k_ring<R>, d, int(RO_SPEC_DRY), rk);
+    if (rk == 1) L.copy_list(h->zeros_d, h->zeros_start_d, h->zeros.size(), h->zeros_total);
+    L.run(RG_COLS_STAG, k_ss_prep<R>, d, rk);
+    L.halo(cw_handle::H_SS0);
+    for (int it = 1; it <= ns; ++it) {
+      L.run(RG_MASS, k_uv<R>, d, rk);
+      if (lbc) L.run(RG_RING, k_ring<R>, d, int(RO_UPDATE_UV), rk);
+      L.halo(cw_handle::H_UV);
+      if (!lbc) {
+        L.run(RG_COLS_STAG, k_ac<R>, d, rk, it, ns, 7);
+      } else {
+        L.run(RG_COLS_STAG, k_ac<R>, d, rk, it, ns, 1);
+        L.run(RG_RING, k_ring<R>, d, int(RO_UPDATE_MU_T), rk);
+        L.run(RG_COLS_STAG, k_ac<R>, d, rk, it, ns, 2);
+        L.run(RG_RING, k_ring<R>, d, int(RO_UPDATE_PH_W), rk);
+        L.run(RG_MASS, k_wprho<R>, d);
+      }
+      L.halo(cw_handle::H_AC);
+    }
+    L.halo(cw_handle::H_POST);
+    L.run(RG_COLS_STAG, k_finish<R>, d, rk, ns);
+    L.halo(cw_handle::H_FIN);
+    if (scalars) {
+      if (rk == 1) L.run(RG_MASS, k_q_tendf_rk1<R>, d);
+      if (rk == 1 && lbc) L.run(RG_RING, k_ring<R>, d, int(RO_RELAX_Q), rk);
+      if (lbc) L.run(RG_RING, k_ring<R>, d, int(RO_SPEC_Q), rk);
+      L.run(RG_MASS, k_q_update<R>, d, rk);
+      if (rk == 3 && any_pd) {
+        L.run(RG_MASS, k_q_pre_pd<R>, d, rk);
+        L.halo(cw_handle::H_Q1PD);
+        L.run(RG_MASS, k_q_scale_pd<R>, d, rk);
+        L.halo(cw_handle::H_SCPD);
+        L.run(RG_MASS, k_q_update_pd<R>, d, rk);
+      }
+      k_q_swap<R><<<unsigned(h->m.size()), 64, 0, h->stream>>>(T.doms, int(h->m.size()));
+      L.check();
+      if (lbc) L.run(RG_RING, k_ring<R>, d, int(RO_FLOW_DEP), rk);
+      L.halo(cw_handle::H_Q2);
+    }
+  }
+  if (lbc) {
+    L.run(RG_RING, k_ring<R>, d, int(RO_FINAL), 3);
+    L.run(RG_MASS, k_p_rho_phi<R>, d, 1);
+    L.halo(cw_handle::H_END_P);
+  }
+  if (terrain) {
+    L.halo(cw_handle::H_WS0);
+    L.run(RG_COLS_MASS, k_w_surface<R>, d);
+    L.halo(cw_handle::H_WS1);
+  }
+}
+
+void enqueue(cw_handle* h, Launcher& L) {
+  if (h->precision == CW_FP64) enqueue_step<double>(h, L, h->t64);
+  else enqueue_step<float>(h, L, h->t32);
+}
+
+void invalidate_graph(cw_handle* h) {
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  h->gexec = nullptr;
+  h->graph = nullptr;
+  h->graph_ok = false;
+}
+
+void run_steps(cw_handle* h, int nsteps) {
+  h->launches_last = 0;
+  if (h->use_graph && !h->graph_ok) {
+    Launcher L{h};
+    CW_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      enqueue(h, L);
+    } catch (...) {
+      cudaGraph_t g;
+      cudaStreamEndCapture(h->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    CW_CUDA(cudaStreamEndCapture(h->stream, &h->graph));
+    CW_CUDA(cudaGraphInstantiate(&h->gexec, h->graph, 0));
+    h->graph_ok = true;
+    h->launches_step = L.count;
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    if (h->use_graph) {
+      CW_CUDA(cudaGraphLaunch(h->gexec, h->stream));
+      h->launches_last += h->launches_step;
+    } else {
+      Launcher L{h};
+      enqueue(h, L);
+      h->launches_step = L.count;
+      h->launches_last += L.count;
+    }
+    for (Member& M : h->m) {
+      if (M.o.lbc) M.dtbc += M.g.dt;
+      if (M.o.n_scalars > 0) M.q_parity ^= 1;  // three swaps per step
+    }
+  }
+}
+
+Member make_member(const cw_grid& g, const cw_options& o) {
+  if (const char* why = unsupported(g, o)) throw std::runtime_error(why);
+  Member M;
+  M.g = g;
+  M.o = o;
+  M.n_sound = sound_steps(g, o);
+  M.esz = o.precision == CW_MIXED ? 4 : 8;
+  return M;
+}
+
+void setup(cw_handle* h) {
+  allocate(h);
+  upload_tables(h);
+  build_blockmaps(h);
+  if (h->precision == CW_FP64) build_halosets_t<double>(h, h->t64);
+  else build_halosets_t<float>(h, h->t32);
+  build_copies(h);
+}
+
+// locate a field: allocation and layout
+struct Loc {
+  char* base;
+  cw_layout L;
+  int esz;
+};
+Loc locate(cw_handle* h, int mi, int field, int n) {
+  if (mi < 0 || mi >= int(h->m.size())) throw std::runtime_error("member index out of range");
+  Member& M = h->m[mi];
+  if (field >= 0 && field < CW_Q_1) return Loc{M.base[field], M.L[field], M.esz};
+  if (n < 0 || n >= M.o.n_scalars) throw std::runtime_error("scalar index out of range");
+  if (field == CW_Q_1) return Loc{M.q1[n], M.Lq, M.esz};
+  if (field == CW_Q_2) return Loc{M.q_parity ? M.qb[n] : M.qa[n], M.Lq, M.esz};
+  if (field == CW_Q_TENDF) return Loc{M.qtf[n], M.Lq, M.esz};
+  throw std::runtime_error("unknown field id");
+}
+
+void copy_in(cw_handle* h, const Loc& l, const double* host, size_t count) {
+  if (count != size_t(l.L.total)) throw std::runtime_error("count != layout.total");
+  if (l.esz == 8) {
+    CW_CUDA(cudaMemcpyAsync(l.base, host, count * 8, cudaMemcpyHostToDevice, h->stream));
+  } else {
+    std::vector<float> f(host, host + count);
+    CW_CUDA(cudaMemcpyAsync(l.base, f.data(), count * 4, cudaMemcpyHostToDevice, h->stream));
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+  }
+}
+void copy_out(cw_handle* h, const Loc& l, double* host, size_t count) {
+  if (count != size_t(l.L.total)) throw std::runtime_error("count != layout.total");
+  if (l.esz == 8) {
+    CW_CUDA(cudaMemcpyAsync(host, l.base, count * 8, cudaMemcpyDeviceToHost, h->stream));
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+  } else {
+    std::vector<float> f(count);
+    CW_CUDA(cudaMemcpyAsync(f.data(), l.base, count * 4, cudaMemcpyDeviceToHost, h->stream));
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+    for (size_t n = 0; n < count; ++n) host[n] = f[n];
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+int cw_create(const cw_grid* g, const cw_options* o, cw_handle** out) {
+  return guarded(nullptr, [&] {
+    if (!g || !o || !out) throw std::runtime_error("null argument");
+    auto h = std::make_unique<cw_handle>();
+    h->precision = o->precision;
+    h->m.push_back(make_member(*g, *o));
+    CW_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+    setup(h.get());
+    *out = h.release();
+    return 0;
+  });
+}
+
+int cw_batch_create(int n, const cw_grid* g, const cw_options* o, cw_handle** out) {
+  return guarded(nullptr, [&] {
+    if (n < 1 || n > kMaxMembers || !g || !o || !out) throw std::runtime_error("bad batch arguments");
+    auto h = std::make_unique<cw_handle>();
+    h->precision = o[0].precision;
+    for (int m = 0; m < n; ++m) {
+      if (o[m].precision != h->precision) throw std::runtime_error("batch members must share the precision");
+      h->m.push_back(make_member(g[m], o[m]));
+      if (h->m.back().n_sound != h->m[0].n_sound) throw std::runtime_error("batch members must share n_sound");
+    }
+    CW_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+    setup(h.get());
+    *out = h.release();
+    return 0;
+  });
+}
+
+int cw_destroy(cw_handle* h) {
+  if (!h) return 0;
+  cudaStreamSynchronize(h->stream);
+  invalidate_graph(h);
+  for (auto& s : h->hs) {
+    cudaFree(s.fd);
+    cudaFree(s.startd);
+  }
+  cudaFree(h->copies_d);
+  cudaFree(h->copies_start_d);
+  cudaFree(h->zeros_d);
+  cudaFree(h->zeros_start_d);
+  cudaFree(h->t64.doms);
+  cudaFree(h->t64.qtab);
+  cudaFree(h->t64.lbcq);
+  cudaFree(h->t32.doms);
+  cudaFree(h->t32.qtab);
+  cudaFree(h->t32.lbcq);
+  cudaFree(h->arena);
+  if (h->own_stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return 0;
+}
+
+int cw_members(cw_handle* h, int* out) {
+  if (!h || !out) return -1;
+  *out = int(h->m.size());
+  return 0;
+}
+
+int cw_member_set_vertical(cw_handle* h, int mi, const cw_vertical* v) {
+  return guarded(h, [&] {
+    if (!h || !v) throw std::runtime_error("null argument");
+    Member& M = h->m.at(size_t(mi));
+    const int nz = M.g.nz, stride = nz + 2;
+    std::vector<double> buf(24 * size_t(stride), 0.0);
+    auto put = [&](int slot, const double* src, int cnt) {
+      if (src) std::copy(src, src + cnt, buf.begin() + size_t(slot) * stride);
+    };
+    put(VA_ZNU, v->znu, nz); put(VA_ZNW, v->znw, nz + 1); put(VA_DNW, v->dnw, nz); put(VA_DN, v->dn, nz + 1);
+    put(VA_RDNW, v->rdnw, nz); put(VA_RDN, v->rdn, nz + 1); put(VA_FNM, v->fnm, nz + 1); put(VA_FNP, v->fnp, nz + 1);
+    put(VA_C1H, v->c1h, nz); put(VA_C2H, v->c2h, nz); put(VA_C1F, v->c1f, nz + 1); put(VA_C2F, v->c2f, nz + 1);
+    put(VA_UB, v->u_base, nz); put(VA_VB, v->v_base, nz);
+    if (M.o.lbc) {  // LateralBC::set_dt (src/dyn/lateral_bc.cpp:198-211): width 5, spec_zone 1, relax_zone 4
+      const int spec_zone = 1, relax_zone = 4;
+      for (int loop = spec_zone + 1; loop <= spec_zone + relax_zone; ++loop) {
+        const double num = double(spec_zone + relax_zone - loop), den = double(relax_zone - 1);
+        buf[size_t(VA_FCX) * stride + loop - 1] = 0.1 / M.g.dt * num / den;
+        buf[size_t(VA_GCX) * stride + loop - 1] = 1.0 / M.g.dt / 50.0 * num / den;
+      }
+    }
+    CW_CUDA(cudaMemcpyAsync(M.vert, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+    M.cf1 = v->cf1; M.cf2 = v->cf2; M.cf3 = v->cf3; M.cfn = v->cfn; M.cfn1 = v->cfn1; M.rdx = v->rdx; M.rdy = v->rdy;
+    M.g.p_top = v->p_top;
+    upload_tables(h);
+    invalidate_graph(h);
+    return 0;
+  });
+}
+int cw_set_vertical(cw_handle* h, const cw_vertical* v) { return cw_member_set_vertical(h, 0, v); }
+
+int cw_member_upload(cw_handle* h, int mi, int field, int n, const double* host, size_t count) {
+  return guarded(h, [&] {
+    if (!h || !host) throw std::runtime_error("null argument");
+    copy_in(h, locate(h, mi, field, n), host, count);
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+  });
+}
+int cw_upload(cw_handle* h, int field, int n, const double* host, size_t count) {
+  return cw_member_upload(h, 0, field, n, host, count);
+}
+int cw_member_download(cw_handle* h, int mi, int field, int n, double* host, size_t count) {
+  return guarded(h, [&] {
+    if (!h || !host) throw std::runtime_error("null argument");
+    copy_out(h, locate(h, mi, field, n), host, count);
+    return 0;
+  });
+}
+int cw_download(cw_handle* h, int field, int n, double* host, size_t count) {
+  return cw_member_download(h, 0, field, n, host, count);
+}
+int cw_member_field_layout(cw_handle* h, int mi, int field, int n, cw_layout* out) {
+  return guarded(h, [&] {
+    if (!h || !out) throw std::runtime_error("null argument");
+    *out = locate(h, mi, field, n).L;
+    return 0;
+  });
+}
+int cw_field_layout(cw_handle* h, int field, int n, cw_layout* out) { return cw_member_field_layout(h, 0, field, n, out); }
+int cw_field_device_ptr(cw_handle* h, int field, int n, void** out) {
+  return guarded(h, [&] {
+    if (!h || !out) throw std::runtime_error("null argument");
+    const Loc l = locate(h, 0, field, n);
+    *out = l.base + size_t(l.L.offset) * l.esz;
+    return 0;
+  });
+}
+
+int cw_member_set_lbc(cw_handle* h, int mi, int var, int side, const double* values, const double* tends, size_t count) {
+  return guarded(h, [&] {
+    if (!h || !values || !tends) throw std::runtime_error("null argument");
+    Member& M = h->m.at(size_t(mi));
+    if (!M.o.lbc) throw std::runtime_error("the handle has no lateral boundaries (lbc = 0)");
+    if (var < 0 || var > 4 || side < 0 || side > 3) throw std::runtime_error("bad boundary variable or side");
+    const size_t n = size_t(lbc_npos(M.g, var, side)) * lbc_nk(M.g, var) * kLbcWidth;
+    if (count != n) throw std::runtime_error("LateralBC::set: wrong slab size");
+    const Loc vl{M.slab[var] + M.slab_off[var][side] * M.esz, cw_layout{}, M.esz};
+    const Loc tl{M.slab[var] + M.slab_off[var][4 + side] * M.esz, cw_layout{}, M.esz};
+    for (const auto& [dst, src] : {std::pair{vl.base, values}, std::pair{tl.base, tends}}) {
+      if (M.esz == 8) {
+        CW_CUDA(cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyHostToDevice, h->stream));
+      } else {
+        std::vector<float> f(src, src + n);
+        CW_CUDA(cudaMemcpyAsync(dst, f.data(), n * 4, cudaMemcpyHostToDevice, h->stream));
+      }
+      CW_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    return 0;
+  });
+}
+int cw_set_lbc(cw_handle* h, int var, int side, const double* values, const double* tends, size_t count) {
+  return cw_member_set_lbc(h, 0, var, side, values, tends, count);
+}
+int cw_member_set_lbc_scalar(cw_handle* h, int mi, int n, int side, const double* values, const double* tends, size_t count) {
+  return guarded(h, [&] {
+    if (!h || !values || !tends) throw std::runtime_error("null argument");
+    Member& M = h->m.at(size_t(mi));
+    if (!M.o.lbc) throw std::runtime_error("the handle has no lateral boundaries (lbc = 0)");
+    if (n < 0 || n >= M.o.n_scalars || side < 0 || side > 3) throw std::runtime_error("bad scalar or side");
+    const size_t cnt = size_t(side < 2 ? M.g.ny : M.g.nx) * M.g.nz * kLbcWidth;
+    if (count != cnt) throw std::runtime_error("LateralBC::set_scalar: wrong slab size");
+    for (int half = 0; half < 2; ++half) {
+      char* dst = M.qslab[n] + M.qslab_off[n][half * 4 + side] * M.esz;
+      const double* src = half ? tends : values;
+      if (M.esz == 8) {
+        CW_CUDA(cudaMemcpyAsync(dst, src, cnt * 8, cudaMemcpyHostToDevice, h->stream));
+      } else {
+        std::vector<float> f(src, src + cnt);
+        CW_CUDA(cudaMemcpyAsync(dst, f.data(), cnt * 4, cudaMemcpyHostToDevice, h->stream));
+      }
+      CW_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    if (!M.q_have[n]) {
+      M.q_have[n] = 1;
+      upload_tables(h);
+      invalidate_graph(h);
+    }
+    return 0;
+  });
+}
+int cw_set_lbc_scalar(cw_handle* h, int n, int side, const double* values, const double* tends, size_t count) {
+  return cw_member_set_lbc_scalar(h, 0, n, side, values, tends, count);
+}
+int cw_member_set_lbc_time(cw_handle* h, int mi, double dtbc) {
+  return guarded(h, [&] {
+    h->m.at(size_t(mi)).dtbc = dtbc;
+    upload_tables(h);
+    return 0;
+  });
+}
+int cw_set_lbc_time(cw_handle* h, double dtbc) { return cw_member_set_lbc_time(h, 0, dtbc); }
+
+int cw_step(cw_handle* h, int nsteps) {
+  return guarded(h, [&] {
+    if (!h || nsteps < 0) throw std::runtime_error("bad arguments");
+    run_steps(h, nsteps);
+    return 0;
+  });
+}
+int cw_set_dt(cw_handle* h, double dt, int n_sound) {
+  return guarded(h, [&] {
+    if (n_sound < 2 || n_sound % 2) throw std::runtime_error("time_step_sound must be even and >= 2");
+    for (Member& M : h->m) {
+      M.g.dt = dt;
+      M.n_sound = n_sound;
+    }
+    upload_tables(h);
+    invalidate_graph(h);
+    return 0;
+  });
+}
+int cw_n_sound(cw_handle* h, int* out) {
+  if (!h || !out) return -1;
+  *out = h->m[0].n_sound;
+  return 0;
+}
+int cw_set_stream(cw_handle* h, void* stream) {
+  return guarded(h, [&] {
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    if (stream) {
+      h->stream = static_cast<cudaStream_t>(stream);
+      h->own_stream = false;
+    } else {
+      CW_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+      h->own_stream = true;
+    }
+    return 0;
+  });
+}
+int cw_sync(cw_handle* h) {
+  return guarded(h, [&] {
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+    CW_CUDA(cudaGetLastError());
+    return 0;
+  });
+}
+const char* cw_last_error(cw_handle* h) { return h ? h->err.c_str() : g_create_err.c_str(); }
+int cw_launch_count(cw_handle* h, long long* out) {
+  if (!h || !out) return -1;
+  *out = h->launches_last;
+  return 0;
+}
+int cw_set_graph(cw_handle* h, int on) {
+  if (!h) return -1;
+  h->use_graph = on != 0;
+  invalidate_graph(h);
+  return 0;
+}
+
+// FieldT::fill_host for every field of a case, plus the vertical arrays and the boundary slabs
+int cw_member_upload_case(cw_handle* h, int mi, cw_case* c) {
+  if (!h || !c) return -1;
+  cw_vertical v{};
+  if (cw_case_vertical(c, &v) != 0) return -1;
+  int rc = cw_member_set_vertical(h, mi, &v);
+  if (rc) return rc;
+  const Member& M = h->m.at(size_t(mi));
+  for (int id = 0; id < CW_Q_1; ++id) {
+    double* data = nullptr;
+    cw_layout L{};
+    cw_case_field(c, id, 0, &data, &L);
+    rc = cw_member_upload(h, mi, id, 0, data, size_t(L.total));
+    if (rc) return rc;
+  }
+  for (int n = 0; n < M.o.n_scalars; ++n)
+    for (int id : {CW_Q_1, CW_Q_2, CW_Q_TENDF}) {
+      double* data = nullptr;
+      cw_layout L{};
+      cw_case_field(c, id, n, &data, &L);
+      rc = cw_member_upload(h, mi, id, n, data, size_t(L.total));
+      if (rc) return rc;
+    }
+  if (M.o.lbc) {
+    for (int var = 0; var < 5; ++var)
+      for (int side = 0; side < 4; ++side) {
+        double *vals = nullptr, *tends = nullptr;
+        size_t cnt = 0;
+        cw_case_lbc(c, 0, var, side, &vals, &tends, &cnt);
+        rc = cw_member_set_lbc(h, mi, var, side, vals, tends, cnt);
+        if (rc) return rc;
+      }
+    for (int n = 0; n < M.o.n_scalars; ++n)
+      for (int side = 0; side < 4; ++side) {
+        double *vals = nullptr, *tends = nullptr;
+        size_t cnt = 0;
+        if (cw_case_lbc(c, 1, n, side, &vals, &tends, &cnt) != 0) continue;
+        rc = cw_member_set_lbc_scalar(h, mi, n, side, vals, tends, cnt);
+        if (rc) return rc;
+      }
+    double dtbc = 0;
+    cw_case_lbc_time(c, &dtbc);
+    rc = cw_member_set_lbc_time(h, mi, dtbc);
+  }
+  return rc;
+}
+int cw_upload_case(cw_handle* h, cw_case* c) { return cw_member_upload_case(h, 0, c); }
+
+}  // extern "C"

@@ -1,0 +1,173 @@
+// SPDX-License-Identifier: GPL-3.0-or-later
+// Device-side data model of the dycore: one Dom per domain (a member of a batch), views in CPPWRF's
+// field layout, the launch geometry shared by every kernel, and the WRF flux statement functions.
+//
+// Every kernel takes a device array of Dom and a BlockMap: block b of a launch belongs to member
+// m = the last index with start[m] <= b, so one launch covers all members of a batch whatever their
+// sizes (a single domain is a batch of one).
+#pragma once
+
+#include <cstdint>
+
+#include "cw_pow.h"
+
+namespace cw {
+
+constexpr int kMaxMembers = 256;
+constexpr int kMaxScalars = 64;
+
+template <class T>
+struct V3 {  // View3 of CPPWRF (src/core/field.hpp:19-23): element (0,0,0), 32-bit strides
+  T* p;
+  int sj, sk;
+  __device__ __forceinline__ T& operator()(int i, int j, int k) const { return p[i + j * sj + k * sk]; }
+};
+template <class T>
+struct VB {  // BView3 / BView2 (field.hpp:35-44): si = sj = 0 for horizontally uniform storage
+  const T* p;
+  int si, sj, sk;
+  __device__ __forceinline__ T operator()(int i, int j, int k) const { return p[i * si + j * sj + k * sk]; }
+  __device__ __forceinline__ T operator()(int i, int j) const { return p[i * si + j * sj]; }
+};
+
+// Lateral boundary slabs of one variable: 4 sides of values then 4 of tendencies, (pos, k, b) pos fastest
+template <class T>
+struct Slabs {
+  const T* v[4];
+  const T* t[4];
+  int npos[4];
+  int nk;
+  int have;
+};
+
+template <class T>
+struct Dom {
+  // grid and options
+  int nx, ny, nz, nyv, two_d, do_y;
+  int bc_x, bc_y, spec_x, spec_y;  // spec_*: specified in that direction (degraded orders, spec zone)
+  int lbc, flat, n_moist, n_scalars, diff_on, top_lid, w_damping, n_sound, moist_adv_opt, scalar_adv_opt;
+  double dt, epssm, smdiv, emdiv, khdif, kvdif, prandtl, hup, vup, w_crit_cfl, dtbc;
+  double rdx, rdy, cf1, cf2, cf3, cfn, cfn1;
+  const double *znu, *znw, *dnw, *dn, *rdnw, *rdn, *fnm, *fnp, *c1h, *c2h, *c1f, *c2f, *u_base, *v_base;
+  const double *fcx, *gcx;  // relaxation weights per row (LateralBC::set_dt)
+  // State
+  V3<T> u1, u2, v1, v2, w1, w2, t1, t2, ph1, ph2, mu1, mu2, p, al, alt, php, ww, mut, muu, muv, muts, muus, muvs,
+      ru, rv, rw, ru_m, rv_m, ww_m, cqu, cqv, cqw, hd;
+  // Tendencies
+  V3<T> ru_tend, rv_tend, rw_tend, t_tend, ph_tend, mu_tend, ru_tendf, rv_tendf, rw_tendf, t_tendf, ph_tendf;
+  // BaseState
+  VB<T> mub, pb, alb, t_init, qv_base, phb, ht, msftx, msfty, msfux, msfuy, msfvx, msfvy, msfvx_inv;
+  // acoustic-step work fields (SmallStep, src/dyn/small_step.hpp:45-49)
+  V3<T> u_save, v_save, w_save, t_save, ph_save, ww1, c2a, pm1, t_2save, a, alpha, gamma, mu_save, mudf, muave,
+      w_rhs, t2a;
+  // scalars: device tables of views (q2 and q_new swap roles after each update)
+  V3<T>* q1;
+  V3<T>* q2;
+  V3<T>* qn;
+  V3<T>* qtf;
+  V3<T>* qscale;
+  // boundary slabs: U V T PH MU, then scalars (n_scalars entries)
+  Slabs<T> lbc_var[5];
+  Slabs<T>* lbc_q;
+};
+
+struct BlockMap {
+  int n;
+  int start[kMaxMembers + 1];
+};
+
+__device__ __forceinline__ int member_of(const BlockMap& bm, int b) {
+  int lo = 0, hi = bm.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (bm.start[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Block geometry of the two launch shapes. Point kernels: PX x PY threads over (i, j), blockIdx over
+// (i-tiles, j-tiles, k) of a member; column kernels: one thread per column, CX x CY columns per block.
+constexpr int PX = 128, PY = 1;
+constexpr int CX = 64, CY = 1;
+__host__ __device__ __forceinline__ int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+// ---- WRF flux statement functions (src/dyn/kernels_common.hpp:11-105) ----
+template <class R>
+__device__ __forceinline__ R sgn1(R a) {
+  return a >= R(0) ? R(1) : R(-1);
+}
+template <class R>
+__device__ __forceinline__ R flux5(R qm3, R qm2, R qm1, R q0, R qp1, R qp2, R ua, R up) {
+  return (R(37) * (q0 + qm1) - R(8) * (qp1 + qm2) + (qp2 + qm3)) / R(60) -
+         up * sgn1(ua) * ((qp2 - qm3) - R(5) * (qp1 - qm2) + R(10) * (q0 - qm1)) / R(60);
+}
+template <class R>
+__device__ __forceinline__ R flux3(R qm2, R qm1, R q0, R qp1, R ua, R up) {
+  return (R(7) * (q0 + qm1) - (qp1 + qm2)) / R(12) + up * sgn1(ua) * ((qp1 - qm2) - R(3) * (q0 - qm1)) / R(12);
+}
+template <class R>
+__device__ __forceinline__ R flux5_pd(R qm3, R qm2, R qm1, R q0, R qp1, R qp2, R ua, R up) {
+  const R f6 = (R(37.) / R(60.)) * (q0 + qm1) - (R(2.) / R(15.)) * (qp1 + qm2) + (R(1.) / R(60.)) * (qp2 + qm3);
+  return f6 - up * sgn1(ua) * (R(1.) / R(60.)) * ((qp2 - qm3) - R(5.) * (qp1 - qm2) + R(10.) * (q0 - qm1));
+}
+template <class R>
+__device__ __forceinline__ R flux3_pd(R qm2, R qm1, R q0, R qp1, R ua, R up) {
+  const R f4 = (R(7.) / R(12.)) * (q0 + qm1) - (R(1.) / R(12.)) * (qp1 + qm2);
+  return f4 + up * sgn1(ua) * (R(1.) / R(12.)) * ((qp1 - qm2) - R(3.) * (q0 - qm1));
+}
+__device__ __forceinline__ int ord_face(int f, int n, int on) {
+  if (!on) return 5;
+  if (f <= 1 || f >= n - 1) return 2;
+  if (f == 2 || f == n - 2) return 3;
+  return 5;
+}
+__device__ __forceinline__ int ord_mass(int f, int n, int on) {
+  if (!on) return 5;
+  if (f <= 1 || f >= n) return 2;
+  if (f == 2 || f == n - 1) return 3;
+  return 5;
+}
+template <class R>
+__device__ __forceinline__ R flux_upwind(R qm1, R q0, R cr) {
+  const R a = cr < R(0) ? -cr : cr;
+  const R lo = cr + a, hi = cr - a;
+  return R(0.5) * (lo < R(1) ? lo : R(1)) * qm1 + R(0.5) * (hi > R(-1) ? hi : R(-1)) * q0;
+}
+
+// physical constants (src/core/constants.hpp:4-18)
+namespace k {
+constexpr double g = 9.81;
+constexpr double r_d = 287.0;
+constexpr double cp = 7.0 * r_d / 2.0;
+constexpr double cpovcv = cp / (cp - r_d);
+constexpr double p1000mb = 100000.0;
+constexpr double t0 = 300.0;
+constexpr double reradius = 1. / 6370.0e03;
+}  // namespace k
+
+// ---- halo fill descriptors (HaloLine, src/core/halo.cpp:52-88) ----
+// One descriptor per field of a fill point; a launch covers every field of every member. Each thread
+// writes one halo cell with its final value, composed from interior sources (x then y, as fill_impl
+// orders the passes). The only in-place update, the wall face of an OddFace field (muu on symmetric
+// x walls), is done by a second launch (pass 1) after every y cell has read the unflipped face.
+struct HaloField {
+  void* p;       // element (0,0,0) (double or float)
+  void* ind;     // non-null: a device V3 whose .p is read at run time (scalars that swap buffers)
+  int sj, sk;
+  int lnx, lny, nk;  // logical extents (staggered) and levels
+  int wi0, wi1, wj0, wj1;
+  int gnx, gny;      // the member's mass-point extents
+  unsigned char periodic_x, periodic_y, flat_x, flat_y, two_d, face_x, face_y, odd_x, odd_y, oddface_x, is_float,
+      pad;
+  long long ncell_x, ncell;  // x-pass cells, all cells
+};
+struct HaloSet {
+  const HaloField* f;       // device array
+  const long long* start;   // device prefix sums of ncell (nf + 1 entries)
+  int nf;
+  long long total;
+  int has_oddface;
+};
+
+}  // namespace cw

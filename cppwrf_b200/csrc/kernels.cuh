@@ -1,0 +1,1015 @@
+// SPDX-License-Identifier: GPL-3.0-or-later
+// The dycore's kernels, templated on the arithmetic type R (double: the plain FP64 form, compiled with
+// --fmad=false so every expression rounds exactly as the reference's CPU build; float: the bulk of the
+// mixed form, whose column sums, tridiagonal solve and p'' integration stay in double).
+//
+// Each point formula restates the reference functor named beside it (src/dyn/*.cpp of CPPWRF) with the
+// same statement and summation order. The launch structure is this library's own: per RK stage one
+// column kernel for rk_step_prep, one point kernel for all five rk_tendency fields, one column kernel
+// for small_step_prep + calc_p_rho + calc_coef_w; per acoustic substep one point kernel (advance_uv)
+// and one column kernel (advance_mu_t + sumflux + advance_w + calc_p_rho); one column kernel for
+// small_step_finish + calc_p_rho_phi; halo refreshes at the reference's refresh points, batched.
+#pragma once
+
+#include "dycore.cuh"
+
+namespace cw {
+
+// ------------------------------------------------------------------ launch geometry
+enum RangeKind {
+  RG_STAG = 0,    // (i, j, k) in [0, nx+1) x [0, nyv) x [0, nz+1)
+  RG_MASS = 1,    // [0, nx) x [0, ny) x [0, nz)
+  RG_COLS_STAG,   // columns [0, nx+1) x [0, nyv)
+  RG_COLS_MASS,   // columns [0, nx) x [0, ny)
+  RG_RING,        // boundary ring: pos in [0, max(nx, ny)+1), k in [0, nz+1), 4 sides x 4 rows
+  RG_MASS_W,      // [0, nx) x [0, ny) x [0, nz+1)
+};
+struct Range {
+  int i0, i1, j0, j1, k0, k1;
+};
+__host__ __device__ __forceinline__ Range range_of(int kind, int nx, int ny, int nz, int nyv) {
+  switch (kind) {
+    case RG_STAG: return {0, nx + 1, 0, nyv, 0, nz + 1};
+    case RG_MASS: return {0, nx, 0, ny, 0, nz};
+    case RG_COLS_STAG: return {0, nx + 1, 0, nyv, 0, 1};
+    case RG_COLS_MASS: return {0, nx, 0, ny, 0, 1};
+    case RG_RING: return {0, (nx > ny ? nx : ny) + 1, 0, nz + 1, 0, 16};
+    default: return {0, nx, 0, ny, 0, nz + 1};
+  }
+}
+__host__ __device__ __forceinline__ bool is_column(int kind) { return kind == RG_COLS_STAG || kind == RG_COLS_MASS; }
+__host__ __device__ __forceinline__ int blocks_of(int kind, int nx, int ny, int nz, int nyv) {
+  const Range r = range_of(kind, nx, ny, nz, nyv);
+  const int tx = is_column(kind) ? CX : PX;
+  return cdiv(r.i1 - r.i0, tx) * (r.j1 - r.j0) * (r.k1 - r.k0);
+}
+// thread -> (member, i, j, k); false for the threads past the range
+template <class R>
+__device__ __forceinline__ bool thread_index(const Dom<R>* __restrict__ doms, const BlockMap& bm, int kind,
+                                             const Dom<R>*& Dp, int& i, int& j, int& k) {
+  const int b = blockIdx.x;
+  const int m = member_of(bm, b);
+  const Dom<R>& D = doms[m];
+  Dp = &D;
+  const Range r = range_of(kind, D.nx, D.ny, D.nz, D.nyv);
+  const int tx = is_column(kind) ? CX : PX;
+  const int bx = cdiv(r.i1 - r.i0, tx), by = r.j1 - r.j0;
+  int local = b - bm.start[m];
+  const int bi = local % bx;
+  local /= bx;
+  j = r.j0 + local % by;
+  k = r.k0 + local / by;
+  i = r.i0 + bi * tx + int(threadIdx.x);
+  return i < r.i1;
+}
+
+// ------------------------------------------------------------------ copies and halos
+struct CopyDesc {
+  void* dst;
+  const void* src;               // nullptr (and src_ind nullptr): write zeros
+  const void* const* src_ind;    // non-null: the source is *src_ind - ind_offset elements (a swapped buffer)
+  long long n;                   // elements
+  int is_float;
+  long long ind_offset;
+};
+static __global__ void k_copy(const CopyDesc* __restrict__ d, int nd, const long long* __restrict__ start) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= start[nd]) return;
+  int lo = 0, hi = nd - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (start[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  const long long e = t - start[lo];
+  const CopyDesc& c = d[lo];
+  if (c.is_float) {
+    const float* src = c.src_ind ? static_cast<const float*>(*c.src_ind) - c.ind_offset : static_cast<const float*>(c.src);
+    static_cast<float*>(c.dst)[e] = src ? src[e] : 0.0f;
+  } else {
+    const double* src = c.src_ind ? static_cast<const double*>(*c.src_ind) - c.ind_offset : static_cast<const double*>(c.src);
+    static_cast<double*>(c.dst)[e] = src ? src[e] : 0.0;
+  }
+}
+
+// HaloLine's source index of halo position i along a direction of n mass points (-1: keep in place)
+__device__ __forceinline__ int halo_src(int i, int n, int face, int periodic, int flat) {
+  if (flat) {
+    const int last = face ? n : n - 1;
+    return i < 0 ? 0 : (i > last ? last : i);
+  }
+  if (periodic) return ((i % n) + n) % n;
+  if (face) return i <= 0 ? -i : 2 * n - i;
+  return i < 0 ? -1 - i : 2 * n - 1 - i;
+}
+// the slot positions of HaloLine: face fields 0,-1,-2,-3 and n..n+3; others -1,-2,-3 and n..n+2
+__device__ __forceinline__ int halo_pos(int a, int n, int face) {
+  const int nl = face ? 4 : 3;
+  return a < nl ? (face ? -a : -1 - a) : n + (a - nl);
+}
+__device__ __forceinline__ bool is_xslot(int i, int n, int face) { return face ? (i <= 0 || i >= n) : (i < 0 || i >= n); }
+
+template <class T>
+__device__ __forceinline__ T halo_xval(const HaloField& f, T* p, int i, int j, int k) {
+  // the value of (i, j) after the x pass (j an interior row)
+  if (!is_xslot(i, f.gnx, f.face_x) || i < f.wi0 || i >= f.wi1) return p[i + j * f.sj + k * f.sk];
+  const int src = halo_src(i, f.gnx, f.face_x, f.periodic_x, f.flat_x);
+  const T v = p[src + j * f.sj + k * f.sk];
+  if (!f.periodic_x && !f.flat_x && src == i) return f.oddface_x ? T(-v) : v;
+  return (!f.periodic_x && !f.flat_x && f.odd_x) ? T(-v) : v;
+}
+
+template <class T>
+__device__ __forceinline__ void halo_cell(const HaloField& f, long long c, int pass) {
+  T* p = static_cast<T*>(f.ind ? static_cast<V3<T>*>(f.ind)->p : f.p);
+  if (c < f.ncell_x) {  // x pass: (k, row j, slot a)
+    const int na = f.face_x ? 8 : 6;
+    const int a = int(c % na);
+    const long long r = c / na;
+    const int j = int(r % f.lny), k = int(r / f.lny);
+    const int i = halo_pos(a, f.gnx, f.face_x);
+    if (i < f.wi0 || i >= f.wi1) return;
+    const int src = halo_src(i, f.gnx, f.face_x, f.periodic_x, f.flat_x);
+    if (!f.periodic_x && !f.flat_x && src == i) {  // wall face: kept, or flipped by pass 1 (OddFace)
+      if (pass == 1 && f.oddface_x) p[i + j * f.sj + k * f.sk] = -p[i + j * f.sj + k * f.sk];
+      return;
+    }
+    if (pass == 1) return;
+    T v = p[src + j * f.sj + k * f.sk];
+    if (!f.periodic_x && !f.flat_x && f.odd_x) v = -v;
+    p[i + j * f.sj + k * f.sk] = v;
+    return;
+  }
+  if (pass == 1) return;
+  // y pass: (k, slot b, column i over the full x extent)
+  const long long cy = c - f.ncell_x;
+  const int wiw = f.wi1 - f.wi0;
+  const int na = f.face_y ? 8 : 6;
+  const int i = f.wi0 + int(cy % wiw);
+  const long long r = cy / wiw;
+  const int b = int(r % na), k = int(r / na);
+  const int jh = halo_pos(b, f.gny, f.face_y);
+  if (jh < f.wj0 || jh >= f.wj1) return;
+  const int src = halo_src(jh, f.gny, f.face_y, f.periodic_y, f.flat_y);
+  if (!f.periodic_y && !f.flat_y && src == jh) return;  // kept (no OddFace in y)
+  T v = halo_xval<T>(f, p, i, src, k);
+  if (!f.periodic_y && !f.flat_y && f.odd_y) v = -v;
+  p[i + jh * f.sj + k * f.sk] = v;
+}
+
+static __global__ void k_halo(HaloSet s, int pass) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= s.total) return;
+  int lo = 0, hi = s.nf - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (s.start[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  const HaloField& f = s.f[lo];
+  const long long c = t - s.start[lo];
+  if (f.is_float) halo_cell<float>(f, c, pass);
+  else halo_cell<double>(f, c, pass);
+}
+
+// ------------------------------------------------------------------ rk_step_prep
+// KMu (large_step.cpp:49-66), KPrep3 (:68-81), KWW (:83-108), KCq (:127-148), per column (i, j) of
+// [0, nx] x [0, nyv): every value a column thread writes depends only on its own column and on halo
+// values that the preceding refresh made current.
+template <class R>
+__device__ __forceinline__ R ww_mu_u(const Dom<R>& D, int i, int j) {
+  return R(0.5) * (D.mu2(i, j, 0) + D.mub(i, j) + D.mu2(i - 1, j, 0) + D.mub(i - 1, j));
+}
+template <class R>
+__device__ __forceinline__ R ww_mu_v(const Dom<R>& D, int i, int j) {
+  return R(0.5) * (D.mu2(i, j, 0) + D.mub(i, j) + D.mu2(i, j - 1, 0) + D.mub(i, j - 1));
+}
+template <class R>
+__device__ __forceinline__ R ww_divv(const Dom<R>& D, int i, int j, int k, R mu1, R mu0, R mv1, R mv0) {
+  const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
+  return D.msftx(i, j) * R(D.dnw[k]) *
+         (R(D.rdx) * ((c1h * mu1 + c2h) * D.u2(i + 1, j, k) / D.msfuy(i + 1, j) - (c1h * mu0 + c2h) * D.u2(i, j, k) / D.msfuy(i, j)) +
+          R(D.rdy) * ((c1h * mv1 + c2h) * D.v2(i, j + 1, k) * D.msfvx_inv(i, j + 1) -
+                      (c1h * mv0 + c2h) * D.v2(i, j, k) * D.msfvx_inv(i, j)));
+}
+
+template <class R>
+__global__ void __launch_bounds__(CX) k_ls_prep(const Dom<R>* __restrict__ doms, BlockMap bm) {
+  const Dom<R>* Dp;
+  int i, j, k0;
+  if (!thread_index(doms, bm, RG_COLS_STAG, Dp, i, j, k0)) return;
+  const Dom<R>& D = *Dp;
+  const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
+  const int spx = D.spec_x, spy = D.spec_y;
+  // KMu
+  R muu = 0, muv = 0, mut = 0;
+  if (i < nx && j < ny) {
+    mut = D.mu2(i, j, 0) + D.mub(i, j);
+    D.mut(i, j, 0) = mut;
+  }
+  if (j < ny) {
+    if (spx && i == 0) muu = R(0.5) * (D.mu2(0, j, 0) + D.mu2(0, j, 0) + D.mub(0, j) + D.mub(0, j));
+    else if (spx && i == nx)
+      muu = R(0.5) * (D.mu2(nx - 1, j, 0) + D.mu2(nx - 1, j, 0) + D.mub(nx - 1, j) + D.mub(nx - 1, j));
+    else muu = R(0.5) * (D.mu2(i, j, 0) + D.mu2(i - 1, j, 0) + D.mub(i, j) + D.mub(i - 1, j));
+    D.muu(i, j, 0) = muu;
+  }
+  if (i < nx && j < nyv) {
+    if (spy && j == 0) muv = R(0.5) * (D.mu2(i, 0, 0) + D.mu2(i, 0, 0) + D.mub(i, 0) + D.mub(i, 0));
+    else if (spy && j == ny)
+      muv = R(0.5) * (D.mu2(i, ny - 1, 0) + D.mu2(i, ny - 1, 0) + D.mub(i, ny - 1) + D.mub(i, ny - 1));
+    else muv = R(0.5) * (D.mu2(i, j, 0) + D.mu2(i, j - 1, 0) + D.mub(i, j) + D.mub(i, j - 1));
+    D.muv(i, j, 0) = muv;
+  }
+  // KPrep3
+  for (int k = 0; k < nz + 1; ++k) {
+    if (j < ny && k < nz) D.ru(i, j, k) = D.u2(i, j, k) * (R(D.c1h[k]) * muu + R(D.c2h[k])) / D.msfuy(i, j);
+    if (i < nx && j < nyv && k < nz) D.rv(i, j, k) = D.v2(i, j, k) * (R(D.c1h[k]) * muv + R(D.c2h[k])) * D.msfvx_inv(i, j);
+    if (i < nx && j < ny) D.rw(i, j, k) = D.w2(i, j, k) * (R(D.c1f[k]) * mut + R(D.c2f[k])) / D.msfty(i, j);
+    if (i < nx && j < ny && k < nz) {
+      D.alt(i, j, k) = D.al(i, j, k) + D.alb(i, j, k);
+      D.php(i, j, k) = R(0.5) * (D.phb(i, j, k) + D.phb(i, j, k + 1) + D.ph2(i, j, k) + D.ph2(i, j, k + 1));
+    }
+  }
+  // KWW (columns of the mass points)
+  if (i < nx && j < ny) {
+    const R mu1 = ww_mu_u(D, i + 1, j), mu0 = ww_mu_u(D, i, j), mv1 = ww_mu_v(D, i, j + 1), mv0 = ww_mu_v(D, i, j);
+    R dmdt = 0;
+    for (int k = 0; k < nz; ++k) dmdt += ww_divv(D, i, j, k, mu1, mu0, mv1, mv0);
+    R w = 0;
+    D.ww(i, j, 0) = 0;
+    for (int k = 1; k < nz; ++k) {
+      w = w - R(D.dnw[k - 1]) * R(D.c1h[k - 1]) * dmdt - ww_divv(D, i, j, k - 1, mu1, mu0, mv1, mv0);
+      D.ww(i, j, k) = w;
+    }
+    D.ww(i, j, nz) = 0;
+  }
+  // KCq
+  if (D.n_moist > 0) {
+    for (int k = 0; k < nz; ++k) {
+      if (j < ny) {
+        R t = 0;
+        for (int s = 0; s < D.n_moist; ++s) t = t + D.q2[s](i, j, k) + D.q2[s](i - 1, j, k);
+        D.cqu(i, j, k) = R(1) / (R(1) + R(0.5) * t);
+      }
+      if (i < nx && j < nyv) {
+        R t = 0;
+        for (int s = 0; s < D.n_moist; ++s) t = t + D.q2[s](i, j, k) + D.q2[s](i, j - 1, k);
+        D.cqv(i, j, k) = R(1) / (R(1) + R(0.5) * t);
+      }
+      if (i < nx && j < ny && k >= 1) {
+        R t = 0;
+        for (int s = 0; s < D.n_moist; ++s) t = t + D.q2[s](i, j, k) + D.q2[s](i, j, k - 1);
+        D.cqw(i, j, k) = R(0.5) * t;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ rk_tendency
+template <class R>
+__device__ __forceinline__ R cqu_(const Dom<R>& D, int i, int j, int k) { return D.n_moist > 0 ? D.cqu(i, j, k) : R(1); }
+template <class R>
+__device__ __forceinline__ R cqv_(const Dom<R>& D, int i, int j, int k) { return D.n_moist > 0 ? D.cqv(i, j, k) : R(1); }
+template <class R>
+__device__ __forceinline__ R cqw_(const Dom<R>& D, int i, int j, int k) { return D.n_moist > 0 ? D.cqw(i, j, k) : R(0); }
+
+// KTendU (large_step.cpp:152-264), no open boundaries, no Coriolis, unmapped
+template <class R>
+__device__ R tu_fx(const Dom<R>& D, int i, int j, int k) {
+  const int o = ord_mass(i, D.nx, D.spec_x);
+  if (o == 2) {
+    if (i <= 1) {
+      const R ub = (D.spec_x && D.u2(i, j, k) < R(0)) ? D.u2(i, j, k) : D.u2(i - 1, j, k);
+      return R(0.25) * (D.ru(i, j, k) + D.ru(i - 1, j, k)) * (D.u2(i, j, k) + ub);
+    }
+    const R ub = (D.spec_x && D.u2(i - 1, j, k) > R(0)) ? D.u2(i - 1, j, k) : D.u2(i, j, k);
+    return R(0.25) * (D.ru(i, j, k) + D.ru(i - 1, j, k)) * (D.u2(i - 1, j, k) + ub);
+  }
+  const R vel = R(0.5) * (D.ru(i, j, k) + D.ru(i - 1, j, k));
+  if (o == 3) return vel * flux3(D.u2(i - 2, j, k), D.u2(i - 1, j, k), D.u2(i, j, k), D.u2(i + 1, j, k), vel, R(D.hup));
+  return vel * flux5(D.u2(i - 3, j, k), D.u2(i - 2, j, k), D.u2(i - 1, j, k), D.u2(i, j, k), D.u2(i + 1, j, k),
+                     D.u2(i + 2, j, k), vel, R(D.hup));
+}
+template <class R>
+__device__ R tu_fy(const Dom<R>& D, int i, int j, int k) {
+  const int o = ord_face(j, D.ny, D.spec_y);
+  if (o == 2) return R(0.25) * (D.rv(i, j, k) + D.rv(i - 1, j, k)) * (D.u2(i, j, k) + D.u2(i, j - 1, k));
+  const R vel = R(0.5) * (D.rv(i, j, k) + D.rv(i - 1, j, k));
+  if (o == 3) return vel * flux3(D.u2(i, j - 2, k), D.u2(i, j - 1, k), D.u2(i, j, k), D.u2(i, j + 1, k), vel, R(D.hup));
+  return vel * flux5(D.u2(i, j - 3, k), D.u2(i, j - 2, k), D.u2(i, j - 1, k), D.u2(i, j, k), D.u2(i, j + 1, k),
+                     D.u2(i, j + 2, k), vel, R(D.hup));
+}
+template <class R>
+__device__ R tu_fz(const Dom<R>& D, int i, int j, int k) {
+  if (k == 0 || k == D.nz) return 0;
+  const R vel = R(0.5) * (D.ww(i - 1, j, k) + D.ww(i, j, k));
+  if (k == 1 || k == D.nz - 1) return vel * (R(D.fnm[k]) * D.u2(i, j, k) + R(D.fnp[k]) * D.u2(i, j, k - 1));
+  return vel * flux3(D.u2(i, j, k - 2), D.u2(i, j, k - 1), D.u2(i, j, k), D.u2(i, j, k + 1), -vel, R(D.vup));
+}
+template <class R, int DI, int DJ>
+__device__ __forceinline__ R pgf_dpn(const Dom<R>& D, int i, int j, int k) {  // p' at w level k, face column
+  auto ps = [&](int kk) { return D.p(i - DI, j - DJ, kk) + D.p(i, j, kk); };
+  const int nz = D.nz;
+  if (k == 0) return R(0.5) * (R(D.cf1) * ps(0) + R(D.cf2) * ps(1) + R(D.cf3) * ps(2));
+  if (k == nz) return D.top_lid ? R(0.5) * (R(D.cfn) * ps(nz - 1) + R(D.cfn1) * ps(nz - 2)) : R(0);
+  return R(0.5) * (R(D.fnm[k]) * ps(k) + R(D.fnp[k]) * ps(k - 1));
+}
+template <class R>
+__device__ R tend_u(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
+  const R rdx = R(D.rdx), rdy = R(D.rdy);
+  const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
+  R t = -(D.msfux(i, j) * rdx) * (tu_fx(D, i + 1, j, k) - tu_fx(D, i, j, k));
+  if (D.do_y) t -= (D.msfux(i, j) * rdy) * (tu_fy(D, i, j + 1, k) - tu_fy(D, i, j, k));
+  t -= R(D.rdnw[k]) * (tu_fz(D, i, j, k + 1) - tu_fz(D, i, j, k));
+  const R rm = D.msfux(i, j) / D.msfuy(i, j);
+  R dpx = rm * R(0.5) * rdx * (c1h * D.muu(i, j, 0) + c2h) *
+          ((D.ph2(i, j, k + 1) - D.ph2(i - 1, j, k + 1) + D.ph2(i, j, k) - D.ph2(i - 1, j, k)) +
+           (D.alt(i, j, k) + D.alt(i - 1, j, k)) * (D.p(i, j, k) - D.p(i - 1, j, k)) +
+           (D.al(i, j, k) + D.al(i - 1, j, k)) * (D.pb(i, j, k) - D.pb(i - 1, j, k)));
+  dpx += rm * rdx * (D.php(i, j, k) - D.php(i - 1, j, k)) *
+         (R(D.rdnw[k]) * (pgf_dpn<R, 1, 0>(D, i, j, k + 1) - pgf_dpn<R, 1, 0>(D, i, j, k)) -
+          R(0.5) * (c1h * D.mu2(i - 1, j, 0) + c1h * D.mu2(i, j, 0)));
+  t -= cqu_(D, i, j, k) * dpx;
+  const R rw4 = R(0.25) * (D.rw(i - 1, j, k + 1) + D.rw(i - 1, j, k) + D.rw(i, j, k + 1) + D.rw(i, j, k));
+  t = t - D.u2(i, j, k) * R(k::reradius) * rw4;
+  if (use_tendf) t += D.ru_tendf(i, j, k) / D.msfuy(i, j);
+  return t;
+}
+
+// KTendV (:267-376)
+template <class R>
+__device__ R tv_fx(const Dom<R>& D, int i, int j, int k) {
+  const int o = ord_face(i, D.nx, D.spec_x);
+  if (o == 2) return R(0.25) * (D.ru(i, j, k) + D.ru(i, j - 1, k)) * (D.v2(i, j, k) + D.v2(i - 1, j, k));
+  const R vel = R(0.5) * (D.ru(i, j, k) + D.ru(i, j - 1, k));
+  if (o == 3) return vel * flux3(D.v2(i - 2, j, k), D.v2(i - 1, j, k), D.v2(i, j, k), D.v2(i + 1, j, k), vel, R(D.hup));
+  return vel * flux5(D.v2(i - 3, j, k), D.v2(i - 2, j, k), D.v2(i - 1, j, k), D.v2(i, j, k), D.v2(i + 1, j, k),
+                     D.v2(i + 2, j, k), vel, R(D.hup));
+}
+template <class R>
+__device__ R tv_fy(const Dom<R>& D, int i, int j, int k) {
+  const int o = ord_mass(j, D.ny, D.spec_y);
+  if (o == 2) {
+    if (j <= 1) {
+      const R vb = (D.spec_y && D.v2(i, j, k) < R(0)) ? D.v2(i, j, k) : D.v2(i, j - 1, k);
+      return R(0.25) * (D.rv(i, j, k) + D.rv(i, j - 1, k)) * (D.v2(i, j, k) + vb);
+    }
+    const R vb = (D.spec_y && D.v2(i, j - 1, k) > R(0)) ? D.v2(i, j - 1, k) : D.v2(i, j, k);
+    return R(0.25) * (D.rv(i, j, k) + D.rv(i, j - 1, k)) * (vb + D.v2(i, j - 1, k));
+  }
+  const R vel = R(0.5) * (D.rv(i, j, k) + D.rv(i, j - 1, k));
+  if (o == 3) return vel * flux3(D.v2(i, j - 2, k), D.v2(i, j - 1, k), D.v2(i, j, k), D.v2(i, j + 1, k), vel, R(D.hup));
+  return vel * flux5(D.v2(i, j - 3, k), D.v2(i, j - 2, k), D.v2(i, j - 1, k), D.v2(i, j, k), D.v2(i, j + 1, k),
+                     D.v2(i, j + 2, k), vel, R(D.hup));
+}
+template <class R>
+__device__ R tv_fz(const Dom<R>& D, int i, int j, int k) {
+  if (k == 0 || k == D.nz) return 0;
+  const R vel = R(0.5) * (D.ww(i, j - 1, k) + D.ww(i, j, k));
+  if (k == 1 || k == D.nz - 1) return vel * (R(D.fnm[k]) * D.v2(i, j, k) + R(D.fnp[k]) * D.v2(i, j, k - 1));
+  return vel * flux3(D.v2(i, j, k - 2), D.v2(i, j, k - 1), D.v2(i, j, k), D.v2(i, j, k + 1), -vel, R(D.vup));
+}
+template <class R>
+__device__ R tend_v(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
+  const R rdx = R(D.rdx), rdy = R(D.rdy);
+  const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
+  const R rm = D.msfvy(i, j) / D.msfvx(i, j);
+  R t = -(D.msfvy(i, j) * rdx) * (tv_fx(D, i + 1, j, k) - tv_fx(D, i, j, k));
+  t -= (D.msfvy(i, j) * rdy) * (tv_fy(D, i, j + 1, k) - tv_fy(D, i, j, k));
+  t -= rm * R(D.rdnw[k]) * (tv_fz(D, i, j, k + 1) - tv_fz(D, i, j, k));
+  R dpy = rm * R(0.5) * rdy * (c1h * D.muv(i, j, 0) + c2h) *
+          ((D.ph2(i, j, k + 1) - D.ph2(i, j - 1, k + 1) + D.ph2(i, j, k) - D.ph2(i, j - 1, k)) +
+           (D.alt(i, j, k) + D.alt(i, j - 1, k)) * (D.p(i, j, k) - D.p(i, j - 1, k)) +
+           (D.al(i, j, k) + D.al(i, j - 1, k)) * (D.pb(i, j, k) - D.pb(i, j - 1, k)));
+  dpy += rm * rdy * (D.php(i, j, k) - D.php(i, j - 1, k)) *
+         (R(D.rdnw[k]) * (pgf_dpn<R, 0, 1>(D, i, j, k + 1) - pgf_dpn<R, 0, 1>(D, i, j, k)) -
+          R(0.5) * (c1h * D.mu2(i, j - 1, 0) + c1h * D.mu2(i, j, 0)));
+  t -= cqv_(D, i, j, k) * dpy;
+  const R rw4 = R(0.25) * (D.rw(i, j - 1, k + 1) + D.rw(i, j - 1, k) + D.rw(i, j, k + 1) + D.rw(i, j, k));
+  t = t - rm * D.v2(i, j, k) * R(k::reradius) * rw4;
+  if (use_tendf) t += D.rv_tendf(i, j, k) * D.msfvx_inv(i, j);
+  return t;
+}
+
+// KTendW (:379-499)
+template <class R>
+__device__ __forceinline__ R tw_rux(const Dom<R>& D, int i, int j, int k) {
+  const int nz = D.nz;
+  if (k < nz) return R(D.fnm[k]) * D.ru(i, j, k) + R(D.fnp[k]) * D.ru(i, j, k - 1);
+  return (R(2) - R(D.fnm[nz - 1])) * D.ru(i, j, nz - 1) - R(D.fnp[nz - 1]) * D.ru(i, j, nz - 2);
+}
+template <class R>
+__device__ __forceinline__ R tw_rvy(const Dom<R>& D, int i, int j, int k) {
+  const int nz = D.nz;
+  if (k < nz) return R(D.fnm[k]) * D.rv(i, j, k) + R(D.fnp[k]) * D.rv(i, j, k - 1);
+  return (R(2) - R(D.fnm[nz - 1])) * D.rv(i, j, nz - 1) - R(D.fnp[nz - 1]) * D.rv(i, j, nz - 2);
+}
+template <class R>
+__device__ R tw_fx(const Dom<R>& D, int i, int j, int k) {
+  const R vel = tw_rux(D, i, j, k);
+  const int o = ord_face(i, D.nx, D.spec_x);
+  if (o == 2) return R(0.5) * vel * (D.w2(i, j, k) + D.w2(i - 1, j, k));
+  if (o == 3) return vel * flux3(D.w2(i - 2, j, k), D.w2(i - 1, j, k), D.w2(i, j, k), D.w2(i + 1, j, k), vel, R(D.hup));
+  return vel * flux5(D.w2(i - 3, j, k), D.w2(i - 2, j, k), D.w2(i - 1, j, k), D.w2(i, j, k), D.w2(i + 1, j, k),
+                     D.w2(i + 2, j, k), vel, R(D.hup));
+}
+template <class R>
+__device__ R tw_fy(const Dom<R>& D, int i, int j, int k) {
+  const R vel = tw_rvy(D, i, j, k);
+  const int o = ord_face(j, D.ny, D.spec_y);
+  if (o == 2) return R(0.5) * vel * (D.w2(i, j, k) + D.w2(i, j - 1, k));
+  if (o == 3) return vel * flux3(D.w2(i, j - 2, k), D.w2(i, j - 1, k), D.w2(i, j, k), D.w2(i, j + 1, k), vel, R(D.hup));
+  return vel * flux5(D.w2(i, j - 3, k), D.w2(i, j - 2, k), D.w2(i, j - 1, k), D.w2(i, j, k), D.w2(i, j + 1, k),
+                     D.w2(i, j + 2, k), vel, R(D.hup));
+}
+template <class R>
+__device__ R tw_fz(const Dom<R>& D, int i, int j, int m) {
+  if (m == 0 || m == D.nz - 1)
+    return R(0.25) * (D.ww(i, j, m + 1) + D.ww(i, j, m)) * (D.w2(i, j, m + 1) + D.w2(i, j, m));
+  const R vel = R(0.5) * (D.ww(i, j, m + 1) + D.ww(i, j, m));
+  return vel * flux3(D.w2(i, j, m - 1), D.w2(i, j, m), D.w2(i, j, m + 1), D.w2(i, j, m + 2), -vel, R(D.vup));
+}
+template <class R>
+__device__ R tend_w(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
+  const int nz = D.nz;
+  const R rdx = R(D.rdx), rdy = R(D.rdy);
+  R t = -(D.msftx(i, j) * rdx) * (tw_fx(D, i + 1, j, k) - tw_fx(D, i, j, k));
+  if (D.do_y) t -= (D.msftx(i, j) * rdy) * (tw_fy(D, i, j + 1, k) - tw_fy(D, i, j, k));
+  const R rmsft = R(1) / D.msfty(i, j);
+  if (k < nz) {
+    t -= R(D.rdn[k]) * (tw_fz(D, i, j, k) - tw_fz(D, i, j, k - 1));
+    const R cqw = cqw_(D, i, j, k), cq1 = R(1) / (R(1) + cqw), cq2 = cqw * cq1;
+    t += rmsft * R(k::g) *
+         (cq1 * R(D.rdn[k]) * (D.p(i, j, k) - D.p(i, j, k - 1)) - R(D.c1f[k]) * D.mu2(i, j, 0) -
+          cq2 * (R(D.c1f[k]) * D.mub(i, j) + R(D.c2f[k])));
+    if (D.w_damping) {  // w_damp, wd_dt = dt
+      const R wd_dt = R(D.dt);
+      const R muf = R(D.c1f[k]) * D.mut(i, j, 0) + R(D.c2f[k]);
+      R cfl = D.ww(i, j, k) / muf * R(D.rdnw[k]) * wd_dt;
+      cfl = cfl < R(0) ? -cfl : cfl;
+      if (cfl > R(1)) t = t - (D.w2(i, j, k) < R(0) ? R(-1) : R(1)) * R(0.3) * (cfl - R(D.w_crit_cfl)) * muf;
+    }
+    const R fnm = R(D.fnm[k]), fnp = R(D.fnp[k]);
+    const R ruw = R(0.5) * (fnm * (D.ru(i, j, k) + D.ru(i + 1, j, k)) + fnp * (D.ru(i, j, k - 1) + D.ru(i + 1, j, k - 1)));
+    const R rvw = R(0.5) * (fnm * (D.rv(i, j, k) + D.rv(i, j + 1, k)) + fnp * (D.rv(i, j, k - 1) + D.rv(i, j + 1, k - 1)));
+    const R rmt = D.msftx(i, j) / D.msfty(i, j);
+    const R uw = R(0.5) * (fnm * (D.u2(i, j, k) + D.u2(i + 1, j, k)) + fnp * (D.u2(i, j, k - 1) + D.u2(i + 1, j, k - 1)));
+    const R vw = R(0.5) * (fnm * (D.v2(i, j, k) + D.v2(i, j + 1, k)) + fnp * (D.v2(i, j, k - 1) + D.v2(i, j + 1, k - 1)));
+    t = t + R(k::reradius) * (ruw * uw + rmt * rvw * vw);
+  } else {
+    t += R(2) * R(D.rdn[nz - 1]) * tw_fz(D, i, j, nz - 1);
+    const R cqw = cqw_(D, i, j, nz - 1), cq1 = R(1) / (R(1) + cqw), cq2 = cqw * cq1;
+    t += rmsft * R(k::g) *
+         (cq1 * R(2) * R(D.rdnw[nz - 1]) * (-D.p(i, j, nz - 1)) - R(D.c1f[nz]) * D.mu2(i, j, 0) -
+          cq2 * (R(D.c1f[nz]) * D.mub(i, j) + R(D.c2f[nz])));
+  }
+  if (use_tendf) t += D.rw_tendf(i, j, k) / D.msfty(i, j);
+  return t;
+}
+
+// KTendT (:502-565) / advect_scalar face fluxes of any mass field q with mass fluxes (ufx, vfy, wfz)
+template <class R>
+__device__ R sc_fx(const Dom<R>& D, const V3<R>& q, const V3<R>& ruf, int i, int j, int k, bool pd) {
+  const R vel = ruf(i, j, k);
+  const int o = ord_face(i, D.nx, D.spec_x);
+  if (o == 2) return R(0.5) * vel * (q(i, j, k) + q(i - 1, j, k));
+  if (o == 3) {
+    if (pd) return vel * flux3_pd(q(i - 2, j, k), q(i - 1, j, k), q(i, j, k), q(i + 1, j, k), vel, R(D.hup));
+    return vel * flux3(q(i - 2, j, k), q(i - 1, j, k), q(i, j, k), q(i + 1, j, k), vel, R(D.hup));
+  }
+  if (pd)
+    return vel * flux5_pd(q(i - 3, j, k), q(i - 2, j, k), q(i - 1, j, k), q(i, j, k), q(i + 1, j, k), q(i + 2, j, k), vel, R(D.hup));
+  return vel * flux5(q(i - 3, j, k), q(i - 2, j, k), q(i - 1, j, k), q(i, j, k), q(i + 1, j, k), q(i + 2, j, k), vel, R(D.hup));
+}
+template <class R>
+__device__ R sc_fy(const Dom<R>& D, const V3<R>& q, const V3<R>& rvf, int i, int j, int k, bool pd) {
+  const R vel = rvf(i, j, k);
+  const int o = ord_face(j, D.ny, D.spec_y);
+  if (o == 2) return R(0.5) * vel * (q(i, j, k) + q(i, j - 1, k));
+  if (o == 3) {
+    if (pd) return vel * flux3_pd(q(i, j - 2, k), q(i, j - 1, k), q(i, j, k), q(i, j + 1, k), vel, R(D.hup));
+    return vel * flux3(q(i, j - 2, k), q(i, j - 1, k), q(i, j, k), q(i, j + 1, k), vel, R(D.hup));
+  }
+  if (pd)
+    return vel * flux5_pd(q(i, j - 3, k), q(i, j - 2, k), q(i, j - 1, k), q(i, j, k), q(i, j + 1, k), q(i, j + 2, k), vel, R(D.hup));
+  return vel * flux5(q(i, j - 3, k), q(i, j - 2, k), q(i, j - 1, k), q(i, j, k), q(i, j + 1, k), q(i, j + 2, k), vel, R(D.hup));
+}
+template <class R>
+__device__ R sc_fz(const Dom<R>& D, const V3<R>& q, const V3<R>& wwf, int i, int j, int k, bool pd) {
+  if (k == 0 || k == D.nz) return 0;
+  const R vel = wwf(i, j, k);
+  if (k == 1 || k == D.nz - 1) return vel * (R(D.fnm[k]) * q(i, j, k) + R(D.fnp[k]) * q(i, j, k - 1));
+  if (pd) return vel * flux3_pd(q(i, j, k - 2), q(i, j, k - 1), q(i, j, k), q(i, j, k + 1), -vel, R(D.vup));
+  return vel * flux3(q(i, j, k - 2), q(i, j, k - 1), q(i, j, k), q(i, j, k + 1), -vel, R(D.vup));
+}
+template <class R>
+__device__ R tend_t(const Dom<R>& D, int i, int j, int k, bool use_tendf, bool use_hd) {
+  R r = -(D.msftx(i, j) * R(D.rdx)) * (sc_fx(D, D.t2, D.ru, i + 1, j, k, false) - sc_fx(D, D.t2, D.ru, i, j, k, false));
+  if (D.do_y) r -= (D.msftx(i, j) * R(D.rdy)) * (sc_fy(D, D.t2, D.rv, i, j + 1, k, false) - sc_fy(D, D.t2, D.rv, i, j, k, false));
+  r -= R(D.rdnw[k]) * (sc_fz(D, D.t2, D.ww, i, j, k + 1, false) - sc_fz(D, D.t2, D.ww, i, j, k, false));
+  if (use_tendf) r += D.t_tendf(i, j, k) / D.msfty(i, j);
+  if (use_hd) r += (R(D.c1h[k]) * D.mut(i, j, 0) + R(D.c2h[k])) * D.hd(i, j, k) / D.msfty(i, j);
+  return r;
+}
+
+// KTendPh (:570-668)
+template <class R>
+__device__ __forceinline__ R tph_wdwn(const Dom<R>& D, int i, int j, int m) {
+  return R(0.5) * (D.ww(i, j, m + 1) + D.ww(i, j, m)) * R(D.rdnw[m]) *
+         (D.ph2(i, j, m + 1) - D.ph2(i, j, m) + D.phb(i, j, m + 1) - D.phb(i, j, m));
+}
+template <class R, int DI, int DJ>
+__device__ __forceinline__ R grad6(const Dom<R>& D, int i, int j, int k) {
+  return R(45) * (D.ph2(i + DI, j + DJ, k) - D.ph2(i - DI, j - DJ, k)) -
+         R(9) * (D.ph2(i + 2 * DI, j + 2 * DJ, k) - D.ph2(i - 2 * DI, j - 2 * DJ, k)) +
+         (D.ph2(i + 3 * DI, j + 3 * DJ, k) - D.ph2(i - 3 * DI, j - 3 * DJ, k)) +
+         R(45) * (D.phb(i + DI, j + DJ, k) - D.phb(i - DI, j - DJ, k)) -
+         R(9) * (D.phb(i + 2 * DI, j + 2 * DJ, k) - D.phb(i - 2 * DI, j - 2 * DJ, k)) +
+         (D.phb(i + 3 * DI, j + 3 * DJ, k) - D.phb(i - 3 * DI, j - 3 * DJ, k));
+}
+template <class R, int DI, int DJ>
+__device__ __forceinline__ R grad4(const Dom<R>& D, int i, int j, int k) {
+  return R(8) * (D.ph2(i + DI, j + DJ, k) - D.ph2(i - DI, j - DJ, k)) -
+         (D.ph2(i + 2 * DI, j + 2 * DJ, k) - D.ph2(i - 2 * DI, j - 2 * DJ, k)) +
+         R(8) * (D.phb(i + DI, j + DJ, k) - D.phb(i - DI, j - DJ, k)) -
+         (D.phb(i + 2 * DI, j + 2 * DJ, k) - D.phb(i - 2 * DI, j - 2 * DJ, k));
+}
+template <class R, int DI, int DJ>
+__device__ __forceinline__ R dfwd(const Dom<R>& D, int i, int j, int k) {
+  return D.phb(i + DI, j + DJ, k) - D.phb(i, j, k) + D.ph2(i + DI, j + DJ, k) - D.ph2(i, j, k);
+}
+__device__ __forceinline__ int ph_horder(int i, int n, int on, int is_x) {
+  if (!on) return 6;
+  if (i <= 0 || i >= n - 1) return 0;
+  if (i == 1 || i == n - 2) return 2;
+  if (i == 2 || i == n - 3) return is_x ? 0 : 4;
+  return 6;
+}
+template <class R>
+__device__ R tend_ph(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
+  const int nz = D.nz;
+  const R c1f = R(D.c1f[k]), c2f = R(D.c2f[k]);
+  R t = 0;
+  if (k < nz) t = t - (R(D.fnm[k]) * tph_wdwn(D, i, j, k) + R(D.fnp[k]) * tph_wdwn(D, i, j, k - 1));
+  t = t + (c1f * D.mut(i, j, 0) + c2f) * R(k::g) * D.w2(i, j, k) / D.msfty(i, j);
+  const R r60 = R(1) / R(60), r12 = R(1) / R(12);
+  if (D.do_y) {
+    const R mvp = c1f * D.muv(i, j + 1, 0) + c2f, mvm = c1f * D.muv(i, j, 0) + c2f;
+    const R vp = k < nz ? D.v2(i, j + 1, k) + D.v2(i, j + 1, k - 1) : R(D.cfn) * D.v2(i, j + 1, nz - 1) + R(D.cfn1) * D.v2(i, j + 1, nz - 2);
+    const R vm = k < nz ? D.v2(i, j, k) + D.v2(i, j, k - 1) : R(D.cfn) * D.v2(i, j, nz - 1) + R(D.cfn1) * D.v2(i, j, nz - 2);
+    const R cy = (k < nz ? R(0.25) : R(0.5)) * R(D.rdy) / D.msfty(i, j);
+    const int o = ph_horder(j, D.ny, D.spec_y, 0);
+    if (o == 6) t = t - cy * ((mvp * vp * D.msfvy(i, j + 1) + mvm * vm * D.msfvy(i, j)) * r60 * grad6<R, 0, 1>(D, i, j, k));
+    else if (o == 4) t = t - cy * ((mvp * vp * D.msfvy(i, j + 1) + mvm * vm * D.msfvy(i, j)) * r12 * grad4<R, 0, 1>(D, i, j, k));
+    else if (o == 2)
+      t = t - cy * (mvp * vp * D.msfvy(i, j + 1) * dfwd<R, 0, 1>(D, i, j, k) + mvm * vm * D.msfvy(i, j) * dfwd<R, 0, 1>(D, i, j - 1, k));
+  }
+  const R mup = c1f * D.muu(i + 1, j, 0) + c2f, mum = c1f * D.muu(i, j, 0) + c2f;
+  const R up = k < nz ? D.u2(i + 1, j, k) + D.u2(i + 1, j, k - 1) : R(D.cfn) * D.u2(i + 1, j, nz - 1) + R(D.cfn1) * D.u2(i + 1, j, nz - 2);
+  const R um = k < nz ? D.u2(i, j, k) + D.u2(i, j, k - 1) : R(D.cfn) * D.u2(i, j, nz - 1) + R(D.cfn1) * D.u2(i, j, nz - 2);
+  const R cx = (k < nz ? R(0.25) : R(0.5)) * R(D.rdx) / D.msfty(i, j);
+  const int o = ph_horder(i, D.nx, D.spec_x, 1);
+  if (o == 6) t = t - cx * ((mup * up * D.msfux(i + 1, j) + mum * um * D.msfux(i, j)) * r60 * grad6<R, 1, 0>(D, i, j, k));
+  else if (o == 2)
+    t = t - cx * (mup * up * D.msfux(i + 1, j) * dfwd<R, 1, 0>(D, i, j, k) + mum * um * D.msfux(i, j) * dfwd<R, 1, 0>(D, i - 1, j, k));
+  else if (o == 4) t = t - cx * ((mup * up * D.msfux(i + 1, j) + mum * um * D.msfux(i, j)) * r12 * grad4<R, 1, 0>(D, i, j, k));
+  if (use_tendf) t = t + D.ph_tendf(i, j, k) / D.msfty(i, j);
+  return t;
+}
+
+// LargeStep::tendencies (large_step.cpp:798-861): the five tendencies of a point, each for the points of
+// its own range: ru (u_i0 .. u_i1), rv (v_j0 .. v_j1, 3-D), rw and ph (levels 1..nz), theta (mass cells).
+// Also mu_tend = 0 (zero_tend of a run with lateral boundaries) at rk 2 and 3.
+template <class R>
+__global__ void __launch_bounds__(PX) k_tend(const Dom<R>* __restrict__ doms, BlockMap bm, int rk) {
+  const Dom<R>* Dp;
+  int i, j, k;
+  if (!thread_index(doms, bm, RG_STAG, Dp, i, j, k)) return;
+  const Dom<R>& D = *Dp;
+  const int nx = D.nx, ny = D.ny, nz = D.nz;
+  const bool use_tendf = D.lbc || D.diff_on;
+  const int ui0 = D.bc_x != CW_BC_PERIODIC ? 1 : 0;
+  const int vj0 = (D.bc_y != CW_BC_PERIODIC && D.do_y) ? 1 : 0;
+  if (i >= ui0 && i < nx && j < ny && k < nz) D.ru_tend(i, j, k) = tend_u(D, i, j, k, use_tendf);
+  if (D.do_y && i < nx && j >= vj0 && j < ny && k < nz) D.rv_tend(i, j, k) = tend_v(D, i, j, k, use_tendf);
+  if (i < nx && j < ny) {
+    if (k >= 1) {
+      D.rw_tend(i, j, k) = tend_w(D, i, j, k, use_tendf);
+      D.ph_tend(i, j, k) = tend_ph(D, i, j, k, D.lbc != 0);
+    }
+    if (k < nz) D.t_tend(i, j, k) = tend_t(D, i, j, k, use_tendf, D.n_moist > 0);
+    if (k == 0 && D.lbc && rk != 1) D.mu_tend(i, j, 0) = 0;
+  }
+}
+
+// ------------------------------------------------------------------ constant-K diffusion (rk 1)
+// DiffusionDriver::dynamics, diff_opt 1 / km_opt 1 (src/dyn/diffusion_driver.cpp:153-187) with the kernels
+// of src/dyn/diffusion/big_step_diffusion.hpp:26-336. KIsotropicKm makes every eddy viscosity a constant
+// (khdif, khdif / prandtl), so it is used directly. The held tendencies start from zero (init_zero_tendency,
+// large_step.cpp:888-894), then the horizontal and vertical diffusion are added in the reference's order.
+template <class R>
+__device__ __forceinline__ R mk(const double* c1, const double* c2, const V3<R>& mut, int i, int j, int k) {
+  return R(c1[k]) * mut(i, j, 0) + R(c2[k]);
+}
+template <class R>
+__device__ R hdiff_u(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, R xk, int i, int j, int k) {
+  const double *c1 = D.c1h, *c2 = D.c2h;
+  const R rdx = R(D.rdx), rdy = R(D.rdy);
+  const R mkrdxm = (D.msftx(i - 1, j) / D.msfty(i - 1, j)) * mk(c1, c2, mut, i - 1, j, k) * xk * rdx;
+  const R mkrdxp = (D.msftx(i, j) / D.msfty(i, j)) * mk(c1, c2, mut, i, j, k) * xk * rdx;
+  const R mrdx = D.msfux(i, j) * D.msfuy(i, j) * rdx;
+  const R mkrdym = ((D.msfuy(i, j) + D.msfuy(i, j - 1)) / (D.msfux(i, j) + D.msfux(i, j - 1))) * R(0.25) *
+                   (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k) + mk(c1, c2, mut, i - 1, j - 1, k) + mk(c1, c2, mut, i - 1, j, k)) *
+                   R(0.25) * (xk + xk + xk + xk) * rdy;
+  const R mkrdyp = ((D.msfuy(i, j) + D.msfuy(i, j + 1)) / (D.msfux(i, j) + D.msfux(i, j + 1))) * R(0.25) *
+                   (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j + 1, k) + mk(c1, c2, mut, i - 1, j + 1, k) + mk(c1, c2, mut, i - 1, j, k)) *
+                   R(0.25) * (xk + xk + xk + xk) * rdy;
+  const R mrdy = D.msfux(i, j) * D.msfuy(i, j) * rdy;
+  return mrdx * (mkrdxp * (f(i + 1, j, k) - f(i, j, k)) - mkrdxm * (f(i, j, k) - f(i - 1, j, k))) +
+         mrdy * (mkrdyp * (f(i, j + 1, k) - f(i, j, k)) - mkrdym * (f(i, j, k) - f(i, j - 1, k)));
+}
+template <class R>
+__device__ R hdiff_v(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, R xk, int i, int j, int k) {
+  const double *c1 = D.c1h, *c2 = D.c2h;
+  const R rdx = R(D.rdx), rdy = R(D.rdy);
+  const R mkrdxm = ((D.msfvx(i, j) + D.msfvx(i - 1, j)) / (D.msfvy(i, j) + D.msfvy(i - 1, j))) * R(0.25) *
+                   (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k) + mk(c1, c2, mut, i - 1, j - 1, k) + mk(c1, c2, mut, i - 1, j, k)) *
+                   R(0.25) * (xk + xk + xk + xk) * rdx;
+  const R mkrdxp = ((D.msfvx(i, j) + D.msfvx(i + 1, j)) / (D.msfvy(i, j) + D.msfvy(i + 1, j))) * R(0.25) *
+                   (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k) + mk(c1, c2, mut, i + 1, j - 1, k) + mk(c1, c2, mut, i + 1, j, k)) *
+                   R(0.25) * (xk + xk + xk + xk) * rdx;
+  const R mrdx = D.msfvx(i, j) * D.msfvy(i, j) * rdx;
+  const R mkrdym = (D.msfty(i, j - 1) / D.msftx(i, j - 1)) * xk * rdy;
+  const R mkrdyp = (D.msfty(i, j) / D.msftx(i, j)) * xk * rdy;
+  const R mrdy = D.msfvx(i, j) * D.msfvy(i, j) * rdy;
+  return mrdx * (mkrdxp * (f(i + 1, j, k) - f(i, j, k)) - mkrdxm * (f(i, j, k) - f(i - 1, j, k))) +
+         mrdy * (mkrdyp * (f(i, j + 1, k) - f(i, j, k)) - mkrdym * (f(i, j, k) - f(i, j - 1, k)));
+}
+template <class R>
+__device__ R hdiff_w(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, R xk, int i, int j, int k) {
+  const double *c1 = D.c1f, *c2 = D.c2f;
+  const R rdx = R(D.rdx), rdy = R(D.rdy);
+  const R mkrdxm = (D.msfux(i, j) / D.msfuy(i, j)) * R(0.25) *
+                   (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i - 1, j, k) + mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i - 1, j, k)) *
+                   R(0.25) * (xk + xk + xk + xk) * rdx;
+  const R mkrdxp = (D.msfux(i + 1, j) / D.msfuy(i + 1, j)) * R(0.25) *
+                   (mk(c1, c2, mut, i + 1, j, k) + mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i + 1, j, k) + mk(c1, c2, mut, i, j, k)) *
+                   R(0.25) * (xk + xk + xk + xk) * rdx;
+  const R mrdx = D.msftx(i, j) * D.msfty(i, j) * rdx;
+  const R mkrdym = (D.msfvy(i, j) * D.msfvx_inv(i, j)) * R(0.25) *
+                   (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k) + mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k)) *
+                   R(0.25) * (xk + xk + xk + xk) * rdy;
+  const R mkrdyp = (D.msfvy(i, j + 1) * D.msfvx_inv(i, j + 1)) * R(0.25) *
+                   (mk(c1, c2, mut, i, j + 1, k) + mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j + 1, k) + mk(c1, c2, mut, i, j, k)) *
+                   R(0.25) * (xk + xk + xk + xk) * rdy;
+  const R mrdy = D.msftx(i, j) * D.msfty(i, j) * rdy;
+  return mrdx * (mkrdxp * (f(i + 1, j, k) - f(i, j, k)) - mkrdxm * (f(i, j, k) - f(i - 1, j, k))) +
+         mrdy * (mkrdyp * (f(i, j + 1, k) - f(i, j, k)) - mkrdym * (f(i, j, k) - f(i, j - 1, k)));
+}
+// KHorizDiffM1 (with_base = false) / KHorizDiff3DMP (base = t_init or qv_base)
+template <class R>
+__device__ R hdiff_m(const Dom<R>& D, const V3<R>& f, const VB<R>* base, const V3<R>& mut, R xk, int i, int j, int k) {
+  const double *c1 = D.c1h, *c2 = D.c2h;
+  const R rdx = R(D.rdx), rdy = R(D.rdy);
+  const R mkrdxm = (D.msfux(i, j) / D.msfuy(i, j)) * R(0.5) * (xk + xk) * R(0.5) * (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i - 1, j, k)) * rdx;
+  const R mkrdxp = (D.msfux(i + 1, j) / D.msfuy(i + 1, j)) * R(0.5) * (xk + xk) * R(0.5) * (mk(c1, c2, mut, i + 1, j, k) + mk(c1, c2, mut, i, j, k)) * rdx;
+  const R mrdx = D.msftx(i, j) * D.msfty(i, j) * rdx;
+  const R mkrdym = (D.msfvy(i, j) * D.msfvx_inv(i, j)) * R(0.5) * (xk + xk) * R(0.5) * (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k)) * rdy;
+  const R mkrdyp = (D.msfvy(i, j + 1) * D.msfvx_inv(i, j + 1)) * R(0.5) * (xk + xk) * R(0.5) * (mk(c1, c2, mut, i, j + 1, k) + mk(c1, c2, mut, i, j, k)) * rdy;
+  const R mrdy = D.msftx(i, j) * D.msfty(i, j) * rdy;
+  if (!base)
+    return mrdx * (mkrdxp * (f(i + 1, j, k) - f(i, j, k)) - mkrdxm * (f(i, j, k) - f(i - 1, j, k))) +
+           mrdy * (mkrdyp * (f(i, j + 1, k) - f(i, j, k)) - mkrdym * (f(i, j, k) - f(i, j - 1, k)));
+  const VB<R>& b = *base;
+  const R dxp = f(i + 1, j, k) - f(i, j, k) - b(i + 1, j, k) + b(i, j, k);
+  const R dxm = f(i, j, k) - f(i - 1, j, k) - b(i, j, k) + b(i - 1, j, k);
+  const R dyp = f(i, j + 1, k) - f(i, j, k) - b(i, j + 1, k) + b(i, j, k);
+  const R dym = f(i, j, k) - f(i, j - 1, k) - b(i, j, k) + b(i, j - 1, k);
+  return mrdx * (mkrdxp * dxp - mkrdxm * dxm) + mrdy * (mkrdyp * dyp - mkrdym * dym);
+}
+// the vertical diffusion flux of a column at interface k (vflux[k] of the reference's column kernels)
+template <class R>
+__device__ __forceinline__ R vflux_w(const Dom<R>& D, const V3<R>& f, R kv, int i, int j, int k) {
+  if (k >= D.nz - 1) return 0;
+  return (kv / D.alt(i, j, k)) * R(D.rdnw[k]) * (f(i, j, k + 1) - f(i, j, k));
+}
+template <class R>
+__device__ __forceinline__ R vflux_m(const Dom<R>& D, const V3<R>& f, const VB<R>* base, R kv, int i, int j, int k) {
+  if (k >= D.nz - 1) return 0;
+  const R dpert = base ? f(i, j, k + 1) - f(i, j, k) - (*base)(i, j, k + 1) + (*base)(i, j, k) : f(i, j, k + 1) - f(i, j, k);
+  return kv * R(D.rdn[k + 1]) / (R(0.5) * (D.alt(i, j, k) + D.alt(i, j, k + 1))) * dpert;
+}
+template <class R, int DI, int DJ>
+__device__ __forceinline__ R vflux_uv(const Dom<R>& D, const V3<R>& f, const double* ub, R kv, int i, int j, int k) {
+  if (k >= D.nz - 1) return 0;
+  const R a = R(0.25) * (D.alt(i, j, k) + D.alt(i - DI, j - DJ, k) + D.alt(i, j, k + 1) + D.alt(i - DI, j - DJ, k + 1));
+  const R dpert = f(i, j, k + 1) - f(i, j, k) - R(ub[k + 1]) + R(ub[k]);
+  return kv * R(D.rdn[k + 1]) / a * dpert;
+}
+// vertical_diffusion 'w' (KVertDiffW1), 'm' / mp (KVertDiffM1 / MP1), u / v (KVertDiffU1 / V1): the
+// increment of level k
+template <class R>
+__device__ __forceinline__ R vdiff_w(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, R kv, int i, int j, int k) {
+  const R G = R(k::g);
+  const R mu = R(D.c1f[k]) * mut(i, j, 0) + R(D.c2f[k]);
+  const R alt_avg = R(0.5) * (D.alt(i, j, k) + D.alt(i, j, k - 1));
+  return R(D.rdn[k]) * G * G / mu / alt_avg * (vflux_w(D, f, kv, i, j, k) - vflux_w(D, f, kv, i, j, k - 1));
+}
+template <class R>
+__device__ __forceinline__ R vdiff_m(const Dom<R>& D, const V3<R>& f, const VB<R>* base, const V3<R>& mut, R kv, int i, int j, int k) {
+  const R G = R(k::g);
+  if (k == 0) {
+    const R vf0 = vflux_m(D, f, base, kv, i, j, 0);
+    return G * G / (R(D.c1h[0]) * mut(i, j, 0) + R(D.c2h[0])) / D.alt(i, j, 0) * R(D.rdnw[0]) * (vf0 - vf0);
+  }
+  const R mu = R(D.c1h[k]) * mut(i, j, 0) + R(D.c2h[k]);
+  return G * G / mu / D.alt(i, j, k) * R(D.rdnw[k]) * (vflux_m(D, f, base, kv, i, j, k) - vflux_m(D, f, base, kv, i, j, k - 1));
+}
+template <class R, int DI, int DJ>
+__device__ __forceinline__ R vdiff_uv(const Dom<R>& D, const V3<R>& f, const double* ub, const V3<R>& muf, R kv, int i, int j, int k) {
+  const R G = R(k::g);
+  if (k == 0) {
+    const R vf0 = vflux_uv<R, DI, DJ>(D, f, ub, kv, i, j, 0);
+    return G * G * R(D.rdnw[0]) / (R(D.c1h[0]) * muf(i, j, 0) + R(D.c2h[0])) /
+           (R(0.5) * (D.alt(i - DI, j - DJ, 0) + D.alt(i, j, 0))) * (vf0 - vf0);
+  }
+  const R mu = R(D.c1h[k]) * muf(i, j, 0) + R(D.c2h[k]);
+  const R a = R(0.5) * (D.alt(i - DI, j - DJ, k) + D.alt(i, j, k));
+  return G * G * R(D.rdnw[k]) / mu / a * (vflux_uv<R, DI, DJ>(D, f, ub, kv, i, j, k) - vflux_uv<R, DI, DJ>(D, f, ub, kv, i, j, k - 1));
+}
+
+// rk 1: zero the held tendencies, add the constant-K diffusion; mu_tend = 0 with lateral boundaries
+template <class R>
+__global__ void __launch_bounds__(PX) k_tendf_rk1(const Dom<R>* __restrict__ doms, BlockMap bm) {
+  const Dom<R>* Dp;
+  int i, j, k;
+  if (!thread_index(doms, bm, RG_STAG, Dp, i, j, k)) return;
+  const Dom<R>& D = *Dp;
+  const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
+  const bool dd = D.diff_on;
+  const bool sp = D.lbc;  // specified boundaries (the diffusion's index ranges)
+  const bool px = D.bc_x == CW_BC_PERIODIC;
+  const R khdif = R(D.khdif), kvdif = R(D.kvdif);
+  const R khh = R(D.khdif / D.prandtl);
+  if (j < ny && k < nz) {  // ru_tendf: U points [0, nx] x [0, ny) x [0, nz)
+    R t = 0;
+    if (dd) {
+      int is = sp ? 1 : 0, ie = sp ? nx : nx + 1;
+      const int js = sp ? 1 : 0, je = sp ? ny - 1 : ny;
+      if (px) { is = 0; ie = nx + 1; }
+      if (i >= is && i < ie && j >= js && j < je) t += hdiff_u(D, D.u2, D.mut, khdif, i, j, k);
+      int vis = sp ? 1 : 0, vie = sp ? nx : nx + 1;
+      if (px) { vis = 0; vie = nx + 1; }
+      if (i >= vis && i < vie && k < nz - 1) t += vdiff_uv<R, 1, 0>(D, D.u2, D.u_base, D.muu, kvdif, i, j, k);
+    }
+    D.ru_tendf(i, j, k) = t;
+  }
+  if (i < nx && j < nyv && k < nz) {  // rv_tendf
+    R t = 0;
+    if (dd && D.do_y) {
+      int is = sp ? 1 : 0, ie = sp ? nx - 1 : nx;
+      const int js = sp ? 1 : 0, je = sp ? ny : ny + 1;
+      if (px) { is = 0; ie = nx; }
+      if (i >= is && i < ie && j >= js && j < je) t += hdiff_v(D, D.v2, D.mut, khdif, i, j, k);
+      const int vjs = sp ? 1 : 0, vje = sp ? ny : ny + 1;
+      if (j >= vjs && j < vje && k < nz - 1) t += vdiff_uv<R, 0, 1>(D, D.v2, D.v_base, D.muv, kvdif, i, j, k);
+    }
+    D.rv_tendf(i, j, k) = t;
+  }
+  if (i < nx && j < ny) {
+    R tw = 0;
+    if (dd && k >= 1 && k < nz) {
+      int is = sp ? 1 : 0, ie = sp ? nx - 1 : nx;
+      const int js = sp ? 1 : 0, je = sp ? ny - 1 : ny;
+      if (px) { is = 0; ie = nx; }
+      if (i >= is && i < ie && j >= js && j < je) tw += hdiff_w(D, D.w2, D.mut, khdif, i, j, k);
+      tw += vdiff_w(D, D.w2, D.mut, kvdif, i, j, k);
+    }
+    D.rw_tendf(i, j, k) = tw;
+    D.ph_tendf(i, j, k) = 0;
+    if (k < nz) {
+      R tt = 0;
+      if (dd) {
+        int is = sp ? 1 : 0, ie = sp ? nx - 1 : nx;
+        const int js = sp ? 1 : 0, je = sp ? ny - 1 : ny;
+        if (px) { is = 0; ie = nx; }
+        if (i >= is && i < ie && j >= js && j < je) tt += hdiff_m(D, D.t2, &D.t_init, D.mut, khh, i, j, k);
+        tt += vdiff_m(D, D.t2, &D.t_init, D.mut, R(3.) * kvdif, i, j, k);
+      }
+      D.t_tendf(i, j, k) = tt;
+    }
+    if (k == 0 && D.lbc) D.mu_tend(i, j, 0) = 0;
+  }
+}
+
+// ------------------------------------------------------------------ lateral boundaries
+// LateralBC (src/dyn/lateral_bc.cpp:21-196): the ring of a variable, slabs (pos, k, b) pos fastest;
+// side order S, N, W, E = slabs ys, ye, xs, xe.
+__device__ __forceinline__ int slab_of_side(int side) { return side < 2 ? side + 2 : side - 2; }
+struct Ring {
+  int ibe, jbe;
+  __device__ __forceinline__ bool map(int pos, int side, int b, int& i, int& j) const {
+    switch (side) {
+      case 0: j = b; i = pos; return pos >= b && pos <= ibe - b;
+      case 1: j = jbe - b; i = pos; return pos >= b && pos <= ibe - b;
+      case 2: i = b; j = pos; return pos >= b + 1 && pos <= jbe - b - 1;
+      default: i = ibe - b; j = pos; return pos >= b + 1 && pos <= jbe - b - 1;
+    }
+  }
+};
+__device__ __forceinline__ Ring ring_for(int nx, int ny, char var) {
+  return Ring{var == 'u' ? nx : nx - 1, var == 'v' ? ny : ny - 1};
+}
+template <class R>
+__device__ __forceinline__ R slab_at(const Slabs<R>& s, int tend, int sl, int pos, int k, int b) {
+  const int np = s.npos[sl];
+  return (tend ? s.t[sl] : s.v[sl])[pos + k * np + b * np * s.nk];
+}
+template <class R>
+__device__ __forceinline__ R slab_val(const Slabs<R>& s, int sl, int pos, int k, int b, R dtbc) {
+  return slab_at(s, 0, sl, pos, k, b) + dtbc * slab_at(s, 1, sl, pos, k, b);
+}
+
+// KRelax (:79-118) at ring point (pos, side, b, k) of one variable
+template <class R, bool Two>
+__device__ void relax_point(const Dom<R>& D, const V3<R>& out, const V3<R>& f, const double* c1, const double* c2,
+                            const VB<R>* msf, const Slabs<R>& s, Ring r, int pos, int side, int b, int k, bool direct) {
+  int i, j;
+  if (!r.map(pos, side, b, i, j)) return;
+  const int sl = slab_of_side(side);
+  const R dtbc = R(D.dtbc);
+  auto BV = [&](int p, int bb) { return slab_val(s, sl, p, k, bb, dtbc); };
+  auto FV = [&](int ii, int jj) -> R {
+    const R x = Two ? f(ii, jj, 0) : f(ii, jj, k);
+    return c1 ? x * (R(c1[k]) * D.mut(ii, jj, 0) + R(c2[k])) : x;
+  };
+  R fls0, fls1, fls2, fls3, fls4;
+  fls0 = BV(pos, b) - FV(i, j);
+  if (side <= 1) {
+    const int im1 = i - 1 > 0 ? i - 1 : 0, ip1 = i + 1 < r.ibe ? i + 1 : r.ibe;
+    const int jin = side == 0 ? j + 1 : j - 1, jout = side == 0 ? j - 1 : j + 1;
+    fls1 = BV(im1, b) - FV(im1, j);
+    fls2 = BV(ip1, b) - FV(ip1, j);
+    fls3 = BV(i, b - 1) - FV(i, jout);
+    fls4 = BV(i, b + 1) - FV(i, jin);
+  } else {
+    const int iin = side == 2 ? i + 1 : i - 1, iout = side == 2 ? i - 1 : i + 1;
+    fls1 = BV(j - 1, b) - FV(i, j - 1);
+    fls2 = BV(j + 1, b) - FV(i, j + 1);
+    fls3 = BV(j, b - 1) - FV(iout, j);
+    fls4 = BV(j, b + 1) - FV(iin, j);
+  }
+  const R fcx = R(D.fcx[b]), gcx = R(D.gcx[b]);
+  const R val = fcx * fls0 - gcx * (fls1 + fls2 + fls3 + fls4 - R(4) * fls0);
+  if (Two) out(i, j, 0) += val;
+  else if (direct) out(i, j, k) = out(i, j, k) + fcx * fls0 - gcx * (fls1 + fls2 + fls3 + fls4 - R(4) * fls0);
+  else out(i, j, k) += msf ? val * (*msf)(i, j) : val;
+}
+
+// The ring kernels: thread (pos, k, 4 sides x rows) of a member; what = which operation
+enum RingOp { RO_RELAX_DRY = 0, RO_SPEC_DRY, RO_UPDATE_UV, RO_UPDATE_MU_T, RO_UPDATE_PH_W, RO_FINAL, RO_RELAX_Q, RO_SPEC_Q, RO_FLOW_DEP };
+template <class R>
+__global__ void __launch_bounds__(PX) k_ring(const Dom<R>* __restrict__ doms, BlockMap bm, int op, int rk) {
+  const Dom<R>* Dp;
+  int pos, k, sb;
+  if (!thread_index(doms, bm, RG_RING, Dp, pos, k, sb)) return;
+  const Dom<R>& D = *Dp;
+  const double dts = double(R(rk == 1 ? D.dt / 3.0 : D.dt / D.n_sound));
+  const int nx = D.nx, ny = D.ny, nz = D.nz;
+  const int side = sb % 4, row = sb / 4;
+  switch (op) {
+    case RO_RELAX_DRY: {  // LateralBC::relax_dry (:294-335): rows 1..3
+      if (row >= 3) return;
+      const int b = 1 + row;
+      if (k < nz) relax_point<R, false>(D, D.ru_tendf, D.ru, nullptr, nullptr, &D.msfuy, D.lbc_var[0], ring_for(nx, ny, 'u'), pos, side, b, k, false);
+      if (k < nz) relax_point<R, false>(D, D.rv_tendf, D.rv, nullptr, nullptr, &D.msfvx, D.lbc_var[1], ring_for(nx, ny, 'v'), pos, side, b, k, false);
+      relax_point<R, false>(D, D.ph_tendf, D.ph2, D.c1f, D.c2f, nullptr, D.lbc_var[3], ring_for(nx, ny, 'h'), pos, side, b, k, false);
+      if (k < nz) relax_point<R, false>(D, D.t_tendf, D.t2, D.c1h, D.c2h, nullptr, D.lbc_var[2], ring_for(nx, ny, 't'), pos, side, b, k, false);
+      if (k == 0) relax_point<R, true>(D, D.mu_tend, D.mu2, nullptr, nullptr, nullptr, D.lbc_var[4], ring_for(nx, ny, 'm'), pos, side, b, 0, false);
+      return;
+    }
+    case RO_SPEC_DRY: {  // spec_dry (:337-351): the spec zone b = 0 takes the boundary tendency
+      if (row != 0) return;
+      int i, j;
+      const int sl = slab_of_side(side);
+      if (k < nz && ring_for(nx, ny, 'u').map(pos, side, 0, i, j)) D.ru_tend(i, j, k) = slab_at(D.lbc_var[0], 1, sl, pos, k, 0);
+      if (k < nz && ring_for(nx, ny, 'v').map(pos, side, 0, i, j)) D.rv_tend(i, j, k) = slab_at(D.lbc_var[1], 1, sl, pos, k, 0);
+      if (ring_for(nx, ny, 'h').map(pos, side, 0, i, j)) D.ph_tend(i, j, k) = slab_at(D.lbc_var[3], 1, sl, pos, k, 0);
+      if (k < nz && ring_for(nx, ny, 't').map(pos, side, 0, i, j)) D.t_tend(i, j, k) = slab_at(D.lbc_var[2], 1, sl, pos, k, 0);
+      if (k == 0 && ring_for(nx, ny, 'm').map(pos, side, 0, i, j)) D.mu_tend(i, j, 0) = slab_at(D.lbc_var[4], 1, sl, pos, 0, 0);
+      return;
+    }
+    case RO_UPDATE_UV: {  // update_uv (:353-361)
+      if (row != 0 || k >= nz) return;
+      int i, j;
+      if (ring_for(nx, ny, 'u').map(pos, side, 0, i, j)) D.u2(i, j, k) += R(dts) * D.ru_tend(i, j, k);
+      if (ring_for(nx, ny, 'v').map(pos, side, 0, i, j)) D.v2(i, j, k) += R(dts) * D.rv_tend(i, j, k);
+      return;
+    }
+    case RO_UPDATE_MU_T: {  // update_mu_t (:363-372)
+      if (row != 0 || k >= nz) return;
+      int i, j;
+      if (!ring_for(nx, ny, 't').map(pos, side, 0, i, j)) return;
+      D.t2(i, j, k) += R(dts) * D.t_tend(i, j, k);
+      if (k == 0) {
+        D.mu2(i, j, 0) += R(dts) * D.mu_tend(i, j, 0);
+        D.muts(i, j, 0) += R(dts) * D.mu_tend(i, j, 0);
+      }
+      return;
+    }
+    case RO_UPDATE_PH_W: {  // update_ph_w (:374-386): KUpdatePh and KZeroGrad on w
+      if (row != 0) return;
+      int i, j;
+      const Ring r = ring_for(nx, ny, 'h');
+      if (!r.map(pos, side, 0, i, j)) return;
+      const R mu_old = D.muts(i, j, 0) - R(dts) * D.mu_tend(i, j, 0);
+      const R m_old = R(D.c1f[k]) * mu_old + R(D.c2f[k]), m_new = R(D.c1f[k]) * D.muts(i, j, 0) + R(D.c2f[k]);
+      D.ph2(i, j, k) = D.ph2(i, j, k) * m_old / m_new + R(dts) * D.ph_tend(i, j, k) / m_new + D.ph_save(i, j, k) * (m_old / m_new - R(1));
+      const int ic = i < 1 ? 1 : (i > r.ibe - 1 ? r.ibe - 1 : i);
+      const int jc = j < 1 ? 1 : (j > r.jbe - 1 ? r.jbe - 1 : j);
+      switch (side) {
+        case 0: D.w2(i, j, k) = D.w2(ic, 1, k); break;
+        case 1: D.w2(i, j, k) = D.w2(ic, r.jbe - 1, k); break;
+        case 2: D.w2(i, j, k) = D.w2(1, jc, k); break;
+        default: D.w2(i, j, k) = D.w2(r.ibe - 1, jc, k); break;
+      }
+      return;
+    }
+    case RO_FINAL: {  // final (:425-455)
+      if (row != 0) return;
+      int i, j;
+      const int sl = slab_of_side(side);
+      const R dtbc = R(D.dtbc);
+      if (k < nz && ring_for(nx, ny, 'u').map(pos, side, 0, i, j)) {
+        const R bval = slab_val(D.lbc_var[0], sl, pos, k, 0, dtbc);
+        D.u2(i, j, k) = D.msfuy(i, j) * bval / (R(D.c1h[k]) * D.muus(i, j, 0) + R(D.c2h[k]));
+      }
+      if (k < nz && ring_for(nx, ny, 'v').map(pos, side, 0, i, j)) {
+        const R bval = slab_val(D.lbc_var[1], sl, pos, k, 0, dtbc);
+        D.v2(i, j, k) = D.msfvx(i, j) * bval / (R(D.c1h[k]) * D.muvs(i, j, 0) + R(D.c2h[k]));
+      }
+      if (k < nz && ring_for(nx, ny, 't').map(pos, side, 0, i, j)) {
+        const R bval = slab_val(D.lbc_var[2], sl, pos, k, 0, dtbc);
+        D.t2(i, j, k) = R(1) * bval / (R(D.c1h[k]) * D.muts(i, j, 0) + R(D.c2h[k]));
+        for (int n = 0; n < D.n_scalars; ++n)
+          if (D.lbc_q[n].have) {
+            const R qb = slab_val(D.lbc_q[n], sl, pos, k, 0, dtbc);
+            D.q2[n](i, j, k) = R(1) * qb / (R(D.c1h[k]) * D.muts(i, j, 0) + R(D.c2h[k]));
+          }
+      }
+      if (ring_for(nx, ny, 'h').map(pos, side, 0, i, j)) {
+        const R bval = slab_val(D.lbc_var[3], sl, pos, k, 0, dtbc);
+        D.ph2(i, j, k) = R(1) * bval / (R(D.c1f[k]) * D.muts(i, j, 0) + R(D.c2f[k]));
+      }
+      if (k == 0 && ring_for(nx, ny, 'm').map(pos, side, 0, i, j)) {
+        const R bval = slab_val(D.lbc_var[4], sl, pos, 0, 0, dtbc);
+        D.mu2(i, j, 0) = R(1) * bval / R(1);
+      }
+      return;
+    }
+    case RO_RELAX_Q: {  // relax_scalars (:388-401)
+      if (row >= 3 || k >= nz) return;
+      for (int n = 0; n < D.n_scalars; ++n)
+        if (D.lbc_q[n].have)
+          relax_point<R, false>(D, D.qtf[n], D.q2[n], D.c1h, D.c2h, nullptr, D.lbc_q[n], ring_for(nx, ny, 'q'), pos, side, 1 + row, k, true);
+      return;
+    }
+    case RO_SPEC_Q: {  // spec_scalars (:403-414)
+      if (row != 0 || k >= nz) return;
+      int i, j;
+      if (!ring_for(nx, ny, 'q').map(pos, side, 0, i, j)) return;
+      for (int n = 0; n < D.n_scalars; ++n)
+        if (D.lbc_q[n].have) D.qtf[n](i, j, k) = slab_at(D.lbc_q[n], 1, slab_of_side(side), pos, k, 0);
+      return;
+    }
+    case RO_FLOW_DEP: {  // flow_dep (:416-423) on the scalars without boundary data
+      if (row != 0 || k >= nz) return;
+      int i, j;
+      const Ring r = ring_for(nx, ny, 'q');
+      if (!r.map(pos, side, 0, i, j)) return;
+      const int ic = i < 1 ? 1 : (i > r.ibe - 1 ? r.ibe - 1 : i);
+      const int jc = j < 1 ? 1 : (j > r.jbe - 1 ? r.jbe - 1 : j);
+      for (int n = 0; n < D.n_scalars; ++n) {
+        if (D.lbc_q[n].have) continue;
+        const V3<R>& f = D.q2[n];
+        switch (side) {
+          case 0: f(i, j, k) = D.rv_m(i, j, k) < R(0) ? f(ic, 1, k) : R(0); break;
+          case 1: f(i, j, k) = D.rv_m(i, j + 1, k) > R(0) ? f(ic, r.jbe - 1, k) : R(0); break;
+          case 2: f(i, j, k) = D.ru_m(i, j, k) < R(0) ? f(1, jc, k) : R(0); break;
+          default: f(i, j, k) = D.ru_m(i + 1, j, k) > R(0) ? f(r.ibe - 1, jc, k) : R(0); break;
+        }
+      }
+      return;
+    }
+  }
+}
+
+// LateralBC::advance_time (lateral_bc.hpp:58): dtbc += dt at the start of every step
+template <class R>
+__global__ void k_advance_time(Dom<R>* doms, int nmembers) {
+  const int m = blockIdx.x;
+  if (m < nmembers && threadIdx.x == 0 && doms[m].lbc) doms[m].dtbc += doms[m].dt;
+}
+
+}  // namespace cw

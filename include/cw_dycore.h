@@ -143,6 +143,25 @@ const char* cw_last_error(cw_handle* h);
 /* Kernel launches of the last cw_step call (the count this library issued). */
 int cw_launch_count(cw_handle* h, long long* out);
 
+/* CUDA-graph replay of the step (StepScope, src/core/backend.hpp:381-399): on by default. */
+int cw_set_graph(cw_handle* h, int on);
+
+/* ---- batches: several domains of uneven sizes in one handle, advanced together by the same launches
+ * (no reference counterpart: CPPWRF advances domains one after the other, src/cases/nest_driver.cpp:871).
+ * Members share the precision and the acoustic step count; member i's fields are addressed by the
+ * cw_member_* variants of the single-domain calls above (cw_upload is cw_member_upload of member 0). */
+int cw_batch_create(int n, const cw_grid* g, const cw_options* o, cw_handle** out);
+int cw_members(cw_handle* h, int* out);
+int cw_member_set_vertical(cw_handle* h, int member, const cw_vertical* v);
+int cw_member_upload(cw_handle* h, int member, int field, int n, const double* host, size_t count);
+int cw_member_download(cw_handle* h, int member, int field, int n, double* host, size_t count);
+int cw_member_field_layout(cw_handle* h, int member, int field, int n, cw_layout* out);
+int cw_member_set_lbc(cw_handle* h, int member, int var, int side, const double* values, const double* tends,
+                      size_t count);
+int cw_member_set_lbc_scalar(cw_handle* h, int member, int n, int side, const double* values, const double* tends,
+                             size_t count);
+int cw_member_set_lbc_time(cw_handle* h, int member, double dtbc);
+
 /* ---- host-side inputs ----
  * A cw_case holds one domain's complete input in host memory, in the same layouts as the handle's
  * fields: State, BaseState, the vertical arrays and the boundary slabs. The generators fill it from a
@@ -158,6 +177,7 @@ int cw_case_vertical(cw_case* c, cw_vertical* out);
 int cw_case_lbc(cw_case* c, int is_scalar, int var, int side, double** values, double** tends, size_t* count);
 int cw_case_lbc_time(cw_case* c, double* dtbc);
 int cw_upload_case(cw_handle* h, cw_case* c);
+int cw_member_upload_case(cw_handle* h, int member, cw_case* c);
 
 /* Idealized cases of CPPWRF (cases::make_case, src/cases/cases.cpp:90-192, and cases::initialize,
  * :224-287, with make_eta_levels "uniform_z", :194-201, and the base profiles of model.cpp:149-177).

@@ -1,0 +1,17 @@
+/* SPDX-License-Identifier: GPL-3.0-or-later
+ * TEST INFRASTRUCTURE ONLY: linked into _ref/ref_harness_own ahead of libm / libmvec, it binds the two
+ * pow entry points the reference's CPU build calls in calc_p_rho_phi (scalar libm pow and libmvec's
+ * 2-lane _ZGVbN2vv_pow, src/core/backend.hpp:118, :169-175) to cw_pow, the pow of the GPU path. The
+ * reference's every other operation is unchanged, so bit-identity with this build is a fair test of them. */
+#include <emmintrin.h>
+
+#include "../cppwrf_b200/csrc/cw_pow.h"
+
+double pow(double x, double y) { return cw_pow(x, y); }
+
+__m128d _ZGVbN2vv_pow(__m128d x, __m128d y) {
+  double a[2], b[2];
+  _mm_storeu_pd(a, x);
+  _mm_storeu_pd(b, y);
+  return _mm_set_pd(cw_pow(a[1], b[1]), cw_pow(a[0], b[0]));
+}

@@ -1,0 +1,93 @@
+# SPDX-License-Identifier: GPL-3.0-or-later
+"""Runs the reference's own compiled dycore (oracle/_ref/ref_harness*, built from the CPPWRF sources by
+oracle/Makefile) on a capi.Case and returns every field. Test infrastructure only."""
+import ctypes as C
+import os
+import struct
+import subprocess
+import tempfile
+
+import numpy as np
+
+from cppwrf_b200 import capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+REFERENCE_SRC = os.environ.get("CPPWRF_REFERENCE", "/root/reference")
+
+
+def available():
+    return os.path.isdir(os.path.join(REFERENCE_SRC, "src", "dyn")) or os.path.exists(os.path.join(REF_DIR, "ref_harness"))
+
+
+def build():
+    if not os.path.exists(os.path.join(REF_DIR, "ref_harness_own")):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REFERENCE_SRC}"], check=True)
+
+
+def _vertical_arrays(case):
+    v = case.vertical()
+    nz = case.g.nz
+    arrs = []
+    for name in ("znu", "dnw", "rdnw", "c1h", "c2h", "c3h", "c4h"):
+        arrs.append(np.ctypeslib.as_array(getattr(v, name), shape=(nz,)))
+    for name in ("znw", "dn", "rdn", "fnm", "fnp", "c1f", "c2f", "c3f", "c4f"):
+        arrs.append(np.ctypeslib.as_array(getattr(v, name), shape=(nz + 1,)))
+    for name in ("u_base", "v_base", "t_base", "qv_base_1d", "z_base"):
+        arrs.append(np.ctypeslib.as_array(getattr(v, name), shape=(nz,)))
+    scal = [v.cf1, v.cf2, v.cf3, v.cfn, v.cfn1, v.rdx, v.rdy, v.p_top, v.t0]
+    return arrs, scal
+
+
+def run(case, nsteps, own_pow=True):
+    """{field name: whole allocation} of the reference after nsteps (Q_* keyed 'Q_2:n')."""
+    build()
+    exe = os.path.join(REF_DIR, "ref_harness_own" if own_pow else "ref_harness")
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(bytes(case.g))
+            f.write(bytes(case.o))
+            arrs, scal = _vertical_arrays(case)
+            for a in arrs:
+                f.write(np.ascontiguousarray(a, dtype="<f8").tobytes())
+            f.write(struct.pack("<9d", *scal))
+            names = [n for n in capi.FIELDS if not n.startswith("Q_")]
+            for name in names:
+                a, L = case.field(name)
+                f.write(struct.pack("<q", a.size))
+                f.write(a.astype("<f8").tobytes())
+            for n in range(case.o.n_scalars):
+                for name in ("Q_1", "Q_2", "Q_TENDF"):
+                    a, L = case.field(name, n)
+                    f.write(struct.pack("<q", a.size))
+                    f.write(a.astype("<f8").tobytes())
+            if case.o.lbc:
+                for var in range(5):
+                    for side in range(4):
+                        vals, tends = case.lbc(var, side)
+                        f.write(struct.pack("<q", vals.size))
+                        f.write(vals.astype("<f8").tobytes())
+                        f.write(tends.astype("<f8").tobytes())
+                for n in range(case.o.n_scalars):
+                    for side in range(4):
+                        r = case.lbc(n, side, scalar=True)
+                        if r is None:
+                            f.write(struct.pack("<q", 0))
+                            continue
+                        f.write(struct.pack("<q", r[0].size))
+                        f.write(r[0].astype("<f8").tobytes())
+                        f.write(r[1].astype("<f8").tobytes())
+                f.write(struct.pack("<d", case.lbc_time()))
+            f.write(struct.pack("<i", nsteps))
+        subprocess.run([exe, fin, fout], check=True)
+        out = {}
+        with open(fout, "rb") as f:
+            for name in names:
+                (n,) = struct.unpack("<q", f.read(8))
+                out[name] = np.frombuffer(f.read(8 * n), dtype="<f8").copy()
+            for q in range(case.o.n_scalars):
+                for name in ("Q_1", "Q_2", "Q_TENDF"):
+                    (n,) = struct.unpack("<q", f.read(8))
+                    out[f"{name}:{q}"] = np.frombuffer(f.read(8 * n), dtype="<f8").copy()
+        return out

@@ -1,0 +1,36 @@
+# SPDX-License-Identifier: GPL-3.0-or-later
+"""Case definitions shared by the tests: the reference's regression configurations and small variants."""
+import json
+import os
+
+from cppwrf_b200 import capi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = json.load(open(os.path.join(HERE, "golden", "reference_snapshots.json")))
+KINDS = {"straka": capi.STRAKA, "warm_bubble": capi.WARM_BUBBLE, "igw": capi.IGW, "rest_state": capi.REST_STATE}
+BCS = {"periodic": capi.PERIODIC, "symmetric": capi.SYMMETRIC}
+
+
+def ideal_case(cfg, lib=None, u0=None, **opt):
+    """A capi.Case of an ideal configuration dict (tests/golden/reference_snapshots.json style)."""
+    g = capi.grid(cfg["nx"], cfg["ny"], cfg["nz"], cfg["dx"], cfg["dt"], cfg["ztop"], dy=cfg["dy"],
+                  bc_x=BCS[cfg["bc_x"]], bc_y=BCS[cfg["bc_y"]])
+    o = capi.default_options(lib, khdif=cfg["khdif"], kvdif=cfg["kvdif"], pr_inv=cfg["pr_inv"])
+    o.diff_opt = 1 if (cfg["khdif"] > 0 or cfg["kvdif"] > 0) else 0
+    for k, v in opt.items():
+        setattr(o, k, v)
+    kw = {} if u0 is None else {"u0": u0}
+    return capi.Case(g, o, lib).gen_ideal(KINDS[cfg["kind"]], **kw)
+
+
+def golden_config(name):
+    return dict(GOLDEN["cases"][name]["config"])
+
+
+# small variants for quick parity runs (same physics as the goldens, fewer points)
+SMALL = {
+    "straka_small": dict(golden_config("straka"), nx=64, nz=32, ztop=3200.0, run_time=3.0),
+    "warm_bubble_small": dict(golden_config("warm_bubble"), nx=48, nz=40, ztop=4000.0, run_time=3.0),
+    "igw_small": dict(golden_config("igw"), nx=60, run_time=18.0),
+    "rest_state_small": dict(golden_config("rest_state"), nx=12, ny=10, nz=16, run_time=30.0),
+}

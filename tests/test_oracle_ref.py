@@ -1,0 +1,76 @@
+# SPDX-License-Identifier: GPL-3.0-or-later
+"""Pins the oracle against the reference's own CPU FP64 dycore compiled from its sources (oracle/_ref), on
+the paths the regression goldens do not reach: terrain, the hybrid coordinate, moist species with the
+positive-definite limiter, specified lateral boundaries (relaxation, spec zone, flow-dependent scalars),
+constant-K diffusion in 3-D, symmetric walls in 3-D. Both sides take pow from cw_pow (the reference
+through symbol interposition), so the comparison is bit for bit. Runs only where the reference sources
+are present (this build's container); the fixtures in tests/golden keep the pin on other machines."""
+import numpy as np
+import pytest
+
+import _oracle
+import _refdump
+import cases
+from cppwrf_b200 import capi
+
+pytestmark = pytest.mark.skipif(not _refdump.available(), reason="reference sources / oracle/_ref not present")
+
+
+def lam_case(nx=24, ny=20, nz=14, seed=3, n_moist=5, n_scalars=5, diff=False, hybrid_opt=2):
+    g = capi.grid(nx, ny, nz, 15000.0, 90.0, 0.0, dy=15000.0, p_top=5000.0, bc_x=capi.SPECIFIED, bc_y=capi.SPECIFIED)
+    o = capi.default_options(None, flat=0, n_moist=n_moist, n_scalars=n_scalars, lbc=1, time_step_sound=4)
+    if diff:
+        o.diff_opt, o.khdif, o.kvdif, o.pr_inv = 1, 3000.0, 1.0, 3.0
+    return capi.Case(g, o).gen_lam(seed=seed, hybrid_opt=hybrid_opt)
+
+
+def compare(orc, ref, case):
+    bad = []
+    for name in [n for n in capi.FIELDS if not n.startswith("Q_")]:
+        a = orc.array(name)
+        b = ref[name]
+        if b.size == 0:
+            continue
+        if not np.array_equal(a.view(np.uint64), b.view(np.uint64)):
+            d = np.nonzero(a.view(np.uint64) != b.view(np.uint64))[0]
+            bad.append(f"{name}: {d.size} differ, first {d[0]}: oracle {a[d[0]]!r} ref {b[d[0]]!r}")
+    for n in range(case.o.n_scalars):
+        for name in ("Q_1", "Q_2", "Q_TENDF"):
+            a, b = orc.array(name, n), ref[f"{name}:{n}"]
+            if not np.array_equal(a.view(np.uint64), b.view(np.uint64)):
+                d = np.nonzero(a.view(np.uint64) != b.view(np.uint64))[0]
+                bad.append(f"{name}[{n}]: {d.size} differ, first {d[0]}: oracle {a[d[0]]!r} ref {b[d[0]]!r}")
+    return bad
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(diff=True), dict(hybrid_opt=0, seed=5), dict(n_moist=2, n_scalars=3)],
+                         ids=["lam", "lam_diffusion", "lam_sigma", "lam_tracer"])
+def test_oracle_equals_reference_lam(kw):
+    case = lam_case(**kw)
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_OWN)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=True)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)
+
+
+def test_oracle_equals_reference_3d_symmetric_diffusion():
+    cfg = dict(cases.golden_config("rest_state"), nx=14, ny=12, nz=12, bc_x="symmetric", bc_y="symmetric",
+               khdif=200.0, kvdif=5.0, run_time=40.0)
+    case = cases.ideal_case(cfg, u0=3.0)
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_OWN)
+    orc.step(4)
+    ref = _refdump.run(case, 4, own_pow=True)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)
+
+
+def test_oracle_equals_reference_default_glibc_pow():
+    """The oracle with glibc's pow (lane rule) against the unmodified reference build."""
+    cfg = dict(cases.SMALL["straka_small"])
+    case = cases.ideal_case(cfg)
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_GLIBC)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=False)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)
