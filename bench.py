@@ -1,0 +1,338 @@
+# SPDX-License-Identifier: GPL-3.0-or-later
+"""Benchmark of the B200 RK3 dynamical core: grid-point-steps/s of the 3-D limited-area workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed] [--impl ours|reference]
+
+Workload (one domain per GPU rank, weak scaling): 119 x 89 x 44 mass points, dx = dy = 15 km, dt = 90 s,
+4 acoustic substeps, hybrid sigma-pressure coordinate (etac 0.2), model top 50 hPa, seeded terrain
+(1.5 km hill + k^-3 orography up to 800 m), 5 moist species (qv qc qr qi qs) advected positive-definite
+at rk 3, specified lateral boundaries (5 rows, relaxation toward the initial state). Every input is
+synthetic (cw_gen_lam, seeded). The step's working set (~110 fields of 5.4 MB) is far larger than the
+126 MB L2, so no flush is needed between steps.
+
+One JSON line on rank 0: value = all ranks' grid points x steps / max over ranks of the device time of the
+K timed steps (CUDA events on the handle's stream), e2e = the same through the C ABI with the prognostic
+state copied from / to pinned host memory every step, roofline of the dominant kernel (per-kernel CUDA
+events, algorithmic bytes below), and the reference CPU build timed on this host.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(nx=119, ny=89, nz=44, dx=15000.0, dt=90.0, time_step_sound=4, p_top=5000.0, n_moist=5,
+                hybrid_opt=2, etac=0.2)
+METRIC = "RK3 grid-point-steps/s (FP64-exact vs mixed, batched); served p50/p99 latency"
+UNIT = "grid-point-steps/s"
+# the state a step reads and writes that persists between steps (the e2e copies, per step, both ways)
+PROGNOSTIC = ["U_2", "V_2", "W_2", "T_2", "PH_2", "MU_2", "P", "AL"]
+
+
+def make_case(capi, precision, seed=1):
+    w = WORKLOAD
+    g = capi.grid(w["nx"], w["ny"], w["nz"], w["dx"], w["dt"], 0.0, dy=w["dx"], p_top=w["p_top"],
+                  bc_x=capi.SPECIFIED, bc_y=capi.SPECIFIED)
+    o = capi.default_options(None, flat=0, n_moist=w["n_moist"], n_scalars=w["n_moist"], lbc=1,
+                             time_step_sound=w["time_step_sound"], precision=precision)
+    return capi.Case(g, o).gen_lam(seed=seed, hybrid_opt=w["hybrid_opt"], etac=w["etac"])
+
+
+# Algorithmic bytes per mass point of one launch: the distinct 3-D arrays the kernel must read and write,
+# each once (staggered extents counted as mass points), for the workload's options (terrain: 3-D base
+# fields; 5 moist species; specified boundaries: the held tendencies are read).
+ALG_ARRAYS = {
+    "k_ls_prep": 7 + 5 + 9,   # u2 v2 w2 al ph2 alb phb + 5 q | ru rv rw alt php ww cqu cqv cqw
+    "k_tend": 24 + 5,         # u2 v2 w2 t2 ph2 ru rv rw ww p al alt php pb phb 5 tendf cqu cqv cqw hd | 5 tend
+    "k_ss_prep": 15 + 18,     # u2 v2 w2 t2 ph2 u1 v1 w1 t1 ph1 ww p alt pb cqw | 5 state 5 saves ww1 c2a al p pm1 a alpha gamma
+    "k_uv": 12 + 2,           # u2 v2 ru_tend rv_tend p al alt ph2 php pb cqu cqv | u2 v2
+    "k_ac": 22 + 11,          # u2 v2 u_save v_save ww1 ww_m ru_m rv_m t2 t_save t_tend w2 ph2 rw_tend ph_tend
+                              # ph_save phb c2a alt a alpha gamma | ww ww_m ru_m rv_m t2 t_2save w2 ph2 w_rhs t2a (+)
+    "k_finish": 15 + 8,       # u2 v2 w2 t2 ph2 ww 5 saves ww1 hd alb pb | u2 v2 w2 t2 ph2 ww al p
+    "k_wprho": 9 + 3,         # ph2 alt t2 t_save c2a pm1 (+ mu muts 2-D) | al p pm1
+    "k_q_update": 3 + 3 + 1,  # per species: q2 q1 qtf + ru_m rv_m ww_m | qn
+    "k_q_update_pd": 4 + 3 + 1,
+    "k_q_scale_pd": 2 + 3 + 1,
+}
+
+
+def clocks_sampler(device):
+    """Samples SM clocks and throttle reasons with nvidia-smi every 200 ms until stopped."""
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+    try:
+        p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200",
+                              "-i", str(device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except OSError:
+        return None
+    rows = []
+
+    def rd():
+        for line in p.stdout:
+            rows.append([x.strip() for x in line.split(",")])
+
+    t = threading.Thread(target=rd, daemon=True)
+    t.start()
+    return p, rows
+
+
+def clocks_summary(sampler):
+    if sampler is None:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+    p, rows = sampler
+    p.terminate()
+    try:
+        p.wait(timeout=5)
+    except subprocess.TimeoutExpired:
+        p.kill()
+    sm, smax, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for r in rows:
+        try:
+            sm.append(float(r[1]))
+            smax.append(float(r[2]))
+        except (ValueError, IndexError):
+            continue
+        for n, v in zip(names, r[5:9]):
+            if v.strip().lower() == "active":
+                reasons.add(n)
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    for path in (os.path.join(ROOT, "MEASURED_PEAKS.json"),):
+        try:
+            d = json.load(open(path))
+            return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+        except (OSError, KeyError, ValueError):
+            pass
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def ncu_traffic(kernel, workload_tag):
+    """DRAM bytes per launch of kernel from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload_tag}.md")
+    try:
+        for line in open(path):
+            m = re.match(r"\s*traffic_bytes_per_launch:\s*([0-9.eE+]+)", line)
+            if m:
+                return float(m.group(1))
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(capi, seconds_target=15.0):
+    """The reference's own CPU FP64 build (oracle/_ref) on a bounded sample of the workload, all host threads;
+    falls back to the oracle port (one thread) when the reference build is absent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    case = make_case(capi, capi.FP64)
+    pts = WORKLOAD["nx"] * WORKLOAD["ny"] * WORKLOAD["nz"]
+    ncores = os.cpu_count() or 1
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if os.path.exists(exe):
+        import refdump
+        t1 = refdump.time_steps(case, 1, threads=ncores)
+        n = max(2, min(200, int(seconds_target / max(t1, 1e-3))))
+        t = refdump.time_steps(case, n, threads=ncores)
+        return {"value": pts * n / t, "unit": UNIT, "cores": ncores, "kind": "reference",
+                "sample": f"{n} RK3 steps of the {WORKLOAD['nx']}x{WORKLOAD['ny']}x{WORKLOAD['nz']} workload, "
+                          f"reference CPU FP64 build (oracle/_ref, OpenMP {ncores} threads), step loop only"}
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle
+    orc = _oracle.Oracle(case)
+    t0 = time.perf_counter()
+    orc.step(1)
+    t1 = time.perf_counter() - t0
+    n = max(1, min(50, int(seconds_target / max(t1, 1e-3))))
+    t0 = time.perf_counter()
+    orc.step(n)
+    t = time.perf_counter() - t0
+    return {"value": pts * n / t, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n} RK3 steps of the workload, the oracle (C restatement, 1 thread)"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    from cppwrf_b200 import capi
+    cb = cpu_baseline(capi, seconds_target=20.0)
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "lam_119x89x44_fp64", **WORKLOAD}, "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line["ms_per_step"] = 1000.0 * WORKLOAD["nx"] * WORKLOAD["ny"] * WORKLOAD["nz"] / cb["value"]
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import torch
+    import torch.distributed as dist
+
+    from cppwrf_b200 import Domain, capi
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    lib = capi.load()
+    lib.cw_use_device(local)
+    prec = capi.MIXED if args.precision == "mixed" else capi.FP64
+    case = make_case(capi, prec, seed=1 + rank)
+    dom = Domain(case.g, case.o).upload_case(case)
+    stream = torch.cuda.Stream()  # a dedicated stream: the handle launches on it, the events are recorded on it
+    lib.cw_set_stream(dom.h, C.c_void_p(stream.cuda_stream))
+    pts = WORKLOAD["nx"] * WORKLOAD["ny"] * WORKLOAD["nz"]
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up (the first step captures the CUDA graph)
+    dom.step(args.warmup)
+    torch.cuda.synchronize()
+    sampler = clocks_sampler(local)
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    dom.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clocks_summary(sampler)
+    ms = e0.elapsed_time(e1)
+    launches = dom.launches()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * pts * args.steps / (ms / 1000.0)
+
+    # e2e: the prognostic state from pinned host memory, one step, the state back, every step
+    host = {}
+    for name in PROGNOSTIC:
+        L = dom.layout(name)
+        host[name] = torch.empty(L.total, dtype=torch.float64).pin_memory()
+        host[name].copy_(torch.from_numpy(dom.field(name)))
+    qhost = []
+    for n in range(case.o.n_scalars):
+        L = dom.layout("Q_2", n)
+        t = torch.empty(L.total, dtype=torch.float64).pin_memory()
+        t.copy_(torch.from_numpy(dom.field("Q_2", n)))
+        qhost.append(t)
+    ebytes = sum(t.numel() * 8 for t in host.values()) + sum(t.numel() * 8 for t in qhost)
+    dp = C.POINTER(C.c_double)
+    n_e2e = max(3, min(args.steps, 20))
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for _ in range(n_e2e):
+        for name, t in host.items():
+            lib.cw_upload(dom.h, capi.F[name], 0, C.cast(t.data_ptr(), dp), t.numel())
+        for n, t in enumerate(qhost):
+            lib.cw_upload(dom.h, capi.F["Q_2"], n, C.cast(t.data_ptr(), dp), t.numel())
+        lib.cw_step(dom.h, 1)
+        for name, t in host.items():
+            lib.cw_download(dom.h, capi.F[name], 0, C.cast(t.data_ptr(), dp), t.numel())
+        for n, t in enumerate(qhost):
+            lib.cw_download(dom.h, capi.F["Q_2"], n, C.cast(t.data_ptr(), dp), t.numel())
+    g1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    ems = max(g0.elapsed_time(g1), wall * 1000.0)
+    if world > 1:
+        t = torch.tensor([ems], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+    e2e = world * pts * n_e2e / (ems / 1000.0)
+
+    # per-kernel device time (eager steps with events around each launch); dominant kernel's roofline
+    nk = C.c_int()
+    lib.cw_profile(dom.h, 2, C.byref(nk))
+    table = []
+    for k in range(nk.value):
+        nm = C.create_string_buffer(64)
+        kms, kn = C.c_double(), C.c_longlong()
+        lib.cw_profile_entry(dom.h, k, nm, 64, C.byref(kms), C.byref(kn))
+        table.append((nm.value.decode(), kms.value, kn.value))
+    table.sort(key=lambda r: -r[1])
+    total_ms = sum(r[1] for r in table)
+    dom_name, dom_ms, dom_n = next((r for r in table if r[0] in ALG_ARRAYS), table[0])
+    esz = 4 if prec == capi.MIXED else 8
+    arrays = ALG_ARRAYS.get(dom_name, 0) * (WORKLOAD["n_moist"] if dom_name.startswith("k_q_") else 1)
+    alg_bytes = arrays * pts * esz
+    avg_s = dom_ms / 1000.0 / dom_n
+    peak, peak_src = measured_peak()
+    achieved = alg_bytes / avg_s / 1e9
+    tag = f"lam119x89x44_{args.precision}"
+    traffic = ncu_traffic(dom_name, tag)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": dom_name, "algorithmic_bytes_per_launch": alg_bytes,
+                "avg_launch_ms": dom_ms / dom_n, "peak_source": peak_src,
+                "kernel_share": {r[0]: round(r[1] / total_ms, 4) for r in table[:8]}}
+    # the whole step against the per-grid-point traffic model (4 416 B FP64 / 2 208 B FP32 per point-step)
+    step_bytes = 4416 if prec == capi.FP64 else 2208
+    step_roofline = {"bytes_per_gp_step": step_bytes, "achieved_GBps": value / world * step_bytes / 1e9,
+                     "frac": value / world * step_bytes / 1e9 / peak}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec == capi.FP64 else "f32+f64",
+            "data": "synthetic (cw_gen_lam, seeded)",
+            "config": {"workload": f"lam_119x89x44_{args.precision}", **WORKLOAD,
+                       "moist_species": "qv qc qr qi qs (PD at rk 3)", "lbc": "specified, width 5",
+                       "parallelism": f"one domain per GPU x{world}",
+                       "l2": "inputs larger than L2: ~110 fields x 5.4 MB per step, no flush"},
+            "clocks": clocks, "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": ebytes,
+                                      "d2h_bytes_per_step": ebytes, "steps": n_e2e},
+            "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roofline}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(capi)
+        except Exception as e:  # noqa: BLE001 - reported, not fatal
+            line["cpu_baseline"] = {"value": None, "error": str(e)}
+    dom.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -92,3 +92,57 @@ class Domain:
 
     def set_graph(self, on):
         self.lib.cw_set_graph(self.h, 1 if on else 0)
+
+
+class Batch:
+    """Several domains of uneven sizes advanced together: every kernel launch covers all members
+    (one handle, cw_batch_create). Members share the precision and the acoustic step count."""
+
+    def __init__(self, grids, options, lib=None):
+        self.lib = lib or capi.load()
+        n = len(grids)
+        self.grids, self.options = list(grids), list(options)
+        ga = (Grid * n)(*grids)
+        oa = (Options * n)(*options)
+        self.h = C.c_void_p()
+        rc = self.lib.cw_batch_create(n, ga, oa, C.byref(self.h))
+        _check(self.lib, None, rc, "cw_batch_create")
+        self.n = n
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.lib.cw_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def upload_case(self, member, case):
+        _check(self.lib, self.h, self.lib.cw_member_upload_case(self.h, member, case.h), "cw_member_upload_case")
+        return self
+
+    def step(self, n=1):
+        _check(self.lib, self.h, self.lib.cw_step(self.h, n), "cw_step")
+        return self
+
+    def sync(self):
+        _check(self.lib, self.h, self.lib.cw_sync(self.h), "cw_sync")
+
+    def launches(self):
+        v = C.c_longlong()
+        self.lib.cw_launch_count(self.h, C.byref(v))
+        return v.value
+
+    def layout(self, member, name, n=0):
+        L = Layout()
+        rc = self.lib.cw_member_field_layout(self.h, member, F[name], n, C.byref(L))
+        _check(self.lib, self.h, rc, "cw_member_field_layout")
+        return L
+
+    def field(self, member, name, n=0):
+        L = self.layout(member, name, n)
+        out = np.empty(L.total, dtype=np.float64)
+        rc = self.lib.cw_member_download(self.h, member, F[name], n, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                         out.size)
+        _check(self.lib, self.h, rc, "cw_member_download")
+        return out

@@ -13,6 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "lib", "libcw_dycore.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+CXX = os.environ.get("CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++20", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off",
          "-Xptxas", "-warn-spills", "--expt-relaxed-constexpr"]
@@ -26,8 +27,7 @@ def build(verbose=False):
         obj = os.path.join(HERE, "lib", os.path.splitext(src)[0] + ".o")
         cmd = [NVCC] + ARCH + FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
         if src.endswith(".cpp"):
-            cmd = [NVCC, "-x", "c++", "-std=c++20", "-O3", "-Xcompiler", "-fPIC,-ffp-contract=off", "-c",
-                   os.path.join(CSRC, src), "-o", obj]
+            cmd = [CXX, "-std=c++20", "-O3", "-fPIC", "-ffp-contract=off", "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

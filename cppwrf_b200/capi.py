@@ -131,6 +131,16 @@ def load(path=None):
         "cw_last_error": (C.c_char_p, [vp]),
         "cw_launch_count": (i, [vp, C.POINTER(C.c_longlong)]),
         "cw_upload_case": (i, [vp, vp]),
+        "cw_member_upload_case": (i, [vp, i, vp]),
+        "cw_profile": (i, [vp, i, ip]),
+        "cw_profile_entry": (i, [vp, i, C.c_char_p, i, dp, C.POINTER(C.c_longlong)]),
+        "cw_use_device": (i, [i]),
+        "cw_set_graph": (i, [vp, i]),
+        "cw_batch_create": (i, [i, C.POINTER(Grid), C.POINTER(Options), C.POINTER(vp)]),
+        "cw_members": (i, [vp, ip]),
+        "cw_member_upload": (i, [vp, i, i, i, dp, sz]),
+        "cw_member_download": (i, [vp, i, i, i, dp, sz]),
+        "cw_member_field_layout": (i, [vp, i, i, i, C.POINTER(Layout)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name, None)
@@ -156,9 +166,14 @@ def grid(nx, ny, nz, dx, dt, ztop=0.0, dy=None, p_top=0.0, bc_x=PERIODIC, bc_y=P
     return Grid(nx, ny, nz, dx, dx if dy is None else dy, dt, ztop, p_top, bc_x, bc_y)
 
 
-def as_array(ptr, n):
-    """A numpy view of n doubles at a C pointer (no copy)."""
-    return np.ctypeslib.as_array(ptr, shape=(n,))
+def as_array(ptr, n, owner=None):
+    """A numpy view of n doubles at a C pointer (no copy); the view keeps `owner` (the object whose
+    destruction frees the memory) alive."""
+    if n == 0:
+        return np.zeros(0)
+    buf = (C.c_double * n).from_address(C.addressof(ptr.contents))
+    buf._owner = owner
+    return np.frombuffer(buf, dtype=np.float64)
 
 
 class Case:
@@ -183,7 +198,7 @@ class Case:
         rc = self.lib.cw_case_field(self.h, F[name], n, C.byref(p), C.byref(L))
         if rc != 0:
             raise KeyError(name)
-        return as_array(p, L.total), L
+        return as_array(p, L.total, self), L
 
     def vertical(self):
         v = Vertical()
@@ -195,7 +210,7 @@ class Case:
         rc = self.lib.cw_case_lbc(self.h, 1 if scalar else 0, var, side, C.byref(vals), C.byref(tends), C.byref(cnt))
         if rc != 0:
             return None
-        return as_array(vals, cnt.value), as_array(tends, cnt.value)
+        return as_array(vals, cnt.value, self), as_array(tends, cnt.value, self)
 
     def lbc_time(self):
         t = C.c_double()

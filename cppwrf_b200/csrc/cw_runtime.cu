@@ -21,7 +21,7 @@
 #include <vector>
 
 #include "cw_fields.hpp"
-#include "kernels_ac.cuh"
+#include "kernels_cb.cuh"
 
 namespace cw {
 
@@ -99,6 +99,8 @@ struct cw_handle {
   DevTables<float> t32;
   BlockMap bmap[6]{};
   int total_blocks[6]{};
+  int nzmax = 0;
+  size_t cb_level_bytes = 0;  // one shared level array of a column block: (nz + 2) x CX doubles
   // halo sets of the fill points
   enum { H_MU1, H_PREP0, H_PREP1, H_SS0, H_UV, H_AC, H_POST, H_FIN, H_Q1PD, H_SCPD, H_Q2, H_END_P, H_WS0, H_WS1, H_N };
   HaloSetHost hs[H_N];
@@ -118,6 +120,12 @@ struct cw_handle {
   long long launches_last = 0;   // launches of the last cw_step call
   std::string err;
   std::vector<void*> extra;      // other device allocations
+  // per-kernel timing of eager steps (cw_profile): events around each launch
+  bool profiling = false;
+  std::vector<std::pair<const char*, std::pair<cudaEvent_t, cudaEvent_t>>> prof_ev;
+  std::vector<std::string> prof_names;
+  std::vector<double> prof_ms;
+  std::vector<long long> prof_n;
 };
 
 namespace {
@@ -353,6 +361,9 @@ void upload_tables(cw_handle* h) {
 }
 
 void build_blockmaps(cw_handle* h) {
+  h->nzmax = 0;
+  for (const Member& M : h->m) h->nzmax = std::max(h->nzmax, M.g.nz);
+  h->cb_level_bytes = size_t(h->nzmax + 2) * CX * sizeof(double);
   for (int kind = 0; kind < 6; ++kind) {
     BlockMap& bm = h->bmap[kind];
     bm.n = int(h->m.size());
@@ -499,9 +510,19 @@ void build_copies(cw_handle* h) {
 struct Launcher {
   cw_handle* h;
   long long count = 0;
+  cudaEvent_t ev0 = nullptr;
+  void begin(const char* name) {
+    if (!h->profiling) return;
+    cudaEvent_t a, b;
+    CW_CUDA(cudaEventCreate(&a));
+    CW_CUDA(cudaEventCreate(&b));
+    CW_CUDA(cudaEventRecord(a, h->stream));
+    h->prof_ev.push_back({name, {a, b}});
+  }
   void check() {
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) throw std::runtime_error(std::string("kernel launch: ") + cudaGetErrorString(e));
+    if (h->profiling) CW_CUDA(cudaEventRecord(h->prof_ev.back().second.second, h->stream));
     ++count;
   }
   void halo(int set) {
@@ -509,9 +530,11 @@ struct Launcher {
     if (s.total == 0) return;
     const int bs = 256;
     const unsigned nb = unsigned((s.total + bs - 1) / bs);
+    begin("k_halo");
     k_halo<<<nb, bs, 0, h->stream>>>(s, 0);
     check();
     if (s.has_oddface) {
+      begin("k_halo");
       k_halo<<<nb, bs, 0, h->stream>>>(s, 1);
       check();
     }
@@ -519,15 +542,38 @@ struct Launcher {
   void copy_list(CopyDesc* d, long long* sd, size_t n, long long total) {
     if (!total) return;
     const int bs = 256;
+    begin("k_copy");
     k_copy<<<unsigned((total + bs - 1) / bs), bs, 0, h->stream>>>(d, int(n), sd);
     check();
   }
+  // a point kernel over the index range kind
   template <class R, class K, class... Args>
-  void run(int kind, K kern, const Dom<R>* doms, Args... args) {
+  void run(const char* name, int kind, K kern, const Dom<R>* doms, Args... args) {
     const int nb = h->total_blocks[kind];
     if (nb == 0) return;
-    const int bs = is_column(kind) ? CX : PX;
-    kern<<<nb, bs, 0, h->stream>>>(doms, h->bmap[kind], args...);
+    begin(name);
+    kern<<<nb, PX, 0, h->stream>>>(doms, h->bmap[kind], args...);
+    check();
+  }
+  // a point kernel over the index range kind, once per species (blockIdx.y)
+  template <class R, class K, class... Args>
+  void run_q(const char* name, int kind, int nq, K kern, const Dom<R>* doms, Args... args) {
+    const int nb = h->total_blocks[kind];
+    if (nb == 0 || nq == 0) return;
+    begin(name);
+    kern<<<dim3(nb, nq), PX, 0, h->stream>>>(doms, h->bmap[kind], args...);
+    check();
+  }
+  // a column-block kernel using `arrays` shared level arrays
+  template <class R, class K, class... Args>
+  void run_cb(const char* name, int kind, int arrays, K kern, const Dom<R>* doms, Args... args) {
+    static_assert(CX == 32, "a column block's lanes are one warp");
+    const int nb = h->total_blocks[kind];
+    if (nb == 0) return;
+    begin(name);
+    const size_t smem = size_t(arrays) * h->cb_level_bytes;
+    CW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    kern<<<nb, dim3(CX, CNW), smem, h->stream>>>(doms, h->bmap[kind], args...);
     check();
   }
 };
@@ -537,7 +583,9 @@ void enqueue_step(cw_handle* h, Launcher& L, DevTables<R>& T) {
   const Dom<R>* d = T.doms;
   const Member& M0 = h->m[0];
   bool lbc = false, terrain = false, scalars = false, any_pd = false;
+  int nq = 0;  // the most species of a member
   for (const Member& M : h->m) {
+    nq = std::max(nq, M.o.n_scalars);
     lbc |= M.o.lbc != 0;
     terrain |= !M.o.flat;
     scalars |= M.o.n_scalars > 0;
@@ -546,6 +594,7 @@ void enqueue_step(cw_handle* h, Launcher& L, DevTables<R>& T) {
   }
   const int n_sound = M0.n_sound;
   if (lbc) {
+    L.begin("k_advance_time");
     k_advance_time<R><<<unsigned(h->m.size()), 1, 0, h->stream>>>(T.doms, int(h->m.size()));
     L.check();
   }
@@ -554,59 +603,48 @@ void enqueue_step(cw_handle* h, Launcher& L, DevTables<R>& T) {
   for (int rk = 1; rk <= 3; ++rk) {
     const int ns = rk == 1 ? 1 : (rk == 2 ? n_sound / 2 : n_sound);
     L.halo(cw_handle::H_PREP0);
-    L.run(RG_COLS_STAG, k_ls_prep<R>, d);
+    L.run_cb("k_ls_prep", RG_COLS_STAG, 1, k_ls_prep<R>, d);
     L.halo(cw_handle::H_PREP1);
-    if (rk == 1) L.run(RG_STAG, k_tendf_rk1<R>, d);
-    if (rk == 1 && lbc) L.run(RG_RING, k_ring<R>, d, int(RO_RELAX_DRY), rk);
-    L.run(RG_STAG, k_tend<R>, d, rk);
-    if (lbc) L.run(RG_RING, k_ring<R>, d, int(RO_SPEC_DRY), rk);
+    if (rk == 1) L.run("k_tendf_rk1", RG_STAG, k_tendf_rk1<R>, d);
+    L.run("k_tend", RG_STAG, k_tend<R>, d, rk);
     if (rk == 1) L.copy_list(h->zeros_d, h->zeros_start_d, h->zeros.size(), h->zeros_total);
-    L.run(RG_COLS_STAG, k_ss_prep<R>, d, rk);
+    L.run_cb("k_ss_prep", RG_COLS_STAG, 3, k_ss_prep<R>, d, rk);
     L.halo(cw_handle::H_SS0);
     for (int it = 1; it <= ns; ++it) {
-      L.run(RG_MASS, k_uv<R>, d, rk);
-      if (lbc) L.run(RG_RING, k_ring<R>, d, int(RO_UPDATE_UV), rk);
+      L.run("k_uv", RG_STAG, k_uv<R>, d, rk);
       L.halo(cw_handle::H_UV);
-      if (!lbc) {
-        L.run(RG_COLS_STAG, k_ac<R>, d, rk, it, ns, 7);
-      } else {
-        L.run(RG_COLS_STAG, k_ac<R>, d, rk, it, ns, 1);
-        L.run(RG_RING, k_ring<R>, d, int(RO_UPDATE_MU_T), rk);
-        L.run(RG_COLS_STAG, k_ac<R>, d, rk, it, ns, 2);
-        L.run(RG_RING, k_ring<R>, d, int(RO_UPDATE_PH_W), rk);
-        L.run(RG_MASS, k_wprho<R>, d);
-      }
+      L.run_cb("k_ac", RG_COLS_STAG, kCbArrays, k_ac<R>, d, rk, it, ns);
+      if (lbc) L.run("k_ring", RG_RING, k_ring<R>, d, int(RO_ZERO_GRAD_W), rk);
       L.halo(cw_handle::H_AC);
     }
     L.halo(cw_handle::H_POST);
-    L.run(RG_COLS_STAG, k_finish<R>, d, rk, ns);
+    L.run_cb("k_finish", RG_COLS_STAG, 0, k_finish<R>, d, rk, ns);
     L.halo(cw_handle::H_FIN);
     if (scalars) {
-      if (rk == 1) L.run(RG_MASS, k_q_tendf_rk1<R>, d);
-      if (rk == 1 && lbc) L.run(RG_RING, k_ring<R>, d, int(RO_RELAX_Q), rk);
-      if (lbc) L.run(RG_RING, k_ring<R>, d, int(RO_SPEC_Q), rk);
-      L.run(RG_MASS, k_q_update<R>, d, rk);
+      if (rk == 1) L.run_q("k_q_tendf_rk1", RG_MASS, nq, k_q_tendf_rk1<R>, d);
+      L.run_q("k_q_update", RG_MASS, nq, k_q_update<R>, d, rk);
       if (rk == 3 && any_pd) {
-        L.run(RG_MASS, k_q_pre_pd<R>, d, rk);
+        L.run_q("k_q_pre_pd", RG_MASS, nq, k_q_pre_pd<R>, d, rk);
         L.halo(cw_handle::H_Q1PD);
-        L.run(RG_MASS, k_q_scale_pd<R>, d, rk);
+        L.run_q("k_q_scale_pd", RG_MASS, nq, k_q_scale_pd<R>, d, rk);
         L.halo(cw_handle::H_SCPD);
-        L.run(RG_MASS, k_q_update_pd<R>, d, rk);
+        L.run_q("k_q_update_pd", RG_MASS, nq, k_q_update_pd<R>, d, rk);
       }
+      L.begin("k_q_swap");
       k_q_swap<R><<<unsigned(h->m.size()), 64, 0, h->stream>>>(T.doms, int(h->m.size()));
       L.check();
-      if (lbc) L.run(RG_RING, k_ring<R>, d, int(RO_FLOW_DEP), rk);
+      if (lbc) L.run("k_ring", RG_RING, k_ring<R>, d, int(RO_FLOW_DEP), rk);
       L.halo(cw_handle::H_Q2);
     }
   }
   if (lbc) {
-    L.run(RG_RING, k_ring<R>, d, int(RO_FINAL), 3);
-    L.run(RG_MASS, k_p_rho_phi<R>, d, 1);
+    L.run("k_ring", RG_RING, k_ring<R>, d, int(RO_FINAL), 3);
+    L.run("k_p_rho_phi", RG_MASS, k_p_rho_phi<R>, d, 1);
     L.halo(cw_handle::H_END_P);
   }
   if (terrain) {
     L.halo(cw_handle::H_WS0);
-    L.run(RG_COLS_MASS, k_w_surface<R>, d);
+    L.run_cb("k_w_surface", RG_COLS_MASS, 0, k_w_surface<R>, d);
     L.halo(cw_handle::H_WS1);
   }
 }
@@ -970,6 +1008,64 @@ int cw_launch_count(cw_handle* h, long long* out) {
   *out = h->launches_last;
   return 0;
 }
+// per-kernel device time of nsteps eager steps (CUDA events around every launch; the steps advance the state)
+int cw_profile(cw_handle* h, int nsteps, int* nkernels) {
+  return guarded(h, [&] {
+    if (!h || !nkernels) throw std::runtime_error("null argument");
+    const bool g = h->use_graph;
+    h->use_graph = false;
+    h->profiling = true;
+    h->prof_ev.clear();
+    try {
+      run_steps(h, nsteps);
+    } catch (...) {
+      h->profiling = false;
+      h->use_graph = g;
+      throw;
+    }
+    h->profiling = false;
+    h->use_graph = g;
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+    h->prof_names.clear();
+    h->prof_ms.clear();
+    h->prof_n.clear();
+    for (auto& [name, ev] : h->prof_ev) {
+      float ms = 0;
+      CW_CUDA(cudaEventElapsedTime(&ms, ev.first, ev.second));
+      cudaEventDestroy(ev.first);
+      cudaEventDestroy(ev.second);
+      size_t k = 0;
+      while (k < h->prof_names.size() && h->prof_names[k] != name) ++k;
+      if (k == h->prof_names.size()) {
+        h->prof_names.emplace_back(name);
+        h->prof_ms.push_back(0);
+        h->prof_n.push_back(0);
+      }
+      h->prof_ms[k] += ms;
+      h->prof_n[k] += 1;
+    }
+    h->prof_ev.clear();
+    *nkernels = int(h->prof_names.size());
+    return 0;
+  });
+}
+int cw_profile_entry(cw_handle* h, int idx, char* name, int len, double* ms, long long* launches) {
+  if (!h || idx < 0 || idx >= int(h->prof_names.size())) return -1;
+  if (name && len > 0) {
+    std::strncpy(name, h->prof_names[idx].c_str(), size_t(len) - 1);
+    name[len - 1] = 0;
+  }
+  if (ms) *ms = h->prof_ms[idx];
+  if (launches) *launches = h->prof_n[idx];
+  return 0;
+}
+int cw_use_device(int device) {
+  return guarded(nullptr, [&] {
+    CW_CUDA(cudaSetDevice(device));
+    return 0;
+  });
+}
+
 int cw_set_graph(cw_handle* h, int on) {
   if (!h) return -1;
   h->use_graph = on != 0;

@@ -86,10 +86,13 @@ __device__ __forceinline__ int member_of(const BlockMap& bm, int b) {
   return lo;
 }
 
-// Block geometry of the two launch shapes. Point kernels: PX x PY threads over (i, j), blockIdx over
-// (i-tiles, j-tiles, k) of a member; column kernels: one thread per column, CX x CY columns per block.
+// Block geometry of the two launch shapes. Point kernels: PX threads along i, blockIdx over (i-tiles, j, k)
+// of a member. Column kernels ("column blocks"): CX columns along i (the lanes of a warp, coalesced) x CNW
+// warps; the pointwise work of the columns' levels is split over the warps, the vertical recurrences run
+// on warp 0 (one lane per column) through shared memory. blockIdx over (i-tiles, j).
 constexpr int PX = 128, PY = 1;
-constexpr int CX = 64, CY = 1;
+constexpr int CX = 32, CNW = 8;
+constexpr int kCbArrays = 6;  // shared-memory level arrays of the acoustic column block: kCbArrays x (nz + 2) x CX doubles
 __host__ __device__ __forceinline__ int cdiv(int a, int b) { return (a + b - 1) / b; }
 
 // ---- WRF flux statement functions (src/dyn/kernels_common.hpp:11-105) ----

@@ -21,7 +21,7 @@ enum RangeKind {
   RG_MASS = 1,    // [0, nx) x [0, ny) x [0, nz)
   RG_COLS_STAG,   // columns [0, nx+1) x [0, nyv)
   RG_COLS_MASS,   // columns [0, nx) x [0, ny)
-  RG_RING,        // boundary ring: pos in [0, max(nx, ny)+1), k in [0, nz+1), 4 sides x 4 rows
+  RG_RING,        // boundary ring b = 0: pos in [0, max(nx, ny)+1), k in [0, nz+1), 4 sides
   RG_MASS_W,      // [0, nx) x [0, ny) x [0, nz+1)
 };
 struct Range {
@@ -33,7 +33,7 @@ __host__ __device__ __forceinline__ Range range_of(int kind, int nx, int ny, int
     case RG_MASS: return {0, nx, 0, ny, 0, nz};
     case RG_COLS_STAG: return {0, nx + 1, 0, nyv, 0, 1};
     case RG_COLS_MASS: return {0, nx, 0, ny, 0, 1};
-    case RG_RING: return {0, (nx > ny ? nx : ny) + 1, 0, nz + 1, 0, 16};
+    case RG_RING: return {0, (nx > ny ? nx : ny) + 1, 0, nz + 1, 0, 4};
     default: return {0, nx, 0, ny, 0, nz + 1};
   }
 }
@@ -191,79 +191,6 @@ __device__ __forceinline__ R ww_divv(const Dom<R>& D, int i, int j, int k, R mu1
          (R(D.rdx) * ((c1h * mu1 + c2h) * D.u2(i + 1, j, k) / D.msfuy(i + 1, j) - (c1h * mu0 + c2h) * D.u2(i, j, k) / D.msfuy(i, j)) +
           R(D.rdy) * ((c1h * mv1 + c2h) * D.v2(i, j + 1, k) * D.msfvx_inv(i, j + 1) -
                       (c1h * mv0 + c2h) * D.v2(i, j, k) * D.msfvx_inv(i, j)));
-}
-
-template <class R>
-__global__ void __launch_bounds__(CX) k_ls_prep(const Dom<R>* __restrict__ doms, BlockMap bm) {
-  const Dom<R>* Dp;
-  int i, j, k0;
-  if (!thread_index(doms, bm, RG_COLS_STAG, Dp, i, j, k0)) return;
-  const Dom<R>& D = *Dp;
-  const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
-  const int spx = D.spec_x, spy = D.spec_y;
-  // KMu
-  R muu = 0, muv = 0, mut = 0;
-  if (i < nx && j < ny) {
-    mut = D.mu2(i, j, 0) + D.mub(i, j);
-    D.mut(i, j, 0) = mut;
-  }
-  if (j < ny) {
-    if (spx && i == 0) muu = R(0.5) * (D.mu2(0, j, 0) + D.mu2(0, j, 0) + D.mub(0, j) + D.mub(0, j));
-    else if (spx && i == nx)
-      muu = R(0.5) * (D.mu2(nx - 1, j, 0) + D.mu2(nx - 1, j, 0) + D.mub(nx - 1, j) + D.mub(nx - 1, j));
-    else muu = R(0.5) * (D.mu2(i, j, 0) + D.mu2(i - 1, j, 0) + D.mub(i, j) + D.mub(i - 1, j));
-    D.muu(i, j, 0) = muu;
-  }
-  if (i < nx && j < nyv) {
-    if (spy && j == 0) muv = R(0.5) * (D.mu2(i, 0, 0) + D.mu2(i, 0, 0) + D.mub(i, 0) + D.mub(i, 0));
-    else if (spy && j == ny)
-      muv = R(0.5) * (D.mu2(i, ny - 1, 0) + D.mu2(i, ny - 1, 0) + D.mub(i, ny - 1) + D.mub(i, ny - 1));
-    else muv = R(0.5) * (D.mu2(i, j, 0) + D.mu2(i, j - 1, 0) + D.mub(i, j) + D.mub(i, j - 1));
-    D.muv(i, j, 0) = muv;
-  }
-  // KPrep3
-  for (int k = 0; k < nz + 1; ++k) {
-    if (j < ny && k < nz) D.ru(i, j, k) = D.u2(i, j, k) * (R(D.c1h[k]) * muu + R(D.c2h[k])) / D.msfuy(i, j);
-    if (i < nx && j < nyv && k < nz) D.rv(i, j, k) = D.v2(i, j, k) * (R(D.c1h[k]) * muv + R(D.c2h[k])) * D.msfvx_inv(i, j);
-    if (i < nx && j < ny) D.rw(i, j, k) = D.w2(i, j, k) * (R(D.c1f[k]) * mut + R(D.c2f[k])) / D.msfty(i, j);
-    if (i < nx && j < ny && k < nz) {
-      D.alt(i, j, k) = D.al(i, j, k) + D.alb(i, j, k);
-      D.php(i, j, k) = R(0.5) * (D.phb(i, j, k) + D.phb(i, j, k + 1) + D.ph2(i, j, k) + D.ph2(i, j, k + 1));
-    }
-  }
-  // KWW (columns of the mass points)
-  if (i < nx && j < ny) {
-    const R mu1 = ww_mu_u(D, i + 1, j), mu0 = ww_mu_u(D, i, j), mv1 = ww_mu_v(D, i, j + 1), mv0 = ww_mu_v(D, i, j);
-    R dmdt = 0;
-    for (int k = 0; k < nz; ++k) dmdt += ww_divv(D, i, j, k, mu1, mu0, mv1, mv0);
-    R w = 0;
-    D.ww(i, j, 0) = 0;
-    for (int k = 1; k < nz; ++k) {
-      w = w - R(D.dnw[k - 1]) * R(D.c1h[k - 1]) * dmdt - ww_divv(D, i, j, k - 1, mu1, mu0, mv1, mv0);
-      D.ww(i, j, k) = w;
-    }
-    D.ww(i, j, nz) = 0;
-  }
-  // KCq
-  if (D.n_moist > 0) {
-    for (int k = 0; k < nz; ++k) {
-      if (j < ny) {
-        R t = 0;
-        for (int s = 0; s < D.n_moist; ++s) t = t + D.q2[s](i, j, k) + D.q2[s](i - 1, j, k);
-        D.cqu(i, j, k) = R(1) / (R(1) + R(0.5) * t);
-      }
-      if (i < nx && j < nyv) {
-        R t = 0;
-        for (int s = 0; s < D.n_moist; ++s) t = t + D.q2[s](i, j, k) + D.q2[s](i, j - 1, k);
-        D.cqv(i, j, k) = R(1) / (R(1) + R(0.5) * t);
-      }
-      if (i < nx && j < ny && k >= 1) {
-        R t = 0;
-        for (int s = 0; s < D.n_moist; ++s) t = t + D.q2[s](i, j, k) + D.q2[s](i, j, k - 1);
-        D.cqw(i, j, k) = R(0.5) * t;
-      }
-    }
-  }
 }
 
 // ------------------------------------------------------------------ rk_tendency
@@ -578,9 +505,106 @@ __device__ R tend_ph(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
   return t;
 }
 
+// ------------------------------------------------------------------ lateral boundaries
+// LateralBC (src/dyn/lateral_bc.cpp:21-196): the ring of a variable, slabs (pos, k, b) pos fastest;
+// side order S, N, W, E = slabs ys, ye, xs, xe.
+__device__ __forceinline__ int slab_of_side(int side) { return side < 2 ? side + 2 : side - 2; }
+struct Ring {
+  int ibe, jbe;
+  __device__ __forceinline__ bool map(int pos, int side, int b, int& i, int& j) const {
+    switch (side) {
+      case 0: j = b; i = pos; return pos >= b && pos <= ibe - b;
+      case 1: j = jbe - b; i = pos; return pos >= b && pos <= ibe - b;
+      case 2: i = b; j = pos; return pos >= b + 1 && pos <= jbe - b - 1;
+      default: i = ibe - b; j = pos; return pos >= b + 1 && pos <= jbe - b - 1;
+    }
+  }
+};
+__device__ __forceinline__ Ring ring_for(int nx, int ny, char var) {
+  return Ring{var == 'u' ? nx : nx - 1, var == 'v' ? ny : ny - 1};
+}
+template <class R>
+__device__ __forceinline__ R slab_at(const Slabs<R>& s, int tend, int sl, int pos, int k, int b) {
+  const int np = s.npos[sl];
+  return (tend ? s.t[sl] : s.v[sl])[pos + k * np + b * np * s.nk];
+}
+template <class R>
+__device__ __forceinline__ R slab_val(const Slabs<R>& s, int sl, int pos, int k, int b, R dtbc) {
+  return slab_at(s, 0, sl, pos, k, b) + dtbc * slab_at(s, 1, sl, pos, k, b);
+}
+
+// The ring row b and side / position of point (i, j) of a variable whose last indices are ibe, jbe (the
+// inverse of Ring::map: south / north rows span pos = b .. ibe - b, west / east columns the rest).
+__device__ __forceinline__ bool ring_locate(int ibe, int jbe, int i, int j, int& side, int& b, int& pos) {
+  if (i < 0 || i > ibe || j < 0 || j > jbe) return false;
+  const int dS = j, dN = jbe - j, dW = i, dE = ibe - i;
+  const int dsn = dS < dN ? dS : dN, dwe = dW < dE ? dW : dE;
+  if (dsn <= dwe) {
+    b = dsn;
+    side = dS <= dN ? 0 : 1;
+    pos = i;
+  } else {
+    b = dwe;
+    side = dW <= dE ? 2 : 3;
+    pos = j;
+  }
+  return b < 5;
+}
+
+// KRelax (lateral_bc.cpp:79-118) at ring point (pos, side, b) level k of one variable: returns
+// fa = fcx * fls0 and fb = gcx * (fls1 + fls2 + fls3 + fls4 - 4 fls0); the relaxation term is fa - fb.
+template <class R, bool Two>
+__device__ void relax_terms(const Dom<R>& D, const V3<R>& f, const double* c1, const double* c2, const Slabs<R>& s,
+                            Ring r, int pos, int side, int b, int k, int i, int j, R& fa, R& fb) {
+  const int sl = slab_of_side(side);
+  const R dtbc = R(D.dtbc);
+  auto BV = [&](int p, int bb) { return slab_val(s, sl, p, k, bb, dtbc); };
+  auto FV = [&](int ii, int jj) -> R {
+    const R x = Two ? f(ii, jj, 0) : f(ii, jj, k);
+    return c1 ? x * (R(c1[k]) * D.mut(ii, jj, 0) + R(c2[k])) : x;
+  };
+  R fls0, fls1, fls2, fls3, fls4;
+  fls0 = BV(pos, b) - FV(i, j);
+  if (side <= 1) {
+    const int im1 = i - 1 > 0 ? i - 1 : 0, ip1 = i + 1 < r.ibe ? i + 1 : r.ibe;
+    const int jin = side == 0 ? j + 1 : j - 1, jout = side == 0 ? j - 1 : j + 1;
+    fls1 = BV(im1, b) - FV(im1, j);
+    fls2 = BV(ip1, b) - FV(ip1, j);
+    fls3 = BV(i, b - 1) - FV(i, jout);
+    fls4 = BV(i, b + 1) - FV(i, jin);
+  } else {
+    const int iin = side == 2 ? i + 1 : i - 1, iout = side == 2 ? i - 1 : i + 1;
+    fls1 = BV(j - 1, b) - FV(i, j - 1);
+    fls2 = BV(j + 1, b) - FV(i, j + 1);
+    fls3 = BV(j, b - 1) - FV(iout, j);
+    fls4 = BV(j, b + 1) - FV(iin, j);
+  }
+  fa = R(D.fcx[b]) * fls0;
+  fb = R(D.gcx[b]) * (fls1 + fls2 + fls3 + fls4 - R(4) * fls0);
+}
+
+// The ring point (side, row b, pos) of (i, j) when it lies in rows b_lo .. b_hi of the variable's ring;
+// then fa, fb of its relaxation term (relax_terms).
+template <class R, bool Two>
+__device__ __forceinline__ bool relax_at(const Dom<R>& D, const V3<R>& f, const double* c1, const double* c2,
+                                         const Slabs<R>& s, Ring r, int i, int j, int k, R& fa, R& fb) {
+  int side, b, pos;
+  if (!ring_locate(r.ibe, r.jbe, i, j, side, b, pos) || b < 1 || b > 3) return false;
+  relax_terms<R, Two>(D, f, c1, c2, s, r, pos, side, b, k, i, j, fa, fb);
+  return true;
+}
+// (i, j) in the spec zone (row 0) of the ring: slab index sl and position pos of its boundary value
+__device__ __forceinline__ bool spec_at(Ring r, int i, int j, int& sl, int& pos) {
+  int side, b;
+  if (!ring_locate(r.ibe, r.jbe, i, j, side, b, pos) || b != 0) return false;
+  sl = slab_of_side(side);
+  return true;
+}
+
 // LargeStep::tendencies (large_step.cpp:798-861): the five tendencies of a point, each for the points of
 // its own range: ru (u_i0 .. u_i1), rv (v_j0 .. v_j1, 3-D), rw and ph (levels 1..nz), theta (mass cells).
-// Also mu_tend = 0 (zero_tend of a run with lateral boundaries) at rk 2 and 3.
+// Also mu_tend = 0 (zero_tend of a run with lateral boundaries) at rk 2 and 3, and with lateral
+// boundaries the spec zone's tendencies from the boundary slabs.
 template <class R>
 __global__ void __launch_bounds__(PX) k_tend(const Dom<R>* __restrict__ doms, BlockMap bm, int rk) {
   const Dom<R>* Dp;
@@ -591,15 +615,23 @@ __global__ void __launch_bounds__(PX) k_tend(const Dom<R>* __restrict__ doms, Bl
   const bool use_tendf = D.lbc || D.diff_on;
   const int ui0 = D.bc_x != CW_BC_PERIODIC ? 1 : 0;
   const int vj0 = (D.bc_y != CW_BC_PERIODIC && D.do_y) ? 1 : 0;
-  if (i >= ui0 && i < nx && j < ny && k < nz) D.ru_tend(i, j, k) = tend_u(D, i, j, k, use_tendf);
-  if (D.do_y && i < nx && j >= vj0 && j < ny && k < nz) D.rv_tend(i, j, k) = tend_v(D, i, j, k, use_tendf);
+  const bool lbc = D.lbc;
+  int sl, pos;
+  // LateralBC::spec_dry (lateral_bc.cpp:337-351): the spec zone (row 0) takes the boundary tendency
+  if (lbc && k < nz && spec_at(ring_for(nx, ny, 'u'), i, j, sl, pos)) D.ru_tend(i, j, k) = slab_at(D.lbc_var[0], 1, sl, pos, k, 0);
+  else if (i >= ui0 && i < nx && j < ny && k < nz) D.ru_tend(i, j, k) = tend_u(D, i, j, k, use_tendf);
+  if (lbc && k < nz && spec_at(ring_for(nx, ny, 'v'), i, j, sl, pos)) D.rv_tend(i, j, k) = slab_at(D.lbc_var[1], 1, sl, pos, k, 0);
+  else if (D.do_y && i < nx && j >= vj0 && j < ny && k < nz) D.rv_tend(i, j, k) = tend_v(D, i, j, k, use_tendf);
   if (i < nx && j < ny) {
-    if (k >= 1) {
-      D.rw_tend(i, j, k) = tend_w(D, i, j, k, use_tendf);
-      D.ph_tend(i, j, k) = tend_ph(D, i, j, k, D.lbc != 0);
+    const bool spec = lbc && spec_at(ring_for(nx, ny, 'h'), i, j, sl, pos);
+    if (k >= 1) D.rw_tend(i, j, k) = tend_w(D, i, j, k, use_tendf);
+    if (spec) D.ph_tend(i, j, k) = slab_at(D.lbc_var[3], 1, sl, pos, k, 0);
+    else if (k >= 1) D.ph_tend(i, j, k) = tend_ph(D, i, j, k, lbc);
+    if (k < nz) D.t_tend(i, j, k) = spec ? slab_at(D.lbc_var[2], 1, sl, pos, k, 0) : tend_t(D, i, j, k, use_tendf, D.n_moist > 0);
+    if (k == 0 && lbc) {
+      if (spec) D.mu_tend(i, j, 0) = slab_at(D.lbc_var[4], 1, sl, pos, 0, 0);
+      else if (rk != 1) D.mu_tend(i, j, 0) = 0;
     }
-    if (k < nz) D.t_tend(i, j, k) = tend_t(D, i, j, k, use_tendf, D.n_moist > 0);
-    if (k == 0 && D.lbc && rk != 1) D.mu_tend(i, j, 0) = 0;
   }
 }
 
@@ -739,7 +771,8 @@ __device__ __forceinline__ R vdiff_uv(const Dom<R>& D, const V3<R>& f, const dou
   return G * G * R(D.rdnw[k]) / mu / a * (vflux_uv<R, DI, DJ>(D, f, ub, kv, i, j, k) - vflux_uv<R, DI, DJ>(D, f, ub, kv, i, j, k - 1));
 }
 
-// rk 1: zero the held tendencies, add the constant-K diffusion; mu_tend = 0 with lateral boundaries
+// rk 1: zero the held tendencies, add the constant-K diffusion; with lateral boundaries mu_tend = 0 and the
+// relaxation of rows 1..3 (LateralBC::relax_dry, lateral_bc.cpp:294-335) added to the held tendencies
 template <class R>
 __global__ void __launch_bounds__(PX) k_tendf_rk1(const Dom<R>* __restrict__ doms, BlockMap bm) {
   const Dom<R>* Dp;
@@ -763,6 +796,9 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const Dom<R>* __restrict__ dom
       if (px) { vis = 0; vie = nx + 1; }
       if (i >= vis && i < vie && k < nz - 1) t += vdiff_uv<R, 1, 0>(D, D.u2, D.u_base, D.muu, kvdif, i, j, k);
     }
+    R fa, fb;
+    if (sp && relax_at<R, false>(D, D.ru, nullptr, nullptr, D.lbc_var[0], ring_for(nx, ny, 'u'), i, j, k, fa, fb))
+      t += (fa - fb) * D.msfuy(i, j);
     D.ru_tendf(i, j, k) = t;
   }
   if (i < nx && j < nyv && k < nz) {  // rv_tendf
@@ -775,6 +811,9 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const Dom<R>* __restrict__ dom
       const int vjs = sp ? 1 : 0, vje = sp ? ny : ny + 1;
       if (j >= vjs && j < vje && k < nz - 1) t += vdiff_uv<R, 0, 1>(D, D.v2, D.v_base, D.muv, kvdif, i, j, k);
     }
+    R fa, fb;
+    if (sp && relax_at<R, false>(D, D.rv, nullptr, nullptr, D.lbc_var[1], ring_for(nx, ny, 'v'), i, j, k, fa, fb))
+      t += (fa - fb) * D.msfvx(i, j);
     D.rv_tendf(i, j, k) = t;
   }
   if (i < nx && j < ny) {
@@ -787,7 +826,10 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const Dom<R>* __restrict__ dom
       tw += vdiff_w(D, D.w2, D.mut, kvdif, i, j, k);
     }
     D.rw_tendf(i, j, k) = tw;
-    D.ph_tendf(i, j, k) = 0;
+    R fa, fb;
+    R tp = 0;
+    if (sp && relax_at<R, false>(D, D.ph2, D.c1f, D.c2f, D.lbc_var[3], ring_for(nx, ny, 'h'), i, j, k, fa, fb)) tp += fa - fb;
+    D.ph_tendf(i, j, k) = tp;
     if (k < nz) {
       R tt = 0;
       if (dd) {
@@ -797,135 +839,34 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const Dom<R>* __restrict__ dom
         if (i >= is && i < ie && j >= js && j < je) tt += hdiff_m(D, D.t2, &D.t_init, D.mut, khh, i, j, k);
         tt += vdiff_m(D, D.t2, &D.t_init, D.mut, R(3.) * kvdif, i, j, k);
       }
+      if (sp && relax_at<R, false>(D, D.t2, D.c1h, D.c2h, D.lbc_var[2], ring_for(nx, ny, 't'), i, j, k, fa, fb)) tt += fa - fb;
       D.t_tendf(i, j, k) = tt;
     }
-    if (k == 0 && D.lbc) D.mu_tend(i, j, 0) = 0;
-  }
-}
-
-// ------------------------------------------------------------------ lateral boundaries
-// LateralBC (src/dyn/lateral_bc.cpp:21-196): the ring of a variable, slabs (pos, k, b) pos fastest;
-// side order S, N, W, E = slabs ys, ye, xs, xe.
-__device__ __forceinline__ int slab_of_side(int side) { return side < 2 ? side + 2 : side - 2; }
-struct Ring {
-  int ibe, jbe;
-  __device__ __forceinline__ bool map(int pos, int side, int b, int& i, int& j) const {
-    switch (side) {
-      case 0: j = b; i = pos; return pos >= b && pos <= ibe - b;
-      case 1: j = jbe - b; i = pos; return pos >= b && pos <= ibe - b;
-      case 2: i = b; j = pos; return pos >= b + 1 && pos <= jbe - b - 1;
-      default: i = ibe - b; j = pos; return pos >= b + 1 && pos <= jbe - b - 1;
+    if (k == 0 && sp) {
+      R tm = 0;
+      if (relax_at<R, true>(D, D.mu2, nullptr, nullptr, D.lbc_var[4], ring_for(nx, ny, 'm'), i, j, 0, fa, fb)) tm += fa - fb;
+      D.mu_tend(i, j, 0) = tm;
     }
   }
-};
-__device__ __forceinline__ Ring ring_for(int nx, int ny, char var) {
-  return Ring{var == 'u' ? nx : nx - 1, var == 'v' ? ny : ny - 1};
-}
-template <class R>
-__device__ __forceinline__ R slab_at(const Slabs<R>& s, int tend, int sl, int pos, int k, int b) {
-  const int np = s.npos[sl];
-  return (tend ? s.t[sl] : s.v[sl])[pos + k * np + b * np * s.nk];
-}
-template <class R>
-__device__ __forceinline__ R slab_val(const Slabs<R>& s, int sl, int pos, int k, int b, R dtbc) {
-  return slab_at(s, 0, sl, pos, k, b) + dtbc * slab_at(s, 1, sl, pos, k, b);
 }
 
-// KRelax (:79-118) at ring point (pos, side, b, k) of one variable
-template <class R, bool Two>
-__device__ void relax_point(const Dom<R>& D, const V3<R>& out, const V3<R>& f, const double* c1, const double* c2,
-                            const VB<R>* msf, const Slabs<R>& s, Ring r, int pos, int side, int b, int k, bool direct) {
-  int i, j;
-  if (!r.map(pos, side, b, i, j)) return;
-  const int sl = slab_of_side(side);
-  const R dtbc = R(D.dtbc);
-  auto BV = [&](int p, int bb) { return slab_val(s, sl, p, k, bb, dtbc); };
-  auto FV = [&](int ii, int jj) -> R {
-    const R x = Two ? f(ii, jj, 0) : f(ii, jj, k);
-    return c1 ? x * (R(c1[k]) * D.mut(ii, jj, 0) + R(c2[k])) : x;
-  };
-  R fls0, fls1, fls2, fls3, fls4;
-  fls0 = BV(pos, b) - FV(i, j);
-  if (side <= 1) {
-    const int im1 = i - 1 > 0 ? i - 1 : 0, ip1 = i + 1 < r.ibe ? i + 1 : r.ibe;
-    const int jin = side == 0 ? j + 1 : j - 1, jout = side == 0 ? j - 1 : j + 1;
-    fls1 = BV(im1, b) - FV(im1, j);
-    fls2 = BV(ip1, b) - FV(ip1, j);
-    fls3 = BV(i, b - 1) - FV(i, jout);
-    fls4 = BV(i, b + 1) - FV(i, jin);
-  } else {
-    const int iin = side == 2 ? i + 1 : i - 1, iout = side == 2 ? i - 1 : i + 1;
-    fls1 = BV(j - 1, b) - FV(i, j - 1);
-    fls2 = BV(j + 1, b) - FV(i, j + 1);
-    fls3 = BV(j, b - 1) - FV(iout, j);
-    fls4 = BV(j, b + 1) - FV(iin, j);
-  }
-  const R fcx = R(D.fcx[b]), gcx = R(D.gcx[b]);
-  const R val = fcx * fls0 - gcx * (fls1 + fls2 + fls3 + fls4 - R(4) * fls0);
-  if (Two) out(i, j, 0) += val;
-  else if (direct) out(i, j, k) = out(i, j, k) + fcx * fls0 - gcx * (fls1 + fls2 + fls3 + fls4 - R(4) * fls0);
-  else out(i, j, k) += msf ? val * (*msf)(i, j) : val;
-}
-
-// The ring kernels: thread (pos, k, 4 sides x rows) of a member; what = which operation
-enum RingOp { RO_RELAX_DRY = 0, RO_SPEC_DRY, RO_UPDATE_UV, RO_UPDATE_MU_T, RO_UPDATE_PH_W, RO_FINAL, RO_RELAX_Q, RO_SPEC_Q, RO_FLOW_DEP };
+// The remaining ring kernels (spec zone b = 0, thread (pos, level, side)): the end-of-step spec_bdy_final,
+// flow_dep_bdy of the scalars without boundary data, zero_grad_bdy of w. The other boundary operations run
+// inside the kernels that compute the same points (k_tendf_rk1, k_tend, k_uv, k_ac, k_q_tendf_rk1).
+enum RingOp { RO_FINAL = 0, RO_FLOW_DEP, RO_ZERO_GRAD_W };
 template <class R>
 __global__ void __launch_bounds__(PX) k_ring(const Dom<R>* __restrict__ doms, BlockMap bm, int op, int rk) {
   const Dom<R>* Dp;
-  int pos, k, sb;
-  if (!thread_index(doms, bm, RG_RING, Dp, pos, k, sb)) return;
+  int pos, k, side;
+  if (!thread_index(doms, bm, RG_RING, Dp, pos, k, side)) return;
   const Dom<R>& D = *Dp;
-  const double dts = double(R(rk == 1 ? D.dt / 3.0 : D.dt / D.n_sound));
+  (void)rk;
   const int nx = D.nx, ny = D.ny, nz = D.nz;
-  const int side = sb % 4, row = sb / 4;
   switch (op) {
-    case RO_RELAX_DRY: {  // LateralBC::relax_dry (:294-335): rows 1..3
-      if (row >= 3) return;
-      const int b = 1 + row;
-      if (k < nz) relax_point<R, false>(D, D.ru_tendf, D.ru, nullptr, nullptr, &D.msfuy, D.lbc_var[0], ring_for(nx, ny, 'u'), pos, side, b, k, false);
-      if (k < nz) relax_point<R, false>(D, D.rv_tendf, D.rv, nullptr, nullptr, &D.msfvx, D.lbc_var[1], ring_for(nx, ny, 'v'), pos, side, b, k, false);
-      relax_point<R, false>(D, D.ph_tendf, D.ph2, D.c1f, D.c2f, nullptr, D.lbc_var[3], ring_for(nx, ny, 'h'), pos, side, b, k, false);
-      if (k < nz) relax_point<R, false>(D, D.t_tendf, D.t2, D.c1h, D.c2h, nullptr, D.lbc_var[2], ring_for(nx, ny, 't'), pos, side, b, k, false);
-      if (k == 0) relax_point<R, true>(D, D.mu_tend, D.mu2, nullptr, nullptr, nullptr, D.lbc_var[4], ring_for(nx, ny, 'm'), pos, side, b, 0, false);
-      return;
-    }
-    case RO_SPEC_DRY: {  // spec_dry (:337-351): the spec zone b = 0 takes the boundary tendency
-      if (row != 0) return;
-      int i, j;
-      const int sl = slab_of_side(side);
-      if (k < nz && ring_for(nx, ny, 'u').map(pos, side, 0, i, j)) D.ru_tend(i, j, k) = slab_at(D.lbc_var[0], 1, sl, pos, k, 0);
-      if (k < nz && ring_for(nx, ny, 'v').map(pos, side, 0, i, j)) D.rv_tend(i, j, k) = slab_at(D.lbc_var[1], 1, sl, pos, k, 0);
-      if (ring_for(nx, ny, 'h').map(pos, side, 0, i, j)) D.ph_tend(i, j, k) = slab_at(D.lbc_var[3], 1, sl, pos, k, 0);
-      if (k < nz && ring_for(nx, ny, 't').map(pos, side, 0, i, j)) D.t_tend(i, j, k) = slab_at(D.lbc_var[2], 1, sl, pos, k, 0);
-      if (k == 0 && ring_for(nx, ny, 'm').map(pos, side, 0, i, j)) D.mu_tend(i, j, 0) = slab_at(D.lbc_var[4], 1, sl, pos, 0, 0);
-      return;
-    }
-    case RO_UPDATE_UV: {  // update_uv (:353-361)
-      if (row != 0 || k >= nz) return;
-      int i, j;
-      if (ring_for(nx, ny, 'u').map(pos, side, 0, i, j)) D.u2(i, j, k) += R(dts) * D.ru_tend(i, j, k);
-      if (ring_for(nx, ny, 'v').map(pos, side, 0, i, j)) D.v2(i, j, k) += R(dts) * D.rv_tend(i, j, k);
-      return;
-    }
-    case RO_UPDATE_MU_T: {  // update_mu_t (:363-372)
-      if (row != 0 || k >= nz) return;
-      int i, j;
-      if (!ring_for(nx, ny, 't').map(pos, side, 0, i, j)) return;
-      D.t2(i, j, k) += R(dts) * D.t_tend(i, j, k);
-      if (k == 0) {
-        D.mu2(i, j, 0) += R(dts) * D.mu_tend(i, j, 0);
-        D.muts(i, j, 0) += R(dts) * D.mu_tend(i, j, 0);
-      }
-      return;
-    }
-    case RO_UPDATE_PH_W: {  // update_ph_w (:374-386): KUpdatePh and KZeroGrad on w
-      if (row != 0) return;
+    case RO_ZERO_GRAD_W: {  // zero_grad_bdy on w (KZeroGrad, lateral_bc.cpp:143-159)
       int i, j;
       const Ring r = ring_for(nx, ny, 'h');
       if (!r.map(pos, side, 0, i, j)) return;
-      const R mu_old = D.muts(i, j, 0) - R(dts) * D.mu_tend(i, j, 0);
-      const R m_old = R(D.c1f[k]) * mu_old + R(D.c2f[k]), m_new = R(D.c1f[k]) * D.muts(i, j, 0) + R(D.c2f[k]);
-      D.ph2(i, j, k) = D.ph2(i, j, k) * m_old / m_new + R(dts) * D.ph_tend(i, j, k) / m_new + D.ph_save(i, j, k) * (m_old / m_new - R(1));
       const int ic = i < 1 ? 1 : (i > r.ibe - 1 ? r.ibe - 1 : i);
       const int jc = j < 1 ? 1 : (j > r.jbe - 1 ? r.jbe - 1 : j);
       switch (side) {
@@ -937,7 +878,6 @@ __global__ void __launch_bounds__(PX) k_ring(const Dom<R>* __restrict__ doms, Bl
       return;
     }
     case RO_FINAL: {  // final (:425-455)
-      if (row != 0) return;
       int i, j;
       const int sl = slab_of_side(side);
       const R dtbc = R(D.dtbc);
@@ -968,23 +908,8 @@ __global__ void __launch_bounds__(PX) k_ring(const Dom<R>* __restrict__ doms, Bl
       }
       return;
     }
-    case RO_RELAX_Q: {  // relax_scalars (:388-401)
-      if (row >= 3 || k >= nz) return;
-      for (int n = 0; n < D.n_scalars; ++n)
-        if (D.lbc_q[n].have)
-          relax_point<R, false>(D, D.qtf[n], D.q2[n], D.c1h, D.c2h, nullptr, D.lbc_q[n], ring_for(nx, ny, 'q'), pos, side, 1 + row, k, true);
-      return;
-    }
-    case RO_SPEC_Q: {  // spec_scalars (:403-414)
-      if (row != 0 || k >= nz) return;
-      int i, j;
-      if (!ring_for(nx, ny, 'q').map(pos, side, 0, i, j)) return;
-      for (int n = 0; n < D.n_scalars; ++n)
-        if (D.lbc_q[n].have) D.qtf[n](i, j, k) = slab_at(D.lbc_q[n], 1, slab_of_side(side), pos, k, 0);
-      return;
-    }
     case RO_FLOW_DEP: {  // flow_dep (:416-423) on the scalars without boundary data
-      if (row != 0 || k >= nz) return;
+      if (k >= nz) return;
       int i, j;
       const Ring r = ring_for(nx, ny, 'q');
       if (!r.map(pos, side, 0, i, j)) return;

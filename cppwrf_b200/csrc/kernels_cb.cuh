@@ -1,0 +1,525 @@
+// SPDX-License-Identifier: GPL-3.0-or-later
+// Column-block kernels: a CTA holds CX neighbouring columns along i (the lanes, so every global access is
+// coalesced along i) and CNW warps. The pointwise work of the levels is split over the warps; the
+// vertical recurrences -- column sums, running integrals, the tridiagonal sweeps -- run on warp 0, one lane
+// per column, in the reference's order, on per-level terms staged in shared memory. Every value is the
+// same expression as the reference's column functor, so the results are bit-identical to it.
+#pragma once
+
+#include "kernels_ac.cuh"
+
+namespace cw {
+
+#define CB_LOOP(k, n) for (int k = int(threadIdx.y); k < (n); k += CNW)
+
+// block -> (member, column i of this lane, row j)
+template <class R>
+__device__ __forceinline__ const Dom<R>& cb_member(const Dom<R>* __restrict__ doms, const BlockMap& bm, int kind, int& i,
+                                                   int& j) {
+  const int b = blockIdx.x;
+  const int m = member_of(bm, b);
+  const Dom<R>& D = doms[m];
+  const Range r = range_of(kind, D.nx, D.ny, D.nz, D.nyv);
+  const int bx = cdiv(r.i1 - r.i0, CX);
+  const int local = b - bm.start[m];
+  i = r.i0 + (local % bx) * CX + int(threadIdx.x);
+  j = r.j0 + local / bx;
+  return D;
+}
+// shared level array a of the block: a[k * CX + lane]
+__device__ __forceinline__ double* cb_array(int a, int nz) {
+  extern __shared__ double cb_smem[];
+  return cb_smem + size_t(a) * (nz + 2) * CX;
+}
+
+// rk_step_prep: KMu (large_step.cpp:49-66), KPrep3 (:68-81), KWW (:83-108), KCq (:127-148)
+template <class R>
+__global__ void __launch_bounds__(CX * CNW, 3) k_ls_prep(const Dom<R>* __restrict__ doms, BlockMap bm) {
+  int i, j;
+  const Dom<R>& D = cb_member(doms, bm, RG_COLS_STAG, i, j);
+  const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
+  const int lane = threadIdx.x;
+  const bool col = i < nx + 1;
+  const bool w0 = threadIdx.y == 0;
+  const int spx = D.spec_x, spy = D.spec_y;
+  double* s_div = cb_array(0, nz);
+  R muu = 0, muv = 0, mut = 0;
+  if (col) {
+    if (i < nx && j < ny) mut = D.mu2(i, j, 0) + D.mub(i, j);
+    if (j < ny) {
+      if (spx && i == 0) muu = R(0.5) * (D.mu2(0, j, 0) + D.mu2(0, j, 0) + D.mub(0, j) + D.mub(0, j));
+      else if (spx && i == nx)
+        muu = R(0.5) * (D.mu2(nx - 1, j, 0) + D.mu2(nx - 1, j, 0) + D.mub(nx - 1, j) + D.mub(nx - 1, j));
+      else muu = R(0.5) * (D.mu2(i, j, 0) + D.mu2(i - 1, j, 0) + D.mub(i, j) + D.mub(i - 1, j));
+    }
+    if (i < nx && j < nyv) {
+      if (spy && j == 0) muv = R(0.5) * (D.mu2(i, 0, 0) + D.mu2(i, 0, 0) + D.mub(i, 0) + D.mub(i, 0));
+      else if (spy && j == ny)
+        muv = R(0.5) * (D.mu2(i, ny - 1, 0) + D.mu2(i, ny - 1, 0) + D.mub(i, ny - 1) + D.mub(i, ny - 1));
+      else muv = R(0.5) * (D.mu2(i, j, 0) + D.mu2(i, j - 1, 0) + D.mub(i, j) + D.mub(i, j - 1));
+    }
+    if (w0) {
+      if (i < nx && j < ny) D.mut(i, j, 0) = mut;
+      if (j < ny) D.muu(i, j, 0) = muu;
+      if (i < nx && j < nyv) D.muv(i, j, 0) = muv;
+    }
+    CB_LOOP(k, nz + 1) {  // KPrep3
+      if (j < ny && k < nz) D.ru(i, j, k) = D.u2(i, j, k) * (R(D.c1h[k]) * muu + R(D.c2h[k])) / D.msfuy(i, j);
+      if (i < nx && j < nyv && k < nz) D.rv(i, j, k) = D.v2(i, j, k) * (R(D.c1h[k]) * muv + R(D.c2h[k])) * D.msfvx_inv(i, j);
+      if (i < nx && j < ny) D.rw(i, j, k) = D.w2(i, j, k) * (R(D.c1f[k]) * mut + R(D.c2f[k])) / D.msfty(i, j);
+      if (i < nx && j < ny && k < nz) {
+        D.alt(i, j, k) = D.al(i, j, k) + D.alb(i, j, k);
+        D.php(i, j, k) = R(0.5) * (D.phb(i, j, k) + D.phb(i, j, k + 1) + D.ph2(i, j, k) + D.ph2(i, j, k + 1));
+      }
+    }
+  }
+  const bool mass = col && i < nx && j < ny;
+  R mu1 = 0, mu0 = 0, mv1 = 0, mv0 = 0;
+  if (mass) {
+    mu1 = ww_mu_u(D, i + 1, j);
+    mu0 = ww_mu_u(D, i, j);
+    mv1 = ww_mu_v(D, i, j + 1);
+    mv0 = ww_mu_v(D, i, j);
+    CB_LOOP(k, nz) s_div[k * CX + lane] = double(ww_divv(D, i, j, k, mu1, mu0, mv1, mv0));
+  }
+  __syncthreads();
+  if (mass && w0) {  // KWW: the column integral, then the running sum, in the reference's order
+    R dmdt = 0;
+    for (int k = 0; k < nz; ++k) dmdt += R(s_div[k * CX + lane]);
+    R w = 0;
+    D.ww(i, j, 0) = 0;
+    for (int k = 1; k < nz; ++k) {
+      w = w - R(D.dnw[k - 1]) * R(D.c1h[k - 1]) * dmdt - R(s_div[(k - 1) * CX + lane]);
+      D.ww(i, j, k) = w;
+    }
+    D.ww(i, j, nz) = 0;
+  }
+  if (col && D.n_moist > 0) {  // KCq
+    CB_LOOP(k, nz) {
+      if (j < ny) {
+        R t = 0;
+        for (int s = 0; s < D.n_moist; ++s) t = t + D.q2[s](i, j, k) + D.q2[s](i - 1, j, k);
+        D.cqu(i, j, k) = R(1) / (R(1) + R(0.5) * t);
+      }
+      if (i < nx && j < nyv) {
+        R t = 0;
+        for (int s = 0; s < D.n_moist; ++s) t = t + D.q2[s](i, j, k) + D.q2[s](i, j - 1, k);
+        D.cqv(i, j, k) = R(1) / (R(1) + R(0.5) * t);
+      }
+      if (i < nx && j < ny && k >= 1) {
+        R t = 0;
+        for (int s = 0; s < D.n_moist; ++s) t = t + D.q2[s](i, j, k) + D.q2[s](i, j, k - 1);
+        D.cqw(i, j, k) = R(0.5) * t;
+      }
+    }
+  }
+}
+
+// small_step_prep (KPrep small_step.cpp:50-93) + calc_p_rho (KPRho :114-119) + calc_coef_w (KCoefW :122-148)
+template <class R>
+__global__ void __launch_bounds__(CX * CNW, 3) k_ss_prep(const Dom<R>* __restrict__ doms, BlockMap bm, int rk) {
+  int i, j;
+  const Dom<R>& D = cb_member(doms, bm, RG_COLS_STAG, i, j);
+  const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
+  const int lane = threadIdx.x;
+  const bool col = i < nx + 1;
+  const bool w0 = threadIdx.y == 0;
+  const bool mass = col && i < nx && j < ny;
+  const bool first = rk == 1;
+  R mts = 0, mus_u = 0, mus_v = 0, mut = 0;
+  if (col) {
+    mts = D.mub(i, j) + D.mu1(i, j, 0);
+    mus_u = first ? D.muu(i, j, 0) : R(0.5) * (mts + D.mub(i - 1, j) + D.mu1(i - 1, j, 0));
+    mus_v = first ? D.muv(i, j, 0) : R(0.5) * (mts + D.mub(i, j - 1) + D.mu1(i, j - 1, 0));
+    if (mass) mut = D.mut(i, j, 0);
+    if (w0) {
+      if (mass) {
+        D.muts(i, j, 0) = mts;
+        D.mu_save(i, j, 0) = D.mu2(i, j, 0);
+        D.mu2(i, j, 0) = D.mu1(i, j, 0) - D.mu2(i, j, 0);
+      }
+      if (j < ny) D.muus(i, j, 0) = mus_u;
+      if (i < nx && j < nyv) D.muvs(i, j, 0) = mus_v;
+    }
+    CB_LOOP(k, nz + 1) {  // KPrep
+      const R c1h = k < nz ? R(D.c1h[k]) : R(0), c2h = k < nz ? R(D.c2h[k]) : R(0);
+      if (j < ny && k < nz) {
+        const R ui = D.u2(i, j, k);
+        D.u_save(i, j, k) = ui;
+        D.u2(i, j, k) = ((c1h * mus_u + c2h) * D.u1(i, j, k) - (c1h * D.muu(i, j, 0) + c2h) * ui) / D.msfuy(i, j);
+      }
+      if (i < nx && j < nyv && k < nz) {
+        const R vi = D.v2(i, j, k);
+        D.v_save(i, j, k) = vi;
+        D.v2(i, j, k) = ((c1h * mus_v + c2h) * D.v1(i, j, k) - (c1h * D.muv(i, j, 0) + c2h) * vi) * D.msfvx_inv(i, j);
+      }
+      if (mass) {
+        if (k < nz) {
+          const R ti = D.t2(i, j, k);
+          D.t_save(i, j, k) = ti;
+          D.t2(i, j, k) = (c1h * mts + c2h) * D.t1(i, j, k) - (c1h * mut + c2h) * ti;
+          D.c2a(i, j, k) = R(k::cpovcv) * (D.pb(i, j, k) + D.p(i, j, k)) / D.alt(i, j, k);
+        }
+        const R wi = D.w2(i, j, k), phi = D.ph2(i, j, k);
+        D.w_save(i, j, k) = wi;
+        D.w2(i, j, k) = ((R(D.c1f[k]) * mts + R(D.c2f[k])) * D.w1(i, j, k) - (R(D.c1f[k]) * mut + R(D.c2f[k])) * wi) / D.msfty(i, j);
+        D.ph_save(i, j, k) = phi;
+        D.ph2(i, j, k) = D.ph1(i, j, k) - phi;
+        D.ww1(i, j, k) = (k == 0 || k == nz) ? R(0) : D.ww(i, j, k);
+      }
+    }
+  }
+  __syncthreads();
+  using A = double;
+  double* s_a = cb_array(0, nz);
+  double* s_b = cb_array(1, nz);
+  double* s_c = cb_array(2, nz);
+  const A dts = rk == 1 ? D.dt / 3.0 : D.dt / D.n_sound;
+  const A cof_h = 0.5 * A(R(dts)) * k::g * (1.0 + A(R(D.epssm)));
+  const A cof = A(R(cof_h * cof_h));
+  const A m = A(mut);
+  auto mh = [&](int kk, A mm) { return D.c1h[kk] * mm + D.c2h[kk]; };
+  auto mf = [&](int kk, A mm) { return D.c1f[kk] * mm + D.c2f[kk]; };
+  auto cq1 = [&](int kk) { return A(R(1) / (R(1) + cqw_(D, i, j, kk))); };
+  if (mass) {
+    CB_LOOP(k, nz) p_rho_point(D, i, j, k, false);
+    // calc_coef_w: the pointwise coefficients a, b, c of each level
+    CB_LOOP(k, nz + 1) {
+      A a = 0, b = 0, cc = 0;
+      if (k == nz) {
+        a = -2. * cof * (D.rdnw[nz - 1] * D.rdnw[nz - 1]) * A(D.c2a(i, j, nz - 1)) * (D.top_lid ? 0.0 : 1.0) /
+            (mh(nz - 1, m) * mf(nz - 1, m));
+        b = 1. + 2. * cof * (D.rdnw[nz - 1] * D.rdnw[nz - 1]) * A(D.c2a(i, j, nz - 1)) / (mh(nz - 1, m) * mf(nz, m));
+      } else if (k >= 1) {
+        if (k >= 2) a = -cq1(k) * cof * D.rdn[k] * D.rdnw[k - 1] * A(D.c2a(i, j, k - 1)) / (mh(k - 1, m) * mf(k - 1, m));
+        const A q1 = cq1(k);
+        b = 1. + q1 * cof * D.rdn[k] *
+                     (D.rdnw[k] * A(D.c2a(i, j, k)) / (mh(k, m) * mf(k, m)) +
+                      D.rdnw[k - 1] * A(D.c2a(i, j, k - 1)) / (mh(k - 1, m) * mf(k, m)));
+        cc = -q1 * cof * D.rdn[k] * D.rdnw[k] * A(D.c2a(i, j, k)) / (mh(k, m) * mf(k + 1, m));
+      }
+      s_a[k * CX + lane] = A(R(a));
+      s_b[k * CX + lane] = b;
+      s_c[k * CX + lane] = cc;
+      D.a(i, j, k) = R(a);
+    }
+  }
+  __syncthreads();
+  if (mass && w0) {  // the forward-elimination factors, a recurrence in k
+    D.alpha(i, j, 0) = 0;
+    D.gamma(i, j, 0) = 0;
+    A gprev = 0;
+    for (int k = 1; k < nz; ++k) {
+      const A al = 1. / (s_b[k * CX + lane] - s_a[k * CX + lane] * gprev);
+      D.alpha(i, j, k) = R(al);
+      gprev = A(R(s_c[k * CX + lane] * A(R(al))));
+      D.gamma(i, j, k) = R(gprev);
+    }
+    D.alpha(i, j, nz) = R(1. / (s_b[nz * CX + lane] - s_a[nz * CX + lane] * gprev));
+    D.gamma(i, j, nz) = 0;
+  }
+}
+
+// One acoustic substep of a column block: advance_mu_t + sumflux (KMuTCol :208-249, KMuTPoint :251-277,
+// KSumEdge :281-290) (phase 1), advance_w (KWRhs / KWExpl / KWSolve :295-408) (phase 2), calc_p_rho with
+// divergence damping (KWPRho :411-416) (phase 4). The column mass sum, the running
+// omega integral and the tridiagonal sweeps are evaluated in double in both forms, on terms staged in
+// shared memory. With lateral boundaries the spec zone's columns take LateralBC::update_mu_t (phase 1) and
+// the phi'' part of update_ph_w (phase 2); the zero-gradient w of that zone needs the neighbours' new w and
+// follows in its own launch.
+template <class R>
+__global__ void __launch_bounds__(CX * CNW, 3) k_ac(const Dom<R>* __restrict__ doms, BlockMap bm, int rk, int it,
+                                                    int nsteps) {
+  constexpr int phase = 7;
+  int i, j;
+  const Dom<R>& D = cb_member(doms, bm, RG_COLS_STAG, i, j);
+  using A = double;
+  const int nx = D.nx, ny = D.ny, nz = D.nz;
+  const int lane = threadIdx.x;
+  const bool w0 = threadIdx.y == 0;
+  const bool col = i < nx + 1;
+  const R dts = R(rk == 1 ? D.dt / 3.0 : D.dt / D.n_sound);
+  const R epssm = R(D.epssm);
+  const bool first = it == 1, last = it == nsteps;
+  const R rn = R(nsteps);
+  const bool mass = col && i < nx && j < ny;
+  const bool spec = mass && edge_mass(D, i, j);
+  const bool dyn = mass && !spec;
+  double* s0 = cb_array(0, nz);
+  double* s1 = cb_array(1, nz);
+  double* s2 = cb_array(2, nz);
+  double* sc = cb_array(3, nz);  // per-column scalars: sc[n * CX + lane]
+  if (phase & 1) {
+    if (col && D.spec_x && i == nx && j < ny)  // KSumEdge, east face
+      CB_LOOP(k, nz) {
+        const R su = (first ? R(0) : D.ru_m(i, j, k)) + D.u2(i, j, k);
+        const R cpl = (R(D.c1h[k]) * D.muu(i, j, 0) + R(D.c2h[k])) * D.u_save(i, j, k);
+        D.ru_m(i, j, k) = last ? su / rn + cpl / D.msfuy(i, j) : su;
+      }
+    if (col && D.spec_y && j == ny && i < nx)  // KSumEdge, north face
+      CB_LOOP(k, nz) {
+        const R su = (first ? R(0) : D.rv_m(i, j, k)) + D.v2(i, j, k);
+        const R cpl = (R(D.c1h[k]) * D.muv(i, j, 0) + R(D.c2h[k])) * D.v_save(i, j, k);
+        D.rv_m(i, j, k) = last ? su / rn + cpl * D.msfvx_inv(i, j) : su;
+      }
+    if (spec) {  // spec zone: sumflux of ww only; mu and mu_ts take dts mu_tend (LateralBC::update_mu_t :363-372)
+      CB_LOOP(k, nz + 1) {
+        const R sw = (first ? R(0) : D.ww_m(i, j, k)) + D.ww(i, j, k);
+        D.ww_m(i, j, k) = last ? sw / rn + D.ww1(i, j, k) : sw;
+      }
+      if (w0) {
+        D.mu2(i, j, 0) += dts * D.mu_tend(i, j, 0);
+        D.muts(i, j, 0) += dts * D.mu_tend(i, j, 0);
+      }
+    }
+    if (dyn) CB_LOOP(k, nz) s0[k * CX + lane] = A(mut_dv(D, i, j, k));  // dv of each level
+    __syncthreads();
+    if (dyn && w0) {  // the column mass tendency: sum over k in order
+      A dmdt = 0;
+      for (int k = 0; k < nz; ++k) dmdt += D.dnw[k] * s0[k * CX + lane];
+      const A mtend = A(D.mu_tend(i, j, 0));
+      const A mu_old = A(D.mu2(i, j, 0));
+      const A mu_new = mu_old + A(dts) * (dmdt + mtend);
+      D.mu2(i, j, 0) = R(mu_new);
+      D.mudf(i, j, 0) = R(dmdt + mtend);
+      D.muts(i, j, 0) = D.mut(i, j, 0) + R(mu_new);
+      D.muave(i, j, 0) = R(0.5) * ((R(1) + epssm) * R(mu_new) + (R(1) - epssm) * R(mu_old));
+      sc[0 * CX + lane] = dmdt;
+      sc[1 * CX + lane] = mtend;
+    }
+    __syncthreads();
+    if (dyn) {  // the decrement of the omega integral at each level
+      const A dmdt = sc[0 * CX + lane], mtend = sc[1 * CX + lane];
+      const A msfty = A(D.msfty(i, j));
+      CB_LOOP(k, nz - 1) {
+        s1[k * CX + lane] = D.dnw[k] * (D.c1h[k] * dmdt + s0[k * CX + lane] + D.c1h[k] * mtend) / msfty;
+        s0[k * CX + lane] = A(D.ww1(i, j, k + 1));
+      }
+    }
+    __syncthreads();
+    if (dyn && w0) {  // ww'' by the running integral
+      A ww_full = 0;
+      s2[0 * CX + lane] = 0;
+      for (int k = 0; k < nz - 1; ++k) {
+        ww_full = ww_full - s1[k * CX + lane];
+        s2[(k + 1) * CX + lane] = A(R(ww_full - s0[k * CX + lane]));
+      }
+      s2[nz * CX + lane] = 0;
+    }
+    __syncthreads();
+    if (dyn) {
+      CB_LOOP(k, nz + 1) {  // ww'' and its time sum
+        const R wpp = R(s2[k * CX + lane]);
+        D.ww(i, j, k) = wpp;
+        const R sw = (first ? R(0) : D.ww_m(i, j, k)) + (k == 0 ? R(0) : wpp);
+        D.ww_m(i, j, k) = last ? sw / rn + D.ww1(i, j, k) : sw;
+      }
+    }
+    if (mass) {
+      CB_LOOP(k, nz) {  // KMuTPoint: time sums of ru, rv; theta''
+        const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
+        const R su = (first ? R(0) : D.ru_m(i, j, k)) + D.u2(i, j, k);
+        D.ru_m(i, j, k) = last ? su / rn + (c1h * D.muu(i, j, 0) + c2h) * D.u_save(i, j, k) / D.msfuy(i, j) : su;
+        if (D.do_y) {
+          const R sv = (first ? R(0) : D.rv_m(i, j, k)) + D.v2(i, j, k);
+          D.rv_m(i, j, k) = last ? sv / rn + (c1h * D.muv(i, j, 0) + c2h) * D.v_save(i, j, k) * D.msfvx_inv(i, j) : sv;
+        }
+        const R tk = D.t2(i, j, k);
+        D.t_2save(i, j, k) = tk;
+        if (spec) {  // theta'' of the spec zone (update_mu_t)
+          D.t2(i, j, k) += dts * D.t_tend(i, j, k);
+          continue;
+        }
+        R hflux = R(0.5) * R(D.rdx) *
+                  (D.u2(i + 1, j, k) * (D.t_save(i + 1, j, k) + D.t_save(i, j, k)) - D.u2(i, j, k) * (D.t_save(i, j, k) + D.t_save(i - 1, j, k)));
+        if (D.do_y)
+          hflux += R(0.5) * R(D.rdy) *
+                   (D.v2(i, j + 1, k) * (D.t_save(i, j + 1, k) + D.t_save(i, j, k)) - D.v2(i, j, k) * (D.t_save(i, j, k) + D.t_save(i, j - 1, k)));
+        const R tn = tk + D.msfty(i, j) * dts * D.t_tend(i, j, k);
+        auto wdtn = [&](int kk) -> R {
+          if (kk == 0 || kk == nz) return R(0);
+          return R(s2[kk * CX + lane]) * (R(D.fnm[kk]) * D.t_save(i, j, kk) + R(D.fnp[kk]) * D.t_save(i, j, kk - 1));
+        };
+        D.t2(i, j, k) = tn - dts * D.msfty(i, j) * (D.msftx(i, j) * hflux + R(D.rdnw[k]) * (wdtn(k + 1) - wdtn(k)));
+      }
+    }
+    __syncthreads();
+  }
+  if (phase & 2) {
+    const R ope = R(1) + epssm, ome = R(1) - epssm;
+    R mut = 0, muts = 0, mav = 0, msfty = 1;
+    double* s_a = cb_array(3, nz);
+    double* s_al = cb_array(4, nz);
+    double* s_ga = cb_array(5, nz);
+    if (spec) {  // phi'' of the spec zone (LateralBC::update_ph_w, KUpdatePh :374-386)
+      const R mts = D.muts(i, j, 0), mold = mts - dts * D.mu_tend(i, j, 0);
+      CB_LOOP(k, nz + 1) {
+        const R m_old = R(D.c1f[k]) * mold + R(D.c2f[k]), m_new = R(D.c1f[k]) * mts + R(D.c2f[k]);
+        D.ph2(i, j, k) = D.ph2(i, j, k) * m_old / m_new + dts * D.ph_tend(i, j, k) / m_new + D.ph_save(i, j, k) * (m_old / m_new - R(1));
+      }
+    }
+    if (dyn) {
+      mut = D.mut(i, j, 0);
+      muts = D.muts(i, j, 0);
+      mav = D.muave(i, j, 0);
+      msfty = D.msfty(i, j);
+      CB_LOOP(k, nz + 1) {  // KWRhs: R (explicit phi'') and t_2ave
+        R r;
+        if (k == 0 || (D.top_lid && k == nz)) {
+          r = 0;
+        } else {
+          R rr = dts * (D.ph_tend(i, j, k) + R(0.5) * R(k::g) * (R(1) - epssm) * D.w2(i, j, k));
+          if (k < nz) {
+            auto wdwn = [&](int mm) {
+              return R(0.5) * (D.ww(i, j, mm) + D.ww(i, j, mm - 1)) * R(D.rdnw[mm - 1]) *
+                     (D.ph_save(i, j, mm) - D.ph_save(i, j, mm - 1) + D.phb(i, j, mm) - D.phb(i, j, mm - 1));
+            };
+            rr -= dts * (R(D.fnm[k]) * wdwn(k + 1) + R(D.fnp[k]) * wdwn(k));
+          }
+          r = D.ph2(i, j, k) + msfty * rr / mf_(D, k, mut);
+        }
+        s0[k * CX + lane] = A(r);
+        if (k < nz) {
+          const R tav = R(0.5) * ((R(1) + epssm) * D.t2(i, j, k) + (R(1) - epssm) * D.t_2save(i, j, k));
+          s1[k * CX + lane] = A((tav + R(D.c1h[k]) * mav * R(k::t0)) / (mh_(D, k, muts) * (R(k::t0) + D.t_save(i, j, k))));
+        }
+      }
+    }
+    __syncthreads();
+    if (dyn) {
+      const R msft_inv = R(1) / msfty;
+      CB_LOOP(k, nz + 1) {  // KWExpl: explicit w''
+        R wn;
+        if (k == 0) {
+          if (!D.flat) {
+            R ws = D.msftx(i, j) * R(0.5) * R(D.rdx) *
+                   ((D.ht(i + 1, j) - D.ht(i, j)) * (R(D.cf1) * D.u2(i + 1, j, 0) + R(D.cf2) * D.u2(i + 1, j, 1) + R(D.cf3) * D.u2(i + 1, j, 2)) +
+                    (D.ht(i, j) - D.ht(i - 1, j)) * (R(D.cf1) * D.u2(i, j, 0) + R(D.cf2) * D.u2(i, j, 1) + R(D.cf3) * D.u2(i, j, 2)));
+            if (D.do_y)
+              ws = msfty * R(0.5) * R(D.rdy) *
+                       ((D.ht(i, j + 1) - D.ht(i, j)) * (R(D.cf1) * D.v2(i, j + 1, 0) + R(D.cf2) * D.v2(i, j + 1, 1) + R(D.cf3) * D.v2(i, j + 1, 2)) +
+                        (D.ht(i, j) - D.ht(i, j - 1)) * (R(D.cf1) * D.v2(i, j, 0) + R(D.cf2) * D.v2(i, j, 1) + R(D.cf3) * D.v2(i, j, 2))) +
+                   ws;
+            wn = ws;
+          } else {
+            wn = 0;
+          }
+        } else {
+          const R r_k = R(s0[k * CX + lane]), r_km1 = R(s0[(k - 1) * CX + lane]);
+          const R ph_k = D.ph2(i, j, k), ph_km1 = D.ph2(i, j, k - 1);
+          if (k < nz) {
+            const R r_kp1 = R(s0[(k + 1) * CX + lane]), ph_kp1 = D.ph2(i, j, k + 1);
+            const R cq1 = R(1) / (R(1) + cqw_(D, i, j, k));
+            wn = D.w2(i, j, k) + dts * D.rw_tend(i, j, k) +
+                 msft_inv * cq1 *
+                     (R(0.5) * dts * R(k::g) * R(D.rdn[k]) *
+                      (D.c2a(i, j, k) * R(D.rdnw[k]) / mh_(D, k, mut) * (ope * (r_kp1 - r_k) + ome * (ph_kp1 - ph_k)) -
+                       D.c2a(i, j, k - 1) * R(D.rdnw[k - 1]) / mh_(D, k - 1, mut) * (ope * (r_k - r_km1) + ome * (ph_k - ph_km1)))) +
+                 dts * R(k::g) * msft_inv *
+                     (R(D.rdn[k]) * (D.c2a(i, j, k) * D.alt(i, j, k) * R(s1[k * CX + lane]) -
+                                     D.c2a(i, j, k - 1) * D.alt(i, j, k - 1) * R(s1[(k - 1) * CX + lane])) -
+                      R(D.c1f[k]) * mav);
+          } else {
+            const int km = nz - 1;
+            wn = D.w2(i, j, k) + dts * D.rw_tend(i, j, k) +
+                 msft_inv * (-R(0.5) * dts * R(k::g) / mh_(D, km, mut) * (R(D.rdnw[km]) * R(D.rdnw[km])) * R(2) * D.c2a(i, j, km) *
+                                 (ope * (r_k - r_km1) + ome * (ph_k - ph_km1)) -
+                             dts * R(k::g) * (R(2) * R(D.rdnw[km]) * D.c2a(i, j, km) * D.alt(i, j, km) * R(s1[km * CX + lane]) +
+                                              R(D.c1f[k]) * mav));
+            if (D.top_lid) wn = 0;
+          }
+        }
+        s2[k * CX + lane] = A(wn);
+        s_a[k * CX + lane] = A(D.a(i, j, k));
+        s_al[k * CX + lane] = A(D.alpha(i, j, k));
+        s_ga[k * CX + lane] = A(D.gamma(i, j, k));
+      }
+    }
+    __syncthreads();
+    if (dyn && w0) {  // KWSolve: forward and backward sweeps
+      A wprev = s2[0 * CX + lane];
+      for (int k = 1; k <= nz; ++k) {
+        const A wk = (s2[k * CX + lane] - s_a[k * CX + lane] * wprev) * s_al[k * CX + lane];
+        wprev = A(R(wk));
+        s2[k * CX + lane] = wprev;
+      }
+      A wnext = wprev;
+      for (int k = nz - 1; k >= 1; --k) {
+        const A wk = s2[k * CX + lane] - s_ga[k * CX + lane] * wnext;
+        wnext = A(R(wk));
+        s2[k * CX + lane] = wnext;
+      }
+    }
+    __syncthreads();
+    if (dyn)
+      CB_LOOP(k, nz + 1) {  // w'' and phi''
+        const R wk = R(s2[k * CX + lane]);
+        D.w2(i, j, k) = wk;
+        if (k >= 1) D.ph2(i, j, k) = R(s0[k * CX + lane]) + msfty * R(0.5) * dts * R(k::g) * ope * wk / mf_(D, k, muts);
+      }
+    __syncthreads();
+  }
+  if ((phase & 4) && mass) CB_LOOP(k, nz) p_rho_point(D, i, j, k, true);
+}
+
+// small_step_finish (KFinish :419-444, KFinishMu :446-453) + calc_p_rho_phi (KPRhoPhi :456-477)
+template <class R>
+__global__ void __launch_bounds__(CX * CNW, 3) k_finish(const Dom<R>* __restrict__ doms, BlockMap bm, int rk, int nsmall) {
+  int i, j;
+  const Dom<R>& D = cb_member(doms, bm, RG_COLS_STAG, i, j);
+  const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
+  const bool col = i < nx + 1;
+  const bool mass = col && i < nx && j < ny;
+  const R dts = R(rk == 1 ? D.dt / 3.0 : D.dt / D.n_sound);
+  const R hd_dt = (rk == 3 && D.n_moist > 0) ? dts * R(nsmall) : R(0);
+  if (col) {
+    CB_LOOP(k, nz + 1) {
+      if (j < ny && k < nz) {
+        const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
+        const R mus_u = R(0.5) * (D.muts(i, j, 0) + D.muts(i - 1, j, 0));
+        D.u2(i, j, k) = (D.msfuy(i, j) * D.u2(i, j, k) + D.u_save(i, j, k) * (c1h * D.muu(i, j, 0) + c2h)) / (c1h * mus_u + c2h);
+      }
+      if (i < nx && j < nyv && k < nz) {
+        const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
+        const R mus_v = R(0.5) * (D.muts(i, j, 0) + D.muts(i, j - 1, 0));
+        D.v2(i, j, k) = (D.msfvx(i, j) * D.v2(i, j, k) + D.v_save(i, j, k) * (c1h * D.muv(i, j, 0) + c2h)) / (c1h * mus_v + c2h);
+      }
+      if (mass) {
+        const R m = D.mut(i, j, 0), mts = D.muts(i, j, 0);
+        D.w2(i, j, k) = (D.msfty(i, j) * D.w2(i, j, k) + D.w_save(i, j, k) * (R(D.c1f[k]) * m + R(D.c2f[k]))) / (R(D.c1f[k]) * mts + R(D.c2f[k]));
+        D.ph2(i, j, k) = D.ph2(i, j, k) + D.ph_save(i, j, k);
+        D.ww(i, j, k) = D.ww(i, j, k) + D.ww1(i, j, k);
+        if (k < nz) {
+          const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
+          D.t2(i, j, k) = (D.t2(i, j, k) - (hd_dt != R(0) ? hd_dt * (c1h * m + c2h) * D.hd(i, j, k) : R(0)) + D.t_save(i, j, k) * (c1h * m + c2h)) /
+                          (c1h * mts + c2h);
+        }
+      }
+    }
+    if (threadIdx.y == 0) {
+      if (mass) D.mu2(i, j, 0) = D.mu2(i, j, 0) + D.mu_save(i, j, 0);
+      if (j < ny) D.muus(i, j, 0) = R(0.5) * (D.muts(i, j, 0) + D.muts(i - 1, j, 0));
+      if (i < nx && j < nyv) D.muvs(i, j, 0) = R(0.5) * (D.muts(i, j, 0) + D.muts(i, j - 1, 0));
+    }
+  }
+  __syncthreads();
+  if (mass) CB_LOOP(k, nz) p_rho_phi_point(D, i, j, k);
+}
+
+// set_w_surface (KSetWSurface, rk3.cpp:173-200), fill = false
+template <class R>
+__global__ void __launch_bounds__(CX * CNW) k_w_surface(const Dom<R>* __restrict__ doms, BlockMap bm) {
+  int i, j;
+  const Dom<R>& D = cb_member(doms, bm, RG_COLS_MASS, i, j);
+  if (threadIdx.y != 0 || i >= D.nx) return;
+  const R cf1 = R(D.cf1), cf2 = R(D.cf2), cf3 = R(D.cf3);
+  const R ws = D.msfty(i, j) * R(0.5) * R(D.rdy) *
+                   ((D.ht(i, j + 1) - D.ht(i, j)) * (cf1 * D.v2(i, j + 1, 0) + cf2 * D.v2(i, j + 1, 1) + cf3 * D.v2(i, j + 1, 2)) +
+                    (D.ht(i, j) - D.ht(i, j - 1)) * (cf1 * D.v2(i, j, 0) + cf2 * D.v2(i, j, 1) + cf3 * D.v2(i, j, 2))) +
+               D.msftx(i, j) * R(0.5) * R(D.rdx) *
+                   ((D.ht(i + 1, j) - D.ht(i, j)) * (cf1 * D.u2(i + 1, j, 0) + cf2 * D.u2(i + 1, j, 1) + cf3 * D.u2(i + 1, j, 2)) +
+                    (D.ht(i, j) - D.ht(i - 1, j)) * (cf1 * D.u2(i, j, 0) + cf2 * D.u2(i, j, 1) + cf3 * D.u2(i, j, 2)));
+  D.w2(i, j, 0) = ws;
+}
+
+}  // namespace cw

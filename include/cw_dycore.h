@@ -143,6 +143,13 @@ const char* cw_last_error(cw_handle* h);
 /* Kernel launches of the last cw_step call (the count this library issued). */
 int cw_launch_count(cw_handle* h, long long* out);
 
+/* Per-kernel device time of nsteps steps run without the graph, with CUDA events around every launch
+ * (the reference's CPPWRF_KTIME table, src/core/backend.cpp:26-65); the steps advance the state.
+ * cw_profile_entry returns kernel idx (0 .. *nkernels-1): its name, total milliseconds and launches. */
+int cw_profile(cw_handle* h, int nsteps, int* nkernels);
+int cw_profile_entry(cw_handle* h, int idx, char* name, int len, double* ms, long long* launches);
+/* cudaSetDevice for the calling host thread before cw_create (one process per GPU, or a thread per GPU). */
+int cw_use_device(int device);
 /* CUDA-graph replay of the step (StepScope, src/core/backend.hpp:381-399): on by default. */
 int cw_set_graph(cw_handle* h, int on);
 

@@ -10,6 +10,7 @@
 // field after the steps, in the same order. The objects are built the way cases::Model::build builds
 // them (src/cases/model.cpp:248-449): Grid, BaseState, State + scalars, Tendencies, RK3, DiffusionDriver
 // (diff_opt 1 / km_opt 1), LateralBC.
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -67,8 +68,8 @@ void save(const real* base_ptr, const Layout& L) {
 }  // namespace
 
 int main(int argc, char** argv) {
-  if (argc != 3) {
-    std::fprintf(stderr, "usage: ref_harness input.bin output.bin\n");
+  if (argc != 3 && argc != 4) {
+    std::fprintf(stderr, "usage: ref_harness input.bin output.bin [--time]\n");
     return 2;
   }
   try {
@@ -201,7 +202,13 @@ int main(int argc, char** argv) {
       rk.set_diffusion(dd.get());
     }
     if (bc) rk.set_lateral_bc(bc.get());
+    const auto t0 = std::chrono::steady_clock::now();
     for (int n = 0; n < nsteps; ++n) rk.step(s, t, b);
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (argc == 4) {  // timing only: the step loop's wall time, no output
+      std::printf("STEP_SECONDS %.9f\n", secs);
+      return 0;
+    }
     out_f = std::fopen(argv[2], "wb");
     if (!out_f) throw std::runtime_error("cannot open output");
     each_field([&](real* p, const Layout& L) { save(p, L); }, [&](const real* p, const Layout& L) { save(p, L); },

@@ -1,6 +1,7 @@
 # SPDX-License-Identifier: GPL-3.0-or-later
-"""Runs the reference's own compiled dycore (oracle/_ref/ref_harness*, built from the CPPWRF sources by
-oracle/Makefile) on a capi.Case and returns every field. Test infrastructure only."""
+"""TEST INFRASTRUCTURE ONLY: runs the reference's own compiled dycore (oracle/_ref/ref_harness*, built from
+the CPPWRF sources by oracle/Makefile) on a capi.Case and returns every field, or times its step loop.
+Used by tests/ (parity pins) and by bench.py's CPU-baseline leg (the reference arm)."""
 import ctypes as C
 import os
 import struct
@@ -39,12 +40,10 @@ def _vertical_arrays(case):
     return arrs, scal
 
 
-def run(case, nsteps, own_pow=True):
-    """{field name: whole allocation} of the reference after nsteps (Q_* keyed 'Q_2:n')."""
-    build()
-    exe = os.path.join(REF_DIR, "ref_harness_own" if own_pow else "ref_harness")
-    with tempfile.TemporaryDirectory() as td:
-        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+def write_input(case, nsteps, fin):
+    """The harness's input file for case and nsteps."""
+    names = [n for n in capi.FIELDS if not n.startswith("Q_")]
+    if True:
         with open(fin, "wb") as f:
             f.write(bytes(case.g))
             f.write(bytes(case.o))
@@ -80,6 +79,34 @@ def run(case, nsteps, own_pow=True):
                         f.write(r[1].astype("<f8").tobytes())
                 f.write(struct.pack("<d", case.lbc_time()))
             f.write(struct.pack("<i", nsteps))
+
+
+def time_steps(case, nsteps, threads=None, own_pow=False):
+    """Wall seconds of the reference's step loop (its own CPU FP64 build, OpenMP threads) for nsteps."""
+    build()
+    exe = os.path.join(REF_DIR, "ref_harness_own" if own_pow else "ref_harness")
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+    env.setdefault("OMP_WAIT_POLICY", "passive")
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        write_input(case, nsteps, fin)
+        r = subprocess.run([exe, fin, fout, "--time"], check=True, capture_output=True, text=True, env=env)
+        for line in r.stdout.splitlines():
+            if line.startswith("STEP_SECONDS"):
+                return float(line.split()[1])
+    raise RuntimeError("ref_harness printed no STEP_SECONDS")
+
+
+def run(case, nsteps, own_pow=True):
+    """{field name: whole allocation} of the reference after nsteps (Q_* keyed 'Q_2:n')."""
+    build()
+    exe = os.path.join(REF_DIR, "ref_harness_own" if own_pow else "ref_harness")
+    names = [n for n in capi.FIELDS if not n.startswith("Q_")]
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        write_input(case, nsteps, fin)
         subprocess.run([exe, fin, fout], check=True)
         out = {}
         with open(fout, "rb") as f:

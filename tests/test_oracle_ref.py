@@ -9,7 +9,8 @@ import numpy as np
 import pytest
 
 import _oracle
-import _refdump
+import _refpath  # noqa: F401
+import refdump as _refdump
 import cases
 from cppwrf_b200 import capi
 

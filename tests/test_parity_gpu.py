@@ -67,3 +67,33 @@ def test_graph_and_eager_identical():
     b.step(2)
     for name in ("U_2", "W_2", "T_2", "PH_2", "MU_2", "P"):
         assert np.array_equal(a.field(name), b.field(name)), name
+
+
+def lam_case(nx=24, ny=20, nz=14, seed=3, n_moist=5, n_scalars=5, diff=False, hybrid_opt=2, precision=capi.FP64):
+    g = capi.grid(nx, ny, nz, 15000.0, 90.0, 0.0, dy=15000.0, p_top=5000.0, bc_x=capi.SPECIFIED, bc_y=capi.SPECIFIED)
+    o = capi.default_options(None, flat=0, n_moist=n_moist, n_scalars=n_scalars, lbc=1, time_step_sound=4,
+                             precision=precision)
+    if diff:
+        o.diff_opt, o.khdif, o.kvdif, o.pr_inv = 1, 3000.0, 1.0, 3.0
+    return capi.Case(g, o).gen_lam(seed=seed, hybrid_opt=hybrid_opt)
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(diff=True), dict(hybrid_opt=0, seed=5), dict(n_moist=2, n_scalars=3),
+                                dict(n_moist=0, n_scalars=0)],
+                         ids=["lam", "lam_diffusion", "lam_sigma", "lam_tracer", "lam_dry"])
+def test_lam_bit_exact(kw):
+    """Terrain, hybrid coordinate, moist species (PD limiter at rk 3), specified boundaries (relaxation,
+    spec zone, flow-dependent scalars), 4 steps."""
+    case = lam_case(**kw)
+    dom, orc = run_pair(case, 4)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
+def test_benchmark_workload_bit_exact():
+    """The benchmark's 119 x 89 x 44 workload (bench.py), 2 steps."""
+    import bench
+    case = bench.make_case(capi, capi.FP64)
+    dom, orc = run_pair(case, 2)
+    bad = compare_all(dom, orc, case, names=capi.STATE_FIELDS)
+    assert not bad, "\n".join(bad)
