@@ -70,9 +70,16 @@ struct Member {
   double cf1 = 0, cf2 = 0, cf3 = 0, cfn = 0, cfn1 = 0, rdx = 0, rdy = 0;
 };
 
+// the members' kernel parameter packs and each pack's block count per index range
+template <class R, int NM>
+struct Packs {
+  std::vector<Pack<R, NM>> p;
+  std::vector<std::array<int, kNumKinds>> blocks;
+};
 template <class R>
-struct DevTables {  // device copies of the Dom array and the scalar tables
-  Dom<R>* doms = nullptr;
+struct DevTables {  // the kernels' views of the members and the device scalar tables
+  Packs<R, 1> one;              // a single domain
+  Packs<R, kPackMembers> many;  // a batch, in packs of kPackMembers
   V3<R>* qtab = nullptr;  // per member: q1, q2, qn, qtf, qscale (5 x n_scalars)
   Slabs<R>* lbcq = nullptr;
 };
@@ -97,8 +104,7 @@ struct cw_handle {
   size_t arena_bytes = 0;
   DevTables<double> t64;
   DevTables<float> t32;
-  BlockMap bmap[6]{};
-  int total_blocks[6]{};
+  double* dtbc_d = nullptr;  // per member: time since the boundary data, advanced by the step on the device
   int nzmax = 0;
   size_t cb_level_bytes = 0;  // one shared level array of a column block: (nz + 2) x CX doubles
   // halo sets of the fill points
@@ -270,7 +276,7 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.hup = o.h_adv_order == 5 ? 1.0 : 0.0;
   D.vup = o.v_adv_order == 3 ? 1.0 : 0.0;
   D.w_crit_cfl = o.w_crit_cfl;
-  D.dtbc = M.dtbc;
+  D.dtbc = h->dtbc_d + mi;
   D.cf1 = M.cf1; D.cf2 = M.cf2; D.cf3 = M.cf3; D.cfn = M.cfn; D.cfn1 = M.cfn1; D.rdx = M.rdx; D.rdy = M.rdy;
   const double* v = M.vert;
   auto va = [&](int a) { return v + M.vert_off[a]; };
@@ -312,10 +318,37 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   return D;
 }
 
+// the members in packs of NM (a single domain: NM = 1; a batch: kPackMembers, the last pack partial)
+template <class R, int NM>
+void build_packs(cw_handle* h, const std::vector<Dom<R>>& doms, Packs<R, NM>& ps) {
+  ps.p.clear();
+  ps.blocks.clear();
+  const size_t nm = doms.size();
+  if ((NM == 1) != (nm == 1)) return;
+  for (size_t m0 = 0; m0 < nm; m0 += NM) {
+    Pack<R, NM> P{};
+    P.n = int(std::min(nm - m0, size_t(NM)));
+    std::array<int, kNumKinds> tot{};
+    for (int kind = 0; kind < kNumKinds; ++kind) {
+      int b = 0;
+      for (int m = 0; m < P.n; ++m) {
+        const Member& M = h->m[m0 + size_t(m)];
+        P.start[kind][m] = b;
+        b += blocks_of(kind, M.g.nx, M.g.ny, M.g.nz, nys(M.g, 'V'));
+      }
+      P.start[kind][P.n] = b;
+      tot[size_t(kind)] = b;
+    }
+    for (int m = 0; m < P.n; ++m) P.d[m] = doms[m0 + size_t(m)];
+    ps.p.push_back(P);
+    ps.blocks.push_back(tot);
+  }
+}
+
 template <class R>
 void upload_tables(cw_handle* h, DevTables<R>& T) {
   const size_t nm = h->m.size();
-  if (!T.doms) CW_CUDA(cudaMalloc(&T.doms, nm * sizeof(Dom<R>)));
+  if (!h->dtbc_d) CW_CUDA(cudaMalloc(&h->dtbc_d, nm * sizeof(double)));
   size_t nq = 0;
   for (const Member& M : h->m) nq += size_t(M.o.n_scalars);
   if (!T.qtab && nq) CW_CUDA(cudaMalloc(&T.qtab, 5 * nq * sizeof(V3<R>)));
@@ -347,7 +380,11 @@ void upload_tables(cw_handle* h, DevTables<R>& T) {
     }
     q0 += size_t(ns);
   }
-  CW_CUDA(cudaMemcpyAsync(T.doms, doms.data(), nm * sizeof(Dom<R>), cudaMemcpyHostToDevice, h->stream));
+  build_packs(h, doms, T.one);
+  build_packs(h, doms, T.many);
+  std::vector<double> dtbc(nm);
+  for (size_t mi = 0; mi < nm; ++mi) dtbc[mi] = h->m[mi].dtbc;
+  CW_CUDA(cudaMemcpyAsync(h->dtbc_d, dtbc.data(), nm * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   if (nq) {
     CW_CUDA(cudaMemcpyAsync(T.qtab, qtab.data(), qtab.size() * sizeof(V3<R>), cudaMemcpyHostToDevice, h->stream));
     CW_CUDA(cudaMemcpyAsync(T.lbcq, lbcq.data(), lbcq.size() * sizeof(Slabs<R>), cudaMemcpyHostToDevice, h->stream));
@@ -360,22 +397,10 @@ void upload_tables(cw_handle* h) {
   else upload_tables<float>(h, h->t32);
 }
 
-void build_blockmaps(cw_handle* h) {
+void size_column_blocks(cw_handle* h) {
   h->nzmax = 0;
   for (const Member& M : h->m) h->nzmax = std::max(h->nzmax, M.g.nz);
   h->cb_level_bytes = size_t(h->nzmax + 2) * CX * sizeof(double);
-  for (int kind = 0; kind < 6; ++kind) {
-    BlockMap& bm = h->bmap[kind];
-    bm.n = int(h->m.size());
-    int s = 0;
-    for (size_t mi = 0; mi < h->m.size(); ++mi) {
-      bm.start[mi] = s;
-      const Member& M = h->m[mi];
-      s += blocks_of(kind, M.g.nx, M.g.ny, M.g.nz, nys(M.g, 'V'));
-    }
-    bm.start[h->m.size()] = s;
-    h->total_blocks[kind] = s;
-  }
 }
 
 // ---- halo sets
@@ -434,6 +459,7 @@ void finish_haloset(cw_handle* h, HaloSetHost& s) {
     CW_CUDA(cudaMemcpy(s.fd, s.f.data(), nf * sizeof(HaloField), cudaMemcpyHostToDevice));
     CW_CUDA(cudaMemcpy(s.startd, start.data(), (nf + 1) * sizeof(long long), cudaMemcpyHostToDevice));
   }
+  if (start[nf] >= (1ll << 31)) throw std::runtime_error("a halo fill of more than 2^31 cells");
   s.set = HaloSet{s.fd, s.startd, nf, start[nf], odd};
 }
 
@@ -546,41 +572,55 @@ struct Launcher {
     k_copy<<<unsigned((total + bs - 1) / bs), bs, 0, h->stream>>>(d, int(n), sd);
     check();
   }
-  // a point kernel over the index range kind
-  template <class R, class K, class... Args>
-  void run(const char* name, int kind, K kern, const Dom<R>* doms, Args... args) {
-    const int nb = h->total_blocks[kind];
-    if (nb == 0) return;
-    begin(name);
-    kern<<<nb, PX, 0, h->stream>>>(doms, h->bmap[kind], args...);
-    check();
+  // a point kernel over the index range kind, one launch per pack
+  template <class R, int NM, class K, class... Args>
+  void run(const char* name, int kind, K kern, const Packs<R, NM>& ps, Args... args) {
+    for (size_t c = 0; c < ps.p.size(); ++c) {
+      const int nb = ps.blocks[c][size_t(kind)];
+      if (nb == 0) continue;
+      begin(name);
+      kern<<<nb, PX, 0, h->stream>>>(ps.p[c], args...);
+      check();
+    }
   }
   // a point kernel over the index range kind, once per species (blockIdx.y)
-  template <class R, class K, class... Args>
-  void run_q(const char* name, int kind, int nq, K kern, const Dom<R>* doms, Args... args) {
-    const int nb = h->total_blocks[kind];
-    if (nb == 0 || nq == 0) return;
-    begin(name);
-    kern<<<dim3(nb, nq), PX, 0, h->stream>>>(doms, h->bmap[kind], args...);
-    check();
+  template <class R, int NM, class K, class... Args>
+  void run_q(const char* name, int kind, int nq, K kern, const Packs<R, NM>& ps, Args... args) {
+    for (size_t c = 0; c < ps.p.size(); ++c) {
+      const int nb = ps.blocks[c][size_t(kind)];
+      if (nb == 0 || nq == 0) continue;
+      begin(name);
+      kern<<<dim3(nb, nq), PX, 0, h->stream>>>(ps.p[c], args...);
+      check();
+    }
   }
   // a column-block kernel using `arrays` shared level arrays
-  template <class R, class K, class... Args>
-  void run_cb(const char* name, int kind, int arrays, K kern, const Dom<R>* doms, Args... args) {
+  template <class R, int NM, class K, class... Args>
+  void run_cb(const char* name, int kind, int arrays, K kern, const Packs<R, NM>& ps, Args... args) {
     static_assert(CX == 32, "a column block's lanes are one warp");
-    const int nb = h->total_blocks[kind];
-    if (nb == 0) return;
-    begin(name);
     const size_t smem = size_t(arrays) * h->cb_level_bytes;
     CW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    kern<<<nb, dim3(CX, CNW), smem, h->stream>>>(doms, h->bmap[kind], args...);
-    check();
+    for (size_t c = 0; c < ps.p.size(); ++c) {
+      const int nb = ps.blocks[c][size_t(kind)];
+      if (nb == 0) continue;
+      begin(name);
+      kern<<<nb, dim3(CX, CNW), smem, h->stream>>>(ps.p[c], args...);
+      check();
+    }
+  }
+  // one block per member
+  template <class R, int NM, class K>
+  void run_members(const char* name, int threads, K kern, const Packs<R, NM>& ps) {
+    for (size_t c = 0; c < ps.p.size(); ++c) {
+      begin(name);
+      kern<<<unsigned(ps.p[c].n), threads, 0, h->stream>>>(ps.p[c]);
+      check();
+    }
   }
 };
 
-template <class R>
-void enqueue_step(cw_handle* h, Launcher& L, DevTables<R>& T) {
-  const Dom<R>* d = T.doms;
+template <class R, int NM>
+void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
   const Member& M0 = h->m[0];
   bool lbc = false, terrain = false, scalars = false, any_pd = false;
   int nq = 0;  // the most species of a member
@@ -594,64 +634,65 @@ void enqueue_step(cw_handle* h, Launcher& L, DevTables<R>& T) {
   }
   const int n_sound = M0.n_sound;
   if (lbc) {
-    L.begin("k_advance_time");
-    k_advance_time<R><<<unsigned(h->m.size()), 1, 0, h->stream>>>(T.doms, int(h->m.size()));
-    L.check();
+    L.run_members("k_advance_time", 1, k_advance_time<R, NM>, d);
   }
   L.copy_list(h->copies_d, h->copies_start_d, h->copies.size(), h->copies_total);
   L.halo(cw_handle::H_MU1);
   for (int rk = 1; rk <= 3; ++rk) {
     const int ns = rk == 1 ? 1 : (rk == 2 ? n_sound / 2 : n_sound);
     L.halo(cw_handle::H_PREP0);
-    L.run_cb("k_ls_prep", RG_COLS_STAG, 1, k_ls_prep<R>, d);
+    L.run_cb("k_ls_prep", RG_COLS_STAG, 1, k_ls_prep<R, NM>, d);
     L.halo(cw_handle::H_PREP1);
-    if (rk == 1) L.run("k_tendf_rk1", RG_STAG, k_tendf_rk1<R>, d);
-    L.run("k_tend", RG_STAG, k_tend<R>, d, rk);
+    if (rk == 1) L.run("k_tendf_rk1", RG_STAG, k_tendf_rk1<R, NM>, d);
+    L.run("k_tend", RG_STAG, k_tend<R, NM>, d, rk);
     if (rk == 1) L.copy_list(h->zeros_d, h->zeros_start_d, h->zeros.size(), h->zeros_total);
-    L.run_cb("k_ss_prep", RG_COLS_STAG, 3, k_ss_prep<R>, d, rk);
+    L.run_cb("k_ss_prep", RG_COLS_STAG, 3, k_ss_prep<R, NM>, d, rk);
     L.halo(cw_handle::H_SS0);
     for (int it = 1; it <= ns; ++it) {
-      L.run("k_uv", RG_STAG, k_uv<R>, d, rk);
+      L.run("k_uv", RG_STAG, k_uv<R, NM>, d, rk);
       L.halo(cw_handle::H_UV);
-      L.run_cb("k_ac", RG_COLS_STAG, kCbArrays, k_ac<R>, d, rk, it, ns);
-      if (lbc) L.run("k_ring", RG_RING, k_ring<R>, d, int(RO_ZERO_GRAD_W), rk);
+      L.run_cb("k_ac", RG_COLS_STAG, kCbArrays, k_ac<R, NM>, d, rk, it, ns);
+      if (lbc) L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_ZERO_GRAD_W), rk);
       L.halo(cw_handle::H_AC);
     }
     L.halo(cw_handle::H_POST);
-    L.run_cb("k_finish", RG_COLS_STAG, 0, k_finish<R>, d, rk, ns);
+    L.run_cb("k_finish", RG_COLS_STAG, 0, k_finish<R, NM>, d, rk, ns);
     L.halo(cw_handle::H_FIN);
     if (scalars) {
-      if (rk == 1) L.run_q("k_q_tendf_rk1", RG_MASS, nq, k_q_tendf_rk1<R>, d);
-      L.run_q("k_q_update", RG_MASS, nq, k_q_update<R>, d, rk);
+      if (rk == 1) L.run_q("k_q_tendf_rk1", RG_MASS, nq, k_q_tendf_rk1<R, NM>, d);
+      L.run_q("k_q_update", RG_MASS, nq, k_q_update<R, NM>, d, rk);
       if (rk == 3 && any_pd) {
-        L.run_q("k_q_pre_pd", RG_MASS, nq, k_q_pre_pd<R>, d, rk);
+        L.run_q("k_q_pre_pd", RG_MASS, nq, k_q_pre_pd<R, NM>, d, rk);
         L.halo(cw_handle::H_Q1PD);
-        L.run_q("k_q_scale_pd", RG_MASS, nq, k_q_scale_pd<R>, d, rk);
+        L.run_q("k_q_scale_pd", RG_MASS, nq, k_q_scale_pd<R, NM>, d, rk);
         L.halo(cw_handle::H_SCPD);
-        L.run_q("k_q_update_pd", RG_MASS, nq, k_q_update_pd<R>, d, rk);
+        L.run_q("k_q_update_pd", RG_MASS, nq, k_q_update_pd<R, NM>, d, rk);
       }
-      L.begin("k_q_swap");
-      k_q_swap<R><<<unsigned(h->m.size()), 64, 0, h->stream>>>(T.doms, int(h->m.size()));
-      L.check();
-      if (lbc) L.run("k_ring", RG_RING, k_ring<R>, d, int(RO_FLOW_DEP), rk);
+      L.run_members("k_q_swap", 64, k_q_swap<R, NM>, d);
+      if (lbc) L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_FLOW_DEP), rk);
       L.halo(cw_handle::H_Q2);
     }
   }
   if (lbc) {
-    L.run("k_ring", RG_RING, k_ring<R>, d, int(RO_FINAL), 3);
-    L.run("k_p_rho_phi", RG_MASS, k_p_rho_phi<R>, d, 1);
+    L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_FINAL), 3);
+    L.run("k_p_rho_phi", RG_MASS, k_p_rho_phi<R, NM>, d, 1);
     L.halo(cw_handle::H_END_P);
   }
   if (terrain) {
     L.halo(cw_handle::H_WS0);
-    L.run_cb("k_w_surface", RG_COLS_MASS, 0, k_w_surface<R>, d);
+    L.run_cb("k_w_surface", RG_COLS_MASS, 0, k_w_surface<R, NM>, d);
     L.halo(cw_handle::H_WS1);
   }
 }
 
+template <class R>
+void enqueue_t(cw_handle* h, Launcher& L, const DevTables<R>& T) {
+  if (h->m.size() == 1) enqueue_step<R, 1>(h, L, T.one);
+  else enqueue_step<R, kPackMembers>(h, L, T.many);
+}
 void enqueue(cw_handle* h, Launcher& L) {
-  if (h->precision == CW_FP64) enqueue_step<double>(h, L, h->t64);
-  else enqueue_step<float>(h, L, h->t32);
+  if (h->precision == CW_FP64) enqueue_t<double>(h, L, h->t64);
+  else enqueue_t<float>(h, L, h->t32);
 }
 
 void invalidate_graph(cw_handle* h) {
@@ -710,7 +751,7 @@ Member make_member(const cw_grid& g, const cw_options& o) {
 void setup(cw_handle* h) {
   allocate(h);
   upload_tables(h);
-  build_blockmaps(h);
+  size_column_blocks(h);
   if (h->precision == CW_FP64) build_halosets_t<double>(h, h->t64);
   else build_halosets_t<float>(h, h->t32);
   build_copies(h);
@@ -805,10 +846,9 @@ int cw_destroy(cw_handle* h) {
   cudaFree(h->copies_start_d);
   cudaFree(h->zeros_d);
   cudaFree(h->zeros_start_d);
-  cudaFree(h->t64.doms);
+  cudaFree(h->dtbc_d);
   cudaFree(h->t64.qtab);
   cudaFree(h->t64.lbcq);
-  cudaFree(h->t32.doms);
   cudaFree(h->t32.qtab);
   cudaFree(h->t32.lbcq);
   cudaFree(h->arena);

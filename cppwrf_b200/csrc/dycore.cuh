@@ -2,9 +2,9 @@
 // Device-side data model of the dycore: one Dom per domain (a member of a batch), views in CPPWRF's
 // field layout, the launch geometry shared by every kernel, and the WRF flux statement functions.
 //
-// Every kernel takes a device array of Dom and a BlockMap: block b of a launch belongs to member
-// m = the last index with start[m] <= b, so one launch covers all members of a batch whatever their
-// sizes (a single domain is a batch of one).
+// Every kernel takes a Pack of members: block b of a launch belongs to member m = the last index with
+// start[m] <= b, so one launch covers all members of a pack whatever their sizes (a single domain is a
+// pack of one).
 #pragma once
 
 #include <cstdint>
@@ -46,7 +46,8 @@ struct Dom {
   int nx, ny, nz, nyv, two_d, do_y;
   int bc_x, bc_y, spec_x, spec_y;  // spec_*: specified in that direction (degraded orders, spec zone)
   int lbc, flat, n_moist, n_scalars, diff_on, top_lid, w_damping, n_sound, moist_adv_opt, scalar_adv_opt;
-  double dt, epssm, smdiv, emdiv, khdif, kvdif, prandtl, hup, vup, w_crit_cfl, dtbc;
+  double dt, epssm, smdiv, emdiv, khdif, kvdif, prandtl, hup, vup, w_crit_cfl;
+  double* dtbc;  // device scalar: time since the boundary data (LateralBC::dtbc), advanced on the device
   double rdx, rdy, cf1, cf2, cf3, cfn, cfn1;
   const double *znu, *znw, *dnw, *dn, *rdnw, *rdn, *fnm, *fnp, *c1h, *c2h, *c1f, *c2f, *u_base, *v_base;
   const double *fcx, *gcx;  // relaxation weights per row (LateralBC::set_dt)
@@ -71,19 +72,31 @@ struct Dom {
   Slabs<T>* lbc_q;
 };
 
-struct BlockMap {
+// The kernels' view of up to NM members, passed by value as a __grid_constant__ parameter: the field
+// descriptors are read from the constant bank (operands of the address arithmetic for a single domain,
+// NM = 1) and no store of a kernel can alias them. start[kind][m] is member m's first block of a launch
+// over the index range `kind`; a batch of more members is launched in packs of kPackMembers.
+constexpr int kNumKinds = 6;
+constexpr int kPackMembers = 12;
+template <class R, int NM>
+struct Pack {
+  Dom<R> d[NM];
   int n;
-  int start[kMaxMembers + 1];
+  int start[kNumKinds][NM + 1];
 };
-
-__device__ __forceinline__ int member_of(const BlockMap& bm, int b) {
-  int lo = 0, hi = bm.n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (bm.start[mid] <= b) lo = mid;
-    else hi = mid - 1;
+template <class R, int NM>
+__device__ __forceinline__ int member_of(const Pack<R, NM>& P, int kind, int b) {
+  if constexpr (NM == 1) {
+    return 0;
+  } else {
+    int lo = 0, hi = P.n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (P.start[kind][mid] <= b) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
   }
-  return lo;
 }
 
 // Block geometry of the two launch shapes. Point kernels: PX threads along i, blockIdx over (i-tiles, j, k)

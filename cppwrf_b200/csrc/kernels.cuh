@@ -44,17 +44,16 @@ __host__ __device__ __forceinline__ int blocks_of(int kind, int nx, int ny, int 
   return cdiv(r.i1 - r.i0, tx) * (r.j1 - r.j0) * (r.k1 - r.k0);
 }
 // thread -> (member, i, j, k); false for the threads past the range
-template <class R>
-__device__ __forceinline__ bool thread_index(const Dom<R>* __restrict__ doms, const BlockMap& bm, int kind,
-                                             const Dom<R>*& Dp, int& i, int& j, int& k) {
+template <class R, int NM>
+__device__ __forceinline__ bool thread_index(const Pack<R, NM>& P, int kind, const Dom<R>*& Dp, int& i, int& j, int& k) {
   const int b = blockIdx.x;
-  const int m = member_of(bm, b);
-  const Dom<R>& D = doms[m];
+  const int m = member_of(P, kind, b);
+  const Dom<R>& D = P.d[m];
   Dp = &D;
   const Range r = range_of(kind, D.nx, D.ny, D.nz, D.nyv);
   const int tx = is_column(kind) ? CX : PX;
   const int bx = cdiv(r.i1 - r.i0, tx), by = r.j1 - r.j0;
-  int local = b - bm.start[m];
+  int local = b - P.start[kind][m];
   const int bi = local % bx;
   local /= bx;
   j = r.j0 + local % by;
@@ -120,13 +119,13 @@ __device__ __forceinline__ T halo_xval(const HaloField& f, T* p, int i, int j, i
 }
 
 template <class T>
-__device__ __forceinline__ void halo_cell(const HaloField& f, long long c, int pass) {
+__device__ __forceinline__ void halo_cell(const HaloField& f, unsigned c, int pass) {
   T* p = static_cast<T*>(f.ind ? static_cast<V3<T>*>(f.ind)->p : f.p);
-  if (c < f.ncell_x) {  // x pass: (k, row j, slot a)
-    const int na = f.face_x ? 8 : 6;
+  if (c < unsigned(f.ncell_x)) {  // x pass: (k, row j, slot a)
+    const unsigned na = f.face_x ? 8 : 6;
     const int a = int(c % na);
-    const long long r = c / na;
-    const int j = int(r % f.lny), k = int(r / f.lny);
+    const unsigned r = c / na;
+    const int j = int(r % unsigned(f.lny)), k = int(r / unsigned(f.lny));
     const int i = halo_pos(a, f.gnx, f.face_x);
     if (i < f.wi0 || i >= f.wi1) return;
     const int src = halo_src(i, f.gnx, f.face_x, f.periodic_x, f.flat_x);
@@ -142,11 +141,11 @@ __device__ __forceinline__ void halo_cell(const HaloField& f, long long c, int p
   }
   if (pass == 1) return;
   // y pass: (k, slot b, column i over the full x extent)
-  const long long cy = c - f.ncell_x;
-  const int wiw = f.wi1 - f.wi0;
-  const int na = f.face_y ? 8 : 6;
+  const unsigned cy = c - unsigned(f.ncell_x);
+  const unsigned wiw = unsigned(f.wi1 - f.wi0);
+  const unsigned na = f.face_y ? 8 : 6;
   const int i = f.wi0 + int(cy % wiw);
-  const long long r = cy / wiw;
+  const unsigned r = cy / wiw;
   const int b = int(r % na), k = int(r / na);
   const int jh = halo_pos(b, f.gny, f.face_y);
   if (jh < f.wj0 || jh >= f.wj1) return;
@@ -157,17 +156,18 @@ __device__ __forceinline__ void halo_cell(const HaloField& f, long long c, int p
   p[i + jh * f.sj + k * f.sk] = v;
 }
 
+// one thread per halo cell of the set (the host keeps a set's cell count below 2^31)
 static __global__ void k_halo(HaloSet s, int pass) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= s.total) return;
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= unsigned(s.total)) return;
   int lo = 0, hi = s.nf - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (s.start[mid] <= t) lo = mid;
+    if (unsigned(s.start[mid]) <= t) lo = mid;
     else hi = mid - 1;
   }
   const HaloField& f = s.f[lo];
-  const long long c = t - s.start[lo];
+  const unsigned c = t - unsigned(s.start[lo]);
   if (f.is_float) halo_cell<float>(f, c, pass);
   else halo_cell<double>(f, c, pass);
 }
@@ -557,7 +557,7 @@ template <class R, bool Two>
 __device__ void relax_terms(const Dom<R>& D, const V3<R>& f, const double* c1, const double* c2, const Slabs<R>& s,
                             Ring r, int pos, int side, int b, int k, int i, int j, R& fa, R& fb) {
   const int sl = slab_of_side(side);
-  const R dtbc = R(D.dtbc);
+  const R dtbc = R(*D.dtbc);
   auto BV = [&](int p, int bb) { return slab_val(s, sl, p, k, bb, dtbc); };
   auto FV = [&](int ii, int jj) -> R {
     const R x = Two ? f(ii, jj, 0) : f(ii, jj, k);
@@ -605,11 +605,11 @@ __device__ __forceinline__ bool spec_at(Ring r, int i, int j, int& sl, int& pos)
 // its own range: ru (u_i0 .. u_i1), rv (v_j0 .. v_j1, 3-D), rw and ph (levels 1..nz), theta (mass cells).
 // Also mu_tend = 0 (zero_tend of a run with lateral boundaries) at rk 2 and 3, and with lateral
 // boundaries the spec zone's tendencies from the boundary slabs.
-template <class R>
-__global__ void __launch_bounds__(PX) k_tend(const Dom<R>* __restrict__ doms, BlockMap bm, int rk) {
+template <class R, int NM>
+__global__ void __launch_bounds__(PX) k_tend(const __grid_constant__ Pack<R, NM> P, int rk) {
   const Dom<R>* Dp;
   int i, j, k;
-  if (!thread_index(doms, bm, RG_STAG, Dp, i, j, k)) return;
+  if (!thread_index(P, RG_STAG, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
   const int nx = D.nx, ny = D.ny, nz = D.nz;
   const bool use_tendf = D.lbc || D.diff_on;
@@ -773,11 +773,11 @@ __device__ __forceinline__ R vdiff_uv(const Dom<R>& D, const V3<R>& f, const dou
 
 // rk 1: zero the held tendencies, add the constant-K diffusion; with lateral boundaries mu_tend = 0 and the
 // relaxation of rows 1..3 (LateralBC::relax_dry, lateral_bc.cpp:294-335) added to the held tendencies
-template <class R>
-__global__ void __launch_bounds__(PX) k_tendf_rk1(const Dom<R>* __restrict__ doms, BlockMap bm) {
+template <class R, int NM>
+__global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R, NM> P) {
   const Dom<R>* Dp;
   int i, j, k;
-  if (!thread_index(doms, bm, RG_STAG, Dp, i, j, k)) return;
+  if (!thread_index(P, RG_STAG, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
   const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
   const bool dd = D.diff_on;
@@ -854,11 +854,11 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const Dom<R>* __restrict__ dom
 // flow_dep_bdy of the scalars without boundary data, zero_grad_bdy of w. The other boundary operations run
 // inside the kernels that compute the same points (k_tendf_rk1, k_tend, k_uv, k_ac, k_q_tendf_rk1).
 enum RingOp { RO_FINAL = 0, RO_FLOW_DEP, RO_ZERO_GRAD_W };
-template <class R>
-__global__ void __launch_bounds__(PX) k_ring(const Dom<R>* __restrict__ doms, BlockMap bm, int op, int rk) {
+template <class R, int NM>
+__global__ void __launch_bounds__(PX) k_ring(const __grid_constant__ Pack<R, NM> P, int op, int rk) {
   const Dom<R>* Dp;
   int pos, k, side;
-  if (!thread_index(doms, bm, RG_RING, Dp, pos, k, side)) return;
+  if (!thread_index(P, RG_RING, Dp, pos, k, side)) return;
   const Dom<R>& D = *Dp;
   (void)rk;
   const int nx = D.nx, ny = D.ny, nz = D.nz;
@@ -880,7 +880,7 @@ __global__ void __launch_bounds__(PX) k_ring(const Dom<R>* __restrict__ doms, Bl
     case RO_FINAL: {  // final (:425-455)
       int i, j;
       const int sl = slab_of_side(side);
-      const R dtbc = R(D.dtbc);
+      const R dtbc = R(*D.dtbc);
       if (k < nz && ring_for(nx, ny, 'u').map(pos, side, 0, i, j)) {
         const R bval = slab_val(D.lbc_var[0], sl, pos, k, 0, dtbc);
         D.u2(i, j, k) = D.msfuy(i, j) * bval / (R(D.c1h[k]) * D.muus(i, j, 0) + R(D.c2h[k]));
@@ -931,10 +931,10 @@ __global__ void __launch_bounds__(PX) k_ring(const Dom<R>* __restrict__ doms, Bl
 }
 
 // LateralBC::advance_time (lateral_bc.hpp:58): dtbc += dt at the start of every step
-template <class R>
-__global__ void k_advance_time(Dom<R>* doms, int nmembers) {
+template <class R, int NM>
+__global__ void k_advance_time(const __grid_constant__ Pack<R, NM> P) {
   const int m = blockIdx.x;
-  if (m < nmembers && threadIdx.x == 0 && doms[m].lbc) doms[m].dtbc += doms[m].dt;
+  if (m < P.n && threadIdx.x == 0 && P.d[m].lbc) *P.d[m].dtbc += P.d[m].dt;
 }
 
 }  // namespace cw

@@ -13,15 +13,14 @@ namespace cw {
 #define CB_LOOP(k, n) for (int k = int(threadIdx.y); k < (n); k += CNW)
 
 // block -> (member, column i of this lane, row j)
-template <class R>
-__device__ __forceinline__ const Dom<R>& cb_member(const Dom<R>* __restrict__ doms, const BlockMap& bm, int kind, int& i,
-                                                   int& j) {
+template <class R, int NM>
+__device__ __forceinline__ const Dom<R>& cb_member(const Pack<R, NM>& P, int kind, int& i, int& j) {
   const int b = blockIdx.x;
-  const int m = member_of(bm, b);
-  const Dom<R>& D = doms[m];
+  const int m = member_of(P, kind, b);
+  const Dom<R>& D = P.d[m];
   const Range r = range_of(kind, D.nx, D.ny, D.nz, D.nyv);
   const int bx = cdiv(r.i1 - r.i0, CX);
-  const int local = b - bm.start[m];
+  const int local = b - P.start[kind][m];
   i = r.i0 + (local % bx) * CX + int(threadIdx.x);
   j = r.j0 + local / bx;
   return D;
@@ -33,10 +32,10 @@ __device__ __forceinline__ double* cb_array(int a, int nz) {
 }
 
 // rk_step_prep: KMu (large_step.cpp:49-66), KPrep3 (:68-81), KWW (:83-108), KCq (:127-148)
-template <class R>
-__global__ void __launch_bounds__(CX * CNW, 3) k_ls_prep(const Dom<R>* __restrict__ doms, BlockMap bm) {
+template <class R, int NM>
+__global__ void __launch_bounds__(CX * CNW, 3) k_ls_prep(const __grid_constant__ Pack<R, NM> P) {
   int i, j;
-  const Dom<R>& D = cb_member(doms, bm, RG_COLS_STAG, i, j);
+  const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j);
   const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
   const int lane = threadIdx.x;
   const bool col = i < nx + 1;
@@ -116,10 +115,10 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ls_prep(const Dom<R>* __restric
 }
 
 // small_step_prep (KPrep small_step.cpp:50-93) + calc_p_rho (KPRho :114-119) + calc_coef_w (KCoefW :122-148)
-template <class R>
-__global__ void __launch_bounds__(CX * CNW, 3) k_ss_prep(const Dom<R>* __restrict__ doms, BlockMap bm, int rk) {
+template <class R, int NM>
+__global__ void __launch_bounds__(CX * CNW, 3) k_ss_prep(const __grid_constant__ Pack<R, NM> P, int rk) {
   int i, j;
-  const Dom<R>& D = cb_member(doms, bm, RG_COLS_STAG, i, j);
+  const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j);
   const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
   const int lane = threadIdx.x;
   const bool col = i < nx + 1;
@@ -227,12 +226,12 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ss_prep(const Dom<R>* __restric
 // shared memory. With lateral boundaries the spec zone's columns take LateralBC::update_mu_t (phase 1) and
 // the phi'' part of update_ph_w (phase 2); the zero-gradient w of that zone needs the neighbours' new w and
 // follows in its own launch.
-template <class R>
-__global__ void __launch_bounds__(CX * CNW, 3) k_ac(const Dom<R>* __restrict__ doms, BlockMap bm, int rk, int it,
+template <class R, int NM>
+__global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack<R, NM> P, int rk, int it,
                                                     int nsteps) {
   constexpr int phase = 7;
   int i, j;
-  const Dom<R>& D = cb_member(doms, bm, RG_COLS_STAG, i, j);
+  const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j);
   using A = double;
   const int nx = D.nx, ny = D.ny, nz = D.nz;
   const int lane = threadIdx.x;
@@ -463,10 +462,10 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const Dom<R>* __restrict__ d
 }
 
 // small_step_finish (KFinish :419-444, KFinishMu :446-453) + calc_p_rho_phi (KPRhoPhi :456-477)
-template <class R>
-__global__ void __launch_bounds__(CX * CNW, 3) k_finish(const Dom<R>* __restrict__ doms, BlockMap bm, int rk, int nsmall) {
+template <class R, int NM>
+__global__ void __launch_bounds__(CX * CNW, 3) k_finish(const __grid_constant__ Pack<R, NM> P, int rk, int nsmall) {
   int i, j;
-  const Dom<R>& D = cb_member(doms, bm, RG_COLS_STAG, i, j);
+  const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j);
   const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
   const bool col = i < nx + 1;
   const bool mass = col && i < nx && j < ny;
@@ -507,10 +506,10 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_finish(const Dom<R>* __restrict
 }
 
 // set_w_surface (KSetWSurface, rk3.cpp:173-200), fill = false
-template <class R>
-__global__ void __launch_bounds__(CX * CNW) k_w_surface(const Dom<R>* __restrict__ doms, BlockMap bm) {
+template <class R, int NM>
+__global__ void __launch_bounds__(CX * CNW) k_w_surface(const __grid_constant__ Pack<R, NM> P) {
   int i, j;
-  const Dom<R>& D = cb_member(doms, bm, RG_COLS_MASS, i, j);
+  const Dom<R>& D = cb_member(P, RG_COLS_MASS, i, j);
   if (threadIdx.y != 0 || i >= D.nx) return;
   const R cf1 = R(D.cf1), cf2 = R(D.cf2), cf3 = R(D.cf3);
   const R ws = D.msfty(i, j) * R(0.5) * R(D.rdy) *

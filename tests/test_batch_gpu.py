@@ -46,3 +46,22 @@ def test_batch_mixed_nz_and_ideal():
         orc.step(2)
         for name in ("U_2", "W_2", "T_2", "MU_2", "P"):
             assert np.array_equal(b.field(m, name).view(np.uint64), orc.array(name).view(np.uint64)), (m, name)
+
+
+def test_batch_more_members_than_a_pack():
+    """A batch larger than one kernel parameter pack (12 members) is launched pack by pack; every member
+    still matches the oracle bit for bit, the species count differing between members."""
+    cases = [lam_case(nx=14 + (m % 5), ny=12 + (m % 3), nz=10, seed=20 + m, n_moist=2 + (m % 2),
+                      n_scalars=2 + (m % 2) + (m % 3)) for m in range(14)]
+    b = Batch([c.g for c in cases], [c.o for c in cases])
+    for m, c in enumerate(cases):
+        b.upload_case(m, c)
+    b.step(2)
+    b.sync()
+    for m, c in enumerate(cases):
+        orc = _oracle.Oracle(c)
+        orc.step(2)
+        for name in ("U_2", "V_2", "W_2", "T_2", "PH_2", "MU_2", "P"):
+            assert np.array_equal(b.field(m, name).view(np.uint64), orc.array(name).view(np.uint64)), (m, name)
+        for n in range(c.o.n_scalars):
+            assert np.array_equal(b.field(m, "Q_2", n).view(np.uint64), orc.array("Q_2", n).view(np.uint64)), (m, n)
