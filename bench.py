@@ -56,10 +56,9 @@ ALG_ARRAYS = {
     "k_tend": 24 + 5,         # u2 v2 w2 t2 ph2 ru rv rw ww p al alt php pb phb 5 tendf cqu cqv cqw hd | 5 tend
     "k_ss_prep": 15 + 18,     # u2 v2 w2 t2 ph2 u1 v1 w1 t1 ph1 ww p alt pb cqw | 5 state 5 saves ww1 c2a al p pm1 a alpha gamma
     "k_uv": 12 + 2,           # u2 v2 ru_tend rv_tend p al alt ph2 php pb cqu cqv | u2 v2
-    "k_ac": 22 + 11,          # u2 v2 u_save v_save ww1 ww_m ru_m rv_m t2 t_save t_tend w2 ph2 rw_tend ph_tend
-                              # ph_save phb c2a alt a alpha gamma | ww ww_m ru_m rv_m t2 t_2save w2 ph2 w_rhs t2a (+)
+    "k_ac": 24 + 11,          # u2 v2 u_save v_save ww1 ww_m ru_m rv_m t2 t_save t_tend w2 ph2 rw_tend ph_tend
+                              # ph_save phb c2a alt a alpha gamma cqw pm1 | ww ww_m ru_m rv_m t2 t_2save w2 ph2 al p pm1
     "k_finish": 15 + 8,       # u2 v2 w2 t2 ph2 ww 5 saves ww1 hd alb pb | u2 v2 w2 t2 ph2 ww al p
-    "k_wprho": 9 + 3,         # ph2 alt t2 t_save c2a pm1 (+ mu muts 2-D) | al p pm1
     "k_q_update": 3 + 3 + 1,  # per species: q2 q1 qtf + ru_m rv_m ww_m | qn
     "k_q_update_pd": 4 + 3 + 1,
     "k_q_scale_pd": 2 + 3 + 1,
