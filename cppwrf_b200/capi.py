@@ -40,6 +40,9 @@ XS, XE, YS, YE = range(4)
 # enum cw_ideal_kind
 REST_STATE, STRAKA, WARM_BUBBLE, IGW = range(4)
 DEFAULT = -1.0e300
+# cw_download_noalloc: scratch capacity (doubles) and return codes
+NOALLOC_SCRATCH_DOUBLES = 1048576
+NOALLOC_EBADARG, NOALLOC_ETOOBIG, NOALLOC_ECUDA = -1, -2, -3
 
 
 class Grid(C.Structure):
@@ -141,6 +144,7 @@ def load(path=None):
         "cw_member_upload": (i, [vp, i, i, i, dp, sz]),
         "cw_member_download": (i, [vp, i, i, i, dp, sz]),
         "cw_member_field_layout": (i, [vp, i, i, i, C.POINTER(Layout)]),
+        "cw_download_noalloc": (i, [vp, i, i, dp, sz]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name, None)

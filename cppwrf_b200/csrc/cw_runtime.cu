@@ -12,10 +12,12 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <utility>
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -1162,3 +1164,67 @@ int cw_member_upload_case(cw_handle* h, int mi, cw_case* c) {
 int cw_upload_case(cw_handle* h, cw_case* c) { return cw_member_upload_case(h, 0, c); }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ download without allocating
+// cw_download stages an FP32 field through a host vector (it widens to double on the host). Some callers
+// cannot allocate at that moment: a checkpoint or state dump written after an allocation has failed (host
+// or device memory exhausted), or a serving loop that has committed the whole device-memory budget to
+// resident domains. cw_download_noalloc widens on the device into a scratch array that is part of the
+// library image (a file-scope __device__ array, no cudaMalloc), then copies it to the caller's buffer.
+namespace {
+
+constexpr size_t kNoallocScratchDoubles = CW_NOALLOC_SCRATCH_DOUBLES;  // 8 MiB
+static __device__ __align__(256) double g_noalloc_scratch[kNoallocScratchDoubles];
+
+// the scratch's address on each device, looked up once per device (the lookup may load the library's
+// device code on that device: the set-up work of the first call)
+constexpr int kNoallocMaxDevices = 64;
+std::atomic<double*> g_noalloc_addr[kNoallocMaxDevices];
+std::mutex g_noalloc_mu;
+
+__global__ void k_widen(const float* __restrict__ src, double* __restrict__ dst, unsigned n) {
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) dst[t] = double(src[t]);
+}
+
+double* noalloc_scratch(int device) {
+  double* p = g_noalloc_addr[device].load(std::memory_order_acquire);
+  if (p) return p;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  p = g_noalloc_addr[device].load(std::memory_order_relaxed);
+  if (p) return p;
+  void* a = nullptr;
+  if (cudaGetSymbolAddress(&a, g_noalloc_scratch) != cudaSuccess) return nullptr;
+  p = static_cast<double*>(a);
+  g_noalloc_addr[device].store(p, std::memory_order_release);
+  return p;
+}
+
+}  // namespace
+
+extern "C" int cw_download_noalloc(cw_handle* h, int field, int n, double* host, size_t count) {
+  if (!h || !host || h->m.empty() || field < 0 || field >= CW_NFIELDS) return CW_NOALLOC_EBADARG;
+  Member& M = h->m[0];
+  const bool scalar = field >= CW_Q_1;
+  if (scalar && (n < 0 || n >= M.o.n_scalars)) return CW_NOALLOC_EBADARG;
+  const Loc l = locate(h, 0, field, scalar ? n : 0);  // arguments checked above: does not throw
+  if (count != size_t(l.L.total)) return CW_NOALLOC_EBADARG;
+  if (l.esz == 8) {  // FP64 storage: a plain copy, no scratch
+    if (cudaMemcpyAsync(host, l.base, count * 8, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess)
+      return CW_NOALLOC_ECUDA;
+    return 0;
+  }
+  if (count > kNoallocScratchDoubles) return CW_NOALLOC_ETOOBIG;
+  int device = -1;
+  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kNoallocMaxDevices) return CW_NOALLOC_ECUDA;
+  double* scratch = noalloc_scratch(device);
+  if (!scratch) return CW_NOALLOC_ECUDA;
+  const unsigned nel = unsigned(count);
+  const unsigned blocks = std::min(4096u, (nel + 255u) / 256u);
+  k_widen<<<blocks, 256, 0, h->stream>>>(reinterpret_cast<const float*>(l.base), scratch, nel);
+  if (cudaGetLastError() != cudaSuccess) return CW_NOALLOC_ECUDA;
+  if (cudaMemcpyAsync(host, scratch, count * 8, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+      cudaStreamSynchronize(h->stream) != cudaSuccess)
+    return CW_NOALLOC_ECUDA;
+  return 0;
+}

@@ -211,6 +211,35 @@ typedef struct cw_lam_params {
 int cw_default_lam_params(cw_lam_params* p);
 int cw_gen_lam(cw_case* c, const cw_lam_params* p);
 
+/* cw_download without any allocation (no counterpart in the reference; CPPWRF's FieldT::download always
+ * stages through host memory).
+ *
+ * For callers that must read a field back at a moment when they cannot allocate: a checkpoint or state
+ * dump taken after a host or device allocation has failed, or a serving loop whose device-memory budget is
+ * fully committed to resident domains. cw_download stages an FP32 field (CW_MIXED handles) through a host
+ * vector; this call widens it to double on the device, in a scratch array that is part of the library's
+ * device image (CW_NOALLOC_SCRATCH_DOUBLES doubles = 8 MiB per device, not allocated at run time), and
+ * copies that to `host`. FP64 fields are copied directly and have no size limit.
+ *
+ * Same arguments and result as cw_download (member 0 of the handle, the whole allocation of the field,
+ * count = its layout's total). Call it with the handle's device current. The first call on each device
+ * looks up the scratch's device address (cudaGetSymbolAddress), which may load the library's device code
+ * on that device: make one call early, before the period in which nothing may be set up. No part of the
+ * scratch has to start at zero: each call writes the count elements it then copies.
+ *
+ * The scratch is shared by every handle on a device: two calls that overlap in time (from two threads, or
+ * on two streams before the first has returned) race on it, so callers serialize them. The call returns
+ * after the copy has completed (it synchronizes the handle's stream). Errors are returned, not stored in
+ * cw_last_error (storing a message could allocate):
+ *   CW_NOALLOC_EBADARG  null handle or buffer, unknown field, species out of range, count != layout total
+ *   CW_NOALLOC_ETOOBIG  an FP32 field of more than CW_NOALLOC_SCRATCH_DOUBLES elements (nothing is copied)
+ *   CW_NOALLOC_ECUDA    a CUDA call failed */
+#define CW_NOALLOC_SCRATCH_DOUBLES 1048576
+#define CW_NOALLOC_EBADARG (-1)
+#define CW_NOALLOC_ETOOBIG (-2)
+#define CW_NOALLOC_ECUDA (-3)
+int cw_download_noalloc(cw_handle* h, int field, int n, double* host, size_t count);
+
 #ifdef __cplusplus
 }
 #endif
