@@ -19,7 +19,7 @@ from . import capi
 from .capi import (DEFAULT, FIELDS, FP64, IGW, MIXED, PERIODIC, REST_STATE, SPECIFIED, STRAKA, SYMMETRIC,
                    WARM_BUBBLE, Case, F, Grid, Layout, Options, default_options, grid, interior)
 
-__all__ = ["Domain", "Batch", "Case", "Grid", "Options", "Layout", "grid", "default_options", "interior", "capi",
+__all__ = ["Domain", "Batch", "Server", "Case", "Grid", "Options", "Layout", "grid", "default_options", "interior", "capi",
            "FIELDS", "F", "PERIODIC", "SYMMETRIC", "SPECIFIED", "FP64", "MIXED", "REST_STATE", "STRAKA",
            "WARM_BUBBLE", "IGW", "DEFAULT"]
 
@@ -146,3 +146,71 @@ class Batch:
                                          out.size)
         _check(self.lib, self.h, rc, "cw_member_download")
         return out
+
+
+class Server:
+    """The served form (include/cw_serve.h): a C++ request loop on its own thread that admits requests by
+    device-memory footprint, keeps them resident and advances them together in batched steps."""
+
+    def __init__(self, budget_bytes=150e9, max_resident=256, precision=MIXED, device=0, keep_results=True, lib=None):
+        self.lib = lib or capi.load()
+        cfg = capi.ServeConfig()
+        self.lib.cw_serve_default_config(C.byref(cfg))
+        cfg.hbm_budget_bytes, cfg.max_resident, cfg.precision = float(budget_bytes), int(max_resident), int(precision)
+        cfg.device, cfg.keep_results = int(device), 1 if keep_results else 0
+        self.h = C.c_void_p()
+        rc = self.lib.cw_serve_create(C.byref(cfg), C.byref(self.h))
+        if rc != 0:
+            raise CwError(f"cw_serve_create failed ({rc})")
+        self.cases = {}
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.lib.cw_serve_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def _err(self, what, rc):
+        msg = self.lib.cw_serve_last_error(self.h)
+        raise CwError(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+    def submit(self, case, nsteps):
+        rid = C.c_longlong()
+        rc = self.lib.cw_serve_submit(self.h, case.h, int(nsteps), C.byref(rid))
+        if rc != 0:
+            self._err("cw_serve_submit", rc)
+        self.cases[rid.value] = (case.g, case.o)
+        return rid.value
+
+    def wait(self, rid, seconds=-1.0):
+        return self.lib.cw_serve_wait(self.h, rid, float(seconds))
+
+    def drain(self):
+        self.lib.cw_serve_drain(self.h)
+
+    def result(self, rid, name, n=0):
+        g, o = self.cases[rid]
+        L = Layout()
+        if self.lib.cw_layout_of(C.byref(g), C.byref(o), F[name], C.byref(L)) != 0:
+            raise KeyError(name)
+        out = np.empty(L.total, dtype=np.float64)
+        rc = self.lib.cw_serve_result(self.h, rid, F[name], n, out.ctypes.data_as(C.POINTER(C.c_double)), out.size)
+        if rc != 0:
+            self._err("cw_serve_result", rc)
+        return out
+
+    def latency(self, rid):
+        v = C.c_double()
+        if self.lib.cw_serve_latency(self.h, rid, C.byref(v)) != 0:
+            self._err("cw_serve_latency", -1)
+        return v.value
+
+    def release(self, rid):
+        self.lib.cw_serve_release(self.h, rid)
+
+    def stats(self):
+        st = capi.ServeStats()
+        self.lib.cw_serve_stats_get(self.h, C.byref(st))
+        return {k: getattr(st, k) for k, _ in capi.ServeStats._fields_}

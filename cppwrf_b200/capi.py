@@ -90,6 +90,18 @@ class LamParams(C.Structure):
         "rh_mean", "rh_pert", "q_patch_max", "theta_pert", "wind_pert", "etac")] + [("hybrid_opt", C.c_int)]
 
 
+class ServeConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_double), ("max_resident", C.c_int), ("precision", C.c_int),
+                ("device", C.c_int), ("keep_results", C.c_int)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [(n, C.c_longlong) for n in ("submitted", "completed", "failed", "rejected", "ticks")] + \
+               [(n, C.c_int) for n in ("resident", "pending", "max_resident_seen")] + \
+               [(n, C.c_double) for n in ("used_bytes", "max_used_bytes", "p50_s", "p99_s", "mean_s", "max_s",
+                                          "gp_steps", "wall_s", "gp_steps_per_s")]
+
+
 _lib = None
 
 
@@ -145,6 +157,22 @@ def load(path=None):
         "cw_member_download": (i, [vp, i, i, i, dp, sz]),
         "cw_member_field_layout": (i, [vp, i, i, i, C.POINTER(Layout)]),
         "cw_download_noalloc": (i, [vp, i, i, dp, sz]),
+        "cw_batch_add": (i, [vp, C.POINTER(Grid), C.POINTER(Options), ip]),
+        "cw_batch_remove": (i, [vp, i]),
+        "cw_footprint": (i, [C.POINTER(Grid), C.POINTER(Options), C.POINTER(sz)]),
+        "cw_case_clone": (i, [vp, C.POINTER(vp)]),
+        "cw_case_config": (i, [vp, C.POINTER(Grid), C.POINTER(Options)]),
+        "cw_serve_default_config": (i, [C.POINTER(ServeConfig)]),
+        "cw_serve_create": (i, [C.POINTER(ServeConfig), C.POINTER(vp)]),
+        "cw_serve_destroy": (i, [vp]),
+        "cw_serve_submit": (i, [vp, vp, i, C.POINTER(C.c_longlong)]),
+        "cw_serve_wait": (i, [vp, C.c_longlong, C.c_double]),
+        "cw_serve_drain": (i, [vp]),
+        "cw_serve_result": (i, [vp, C.c_longlong, i, i, dp, sz]),
+        "cw_serve_latency": (i, [vp, C.c_longlong, dp]),
+        "cw_serve_release": (i, [vp, C.c_longlong]),
+        "cw_serve_stats_get": (i, [vp, C.POINTER(ServeStats)]),
+        "cw_serve_last_error": (C.c_char_p, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name, None)

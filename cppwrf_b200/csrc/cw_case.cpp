@@ -270,6 +270,23 @@ int cw_case_destroy(cw_case* c) {
   return 0;
 }
 
+int cw_case_clone(const cw_case* c, cw_case** out) {
+  if (!c || !out) return -1;
+  try {
+    *out = new cw_case(*c);
+  } catch (...) {
+    return -3;
+  }
+  return 0;
+}
+
+int cw_case_config(const cw_case* c, cw_grid* g, cw_options* o) {
+  if (!c) return -1;
+  if (g) *g = c->g;
+  if (o) *o = c->o;
+  return 0;
+}
+
 int cw_case_field(cw_case* c, int field, int n, double** data, cw_layout* layout) {
   if (!c) return -1;
   if (field >= 0 && field < CW_Q_1) {

@@ -69,6 +69,8 @@ struct Member {
   std::vector<char> q_have;
   double dtbc = 0;
   int q_parity = 0;
+  char* arena = nullptr;  // the member's device allocation (every pointer above points into it)
+  size_t arena_bytes = 0;
   double cf1 = 0, cf2 = 0, cf3 = 0, cfn = 0, cfn1 = 0, rdx = 0, rdy = 0;
 };
 
@@ -102,8 +104,6 @@ struct cw_handle {
   std::vector<Member> m;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
-  char* arena = nullptr;
-  size_t arena_bytes = 0;
   DevTables<double> t64;
   DevTables<float> t32;
   double* dtbc_d = nullptr;  // per member: time since the boundary data, advanced by the step on the device
@@ -162,99 +162,105 @@ VB<R> viewb(char* base, const cw_layout& L) {
 }
 
 // the device arena: every field of every member, vertical arrays, slabs
-void allocate(cw_handle* h) {
+// one member's allocation plan: byte offsets of every field, work field, scalar, vertical array and slab
+struct Plan {
+  std::vector<size_t> f, w, q1, qa, qb, qtf, qsc, qslab;
+  size_t vert = 0;
+  size_t slab[5]{};
   size_t total = 0;
+};
+Plan plan_member(Member& M) {
+  Plan P;
   auto take = [&](size_t bytes) {
-    const size_t off = total;
-    total += align_up(bytes);
+    const size_t off = P.total;
+    P.total += align_up(bytes);
     return off;
   };
-  struct Plan {
-    std::vector<size_t> f, w, q1, qa, qb, qtf, qsc, qslab;
-    size_t vert;
-    size_t slab[5];
-  };
-  std::vector<Plan> plan(h->m.size());
-  for (size_t mi = 0; mi < h->m.size(); ++mi) {
-    Member& M = h->m[mi];
-    Plan& P = plan[mi];
-    M.L.resize(CW_Q_1);
-    for (int id = 0; id < CW_Q_1; ++id) {
-      M.L[id] = field_layout(M.g, M.o, id);
-      P.f.push_back(take(field_bytes(M.L[id], M.esz)));
-    }
-    M.LW.resize(W_N);
-    for (int w = 0; w < W_N; ++w) {
-      const FieldKind k = work_kind(w);
-      M.LW[w] = layout_make(M.g, k.stagger, k.rank, false);
-      P.w.push_back(take(field_bytes(M.LW[w], M.esz)));
-    }
-    M.Lq = layout_make(M.g, 'M', 3, false);
-    for (int n = 0; n < M.o.n_scalars; ++n) {
-      P.q1.push_back(take(field_bytes(M.Lq, M.esz)));
-      P.qa.push_back(take(field_bytes(M.Lq, M.esz)));
-      P.qb.push_back(take(field_bytes(M.Lq, M.esz)));
-      P.qtf.push_back(take(field_bytes(M.Lq, M.esz)));
-      P.qsc.push_back(take(field_bytes(M.Lq, M.esz)));
-    }
-    P.vert = take(24 * size_t(M.g.nz + 2) * sizeof(double));
-    for (int v = 0; v < 5; ++v) {
-      size_t n = 0;
-      if (M.o.lbc)
-        for (int half = 0; half < 2; ++half)
-          for (int s = 0; s < 4; ++s) {
-            M.slab_off[v][half * 4 + s] = n;
-            n += size_t(lbc_npos(M.g, v, s)) * lbc_nk(M.g, v) * kLbcWidth;
-          }
-      P.slab[v] = M.o.lbc ? take(n * M.esz) : 0;
-    }
-    M.qslab_off.assign(M.o.n_scalars, {});
-    M.q_have.assign(M.o.n_scalars, 0);
-    for (int n = 0; n < M.o.n_scalars; ++n) {
-      size_t cnt = 0;
-      if (M.o.lbc)
-        for (int half = 0; half < 2; ++half)
-          for (int s = 0; s < 4; ++s) {
-            M.qslab_off[n][half * 4 + s] = cnt;
-            cnt += size_t(s < 2 ? M.g.ny : M.g.nx) * M.g.nz * kLbcWidth;
-          }
-      P.qslab.push_back(M.o.lbc ? take(cnt * M.esz) : 0);
-    }
+  M.L.resize(CW_Q_1);
+  for (int id = 0; id < CW_Q_1; ++id) {
+    M.L[id] = field_layout(M.g, M.o, id);
+    P.f.push_back(take(field_bytes(M.L[id], M.esz)));
   }
-  CW_CUDA(cudaMalloc(&h->arena, total));
-  CW_CUDA(cudaMemsetAsync(h->arena, 0, total, h->stream));
-  h->arena_bytes = total;
-  for (size_t mi = 0; mi < h->m.size(); ++mi) {
-    Member& M = h->m[mi];
-    Plan& P = plan[mi];
-    for (int id = 0; id < CW_Q_1; ++id) M.base.push_back(h->arena + P.f[id]);
-    for (int w = 0; w < W_N; ++w) M.wbase.push_back(h->arena + P.w[w]);
-    for (int n = 0; n < M.o.n_scalars; ++n) {
-      M.q1.push_back(h->arena + P.q1[n]);
-      M.qa.push_back(h->arena + P.qa[n]);
-      M.qb.push_back(h->arena + P.qb[n]);
-      M.qtf.push_back(h->arena + P.qtf[n]);
-      M.qsc.push_back(h->arena + P.qsc[n]);
-      M.qslab.push_back(M.o.lbc ? h->arena + P.qslab[n] : nullptr);
-    }
-    M.vert = reinterpret_cast<double*>(h->arena + P.vert);
-    for (int a = 0; a < 24; ++a) M.vert_off[a] = size_t(a) * (M.g.nz + 2);
-    for (int v = 0; v < 5; ++v) M.slab[v] = M.o.lbc ? h->arena + P.slab[v] : nullptr;
+  M.LW.resize(W_N);
+  for (int w = 0; w < W_N; ++w) {
+    const FieldKind k = work_kind(w);
+    M.LW[w] = layout_make(M.g, k.stagger, k.rank, false);
+    P.w.push_back(take(field_bytes(M.LW[w], M.esz)));
   }
+  M.Lq = layout_make(M.g, 'M', 3, false);
+  for (int n = 0; n < M.o.n_scalars; ++n) {
+    P.q1.push_back(take(field_bytes(M.Lq, M.esz)));
+    P.qa.push_back(take(field_bytes(M.Lq, M.esz)));
+    P.qb.push_back(take(field_bytes(M.Lq, M.esz)));
+    P.qtf.push_back(take(field_bytes(M.Lq, M.esz)));
+    P.qsc.push_back(take(field_bytes(M.Lq, M.esz)));
+  }
+  P.vert = take(24 * size_t(M.g.nz + 2) * sizeof(double));
+  for (int v = 0; v < 5; ++v) {
+    size_t n = 0;
+    if (M.o.lbc)
+      for (int half = 0; half < 2; ++half)
+        for (int sd = 0; sd < 4; ++sd) {
+          M.slab_off[v][half * 4 + sd] = n;
+          n += size_t(lbc_npos(M.g, v, sd)) * lbc_nk(M.g, v) * kLbcWidth;
+        }
+    P.slab[v] = M.o.lbc ? take(n * M.esz) : 0;
+  }
+  M.qslab_off.assign(M.o.n_scalars, {});
+  M.q_have.assign(M.o.n_scalars, 0);
+  for (int n = 0; n < M.o.n_scalars; ++n) {
+    size_t cnt = 0;
+    if (M.o.lbc)
+      for (int half = 0; half < 2; ++half)
+        for (int sd = 0; sd < 4; ++sd) {
+          M.qslab_off[n][half * 4 + sd] = cnt;
+          cnt += size_t(sd < 2 ? M.g.ny : M.g.nx) * M.g.nz * kLbcWidth;
+        }
+    P.qslab.push_back(M.o.lbc ? take(cnt * M.esz) : 0);
+  }
+  return P;
+}
+
+// the member's device arena (one cudaMalloc): every field, work field, scalar, vertical array and slab
+void allocate_member(cw_handle* h, Member& M) {
+  const Plan P = plan_member(M);
+  CW_CUDA(cudaMalloc(&M.arena, P.total));
+  M.arena_bytes = P.total;
+  CW_CUDA(cudaMemsetAsync(M.arena, 0, P.total, h->stream));
+  char* A = M.arena;
+  M.base.clear();
+  M.wbase.clear();
+  M.q1.clear(); M.qa.clear(); M.qb.clear(); M.qtf.clear(); M.qsc.clear(); M.qslab.clear();
+  for (int id = 0; id < CW_Q_1; ++id) M.base.push_back(A + P.f[id]);
+  for (int w = 0; w < W_N; ++w) M.wbase.push_back(A + P.w[w]);
+  for (int n = 0; n < M.o.n_scalars; ++n) {
+    M.q1.push_back(A + P.q1[n]);
+    M.qa.push_back(A + P.qa[n]);
+    M.qb.push_back(A + P.qb[n]);
+    M.qtf.push_back(A + P.qtf[n]);
+    M.qsc.push_back(A + P.qsc[n]);
+    M.qslab.push_back(M.o.lbc ? A + P.qslab[n] : nullptr);
+  }
+  M.vert = reinterpret_cast<double*>(A + P.vert);
+  for (int a = 0; a < 24; ++a) M.vert_off[a] = size_t(a) * (M.g.nz + 2);
+  for (int v = 0; v < 5; ++v) M.slab[v] = M.o.lbc ? A + P.slab[v] : nullptr;
   // BaseState defaults: map factors and cosa = 1 (src/dyn/state.cpp:80-83)
-  for (Member& M : h->m)
-    for (int id : {CW_MSFTX, CW_MSFTY, CW_MSFUX, CW_MSFUY, CW_MSFVX, CW_MSFVY, CW_MSFVX_INV, CW_COSA}) {
-      const size_t n = size_t(M.L[id].total);
-      if (M.esz == 8) {
-        std::vector<double> one(n, 1.0);
-        CW_CUDA(cudaMemcpyAsync(M.base[id], one.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
-        CW_CUDA(cudaStreamSynchronize(h->stream));
-      } else {
-        std::vector<float> one(n, 1.0f);
-        CW_CUDA(cudaMemcpyAsync(M.base[id], one.data(), n * 4, cudaMemcpyHostToDevice, h->stream));
-        CW_CUDA(cudaStreamSynchronize(h->stream));
-      }
+  for (int id : {CW_MSFTX, CW_MSFTY, CW_MSFUX, CW_MSFUY, CW_MSFVX, CW_MSFVY, CW_MSFVX_INV, CW_COSA}) {
+    const size_t n = size_t(M.L[id].total);
+    if (M.esz == 8) {
+      std::vector<double> one(n, 1.0);
+      CW_CUDA(cudaMemcpyAsync(M.base[id], one.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
+      CW_CUDA(cudaStreamSynchronize(h->stream));
+    } else {
+      std::vector<float> one(n, 1.0f);
+      CW_CUDA(cudaMemcpyAsync(M.base[id], one.data(), n * 4, cudaMemcpyHostToDevice, h->stream));
+      CW_CUDA(cudaStreamSynchronize(h->stream));
     }
+  }
+}
+
+void allocate(cw_handle* h) {
+  for (Member& M : h->m) allocate_member(h, M);
 }
 
 // vertical array slots in Member::vert
@@ -350,6 +356,7 @@ void build_packs(cw_handle* h, const std::vector<Dom<R>>& doms, Packs<R, NM>& ps
 template <class R>
 void upload_tables(cw_handle* h, DevTables<R>& T) {
   const size_t nm = h->m.size();
+  if (nm == 0) return;
   if (!h->dtbc_d) CW_CUDA(cudaMalloc(&h->dtbc_d, nm * sizeof(double)));
   size_t nq = 0;
   for (const Member& M : h->m) nq += size_t(M.o.n_scalars);
@@ -522,6 +529,7 @@ void build_copies(cw_handle* h) {
     q0 += size_t(ns);
   }
   auto up = [&](std::vector<CopyDesc>& v, CopyDesc*& d, long long*& sd, long long& total) {
+    if (v.empty()) return;
     std::vector<long long> st(v.size() + 1, 0);
     for (size_t n = 0; n < v.size(); ++n) st[n + 1] = st[n] + v[n].n;
     total = st.back();
@@ -707,6 +715,7 @@ void invalidate_graph(cw_handle* h) {
 
 void run_steps(cw_handle* h, int nsteps) {
   h->launches_last = 0;
+  if (h->m.empty()) return;
   if (h->use_graph && !h->graph_ok) {
     Launcher L{h};
     CW_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -750,13 +759,52 @@ Member make_member(const cw_grid& g, const cw_options& o) {
   return M;
 }
 
-void setup(cw_handle* h) {
-  allocate(h);
+// the handle-level device tables (scalar tables, boundary clocks, halo and copy descriptors), freed before
+// they are rebuilt for a new set of members
+void free_tables(cw_handle* h) {
+  for (auto& hs : h->hs) {
+    cudaFree(hs.fd);
+    cudaFree(hs.startd);
+    hs = HaloSetHost{};
+  }
+  cudaFree(h->copies_d);
+  cudaFree(h->copies_start_d);
+  cudaFree(h->zeros_d);
+  cudaFree(h->zeros_start_d);
+  h->copies.clear();
+  h->zeros.clear();
+  h->copies_d = h->zeros_d = nullptr;
+  h->copies_start_d = h->zeros_start_d = nullptr;
+  h->copies_total = h->zeros_total = 0;
+  cudaFree(h->dtbc_d);
+  h->dtbc_d = nullptr;
+  cudaFree(h->t64.qtab);
+  cudaFree(h->t64.lbcq);
+  cudaFree(h->t32.qtab);
+  cudaFree(h->t32.lbcq);
+  h->t64 = DevTables<double>{};
+  h->t32 = DevTables<float>{};
+}
+
+void build_tables(cw_handle* h) {
   upload_tables(h);
   size_column_blocks(h);
   if (h->precision == CW_FP64) build_halosets_t<double>(h, h->t64);
   else build_halosets_t<float>(h, h->t32);
   build_copies(h);
+}
+
+// a new set of members: every handle-level table is rebuilt and the step is captured again
+void rebuild(cw_handle* h) {
+  CW_CUDA(cudaStreamSynchronize(h->stream));
+  invalidate_graph(h);
+  free_tables(h);
+  build_tables(h);
+}
+
+void setup(cw_handle* h) {
+  allocate(h);
+  build_tables(h);
 }
 
 // locate a field: allocation and layout
@@ -820,7 +868,7 @@ int cw_create(const cw_grid* g, const cw_options* o, cw_handle** out) {
 
 int cw_batch_create(int n, const cw_grid* g, const cw_options* o, cw_handle** out) {
   return guarded(nullptr, [&] {
-    if (n < 1 || n > kMaxMembers || !g || !o || !out) throw std::runtime_error("bad batch arguments");
+    if (n < 0 || n > kMaxMembers || (n > 0 && !g) || !o || !out) throw std::runtime_error("bad batch arguments");
     auto h = std::make_unique<cw_handle>();
     h->precision = o[0].precision;
     for (int m = 0; m < n; ++m) {
@@ -836,24 +884,57 @@ int cw_batch_create(int n, const cw_grid* g, const cw_options* o, cw_handle** ou
   });
 }
 
+int cw_batch_add(cw_handle* h, const cw_grid* g, const cw_options* o, int* member) {
+  return guarded(h, [&] {
+    if (!h || !g || !o) throw std::runtime_error("null argument");
+    if (int(h->m.size()) >= kMaxMembers) throw std::runtime_error("the batch is full");
+    if (o->precision != h->precision) throw std::runtime_error("batch members must share the precision");
+    Member M = make_member(*g, *o);
+    if (!h->m.empty() && M.n_sound != h->m[0].n_sound) throw std::runtime_error("batch members must share n_sound");
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+    allocate_member(h, M);
+    h->m.push_back(std::move(M));
+    try {
+      rebuild(h);
+    } catch (...) {
+      cudaFree(h->m.back().arena);
+      h->m.pop_back();
+      rebuild(h);
+      throw;
+    }
+    if (member) *member = int(h->m.size()) - 1;
+    return 0;
+  });
+}
+
+int cw_batch_remove(cw_handle* h, int member) {
+  return guarded(h, [&] {
+    if (!h || member < 0 || member >= int(h->m.size())) throw std::runtime_error("member index out of range");
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+    invalidate_graph(h);
+    free_tables(h);
+    cudaFree(h->m[size_t(member)].arena);
+    h->m.erase(h->m.begin() + member);
+    build_tables(h);
+    return 0;
+  });
+}
+
+int cw_footprint(const cw_grid* g, const cw_options* o, size_t* bytes) {
+  return guarded(nullptr, [&] {
+    if (!g || !o || !bytes) throw std::runtime_error("null argument");
+    Member M = make_member(*g, *o);
+    *bytes = plan_member(M).total;
+    return 0;
+  });
+}
+
 int cw_destroy(cw_handle* h) {
   if (!h) return 0;
   cudaStreamSynchronize(h->stream);
   invalidate_graph(h);
-  for (auto& s : h->hs) {
-    cudaFree(s.fd);
-    cudaFree(s.startd);
-  }
-  cudaFree(h->copies_d);
-  cudaFree(h->copies_start_d);
-  cudaFree(h->zeros_d);
-  cudaFree(h->zeros_start_d);
-  cudaFree(h->dtbc_d);
-  cudaFree(h->t64.qtab);
-  cudaFree(h->t64.lbcq);
-  cudaFree(h->t32.qtab);
-  cudaFree(h->t32.lbcq);
-  cudaFree(h->arena);
+  free_tables(h);
+  for (Member& M : h->m) cudaFree(M.arena);
   if (h->own_stream) cudaStreamDestroy(h->stream);
   delete h;
   return 0;

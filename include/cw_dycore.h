@@ -159,6 +159,16 @@ int cw_set_graph(cw_handle* h, int on);
  * cw_member_* variants of the single-domain calls above (cw_upload is cw_member_upload of member 0). */
 int cw_batch_create(int n, const cw_grid* g, const cw_options* o, cw_handle** out);
 int cw_members(cw_handle* h, int* out);
+/* Members joining and leaving a batch (continuous batching of the served form; no reference counterpart).
+ * n = 0 in cw_batch_create makes an empty batch whose precision is o[0].precision. cw_batch_add allocates
+ * a new member (its fields zeroed, map factors 1) as the last index; cw_batch_remove frees one member and
+ * moves the members after it down by one index. Both rebuild the handle's tables; the next cw_step captures
+ * the step again. cw_step on an empty batch does nothing. */
+int cw_batch_add(cw_handle* h, const cw_grid* g, const cw_options* o, int* member);
+int cw_batch_remove(cw_handle* h, int member);
+/* Device bytes one domain takes in a handle (fields, work fields, scalars, slabs, vertical arrays): the
+ * footprint the served form admits by. Needs no device. */
+int cw_footprint(const cw_grid* g, const cw_options* o, size_t* bytes);
 int cw_member_set_vertical(cw_handle* h, int member, const cw_vertical* v);
 int cw_member_upload(cw_handle* h, int member, int field, int n, const double* host, size_t count);
 int cw_member_download(cw_handle* h, int member, int field, int n, double* host, size_t count);
@@ -177,6 +187,9 @@ int cw_member_set_lbc_time(cw_handle* h, int member, double dtbc);
 typedef struct cw_case cw_case;
 int cw_case_create(const cw_grid* g, const cw_options* o, cw_case** out);
 int cw_case_destroy(cw_case* c);
+/* a deep copy of a case; the grid and options a case was made for */
+int cw_case_clone(const cw_case* c, cw_case** out);
+int cw_case_config(const cw_case* c, cw_grid* g, cw_options* o);
 /* host array of a field (the whole allocation) and its layout */
 int cw_case_field(cw_case* c, int field, int n, double** data, cw_layout* layout);
 int cw_case_vertical(cw_case* c, cw_vertical* out);

@@ -65,3 +65,47 @@ def test_create_without_gpu_reports_error():
         lib.cw_destroy(h)
     else:
         assert lib.cw_last_error(None)
+
+
+def test_footprint_without_gpu():
+    """cw_footprint needs no device: the mixed form takes about half the bytes of the FP64 form."""
+    lib = capi.load()
+    g = capi.grid(119, 89, 44, 15000.0, 90.0, 0.0, dy=15000.0, p_top=5000.0, bc_x=capi.SPECIFIED, bc_y=capi.SPECIFIED)
+    sizes = {}
+    for prec in (capi.FP64, capi.MIXED):
+        o = capi.default_options(lib, flat=0, n_moist=5, n_scalars=5, lbc=1, time_step_sound=4, precision=prec)
+        b = C.c_size_t()
+        assert lib.cw_footprint(C.byref(g), C.byref(o), C.byref(b)) == 0
+        sizes[prec] = b.value
+    L = capi.Layout()
+    assert lib.cw_layout_of(C.byref(g), C.byref(o), capi.F["T_2"], C.byref(L)) == 0
+    assert sizes[capi.FP64] > 60 * L.total * 8  # the 3-D state, tendencies, work fields and 5 x 5 scalar arrays
+    assert 0.45 < sizes[capi.MIXED] / sizes[capi.FP64] < 0.55
+
+
+def test_case_clone_is_a_deep_copy():
+    import cases
+    c = cases.ideal_case(cases.SMALL["straka_small"])
+    lib = capi.load()
+    h2 = C.c_void_p()
+    assert lib.cw_case_clone(c.h, C.byref(h2)) == 0
+    p, L = C.POINTER(C.c_double)(), capi.Layout()
+    assert lib.cw_case_field(h2, capi.F["T_2"], 0, C.byref(p), C.byref(L)) == 0
+    a = np.ctypeslib.as_array(p, shape=(L.total,)).copy()
+    t, _ = c.field("T_2")
+    assert np.array_equal(a, t)
+    t[:] = 0.0  # the clone does not share storage
+    b = np.ctypeslib.as_array(p, shape=(L.total,))
+    assert np.array_equal(b, a)
+    g, o = capi.Grid(), capi.Options()
+    assert lib.cw_case_config(h2, C.byref(g), C.byref(o)) == 0 and (g.nx, g.nz) == (c.g.nx, c.g.nz)
+    lib.cw_case_destroy(h2)
+
+
+def test_serve_create_without_gpu_fails_cleanly():
+    lib = capi.load()
+    cfg = capi.ServeConfig()
+    lib.cw_serve_default_config(C.byref(cfg))
+    assert cfg.hbm_budget_bytes == 150e9
+    h = C.c_void_p()
+    assert lib.cw_serve_create(C.byref(cfg), C.byref(h)) != 0
