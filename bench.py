@@ -39,13 +39,14 @@ UNIT = "grid-point-steps/s"
 PROGNOSTIC = ["U_2", "V_2", "W_2", "T_2", "PH_2", "MU_2", "P", "AL"]
 
 
-def make_case(capi, precision, seed=1):
-    w = WORKLOAD
+def make_case(capi, precision, seed=1, w=None, **lam):
+    """A limited-area case of the workload's shape (or of w: nx, ny, nz, dx, dt, time_step_sound, ...)."""
+    w = dict(WORKLOAD, **(w or {}))
     g = capi.grid(w["nx"], w["ny"], w["nz"], w["dx"], w["dt"], 0.0, dy=w["dx"], p_top=w["p_top"],
                   bc_x=capi.SPECIFIED, bc_y=capi.SPECIFIED)
     o = capi.default_options(None, flat=0, n_moist=w["n_moist"], n_scalars=w["n_moist"], lbc=1,
                              time_step_sound=w["time_step_sound"], precision=precision)
-    return capi.Case(g, o).gen_lam(seed=seed, hybrid_opt=w["hybrid_opt"], etac=w["etac"])
+    return capi.Case(g, o).gen_lam(seed=seed, hybrid_opt=w["hybrid_opt"], etac=w["etac"], **lam)
 
 
 # Algorithmic bytes per mass point of one launch: the distinct 3-D arrays the kernel must read and write,
@@ -178,6 +179,169 @@ def run_reference(args, rank):
     return 0
 
 
+# ---------------------------------------------------------------- further workloads
+def _timed_steps(torch, stream, fn, steps):
+    """device ms of fn(steps) on stream (CUDA events)."""
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def _errors(capi, a_dom, b_dom, case):
+    """relative L2 and max-abs of the mixed form against the FP64 form per prognostic (interior points)."""
+    out = {}
+    names = {"u": ("U_2", 0), "v": ("V_2", 0), "w": ("W_2", 0), "theta": ("T_2", 0), "phi'": ("PH_2", 0),
+             "mu'": ("MU_2", 0), "qv": ("Q_2", 0)}
+    for key, (name, n) in names.items():
+        L = b_dom.layout(name, n)
+        a = capi.interior(a_dom.field(name, n), L)
+        b = capi.interior(b_dom.field(name, n), L)
+        d = a - b
+        out[key] = {"rel_l2": float(np.linalg.norm(d) / max(np.linalg.norm(b), 1e-300)),
+                    "max_abs": float(np.max(np.abs(d))), "finite": bool(np.all(np.isfinite(a)))}
+    return out
+
+
+def run_precision(args, torch, capi, Domain):
+    """400 x 400 x 60 at dx 3 km, dt 18 s, 6 acoustic substeps: the mixed form against the FP64 form (which is
+    bit-identical to the oracle) at 1 h and 6 h of simulated time, and the throughput of both."""
+    w = dict(nx=400, ny=400, nz=60, dx=3000.0, dt=18.0, time_step_sound=6)
+    lib = capi.load()
+    doms, stream = {}, torch.cuda.Stream()
+    for prec in (capi.FP64, capi.MIXED):
+        c = make_case(capi, prec, seed=3, w=w)
+        d = Domain(c.g, c.o).upload_case(c)
+        lib.cw_set_stream(d.h, C.c_void_p(stream.cuda_stream))
+        doms[prec] = d
+    pts = w["nx"] * w["ny"] * w["nz"]
+    res, times = {}, {capi.FP64: 0.0, capi.MIXED: 0.0}
+    done = 0
+    for hours in (1, 6):
+        target = int(round(hours * 3600 / w["dt"]))
+        for prec, d in doms.items():
+            times[prec] += _timed_steps(torch, stream, d.step, target - done)
+        done = target
+        res[f"{hours}h"] = _errors(capi, doms[capi.MIXED], doms[capi.FP64], None)
+    v64 = pts * done / (times[capi.FP64] / 1000.0)
+    v32 = pts * done / (times[capi.MIXED] / 1000.0)
+    line = {"metric": METRIC, "value": v32, "unit": UNIT, "n_gpus": 1, "steps": done, "warmup": 0,
+            "ms_per_step": times[capi.MIXED] / done, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (cw_gen_lam, seeded)",
+            "config": {"workload": "precision_400x400x60", **w, "n_moist": 5, "hybrid_opt": 2},
+            "fp64_value": v64, "mixed_over_fp64": v32 / v64, "errors_mixed_vs_fp64": res}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def ensemble_members(rng, n=64):
+    out = []
+    for m in range(n):
+        out.append(dict(nx=int(rng.integers(60, 201)), ny=int(rng.integers(60, 201)),
+                        nz=int(rng.choice([35, 44, 50, 60])), seed=1000 + m))
+    return out
+
+
+def run_ensemble(args, torch, capi, Domain, Batch):
+    """64 members of uneven sizes (nx, ny in [60, 200], nz in {35, 44, 50, 60}, dx 15 km): the batched mixed
+    and FP64 forms against the members run one after the other as plain FP64 domains."""
+    lib = capi.load()
+    rng = np.random.default_rng(2024)
+    spec = ensemble_members(rng)
+    stream = torch.cuda.Stream()
+    gp = sum(m["nx"] * m["ny"] * m["nz"] for m in spec)
+    out = {}
+    cases = [make_case(capi, capi.FP64, seed=m["seed"], w=m, theta_pert=0.5, wind_pert=1.0) for m in spec]
+    for prec in (capi.MIXED, capi.FP64):
+        opts = []
+        for c in cases:
+            o = capi.Options.from_buffer_copy(c.o)
+            o.precision = prec
+            opts.append(o)
+        b = Batch([c.g for c in cases], opts)
+        for k, c in enumerate(cases):
+            b.upload_case(k, c)
+        lib.cw_set_stream(b.h, C.c_void_p(stream.cuda_stream))
+        b.step(args.warmup)
+        ms = _timed_steps(torch, stream, b.step, args.steps)
+        out[prec] = (gp * args.steps / (ms / 1000.0), ms / args.steps, b.launches() // max(args.steps, 1))
+        b.close()
+    # plain FP64: every member alone, one after the other
+    plain_ms = 0.0
+    for c in cases:
+        d = Domain(c.g, c.o).upload_case(c)
+        lib.cw_set_stream(d.h, C.c_void_p(stream.cuda_stream))
+        d.step(1)
+        plain_ms += _timed_steps(torch, stream, d.step, args.steps)
+        d.close()
+    plain = gp * args.steps / (plain_ms / 1000.0)
+    line = {"metric": METRIC, "value": out[capi.MIXED][0], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": out[capi.MIXED][1], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (cw_gen_lam, seeded; per-member theta and wind noise)",
+            "config": {"workload": "ensemble_64", "members": len(spec), "grid_points": gp, "dx": 15000.0, "dt": 90.0,
+                       "time_step_sound": 4, "sizes_seed": 2024},
+            "fp64_batched_value": out[capi.FP64][0], "fp64_plain_serial_value": plain,
+            "mixed_batched_over_fp64_plain": out[capi.MIXED][0] / plain,
+            "launches_per_step": out[capi.MIXED][2]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def served_requests(rng, n, rate):
+    t, out = 0.0, []
+    for r in range(n):
+        t += float(rng.exponential(1.0 / rate))
+        nx = int(round(np.exp(rng.uniform(np.log(40), np.log(300)))))
+        ny = int(round(np.exp(rng.uniform(np.log(40), np.log(300)))))
+        out.append(dict(t=t, nx=nx, ny=ny, nz=int(rng.integers(35, 61)), steps=int(rng.integers(30, 361)),
+                        seed=5000 + r))
+    return out
+
+
+def run_served(args, torch, capi, Domain, Server):
+    """Poisson arrivals of forecast requests (40..300 squared, nz 35..60, 30..360 steps) into the served
+    mixed-precision form under a 150 GB budget: p50 / p99 latency and aggregate gp-steps/s, beside the same
+    requests solved one after the other as plain FP64 domains."""
+    lib = capi.load()
+    rng = np.random.default_rng(77)
+    reqs = served_requests(rng, args.requests, args.rate)
+    cases = [make_case(capi, capi.MIXED, seed=r["seed"], w=r) for r in reqs]
+    srv = Server(budget_bytes=150e9, precision=capi.MIXED, keep_results=False)
+    t0 = time.perf_counter()
+    for r, c in zip(reqs, cases):
+        dt = r["t"] - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        srv.submit(c, r["steps"])
+    srv.drain()
+    st = srv.stats()
+    srv.close()
+    gps = sum(r["nx"] * r["ny"] * r["nz"] * r["steps"] for r in reqs)
+    # plain FP64, one request after the other (device time of the steps)
+    stream = torch.cuda.Stream()
+    plain_ms = 0.0
+    for r in reqs:
+        c = make_case(capi, capi.FP64, seed=r["seed"], w=r)
+        d = Domain(c.g, c.o).upload_case(c)
+        lib.cw_set_stream(d.h, C.c_void_p(stream.cuda_stream))
+        plain_ms += _timed_steps(torch, stream, d.step, r["steps"])
+        d.close()
+    plain = gps / (plain_ms / 1000.0)
+    line = {"metric": METRIC, "value": st["gp_steps_per_s"], "unit": UNIT, "n_gpus": 1, "steps": None,
+            "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic (cw_gen_lam, seeded per request; Poisson arrivals)",
+            "config": {"workload": "served_stream", "requests": len(reqs), "rate_per_s": args.rate,
+                       "hbm_budget_bytes": 150e9, "sizes": "log-uniform 40..300, nz 35..60, 30..360 steps"},
+            "p50_latency_s": st["p50_s"], "p99_latency_s": st["p99_s"], "mean_latency_s": st["mean_s"],
+            "served_stats": st, "fp64_plain_serial_value": plain, "served_over_fp64_plain": st["gp_steps_per_s"] / plain,
+            "note": "value = completed gp-steps / (last completion - first submission), host clock"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -186,6 +350,10 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["lam", "precision", "ensemble", "served"], default="lam",
+                    help="lam: the headline 119x89x44 line; the others: BASELINE configs 3, 4 and 5 (1 GPU)")
+    ap.add_argument("--requests", type=int, default=24, help="served: number of requests")
+    ap.add_argument("--rate", type=float, default=2.0, help="served: Poisson arrival rate per second")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -200,6 +368,16 @@ def main():
     from cppwrf_b200 import Domain, capi
 
     torch.cuda.set_device(local)
+    if args.workload != "lam":
+        from cppwrf_b200 import Batch, Server
+        capi.load().cw_use_device(local)
+        if rank != 0:
+            return 0
+        if args.workload == "precision":
+            return run_precision(args, torch, capi, Domain)
+        if args.workload == "ensemble":
+            return run_ensemble(args, torch, capi, Domain, Batch)
+        return run_served(args, torch, capi, Domain, Server)
     if world > 1:
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         import datetime

@@ -27,12 +27,13 @@ def build(verbose=False):
         obj = os.path.join(HERE, "lib", os.path.splitext(src)[0] + ".o")
         cmd = [NVCC] + ARCH + FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
         if src.endswith(".cpp"):
-            cmd = [CXX, "-std=c++20", "-O3", "-fPIC", "-ffp-contract=off", "-c", os.path.join(CSRC, src), "-o", obj]
+            cmd = [CXX, "-std=c++20", "-O3", "-fPIC", "-ffp-contract=off", "-fopenmp", "-c", os.path.join(CSRC, src),
+                   "-o", obj]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static"]
+    cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-Xcompiler", "-fopenmp", "-lgomp"]
     subprocess.run(cmd, check=True)
     return LIB
 

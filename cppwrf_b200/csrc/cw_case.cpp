@@ -637,13 +637,13 @@ int cw_gen_lam(cw_case* c, const cw_lam_params* pp) {
     Noise orog(rng, Lx, Ly, 0.0, 24, 1.5, 6);
     std::vector<double> oro(size_t(nx) * ny);
     double omin = 1e300, omax = -1e300;
+#pragma omp parallel for collapse(2) schedule(static)
     for (int j = 0; j < ny; ++j)
-      for (int i = 0; i < nx; ++i) {
-        const double v = orog((i + 0.5) * G.dx, (j + 0.5) * G.dy, 0.0);
-        oro[size_t(j) * nx + i] = v;
-        omin = std::min(omin, v);
-        omax = std::max(omax, v);
-      }
+      for (int i = 0; i < nx; ++i) oro[size_t(j) * nx + i] = orog((i + 0.5) * G.dx, (j + 0.5) * G.dy, 0.0);
+    for (double v : oro) {
+      omin = std::min(omin, v);
+      omax = std::max(omax, v);
+    }
     auto ht_at = [&](int i, int j) {
       const double x = (i + 0.5) * G.dx - 0.5 * Lx, y = (j + 0.5) * G.dy - 0.5 * Ly;
       const double hill = pp->hill_height * std::exp(-(x * x + y * y) / (hw * hw));
@@ -651,6 +651,7 @@ int cw_gen_lam(cw_case* c, const cw_lam_params* pp) {
       return hill + o2;
     };
     // ---- base state
+#pragma omp parallel for collapse(2) schedule(static)
     for (int j = 0; j < ny; ++j)
       for (int i = 0; i < nx; ++i) {
         const double ht = ht_at(i, j);
@@ -676,6 +677,7 @@ int cw_gen_lam(cw_case* c, const cw_lam_params* pp) {
     Noise nrh(rng, Lx, Ly, G.ztop > 0 ? G.ztop : 20000.0, 16, 1.0, 5);
     Noise nu(rng, Lx, Ly, 15000.0, 16, 1.0, 4), nv(rng, Lx, Ly, 15000.0, 16, 1.0, 4), nth(rng, Lx, Ly, 15000.0, 16, 1.0, 4);
     std::vector<double> qv(size_t(nx) * ny * nz, 0.0);
+#pragma omp parallel for collapse(2) schedule(static)
     for (int k = 0; k < nz; ++k)
       for (int j = 0; j < ny; ++j)
         for (int i = 0; i < nx; ++i) {
@@ -694,6 +696,7 @@ int cw_gen_lam(cw_case* c, const cw_lam_params* pp) {
           c->at(CW_ALT, i, j, k) = alt;
           c->at(CW_AL, i, j, k) = alt - c->at(CW_ALB, i, j, k);
         }
+#pragma omp parallel for collapse(2) schedule(static)
     for (int j = 0; j < ny; ++j)
       for (int i = 0; i < nx; ++i) {
         const double mub = c->at(CW_MUB, i, j, 0);
@@ -706,11 +709,13 @@ int cw_gen_lam(cw_case* c, const cw_lam_params* pp) {
       }
     const double up = pp->u_pert + pp->wind_pert;
     const cw_layout& Lu = c->L[CW_U_2];
+#pragma omp parallel for collapse(2) schedule(static)
     for (int k = 0; k < nz; ++k)
       for (int j = 0; j < Lu.ny; ++j)
         for (int i = 0; i < Lu.nx; ++i)
           c->at(CW_U_2, i, j, k) = pp->u_mean + up * nu(i * G.dx, (j + 0.5) * G.dy, (k + 0.5) * 300.0);
     const cw_layout& Lv = c->L[CW_V_2];
+#pragma omp parallel for collapse(2) schedule(static)
     for (int k = 0; k < nz; ++k)
       for (int j = 0; j < Lv.ny; ++j)
         for (int i = 0; i < Lv.nx; ++i) c->at(CW_V_2, i, j, k) = up * nv((i + 0.5) * G.dx, j * G.dy, (k + 0.5) * 300.0);
@@ -734,6 +739,7 @@ int cw_gen_lam(cw_case* c, const cw_lam_params* pp) {
         blobs.push_back(Blob{Lx * (0.15 + 0.7 * rng.uniform()), Ly * (0.15 + 0.7 * rng.uniform()),
                              (ice ? 6000.0 : 1500.0) + 3000.0 * rng.uniform(), (3 + 5 * rng.uniform()) * G.dx,
                              800.0 + 1200.0 * rng.uniform(), pp->q_patch_max * (0.2 + 0.8 * rng.uniform())});
+#pragma omp parallel for collapse(2) schedule(static)
       for (int k = 0; k < nz; ++k)
         for (int j = 0; j < ny; ++j)
           for (int i = 0; i < nx; ++i) {
@@ -754,6 +760,7 @@ int cw_gen_lam(cw_case* c, const cw_lam_params* pp) {
       fill_default_halo(c, id);
     for (int n = 0; n < ns; ++n) host_fill_halo(G, c->Lq, c->q2[n].data(), false, false);
     // cf1..cf3 of set_levels (hybrid coefficients do not change them)
+#pragma omp parallel for collapse(2) schedule(static)
     for (int j = 0; j < ny; ++j)
       for (int i = 0; i < nx; ++i) {
         auto ht = [&](int ii, int jj) { return c->at(CW_HT, ii, jj, 0); };
