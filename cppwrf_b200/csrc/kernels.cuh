@@ -617,21 +617,46 @@ __global__ void __launch_bounds__(PX) k_tend(const __grid_constant__ Pack<R, NM>
   const int vj0 = (D.bc_y != CW_BC_PERIODIC && D.do_y) ? 1 : 0;
   const bool lbc = D.lbc;
   int sl, pos;
+  // every tendency is computed before the first store (the stores cannot alias the loads then)
   // LateralBC::spec_dry (lateral_bc.cpp:337-351): the spec zone (row 0) takes the boundary tendency
-  if (lbc && k < nz && spec_at(ring_for(nx, ny, 'u'), i, j, sl, pos)) D.ru_tend(i, j, k) = slab_at(D.lbc_var[0], 1, sl, pos, k, 0);
-  else if (i >= ui0 && i < nx && j < ny && k < nz) D.ru_tend(i, j, k) = tend_u(D, i, j, k, use_tendf);
-  if (lbc && k < nz && spec_at(ring_for(nx, ny, 'v'), i, j, sl, pos)) D.rv_tend(i, j, k) = slab_at(D.lbc_var[1], 1, sl, pos, k, 0);
-  else if (D.do_y && i < nx && j >= vj0 && j < ny && k < nz) D.rv_tend(i, j, k) = tend_v(D, i, j, k, use_tendf);
-  if (i < nx && j < ny) {
-    const bool spec = lbc && spec_at(ring_for(nx, ny, 'h'), i, j, sl, pos);
-    if (k >= 1) D.rw_tend(i, j, k) = tend_w(D, i, j, k, use_tendf);
-    if (spec) D.ph_tend(i, j, k) = slab_at(D.lbc_var[3], 1, sl, pos, k, 0);
-    else if (k >= 1) D.ph_tend(i, j, k) = tend_ph(D, i, j, k, lbc);
-    if (k < nz) D.t_tend(i, j, k) = spec ? slab_at(D.lbc_var[2], 1, sl, pos, k, 0) : tend_t(D, i, j, k, use_tendf, D.n_moist > 0);
-    if (k == 0 && lbc) {
-      if (spec) D.mu_tend(i, j, 0) = slab_at(D.lbc_var[4], 1, sl, pos, 0, 0);
-      else if (rk != 1) D.mu_tend(i, j, 0) = 0;
+  bool has_u = true, has_v = true;
+  R tu = 0, tv = 0;
+  if (lbc && k < nz && spec_at(ring_for(nx, ny, 'u'), i, j, sl, pos)) tu = slab_at(D.lbc_var[0], 1, sl, pos, k, 0);
+  else if (i >= ui0 && i < nx && j < ny && k < nz) tu = tend_u(D, i, j, k, use_tendf);
+  else has_u = false;
+  if (lbc && k < nz && spec_at(ring_for(nx, ny, 'v'), i, j, sl, pos)) tv = slab_at(D.lbc_var[1], 1, sl, pos, k, 0);
+  else if (D.do_y && i < nx && j >= vj0 && j < ny && k < nz) tv = tend_v(D, i, j, k, use_tendf);
+  else has_v = false;
+  const bool mass = i < nx && j < ny;
+  const bool spec = mass && lbc && spec_at(ring_for(nx, ny, 'h'), i, j, sl, pos);
+  R tw = 0, tp = 0, tt = 0, tm = 0;
+  bool has_p = false, has_m = false;
+  if (mass) {
+    if (k >= 1) tw = tend_w(D, i, j, k, use_tendf);
+    if (spec) {
+      tp = slab_at(D.lbc_var[3], 1, sl, pos, k, 0);
+      has_p = true;
+    } else if (k >= 1) {
+      tp = tend_ph(D, i, j, k, lbc);
+      has_p = true;
     }
+    if (k < nz) tt = spec ? slab_at(D.lbc_var[2], 1, sl, pos, k, 0) : tend_t(D, i, j, k, use_tendf, D.n_moist > 0);
+    if (k == 0 && lbc) {
+      if (spec) {
+        tm = slab_at(D.lbc_var[4], 1, sl, pos, 0, 0);
+        has_m = true;
+      } else if (rk != 1) {
+        has_m = true;
+      }
+    }
+  }
+  if (has_u) D.ru_tend(i, j, k) = tu;
+  if (has_v) D.rv_tend(i, j, k) = tv;
+  if (mass) {
+    if (k >= 1) D.rw_tend(i, j, k) = tw;
+    if (has_p) D.ph_tend(i, j, k) = tp;
+    if (k < nz) D.t_tend(i, j, k) = tt;
+    if (has_m) D.mu_tend(i, j, 0) = tm;
   }
 }
 

@@ -30,15 +30,18 @@ __device__ __forceinline__ R mf_(const Dom<R>& D, int k, R m) { return R(D.c1f[k
 template <class R>
 __device__ __forceinline__ void p_rho_point(const Dom<R>& D, int i, int j, int k, bool damp) {
   using A = double;
+  // every load before the first store
   const A c1h = D.c1h[k];
-  const A m = c1h * A(D.muts(i, j, 0)) + A(D.c2h[k]);
-  const A alt = A(D.alt(i, j, k)), mu = A(D.mu2(i, j, 0)), ts = A(D.t_save(i, j, k));
-  const A a = -((1. / m) * (alt * (c1h * mu) + A(D.rdnw[k]) * (A(D.ph2(i, j, k + 1)) - A(D.ph2(i, j, k)))));
+  const A muts = A(D.muts(i, j, 0)), alt = A(D.alt(i, j, k)), mu = A(D.mu2(i, j, 0)), ts = A(D.t_save(i, j, k));
+  const A ph_kp = A(D.ph2(i, j, k + 1)), ph_k = A(D.ph2(i, j, k)), t2 = A(D.t2(i, j, k)), c2a = A(D.c2a(i, j, k));
+  const A pm1 = damp ? A(D.pm1(i, j, k)) : A(0);
+  const A m = c1h * muts + A(D.c2h[k]);
+  const A a = -((1. / m) * (alt * (c1h * mu) + A(D.rdnw[k]) * (ph_kp - ph_k)));
+  A pp = c2a * (alt * (t2 - c1h * mu * ts) / (m * (k::t0 + ts)) - a);
   D.al(i, j, k) = R(a);
-  A pp = A(D.c2a(i, j, k)) * (alt * (A(D.t2(i, j, k)) - c1h * mu * ts) / (m * (k::t0 + ts)) - a);
   if (damp) {
     const A ptmp = pp;
-    pp = pp + A(D.smdiv) * (pp - A(D.pm1(i, j, k)));
+    pp = pp + A(D.smdiv) * (pp - pm1);
     D.pm1(i, j, k) = R(ptmp);
   } else {
     D.pm1(i, j, k) = R(pp);
@@ -77,28 +80,42 @@ __global__ void __launch_bounds__(PX) k_uv(const __grid_constant__ Pack<R, NM> P
   const Dom<R>& D = *Dp;
   if (k >= D.nz) return;
   const R dts = R(rk == 1 ? D.dt / 3.0 : D.dt / D.n_sound);
+  // both new values are computed before either store (the stores cannot alias the loads then)
+  bool su = false, sv = false;
+  R un = 0, vn = 0;
   if (D.lbc) {
     int sl, pos;
-    if (spec_at(ring_for(D.nx, D.ny, 'u'), i, j, sl, pos)) D.u2(i, j, k) += dts * D.ru_tend(i, j, k);
-    if (spec_at(ring_for(D.nx, D.ny, 'v'), i, j, sl, pos)) D.v2(i, j, k) += dts * D.rv_tend(i, j, k);
+    if (spec_at(ring_for(D.nx, D.ny, 'u'), i, j, sl, pos)) {
+      un = D.u2(i, j, k) + dts * D.ru_tend(i, j, k);
+      su = true;
+    }
+    if (spec_at(ring_for(D.nx, D.ny, 'v'), i, j, sl, pos)) {
+      vn = D.v2(i, j, k) + dts * D.rv_tend(i, j, k);
+      sv = true;
+    }
   }
-  if (i >= D.nx || j >= D.ny) return;
-  const int ui0 = D.bc_x != CW_BC_PERIODIC ? 1 : 0, ui1 = D.nx;
-  const int vj0 = (D.bc_y != CW_BC_PERIODIC && D.do_y) ? 1 : 0, vj1 = D.ny;
-  const R emdx = R(D.emdiv) * (R(1.) / R(D.rdx)), emdy = D.do_y ? R(D.emdiv) * (R(1.) / R(D.rdy)) : R(0);
-  const R c1h = R(D.c1h[k]);
-  if (i >= ui0 && i < ui1 && !edge_uface(D, i, j)) {
-    const R mudf_x = -emdx * (D.mudf(i, j, 0) - D.mudf(i - 1, j, 0)) / D.msfuy(i, j);
-    D.u2(i, j, k) = D.u2(i, j, k) + dts * D.ru_tend(i, j, k) -
-                    dts * cqu_(D, i, j, k) * uv_dp<R, 1, 0>(D, i, j, k, D.muu(i, j, 0), R(D.rdx), D.msfux(i, j) / D.msfuy(i, j)) +
-                    c1h * mudf_x;
+  if (i < D.nx && j < D.ny) {
+    const int ui0 = D.bc_x != CW_BC_PERIODIC ? 1 : 0, ui1 = D.nx;
+    const int vj0 = (D.bc_y != CW_BC_PERIODIC && D.do_y) ? 1 : 0, vj1 = D.ny;
+    const R emdx = R(D.emdiv) * (R(1.) / R(D.rdx)), emdy = D.do_y ? R(D.emdiv) * (R(1.) / R(D.rdy)) : R(0);
+    const R c1h = R(D.c1h[k]);
+    if (i >= ui0 && i < ui1 && !edge_uface(D, i, j)) {
+      const R mudf_x = -emdx * (D.mudf(i, j, 0) - D.mudf(i - 1, j, 0)) / D.msfuy(i, j);
+      un = D.u2(i, j, k) + dts * D.ru_tend(i, j, k) -
+           dts * cqu_(D, i, j, k) * uv_dp<R, 1, 0>(D, i, j, k, D.muu(i, j, 0), R(D.rdx), D.msfux(i, j) / D.msfuy(i, j)) +
+           c1h * mudf_x;
+      su = true;
+    }
+    if (D.do_y && j >= vj0 && j < vj1 && !edge_vface(D, i, j)) {
+      const R mudf_y = -emdy * (D.mudf(i, j, 0) - D.mudf(i, j - 1, 0)) * D.msfvx_inv(i, j);
+      vn = D.v2(i, j, k) + dts * D.rv_tend(i, j, k) -
+           dts * cqv_(D, i, j, k) * uv_dp<R, 0, 1>(D, i, j, k, D.muv(i, j, 0), R(D.rdy), D.msfvy(i, j) / D.msfvx(i, j)) +
+           c1h * mudf_y;
+      sv = true;
+    }
   }
-  if (D.do_y && j >= vj0 && j < vj1 && !edge_vface(D, i, j)) {
-    const R mudf_y = -emdy * (D.mudf(i, j, 0) - D.mudf(i, j - 1, 0)) * D.msfvx_inv(i, j);
-    D.v2(i, j, k) = D.v2(i, j, k) + dts * D.rv_tend(i, j, k) -
-                    dts * cqv_(D, i, j, k) * uv_dp<R, 0, 1>(D, i, j, k, D.muv(i, j, 0), R(D.rdy), D.msfvy(i, j) / D.msfvx(i, j)) +
-                    c1h * mudf_y;
-  }
+  if (su) D.u2(i, j, k) = un;
+  if (sv) D.v2(i, j, k) = vn;
 }
 
 // KMuTDiv (:194-206): the mass divergence of level k of column (i, j)

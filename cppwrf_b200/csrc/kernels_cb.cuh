@@ -62,13 +62,27 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ls_prep(const __grid_constant__
       if (j < ny) D.muu(i, j, 0) = muu;
       if (i < nx && j < nyv) D.muv(i, j, 0) = muv;
     }
-    CB_LOOP(k, nz + 1) {  // KPrep3
-      if (j < ny && k < nz) D.ru(i, j, k) = D.u2(i, j, k) * (R(D.c1h[k]) * muu + R(D.c2h[k])) / D.msfuy(i, j);
-      if (i < nx && j < nyv && k < nz) D.rv(i, j, k) = D.v2(i, j, k) * (R(D.c1h[k]) * muv + R(D.c2h[k])) * D.msfvx_inv(i, j);
-      if (i < nx && j < ny) D.rw(i, j, k) = D.w2(i, j, k) * (R(D.c1f[k]) * mut + R(D.c2f[k])) / D.msfty(i, j);
-      if (i < nx && j < ny && k < nz) {
-        D.alt(i, j, k) = D.al(i, j, k) + D.alb(i, j, k);
-        D.php(i, j, k) = R(0.5) * (D.phb(i, j, k) + D.phb(i, j, k + 1) + D.ph2(i, j, k) + D.ph2(i, j, k + 1));
+    CB_LOOP(k, nz + 1) {  // KPrep3 (every load of a level before its first store)
+      const bool has_u = j < ny && k < nz, has_v = i < nx && j < nyv && k < nz, has_w = i < nx && j < ny;
+      const bool has_m = has_w && k < nz;
+      const R u2 = has_u ? D.u2(i, j, k) : R(0), msfuy = has_u ? D.msfuy(i, j) : R(1);
+      const R v2 = has_v ? D.v2(i, j, k) : R(0), mvxi = has_v ? D.msfvx_inv(i, j) : R(0);
+      const R w2 = has_w ? D.w2(i, j, k) : R(0), msfty = has_w ? D.msfty(i, j) : R(1);
+      R al = 0, alb = 0, phb0 = 0, phb1 = 0, ph0 = 0, ph1 = 0;
+      if (has_m) {
+        al = D.al(i, j, k);
+        alb = D.alb(i, j, k);
+        phb0 = D.phb(i, j, k);
+        phb1 = D.phb(i, j, k + 1);
+        ph0 = D.ph2(i, j, k);
+        ph1 = D.ph2(i, j, k + 1);
+      }
+      if (has_u) D.ru(i, j, k) = u2 * (R(D.c1h[k]) * muu + R(D.c2h[k])) / msfuy;
+      if (has_v) D.rv(i, j, k) = v2 * (R(D.c1h[k]) * muv + R(D.c2h[k])) * mvxi;
+      if (has_w) D.rw(i, j, k) = w2 * (R(D.c1f[k]) * mut + R(D.c2f[k])) / msfty;
+      if (has_m) {
+        D.alt(i, j, k) = al + alb;
+        D.php(i, j, k) = R(0.5) * (phb0 + phb1 + ph0 + ph1);
       }
     }
   }
@@ -94,22 +108,19 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ls_prep(const __grid_constant__
     D.ww(i, j, nz) = 0;
   }
   if (col && D.n_moist > 0) {  // KCq
-    CB_LOOP(k, nz) {
-      if (j < ny) {
-        R t = 0;
-        for (int s = 0; s < D.n_moist; ++s) t = t + D.q2[s](i, j, k) + D.q2[s](i - 1, j, k);
-        D.cqu(i, j, k) = R(1) / (R(1) + R(0.5) * t);
+    CB_LOOP(k, nz) {  // the three sums over species first, then the stores
+      const bool has_u = j < ny, has_v = i < nx && j < nyv, has_w = i < nx && j < ny && k >= 1;
+      R tu = 0, tv = 0, tw = 0;
+      for (int s = 0; s < D.n_moist; ++s) {
+        const V3<R> q = D.q2[s];
+        const R q0 = q(i, j, k);
+        if (has_u) tu = tu + q0 + q(i - 1, j, k);
+        if (has_v) tv = tv + q0 + q(i, j - 1, k);
+        if (has_w) tw = tw + q0 + q(i, j, k - 1);
       }
-      if (i < nx && j < nyv) {
-        R t = 0;
-        for (int s = 0; s < D.n_moist; ++s) t = t + D.q2[s](i, j, k) + D.q2[s](i, j - 1, k);
-        D.cqv(i, j, k) = R(1) / (R(1) + R(0.5) * t);
-      }
-      if (i < nx && j < ny && k >= 1) {
-        R t = 0;
-        for (int s = 0; s < D.n_moist; ++s) t = t + D.q2[s](i, j, k) + D.q2[s](i, j, k - 1);
-        D.cqw(i, j, k) = R(0.5) * t;
-      }
+      if (has_u) D.cqu(i, j, k) = R(1) / (R(1) + R(0.5) * tu);
+      if (has_v) D.cqv(i, j, k) = R(1) / (R(1) + R(0.5) * tv);
+      if (has_w) D.cqw(i, j, k) = R(0.5) * tw;
     }
   }
 }
@@ -140,31 +151,57 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ss_prep(const __grid_constant__
       if (j < ny) D.muus(i, j, 0) = mus_u;
       if (i < nx && j < nyv) D.muvs(i, j, 0) = mus_v;
     }
-    CB_LOOP(k, nz + 1) {  // KPrep
+    CB_LOOP(k, nz + 1) {  // KPrep (every load of a level before its first store)
       const R c1h = k < nz ? R(D.c1h[k]) : R(0), c2h = k < nz ? R(D.c2h[k]) : R(0);
-      if (j < ny && k < nz) {
-        const R ui = D.u2(i, j, k);
-        D.u_save(i, j, k) = ui;
-        D.u2(i, j, k) = ((c1h * mus_u + c2h) * D.u1(i, j, k) - (c1h * D.muu(i, j, 0) + c2h) * ui) / D.msfuy(i, j);
+      const bool has_u = j < ny && k < nz, has_v = i < nx && j < nyv && k < nz;
+      R ui = 0, u1 = 0, muu = 0, msfuy = 1, vi = 0, v1 = 0, muv = 0, mvxi = 0;
+      if (has_u) {
+        ui = D.u2(i, j, k);
+        u1 = D.u1(i, j, k);
+        muu = D.muu(i, j, 0);
+        msfuy = D.msfuy(i, j);
       }
-      if (i < nx && j < nyv && k < nz) {
-        const R vi = D.v2(i, j, k);
+      if (has_v) {
+        vi = D.v2(i, j, k);
+        v1 = D.v1(i, j, k);
+        muv = D.muv(i, j, 0);
+        mvxi = D.msfvx_inv(i, j);
+      }
+      R ti = 0, t1 = 0, pb = 0, pp = 0, alt = 1, wi = 0, w1 = 0, msfty = 1, phi = 0, ph1 = 0, ww = 0;
+      if (mass) {
+        if (k < nz) {
+          ti = D.t2(i, j, k);
+          t1 = D.t1(i, j, k);
+          pb = D.pb(i, j, k);
+          pp = D.p(i, j, k);
+          alt = D.alt(i, j, k);
+        }
+        wi = D.w2(i, j, k);
+        w1 = D.w1(i, j, k);
+        msfty = D.msfty(i, j);
+        phi = D.ph2(i, j, k);
+        ph1 = D.ph1(i, j, k);
+        ww = (k == 0 || k == nz) ? R(0) : D.ww(i, j, k);
+      }
+      if (has_u) {
+        D.u_save(i, j, k) = ui;
+        D.u2(i, j, k) = ((c1h * mus_u + c2h) * u1 - (c1h * muu + c2h) * ui) / msfuy;
+      }
+      if (has_v) {
         D.v_save(i, j, k) = vi;
-        D.v2(i, j, k) = ((c1h * mus_v + c2h) * D.v1(i, j, k) - (c1h * D.muv(i, j, 0) + c2h) * vi) * D.msfvx_inv(i, j);
+        D.v2(i, j, k) = ((c1h * mus_v + c2h) * v1 - (c1h * muv + c2h) * vi) * mvxi;
       }
       if (mass) {
         if (k < nz) {
-          const R ti = D.t2(i, j, k);
           D.t_save(i, j, k) = ti;
-          D.t2(i, j, k) = (c1h * mts + c2h) * D.t1(i, j, k) - (c1h * mut + c2h) * ti;
-          D.c2a(i, j, k) = R(k::cpovcv) * (D.pb(i, j, k) + D.p(i, j, k)) / D.alt(i, j, k);
+          D.t2(i, j, k) = (c1h * mts + c2h) * t1 - (c1h * mut + c2h) * ti;
+          D.c2a(i, j, k) = R(k::cpovcv) * (pb + pp) / alt;
         }
-        const R wi = D.w2(i, j, k), phi = D.ph2(i, j, k);
         D.w_save(i, j, k) = wi;
-        D.w2(i, j, k) = ((R(D.c1f[k]) * mts + R(D.c2f[k])) * D.w1(i, j, k) - (R(D.c1f[k]) * mut + R(D.c2f[k])) * wi) / D.msfty(i, j);
+        D.w2(i, j, k) = ((R(D.c1f[k]) * mts + R(D.c2f[k])) * w1 - (R(D.c1f[k]) * mut + R(D.c2f[k])) * wi) / msfty;
         D.ph_save(i, j, k) = phi;
-        D.ph2(i, j, k) = D.ph1(i, j, k) - phi;
-        D.ww1(i, j, k) = (k == 0 || k == nz) ? R(0) : D.ww(i, j, k);
+        D.ph2(i, j, k) = ph1 - phi;
+        D.ww1(i, j, k) = ww;
       }
     }
   }
@@ -309,37 +346,54 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
     if (dyn) {
       CB_LOOP(k, nz + 1) {  // ww'' and its time sum
         const R wpp = R(s2[k * CX + lane]);
+        const R wwm = first ? R(0) : D.ww_m(i, j, k), ww1 = D.ww1(i, j, k);
+        const R sw = wwm + (k == 0 ? R(0) : wpp);
         D.ww(i, j, k) = wpp;
-        const R sw = (first ? R(0) : D.ww_m(i, j, k)) + (k == 0 ? R(0) : wpp);
-        D.ww_m(i, j, k) = last ? sw / rn + D.ww1(i, j, k) : sw;
+        D.ww_m(i, j, k) = last ? sw / rn + ww1 : sw;
       }
     }
     if (mass) {
-      CB_LOOP(k, nz) {  // KMuTPoint: time sums of ru, rv; theta''
+      CB_LOOP(k, nz) {  // KMuTPoint: time sums of ru, rv; theta'' (every load issued before the first store)
         const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
-        const R su = (first ? R(0) : D.ru_m(i, j, k)) + D.u2(i, j, k);
-        D.ru_m(i, j, k) = last ? su / rn + (c1h * D.muu(i, j, 0) + c2h) * D.u_save(i, j, k) / D.msfuy(i, j) : su;
+        const R u_k = D.u2(i, j, k), rum = first ? R(0) : D.ru_m(i, j, k), usv = D.u_save(i, j, k);
+        const R muu = D.muu(i, j, 0), msfuy = D.msfuy(i, j);
+        R v_k = 0, rvm = 0, vsv = 0, muv = 0, mvxi = 0;
         if (D.do_y) {
-          const R sv = (first ? R(0) : D.rv_m(i, j, k)) + D.v2(i, j, k);
-          D.rv_m(i, j, k) = last ? sv / rn + (c1h * D.muv(i, j, 0) + c2h) * D.v_save(i, j, k) * D.msfvx_inv(i, j) : sv;
+          v_k = D.v2(i, j, k);
+          rvm = first ? R(0) : D.rv_m(i, j, k);
+          vsv = D.v_save(i, j, k);
+          muv = D.muv(i, j, 0);
+          mvxi = D.msfvx_inv(i, j);
         }
-        const R tk = D.t2(i, j, k);
-        D.t_2save(i, j, k) = tk;
+        const R tk = D.t2(i, j, k), ttend = D.t_tend(i, j, k);
+        R tnew;
         if (spec) {  // theta'' of the spec zone (update_mu_t)
-          D.t2(i, j, k) += dts * D.t_tend(i, j, k);
-          continue;
+          tnew = tk + dts * ttend;
+        } else {
+          const R u_ip = D.u2(i + 1, j, k), ts = D.t_save(i, j, k), ts_ip = D.t_save(i + 1, j, k), ts_im = D.t_save(i - 1, j, k);
+          R v_jp = 0, ts_jp = 0, ts_jm = 0;
+          if (D.do_y) {
+            v_jp = D.v2(i, j + 1, k);
+            ts_jp = D.t_save(i, j + 1, k);
+            ts_jm = D.t_save(i, j - 1, k);
+          }
+          const R ts_kp = k + 1 < nz ? D.t_save(i, j, k + 1) : R(0), ts_km = k >= 1 ? D.t_save(i, j, k - 1) : R(0);
+          const R msfty = D.msfty(i, j), msftx = D.msftx(i, j);
+          R hflux = R(0.5) * R(D.rdx) * (u_ip * (ts_ip + ts) - u_k * (ts + ts_im));
+          if (D.do_y) hflux += R(0.5) * R(D.rdy) * (v_jp * (ts_jp + ts) - v_k * (ts + ts_jm));
+          const R tn = tk + msfty * dts * ttend;
+          const R wd_kp = (k + 1 == nz) ? R(0) : R(s2[(k + 1) * CX + lane]) * (R(D.fnm[k + 1]) * ts_kp + R(D.fnp[k + 1]) * ts);
+          const R wd_k = (k == 0) ? R(0) : R(s2[k * CX + lane]) * (R(D.fnm[k]) * ts + R(D.fnp[k]) * ts_km);
+          tnew = tn - dts * msfty * (msftx * hflux + R(D.rdnw[k]) * (wd_kp - wd_k));
         }
-        R hflux = R(0.5) * R(D.rdx) *
-                  (D.u2(i + 1, j, k) * (D.t_save(i + 1, j, k) + D.t_save(i, j, k)) - D.u2(i, j, k) * (D.t_save(i, j, k) + D.t_save(i - 1, j, k)));
-        if (D.do_y)
-          hflux += R(0.5) * R(D.rdy) *
-                   (D.v2(i, j + 1, k) * (D.t_save(i, j + 1, k) + D.t_save(i, j, k)) - D.v2(i, j, k) * (D.t_save(i, j, k) + D.t_save(i, j - 1, k)));
-        const R tn = tk + D.msfty(i, j) * dts * D.t_tend(i, j, k);
-        auto wdtn = [&](int kk) -> R {
-          if (kk == 0 || kk == nz) return R(0);
-          return R(s2[kk * CX + lane]) * (R(D.fnm[kk]) * D.t_save(i, j, kk) + R(D.fnp[kk]) * D.t_save(i, j, kk - 1));
-        };
-        D.t2(i, j, k) = tn - dts * D.msfty(i, j) * (D.msftx(i, j) * hflux + R(D.rdnw[k]) * (wdtn(k + 1) - wdtn(k)));
+        const R su = rum + u_k;
+        D.ru_m(i, j, k) = last ? su / rn + (c1h * muu + c2h) * usv / msfuy : su;
+        if (D.do_y) {
+          const R sv = rvm + v_k;
+          D.rv_m(i, j, k) = last ? sv / rn + (c1h * muv + c2h) * vsv * mvxi : sv;
+        }
+        D.t_2save(i, j, k) = tk;
+        D.t2(i, j, k) = tnew;
       }
     }
     __syncthreads();
@@ -472,27 +526,58 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_finish(const __grid_constant__ 
   const R dts = R(rk == 1 ? D.dt / 3.0 : D.dt / D.n_sound);
   const R hd_dt = (rk == 3 && D.n_moist > 0) ? dts * R(nsmall) : R(0);
   if (col) {
-    CB_LOOP(k, nz + 1) {
-      if (j < ny && k < nz) {
-        const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
-        const R mus_u = R(0.5) * (D.muts(i, j, 0) + D.muts(i - 1, j, 0));
-        D.u2(i, j, k) = (D.msfuy(i, j) * D.u2(i, j, k) + D.u_save(i, j, k) * (c1h * D.muu(i, j, 0) + c2h)) / (c1h * mus_u + c2h);
+    CB_LOOP(k, nz + 1) {  // every load of a level before its first store
+      const bool has_u = j < ny && k < nz, has_v = i < nx && j < nyv && k < nz;
+      const R c1h = k < nz ? R(D.c1h[k]) : R(0), c2h = k < nz ? R(D.c2h[k]) : R(0);
+      R u2 = 0, usv = 0, msfuy = 0, muu = 0, mts_u0 = 0, mts_u1 = 0;
+      if (has_u) {
+        u2 = D.u2(i, j, k);
+        usv = D.u_save(i, j, k);
+        msfuy = D.msfuy(i, j);
+        muu = D.muu(i, j, 0);
+        mts_u0 = D.muts(i, j, 0);
+        mts_u1 = D.muts(i - 1, j, 0);
       }
-      if (i < nx && j < nyv && k < nz) {
-        const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
-        const R mus_v = R(0.5) * (D.muts(i, j, 0) + D.muts(i, j - 1, 0));
-        D.v2(i, j, k) = (D.msfvx(i, j) * D.v2(i, j, k) + D.v_save(i, j, k) * (c1h * D.muv(i, j, 0) + c2h)) / (c1h * mus_v + c2h);
+      R v2 = 0, vsv = 0, msfvx = 0, muv = 0, mts_v0 = 0, mts_v1 = 0;
+      if (has_v) {
+        v2 = D.v2(i, j, k);
+        vsv = D.v_save(i, j, k);
+        msfvx = D.msfvx(i, j);
+        muv = D.muv(i, j, 0);
+        mts_v0 = D.muts(i, j, 0);
+        mts_v1 = D.muts(i, j - 1, 0);
+      }
+      R m = 0, mts = 0, w2 = 0, wsv = 0, msfty = 0, ph2 = 0, phsv = 0, ww = 0, ww1 = 0, t2 = 0, tsv = 0, hd = 0;
+      if (mass) {
+        m = D.mut(i, j, 0);
+        mts = D.muts(i, j, 0);
+        w2 = D.w2(i, j, k);
+        wsv = D.w_save(i, j, k);
+        msfty = D.msfty(i, j);
+        ph2 = D.ph2(i, j, k);
+        phsv = D.ph_save(i, j, k);
+        ww = D.ww(i, j, k);
+        ww1 = D.ww1(i, j, k);
+        if (k < nz) {
+          t2 = D.t2(i, j, k);
+          tsv = D.t_save(i, j, k);
+          if (hd_dt != R(0)) hd = D.hd(i, j, k);
+        }
+      }
+      if (has_u) {
+        const R mus_u = R(0.5) * (mts_u0 + mts_u1);
+        D.u2(i, j, k) = (msfuy * u2 + usv * (c1h * muu + c2h)) / (c1h * mus_u + c2h);
+      }
+      if (has_v) {
+        const R mus_v = R(0.5) * (mts_v0 + mts_v1);
+        D.v2(i, j, k) = (msfvx * v2 + vsv * (c1h * muv + c2h)) / (c1h * mus_v + c2h);
       }
       if (mass) {
-        const R m = D.mut(i, j, 0), mts = D.muts(i, j, 0);
-        D.w2(i, j, k) = (D.msfty(i, j) * D.w2(i, j, k) + D.w_save(i, j, k) * (R(D.c1f[k]) * m + R(D.c2f[k]))) / (R(D.c1f[k]) * mts + R(D.c2f[k]));
-        D.ph2(i, j, k) = D.ph2(i, j, k) + D.ph_save(i, j, k);
-        D.ww(i, j, k) = D.ww(i, j, k) + D.ww1(i, j, k);
-        if (k < nz) {
-          const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
-          D.t2(i, j, k) = (D.t2(i, j, k) - (hd_dt != R(0) ? hd_dt * (c1h * m + c2h) * D.hd(i, j, k) : R(0)) + D.t_save(i, j, k) * (c1h * m + c2h)) /
-                          (c1h * mts + c2h);
-        }
+        D.w2(i, j, k) = (msfty * w2 + wsv * (R(D.c1f[k]) * m + R(D.c2f[k]))) / (R(D.c1f[k]) * mts + R(D.c2f[k]));
+        D.ph2(i, j, k) = ph2 + phsv;
+        D.ww(i, j, k) = ww + ww1;
+        if (k < nz)
+          D.t2(i, j, k) = (t2 - (hd_dt != R(0) ? hd_dt * (c1h * m + c2h) * hd : R(0)) + tsv * (c1h * m + c2h)) / (c1h * mts + c2h);
       }
     }
     if (threadIdx.y == 0) {
