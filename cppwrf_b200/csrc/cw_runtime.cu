@@ -90,9 +90,7 @@ struct DevTables {  // the kernels' views of the members and the device scalar t
 
 struct HaloSetHost {
   std::vector<HaloField> f;
-  HaloField* fd = nullptr;
-  long long* startd = nullptr;
-  HaloSet set{};
+  std::vector<HaloChunk> chunks;  // the fields in launch-sized chunks
 };
 
 }  // namespace cw
@@ -107,6 +105,8 @@ struct cw_handle {
   DevTables<double> t64;
   DevTables<float> t32;
   double* dtbc_d = nullptr;  // per member: time since the boundary data, advanced by the step on the device
+  double* staging = nullptr;  // FP32 field transfers: doubles converted on the device
+  size_t staging_n = 0;
   int nzmax = 0;
   size_t cb_level_bytes = 0;  // one shared level array of a column block: (nz + 2) x CX doubles
   // halo sets of the fill points
@@ -454,24 +454,23 @@ HaloField halo_field(const Member& M, const HaloItem& it) {
   return f;
 }
 
-void finish_haloset(cw_handle* h, HaloSetHost& s) {
-  const int nf = int(s.f.size());
-  std::vector<long long> start(nf + 1, 0);
-  int odd = 0;
-  for (int n = 0; n < nf; ++n) {
-    start[n + 1] = start[n] + s.f[n].ncell;
-    odd |= s.f[n].oddface_x;
+void finish_haloset(cw_handle*, HaloSetHost& s) {
+  s.chunks.clear();
+  for (size_t f0 = 0; f0 < s.f.size(); f0 += kHaloChunk) {
+    HaloChunk c{};
+    c.nf = int(std::min(s.f.size() - f0, size_t(kHaloChunk)));
+    long long total = 0;
+    for (int n = 0; n < c.nf; ++n) {
+      c.f[n] = s.f[f0 + size_t(n)];
+      c.start[n] = unsigned(total);
+      total += c.f[n].ncell;
+      c.has_oddface |= c.f[n].oddface_x;
+    }
+    if (total >= (1ll << 31)) throw std::runtime_error("a halo fill of more than 2^31 cells");
+    c.start[c.nf] = unsigned(total);
+    s.chunks.push_back(c);
   }
-  if (nf) {
-    CW_CUDA(cudaMalloc(&s.fd, nf * sizeof(HaloField)));
-    CW_CUDA(cudaMalloc(&s.startd, (nf + 1) * sizeof(long long)));
-    CW_CUDA(cudaMemcpy(s.fd, s.f.data(), nf * sizeof(HaloField), cudaMemcpyHostToDevice));
-    CW_CUDA(cudaMemcpy(s.startd, start.data(), (nf + 1) * sizeof(long long), cudaMemcpyHostToDevice));
-  }
-  if (start[nf] >= (1ll << 31)) throw std::runtime_error("a halo fill of more than 2^31 cells");
-  s.set = HaloSet{s.fd, s.startd, nf, start[nf], odd};
 }
-
 template <class R>
 void build_halosets_t(cw_handle* h, DevTables<R>& T) {
   size_t q0 = 0;
@@ -562,17 +561,19 @@ struct Launcher {
     ++count;
   }
   void halo(int set) {
-    const HaloSet& s = h->hs[set].set;
-    if (s.total == 0) return;
-    const int bs = 256;
-    const unsigned nb = unsigned((s.total + bs - 1) / bs);
-    begin("k_halo");
-    k_halo<<<nb, bs, 0, h->stream>>>(s, 0);
-    check();
-    if (s.has_oddface) {
+    for (const HaloChunk& c : h->hs[set].chunks) {
+      const unsigned total = c.start[c.nf];
+      if (total == 0) continue;
+      const int bs = 256;
+      const unsigned nb = (total + bs - 1) / bs;
       begin("k_halo");
-      k_halo<<<nb, bs, 0, h->stream>>>(s, 1);
+      k_halo<<<nb, bs, 0, h->stream>>>(c, 0);
       check();
+      if (c.has_oddface) {
+        begin("k_halo");
+        k_halo<<<nb, bs, 0, h->stream>>>(c, 1);
+        check();
+      }
     }
   }
   void copy_list(CopyDesc* d, long long* sd, size_t n, long long total) {
@@ -762,11 +763,7 @@ Member make_member(const cw_grid& g, const cw_options& o) {
 // the handle-level device tables (scalar tables, boundary clocks, halo and copy descriptors), freed before
 // they are rebuilt for a new set of members
 void free_tables(cw_handle* h) {
-  for (auto& hs : h->hs) {
-    cudaFree(hs.fd);
-    cudaFree(hs.startd);
-    hs = HaloSetHost{};
-  }
+  for (auto& hs : h->hs) hs = HaloSetHost{};
   cudaFree(h->copies_d);
   cudaFree(h->copies_start_d);
   cudaFree(h->zeros_d);
@@ -824,27 +821,52 @@ Loc locate(cw_handle* h, int mi, int field, int n) {
   throw std::runtime_error("unknown field id");
 }
 
+__global__ void k_widen(const float* __restrict__ src, double* __restrict__ dst, unsigned n) {
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) dst[t] = double(src[t]);
+}
+__global__ void k_narrow(const double* __restrict__ src, float* __restrict__ dst, unsigned n) {
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) dst[t] = float(src[t]);
+}
+
+// the handle's double staging buffer of at least n elements (FP32 fields are converted on the device)
+double* staging(cw_handle* h, size_t n) {
+  if (h->staging_n < n) {
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+    cudaFree(h->staging);
+    h->staging = nullptr;
+    h->staging_n = 0;
+    CW_CUDA(cudaMalloc(&h->staging, n * sizeof(double)));
+    h->staging_n = n;
+  }
+  return h->staging;
+}
+
 void copy_in(cw_handle* h, const Loc& l, const double* host, size_t count) {
   if (count != size_t(l.L.total)) throw std::runtime_error("count != layout.total");
+  if (count >= (size_t(1) << 32)) throw std::runtime_error("field too large");
   if (l.esz == 8) {
     CW_CUDA(cudaMemcpyAsync(l.base, host, count * 8, cudaMemcpyHostToDevice, h->stream));
-  } else {
-    std::vector<float> f(host, host + count);
-    CW_CUDA(cudaMemcpyAsync(l.base, f.data(), count * 4, cudaMemcpyHostToDevice, h->stream));
-    CW_CUDA(cudaStreamSynchronize(h->stream));
+  } else {  // doubles to the staging buffer, narrowed to float on the device (round to nearest)
+    double* st = staging(h, count);
+    CW_CUDA(cudaMemcpyAsync(st, host, count * 8, cudaMemcpyHostToDevice, h->stream));
+    const unsigned n = unsigned(count), blocks = std::min(4096u, (n + 255u) / 256u);
+    k_narrow<<<blocks, 256, 0, h->stream>>>(st, reinterpret_cast<float*>(l.base), n);
+    CW_CUDA(cudaGetLastError());
   }
 }
 void copy_out(cw_handle* h, const Loc& l, double* host, size_t count) {
   if (count != size_t(l.L.total)) throw std::runtime_error("count != layout.total");
+  if (count >= (size_t(1) << 32)) throw std::runtime_error("field too large");
   if (l.esz == 8) {
     CW_CUDA(cudaMemcpyAsync(host, l.base, count * 8, cudaMemcpyDeviceToHost, h->stream));
-    CW_CUDA(cudaStreamSynchronize(h->stream));
-  } else {
-    std::vector<float> f(count);
-    CW_CUDA(cudaMemcpyAsync(f.data(), l.base, count * 4, cudaMemcpyDeviceToHost, h->stream));
-    CW_CUDA(cudaStreamSynchronize(h->stream));
-    for (size_t n = 0; n < count; ++n) host[n] = f[n];
+  } else {  // widened to double on the device, then copied
+    double* st = staging(h, count);
+    const unsigned n = unsigned(count), blocks = std::min(4096u, (n + 255u) / 256u);
+    k_widen<<<blocks, 256, 0, h->stream>>>(reinterpret_cast<const float*>(l.base), st, n);
+    CW_CUDA(cudaGetLastError());
+    CW_CUDA(cudaMemcpyAsync(host, st, count * 8, cudaMemcpyDeviceToHost, h->stream));
   }
+  CW_CUDA(cudaStreamSynchronize(h->stream));
 }
 
 }  // namespace
@@ -934,6 +956,7 @@ int cw_destroy(cw_handle* h) {
   cudaStreamSynchronize(h->stream);
   invalidate_graph(h);
   free_tables(h);
+  cudaFree(h->staging);
   for (Member& M : h->m) cudaFree(M.arena);
   if (h->own_stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -1262,10 +1285,6 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoallocScratchDoubles
 constexpr int kNoallocMaxDevices = 64;
 std::atomic<double*> g_noalloc_addr[kNoallocMaxDevices];
 std::mutex g_noalloc_mu;
-
-__global__ void k_widen(const float* __restrict__ src, double* __restrict__ dst, unsigned n) {
-  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) dst[t] = double(src[t]);
-}
 
 double* noalloc_scratch(int device) {
   double* p = g_noalloc_addr[device].load(std::memory_order_acquire);

@@ -178,11 +178,13 @@ struct HaloField {
       pad;
   long long ncell_x, ncell;  // x-pass cells, all cells
 };
-struct HaloSet {
-  const HaloField* f;       // device array
-  const long long* start;   // device prefix sums of ncell (nf + 1 entries)
+// The fields of one launch, passed by value as a __grid_constant__ parameter (no descriptor is read from
+// global memory); a fill point with more fields is launched in chunks of kHaloChunk.
+constexpr int kHaloChunk = 24;
+struct HaloChunk {
+  HaloField f[kHaloChunk];
+  unsigned start[kHaloChunk + 1];  // prefix sums of the fields' cell counts
   int nf;
-  long long total;
   int has_oddface;
 };
 

@@ -156,18 +156,18 @@ __device__ __forceinline__ void halo_cell(const HaloField& f, unsigned c, int pa
   p[i + jh * f.sj + k * f.sk] = v;
 }
 
-// one thread per halo cell of the set (the host keeps a set's cell count below 2^31)
-static __global__ void k_halo(HaloSet s, int pass) {
+// one thread per halo cell of the chunk (the host keeps a chunk's cell count below 2^31)
+static __global__ void k_halo(const __grid_constant__ HaloChunk s, int pass) {
   const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= unsigned(s.total)) return;
+  if (t >= s.start[s.nf]) return;
   int lo = 0, hi = s.nf - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (unsigned(s.start[mid]) <= t) lo = mid;
+    if (s.start[mid] <= t) lo = mid;
     else hi = mid - 1;
   }
   const HaloField& f = s.f[lo];
-  const unsigned c = t - unsigned(s.start[lo]);
+  const unsigned c = t - s.start[lo];
   if (f.is_float) halo_cell<float>(f, c, pass);
   else halo_cell<double>(f, c, pass);
 }
