@@ -60,6 +60,8 @@ struct Member {
   std::vector<char*> wbase;
   cw_layout Lq{};
   std::vector<char*> q1, qa, qb, qtf, qsc;  // scalar allocations; q_2 is qa or qb by the parity
+  std::vector<char*> qpd;                    // PD face fluxes, 6 per species (dh, lo on x, y, z faces), when PD
+  cw_layout Lpd[3]{};                        // their layouts: U, V, W staggering
   double* vert = nullptr;           // device 1-D arrays (double)
   size_t vert_off[24]{};
   char* slab[5] = {};               // LBC slabs per variable (values 4 sides, tendencies 4 sides)
@@ -84,7 +86,7 @@ template <class R>
 struct DevTables {  // the kernels' views of the members and the device scalar tables
   Packs<R, 1> one;              // a single domain
   Packs<R, kPackMembers> many;  // a batch, in packs of kPackMembers
-  V3<R>* qtab = nullptr;  // per member: q1, q2, qn, qtf, qscale (5 x n_scalars)
+  V3<R>* qtab = nullptr;  // per member: q1, q2, qn, qtf, qscale, 6 PD faces (kQTab x n_scalars)
   Slabs<R>* lbcq = nullptr;
 };
 
@@ -162,9 +164,16 @@ VB<R> viewb(char* base, const cw_layout& L) {
 }
 
 // the device arena: every field of every member, vertical arrays, slabs
+// some species of the member is advected positive-definite (the PD face-flux arrays are needed)
+bool pd_any(const cw_options& o) {
+  for (int n = 0; n < o.n_scalars; ++n)
+    if ((n < o.n_moist ? o.moist_adv_opt : o.scalar_adv_opt) == 1) return true;
+  return false;
+}
+
 // one member's allocation plan: byte offsets of every field, work field, scalar, vertical array and slab
 struct Plan {
-  std::vector<size_t> f, w, q1, qa, qb, qtf, qsc, qslab;
+  std::vector<size_t> f, w, q1, qa, qb, qtf, qsc, qslab, qpd;
   size_t vert = 0;
   size_t slab[5]{};
   size_t total = 0;
@@ -194,6 +203,13 @@ Plan plan_member(Member& M) {
     P.qb.push_back(take(field_bytes(M.Lq, M.esz)));
     P.qtf.push_back(take(field_bytes(M.Lq, M.esz)));
     P.qsc.push_back(take(field_bytes(M.Lq, M.esz)));
+  }
+  if (pd_any(M.o)) {
+    M.Lpd[0] = layout_make(M.g, 'U', 3, false);
+    M.Lpd[1] = layout_make(M.g, 'V', 3, false);
+    M.Lpd[2] = layout_make(M.g, 'W', 3, false);
+    for (int n = 0; n < M.o.n_scalars; ++n)
+      for (int f = 0; f < 6; ++f) P.qpd.push_back(take(field_bytes(M.Lpd[f / 2], M.esz)));
   }
   P.vert = take(24 * size_t(M.g.nz + 2) * sizeof(double));
   for (int v = 0; v < 5; ++v) {
@@ -230,7 +246,8 @@ void allocate_member(cw_handle* h, Member& M) {
   char* A = M.arena;
   M.base.clear();
   M.wbase.clear();
-  M.q1.clear(); M.qa.clear(); M.qb.clear(); M.qtf.clear(); M.qsc.clear(); M.qslab.clear();
+  M.q1.clear(); M.qa.clear(); M.qb.clear(); M.qtf.clear(); M.qsc.clear(); M.qslab.clear(); M.qpd.clear();
+  for (size_t off : P.qpd) M.qpd.push_back(A + off);
   for (int id = 0; id < CW_Q_1; ++id) M.base.push_back(A + P.f[id]);
   for (int w = 0; w < W_N; ++w) M.wbase.push_back(A + P.w[w]);
   for (int n = 0; n < M.o.n_scalars; ++n) {
@@ -312,6 +329,7 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.muave = w3(W_MUAVE); D.w_rhs = w3(W_W_RHS); D.t2a = w3(W_T2A);
   const int ns = o.n_scalars;
   D.q1 = qtab_d; D.q2 = qtab_d + ns; D.qn = qtab_d + 2 * ns; D.qtf = qtab_d + 3 * ns; D.qscale = qtab_d + 4 * ns;
+  D.qpd = qtab_d + 5 * ns;
   for (int var = 0; var < 5; ++var) {
     Slabs<R>& s = D.lbc_var[var];
     s.nk = lbc_nk(g, var);
@@ -360,24 +378,26 @@ void upload_tables(cw_handle* h, DevTables<R>& T) {
   if (!h->dtbc_d) CW_CUDA(cudaMalloc(&h->dtbc_d, nm * sizeof(double)));
   size_t nq = 0;
   for (const Member& M : h->m) nq += size_t(M.o.n_scalars);
-  if (!T.qtab && nq) CW_CUDA(cudaMalloc(&T.qtab, 5 * nq * sizeof(V3<R>)));
+  if (!T.qtab && nq) CW_CUDA(cudaMalloc(&T.qtab, kQTab * nq * sizeof(V3<R>)));
   if (!T.lbcq && nq) CW_CUDA(cudaMalloc(&T.lbcq, nq * sizeof(Slabs<R>)));
   std::vector<Dom<R>> doms(nm);
-  std::vector<V3<R>> qtab(5 * nq);
+  std::vector<V3<R>> qtab(kQTab * nq);
   std::vector<Slabs<R>> lbcq(nq);
   size_t q0 = 0;
   for (size_t mi = 0; mi < nm; ++mi) {
     Member& M = h->m[mi];
     const int ns = M.o.n_scalars;
-    doms[mi] = make_dom<R>(h, mi, T.qtab ? T.qtab + 5 * q0 : nullptr, T.lbcq ? T.lbcq + q0 : nullptr);
+    doms[mi] = make_dom<R>(h, mi, T.qtab ? T.qtab + kQTab * q0 : nullptr, T.lbcq ? T.lbcq + q0 : nullptr);
     for (int n = 0; n < ns; ++n) {
       char* q2 = M.q_parity ? M.qb[n] : M.qa[n];
       char* qn = M.q_parity ? M.qa[n] : M.qb[n];
-      qtab[5 * q0 + n] = view3<R>(M.q1[n], M.Lq);
-      qtab[5 * q0 + ns + n] = view3<R>(q2, M.Lq);
-      qtab[5 * q0 + 2 * ns + n] = view3<R>(qn, M.Lq);
-      qtab[5 * q0 + 3 * ns + n] = view3<R>(M.qtf[n], M.Lq);
-      qtab[5 * q0 + 4 * ns + n] = view3<R>(M.qsc[n], M.Lq);
+      qtab[kQTab * q0 + n] = view3<R>(M.q1[n], M.Lq);
+      qtab[kQTab * q0 + ns + n] = view3<R>(q2, M.Lq);
+      qtab[kQTab * q0 + 2 * ns + n] = view3<R>(qn, M.Lq);
+      qtab[kQTab * q0 + 3 * ns + n] = view3<R>(M.qtf[n], M.Lq);
+      qtab[kQTab * q0 + 4 * ns + n] = view3<R>(M.qsc[n], M.Lq);
+      if (!M.qpd.empty())
+        for (int f = 0; f < 6; ++f) qtab[kQTab * q0 + 5 * ns + 6 * n + f] = view3<R>(M.qpd[6 * size_t(n) + f], M.Lpd[f / 2]);
       Slabs<R>& s = lbcq[q0 + n];
       s.nk = M.g.nz;
       s.have = M.o.lbc && M.q_have[n];
@@ -498,7 +518,7 @@ void build_halosets_t(cw_handle* h, DevTables<R>& T) {
     for (int n = 0; n < ns; ++n) {
       add(cw_handle::H_Q1PD, {HaloItem{M.q1[n], nullptr, M.Lq, HP_DEFAULT}});
       add(cw_handle::H_SCPD, {HaloItem{M.qsc[n], nullptr, M.Lq, HP_DEFAULT}});
-      add(cw_handle::H_Q2, {HaloItem{nullptr, T.qtab + 5 * q0 + ns + n, M.Lq, HP_DEFAULT}});
+      add(cw_handle::H_Q2, {HaloItem{nullptr, T.qtab + kQTab * q0 + ns + n, M.Lq, HP_DEFAULT}});
     }
     add(cw_handle::H_END_P, {F(CW_P), F(CW_AL)});
     add(cw_handle::H_WS0, {F(CW_U_2), F(CW_V_2)});
@@ -519,8 +539,8 @@ void build_copies(cw_handle* h) {
     for (int n = 0; n < ns; ++n) {
       // src through the device table entry q2[n].p (the element (0,0,0) pointer): offset back to the allocation
       const void* const* ind = nullptr;
-      if (h->precision == CW_FP64) ind = reinterpret_cast<const void* const*>(&(h->t64.qtab + 5 * q0 + ns + n)->p);
-      else ind = reinterpret_cast<const void* const*>(&(h->t32.qtab + 5 * q0 + ns + n)->p);
+      if (h->precision == CW_FP64) ind = reinterpret_cast<const void* const*>(&(h->t64.qtab + kQTab * q0 + ns + n)->p);
+      else ind = reinterpret_cast<const void* const*>(&(h->t32.qtab + kQTab * q0 + ns + n)->p);
       CopyDesc c{M.q1[n], nullptr, ind, M.Lq.total, M.esz == 4, M.Lq.offset};
       h->copies.push_back(c);
     }
@@ -675,6 +695,7 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
       if (rk == 3 && any_pd) {
         L.run_q("k_q_pre_pd", RG_MASS, nq, k_q_pre_pd<R, NM>, d, rk);
         L.halo(cw_handle::H_Q1PD);
+        L.run_q("k_q_face_pd", RG_STAG, nq, k_q_face_pd<R, NM>, d, rk);
         L.run_q("k_q_scale_pd", RG_MASS, nq, k_q_scale_pd<R, NM>, d, rk);
         L.halo(cw_handle::H_SCPD);
         L.run_q("k_q_update_pd", RG_MASS, nq, k_q_update_pd<R, NM>, d, rk);

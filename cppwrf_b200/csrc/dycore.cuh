@@ -15,6 +15,7 @@ namespace cw {
 
 constexpr int kMaxMembers = 256;
 constexpr int kMaxScalars = 64;
+constexpr int kQTab = 11;  // views per species in a member's scalar table: q1 q2 qn qtf qscale + 6 PD faces
 
 template <class T>
 struct V3 {  // View3 of CPPWRF (src/core/field.hpp:19-23): element (0,0,0), 32-bit strides
@@ -67,6 +68,7 @@ struct Dom {
   V3<T>* qn;
   V3<T>* qtf;
   V3<T>* qscale;
+  V3<T>* qpd;  // PD face fluxes of species n: qpd[6 n + f], f = dh_x, lo_x, dh_y, lo_y, dh_z, lo_z
   // boundary slabs: U V T PH MU, then scalars (n_scalars entries)
   Slabs<T> lbc_var[5];
   Slabs<T>* lbc_q;

@@ -271,7 +271,40 @@ __device__ void pd_fz(const Dom<R>& D, const V3<R>& q, const V3<R>& qo, R dt, in
   lo = mu * (dz / dt) * flux_upwind(qo(i, j, k - 1), qo(i, j, k), cr);
   dh = sc_fz(D, q, D.ww_m, i, j, k, true) - lo;
 }
-// KScalePD (:215-241)
+// KFacePDX / KFacePDY / KFacePDZ (:159-171 with the PD statement functions): every face flux of the PD
+// species once, dh and lo, into the species' face arrays (x faces 0..nx, y faces 0..ny, z faces 0..nz)
+template <class R, int NM>
+__global__ void __launch_bounds__(PX) k_q_face_pd(const __grid_constant__ Pack<R, NM> P, int rk) {
+  const Dom<R>* Dp;
+  int i, j, k;
+  if (!thread_index(P, RG_STAG, Dp, i, j, k)) return;
+  const Dom<R>& D = *Dp;
+  const int n = blockIdx.y;  // the species
+  if (n >= D.n_scalars || !q_is_pd(D, n, rk)) return;
+  const int nx = D.nx, ny = D.ny, nz = D.nz;
+  const R dt = R(rk == 1 ? D.dt / 3.0 : (rk == 2 ? 0.5 * D.dt : D.dt));
+  const V3<R>& q = D.q2[n];
+  const V3<R>& qo = D.q1[n];
+  const bool fx = j < ny && k < nz, fy = D.do_y && i < nx && k < nz, fz = i < nx && j < ny;
+  R dhx = 0, lox = 0, dhy = 0, loy = 0, dhz = 0, loz = 0;
+  if (fx) pd_fx(D, q, qo, dt, i, j, k, dhx, lox);
+  if (fy) pd_fy(D, q, qo, dt, i, j, k, dhy, loy);
+  if (fz) pd_fz(D, q, qo, dt, i, j, k, dhz, loz);
+  const V3<R>* f = D.qpd + 6 * n;
+  if (fx) {
+    f[0](i, j, k) = dhx;
+    f[1](i, j, k) = lox;
+  }
+  if (fy) {
+    f[2](i, j, k) = dhy;
+    f[3](i, j, k) = loy;
+  }
+  if (fz) {
+    f[4](i, j, k) = dhz;
+    f[5](i, j, k) = loz;
+  }
+}
+// KScalePD (:215-241) from the stored face fluxes
 template <class R, int NM>
 __global__ void __launch_bounds__(PX) k_q_scale_pd(const __grid_constant__ Pack<R, NM> P, int rk) {
   const Dom<R>* Dp;
@@ -287,17 +320,17 @@ __global__ void __launch_bounds__(PX) k_q_scale_pd(const __grid_constant__ Pack<
     D.qscale[n](i, j, k) = 1;
     return;
   }
-  const V3<R>& q = D.q2[n];
   const V3<R>& qo = D.q1[n];
-  R dhx0, lox0, dhx1, lox1, dhy0 = 0, loy0 = 0, dhy1 = 0, loy1 = 0, dhz0, loz0, dhz1, loz1;
-  pd_fx(D, q, qo, dt, i, j, k, dhx0, lox0);
-  pd_fx(D, q, qo, dt, i + 1, j, k, dhx1, lox1);
+  const V3<R>* f = D.qpd + 6 * n;
+  const R dhx0 = f[0](i, j, k), lox0 = f[1](i, j, k), dhx1 = f[0](i + 1, j, k), lox1 = f[1](i + 1, j, k);
+  R dhy0 = 0, loy0 = 0, dhy1 = 0, loy1 = 0;
   if (D.do_y) {
-    pd_fy(D, q, qo, dt, i, j, k, dhy0, loy0);
-    pd_fy(D, q, qo, dt, i, j + 1, k, dhy1, loy1);
+    dhy0 = f[2](i, j, k);
+    loy0 = f[3](i, j, k);
+    dhy1 = f[2](i, j + 1, k);
+    loy1 = f[3](i, j + 1, k);
   }
-  pd_fz(D, q, qo, dt, i, j, k, dhz0, loz0);
-  pd_fz(D, q, qo, dt, i, j, k + 1, dhz1, loz1);
+  const R dhz0 = f[4](i, j, k), loz0 = f[5](i, j, k), dhz1 = f[4](i, j, k + 1), loz1 = f[5](i, j, k + 1);
   const R mxy = D.msftx(i, j) * D.msfty(i, j);
   R hlow = R(D.rdx) * (lox1 - lox0);
   if (D.do_y) hlow += R(D.rdy) * (loy1 - loy0);
@@ -307,14 +340,14 @@ __global__ void __launch_bounds__(PX) k_q_scale_pd(const __grid_constant__ Pack<
   if (D.do_y) hout += R(D.rdy) * ((dhy1 > 0 ? dhy1 : R(0)) - (dhy0 < 0 ? dhy0 : R(0)));
   const R out = mxy * hout + D.msfty(i, j) * R(D.rdnw[k]) * ((dhz1 < 0 ? dhz1 : R(0)) - (dhz0 > 0 ? dhz0 : R(0)));
   const R flux_out = dt * out;
-  R s = 1;
+  R sc = 1;
   if (flux_out > ph_low) {
-    s = ph_low / (flux_out + R(1e-20));
-    if (s < 0) s = 0;
+    sc = ph_low / (flux_out + R(1e-20));
+    if (sc < 0) sc = 0;
   }
-  D.qscale[n](i, j, k) = s;
+  D.qscale[n](i, j, k) = sc;
 }
-// KUpdatePD (:244-291)
+// KUpdatePD (:244-291) from the stored face fluxes
 template <class R, int NM>
 __global__ void __launch_bounds__(PX) k_q_update_pd(const __grid_constant__ Pack<R, NM> P, int rk) {
   const Dom<R>* Dp;
@@ -326,30 +359,26 @@ __global__ void __launch_bounds__(PX) k_q_update_pd(const __grid_constant__ Pack
   const int n = blockIdx.y;  // the species
   if (n >= D.n_scalars) return;
   if (!q_is_pd(D, n, rk)) return;
-  const V3<R>& q = D.q2[n];
   const V3<R>& qo = D.q1[n];
   const V3<R>& sc = D.qscale[n];
   if (spec_cell(D, i, j)) {
     D.qn[n](i, j, k) = m_full(D, k, mub, mu1) * qo(i, j, k) / m_full(D, k, mub, mu2);
     return;
   }
-  R dhx0, lox0, dhx1, lox1, dhy0 = 0, loy0 = 0, dhy1 = 0, loy1 = 0, dhz0, loz0, dhz1, loz1;
-  pd_fx(D, q, qo, dt, i, j, k, dhx0, lox0);
-  pd_fx(D, q, qo, dt, i + 1, j, k, dhx1, lox1);
-  if (D.do_y) {
-    pd_fy(D, q, qo, dt, i, j, k, dhy0, loy0);
-    pd_fy(D, q, qo, dt, i, j + 1, k, dhy1, loy1);
-  }
-  pd_fz(D, q, qo, dt, i, j, k, dhz0, loz0);
-  pd_fz(D, q, qo, dt, i, j, k + 1, dhz1, loz1);
+  const V3<R>* f = D.qpd + 6 * n;
+  const R dhx0 = f[0](i, j, k), lox0 = f[1](i, j, k), dhx1 = f[0](i + 1, j, k), lox1 = f[1](i + 1, j, k);
+  const R dhz0 = f[4](i, j, k), loz0 = f[5](i, j, k), dhz1 = f[4](i, j, k + 1), loz1 = f[5](i, j, k + 1);
+  const R s0 = sc(i, j, k), sxm = sc(i - 1, j, k), sxp = sc(i + 1, j, k);
+  const R szm = k == 0 ? R(0) : sc(i, j, k - 1), szp = (k + 1 == D.nz) ? R(0) : sc(i, j, k + 1);
   auto lim = [](R d, R s_up, R s_dn) { return d * (d > 0 ? s_up : (d < 0 ? s_dn : R(1))); };
-  const R dx0 = lim(dhx0, sc(i - 1, j, k), sc(i, j, k)), dx1 = lim(dhx1, sc(i, j, k), sc(i + 1, j, k));
-  const R dz0 = (k == 0) ? R(0) : lim(dhz0, sc(i, j, k), sc(i, j, k - 1));
-  const R dz1 = (k + 1 == D.nz) ? R(0) : lim(dhz1, sc(i, j, k + 1), sc(i, j, k));
+  const R dx0 = lim(dhx0, sxm, s0), dx1 = lim(dhx1, s0, sxp);
+  const R dz0 = (k == 0) ? R(0) : lim(dhz0, s0, szm);
+  const R dz1 = (k + 1 == D.nz) ? R(0) : lim(dhz1, szp, s0);
   R tend = -R(D.rdnw[k]) * (dz1 - dz0 + loz1 - loz0);
   tend -= D.msftx(i, j) * (R(D.rdx) * (dx1 - dx0 + lox1 - lox0));
   if (D.do_y) {
-    const R dy0 = lim(dhy0, sc(i, j - 1, k), sc(i, j, k)), dy1 = lim(dhy1, sc(i, j, k), sc(i, j + 1, k));
+    const R dhy0 = f[2](i, j, k), loy0 = f[3](i, j, k), dhy1 = f[2](i, j + 1, k), loy1 = f[3](i, j + 1, k);
+    const R dy0 = lim(dhy0, sc(i, j - 1, k), s0), dy1 = lim(dhy1, s0, sc(i, j + 1, k));
     tend -= D.msftx(i, j) * (R(D.rdy) * (dy1 - dy0 + loy1 - loy0));
   }
   D.qn[n](i, j, k) = (m_full(D, k, mub, mu1) * qo(i, j, k) + dt * (tend * D.msfty(i, j))) / m_full(D, k, mub, mu2);
