@@ -11,6 +11,9 @@
 namespace cw {
 
 #define CB_LOOP(k, n) for (int k = int(threadIdx.y); k < (n); k += CNW)
+// the same for a body whose only stores go to shared memory: unrolled, the loads of the next level can be
+// issued before the stores of this one (shared stores cannot alias global loads)
+#define CB_LOOP_SH(k, n) _Pragma("unroll 2") for (int k = int(threadIdx.y); k < (n); k += CNW)
 
 // block -> (member, column i of this lane, row j)
 template <class R, int NM>
@@ -93,7 +96,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ls_prep(const __grid_constant__
     mu0 = ww_mu_u(D, i, j);
     mv1 = ww_mu_v(D, i, j + 1);
     mv0 = ww_mu_v(D, i, j);
-    CB_LOOP(k, nz) s_div[k * CX + lane] = double(ww_divv(D, i, j, k, mu1, mu0, mv1, mv0));
+    CB_LOOP_SH(k, nz) s_div[k * CX + lane] = double(ww_divv(D, i, j, k, mu1, mu0, mv1, mv0));
   }
   __syncthreads();
   if (mass && w0) {  // KWW: the column integral, then the running sum, in the reference's order
@@ -285,6 +288,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
   double* s1 = cb_array(1, nz);
   double* s2 = cb_array(2, nz);
   double* sc = cb_array(3, nz);  // per-column scalars: sc[n * CX + lane]
+  double* s_t2s = cb_array(4, nz);  // theta'' before the substep's update (t_2save), phase 1 to phase 2
   if (phase & 1) {
     if (col && D.spec_x && i == nx && j < ny)  // KSumEdge, east face
       CB_LOOP(k, nz) {
@@ -308,7 +312,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
         D.muts(i, j, 0) += dts * D.mu_tend(i, j, 0);
       }
     }
-    if (dyn) CB_LOOP(k, nz) s0[k * CX + lane] = A(mut_dv(D, i, j, k));  // dv of each level
+    if (dyn) CB_LOOP_SH(k, nz) s0[k * CX + lane] = A(mut_dv(D, i, j, k));  // dv of each level
     __syncthreads();
     if (dyn && w0) {  // the column mass tendency: sum over k in order
       A dmdt = 0;
@@ -327,7 +331,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
     if (dyn) {  // the decrement of the omega integral at each level
       const A dmdt = sc[0 * CX + lane], mtend = sc[1 * CX + lane];
       const A msfty = A(D.msfty(i, j));
-      CB_LOOP(k, nz - 1) {
+      CB_LOOP_SH(k, nz - 1) {
         s1[k * CX + lane] = D.dnw[k] * (D.c1h[k] * dmdt + s0[k * CX + lane] + D.c1h[k] * mtend) / msfty;
         s0[k * CX + lane] = A(D.ww1(i, j, k + 1));
       }
@@ -392,7 +396,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
           const R sv = rvm + v_k;
           D.rv_m(i, j, k) = last ? sv / rn + (c1h * muv + c2h) * vsv * mvxi : sv;
         }
-        D.t_2save(i, j, k) = tk;
+        s_t2s[k * CX + lane] = double(tk);  // t_2save: kept in shared memory for advance_w
         D.t2(i, j, k) = tnew;
       }
     }
@@ -416,7 +420,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
       muts = D.muts(i, j, 0);
       mav = D.muave(i, j, 0);
       msfty = D.msfty(i, j);
-      CB_LOOP(k, nz + 1) {  // KWRhs: R (explicit phi'') and t_2ave
+      CB_LOOP_SH(k, nz + 1) {  // KWRhs: R (explicit phi'') and t_2ave
         R r;
         if (k == 0 || (D.top_lid && k == nz)) {
           r = 0;
@@ -433,7 +437,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
         }
         s0[k * CX + lane] = A(r);
         if (k < nz) {
-          const R tav = R(0.5) * ((R(1) + epssm) * D.t2(i, j, k) + (R(1) - epssm) * D.t_2save(i, j, k));
+          const R tav = R(0.5) * ((R(1) + epssm) * D.t2(i, j, k) + (R(1) - epssm) * R(s_t2s[k * CX + lane]));
           s1[k * CX + lane] = A((tav + R(D.c1h[k]) * mav * R(k::t0)) / (mh_(D, k, muts) * (R(k::t0) + D.t_save(i, j, k))));
         }
       }
@@ -441,7 +445,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
     __syncthreads();
     if (dyn) {
       const R msft_inv = R(1) / msfty;
-      CB_LOOP(k, nz + 1) {  // KWExpl: explicit w''
+      CB_LOOP_SH(k, nz + 1) {  // KWExpl: explicit w''
         R wn;
         if (k == 0) {
           if (!D.flat) {
