@@ -66,6 +66,28 @@ ALG_ARRAYS = {
 }
 
 
+# ---------------------------------------------------------------- multi-GPU plumbing (one domain per rank)
+def shard_seed(rank):
+    """Each rank advances its own domain of the workload (independent members: weak scaling, no exchange)."""
+    return 1 + rank
+
+
+def max_over_ranks(value, world, device):
+    """The maximum of a per-rank time over all ranks (the job's time): an all-reduce MAX of one number."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def weak_value(world, pts, steps, ms):
+    """Whole-job grid-point-steps/s: every rank's points x steps over the slowest rank's time."""
+    return world * pts * steps / (ms / 1000.0)
+
+
 def clocks_sampler(device):
     """Samples SM clocks and throttle reasons with nvidia-smi every 200 ms until stopped."""
     q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -385,7 +407,7 @@ def main():
     lib = capi.load()
     lib.cw_use_device(local)
     prec = capi.MIXED if args.precision == "mixed" else capi.FP64
-    case = make_case(capi, prec, seed=1 + rank)
+    case = make_case(capi, prec, seed=shard_seed(rank))
     dom = Domain(case.g, case.o).upload_case(case)
     stream = torch.cuda.Stream()  # a dedicated stream: the handle launches on it, the events are recorded on it
     lib.cw_set_stream(dom.h, C.c_void_p(stream.cuda_stream))
@@ -411,11 +433,8 @@ def main():
     clocks = clocks_summary(sampler)
     ms = e0.elapsed_time(e1)
     launches = dom.launches()
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * pts * args.steps / (ms / 1000.0)
+    ms = max_over_ranks(ms, world, "cuda")
+    value = weak_value(world, pts, args.steps, ms)
 
     # e2e: the prognostic state from pinned host memory, one step, the state back, every step
     host = {}
@@ -452,11 +471,8 @@ def main():
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     ems = max(g0.elapsed_time(g1), wall * 1000.0)
-    if world > 1:
-        t = torch.tensor([ems], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ems = float(t.item())
-    e2e = world * pts * n_e2e / (ems / 1000.0)
+    ems = max_over_ranks(ems, world, "cuda")
+    e2e = weak_value(world, pts, n_e2e, ems)
 
     # per-kernel device time (eager steps with events around each launch); dominant kernel's roofline
     nk = C.c_int()
