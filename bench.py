@@ -372,12 +372,15 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default block shapes")
     ap.add_argument("--workload", choices=["lam", "precision", "ensemble", "served"], default="lam",
                     help="lam: the headline 119x89x44 line; the others: BASELINE configs 3, 4 and 5 (1 GPU)")
     ap.add_argument("--requests", type=int, default=24, help="served: number of requests")
     ap.add_argument("--rate", type=float, default=2.0, help="served: Poisson arrival rate per second")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if not args.no_autotune:
+        args.warmup = max(args.warmup, 5)  # 3 tuning steps, the graph capture, one replay
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -409,6 +412,8 @@ def main():
     prec = capi.MIXED if args.precision == "mixed" else capi.FP64
     case = make_case(capi, prec, seed=shard_seed(rank))
     dom = Domain(case.g, case.o).upload_case(case)
+    if not args.no_autotune:
+        dom.set_autotune(True)  # the first warm-up steps pick each point kernel's block shape
     stream = torch.cuda.Stream()  # a dedicated stream: the handle launches on it, the events are recorded on it
     lib.cw_set_stream(dom.h, C.c_void_p(stream.cuda_stream))
     pts = WORKLOAD["nx"] * WORKLOAD["ny"] * WORKLOAD["nz"]
@@ -510,7 +515,11 @@ def main():
             "config": {"workload": f"lam_119x89x44_{args.precision}", **WORKLOAD,
                        "moist_species": "qv qc qr qi qs (PD at rk 3)", "lbc": "specified, width 5",
                        "parallelism": f"one domain per GPU x{world}",
-                       "l2": "inputs larger than L2: ~110 fields x 5.4 MB per step, no flush"},
+                       "l2": "inputs larger than L2: ~110 fields x 5.4 MB per step, no flush",
+                       "block_shapes": {k: ["128x1", "64x2", "32x4"][dom.autotune_choice(k)]
+                                        for k in ("k_tend", "k_tendf_rk1", "k_uv", "k_q_update", "k_q_face_pd",
+                                                  "k_q_scale_pd", "k_q_update_pd", "k_p_rho_phi")
+                                        if dom.autotune_choice(k) >= 0}},
             "clocks": clocks, "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": ebytes,
                                       "d2h_bytes_per_step": ebytes, "steps": n_e2e},
             "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roofline}

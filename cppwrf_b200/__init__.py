@@ -93,6 +93,16 @@ class Domain:
     def set_graph(self, on):
         self.lib.cw_set_graph(self.h, 1 if on else 0)
 
+    def set_autotune(self, on=True):
+        """The next three steps time the point kernels' block shapes; each kernel then keeps its fastest."""
+        self.lib.cw_set_autotune(self.h, 1 if on else 0)
+        return self
+
+    def autotune_choice(self, kernel):
+        v = C.c_int()
+        self.lib.cw_autotune_choice(self.h, kernel.encode(), C.byref(v))
+        return v.value
+
 
 class Batch:
     """Several domains of uneven sizes advanced together: every kernel launch covers all members
@@ -119,6 +129,10 @@ class Batch:
 
     def upload_case(self, member, case):
         _check(self.lib, self.h, self.lib.cw_member_upload_case(self.h, member, case.h), "cw_member_upload_case")
+        return self
+
+    def set_autotune(self, on=True):
+        self.lib.cw_set_autotune(self.h, 1 if on else 0)
         return self
 
     def step(self, n=1):

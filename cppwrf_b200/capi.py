@@ -159,6 +159,8 @@ def load(path=None):
         "cw_download_noalloc": (i, [vp, i, i, dp, sz]),
         "cw_batch_add": (i, [vp, C.POINTER(Grid), C.POINTER(Options), ip]),
         "cw_batch_remove": (i, [vp, i]),
+        "cw_set_autotune": (i, [vp, i]),
+        "cw_autotune_choice": (i, [vp, C.c_char_p, ip]),
         "cw_footprint": (i, [C.POINTER(Grid), C.POINTER(Options), C.POINTER(sz)]),
         "cw_case_clone": (i, [vp, C.POINTER(vp)]),
         "cw_case_config": (i, [vp, C.POINTER(Grid), C.POINTER(Options)]),

@@ -80,7 +80,7 @@ struct Member {
 template <class R, int NM>
 struct Packs {
   std::vector<Pack<R, NM>> p;
-  std::vector<std::array<int, kNumKinds>> blocks;
+  std::vector<std::array<std::array<int, kNumShapes>, kNumKinds>> blocks;  // [pack][kind][shape]
 };
 template <class R>
 struct DevTables {  // the kernels' views of the members and the device scalar tables
@@ -131,6 +131,12 @@ struct cw_handle {
   std::string err;
   std::vector<void*> extra;      // other device allocations
   // per-kernel timing of eager steps (cw_profile): events around each launch
+  // block-shape autotuning of the point kernels: the first kNumShapes steps each run every tunable kernel
+  // with one shape (eager, timed per launch); then each kernel keeps its fastest shape
+  bool autotune = false, tuned = false;
+  int tuning_shape = -1, tune_steps_done = 0;
+  std::vector<std::pair<std::string, int>> shape_choice;
+  std::vector<std::pair<std::string, std::array<double, kNumShapes>>> tune_ms;
   bool profiling = false;
   std::vector<std::pair<const char*, std::pair<cudaEvent_t, cudaEvent_t>>> prof_ev;
   std::vector<std::string> prof_names;
@@ -354,17 +360,18 @@ void build_packs(cw_handle* h, const std::vector<Dom<R>>& doms, Packs<R, NM>& ps
   for (size_t m0 = 0; m0 < nm; m0 += NM) {
     Pack<R, NM> P{};
     P.n = int(std::min(nm - m0, size_t(NM)));
-    std::array<int, kNumKinds> tot{};
-    for (int kind = 0; kind < kNumKinds; ++kind) {
-      int b = 0;
-      for (int m = 0; m < P.n; ++m) {
-        const Member& M = h->m[m0 + size_t(m)];
-        P.start[kind][m] = b;
-        b += blocks_of(kind, M.g.nx, M.g.ny, M.g.nz, nys(M.g, 'V'));
+    std::array<std::array<int, kNumShapes>, kNumKinds> tot{};
+    for (int kind = 0; kind < kNumKinds; ++kind)
+      for (int sh = 0; sh < kNumShapes; ++sh) {
+        int b = 0;
+        for (int m = 0; m < P.n; ++m) {
+          const Member& M = h->m[m0 + size_t(m)];
+          P.start[kind][sh][m] = b;
+          b += blocks_of(kind, M.g.nx, M.g.ny, M.g.nz, nys(M.g, 'V'), sh);
+        }
+        P.start[kind][sh][P.n] = b;
+        tot[size_t(kind)][size_t(sh)] = b;
       }
-      P.start[kind][P.n] = b;
-      tot[size_t(kind)] = b;
-    }
     for (int m = 0; m < P.n; ++m) P.d[m] = doms[m0 + size_t(m)];
     ps.p.push_back(P);
     ps.blocks.push_back(tot);
@@ -603,25 +610,34 @@ struct Launcher {
     k_copy<<<unsigned((total + bs - 1) / bs), bs, 0, h->stream>>>(d, int(n), sd);
     check();
   }
-  // a point kernel over the index range kind, one launch per pack
+  // the block shape of a point kernel: the one being timed while tuning, else the tuned choice (0 by default)
+  int shape_for(const char* name) const {
+    if (h->tuning_shape >= 0) return h->tuning_shape;
+    for (const auto& [n, sh] : h->shape_choice)
+      if (n == name) return sh;
+    return 0;
+  }
+  // a point kernel of fixed shape 0 over the index range kind, one launch per pack
   template <class R, int NM, class K, class... Args>
   void run(const char* name, int kind, K kern, const Packs<R, NM>& ps, Args... args) {
     for (size_t c = 0; c < ps.p.size(); ++c) {
-      const int nb = ps.blocks[c][size_t(kind)];
+      const int nb = ps.blocks[c][size_t(kind)][0];
       if (nb == 0) continue;
       begin(name);
       kern<<<nb, PX, 0, h->stream>>>(ps.p[c], args...);
       check();
     }
   }
-  // a point kernel over the index range kind, once per species (blockIdx.y)
+  // a point kernel with a tunable block shape (one instantiation per shape), nq > 0: once per species
   template <class R, int NM, class K, class... Args>
-  void run_q(const char* name, int kind, int nq, K kern, const Packs<R, NM>& ps, Args... args) {
+  void run_t(const char* name, int kind, int nq, const std::array<K, kNumShapes>& kerns, const Packs<R, NM>& ps,
+             Args... args) {
+    const int sh = shape_for(name);
     for (size_t c = 0; c < ps.p.size(); ++c) {
-      const int nb = ps.blocks[c][size_t(kind)];
+      const int nb = ps.blocks[c][size_t(kind)][size_t(sh)];
       if (nb == 0 || nq == 0) continue;
       begin(name);
-      kern<<<dim3(nb, nq), PX, 0, h->stream>>>(ps.p[c], args...);
+      kerns[size_t(sh)]<<<dim3(nb, nq), PX, 0, h->stream>>>(ps.p[c], args...);
       check();
     }
   }
@@ -632,7 +648,7 @@ struct Launcher {
     const size_t smem = size_t(arrays) * h->cb_level_bytes;
     CW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     for (size_t c = 0; c < ps.p.size(); ++c) {
-      const int nb = ps.blocks[c][size_t(kind)];
+      const int nb = ps.blocks[c][size_t(kind)][0];
       if (nb == 0) continue;
       begin(name);
       kern<<<nb, dim3(CX, CNW), smem, h->stream>>>(ps.p[c], args...);
@@ -649,6 +665,9 @@ struct Launcher {
     }
   }
 };
+
+// the three block-shape instantiations of a tunable point kernel
+#define KV(kern) std::array{kern<R, NM, 0>, kern<R, NM, 1>, kern<R, NM, 2>}
 
 template <class R, int NM>
 void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
@@ -674,13 +693,13 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
     L.halo(cw_handle::H_PREP0);
     L.run_cb("k_ls_prep", RG_COLS_STAG, 1, k_ls_prep<R, NM>, d);
     L.halo(cw_handle::H_PREP1);
-    if (rk == 1) L.run("k_tendf_rk1", RG_STAG, k_tendf_rk1<R, NM>, d);
-    L.run("k_tend", RG_STAG, k_tend<R, NM>, d, rk);
+    if (rk == 1) L.run_t("k_tendf_rk1", RG_STAG, 1, KV(k_tendf_rk1), d);
+    L.run_t("k_tend", RG_STAG, 1, KV(k_tend), d, rk);
     if (rk == 1) L.copy_list(h->zeros_d, h->zeros_start_d, h->zeros.size(), h->zeros_total);
     L.run_cb("k_ss_prep", RG_COLS_STAG, 3, k_ss_prep<R, NM>, d, rk);
     L.halo(cw_handle::H_SS0);
     for (int it = 1; it <= ns; ++it) {
-      L.run("k_uv", RG_STAG, k_uv<R, NM>, d, rk);
+      L.run_t("k_uv", RG_STAG, 1, KV(k_uv), d, rk);
       L.halo(cw_handle::H_UV);
       L.run_cb("k_ac", RG_COLS_STAG, kCbArrays, k_ac<R, NM>, d, rk, it, ns);
       if (lbc) L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_ZERO_GRAD_W), rk);
@@ -690,15 +709,15 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
     L.run_cb("k_finish", RG_COLS_STAG, 0, k_finish<R, NM>, d, rk, ns);
     L.halo(cw_handle::H_FIN);
     if (scalars) {
-      if (rk == 1) L.run_q("k_q_tendf_rk1", RG_MASS, nq, k_q_tendf_rk1<R, NM>, d);
-      L.run_q("k_q_update", RG_MASS, nq, k_q_update<R, NM>, d, rk);
+      if (rk == 1) L.run_t("k_q_tendf_rk1", RG_MASS, nq, KV(k_q_tendf_rk1), d);
+      L.run_t("k_q_update", RG_MASS, nq, KV(k_q_update), d, rk);
       if (rk == 3 && any_pd) {
-        L.run_q("k_q_pre_pd", RG_MASS, nq, k_q_pre_pd<R, NM>, d, rk);
+        L.run_t("k_q_pre_pd", RG_MASS, nq, KV(k_q_pre_pd), d, rk);
         L.halo(cw_handle::H_Q1PD);
-        L.run_q("k_q_face_pd", RG_STAG, nq, k_q_face_pd<R, NM>, d, rk);
-        L.run_q("k_q_scale_pd", RG_MASS, nq, k_q_scale_pd<R, NM>, d, rk);
+        L.run_t("k_q_face_pd", RG_STAG, nq, KV(k_q_face_pd), d, rk);
+        L.run_t("k_q_scale_pd", RG_MASS, nq, KV(k_q_scale_pd), d, rk);
         L.halo(cw_handle::H_SCPD);
-        L.run_q("k_q_update_pd", RG_MASS, nq, k_q_update_pd<R, NM>, d, rk);
+        L.run_t("k_q_update_pd", RG_MASS, nq, KV(k_q_update_pd), d, rk);
       }
       L.run_members("k_q_swap", 64, k_q_swap<R, NM>, d);
       if (lbc) L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_FLOW_DEP), rk);
@@ -707,7 +726,7 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
   }
   if (lbc) {
     L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_FINAL), 3);
-    L.run("k_p_rho_phi", RG_MASS, k_p_rho_phi<R, NM>, d, 1);
+    L.run_t("k_p_rho_phi", RG_MASS, 1, KV(k_p_rho_phi), d, 1);
     L.halo(cw_handle::H_END_P);
   }
   if (terrain) {
@@ -735,9 +754,67 @@ void invalidate_graph(cw_handle* h) {
   h->graph_ok = false;
 }
 
+// one eager step with every tunable point kernel in block shape `shape`, each launch timed by events
+void tune_step(cw_handle* h, int shape) {
+  auto saved = std::move(h->prof_ev);
+  h->prof_ev.clear();
+  const bool was = h->profiling;
+  h->profiling = true;
+  h->tuning_shape = shape;
+  Launcher L{h};
+  try {
+    enqueue(h, L);
+  } catch (...) {
+    h->profiling = was;
+    h->tuning_shape = -1;
+    throw;
+  }
+  h->profiling = was;
+  h->tuning_shape = -1;
+  CW_CUDA(cudaStreamSynchronize(h->stream));
+  for (auto& [name, ev] : h->prof_ev) {
+    float ms = 0;
+    CW_CUDA(cudaEventElapsedTime(&ms, ev.first, ev.second));
+    cudaEventDestroy(ev.first);
+    cudaEventDestroy(ev.second);
+    auto it = std::find_if(h->tune_ms.begin(), h->tune_ms.end(), [&](const auto& e) { return e.first == name; });
+    if (it == h->tune_ms.end()) {
+      h->tune_ms.push_back({name, {}});
+      it = h->tune_ms.end() - 1;
+    }
+    it->second[size_t(shape)] += ms;
+  }
+  h->prof_ev = std::move(saved);
+  h->launches_last += L.count;
+}
+
+// after one tuning step per shape: every kernel keeps its fastest shape (the lowest on a tie)
+void finish_tuning(cw_handle* h) {
+  h->shape_choice.clear();
+  for (const auto& [name, ms] : h->tune_ms) {
+    int best = 0;
+    for (int sh = 1; sh < kNumShapes; ++sh)
+      if (ms[size_t(sh)] < ms[size_t(best)]) best = sh;
+    h->shape_choice.push_back({name, best});
+  }
+  h->tuned = true;
+  invalidate_graph(h);
+}
+
 void run_steps(cw_handle* h, int nsteps) {
   h->launches_last = 0;
   if (h->m.empty()) return;
+  while (h->autotune && !h->tuned && nsteps > 0) {  // tuning steps advance the state like any other step
+    const int sh = int(h->tune_ms.empty() ? 0 : h->tune_steps_done);
+    tune_step(h, sh);
+    for (Member& M : h->m) {
+      if (M.o.lbc) M.dtbc += M.g.dt;
+      if (M.o.n_scalars > 0) M.q_parity ^= 1;
+    }
+    --nsteps;
+    if (++h->tune_steps_done == kNumShapes) finish_tuning(h);
+  }
+  if (nsteps == 0) return;
   if (h->use_graph && !h->graph_ok) {
     Launcher L{h};
     CW_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -1224,6 +1301,24 @@ int cw_profile_entry(cw_handle* h, int idx, char* name, int len, double* ms, lon
   }
   if (ms) *ms = h->prof_ms[idx];
   if (launches) *launches = h->prof_n[idx];
+  return 0;
+}
+int cw_set_autotune(cw_handle* h, int on) {
+  if (!h) return -1;
+  h->autotune = on != 0;
+  h->tuned = false;
+  h->tune_steps_done = 0;
+  h->tune_ms.clear();
+  h->shape_choice.clear();
+  invalidate_graph(h);
+  return 0;
+}
+int cw_autotune_choice(cw_handle* h, const char* kernel, int* shape) {
+  if (!h || !kernel || !shape) return -1;
+  *shape = -1;
+  if (!h->tuned) return 0;
+  for (const auto& [n, sh] : h->shape_choice)
+    if (n == kernel) *shape = sh;
   return 0;
 }
 int cw_use_device(int device) {

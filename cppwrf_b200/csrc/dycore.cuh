@@ -79,22 +79,23 @@ struct Dom {
 // NM = 1) and no store of a kernel can alias them. start[kind][m] is member m's first block of a launch
 // over the index range `kind`; a batch of more members is launched in packs of kPackMembers.
 constexpr int kNumKinds = 6;
+constexpr int kNumShapes = 3;  // point-kernel block shapes (autotuned per kernel): 128 x 1, 64 x 2, 32 x 4
 constexpr int kPackMembers = 12;
 template <class R, int NM>
 struct Pack {
   Dom<R> d[NM];
   int n;
-  int start[kNumKinds][NM + 1];
+  int start[kNumKinds][kNumShapes][NM + 1];
 };
 template <class R, int NM>
-__device__ __forceinline__ int member_of(const Pack<R, NM>& P, int kind, int b) {
+__device__ __forceinline__ int member_of(const Pack<R, NM>& P, int kind, int shape, int b) {
   if constexpr (NM == 1) {
     return 0;
   } else {
     int lo = 0, hi = P.n - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (P.start[kind][mid] <= b) lo = mid;
+      if (P.start[kind][shape][mid] <= b) lo = mid;
       else hi = mid - 1;
     }
     return lo;
@@ -106,6 +107,9 @@ __device__ __forceinline__ int member_of(const Pack<R, NM>& P, int kind, int b) 
 // warps; the pointwise work of the columns' levels is split over the warps, the vertical recurrences run
 // on warp 0 (one lane per column) through shared memory. blockIdx over (i-tiles, j).
 constexpr int PX = 128, PY = 1;
+// point-kernel shape s: shape_x(s) points along i times shape_y(s) rows along j in one block of PX threads
+__host__ __device__ constexpr int shape_x(int s) { return s == 0 ? PX : (s == 1 ? PX / 2 : PX / 4); }
+__host__ __device__ constexpr int shape_y(int s) { return PX / shape_x(s); }
 constexpr int CX = 32, CNW = 8;
 constexpr int kCbArrays = 6;  // shared-memory level arrays of the acoustic column block: kCbArrays x (nz + 2) x CX doubles
 __host__ __device__ __forceinline__ int cdiv(int a, int b) { return (a + b - 1) / b; }

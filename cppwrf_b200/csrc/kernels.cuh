@@ -38,28 +38,29 @@ __host__ __device__ __forceinline__ Range range_of(int kind, int nx, int ny, int
   }
 }
 __host__ __device__ __forceinline__ bool is_column(int kind) { return kind == RG_COLS_STAG || kind == RG_COLS_MASS; }
-__host__ __device__ __forceinline__ int blocks_of(int kind, int nx, int ny, int nz, int nyv) {
+__host__ __device__ __forceinline__ int blocks_of(int kind, int nx, int ny, int nz, int nyv, int shape = 0) {
   const Range r = range_of(kind, nx, ny, nz, nyv);
-  const int tx = is_column(kind) ? CX : PX;
-  return cdiv(r.i1 - r.i0, tx) * (r.j1 - r.j0) * (r.k1 - r.k0);
+  if (is_column(kind)) return cdiv(r.i1 - r.i0, CX) * (r.j1 - r.j0) * (r.k1 - r.k0);
+  return cdiv(r.i1 - r.i0, shape_x(shape)) * cdiv(r.j1 - r.j0, shape_y(shape)) * (r.k1 - r.k0);
 }
-// thread -> (member, i, j, k); false for the threads past the range
-template <class R, int NM>
+// thread -> (member, i, j, k) of a point kernel launched with block shape SH; false past the range
+template <int SH, class R, int NM>
 __device__ __forceinline__ bool thread_index(const Pack<R, NM>& P, int kind, const Dom<R>*& Dp, int& i, int& j, int& k) {
+  constexpr int sx = shape_x(SH), sy = shape_y(SH);
   const int b = blockIdx.x;
-  const int m = member_of(P, kind, b);
+  const int m = member_of(P, kind, SH, b);
   const Dom<R>& D = P.d[m];
   Dp = &D;
   const Range r = range_of(kind, D.nx, D.ny, D.nz, D.nyv);
-  const int tx = is_column(kind) ? CX : PX;
-  const int bx = cdiv(r.i1 - r.i0, tx), by = r.j1 - r.j0;
-  int local = b - P.start[kind][m];
+  const int bx = cdiv(r.i1 - r.i0, sx), by = cdiv(r.j1 - r.j0, sy);
+  int local = b - P.start[kind][SH][m];
   const int bi = local % bx;
   local /= bx;
-  j = r.j0 + local % by;
+  const int bj = local % by;
   k = r.k0 + local / by;
-  i = r.i0 + bi * tx + int(threadIdx.x);
-  return i < r.i1;
+  i = r.i0 + bi * sx + int(threadIdx.x) % sx;
+  j = r.j0 + bj * sy + int(threadIdx.x) / sx;
+  return i < r.i1 && j < r.j1;
 }
 
 // ------------------------------------------------------------------ copies and halos
@@ -605,11 +606,11 @@ __device__ __forceinline__ bool spec_at(Ring r, int i, int j, int& sl, int& pos)
 // its own range: ru (u_i0 .. u_i1), rv (v_j0 .. v_j1, 3-D), rw and ph (levels 1..nz), theta (mass cells).
 // Also mu_tend = 0 (zero_tend of a run with lateral boundaries) at rk 2 and 3, and with lateral
 // boundaries the spec zone's tendencies from the boundary slabs.
-template <class R, int NM>
+template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_tend(const __grid_constant__ Pack<R, NM> P, int rk) {
   const Dom<R>* Dp;
   int i, j, k;
-  if (!thread_index(P, RG_STAG, Dp, i, j, k)) return;
+  if (!thread_index<SH>(P, RG_STAG, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
   const int nx = D.nx, ny = D.ny, nz = D.nz;
   const bool use_tendf = D.lbc || D.diff_on;
@@ -798,11 +799,11 @@ __device__ __forceinline__ R vdiff_uv(const Dom<R>& D, const V3<R>& f, const dou
 
 // rk 1: zero the held tendencies, add the constant-K diffusion; with lateral boundaries mu_tend = 0 and the
 // relaxation of rows 1..3 (LateralBC::relax_dry, lateral_bc.cpp:294-335) added to the held tendencies
-template <class R, int NM>
+template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R, NM> P) {
   const Dom<R>* Dp;
   int i, j, k;
-  if (!thread_index(P, RG_STAG, Dp, i, j, k)) return;
+  if (!thread_index<SH>(P, RG_STAG, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
   const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
   const bool dd = D.diff_on;
@@ -883,7 +884,7 @@ template <class R, int NM>
 __global__ void __launch_bounds__(PX) k_ring(const __grid_constant__ Pack<R, NM> P, int op, int rk) {
   const Dom<R>* Dp;
   int pos, k, side;
-  if (!thread_index(P, RG_RING, Dp, pos, k, side)) return;
+  if (!thread_index<0>(P, RG_RING, Dp, pos, k, side)) return;
   const Dom<R>& D = *Dp;
   (void)rk;
   const int nx = D.nx, ny = D.ny, nz = D.nz;

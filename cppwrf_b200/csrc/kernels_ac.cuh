@@ -72,11 +72,11 @@ __device__ __forceinline__ R uv_dp(const Dom<R>& D, int i, int j, int k, R mface
 }
 // over the staggered index range; with lateral boundaries the spec zone's faces take
 // u += dts ru_tend (LateralBC::update_uv, lateral_bc.cpp:353-361) instead
-template <class R, int NM>
+template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_uv(const __grid_constant__ Pack<R, NM> P, int rk) {
   const Dom<R>* Dp;
   int i, j, k;
-  if (!thread_index(P, RG_STAG, Dp, i, j, k)) return;
+  if (!thread_index<SH>(P, RG_STAG, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
   if (k >= D.nz) return;
   const R dts = R(rk == 1 ? D.dt / 3.0 : D.dt / D.n_sound);
@@ -140,11 +140,11 @@ __device__ __forceinline__ void p_rho_phi_point(const Dom<R>& D, int i, int j, i
   const double base = double(R(k::r_d) * (R(k::t0) + D.t2(i, j, k)) / (R(k::p1000mb) * (a + D.alb(i, j, k))));
   D.p(i, j, k) = R(k::p1000mb * cw_pow(base, k::cpovcv) - double(D.pb(i, j, k)));
 }
-template <class R, int NM>
+template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_p_rho_phi(const __grid_constant__ Pack<R, NM> P, int interior) {
   const Dom<R>* Dp;
   int i, j, k;
-  if (!thread_index(P, RG_MASS, Dp, i, j, k)) return;
+  if (!thread_index<SH>(P, RG_MASS, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
   if (interior) {  // calc_p_rho_phi_interior (:622-633): spec_zone 1 off each non-periodic side
     const int sz = 1;
@@ -173,11 +173,11 @@ __device__ __forceinline__ R m_full(const Dom<R>& D, int k, R mub, R mu) { retur
 // species with boundary data the relaxation of rows 1..3 (relax_scalars, lateral_bc.cpp:388-401) and the
 // spec zone's boundary tendency (spec_scalars, :403-414; the held tendency is not changed after rk 1, so
 // writing it once per step is the same as the reference's once per stage)
-template <class R, int NM>
+template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_q_tendf_rk1(const __grid_constant__ Pack<R, NM> P) {
   const Dom<R>* Dp;
   int i, j, k;
-  if (!thread_index(P, RG_MASS, Dp, i, j, k)) return;
+  if (!thread_index<SH>(P, RG_MASS, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
   const bool sp = D.lbc, px = D.bc_x == CW_BC_PERIODIC;
   int is = sp ? 1 : 0, ie = sp ? D.nx - 1 : D.nx;
@@ -211,11 +211,11 @@ __device__ R q_adv(const Dom<R>& D, const V3<R>& q, int i, int j, int k) {
   return r - R(D.rdnw[k]) * (sc_fz(D, q, D.ww_m, i, j, k + 1, false) - sc_fz(D, q, D.ww_m, i, j, k, false));
 }
 // KUpdate (:145-156) for the non-PD species of this stage
-template <class R, int NM>
+template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_q_update(const __grid_constant__ Pack<R, NM> P, int rk) {
   const Dom<R>* Dp;
   int i, j, k;
-  if (!thread_index(P, RG_MASS, Dp, i, j, k)) return;
+  if (!thread_index<SH>(P, RG_MASS, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
   const R dt_rk = R(rk == 1 ? D.dt / 3.0 : (rk == 2 ? 0.5 * D.dt : D.dt));
   const R mub = D.mub(i, j), mu1 = D.mu1(i, j, 0), mu2 = D.mu2(i, j, 0);
@@ -227,11 +227,11 @@ __global__ void __launch_bounds__(PX) k_q_update(const __grid_constant__ Pack<R,
   D.qn[n](i, j, k) = (m_full(D, k, mub, mu1) * D.q1[n](i, j, k) + dt_rk * tend) / m_full(D, k, mub, mu2);
 }
 // KPreUpdatePD (:174-180)
-template <class R, int NM>
+template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_q_pre_pd(const __grid_constant__ Pack<R, NM> P, int rk) {
   const Dom<R>* Dp;
   int i, j, k;
-  if (!thread_index(P, RG_MASS, Dp, i, j, k)) return;
+  if (!thread_index<SH>(P, RG_MASS, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
   const R dt_rk = R(rk == 1 ? D.dt / 3.0 : (rk == 2 ? 0.5 * D.dt : D.dt));
   const R m = m_full(D, k, D.mub(i, j), D.mu1(i, j, 0));
@@ -273,11 +273,11 @@ __device__ void pd_fz(const Dom<R>& D, const V3<R>& q, const V3<R>& qo, R dt, in
 }
 // KFacePDX / KFacePDY / KFacePDZ (:159-171 with the PD statement functions): every face flux of the PD
 // species once, dh and lo, into the species' face arrays (x faces 0..nx, y faces 0..ny, z faces 0..nz)
-template <class R, int NM>
+template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_q_face_pd(const __grid_constant__ Pack<R, NM> P, int rk) {
   const Dom<R>* Dp;
   int i, j, k;
-  if (!thread_index(P, RG_STAG, Dp, i, j, k)) return;
+  if (!thread_index<SH>(P, RG_STAG, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
   const int n = blockIdx.y;  // the species
   if (n >= D.n_scalars || !q_is_pd(D, n, rk)) return;
@@ -305,11 +305,11 @@ __global__ void __launch_bounds__(PX) k_q_face_pd(const __grid_constant__ Pack<R
   }
 }
 // KScalePD (:215-241) from the stored face fluxes
-template <class R, int NM>
+template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_q_scale_pd(const __grid_constant__ Pack<R, NM> P, int rk) {
   const Dom<R>* Dp;
   int i, j, k;
-  if (!thread_index(P, RG_MASS, Dp, i, j, k)) return;
+  if (!thread_index<SH>(P, RG_MASS, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
   const R dt = R(rk == 1 ? D.dt / 3.0 : (rk == 2 ? 0.5 * D.dt : D.dt));
   const bool edge = (D.spec_x && (i == 0 || i == D.nx - 1)) || (D.spec_y && (j == 0 || j == D.ny - 1));
@@ -348,11 +348,11 @@ __global__ void __launch_bounds__(PX) k_q_scale_pd(const __grid_constant__ Pack<
   D.qscale[n](i, j, k) = sc;
 }
 // KUpdatePD (:244-291) from the stored face fluxes
-template <class R, int NM>
+template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_q_update_pd(const __grid_constant__ Pack<R, NM> P, int rk) {
   const Dom<R>* Dp;
   int i, j, k;
-  if (!thread_index(P, RG_MASS, Dp, i, j, k)) return;
+  if (!thread_index<SH>(P, RG_MASS, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
   const R dt = R(rk == 1 ? D.dt / 3.0 : (rk == 2 ? 0.5 * D.dt : D.dt));
   const R mub = D.mub(i, j), mu1 = D.mu1(i, j, 0), mu2 = D.mu2(i, j, 0);

@@ -19,11 +19,11 @@ namespace cw {
 template <class R, int NM>
 __device__ __forceinline__ const Dom<R>& cb_member(const Pack<R, NM>& P, int kind, int& i, int& j) {
   const int b = blockIdx.x;
-  const int m = member_of(P, kind, b);
+  const int m = member_of(P, kind, 0, b);
   const Dom<R>& D = P.d[m];
   const Range r = range_of(kind, D.nx, D.ny, D.nz, D.nyv);
   const int bx = cdiv(r.i1 - r.i0, CX);
-  const int local = b - P.start[kind][m];
+  const int local = b - P.start[kind][0][m];
   i = r.i0 + (local % bx) * CX + int(threadIdx.x);
   j = r.j0 + local / bx;
   return D;

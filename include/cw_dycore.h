@@ -164,6 +164,13 @@ int cw_members(cw_handle* h, int* out);
  * a new member (its fields zeroed, map factors 1) as the last index; cw_batch_remove frees one member and
  * moves the members after it down by one index. Both rebuild the handle's tables; the next cw_step captures
  * the step again. cw_step on an empty batch does nothing. */
+/* Block-shape autotuning of the point kernels (no reference counterpart). With on = 1 the next three
+ * cw_step steps run every tunable kernel in one of its block shapes (0: 128 x 1, 1: 64 x 2, 2: 32 x 4
+ * points along i x j), timed per launch; afterwards each kernel keeps its fastest shape and the step is
+ * captured again. The tuning steps are ordinary steps: every shape computes the same values. Calling it
+ * again re-tunes. cw_autotune_choice gives a kernel's chosen shape (-1 before the tuning has finished). */
+int cw_set_autotune(cw_handle* h, int on);
+int cw_autotune_choice(cw_handle* h, const char* kernel, int* shape);
 int cw_batch_add(cw_handle* h, const cw_grid* g, const cw_options* o, int* member);
 int cw_batch_remove(cw_handle* h, int member);
 /* Device bytes one domain takes in a handle (fields, work fields, scalars, slabs, vertical arrays): the
