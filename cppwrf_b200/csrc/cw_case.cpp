@@ -360,13 +360,14 @@ double or_default(double v, double d) { return v < -1e299 ? d : v; }
 }  // namespace
 
 // cases::make_case + init_ideal + cases::initialize for the dry ideal cases (no moisture, flat terrain).
-// The grid's p_top becomes the sounding's pressure at ztop (src/cases/model.cpp:96-99).
+// The grid's p_top becomes the sounding's pressure at ztop (src/cases/model.cpp:96-99). Passive tracers
+// (n_scalars > 0 with n_moist = 0) start at zero; the caller fills them.
 int cw_gen_ideal(cw_case* c, const cw_ideal_params* pp) {
   if (!c || !pp) return -1;
   using namespace cw::cst;
   try {
     cw_grid& G = c->g;
-    if (!c->o.flat || c->o.n_scalars != 0 || c->o.lbc) return -2;
+    if (!c->o.flat || c->o.n_moist != 0 || c->o.lbc) return -2;
     const int kind = pp->kind;
     const double pi = std::numbers::pi;
     const double xcenter = 0.5 * G.nx * G.dx;

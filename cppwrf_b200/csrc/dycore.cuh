@@ -22,13 +22,16 @@ struct V3 {  // View3 of CPPWRF (src/core/field.hpp:19-23): element (0,0,0), 32-
   T* p;
   int sj, sk;
   __device__ __forceinline__ T& operator()(int i, int j, int k) const { return p[i + j * sj + k * sk]; }
+  // a load through the read-only path: only for a field no thread of the kernel writes (the compiler may
+  // then move it ahead of the kernel's stores)
+  __device__ __forceinline__ T ld(int i, int j, int k) const { return __ldg(p + (i + j * sj + k * sk)); }
 };
 template <class T>
 struct VB {  // BView3 / BView2 (field.hpp:35-44): si = sj = 0 for horizontally uniform storage
   const T* p;
   int si, sj, sk;
-  __device__ __forceinline__ T operator()(int i, int j, int k) const { return p[i * si + j * sj + k * sk]; }
-  __device__ __forceinline__ T operator()(int i, int j) const { return p[i * si + j * sj]; }
+  __device__ __forceinline__ T operator()(int i, int j, int k) const { return __ldg(p + (i * si + j * sj + k * sk)); }
+  __device__ __forceinline__ T operator()(int i, int j) const { return __ldg(p + (i * si + j * sj)); }
 };
 
 // Lateral boundary slabs of one variable: 4 sides of values then 4 of tendencies, (pos, k, b) pos fastest

@@ -178,29 +178,32 @@ static __global__ void k_halo(const __grid_constant__ HaloChunk s, int pass) {
 // [0, nx] x [0, nyv): every value a column thread writes depends only on its own column and on halo
 // values that the preceding refresh made current.
 template <class R>
+// (k_ls_prep: mu, u and v are read-only there)
 __device__ __forceinline__ R ww_mu_u(const Dom<R>& D, int i, int j) {
-  return R(0.5) * (D.mu2(i, j, 0) + D.mub(i, j) + D.mu2(i - 1, j, 0) + D.mub(i - 1, j));
+  return R(0.5) * (D.mu2.ld(i, j, 0) + D.mub(i, j) + D.mu2.ld(i - 1, j, 0) + D.mub(i - 1, j));
 }
 template <class R>
 __device__ __forceinline__ R ww_mu_v(const Dom<R>& D, int i, int j) {
-  return R(0.5) * (D.mu2(i, j, 0) + D.mub(i, j) + D.mu2(i, j - 1, 0) + D.mub(i, j - 1));
+  return R(0.5) * (D.mu2.ld(i, j, 0) + D.mub(i, j) + D.mu2.ld(i, j - 1, 0) + D.mub(i, j - 1));
 }
 template <class R>
 __device__ __forceinline__ R ww_divv(const Dom<R>& D, int i, int j, int k, R mu1, R mu0, R mv1, R mv0) {
   const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
   return D.msftx(i, j) * R(D.dnw[k]) *
-         (R(D.rdx) * ((c1h * mu1 + c2h) * D.u2(i + 1, j, k) / D.msfuy(i + 1, j) - (c1h * mu0 + c2h) * D.u2(i, j, k) / D.msfuy(i, j)) +
-          R(D.rdy) * ((c1h * mv1 + c2h) * D.v2(i, j + 1, k) * D.msfvx_inv(i, j + 1) -
-                      (c1h * mv0 + c2h) * D.v2(i, j, k) * D.msfvx_inv(i, j)));
+         (R(D.rdx) * ((c1h * mu1 + c2h) * D.u2.ld(i + 1, j, k) / D.msfuy(i + 1, j) - (c1h * mu0 + c2h) * D.u2.ld(i, j, k) / D.msfuy(i, j)) +
+          R(D.rdy) * ((c1h * mv1 + c2h) * D.v2.ld(i, j + 1, k) * D.msfvx_inv(i, j + 1) -
+                      (c1h * mv0 + c2h) * D.v2.ld(i, j, k) * D.msfvx_inv(i, j)));
 }
 
 // ------------------------------------------------------------------ rk_tendency
 template <class R>
-__device__ __forceinline__ R cqu_(const Dom<R>& D, int i, int j, int k) { return D.n_moist > 0 ? D.cqu(i, j, k) : R(1); }
+__device__ __forceinline__ R cqu_(const Dom<R>& D, int i, int j, int k) { return D.n_moist > 0 ? D.cqu.ld(i, j, k) : R(1); }
 template <class R>
-__device__ __forceinline__ R cqv_(const Dom<R>& D, int i, int j, int k) { return D.n_moist > 0 ? D.cqv(i, j, k) : R(1); }
+__device__ __forceinline__ R cqv_(const Dom<R>& D, int i, int j, int k) { return D.n_moist > 0 ? D.cqv.ld(i, j, k) : R(1); }
 template <class R>
-__device__ __forceinline__ R cqw_(const Dom<R>& D, int i, int j, int k) { return D.n_moist > 0 ? D.cqw(i, j, k) : R(0); }
+__device__ __forceinline__ R cqw_(const Dom<R>& D, int i, int j, int k) { return D.n_moist > 0 ? D.cqw.ld(i, j, k) : R(0); }
+// (cqu, cqv, cqw are written only by k_ls_prep, which does not read them). The tendency, flux and diffusion
+// functions below read only fields that no thread of their kernels writes: the read-only load path (.ld).
 
 // KTendU (large_step.cpp:152-264), no open boundaries, no Coriolis, unmapped
 template <class R>
@@ -208,36 +211,36 @@ __device__ R tu_fx(const Dom<R>& D, int i, int j, int k) {
   const int o = ord_mass(i, D.nx, D.spec_x);
   if (o == 2) {
     if (i <= 1) {
-      const R ub = (D.spec_x && D.u2(i, j, k) < R(0)) ? D.u2(i, j, k) : D.u2(i - 1, j, k);
-      return R(0.25) * (D.ru(i, j, k) + D.ru(i - 1, j, k)) * (D.u2(i, j, k) + ub);
+      const R ub = (D.spec_x && D.u2.ld(i, j, k) < R(0)) ? D.u2.ld(i, j, k) : D.u2.ld(i - 1, j, k);
+      return R(0.25) * (D.ru.ld(i, j, k) + D.ru.ld(i - 1, j, k)) * (D.u2.ld(i, j, k) + ub);
     }
-    const R ub = (D.spec_x && D.u2(i - 1, j, k) > R(0)) ? D.u2(i - 1, j, k) : D.u2(i, j, k);
-    return R(0.25) * (D.ru(i, j, k) + D.ru(i - 1, j, k)) * (D.u2(i - 1, j, k) + ub);
+    const R ub = (D.spec_x && D.u2.ld(i - 1, j, k) > R(0)) ? D.u2.ld(i - 1, j, k) : D.u2.ld(i, j, k);
+    return R(0.25) * (D.ru.ld(i, j, k) + D.ru.ld(i - 1, j, k)) * (D.u2.ld(i - 1, j, k) + ub);
   }
-  const R vel = R(0.5) * (D.ru(i, j, k) + D.ru(i - 1, j, k));
-  if (o == 3) return vel * flux3(D.u2(i - 2, j, k), D.u2(i - 1, j, k), D.u2(i, j, k), D.u2(i + 1, j, k), vel, R(D.hup));
-  return vel * flux5(D.u2(i - 3, j, k), D.u2(i - 2, j, k), D.u2(i - 1, j, k), D.u2(i, j, k), D.u2(i + 1, j, k),
-                     D.u2(i + 2, j, k), vel, R(D.hup));
+  const R vel = R(0.5) * (D.ru.ld(i, j, k) + D.ru.ld(i - 1, j, k));
+  if (o == 3) return vel * flux3(D.u2.ld(i - 2, j, k), D.u2.ld(i - 1, j, k), D.u2.ld(i, j, k), D.u2.ld(i + 1, j, k), vel, R(D.hup));
+  return vel * flux5(D.u2.ld(i - 3, j, k), D.u2.ld(i - 2, j, k), D.u2.ld(i - 1, j, k), D.u2.ld(i, j, k), D.u2.ld(i + 1, j, k),
+                     D.u2.ld(i + 2, j, k), vel, R(D.hup));
 }
 template <class R>
 __device__ R tu_fy(const Dom<R>& D, int i, int j, int k) {
   const int o = ord_face(j, D.ny, D.spec_y);
-  if (o == 2) return R(0.25) * (D.rv(i, j, k) + D.rv(i - 1, j, k)) * (D.u2(i, j, k) + D.u2(i, j - 1, k));
-  const R vel = R(0.5) * (D.rv(i, j, k) + D.rv(i - 1, j, k));
-  if (o == 3) return vel * flux3(D.u2(i, j - 2, k), D.u2(i, j - 1, k), D.u2(i, j, k), D.u2(i, j + 1, k), vel, R(D.hup));
-  return vel * flux5(D.u2(i, j - 3, k), D.u2(i, j - 2, k), D.u2(i, j - 1, k), D.u2(i, j, k), D.u2(i, j + 1, k),
-                     D.u2(i, j + 2, k), vel, R(D.hup));
+  if (o == 2) return R(0.25) * (D.rv.ld(i, j, k) + D.rv.ld(i - 1, j, k)) * (D.u2.ld(i, j, k) + D.u2.ld(i, j - 1, k));
+  const R vel = R(0.5) * (D.rv.ld(i, j, k) + D.rv.ld(i - 1, j, k));
+  if (o == 3) return vel * flux3(D.u2.ld(i, j - 2, k), D.u2.ld(i, j - 1, k), D.u2.ld(i, j, k), D.u2.ld(i, j + 1, k), vel, R(D.hup));
+  return vel * flux5(D.u2.ld(i, j - 3, k), D.u2.ld(i, j - 2, k), D.u2.ld(i, j - 1, k), D.u2.ld(i, j, k), D.u2.ld(i, j + 1, k),
+                     D.u2.ld(i, j + 2, k), vel, R(D.hup));
 }
 template <class R>
 __device__ R tu_fz(const Dom<R>& D, int i, int j, int k) {
   if (k == 0 || k == D.nz) return 0;
-  const R vel = R(0.5) * (D.ww(i - 1, j, k) + D.ww(i, j, k));
-  if (k == 1 || k == D.nz - 1) return vel * (R(D.fnm[k]) * D.u2(i, j, k) + R(D.fnp[k]) * D.u2(i, j, k - 1));
-  return vel * flux3(D.u2(i, j, k - 2), D.u2(i, j, k - 1), D.u2(i, j, k), D.u2(i, j, k + 1), -vel, R(D.vup));
+  const R vel = R(0.5) * (D.ww.ld(i - 1, j, k) + D.ww.ld(i, j, k));
+  if (k == 1 || k == D.nz - 1) return vel * (R(D.fnm[k]) * D.u2.ld(i, j, k) + R(D.fnp[k]) * D.u2.ld(i, j, k - 1));
+  return vel * flux3(D.u2.ld(i, j, k - 2), D.u2.ld(i, j, k - 1), D.u2.ld(i, j, k), D.u2.ld(i, j, k + 1), -vel, R(D.vup));
 }
 template <class R, int DI, int DJ>
 __device__ __forceinline__ R pgf_dpn(const Dom<R>& D, int i, int j, int k) {  // p' at w level k, face column
-  auto ps = [&](int kk) { return D.p(i - DI, j - DJ, kk) + D.p(i, j, kk); };
+  auto ps = [&](int kk) { return D.p.ld(i - DI, j - DJ, kk) + D.p.ld(i, j, kk); };
   const int nz = D.nz;
   if (k == 0) return R(0.5) * (R(D.cf1) * ps(0) + R(D.cf2) * ps(1) + R(D.cf3) * ps(2));
   if (k == nz) return D.top_lid ? R(0.5) * (R(D.cfn) * ps(nz - 1) + R(D.cfn1) * ps(nz - 2)) : R(0);
@@ -251,17 +254,17 @@ __device__ R tend_u(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
   if (D.do_y) t -= (D.msfux(i, j) * rdy) * (tu_fy(D, i, j + 1, k) - tu_fy(D, i, j, k));
   t -= R(D.rdnw[k]) * (tu_fz(D, i, j, k + 1) - tu_fz(D, i, j, k));
   const R rm = D.msfux(i, j) / D.msfuy(i, j);
-  R dpx = rm * R(0.5) * rdx * (c1h * D.muu(i, j, 0) + c2h) *
-          ((D.ph2(i, j, k + 1) - D.ph2(i - 1, j, k + 1) + D.ph2(i, j, k) - D.ph2(i - 1, j, k)) +
-           (D.alt(i, j, k) + D.alt(i - 1, j, k)) * (D.p(i, j, k) - D.p(i - 1, j, k)) +
-           (D.al(i, j, k) + D.al(i - 1, j, k)) * (D.pb(i, j, k) - D.pb(i - 1, j, k)));
-  dpx += rm * rdx * (D.php(i, j, k) - D.php(i - 1, j, k)) *
+  R dpx = rm * R(0.5) * rdx * (c1h * D.muu.ld(i, j, 0) + c2h) *
+          ((D.ph2.ld(i, j, k + 1) - D.ph2.ld(i - 1, j, k + 1) + D.ph2.ld(i, j, k) - D.ph2.ld(i - 1, j, k)) +
+           (D.alt.ld(i, j, k) + D.alt.ld(i - 1, j, k)) * (D.p.ld(i, j, k) - D.p.ld(i - 1, j, k)) +
+           (D.al.ld(i, j, k) + D.al.ld(i - 1, j, k)) * (D.pb(i, j, k) - D.pb(i - 1, j, k)));
+  dpx += rm * rdx * (D.php.ld(i, j, k) - D.php.ld(i - 1, j, k)) *
          (R(D.rdnw[k]) * (pgf_dpn<R, 1, 0>(D, i, j, k + 1) - pgf_dpn<R, 1, 0>(D, i, j, k)) -
-          R(0.5) * (c1h * D.mu2(i - 1, j, 0) + c1h * D.mu2(i, j, 0)));
+          R(0.5) * (c1h * D.mu2.ld(i - 1, j, 0) + c1h * D.mu2.ld(i, j, 0)));
   t -= cqu_(D, i, j, k) * dpx;
-  const R rw4 = R(0.25) * (D.rw(i - 1, j, k + 1) + D.rw(i - 1, j, k) + D.rw(i, j, k + 1) + D.rw(i, j, k));
-  t = t - D.u2(i, j, k) * R(k::reradius) * rw4;
-  if (use_tendf) t += D.ru_tendf(i, j, k) / D.msfuy(i, j);
+  const R rw4 = R(0.25) * (D.rw.ld(i - 1, j, k + 1) + D.rw.ld(i - 1, j, k) + D.rw.ld(i, j, k + 1) + D.rw.ld(i, j, k));
+  t = t - D.u2.ld(i, j, k) * R(k::reradius) * rw4;
+  if (use_tendf) t += D.ru_tendf.ld(i, j, k) / D.msfuy(i, j);
   return t;
 }
 
@@ -269,34 +272,34 @@ __device__ R tend_u(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
 template <class R>
 __device__ R tv_fx(const Dom<R>& D, int i, int j, int k) {
   const int o = ord_face(i, D.nx, D.spec_x);
-  if (o == 2) return R(0.25) * (D.ru(i, j, k) + D.ru(i, j - 1, k)) * (D.v2(i, j, k) + D.v2(i - 1, j, k));
-  const R vel = R(0.5) * (D.ru(i, j, k) + D.ru(i, j - 1, k));
-  if (o == 3) return vel * flux3(D.v2(i - 2, j, k), D.v2(i - 1, j, k), D.v2(i, j, k), D.v2(i + 1, j, k), vel, R(D.hup));
-  return vel * flux5(D.v2(i - 3, j, k), D.v2(i - 2, j, k), D.v2(i - 1, j, k), D.v2(i, j, k), D.v2(i + 1, j, k),
-                     D.v2(i + 2, j, k), vel, R(D.hup));
+  if (o == 2) return R(0.25) * (D.ru.ld(i, j, k) + D.ru.ld(i, j - 1, k)) * (D.v2.ld(i, j, k) + D.v2.ld(i - 1, j, k));
+  const R vel = R(0.5) * (D.ru.ld(i, j, k) + D.ru.ld(i, j - 1, k));
+  if (o == 3) return vel * flux3(D.v2.ld(i - 2, j, k), D.v2.ld(i - 1, j, k), D.v2.ld(i, j, k), D.v2.ld(i + 1, j, k), vel, R(D.hup));
+  return vel * flux5(D.v2.ld(i - 3, j, k), D.v2.ld(i - 2, j, k), D.v2.ld(i - 1, j, k), D.v2.ld(i, j, k), D.v2.ld(i + 1, j, k),
+                     D.v2.ld(i + 2, j, k), vel, R(D.hup));
 }
 template <class R>
 __device__ R tv_fy(const Dom<R>& D, int i, int j, int k) {
   const int o = ord_mass(j, D.ny, D.spec_y);
   if (o == 2) {
     if (j <= 1) {
-      const R vb = (D.spec_y && D.v2(i, j, k) < R(0)) ? D.v2(i, j, k) : D.v2(i, j - 1, k);
-      return R(0.25) * (D.rv(i, j, k) + D.rv(i, j - 1, k)) * (D.v2(i, j, k) + vb);
+      const R vb = (D.spec_y && D.v2.ld(i, j, k) < R(0)) ? D.v2.ld(i, j, k) : D.v2.ld(i, j - 1, k);
+      return R(0.25) * (D.rv.ld(i, j, k) + D.rv.ld(i, j - 1, k)) * (D.v2.ld(i, j, k) + vb);
     }
-    const R vb = (D.spec_y && D.v2(i, j - 1, k) > R(0)) ? D.v2(i, j - 1, k) : D.v2(i, j, k);
-    return R(0.25) * (D.rv(i, j, k) + D.rv(i, j - 1, k)) * (vb + D.v2(i, j - 1, k));
+    const R vb = (D.spec_y && D.v2.ld(i, j - 1, k) > R(0)) ? D.v2.ld(i, j - 1, k) : D.v2.ld(i, j, k);
+    return R(0.25) * (D.rv.ld(i, j, k) + D.rv.ld(i, j - 1, k)) * (vb + D.v2.ld(i, j - 1, k));
   }
-  const R vel = R(0.5) * (D.rv(i, j, k) + D.rv(i, j - 1, k));
-  if (o == 3) return vel * flux3(D.v2(i, j - 2, k), D.v2(i, j - 1, k), D.v2(i, j, k), D.v2(i, j + 1, k), vel, R(D.hup));
-  return vel * flux5(D.v2(i, j - 3, k), D.v2(i, j - 2, k), D.v2(i, j - 1, k), D.v2(i, j, k), D.v2(i, j + 1, k),
-                     D.v2(i, j + 2, k), vel, R(D.hup));
+  const R vel = R(0.5) * (D.rv.ld(i, j, k) + D.rv.ld(i, j - 1, k));
+  if (o == 3) return vel * flux3(D.v2.ld(i, j - 2, k), D.v2.ld(i, j - 1, k), D.v2.ld(i, j, k), D.v2.ld(i, j + 1, k), vel, R(D.hup));
+  return vel * flux5(D.v2.ld(i, j - 3, k), D.v2.ld(i, j - 2, k), D.v2.ld(i, j - 1, k), D.v2.ld(i, j, k), D.v2.ld(i, j + 1, k),
+                     D.v2.ld(i, j + 2, k), vel, R(D.hup));
 }
 template <class R>
 __device__ R tv_fz(const Dom<R>& D, int i, int j, int k) {
   if (k == 0 || k == D.nz) return 0;
-  const R vel = R(0.5) * (D.ww(i, j - 1, k) + D.ww(i, j, k));
-  if (k == 1 || k == D.nz - 1) return vel * (R(D.fnm[k]) * D.v2(i, j, k) + R(D.fnp[k]) * D.v2(i, j, k - 1));
-  return vel * flux3(D.v2(i, j, k - 2), D.v2(i, j, k - 1), D.v2(i, j, k), D.v2(i, j, k + 1), -vel, R(D.vup));
+  const R vel = R(0.5) * (D.ww.ld(i, j - 1, k) + D.ww.ld(i, j, k));
+  if (k == 1 || k == D.nz - 1) return vel * (R(D.fnm[k]) * D.v2.ld(i, j, k) + R(D.fnp[k]) * D.v2.ld(i, j, k - 1));
+  return vel * flux3(D.v2.ld(i, j, k - 2), D.v2.ld(i, j, k - 1), D.v2.ld(i, j, k), D.v2.ld(i, j, k + 1), -vel, R(D.vup));
 }
 template <class R>
 __device__ R tend_v(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
@@ -306,17 +309,17 @@ __device__ R tend_v(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
   R t = -(D.msfvy(i, j) * rdx) * (tv_fx(D, i + 1, j, k) - tv_fx(D, i, j, k));
   t -= (D.msfvy(i, j) * rdy) * (tv_fy(D, i, j + 1, k) - tv_fy(D, i, j, k));
   t -= rm * R(D.rdnw[k]) * (tv_fz(D, i, j, k + 1) - tv_fz(D, i, j, k));
-  R dpy = rm * R(0.5) * rdy * (c1h * D.muv(i, j, 0) + c2h) *
-          ((D.ph2(i, j, k + 1) - D.ph2(i, j - 1, k + 1) + D.ph2(i, j, k) - D.ph2(i, j - 1, k)) +
-           (D.alt(i, j, k) + D.alt(i, j - 1, k)) * (D.p(i, j, k) - D.p(i, j - 1, k)) +
-           (D.al(i, j, k) + D.al(i, j - 1, k)) * (D.pb(i, j, k) - D.pb(i, j - 1, k)));
-  dpy += rm * rdy * (D.php(i, j, k) - D.php(i, j - 1, k)) *
+  R dpy = rm * R(0.5) * rdy * (c1h * D.muv.ld(i, j, 0) + c2h) *
+          ((D.ph2.ld(i, j, k + 1) - D.ph2.ld(i, j - 1, k + 1) + D.ph2.ld(i, j, k) - D.ph2.ld(i, j - 1, k)) +
+           (D.alt.ld(i, j, k) + D.alt.ld(i, j - 1, k)) * (D.p.ld(i, j, k) - D.p.ld(i, j - 1, k)) +
+           (D.al.ld(i, j, k) + D.al.ld(i, j - 1, k)) * (D.pb(i, j, k) - D.pb(i, j - 1, k)));
+  dpy += rm * rdy * (D.php.ld(i, j, k) - D.php.ld(i, j - 1, k)) *
          (R(D.rdnw[k]) * (pgf_dpn<R, 0, 1>(D, i, j, k + 1) - pgf_dpn<R, 0, 1>(D, i, j, k)) -
-          R(0.5) * (c1h * D.mu2(i, j - 1, 0) + c1h * D.mu2(i, j, 0)));
+          R(0.5) * (c1h * D.mu2.ld(i, j - 1, 0) + c1h * D.mu2.ld(i, j, 0)));
   t -= cqv_(D, i, j, k) * dpy;
-  const R rw4 = R(0.25) * (D.rw(i, j - 1, k + 1) + D.rw(i, j - 1, k) + D.rw(i, j, k + 1) + D.rw(i, j, k));
-  t = t - rm * D.v2(i, j, k) * R(k::reradius) * rw4;
-  if (use_tendf) t += D.rv_tendf(i, j, k) * D.msfvx_inv(i, j);
+  const R rw4 = R(0.25) * (D.rw.ld(i, j - 1, k + 1) + D.rw.ld(i, j - 1, k) + D.rw.ld(i, j, k + 1) + D.rw.ld(i, j, k));
+  t = t - rm * D.v2.ld(i, j, k) * R(k::reradius) * rw4;
+  if (use_tendf) t += D.rv_tendf.ld(i, j, k) * D.msfvx_inv(i, j);
   return t;
 }
 
@@ -324,39 +327,39 @@ __device__ R tend_v(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
 template <class R>
 __device__ __forceinline__ R tw_rux(const Dom<R>& D, int i, int j, int k) {
   const int nz = D.nz;
-  if (k < nz) return R(D.fnm[k]) * D.ru(i, j, k) + R(D.fnp[k]) * D.ru(i, j, k - 1);
-  return (R(2) - R(D.fnm[nz - 1])) * D.ru(i, j, nz - 1) - R(D.fnp[nz - 1]) * D.ru(i, j, nz - 2);
+  if (k < nz) return R(D.fnm[k]) * D.ru.ld(i, j, k) + R(D.fnp[k]) * D.ru.ld(i, j, k - 1);
+  return (R(2) - R(D.fnm[nz - 1])) * D.ru.ld(i, j, nz - 1) - R(D.fnp[nz - 1]) * D.ru.ld(i, j, nz - 2);
 }
 template <class R>
 __device__ __forceinline__ R tw_rvy(const Dom<R>& D, int i, int j, int k) {
   const int nz = D.nz;
-  if (k < nz) return R(D.fnm[k]) * D.rv(i, j, k) + R(D.fnp[k]) * D.rv(i, j, k - 1);
-  return (R(2) - R(D.fnm[nz - 1])) * D.rv(i, j, nz - 1) - R(D.fnp[nz - 1]) * D.rv(i, j, nz - 2);
+  if (k < nz) return R(D.fnm[k]) * D.rv.ld(i, j, k) + R(D.fnp[k]) * D.rv.ld(i, j, k - 1);
+  return (R(2) - R(D.fnm[nz - 1])) * D.rv.ld(i, j, nz - 1) - R(D.fnp[nz - 1]) * D.rv.ld(i, j, nz - 2);
 }
 template <class R>
 __device__ R tw_fx(const Dom<R>& D, int i, int j, int k) {
   const R vel = tw_rux(D, i, j, k);
   const int o = ord_face(i, D.nx, D.spec_x);
-  if (o == 2) return R(0.5) * vel * (D.w2(i, j, k) + D.w2(i - 1, j, k));
-  if (o == 3) return vel * flux3(D.w2(i - 2, j, k), D.w2(i - 1, j, k), D.w2(i, j, k), D.w2(i + 1, j, k), vel, R(D.hup));
-  return vel * flux5(D.w2(i - 3, j, k), D.w2(i - 2, j, k), D.w2(i - 1, j, k), D.w2(i, j, k), D.w2(i + 1, j, k),
-                     D.w2(i + 2, j, k), vel, R(D.hup));
+  if (o == 2) return R(0.5) * vel * (D.w2.ld(i, j, k) + D.w2.ld(i - 1, j, k));
+  if (o == 3) return vel * flux3(D.w2.ld(i - 2, j, k), D.w2.ld(i - 1, j, k), D.w2.ld(i, j, k), D.w2.ld(i + 1, j, k), vel, R(D.hup));
+  return vel * flux5(D.w2.ld(i - 3, j, k), D.w2.ld(i - 2, j, k), D.w2.ld(i - 1, j, k), D.w2.ld(i, j, k), D.w2.ld(i + 1, j, k),
+                     D.w2.ld(i + 2, j, k), vel, R(D.hup));
 }
 template <class R>
 __device__ R tw_fy(const Dom<R>& D, int i, int j, int k) {
   const R vel = tw_rvy(D, i, j, k);
   const int o = ord_face(j, D.ny, D.spec_y);
-  if (o == 2) return R(0.5) * vel * (D.w2(i, j, k) + D.w2(i, j - 1, k));
-  if (o == 3) return vel * flux3(D.w2(i, j - 2, k), D.w2(i, j - 1, k), D.w2(i, j, k), D.w2(i, j + 1, k), vel, R(D.hup));
-  return vel * flux5(D.w2(i, j - 3, k), D.w2(i, j - 2, k), D.w2(i, j - 1, k), D.w2(i, j, k), D.w2(i, j + 1, k),
-                     D.w2(i, j + 2, k), vel, R(D.hup));
+  if (o == 2) return R(0.5) * vel * (D.w2.ld(i, j, k) + D.w2.ld(i, j - 1, k));
+  if (o == 3) return vel * flux3(D.w2.ld(i, j - 2, k), D.w2.ld(i, j - 1, k), D.w2.ld(i, j, k), D.w2.ld(i, j + 1, k), vel, R(D.hup));
+  return vel * flux5(D.w2.ld(i, j - 3, k), D.w2.ld(i, j - 2, k), D.w2.ld(i, j - 1, k), D.w2.ld(i, j, k), D.w2.ld(i, j + 1, k),
+                     D.w2.ld(i, j + 2, k), vel, R(D.hup));
 }
 template <class R>
 __device__ R tw_fz(const Dom<R>& D, int i, int j, int m) {
   if (m == 0 || m == D.nz - 1)
-    return R(0.25) * (D.ww(i, j, m + 1) + D.ww(i, j, m)) * (D.w2(i, j, m + 1) + D.w2(i, j, m));
-  const R vel = R(0.5) * (D.ww(i, j, m + 1) + D.ww(i, j, m));
-  return vel * flux3(D.w2(i, j, m - 1), D.w2(i, j, m), D.w2(i, j, m + 1), D.w2(i, j, m + 2), -vel, R(D.vup));
+    return R(0.25) * (D.ww.ld(i, j, m + 1) + D.ww.ld(i, j, m)) * (D.w2.ld(i, j, m + 1) + D.w2.ld(i, j, m));
+  const R vel = R(0.5) * (D.ww.ld(i, j, m + 1) + D.ww.ld(i, j, m));
+  return vel * flux3(D.w2.ld(i, j, m - 1), D.w2.ld(i, j, m), D.w2.ld(i, j, m + 1), D.w2.ld(i, j, m + 2), -vel, R(D.vup));
 }
 template <class R>
 __device__ R tend_w(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
@@ -369,103 +372,103 @@ __device__ R tend_w(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
     t -= R(D.rdn[k]) * (tw_fz(D, i, j, k) - tw_fz(D, i, j, k - 1));
     const R cqw = cqw_(D, i, j, k), cq1 = R(1) / (R(1) + cqw), cq2 = cqw * cq1;
     t += rmsft * R(k::g) *
-         (cq1 * R(D.rdn[k]) * (D.p(i, j, k) - D.p(i, j, k - 1)) - R(D.c1f[k]) * D.mu2(i, j, 0) -
+         (cq1 * R(D.rdn[k]) * (D.p.ld(i, j, k) - D.p.ld(i, j, k - 1)) - R(D.c1f[k]) * D.mu2.ld(i, j, 0) -
           cq2 * (R(D.c1f[k]) * D.mub(i, j) + R(D.c2f[k])));
     if (D.w_damping) {  // w_damp, wd_dt = dt
       const R wd_dt = R(D.dt);
-      const R muf = R(D.c1f[k]) * D.mut(i, j, 0) + R(D.c2f[k]);
-      R cfl = D.ww(i, j, k) / muf * R(D.rdnw[k]) * wd_dt;
+      const R muf = R(D.c1f[k]) * D.mut.ld(i, j, 0) + R(D.c2f[k]);
+      R cfl = D.ww.ld(i, j, k) / muf * R(D.rdnw[k]) * wd_dt;
       cfl = cfl < R(0) ? -cfl : cfl;
-      if (cfl > R(1)) t = t - (D.w2(i, j, k) < R(0) ? R(-1) : R(1)) * R(0.3) * (cfl - R(D.w_crit_cfl)) * muf;
+      if (cfl > R(1)) t = t - (D.w2.ld(i, j, k) < R(0) ? R(-1) : R(1)) * R(0.3) * (cfl - R(D.w_crit_cfl)) * muf;
     }
     const R fnm = R(D.fnm[k]), fnp = R(D.fnp[k]);
-    const R ruw = R(0.5) * (fnm * (D.ru(i, j, k) + D.ru(i + 1, j, k)) + fnp * (D.ru(i, j, k - 1) + D.ru(i + 1, j, k - 1)));
-    const R rvw = R(0.5) * (fnm * (D.rv(i, j, k) + D.rv(i, j + 1, k)) + fnp * (D.rv(i, j, k - 1) + D.rv(i, j + 1, k - 1)));
+    const R ruw = R(0.5) * (fnm * (D.ru.ld(i, j, k) + D.ru.ld(i + 1, j, k)) + fnp * (D.ru.ld(i, j, k - 1) + D.ru.ld(i + 1, j, k - 1)));
+    const R rvw = R(0.5) * (fnm * (D.rv.ld(i, j, k) + D.rv.ld(i, j + 1, k)) + fnp * (D.rv.ld(i, j, k - 1) + D.rv.ld(i, j + 1, k - 1)));
     const R rmt = D.msftx(i, j) / D.msfty(i, j);
-    const R uw = R(0.5) * (fnm * (D.u2(i, j, k) + D.u2(i + 1, j, k)) + fnp * (D.u2(i, j, k - 1) + D.u2(i + 1, j, k - 1)));
-    const R vw = R(0.5) * (fnm * (D.v2(i, j, k) + D.v2(i, j + 1, k)) + fnp * (D.v2(i, j, k - 1) + D.v2(i, j + 1, k - 1)));
+    const R uw = R(0.5) * (fnm * (D.u2.ld(i, j, k) + D.u2.ld(i + 1, j, k)) + fnp * (D.u2.ld(i, j, k - 1) + D.u2.ld(i + 1, j, k - 1)));
+    const R vw = R(0.5) * (fnm * (D.v2.ld(i, j, k) + D.v2.ld(i, j + 1, k)) + fnp * (D.v2.ld(i, j, k - 1) + D.v2.ld(i, j + 1, k - 1)));
     t = t + R(k::reradius) * (ruw * uw + rmt * rvw * vw);
   } else {
     t += R(2) * R(D.rdn[nz - 1]) * tw_fz(D, i, j, nz - 1);
     const R cqw = cqw_(D, i, j, nz - 1), cq1 = R(1) / (R(1) + cqw), cq2 = cqw * cq1;
     t += rmsft * R(k::g) *
-         (cq1 * R(2) * R(D.rdnw[nz - 1]) * (-D.p(i, j, nz - 1)) - R(D.c1f[nz]) * D.mu2(i, j, 0) -
+         (cq1 * R(2) * R(D.rdnw[nz - 1]) * (-D.p.ld(i, j, nz - 1)) - R(D.c1f[nz]) * D.mu2.ld(i, j, 0) -
           cq2 * (R(D.c1f[nz]) * D.mub(i, j) + R(D.c2f[nz])));
   }
-  if (use_tendf) t += D.rw_tendf(i, j, k) / D.msfty(i, j);
+  if (use_tendf) t += D.rw_tendf.ld(i, j, k) / D.msfty(i, j);
   return t;
 }
 
 // KTendT (:502-565) / advect_scalar face fluxes of any mass field q with mass fluxes (ufx, vfy, wfz)
 template <class R>
 __device__ R sc_fx(const Dom<R>& D, const V3<R>& q, const V3<R>& ruf, int i, int j, int k, bool pd) {
-  const R vel = ruf(i, j, k);
+  const R vel = ruf.ld(i, j, k);
   const int o = ord_face(i, D.nx, D.spec_x);
-  if (o == 2) return R(0.5) * vel * (q(i, j, k) + q(i - 1, j, k));
+  if (o == 2) return R(0.5) * vel * (q.ld(i, j, k) + q.ld(i - 1, j, k));
   if (o == 3) {
-    if (pd) return vel * flux3_pd(q(i - 2, j, k), q(i - 1, j, k), q(i, j, k), q(i + 1, j, k), vel, R(D.hup));
-    return vel * flux3(q(i - 2, j, k), q(i - 1, j, k), q(i, j, k), q(i + 1, j, k), vel, R(D.hup));
+    if (pd) return vel * flux3_pd(q.ld(i - 2, j, k), q.ld(i - 1, j, k), q.ld(i, j, k), q.ld(i + 1, j, k), vel, R(D.hup));
+    return vel * flux3(q.ld(i - 2, j, k), q.ld(i - 1, j, k), q.ld(i, j, k), q.ld(i + 1, j, k), vel, R(D.hup));
   }
   if (pd)
-    return vel * flux5_pd(q(i - 3, j, k), q(i - 2, j, k), q(i - 1, j, k), q(i, j, k), q(i + 1, j, k), q(i + 2, j, k), vel, R(D.hup));
-  return vel * flux5(q(i - 3, j, k), q(i - 2, j, k), q(i - 1, j, k), q(i, j, k), q(i + 1, j, k), q(i + 2, j, k), vel, R(D.hup));
+    return vel * flux5_pd(q.ld(i - 3, j, k), q.ld(i - 2, j, k), q.ld(i - 1, j, k), q.ld(i, j, k), q.ld(i + 1, j, k), q.ld(i + 2, j, k), vel, R(D.hup));
+  return vel * flux5(q.ld(i - 3, j, k), q.ld(i - 2, j, k), q.ld(i - 1, j, k), q.ld(i, j, k), q.ld(i + 1, j, k), q.ld(i + 2, j, k), vel, R(D.hup));
 }
 template <class R>
 __device__ R sc_fy(const Dom<R>& D, const V3<R>& q, const V3<R>& rvf, int i, int j, int k, bool pd) {
-  const R vel = rvf(i, j, k);
+  const R vel = rvf.ld(i, j, k);
   const int o = ord_face(j, D.ny, D.spec_y);
-  if (o == 2) return R(0.5) * vel * (q(i, j, k) + q(i, j - 1, k));
+  if (o == 2) return R(0.5) * vel * (q.ld(i, j, k) + q.ld(i, j - 1, k));
   if (o == 3) {
-    if (pd) return vel * flux3_pd(q(i, j - 2, k), q(i, j - 1, k), q(i, j, k), q(i, j + 1, k), vel, R(D.hup));
-    return vel * flux3(q(i, j - 2, k), q(i, j - 1, k), q(i, j, k), q(i, j + 1, k), vel, R(D.hup));
+    if (pd) return vel * flux3_pd(q.ld(i, j - 2, k), q.ld(i, j - 1, k), q.ld(i, j, k), q.ld(i, j + 1, k), vel, R(D.hup));
+    return vel * flux3(q.ld(i, j - 2, k), q.ld(i, j - 1, k), q.ld(i, j, k), q.ld(i, j + 1, k), vel, R(D.hup));
   }
   if (pd)
-    return vel * flux5_pd(q(i, j - 3, k), q(i, j - 2, k), q(i, j - 1, k), q(i, j, k), q(i, j + 1, k), q(i, j + 2, k), vel, R(D.hup));
-  return vel * flux5(q(i, j - 3, k), q(i, j - 2, k), q(i, j - 1, k), q(i, j, k), q(i, j + 1, k), q(i, j + 2, k), vel, R(D.hup));
+    return vel * flux5_pd(q.ld(i, j - 3, k), q.ld(i, j - 2, k), q.ld(i, j - 1, k), q.ld(i, j, k), q.ld(i, j + 1, k), q.ld(i, j + 2, k), vel, R(D.hup));
+  return vel * flux5(q.ld(i, j - 3, k), q.ld(i, j - 2, k), q.ld(i, j - 1, k), q.ld(i, j, k), q.ld(i, j + 1, k), q.ld(i, j + 2, k), vel, R(D.hup));
 }
 template <class R>
 __device__ R sc_fz(const Dom<R>& D, const V3<R>& q, const V3<R>& wwf, int i, int j, int k, bool pd) {
   if (k == 0 || k == D.nz) return 0;
-  const R vel = wwf(i, j, k);
-  if (k == 1 || k == D.nz - 1) return vel * (R(D.fnm[k]) * q(i, j, k) + R(D.fnp[k]) * q(i, j, k - 1));
-  if (pd) return vel * flux3_pd(q(i, j, k - 2), q(i, j, k - 1), q(i, j, k), q(i, j, k + 1), -vel, R(D.vup));
-  return vel * flux3(q(i, j, k - 2), q(i, j, k - 1), q(i, j, k), q(i, j, k + 1), -vel, R(D.vup));
+  const R vel = wwf.ld(i, j, k);
+  if (k == 1 || k == D.nz - 1) return vel * (R(D.fnm[k]) * q.ld(i, j, k) + R(D.fnp[k]) * q.ld(i, j, k - 1));
+  if (pd) return vel * flux3_pd(q.ld(i, j, k - 2), q.ld(i, j, k - 1), q.ld(i, j, k), q.ld(i, j, k + 1), -vel, R(D.vup));
+  return vel * flux3(q.ld(i, j, k - 2), q.ld(i, j, k - 1), q.ld(i, j, k), q.ld(i, j, k + 1), -vel, R(D.vup));
 }
 template <class R>
 __device__ R tend_t(const Dom<R>& D, int i, int j, int k, bool use_tendf, bool use_hd) {
   R r = -(D.msftx(i, j) * R(D.rdx)) * (sc_fx(D, D.t2, D.ru, i + 1, j, k, false) - sc_fx(D, D.t2, D.ru, i, j, k, false));
   if (D.do_y) r -= (D.msftx(i, j) * R(D.rdy)) * (sc_fy(D, D.t2, D.rv, i, j + 1, k, false) - sc_fy(D, D.t2, D.rv, i, j, k, false));
   r -= R(D.rdnw[k]) * (sc_fz(D, D.t2, D.ww, i, j, k + 1, false) - sc_fz(D, D.t2, D.ww, i, j, k, false));
-  if (use_tendf) r += D.t_tendf(i, j, k) / D.msfty(i, j);
-  if (use_hd) r += (R(D.c1h[k]) * D.mut(i, j, 0) + R(D.c2h[k])) * D.hd(i, j, k) / D.msfty(i, j);
+  if (use_tendf) r += D.t_tendf.ld(i, j, k) / D.msfty(i, j);
+  if (use_hd) r += (R(D.c1h[k]) * D.mut.ld(i, j, 0) + R(D.c2h[k])) * D.hd.ld(i, j, k) / D.msfty(i, j);
   return r;
 }
 
 // KTendPh (:570-668)
 template <class R>
 __device__ __forceinline__ R tph_wdwn(const Dom<R>& D, int i, int j, int m) {
-  return R(0.5) * (D.ww(i, j, m + 1) + D.ww(i, j, m)) * R(D.rdnw[m]) *
-         (D.ph2(i, j, m + 1) - D.ph2(i, j, m) + D.phb(i, j, m + 1) - D.phb(i, j, m));
+  return R(0.5) * (D.ww.ld(i, j, m + 1) + D.ww.ld(i, j, m)) * R(D.rdnw[m]) *
+         (D.ph2.ld(i, j, m + 1) - D.ph2.ld(i, j, m) + D.phb(i, j, m + 1) - D.phb(i, j, m));
 }
 template <class R, int DI, int DJ>
 __device__ __forceinline__ R grad6(const Dom<R>& D, int i, int j, int k) {
-  return R(45) * (D.ph2(i + DI, j + DJ, k) - D.ph2(i - DI, j - DJ, k)) -
-         R(9) * (D.ph2(i + 2 * DI, j + 2 * DJ, k) - D.ph2(i - 2 * DI, j - 2 * DJ, k)) +
-         (D.ph2(i + 3 * DI, j + 3 * DJ, k) - D.ph2(i - 3 * DI, j - 3 * DJ, k)) +
+  return R(45) * (D.ph2.ld(i + DI, j + DJ, k) - D.ph2.ld(i - DI, j - DJ, k)) -
+         R(9) * (D.ph2.ld(i + 2 * DI, j + 2 * DJ, k) - D.ph2.ld(i - 2 * DI, j - 2 * DJ, k)) +
+         (D.ph2.ld(i + 3 * DI, j + 3 * DJ, k) - D.ph2.ld(i - 3 * DI, j - 3 * DJ, k)) +
          R(45) * (D.phb(i + DI, j + DJ, k) - D.phb(i - DI, j - DJ, k)) -
          R(9) * (D.phb(i + 2 * DI, j + 2 * DJ, k) - D.phb(i - 2 * DI, j - 2 * DJ, k)) +
          (D.phb(i + 3 * DI, j + 3 * DJ, k) - D.phb(i - 3 * DI, j - 3 * DJ, k));
 }
 template <class R, int DI, int DJ>
 __device__ __forceinline__ R grad4(const Dom<R>& D, int i, int j, int k) {
-  return R(8) * (D.ph2(i + DI, j + DJ, k) - D.ph2(i - DI, j - DJ, k)) -
-         (D.ph2(i + 2 * DI, j + 2 * DJ, k) - D.ph2(i - 2 * DI, j - 2 * DJ, k)) +
+  return R(8) * (D.ph2.ld(i + DI, j + DJ, k) - D.ph2.ld(i - DI, j - DJ, k)) -
+         (D.ph2.ld(i + 2 * DI, j + 2 * DJ, k) - D.ph2.ld(i - 2 * DI, j - 2 * DJ, k)) +
          R(8) * (D.phb(i + DI, j + DJ, k) - D.phb(i - DI, j - DJ, k)) -
          (D.phb(i + 2 * DI, j + 2 * DJ, k) - D.phb(i - 2 * DI, j - 2 * DJ, k));
 }
 template <class R, int DI, int DJ>
 __device__ __forceinline__ R dfwd(const Dom<R>& D, int i, int j, int k) {
-  return D.phb(i + DI, j + DJ, k) - D.phb(i, j, k) + D.ph2(i + DI, j + DJ, k) - D.ph2(i, j, k);
+  return D.phb(i + DI, j + DJ, k) - D.phb(i, j, k) + D.ph2.ld(i + DI, j + DJ, k) - D.ph2.ld(i, j, k);
 }
 __device__ __forceinline__ int ph_horder(int i, int n, int on, int is_x) {
   if (!on) return 6;
@@ -480,12 +483,12 @@ __device__ R tend_ph(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
   const R c1f = R(D.c1f[k]), c2f = R(D.c2f[k]);
   R t = 0;
   if (k < nz) t = t - (R(D.fnm[k]) * tph_wdwn(D, i, j, k) + R(D.fnp[k]) * tph_wdwn(D, i, j, k - 1));
-  t = t + (c1f * D.mut(i, j, 0) + c2f) * R(k::g) * D.w2(i, j, k) / D.msfty(i, j);
+  t = t + (c1f * D.mut.ld(i, j, 0) + c2f) * R(k::g) * D.w2.ld(i, j, k) / D.msfty(i, j);
   const R r60 = R(1) / R(60), r12 = R(1) / R(12);
   if (D.do_y) {
-    const R mvp = c1f * D.muv(i, j + 1, 0) + c2f, mvm = c1f * D.muv(i, j, 0) + c2f;
-    const R vp = k < nz ? D.v2(i, j + 1, k) + D.v2(i, j + 1, k - 1) : R(D.cfn) * D.v2(i, j + 1, nz - 1) + R(D.cfn1) * D.v2(i, j + 1, nz - 2);
-    const R vm = k < nz ? D.v2(i, j, k) + D.v2(i, j, k - 1) : R(D.cfn) * D.v2(i, j, nz - 1) + R(D.cfn1) * D.v2(i, j, nz - 2);
+    const R mvp = c1f * D.muv.ld(i, j + 1, 0) + c2f, mvm = c1f * D.muv.ld(i, j, 0) + c2f;
+    const R vp = k < nz ? D.v2.ld(i, j + 1, k) + D.v2.ld(i, j + 1, k - 1) : R(D.cfn) * D.v2.ld(i, j + 1, nz - 1) + R(D.cfn1) * D.v2.ld(i, j + 1, nz - 2);
+    const R vm = k < nz ? D.v2.ld(i, j, k) + D.v2.ld(i, j, k - 1) : R(D.cfn) * D.v2.ld(i, j, nz - 1) + R(D.cfn1) * D.v2.ld(i, j, nz - 2);
     const R cy = (k < nz ? R(0.25) : R(0.5)) * R(D.rdy) / D.msfty(i, j);
     const int o = ph_horder(j, D.ny, D.spec_y, 0);
     if (o == 6) t = t - cy * ((mvp * vp * D.msfvy(i, j + 1) + mvm * vm * D.msfvy(i, j)) * r60 * grad6<R, 0, 1>(D, i, j, k));
@@ -493,16 +496,16 @@ __device__ R tend_ph(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
     else if (o == 2)
       t = t - cy * (mvp * vp * D.msfvy(i, j + 1) * dfwd<R, 0, 1>(D, i, j, k) + mvm * vm * D.msfvy(i, j) * dfwd<R, 0, 1>(D, i, j - 1, k));
   }
-  const R mup = c1f * D.muu(i + 1, j, 0) + c2f, mum = c1f * D.muu(i, j, 0) + c2f;
-  const R up = k < nz ? D.u2(i + 1, j, k) + D.u2(i + 1, j, k - 1) : R(D.cfn) * D.u2(i + 1, j, nz - 1) + R(D.cfn1) * D.u2(i + 1, j, nz - 2);
-  const R um = k < nz ? D.u2(i, j, k) + D.u2(i, j, k - 1) : R(D.cfn) * D.u2(i, j, nz - 1) + R(D.cfn1) * D.u2(i, j, nz - 2);
+  const R mup = c1f * D.muu.ld(i + 1, j, 0) + c2f, mum = c1f * D.muu.ld(i, j, 0) + c2f;
+  const R up = k < nz ? D.u2.ld(i + 1, j, k) + D.u2.ld(i + 1, j, k - 1) : R(D.cfn) * D.u2.ld(i + 1, j, nz - 1) + R(D.cfn1) * D.u2.ld(i + 1, j, nz - 2);
+  const R um = k < nz ? D.u2.ld(i, j, k) + D.u2.ld(i, j, k - 1) : R(D.cfn) * D.u2.ld(i, j, nz - 1) + R(D.cfn1) * D.u2.ld(i, j, nz - 2);
   const R cx = (k < nz ? R(0.25) : R(0.5)) * R(D.rdx) / D.msfty(i, j);
   const int o = ph_horder(i, D.nx, D.spec_x, 1);
   if (o == 6) t = t - cx * ((mup * up * D.msfux(i + 1, j) + mum * um * D.msfux(i, j)) * r60 * grad6<R, 1, 0>(D, i, j, k));
   else if (o == 2)
     t = t - cx * (mup * up * D.msfux(i + 1, j) * dfwd<R, 1, 0>(D, i, j, k) + mum * um * D.msfux(i, j) * dfwd<R, 1, 0>(D, i - 1, j, k));
   else if (o == 4) t = t - cx * ((mup * up * D.msfux(i + 1, j) + mum * um * D.msfux(i, j)) * r12 * grad4<R, 1, 0>(D, i, j, k));
-  if (use_tendf) t = t + D.ph_tendf(i, j, k) / D.msfty(i, j);
+  if (use_tendf) t = t + D.ph_tendf.ld(i, j, k) / D.msfty(i, j);
   return t;
 }
 
@@ -561,8 +564,8 @@ __device__ void relax_terms(const Dom<R>& D, const V3<R>& f, const double* c1, c
   const R dtbc = R(*D.dtbc);
   auto BV = [&](int p, int bb) { return slab_val(s, sl, p, k, bb, dtbc); };
   auto FV = [&](int ii, int jj) -> R {
-    const R x = Two ? f(ii, jj, 0) : f(ii, jj, k);
-    return c1 ? x * (R(c1[k]) * D.mut(ii, jj, 0) + R(c2[k])) : x;
+    const R x = Two ? f.ld(ii, jj, 0) : f.ld(ii, jj, k);
+    return c1 ? x * (R(c1[k]) * D.mut.ld(ii, jj, 0) + R(c2[k])) : x;
   };
   R fls0, fls1, fls2, fls3, fls4;
   fls0 = BV(pos, b) - FV(i, j);
@@ -668,7 +671,7 @@ __global__ void __launch_bounds__(PX) k_tend(const __grid_constant__ Pack<R, NM>
 // large_step.cpp:888-894), then the horizontal and vertical diffusion are added in the reference's order.
 template <class R>
 __device__ __forceinline__ R mk(const double* c1, const double* c2, const V3<R>& mut, int i, int j, int k) {
-  return R(c1[k]) * mut(i, j, 0) + R(c2[k]);
+  return R(c1[k]) * mut.ld(i, j, 0) + R(c2[k]);
 }
 template <class R>
 __device__ R hdiff_u(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, R xk, int i, int j, int k) {
@@ -684,8 +687,8 @@ __device__ R hdiff_u(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, R xk, in
                    (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j + 1, k) + mk(c1, c2, mut, i - 1, j + 1, k) + mk(c1, c2, mut, i - 1, j, k)) *
                    R(0.25) * (xk + xk + xk + xk) * rdy;
   const R mrdy = D.msfux(i, j) * D.msfuy(i, j) * rdy;
-  return mrdx * (mkrdxp * (f(i + 1, j, k) - f(i, j, k)) - mkrdxm * (f(i, j, k) - f(i - 1, j, k))) +
-         mrdy * (mkrdyp * (f(i, j + 1, k) - f(i, j, k)) - mkrdym * (f(i, j, k) - f(i, j - 1, k)));
+  return mrdx * (mkrdxp * (f.ld(i + 1, j, k) - f.ld(i, j, k)) - mkrdxm * (f.ld(i, j, k) - f.ld(i - 1, j, k))) +
+         mrdy * (mkrdyp * (f.ld(i, j + 1, k) - f.ld(i, j, k)) - mkrdym * (f.ld(i, j, k) - f.ld(i, j - 1, k)));
 }
 template <class R>
 __device__ R hdiff_v(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, R xk, int i, int j, int k) {
@@ -701,8 +704,8 @@ __device__ R hdiff_v(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, R xk, in
   const R mkrdym = (D.msfty(i, j - 1) / D.msftx(i, j - 1)) * xk * rdy;
   const R mkrdyp = (D.msfty(i, j) / D.msftx(i, j)) * xk * rdy;
   const R mrdy = D.msfvx(i, j) * D.msfvy(i, j) * rdy;
-  return mrdx * (mkrdxp * (f(i + 1, j, k) - f(i, j, k)) - mkrdxm * (f(i, j, k) - f(i - 1, j, k))) +
-         mrdy * (mkrdyp * (f(i, j + 1, k) - f(i, j, k)) - mkrdym * (f(i, j, k) - f(i, j - 1, k)));
+  return mrdx * (mkrdxp * (f.ld(i + 1, j, k) - f.ld(i, j, k)) - mkrdxm * (f.ld(i, j, k) - f.ld(i - 1, j, k))) +
+         mrdy * (mkrdyp * (f.ld(i, j + 1, k) - f.ld(i, j, k)) - mkrdym * (f.ld(i, j, k) - f.ld(i, j - 1, k)));
 }
 template <class R>
 __device__ R hdiff_w(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, R xk, int i, int j, int k) {
@@ -722,8 +725,8 @@ __device__ R hdiff_w(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, R xk, in
                    (mk(c1, c2, mut, i, j + 1, k) + mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j + 1, k) + mk(c1, c2, mut, i, j, k)) *
                    R(0.25) * (xk + xk + xk + xk) * rdy;
   const R mrdy = D.msftx(i, j) * D.msfty(i, j) * rdy;
-  return mrdx * (mkrdxp * (f(i + 1, j, k) - f(i, j, k)) - mkrdxm * (f(i, j, k) - f(i - 1, j, k))) +
-         mrdy * (mkrdyp * (f(i, j + 1, k) - f(i, j, k)) - mkrdym * (f(i, j, k) - f(i, j - 1, k)));
+  return mrdx * (mkrdxp * (f.ld(i + 1, j, k) - f.ld(i, j, k)) - mkrdxm * (f.ld(i, j, k) - f.ld(i - 1, j, k))) +
+         mrdy * (mkrdyp * (f.ld(i, j + 1, k) - f.ld(i, j, k)) - mkrdym * (f.ld(i, j, k) - f.ld(i, j - 1, k)));
 }
 // KHorizDiffM1 (with_base = false) / KHorizDiff3DMP (base = t_init or qv_base)
 template <class R>
@@ -737,32 +740,32 @@ __device__ R hdiff_m(const Dom<R>& D, const V3<R>& f, const VB<R>* base, const V
   const R mkrdyp = (D.msfvy(i, j + 1) * D.msfvx_inv(i, j + 1)) * R(0.5) * (xk + xk) * R(0.5) * (mk(c1, c2, mut, i, j + 1, k) + mk(c1, c2, mut, i, j, k)) * rdy;
   const R mrdy = D.msftx(i, j) * D.msfty(i, j) * rdy;
   if (!base)
-    return mrdx * (mkrdxp * (f(i + 1, j, k) - f(i, j, k)) - mkrdxm * (f(i, j, k) - f(i - 1, j, k))) +
-           mrdy * (mkrdyp * (f(i, j + 1, k) - f(i, j, k)) - mkrdym * (f(i, j, k) - f(i, j - 1, k)));
+    return mrdx * (mkrdxp * (f.ld(i + 1, j, k) - f.ld(i, j, k)) - mkrdxm * (f.ld(i, j, k) - f.ld(i - 1, j, k))) +
+           mrdy * (mkrdyp * (f.ld(i, j + 1, k) - f.ld(i, j, k)) - mkrdym * (f.ld(i, j, k) - f.ld(i, j - 1, k)));
   const VB<R>& b = *base;
-  const R dxp = f(i + 1, j, k) - f(i, j, k) - b(i + 1, j, k) + b(i, j, k);
-  const R dxm = f(i, j, k) - f(i - 1, j, k) - b(i, j, k) + b(i - 1, j, k);
-  const R dyp = f(i, j + 1, k) - f(i, j, k) - b(i, j + 1, k) + b(i, j, k);
-  const R dym = f(i, j, k) - f(i, j - 1, k) - b(i, j, k) + b(i, j - 1, k);
+  const R dxp = f.ld(i + 1, j, k) - f.ld(i, j, k) - b(i + 1, j, k) + b(i, j, k);
+  const R dxm = f.ld(i, j, k) - f.ld(i - 1, j, k) - b(i, j, k) + b(i - 1, j, k);
+  const R dyp = f.ld(i, j + 1, k) - f.ld(i, j, k) - b(i, j + 1, k) + b(i, j, k);
+  const R dym = f.ld(i, j, k) - f.ld(i, j - 1, k) - b(i, j, k) + b(i, j - 1, k);
   return mrdx * (mkrdxp * dxp - mkrdxm * dxm) + mrdy * (mkrdyp * dyp - mkrdym * dym);
 }
 // the vertical diffusion flux of a column at interface k (vflux[k] of the reference's column kernels)
 template <class R>
 __device__ __forceinline__ R vflux_w(const Dom<R>& D, const V3<R>& f, R kv, int i, int j, int k) {
   if (k >= D.nz - 1) return 0;
-  return (kv / D.alt(i, j, k)) * R(D.rdnw[k]) * (f(i, j, k + 1) - f(i, j, k));
+  return (kv / D.alt.ld(i, j, k)) * R(D.rdnw[k]) * (f.ld(i, j, k + 1) - f.ld(i, j, k));
 }
 template <class R>
 __device__ __forceinline__ R vflux_m(const Dom<R>& D, const V3<R>& f, const VB<R>* base, R kv, int i, int j, int k) {
   if (k >= D.nz - 1) return 0;
-  const R dpert = base ? f(i, j, k + 1) - f(i, j, k) - (*base)(i, j, k + 1) + (*base)(i, j, k) : f(i, j, k + 1) - f(i, j, k);
-  return kv * R(D.rdn[k + 1]) / (R(0.5) * (D.alt(i, j, k) + D.alt(i, j, k + 1))) * dpert;
+  const R dpert = base ? f.ld(i, j, k + 1) - f.ld(i, j, k) - (*base)(i, j, k + 1) + (*base)(i, j, k) : f.ld(i, j, k + 1) - f.ld(i, j, k);
+  return kv * R(D.rdn[k + 1]) / (R(0.5) * (D.alt.ld(i, j, k) + D.alt.ld(i, j, k + 1))) * dpert;
 }
 template <class R, int DI, int DJ>
 __device__ __forceinline__ R vflux_uv(const Dom<R>& D, const V3<R>& f, const double* ub, R kv, int i, int j, int k) {
   if (k >= D.nz - 1) return 0;
-  const R a = R(0.25) * (D.alt(i, j, k) + D.alt(i - DI, j - DJ, k) + D.alt(i, j, k + 1) + D.alt(i - DI, j - DJ, k + 1));
-  const R dpert = f(i, j, k + 1) - f(i, j, k) - R(ub[k + 1]) + R(ub[k]);
+  const R a = R(0.25) * (D.alt.ld(i, j, k) + D.alt.ld(i - DI, j - DJ, k) + D.alt.ld(i, j, k + 1) + D.alt.ld(i - DI, j - DJ, k + 1));
+  const R dpert = f.ld(i, j, k + 1) - f.ld(i, j, k) - R(ub[k + 1]) + R(ub[k]);
   return kv * R(D.rdn[k + 1]) / a * dpert;
 }
 // vertical_diffusion 'w' (KVertDiffW1), 'm' / mp (KVertDiffM1 / MP1), u / v (KVertDiffU1 / V1): the
@@ -770,8 +773,8 @@ __device__ __forceinline__ R vflux_uv(const Dom<R>& D, const V3<R>& f, const dou
 template <class R>
 __device__ __forceinline__ R vdiff_w(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, R kv, int i, int j, int k) {
   const R G = R(k::g);
-  const R mu = R(D.c1f[k]) * mut(i, j, 0) + R(D.c2f[k]);
-  const R alt_avg = R(0.5) * (D.alt(i, j, k) + D.alt(i, j, k - 1));
+  const R mu = R(D.c1f[k]) * mut.ld(i, j, 0) + R(D.c2f[k]);
+  const R alt_avg = R(0.5) * (D.alt.ld(i, j, k) + D.alt.ld(i, j, k - 1));
   return R(D.rdn[k]) * G * G / mu / alt_avg * (vflux_w(D, f, kv, i, j, k) - vflux_w(D, f, kv, i, j, k - 1));
 }
 template <class R>
@@ -779,21 +782,21 @@ __device__ __forceinline__ R vdiff_m(const Dom<R>& D, const V3<R>& f, const VB<R
   const R G = R(k::g);
   if (k == 0) {
     const R vf0 = vflux_m(D, f, base, kv, i, j, 0);
-    return G * G / (R(D.c1h[0]) * mut(i, j, 0) + R(D.c2h[0])) / D.alt(i, j, 0) * R(D.rdnw[0]) * (vf0 - vf0);
+    return G * G / (R(D.c1h[0]) * mut.ld(i, j, 0) + R(D.c2h[0])) / D.alt.ld(i, j, 0) * R(D.rdnw[0]) * (vf0 - vf0);
   }
-  const R mu = R(D.c1h[k]) * mut(i, j, 0) + R(D.c2h[k]);
-  return G * G / mu / D.alt(i, j, k) * R(D.rdnw[k]) * (vflux_m(D, f, base, kv, i, j, k) - vflux_m(D, f, base, kv, i, j, k - 1));
+  const R mu = R(D.c1h[k]) * mut.ld(i, j, 0) + R(D.c2h[k]);
+  return G * G / mu / D.alt.ld(i, j, k) * R(D.rdnw[k]) * (vflux_m(D, f, base, kv, i, j, k) - vflux_m(D, f, base, kv, i, j, k - 1));
 }
 template <class R, int DI, int DJ>
 __device__ __forceinline__ R vdiff_uv(const Dom<R>& D, const V3<R>& f, const double* ub, const V3<R>& muf, R kv, int i, int j, int k) {
   const R G = R(k::g);
   if (k == 0) {
     const R vf0 = vflux_uv<R, DI, DJ>(D, f, ub, kv, i, j, 0);
-    return G * G * R(D.rdnw[0]) / (R(D.c1h[0]) * muf(i, j, 0) + R(D.c2h[0])) /
-           (R(0.5) * (D.alt(i - DI, j - DJ, 0) + D.alt(i, j, 0))) * (vf0 - vf0);
+    return G * G * R(D.rdnw[0]) / (R(D.c1h[0]) * muf.ld(i, j, 0) + R(D.c2h[0])) /
+           (R(0.5) * (D.alt.ld(i - DI, j - DJ, 0) + D.alt.ld(i, j, 0))) * (vf0 - vf0);
   }
-  const R mu = R(D.c1h[k]) * muf(i, j, 0) + R(D.c2h[k]);
-  const R a = R(0.5) * (D.alt(i - DI, j - DJ, k) + D.alt(i, j, k));
+  const R mu = R(D.c1h[k]) * muf.ld(i, j, 0) + R(D.c2h[k]);
+  const R a = R(0.5) * (D.alt.ld(i - DI, j - DJ, k) + D.alt.ld(i, j, k));
   return G * G * R(D.rdnw[k]) / mu / a * (vflux_uv<R, DI, DJ>(D, f, ub, kv, i, j, k) - vflux_uv<R, DI, DJ>(D, f, ub, kv, i, j, k - 1));
 }
 

@@ -27,13 +27,16 @@ __device__ __forceinline__ R mf_(const Dom<R>& D, int k, R m) { return R(D.c1f[k
 
 // p_rho_point (small_step.cpp:97-112): calc_p_rho, with smdiv divergence damping when damp.
 // The mixed form evaluates it in double (the hydrostatic p'' / al'' relation).
-template <class R>
+// RO: alt, t_save and c2a are read-only in the calling kernel (the read-only load path)
+template <bool RO, class R>
 __device__ __forceinline__ void p_rho_point(const Dom<R>& D, int i, int j, int k, bool damp) {
   using A = double;
   // every load before the first store
   const A c1h = D.c1h[k];
-  const A muts = A(D.muts(i, j, 0)), alt = A(D.alt(i, j, k)), mu = A(D.mu2(i, j, 0)), ts = A(D.t_save(i, j, k));
-  const A ph_kp = A(D.ph2(i, j, k + 1)), ph_k = A(D.ph2(i, j, k)), t2 = A(D.t2(i, j, k)), c2a = A(D.c2a(i, j, k));
+  const A muts = A(D.muts(i, j, 0)), alt = A(RO ? D.alt.ld(i, j, k) : D.alt(i, j, k)), mu = A(D.mu2(i, j, 0));
+  const A ts = A(RO ? D.t_save.ld(i, j, k) : D.t_save(i, j, k));
+  const A ph_kp = A(D.ph2(i, j, k + 1)), ph_k = A(D.ph2(i, j, k)), t2 = A(D.t2(i, j, k));
+  const A c2a = A(RO ? D.c2a.ld(i, j, k) : D.c2a(i, j, k));
   const A pm1 = damp ? A(D.pm1(i, j, k)) : A(0);
   const A m = c1h * muts + A(D.c2h[k]);
   const A a = -((1. / m) * (alt * (c1h * mu) + A(D.rdnw[k]) * (ph_kp - ph_k)));
@@ -52,7 +55,7 @@ __device__ __forceinline__ void p_rho_point(const Dom<R>& D, int i, int j, int k
 // advance_uv (KUV :151-190): the faces i, j of cells i, j
 template <class R, int DI, int DJ>
 __device__ __forceinline__ R uv_dpn(const Dom<R>& D, int i, int j, int k) {
-  auto ps = [&](int kk) { return D.p(i, j, kk) + D.p(i - DI, j - DJ, kk); };
+  auto ps = [&](int kk) { return D.p.ld(i, j, kk) + D.p.ld(i - DI, j - DJ, kk); };
   const int nz = D.nz;
   if (k == 0) return R(0.5) * (R(D.cf1) * ps(0) + R(D.cf2) * ps(1) + R(D.cf3) * ps(2));
   if (k == nz) return D.top_lid ? R(0.5) * (R(D.cf1) * ps(nz - 1) + R(D.cf2) * ps(nz - 2) + R(D.cf3) * ps(nz - 3)) : R(0);
@@ -62,12 +65,12 @@ template <class R, int DI, int DJ>
 __device__ __forceinline__ R uv_dp(const Dom<R>& D, int i, int j, int k, R mface, R rd, R rm) {
   const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
   R d = rm * R(0.5) * rd * (c1h * mface + c2h) *
-        (((D.ph2(i, j, k + 1) - D.ph2(i - DI, j - DJ, k + 1)) + (D.ph2(i, j, k) - D.ph2(i - DI, j - DJ, k))) +
-         (D.alt(i, j, k) + D.alt(i - DI, j - DJ, k)) * (D.p(i, j, k) - D.p(i - DI, j - DJ, k)) +
-         (D.al(i, j, k) + D.al(i - DI, j - DJ, k)) * (D.pb(i, j, k) - D.pb(i - DI, j - DJ, k)));
-  d += rm * rd * (D.php(i, j, k) - D.php(i - DI, j - DJ, k)) *
+        (((D.ph2.ld(i, j, k + 1) - D.ph2.ld(i - DI, j - DJ, k + 1)) + (D.ph2.ld(i, j, k) - D.ph2.ld(i - DI, j - DJ, k))) +
+         (D.alt.ld(i, j, k) + D.alt.ld(i - DI, j - DJ, k)) * (D.p.ld(i, j, k) - D.p.ld(i - DI, j - DJ, k)) +
+         (D.al.ld(i, j, k) + D.al.ld(i - DI, j - DJ, k)) * (D.pb(i, j, k) - D.pb(i - DI, j - DJ, k)));
+  d += rm * rd * (D.php.ld(i, j, k) - D.php.ld(i - DI, j - DJ, k)) *
        (R(D.rdnw[k]) * (uv_dpn<R, DI, DJ>(D, i, j, k + 1) - uv_dpn<R, DI, DJ>(D, i, j, k)) -
-        R(0.5) * (c1h * D.mu2(i - DI, j - DJ, 0) + c1h * D.mu2(i, j, 0)));
+        R(0.5) * (c1h * D.mu2.ld(i - DI, j - DJ, 0) + c1h * D.mu2.ld(i, j, 0)));
   return d;
 }
 // over the staggered index range; with lateral boundaries the spec zone's faces take
@@ -86,11 +89,11 @@ __global__ void __launch_bounds__(PX) k_uv(const __grid_constant__ Pack<R, NM> P
   if (D.lbc) {
     int sl, pos;
     if (spec_at(ring_for(D.nx, D.ny, 'u'), i, j, sl, pos)) {
-      un = D.u2(i, j, k) + dts * D.ru_tend(i, j, k);
+      un = D.u2(i, j, k) + dts * D.ru_tend.ld(i, j, k);
       su = true;
     }
     if (spec_at(ring_for(D.nx, D.ny, 'v'), i, j, sl, pos)) {
-      vn = D.v2(i, j, k) + dts * D.rv_tend(i, j, k);
+      vn = D.v2(i, j, k) + dts * D.rv_tend.ld(i, j, k);
       sv = true;
     }
   }
@@ -100,16 +103,16 @@ __global__ void __launch_bounds__(PX) k_uv(const __grid_constant__ Pack<R, NM> P
     const R emdx = R(D.emdiv) * (R(1.) / R(D.rdx)), emdy = D.do_y ? R(D.emdiv) * (R(1.) / R(D.rdy)) : R(0);
     const R c1h = R(D.c1h[k]);
     if (i >= ui0 && i < ui1 && !edge_uface(D, i, j)) {
-      const R mudf_x = -emdx * (D.mudf(i, j, 0) - D.mudf(i - 1, j, 0)) / D.msfuy(i, j);
-      un = D.u2(i, j, k) + dts * D.ru_tend(i, j, k) -
-           dts * cqu_(D, i, j, k) * uv_dp<R, 1, 0>(D, i, j, k, D.muu(i, j, 0), R(D.rdx), D.msfux(i, j) / D.msfuy(i, j)) +
+      const R mudf_x = -emdx * (D.mudf.ld(i, j, 0) - D.mudf.ld(i - 1, j, 0)) / D.msfuy(i, j);
+      un = D.u2(i, j, k) + dts * D.ru_tend.ld(i, j, k) -
+           dts * cqu_(D, i, j, k) * uv_dp<R, 1, 0>(D, i, j, k, D.muu.ld(i, j, 0), R(D.rdx), D.msfux(i, j) / D.msfuy(i, j)) +
            c1h * mudf_x;
       su = true;
     }
     if (D.do_y && j >= vj0 && j < vj1 && !edge_vface(D, i, j)) {
-      const R mudf_y = -emdy * (D.mudf(i, j, 0) - D.mudf(i, j - 1, 0)) * D.msfvx_inv(i, j);
-      vn = D.v2(i, j, k) + dts * D.rv_tend(i, j, k) -
-           dts * cqv_(D, i, j, k) * uv_dp<R, 0, 1>(D, i, j, k, D.muv(i, j, 0), R(D.rdy), D.msfvy(i, j) / D.msfvx(i, j)) +
+      const R mudf_y = -emdy * (D.mudf.ld(i, j, 0) - D.mudf.ld(i, j - 1, 0)) * D.msfvx_inv(i, j);
+      vn = D.v2(i, j, k) + dts * D.rv_tend.ld(i, j, k) -
+           dts * cqv_(D, i, j, k) * uv_dp<R, 0, 1>(D, i, j, k, D.muv.ld(i, j, 0), R(D.rdy), D.msfvy(i, j) / D.msfvx(i, j)) +
            c1h * mudf_y;
       sv = true;
     }
@@ -118,16 +121,17 @@ __global__ void __launch_bounds__(PX) k_uv(const __grid_constant__ Pack<R, NM> P
   if (sv) D.v2(i, j, k) = vn;
 }
 
-// KMuTDiv (:194-206): the mass divergence of level k of column (i, j)
+// KMuTDiv (:194-206): the mass divergence of level k of column (i, j) (k_ac, where u, v, their saves
+// and the face masses are read-only)
 template <class R>
 __device__ __forceinline__ R mut_dv(const Dom<R>& D, int i, int j, int k) {
   const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
-  const R fx = (D.u2(i + 1, j, k) + (c1h * D.muu(i + 1, j, 0) + c2h) * D.u_save(i + 1, j, k) / D.msfuy(i + 1, j)) -
-               (D.u2(i, j, k) + (c1h * D.muu(i, j, 0) + c2h) * D.u_save(i, j, k) / D.msfuy(i, j));
+  const R fx = (D.u2.ld(i + 1, j, k) + (c1h * D.muu.ld(i + 1, j, 0) + c2h) * D.u_save.ld(i + 1, j, k) / D.msfuy(i + 1, j)) -
+               (D.u2.ld(i, j, k) + (c1h * D.muu.ld(i, j, 0) + c2h) * D.u_save.ld(i, j, k) / D.msfuy(i, j));
   R d = R(D.rdx) * fx;
   if (D.do_y)
-    d += R(D.rdy) * ((D.v2(i, j + 1, k) + (c1h * D.muv(i, j + 1, 0) + c2h) * D.v_save(i, j + 1, k) * D.msfvx_inv(i, j + 1)) -
-                     (D.v2(i, j, k) + (c1h * D.muv(i, j, 0) + c2h) * D.v_save(i, j, k) * D.msfvx_inv(i, j)));
+    d += R(D.rdy) * ((D.v2.ld(i, j + 1, k) + (c1h * D.muv.ld(i, j + 1, 0) + c2h) * D.v_save.ld(i, j + 1, k) * D.msfvx_inv(i, j + 1)) -
+                     (D.v2.ld(i, j, k) + (c1h * D.muv.ld(i, j, 0) + c2h) * D.v_save.ld(i, j, k) * D.msfvx_inv(i, j)));
   return D.msftx(i, j) * D.msfty(i, j) * d;
 }
 

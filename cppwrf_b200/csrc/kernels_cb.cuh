@@ -47,18 +47,18 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ls_prep(const __grid_constant__
   double* s_div = cb_array(0, nz);
   R muu = 0, muv = 0, mut = 0;
   if (col) {
-    if (i < nx && j < ny) mut = D.mu2(i, j, 0) + D.mub(i, j);
+    if (i < nx && j < ny) mut = D.mu2.ld(i, j, 0) + D.mub(i, j);
     if (j < ny) {
-      if (spx && i == 0) muu = R(0.5) * (D.mu2(0, j, 0) + D.mu2(0, j, 0) + D.mub(0, j) + D.mub(0, j));
+      if (spx && i == 0) muu = R(0.5) * (D.mu2.ld(0, j, 0) + D.mu2.ld(0, j, 0) + D.mub(0, j) + D.mub(0, j));
       else if (spx && i == nx)
-        muu = R(0.5) * (D.mu2(nx - 1, j, 0) + D.mu2(nx - 1, j, 0) + D.mub(nx - 1, j) + D.mub(nx - 1, j));
-      else muu = R(0.5) * (D.mu2(i, j, 0) + D.mu2(i - 1, j, 0) + D.mub(i, j) + D.mub(i - 1, j));
+        muu = R(0.5) * (D.mu2.ld(nx - 1, j, 0) + D.mu2.ld(nx - 1, j, 0) + D.mub(nx - 1, j) + D.mub(nx - 1, j));
+      else muu = R(0.5) * (D.mu2.ld(i, j, 0) + D.mu2.ld(i - 1, j, 0) + D.mub(i, j) + D.mub(i - 1, j));
     }
     if (i < nx && j < nyv) {
-      if (spy && j == 0) muv = R(0.5) * (D.mu2(i, 0, 0) + D.mu2(i, 0, 0) + D.mub(i, 0) + D.mub(i, 0));
+      if (spy && j == 0) muv = R(0.5) * (D.mu2.ld(i, 0, 0) + D.mu2.ld(i, 0, 0) + D.mub(i, 0) + D.mub(i, 0));
       else if (spy && j == ny)
-        muv = R(0.5) * (D.mu2(i, ny - 1, 0) + D.mu2(i, ny - 1, 0) + D.mub(i, ny - 1) + D.mub(i, ny - 1));
-      else muv = R(0.5) * (D.mu2(i, j, 0) + D.mu2(i, j - 1, 0) + D.mub(i, j) + D.mub(i, j - 1));
+        muv = R(0.5) * (D.mu2.ld(i, ny - 1, 0) + D.mu2.ld(i, ny - 1, 0) + D.mub(i, ny - 1) + D.mub(i, ny - 1));
+      else muv = R(0.5) * (D.mu2.ld(i, j, 0) + D.mu2.ld(i, j - 1, 0) + D.mub(i, j) + D.mub(i, j - 1));
     }
     if (w0) {
       if (i < nx && j < ny) D.mut(i, j, 0) = mut;
@@ -68,17 +68,17 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ls_prep(const __grid_constant__
     CB_LOOP(k, nz + 1) {  // KPrep3 (every load of a level before its first store)
       const bool has_u = j < ny && k < nz, has_v = i < nx && j < nyv && k < nz, has_w = i < nx && j < ny;
       const bool has_m = has_w && k < nz;
-      const R u2 = has_u ? D.u2(i, j, k) : R(0), msfuy = has_u ? D.msfuy(i, j) : R(1);
-      const R v2 = has_v ? D.v2(i, j, k) : R(0), mvxi = has_v ? D.msfvx_inv(i, j) : R(0);
-      const R w2 = has_w ? D.w2(i, j, k) : R(0), msfty = has_w ? D.msfty(i, j) : R(1);
+      const R u2 = has_u ? D.u2.ld(i, j, k) : R(0), msfuy = has_u ? D.msfuy(i, j) : R(1);
+      const R v2 = has_v ? D.v2.ld(i, j, k) : R(0), mvxi = has_v ? D.msfvx_inv(i, j) : R(0);
+      const R w2 = has_w ? D.w2.ld(i, j, k) : R(0), msfty = has_w ? D.msfty(i, j) : R(1);
       R al = 0, alb = 0, phb0 = 0, phb1 = 0, ph0 = 0, ph1 = 0;
       if (has_m) {
-        al = D.al(i, j, k);
+        al = D.al.ld(i, j, k);
         alb = D.alb(i, j, k);
         phb0 = D.phb(i, j, k);
         phb1 = D.phb(i, j, k + 1);
-        ph0 = D.ph2(i, j, k);
-        ph1 = D.ph2(i, j, k + 1);
+        ph0 = D.ph2.ld(i, j, k);
+        ph1 = D.ph2.ld(i, j, k + 1);
       }
       if (has_u) D.ru(i, j, k) = u2 * (R(D.c1h[k]) * muu + R(D.c2h[k])) / msfuy;
       if (has_v) D.rv(i, j, k) = v2 * (R(D.c1h[k]) * muv + R(D.c2h[k])) * mvxi;
@@ -141,15 +141,15 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ss_prep(const __grid_constant__
   const bool first = rk == 1;
   R mts = 0, mus_u = 0, mus_v = 0, mut = 0;
   if (col) {
-    mts = D.mub(i, j) + D.mu1(i, j, 0);
-    mus_u = first ? D.muu(i, j, 0) : R(0.5) * (mts + D.mub(i - 1, j) + D.mu1(i - 1, j, 0));
-    mus_v = first ? D.muv(i, j, 0) : R(0.5) * (mts + D.mub(i, j - 1) + D.mu1(i, j - 1, 0));
-    if (mass) mut = D.mut(i, j, 0);
+    mts = D.mub(i, j) + D.mu1.ld(i, j, 0);
+    mus_u = first ? D.muu.ld(i, j, 0) : R(0.5) * (mts + D.mub(i - 1, j) + D.mu1.ld(i - 1, j, 0));
+    mus_v = first ? D.muv.ld(i, j, 0) : R(0.5) * (mts + D.mub(i, j - 1) + D.mu1.ld(i, j - 1, 0));
+    if (mass) mut = D.mut.ld(i, j, 0);
     if (w0) {
       if (mass) {
         D.muts(i, j, 0) = mts;
         D.mu_save(i, j, 0) = D.mu2(i, j, 0);
-        D.mu2(i, j, 0) = D.mu1(i, j, 0) - D.mu2(i, j, 0);
+        D.mu2(i, j, 0) = D.mu1.ld(i, j, 0) - D.mu2(i, j, 0);
       }
       if (j < ny) D.muus(i, j, 0) = mus_u;
       if (i < nx && j < nyv) D.muvs(i, j, 0) = mus_v;
@@ -160,31 +160,31 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ss_prep(const __grid_constant__
       R ui = 0, u1 = 0, muu = 0, msfuy = 1, vi = 0, v1 = 0, muv = 0, mvxi = 0;
       if (has_u) {
         ui = D.u2(i, j, k);
-        u1 = D.u1(i, j, k);
-        muu = D.muu(i, j, 0);
+        u1 = D.u1.ld(i, j, k);
+        muu = D.muu.ld(i, j, 0);
         msfuy = D.msfuy(i, j);
       }
       if (has_v) {
         vi = D.v2(i, j, k);
-        v1 = D.v1(i, j, k);
-        muv = D.muv(i, j, 0);
+        v1 = D.v1.ld(i, j, k);
+        muv = D.muv.ld(i, j, 0);
         mvxi = D.msfvx_inv(i, j);
       }
       R ti = 0, t1 = 0, pb = 0, pp = 0, alt = 1, wi = 0, w1 = 0, msfty = 1, phi = 0, ph1 = 0, ww = 0;
       if (mass) {
         if (k < nz) {
           ti = D.t2(i, j, k);
-          t1 = D.t1(i, j, k);
+          t1 = D.t1.ld(i, j, k);
           pb = D.pb(i, j, k);
           pp = D.p(i, j, k);
-          alt = D.alt(i, j, k);
+          alt = D.alt.ld(i, j, k);
         }
         wi = D.w2(i, j, k);
-        w1 = D.w1(i, j, k);
+        w1 = D.w1.ld(i, j, k);
         msfty = D.msfty(i, j);
         phi = D.ph2(i, j, k);
-        ph1 = D.ph1(i, j, k);
-        ww = (k == 0 || k == nz) ? R(0) : D.ww(i, j, k);
+        ph1 = D.ph1.ld(i, j, k);
+        ww = (k == 0 || k == nz) ? R(0) : D.ww.ld(i, j, k);
       }
       if (has_u) {
         D.u_save(i, j, k) = ui;
@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ss_prep(const __grid_constant__
   auto mf = [&](int kk, A mm) { return D.c1f[kk] * mm + D.c2f[kk]; };
   auto cq1 = [&](int kk) { return A(R(1) / (R(1) + cqw_(D, i, j, kk))); };
   if (mass) {
-    CB_LOOP(k, nz) p_rho_point(D, i, j, k, false);
+    CB_LOOP(k, nz) p_rho_point<false>(D, i, j, k, false);
     // calc_coef_w: the pointwise coefficients a, b, c of each level
     CB_LOOP(k, nz + 1) {
       A a = 0, b = 0, cc = 0;
@@ -292,24 +292,24 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
   if (phase & 1) {
     if (col && D.spec_x && i == nx && j < ny)  // KSumEdge, east face
       CB_LOOP(k, nz) {
-        const R su = (first ? R(0) : D.ru_m(i, j, k)) + D.u2(i, j, k);
-        const R cpl = (R(D.c1h[k]) * D.muu(i, j, 0) + R(D.c2h[k])) * D.u_save(i, j, k);
+        const R su = (first ? R(0) : D.ru_m(i, j, k)) + D.u2.ld(i, j, k);
+        const R cpl = (R(D.c1h[k]) * D.muu.ld(i, j, 0) + R(D.c2h[k])) * D.u_save.ld(i, j, k);
         D.ru_m(i, j, k) = last ? su / rn + cpl / D.msfuy(i, j) : su;
       }
     if (col && D.spec_y && j == ny && i < nx)  // KSumEdge, north face
       CB_LOOP(k, nz) {
-        const R su = (first ? R(0) : D.rv_m(i, j, k)) + D.v2(i, j, k);
-        const R cpl = (R(D.c1h[k]) * D.muv(i, j, 0) + R(D.c2h[k])) * D.v_save(i, j, k);
+        const R su = (first ? R(0) : D.rv_m(i, j, k)) + D.v2.ld(i, j, k);
+        const R cpl = (R(D.c1h[k]) * D.muv.ld(i, j, 0) + R(D.c2h[k])) * D.v_save.ld(i, j, k);
         D.rv_m(i, j, k) = last ? su / rn + cpl * D.msfvx_inv(i, j) : su;
       }
     if (spec) {  // spec zone: sumflux of ww only; mu and mu_ts take dts mu_tend (LateralBC::update_mu_t :363-372)
       CB_LOOP(k, nz + 1) {
         const R sw = (first ? R(0) : D.ww_m(i, j, k)) + D.ww(i, j, k);
-        D.ww_m(i, j, k) = last ? sw / rn + D.ww1(i, j, k) : sw;
+        D.ww_m(i, j, k) = last ? sw / rn + D.ww1.ld(i, j, k) : sw;
       }
       if (w0) {
-        D.mu2(i, j, 0) += dts * D.mu_tend(i, j, 0);
-        D.muts(i, j, 0) += dts * D.mu_tend(i, j, 0);
+        D.mu2(i, j, 0) += dts * D.mu_tend.ld(i, j, 0);
+        D.muts(i, j, 0) += dts * D.mu_tend.ld(i, j, 0);
       }
     }
     if (dyn) CB_LOOP_SH(k, nz) s0[k * CX + lane] = A(mut_dv(D, i, j, k));  // dv of each level
@@ -317,12 +317,12 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
     if (dyn && w0) {  // the column mass tendency: sum over k in order
       A dmdt = 0;
       for (int k = 0; k < nz; ++k) dmdt += D.dnw[k] * s0[k * CX + lane];
-      const A mtend = A(D.mu_tend(i, j, 0));
+      const A mtend = A(D.mu_tend.ld(i, j, 0));
       const A mu_old = A(D.mu2(i, j, 0));
       const A mu_new = mu_old + A(dts) * (dmdt + mtend);
       D.mu2(i, j, 0) = R(mu_new);
       D.mudf(i, j, 0) = R(dmdt + mtend);
-      D.muts(i, j, 0) = D.mut(i, j, 0) + R(mu_new);
+      D.muts(i, j, 0) = D.mut.ld(i, j, 0) + R(mu_new);
       D.muave(i, j, 0) = R(0.5) * ((R(1) + epssm) * R(mu_new) + (R(1) - epssm) * R(mu_old));
       sc[0 * CX + lane] = dmdt;
       sc[1 * CX + lane] = mtend;
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
       const A msfty = A(D.msfty(i, j));
       CB_LOOP_SH(k, nz - 1) {
         s1[k * CX + lane] = D.dnw[k] * (D.c1h[k] * dmdt + s0[k * CX + lane] + D.c1h[k] * mtend) / msfty;
-        s0[k * CX + lane] = A(D.ww1(i, j, k + 1));
+        s0[k * CX + lane] = A(D.ww1.ld(i, j, k + 1));
       }
     }
     __syncthreads();
@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
     if (dyn) {
       CB_LOOP(k, nz + 1) {  // ww'' and its time sum
         const R wpp = R(s2[k * CX + lane]);
-        const R wwm = first ? R(0) : D.ww_m(i, j, k), ww1 = D.ww1(i, j, k);
+        const R wwm = first ? R(0) : D.ww_m(i, j, k), ww1 = D.ww1.ld(i, j, k);
         const R sw = wwm + (k == 0 ? R(0) : wpp);
         D.ww(i, j, k) = wpp;
         D.ww_m(i, j, k) = last ? sw / rn + ww1 : sw;
@@ -359,29 +359,29 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
     if (mass) {
       CB_LOOP(k, nz) {  // KMuTPoint: time sums of ru, rv; theta'' (every load issued before the first store)
         const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
-        const R u_k = D.u2(i, j, k), rum = first ? R(0) : D.ru_m(i, j, k), usv = D.u_save(i, j, k);
-        const R muu = D.muu(i, j, 0), msfuy = D.msfuy(i, j);
+        const R u_k = D.u2.ld(i, j, k), rum = first ? R(0) : D.ru_m(i, j, k), usv = D.u_save.ld(i, j, k);
+        const R muu = D.muu.ld(i, j, 0), msfuy = D.msfuy(i, j);
         R v_k = 0, rvm = 0, vsv = 0, muv = 0, mvxi = 0;
         if (D.do_y) {
-          v_k = D.v2(i, j, k);
+          v_k = D.v2.ld(i, j, k);
           rvm = first ? R(0) : D.rv_m(i, j, k);
-          vsv = D.v_save(i, j, k);
-          muv = D.muv(i, j, 0);
+          vsv = D.v_save.ld(i, j, k);
+          muv = D.muv.ld(i, j, 0);
           mvxi = D.msfvx_inv(i, j);
         }
-        const R tk = D.t2(i, j, k), ttend = D.t_tend(i, j, k);
+        const R tk = D.t2(i, j, k), ttend = D.t_tend.ld(i, j, k);
         R tnew;
         if (spec) {  // theta'' of the spec zone (update_mu_t)
           tnew = tk + dts * ttend;
         } else {
-          const R u_ip = D.u2(i + 1, j, k), ts = D.t_save(i, j, k), ts_ip = D.t_save(i + 1, j, k), ts_im = D.t_save(i - 1, j, k);
+          const R u_ip = D.u2.ld(i + 1, j, k), ts = D.t_save.ld(i, j, k), ts_ip = D.t_save.ld(i + 1, j, k), ts_im = D.t_save.ld(i - 1, j, k);
           R v_jp = 0, ts_jp = 0, ts_jm = 0;
           if (D.do_y) {
-            v_jp = D.v2(i, j + 1, k);
-            ts_jp = D.t_save(i, j + 1, k);
-            ts_jm = D.t_save(i, j - 1, k);
+            v_jp = D.v2.ld(i, j + 1, k);
+            ts_jp = D.t_save.ld(i, j + 1, k);
+            ts_jm = D.t_save.ld(i, j - 1, k);
           }
-          const R ts_kp = k + 1 < nz ? D.t_save(i, j, k + 1) : R(0), ts_km = k >= 1 ? D.t_save(i, j, k - 1) : R(0);
+          const R ts_kp = k + 1 < nz ? D.t_save.ld(i, j, k + 1) : R(0), ts_km = k >= 1 ? D.t_save.ld(i, j, k - 1) : R(0);
           const R msfty = D.msfty(i, j), msftx = D.msftx(i, j);
           R hflux = R(0.5) * R(D.rdx) * (u_ip * (ts_ip + ts) - u_k * (ts + ts_im));
           if (D.do_y) hflux += R(0.5) * R(D.rdy) * (v_jp * (ts_jp + ts) - v_k * (ts + ts_jm));
@@ -409,14 +409,14 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
     double* s_al = cb_array(4, nz);
     double* s_ga = cb_array(5, nz);
     if (spec) {  // phi'' of the spec zone (LateralBC::update_ph_w, KUpdatePh :374-386)
-      const R mts = D.muts(i, j, 0), mold = mts - dts * D.mu_tend(i, j, 0);
+      const R mts = D.muts(i, j, 0), mold = mts - dts * D.mu_tend.ld(i, j, 0);
       CB_LOOP(k, nz + 1) {
         const R m_old = R(D.c1f[k]) * mold + R(D.c2f[k]), m_new = R(D.c1f[k]) * mts + R(D.c2f[k]);
-        D.ph2(i, j, k) = D.ph2(i, j, k) * m_old / m_new + dts * D.ph_tend(i, j, k) / m_new + D.ph_save(i, j, k) * (m_old / m_new - R(1));
+        D.ph2(i, j, k) = D.ph2(i, j, k) * m_old / m_new + dts * D.ph_tend.ld(i, j, k) / m_new + D.ph_save.ld(i, j, k) * (m_old / m_new - R(1));
       }
     }
     if (dyn) {
-      mut = D.mut(i, j, 0);
+      mut = D.mut.ld(i, j, 0);
       muts = D.muts(i, j, 0);
       mav = D.muave(i, j, 0);
       msfty = D.msfty(i, j);
@@ -425,11 +425,11 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
         if (k == 0 || (D.top_lid && k == nz)) {
           r = 0;
         } else {
-          R rr = dts * (D.ph_tend(i, j, k) + R(0.5) * R(k::g) * (R(1) - epssm) * D.w2(i, j, k));
+          R rr = dts * (D.ph_tend.ld(i, j, k) + R(0.5) * R(k::g) * (R(1) - epssm) * D.w2(i, j, k));
           if (k < nz) {
             auto wdwn = [&](int mm) {
               return R(0.5) * (D.ww(i, j, mm) + D.ww(i, j, mm - 1)) * R(D.rdnw[mm - 1]) *
-                     (D.ph_save(i, j, mm) - D.ph_save(i, j, mm - 1) + D.phb(i, j, mm) - D.phb(i, j, mm - 1));
+                     (D.ph_save.ld(i, j, mm) - D.ph_save.ld(i, j, mm - 1) + D.phb(i, j, mm) - D.phb(i, j, mm - 1));
             };
             rr -= dts * (R(D.fnm[k]) * wdwn(k + 1) + R(D.fnp[k]) * wdwn(k));
           }
@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
         s0[k * CX + lane] = A(r);
         if (k < nz) {
           const R tav = R(0.5) * ((R(1) + epssm) * D.t2(i, j, k) + (R(1) - epssm) * R(s_t2s[k * CX + lane]));
-          s1[k * CX + lane] = A((tav + R(D.c1h[k]) * mav * R(k::t0)) / (mh_(D, k, muts) * (R(k::t0) + D.t_save(i, j, k))));
+          s1[k * CX + lane] = A((tav + R(D.c1h[k]) * mav * R(k::t0)) / (mh_(D, k, muts) * (R(k::t0) + D.t_save.ld(i, j, k))));
         }
       }
     }
@@ -450,12 +450,12 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
         if (k == 0) {
           if (!D.flat) {
             R ws = D.msftx(i, j) * R(0.5) * R(D.rdx) *
-                   ((D.ht(i + 1, j) - D.ht(i, j)) * (R(D.cf1) * D.u2(i + 1, j, 0) + R(D.cf2) * D.u2(i + 1, j, 1) + R(D.cf3) * D.u2(i + 1, j, 2)) +
-                    (D.ht(i, j) - D.ht(i - 1, j)) * (R(D.cf1) * D.u2(i, j, 0) + R(D.cf2) * D.u2(i, j, 1) + R(D.cf3) * D.u2(i, j, 2)));
+                   ((D.ht(i + 1, j) - D.ht(i, j)) * (R(D.cf1) * D.u2.ld(i + 1, j, 0) + R(D.cf2) * D.u2.ld(i + 1, j, 1) + R(D.cf3) * D.u2.ld(i + 1, j, 2)) +
+                    (D.ht(i, j) - D.ht(i - 1, j)) * (R(D.cf1) * D.u2.ld(i, j, 0) + R(D.cf2) * D.u2.ld(i, j, 1) + R(D.cf3) * D.u2.ld(i, j, 2)));
             if (D.do_y)
               ws = msfty * R(0.5) * R(D.rdy) *
-                       ((D.ht(i, j + 1) - D.ht(i, j)) * (R(D.cf1) * D.v2(i, j + 1, 0) + R(D.cf2) * D.v2(i, j + 1, 1) + R(D.cf3) * D.v2(i, j + 1, 2)) +
-                        (D.ht(i, j) - D.ht(i, j - 1)) * (R(D.cf1) * D.v2(i, j, 0) + R(D.cf2) * D.v2(i, j, 1) + R(D.cf3) * D.v2(i, j, 2))) +
+                       ((D.ht(i, j + 1) - D.ht(i, j)) * (R(D.cf1) * D.v2.ld(i, j + 1, 0) + R(D.cf2) * D.v2.ld(i, j + 1, 1) + R(D.cf3) * D.v2.ld(i, j + 1, 2)) +
+                        (D.ht(i, j) - D.ht(i, j - 1)) * (R(D.cf1) * D.v2.ld(i, j, 0) + R(D.cf2) * D.v2.ld(i, j, 1) + R(D.cf3) * D.v2.ld(i, j, 2))) +
                    ws;
             wn = ws;
           } else {
@@ -467,29 +467,29 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
           if (k < nz) {
             const R r_kp1 = R(s0[(k + 1) * CX + lane]), ph_kp1 = D.ph2(i, j, k + 1);
             const R cq1 = R(1) / (R(1) + cqw_(D, i, j, k));
-            wn = D.w2(i, j, k) + dts * D.rw_tend(i, j, k) +
+            wn = D.w2(i, j, k) + dts * D.rw_tend.ld(i, j, k) +
                  msft_inv * cq1 *
                      (R(0.5) * dts * R(k::g) * R(D.rdn[k]) *
-                      (D.c2a(i, j, k) * R(D.rdnw[k]) / mh_(D, k, mut) * (ope * (r_kp1 - r_k) + ome * (ph_kp1 - ph_k)) -
-                       D.c2a(i, j, k - 1) * R(D.rdnw[k - 1]) / mh_(D, k - 1, mut) * (ope * (r_k - r_km1) + ome * (ph_k - ph_km1)))) +
+                      (D.c2a.ld(i, j, k) * R(D.rdnw[k]) / mh_(D, k, mut) * (ope * (r_kp1 - r_k) + ome * (ph_kp1 - ph_k)) -
+                       D.c2a.ld(i, j, k - 1) * R(D.rdnw[k - 1]) / mh_(D, k - 1, mut) * (ope * (r_k - r_km1) + ome * (ph_k - ph_km1)))) +
                  dts * R(k::g) * msft_inv *
-                     (R(D.rdn[k]) * (D.c2a(i, j, k) * D.alt(i, j, k) * R(s1[k * CX + lane]) -
-                                     D.c2a(i, j, k - 1) * D.alt(i, j, k - 1) * R(s1[(k - 1) * CX + lane])) -
+                     (R(D.rdn[k]) * (D.c2a.ld(i, j, k) * D.alt.ld(i, j, k) * R(s1[k * CX + lane]) -
+                                     D.c2a.ld(i, j, k - 1) * D.alt.ld(i, j, k - 1) * R(s1[(k - 1) * CX + lane])) -
                       R(D.c1f[k]) * mav);
           } else {
             const int km = nz - 1;
-            wn = D.w2(i, j, k) + dts * D.rw_tend(i, j, k) +
-                 msft_inv * (-R(0.5) * dts * R(k::g) / mh_(D, km, mut) * (R(D.rdnw[km]) * R(D.rdnw[km])) * R(2) * D.c2a(i, j, km) *
+            wn = D.w2(i, j, k) + dts * D.rw_tend.ld(i, j, k) +
+                 msft_inv * (-R(0.5) * dts * R(k::g) / mh_(D, km, mut) * (R(D.rdnw[km]) * R(D.rdnw[km])) * R(2) * D.c2a.ld(i, j, km) *
                                  (ope * (r_k - r_km1) + ome * (ph_k - ph_km1)) -
-                             dts * R(k::g) * (R(2) * R(D.rdnw[km]) * D.c2a(i, j, km) * D.alt(i, j, km) * R(s1[km * CX + lane]) +
+                             dts * R(k::g) * (R(2) * R(D.rdnw[km]) * D.c2a.ld(i, j, km) * D.alt.ld(i, j, km) * R(s1[km * CX + lane]) +
                                               R(D.c1f[k]) * mav));
             if (D.top_lid) wn = 0;
           }
         }
         s2[k * CX + lane] = A(wn);
-        s_a[k * CX + lane] = A(D.a(i, j, k));
-        s_al[k * CX + lane] = A(D.alpha(i, j, k));
-        s_ga[k * CX + lane] = A(D.gamma(i, j, k));
+        s_a[k * CX + lane] = A(D.a.ld(i, j, k));
+        s_al[k * CX + lane] = A(D.alpha.ld(i, j, k));
+        s_ga[k * CX + lane] = A(D.gamma.ld(i, j, k));
       }
     }
     __syncthreads();
@@ -516,7 +516,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
       }
     __syncthreads();
   }
-  if ((phase & 4) && mass) CB_LOOP(k, nz) p_rho_point(D, i, j, k, true);
+  if ((phase & 4) && mass) CB_LOOP(k, nz) p_rho_point<true>(D, i, j, k, true);
 }
 
 // small_step_finish (KFinish :419-444, KFinishMu :446-453) + calc_p_rho_phi (KPRhoPhi :456-477)
@@ -536,36 +536,36 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_finish(const __grid_constant__ 
       R u2 = 0, usv = 0, msfuy = 0, muu = 0, mts_u0 = 0, mts_u1 = 0;
       if (has_u) {
         u2 = D.u2(i, j, k);
-        usv = D.u_save(i, j, k);
+        usv = D.u_save.ld(i, j, k);
         msfuy = D.msfuy(i, j);
-        muu = D.muu(i, j, 0);
-        mts_u0 = D.muts(i, j, 0);
-        mts_u1 = D.muts(i - 1, j, 0);
+        muu = D.muu.ld(i, j, 0);
+        mts_u0 = D.muts.ld(i, j, 0);
+        mts_u1 = D.muts.ld(i - 1, j, 0);
       }
       R v2 = 0, vsv = 0, msfvx = 0, muv = 0, mts_v0 = 0, mts_v1 = 0;
       if (has_v) {
         v2 = D.v2(i, j, k);
-        vsv = D.v_save(i, j, k);
+        vsv = D.v_save.ld(i, j, k);
         msfvx = D.msfvx(i, j);
-        muv = D.muv(i, j, 0);
-        mts_v0 = D.muts(i, j, 0);
-        mts_v1 = D.muts(i, j - 1, 0);
+        muv = D.muv.ld(i, j, 0);
+        mts_v0 = D.muts.ld(i, j, 0);
+        mts_v1 = D.muts.ld(i, j - 1, 0);
       }
       R m = 0, mts = 0, w2 = 0, wsv = 0, msfty = 0, ph2 = 0, phsv = 0, ww = 0, ww1 = 0, t2 = 0, tsv = 0, hd = 0;
       if (mass) {
-        m = D.mut(i, j, 0);
-        mts = D.muts(i, j, 0);
+        m = D.mut.ld(i, j, 0);
+        mts = D.muts.ld(i, j, 0);
         w2 = D.w2(i, j, k);
-        wsv = D.w_save(i, j, k);
+        wsv = D.w_save.ld(i, j, k);
         msfty = D.msfty(i, j);
         ph2 = D.ph2(i, j, k);
-        phsv = D.ph_save(i, j, k);
+        phsv = D.ph_save.ld(i, j, k);
         ww = D.ww(i, j, k);
-        ww1 = D.ww1(i, j, k);
+        ww1 = D.ww1.ld(i, j, k);
         if (k < nz) {
           t2 = D.t2(i, j, k);
-          tsv = D.t_save(i, j, k);
-          if (hd_dt != R(0)) hd = D.hd(i, j, k);
+          tsv = D.t_save.ld(i, j, k);
+          if (hd_dt != R(0)) hd = D.hd.ld(i, j, k);
         }
       }
       if (has_u) {
@@ -586,8 +586,8 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_finish(const __grid_constant__ 
     }
     if (threadIdx.y == 0) {
       if (mass) D.mu2(i, j, 0) = D.mu2(i, j, 0) + D.mu_save(i, j, 0);
-      if (j < ny) D.muus(i, j, 0) = R(0.5) * (D.muts(i, j, 0) + D.muts(i - 1, j, 0));
-      if (i < nx && j < nyv) D.muvs(i, j, 0) = R(0.5) * (D.muts(i, j, 0) + D.muts(i, j - 1, 0));
+      if (j < ny) D.muus(i, j, 0) = R(0.5) * (D.muts.ld(i, j, 0) + D.muts.ld(i - 1, j, 0));
+      if (i < nx && j < nyv) D.muvs(i, j, 0) = R(0.5) * (D.muts.ld(i, j, 0) + D.muts.ld(i, j - 1, 0));
     }
   }
   __syncthreads();

@@ -6,6 +6,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from cppwrf_b200 import capi
 
@@ -109,3 +110,19 @@ def test_serve_create_without_gpu_fails_cleanly():
     assert cfg.hbm_budget_bytes == 150e9
     h = C.c_void_p()
     assert lib.cw_serve_create(C.byref(cfg), C.byref(h)) != 0
+
+
+@pytest.mark.parametrize("change,needle", [
+    (dict(bc_x=3), "open"), (dict(damp_opt=3), "damp_opt"), (dict(hypsometric_opt=2), "hypsometric"),
+    (dict(nz=130), "nz"), (dict(diff_opt=2), "diff_opt")])
+def test_unsupported_options_are_refused_with_a_reason(change, needle):
+    """Options outside the path are refused at cw_create with a message naming them (before any device work,
+    so this runs without a GPU)."""
+    lib = capi.load()
+    g = capi.grid(change.get("nx", 16), 12, change.get("nz", 10), 1000.0, 5.0, 10000.0,
+                  bc_x=change.get("bc_x", capi.PERIODIC), bc_y=capi.PERIODIC)
+    o = capi.default_options(lib, **{k: v for k, v in change.items() if k not in ("bc_x", "nz")})
+    h = C.c_void_p()
+    assert lib.cw_create(C.byref(g), C.byref(o), C.byref(h)) != 0
+    msg = lib.cw_last_error(None).decode()
+    assert needle in msg.lower(), msg
