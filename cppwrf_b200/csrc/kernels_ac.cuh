@@ -121,20 +121,6 @@ __global__ void __launch_bounds__(PX) k_uv(const __grid_constant__ Pack<R, NM> P
   if (sv) D.v2(i, j, k) = vn;
 }
 
-// KMuTDiv (:194-206): the mass divergence of level k of column (i, j) (k_ac, where u, v, their saves
-// and the face masses are read-only)
-template <class R>
-__device__ __forceinline__ R mut_dv(const Dom<R>& D, int i, int j, int k) {
-  const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
-  const R fx = (D.u2.ld(i + 1, j, k) + (c1h * D.muu.ld(i + 1, j, 0) + c2h) * D.u_save.ld(i + 1, j, k) / D.msfuy(i + 1, j)) -
-               (D.u2.ld(i, j, k) + (c1h * D.muu.ld(i, j, 0) + c2h) * D.u_save.ld(i, j, k) / D.msfuy(i, j));
-  R d = R(D.rdx) * fx;
-  if (D.do_y)
-    d += R(D.rdy) * ((D.v2.ld(i, j + 1, k) + (c1h * D.muv.ld(i, j + 1, 0) + c2h) * D.v_save.ld(i, j + 1, k) * D.msfvx_inv(i, j + 1)) -
-                     (D.v2.ld(i, j, k) + (c1h * D.muv.ld(i, j, 0) + c2h) * D.v_save.ld(i, j, k) * D.msfvx_inv(i, j)));
-  return D.msftx(i, j) * D.msfty(i, j) * d;
-}
-
 // calc_p_rho_phi, hypsometric_opt 1 (KPRhoPhi :456-477) at (i, j, k); pow = cw_pow
 template <class R>
 __device__ __forceinline__ void p_rho_phi_point(const Dom<R>& D, int i, int j, int k) {

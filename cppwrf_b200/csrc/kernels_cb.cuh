@@ -312,7 +312,43 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
         D.muts(i, j, 0) += dts * D.mu_tend.ld(i, j, 0);
       }
     }
-    if (dyn) CB_LOOP_SH(k, nz) s0[k * CX + lane] = A(mut_dv(D, i, j, k));  // dv of each level
+    if (mass)
+      CB_LOOP(k, nz) {  // dv of each level (KMuTDiv), the time sums of ru, rv (KMuTPoint), ww1 staged
+        const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
+        const R u_k = D.u2.ld(i, j, k), usv = D.u_save.ld(i, j, k), muu = D.muu.ld(i, j, 0), msfuy = D.msfuy(i, j);
+        const R rum = first ? R(0) : D.ru_m(i, j, k);
+        R v_k = 0, vsv = 0, muv = 0, mvxi = 0, rvm = 0;
+        if (D.do_y) {
+          v_k = D.v2.ld(i, j, k);
+          vsv = D.v_save.ld(i, j, k);
+          muv = D.muv.ld(i, j, 0);
+          mvxi = D.msfvx_inv(i, j);
+          rvm = first ? R(0) : D.rv_m(i, j, k);
+        }
+        if (dyn) {
+          const R u_ip = D.u2.ld(i + 1, j, k), usv_ip = D.u_save.ld(i + 1, j, k), muu_ip = D.muu.ld(i + 1, j, 0);
+          const R msfuy_ip = D.msfuy(i + 1, j);
+          R v_jp = 0, vsv_jp = 0, muv_jp = 0, mvxi_jp = 0;
+          if (D.do_y) {
+            v_jp = D.v2.ld(i, j + 1, k);
+            vsv_jp = D.v_save.ld(i, j + 1, k);
+            muv_jp = D.muv.ld(i, j + 1, 0);
+            mvxi_jp = D.msfvx_inv(i, j + 1);
+          }
+          if (k + 1 < nz) s2[(k + 1) * CX + lane] = A(D.ww1.ld(i, j, k + 1));
+          // KMuTDiv (small_step.cpp:194-206), the expression of mut_dv
+          const R fx = (u_ip + (c1h * muu_ip + c2h) * usv_ip / msfuy_ip) - (u_k + (c1h * muu + c2h) * usv / msfuy);
+          R d = R(D.rdx) * fx;
+          if (D.do_y) d += R(D.rdy) * ((v_jp + (c1h * muv_jp + c2h) * vsv_jp * mvxi_jp) - (v_k + (c1h * muv + c2h) * vsv * mvxi));
+          s0[k * CX + lane] = A(D.msftx(i, j) * D.msfty(i, j) * d);
+        }
+        const R su = rum + u_k;
+        D.ru_m(i, j, k) = last ? su / rn + (c1h * muu + c2h) * usv / msfuy : su;
+        if (D.do_y) {
+          const R sv = rvm + v_k;
+          D.rv_m(i, j, k) = last ? sv / rn + (c1h * muv + c2h) * vsv * mvxi : sv;
+        }
+      }
     __syncthreads();
     if (dyn && w0) {  // the column mass tendency: sum over k in order
       A dmdt = 0;
@@ -331,73 +367,62 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
     if (dyn) {  // the decrement of the omega integral at each level
       const A dmdt = sc[0 * CX + lane], mtend = sc[1 * CX + lane];
       const A msfty = A(D.msfty(i, j));
-      CB_LOOP_SH(k, nz - 1) {
-        s1[k * CX + lane] = D.dnw[k] * (D.c1h[k] * dmdt + s0[k * CX + lane] + D.c1h[k] * mtend) / msfty;
-        s0[k * CX + lane] = A(D.ww1.ld(i, j, k + 1));
-      }
+      CB_LOOP_SH(k, nz - 1) s1[k * CX + lane] = D.dnw[k] * (D.c1h[k] * dmdt + s0[k * CX + lane] + D.c1h[k] * mtend) / msfty;
     }
     __syncthreads();
-    if (dyn && w0) {  // ww'' by the running integral
+    if (dyn && w0) {  // ww'' by the running integral (ww1 of level k + 1 staged in s2[k + 1])
       A ww_full = 0;
       s2[0 * CX + lane] = 0;
       for (int k = 0; k < nz - 1; ++k) {
         ww_full = ww_full - s1[k * CX + lane];
-        s2[(k + 1) * CX + lane] = A(R(ww_full - s0[k * CX + lane]));
+        s2[(k + 1) * CX + lane] = A(R(ww_full - s2[(k + 1) * CX + lane]));
       }
       s2[nz * CX + lane] = 0;
     }
     __syncthreads();
-    if (dyn) {
-      CB_LOOP(k, nz + 1) {  // ww'' and its time sum
-        const R wpp = R(s2[k * CX + lane]);
-        const R wwm = first ? R(0) : D.ww_m(i, j, k), ww1 = D.ww1.ld(i, j, k);
-        const R sw = wwm + (k == 0 ? R(0) : wpp);
-        D.ww(i, j, k) = wpp;
-        D.ww_m(i, j, k) = last ? sw / rn + ww1 : sw;
-      }
-    }
     if (mass) {
-      CB_LOOP(k, nz) {  // KMuTPoint: time sums of ru, rv; theta'' (every load issued before the first store)
-        const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
-        const R u_k = D.u2.ld(i, j, k), rum = first ? R(0) : D.ru_m(i, j, k), usv = D.u_save.ld(i, j, k);
-        const R muu = D.muu.ld(i, j, 0), msfuy = D.msfuy(i, j);
-        R v_k = 0, rvm = 0, vsv = 0, muv = 0, mvxi = 0;
-        if (D.do_y) {
-          v_k = D.v2.ld(i, j, k);
-          rvm = first ? R(0) : D.rv_m(i, j, k);
-          vsv = D.v_save.ld(i, j, k);
-          muv = D.muv.ld(i, j, 0);
-          mvxi = D.msfvx_inv(i, j);
+      CB_LOOP(k, nz + 1) {  // ww'' and its time sum; theta'' (KMuTPoint), every load before the first store
+        R wpp = 0, wwm = 0, ww1 = 0;
+        if (dyn) {
+          wpp = R(s2[k * CX + lane]);
+          wwm = first ? R(0) : D.ww_m(i, j, k);
+          ww1 = D.ww1.ld(i, j, k);
         }
-        const R tk = D.t2(i, j, k), ttend = D.t_tend.ld(i, j, k);
-        R tnew;
-        if (spec) {  // theta'' of the spec zone (update_mu_t)
-          tnew = tk + dts * ttend;
-        } else {
-          const R u_ip = D.u2.ld(i + 1, j, k), ts = D.t_save.ld(i, j, k), ts_ip = D.t_save.ld(i + 1, j, k), ts_im = D.t_save.ld(i - 1, j, k);
-          R v_jp = 0, ts_jp = 0, ts_jm = 0;
-          if (D.do_y) {
-            v_jp = D.v2.ld(i, j + 1, k);
-            ts_jp = D.t_save.ld(i, j + 1, k);
-            ts_jm = D.t_save.ld(i, j - 1, k);
+        R tk = 0, tnew = 0;
+        if (k < nz) {
+          tk = D.t2(i, j, k);
+          const R ttend = D.t_tend.ld(i, j, k);
+          if (spec) {  // theta'' of the spec zone (update_mu_t)
+            tnew = tk + dts * ttend;
+          } else {
+            const R u_k = D.u2.ld(i, j, k), u_ip = D.u2.ld(i + 1, j, k);
+            const R ts = D.t_save.ld(i, j, k), ts_ip = D.t_save.ld(i + 1, j, k), ts_im = D.t_save.ld(i - 1, j, k);
+            R v_k = 0, v_jp = 0, ts_jp = 0, ts_jm = 0;
+            if (D.do_y) {
+              v_k = D.v2.ld(i, j, k);
+              v_jp = D.v2.ld(i, j + 1, k);
+              ts_jp = D.t_save.ld(i, j + 1, k);
+              ts_jm = D.t_save.ld(i, j - 1, k);
+            }
+            const R ts_kp = k + 1 < nz ? D.t_save.ld(i, j, k + 1) : R(0), ts_km = k >= 1 ? D.t_save.ld(i, j, k - 1) : R(0);
+            const R msfty = D.msfty(i, j), msftx = D.msftx(i, j);
+            R hflux = R(0.5) * R(D.rdx) * (u_ip * (ts_ip + ts) - u_k * (ts + ts_im));
+            if (D.do_y) hflux += R(0.5) * R(D.rdy) * (v_jp * (ts_jp + ts) - v_k * (ts + ts_jm));
+            const R tn = tk + msfty * dts * ttend;
+            const R wd_kp = (k + 1 == nz) ? R(0) : R(s2[(k + 1) * CX + lane]) * (R(D.fnm[k + 1]) * ts_kp + R(D.fnp[k + 1]) * ts);
+            const R wd_k = (k == 0) ? R(0) : R(s2[k * CX + lane]) * (R(D.fnm[k]) * ts + R(D.fnp[k]) * ts_km);
+            tnew = tn - dts * msfty * (msftx * hflux + R(D.rdnw[k]) * (wd_kp - wd_k));
           }
-          const R ts_kp = k + 1 < nz ? D.t_save.ld(i, j, k + 1) : R(0), ts_km = k >= 1 ? D.t_save.ld(i, j, k - 1) : R(0);
-          const R msfty = D.msfty(i, j), msftx = D.msftx(i, j);
-          R hflux = R(0.5) * R(D.rdx) * (u_ip * (ts_ip + ts) - u_k * (ts + ts_im));
-          if (D.do_y) hflux += R(0.5) * R(D.rdy) * (v_jp * (ts_jp + ts) - v_k * (ts + ts_jm));
-          const R tn = tk + msfty * dts * ttend;
-          const R wd_kp = (k + 1 == nz) ? R(0) : R(s2[(k + 1) * CX + lane]) * (R(D.fnm[k + 1]) * ts_kp + R(D.fnp[k + 1]) * ts);
-          const R wd_k = (k == 0) ? R(0) : R(s2[k * CX + lane]) * (R(D.fnm[k]) * ts + R(D.fnp[k]) * ts_km);
-          tnew = tn - dts * msfty * (msftx * hflux + R(D.rdnw[k]) * (wd_kp - wd_k));
         }
-        const R su = rum + u_k;
-        D.ru_m(i, j, k) = last ? su / rn + (c1h * muu + c2h) * usv / msfuy : su;
-        if (D.do_y) {
-          const R sv = rvm + v_k;
-          D.rv_m(i, j, k) = last ? sv / rn + (c1h * muv + c2h) * vsv * mvxi : sv;
+        if (dyn) {
+          const R sw = wwm + (k == 0 ? R(0) : wpp);
+          D.ww(i, j, k) = wpp;
+          D.ww_m(i, j, k) = last ? sw / rn + ww1 : sw;
         }
-        s_t2s[k * CX + lane] = double(tk);  // t_2save: kept in shared memory for advance_w
-        D.t2(i, j, k) = tnew;
+        if (k < nz) {
+          s_t2s[k * CX + lane] = double(tk);  // t_2save: kept in shared memory for advance_w
+          D.t2(i, j, k) = tnew;
+        }
       }
     }
     __syncthreads();
