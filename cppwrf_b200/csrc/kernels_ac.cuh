@@ -27,15 +27,16 @@ __device__ __forceinline__ R mf_(const Dom<R>& D, int k, R m) { return R(D.c1f[k
 
 // p_rho_point (small_step.cpp:97-112): calc_p_rho, with smdiv divergence damping when damp.
 // The mixed form evaluates it in double (the hydrostatic p'' / al'' relation).
-// RO: alt, t_save and c2a are read-only in the calling kernel (the read-only load path)
+// RO: alt, t_save and c2a are read-only in the calling kernel (the read-only load path). ph_k, ph_kp: the
+// values of phi'' at levels k and k + 1.
 template <bool RO, class R>
-__device__ __forceinline__ void p_rho_point(const Dom<R>& D, int i, int j, int k, bool damp) {
+__device__ __forceinline__ void p_rho_point_ph(const Dom<R>& D, int i, int j, int k, bool damp, R ph_k_in, R ph_kp_in) {
   using A = double;
   // every load before the first store
   const A c1h = D.c1h[k];
   const A muts = A(D.muts(i, j, 0)), alt = A(RO ? D.alt.ld(i, j, k) : D.alt(i, j, k)), mu = A(D.mu2(i, j, 0));
   const A ts = A(RO ? D.t_save.ld(i, j, k) : D.t_save(i, j, k));
-  const A ph_kp = A(D.ph2(i, j, k + 1)), ph_k = A(D.ph2(i, j, k)), t2 = A(D.t2(i, j, k));
+  const A ph_kp = A(ph_kp_in), ph_k = A(ph_k_in), t2 = A(D.t2(i, j, k));
   const A c2a = A(RO ? D.c2a.ld(i, j, k) : D.c2a(i, j, k));
   const A pm1 = damp ? A(D.pm1(i, j, k)) : A(0);
   const A m = c1h * muts + A(D.c2h[k]);
@@ -50,6 +51,10 @@ __device__ __forceinline__ void p_rho_point(const Dom<R>& D, int i, int j, int k
     D.pm1(i, j, k) = R(pp);
   }
   D.p(i, j, k) = R(pp);
+}
+template <bool RO, class R>
+__device__ __forceinline__ void p_rho_point(const Dom<R>& D, int i, int j, int k, bool damp) {
+  p_rho_point_ph<RO>(D, i, j, k, damp, D.ph2(i, j, k), D.ph2(i, j, k + 1));
 }
 
 // advance_uv (KUV :151-190): the faces i, j of cells i, j

@@ -533,15 +533,28 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
       }
     }
     __syncthreads();
-    if (dyn)
-      CB_LOOP(k, nz + 1) {  // w'' and phi''
-        const R wk = R(s2[k * CX + lane]);
-        D.w2(i, j, k) = wk;
-        if (k >= 1) D.ph2(i, j, k) = R(s0[k * CX + lane]) + msfty * R(0.5) * dts * R(k::g) * ope * wk / mf_(D, k, muts);
+    // w'' and phi'' (dyn columns), then calc_p_rho of the level (every mass column, phase 4) from the new
+    // phi'' of levels k and k + 1: recomputed from the shared terms here (the same expression as the store),
+    // read back for the spec zone (written before the last barriers) and for the unchanged level 0
+    auto ph_new = [&](int m) { return R(s0[m * CX + lane]) + msfty * R(0.5) * dts * R(k::g) * ope * R(s2[m * CX + lane]) / mf_(D, m, muts); };
+    if (mass)
+      CB_LOOP(k, nz + 1) {
+        R wk = 0, phk = 0, phkp = 0;
+        if (dyn) {
+          wk = R(s2[k * CX + lane]);
+          phk = k >= 1 ? ph_new(k) : D.ph2(i, j, 0);
+          if (k < nz) phkp = ph_new(k + 1);
+        } else if (k < nz) {
+          phk = D.ph2(i, j, k);
+          phkp = D.ph2(i, j, k + 1);
+        }
+        if (dyn) {
+          D.w2(i, j, k) = wk;
+          if (k >= 1) D.ph2(i, j, k) = phk;
+        }
+        if ((phase & 4) && k < nz) p_rho_point_ph<true>(D, i, j, k, true, phk, phkp);
       }
-    __syncthreads();
   }
-  if ((phase & 4) && mass) CB_LOOP(k, nz) p_rho_point<true>(D, i, j, k, true);
 }
 
 // small_step_finish (KFinish :419-444, KFinishMu :446-453) + calc_p_rho_phi (KPRhoPhi :456-477)
