@@ -673,8 +673,15 @@ template <class R, int NM>
 void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
   const Member& M0 = h->m[0];
   bool lbc = false, terrain = false, scalars = false, any_pd = false;
+  // every member specified on all four sides: the acoustic substeps read no halo cell of the fields the
+  // per-substep fills (H_SS0, H_UV, H_AC) would refresh (the faces next to the boundary are the spec
+  // zone's, updated from the boundary data), and the fills after the substeps (H_POST, H_FIN) refresh them
+  // before anything reads them; those fills, and the spec zone's zero-gradient w of every substep but the
+  // last (overwritten by the next one, read only after the substeps), are left out
+  bool spec_all = true;
   int nq = 0;  // the most species of a member
   for (const Member& M : h->m) {
+    spec_all &= M.o.lbc != 0 && flat_x(M.g) && flat_y(M.g) && !two_d(M.g);
     nq = std::max(nq, M.o.n_scalars);
     lbc |= M.o.lbc != 0;
     terrain |= !M.o.flat;
@@ -697,13 +704,13 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
     L.run_t("k_tend", RG_STAG, 1, KV(k_tend), d, rk);
     if (rk == 1) L.copy_list(h->zeros_d, h->zeros_start_d, h->zeros.size(), h->zeros_total);
     L.run_cb("k_ss_prep", RG_COLS_STAG, 3, k_ss_prep<R, NM>, d, rk);
-    L.halo(cw_handle::H_SS0);
+    if (!spec_all) L.halo(cw_handle::H_SS0);
     for (int it = 1; it <= ns; ++it) {
       L.run_t("k_uv", RG_STAG, 1, KV(k_uv), d, rk);
-      L.halo(cw_handle::H_UV);
+      if (!spec_all) L.halo(cw_handle::H_UV);
       L.run_cb("k_ac", RG_COLS_STAG, kCbArrays, k_ac<R, NM>, d, rk, it, ns);
-      if (lbc) L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_ZERO_GRAD_W), rk);
-      L.halo(cw_handle::H_AC);
+      if (lbc && (!spec_all || it == ns)) L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_ZERO_GRAD_W), rk);
+      if (!spec_all) L.halo(cw_handle::H_AC);
     }
     L.halo(cw_handle::H_POST);
     L.run_cb("k_finish", RG_COLS_STAG, 0, k_finish<R, NM>, d, rk, ns);
