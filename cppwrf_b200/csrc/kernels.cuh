@@ -247,11 +247,11 @@ __device__ __forceinline__ R pgf_dpn(const Dom<R>& D, int i, int j, int k) {  //
   return R(0.5) * (R(D.fnm[k]) * ps(k) + R(D.fnp[k]) * ps(k - 1));
 }
 template <class R>
-__device__ R tend_u(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
+__device__ R tend_u(const Dom<R>& D, int i, int j, int k, bool use_tendf, R fx0, R fx1, R fy0, R fy1) {
   const R rdx = R(D.rdx), rdy = R(D.rdy);
   const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
-  R t = -(D.msfux(i, j) * rdx) * (tu_fx(D, i + 1, j, k) - tu_fx(D, i, j, k));
-  if (D.do_y) t -= (D.msfux(i, j) * rdy) * (tu_fy(D, i, j + 1, k) - tu_fy(D, i, j, k));
+  R t = -(D.msfux(i, j) * rdx) * (fx1 - fx0);
+  if (D.do_y) t -= (D.msfux(i, j) * rdy) * (fy1 - fy0);
   t -= R(D.rdnw[k]) * (tu_fz(D, i, j, k + 1) - tu_fz(D, i, j, k));
   const R rm = D.msfux(i, j) / D.msfuy(i, j);
   R dpx = rm * R(0.5) * rdx * (c1h * D.muu.ld(i, j, 0) + c2h) *
@@ -302,12 +302,12 @@ __device__ R tv_fz(const Dom<R>& D, int i, int j, int k) {
   return vel * flux3(D.v2.ld(i, j, k - 2), D.v2.ld(i, j, k - 1), D.v2.ld(i, j, k), D.v2.ld(i, j, k + 1), -vel, R(D.vup));
 }
 template <class R>
-__device__ R tend_v(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
+__device__ R tend_v(const Dom<R>& D, int i, int j, int k, bool use_tendf, R fx0, R fx1, R fy0, R fy1) {
   const R rdx = R(D.rdx), rdy = R(D.rdy);
   const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
   const R rm = D.msfvy(i, j) / D.msfvx(i, j);
-  R t = -(D.msfvy(i, j) * rdx) * (tv_fx(D, i + 1, j, k) - tv_fx(D, i, j, k));
-  t -= (D.msfvy(i, j) * rdy) * (tv_fy(D, i, j + 1, k) - tv_fy(D, i, j, k));
+  R t = -(D.msfvy(i, j) * rdx) * (fx1 - fx0);
+  t -= (D.msfvy(i, j) * rdy) * (fy1 - fy0);
   t -= rm * R(D.rdnw[k]) * (tv_fz(D, i, j, k + 1) - tv_fz(D, i, j, k));
   R dpy = rm * R(0.5) * rdy * (c1h * D.muv.ld(i, j, 0) + c2h) *
           ((D.ph2.ld(i, j, k + 1) - D.ph2.ld(i, j - 1, k + 1) + D.ph2.ld(i, j, k) - D.ph2.ld(i, j - 1, k)) +
@@ -362,11 +362,11 @@ __device__ R tw_fz(const Dom<R>& D, int i, int j, int m) {
   return vel * flux3(D.w2.ld(i, j, m - 1), D.w2.ld(i, j, m), D.w2.ld(i, j, m + 1), D.w2.ld(i, j, m + 2), -vel, R(D.vup));
 }
 template <class R>
-__device__ R tend_w(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
+__device__ R tend_w(const Dom<R>& D, int i, int j, int k, bool use_tendf, R fx0, R fx1, R fy0, R fy1) {
   const int nz = D.nz;
   const R rdx = R(D.rdx), rdy = R(D.rdy);
-  R t = -(D.msftx(i, j) * rdx) * (tw_fx(D, i + 1, j, k) - tw_fx(D, i, j, k));
-  if (D.do_y) t -= (D.msftx(i, j) * rdy) * (tw_fy(D, i, j + 1, k) - tw_fy(D, i, j, k));
+  R t = -(D.msftx(i, j) * rdx) * (fx1 - fx0);
+  if (D.do_y) t -= (D.msftx(i, j) * rdy) * (fy1 - fy0);
   const R rmsft = R(1) / D.msfty(i, j);
   if (k < nz) {
     t -= R(D.rdn[k]) * (tw_fz(D, i, j, k) - tw_fz(D, i, j, k - 1));
@@ -435,9 +435,9 @@ __device__ R sc_fz(const Dom<R>& D, const V3<R>& q, const V3<R>& wwf, int i, int
   return vel * flux3(q.ld(i, j, k - 2), q.ld(i, j, k - 1), q.ld(i, j, k), q.ld(i, j, k + 1), -vel, R(D.vup));
 }
 template <class R>
-__device__ R tend_t(const Dom<R>& D, int i, int j, int k, bool use_tendf, bool use_hd) {
-  R r = -(D.msftx(i, j) * R(D.rdx)) * (sc_fx(D, D.t2, D.ru, i + 1, j, k, false) - sc_fx(D, D.t2, D.ru, i, j, k, false));
-  if (D.do_y) r -= (D.msftx(i, j) * R(D.rdy)) * (sc_fy(D, D.t2, D.rv, i, j + 1, k, false) - sc_fy(D, D.t2, D.rv, i, j, k, false));
+__device__ R tend_t(const Dom<R>& D, int i, int j, int k, bool use_tendf, bool use_hd, R fx0, R fx1, R fy0, R fy1) {
+  R r = -(D.msftx(i, j) * R(D.rdx)) * (fx1 - fx0);
+  if (D.do_y) r -= (D.msftx(i, j) * R(D.rdy)) * (fy1 - fy0);
   r -= R(D.rdnw[k]) * (sc_fz(D, D.t2, D.ww, i, j, k + 1, false) - sc_fz(D, D.t2, D.ww, i, j, k, false));
   if (use_tendf) r += D.t_tendf.ld(i, j, k) / D.msfty(i, j);
   if (use_hd) r += (R(D.c1h[k]) * D.mut.ld(i, j, 0) + R(D.c2h[k])) * D.hd.ld(i, j, k) / D.msfty(i, j);
@@ -611,32 +611,87 @@ __device__ __forceinline__ bool spec_at(Ring r, int i, int j, int& sl, int& pos)
 // boundaries the spec zone's tendencies from the boundary slabs.
 template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_tend(const __grid_constant__ Pack<R, NM> P, int rk) {
+  constexpr int SX = shape_x(SH), SY = shape_y(SH);
+  // the horizontal face fluxes of the block's tile, each evaluated once (u, v, w, theta): x faces i0 .. i0 + SX
+  // of each row, y faces j0 .. j0 + SY of each column
+  __shared__ R sfx[4][SY][SX + 1];
+  __shared__ R sfy[4][SY + 1][SX];
   const Dom<R>* Dp;
   int i, j, k;
-  if (!thread_index<SH>(P, RG_STAG, Dp, i, j, k)) return;
+  const bool in = thread_index<SH>(P, RG_STAG, Dp, i, j, k);
   const Dom<R>& D = *Dp;
+  const int tx = int(threadIdx.x) % SX, ty = int(threadIdx.x) / SX;
   const int nx = D.nx, ny = D.ny, nz = D.nz;
   const bool use_tendf = D.lbc || D.diff_on;
   const int ui0 = D.bc_x != CW_BC_PERIODIC ? 1 : 0;
   const int vj0 = (D.bc_y != CW_BC_PERIODIC && D.do_y) ? 1 : 0;
+  const bool dy = D.do_y;
+  // the faces a point of each tendency's range uses (x faces f of its row, y faces f of its column)
+  auto ux = [&](int f) { return j < ny && k < nz && f >= ui0 && f <= nx; };
+  auto uy = [&](int f) { return dy && i >= ui0 && i < nx && k < nz && f >= 0 && f <= ny; };
+  auto vx = [&](int f) { return dy && j >= vj0 && j < ny && k < nz && f >= 0 && f <= nx; };
+  auto vy = [&](int f) { return dy && i < nx && k < nz && f >= vj0 && f <= ny; };
+  auto wx = [&](int f) { return j < ny && k >= 1 && f >= 0 && f <= nx; };
+  auto wy = [&](int f) { return dy && i < nx && k >= 1 && f >= 0 && f <= ny; };
+  auto tx_ = [&](int f) { return j < ny && k < nz && f >= 0 && f <= nx; };
+  auto ty_ = [&](int f) { return dy && i < nx && k < nz && f >= 0 && f <= ny; };
+  const bool xe = tx == SX - 1, ye = ty == SY - 1;  // the tile's last column / row also takes the next face
+  if (ux(i)) sfx[0][ty][tx] = tu_fx(D, i, j, k);
+  if (xe && ux(i + 1)) sfx[0][ty][SX] = tu_fx(D, i + 1, j, k);
+  if (uy(j)) sfy[0][ty][tx] = tu_fy(D, i, j, k);
+  if (ye && uy(j + 1)) sfy[0][SY][tx] = tu_fy(D, i, j + 1, k);
+  if (vx(i)) sfx[1][ty][tx] = tv_fx(D, i, j, k);
+  if (xe && vx(i + 1)) sfx[1][ty][SX] = tv_fx(D, i + 1, j, k);
+  if (vy(j)) sfy[1][ty][tx] = tv_fy(D, i, j, k);
+  if (ye && vy(j + 1)) sfy[1][SY][tx] = tv_fy(D, i, j + 1, k);
+  if (wx(i)) sfx[2][ty][tx] = tw_fx(D, i, j, k);
+  if (xe && wx(i + 1)) sfx[2][ty][SX] = tw_fx(D, i + 1, j, k);
+  if (wy(j)) sfy[2][ty][tx] = tw_fy(D, i, j, k);
+  if (ye && wy(j + 1)) sfy[2][SY][tx] = tw_fy(D, i, j + 1, k);
+  if (tx_(i)) sfx[3][ty][tx] = sc_fx(D, D.t2, D.ru, i, j, k, false);
+  if (xe && tx_(i + 1)) sfx[3][ty][SX] = sc_fx(D, D.t2, D.ru, i + 1, j, k, false);
+  if (ty_(j)) sfy[3][ty][tx] = sc_fy(D, D.t2, D.rv, i, j, k, false);
+  if (ye && ty_(j + 1)) sfy[3][SY][tx] = sc_fy(D, D.t2, D.rv, i, j + 1, k, false);
+  __syncthreads();
+  if (!in) return;
+  auto F = [&](int v, R& fx0, R& fx1, R& fy0, R& fy1) {
+    fx0 = sfx[v][ty][tx];
+    fx1 = sfx[v][ty][tx + 1];
+    fy0 = sfy[v][ty][tx];
+    fy1 = sfy[v][ty + 1][tx];
+  };
+  R fx0, fx1, fy0, fy1;
   const bool lbc = D.lbc;
   int sl, pos;
   // every tendency is computed before the first store (the stores cannot alias the loads then)
   // LateralBC::spec_dry (lateral_bc.cpp:337-351): the spec zone (row 0) takes the boundary tendency
   bool has_u = true, has_v = true;
   R tu = 0, tv = 0;
-  if (lbc && k < nz && spec_at(ring_for(nx, ny, 'u'), i, j, sl, pos)) tu = slab_at(D.lbc_var[0], 1, sl, pos, k, 0);
-  else if (i >= ui0 && i < nx && j < ny && k < nz) tu = tend_u(D, i, j, k, use_tendf);
-  else has_u = false;
-  if (lbc && k < nz && spec_at(ring_for(nx, ny, 'v'), i, j, sl, pos)) tv = slab_at(D.lbc_var[1], 1, sl, pos, k, 0);
-  else if (D.do_y && i < nx && j >= vj0 && j < ny && k < nz) tv = tend_v(D, i, j, k, use_tendf);
-  else has_v = false;
+  if (lbc && k < nz && spec_at(ring_for(nx, ny, 'u'), i, j, sl, pos)) {
+    tu = slab_at(D.lbc_var[0], 1, sl, pos, k, 0);
+  } else if (i >= ui0 && i < nx && j < ny && k < nz) {
+    F(0, fx0, fx1, fy0, fy1);
+    tu = tend_u(D, i, j, k, use_tendf, fx0, fx1, fy0, fy1);
+  } else {
+    has_u = false;
+  }
+  if (lbc && k < nz && spec_at(ring_for(nx, ny, 'v'), i, j, sl, pos)) {
+    tv = slab_at(D.lbc_var[1], 1, sl, pos, k, 0);
+  } else if (dy && i < nx && j >= vj0 && j < ny && k < nz) {
+    F(1, fx0, fx1, fy0, fy1);
+    tv = tend_v(D, i, j, k, use_tendf, fx0, fx1, fy0, fy1);
+  } else {
+    has_v = false;
+  }
   const bool mass = i < nx && j < ny;
   const bool spec = mass && lbc && spec_at(ring_for(nx, ny, 'h'), i, j, sl, pos);
   R tw = 0, tp = 0, tt = 0, tm = 0;
   bool has_p = false, has_m = false;
   if (mass) {
-    if (k >= 1) tw = tend_w(D, i, j, k, use_tendf);
+    if (k >= 1) {
+      F(2, fx0, fx1, fy0, fy1);
+      tw = tend_w(D, i, j, k, use_tendf, fx0, fx1, fy0, fy1);
+    }
     if (spec) {
       tp = slab_at(D.lbc_var[3], 1, sl, pos, k, 0);
       has_p = true;
@@ -644,7 +699,14 @@ __global__ void __launch_bounds__(PX) k_tend(const __grid_constant__ Pack<R, NM>
       tp = tend_ph(D, i, j, k, lbc);
       has_p = true;
     }
-    if (k < nz) tt = spec ? slab_at(D.lbc_var[2], 1, sl, pos, k, 0) : tend_t(D, i, j, k, use_tendf, D.n_moist > 0);
+    if (k < nz) {
+      if (spec) {
+        tt = slab_at(D.lbc_var[2], 1, sl, pos, k, 0);
+      } else {
+        F(3, fx0, fx1, fy0, fy1);
+        tt = tend_t(D, i, j, k, use_tendf, D.n_moist > 0, fx0, fx1, fy0, fy1);
+      }
+    }
     if (k == 0 && lbc) {
       if (spec) {
         tm = slab_at(D.lbc_var[4], 1, sl, pos, 0, 0);
