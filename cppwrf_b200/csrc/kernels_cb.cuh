@@ -101,15 +101,17 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ls_prep(const __grid_constant__
   __syncthreads();
   if (mass && w0) {  // KWW: the column integral, then the running sum, in the reference's order
     R dmdt = 0;
+#pragma unroll 4
     for (int k = 0; k < nz; ++k) dmdt += R(s_div[k * CX + lane]);
     R w = 0;
-    D.ww(i, j, 0) = 0;
-    for (int k = 1; k < nz; ++k) {
+#pragma unroll 4
+    for (int k = 1; k < nz; ++k) {  // ww of level k into the slot of the divergence it consumed
       w = w - R(D.dnw[k - 1]) * R(D.c1h[k - 1]) * dmdt - R(s_div[(k - 1) * CX + lane]);
-      D.ww(i, j, k) = w;
+      s_div[(k - 1) * CX + lane] = double(w);
     }
-    D.ww(i, j, nz) = 0;
   }
+  __syncthreads();
+  if (mass) CB_LOOP(k, nz + 1) D.ww(i, j, k) = (k == 0 || k == nz) ? R(0) : R(s_div[(k - 1) * CX + lane]);
   if (col && D.n_moist > 0) {  // KCq
     CB_LOOP(k, nz) {  // the three sums over species first, then the stores
       const bool has_u = j < ny, has_v = i < nx && j < nyv, has_w = i < nx && j < ny && k >= 1;
@@ -248,6 +250,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ss_prep(const __grid_constant__
     D.alpha(i, j, 0) = 0;
     D.gamma(i, j, 0) = 0;
     A gprev = 0;
+#pragma unroll 4
     for (int k = 1; k < nz; ++k) {
       const A al = 1. / (s_b[k * CX + lane] - s_a[k * CX + lane] * gprev);
       D.alpha(i, j, k) = R(al);
@@ -340,7 +343,9 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
           const R fx = (u_ip + (c1h * muu_ip + c2h) * usv_ip / msfuy_ip) - (u_k + (c1h * muu + c2h) * usv / msfuy);
           R d = R(D.rdx) * fx;
           if (D.do_y) d += R(D.rdy) * ((v_jp + (c1h * muv_jp + c2h) * vsv_jp * mvxi_jp) - (v_k + (c1h * muv + c2h) * vsv * mvxi));
-          s0[k * CX + lane] = A(D.msftx(i, j) * D.msfty(i, j) * d);
+          const A dv = A(D.msftx(i, j) * D.msfty(i, j) * d);
+          s0[k * CX + lane] = dv;
+          s1[k * CX + lane] = D.dnw[k] * dv;  // the term of the column sum, for the serial sum below
         }
         const R su = rum + u_k;
         D.ru_m(i, j, k) = last ? su / rn + (c1h * muu + c2h) * usv / msfuy : su;
@@ -352,7 +357,8 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
     __syncthreads();
     if (dyn && w0) {  // the column mass tendency: sum over k in order
       A dmdt = 0;
-      for (int k = 0; k < nz; ++k) dmdt += D.dnw[k] * s0[k * CX + lane];
+#pragma unroll 4
+      for (int k = 0; k < nz; ++k) dmdt += s1[k * CX + lane];
       const A mtend = A(D.mu_tend.ld(i, j, 0));
       const A mu_old = A(D.mu2(i, j, 0));
       const A mu_new = mu_old + A(dts) * (dmdt + mtend);
@@ -373,6 +379,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
     if (dyn && w0) {  // ww'' by the running integral (ww1 of level k + 1 staged in s2[k + 1])
       A ww_full = 0;
       s2[0 * CX + lane] = 0;
+#pragma unroll 4
       for (int k = 0; k < nz - 1; ++k) {
         ww_full = ww_full - s1[k * CX + lane];
         s2[(k + 1) * CX + lane] = A(R(ww_full - s2[(k + 1) * CX + lane]));
@@ -520,12 +527,14 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
     __syncthreads();
     if (dyn && w0) {  // KWSolve: forward and backward sweeps
       A wprev = s2[0 * CX + lane];
+#pragma unroll 4
       for (int k = 1; k <= nz; ++k) {
         const A wk = (s2[k * CX + lane] - s_a[k * CX + lane] * wprev) * s_al[k * CX + lane];
         wprev = A(R(wk));
         s2[k * CX + lane] = wprev;
       }
       A wnext = wprev;
+#pragma unroll 4
       for (int k = nz - 1; k >= 1; --k) {
         const A wk = s2[k * CX + lane] - s_ga[k * CX + lane] * wnext;
         wnext = A(R(wk));
