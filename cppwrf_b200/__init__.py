@@ -93,6 +93,14 @@ class Domain:
     def set_graph(self, on):
         self.lib.cw_set_graph(self.h, 1 if on else 0)
 
+    def check_finite(self, member=0):
+        """None when the prognostic state is finite, else (field name, species, i, j, k) of the first
+        non-finite value."""
+        f, n, i, j, k = (C.c_int() for _ in range(5))
+        rc = self.lib.cw_check_finite(self.h, member, C.byref(f), C.byref(n), C.byref(i), C.byref(j), C.byref(k))
+        _check(self.lib, self.h, 0 if rc >= 0 else rc, "cw_check_finite")
+        return None if rc == 0 else (FIELDS[f.value], n.value, i.value, j.value, k.value)
+
     def set_autotune(self, on=True):
         """The next three steps time the point kernels' block shapes; each kernel then keeps its fastest."""
         self.lib.cw_set_autotune(self.h, 1 if on else 0)

@@ -160,6 +160,7 @@ def load(path=None):
         "cw_batch_add": (i, [vp, C.POINTER(Grid), C.POINTER(Options), ip]),
         "cw_batch_remove": (i, [vp, i]),
         "cw_set_autotune": (i, [vp, i]),
+        "cw_check_finite": (i, [vp, i, ip, ip, ip, ip, ip]),
         "cw_autotune_choice": (i, [vp, C.c_char_p, ip]),
         "cw_footprint": (i, [C.POINTER(Grid), C.POINTER(Options), C.POINTER(sz)]),
         "cw_case_clone": (i, [vp, C.POINTER(vp)]),

@@ -107,6 +107,7 @@ struct cw_handle {
   DevTables<double> t64;
   DevTables<float> t32;
   double* dtbc_d = nullptr;  // per member: time since the boundary data, advanced by the step on the device
+  unsigned long long* diag = nullptr;  // cw_check_finite's result
   double* staging = nullptr;  // FP32 field transfers: doubles converted on the device
   size_t staging_n = 0;
   int nzmax = 0;
@@ -974,6 +975,19 @@ void copy_out(cw_handle* h, const Loc& l, double* host, size_t count) {
   CW_CUDA(cudaStreamSynchronize(h->stream));
 }
 
+// ---- non-finite detection (the reference's run.check_nonfinite_every_step)
+// the smallest key (field slot, k, j, i) of a non-finite interior value of one field
+template <class T>
+__global__ void k_nonfinite(const T* __restrict__ p, int sj, int sk, int nx, int ny, int nz, unsigned long long base,
+                            unsigned long long* out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)nx * ny * nz;
+  if (t >= n) return;
+  const int i = int(t % nx), j = int((t / nx) % ny), k = int(t / ((long long)nx * ny));
+  const T v = p[i + j * (long long)sj + k * (long long)sk];
+  if (!isfinite(v)) atomicMin(out, base + (unsigned long long)t);
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ C ABI
@@ -1062,6 +1076,7 @@ int cw_destroy(cw_handle* h) {
   invalidate_graph(h);
   free_tables(h);
   cudaFree(h->staging);
+  cudaFree(h->diag);
   for (Member& M : h->m) cudaFree(M.arena);
   if (h->own_stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -1310,6 +1325,49 @@ int cw_profile_entry(cw_handle* h, int idx, char* name, int len, double* ms, lon
   if (launches) *launches = h->prof_n[idx];
   return 0;
 }
+int cw_check_finite(cw_handle* h, int mi, int* field, int* n, int* i, int* j, int* k) {
+  return guarded(h, [&] {
+    if (!h || mi < 0 || mi >= int(h->m.size())) throw std::runtime_error("member index out of range");
+    Member& M = h->m[size_t(mi)];
+    if (!h->diag) CW_CUDA(cudaMalloc(&h->diag, sizeof(unsigned long long)));
+    const unsigned long long none = ~0ull;
+    CW_CUDA(cudaMemcpyAsync(h->diag, &none, sizeof(none), cudaMemcpyHostToDevice, h->stream));
+    // the prognostic state, slot s: U_2 V_2 W_2 T_2 PH_2 MU_2 P AL, then Q_2 of each species
+    const int ids[8] = {CW_U_2, CW_V_2, CW_W_2, CW_T_2, CW_PH_2, CW_MU_2, CW_P, CW_AL};
+    const int nslot = 8 + M.o.n_scalars;
+    const unsigned long long span = 1ull << 40;
+    for (int sl = 0; sl < nslot; ++sl) {
+      const Loc l = sl < 8 ? locate(h, mi, ids[sl], 0) : locate(h, mi, CW_Q_2, sl - 8);
+      const cw_layout& L = l.L;
+      const long long npts = (long long)L.nx * L.ny * L.nz;
+      const unsigned blocks = unsigned((npts + 255) / 256);
+      if (l.esz == 8)
+        k_nonfinite<double><<<blocks, 256, 0, h->stream>>>(reinterpret_cast<const double*>(l.base) + L.offset, int(L.sj),
+                                                            int(L.sk), L.nx, L.ny, L.nz, span * sl, h->diag);
+      else
+        k_nonfinite<float><<<blocks, 256, 0, h->stream>>>(reinterpret_cast<const float*>(l.base) + L.offset, int(L.sj),
+                                                           int(L.sk), L.nx, L.ny, L.nz, span * sl, h->diag);
+      CW_CUDA(cudaGetLastError());
+    }
+    unsigned long long key = none;
+    CW_CUDA(cudaMemcpyAsync(&key, h->diag, sizeof(key), cudaMemcpyDeviceToHost, h->stream));
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+    if (key == none) {
+      if (field) *field = -1;
+      return 0;
+    }
+    const int sl = int(key / span);
+    const long long t = (long long)(key % span);
+    const Loc l = sl < 8 ? locate(h, mi, ids[sl], 0) : locate(h, mi, CW_Q_2, sl - 8);
+    if (field) *field = sl < 8 ? ids[sl] : CW_Q_2;
+    if (n) *n = sl < 8 ? 0 : sl - 8;
+    if (i) *i = int(t % l.L.nx);
+    if (j) *j = int((t / l.L.nx) % l.L.ny);
+    if (k) *k = int(t / ((long long)l.L.nx * l.L.ny));
+    return 1;
+  });
+}
+
 int cw_set_autotune(cw_handle* h, int on) {
   if (!h) return -1;
   h->autotune = on != 0;

@@ -164,6 +164,11 @@ int cw_members(cw_handle* h, int* out);
  * a new member (its fields zeroed, map factors 1) as the last index; cw_batch_remove frees one member and
  * moves the members after it down by one index. Both rebuild the handle's tables; the next cw_step captures
  * the step again. cw_step on an empty batch does nothing. */
+/* Non-finite detection (CPPWRF's run.check_nonfinite_every_step, tests/robustness/run_test.sh:51-64): scans the
+ * interior of member's prognostic state (U_2 V_2 W_2 T_2 PH_2 MU_2 P AL, then Q_2 of each species) and returns 0
+ * when every value is finite (field = -1), 1 with the first non-finite value's field id, species n and point
+ * (i, j, k) in that order of fields and then k, j, i, < 0 on error. It synchronizes the handle's stream. */
+int cw_check_finite(cw_handle* h, int member, int* field, int* n, int* i, int* j, int* k);
 /* Block-shape autotuning of the point kernels (no reference counterpart). With on = 1 the next three
  * cw_step steps run every tunable kernel in one of its block shapes (0: 128 x 1, 1: 64 x 2, 2: 32 x 4
  * points along i x j), timed per launch; afterwards each kernel keeps its fastest shape and the step is
