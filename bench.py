@@ -342,16 +342,22 @@ def run_served(args, torch, capi, Domain, Server):
     st = srv.stats()
     srv.close()
     gps = sum(r["nx"] * r["ny"] * r["nz"] * r["steps"] for r in reqs)
-    # plain FP64, one request after the other (device time of the steps)
+    # plain FP64, one request after the other: the device time of the steps alone, and the wall time of the
+    # whole solve (domain set-up, upload, steps, read-back of the prognostic state), the served path's equal
     stream = torch.cuda.Stream()
-    plain_ms = 0.0
+    plain_ms, plain_wall = 0.0, 0.0
     for r in reqs:
         c = make_case(capi, capi.FP64, seed=r["seed"], w=r)
+        t0 = time.perf_counter()
         d = Domain(c.g, c.o).upload_case(c)
         lib.cw_set_stream(d.h, C.c_void_p(stream.cuda_stream))
         plain_ms += _timed_steps(torch, stream, d.step, r["steps"])
+        for name in ("U_2", "V_2", "W_2", "T_2", "PH_2", "MU_2", "P", "AL"):
+            d.field(name)
         d.close()
+        plain_wall += time.perf_counter() - t0
     plain = gps / (plain_ms / 1000.0)
+    plain_w = gps / plain_wall
     line = {"metric": METRIC, "value": st["gp_steps_per_s"], "unit": UNIT, "n_gpus": 1, "steps": None,
             "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64", "data": "synthetic (cw_gen_lam, seeded per request; Poisson arrivals)",
@@ -359,7 +365,9 @@ def run_served(args, torch, capi, Domain, Server):
                        "hbm_budget_bytes": 150e9, "sizes": "log-uniform 40..300, nz 35..60, 30..360 steps"},
             "p50_latency_s": st["p50_s"], "p99_latency_s": st["p99_s"], "mean_latency_s": st["mean_s"],
             "served_stats": st, "fp64_plain_serial_value": plain, "served_over_fp64_plain": st["gp_steps_per_s"] / plain,
-            "note": "value = completed gp-steps / (last completion - first submission), host clock"}
+            "fp64_plain_serial_wall_value": plain_w, "served_over_fp64_plain_wall": st["gp_steps_per_s"] / plain_w,
+            "note": "value = completed gp-steps / (last completion - first submission), host clock, arrival gaps "
+                    "included; fp64_plain_serial_value: device time of the steps only; _wall_value: whole solves"}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -159,6 +159,7 @@ def load(path=None):
         "cw_download_noalloc": (i, [vp, i, i, dp, sz]),
         "cw_batch_add": (i, [vp, C.POINTER(Grid), C.POINTER(Options), ip]),
         "cw_batch_remove": (i, [vp, i]),
+        "cw_batch_adopt": (i, [vp, vp, ip]),
         "cw_set_autotune": (i, [vp, i]),
         "cw_check_finite": (i, [vp, i, ip, ip, ip, ip, ip]),
         "cw_autotune_choice": (i, [vp, C.c_char_p, ip]),

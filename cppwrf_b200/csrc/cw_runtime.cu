@@ -92,7 +92,8 @@ struct DevTables {  // the kernels' views of the members and the device scalar t
 
 struct HaloSetHost {
   std::vector<HaloField> f;
-  std::vector<HaloChunk> chunks;  // the fields in launch-sized chunks
+  std::vector<HaloChunk<kHaloSmall>> small;  // the fields in one small chunk (most single domains), or
+  std::vector<HaloChunk<kHaloLarge>> large;  // in large chunks
 };
 
 }  // namespace cw
@@ -482,22 +483,28 @@ HaloField halo_field(const Member& M, const HaloItem& it) {
   return f;
 }
 
-void finish_haloset(cw_handle*, HaloSetHost& s) {
-  s.chunks.clear();
-  for (size_t f0 = 0; f0 < s.f.size(); f0 += kHaloChunk) {
-    HaloChunk c{};
-    c.nf = int(std::min(s.f.size() - f0, size_t(kHaloChunk)));
+template <int NF>
+void chunk_fields(const std::vector<HaloField>& f, std::vector<HaloChunk<NF>>& out) {
+  for (size_t f0 = 0; f0 < f.size(); f0 += NF) {
+    HaloChunk<NF> c{};
+    c.nf = int(std::min(f.size() - f0, size_t(NF)));
     long long total = 0;
     for (int n = 0; n < c.nf; ++n) {
-      c.f[n] = s.f[f0 + size_t(n)];
+      c.f[n] = f[f0 + size_t(n)];
       c.start[n] = unsigned(total);
       total += c.f[n].ncell;
       c.has_oddface |= c.f[n].oddface_x;
     }
     if (total >= (1ll << 31)) throw std::runtime_error("a halo fill of more than 2^31 cells");
     c.start[c.nf] = unsigned(total);
-    s.chunks.push_back(c);
+    out.push_back(c);
   }
+}
+void finish_haloset(cw_handle*, HaloSetHost& s) {
+  s.small.clear();
+  s.large.clear();
+  if (s.f.size() <= size_t(kHaloSmall)) chunk_fields(s.f, s.small);
+  else chunk_fields(s.f, s.large);
 }
 template <class R>
 void build_halosets_t(cw_handle* h, DevTables<R>& T) {
@@ -588,21 +595,26 @@ struct Launcher {
     if (h->profiling) CW_CUDA(cudaEventRecord(h->prof_ev.back().second.second, h->stream));
     ++count;
   }
-  void halo(int set) {
-    for (const HaloChunk& c : h->hs[set].chunks) {
+  template <int NF>
+  void halo_chunks(const std::vector<HaloChunk<NF>>& chunks) {
+    for (const HaloChunk<NF>& c : chunks) {
       const unsigned total = c.start[c.nf];
       if (total == 0) continue;
       const int bs = 256;
       const unsigned nb = (total + bs - 1) / bs;
       begin("k_halo");
-      k_halo<<<nb, bs, 0, h->stream>>>(c, 0);
+      k_halo<NF><<<nb, bs, 0, h->stream>>>(c, 0);
       check();
       if (c.has_oddface) {
         begin("k_halo");
-        k_halo<<<nb, bs, 0, h->stream>>>(c, 1);
+        k_halo<NF><<<nb, bs, 0, h->stream>>>(c, 1);
         check();
       }
     }
+  }
+  void halo(int set) {
+    halo_chunks(h->hs[set].small);
+    halo_chunks(h->hs[set].large);
   }
   void copy_list(CopyDesc* d, long long* sd, size_t n, long long total) {
     if (!total) return;
@@ -1043,6 +1055,25 @@ int cw_batch_add(cw_handle* h, const cw_grid* g, const cw_options* o, int* membe
       rebuild(h);
       throw;
     }
+    if (member) *member = int(h->m.size()) - 1;
+    return 0;
+  });
+}
+
+int cw_batch_adopt(cw_handle* h, cw_handle* single, int* member) {
+  return guarded(h, [&] {
+    if (!h || !single || single == h) throw std::runtime_error("bad arguments");
+    if (single->m.size() != 1) throw std::runtime_error("the adopted handle must hold one domain");
+    if (single->precision != h->precision) throw std::runtime_error("batch members must share the precision");
+    if (int(h->m.size()) >= kMaxMembers) throw std::runtime_error("the batch is full");
+    if (!h->m.empty() && single->m[0].n_sound != h->m[0].n_sound) throw std::runtime_error("batch members must share n_sound");
+    CW_CUDA(cudaStreamSynchronize(single->stream));
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+    invalidate_graph(single);
+    free_tables(single);
+    h->m.push_back(std::move(single->m[0]));  // the domain's allocation changes hands, its contents stay
+    single->m.clear();
+    rebuild(h);
     if (member) *member = int(h->m.size()) - 1;
     return 0;
   });

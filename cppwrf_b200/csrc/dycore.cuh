@@ -188,11 +188,13 @@ struct HaloField {
   long long ncell_x, ncell;  // x-pass cells, all cells
 };
 // The fields of one launch, passed by value as a __grid_constant__ parameter (no descriptor is read from
-// global memory); a fill point with more fields is launched in chunks of kHaloChunk.
-constexpr int kHaloChunk = 24;
+// global memory). Two capacities: a fill point of a single domain fits the small one; a batch's fill point
+// uses the large one (160 x 88 B of descriptors, inside the 32 KB parameter limit), in chunks when larger.
+constexpr int kHaloSmall = 16, kHaloLarge = 160;
+template <int NF>
 struct HaloChunk {
-  HaloField f[kHaloChunk];
-  unsigned start[kHaloChunk + 1];  // prefix sums of the fields' cell counts
+  HaloField f[NF];
+  unsigned start[NF + 1];  // prefix sums of the fields' cell counts
   int nf;
   int has_oddface;
 };

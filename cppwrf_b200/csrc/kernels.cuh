@@ -158,7 +158,8 @@ __device__ __forceinline__ void halo_cell(const HaloField& f, unsigned c, int pa
 }
 
 // one thread per halo cell of the chunk (the host keeps a chunk's cell count below 2^31)
-static __global__ void k_halo(const __grid_constant__ HaloChunk s, int pass) {
+template <int NF>
+__global__ void k_halo(const __grid_constant__ HaloChunk<NF> s, int pass) {
   const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= s.start[s.nf]) return;
   int lo = 0, hi = s.nf - 1;

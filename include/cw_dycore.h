@@ -178,6 +178,10 @@ int cw_set_autotune(cw_handle* h, int on);
 int cw_autotune_choice(cw_handle* h, const char* kernel, int* shape);
 int cw_batch_add(cw_handle* h, const cw_grid* g, const cw_options* o, int* member);
 int cw_batch_remove(cw_handle* h, int member);
+/* Moves the one domain of handle `single` (made with cw_create and filled, e.g. on another thread while the
+ * batch steps) into the batch as its last member, without copying its fields; `single` is left empty (destroy
+ * it). Same precision and acoustic step count as the batch's members. */
+int cw_batch_adopt(cw_handle* h, cw_handle* single, int* member);
 /* Device bytes one domain takes in a handle (fields, work fields, scalars, slabs, vertical arrays): the
  * footprint the served form admits by. Needs no device. */
 int cw_footprint(const cw_grid* g, const cw_options* o, size_t* bytes);
