@@ -612,11 +612,37 @@ struct Launcher {
       }
     }
   }
-  void halo(int set) {
-    halo_chunks(h->hs[set].small);
-    halo_chunks(h->hs[set].large);
+  // halo fill points are deferred until the next kernel: consecutive fill points (nothing launched between
+  // them) become one launch over the union of their fields
+  std::vector<int> pend;
+  void halo(int set) { pend.push_back(set); }
+  void flush() {
+    if (pend.empty()) return;
+    if (pend.size() == 1) {
+      halo_chunks(h->hs[pend[0]].small);
+      halo_chunks(h->hs[pend[0]].large);
+    } else {
+      std::vector<HaloField> f;
+      for (int set : pend)
+        for (const HaloField& x : h->hs[set].f) {
+          bool dup = false;
+          for (const HaloField& y : f) dup |= y.p == x.p && y.ind == x.ind;
+          if (!dup) f.push_back(x);
+        }
+      if (f.size() <= size_t(kHaloSmall)) {
+        std::vector<HaloChunk<kHaloSmall>> c;
+        chunk_fields(f, c);
+        halo_chunks(c);
+      } else {
+        std::vector<HaloChunk<kHaloLarge>> c;
+        chunk_fields(f, c);
+        halo_chunks(c);
+      }
+    }
+    pend.clear();
   }
   void copy_list(CopyDesc* d, long long* sd, size_t n, long long total) {
+    flush();
     if (!total) return;
     const int bs = 256;
     begin("k_copy");
@@ -633,6 +659,7 @@ struct Launcher {
   // a point kernel of fixed shape 0 over the index range kind, one launch per pack
   template <class R, int NM, class K, class... Args>
   void run(const char* name, int kind, K kern, const Packs<R, NM>& ps, Args... args) {
+    flush();
     for (size_t c = 0; c < ps.p.size(); ++c) {
       const int nb = ps.blocks[c][size_t(kind)][0];
       if (nb == 0) continue;
@@ -645,6 +672,7 @@ struct Launcher {
   template <class R, int NM, class K, class... Args>
   void run_t(const char* name, int kind, int nq, const std::array<K, kNumShapes>& kerns, const Packs<R, NM>& ps,
              Args... args) {
+    flush();
     const int sh = shape_for(name);
     for (size_t c = 0; c < ps.p.size(); ++c) {
       const int nb = ps.blocks[c][size_t(kind)][size_t(sh)];
@@ -657,6 +685,7 @@ struct Launcher {
   // a column-block kernel using `arrays` shared level arrays
   template <class R, int NM, class K, class... Args>
   void run_cb(const char* name, int kind, int arrays, K kern, const Packs<R, NM>& ps, Args... args) {
+    flush();
     static_assert(CX == 32, "a column block's lanes are one warp");
     const size_t smem = size_t(arrays) * h->cb_level_bytes;
     CW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
@@ -671,6 +700,7 @@ struct Launcher {
   // one block per member
   template <class R, int NM, class K>
   void run_members(const char* name, int threads, K kern, const Packs<R, NM>& ps) {
+    flush();
     for (size_t c = 0; c < ps.p.size(); ++c) {
       begin(name);
       kern<<<unsigned(ps.p[c].n), threads, 0, h->stream>>>(ps.p[c]);
@@ -754,6 +784,7 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
     L.run_cb("k_w_surface", RG_COLS_MASS, 0, k_w_surface<R, NM>, d);
     L.halo(cw_handle::H_WS1);
   }
+  L.flush();
 }
 
 template <class R>

@@ -197,29 +197,41 @@ __global__ void __launch_bounds__(PX) k_q_tendf_rk1(const __grid_constant__ Pack
   D.qtf[n](i, j, k) = t;
 }
 
-// advect_scalar (Fluxes::adv :126-139) of species n at a cell
+// advect_scalar (Fluxes::adv :126-139) of species n at a cell, from its horizontal face fluxes
 template <class R>
-__device__ R q_adv(const Dom<R>& D, const V3<R>& q, int i, int j, int k) {
+__device__ R q_adv(const Dom<R>& D, const V3<R>& q, int i, int j, int k, R fx0, R fx1, R fy0, R fy1) {
   if (spec_cell(D, i, j)) return 0;
-  R r = -(D.msftx(i, j) * R(D.rdx)) * (sc_fx(D, q, D.ru_m, i + 1, j, k, false) - sc_fx(D, q, D.ru_m, i, j, k, false));
-  if (D.do_y) r -= (D.msftx(i, j) * R(D.rdy)) * (sc_fy(D, q, D.rv_m, i, j + 1, k, false) - sc_fy(D, q, D.rv_m, i, j, k, false));
+  R r = -(D.msftx(i, j) * R(D.rdx)) * (fx1 - fx0);
+  if (D.do_y) r -= (D.msftx(i, j) * R(D.rdy)) * (fy1 - fy0);
   return r - R(D.rdnw[k]) * (sc_fz(D, q, D.ww_m, i, j, k + 1, false) - sc_fz(D, q, D.ww_m, i, j, k, false));
 }
-// KUpdate (:145-156) for the non-PD species of this stage
+// KUpdate (:145-156) for the non-PD species of this stage; the horizontal face fluxes of the block's tile
+// once, in shared memory
 template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_q_update(const __grid_constant__ Pack<R, NM> P, int rk) {
+  constexpr int SX = shape_x(SH), SY = shape_y(SH);
+  __shared__ R sfx[SY][SX + 1];
+  __shared__ R sfy[SY + 1][SX];
   const Dom<R>* Dp;
   int i, j, k;
-  if (!thread_index<SH>(P, RG_MASS, Dp, i, j, k)) return;
+  const bool in = thread_index<SH>(P, RG_MASS, Dp, i, j, k);
   const Dom<R>& D = *Dp;
+  const int n = blockIdx.y;  // the species (uniform in the block)
+  if (n >= D.n_scalars || q_is_pd(D, n, rk)) return;
+  const int tx = int(threadIdx.x) % SX, ty = int(threadIdx.x) / SX;
+  const int nx = D.nx, ny = D.ny;
+  const V3<R> q = D.q2[n];
+  if (j < ny && i <= nx) sfx[ty][tx] = sc_fx(D, q, D.ru_m, i, j, k, false);
+  if (tx == SX - 1 && j < ny && i + 1 <= nx) sfx[ty][SX] = sc_fx(D, q, D.ru_m, i + 1, j, k, false);
+  if (D.do_y && i < nx && j <= ny) sfy[ty][tx] = sc_fy(D, q, D.rv_m, i, j, k, false);
+  if (D.do_y && ty == SY - 1 && i < nx && j + 1 <= ny) sfy[SY][tx] = sc_fy(D, q, D.rv_m, i, j + 1, k, false);
+  __syncthreads();
+  if (!in) return;
   const R dt_rk = R(rk == 1 ? D.dt / 3.0 : (rk == 2 ? 0.5 * D.dt : D.dt));
-  const R mub = D.mub(i, j), mu1 = D.mu1(i, j, 0), mu2 = D.mu2(i, j, 0);
-  const int n = blockIdx.y;  // the species
-  if (n >= D.n_scalars) return;
-  if (q_is_pd(D, n, rk)) return;
-  R tend = q_adv(D, D.q2[n], i, j, k) * D.msfty(i, j);
-  tend += D.qtf[n](i, j, k);
-  D.qn[n](i, j, k) = (m_full(D, k, mub, mu1) * D.q1[n](i, j, k) + dt_rk * tend) / m_full(D, k, mub, mu2);
+  const R mub = D.mub(i, j), mu1 = D.mu1.ld(i, j, 0), mu2 = D.mu2.ld(i, j, 0);
+  R tend = q_adv(D, q, i, j, k, sfx[ty][tx], sfx[ty][tx + 1], sfy[ty][tx], sfy[ty + 1][tx]) * D.msfty(i, j);
+  tend += D.qtf[n].ld(i, j, k);
+  D.qn[n](i, j, k) = (m_full(D, k, mub, mu1) * D.q1[n].ld(i, j, k) + dt_rk * tend) / m_full(D, k, mub, mu2);
 }
 // KPreUpdatePD (:174-180)
 template <class R, int NM, int SH>
