@@ -764,7 +764,7 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
       if (rk == 3 && any_pd) {
         L.run_t("k_q_pre_pd", RG_MASS, nq, KV(k_q_pre_pd), d, rk);
         L.halo(cw_handle::H_Q1PD);
-        L.run_t("k_q_face_pd", RG_STAG, nq, KV(k_q_face_pd), d, rk);
+        L.run_t("k_q_face_pd", RG_STAG, 1, KV(k_q_face_pd), d, rk);
         L.run_t("k_q_scale_pd", RG_MASS, nq, KV(k_q_scale_pd), d, rk);
         L.halo(cw_handle::H_SCPD);
         L.run_t("k_q_update_pd", RG_MASS, nq, KV(k_q_update_pd), d, rk);

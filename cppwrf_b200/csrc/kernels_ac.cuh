@@ -279,36 +279,69 @@ __device__ void pd_fz(const Dom<R>& D, const V3<R>& q, const V3<R>& qo, R dt, in
   dh = sc_fz(D, q, D.ww_m, i, j, k, true) - lo;
 }
 // KFacePDX / KFacePDY / KFacePDZ (:159-171 with the PD statement functions): every face flux of the PD
-// species once, dh and lo, into the species' face arrays (x faces 0..nx, y faces 0..ny, z faces 0..nz)
+// species once, dh and lo, into the species' face arrays (x faces 0..nx, y faces 0..ny, z faces 0..nz). One
+// thread per face point for all species: the Courant number and the mass factor of a face (the expressions
+// of pd_fx / pd_fy / pd_fz) do not depend on the species and are evaluated once.
 template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_q_face_pd(const __grid_constant__ Pack<R, NM> P, int rk) {
   const Dom<R>* Dp;
   int i, j, k;
   if (!thread_index<SH>(P, RG_STAG, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
-  const int n = blockIdx.y;  // the species
-  if (n >= D.n_scalars || !q_is_pd(D, n, rk)) return;
   const int nx = D.nx, ny = D.ny, nz = D.nz;
   const R dt = R(rk == 1 ? D.dt / 3.0 : (rk == 2 ? 0.5 * D.dt : D.dt));
-  const V3<R>& q = D.q2[n];
-  const V3<R>& qo = D.q1[n];
   const bool fx = j < ny && k < nz, fy = D.do_y && i < nx && k < nz, fz = i < nx && j < ny;
-  R dhx = 0, lox = 0, dhy = 0, loy = 0, dhz = 0, loz = 0;
-  if (fx) pd_fx(D, q, qo, dt, i, j, k, dhx, lox);
-  if (fy) pd_fy(D, q, qo, dt, i, j, k, dhy, loy);
-  if (fz) pd_fz(D, q, qo, dt, i, j, k, dhz, loz);
-  const V3<R>* f = D.qpd + 6 * n;
+  const bool zin = fz && k != 0 && k != nz;
+  R crx = 0, facx = 0, cry = 0, facy = 0, crz = 0, facz = 0;
   if (fx) {
-    f[0](i, j, k) = dhx;
-    f[1](i, j, k) = lox;
+    const R dx = R(2) / (D.msfty(i, j) + D.msfty(i - 1, j)) / R(D.rdx), mu = R(0.5) * (pd_mh(D, i, j, k) + pd_mh(D, i - 1, j, k)),
+            vel = D.ru_m.ld(i, j, k);
+    crx = (D.spec_x && i == 1) ? (vel / mu) * dt / dx : vel * dt / dx / mu;
+    facx = mu * (dx / dt);
   }
   if (fy) {
-    f[2](i, j, k) = dhy;
-    f[3](i, j, k) = loy;
+    const R dy = R(2) / (D.msftx(i, j) + D.msftx(i, j - 1)) / R(D.rdy), mu = R(0.5) * (pd_mh(D, i, j, k) + pd_mh(D, i, j - 1, k)),
+            vel = D.rv_m.ld(i, j, k);
+    cry = vel * dt / dy / mu;
+    facy = mu * (dy / dt);
   }
-  if (fz) {
-    f[4](i, j, k) = dhz;
-    f[5](i, j, k) = loz;
+  if (zin) {
+    const R dz = R(2) / (R(D.rdnw[k]) + R(D.rdnw[k - 1])), mu = pd_mh(D, i, j, k), vel = D.ww_m.ld(i, j, k);
+    crz = vel * dt / dz / mu;
+    facz = mu * (dz / dt);
+  }
+  for (int n = 0; n < D.n_scalars; ++n) {
+    if (!q_is_pd(D, n, rk)) continue;
+    const V3<R> q = D.q2[n], qo = D.q1[n];
+    R dhx = 0, lox = 0, dhy = 0, loy = 0, dhz = 0, loz = 0;
+    if (fx) {
+      lox = facx * flux_upwind(qo.ld(i - 1, j, k), qo.ld(i, j, k), crx);
+      dhx = sc_fx(D, q, D.ru_m, i, j, k, true) - lox;
+    }
+    if (fy) {
+      loy = facy * flux_upwind(qo.ld(i, j - 1, k), qo.ld(i, j, k), cry);
+      dhy = sc_fy(D, q, D.rv_m, i, j, k, true) - loy;
+    }
+    if (zin) {
+      loz = facz * flux_upwind(qo.ld(i, j, k - 1), qo.ld(i, j, k), crz);
+      dhz = sc_fz(D, q, D.ww_m, i, j, k, true) - loz;
+    } else if (fz) {
+      loz = 0;
+      dhz = R(0) - R(0);
+    }
+    const V3<R>* f = D.qpd + 6 * n;
+    if (fx) {
+      f[0](i, j, k) = dhx;
+      f[1](i, j, k) = lox;
+    }
+    if (fy) {
+      f[2](i, j, k) = dhy;
+      f[3](i, j, k) = loy;
+    }
+    if (fz) {
+      f[4](i, j, k) = dhz;
+      f[5](i, j, k) = loz;
+    }
   }
 }
 // KScalePD (:215-241) from the stored face fluxes
