@@ -101,6 +101,19 @@ class Domain:
         _check(self.lib, self.h, 0 if rc >= 0 else rc, "cw_check_finite")
         return None if rc == 0 else (FIELDS[f.value], n.value, i.value, j.value, k.value)
 
+    def diagnostics(self, member=0):
+        """dyn::Diagnostics::compute of the current state (the diag.csv values, plus max_abs_q), as a dict."""
+        d = capi.Diag()
+        _check(self.lib, self.h, self.lib.cw_diagnostics(self.h, member, C.byref(d)), "cw_diagnostics")
+        return d.as_dict()
+
+    def snapshot(self, directory, step, time, q_names=None, member=0):
+        """Writes directory/snap_<step>.{json,bin} in CPPWRF's snapshot format."""
+        na = capi.names_array(q_names)
+        rc = self.lib.cw_snapshot_write(self.h, member, str(directory).encode(), step, time, na[0] if na else None)
+        if rc != 0:
+            raise CwError(f"cw_snapshot_write: {self.lib.cw_output_last_error().decode()}")
+
     def set_autotune(self, on=True):
         """The next three steps time the point kernels' block shapes; each kernel then keeps its fastest."""
         self.lib.cw_set_autotune(self.h, 1 if on else 0)
@@ -154,6 +167,19 @@ class Batch:
         v = C.c_longlong()
         self.lib.cw_launch_count(self.h, C.byref(v))
         return v.value
+
+    def diagnostics(self, member):
+        """dyn::Diagnostics::compute of the current state (the diag.csv values, plus max_abs_q), as a dict."""
+        d = capi.Diag()
+        _check(self.lib, self.h, self.lib.cw_diagnostics(self.h, member, C.byref(d)), "cw_diagnostics")
+        return d.as_dict()
+
+    def snapshot(self, member, directory, step, time, q_names=None):
+        """Writes directory/snap_<step>.{json,bin} in CPPWRF's snapshot format."""
+        na = capi.names_array(q_names)
+        rc = self.lib.cw_snapshot_write(self.h, member, str(directory).encode(), step, time, na[0] if na else None)
+        if rc != 0:
+            raise CwError(f"cw_snapshot_write: {self.lib.cw_output_last_error().decode()}")
 
     def layout(self, member, name, n=0):
         L = Layout()

@@ -17,7 +17,7 @@ CXX = os.environ.get("CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++20", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off",
          "-Xptxas", "-warn-spills", "--expt-relaxed-constexpr"]
-SOURCES = ["cw_runtime.cu", "cw_case.cpp", "cw_serve.cpp"]
+SOURCES = ["cw_runtime.cu", "cw_case.cpp", "cw_serve.cpp", "cw_output.cpp"]
 
 
 def build(verbose=False):

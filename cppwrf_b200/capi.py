@@ -102,6 +102,23 @@ class ServeStats(C.Structure):
                                           "gp_steps", "wall_s", "gp_steps_per_s")]
 
 
+# cw_diag (include/cw_output.h): dyn::DiagRow in the order of the diag.csv columns, then max_abs_q
+DIAG_KEYS = ("max_abs_u", "max_abs_v", "max_abs_w", "min_th_pert", "max_th_pert", "dry_mass", "theta_mass",
+             "total_energy", "max_abs_q")
+
+
+class Diag(C.Structure):
+    _fields_ = [(n, C.c_double) for n in DIAG_KEYS]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n in DIAG_KEYS}
+
+
+class SnapshotFields(C.Structure):
+    _fields_ = [(n, _DP) for n in ("u_2", "v_2", "w_2", "t_2", "p", "ph_2", "mu_2", "pb", "phb", "t_init", "mub")] + \
+               [("q_2", C.POINTER(_DP))]
+
+
 _lib = None
 
 
@@ -166,6 +183,14 @@ def load(path=None):
         "cw_footprint": (i, [C.POINTER(Grid), C.POINTER(Options), C.POINTER(sz)]),
         "cw_case_clone": (i, [vp, C.POINTER(vp)]),
         "cw_case_config": (i, [vp, C.POINTER(Grid), C.POINTER(Options)]),
+        "cw_member_config": (i, [vp, i, C.POINTER(Grid), C.POINTER(Options)]),
+        "cw_diagnostics": (i, [vp, i, C.POINTER(Diag)]),
+        "cw_diag_header": (i, [C.c_char_p, sz]),
+        "cw_diag_format_row": (i, [C.c_longlong, C.c_double, C.POINTER(Diag), C.c_double, C.c_char_p, sz]),
+        "cw_snapshot_write_host": (i, [C.c_char_p, C.c_longlong, C.c_double, C.POINTER(Grid), C.POINTER(Options),
+                                       C.POINTER(SnapshotFields), C.POINTER(C.c_char_p)]),
+        "cw_snapshot_write": (i, [vp, i, C.c_char_p, C.c_longlong, C.c_double, C.POINTER(C.c_char_p)]),
+        "cw_output_last_error": (C.c_char_p, []),
         "cw_serve_default_config": (i, [C.POINTER(ServeConfig)]),
         "cw_serve_create": (i, [C.POINTER(ServeConfig), C.POINTER(vp)]),
         "cw_serve_destroy": (i, [vp]),
@@ -187,6 +212,47 @@ def load(path=None):
     if path is None:
         _lib = lib
     return lib
+
+
+def diag_header(lib=None):
+    """The diag.csv header line (io::DiagWriter)."""
+    lib = lib or load()
+    buf = C.create_string_buffer(512)
+    if lib.cw_diag_header(buf, 512) < 0:
+        raise RuntimeError("cw_diag_header")
+    return buf.value.decode()
+
+
+def diag_row(step, time, diag, wall_s, lib=None):
+    """One diag.csv line (io::DiagWriter::row) of a cw_diag (a Diag or a dict of DIAG_KEYS)."""
+    lib = lib or load()
+    d = diag if isinstance(diag, Diag) else Diag(*[diag.get(k, 0.0) for k in DIAG_KEYS])
+    buf = C.create_string_buffer(1024)
+    if lib.cw_diag_format_row(step, time, C.byref(d), wall_s, buf, 1024) < 0:
+        raise RuntimeError("cw_diag_format_row")
+    return buf.value.decode()
+
+
+def names_array(names):
+    if names is None:
+        return None
+    arr = (C.c_char_p * len(names))(*[n.encode() for n in names])
+    return C.cast(arr, C.POINTER(C.c_char_p)), arr
+
+
+def snapshot_write_host(directory, step, time, g, o, fields, q_fields=(), q_names=None, lib=None):
+    """cw_snapshot_write_host over whole-allocation float64 arrays: fields = {"u_2": array, ..., "mub": array}."""
+    lib = lib or load()
+    keep = [np.ascontiguousarray(fields[n], dtype=np.float64) for n in
+            ("u_2", "v_2", "w_2", "t_2", "p", "ph_2", "mu_2", "pb", "phb", "t_init", "mub")]
+    qs = [np.ascontiguousarray(q, dtype=np.float64) for q in q_fields]
+    qp = (_DP * max(1, len(qs)))(*[q.ctypes.data_as(_DP) for q in qs])
+    f = SnapshotFields(*[a.ctypes.data_as(_DP) for a in keep], C.cast(qp, C.POINTER(_DP)))
+    na = names_array(q_names)
+    rc = lib.cw_snapshot_write_host(str(directory).encode(), step, time, C.byref(g), C.byref(o), C.byref(f),
+                                    na[0] if na else None)
+    if rc != 0:
+        raise RuntimeError(lib.cw_output_last_error().decode())
 
 
 def default_options(lib=None, **kw):

@@ -1,7 +1,7 @@
 // SPDX-License-Identifier: GPL-3.0-or-later
 // Host runtime of the dycore: handles (one or many domains), the device arena, the per-domain Dom
 // tables, the halo refresh sets, the RK3 step as a sequence of batched launches (captured once into a
-// CUDA graph and replayed), and the C ABI of include/cw_dycore.h.
+// CUDA graph and replayed), and the C ABI of include/cw_dycore.h (with cw_diagnostics of include/cw_output.h).
 //
 // The step order is CPPWRF's RK3::step (src/dyn/rk3.cpp:166-250): copy of the time-t state, then per RK
 // stage rk_step_prep, rk_tendency (+ stage-1 diffusion and boundary relaxation), the acoustic loop,
@@ -22,8 +22,10 @@
 #include <string>
 #include <vector>
 
+#include "../../include/cw_output.h"
 #include "cw_fields.hpp"
 #include "kernels_cb.cuh"
+#include "kernels_diag.cuh"
 
 namespace cw {
 
@@ -109,6 +111,8 @@ struct cw_handle {
   DevTables<float> t32;
   double* dtbc_d = nullptr;  // per member: time since the boundary data, advanced by the step on the device
   unsigned long long* diag = nullptr;  // cw_check_finite's result
+  double* diag_part = nullptr;         // cw_diagnostics' per-level partials
+  size_t diag_part_n = 0;
   double* staging = nullptr;  // FP32 field transfers: doubles converted on the device
   size_t staging_n = 0;
   int nzmax = 0;
@@ -1031,6 +1035,53 @@ __global__ void k_nonfinite(const T* __restrict__ p, int sj, int sk, int nx, int
   if (!isfinite(v)) atomicMin(out, base + (unsigned long long)t);
 }
 
+// cw_diagnostics of member mi: the per-level partials on the device, folded over the levels in order here
+// (Reducer::run's host loop, src/core/backend.hpp:857-859; Diagnostics::compute, src/dyn/diagnostics.cpp:56-80)
+template <class R>
+void diagnostics_t(cw_handle* h, int mi, DevTables<R>& T, cw_diag* out) {
+  size_t q0 = 0;
+  for (int m = 0; m < mi; ++m) q0 += size_t(h->m[size_t(m)].o.n_scalars);
+  const Dom<R> D = make_dom<R>(h, size_t(mi), T.qtab ? T.qtab + kQTab * q0 : nullptr, T.lbcq ? T.lbcq + q0 : nullptr);
+  const Member& M = h->m[size_t(mi)];
+  const int nz = M.g.nz, K1 = nz + 1;
+  const size_t need = size_t(DG_NPART) * size_t(K1);
+  if (h->diag_part_n < need) {
+    cudaFree(h->diag_part);
+    h->diag_part = nullptr;
+    h->diag_part_n = 0;
+    CW_CUDA(cudaMalloc(&h->diag_part, need * sizeof(double)));
+    h->diag_part_n = need;
+  }
+  constexpr double r_d = 287.0, r_v = 461.6, cp = 7.0 * r_d / 2.0;  // src/core/constants.hpp:5-14
+  const DiagConst c{r_v / r_d, r_d / cp, cp - r_d};
+  k_diag<R><<<dim3(unsigned(K1), 4), kDiagThreads, 0, h->stream>>>(D, c, h->diag_part);
+  CW_CUDA(cudaGetLastError());
+  std::vector<double> hp(need);
+  CW_CUDA(cudaMemcpyAsync(hp.data(), h->diag_part, need * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CW_CUDA(cudaStreamSynchronize(h->stream));
+  auto fold_max = [&](int q, int nk) {
+    double a = -1e308;
+    for (int k = 0; k < nk; ++k) a = hp[size_t(q) * K1 + k] > a ? hp[size_t(q) * K1 + k] : a;
+    return a;
+  };
+  auto fold_sum = [&](int q, int nk) {
+    double a = 0.0;
+    for (int k = 0; k < nk; ++k) a = a + hp[size_t(q) * K1 + k];
+    return a;
+  };
+  const double area = M.g.dx * (two_d(M.g) ? 1.0 : M.g.dy) / 9.81;
+  out->max_abs_u = fold_max(DG_MAX_U, nz);
+  out->max_abs_v = fold_max(DG_MAX_V, nz);
+  out->max_abs_w = fold_max(DG_MAX_W, nz + 1);
+  out->max_th_pert = fold_max(DG_MAX_THP, nz);
+  out->min_th_pert = -fold_max(DG_MAX_THM, nz);
+  out->dry_mass = area * fold_sum(DG_SUM_MASS, 1);
+  out->theta_mass = area * fold_sum(DG_SUM_THETA, nz);
+  out->total_energy = area * fold_sum(DG_SUM_ENERGY, nz);
+  const double mq = fold_max(DG_MAX_Q, nz);
+  out->max_abs_q = 0.0 < mq ? mq : 0.0;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ C ABI
@@ -1139,6 +1190,7 @@ int cw_destroy(cw_handle* h) {
   free_tables(h);
   cudaFree(h->staging);
   cudaFree(h->diag);
+  cudaFree(h->diag_part);
   for (Member& M : h->m) cudaFree(M.arena);
   if (h->own_stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -1149,6 +1201,15 @@ int cw_members(cw_handle* h, int* out) {
   if (!h || !out) return -1;
   *out = int(h->m.size());
   return 0;
+}
+
+int cw_member_config(cw_handle* h, int mi, cw_grid* g, cw_options* o) {
+  return guarded(h, [&] {
+    if (!h || mi < 0 || mi >= int(h->m.size())) throw std::runtime_error("member index out of range");
+    if (g) *g = h->m[size_t(mi)].g;
+    if (o) *o = h->m[size_t(mi)].o;
+    return 0;
+  });
 }
 
 int cw_member_set_vertical(cw_handle* h, int mi, const cw_vertical* v) {
@@ -1427,6 +1488,15 @@ int cw_check_finite(cw_handle* h, int mi, int* field, int* n, int* i, int* j, in
     if (j) *j = int((t / l.L.nx) % l.L.ny);
     if (k) *k = int(t / ((long long)l.L.nx * l.L.ny));
     return 1;
+  });
+}
+
+int cw_diagnostics(cw_handle* h, int mi, cw_diag* out) {
+  return guarded(h, [&] {
+    if (!h || !out || mi < 0 || mi >= int(h->m.size())) throw std::runtime_error("bad diagnostics arguments");
+    if (h->precision == CW_FP64) diagnostics_t<double>(h, mi, h->t64, out);
+    else diagnostics_t<float>(h, mi, h->t32, out);
+    return 0;
   });
 }
 

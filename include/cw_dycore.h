@@ -185,6 +185,8 @@ int cw_batch_adopt(cw_handle* h, cw_handle* single, int* member);
 /* Device bytes one domain takes in a handle (fields, work fields, scalars, slabs, vertical arrays): the
  * footprint the served form admits by. Needs no device. */
 int cw_footprint(const cw_grid* g, const cw_options* o, size_t* bytes);
+/* The grid and options a member was made with. */
+int cw_member_config(cw_handle* h, int member, cw_grid* g, cw_options* o);
 int cw_member_set_vertical(cw_handle* h, int member, const cw_vertical* v);
 int cw_member_upload(cw_handle* h, int member, int field, int n, const double* host, size_t count);
 int cw_member_download(cw_handle* h, int member, int field, int n, double* host, size_t count);

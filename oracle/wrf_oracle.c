@@ -2202,3 +2202,88 @@ int or_step(or_dom* d, int nsteps) {
   return 0;
 }
 const char* or_last_error(or_dom* d) { return d ? d->err : ""; }
+
+/* ------------------------------------------------------------------ diagnostics
+ * dyn::Diagnostics::compute (src/dyn/diagnostics.cpp:56-80) with the functors of :18-51, reduced in the
+ * reference CPU build's order (Reducer::run, src/core/backend.hpp:836-860): per level k a running sum from
+ * 0.0 over j (outer) and i (inner), or a running maximum from -1e308, then the levels folded in order. */
+#define RVOVRD (461.6 / 287.0)
+static double dg_absnan(double v) { return (v != v || v - v != 0.0) ? INFINITY : (v < 0 ? -v : v); }
+
+static double dg_max_abs(const fld* f, int nx, int ny, int nz) {
+  double acc = -1e308;
+  for (int k = 0; k < nz; ++k) {
+    double a = -1e308;
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const double v = dg_absnan(AT(f, i, j, k));
+        a = v > a ? v : a;
+      }
+    acc = a > acc ? a : acc;
+  }
+  return acc;
+}
+
+static double dg_thp(const or_dom* d, int i, int j, int k, double sign, int moist) {
+  double th = AT(&d->f[CW_T_2], i, j, k);
+  if (moist) th = (th + T0) / (1.0 + RVOVRD * AT(&d->q2[0], i, j, k)) - T0;
+  const double v = th - AT(&d->f[CW_T_INIT], i, j, k);
+  return v != v ? INFINITY : sign * v;
+}
+
+static double dg_energy(const or_dom* d, int i, int j, int k) {
+  const fld *u = &d->f[CW_U_2], *v = &d->f[CW_V_2], *w = &d->f[CW_W_2], *t = &d->f[CW_T_2], *p = &d->f[CW_P];
+  const fld *ph = &d->f[CW_PH_2], *mu = &d->f[CW_MU_2], *mub = &d->f[CW_MUB], *pb = &d->f[CW_PB], *phb = &d->f[CW_PHB];
+  const double m = d->c1h[k] * (AT(mu, i, j, 0) + AT(mub, i, j, 0)) + d->c2h[k];
+  const double uc = 0.5 * (AT(u, i, j, k) + AT(u, i + 1, j, k));
+  const double vc = 0.5 * (AT(v, i, j, k) + AT(v, i, j + 1, k));
+  const double wc = 0.5 * (AT(w, i, j, k) + AT(w, i, j, k + 1));
+  const double base = (AT(p, i, j, k) + AT(pb, i, j, k)) / P1000MB;
+  const double rcp = R_D / CP;
+  const double T = (AT(t, i, j, k) + T0) * (d->pow_mode == OR_POW_GLIBC ? pow(base, rcp) : cw_pow(base, rcp));
+  const double phm = 0.5 * (AT(ph, i, j, k) + AT(ph, i, j, k + 1) + AT(phb, i, j, k) + AT(phb, i, j, k + 1));
+  return -d->dnw[k] * m * (0.5 * (uc * uc + vc * vc + wc * wc) + CV * T + phm);
+}
+
+int or_diagnostics(or_dom* d, double out[9]) {
+  const cw_grid* g = &d->g;
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  out[0] = dg_max_abs(&d->f[CW_U_2], nxs(g, ST_U), ny, nz);
+  out[1] = dg_max_abs(&d->f[CW_V_2], nx, nys(g, ST_V), nz);
+  out[2] = dg_max_abs(&d->f[CW_W_2], nx, ny, nz + 1);
+  double mq = 0;
+  for (int n = 0; n < d->o.n_scalars; ++n) {
+    const double v = dg_max_abs(&d->q2[n], nx, ny, nz);
+    mq = mq < v ? v : mq;
+  }
+  out[8] = mq;
+  const int moist = d->o.n_moist > 0; /* species 0 is qv (State::P_QV) */
+  double mx = -1e308, mn = -1e308, sm = 0, se = 0;
+  for (int k = 0; k < nz; ++k) {
+    double a = -1e308, b = -1e308, s = 0.0, e = 0.0;
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const double vp = dg_thp(d, i, j, k, 1.0, moist), vm = dg_thp(d, i, j, k, -1.0, moist);
+        a = vp > a ? vp : a;
+        b = vm > b ? vm : b;
+        const double m = d->c1h[k] * (AT(&d->f[CW_MU_2], i, j, 0) + AT(&d->f[CW_MUB], i, j, 0)) + d->c2h[k];
+        s = s + -d->dnw[k] * m * (AT(&d->f[CW_T_2], i, j, k) + T0);
+        e = e + dg_energy(d, i, j, k);
+      }
+    mx = a > mx ? a : mx;
+    mn = b > mn ? b : mn;
+    sm = sm + s;
+    se = se + e;
+  }
+  double dm = 0.0, s0 = 0.0;
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) s0 = s0 + (AT(&d->f[CW_MU_2], i, j, 0) + AT(&d->f[CW_MUB], i, j, 0));
+  dm = dm + s0;
+  const double area = g->dx * (two_d(g) ? 1.0 : g->dy) / G_;
+  out[3] = -mn;
+  out[4] = mx;
+  out[5] = area * dm;
+  out[6] = area * sm;
+  out[7] = area * se;
+  return 0;
+}

@@ -38,6 +38,8 @@ int or_set_lbc_time(or_dom* d, double dtbc);
 void or_set_pow_mode(or_dom* d, int mode);
 int or_n_sound(or_dom* d);
 int or_step(or_dom* d, int nsteps);
+/* dyn::Diagnostics::compute: max|u| max|v| max|w| min th' max th' dry_mass theta_mass total_energy max|q| */
+int or_diagnostics(or_dom* d, double out[9]);
 const char* or_last_error(or_dom* d);
 
 #ifdef __cplusplus

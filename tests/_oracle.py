@@ -14,6 +14,9 @@ from cppwrf_b200 import capi
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_LIB = os.path.join(ROOT, "oracle", "lib", "liboracle.so")
 POW_OWN, POW_GLIBC = 0, 1
+# DiagRow (src/dyn/diagnostics.hpp:13-17), in the order of the diag.csv columns, then max_abs_q
+DIAG_KEYS = ("max_abs_u", "max_abs_v", "max_abs_w", "min_th_pert", "max_th_pert", "dry_mass", "theta_mass",
+             "total_energy", "max_abs_q")
 _lib = None
 
 
@@ -40,6 +43,7 @@ def load():
             ("or_set_pow_mode", None, [vp, i]),
             ("or_n_sound", i, [vp]),
             ("or_step", i, [vp, i]),
+            ("or_diagnostics", i, [vp, dp]),
         ]:
             f = getattr(lib, name)
             f.restype = res
@@ -105,6 +109,12 @@ class Oracle:
 
     def n_sound(self):
         return self.lib.or_n_sound(self.h)
+
+    def diagnostics(self):
+        """dyn::Diagnostics::compute of the current state: a dict of the DiagRow values."""
+        out = (C.c_double * 9)()
+        self.lib.or_diagnostics(self.h, out)
+        return dict(zip(DIAG_KEYS, list(out)))
 
 
 def snapshot_vars(get, layout, g, base_get, base_layout):

@@ -27,6 +27,16 @@ def golden_config(name):
     return dict(GOLDEN["cases"][name]["config"])
 
 
+def lam_case(nx=24, ny=20, nz=14, seed=3, n_moist=5, n_scalars=5, diff=False, hybrid_opt=2, precision=capi.FP64):
+    """A limited-area case (terrain, hybrid coordinate, moist species, specified boundaries) from a seed."""
+    g = capi.grid(nx, ny, nz, 15000.0, 90.0, 0.0, dy=15000.0, p_top=5000.0, bc_x=capi.SPECIFIED, bc_y=capi.SPECIFIED)
+    o = capi.default_options(None, flat=0, n_moist=n_moist, n_scalars=n_scalars, lbc=1, time_step_sound=4,
+                             precision=precision)
+    if diff:
+        o.diff_opt, o.khdif, o.kvdif, o.pr_inv = 1, 3000.0, 1.0, 3.0
+    return capi.Case(g, o).gen_lam(seed=seed, hybrid_opt=hybrid_opt)
+
+
 # small variants for quick parity runs (same physics as the goldens, fewer points)
 SMALL = {
     "straka_small": dict(golden_config("straka"), nx=64, nz=32, ztop=3200.0, run_time=3.0),

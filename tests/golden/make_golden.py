@@ -3,9 +3,10 @@
 
 CPPWRF ships, for each ideal case, the end state of its CPU FP64 build after two steps
 (tools/regression/golden/<case>_cpu_fp64/snap_000002.{json,bin}, runs made by
-tools/regression/run.sh --quick; run lengths at run.sh:146-150). This script records, per variable
-of each snapshot, the SHA-256 of its little-endian float64 bytes in the snapshot's (k, j, i) order
-plus its shape and a few sample values, together with the case's configuration
+tools/regression/run.sh --quick; run lengths at run.sh:146-150) and the run's diag.csv (one row per
+step, io::DiagWriter). This script records, per variable of each snapshot, the SHA-256 of its
+little-endian float64 bytes in the snapshot's (k, j, i) order plus its shape and a few sample values,
+the snapshot's JSON text and the diag.csv lines verbatim, together with the case's configuration
 (configs/<case>.ini). The oracle test recomputes the same variables and compares hashes, which is a
 bit-for-bit comparison without committing megabytes of binary data.
 
@@ -54,7 +55,10 @@ def main():
                 "sum": float(a.sum()),
                 "samples": [float(x) for x in a.ravel()[:: max(1, a.size // 7)][:8]],
             }
-        out["cases"][name] = {"config": cfg, "step": meta["step"], "time": meta["time"], "variables": vars_}
+        snap_json = open(os.path.join(d, "snap_000002.json")).read()
+        diag_csv = open(os.path.join(d, "diag.csv")).read().splitlines()
+        out["cases"][name] = {"config": cfg, "step": meta["step"], "time": meta["time"], "variables": vars_,
+                              "snap_json": snap_json, "diag_csv": diag_csv}
     path = os.path.join(HERE, "reference_snapshots.json")
     json.dump(out, open(path, "w"), indent=1)
     print("wrote", path)

@@ -6,7 +6,7 @@ import pytest
 
 import _oracle
 from cppwrf_b200 import Batch, Domain, capi
-from test_parity_gpu import lam_case
+from cases import lam_case
 
 pytestmark = pytest.mark.gpu
 

@@ -12,17 +12,10 @@ import _oracle
 import _refpath  # noqa: F401
 import refdump as _refdump
 import cases
+from cases import lam_case
 from cppwrf_b200 import capi
 
 pytestmark = pytest.mark.skipif(not _refdump.available(), reason="reference sources / oracle/_ref not present")
-
-
-def lam_case(nx=24, ny=20, nz=14, seed=3, n_moist=5, n_scalars=5, diff=False, hybrid_opt=2):
-    g = capi.grid(nx, ny, nz, 15000.0, 90.0, 0.0, dy=15000.0, p_top=5000.0, bc_x=capi.SPECIFIED, bc_y=capi.SPECIFIED)
-    o = capi.default_options(None, flat=0, n_moist=n_moist, n_scalars=n_scalars, lbc=1, time_step_sound=4)
-    if diff:
-        o.diff_opt, o.khdif, o.kvdif, o.pr_inv = 1, 3000.0, 1.0, 3.0
-    return capi.Case(g, o).gen_lam(seed=seed, hybrid_opt=hybrid_opt)
 
 
 def compare(orc, ref, case):

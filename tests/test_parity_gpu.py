@@ -7,6 +7,7 @@ import pytest
 
 import _oracle
 import cases
+from cases import lam_case
 from cppwrf_b200 import Domain, capi
 
 pytestmark = pytest.mark.gpu
@@ -67,15 +68,6 @@ def test_graph_and_eager_identical():
     b.step(2)
     for name in ("U_2", "W_2", "T_2", "PH_2", "MU_2", "P"):
         assert np.array_equal(a.field(name), b.field(name)), name
-
-
-def lam_case(nx=24, ny=20, nz=14, seed=3, n_moist=5, n_scalars=5, diff=False, hybrid_opt=2, precision=capi.FP64):
-    g = capi.grid(nx, ny, nz, 15000.0, 90.0, 0.0, dy=15000.0, p_top=5000.0, bc_x=capi.SPECIFIED, bc_y=capi.SPECIFIED)
-    o = capi.default_options(None, flat=0, n_moist=n_moist, n_scalars=n_scalars, lbc=1, time_step_sound=4,
-                             precision=precision)
-    if diff:
-        o.diff_opt, o.khdif, o.kvdif, o.pr_inv = 1, 3000.0, 1.0, 3.0
-    return capi.Case(g, o).gen_lam(seed=seed, hybrid_opt=hybrid_opt)
 
 
 @pytest.mark.parametrize("kw", [dict(), dict(diff=True), dict(hybrid_opt=0, seed=5), dict(n_moist=2, n_scalars=3),

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from cppwrf_b200 import Domain, capi
-from test_parity_gpu import lam_case
+from cases import lam_case
 
 pytestmark = pytest.mark.gpu
 
