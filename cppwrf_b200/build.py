@@ -2,8 +2,8 @@
 """Builds libcw_dycore.so in-tree (cppwrf_b200/lib/) with nvcc for sm_100a.
 
 The FP64 form must round every operation as the reference's CPU build does: --fmad=false (no FMA
-contraction), IEEE division and square root (nvcc's defaults, asserted below by the absence of any
-fast-math flag), and -ffp-contract=off for the host compiler.
+contraction), IEEE division and square root (nvcc's defaults: no fast-math flag in FLAGS), and
+-ffp-contract=off for the host compiler. The mixed form's step is a separate translation unit with MIXED_FLAGS.
 """
 import os
 import subprocess
@@ -17,7 +17,11 @@ CXX = os.environ.get("CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++20", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off",
          "-Xptxas", "-warn-spills", "--expt-relaxed-constexpr"]
-SOURCES = ["cw_runtime.cu", "cw_case.cpp", "cw_serve.cpp", "cw_output.cpp"]
+SOURCES = ["cw_runtime.cu", "cw_step_mixed.cu", "cw_case.cpp", "cw_serve.cpp", "cw_output.cpp"]
+# The mixed form's kernels (their own translation unit) are held to a tolerance, not to bit identity: FMA
+# contraction, approximate single-precision division and square root, single-precision denormals flushed.
+MIXED_FLAGS = [f for f in FLAGS if f != "--fmad=false"] + ["--fmad=true", "--prec-div=false", "--prec-sqrt=false",
+                                                           "-ftz=true"]
 
 
 def build(verbose=False):
@@ -25,7 +29,8 @@ def build(verbose=False):
     objs = []
     for src in SOURCES:
         obj = os.path.join(HERE, "lib", os.path.splitext(src)[0] + ".o")
-        cmd = [NVCC] + ARCH + FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
+        flags = MIXED_FLAGS if src == "cw_step_mixed.cu" else FLAGS
+        cmd = [NVCC] + ARCH + flags + ["-c", os.path.join(CSRC, src), "-o", obj]
         if src.endswith(".cpp"):
             cmd = [CXX, "-std=c++20", "-O3", "-fPIC", "-ffp-contract=off", "-fopenmp", "-c", os.path.join(CSRC, src),
                    "-o", obj]

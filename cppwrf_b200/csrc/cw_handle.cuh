@@ -1,0 +1,173 @@
+// SPDX-License-Identifier: GPL-3.0-or-later
+// The handle of the dycore's host runtime: its members (domains), device tables, halo sets and step state,
+// shared by the translation units that enqueue the step (cw_runtime.cu: the FP64 form; cw_step_mixed.cu: the
+// mixed form).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <utility>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/cw_output.h"
+#include "cw_fields.hpp"
+#include "kernels_cb.cuh"
+#include "kernels_diag.cuh"
+
+namespace cw {
+
+#define CW_CUDA(x)                                                                          \
+  do {                                                                                      \
+    cudaError_t e_ = (x);                                                                   \
+    if (e_ != cudaSuccess) throw std::runtime_error(std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
+
+// the work fields of one domain beyond State / Tendencies / BaseState (SmallStep's fields)
+enum Work { W_U_SAVE, W_V_SAVE, W_W_SAVE, W_T_SAVE, W_PH_SAVE, W_WW1, W_C2A, W_PM1, W_T_2SAVE, W_A, W_ALPHA, W_GAMMA,
+            W_MU_SAVE, W_MUDF, W_MUAVE, W_W_RHS, W_T2A, W_N };
+inline FieldKind work_kind(int w) {
+  switch (w) {
+    case W_U_SAVE: return {'U', 3, false};
+    case W_V_SAVE: return {'V', 3, false};
+    case W_W_SAVE: case W_PH_SAVE: case W_WW1: case W_A: case W_ALPHA: case W_GAMMA: case W_W_RHS: return {'W', 3, false};
+    case W_MU_SAVE: case W_MUDF: case W_MUAVE: return {'M', 2, false};
+    default: return {'M', 3, false};
+  }
+}
+
+struct Member {
+  cw_grid g{};
+  cw_options o{};
+  int n_sound = 0;
+  int esz = 8;  // element size of the fields (8: FP64 form, 4: mixed form)
+  std::vector<cw_layout> L;         // CW_U_1 .. CW_COSA
+  std::vector<char*> base;          // allocation of each field
+  std::vector<cw_layout> LW;
+  std::vector<char*> wbase;
+  cw_layout Lq{};
+  std::vector<char*> q1, qa, qb, qtf, qsc;  // scalar allocations; q_2 is qa or qb by the parity
+  std::vector<char*> qpd;                    // PD face fluxes, 6 per species (dh, lo on x, y, z faces), when PD
+  cw_layout Lpd[3]{};                        // their layouts: U, V, W staggering
+  double* vert = nullptr;           // device 1-D arrays (double)
+  size_t vert_off[24]{};
+  char* slab[5] = {};               // LBC slabs per variable (values 4 sides, tendencies 4 sides)
+  size_t slab_off[5][8]{};
+  std::vector<char*> qslab;
+  std::vector<std::array<size_t, 8>> qslab_off;
+  std::vector<char> q_have;
+  double dtbc = 0;
+  int q_parity = 0;
+  char* arena = nullptr;  // the member's device allocation (every pointer above points into it)
+  size_t arena_bytes = 0;
+  double cf1 = 0, cf2 = 0, cf3 = 0, cfn = 0, cfn1 = 0, rdx = 0, rdy = 0;
+};
+
+// the members' kernel parameter packs and each pack's block count per index range
+template <class R, int NM>
+struct Packs {
+  std::vector<Pack<R, NM>> p;
+  std::vector<std::array<std::array<int, kNumShapes>, kNumKinds>> blocks;  // [pack][kind][shape]
+};
+template <class R>
+struct DevTables {  // the kernels' views of the members and the device scalar tables
+  Packs<R, 1> one;              // a single domain
+  Packs<R, kPackMembers> many;  // a batch, in packs of kPackMembers
+  V3<R>* qtab = nullptr;  // per member: q1, q2, qn, qtf, qscale, 6 PD faces (kQTab x n_scalars)
+  Slabs<R>* lbcq = nullptr;
+};
+
+struct HaloSetHost {
+  std::vector<HaloField> f;
+  std::vector<HaloChunk<kHaloSmall>> small;  // the fields in one small chunk (most single domains), or
+  std::vector<HaloChunk<kHaloLarge>> large;  // in large chunks
+};
+
+}  // namespace cw
+
+using namespace cw;
+
+struct cw_handle {
+  int precision = CW_FP64;
+  std::vector<Member> m;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  DevTables<double> t64;
+  DevTables<float> t32;
+  double* dtbc_d = nullptr;  // per member: time since the boundary data, advanced by the step on the device
+  unsigned long long* diag = nullptr;  // cw_check_finite's result
+  double* diag_part = nullptr;         // cw_diagnostics' per-level partials
+  size_t diag_part_n = 0;
+  double* staging = nullptr;  // FP32 field transfers: doubles converted on the device
+  size_t staging_n = 0;
+  int nzmax = 0;
+  size_t cb_level_bytes = 0;  // one shared level array of a column block: (nz + 2) x CX doubles
+  // halo sets of the fill points
+  enum { H_MU1, H_PREP0, H_PREP1, H_SS0, H_UV, H_AC, H_POST, H_FIN, H_Q1PD, H_SCPD, H_Q2, H_END_P, H_WS0, H_WS1, H_N };
+  HaloSetHost hs[H_N];
+  std::vector<CopyDesc> copies;
+  CopyDesc* copies_d = nullptr;
+  long long* copies_start_d = nullptr;
+  long long copies_total = 0;
+  std::vector<CopyDesc> zeros;  // mudf reset
+  CopyDesc* zeros_d = nullptr;
+  long long* zeros_start_d = nullptr;
+  long long zeros_total = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  bool graph_ok = false;
+  bool use_graph = true;
+  long long launches_step = 0;   // launches of one step
+  long long launches_last = 0;   // launches of the last cw_step call
+  std::string err;
+  std::vector<void*> extra;      // other device allocations
+  // per-kernel timing of eager steps (cw_profile): events around each launch
+  // block-shape autotuning of the point kernels: the first kNumShapes steps each run every tunable kernel
+  // with one shape (eager, timed per launch); then each kernel keeps its fastest shape
+  bool autotune = false, tuned = false;
+  int tuning_shape = -1, tune_steps_done = 0;
+  std::vector<std::pair<std::string, int>> shape_choice;
+  std::vector<std::pair<std::string, std::array<double, kNumShapes>>> tune_ms;
+  bool profiling = false;
+  std::vector<std::pair<const char*, std::pair<cudaEvent_t, cudaEvent_t>>> prof_ev;
+  std::vector<std::string> prof_names;
+  std::vector<double> prof_ms;
+  std::vector<long long> prof_n;
+};
+
+namespace cw {
+
+// a fill point's fields in launch chunks of NF descriptors
+template <int NF>
+void chunk_fields(const std::vector<HaloField>& f, std::vector<HaloChunk<NF>>& out) {
+  for (size_t f0 = 0; f0 < f.size(); f0 += NF) {
+    HaloChunk<NF> c{};
+    c.nf = int(std::min(f.size() - f0, size_t(NF)));
+    long long total = 0;
+    for (int n = 0; n < c.nf; ++n) {
+      c.f[n] = f[f0 + size_t(n)];
+      c.start[n] = unsigned(total);
+      total += c.f[n].ncell;
+      c.has_oddface |= c.f[n].oddface_x;
+    }
+    if (total >= (1ll << 31)) throw std::runtime_error("a halo fill of more than 2^31 cells");
+    c.start[c.nf] = unsigned(total);
+    out.push_back(c);
+  }
+}
+
+// the mixed form's step (cw_step_mixed.cu): enqueues one step of h on its stream, returns the launches
+long long enqueue_mixed(cw_handle* h);
+
+}  // namespace cw

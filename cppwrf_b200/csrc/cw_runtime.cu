@@ -8,147 +8,7 @@
 // small_step_finish, scalar transport and calc_p_rho_phi; spec_bdy_final and set_w_surface at the end.
 // Halos are refreshed where the reference refreshes them; refreshes with no kernel in between that
 // reads the refreshed cells are merged into one launch.
-#include <cuda_runtime.h>
-
-#include <algorithm>
-#include <array>
-#include <atomic>
-#include <utility>
-#include <cstdio>
-#include <cstring>
-#include <memory>
-#include <mutex>
-#include <stdexcept>
-#include <string>
-#include <vector>
-
-#include "../../include/cw_output.h"
-#include "cw_fields.hpp"
-#include "kernels_cb.cuh"
-#include "kernels_diag.cuh"
-
-namespace cw {
-
-#define CW_CUDA(x)                                                                          \
-  do {                                                                                      \
-    cudaError_t e_ = (x);                                                                   \
-    if (e_ != cudaSuccess) throw std::runtime_error(std::string(#x) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
-constexpr size_t kAlign = 256;
-inline size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
-
-// the work fields of one domain beyond State / Tendencies / BaseState (SmallStep's fields)
-enum Work { W_U_SAVE, W_V_SAVE, W_W_SAVE, W_T_SAVE, W_PH_SAVE, W_WW1, W_C2A, W_PM1, W_T_2SAVE, W_A, W_ALPHA, W_GAMMA,
-            W_MU_SAVE, W_MUDF, W_MUAVE, W_W_RHS, W_T2A, W_N };
-inline FieldKind work_kind(int w) {
-  switch (w) {
-    case W_U_SAVE: return {'U', 3, false};
-    case W_V_SAVE: return {'V', 3, false};
-    case W_W_SAVE: case W_PH_SAVE: case W_WW1: case W_A: case W_ALPHA: case W_GAMMA: case W_W_RHS: return {'W', 3, false};
-    case W_MU_SAVE: case W_MUDF: case W_MUAVE: return {'M', 2, false};
-    default: return {'M', 3, false};
-  }
-}
-
-struct Member {
-  cw_grid g{};
-  cw_options o{};
-  int n_sound = 0;
-  int esz = 8;  // element size of the fields (8: FP64 form, 4: mixed form)
-  std::vector<cw_layout> L;         // CW_U_1 .. CW_COSA
-  std::vector<char*> base;          // allocation of each field
-  std::vector<cw_layout> LW;
-  std::vector<char*> wbase;
-  cw_layout Lq{};
-  std::vector<char*> q1, qa, qb, qtf, qsc;  // scalar allocations; q_2 is qa or qb by the parity
-  std::vector<char*> qpd;                    // PD face fluxes, 6 per species (dh, lo on x, y, z faces), when PD
-  cw_layout Lpd[3]{};                        // their layouts: U, V, W staggering
-  double* vert = nullptr;           // device 1-D arrays (double)
-  size_t vert_off[24]{};
-  char* slab[5] = {};               // LBC slabs per variable (values 4 sides, tendencies 4 sides)
-  size_t slab_off[5][8]{};
-  std::vector<char*> qslab;
-  std::vector<std::array<size_t, 8>> qslab_off;
-  std::vector<char> q_have;
-  double dtbc = 0;
-  int q_parity = 0;
-  char* arena = nullptr;  // the member's device allocation (every pointer above points into it)
-  size_t arena_bytes = 0;
-  double cf1 = 0, cf2 = 0, cf3 = 0, cfn = 0, cfn1 = 0, rdx = 0, rdy = 0;
-};
-
-// the members' kernel parameter packs and each pack's block count per index range
-template <class R, int NM>
-struct Packs {
-  std::vector<Pack<R, NM>> p;
-  std::vector<std::array<std::array<int, kNumShapes>, kNumKinds>> blocks;  // [pack][kind][shape]
-};
-template <class R>
-struct DevTables {  // the kernels' views of the members and the device scalar tables
-  Packs<R, 1> one;              // a single domain
-  Packs<R, kPackMembers> many;  // a batch, in packs of kPackMembers
-  V3<R>* qtab = nullptr;  // per member: q1, q2, qn, qtf, qscale, 6 PD faces (kQTab x n_scalars)
-  Slabs<R>* lbcq = nullptr;
-};
-
-struct HaloSetHost {
-  std::vector<HaloField> f;
-  std::vector<HaloChunk<kHaloSmall>> small;  // the fields in one small chunk (most single domains), or
-  std::vector<HaloChunk<kHaloLarge>> large;  // in large chunks
-};
-
-}  // namespace cw
-
-using namespace cw;
-
-struct cw_handle {
-  int precision = CW_FP64;
-  std::vector<Member> m;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  DevTables<double> t64;
-  DevTables<float> t32;
-  double* dtbc_d = nullptr;  // per member: time since the boundary data, advanced by the step on the device
-  unsigned long long* diag = nullptr;  // cw_check_finite's result
-  double* diag_part = nullptr;         // cw_diagnostics' per-level partials
-  size_t diag_part_n = 0;
-  double* staging = nullptr;  // FP32 field transfers: doubles converted on the device
-  size_t staging_n = 0;
-  int nzmax = 0;
-  size_t cb_level_bytes = 0;  // one shared level array of a column block: (nz + 2) x CX doubles
-  // halo sets of the fill points
-  enum { H_MU1, H_PREP0, H_PREP1, H_SS0, H_UV, H_AC, H_POST, H_FIN, H_Q1PD, H_SCPD, H_Q2, H_END_P, H_WS0, H_WS1, H_N };
-  HaloSetHost hs[H_N];
-  std::vector<CopyDesc> copies;
-  CopyDesc* copies_d = nullptr;
-  long long* copies_start_d = nullptr;
-  long long copies_total = 0;
-  std::vector<CopyDesc> zeros;  // mudf reset
-  CopyDesc* zeros_d = nullptr;
-  long long* zeros_start_d = nullptr;
-  long long zeros_total = 0;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t gexec = nullptr;
-  bool graph_ok = false;
-  bool use_graph = true;
-  long long launches_step = 0;   // launches of one step
-  long long launches_last = 0;   // launches of the last cw_step call
-  std::string err;
-  std::vector<void*> extra;      // other device allocations
-  // per-kernel timing of eager steps (cw_profile): events around each launch
-  // block-shape autotuning of the point kernels: the first kNumShapes steps each run every tunable kernel
-  // with one shape (eager, timed per launch); then each kernel keeps its fastest shape
-  bool autotune = false, tuned = false;
-  int tuning_shape = -1, tune_steps_done = 0;
-  std::vector<std::pair<std::string, int>> shape_choice;
-  std::vector<std::pair<std::string, std::array<double, kNumShapes>>> tune_ms;
-  bool profiling = false;
-  std::vector<std::pair<const char*, std::pair<cudaEvent_t, cudaEvent_t>>> prof_ev;
-  std::vector<std::string> prof_names;
-  std::vector<double> prof_ms;
-  std::vector<long long> prof_n;
-};
+#include "cw_step.cuh"
 
 namespace {
 thread_local std::string g_create_err;
@@ -487,23 +347,6 @@ HaloField halo_field(const Member& M, const HaloItem& it) {
   return f;
 }
 
-template <int NF>
-void chunk_fields(const std::vector<HaloField>& f, std::vector<HaloChunk<NF>>& out) {
-  for (size_t f0 = 0; f0 < f.size(); f0 += NF) {
-    HaloChunk<NF> c{};
-    c.nf = int(std::min(f.size() - f0, size_t(NF)));
-    long long total = 0;
-    for (int n = 0; n < c.nf; ++n) {
-      c.f[n] = f[f0 + size_t(n)];
-      c.start[n] = unsigned(total);
-      total += c.f[n].ncell;
-      c.has_oddface |= c.f[n].oddface_x;
-    }
-    if (total >= (1ll << 31)) throw std::runtime_error("a halo fill of more than 2^31 cells");
-    c.start[c.nf] = unsigned(total);
-    out.push_back(c);
-  }
-}
 void finish_haloset(cw_handle*, HaloSetHost& s) {
   s.small.clear();
   s.large.clear();
@@ -581,224 +424,11 @@ void build_copies(cw_handle* h) {
 }
 
 // ---- the step
-struct Launcher {
-  cw_handle* h;
-  long long count = 0;
-  cudaEvent_t ev0 = nullptr;
-  void begin(const char* name) {
-    if (!h->profiling) return;
-    cudaEvent_t a, b;
-    CW_CUDA(cudaEventCreate(&a));
-    CW_CUDA(cudaEventCreate(&b));
-    CW_CUDA(cudaEventRecord(a, h->stream));
-    h->prof_ev.push_back({name, {a, b}});
-  }
-  void check() {
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) throw std::runtime_error(std::string("kernel launch: ") + cudaGetErrorString(e));
-    if (h->profiling) CW_CUDA(cudaEventRecord(h->prof_ev.back().second.second, h->stream));
-    ++count;
-  }
-  template <int NF>
-  void halo_chunks(const std::vector<HaloChunk<NF>>& chunks) {
-    for (const HaloChunk<NF>& c : chunks) {
-      const unsigned total = c.start[c.nf];
-      if (total == 0) continue;
-      const int bs = 256;
-      const unsigned nb = (total + bs - 1) / bs;
-      begin("k_halo");
-      k_halo<NF><<<nb, bs, 0, h->stream>>>(c, 0);
-      check();
-      if (c.has_oddface) {
-        begin("k_halo");
-        k_halo<NF><<<nb, bs, 0, h->stream>>>(c, 1);
-        check();
-      }
-    }
-  }
-  // halo fill points are deferred until the next kernel: consecutive fill points (nothing launched between
-  // them) become one launch over the union of their fields
-  std::vector<int> pend;
-  void halo(int set) { pend.push_back(set); }
-  void flush() {
-    if (pend.empty()) return;
-    if (pend.size() == 1) {
-      halo_chunks(h->hs[pend[0]].small);
-      halo_chunks(h->hs[pend[0]].large);
-    } else {
-      std::vector<HaloField> f;
-      for (int set : pend)
-        for (const HaloField& x : h->hs[set].f) {
-          bool dup = false;
-          for (const HaloField& y : f) dup |= y.p == x.p && y.ind == x.ind;
-          if (!dup) f.push_back(x);
-        }
-      if (f.size() <= size_t(kHaloSmall)) {
-        std::vector<HaloChunk<kHaloSmall>> c;
-        chunk_fields(f, c);
-        halo_chunks(c);
-      } else {
-        std::vector<HaloChunk<kHaloLarge>> c;
-        chunk_fields(f, c);
-        halo_chunks(c);
-      }
-    }
-    pend.clear();
-  }
-  void copy_list(CopyDesc* d, long long* sd, size_t n, long long total) {
-    flush();
-    if (!total) return;
-    const int bs = 256;
-    begin("k_copy");
-    k_copy<<<unsigned((total + bs - 1) / bs), bs, 0, h->stream>>>(d, int(n), sd);
-    check();
-  }
-  // the block shape of a point kernel: the one being timed while tuning, else the tuned choice (0 by default)
-  int shape_for(const char* name) const {
-    if (h->tuning_shape >= 0) return h->tuning_shape;
-    for (const auto& [n, sh] : h->shape_choice)
-      if (n == name) return sh;
-    return 0;
-  }
-  // a point kernel of fixed shape 0 over the index range kind, one launch per pack
-  template <class R, int NM, class K, class... Args>
-  void run(const char* name, int kind, K kern, const Packs<R, NM>& ps, Args... args) {
-    flush();
-    for (size_t c = 0; c < ps.p.size(); ++c) {
-      const int nb = ps.blocks[c][size_t(kind)][0];
-      if (nb == 0) continue;
-      begin(name);
-      kern<<<nb, PX, 0, h->stream>>>(ps.p[c], args...);
-      check();
-    }
-  }
-  // a point kernel with a tunable block shape (one instantiation per shape), nq > 0: once per species
-  template <class R, int NM, class K, class... Args>
-  void run_t(const char* name, int kind, int nq, const std::array<K, kNumShapes>& kerns, const Packs<R, NM>& ps,
-             Args... args) {
-    flush();
-    const int sh = shape_for(name);
-    for (size_t c = 0; c < ps.p.size(); ++c) {
-      const int nb = ps.blocks[c][size_t(kind)][size_t(sh)];
-      if (nb == 0 || nq == 0) continue;
-      begin(name);
-      kerns[size_t(sh)]<<<dim3(nb, nq), PX, 0, h->stream>>>(ps.p[c], args...);
-      check();
-    }
-  }
-  // a column-block kernel using `arrays` shared level arrays
-  template <class R, int NM, class K, class... Args>
-  void run_cb(const char* name, int kind, int arrays, K kern, const Packs<R, NM>& ps, Args... args) {
-    flush();
-    static_assert(CX == 32, "a column block's lanes are one warp");
-    const size_t smem = size_t(arrays) * h->cb_level_bytes;
-    CW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    for (size_t c = 0; c < ps.p.size(); ++c) {
-      const int nb = ps.blocks[c][size_t(kind)][0];
-      if (nb == 0) continue;
-      begin(name);
-      kern<<<nb, dim3(CX, CNW), smem, h->stream>>>(ps.p[c], args...);
-      check();
-    }
-  }
-  // one block per member
-  template <class R, int NM, class K>
-  void run_members(const char* name, int threads, K kern, const Packs<R, NM>& ps) {
-    flush();
-    for (size_t c = 0; c < ps.p.size(); ++c) {
-      begin(name);
-      kern<<<unsigned(ps.p[c].n), threads, 0, h->stream>>>(ps.p[c]);
-      check();
-    }
-  }
-};
-
-// the three block-shape instantiations of a tunable point kernel
-#define KV(kern) std::array{kern<R, NM, 0>, kern<R, NM, 1>, kern<R, NM, 2>}
-
-template <class R, int NM>
-void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
-  const Member& M0 = h->m[0];
-  bool lbc = false, terrain = false, scalars = false, any_pd = false;
-  // every member specified on all four sides: the acoustic substeps read no halo cell of the fields the
-  // per-substep fills (H_SS0, H_UV, H_AC) would refresh (the faces next to the boundary are the spec
-  // zone's, updated from the boundary data), and the fills after the substeps (H_POST, H_FIN) refresh them
-  // before anything reads them; those fills, and the spec zone's zero-gradient w of every substep but the
-  // last (overwritten by the next one, read only after the substeps), are left out
-  bool spec_all = true;
-  int nq = 0;  // the most species of a member
-  for (const Member& M : h->m) {
-    spec_all &= M.o.lbc != 0 && flat_x(M.g) && flat_y(M.g) && !two_d(M.g);
-    nq = std::max(nq, M.o.n_scalars);
-    lbc |= M.o.lbc != 0;
-    terrain |= !M.o.flat;
-    scalars |= M.o.n_scalars > 0;
-    for (int n = 0; n < M.o.n_scalars; ++n)
-      any_pd |= (n < M.o.n_moist ? M.o.moist_adv_opt : M.o.scalar_adv_opt) == 1;
-  }
-  const int n_sound = M0.n_sound;
-  if (lbc) {
-    L.run_members("k_advance_time", 1, k_advance_time<R, NM>, d);
-  }
-  L.copy_list(h->copies_d, h->copies_start_d, h->copies.size(), h->copies_total);
-  L.halo(cw_handle::H_MU1);
-  for (int rk = 1; rk <= 3; ++rk) {
-    const int ns = rk == 1 ? 1 : (rk == 2 ? n_sound / 2 : n_sound);
-    L.halo(cw_handle::H_PREP0);
-    L.run_cb("k_ls_prep", RG_COLS_STAG, 1, k_ls_prep<R, NM>, d);
-    L.halo(cw_handle::H_PREP1);
-    if (rk == 1) L.run_t("k_tendf_rk1", RG_STAG, 1, KV(k_tendf_rk1), d);
-    L.run_t("k_tend", RG_STAG, 1, KV(k_tend), d, rk);
-    if (rk == 1) L.copy_list(h->zeros_d, h->zeros_start_d, h->zeros.size(), h->zeros_total);
-    L.run_cb("k_ss_prep", RG_COLS_STAG, 3, k_ss_prep<R, NM>, d, rk);
-    if (!spec_all) L.halo(cw_handle::H_SS0);
-    for (int it = 1; it <= ns; ++it) {
-      L.run_t("k_uv", RG_STAG, 1, KV(k_uv), d, rk);
-      if (!spec_all) L.halo(cw_handle::H_UV);
-      L.run_cb("k_ac", RG_COLS_STAG, kCbArrays, k_ac<R, NM>, d, rk, it, ns);
-      if (lbc && (!spec_all || it == ns)) L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_ZERO_GRAD_W), rk);
-      if (!spec_all) L.halo(cw_handle::H_AC);
-    }
-    L.halo(cw_handle::H_POST);
-    L.run_cb("k_finish", RG_COLS_STAG, 0, k_finish<R, NM>, d, rk, ns);
-    L.halo(cw_handle::H_FIN);
-    if (scalars) {
-      if (rk == 1) L.run_t("k_q_tendf_rk1", RG_MASS, nq, KV(k_q_tendf_rk1), d);
-      L.run_t("k_q_update", RG_MASS, nq, KV(k_q_update), d, rk);
-      if (rk == 3 && any_pd) {
-        L.run_t("k_q_pre_pd", RG_MASS, nq, KV(k_q_pre_pd), d, rk);
-        L.halo(cw_handle::H_Q1PD);
-        L.run_t("k_q_face_pd", RG_STAG, 1, KV(k_q_face_pd), d, rk);
-        L.run_t("k_q_scale_pd", RG_MASS, nq, KV(k_q_scale_pd), d, rk);
-        L.halo(cw_handle::H_SCPD);
-        L.run_t("k_q_update_pd", RG_MASS, nq, KV(k_q_update_pd), d, rk);
-      }
-      L.run_members("k_q_swap", 64, k_q_swap<R, NM>, d);
-      if (lbc) L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_FLOW_DEP), rk);
-      L.halo(cw_handle::H_Q2);
-    }
-  }
-  if (lbc) {
-    L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_FINAL), 3);
-    L.run_t("k_p_rho_phi", RG_MASS, 1, KV(k_p_rho_phi), d, 1);
-    L.halo(cw_handle::H_END_P);
-  }
-  if (terrain) {
-    L.halo(cw_handle::H_WS0);
-    L.run_cb("k_w_surface", RG_COLS_MASS, 0, k_w_surface<R, NM>, d);
-    L.halo(cw_handle::H_WS1);
-  }
-  L.flush();
-}
-
-template <class R>
-void enqueue_t(cw_handle* h, Launcher& L, const DevTables<R>& T) {
-  if (h->m.size() == 1) enqueue_step<R, 1>(h, L, T.one);
-  else enqueue_step<R, kPackMembers>(h, L, T.many);
-}
+// the FP64 form's kernels are instantiated in this file (compiled without FMA contraction); the mixed form's in
+// cw_step_mixed.cu, compiled with its own floating-point options
 void enqueue(cw_handle* h, Launcher& L) {
   if (h->precision == CW_FP64) enqueue_t<double>(h, L, h->t64);
-  else enqueue_t<float>(h, L, h->t32);
+  else L.count += enqueue_mixed(h);
 }
 
 void invalidate_graph(cw_handle* h) {

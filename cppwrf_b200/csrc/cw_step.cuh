@@ -1,0 +1,232 @@
+// SPDX-License-Identifier: GPL-3.0-or-later
+// The RK3 step as a sequence of batched launches (CPPWRF's RK3::step, src/dyn/rk3.cpp:166-250): the launcher
+// (deferred and merged halo fills, per-kernel profiling and block-shape selection) and the step's launch order.
+//
+// Included by the two translation units that instantiate the step's kernels, each for its own precision under
+// its own floating-point options: cw_runtime.cu (FP64, no FMA contraction, IEEE division: bit-identical to the
+// reference's CPU build) and cw_step_mixed.cu (FP32 fields). Everything here has internal linkage, so that each
+// unit's launches refer to the kernels it compiled.
+#pragma once
+
+#include "cw_handle.cuh"
+
+namespace {
+using namespace cw;
+
+struct Launcher {
+  cw_handle* h;
+  long long count = 0;
+  cudaEvent_t ev0 = nullptr;
+  void begin(const char* name) {
+    if (!h->profiling) return;
+    cudaEvent_t a, b;
+    CW_CUDA(cudaEventCreate(&a));
+    CW_CUDA(cudaEventCreate(&b));
+    CW_CUDA(cudaEventRecord(a, h->stream));
+    h->prof_ev.push_back({name, {a, b}});
+  }
+  void check() {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw std::runtime_error(std::string("kernel launch: ") + cudaGetErrorString(e));
+    if (h->profiling) CW_CUDA(cudaEventRecord(h->prof_ev.back().second.second, h->stream));
+    ++count;
+  }
+  template <int NF>
+  void halo_chunks(const std::vector<HaloChunk<NF>>& chunks) {
+    for (const HaloChunk<NF>& c : chunks) {
+      const unsigned total = c.start[c.nf];
+      if (total == 0) continue;
+      const int bs = 256;
+      const unsigned nb = (total + bs - 1) / bs;
+      begin("k_halo");
+      k_halo<NF><<<nb, bs, 0, h->stream>>>(c, 0);
+      check();
+      if (c.has_oddface) {
+        begin("k_halo");
+        k_halo<NF><<<nb, bs, 0, h->stream>>>(c, 1);
+        check();
+      }
+    }
+  }
+  // halo fill points are deferred until the next kernel: consecutive fill points (nothing launched between
+  // them) become one launch over the union of their fields
+  std::vector<int> pend;
+  void halo(int set) { pend.push_back(set); }
+  void flush() {
+    if (pend.empty()) return;
+    if (pend.size() == 1) {
+      halo_chunks(h->hs[pend[0]].small);
+      halo_chunks(h->hs[pend[0]].large);
+    } else {
+      std::vector<HaloField> f;
+      for (int set : pend)
+        for (const HaloField& x : h->hs[set].f) {
+          bool dup = false;
+          for (const HaloField& y : f) dup |= y.p == x.p && y.ind == x.ind;
+          if (!dup) f.push_back(x);
+        }
+      if (f.size() <= size_t(kHaloSmall)) {
+        std::vector<HaloChunk<kHaloSmall>> c;
+        chunk_fields(f, c);
+        halo_chunks(c);
+      } else {
+        std::vector<HaloChunk<kHaloLarge>> c;
+        chunk_fields(f, c);
+        halo_chunks(c);
+      }
+    }
+    pend.clear();
+  }
+  void copy_list(CopyDesc* d, long long* sd, size_t n, long long total) {
+    flush();
+    if (!total) return;
+    const int bs = 256;
+    begin("k_copy");
+    k_copy<<<unsigned((total + bs - 1) / bs), bs, 0, h->stream>>>(d, int(n), sd);
+    check();
+  }
+  // the block shape of a point kernel: the one being timed while tuning, else the tuned choice (0 by default)
+  int shape_for(const char* name) const {
+    if (h->tuning_shape >= 0) return h->tuning_shape;
+    for (const auto& [n, sh] : h->shape_choice)
+      if (n == name) return sh;
+    return 0;
+  }
+  // a point kernel of fixed shape 0 over the index range kind, one launch per pack
+  template <class R, int NM, class K, class... Args>
+  void run(const char* name, int kind, K kern, const Packs<R, NM>& ps, Args... args) {
+    flush();
+    for (size_t c = 0; c < ps.p.size(); ++c) {
+      const int nb = ps.blocks[c][size_t(kind)][0];
+      if (nb == 0) continue;
+      begin(name);
+      kern<<<nb, PX, 0, h->stream>>>(ps.p[c], args...);
+      check();
+    }
+  }
+  // a point kernel with a tunable block shape (one instantiation per shape), nq > 0: once per species
+  template <class R, int NM, class K, class... Args>
+  void run_t(const char* name, int kind, int nq, const std::array<K, kNumShapes>& kerns, const Packs<R, NM>& ps,
+             Args... args) {
+    flush();
+    const int sh = shape_for(name);
+    for (size_t c = 0; c < ps.p.size(); ++c) {
+      const int nb = ps.blocks[c][size_t(kind)][size_t(sh)];
+      if (nb == 0 || nq == 0) continue;
+      begin(name);
+      kerns[size_t(sh)]<<<dim3(nb, nq), PX, 0, h->stream>>>(ps.p[c], args...);
+      check();
+    }
+  }
+  // a column-block kernel using `arrays` shared level arrays
+  template <class R, int NM, class K, class... Args>
+  void run_cb(const char* name, int kind, int arrays, K kern, const Packs<R, NM>& ps, Args... args) {
+    flush();
+    static_assert(CX == 32, "a column block's lanes are one warp");
+    const size_t smem = size_t(arrays) * h->cb_level_bytes;
+    CW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    for (size_t c = 0; c < ps.p.size(); ++c) {
+      const int nb = ps.blocks[c][size_t(kind)][0];
+      if (nb == 0) continue;
+      begin(name);
+      kern<<<nb, dim3(CX, CNW), smem, h->stream>>>(ps.p[c], args...);
+      check();
+    }
+  }
+  // one block per member
+  template <class R, int NM, class K>
+  void run_members(const char* name, int threads, K kern, const Packs<R, NM>& ps) {
+    flush();
+    for (size_t c = 0; c < ps.p.size(); ++c) {
+      begin(name);
+      kern<<<unsigned(ps.p[c].n), threads, 0, h->stream>>>(ps.p[c]);
+      check();
+    }
+  }
+};
+
+// the three block-shape instantiations of a tunable point kernel
+#define KV(kern) std::array{kern<R, NM, 0>, kern<R, NM, 1>, kern<R, NM, 2>}
+
+template <class R, int NM>
+void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
+  const Member& M0 = h->m[0];
+  bool lbc = false, terrain = false, scalars = false, any_pd = false;
+  // every member specified on all four sides: the acoustic substeps read no halo cell of the fields the
+  // per-substep fills (H_SS0, H_UV, H_AC) would refresh (the faces next to the boundary are the spec
+  // zone's, updated from the boundary data), and the fills after the substeps (H_POST, H_FIN) refresh them
+  // before anything reads them; those fills, and the spec zone's zero-gradient w of every substep but the
+  // last (overwritten by the next one, read only after the substeps), are left out
+  bool spec_all = true;
+  int nq = 0;  // the most species of a member
+  for (const Member& M : h->m) {
+    spec_all &= M.o.lbc != 0 && flat_x(M.g) && flat_y(M.g) && !two_d(M.g);
+    nq = std::max(nq, M.o.n_scalars);
+    lbc |= M.o.lbc != 0;
+    terrain |= !M.o.flat;
+    scalars |= M.o.n_scalars > 0;
+    for (int n = 0; n < M.o.n_scalars; ++n)
+      any_pd |= (n < M.o.n_moist ? M.o.moist_adv_opt : M.o.scalar_adv_opt) == 1;
+  }
+  const int n_sound = M0.n_sound;
+  if (lbc) {
+    L.run_members("k_advance_time", 1, k_advance_time<R, NM>, d);
+  }
+  L.copy_list(h->copies_d, h->copies_start_d, h->copies.size(), h->copies_total);
+  L.halo(cw_handle::H_MU1);
+  for (int rk = 1; rk <= 3; ++rk) {
+    const int ns = rk == 1 ? 1 : (rk == 2 ? n_sound / 2 : n_sound);
+    L.halo(cw_handle::H_PREP0);
+    L.run_cb("k_ls_prep", RG_COLS_STAG, 1, k_ls_prep<R, NM>, d);
+    L.halo(cw_handle::H_PREP1);
+    if (rk == 1) L.run_t("k_tendf_rk1", RG_STAG, 1, KV(k_tendf_rk1), d);
+    L.run_t("k_tend", RG_STAG, 1, KV(k_tend), d, rk);
+    if (rk == 1) L.copy_list(h->zeros_d, h->zeros_start_d, h->zeros.size(), h->zeros_total);
+    L.run_cb("k_ss_prep", RG_COLS_STAG, 3, k_ss_prep<R, NM>, d, rk);
+    if (!spec_all) L.halo(cw_handle::H_SS0);
+    for (int it = 1; it <= ns; ++it) {
+      L.run_t("k_uv", RG_STAG, 1, KV(k_uv), d, rk);
+      if (!spec_all) L.halo(cw_handle::H_UV);
+      L.run_cb("k_ac", RG_COLS_STAG, kCbArrays, k_ac<R, NM>, d, rk, it, ns);
+      if (lbc && (!spec_all || it == ns)) L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_ZERO_GRAD_W), rk);
+      if (!spec_all) L.halo(cw_handle::H_AC);
+    }
+    L.halo(cw_handle::H_POST);
+    L.run_cb("k_finish", RG_COLS_STAG, 0, k_finish<R, NM>, d, rk, ns);
+    L.halo(cw_handle::H_FIN);
+    if (scalars) {
+      if (rk == 1) L.run_t("k_q_tendf_rk1", RG_MASS, nq, KV(k_q_tendf_rk1), d);
+      L.run_t("k_q_update", RG_MASS, nq, KV(k_q_update), d, rk);
+      if (rk == 3 && any_pd) {
+        L.run_t("k_q_pre_pd", RG_MASS, nq, KV(k_q_pre_pd), d, rk);
+        L.halo(cw_handle::H_Q1PD);
+        L.run_t("k_q_face_pd", RG_STAG, 1, KV(k_q_face_pd), d, rk);
+        L.run_t("k_q_scale_pd", RG_MASS, nq, KV(k_q_scale_pd), d, rk);
+        L.halo(cw_handle::H_SCPD);
+        L.run_t("k_q_update_pd", RG_MASS, nq, KV(k_q_update_pd), d, rk);
+      }
+      L.run_members("k_q_swap", 64, k_q_swap<R, NM>, d);
+      if (lbc) L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_FLOW_DEP), rk);
+      L.halo(cw_handle::H_Q2);
+    }
+  }
+  if (lbc) {
+    L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_FINAL), 3);
+    L.run_t("k_p_rho_phi", RG_MASS, 1, KV(k_p_rho_phi), d, 1);
+    L.halo(cw_handle::H_END_P);
+  }
+  if (terrain) {
+    L.halo(cw_handle::H_WS0);
+    L.run_cb("k_w_surface", RG_COLS_MASS, 0, k_w_surface<R, NM>, d);
+    L.halo(cw_handle::H_WS1);
+  }
+  L.flush();
+}
+
+template <class R>
+void enqueue_t(cw_handle* h, Launcher& L, const DevTables<R>& T) {
+  if (h->m.size() == 1) enqueue_step<R, 1>(h, L, T.one);
+  else enqueue_step<R, kPackMembers>(h, L, T.many);
+}
+
+}  // namespace
