@@ -25,7 +25,7 @@ FIELDS = [
     "RU_TEND", "RV_TEND", "RW_TEND", "T_TEND", "PH_TEND", "MU_TEND",
     "RU_TENDF", "RV_TENDF", "RW_TENDF", "T_TENDF", "PH_TENDF",
     "MUB", "PB", "ALB", "T_INIT", "QV_BASE", "PHB", "HT",
-    "MSFTX", "MSFTY", "MSFUX", "MSFUY", "MSFVX", "MSFVY", "MSFVX_INV", "F", "E", "SINA", "COSA",
+    "MSFTX", "MSFTY", "MSFUX", "MSFUY", "MSFVX", "MSFVY", "MSFVX_INV", "F", "E", "SINA", "COSA", "RAINNC", "RAINNCV",
     "Q_1", "Q_2", "Q_TENDF",
 ]
 F = {name: n for n, name in enumerate(FIELDS)}
@@ -38,7 +38,7 @@ STATE_FIELDS = ["U_2", "V_2", "W_2", "T_2", "PH_2", "MU_2", "P", "AL", "WW", "RU
 LBC_U, LBC_V, LBC_T, LBC_PH, LBC_MU = range(5)
 XS, XE, YS, YE = range(4)
 # enum cw_ideal_kind
-REST_STATE, STRAKA, WARM_BUBBLE, IGW = range(4)
+REST_STATE, STRAKA, WARM_BUBBLE, IGW, SQUALL2D = range(5)
 DEFAULT = -1.0e300
 # cw_download_noalloc: scratch capacity (doubles) and return codes
 NOALLOC_SCRATCH_DOUBLES = 1048576
@@ -59,7 +59,7 @@ class Options(C.Structure):
                 ("dampcoef", C.c_double), ("time_step_sound", C.c_int), ("moist_adv_opt", C.c_int),
                 ("scalar_adv_opt", C.c_int), ("tke_adv_opt", C.c_int), ("diff_opt", C.c_int), ("km_opt", C.c_int),
                 ("flat", C.c_int), ("n_moist", C.c_int), ("n_scalars", C.c_int), ("lbc", C.c_int),
-                ("precision", C.c_int)]
+                ("precision", C.c_int), ("mp_physics", C.c_int), ("mp_tend_lim", C.c_double)]
 
 
 _DP = C.POINTER(C.c_double)
@@ -116,7 +116,7 @@ class Diag(C.Structure):
 
 class SnapshotFields(C.Structure):
     _fields_ = [(n, _DP) for n in ("u_2", "v_2", "w_2", "t_2", "p", "ph_2", "mu_2", "pb", "phb", "t_init", "mub")] + \
-               [("q_2", C.POINTER(_DP))]
+               [("q_2", C.POINTER(_DP)), ("rainnc", _DP), ("rainncv", _DP)]
 
 
 _lib = None
@@ -247,7 +247,9 @@ def snapshot_write_host(directory, step, time, g, o, fields, q_fields=(), q_name
             ("u_2", "v_2", "w_2", "t_2", "p", "ph_2", "mu_2", "pb", "phb", "t_init", "mub")]
     qs = [np.ascontiguousarray(q, dtype=np.float64) for q in q_fields]
     qp = (_DP * max(1, len(qs)))(*[q.ctypes.data_as(_DP) for q in qs])
-    f = SnapshotFields(*[a.ctypes.data_as(_DP) for a in keep], C.cast(qp, C.POINTER(_DP)))
+    rain = [np.ascontiguousarray(fields[n], dtype=np.float64) if n in fields else None for n in ("rainnc", "rainncv")]
+    f = SnapshotFields(*[a.ctypes.data_as(_DP) for a in keep], C.cast(qp, C.POINTER(_DP)),
+                       *[r.ctypes.data_as(_DP) if r is not None else None for r in rain])
     na = names_array(q_names)
     rc = lib.cw_snapshot_write_host(str(directory).encode(), step, time, C.byref(g), C.byref(o), C.byref(f),
                                     na[0] if na else None)

@@ -9,6 +9,7 @@
 //
 // Limited-area case: a from-scratch generator (see cw_gen_lam below) for a 3-D domain with terrain,
 // the hybrid sigma-pressure coordinate, moist species and specified lateral boundaries.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -57,6 +58,7 @@ struct cw_case {
     return f[id][size_t(l.offset + i * l.si + j * l.sj + k * l.sk)];
   }
   size_t idx(const cw_layout& l, int i, int j, int k) const { return size_t(l.offset + i * l.si + j * l.sj + k * l.sk); }
+  double& at_q(int n, int i, int j, int k) { return q2[size_t(n)][idx(Lq, i, j, k)]; }
 };
 
 namespace {
@@ -96,6 +98,8 @@ void host_fill_halo(const cw_grid& g, const cw_layout& L, double* base, bool odd
       for (int a = 0; a < (vy ? 8 : 6); ++a)
         line(p + i + k * L.sk, L.sj, g.ny, vy, g.bc_y == CW_BC_PERIODIC, odd_y, cw::flat_y(g), L.wj0, L.wj1, a);
 }
+
+void fill_q_halo(cw_case* c, int n) { host_fill_halo(c->g, c->Lq, c->q2[size_t(n)].data(), false, false); }
 
 void fill_default_halo(cw_case* c, int id) {
   const cw_layout& L = c->L[id];
@@ -157,6 +161,26 @@ struct Sounding {
     }
     return 0.5 * (lo + hi);
   }
+  // the weight of the water vapour above z (Pa), linear between the table's points
+  double vapour_load(double z) const {
+    if (!qv_) return 0.0;
+    const double s = z / dz_;
+    const int m = int(std::floor(s));
+    if (m < 0 || m + 1 >= int(w_.size())) throw std::runtime_error("Sounding::vapour_load out of range");
+    const double a = s - m;
+    return (1.0 - a) * w_[m] + a * w_[m + 1];
+  }
+  double pd(double z) const { return p(z) - vapour_load(z); }  // dry-air pressure
+  double z_of_pd(double pp) const {
+    if (!qv_) return z_of_p(pp);
+    double lo = 0, hi = (pi_.size() - 2) * dz_;
+    if (pp > pd(lo) || pp < pd(hi)) throw std::runtime_error("Sounding::z_of_pd out of range");
+    for (int it = 0; it < 200 && hi - lo > 1e-9; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      (pd(mid) > pp ? lo : hi) = mid;
+    }
+    return 0.5 * (lo + hi);
+  }
 };
 
 // BaseState::set_levels, hybrid_opt = 0 (src/dyn/state.cpp:86-116)
@@ -202,6 +226,7 @@ int cw_default_options(cw_options* o) {
   o->moist_adv_opt = 1; o->scalar_adv_opt = 1; o->tke_adv_opt = 1;
   o->diff_opt = 0; o->km_opt = 1;
   o->flat = 1; o->n_moist = 0; o->n_scalars = 0; o->lbc = 0; o->precision = CW_FP64;
+  o->mp_physics = 0; o->mp_tend_lim = 10.0;
   return 0;
 }
 
@@ -339,7 +364,7 @@ int cw_case_lbc_time(cw_case* c, double* dtbc) {
 }
 
 int cw_default_ideal_params(cw_ideal_params* p, int kind) {
-  if (!p || kind < 0 || kind > 3) return -1;
+  if (!p || kind < 0 || kind > 4) return -1;
   p->kind = kind;
   p->theta0 = p->n_bv = p->u0 = p->xc = p->zc = p->xr = p->zr = p->amplitude = p->radius = p->a = CW_DEFAULT;
   p->p_surf = 1.0e5;
@@ -350,28 +375,71 @@ namespace {
 struct IdealCtx {
   int kind;
   double theta0, n_bv, u0;
+  // squall2d: Weisman & Klemp (1982) sounding (make_case, src/cases/cases.cpp:135-173)
+  double theta_tr = 343.0, z_tr = 12000.0, t_tr = 213.0, qv_max = 0.014;
+  const std::vector<double>* qtab = nullptr;  // qv on a 50 m table (nullptr: no vapour)
+  double dzt = 50.0;
+  int nt = 0;
 };
 double ideal_theta(double z, const void* v) {
+  using namespace cw::cst;
   const IdealCtx* c = static_cast<const IdealCtx*>(v);
-  if (c->kind == CW_IDEAL_REST_STATE || c->kind == CW_IDEAL_IGW) return c->theta0 * std::exp(c->n_bv * c->n_bv * z / cw::cst::g);
+  if (c->kind == CW_IDEAL_REST_STATE || c->kind == CW_IDEAL_IGW) return c->theta0 * std::exp(c->n_bv * c->n_bv * z / g);
+  if (c->kind == CW_IDEAL_SQUALL2D)
+    return z <= c->z_tr ? c->theta0 + (c->theta_tr - c->theta0) * std::pow(z / c->z_tr, 1.25)
+                        : c->theta_tr * std::exp(g / (cp * c->t_tr) * (z - c->z_tr));
   return 300.0;
+}
+double squall_rh(const IdealCtx* c, double z) { return z <= c->z_tr ? 1.0 - 0.75 * std::pow(z / c->z_tr, 1.25) : 0.25; }
+// the case's qv(z): linear in the table (qv = 0 without one)
+double ideal_qv(double z, const void* v) {
+  const IdealCtx* c = static_cast<const IdealCtx*>(v);
+  if (!c->qtab) return 0.0;
+  const double f = std::clamp(z / c->dzt, 0.0, double(c->nt - 1) - 1e-9);
+  const int n = int(f);
+  const std::vector<double>& q = *c->qtab;
+  return q[n] + (f - n) * (q[n + 1] - q[n]);
+}
+// the qv table of squall2d: qv = min(qv_max, RH ep_2 e_s / (p - e_s)) with p from a sounding that carries the
+// previous iteration's qv (8 fixed-point iterations; cases.cpp:149-167)
+void squall_qv_table(IdealCtx& c, double p_surf, double zmax, std::vector<double>& tab) {
+  using namespace cw::cst;
+  c.nt = int(zmax / c.dzt) + 2;
+  tab.assign(size_t(c.nt), 0.0);
+  for (int it = 0; it < 8; ++it) {
+    c.qtab = it == 0 ? nullptr : &tab;
+    Sounding snd(ideal_theta, it == 0 ? nullptr : ideal_qv, &c, p_surf, zmax, 0.5);
+    std::vector<double> q(size_t(c.nt));
+    for (int n = 0; n < c.nt; ++n) {
+      const double z = std::min(n * c.dzt, zmax), pz = snd.p(z), T = ideal_theta(z, &c) * std::pow(pz / p1000mb, rcp);
+      const double es = 611.2 * std::exp(17.67 * (T - 273.15) / (T - 29.65));
+      q[size_t(n)] = std::min(c.qv_max, squall_rh(&c, z) * ep_2 * es / (pz - es));
+    }
+    tab = q;
+  }
+  c.qtab = &tab;
 }
 double or_default(double v, double d) { return v < -1e299 ? d : v; }
 }  // namespace
 
-// cases::make_case + init_ideal + cases::initialize for the dry ideal cases (no moisture, flat terrain).
-// The grid's p_top becomes the sounding's pressure at ztop (src/cases/model.cpp:96-99). Passive tracers
-// (n_scalars > 0 with n_moist = 0) start at zero; the caller fills them.
+// cases::make_case + init_ideal + cases::initialize for the ideal cases (flat terrain; src/cases/cases.cpp:90-192,
+// :224-287, model.cpp:88-179). The grid's p_top becomes the dry sounding's pressure at ztop (model.cpp:96-99).
+// With moist species (species 0 is qv, State::P_QV >= 0) the full state is WRF's moist one (initialize_moist,
+// cases.cpp:292-353): dry-mass mu' from the vapour load, hydrostatic p' with moisture loading, theta_m; qv = 0
+// unless the case has vapour (squall2d). The other scalars start at zero; the caller fills them.
 int cw_gen_ideal(cw_case* c, const cw_ideal_params* pp) {
   if (!c || !pp) return -1;
   using namespace cw::cst;
   try {
     cw_grid& G = c->g;
-    if (!c->o.flat || c->o.n_moist != 0 || c->o.lbc) return -2;
+    if (!c->o.flat || c->o.lbc) return -2;
     const int kind = pp->kind;
+    const bool moist = c->o.n_moist > 0;
+    if (kind == CW_IDEAL_SQUALL2D && !moist) return -2;
     const double pi = std::numbers::pi;
     const double xcenter = 0.5 * G.nx * G.dx;
     IdealCtx ctx{kind, 300.0, 0.01, 0.0};
+    std::vector<double> qtab;
     double xc = 0, zc = 0, xr = 0, zr = 0, amp = 0, rad = 0, aa = 0, u_env = 0;
     switch (kind) {
       case CW_IDEAL_REST_STATE:
@@ -396,6 +464,13 @@ int cw_gen_ideal(cw_case* c, const cw_ideal_params* pp) {
         aa = or_default(pp->a, 5000.0);
         xc = or_default(pp->xc, 100000.0);
         break;
+      case CW_IDEAL_SQUALL2D:  // no wind: u_shear tanh(z / 3 km) - u_shift = 0
+        ctx.theta0 = or_default(pp->theta0, 300.0);
+        xc = or_default(pp->xc, xcenter); zc = or_default(pp->zc, 1400.0);
+        xr = or_default(pp->xr, 10000.0); zr = or_default(pp->zr, 1400.0);
+        amp = or_default(pp->amplitude, 2.0);
+        squall_qv_table(ctx, pp->p_surf, G.ztop * 1.2 + 1000.0, qtab);
+        break;
       default: return -1;
     }
     const double Hz = G.ztop;
@@ -418,10 +493,20 @@ int cw_gen_ideal(cw_case* c, const cw_ideal_params* pp) {
           const double t = (x - xc) / aa;
           return amp * std::sin(pi * z / Hz) / (1.0 + t * t);
         }
+        case CW_IDEAL_SQUALL2D: {
+          const double a = (x - xc) / xr, b = (z - zc) / zr;
+          const double L = std::sqrt(a * a + b * b);
+          if (!(L <= 1.0)) return 0.0;
+          const double cl = std::cos(0.5 * pi * L);
+          return amp * (cl * cl);
+        }
         default: return 0.0;
       }
     };
-    Sounding snd(ideal_theta, nullptr, &ctx, pp->p_surf, G.ztop * 1.2 + 1000.0, 0.5);
+    // the dry sounding (eta levels, base state) and, with moisture, the moist one of the full state
+    IdealCtx dry = ctx;
+    dry.qtab = nullptr;
+    Sounding snd(ideal_theta, nullptr, &dry, pp->p_surf, G.ztop * 1.2 + 1000.0, 0.5);
     G.p_top = snd.p(G.ztop);
     c->p_top = G.p_top;
     const int nz = G.nz;
@@ -484,11 +569,67 @@ int cw_gen_ideal(cw_case* c, const cw_ideal_params* pp) {
     c->f[CW_T_1] = c->f[CW_T_2];
     c->f[CW_PH_1] = c->f[CW_PH_2];
     c->f[CW_MU_1] = c->f[CW_MU_2];
+    if (moist) {  // initialize_moist (cases.cpp:292-353), use_theta_m = 1
+      Sounding msnd(ideal_theta, ideal_qv, &ctx, pp->p_surf, G.ztop * 1.2 + 1000.0, 0.5);
+      const double pd_surf = pp->p_surf - msnd.vapour_load(0.0);
+      const double mu1 = pd_surf - G.p_top - mub;
+      std::vector<double> qv(nz), thd(nz), th(nz), p(nz);
+      for (int k = 0; k < nz; ++k) {
+        const double p_level = c->c3h[k] * (pd_surf - G.p_top) + c->c4h[k] + G.p_top;
+        const double z = msnd.z_of_pd(p_level);
+        qv[k] = msnd.qv(z);
+        thd[k] = msnd.theta(z);
+      }
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+          const double x = (i + 0.5) * G.dx;
+          for (int k = 0; k < nz; ++k) th[k] = thd[k] + theta_pert(x, zm[k], exn[k]);
+          auto eos = [&](int k, double pk) {  // alt = R_d/p0 theta (1 + rvovrd qv) ((p + pb)/p0)^cvpm
+            const double qvf = 1.0 + rvovrd * qv[k];
+            const double alt = (r_d / p1000mb) * th[k] * qvf * std::pow((pk + pb[k]) / p1000mb, cvpm);
+            c->at(CW_ALT, i, j, k) = alt;
+            c->at(CW_AL, i, j, k) = alt - alb[k];
+            c->at(CW_P, i, j, k) = pk;
+          };
+          int k = nz - 1;  // hydrostatic p' from the top with the moisture load
+          double qvf1 = 0.5 * (qv[k] + qv[k]);
+          double qvf2 = 1.0 / (1.0 + qvf1);
+          qvf1 = qvf1 * qvf2;
+          double pk = -0.5 * ((c->c1f[nz] * mu1) + qvf1 * (c->c1f[nz] * mub + c->c2f[nz])) / c->rdnw[k] / qvf2;
+          eos(k, pk);
+          for (k = nz - 2; k >= 0; --k) {
+            qvf1 = 0.5 * (qv[k] + qv[k + 1]);
+            qvf2 = 1.0 / (1.0 + qvf1);
+            qvf1 = qvf1 * qvf2;
+            pk = pk - ((c->c1f[k + 1] * mu1) + qvf1 * (c->c1f[k + 1] * mub + c->c2f[k + 1])) / qvf2 / c->rdn[k + 1];
+            eos(k, pk);
+          }
+          double ph = 0.0;
+          c->at(CW_PH_2, i, j, 0) = 0.0;
+          for (k = 0; k < nz; ++k) {
+            ph = ph - c->dnw[k] * (((c->c1h[k] * mub + c->c2h[k]) + c->c1h[k] * mu1) * c->at(CW_AL, i, j, k) +
+                                   c->c1h[k] * mu1 * alb[k]);
+            c->at(CW_PH_2, i, j, k + 1) = ph;
+          }
+          for (k = 0; k < nz; ++k) {
+            c->at(CW_T_2, i, j, k) = th[k] * (1.0 + rvovrd * qv[k]) - t0;  // theta_m - t0
+            c->at_q(0, i, j, k) = qv[k];
+          }
+          c->at(CW_MU_2, i, j, 0) = mu1;
+        }
+      for (int k = 0; k < nz; ++k) c->f[CW_QV_BASE][k] = qv[k];
+      for (int id : {CW_T_2, CW_AL, CW_ALT, CW_PH_2, CW_P, CW_MU_2}) fill_default_halo(c, id);
+      fill_q_halo(c, 0);
+      c->f[CW_T_1] = c->f[CW_T_2];
+      c->f[CW_PH_1] = c->f[CW_PH_2];
+      c->f[CW_MU_1] = c->f[CW_MU_2];
+      c->q1[0] = c->q2[0];
+    }
     for (int k = 0; k < nz; ++k) {  // model.cpp:149-177: the column (0, 0)
       c->u_base[k] = c->at(CW_U_2, 0, 0, k);
       c->v_base[k] = c->at(CW_V_2, 0, 0, k);
       c->t_base[k] = c->f[CW_T_INIT][k];
-      c->qv_base_1d[k] = 0.0;
+      c->qv_base_1d[k] = c->f[CW_QV_BASE][k];
       c->z_base[k] = 0.5 * (phb[k] + phb[k + 1]) / g;
     }
   } catch (const std::exception&) {

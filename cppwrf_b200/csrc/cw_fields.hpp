@@ -71,7 +71,8 @@ inline FieldKind field_kind(const cw_options& o, int id) {
     case CW_W_1: case CW_W_2: case CW_PH_1: case CW_PH_2: case CW_WW: case CW_RW: case CW_WW_M: case CW_CQW:
     case CW_RW_TEND: case CW_PH_TEND: case CW_RW_TENDF: case CW_PH_TENDF:
       return {'W', 3, false};
-    case CW_MU_1: case CW_MU_2: case CW_MUT: case CW_MUTS: case CW_MU_TEND: return {'M', 2, false};
+    case CW_MU_1: case CW_MU_2: case CW_MUT: case CW_MUTS: case CW_MU_TEND: case CW_RAINNC: case CW_RAINNCV:
+      return {'M', 2, false};
     case CW_MUU: case CW_MUUS: return {'U', 2, false};
     case CW_MUV: case CW_MUVS: return {'V', 2, false};
     case CW_MUB: case CW_HT: return {'M', 2, o.flat != 0};
@@ -130,6 +131,9 @@ inline const char* unsupported(const cw_grid& g, const cw_options& o) {
   if (o.precision != CW_FP64 && o.precision != CW_MIXED) return "precision must be CW_FP64 or CW_MIXED";
   const int ns = sound_steps(g, o);
   if (ns < 2 || ns % 2) return "time_step_sound must be even and >= 2";
+  if (o.mp_physics != 0 && o.mp_physics != 1) return "mp_physics must be 0 or 1 (Kessler)";
+  if (o.mp_physics == 1 && o.n_moist < 3) return "Kessler microphysics needs the moist species qv, qc, qr (0, 1, 2)";
+  if (o.mp_physics == 1 && !(o.mp_tend_lim > 0)) return "mp_tend_lim must be > 0";
   return nullptr;
 }
 

@@ -144,7 +144,7 @@ int cw_snapshot_write_host(const char* dir, long long step, double time, const c
   return guarded_out([&] {
     if (!dir || !g || !o || !f) throw std::runtime_error("snapshot: null argument");
     if (!f->u_2 || !f->v_2 || !f->w_2 || !f->t_2 || !f->p || !f->ph_2 || !f->mu_2 || !f->pb || !f->phb || !f->t_init ||
-        !f->mub || (o->n_scalars > 0 && !f->q_2))
+        !f->mub || (o->n_scalars > 0 && !f->q_2) || (o->mp_physics != 0 && (!f->rainnc || !f->rainncv)))
       throw std::runtime_error("snapshot: a field array is missing");
     using namespace cw;
     auto lay = [&](int id) { return field_layout(*g, *o, id); };
@@ -187,10 +187,17 @@ int cw_snapshot_write_host(const char* dir, long long step, double time, const c
     });
     for (int n = 0; n < o->n_scalars; ++n) {
       if (!f->q_2[n]) throw std::runtime_error("snapshot: scalar array missing");
+      static const char* const kessler[3] = {"qv", "qc", "qr"};
       std::string name = q_names && q_names[n] ? std::string(q_names[n])
-                                               : (moist && n == 0 ? std::string("qv") : "q" + std::to_string(n));
+                         : (moist && n == 0) || (o->mp_physics == 1 && n < 3) ? std::string(kessler[n])
+                                                                              : "q" + std::to_string(n);
       const double* q = f->q_2[n];
       add(name, 'M', nx, ny, nz, [&](int i, int j, int k) { return at(q, Lq, i, j, k); });
+    }
+    if (o->mp_physics != 0) {  // PhysicsCoupling::rainnc, rainncv: the snapshot's extra 2-D fields
+      const cw_layout Lr = lay(CW_RAINNC);
+      add("rainnc", 'M', nx, ny, 1, [&](int i, int j, int) { return at(f->rainnc, Lr, i, j, 0); });
+      add("rainncv", 'M', nx, ny, 1, [&](int i, int j, int) { return at(f->rainncv, Lr, i, j, 0); });
     }
     // the binary file: the variables one after the other, contiguous (k, j, i), little-endian float64
     size_t total = 0;
@@ -237,7 +244,7 @@ int cw_snapshot_write(cw_handle* h, int member, const char* dir, long long step,
     cw_grid g{};
     cw_options o{};
     if (cw_member_config(h, member, &g, &o) != 0) throw std::runtime_error(cw_last_error(h));
-    std::vector<double> u, v, w, t, p, ph, mu, pb, phb, ti, mub;
+    std::vector<double> u, v, w, t, p, ph, mu, pb, phb, ti, mub, rain, rainv;
     cw_snapshot_fields f{};
     f.u_2 = get(CW_U_2, 0, u); f.v_2 = get(CW_V_2, 0, v); f.w_2 = get(CW_W_2, 0, w); f.t_2 = get(CW_T_2, 0, t);
     f.p = get(CW_P, 0, p); f.ph_2 = get(CW_PH_2, 0, ph); f.mu_2 = get(CW_MU_2, 0, mu); f.pb = get(CW_PB, 0, pb);
@@ -246,6 +253,10 @@ int cw_snapshot_write(cw_handle* h, int member, const char* dir, long long step,
     std::vector<const double*> qp(size_t(o.n_scalars));
     for (int n = 0; n < o.n_scalars; ++n) qp[size_t(n)] = get(CW_Q_2, n, q[size_t(n)]);
     f.q_2 = qp.data();
+    if (o.mp_physics != 0) {
+      f.rainnc = get(CW_RAINNC, 0, rain);
+      f.rainncv = get(CW_RAINNCV, 0, rainv);
+    }
     if (cw_snapshot_write_host(dir, step, time, &g, &o, &f, q_names) != 0) throw std::runtime_error(g_err);
     return 0;
   });

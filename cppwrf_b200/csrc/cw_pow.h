@@ -18,6 +18,8 @@
  * the oracle's interposed mode both call cw_pow instead. The accuracy is checked against
  * glibc pow and against a 60-digit decimal evaluation in tests/test_pow.py.
  *
+ * cw_exp(x) is the same exponential on a double argument.
+ *
  * Domain: any double x, y; special values follow C99 Annex F for the cases the dycore can meet
  * (x > 0 finite; NaN, 0, infinities and negative x are handled for robustness).
  */
@@ -239,6 +241,13 @@ CW_HD double cw_pow(double x, double y) {
   e = CW_ADD(e, CW_MUL(y, ll));
   cw_fast_two_sum(th, e, &th, &tl);
   return CW_MUL(sign, cw_exp_dd(th, tl));
+}
+
+/* exp(x): the exponential core of cw_pow on a double argument (the Kessler microphysics' saturation vapour
+ * pressure; the reference's CPU build takes glibc's exp there) */
+CW_HD double cw_exp(double x) {
+  if (x != x) return CW_ADD(x, x);
+  return cw_exp_dd(x, 0.0);
 }
 
 #endif /* CW_POW_H */

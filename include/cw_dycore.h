@@ -59,6 +59,10 @@ typedef struct cw_options {
   int n_scalars; /* moist species + passive tracers */
   int lbc;       /* 1: a LateralBC is attached (RK3::set_lateral_bc, width 5 / spec 1 / relax 4) */
   int precision; /* enum cw_precision */
+  /* PhysicsParams (src/dyn/physics_coupling.hpp:23-35): 0 none, 1 Kessler (species 0, 1, 2 are qv, qc, qr),
+   * run after the RK3 loop as solve_em does (src/dyn/rk3.cpp:150-158) */
+  int mp_physics;
+  double mp_tend_lim; /* K/s, limit on the microphysics heating rate */
 } cw_options;
 
 /* Fills o with the reference defaults (the values Model::build takes when a key is absent). */
@@ -84,6 +88,7 @@ enum cw_field {
   CW_RU_TENDF, CW_RV_TENDF, CW_RW_TENDF, CW_T_TENDF, CW_PH_TENDF,
   CW_MUB, CW_PB, CW_ALB, CW_T_INIT, CW_QV_BASE, CW_PHB, CW_HT,
   CW_MSFTX, CW_MSFTY, CW_MSFUX, CW_MSFUY, CW_MSFVX, CW_MSFVY, CW_MSFVX_INV, CW_F, CW_E, CW_SINA, CW_COSA,
+  CW_RAINNC, CW_RAINNCV, /* PhysicsCoupling::rainnc, rainncv (physics_coupling.hpp:54): grid-scale rain [mm] */
   CW_Q_1, CW_Q_2, CW_Q_TENDF, /* with index n */
   CW_NFIELDS
 };
@@ -222,7 +227,8 @@ int cw_member_upload_case(cw_handle* h, int member, cw_case* c);
  * kind: CW_IDEAL_REST_STATE (theta0 exp(N^2 z / g), uniform u0), CW_IDEAL_STRAKA (cold bubble),
  * CW_IDEAL_WARM_BUBBLE (Bryan-Fritsch thermal), CW_IDEAL_IGW (Skamarock-Klemp gravity wave).
  * Parameters left at CW_DEFAULT take the reference's defaults for the kind. */
-enum cw_ideal_kind { CW_IDEAL_REST_STATE = 0, CW_IDEAL_STRAKA = 1, CW_IDEAL_WARM_BUBBLE = 2, CW_IDEAL_IGW = 3 };
+enum cw_ideal_kind { CW_IDEAL_REST_STATE = 0, CW_IDEAL_STRAKA = 1, CW_IDEAL_WARM_BUBBLE = 2, CW_IDEAL_IGW = 3,
+                     CW_IDEAL_SQUALL2D = 4 };
 #define CW_DEFAULT (-1.0e300)
 typedef struct cw_ideal_params {
   int kind;

@@ -37,16 +37,18 @@ int cw_diag_header(char* buf, size_t n);
 int cw_diag_format_row(long long step, double time, const cw_diag* d, double wall_s, char* buf, size_t n);
 
 /* Whole-allocation host arrays (the fields' layouts, cw_layout_of) of the state a snapshot is made of. q_2:
- * n_scalars arrays (may be NULL without scalars). */
+ * n_scalars arrays (may be NULL without scalars); rainnc, rainncv: with mp_physics != 0. */
 typedef struct cw_snapshot_fields {
   const double *u_2, *v_2, *w_2, *t_2, *p, *ph_2, *mu_2;
   const double *pb, *phb, *t_init, *mub;
   const double* const* q_2;
+  const double *rainnc, *rainncv;
 } cw_snapshot_fields;
 
 /* Writes dir/snap_<step, 6 digits>.bin and .json (each through a temporary file and a rename): u v w th_pert
- * theta [theta_m] p p_pert ph mu mu_pert z_m and the scalars, float64, (k, j, i) order. q_names: n_scalars
- * names (NULL: species 0 "qv" when there are moist species, the others "q<n>"). */
+ * theta [theta_m] p p_pert ph mu mu_pert z_m, the scalars, and with microphysics rainnc, rainncv (the physics'
+ * extra 2-D fields), float64, (k, j, i) order. q_names: n_scalars names (NULL: species 0 "qv" when there are moist species,
+ * with Kessler 1 and 2 "qc" and "qr", the others "q<n>"). */
 int cw_snapshot_write_host(const char* dir, long long step, double time, const cw_grid* g, const cw_options* o,
                            const cw_snapshot_fields* f, const char* const* q_names);
 /* The same of a member of a handle (its fields downloaded first). */

@@ -26,6 +26,7 @@
 
 /* glibc's libmvec 2-lane pow, the reference CPU build's vm::pow (src/core/backend.hpp:118, :171) */
 extern __m128d _ZGVbN2vv_pow(__m128d, __m128d);
+extern __m128d _ZGVbN2v_exp(__m128d);
 
 /* ------------------------------------------------------------------ constants
  * src/core/constants.hpp:4-18 (WRF module_model_constants) */
@@ -159,7 +160,8 @@ static void field_kind(const cw_options* o, int id, char* s, int* rank, int* uni
     case CW_V_1: case CW_V_2: case CW_RV: case CW_RV_M: case CW_CQV: case CW_RV_TEND: case CW_RV_TENDF: *s = ST_V; break;
     case CW_W_1: case CW_W_2: case CW_PH_1: case CW_PH_2: case CW_WW: case CW_RW: case CW_WW_M: case CW_CQW:
     case CW_RW_TEND: case CW_PH_TEND: case CW_RW_TENDF: case CW_PH_TENDF: *s = ST_W; break;
-    case CW_MU_1: case CW_MU_2: case CW_MUT: case CW_MUTS: case CW_MU_TEND: *s = ST_M; *rank = 2; break;
+    case CW_MU_1: case CW_MU_2: case CW_MUT: case CW_MUTS: case CW_MU_TEND: case CW_RAINNC: case CW_RAINNCV:
+      *s = ST_M; *rank = 2; break;
     case CW_MUU: case CW_MUUS: *s = ST_U; *rank = 2; break;
     case CW_MUV: case CW_MUVS: *s = ST_V; *rank = 2; break;
     case CW_MUB: case CW_HT: *s = ST_M; *rank = 2; *uniform = o->flat; break;
@@ -1973,6 +1975,163 @@ static void tendencies(or_dom* d, int rk) {
 
 static void copy_fld(fld* dst, const fld* src) { memcpy(dst->a, src->a, (size_t)src->L.total * sizeof(double)); }
 
+/* ------------------------------------------------------------------ microphysics coupling
+ * PhysicsCoupling::step for mp_physics = 1 (src/dyn/physics_coupling.cpp:262-456): moist_physics_prep_em (KPrep
+ * :42-60, KSaveQc :78-81), Kessler (src/phys/mp_kessler/kessler.hpp:47-159) on the columns outside the spec zone,
+ * moist_physics_finish_em (KFinish :63-76), halos. Species 0, 1, 2 are qv, qc, qr. pow and exp by the mode:
+ * glibc (libmvec's 2-lane functions on the lanes of WRF's vectorised loops, vm::lane) or cw_pow / cw_exp. */
+static int vm_lane(int i, int n) { return n > 1 && !((n & 1) && i == n - 1); }
+static double mp_pow(const or_dom* d, double a, double b, int i, int n) {
+  if (d->pow_mode != OR_POW_GLIBC) return cw_pow(a, b);
+  if (vm_lane(i, n)) return _mm_cvtsd_f64(_ZGVbN2vv_pow(_mm_set1_pd(a), _mm_set1_pd(b)));
+  return pow(a, b);
+}
+static double mp_rpow(const or_dom* d, double a, double b) { return d->pow_mode == OR_POW_GLIBC ? pow(a, b) : cw_pow(a, b); }
+static double mp_exp(const or_dom* d, double a, int i, int n) {
+  if (d->pow_mode != OR_POW_GLIBC) return cw_exp(a);
+  if (vm_lane(i, n)) return _mm_cvtsd_f64(_ZGVbN2v_exp(_mm_set1_pd(a)));
+  return exp(a);
+}
+static double c_max(double a, double b) { return a < b ? b : a; } /* std::max */
+static double c_min(double a, double b) { return b < a ? b : a; } /* std::min */
+
+#define KS_LEVELS 128
+typedef struct {
+  fld *th, *rho, *pii, *z, *dz8w;
+} mp_work;
+
+static void kessler_column(or_dom* d, const mp_work* w, int i, int j, double dt, int i0, int ni) {
+  fld *qv = &d->q2[0], *qc = &d->q2[1], *qr = &d->q2[2], *t = w->th;
+  const int nz = d->g.nz;
+  const double xlv = 2.5e6, cp = CP, ep2 = R_D / 461.6, svp1 = 0.6112, svp2 = 17.67, svp3 = 29.65, svpt0 = 273.15,
+               rhowater = 1000.0;
+  double vt[KS_LEVELS] = {0}, prodk[KS_LEVELS] = {0}, vtden[KS_LEVELS] = {0}, rdzk[KS_LEVELS] = {0},
+         rhok[KS_LEVELS] = {0}, factor[KS_LEVELS] = {0}, rdzw[KS_LEVELS] = {0}, prod[KS_LEVELS] = {0};
+  const double f5 = svp2 * (svpt0 - svp3) * xlv / cp;
+  const double c1 = 0.001, c2 = 0.001, c3 = 2.2, c4 = 0.875, max_cr_sedimentation = 0.75;
+  double crmax = 0;
+  for (int k = 0; k < nz; ++k) {
+    prodk[k] = AT(qr, i, j, k);
+    rhok[k] = AT(w->rho, i, j, k);
+    const double qrr = c_max(0, AT(qr, i, j, k) * 0.001 * rhok[k]);
+    vtden[k] = sqrt(rhok[0] / rhok[k]);
+    vt[k] = 36.34 * mp_rpow(d, qrr, 0.1364) * vtden[k];
+    rdzw[k] = 1.0 / AT(w->dz8w, i, j, k);
+    crmax = c_max(vt[k] * dt * rdzw[k], crmax);
+  }
+  for (int k = 0; k < nz - 1; ++k) rdzk[k] = 1.0 / (AT(w->z, i, j, k + 1) - AT(w->z, i, j, k));
+  rdzk[nz - 1] = 1.0 / (AT(w->z, i, j, nz - 1) - AT(w->z, i, j, nz - 2));
+  int nfall = (int)round(0.5 + crmax / max_cr_sedimentation);
+  nfall = 1 < nfall ? nfall : 1;
+  double dtfall = dt / nfall, time_sediment = dt;
+  fld *rainnc = F_(CW_RAINNC), *rainncv = F_(CW_RAINNCV);
+  while (nfall > 0) {
+    time_sediment = time_sediment - dtfall;
+    for (int k = 0; k < nz - 1; ++k) factor[k] = dtfall * rdzk[k] / rhok[k];
+    factor[nz - 1] = dtfall * rdzk[nz - 1];
+    const double ppt = rhok[0] * prodk[0] * vt[0] * dtfall / rhowater;
+    AT(rainncv, i, j, 0) = ppt * 1000.0;
+    AT(rainnc, i, j, 0) = AT(rainnc, i, j, 0) + ppt * 1000.0;
+    for (int k = 0; k < nz - 1; ++k)
+      prodk[k] = prodk[k] - factor[k] * (rhok[k] * prodk[k] * vt[k] - rhok[k + 1] * prodk[k + 1] * vt[k + 1]);
+    prodk[nz - 1] = prodk[nz - 1] - factor[nz - 1] * prodk[nz - 1] * vt[nz - 1];
+    if (nfall > 1) {
+      nfall = nfall - 1;
+      crmax = 0;
+      for (int k = 0; k < nz; ++k) {
+        const double qrr = c_max(0, prodk[k] * 0.001 * rhok[k]);
+        vt[k] = 36.34 * mp_pow(d, qrr, 0.1364, k, nz) * vtden[k];
+        crmax = c_max(vt[k] * time_sediment * rdzw[k], crmax);
+      }
+      int nfall_new = (int)round(0.5 + crmax / max_cr_sedimentation);
+      nfall_new = 1 < nfall_new ? nfall_new : 1;
+      if (nfall_new != nfall) {
+        nfall = nfall_new;
+        dtfall = time_sediment / nfall;
+      }
+    } else {
+      for (int k = 0; k < nz; ++k) prod[k] = prodk[k];
+      nfall = 0;
+    }
+  }
+  const int li = i - i0;
+  for (int k = 0; k < nz; ++k) {
+    const double factorn = 1.0 / (1.0 + c3 * dt * mp_pow(d, c_max(0.0, AT(qr, i, j, k)), c4, li, ni));
+    const double qrprod = AT(qc, i, j, k) * (1.0 - factorn) + factorn * c1 * dt * c_max(AT(qc, i, j, k) - c2, 0.0);
+    const double rcgs = 0.001 * AT(w->rho, i, j, k);
+    AT(qc, i, j, k) = c_max(AT(qc, i, j, k) - qrprod, 0.0);
+    AT(qr, i, j, k) = (AT(qr, i, j, k) + prod[k] - AT(qr, i, j, k));
+    AT(qr, i, j, k) = c_max(AT(qr, i, j, k) + qrprod, 0.0);
+    const double pii = AT(w->pii, i, j, k);
+    const double temp = pii * AT(t, i, j, k);
+    const double pressure = 1.000e+05 * mp_pow(d, pii, 1004.0 / 287.0, li, ni);
+    const double gam = 2.5e+06 / (1004.0 * pii);
+    const double es = 1000.0 * svp1 * mp_exp(d, svp2 * (temp - svpt0) / (temp - svp3), li, ni);
+    const double qvs = ep2 * es / (pressure - es);
+    prod[k] = (AT(qv, i, j, k) - qvs) / (1.0 + pressure / (pressure - es) * qvs * f5 / ((temp - svp3) * (temp - svp3)));
+    const double dim_qvs_qv = c_max(0.0, qvs - AT(qv, i, j, k));
+    const double rq = rcgs * AT(qr, i, j, k);
+    const double ern_num = (1.6 + 124.9 * mp_pow(d, rq, 0.2046, li, ni)) * mp_pow(d, rq, 0.525, li, ni);
+    const double ern_den = 2.55e8 / (pressure * qvs) + 5.4e5;
+    const double ern_term1 = dt * (ern_num / ern_den) * (dim_qvs_qv / (rcgs * qvs));
+    const double ern_term2 = c_max(-prod[k] - AT(qc, i, j, k), 0.0);
+    const double ern = c_min(ern_term1, c_min(ern_term2, AT(qr, i, j, k)));
+    const double product = c_max(prod[k], -AT(qc, i, j, k));
+    AT(t, i, j, k) = AT(t, i, j, k) + gam * (product - ern);
+    AT(qv, i, j, k) = c_max(AT(qv, i, j, k) - product + ern, 0.0);
+    AT(qc, i, j, k) = AT(qc, i, j, k) + product;
+    AT(qr, i, j, k) = AT(qr, i, j, k) - ern;
+  }
+}
+
+static void physics_step(or_dom* d) {
+  const cw_grid* g = &d->g;
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  const double dt = g->dt, rvrd = 461.6 / R_D, lim = d->o.mp_tend_lim;
+  mp_work w;
+  fld th, rho, pii, z, dz8w, hd_old, qv_old;
+  fld* all[] = {&th, &rho, &pii, &z, &dz8w, &hd_old, &qv_old};
+  for (size_t n = 0; n < sizeof all / sizeof all[0]; ++n) fld_alloc(all[n], g, ST_M, 3, 0);
+  w.th = &th; w.rho = &rho; w.pii = &pii; w.z = &z; w.dz8w = &dz8w;
+  fld *t = F_(CW_T_2), *ph = F_(CW_PH_2), *phb = F_(CW_PHB), *al = F_(CW_AL), *alb = F_(CW_ALB), *p = F_(CW_P),
+      *pb = F_(CW_PB), *hd = F_(CW_H_DIABATIC), *qv = &d->q2[0];
+  const int pz = specified(g) ? 1 : 0;
+  const int pi0 = g->bc_x == CW_BC_PERIODIC ? 0 : pz, pni = nx - 2 * pi0;
+  for (int k = 0; k < nz; ++k)  /* KPrep (qc_diabatic and the other WRF diagnostics are not kept) */
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const double zw0 = (AT(ph, i, j, k) + AT(phb, i, j, k)) / G_;
+        const double zw1 = (AT(ph, i, j, k + 1) + AT(phb, i, j, k + 1)) / G_;
+        AT(&dz8w, i, j, k) = zw1 - zw0;
+        AT(&z, i, j, k) = 0.5 * (zw0 + zw1);
+        const double q = AT(qv, i, j, k);
+        const double thv = (AT(t, i, j, k) + T0) / (1.0 + rvrd * q);
+        AT(&th, i, j, k) = thv;
+        AT(&hd_old, i, j, k) = thv;
+        AT(&qv_old, i, j, k) = q;
+        AT(&rho, i, j, k) = 1.0 / (AT(al, i, j, k) + AT(alb, i, j, k));
+        AT(&pii, i, j, k) = mp_pow(d, (AT(p, i, j, k) + AT(pb, i, j, k)) / P1000MB, R_D / CP, i - pi0, pni);
+      }
+  const int sx = g->bc_x == CW_BC_SPECIFIED ? 1 : 0, sy = g->bc_y == CW_BC_SPECIFIED ? 1 : 0;
+  for (int j = sy; j < ny - sy; ++j)
+    for (int i = sx; i < nx - sx; ++i) kessler_column(d, &w, i, j, dt, sx, nx - 2 * sx);
+  for (int k = 0; k < nz; ++k)  /* KFinish */
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const double thn = AT(&th, i, j, k), th_old = AT(&hd_old, i, j, k), q = AT(qv, i, j, k), q_old = AT(&qv_old, i, j, k);
+        double mpten = thn - th_old;
+        mpten = mpten < lim * dt ? mpten : lim * dt;
+        mpten = mpten > -lim * dt ? mpten : -lim * dt;
+        const double qvten = q - q_old;
+        AT(t, i, j, k) = th_old * (1.0 + rvrd * q_old) + mpten * (1.0 + rvrd * q) + rvrd * qvten * thn - T0;
+        AT(hd, i, j, k) = (mpten * (1.0 + rvrd * q) + rvrd * qvten * thn) / dt;
+      }
+  fill_halo(d, t);
+  fill_halo(d, hd);
+  for (int n = 0; n < d->o.n_moist; ++n) fill_halo(d, &d->q2[n]);
+  for (size_t n = 0; n < sizeof all / sizeof all[0]; ++n) fld_free(all[n]);
+}
+
 static void rk3_step(or_dom* d) {
   const cw_grid* g = &d->g;
   if (d->o.lbc) d->dtbc += g->dt;
@@ -1996,6 +2155,13 @@ static void rk3_step(or_dom* d) {
     scalars_run_stage(d, rk, dt_rk);
     calc_p_rho_phi_range(d, 0, g->nx, 0, g->ny);
   }
+  if (d->o.mp_physics == 1) {  /* solve_em after the RK loop (rk3.cpp:150-158) */
+    physics_step(d);
+    const int sz = 1;
+    const int px = g->bc_x == CW_BC_PERIODIC, py = g->bc_y == CW_BC_PERIODIC;
+    if (d->o.lbc) calc_p_rho_phi_range(d, px ? 0 : sz, px ? g->nx : g->nx - sz, py ? 0 : sz, py ? g->ny : g->ny - sz);
+    else calc_p_rho_phi_range(d, 0, g->nx, 0, g->ny);
+  }
   if (d->o.lbc) {
     lbc_final(d);
     const int sz = 1;
@@ -2011,6 +2177,7 @@ or_dom* or_create(const cw_grid* g, const cw_options* o) {
   d->g = *g;
   d->o = *o;
   if (g->bc_x == CW_BC_OPEN || g->bc_y == CW_BC_OPEN || o->damp_opt == 3 || o->hypsometric_opt != 1 ||
+      (o->mp_physics != 0 && (o->mp_physics != 1 || o->n_moist < 3 || g->nz > KS_LEVELS)) ||
       (o->diff_opt != 0 && (o->diff_opt != 1 || o->km_opt != 1))) {
     free(d);
     return NULL;

@@ -7,7 +7,8 @@ from cppwrf_b200 import capi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = json.load(open(os.path.join(HERE, "golden", "reference_snapshots.json")))
-KINDS = {"straka": capi.STRAKA, "warm_bubble": capi.WARM_BUBBLE, "igw": capi.IGW, "rest_state": capi.REST_STATE}
+KINDS = {"straka": capi.STRAKA, "warm_bubble": capi.WARM_BUBBLE, "igw": capi.IGW, "rest_state": capi.REST_STATE,
+         "squall2d": capi.SQUALL2D}
 BCS = {"periodic": capi.PERIODIC, "symmetric": capi.SYMMETRIC}
 
 
@@ -17,6 +18,9 @@ def ideal_case(cfg, lib=None, u0=None, **opt):
                   bc_x=BCS[cfg["bc_x"]], bc_y=BCS[cfg["bc_y"]])
     o = capi.default_options(lib, khdif=cfg["khdif"], kvdif=cfg["kvdif"], pr_inv=cfg["pr_inv"])
     o.diff_opt = 1 if (cfg["khdif"] > 0 or cfg["kvdif"] > 0) else 0
+    o.n_moist = cfg.get("n_moist", 0)
+    o.n_scalars = cfg.get("n_scalars", o.n_moist)
+    o.mp_physics = cfg.get("mp_physics", 0)
     for k, v in opt.items():
         setattr(o, k, v)
     kw = {} if u0 is None else {"u0": u0}

@@ -35,6 +35,10 @@ CASES = {
     "rest_state": dict(kind="rest_state", nx=24, ny=24, nz=40, dx=2000.0, dy=2000.0, ztop=20000.0,
                        bc_x="periodic", bc_y="periodic", dt=10.0, khdif=0.0, kvdif=0.0, pr_inv=3.0,
                        run_time=20.0),
+    # moist convection with Kessler microphysics (configs/squall2d.ini: species qv, qc, qr; mp_physics = 1)
+    "squall2d": dict(kind="squall2d", nx=120, ny=1, nz=40, dx=1000.0, dy=1000.0, ztop=20000.0, bc_x="periodic",
+                     bc_y="periodic", dt=6.0, khdif=0.0, kvdif=0.0, pr_inv=3.0, run_time=12.0, n_moist=3,
+                     mp_physics=1),
 }
 
 

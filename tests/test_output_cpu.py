@@ -6,6 +6,8 @@
 - cw_diag_header / cw_diag_format_row reproduce the golden diag.csv text (io::DiagWriter's number formatting).
 - cw_snapshot_write_host, given the oracle's state at the golden step, writes a snap_000002.bin whose every
   variable has the golden's SHA-256 and a snap_000002.json identical to the golden's text.
+- squall2d (moist convection, Kessler microphysics after the RK3 loop): the case generator, the oracle's physics
+  coupling and the writer reproduce that golden too (theta_m, qv, qc, qr, rainnc, rainncv included).
 - The moist variables of a snapshot (dry theta from theta_m, theta_m, the species under their names).
 """
 import ctypes as C
@@ -20,7 +22,7 @@ import _oracle
 import cases
 from cppwrf_b200 import capi
 
-CASES = ["straka", "warm_bubble", "igw", "rest_state"]
+CASES = ["straka", "warm_bubble", "igw", "rest_state", "squall2d"]
 
 
 def _golden_rows(name):
@@ -55,9 +57,8 @@ def test_diag_csv_text(name):
 
 
 def _snapshot_fields(orc):
-    return {"u_2": orc.array("U_2"), "v_2": orc.array("V_2"), "w_2": orc.array("W_2"), "t_2": orc.array("T_2"),
-            "p": orc.array("P"), "ph_2": orc.array("PH_2"), "mu_2": orc.array("MU_2"), "pb": orc.array("PB"),
-            "phb": orc.array("PHB"), "t_init": orc.array("T_INIT"), "mub": orc.array("MUB")}
+    names = ("U_2", "V_2", "W_2", "T_2", "P", "PH_2", "MU_2", "PB", "PHB", "T_INIT", "MUB", "RAINNC", "RAINNCV")
+    return {n.lower(): orc.array(n) for n in names}
 
 
 def _read_snapshot(directory, step):
@@ -78,7 +79,8 @@ def test_snapshot_writer_matches_golden(name, tmp_path):
     case = cases.ideal_case(cfg)
     orc = _oracle.Oracle(case, pow_mode=_oracle.POW_GLIBC)
     orc.step(gold["step"])
-    capi.snapshot_write_host(tmp_path, gold["step"], float(gold["time"]), case.g, case.o, _snapshot_fields(orc))
+    qs = [orc.array("Q_2", n) for n in range(case.o.n_scalars)]
+    capi.snapshot_write_host(tmp_path, gold["step"], float(gold["time"]), case.g, case.o, _snapshot_fields(orc), qs)
     text, meta, vars_ = _read_snapshot(str(tmp_path), gold["step"])
     assert text == gold["snap_json"]
     for var, ref in gold["variables"].items():
