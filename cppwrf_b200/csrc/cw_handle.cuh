@@ -22,6 +22,7 @@
 #include "cw_fields.hpp"
 #include "kernels_cb.cuh"
 #include "kernels_diag.cuh"
+#include "kernels_mp.cuh"
 
 namespace cw {
 
@@ -114,7 +115,8 @@ struct cw_handle {
   int nzmax = 0;
   size_t cb_level_bytes = 0;  // one shared level array of a column block: (nz + 2) x CX doubles
   // halo sets of the fill points
-  enum { H_MU1, H_PREP0, H_PREP1, H_SS0, H_UV, H_AC, H_POST, H_FIN, H_Q1PD, H_SCPD, H_Q2, H_END_P, H_WS0, H_WS1, H_N };
+  enum { H_MU1, H_PREP0, H_PREP1, H_SS0, H_UV, H_AC, H_POST, H_FIN, H_Q1PD, H_SCPD, H_Q2, H_END_P, H_WS0, H_WS1, H_MP,
+         H_MP_P, H_N };
   HaloSetHost hs[H_N];
   std::vector<CopyDesc> copies;
   CopyDesc* copies_d = nullptr;

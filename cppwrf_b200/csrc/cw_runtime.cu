@@ -168,6 +168,7 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.lbc = o.lbc; D.flat = o.flat; D.n_moist = o.n_moist; D.n_scalars = o.n_scalars;
   D.diff_on = o.diff_opt == 1; D.top_lid = o.top_lid; D.w_damping = o.w_damping; D.n_sound = M.n_sound;
   D.moist_adv_opt = o.moist_adv_opt; D.scalar_adv_opt = o.scalar_adv_opt;
+  D.mp_physics = o.mp_physics; D.mp_tend_lim = o.mp_tend_lim;
   D.dt = g.dt; D.epssm = o.epssm; D.smdiv = o.smdiv; D.emdiv = o.emdiv; D.khdif = o.khdif; D.kvdif = o.kvdif;
   D.prandtl = 1.0 / o.pr_inv;
   D.hup = o.h_adv_order == 5 ? 1.0 : 0.0;
@@ -183,6 +184,7 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   auto f3 = [&](int id) { return view3<R>(M.base[id], M.L[id]); };
   auto fb = [&](int id) { return viewb<R>(M.base[id], M.L[id]); };
   auto w3 = [&](int w) { return view3<R>(M.wbase[w], M.LW[w]); };
+  D.rainnc = f3(CW_RAINNC); D.rainncv = f3(CW_RAINNCV);
   D.u1 = f3(CW_U_1); D.u2 = f3(CW_U_2); D.v1 = f3(CW_V_1); D.v2 = f3(CW_V_2); D.w1 = f3(CW_W_1); D.w2 = f3(CW_W_2);
   D.t1 = f3(CW_T_1); D.t2 = f3(CW_T_2); D.ph1 = f3(CW_PH_1); D.ph2 = f3(CW_PH_2); D.mu1 = f3(CW_MU_1); D.mu2 = f3(CW_MU_2);
   D.p = f3(CW_P); D.al = f3(CW_AL); D.alt = f3(CW_ALT); D.php = f3(CW_PHP); D.ww = f3(CW_WW); D.mut = f3(CW_MUT);
@@ -383,6 +385,11 @@ void build_halosets_t(cw_handle* h, DevTables<R>& T) {
       add(cw_handle::H_Q2, {HaloItem{nullptr, T.qtab + kQTab * q0 + ns + n, M.Lq, HP_DEFAULT}});
     }
     add(cw_handle::H_END_P, {F(CW_P), F(CW_AL)});
+    if (M.o.mp_physics != 0) {  // PhysicsCoupling::step's halos (physics_coupling.cpp:452-456), then calc_p_rho_phi's
+      add(cw_handle::H_MP, {F(CW_T_2), F(CW_H_DIABATIC)});
+      for (int n = 0; n < M.o.n_moist; ++n) add(cw_handle::H_MP, {HaloItem{nullptr, T.qtab + kQTab * q0 + ns + n, M.Lq, HP_DEFAULT}});
+      add(cw_handle::H_MP_P, {F(CW_P), F(CW_AL)});
+    }
     add(cw_handle::H_WS0, {F(CW_U_2), F(CW_V_2)});
     add(cw_handle::H_WS1, {F(CW_W_2)});
     q0 += size_t(ns);

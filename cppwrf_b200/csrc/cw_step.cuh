@@ -151,7 +151,7 @@ struct Launcher {
 template <class R, int NM>
 void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
   const Member& M0 = h->m[0];
-  bool lbc = false, terrain = false, scalars = false, any_pd = false;
+  bool lbc = false, terrain = false, scalars = false, any_pd = false, mp = false;
   // every member specified on all four sides: the acoustic substeps read no halo cell of the fields the
   // per-substep fills (H_SS0, H_UV, H_AC) would refresh (the faces next to the boundary are the spec
   // zone's, updated from the boundary data), and the fills after the substeps (H_POST, H_FIN) refresh them
@@ -163,6 +163,7 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
     spec_all &= M.o.lbc != 0 && flat_x(M.g) && flat_y(M.g) && !two_d(M.g);
     nq = std::max(nq, M.o.n_scalars);
     lbc |= M.o.lbc != 0;
+    mp |= M.o.mp_physics != 0;
     terrain |= !M.o.flat;
     scalars |= M.o.n_scalars > 0;
     for (int n = 0; n < M.o.n_scalars; ++n)
@@ -209,6 +210,12 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
       if (lbc) L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_FLOW_DEP), rk);
       L.halo(cw_handle::H_Q2);
     }
+  }
+  if (mp) {  // the microphysics after the RK loop (PhysicsCoupling::step), then calc_p_rho_phi (rk3.cpp:150-158)
+    L.run_cb("k_kessler", RG_COLS_MASS, kCbArrays, k_kessler<R, NM>, d);
+    L.halo(cw_handle::H_MP);
+    L.run_t("k_p_rho_phi", RG_MASS, 1, KV(k_p_rho_phi), d, 2);
+    L.halo(cw_handle::H_MP_P);
   }
   if (lbc) {
     L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_FINAL), 3);

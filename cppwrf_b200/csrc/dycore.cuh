@@ -50,12 +50,15 @@ struct Dom {
   int nx, ny, nz, nyv, two_d, do_y;
   int bc_x, bc_y, spec_x, spec_y;  // spec_*: specified in that direction (degraded orders, spec zone)
   int lbc, flat, n_moist, n_scalars, diff_on, top_lid, w_damping, n_sound, moist_adv_opt, scalar_adv_opt;
+  int mp_physics;  // 1: Kessler after the RK3 loop (species 0, 1, 2 = qv, qc, qr)
+  double mp_tend_lim;
   double dt, epssm, smdiv, emdiv, khdif, kvdif, prandtl, hup, vup, w_crit_cfl;
   double* dtbc;  // device scalar: time since the boundary data (LateralBC::dtbc), advanced on the device
   double rdx, rdy, cf1, cf2, cf3, cfn, cfn1;
   const double *znu, *znw, *dnw, *dn, *rdnw, *rdn, *fnm, *fnp, *c1h, *c2h, *c1f, *c2f, *u_base, *v_base;
   const double *fcx, *gcx;  // relaxation weights per row (LateralBC::set_dt)
   // State
+  V3<T> rainnc, rainncv;  // accumulated / last-step grid-scale rain [mm] (2-D)
   V3<T> u1, u2, v1, v2, w1, w2, t1, t2, ph1, ph2, mu1, mu2, p, al, alt, php, ww, mut, muu, muv, muts, muus, muvs,
       ru, rv, rw, ru_m, rv_m, ww_m, cqu, cqv, cqw, hd;
   // Tendencies

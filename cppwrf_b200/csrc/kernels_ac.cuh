@@ -135,13 +135,16 @@ __device__ __forceinline__ void p_rho_phi_point(const Dom<R>& D, int i, int j, i
   const double base = double(R(k::r_d) * (R(k::t0) + D.t2(i, j, k)) / (R(k::p1000mb) * (a + D.alb(i, j, k))));
   D.p(i, j, k) = R(k::p1000mb * cw_pow(base, k::cpovcv) - double(D.pb(i, j, k)));
 }
+// mode 0: every mass point; 1: calc_p_rho_phi_interior (after spec_bdy_final); 2: after the microphysics, only in
+// the members that have it, on the interior where the member has boundary data (rk3.cpp:150-158)
 template <class R, int NM, int SH>
-__global__ void __launch_bounds__(PX) k_p_rho_phi(const __grid_constant__ Pack<R, NM> P, int interior) {
+__global__ void __launch_bounds__(PX) k_p_rho_phi(const __grid_constant__ Pack<R, NM> P, int mode) {
   const Dom<R>* Dp;
   int i, j, k;
   if (!thread_index<SH>(P, RG_MASS, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
-  if (interior) {  // calc_p_rho_phi_interior (:622-633): spec_zone 1 off each non-periodic side
+  if (mode == 2 && D.mp_physics == 0) return;
+  if (mode == 1 || (mode == 2 && D.lbc)) {  // calc_p_rho_phi_interior (:622-633): spec_zone 1 off each non-periodic side
     const int sz = 1;
     if (D.bc_x != CW_BC_PERIODIC && (i < sz || i >= D.nx - sz)) return;
     if (D.bc_y != CW_BC_PERIODIC && (j < sz || j >= D.ny - sz)) return;

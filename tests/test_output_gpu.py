@@ -19,7 +19,7 @@ from cases import lam_case
 from cppwrf_b200 import Batch, Domain, capi
 
 pytestmark = pytest.mark.gpu
-CASES = ["straka", "warm_bubble", "igw", "rest_state"]
+CASES = ["straka", "warm_bubble", "igw", "rest_state", "squall2d"]
 
 
 def _same(a, b):
@@ -57,10 +57,10 @@ def test_snapshot_of_device_state(name, tmp_path):
     orc.step(gold["step"])
     dev, host = tmp_path / "dev", tmp_path / "host"
     dom.snapshot(dev, gold["step"], float(gold["time"]))
-    fields = {"u_2": orc.array("U_2"), "v_2": orc.array("V_2"), "w_2": orc.array("W_2"), "t_2": orc.array("T_2"),
-              "p": orc.array("P"), "ph_2": orc.array("PH_2"), "mu_2": orc.array("MU_2"), "pb": orc.array("PB"),
-              "phb": orc.array("PHB"), "t_init": orc.array("T_INIT"), "mub": orc.array("MUB")}
-    capi.snapshot_write_host(host, gold["step"], float(gold["time"]), case.g, case.o, fields)
+    names = ("U_2", "V_2", "W_2", "T_2", "P", "PH_2", "MU_2", "PB", "PHB", "T_INIT", "MUB", "RAINNC", "RAINNCV")
+    fields = {n.lower(): orc.array(n) for n in names}
+    qs = [orc.array("Q_2", n) for n in range(case.o.n_scalars)]
+    capi.snapshot_write_host(host, gold["step"], float(gold["time"]), case.g, case.o, fields, qs)
     assert open(dev / "snap_000002.json").read() == gold["snap_json"]
     assert open(dev / "snap_000002.bin", "rb").read() == open(host / "snap_000002.bin", "rb").read()
 
