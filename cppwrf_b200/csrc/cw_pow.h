@@ -18,7 +18,7 @@
  * the oracle's interposed mode both call cw_pow instead. The accuracy is checked against
  * glibc pow and against a 60-digit decimal evaluation in tests/test_pow.py.
  *
- * cw_exp(x) is the same exponential on a double argument.
+ * cw_exp(x) is the same exponential on a double argument; cw_sin(x) a double-double Taylor series for |x| <= 2.
  *
  * Domain: any double x, y; special values follow C99 Annex F for the cases the dycore can meet
  * (x > 0 finite; NaN, 0, infinities and negative x are handled for robustness).
@@ -248,6 +248,41 @@ CW_HD double cw_pow(double x, double y) {
 CW_HD double cw_exp(double x) {
   if (x != x) return CW_ADD(x, x);
   return cw_exp_dd(x, 0.0);
+}
+
+/* sin(x) for |x| <= 2 (NaN outside): the Taylor series sin x = x sum_n (-1)^n x^(2n) / (2n+1)!, its terms n >= 4
+ * (below 2.5e-3 of the sum) in double and the first four in double-double, the last kept term 4^14 / 29! < 2^-75
+ * (advance_w's Rayleigh damping of w, damp_opt 3: sin of arguments in [0, pi/2]; the reference's CPU build takes
+ * glibc's sin there) */
+CW_HD double cw_sin(double x) {
+  if (x != x) return CW_ADD(x, x);
+  if (x == 0.0) return x;
+  if (!(x <= 2.0 && x >= -2.0)) return CW_DIV(0.0, 0.0);
+  double zh, zl;
+  cw_two_prod(x, x, &zh, &zl);
+  const double z = zh;
+  double t = 0x1.259f98b4358adp-103;               /* 1/29! */
+  t = CW_ADD(-0x1.d1ab1c2dccea3p-94, CW_MUL(z, t)); /* 1/27! */
+  t = CW_ADD(0x1.3f3ccdd165fa9p-84, CW_MUL(z, t));  /* 1/25! */
+  t = CW_ADD(-0x1.761b41316381ap-75, CW_MUL(z, t)); /* 1/23! */
+  t = CW_ADD(0x1.71b8ef6dcf572p-66, CW_MUL(z, t));  /* 1/21! */
+  t = CW_ADD(-0x1.2f49b46814157p-57, CW_MUL(z, t)); /* 1/19! */
+  t = CW_ADD(0x1.952c77030ad4ap-49, CW_MUL(z, t));  /* 1/17! */
+  t = CW_ADD(-0x1.ae7f3e733b81fp-41, CW_MUL(z, t)); /* 1/15! */
+  t = CW_ADD(0x1.6124613a86d09p-33, CW_MUL(z, t));  /* 1/13! */
+  t = CW_ADD(-0x1.ae64567f544e4p-26, CW_MUL(z, t)); /* 1/11! */
+  t = CW_ADD(0x1.71de3a556c734p-19, CW_MUL(z, t));  /* 1/9! */
+  double ah, al;
+  cw_dd_add(-0x1.a01a01a01a01ap-13, -0x1.a01a01a01a01ap-73, CW_MUL(z, t), 0.0, &ah, &al); /* -1/7! + z t */
+  cw_dd_mul(zh, zl, ah, al, &ah, &al);
+  cw_dd_add(0x1.1111111111111p-7, 0x1.1111111111111p-63, ah, al, &ah, &al); /* 1/5! + z A */
+  cw_dd_mul(zh, zl, ah, al, &ah, &al);
+  cw_dd_add(-0x1.5555555555555p-3, -0x1.5555555555555p-57, ah, al, &ah, &al); /* -1/3! + z A */
+  cw_dd_mul(zh, zl, ah, al, &ah, &al);
+  cw_dd_add(1.0, 0.0, ah, al, &ah, &al); /* 1 + z A */
+  double sh, sl;
+  cw_dd_mul(x, 0.0, ah, al, &sh, &sl);
+  return CW_ADD(sh, sl);
 }
 
 #endif /* CW_POW_H */

@@ -169,6 +169,7 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.diff_on = o.diff_opt == 1; D.top_lid = o.top_lid; D.w_damping = o.w_damping; D.n_sound = M.n_sound;
   D.moist_adv_opt = o.moist_adv_opt; D.scalar_adv_opt = o.scalar_adv_opt;
   D.mp_physics = o.mp_physics; D.mp_tend_lim = o.mp_tend_lim;
+  D.damp_opt = o.damp_opt; D.zdamp = o.zdamp; D.dampcoef = o.dampcoef;
   D.dt = g.dt; D.epssm = o.epssm; D.smdiv = o.smdiv; D.emdiv = o.emdiv; D.khdif = o.khdif; D.kvdif = o.kvdif;
   D.prandtl = 1.0 / o.pr_inv;
   D.hup = o.h_adv_order == 5 ? 1.0 : 0.0;

@@ -50,6 +50,8 @@ struct Dom {
   int nx, ny, nz, nyv, two_d, do_y;
   int bc_x, bc_y, spec_x, spec_y;  // spec_*: specified in that direction (degraded orders, spec zone)
   int lbc, flat, n_moist, n_scalars, diff_on, top_lid, w_damping, n_sound, moist_adv_opt, scalar_adv_opt;
+  int damp_opt;  // 3: implicit Rayleigh damping of w in the upper zdamp metres (advance_w)
+  double zdamp, dampcoef;
   int mp_physics;  // 1: Kessler after the RK3 loop (species 0, 1, 2 = qv, qc, qr)
   double mp_tend_lim;
   double dt, epssm, smdiv, emdiv, khdif, kvdif, prandtl, hup, vup, w_crit_cfl;

@@ -542,6 +542,24 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
       }
     }
     __syncthreads();
+    if (D.damp_opt == 3) {  // damp_opt 3: implicit Rayleigh damping of w toward 0 near the top (KWSolve :393-404)
+      if (dyn) {
+        const R dampmag = dts * R(D.dampcoef), hdepth = R(D.zdamp), pi = R(0x1.921fb54442d18p+1);  // 4 atan(1)
+        const R htop = (D.ph_save.ld(i, j, nz) + D.phb(i, j, nz)) / R(k::g), hbot = htop - hdepth;
+        CB_LOOP_SH(k, nz + 1) {
+          if (k >= 1) {
+            const R hk = (D.ph_save.ld(i, j, k) + D.phb(i, j, k)) / R(k::g);
+            R dampwt = 0;
+            if (hk >= hbot) {
+              const R sn = R(cw_sin(double(R(0.5) * pi * (hk - hbot) / hdepth)));
+              dampwt = dampmag * sn * sn;
+            }
+            s2[k * CX + lane] = A(R((R(s2[k * CX + lane]) - dampwt * mf_(D, k, mut) * D.w_save.ld(i, j, k)) / (R(1) + dampwt)));
+          }
+        }
+      }
+      __syncthreads();  // the member's option: uniform over the block
+    }
     // w'' and phi'' (dyn columns), then calc_p_rho of the level (every mass column, phase 4) from the new
     // phi'' of levels k and k + 1: recomputed from the shared terms here (the same expression as the store),
     // read back for the spec zone (written before the last barriers) and for the unchanged level 0

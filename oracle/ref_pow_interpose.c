@@ -1,7 +1,8 @@
 /* SPDX-License-Identifier: GPL-3.0-or-later
  * TEST INFRASTRUCTURE ONLY: linked into _ref/ref_harness_own ahead of libm / libmvec, it binds the two
  * pow entry points the reference's CPU build calls in calc_p_rho_phi (scalar libm pow and libmvec's
- * 2-lane _ZGVbN2vv_pow, src/core/backend.hpp:118, :169-175) to cw_pow, the pow of the GPU path. The
+ * 2-lane _ZGVbN2vv_pow, src/core/backend.hpp:118, :169-175) to cw_pow, the pow of the GPU path, and the
+ * scalar sin of advance_w's damp_opt 3 damping (src/dyn/small_step.cpp:400, its only sin) to cw_sin. The
  * reference's every other operation is unchanged, so bit-identity with this build is a fair test of them. */
 #include <emmintrin.h>
 
@@ -15,3 +16,5 @@ __m128d _ZGVbN2vv_pow(__m128d x, __m128d y) {
   _mm_storeu_pd(b, y);
   return _mm_set_pd(cw_pow(a[1], b[1]), cw_pow(a[0], b[0]));
 }
+
+double sin(double x) { return cw_sin(x); }

@@ -10,8 +10,9 @@
  * periodic / symmetric / specified lateral boundaries, flat or terrain base state, any hybrid
  * coefficients, moist species (calc_cq, positive-definite scalar advection at rk 3), passive
  * tracers, constant-K diffusion (diff_opt 1, km_opt 1), specified lateral boundaries (width 5),
- * top_lid, w_damping, h/v_adv_order 5/6, 3/4. Not restated (rejected by or_create): open
- * boundaries, map factors other than 1, Coriolis, damp_opt 3, hypsometric_opt 2.
+ * top_lid, w_damping, h/v_adv_order 5/6, 3/4, damp_opt 3 (sin by the pow mode: glibc's or cw_sin), Kessler
+ * microphysics. Not restated (rejected by or_create): open boundaries, map factors other than 1, Coriolis,
+ * damp_opt 1 and 2, hypsometric_opt 2.
  */
 #include "wrf_oracle.h"
 
@@ -1598,6 +1599,20 @@ static void small_run_stage(or_dom* d, double dts, int n_small, int rk_step) {
         for (int k = 1; k <= nz; ++k)
           AT(w, i, j, k) = (AT(w, i, j, k) - AT(a, i, j, k) * AT(w, i, j, k - 1)) * AT(alpha, i, j, k);
         for (int k = nz - 1; k >= 1; --k) AT(w, i, j, k) = AT(w, i, j, k) - AT(gamma, i, j, k) * AT(w, i, j, k + 1);
+        if (d->o.damp_opt == 3) { /* implicit Rayleigh damping of w near the top (KWSolve :393-404) */
+          const double dampmag = dts * d->o.dampcoef, hdepth = d->o.zdamp, pi = 4.0 * atan(1.0), m = AT(F_(CW_MUT), i, j, 0);
+          const double htop = (AT(&d->ph_save, i, j, nz) + AT(F_(CW_PHB), i, j, nz)) / G_, hbot = htop - hdepth;
+          for (int k = nz; k >= 1; --k) {
+            const double hk = (AT(&d->ph_save, i, j, k) + AT(F_(CW_PHB), i, j, k)) / G_;
+            double dampwt = 0;
+            if (hk >= hbot) {
+              const double x = H * pi * (hk - hbot) / hdepth;
+              const double sn = d->pow_mode == OR_POW_GLIBC ? sin(x) : cw_sin(x);
+              dampwt = dampmag * sn * sn;
+            }
+            AT(w, i, j, k) = (AT(w, i, j, k) - dampwt * mf_(d, k, m) * AT(&d->w_save, i, j, k)) / (1.0 + dampwt);
+          }
+        }
         for (int k = nz; k >= 1; --k)
           AT(ph, i, j, k) = AT(R, i, j, k) + AT(msfty, i, j, 0) * H * dts * G_ * ope * AT(w, i, j, k) / mf_(d, k, mts);
       }
@@ -2176,7 +2191,7 @@ or_dom* or_create(const cw_grid* g, const cw_options* o) {
   or_dom* d = (or_dom*)calloc(1, sizeof(or_dom));
   d->g = *g;
   d->o = *o;
-  if (g->bc_x == CW_BC_OPEN || g->bc_y == CW_BC_OPEN || o->damp_opt == 3 || o->hypsometric_opt != 1 ||
+  if (g->bc_x == CW_BC_OPEN || g->bc_y == CW_BC_OPEN || (o->damp_opt != 0 && o->damp_opt != 3) || o->hypsometric_opt != 1 ||
       (o->mp_physics != 0 && (o->mp_physics != 1 || o->n_moist < 3 || g->nz > KS_LEVELS)) ||
       (o->diff_opt != 0 && (o->diff_opt != 1 || o->km_opt != 1))) {
     free(d);

@@ -68,3 +68,20 @@ def test_oracle_equals_reference_default_glibc_pow():
     ref = _refdump.run(case, 3, own_pow=False)
     bad = compare(orc, ref, case)
     assert not bad, "\n".join(bad)
+
+
+@pytest.mark.parametrize("own", [True, False], ids=["cw_pow_cw_sin", "glibc"])
+def test_oracle_equals_reference_w_rayleigh_damping(own):
+    """damp_opt 3 (advance_w's implicit Rayleigh damping of w in the upper 8 km): with our pow and sin in both,
+    and with glibc's in both."""
+    case = lam_case(seed=7)
+    case.o.damp_opt, case.o.zdamp, case.o.dampcoef = 3, 8000.0, 0.2
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_OWN if own else _oracle.POW_GLIBC)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=own)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)
+    plain = lam_case(seed=7)
+    undamped = _oracle.Oracle(plain, pow_mode=_oracle.POW_OWN if own else _oracle.POW_GLIBC)
+    undamped.step(3)
+    assert not np.array_equal(orc.array("W_2"), undamped.array("W_2"))  # the damping acted

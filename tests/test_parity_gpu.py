@@ -82,6 +82,15 @@ def test_lam_bit_exact(kw):
     assert not bad, "\n".join(bad)
 
 
+def test_lam_w_rayleigh_damping_bit_exact():
+    """damp_opt 3: advance_w's implicit Rayleigh damping of w in the upper 8 km (sin = cw_sin on both sides)."""
+    case = lam_case(seed=7)
+    case.o.damp_opt, case.o.zdamp, case.o.dampcoef = 3, 8000.0, 0.2
+    dom, orc = run_pair(case, 4)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
 def test_benchmark_workload_bit_exact():
     """The benchmark's 119 x 89 x 44 workload (bench.py), 2 steps."""
     import bench

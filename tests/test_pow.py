@@ -1,5 +1,5 @@
 # SPDX-License-Identifier: GPL-3.0-or-later
-"""Accuracy of cw_pow (the dycore's own pow): against glibc's pow and against a 60-digit decimal evaluation."""
+"""Accuracy of the dycore's own pow, exp and sin (cw_pow.h): against glibc's and against 60-digit decimal evaluations."""
 import ctypes as C
 import math
 import os
@@ -14,6 +14,8 @@ ROOT = _oracle.ROOT
 SRC = r"""
 #include "cw_pow.h"
 double cwp(double x, double y) { return cw_pow(x, y); }
+double cwe(double x) { return cw_exp(x); }
+double cws(double x) { return cw_sin(x); }
 """
 
 
@@ -26,6 +28,9 @@ def _lib(tmp_path):
     lib = C.CDLL(str(so))
     lib.cwp.restype = C.c_double
     lib.cwp.argtypes = [C.c_double, C.c_double]
+    for f in (lib.cwe, lib.cws):
+        f.restype = C.c_double
+        f.argtypes = [C.c_double]
     return lib
 
 
@@ -66,3 +71,47 @@ def test_pow_special_values(tmp_path):
     assert lib.cwp(-2.0, 3.0) == -8.0
     assert math.isinf(lib.cwp(math.inf, 1.4))
     assert lib.cwp(1e-310, 1.4) == math.pow(1e-310, 1.4)
+
+
+def _dec_sin(x):
+    getcontext().prec = 60
+    x = Decimal(x)
+    s, term, n = Decimal(0), x, 1
+    while term != 0 and (s == 0 or abs(term) > abs(s) * Decimal(10) ** -58):
+        s += term
+        term = -term * x * x / ((n + 1) * (n + 2))
+        n += 2
+    return s
+
+
+def test_sin_within_half_ulp_plus(tmp_path):
+    """cw_sin on damp_opt 3's range [0, pi/2] (and to |x| <= 2): within 0.5001 ulp of the exact value."""
+    lib = _lib(tmp_path)
+    rng = np.random.default_rng(3)
+    worst = Decimal(0)
+    for x in list(rng.uniform(0.0, 2.0, 400)) + [1e-300, 1e-8, math.pi / 2]:
+        got = lib.cws(float(x))
+        exact = _dec_sin(float(x))
+        worst = max(worst, abs(Decimal(got) - exact) / Decimal(math.ulp(float(exact))))
+    assert worst < Decimal("0.5001"), worst
+    assert math.copysign(1.0, lib.cws(-0.0)) == -1.0 and lib.cws(-1.0) == -lib.cws(1.0)
+    assert math.isnan(lib.cws(2.5)) and math.isnan(lib.cws(math.nan))
+
+
+def test_sin_agrees_with_glibc_to_one_ulp(tmp_path):
+    lib = _lib(tmp_path)
+    for x in np.random.default_rng(4).uniform(0.0, math.pi / 2, 5000):
+        a, b = lib.cws(float(x)), math.sin(float(x))
+        assert abs(a - b) <= math.ulp(b), (x, a, b)
+
+
+def test_exp_within_half_ulp_plus(tmp_path):
+    """cw_exp (the Kessler saturation vapour pressure) within 0.5001 ulp of the exact value."""
+    lib = _lib(tmp_path)
+    getcontext().prec = 60
+    worst = Decimal(0)
+    for x in np.random.default_rng(5).uniform(-30.0, 30.0, 400):
+        exact = Decimal(float(x)).exp()
+        worst = max(worst, abs(Decimal(lib.cwe(float(x))) - exact) / Decimal(math.ulp(float(exact))))
+    assert worst < Decimal("0.5001"), worst
+    assert lib.cwe(0.0) == 1.0 and math.isinf(lib.cwe(800.0)) and lib.cwe(-800.0) == 0.0 and math.isnan(lib.cwe(math.nan))
