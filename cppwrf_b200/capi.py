@@ -59,7 +59,8 @@ class Options(C.Structure):
                 ("dampcoef", C.c_double), ("time_step_sound", C.c_int), ("moist_adv_opt", C.c_int),
                 ("scalar_adv_opt", C.c_int), ("tke_adv_opt", C.c_int), ("diff_opt", C.c_int), ("km_opt", C.c_int),
                 ("flat", C.c_int), ("n_moist", C.c_int), ("n_scalars", C.c_int), ("lbc", C.c_int),
-                ("precision", C.c_int), ("mp_physics", C.c_int), ("mp_tend_lim", C.c_double)]
+                ("precision", C.c_int), ("mp_physics", C.c_int), ("mp_tend_lim", C.c_double),
+                ("diff_6th_opt", C.c_int), ("diff_6th_factor", C.c_double)]
 
 
 _DP = C.POINTER(C.c_double)

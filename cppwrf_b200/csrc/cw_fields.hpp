@@ -132,6 +132,7 @@ inline const char* unsupported(const cw_grid& g, const cw_options& o) {
   if (o.precision != CW_FP64 && o.precision != CW_MIXED) return "precision must be CW_FP64 or CW_MIXED";
   const int ns = sound_steps(g, o);
   if (ns < 2 || ns % 2) return "time_step_sound must be even and >= 2";
+  if (o.diff_6th_opt < 0 || o.diff_6th_opt > 2) return "diff_6th_opt must be 0, 1 or 2";
   if (o.mp_physics != 0 && o.mp_physics != 1) return "mp_physics must be 0 or 1 (Kessler)";
   if (o.mp_physics == 1 && o.n_moist < 3) return "Kessler microphysics needs the moist species qv, qc, qr (0, 1, 2)";
   if (o.mp_physics == 1 && !(o.mp_tend_lim > 0)) return "mp_tend_lim must be > 0";

@@ -170,6 +170,8 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.moist_adv_opt = o.moist_adv_opt; D.scalar_adv_opt = o.scalar_adv_opt;
   D.mp_physics = o.mp_physics; D.mp_tend_lim = o.mp_tend_lim;
   D.damp_opt = o.damp_opt; D.zdamp = o.zdamp; D.dampcoef = o.dampcoef;
+  D.diff_6th_opt = o.diff_6th_opt; D.diff_6th_factor = o.diff_6th_factor;
+  D.dd_on = o.diff_opt == 1 || o.diff_6th_opt != 0;  // DiffusionConfig::on (damp_opt 2 is not supported)
   D.dt = g.dt; D.epssm = o.epssm; D.smdiv = o.smdiv; D.emdiv = o.emdiv; D.khdif = o.khdif; D.kvdif = o.kvdif;
   D.prandtl = 1.0 / o.pr_inv;
   D.hup = o.h_adv_order == 5 ? 1.0 : 0.0;

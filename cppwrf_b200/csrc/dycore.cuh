@@ -50,6 +50,9 @@ struct Dom {
   int nx, ny, nz, nyv, two_d, do_y;
   int bc_x, bc_y, spec_x, spec_y;  // spec_*: specified in that direction (degraded orders, spec zone)
   int lbc, flat, n_moist, n_scalars, diff_on, top_lid, w_damping, n_sound, moist_adv_opt, scalar_adv_opt;
+  int dd_on;     // a DiffusionDriver is attached (diff_opt 1 or the sixth-order filter): the tendf enter the tendencies
+  int diff_6th_opt;
+  double diff_6th_factor;
   int damp_opt;  // 3: implicit Rayleigh damping of w in the upper zdamp metres (advance_w)
   double zdamp, dampcoef;
   int mp_physics;  // 1: Kessler after the RK3 loop (species 0, 1, 2 = qv, qc, qr)

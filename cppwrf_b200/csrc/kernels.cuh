@@ -623,7 +623,7 @@ __global__ void __launch_bounds__(PX) k_tend(const __grid_constant__ Pack<R, NM>
   const Dom<R>& D = *Dp;
   const int tx = int(threadIdx.x) % SX, ty = int(threadIdx.x) / SX;
   const int nx = D.nx, ny = D.ny, nz = D.nz;
-  const bool use_tendf = D.lbc || D.diff_on;
+  const bool use_tendf = D.lbc || D.dd_on;
   const int ui0 = D.bc_x != CW_BC_PERIODIC ? 1 : 0;
   const int vj0 = (D.bc_y != CW_BC_PERIODIC && D.do_y) ? 1 : 0;
   const bool dy = D.do_y;
@@ -865,6 +865,74 @@ __device__ __forceinline__ R vdiff_uv(const Dom<R>& D, const V3<R>& f, const dou
 
 // rk 1: zero the held tendencies, add the constant-K diffusion; with lateral boundaries mu_tend = 0 and the
 // relaxation of rows 1..3 (LateralBC::relax_dry, lateral_bc.cpp:294-335) added to the held tendencies
+// sixth_order_diffusion (src/dyn/diffusion/sixth_order.hpp:13-183): the sixth-order horizontal filter of the first
+// RK stage. d6(f, c) is the flux difference of the face below point c along (DI, DJ), zeroed against the local
+// gradient when flux-limited (diff_6th_opt 2); the kinds differ in the masses averaged to the faces.
+template <class R, int DI, int DJ>
+__device__ __forceinline__ R d6(const V3<R>& f, int i, int j, int k, int opt) {
+  auto F = [&](int s) { return f.ld(i + s * DI, j + s * DJ, k); };
+  R d = R(10.0) * (F(0) - F(-1)) - R(5.0) * (F(1) - F(-2)) + (F(2) - F(-3));
+  if (opt == 2 && d * (F(0) - F(-1)) <= R(0)) d = R(0);
+  return d;
+}
+// the filter's index ranges (sixth_order.hpp:151-180): kind 'u', 'v', or 'm' (also w's levels 1..nz-1)
+__device__ __forceinline__ bool d6_in(char kind, int nx, int ny, bool sp, bool px, int i, int j) {
+  int is = 0, js = 0, ie, je;
+  if (kind == 'u') {
+    ie = nx + 1; je = ny;
+    if (sp) { is = 3; ie = nx - 2; js = 3; je = ny - 3; }
+    if (px) { is = 0; ie = nx + 1; }
+  } else if (kind == 'v') {
+    ie = nx; je = ny + 1;
+    if (sp) { is = 3; ie = nx - 3; js = 3; je = ny - 2; }
+    if (px) { is = 0; ie = nx; }
+  } else {
+    ie = nx; je = ny;
+    if (sp) { is = 3; ie = nx - 3; js = 3; je = ny - 3; }
+    if (px) { is = 0; ie = nx; }
+  }
+  return i >= is && i < ie && j >= js && j < je;
+}
+// the x and y parts of the filter's tendency at (i, j, k) (KSixthOrderU / V / M), coef = factor / 64 / (2 dt)
+template <class R>
+__device__ __forceinline__ void d6_tend(const Dom<R>& D, char kind, const V3<R>& f, const V3<R>& mut, const double* c1v,
+                                        const double* c2v, R coef, int i, int j, int k, R& tx, R& ty) {
+  const int opt = D.diff_6th_opt;
+  const R c1 = R(c1v[k]), c2 = R(c2v[k]);
+  auto M = [&](int a, int b) { return c1 * mut.ld(a, b, 0) + c2; };
+  const R fx0 = d6<R, 1, 0>(f, i, j, k, opt), fx1 = d6<R, 1, 0>(f, i + 1, j, k, opt);
+  const R fy0 = d6<R, 0, 1>(f, i, j, k, opt), fy1 = d6<R, 0, 1>(f, i, j + 1, k, opt);
+  R mx0, mx1, my0, my1, sx, sy;
+  if (kind == 'u') {
+    mx0 = M(i - 1, j);
+    mx1 = M(i, j);
+    my0 = R(0.25) * (M(i - 1, j - 1) + M(i, j - 1) + M(i - 1, j) + M(i, j));
+    my1 = R(0.25) * (M(i - 1, j) + M(i, j) + M(i - 1, j + 1) + M(i, j + 1));
+    sx = D.msfux(i, j);
+    sy = D.msfuy(i, j);
+  } else if (kind == 'v') {
+    mx0 = R(0.25) * (M(i - 1, j - 1) + M(i, j - 1) + M(i - 1, j) + M(i, j));
+    mx1 = R(0.25) * (M(i, j - 1) + M(i + 1, j - 1) + M(i, j) + M(i + 1, j));
+    my0 = M(i, j - 1);
+    my1 = M(i, j);
+    sx = D.msfvx(i, j);
+    sy = D.msfvy(i, j);
+  } else {
+    mx0 = R(0.5) * (M(i - 1, j) + M(i, j));
+    mx1 = R(0.5) * (M(i, j) + M(i + 1, j));
+    my0 = R(0.5) * (M(i, j - 1) + M(i, j));
+    my1 = R(0.5) * (M(i, j) + M(i, j + 1));
+    sx = D.msftx(i, j);
+    sy = D.msfty(i, j);
+  }
+  tx = coef * sx * (mx1 * fx1 - mx0 * fx0);
+  ty = coef * sy * (my1 * fy1 - my0 * fy0);
+}
+template <class R>
+__device__ __forceinline__ R d6_coef(const Dom<R>& D, R dt) {
+  return R(D.diff_6th_factor) * R(0.015625) / (R(2.0) * dt);
+}
+
 template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R, NM> P) {
   const Dom<R>* Dp;
@@ -877,6 +945,8 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
   const bool px = D.bc_x == CW_BC_PERIODIC;
   const R khdif = R(D.khdif), kvdif = R(D.kvdif);
   const R khh = R(D.khdif / D.prandtl);
+  const bool d6on = D.diff_6th_opt != 0 && D.diff_6th_factor != 0.0;  // sixth_order_diffusion (diffusion_driver.cpp:266-280)
+  const R c6 = d6_coef(D, R(D.dt));
   if (j < ny && k < nz) {  // ru_tendf: U points [0, nx] x [0, ny) x [0, nz)
     R t = 0;
     if (dd) {
@@ -887,6 +957,11 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
       int vis = sp ? 1 : 0, vie = sp ? nx : nx + 1;
       if (px) { vis = 0; vie = nx + 1; }
       if (i >= vis && i < vie && k < nz - 1) t += vdiff_uv<R, 1, 0>(D, D.u2, D.u_base, D.muu, kvdif, i, j, k);
+    }
+    if (d6on && d6_in('u', nx, ny, sp, px, i, j)) {
+      R tx, ty;
+      d6_tend(D, 'u', D.u2, D.mut, D.c1h, D.c2h, c6, i, j, k, tx, ty);
+      t = t + tx + ty;
     }
     R fa, fb;
     if (sp && relax_at<R, false>(D, D.ru, nullptr, nullptr, D.lbc_var[0], ring_for(nx, ny, 'u'), i, j, k, fa, fb))
@@ -903,6 +978,11 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
       const int vjs = sp ? 1 : 0, vje = sp ? ny : ny + 1;
       if (j >= vjs && j < vje && k < nz - 1) t += vdiff_uv<R, 0, 1>(D, D.v2, D.v_base, D.muv, kvdif, i, j, k);
     }
+    if (d6on && D.do_y && d6_in('v', nx, ny, sp, px, i, j)) {
+      R tx, ty;
+      d6_tend(D, 'v', D.v2, D.mut, D.c1h, D.c2h, c6, i, j, k, tx, ty);
+      t = t + tx + ty;
+    }
     R fa, fb;
     if (sp && relax_at<R, false>(D, D.rv, nullptr, nullptr, D.lbc_var[1], ring_for(nx, ny, 'v'), i, j, k, fa, fb))
       t += (fa - fb) * D.msfvx(i, j);
@@ -917,6 +997,11 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
       if (i >= is && i < ie && j >= js && j < je) tw += hdiff_w(D, D.w2, D.mut, khdif, i, j, k);
       tw += vdiff_w(D, D.w2, D.mut, kvdif, i, j, k);
     }
+    if (d6on && k >= 1 && k < nz && d6_in('m', nx, ny, sp, px, i, j)) {
+      R tx, ty;
+      d6_tend(D, 'w', D.w2, D.mut, D.c1f, D.c2f, c6, i, j, k, tx, ty);
+      tw = tw + tx + ty;
+    }
     D.rw_tendf(i, j, k) = tw;
     R fa, fb;
     R tp = 0;
@@ -930,6 +1015,11 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
         if (px) { is = 0; ie = nx; }
         if (i >= is && i < ie && j >= js && j < je) tt += hdiff_m(D, D.t2, &D.t_init, D.mut, khh, i, j, k);
         tt += vdiff_m(D, D.t2, &D.t_init, D.mut, R(3.) * kvdif, i, j, k);
+      }
+      if (d6on && d6_in('m', nx, ny, sp, px, i, j)) {
+        R tx, ty;
+        d6_tend(D, 'm', D.t2, D.mut, D.c1h, D.c2h, c6, i, j, k, tx, ty);
+        tt = tt + tx + ty;
       }
       if (sp && relax_at<R, false>(D, D.t2, D.c1h, D.c2h, D.lbc_var[2], ring_for(nx, ny, 't'), i, j, k, fa, fb)) tt += fa - fb;
       D.t_tendf(i, j, k) = tt;

@@ -191,6 +191,11 @@ __global__ void __launch_bounds__(PX) k_q_tendf_rk1(const __grid_constant__ Pack
     const bool qv = n == 0 && D.n_moist > 0;
     t += vdiff_m(D, D.q2[n], qv ? &D.qv_base : (const VB<R>*)nullptr, D.muts, kvdq, i, j, k);
   }
+  if (D.diff_6th_opt != 0 && D.diff_6th_factor != 0.0 && d6_in('m', D.nx, D.ny, sp, px, i, j)) {
+    R tx, ty;  // DiffusionDriver::scalar (diffusion_driver.cpp:323-326): muts and the stage's dt / 3
+    d6_tend(D, 'm', D.q2[n], D.muts, D.c1h, D.c2h, d6_coef(D, R(D.dt / 3.0)), i, j, k, tx, ty);
+    t = t + tx + ty;
+  }
   if (sp && D.lbc_q[n].have) {
     R fa, fb;
     int sl, pos;

@@ -63,6 +63,10 @@ typedef struct cw_options {
    * run after the RK3 loop as solve_em does (src/dyn/rk3.cpp:150-158) */
   int mp_physics;
   double mp_tend_lim; /* K/s, limit on the microphysics heating rate */
+  /* DiffusionConfig (src/dyn/diffusion_driver.hpp:42-43): sixth-order horizontal filter at the first RK stage,
+   * 0 off, 1 linear, 2 flux-limited (monotonic); its factor */
+  int diff_6th_opt;
+  double diff_6th_factor;
 } cw_options;
 
 /* Fills o with the reference defaults (the values Model::build takes when a key is absent). */

@@ -950,6 +950,66 @@ static void vdiff_uv(or_dom* d, fld* field, const double* ubase, fld* muu, fld* 
 
 static double prandtl(or_dom* d) { return 1.0 / d->o.pr_inv; }
 
+/* sixth_order_diffusion (src/dyn/diffusion/sixth_order.hpp:13-183), diff_6th_opt 1 (linear) or 2 (flux-limited) */
+static double d6_flux(const fld* f, int i, int j, int k, int di, int dj, int opt) {
+#define F6(s) AT(f, i + (s) * di, j + (s) * dj, k)
+  double dd = 10.0 * (F6(0) - F6(-1)) - 5.0 * (F6(1) - F6(-2)) + (F6(2) - F6(-3));
+  if (opt == 2 && dd * (F6(0) - F6(-1)) <= 0) dd = 0;
+#undef F6
+  return dd;
+}
+static void sixth_order(or_dom* d, char kind, fld* f, fld* tend, fld* mut, double dt, const double* c1v, const double* c2v) {
+  const cw_grid* g = &d->g;
+  const int nx = g->nx, ny = g->ny, nz = g->nz, opt = d->o.diff_6th_opt;
+  if (opt == 0 || d->o.diff_6th_factor == 0) return;
+  const double coef = d->o.diff_6th_factor * 0.015625 / (2.0 * dt);
+  const int sp = specified(g), px = g->bc_x == CW_BC_PERIODIC;
+  int is = 0, js = 0, ie, je, k0 = 0;
+  if (kind == 'u') {
+    ie = nx + 1; je = ny;
+    if (sp) { is = 3; ie = nx - 2; js = 3; je = ny - 3; }
+    if (px) { is = 0; ie = nx + 1; }
+  } else if (kind == 'v') {
+    ie = nx; je = ny + 1;
+    if (sp) { is = 3; ie = nx - 3; js = 3; je = ny - 2; }
+    if (px) { is = 0; ie = nx; }
+  } else {
+    ie = nx; je = ny;
+    if (sp) { is = 3; ie = nx - 3; js = 3; je = ny - 3; }
+    if (px) { is = 0; ie = nx; }
+    if (kind == 'w') k0 = 1;
+  }
+  fld *sxf, *syf;
+  if (kind == 'u') { sxf = F_(CW_MSFUX); syf = F_(CW_MSFUY); }
+  else if (kind == 'v') { sxf = F_(CW_MSFVX); syf = F_(CW_MSFVY); }
+  else { sxf = F_(CW_MSFTX); syf = F_(CW_MSFTY); }
+  for (int k = k0; k < nz; ++k)
+    for (int j = js; j < je; ++j)
+      for (int i = is; i < ie; ++i) {
+        const double c1 = c1v[k], c2 = c2v[k];
+#define M6(a, b) (c1 * AT(mut, a, b, 0) + c2)
+        const double fx0 = d6_flux(f, i, j, k, 1, 0, opt), fx1 = d6_flux(f, i + 1, j, k, 1, 0, opt);
+        const double fy0 = d6_flux(f, i, j, k, 0, 1, opt), fy1 = d6_flux(f, i, j + 1, k, 0, 1, opt);
+        double mx0, mx1, my0, my1;
+        if (kind == 'u') {
+          mx0 = M6(i - 1, j); mx1 = M6(i, j);
+          my0 = 0.25 * (M6(i - 1, j - 1) + M6(i, j - 1) + M6(i - 1, j) + M6(i, j));
+          my1 = 0.25 * (M6(i - 1, j) + M6(i, j) + M6(i - 1, j + 1) + M6(i, j + 1));
+        } else if (kind == 'v') {
+          mx0 = 0.25 * (M6(i - 1, j - 1) + M6(i, j - 1) + M6(i - 1, j) + M6(i, j));
+          mx1 = 0.25 * (M6(i, j - 1) + M6(i + 1, j - 1) + M6(i, j) + M6(i + 1, j));
+          my0 = M6(i, j - 1); my1 = M6(i, j);
+        } else {
+          mx0 = 0.5 * (M6(i - 1, j) + M6(i, j)); mx1 = 0.5 * (M6(i, j) + M6(i + 1, j));
+          my0 = 0.5 * (M6(i, j - 1) + M6(i, j)); my1 = 0.5 * (M6(i, j) + M6(i, j + 1));
+        }
+#undef M6
+        const double tx = coef * AT(sxf, i, j, 0) * (mx1 * fx1 - mx0 * fx0);
+        const double ty = coef * AT(syf, i, j, 0) * (my1 * fy1 - my0 * fy0);
+        AT(tend, i, j, k) = AT(tend, i, j, k) + tx + ty;
+      }
+}
+
 static void diffusion_prepare(or_dom* d) {
   const cw_grid* g = &d->g;
   const double pr = prandtl(d);
@@ -972,47 +1032,54 @@ static void diffusion_dynamics(or_dom* d) {
   const int nx = g->nx, ny = g->ny, nz = g->nz, do_y = !two_d(g);
   int is, ie, js, je;
   fld *mut = F_(CW_MUT);
-  hdiff_range(d, 'u', &is, &ie, &js, &je);
-  for (int k = 0; k < nz; ++k)
-    for (int j = js; j < je; ++j)
-      for (int i = is; i < ie; ++i)
-        AT(F_(CW_RU_TENDF), i, j, k) += hdiff_u(d, F_(CW_U_2), mut, &d->xkmh, d->c1h, d->c2h, i, j, k);
-  if (do_y) {
-    hdiff_range(d, 'v', &is, &ie, &js, &je);
+  if (d->o.diff_opt == 1) {
+    hdiff_range(d, 'u', &is, &ie, &js, &je);
     for (int k = 0; k < nz; ++k)
       for (int j = js; j < je; ++j)
         for (int i = is; i < ie; ++i)
-          AT(F_(CW_RV_TENDF), i, j, k) += hdiff_v(d, F_(CW_V_2), mut, &d->xkmh, d->c1h, d->c2h, i, j, k);
-  }
-  hdiff_range(d, 'w', &is, &ie, &js, &je);
-  for (int k = 1; k < nz; ++k)
-    for (int j = js; j < je; ++j)
-      for (int i = is; i < ie; ++i)
-        AT(F_(CW_RW_TENDF), i, j, k) += hdiff_w(d, F_(CW_W_2), mut, &d->xkmh, d->c1f, d->c2f, i, j, k);
-  hdiff_range(d, 'm', &is, &ie, &js, &je);
-  for (int k = 0; k < nz; ++k)
-    for (int j = js; j < je; ++j)
-      for (int i = is; i < ie; ++i)
-        AT(F_(CW_T_TENDF), i, j, k) += hdiff_m(d, F_(CW_T_2), F_(CW_T_INIT), mut, &d->xkhh, d->c1h, d->c2h, i, j, k);
-  { /* vertical_diffusion_u (big_step_diffusion.hpp:459-479) */
-    const int sp = specified(g);
-    int vis = sp ? 1 : 0, vie = sp ? nx : nx + 1;
-    if (g->bc_x == CW_BC_PERIODIC) { vis = 0; vie = nx + 1; }
+          AT(F_(CW_RU_TENDF), i, j, k) += hdiff_u(d, F_(CW_U_2), mut, &d->xkmh, d->c1h, d->c2h, i, j, k);
+    if (do_y) {
+      hdiff_range(d, 'v', &is, &ie, &js, &je);
+      for (int k = 0; k < nz; ++k)
+        for (int j = js; j < je; ++j)
+          for (int i = is; i < ie; ++i)
+            AT(F_(CW_RV_TENDF), i, j, k) += hdiff_v(d, F_(CW_V_2), mut, &d->xkmh, d->c1h, d->c2h, i, j, k);
+    }
+    hdiff_range(d, 'w', &is, &ie, &js, &je);
+    for (int k = 1; k < nz; ++k)
+      for (int j = js; j < je; ++j)
+        for (int i = is; i < ie; ++i)
+          AT(F_(CW_RW_TENDF), i, j, k) += hdiff_w(d, F_(CW_W_2), mut, &d->xkmh, d->c1f, d->c2f, i, j, k);
+    hdiff_range(d, 'm', &is, &ie, &js, &je);
+    for (int k = 0; k < nz; ++k)
+      for (int j = js; j < je; ++j)
+        for (int i = is; i < ie; ++i)
+          AT(F_(CW_T_TENDF), i, j, k) += hdiff_m(d, F_(CW_T_2), F_(CW_T_INIT), mut, &d->xkhh, d->c1h, d->c2h, i, j, k);
+    { /* vertical_diffusion_u (big_step_diffusion.hpp:459-479) */
+      const int sp = specified(g);
+      int vis = sp ? 1 : 0, vie = sp ? nx : nx + 1;
+      if (g->bc_x == CW_BC_PERIODIC) { vis = 0; vie = nx + 1; }
+      for (int j = 0; j < ny; ++j)
+        for (int i = vis; i < vie; ++i)
+          vdiff_uv(d, F_(CW_U_2), d->u_base, F_(CW_MUU), F_(CW_RU_TENDF), d->o.kvdif, 1, 0, i, j);
+    }
+    if (do_y) { /* vertical_diffusion_v (:481-500) */
+      const int sp = specified(g);
+      const int vjs = sp ? 1 : 0, vje = sp ? ny : ny + 1;
+      for (int j = vjs; j < vje; ++j)
+        for (int i = 0; i < nx; ++i)
+          vdiff_uv(d, F_(CW_V_2), d->v_base, F_(CW_MUV), F_(CW_RV_TENDF), d->o.kvdif, 0, 1, i, j);
+    }
     for (int j = 0; j < ny; ++j)
-      for (int i = vis; i < vie; ++i)
-        vdiff_uv(d, F_(CW_U_2), d->u_base, F_(CW_MUU), F_(CW_RU_TENDF), d->o.kvdif, 1, 0, i, j);
+      for (int i = 0; i < nx; ++i) vdiff_w(d, F_(CW_W_2), F_(CW_RW_TENDF), mut, d->o.kvdif, i, j);
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) vdiff_m(d, F_(CW_T_2), F_(CW_T_INIT), F_(CW_T_TENDF), mut, 3. * d->o.kvdif, i, j);
   }
-  if (do_y) { /* vertical_diffusion_v (:481-500) */
-    const int sp = specified(g);
-    const int vjs = sp ? 1 : 0, vje = sp ? ny : ny + 1;
-    for (int j = vjs; j < vje; ++j)
-      for (int i = 0; i < nx; ++i)
-        vdiff_uv(d, F_(CW_V_2), d->v_base, F_(CW_MUV), F_(CW_RV_TENDF), d->o.kvdif, 0, 1, i, j);
-  }
-  for (int j = 0; j < ny; ++j)
-    for (int i = 0; i < nx; ++i) vdiff_w(d, F_(CW_W_2), F_(CW_RW_TENDF), mut, d->o.kvdif, i, j);
-  for (int j = 0; j < ny; ++j)
-    for (int i = 0; i < nx; ++i) vdiff_m(d, F_(CW_T_2), F_(CW_T_INIT), F_(CW_T_TENDF), mut, 3. * d->o.kvdif, i, j);
+  /* the sixth-order filter after the second-order terms (diffusion_driver.cpp:266-280) */
+  sixth_order(d, 'u', F_(CW_U_2), F_(CW_RU_TENDF), mut, g->dt, d->c1h, d->c2h);
+  if (do_y) sixth_order(d, 'v', F_(CW_V_2), F_(CW_RV_TENDF), mut, g->dt, d->c1h, d->c2h);
+  sixth_order(d, 'w', F_(CW_W_2), F_(CW_RW_TENDF), mut, g->dt, d->c1f, d->c2f);
+  sixth_order(d, 'm', F_(CW_T_2), F_(CW_T_TENDF), mut, g->dt, d->c1h, d->c2h);
 }
 
 static void diffusion_scalar(or_dom* d, int n) {
@@ -1020,14 +1087,17 @@ static void diffusion_scalar(or_dom* d, int n) {
   const int nx = g->nx, ny = g->ny, nz = g->nz;
   fld *q = &d->q2[n], *tend = &d->qtf[n], *muts = F_(CW_MUTS);
   int is, ie, js, je;
-  hdiff_range(d, 'm', &is, &ie, &js, &je);
-  for (int k = 0; k < nz; ++k)
-    for (int j = js; j < je; ++j)
-      for (int i = is; i < ie; ++i) AT(tend, i, j, k) += hdiff_m(d, q, NULL, muts, &d->xkhh, d->c1h, d->c2h, i, j, k);
-  const double kvdq = d->o.kvdif / prandtl(d);
-  const int is_qv = n < d->o.n_moist && n == 0; /* qv is the first moist species */
-  for (int j = 0; j < ny; ++j)
-    for (int i = 0; i < nx; ++i) vdiff_m(d, q, is_qv ? F_(CW_QV_BASE) : NULL, tend, muts, kvdq, i, j);
+  if (d->o.diff_opt == 1) {
+    hdiff_range(d, 'm', &is, &ie, &js, &je);
+    for (int k = 0; k < nz; ++k)
+      for (int j = js; j < je; ++j)
+        for (int i = is; i < ie; ++i) AT(tend, i, j, k) += hdiff_m(d, q, NULL, muts, &d->xkhh, d->c1h, d->c2h, i, j, k);
+    const double kvdq = d->o.kvdif / prandtl(d);
+    const int is_qv = n < d->o.n_moist && n == 0; /* qv is the first moist species */
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) vdiff_m(d, q, is_qv ? F_(CW_QV_BASE) : NULL, tend, muts, kvdq, i, j);
+  }
+  sixth_order(d, 'm', q, tend, muts, g->dt / 3.0, d->c1h, d->c2h); /* rk 1: dt_rk = dt / 3, muts */
 }
 
 /* ------------------------------------------------------------------ lateral boundaries
@@ -1901,7 +1971,7 @@ static void scalars_run_stage(or_dom* d, int rk, double dt_rk) {
   const int ns = d->o.n_scalars;
   if (ns == 0) return;
   if (rk == 1) {
-    if (d->o.diff_opt == 1)
+    if (d->o.diff_opt == 1 || d->o.diff_6th_opt != 0)
       for (int n = 0; n < ns; ++n) diffusion_scalar(d, n);
     if (d->o.lbc)
       for (int n = 0; n < ns; ++n) relax_scalar(d, n);
@@ -1952,7 +2022,7 @@ static void tendencies(or_dom* d, int rk) {
   const cw_grid* g = &d->g;
   const int nx = g->nx, ny = g->ny, nz = g->nz, do_y = !two_d(g);
   tctx c = {d, spec_of(g), d->o.h_adv_order == 5 ? 1.0 : 0.0, d->o.v_adv_order == 3 ? 1.0 : 0.0, nz, do_y, d->o.top_lid};
-  const int dd_on = d->o.diff_opt == 1;
+  const int dd_on = d->o.diff_opt == 1 || d->o.diff_6th_opt != 0; /* a DiffusionDriver (DiffusionConfig::on) */
   if (rk == 1) { /* zero_tendf (large_step.cpp:888-894) */
     zero_cells(d, F_(CW_PH_TENDF));
     zero_cells(d, F_(CW_RU_TENDF));
@@ -2192,6 +2262,7 @@ or_dom* or_create(const cw_grid* g, const cw_options* o) {
   d->g = *g;
   d->o = *o;
   if (g->bc_x == CW_BC_OPEN || g->bc_y == CW_BC_OPEN || (o->damp_opt != 0 && o->damp_opt != 3) || o->hypsometric_opt != 1 ||
+      o->diff_6th_opt < 0 || o->diff_6th_opt > 2 ||
       (o->mp_physics != 0 && (o->mp_physics != 1 || o->n_moist < 3 || g->nz > KS_LEVELS)) ||
       (o->diff_opt != 0 && (o->diff_opt != 1 || o->km_opt != 1))) {
     free(d);

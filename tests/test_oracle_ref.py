@@ -85,3 +85,26 @@ def test_oracle_equals_reference_w_rayleigh_damping(own):
     undamped = _oracle.Oracle(plain, pow_mode=_oracle.POW_OWN if own else _oracle.POW_GLIBC)
     undamped.step(3)
     assert not np.array_equal(orc.array("W_2"), undamped.array("W_2"))  # the damping acted
+
+
+@pytest.mark.parametrize("opt,diff", [(1, False), (2, True)], ids=["linear", "flux_limited_with_k"])
+def test_oracle_equals_reference_sixth_order_filter(opt, diff):
+    """diff_6th_opt 1 / 2: the sixth-order horizontal filter of the first RK stage (dynamics and every scalar), alone
+    and after constant-K diffusion, on a LAM case (specified boundaries: the filter skips three rows)."""
+    case = lam_case(seed=9, diff=diff)
+    case.o.diff_6th_opt, case.o.diff_6th_factor = opt, 0.12
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_OWN)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=True)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)
+
+
+def test_oracle_equals_reference_sixth_order_periodic_2d():
+    cfg = dict(cases.SMALL["straka_small"])
+    case = cases.ideal_case(cfg, diff_6th_opt=2, diff_6th_factor=0.25)
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_GLIBC)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=False)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)

@@ -91,6 +91,23 @@ def test_lam_w_rayleigh_damping_bit_exact():
     assert not bad, "\n".join(bad)
 
 
+@pytest.mark.parametrize("opt,diff", [(1, False), (2, True)], ids=["linear", "flux_limited_with_k"])
+def test_lam_sixth_order_filter_bit_exact(opt, diff):
+    """diff_6th_opt 1 / 2: the sixth-order horizontal filter (dynamics and scalars) at the first RK stage."""
+    case = lam_case(seed=9, diff=diff)
+    case.o.diff_6th_opt, case.o.diff_6th_factor = opt, 0.12
+    dom, orc = run_pair(case, 4)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
+def test_periodic_2d_sixth_order_filter_bit_exact():
+    case = cases.ideal_case(dict(cases.SMALL["straka_small"]), diff_6th_opt=2, diff_6th_factor=0.25)
+    dom, orc = run_pair(case, 3)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
 def test_benchmark_workload_bit_exact():
     """The benchmark's 119 x 89 x 44 workload (bench.py), 2 steps."""
     import bench
