@@ -126,14 +126,20 @@ __global__ void __launch_bounds__(PX) k_uv(const __grid_constant__ Pack<R, NM> P
   if (sv) D.v2(i, j, k) = vn;
 }
 
-// calc_p_rho_phi, hypsometric_opt 1 (KPRhoPhi :456-477) at (i, j, k); pow = cw_pow
+// calc_p_rho_phi, hypsometric_opt 1 (KPRhoPhi :456-477) at (i, j, k); pow in double: cw_pow in the FP64 form
+// (bit-identical with the oracle), CUDA's pow in the mixed form
+template <class R>
+__device__ __forceinline__ double eos_pow(double base) {
+  if constexpr (sizeof(R) == 4) return ::pow(base, k::cpovcv);
+  else return cw_pow(base, k::cpovcv);
+}
 template <class R>
 __device__ __forceinline__ void p_rho_phi_point(const Dom<R>& D, int i, int j, int k) {
   const R a = R(-1) / (R(D.c1h[k]) * D.muts(i, j, 0) + R(D.c2h[k])) *
               (D.alb(i, j, k) * (R(D.c1h[k]) * D.mu2(i, j, 0)) + R(D.rdnw[k]) * (D.ph2(i, j, k + 1) - D.ph2(i, j, k)));
   D.al(i, j, k) = a;
   const double base = double(R(k::r_d) * (R(k::t0) + D.t2(i, j, k)) / (R(k::p1000mb) * (a + D.alb(i, j, k))));
-  D.p(i, j, k) = R(k::p1000mb * cw_pow(base, k::cpovcv) - double(D.pb(i, j, k)));
+  D.p(i, j, k) = R(k::p1000mb * eos_pow<R>(base) - double(D.pb(i, j, k)));
 }
 // mode 0: every mass point; 1: calc_p_rho_phi_interior (after spec_bdy_final); 2: after the microphysics, only in
 // the members that have it, on the interior where the member has boundary data (rk3.cpp:150-158)
