@@ -154,7 +154,7 @@ void allocate(cw_handle* h) {
 
 // vertical array slots in Member::vert
 enum { VA_ZNU, VA_ZNW, VA_DNW, VA_DN, VA_RDNW, VA_RDN, VA_FNM, VA_FNP, VA_C1H, VA_C2H, VA_C1F, VA_C2F, VA_UB, VA_VB,
-       VA_FCX, VA_GCX };
+       VA_FCX, VA_GCX, VA_TB, VA_ZB };
 
 template <class R>
 Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
@@ -171,7 +171,7 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.mp_physics = o.mp_physics; D.mp_tend_lim = o.mp_tend_lim;
   D.damp_opt = o.damp_opt; D.zdamp = o.zdamp; D.dampcoef = o.dampcoef;
   D.diff_6th_opt = o.diff_6th_opt; D.diff_6th_factor = o.diff_6th_factor;
-  D.dd_on = o.diff_opt == 1 || o.diff_6th_opt != 0;  // DiffusionConfig::on (damp_opt 2 is not supported)
+  D.dd_on = o.diff_opt == 1 || o.diff_6th_opt != 0 || o.damp_opt == 2;  // DiffusionConfig::on
   D.dt = g.dt; D.epssm = o.epssm; D.smdiv = o.smdiv; D.emdiv = o.emdiv; D.khdif = o.khdif; D.kvdif = o.kvdif;
   D.prandtl = 1.0 / o.pr_inv;
   D.hup = o.h_adv_order == 5 ? 1.0 : 0.0;
@@ -184,6 +184,7 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.znu = va(VA_ZNU); D.znw = va(VA_ZNW); D.dnw = va(VA_DNW); D.dn = va(VA_DN); D.rdnw = va(VA_RDNW); D.rdn = va(VA_RDN);
   D.fnm = va(VA_FNM); D.fnp = va(VA_FNP); D.c1h = va(VA_C1H); D.c2h = va(VA_C2H); D.c1f = va(VA_C1F); D.c2f = va(VA_C2F);
   D.u_base = va(VA_UB); D.v_base = va(VA_VB); D.fcx = va(VA_FCX); D.gcx = va(VA_GCX);
+  D.t_base = va(VA_TB); D.z_base = va(VA_ZB);
   auto f3 = [&](int id) { return view3<R>(M.base[id], M.L[id]); };
   auto fb = [&](int id) { return viewb<R>(M.base[id], M.L[id]); };
   auto w3 = [&](int w) { return view3<R>(M.wbase[w], M.LW[w]); };
@@ -864,7 +865,7 @@ int cw_member_set_vertical(cw_handle* h, int mi, const cw_vertical* v) {
     put(VA_ZNU, v->znu, nz); put(VA_ZNW, v->znw, nz + 1); put(VA_DNW, v->dnw, nz); put(VA_DN, v->dn, nz + 1);
     put(VA_RDNW, v->rdnw, nz); put(VA_RDN, v->rdn, nz + 1); put(VA_FNM, v->fnm, nz + 1); put(VA_FNP, v->fnp, nz + 1);
     put(VA_C1H, v->c1h, nz); put(VA_C2H, v->c2h, nz); put(VA_C1F, v->c1f, nz + 1); put(VA_C2F, v->c2f, nz + 1);
-    put(VA_UB, v->u_base, nz); put(VA_VB, v->v_base, nz);
+    put(VA_UB, v->u_base, nz); put(VA_VB, v->v_base, nz); put(VA_TB, v->t_base, nz); put(VA_ZB, v->z_base, nz);
     if (M.o.lbc) {  // LateralBC::set_dt (src/dyn/lateral_bc.cpp:198-211): width 5, spec_zone 1, relax_zone 4
       const int spec_zone = 1, relax_zone = 4;
       for (int loop = spec_zone + 1; loop <= spec_zone + relax_zone; ++loop) {

@@ -933,6 +933,87 @@ __device__ __forceinline__ R d6_coef(const Dom<R>& D, R dt) {
   return R(D.diff_6th_factor) * R(0.015625) / (R(2.0) * dt);
 }
 
+// rk_rayleigh_damp, damp_opt 2 (src/dyn/diffusion/rayleigh_damp.hpp:26-245): at the first RK stage u, v, w and theta
+// relax toward the base-state profile in the upper zdamp metres, with weight dampcoef sin^2(pi/2 (1 - (ztop - z) /
+// zdamp)). Restated per point: the reference walks down each column from the top while the level's height is
+// within zdamp of the top; level k >= 1 is damped when every level from k to the top is. The base value at the
+// height is interpolated linearly in z_base. sin = cw_sin.
+template <class R>
+__device__ R ray_weight(const Dom<R>& D, R ztop, R z) {
+  const R ratio = (ztop - z) / R(D.zdamp);
+  const R m = ratio < R(1.0) ? ratio : R(1.0);
+  const R dcoef = R(1.0) - m;
+  const R s = R(cw_sin(double(R(0.5) * R(0x1.921fb54442d18p+1) * dcoef)));  // 2 asin(1) = pi
+  return s * s;
+}
+// the u / v / theta term mu (w dampcoef) (val - base(z)) of level k, zlev(kk) the column's level heights; false when
+// the level is not damped
+template <class R, class Z>
+__device__ bool ray_term(const Dom<R>& D, const double* base, R ztop, Z zlev, R mu, R val, int k, R& term) {
+  const int ktf = D.nz - 1;
+  if (k < 1) return false;
+  const R thr = ztop - R(D.zdamp);
+  for (int kk = ktf; kk >= k; --kk)
+    if (!(zlev(kk) >= thr)) return false;
+  const R z = zlev(k);
+  int k2 = ktf;
+  while (k2 > 0 && R(D.z_base[k2]) > z) k2 = k2 - 1;
+  R b;
+  if (k2 + 1 > ktf)
+    b = R(base[k2]) + (R(base[k2]) - R(base[k2 - 1])) * (z - R(D.z_base[k2])) / (R(D.z_base[k2]) - R(D.z_base[k2 - 1]));
+  else
+    b = R(base[k2]) + (R(base[k2 + 1]) - R(base[k2])) * (z - R(D.z_base[k2])) / (R(D.z_base[k2 + 1]) - R(D.z_base[k2]));
+  term = mu * (ray_weight(D, ztop, z) * R(D.dampcoef)) * (val - b);
+  return true;
+}
+template <class R>
+__device__ __forceinline__ R phz(const Dom<R>& D, int i, int j, int k) { return D.phb(i, j, k) + D.ph2.ld(i, j, k); }
+// the column pair (a, b) of a u (v) point along its direction, as KRayleighDampU (V) picks it
+__device__ __forceinline__ void ray_pair(int i, int n, bool periodic, int& a, int& b) {
+  a = (i == n) ? (periodic ? 0 : n - 1) : i;
+  b = (i == 0) ? (periodic ? n - 1 : 0) : i - 1;
+}
+template <class R>
+__device__ bool ray_u(const Dom<R>& D, int i, int j, int k, R& term) {
+  const int nz = D.nz;
+  int a, b;
+  ray_pair(i, D.nx, D.bc_x == CW_BC_PERIODIC, a, b);
+  const R ztop = R(0.5) * (D.phb(a, j, nz) + D.phb(b, j, nz) + D.ph2.ld(a, j, nz) + D.ph2.ld(b, j, nz)) / R(k::g);
+  auto zlev = [&](int kk) {
+    return R(0.25) * (D.phb(a, j, kk) + D.phb(a, j, kk + 1) + D.phb(b, j, kk) + D.phb(b, j, kk + 1) + D.ph2.ld(a, j, kk) +
+                      D.ph2.ld(a, j, kk + 1) + D.ph2.ld(b, j, kk) + D.ph2.ld(b, j, kk + 1)) / R(k::g);
+  };
+  return ray_term(D, D.u_base, ztop, zlev, R(D.c1h[k]) * D.muu.ld(i, j, 0) + R(D.c2h[k]), D.u2.ld(i, j, k), k, term);
+}
+template <class R>
+__device__ bool ray_v(const Dom<R>& D, int i, int j, int k, R& term) {
+  const int nz = D.nz;
+  int a, b;
+  ray_pair(j, D.ny, D.bc_y == CW_BC_PERIODIC, a, b);
+  const R ztop = R(0.5) * (D.phb(i, a, nz) + D.phb(i, b, nz) + D.ph2.ld(i, a, nz) + D.ph2.ld(i, b, nz)) / R(k::g);
+  auto zlev = [&](int kk) {
+    return R(0.25) * (D.phb(i, a, kk) + D.phb(i, a, kk + 1) + D.phb(i, b, kk) + D.phb(i, b, kk + 1) + D.ph2.ld(i, a, kk) +
+                      D.ph2.ld(i, a, kk + 1) + D.ph2.ld(i, b, kk) + D.ph2.ld(i, b, kk + 1)) / R(k::g);
+  };
+  return ray_term(D, D.v_base, ztop, zlev, R(D.c1h[k]) * D.muv.ld(i, j, 0) + R(D.c2h[k]), D.v2.ld(i, j, k), k, term);
+}
+template <class R>
+__device__ bool ray_t(const Dom<R>& D, int i, int j, int k, R& term) {
+  const R ztop = phz(D, i, j, D.nz) / R(k::g);
+  auto zlev = [&](int kk) {
+    return R(0.5) * (D.phb(i, j, kk) + D.phb(i, j, kk + 1) + D.ph2.ld(i, j, kk) + D.ph2.ld(i, j, kk + 1)) / R(k::g);
+  };
+  return ray_term(D, D.t_base, ztop, zlev, R(D.c1h[k]) * D.mut.ld(i, j, 0) + R(D.c2h[k]), D.t2.ld(i, j, k), k, term);
+}
+// w: every level (0..nz) within zdamp of the top, toward w = 0
+template <class R>
+__device__ bool ray_w(const Dom<R>& D, int i, int j, int k, R& term) {
+  const R ztop = phz(D, i, j, D.nz) / R(k::g), z = phz(D, i, j, k) / R(k::g);
+  if (!(z >= ztop - R(D.zdamp))) return false;
+  term = (R(D.c1f[k]) * D.mut.ld(i, j, 0) + R(D.c2f[k])) * (ray_weight(D, ztop, z) * R(D.dampcoef)) * D.w2.ld(i, j, k);
+  return true;
+}
+
 template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R, NM> P) {
   const Dom<R>* Dp;
@@ -963,6 +1044,8 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
       d6_tend(D, 'u', D.u2, D.mut, D.c1h, D.c2h, c6, i, j, k, tx, ty);
       t = t + tx + ty;
     }
+    R rt;
+    if (D.damp_opt == 2 && ray_u(D, i, j, k, rt)) t = t - rt;
     R fa, fb;
     if (sp && relax_at<R, false>(D, D.ru, nullptr, nullptr, D.lbc_var[0], ring_for(nx, ny, 'u'), i, j, k, fa, fb))
       t += (fa - fb) * D.msfuy(i, j);
@@ -983,6 +1066,11 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
       d6_tend(D, 'v', D.v2, D.mut, D.c1h, D.c2h, c6, i, j, k, tx, ty);
       t = t + tx + ty;
     }
+    R rt;
+    if (D.damp_opt == 2 && ray_v(D, i, j, k, rt)) {
+      t = t - rt;
+      if (D.two_d) t = t - rt;  // the reference's columns j = 0 and j = ny are the same storage in 2-D
+    }
     R fa, fb;
     if (sp && relax_at<R, false>(D, D.rv, nullptr, nullptr, D.lbc_var[1], ring_for(nx, ny, 'v'), i, j, k, fa, fb))
       t += (fa - fb) * D.msfvx(i, j);
@@ -1002,6 +1090,8 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
       d6_tend(D, 'w', D.w2, D.mut, D.c1f, D.c2f, c6, i, j, k, tx, ty);
       tw = tw + tx + ty;
     }
+    R rt;
+    if (D.damp_opt == 2 && ray_w(D, i, j, k, rt)) tw = tw - rt;
     D.rw_tendf(i, j, k) = tw;
     R fa, fb;
     R tp = 0;
@@ -1021,6 +1111,7 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
         d6_tend(D, 'm', D.t2, D.mut, D.c1h, D.c2h, c6, i, j, k, tx, ty);
         tt = tt + tx + ty;
       }
+      if (D.damp_opt == 2 && ray_t(D, i, j, k, rt)) tt = tt - rt;
       if (sp && relax_at<R, false>(D, D.t2, D.c1h, D.c2h, D.lbc_var[2], ring_for(nx, ny, 't'), i, j, k, fa, fb)) tt += fa - fb;
       D.t_tendf(i, j, k) = tt;
     }

@@ -194,7 +194,7 @@ int main(int argc, char** argv) {
     sp.h_adv_order = co.h_adv_order; sp.v_adv_order = co.v_adv_order;
     dyn::RK3 rk(g, lp, ap, co.time_step_sound, sp);
     std::unique_ptr<dyn::DiffusionDriver> dd;
-    if (co.diff_opt == 1 || co.diff_6th_opt != 0) {  // DiffusionConfig::on (model.cpp:439)
+    if (co.diff_opt == 1 || co.diff_6th_opt != 0 || co.damp_opt == 2) {  // DiffusionConfig::on (model.cpp:439)
       dyn::DiffusionConfig dc;
       dc.diff_opt = co.diff_opt; dc.km_opt = co.km_opt; dc.damp_opt = co.damp_opt; dc.zdamp = co.zdamp; dc.dampcoef = co.dampcoef;
       dc.diff_6th_opt = co.diff_6th_opt; dc.diff_6th_factor = co.diff_6th_factor;

@@ -2,7 +2,8 @@
  * TEST INFRASTRUCTURE ONLY: linked into _ref/ref_harness_own ahead of libm / libmvec, it binds the two
  * pow entry points the reference's CPU build calls in calc_p_rho_phi (scalar libm pow and libmvec's
  * 2-lane _ZGVbN2vv_pow, src/core/backend.hpp:118, :169-175) to cw_pow, the pow of the GPU path, and the
- * scalar sin of advance_w's damp_opt 3 damping (src/dyn/small_step.cpp:400, its only sin) to cw_sin. The
+ * scalar and libmvec 2-lane sin of the Rayleigh dampings (damp_opt 3, src/dyn/small_step.cpp:400; damp_opt 2,
+ * src/dyn/diffusion/rayleigh_damp.hpp:16-25, :136) to cw_sin. The
  * reference's every other operation is unchanged, so bit-identity with this build is a fair test of them. */
 #include <emmintrin.h>
 
@@ -18,3 +19,9 @@ __m128d _ZGVbN2vv_pow(__m128d x, __m128d y) {
 }
 
 double sin(double x) { return cw_sin(x); }
+
+__m128d _ZGVbN2v_sin(__m128d x) {
+  double a[2];
+  _mm_storeu_pd(a, x);
+  return _mm_set_pd(cw_sin(a[1]), cw_sin(a[0]));
+}

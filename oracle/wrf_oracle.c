@@ -10,9 +10,9 @@
  * periodic / symmetric / specified lateral boundaries, flat or terrain base state, any hybrid
  * coefficients, moist species (calc_cq, positive-definite scalar advection at rk 3), passive
  * tracers, constant-K diffusion (diff_opt 1, km_opt 1), specified lateral boundaries (width 5),
- * top_lid, w_damping, h/v_adv_order 5/6, 3/4, damp_opt 3 (sin by the pow mode: glibc's or cw_sin), Kessler
- * microphysics. Not restated (rejected by or_create): open boundaries, map factors other than 1, Coriolis,
- * damp_opt 1 and 2, hypsometric_opt 2.
+ * top_lid, w_damping, h/v_adv_order 5/6, 3/4, damp_opt 2 and 3 (sin by the pow mode: glibc's or cw_sin), the
+ * sixth-order filter, Kessler microphysics. Not restated (rejected by or_create): open boundaries, map factors
+ * other than 1, Coriolis, damp_opt 1, hypsometric_opt 2.
  */
 #include "wrf_oracle.h"
 
@@ -1010,6 +1010,106 @@ static void sixth_order(or_dom* d, char kind, fld* f, fld* tend, fld* mut, doubl
       }
 }
 
+/* rk_rayleigh_damp, damp_opt 2 (src/dyn/diffusion/rayleigh_damp.hpp:26-245), column by column; sin: glibc's (libmvec's
+ * on the lanes of the vectorised k loops, scalar for w) or cw_sin */
+extern __m128d _ZGVbN2v_sin(__m128d);
+#define RAY_LEVELS 128
+static double ray_sin(const or_dom* d, double x, int lane_k, int nk, int vec) {
+  if (d->pow_mode != OR_POW_GLIBC) return cw_sin(x);
+  if (vec && nk > 1 && !((nk & 1) && lane_k == nk - 1)) /* vm::lane */ return _mm_cvtsd_f64(_ZGVbN2v_sin(_mm_set1_pd(x)));
+  return sin(x);
+}
+/* the damping of one u / v / theta column: levels from the top while within zdamp, base value interpolated */
+static void ray_column(or_dom* d, double ztop, const double* zl, const double* base, const double* mu_k, const double* val,
+                       double* tend_k[]) {
+  const int ktf = d->g.nz - 1;
+  const double pii = 2.0 * asin(1.0);
+  double z00[RAY_LEVELS], b00[RAY_LEVELS];
+  int k1 = ktf;
+  double z = ztop;
+  while (k1 >= 0 && z >= (ztop - d->o.zdamp)) {
+    z = zl[k1];
+    z00[k1] = z;
+    k1 = k1 - 1;
+  }
+  k1 = k1 + 2;
+  for (int k = k1; k <= ktf; ++k) {
+    int k2 = ktf;
+    while (k2 > 0 && d->z_base[k2] > z00[k]) k2 = k2 - 1;
+    if (k2 + 1 > ktf)
+      b00[k] = base[k2] + (base[k2] - base[k2 - 1]) * (z00[k] - d->z_base[k2]) / (d->z_base[k2] - d->z_base[k2 - 1]);
+    else
+      b00[k] = base[k2] + (base[k2 + 1] - base[k2]) * (z00[k] - d->z_base[k2]) / (d->z_base[k2 + 1] - d->z_base[k2]);
+  }
+  const int nk = ktf - k1 + 1;
+  for (int k = k1; k <= ktf; ++k) {
+    const double ratio = (ztop - z00[k]) / d->o.zdamp;
+    const double m = ratio < 1.0 ? ratio : 1.0;
+    double dcoef = 1.0 - m;
+    const double sn = ray_sin(d, 0.5 * pii * dcoef, k - k1, nk, 1);
+    dcoef = sn * sn;
+    *tend_k[k] = *tend_k[k] - mu_k[k] * (dcoef * d->o.dampcoef) * (val[k] - b00[k]);
+  }
+}
+static void rayleigh_damp(or_dom* d) {
+  const cw_grid* g = &d->g;
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  fld *ph = F_(CW_PH_2), *phb = F_(CW_PHB), *mut = F_(CW_MUT);
+  const double pii = 2.0 * asin(1.0);
+  double zl[RAY_LEVELS], mu[RAY_LEVELS], val[RAY_LEVELS];
+  double* tk[RAY_LEVELS];
+  const int px = g->bc_x == CW_BC_PERIODIC, py = g->bc_y == CW_BC_PERIODIC;
+  for (int j = 0; j < ny; ++j) /* KRayleighDampU over (i, j) in [0, nx] x [0, ny) */
+    for (int i = 0; i <= nx; ++i) {
+      const int a = (i == nx) ? (px ? 0 : nx - 1) : i, b = (i == 0) ? (px ? nx - 1 : 0) : i - 1;
+      const double ztop = 0.5 * (AT(phb, a, j, nz) + AT(phb, b, j, nz) + AT(ph, a, j, nz) + AT(ph, b, j, nz)) / G_;
+      for (int k = 0; k < nz; ++k) {
+        zl[k] = 0.25 * (AT(phb, a, j, k) + AT(phb, a, j, k + 1) + AT(phb, b, j, k) + AT(phb, b, j, k + 1) + AT(ph, a, j, k) +
+                        AT(ph, a, j, k + 1) + AT(ph, b, j, k) + AT(ph, b, j, k + 1)) / G_;
+        mu[k] = d->c1h[k] * AT(F_(CW_MUU), i, j, 0) + d->c2h[k];
+        val[k] = AT(F_(CW_U_2), i, j, k);
+        tk[k] = &AT(F_(CW_RU_TENDF), i, j, k);
+      }
+      ray_column(d, ztop, zl, d->u_base, mu, val, tk);
+    }
+  for (int j = 0; j <= ny; ++j) /* KRayleighDampV over [0, nx) x [0, ny] (in 2-D row ny is row 0's storage) */
+    for (int i = 0; i < nx; ++i) {
+      const int a = (j == ny) ? (py ? 0 : ny - 1) : j, b = (j == 0) ? (py ? ny - 1 : 0) : j - 1;
+      const double ztop = 0.5 * (AT(phb, i, a, nz) + AT(phb, i, b, nz) + AT(ph, i, a, nz) + AT(ph, i, b, nz)) / G_;
+      for (int k = 0; k < nz; ++k) {
+        zl[k] = 0.25 * (AT(phb, i, a, k) + AT(phb, i, a, k + 1) + AT(phb, i, b, k) + AT(phb, i, b, k + 1) + AT(ph, i, a, k) +
+                        AT(ph, i, a, k + 1) + AT(ph, i, b, k) + AT(ph, i, b, k + 1)) / G_;
+        mu[k] = d->c1h[k] * AT(F_(CW_MUV), i, j, 0) + d->c2h[k];
+        val[k] = AT(F_(CW_V_2), i, j, k);
+        tk[k] = &AT(F_(CW_RV_TENDF), i, j, k);
+      }
+      ray_column(d, ztop, zl, d->v_base, mu, val, tk);
+    }
+  for (int j = 0; j < ny; ++j) /* KRayleighDampWT */
+    for (int i = 0; i < nx; ++i) {
+      const double ztop = (AT(phb, i, j, nz) + AT(ph, i, j, nz)) / G_;
+      for (int k = 0; k <= nz; ++k) {
+        const double z = (AT(phb, i, j, k) + AT(ph, i, j, k)) / G_;
+        if (z >= (ztop - d->o.zdamp)) {
+          const double ratio = (ztop - z) / d->o.zdamp;
+          const double m = ratio < 1.0 ? ratio : 1.0;
+          double dcoef = 1.0 - m;
+          const double sn = ray_sin(d, 0.5 * pii * dcoef, 0, 1, 0);
+          dcoef = sn * sn;
+          AT(F_(CW_RW_TENDF), i, j, k) = AT(F_(CW_RW_TENDF), i, j, k) -
+                                         (d->c1f[k] * AT(mut, i, j, 0) + d->c2f[k]) * (dcoef * d->o.dampcoef) * AT(F_(CW_W_2), i, j, k);
+        }
+      }
+      for (int k = 0; k < nz; ++k) {
+        zl[k] = 0.5 * (AT(phb, i, j, k) + AT(phb, i, j, k + 1) + AT(ph, i, j, k) + AT(ph, i, j, k + 1)) / G_;
+        mu[k] = d->c1h[k] * AT(mut, i, j, 0) + d->c2h[k];
+        val[k] = AT(F_(CW_T_2), i, j, k);
+        tk[k] = &AT(F_(CW_T_TENDF), i, j, k);
+      }
+      ray_column(d, ztop, zl, d->t_base, mu, val, tk);
+    }
+}
+
 static void diffusion_prepare(or_dom* d) {
   const cw_grid* g = &d->g;
   const double pr = prandtl(d);
@@ -1080,6 +1180,7 @@ static void diffusion_dynamics(or_dom* d) {
   if (do_y) sixth_order(d, 'v', F_(CW_V_2), F_(CW_RV_TENDF), mut, g->dt, d->c1h, d->c2h);
   sixth_order(d, 'w', F_(CW_W_2), F_(CW_RW_TENDF), mut, g->dt, d->c1f, d->c2f);
   sixth_order(d, 'm', F_(CW_T_2), F_(CW_T_TENDF), mut, g->dt, d->c1h, d->c2h);
+  if (d->o.damp_opt == 2) rayleigh_damp(d); /* after the diffusion (diffusion_driver.cpp:281-289) */
 }
 
 static void diffusion_scalar(or_dom* d, int n) {
@@ -2022,7 +2123,7 @@ static void tendencies(or_dom* d, int rk) {
   const cw_grid* g = &d->g;
   const int nx = g->nx, ny = g->ny, nz = g->nz, do_y = !two_d(g);
   tctx c = {d, spec_of(g), d->o.h_adv_order == 5 ? 1.0 : 0.0, d->o.v_adv_order == 3 ? 1.0 : 0.0, nz, do_y, d->o.top_lid};
-  const int dd_on = d->o.diff_opt == 1 || d->o.diff_6th_opt != 0; /* a DiffusionDriver (DiffusionConfig::on) */
+  const int dd_on = d->o.diff_opt == 1 || d->o.diff_6th_opt != 0 || d->o.damp_opt == 2; /* DiffusionConfig::on */
   if (rk == 1) { /* zero_tendf (large_step.cpp:888-894) */
     zero_cells(d, F_(CW_PH_TENDF));
     zero_cells(d, F_(CW_RU_TENDF));
@@ -2261,7 +2362,7 @@ or_dom* or_create(const cw_grid* g, const cw_options* o) {
   or_dom* d = (or_dom*)calloc(1, sizeof(or_dom));
   d->g = *g;
   d->o = *o;
-  if (g->bc_x == CW_BC_OPEN || g->bc_y == CW_BC_OPEN || (o->damp_opt != 0 && o->damp_opt != 3) || o->hypsometric_opt != 1 ||
+  if (g->bc_x == CW_BC_OPEN || g->bc_y == CW_BC_OPEN || (o->damp_opt != 0 && o->damp_opt != 2 && o->damp_opt != 3) || o->hypsometric_opt != 1 ||
       o->diff_6th_opt < 0 || o->diff_6th_opt > 2 ||
       (o->mp_physics != 0 && (o->mp_physics != 1 || o->n_moist < 3 || g->nz > KS_LEVELS)) ||
       (o->diff_opt != 0 && (o->diff_opt != 1 || o->km_opt != 1))) {

@@ -108,3 +108,26 @@ def test_oracle_equals_reference_sixth_order_periodic_2d():
     ref = _refdump.run(case, 3, own_pow=False)
     bad = compare(orc, ref, case)
     assert not bad, "\n".join(bad)
+
+
+@pytest.mark.parametrize("own", [True, False], ids=["cw_sin", "glibc"])
+def test_oracle_equals_reference_rayleigh_damping_to_base_state(own):
+    """damp_opt 2: the first stage's Rayleigh damping of u, v, w, theta toward the base-state profile in the upper
+    8 km (libmvec's sin on the lanes of the reference's vectorised level loops in the glibc build)."""
+    case = lam_case(seed=11)
+    case.o.damp_opt, case.o.zdamp, case.o.dampcoef = 2, 8000.0, 0.003
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_OWN if own else _oracle.POW_GLIBC)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=own)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)
+
+
+def test_oracle_equals_reference_rayleigh_damping_2d():
+    cfg = dict(cases.SMALL["igw_small"])
+    case = cases.ideal_case(cfg, damp_opt=2, zdamp=4000.0, dampcoef=0.01)
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_GLIBC)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=False)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)

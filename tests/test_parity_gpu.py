@@ -108,6 +108,22 @@ def test_periodic_2d_sixth_order_filter_bit_exact():
     assert not bad, "\n".join(bad)
 
 
+def test_lam_rayleigh_damping_to_base_state_bit_exact():
+    """damp_opt 2: u, v, w, theta damped toward the base-state profile in the upper 8 km at the first stage."""
+    case = lam_case(seed=11)
+    case.o.damp_opt, case.o.zdamp, case.o.dampcoef = 2, 8000.0, 0.003
+    dom, orc = run_pair(case, 4)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
+def test_2d_rayleigh_damping_bit_exact():
+    case = cases.ideal_case(dict(cases.SMALL["igw_small"]), damp_opt=2, zdamp=4000.0, dampcoef=0.01)
+    dom, orc = run_pair(case, 3)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
 def test_benchmark_workload_bit_exact():
     """The benchmark's 119 x 89 x 44 workload (bench.py), 2 steps."""
     import bench
