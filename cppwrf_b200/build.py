@@ -19,9 +19,9 @@ FLAGS = ["-std=c++20", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,
          "-Xptxas", "-warn-spills", "--expt-relaxed-constexpr"]
 SOURCES = ["cw_runtime.cu", "cw_step_mixed.cu", "cw_case.cpp", "cw_serve.cpp", "cw_output.cpp"]
 # The mixed form's kernels (their own translation unit) are held to a tolerance, not to bit identity: FMA
-# contraction, approximate single-precision division and square root, single-precision denormals flushed.
-MIXED_FLAGS = [f for f in FLAGS if f != "--fmad=false"] + ["--fmad=true", "--prec-div=false", "--prec-sqrt=false",
-                                                           "-ftz=true"]
+# contraction and single-precision denormals flushed; division and square root stay IEEE (approximate FP32
+# division raised the 1 h relative-L2 error of v, phi' and mu' above 1e-4 on the 400 x 400 x 60 case).
+MIXED_FLAGS = [f for f in FLAGS if f != "--fmad=false"] + ["--fmad=true", "-ftz=true"]
 
 
 def build(verbose=False):
