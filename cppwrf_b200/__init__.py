@@ -101,6 +101,12 @@ class Domain:
         _check(self.lib, self.h, 0 if rc >= 0 else rc, "cw_check_finite")
         return None if rc == 0 else (FIELDS[f.value], n.value, i.value, j.value, k.value)
 
+    def cfl_max(self, member=0):
+        """(vertical, horizontal) CFL maxima of each RK stage of the last step (cw_set_cfl_diagnostics first)."""
+        v, hz = (C.c_double * 3)(), (C.c_double * 3)()
+        _check(self.lib, self.h, self.lib.cw_cfl_max(self.h, member, v, hz), "cw_cfl_max")
+        return list(zip(v, hz))
+
     def diagnostics(self, member=0):
         """dyn::Diagnostics::compute of the current state (the diag.csv values, plus max_abs_q), as a dict."""
         d = capi.Diag()
@@ -113,6 +119,10 @@ class Domain:
         rc = self.lib.cw_snapshot_write(self.h, member, str(directory).encode(), step, time, na[0] if na else None)
         if rc != 0:
             raise CwError(f"cw_snapshot_write: {self.lib.cw_output_last_error().decode()}")
+
+    def set_cfl_diagnostics(self, on=True):
+        self.lib.cw_set_cfl_diagnostics(self.h, 1 if on else 0)
+        return self
 
     def set_autotune(self, on=True):
         """The next three steps time the point kernels' block shapes; each kernel then keeps its fastest."""

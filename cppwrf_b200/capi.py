@@ -185,6 +185,8 @@ def load(path=None):
         "cw_case_clone": (i, [vp, C.POINTER(vp)]),
         "cw_case_config": (i, [vp, C.POINTER(Grid), C.POINTER(Options)]),
         "cw_member_config": (i, [vp, i, C.POINTER(Grid), C.POINTER(Options)]),
+        "cw_set_cfl_diagnostics": (i, [vp, i]),
+        "cw_cfl_max": (i, [vp, i, dp, dp]),
         "cw_diagnostics": (i, [vp, i, C.POINTER(Diag)]),
         "cw_diag_header": (i, [C.c_char_p, sz]),
         "cw_diag_format_row": (i, [C.c_longlong, C.c_double, C.POINTER(Diag), C.c_double, C.c_char_p, sz]),

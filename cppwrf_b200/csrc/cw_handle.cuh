@@ -107,6 +107,8 @@ struct cw_handle {
   DevTables<double> t64;
   DevTables<float> t32;
   double* dtbc_d = nullptr;  // per member: time since the boundary data, advanced by the step on the device
+  unsigned long long* cfl_d = nullptr;  // per member: 3 stages x (vertical, horizontal) CFL maxima of the last step
+  bool cfl_on = false;                  // cw_set_cfl_diagnostics
   unsigned long long* diag = nullptr;  // cw_check_finite's result
   double* diag_part = nullptr;         // cw_diagnostics' per-level partials
   size_t diag_part_n = 0;

@@ -178,6 +178,7 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.vup = o.v_adv_order == 3 ? 1.0 : 0.0;
   D.w_crit_cfl = o.w_crit_cfl;
   D.dtbc = h->dtbc_d + mi;
+  D.cfl = h->cfl_d + 6 * mi;
   D.cf1 = M.cf1; D.cf2 = M.cf2; D.cf3 = M.cf3; D.cfn = M.cfn; D.cfn1 = M.cfn1; D.rdx = M.rdx; D.rdy = M.rdy;
   const double* v = M.vert;
   auto va = [&](int a) { return v + M.vert_off[a]; };
@@ -255,6 +256,10 @@ void upload_tables(cw_handle* h, DevTables<R>& T) {
   const size_t nm = h->m.size();
   if (nm == 0) return;
   if (!h->dtbc_d) CW_CUDA(cudaMalloc(&h->dtbc_d, nm * sizeof(double)));
+  if (!h->cfl_d) {
+    CW_CUDA(cudaMalloc(&h->cfl_d, 6 * nm * sizeof(unsigned long long)));
+    CW_CUDA(cudaMemsetAsync(h->cfl_d, 0, 6 * nm * sizeof(unsigned long long), h->stream));
+  }
   size_t nq = 0;
   for (const Member& M : h->m) nq += size_t(M.o.n_scalars);
   if (!T.qtab && nq) CW_CUDA(cudaMalloc(&T.qtab, kQTab * nq * sizeof(V3<R>)));
@@ -569,6 +574,8 @@ void free_tables(cw_handle* h) {
   h->copies_total = h->zeros_total = 0;
   cudaFree(h->dtbc_d);
   h->dtbc_d = nullptr;
+  cudaFree(h->cfl_d);  // member count changes with the tables: reallocated (zeroed) with them
+  h->cfl_d = nullptr;
   cudaFree(h->t64.qtab);
   cudaFree(h->t64.lbcq);
   cudaFree(h->t32.qtab);
@@ -1137,6 +1144,28 @@ int cw_diagnostics(cw_handle* h, int mi, cw_diag* out) {
     if (!h || !out || mi < 0 || mi >= int(h->m.size())) throw std::runtime_error("bad diagnostics arguments");
     if (h->precision == CW_FP64) diagnostics_t<double>(h, mi, h->t64, out);
     else diagnostics_t<float>(h, mi, h->t32, out);
+    return 0;
+  });
+}
+
+int cw_set_cfl_diagnostics(cw_handle* h, int on) {
+  if (!h) return -1;
+  h->cfl_on = on != 0;
+  invalidate_graph(h);
+  return 0;
+}
+
+int cw_cfl_max(cw_handle* h, int mi, double* vert, double* horiz) {
+  return guarded(h, [&] {
+    if (!h || !vert || !horiz || mi < 0 || mi >= int(h->m.size())) throw std::runtime_error("bad cfl arguments");
+    if (!h->cfl_on) throw std::runtime_error("CFL diagnostics are off (cw_set_cfl_diagnostics)");
+    unsigned long long b[6];
+    CW_CUDA(cudaMemcpyAsync(b, h->cfl_d + 6 * size_t(mi), sizeof b, cudaMemcpyDeviceToHost, h->stream));
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+    for (int r = 0; r < 3; ++r) {
+      vert[r] = b[2 * r] ? __builtin_bit_cast(double, b[2 * r]) : 0.0;
+      horiz[r] = b[2 * r + 1] ? __builtin_bit_cast(double, b[2 * r + 1]) : 0.0;
+    }
     return 0;
   });
 }

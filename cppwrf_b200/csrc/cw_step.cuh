@@ -173,6 +173,7 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
   if (lbc) {
     L.run_members("k_advance_time", 1, k_advance_time<R, NM>, d);
   }
+  if (h->cfl_on) CW_CUDA(cudaMemsetAsync(h->cfl_d, 0, 6 * h->m.size() * sizeof(unsigned long long), h->stream));
   L.copy_list(h->copies_d, h->copies_start_d, h->copies.size(), h->copies_total);
   L.halo(cw_handle::H_MU1);
   for (int rk = 1; rk <= 3; ++rk) {
@@ -182,6 +183,7 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
     L.halo(cw_handle::H_PREP1);
     if (rk == 1) L.run_t("k_tendf_rk1", RG_STAG, 1, KV(k_tendf_rk1), d);
     L.run_t("k_tend", RG_STAG, 1, KV(k_tend), d, rk);
+    if (h->cfl_on) L.run_t("k_cfl", RG_MASS, 1, KV(k_cfl), d, rk);
     if (rk == 1) L.copy_list(h->zeros_d, h->zeros_start_d, h->zeros.size(), h->zeros_total);
     L.run_cb("k_ss_prep", RG_COLS_STAG, 3, k_ss_prep<R, NM>, d, rk);
     if (!spec_all) L.halo(cw_handle::H_SS0);

@@ -59,6 +59,7 @@ struct Dom {
   double mp_tend_lim;
   double dt, epssm, smdiv, emdiv, khdif, kvdif, prandtl, hup, vup, w_crit_cfl;
   double* dtbc;  // device scalar: time since the boundary data (LateralBC::dtbc), advanced on the device
+  unsigned long long* cfl;  // per RK stage: the vertical and horizontal CFL maxima (bits of positive doubles)
   double rdx, rdy, cf1, cf2, cf3, cfn, cfn1;
   const double *znu, *znw, *dnw, *dn, *rdnw, *rdn, *fnm, *fnp, *c1h, *c2h, *c1f, *c2f, *u_base, *v_base;
   const double *fcx, *gcx;  // relaxation weights per row (LateralBC::set_dt)

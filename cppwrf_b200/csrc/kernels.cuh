@@ -1204,6 +1204,40 @@ __global__ void __launch_bounds__(PX) k_ring(const __grid_constant__ Pack<R, NM>
 }
 
 // LateralBC::advance_time (lateral_bc.hpp:58): dtbc += dt at the start of every step
+// LargeStep::cfl_max (src/dyn/large_step.cpp:672-687, :865-877) after stage rk's tendencies: the largest vertical
+// Courant number |ww / (c1f mut + c2f) rdnw dt| and horizontal one max(|u rdx msfux dt|, |v rdy msfvy dt|) over the
+// mass points of levels 1 .. nz-1. Maxima do not depend on the order: each block folds its values and raises the
+// member's maxima by an atomic max on the bits of the positive doubles (NaN and zero never enter, as in WRF's
+// running maxima, which start at 0).
+template <class R, int NM, int SH>
+__global__ void __launch_bounds__(PX) k_cfl(const __grid_constant__ Pack<R, NM> P, int rk) {
+  const Dom<R>* Dp;
+  int i, j, k;
+  const bool in = thread_index<SH>(P, RG_MASS, Dp, i, j, k);
+  const Dom<R>& D = *Dp;
+  double vert = 0, horiz = 0;
+  if (in && k >= 1) {
+    const R dt = R(D.dt);
+    const R x = D.ww.ld(i, j, k) / (R(D.c1f[k]) * D.mut.ld(i, j, 0) + R(D.c2f[k])) * R(D.rdnw[k]) * dt;
+    vert = double(x < R(0) ? -x : x);
+    R a = D.u2.ld(i, j, k) * R(D.rdx) * D.msfux(i, j) * dt, b = D.v2.ld(i, j, k) * R(D.rdy) * D.msfvy(i, j) * dt;
+    a = a < R(0) ? -a : a;
+    b = b < R(0) ? -b : b;
+    horiz = double(b > a ? b : a);
+  }
+  if (!(vert > 0)) vert = 0;
+  if (!(horiz > 0)) horiz = 0;
+  for (int o = 16; o > 0; o >>= 1) {
+    const double v2 = __shfl_xor_sync(0xffffffffu, vert, o), h2 = __shfl_xor_sync(0xffffffffu, horiz, o);
+    vert = v2 > vert ? v2 : vert;
+    horiz = h2 > horiz ? h2 : horiz;
+  }
+  if ((threadIdx.x & 31) == 0) {  // every block lies in one member (pack block ranges)
+    if (vert > 0) atomicMax(D.cfl + 2 * (rk - 1), (unsigned long long)__double_as_longlong(vert));
+    if (horiz > 0) atomicMax(D.cfl + 2 * (rk - 1) + 1, (unsigned long long)__double_as_longlong(horiz));
+  }
+}
+
 template <class R, int NM>
 __global__ void k_advance_time(const __grid_constant__ Pack<R, NM> P) {
   const int m = blockIdx.x;

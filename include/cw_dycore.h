@@ -184,6 +184,12 @@ int cw_check_finite(cw_handle* h, int member, int* field, int* n, int* i, int* j
  * captured again. The tuning steps are ordinary steps: every shape computes the same values. Calling it
  * again re-tunes. cw_autotune_choice gives a kernel's chosen shape (-1 before the tuning has finished). */
 int cw_set_autotune(cw_handle* h, int on);
+/* LargeStep::cfl_max (src/dyn/large_step.cpp:865-877), the maxima behind RK3::on_cfl (rk3.hpp) that the reference's
+ * adaptive time step (src/cases/adapt_timestep.cpp) and w_damp read: with on = 1 every step records, after each RK
+ * stage's tendencies, the largest vertical and horizontal Courant numbers of levels 1 .. nz-1 (a small reduction
+ * launch per stage; the step is captured again). cw_cfl_max gives a member's values of the last step, stages 1..3. */
+int cw_set_cfl_diagnostics(cw_handle* h, int on);
+int cw_cfl_max(cw_handle* h, int member, double vert[3], double horiz[3]);
 int cw_autotune_choice(cw_handle* h, const char* kernel, int* shape);
 int cw_batch_add(cw_handle* h, const cw_grid* g, const cw_options* o, int* member);
 int cw_batch_remove(cw_handle* h, int member);

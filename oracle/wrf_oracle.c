@@ -83,6 +83,7 @@ struct or_dom {
   slabset lbc[5];
   slabset* lbcq; /* per scalar */
   double dtbc, fcx[5], gcx[5];
+  double cfl[6]; /* LargeStep::cfl_max of each RK stage of the last step: (vertical, horizontal) */
   char err[256];
 };
 
@@ -2318,6 +2319,28 @@ static void physics_step(or_dom* d) {
   for (size_t n = 0; n < sizeof all / sizeof all[0]; ++n) fld_free(all[n]);
 }
 
+/* LargeStep::cfl_max (src/dyn/large_step.cpp:672-687, :865-877): Reducer maxima from -1e308 over levels 1..nz-1 of
+ * the mass points, then 0 unless positive */
+static void cfl_max(or_dom* d, int rk) {
+  const cw_grid* g = &d->g;
+  double v = -1e308, h = -1e308;
+  for (int k = 1; k < g->nz; ++k)
+    for (int j = 0; j < g->ny; ++j)
+      for (int i = 0; i < g->nx; ++i) {
+        const double x = AT(F_(CW_WW), i, j, k) / (d->c1f[k] * AT(F_(CW_MUT), i, j, 0) + d->c2f[k]) * d->rdnw[k] * g->dt;
+        const double xv = x < 0 ? -x : x;
+        v = xv > v ? xv : v;
+        double a = AT(F_(CW_U_2), i, j, k) * d->rdx * AT(F_(CW_MSFUX), i, j, 0) * g->dt;
+        double b = AT(F_(CW_V_2), i, j, k) * d->rdy * AT(F_(CW_MSFVY), i, j, 0) * g->dt;
+        a = a < 0 ? -a : a;
+        b = b < 0 ? -b : b;
+        const double xh = b > a ? b : a;
+        h = xh > h ? xh : h;
+      }
+  d->cfl[2 * (rk - 1)] = v > 0.0 ? v : 0.0;
+  d->cfl[2 * (rk - 1) + 1] = h > 0.0 ? h : 0.0;
+}
+
 static void rk3_step(or_dom* d) {
   const cw_grid* g = &d->g;
   if (d->o.lbc) d->dtbc += g->dt;
@@ -2337,6 +2360,7 @@ static void rk3_step(or_dom* d) {
     large_prep(d);
     if (rk == 1 && d->o.diff_opt == 1) diffusion_prepare(d);
     tendencies(d, rk);
+    cfl_max(d, rk);
     small_run_stage(d, dts_rk, ns, rk);
     scalars_run_stage(d, rk, dt_rk);
     calc_p_rho_phi_range(d, 0, g->nx, 0, g->ny);
@@ -2639,5 +2663,10 @@ int or_diagnostics(or_dom* d, double out[9]) {
   out[5] = area * dm;
   out[6] = area * sm;
   out[7] = area * se;
+  return 0;
+}
+
+int or_cfl_max(or_dom* d, double out[6]) {
+  memcpy(out, d->cfl, sizeof d->cfl);
   return 0;
 }

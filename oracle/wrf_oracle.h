@@ -40,6 +40,8 @@ int or_n_sound(or_dom* d);
 int or_step(or_dom* d, int nsteps);
 /* dyn::Diagnostics::compute: max|u| max|v| max|w| min th' max th' dry_mass theta_mass total_energy max|q| */
 int or_diagnostics(or_dom* d, double out[9]);
+/* LargeStep::cfl_max after each RK stage's tendencies in the last step: (vertical, horizontal) for stages 1..3 */
+int or_cfl_max(or_dom* d, double out[6]);
 const char* or_last_error(or_dom* d);
 
 #ifdef __cplusplus

@@ -44,6 +44,7 @@ def load():
             ("or_n_sound", i, [vp]),
             ("or_step", i, [vp, i]),
             ("or_diagnostics", i, [vp, dp]),
+            ("or_cfl_max", i, [vp, dp]),
         ]:
             f = getattr(lib, name)
             f.restype = res
@@ -109,6 +110,12 @@ class Oracle:
 
     def n_sound(self):
         return self.lib.or_n_sound(self.h)
+
+    def cfl_max(self):
+        """(vertical, horizontal) CFL maxima of each RK stage of the last step."""
+        out = (C.c_double * 6)()
+        self.lib.or_cfl_max(self.h, out)
+        return [(out[2 * r], out[2 * r + 1]) for r in range(3)]
 
     def diagnostics(self):
         """dyn::Diagnostics::compute of the current state: a dict of the DiagRow values."""

@@ -124,6 +124,22 @@ def test_2d_rayleigh_damping_bit_exact():
     assert not bad, "\n".join(bad)
 
 
+def test_cfl_maxima_equal_oracle():
+    """LargeStep::cfl_max of every RK stage (the adaptive time step's input): the device maxima equal the oracle's,
+    and recording them changes no field."""
+    case = lam_case(seed=13)
+    dom = Domain(case.g, case.o).upload_case(case).set_cfl_diagnostics()
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_OWN)
+    for _ in range(2):
+        dom.step(2)
+        orc.step(2)
+        got, want = dom.cfl_max(), orc.cfl_max()
+        assert got == want, (got, want)
+        assert all(v > 0 and h > 0 for v, h in got)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
 def test_benchmark_workload_bit_exact():
     """The benchmark's 119 x 89 x 44 workload (bench.py), 2 steps."""
     import bench
