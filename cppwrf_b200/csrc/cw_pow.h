@@ -4,12 +4,12 @@
  *   x = 2^e * m, m in [sqrt(1/2), sqrt(2)),   log m = 2 atanh(s), s = (m - 1) / (m + 1)
  *   y log x in double-double,                  exp(t) = 2^k * (1 + expm1(r / 256))^256 by the
  *                                              doubling identity expm1(2a) = expm1(a) * (2 + expm1(a))
- * with Dekker/Knuth error-free transformations (two_sum, Veltkamp split, two_prod) and
- * truncated Taylor series. Only IEEE-754 double add, subtract, multiply, divide, floor and
- * power-of-two scaling are used, each spelled as an explicit rounding operation, so the same
- * source gives bit-identical results on the host (C or C++, compiled with -ffp-contract=off)
- * and on the device (the operations are __dadd_rn / __dmul_rn / __ddiv_rn, which nvcc never
- * contracts into FMA, whatever --fmad says).
+ * with error-free transformations (Knuth's two_sum; the exact product error from one fused
+ * multiply-add) and truncated Taylor series. Only IEEE-754 double add, subtract, multiply,
+ * divide, fused multiply-add, floor and power-of-two scaling are used, each spelled as an
+ * explicit rounding operation, so the same source gives bit-identical results on the host (C or
+ * C++ fma(), compiled with -ffp-contract=off) and on the device (__dadd_rn / __dmul_rn /
+ * __ddiv_rn / __fma_rn, which nvcc never contracts or reassociates, whatever --fmad says).
  *
  * Why the dycore needs its own: calc_p_rho_phi evaluates p = p1000 * pow(R theta / (p1000 a), cp/cv)
  * (reference src/dyn/small_step.cpp:474-475). The reference's CPU FP64 build takes that pow from
@@ -38,6 +38,7 @@
 #define CW_MUL(a, b) __dmul_rn((a), (b))
 #define CW_DIV(a, b) __ddiv_rn((a), (b))
 #define CW_FLOOR(a) floor(a)
+#define CW_FMA(a, b, c) __fma_rn((a), (b), (c))
 #define CW_BITS(d) ((unsigned long long)__double_as_longlong(d))
 #define CW_FROMBITS(u) __longlong_as_double((long long)(u))
 #else
@@ -48,6 +49,7 @@
 #define CW_MUL(a, b) ((a) * (b))
 #define CW_DIV(a, b) ((a) / (b))
 #define CW_FLOOR(a) floor(a)
+#define CW_FMA(a, b, c) fma((a), (b), (c))
 CW_HD unsigned long long cw_bits_host(double d) {
   unsigned long long u;
   memcpy(&u, &d, sizeof u);
@@ -76,21 +78,12 @@ CW_HD void cw_fast_two_sum(double a, double b, double* s, double* e) {
   *s = t;
   *e = CW_SUB(b, CW_SUB(t, a));
 }
-/* Veltkamp split: a = hi + lo, each with at most 26 significant bits */
-CW_HD void cw_split(double a, double* hi, double* lo) {
-  const double t = CW_MUL(134217729.0, a); /* 2^27 + 1 */
-  const double h = CW_SUB(t, CW_SUB(t, a));
-  *hi = h;
-  *lo = CW_SUB(a, h);
-}
-/* p + e = a * b exactly (Dekker) */
+/* p + e = a * b exactly: the rounding error of a double product is itself a double, and one fused multiply-add
+ * (a single rounding of a*b - p, exact here) yields it; Dekker's split product gives the same e without an fma */
 CW_HD void cw_two_prod(double a, double b, double* p, double* e) {
-  double ah, al, bh, bl;
   const double q = CW_MUL(a, b);
-  cw_split(a, &ah, &al);
-  cw_split(b, &bh, &bl);
   *p = q;
-  *e = CW_ADD(CW_ADD(CW_ADD(CW_SUB(CW_MUL(ah, bh), q), CW_MUL(ah, bl)), CW_MUL(al, bh)), CW_MUL(al, bl));
+  *e = CW_FMA(a, b, -q);
 }
 
 /* ---- double-double arithmetic (hi, lo), |lo| <= ulp(hi)/2 ---- */
