@@ -18,7 +18,8 @@
  * the oracle's interposed mode both call cw_pow instead. The accuracy is checked against
  * glibc pow and against a 60-digit decimal evaluation in tests/test_pow.py.
  *
- * cw_exp(x) is the same exponential on a double argument; cw_sin(x) a double-double Taylor series for |x| <= 2.
+ * cw_exp(x) is the same exponential on a double argument, cw_log(x) the same logarithm rounded to double;
+ * cw_sin(x) a double-double Taylor series for |x| <= 2.
  *
  * Domain: any double x, y; special values follow C99 Annex F for the cases the dycore can meet
  * (x > 0 finite; NaN, 0, infinities and negative x are handled for robustness).
@@ -241,6 +242,21 @@ CW_HD double cw_pow(double x, double y) {
 CW_HD double cw_exp(double x) {
   if (x != x) return CW_ADD(x, x);
   return cw_exp_dd(x, 0.0);
+}
+
+/* log(x): the double-double logarithm of cw_pow rounded to double (calc_p_rho_phi's hypsometric_opt 2,
+ * al = dphi / (p_mid log(p_bottom / p_top)); the reference's CPU build takes glibc's log there, libmvec's on the
+ * lanes of its vectorised loop) */
+CW_HD double cw_log(double x) {
+  if (x != x) return CW_ADD(x, x);
+  if (x < 0.0) return CW_DIV(0.0, 0.0);
+  const double inf = CW_MUL(0x1p1023, 2.0);
+  if (x == 0.0) return -inf;
+  if (x == inf) return inf;
+  if (x == 1.0) return 0.0;
+  double h, l;
+  cw_log_dd(x, &h, &l);
+  return CW_ADD(h, l);
 }
 
 /* sin(x) for |x| <= 2 (NaN outside): the Taylor series sin x = x sum_n (-1)^n x^(2n) / (2n+1)!, its terms n >= 4

@@ -154,7 +154,7 @@ void allocate(cw_handle* h) {
 
 // vertical array slots in Member::vert
 enum { VA_ZNU, VA_ZNW, VA_DNW, VA_DN, VA_RDNW, VA_RDN, VA_FNM, VA_FNP, VA_C1H, VA_C2H, VA_C1F, VA_C2F, VA_UB, VA_VB,
-       VA_FCX, VA_GCX, VA_TB, VA_ZB };
+       VA_FCX, VA_GCX, VA_TB, VA_ZB, VA_C3H, VA_C4H, VA_C3F, VA_C4F };
 
 template <class R>
 Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
@@ -186,6 +186,8 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.fnm = va(VA_FNM); D.fnp = va(VA_FNP); D.c1h = va(VA_C1H); D.c2h = va(VA_C2H); D.c1f = va(VA_C1F); D.c2f = va(VA_C2F);
   D.u_base = va(VA_UB); D.v_base = va(VA_VB); D.fcx = va(VA_FCX); D.gcx = va(VA_GCX);
   D.t_base = va(VA_TB); D.z_base = va(VA_ZB);
+  D.c3h = va(VA_C3H); D.c4h = va(VA_C4H); D.c3f = va(VA_C3F); D.c4f = va(VA_C4F);
+  D.hypsometric_opt = o.hypsometric_opt; D.p_top = g.p_top;
   auto f3 = [&](int id) { return view3<R>(M.base[id], M.L[id]); };
   auto fb = [&](int id) { return viewb<R>(M.base[id], M.L[id]); };
   auto w3 = [&](int w) { return view3<R>(M.wbase[w], M.LW[w]); };
@@ -873,6 +875,7 @@ int cw_member_set_vertical(cw_handle* h, int mi, const cw_vertical* v) {
     put(VA_RDNW, v->rdnw, nz); put(VA_RDN, v->rdn, nz + 1); put(VA_FNM, v->fnm, nz + 1); put(VA_FNP, v->fnp, nz + 1);
     put(VA_C1H, v->c1h, nz); put(VA_C2H, v->c2h, nz); put(VA_C1F, v->c1f, nz + 1); put(VA_C2F, v->c2f, nz + 1);
     put(VA_UB, v->u_base, nz); put(VA_VB, v->v_base, nz); put(VA_TB, v->t_base, nz); put(VA_ZB, v->z_base, nz);
+    put(VA_C3H, v->c3h, nz); put(VA_C4H, v->c4h, nz); put(VA_C3F, v->c3f, nz + 1); put(VA_C4F, v->c4f, nz + 1);
     if (M.o.lbc) {  // LateralBC::set_dt (src/dyn/lateral_bc.cpp:198-211): width 5, spec_zone 1, relax_zone 4
       const int spec_zone = 1, relax_zone = 4;
       for (int loop = spec_zone + 1; loop <= spec_zone + relax_zone; ++loop) {

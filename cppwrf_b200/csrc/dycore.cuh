@@ -64,6 +64,9 @@ struct Dom {
   const double *znu, *znw, *dnw, *dn, *rdnw, *rdn, *fnm, *fnp, *c1h, *c2h, *c1f, *c2f, *u_base, *v_base;
   const double *fcx, *gcx;  // relaxation weights per row (LateralBC::set_dt)
   const double *t_base, *z_base;  // BaseState 1-D profiles (damp_opt 2's base state)
+  const double *c3h, *c4h, *c3f, *c4f;  // hybrid coefficients of the dry pressure (hypsometric_opt 2)
+  int hypsometric_opt;  // calc_p_rho_phi: 1 linear in the column mass, 2 log-linear in pressure
+  double p_top;
   // State
   V3<T> rainnc, rainncv;  // accumulated / last-step grid-scale rain [mm] (2-D)
   V3<T> u1, u2, v1, v2, w1, w2, t1, t2, ph1, ph2, mu1, mu2, p, al, alt, php, ww, mut, muu, muv, muts, muus, muvs,

@@ -126,17 +126,35 @@ __global__ void __launch_bounds__(PX) k_uv(const __grid_constant__ Pack<R, NM> P
   if (sv) D.v2(i, j, k) = vn;
 }
 
-// calc_p_rho_phi, hypsometric_opt 1 (KPRhoPhi :456-477) at (i, j, k); pow in double: cw_pow in the FP64 form
-// (bit-identical with the oracle), CUDA's pow in the mixed form
+// calc_p_rho_phi (KPRhoPhi :456-477) at (i, j, k); pow and log in double: cw_pow / cw_log in the FP64 form
+// (bit-identical with the oracle), CUDA's in the mixed form
 template <class R>
 __device__ __forceinline__ double eos_pow(double base) {
   if constexpr (sizeof(R) == 4) return ::pow(base, k::cpovcv);
   else return cw_pow(base, k::cpovcv);
 }
 template <class R>
+__device__ __forceinline__ double hypso_log(double x) {
+  if constexpr (sizeof(R) == 4) return ::log(x);
+  else return cw_log(x);
+}
+template <class R>
 __device__ __forceinline__ void p_rho_phi_point(const Dom<R>& D, int i, int j, int k) {
-  const R a = R(-1) / (R(D.c1h[k]) * D.muts(i, j, 0) + R(D.c2h[k])) *
-              (D.alb(i, j, k) * (R(D.c1h[k]) * D.mu2(i, j, 0)) + R(D.rdnw[k]) * (D.ph2(i, j, k + 1) - D.ph2(i, j, k)));
+  R a;
+  if (D.hypsometric_opt == 2) {
+    // log-linear in pressure: the total inverse density of the layer is its geopotential thickness over
+    // p_mid log(p_bottom / p_top), the dry pressures from the hybrid coefficients; in double in both forms (the
+    // perturbation is a small difference of totals)
+    const double m = double(D.muts(i, j, 0)), ptop = D.p_top;
+    const double pfu = D.c3f[k + 1] * m + D.c4f[k + 1] + ptop, pfd = D.c3f[k] * m + D.c4f[k] + ptop;
+    const double phm = D.c3h[k] * m + D.c4h[k] + ptop;
+    a = R((double(D.ph2(i, j, k + 1)) - double(D.ph2(i, j, k)) + double(D.phb(i, j, k + 1)) - double(D.phb(i, j, k))) /
+              phm / hypso_log<R>(pfd / pfu) -
+          double(D.alb(i, j, k)));
+  } else {
+    a = R(-1) / (R(D.c1h[k]) * D.muts(i, j, 0) + R(D.c2h[k])) *
+        (D.alb(i, j, k) * (R(D.c1h[k]) * D.mu2(i, j, 0)) + R(D.rdnw[k]) * (D.ph2(i, j, k + 1) - D.ph2(i, j, k)));
+  }
   D.al(i, j, k) = a;
   const double base = double(R(k::r_d) * (R(k::t0) + D.t2(i, j, k)) / (R(k::p1000mb) * (a + D.alb(i, j, k))));
   D.p(i, j, k) = R(k::p1000mb * eos_pow<R>(base) - double(D.pb(i, j, k)));

@@ -3,7 +3,8 @@
  * pow entry points the reference's CPU build calls in calc_p_rho_phi (scalar libm pow and libmvec's
  * 2-lane _ZGVbN2vv_pow, src/core/backend.hpp:118, :169-175) to cw_pow, the pow of the GPU path, and the
  * scalar and libmvec 2-lane sin of the Rayleigh dampings (damp_opt 3, src/dyn/small_step.cpp:400; damp_opt 2,
- * src/dyn/diffusion/rayleigh_damp.hpp:16-25, :136) to cw_sin. The
+ * src/dyn/diffusion/rayleigh_damp.hpp:16-25, :136) to cw_sin, and the scalar and libmvec 2-lane log of
+ * calc_p_rho_phi's hypsometric_opt 2 (src/dyn/small_step.cpp:467, src/core/backend.hpp:176-184) to cw_log. The
  * reference's every other operation is unchanged, so bit-identity with this build is a fair test of them. */
 #include <emmintrin.h>
 
@@ -24,4 +25,12 @@ __m128d _ZGVbN2v_sin(__m128d x) {
   double a[2];
   _mm_storeu_pd(a, x);
   return _mm_set_pd(cw_sin(a[1]), cw_sin(a[0]));
+}
+
+double log(double x) { return cw_log(x); }
+
+__m128d _ZGVbN2v_log(__m128d x) {
+  double a[2];
+  _mm_storeu_pd(a, x);
+  return _mm_set_pd(cw_log(a[1]), cw_log(a[0]));
 }

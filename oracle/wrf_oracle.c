@@ -11,8 +11,8 @@
  * coefficients, moist species (calc_cq, positive-definite scalar advection at rk 3), passive
  * tracers, constant-K diffusion (diff_opt 1, km_opt 1), specified lateral boundaries (width 5),
  * top_lid, w_damping, h/v_adv_order 5/6, 3/4, damp_opt 2 and 3 (sin by the pow mode: glibc's or cw_sin), the
- * sixth-order filter, Kessler microphysics. Not restated (rejected by or_create): open boundaries, map factors
- * other than 1, Coriolis, damp_opt 1, hypsometric_opt 2.
+ * sixth-order filter, hypsometric_opt 1 and 2 (log by the pow mode), Kessler microphysics. Not restated (rejected
+ * by or_create): open boundaries, map factors other than 1, Coriolis, damp_opt 1.
  */
 #include "wrf_oracle.h"
 
@@ -28,6 +28,7 @@
 /* glibc's libmvec 2-lane pow, the reference CPU build's vm::pow (src/core/backend.hpp:118, :171) */
 extern __m128d _ZGVbN2vv_pow(__m128d, __m128d);
 extern __m128d _ZGVbN2v_exp(__m128d);
+extern __m128d _ZGVbN2v_log(__m128d);
 
 /* ------------------------------------------------------------------ constants
  * src/core/constants.hpp:4-18 (WRF module_model_constants) */
@@ -1844,7 +1845,8 @@ static void small_run_stage(or_dom* d, double dts, int n_small, int rk_step) {
   fill_halo(d, mu);
 }
 
-/* calc_p_rho_phi, hypsometric_opt 1 (KPRhoPhi :456-477; SmallStep::calc_p_rho_phi(_interior) :609-633) */
+/* calc_p_rho_phi, hypsometric_opt 1 (linear) or 2 (log-linear in pressure) (KPRhoPhi :456-477;
+ * SmallStep::calc_p_rho_phi(_interior) :609-633) */
 static double eos_pow(or_dom* d, double base, int lane_i, int lane_n) {
   if (d->pow_mode == OR_POW_GLIBC) {
     const int lane = lane_n > 1 && !((lane_n & 1) && lane_i == lane_n - 1); /* vm::lane, backend.hpp:144 */
@@ -1853,15 +1855,33 @@ static double eos_pow(or_dom* d, double base, int lane_i, int lane_n) {
   }
   return cw_pow(base, CPOVCV);
 }
+static double hypso_log(or_dom* d, double x, int lane_i, int lane_n) {
+  if (d->pow_mode == OR_POW_GLIBC) {
+    const int lane = lane_n > 1 && !((lane_n & 1) && lane_i == lane_n - 1); /* vm::lane, backend.hpp:144 */
+    if (lane) return _mm_cvtsd_f64(_ZGVbN2v_log(_mm_set1_pd(x)));
+    return log(x);
+  }
+  return cw_log(x);
+}
 static void calc_p_rho_phi_range(or_dom* d, int i0, int i1, int j0, int j1) {
   fld *al = F_(CW_AL), *p = F_(CW_P), *ph = F_(CW_PH_2), *t = F_(CW_T_2), *mu = F_(CW_MU_2), *muts = F_(CW_MUTS),
-      *alb = F_(CW_ALB), *pb = F_(CW_PB);
-  const int n = i1 - i0;
+      *alb = F_(CW_ALB), *pb = F_(CW_PB), *phb = F_(CW_PHB);
+  const int n = i1 - i0, hypso = d->o.hypsometric_opt;
+  const double ptop = d->p_top;
   for (int k = 0; k < d->g.nz; ++k)
     for (int j = j0; j < j1; ++j)
       for (int i = i0; i < i1; ++i) {
-        const double a = -1.0 / (d->c1h[k] * AT(muts, i, j, 0) + d->c2h[k]) *
-                         (AT(alb, i, j, k) * (d->c1h[k] * AT(mu, i, j, 0)) + d->rdnw[k] * (AT(ph, i, j, k + 1) - AT(ph, i, j, k)));
+        double a;
+        if (hypso == 2) {
+          const double m = AT(muts, i, j, 0);
+          const double pfu = d->c3f[k + 1] * m + d->c4f[k + 1] + ptop, pfd = d->c3f[k] * m + d->c4f[k] + ptop;
+          const double phm = d->c3h[k] * m + d->c4h[k] + ptop;
+          a = (AT(ph, i, j, k + 1) - AT(ph, i, j, k) + AT(phb, i, j, k + 1) - AT(phb, i, j, k)) / phm /
+                  hypso_log(d, pfd / pfu, i - i0, n) - AT(alb, i, j, k);
+        } else {
+          a = -1.0 / (d->c1h[k] * AT(muts, i, j, 0) + d->c2h[k]) *
+              (AT(alb, i, j, k) * (d->c1h[k] * AT(mu, i, j, 0)) + d->rdnw[k] * (AT(ph, i, j, k + 1) - AT(ph, i, j, k)));
+        }
         AT(al, i, j, k) = a;
         const double base = R_D * (T0 + AT(t, i, j, k)) / (P1000MB * (a + AT(alb, i, j, k)));
         AT(p, i, j, k) = P1000MB * eos_pow(d, base, i - i0, n) - AT(pb, i, j, k);
@@ -2386,7 +2406,7 @@ or_dom* or_create(const cw_grid* g, const cw_options* o) {
   or_dom* d = (or_dom*)calloc(1, sizeof(or_dom));
   d->g = *g;
   d->o = *o;
-  if (g->bc_x == CW_BC_OPEN || g->bc_y == CW_BC_OPEN || (o->damp_opt != 0 && o->damp_opt != 2 && o->damp_opt != 3) || o->hypsometric_opt != 1 ||
+  if (g->bc_x == CW_BC_OPEN || g->bc_y == CW_BC_OPEN || (o->damp_opt != 0 && o->damp_opt != 2 && o->damp_opt != 3) || (o->hypsometric_opt != 1 && o->hypsometric_opt != 2) ||
       o->diff_6th_opt < 0 || o->diff_6th_opt > 2 ||
       (o->mp_physics != 0 && (o->mp_physics != 1 || o->n_moist < 3 || g->nz > KS_LEVELS)) ||
       (o->diff_opt != 0 && (o->diff_opt != 1 || o->km_opt != 1))) {

@@ -131,3 +131,31 @@ def test_oracle_equals_reference_rayleigh_damping_2d():
     ref = _refdump.run(case, 3, own_pow=False)
     bad = compare(orc, ref, case)
     assert not bad, "\n".join(bad)
+
+
+@pytest.mark.parametrize("own", [True, False], ids=["cw_log", "glibc"])
+def test_oracle_equals_reference_hypsometric_log_pressure(own):
+    """hypsometric_opt 2: calc_p_rho_phi's inverse density from the geopotential thickness over the log of the
+    layer's pressure ratio (libmvec's log on the lanes of the reference's i loop in the glibc build, on the whole
+    domain and on the interior after the boundary update)."""
+    case = lam_case(seed=15)
+    case.o.hypsometric_opt = 2
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_OWN if own else _oracle.POW_GLIBC)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=own)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)
+    linear = lam_case(seed=15)
+    lin = _oracle.Oracle(linear, pow_mode=_oracle.POW_OWN if own else _oracle.POW_GLIBC)
+    lin.step(3)
+    assert not np.array_equal(orc.array("AL"), lin.array("AL"))
+
+
+def test_oracle_equals_reference_hypsometric_log_pressure_2d():
+    cfg = dict(cases.SMALL["igw_small"])
+    case = cases.ideal_case(cfg, hypsometric_opt=2)
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_GLIBC)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=False)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)

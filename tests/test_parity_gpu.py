@@ -124,6 +124,23 @@ def test_2d_rayleigh_damping_bit_exact():
     assert not bad, "\n".join(bad)
 
 
+def test_lam_hypsometric_log_pressure_bit_exact():
+    """hypsometric_opt 2: calc_p_rho_phi's inverse density from the geopotential thickness over the log of the
+    layer's pressure ratio (log = cw_log on both sides), on the whole domain and on the interior."""
+    case = lam_case(seed=15)
+    case.o.hypsometric_opt = 2
+    dom, orc = run_pair(case, 4)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
+def test_2d_hypsometric_log_pressure_bit_exact():
+    case = cases.ideal_case(dict(cases.SMALL["igw_small"]), hypsometric_opt=2)
+    dom, orc = run_pair(case, 3)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
 def test_cfl_maxima_equal_oracle():
     """LargeStep::cfl_max of every RK stage (the adaptive time step's input): the device maxima equal the oracle's,
     and recording them changes no field."""

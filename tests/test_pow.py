@@ -1,5 +1,5 @@
 # SPDX-License-Identifier: GPL-3.0-or-later
-"""Accuracy of the dycore's own pow, exp and sin (cw_pow.h): against glibc's and against 60-digit decimal evaluations."""
+"""Accuracy of the dycore's own pow, exp, log and sin (cw_pow.h): against glibc's and against 60-digit decimal evaluations."""
 import ctypes as C
 import math
 import os
@@ -16,6 +16,7 @@ SRC = r"""
 double cwp(double x, double y) { return cw_pow(x, y); }
 double cwe(double x) { return cw_exp(x); }
 double cws(double x) { return cw_sin(x); }
+double cwl(double x) { return cw_log(x); }
 """
 
 
@@ -28,7 +29,7 @@ def _lib(tmp_path):
     lib = C.CDLL(str(so))
     lib.cwp.restype = C.c_double
     lib.cwp.argtypes = [C.c_double, C.c_double]
-    for f in (lib.cwe, lib.cws):
+    for f in (lib.cwe, lib.cws, lib.cwl):
         f.restype = C.c_double
         f.argtypes = [C.c_double]
     return lib
@@ -115,3 +116,26 @@ def test_exp_within_half_ulp_plus(tmp_path):
         worst = max(worst, abs(Decimal(lib.cwe(float(x))) - exact) / Decimal(math.ulp(float(exact))))
     assert worst < Decimal("0.5001"), worst
     assert lib.cwe(0.0) == 1.0 and math.isinf(lib.cwe(800.0)) and lib.cwe(-800.0) == 0.0 and math.isnan(lib.cwe(math.nan))
+
+
+def test_log_within_half_ulp_plus(tmp_path):
+    """cw_log (hypsometric_opt 2: log of the ratio of the pressures at a layer's faces, just above 1, and any
+    positive argument) within 0.5001 ulp of the exact value."""
+    lib = _lib(tmp_path)
+    getcontext().prec = 60
+    rng = np.random.default_rng(6)
+    xs = list(rng.uniform(1.0, 1.5, 300)) + list(np.exp(rng.uniform(-700.0, 700.0, 200))) + [1e-310, 0.5, 2.0, 1 + 2**-52]
+    worst = Decimal(0)
+    for x in xs:
+        exact = Decimal(float(x)).ln()
+        worst = max(worst, abs(Decimal(lib.cwl(float(x))) - exact) / Decimal(math.ulp(float(exact))))
+    assert worst < Decimal("0.5001"), worst
+    assert lib.cwl(1.0) == 0.0 and math.isinf(lib.cwl(0.0)) and lib.cwl(0.0) < 0
+    assert math.isnan(lib.cwl(-1.0)) and math.isnan(lib.cwl(math.nan)) and lib.cwl(math.inf) == math.inf
+
+
+def test_log_agrees_with_glibc_to_one_ulp(tmp_path):
+    lib = _lib(tmp_path)
+    for x in np.random.default_rng(7).uniform(1.0, 1.5, 5000):
+        a, b = lib.cwl(float(x)), math.log(float(x))
+        assert abs(a - b) <= math.ulp(b), (x, a, b)
