@@ -116,7 +116,6 @@ constexpr int kLbcWidth = 5;
 inline const char* unsupported(const cw_grid& g, const cw_options& o) {
   if (g.nx < 4 || g.ny < 1 || g.nz < 3) return "grid: need nx >= 4, ny >= 1, nz >= 3";
   if (!two_d(g) && g.ny < 4) return "grid: 3-D runs need ny >= 4";
-  if (g.bc_x == CW_BC_OPEN || g.bc_y == CW_BC_OPEN) return "open lateral boundaries are not supported";
   if ((g.bc_x == CW_BC_SPECIFIED) != (g.bc_y == CW_BC_SPECIFIED && !two_d(g)) && specified(g))
     return "specified boundaries: both directions of a 3-D grid";
   if (specified(g) && !o.lbc) return "specified boundaries need lbc = 1";

@@ -165,6 +165,8 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.nx = g.nx; D.ny = g.ny; D.nz = g.nz; D.nyv = nys(g, 'V'); D.two_d = two_d(g); D.do_y = !two_d(g);
   D.bc_x = g.bc_x; D.bc_y = g.bc_y;
   D.spec_x = flat_x(g); D.spec_y = flat_y(g) && !two_d(g);
+  D.open_x = g.bc_x == CW_BC_OPEN; D.open_y = g.bc_y == CW_BC_OPEN && !two_d(g);
+  D.sx = D.spec_x && !D.open_x; D.sy = D.spec_y && !D.open_y;
   D.lbc = o.lbc; D.flat = o.flat; D.n_moist = o.n_moist; D.n_scalars = o.n_scalars;
   D.diff_on = o.diff_opt == 1; D.top_lid = o.top_lid; D.w_damping = o.w_damping; D.n_sound = M.n_sound;
   D.moist_adv_opt = o.moist_adv_opt; D.scalar_adv_opt = o.scalar_adv_opt;

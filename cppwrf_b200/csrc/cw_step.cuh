@@ -147,11 +147,12 @@ struct Launcher {
 
 // the three block-shape instantiations of a tunable point kernel
 #define KV(kern) std::array{kern<R, NM, 0>, kern<R, NM, 1>, kern<R, NM, 2>}
+#define KV_OP(kern, op) std::array{kern<R, NM, 0, op>, kern<R, NM, 1, op>, kern<R, NM, 2, op>}
 
 template <class R, int NM>
 void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
   const Member& M0 = h->m[0];
-  bool lbc = false, terrain = false, scalars = false, any_pd = false, mp = false;
+  bool lbc = false, terrain = false, scalars = false, any_pd = false, mp = false, open = false;
   // every member specified on all four sides: the acoustic substeps read no halo cell of the fields the
   // per-substep fills (H_SS0, H_UV, H_AC) would refresh (the faces next to the boundary are the spec
   // zone's, updated from the boundary data), and the fills after the substeps (H_POST, H_FIN) refresh them
@@ -163,6 +164,7 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
     spec_all &= M.o.lbc != 0 && flat_x(M.g) && flat_y(M.g) && !two_d(M.g);
     nq = std::max(nq, M.o.n_scalars);
     lbc |= M.o.lbc != 0;
+    open |= M.g.bc_x == CW_BC_OPEN || M.g.bc_y == CW_BC_OPEN;
     mp |= M.o.mp_physics != 0;
     terrain |= !M.o.flat;
     scalars |= M.o.n_scalars > 0;
@@ -182,7 +184,8 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
     L.run_cb("k_ls_prep", RG_COLS_STAG, 1, k_ls_prep<R, NM>, d);
     L.halo(cw_handle::H_PREP1);
     if (rk == 1) L.run_t("k_tendf_rk1", RG_STAG, 1, KV(k_tendf_rk1), d);
-    L.run_t("k_tend", RG_STAG, 1, KV(k_tend), d, rk);
+    if (open) L.run_t("k_tend", RG_STAG, 1, KV_OP(k_tend, true), d, rk);
+    else L.run_t("k_tend", RG_STAG, 1, KV_OP(k_tend, false), d, rk);
     if (h->cfl_on) L.run_t("k_cfl", RG_MASS, 1, KV(k_cfl), d, rk);
     if (rk == 1) L.copy_list(h->zeros_d, h->zeros_start_d, h->zeros.size(), h->zeros_total);
     L.run_cb("k_ss_prep", RG_COLS_STAG, 3, k_ss_prep<R, NM>, d, rk);

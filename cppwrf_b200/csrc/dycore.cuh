@@ -48,7 +48,9 @@ template <class T>
 struct Dom {
   // grid and options
   int nx, ny, nz, nyv, two_d, do_y;
-  int bc_x, bc_y, spec_x, spec_y;  // spec_*: specified in that direction (degraded orders, spec zone)
+  int bc_x, bc_y, spec_x, spec_y;  // spec_*: specified or open in that direction (degraded orders)
+  int sx, sy;                      // specified in that direction (spec zone, upstream boundary velocity)
+  int open_x, open_y;              // open (radiation) in that direction; open_y is 0 in 2-D
   int lbc, flat, n_moist, n_scalars, diff_on, top_lid, w_damping, n_sound, moist_adv_opt, scalar_adv_opt;
   int dd_on;     // a DiffusionDriver is attached (diff_opt 1 or the sixth-order filter): the tendf enter the tendencies
   int diff_6th_opt;
@@ -182,6 +184,7 @@ constexpr double cpovcv = cp / (cp - r_d);
 constexpr double p1000mb = 100000.0;
 constexpr double t0 = 300.0;
 constexpr double reradius = 1. / 6370.0e03;
+constexpr double cb = 25.;  // phase speed of the open (radiative) lateral boundaries
 }  // namespace k
 
 // ---- halo fill descriptors (HaloLine, src/core/halo.cpp:52-88) ----

@@ -206,16 +206,16 @@ __device__ __forceinline__ R cqw_(const Dom<R>& D, int i, int j, int k) { return
 // (cqu, cqv, cqw are written only by k_ls_prep, which does not read them). The tendency, flux and diffusion
 // functions below read only fields that no thread of their kernels writes: the read-only load path (.ld).
 
-// KTendU (large_step.cpp:152-264), no open boundaries, no Coriolis, unmapped
+// KTendU (large_step.cpp:152-264), no Coriolis, unmapped
 template <class R>
 __device__ R tu_fx(const Dom<R>& D, int i, int j, int k) {
   const int o = ord_mass(i, D.nx, D.spec_x);
   if (o == 2) {
     if (i <= 1) {
-      const R ub = (D.spec_x && D.u2.ld(i, j, k) < R(0)) ? D.u2.ld(i, j, k) : D.u2.ld(i - 1, j, k);
+      const R ub = (D.sx && D.u2.ld(i, j, k) < R(0)) ? D.u2.ld(i, j, k) : D.u2.ld(i - 1, j, k);
       return R(0.25) * (D.ru.ld(i, j, k) + D.ru.ld(i - 1, j, k)) * (D.u2.ld(i, j, k) + ub);
     }
-    const R ub = (D.spec_x && D.u2.ld(i - 1, j, k) > R(0)) ? D.u2.ld(i - 1, j, k) : D.u2.ld(i, j, k);
+    const R ub = (D.sx && D.u2.ld(i - 1, j, k) > R(0)) ? D.u2.ld(i - 1, j, k) : D.u2.ld(i, j, k);
     return R(0.25) * (D.ru.ld(i, j, k) + D.ru.ld(i - 1, j, k)) * (D.u2.ld(i - 1, j, k) + ub);
   }
   const R vel = R(0.5) * (D.ru.ld(i, j, k) + D.ru.ld(i - 1, j, k));
@@ -247,13 +247,54 @@ __device__ __forceinline__ R pgf_dpn(const Dom<R>& D, int i, int j, int k) {  //
   if (k == nz) return D.top_lid ? R(0.5) * (R(D.cfn) * ps(nz - 1) + R(D.cfn1) * ps(nz - 2)) : R(0);
   return R(0.5) * (R(D.fnm[k]) * ps(k) + R(D.fnp[k]) * ps(k - 1));
 }
+// advect_u open_ys / open_ye (KTendU::open_y_term, :193-208): the v-flux terms of the outermost rows
 template <class R>
+__device__ R tu_open_y(const Dom<R>& D, int i, int j, int k) {
+  const int imin = 0, imax = D.nx - 1;
+  const int ip = i < imax ? i : imax, im = i - 1 > imin ? i - 1 : imin;
+  const R mrdy = D.msfux(i, j) * R(D.rdy);
+  if (j == 0) {
+    const R vw = R(0.5) * (D.rv.ld(ip, 0, k) + D.rv.ld(im, 0, k));
+    const R vb = vw < R(0) ? vw : R(0);
+    const R dvm = D.rv.ld(ip, 1, k) - D.rv.ld(ip, 0, k), dvp = D.rv.ld(im, 1, k) - D.rv.ld(im, 0, k);
+    return mrdy * (vb * (D.u2.ld(i, 1, k) - D.u2.ld(i, 0, k)) + R(0.5) * D.u2.ld(i, 0, k) * (dvm + dvp));
+  }
+  const int je = D.ny;
+  const R vw = R(0.5) * (D.rv.ld(ip, je, k) + D.rv.ld(im, je, k));
+  const R vb = vw > R(0) ? vw : R(0);
+  const R dvm = D.rv.ld(ip, je, k) - D.rv.ld(ip, je - 1, k), dvp = D.rv.ld(im, je, k) - D.rv.ld(im, je - 1, k);
+  return mrdy * (vb * (D.u2.ld(i, je - 1, k) - D.u2.ld(i, je - 2, k)) + R(0.5) * D.u2.ld(i, je - 1, k) * (dvm + dvp));
+}
+// an open x boundary face of u (:210-227): the radiation condition with phase speed cb, the vertical advection
+// unless y is open too, and the held tendency
+template <class R>
+__device__ R tend_u_open_face(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
+  const R rdx = R(D.rdx), c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
+  R t;
+  if (i == 0) {
+    R ub = D.ru.ld(0, j, k) - R(k::cb) * (c1h * D.mut.ld(0, j, 0) + c2h);
+    ub = ub < R(0) ? ub : R(0);
+    t = R(0) - rdx * ub * (D.u2.ld(1, j, k) - D.u2.ld(0, j, k));
+  } else {
+    R ub = D.ru.ld(i, j, k) + R(k::cb) * (c1h * D.mut.ld(i - 1, j, 0) + c2h);
+    ub = ub > R(0) ? ub : R(0);
+    t = R(0) - rdx * ub * (D.u2.ld(i, j, k) - D.u2.ld(i - 1, j, k));
+  }
+  if (!D.open_y) t -= R(D.rdnw[k]) * (tu_fz(D, i, j, k + 1) - tu_fz(D, i, j, k));
+  if (use_tendf) t += D.ru_tendf.ld(i, j, k) / D.msfuy(i, j);
+  return t;
+}
+// OP: the kernel variant for packs with an open boundary (the checks compile away in the other)
+template <bool OP, class R>
 __device__ R tend_u(const Dom<R>& D, int i, int j, int k, bool use_tendf, R fx0, R fx1, R fy0, R fy1) {
   const R rdx = R(D.rdx), rdy = R(D.rdy);
   const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
   R t = -(D.msfux(i, j) * rdx) * (fx1 - fx0);
-  if (D.do_y) t -= (D.msfux(i, j) * rdy) * (fy1 - fy0);
-  t -= R(D.rdnw[k]) * (tu_fz(D, i, j, k + 1) - tu_fz(D, i, j, k));
+  if (D.do_y) {  // open_ys / ye: the outermost rows take the open terms instead of the y flux divergence
+    if (!(OP && D.open_y && (j == 0 || j == D.ny - 1))) t -= (D.msfux(i, j) * rdy) * (fy1 - fy0);
+    else t -= tu_open_y(D, i, j, k);
+  }
+  if (!(OP && D.open_y && D.spec_x && (i == 0 || i == D.nx))) t -= R(D.rdnw[k]) * (tu_fz(D, i, j, k + 1) - tu_fz(D, i, j, k));
   const R rm = D.msfux(i, j) / D.msfuy(i, j);
   R dpx = rm * R(0.5) * rdx * (c1h * D.muu.ld(i, j, 0) + c2h) *
           ((D.ph2.ld(i, j, k + 1) - D.ph2.ld(i - 1, j, k + 1) + D.ph2.ld(i, j, k) - D.ph2.ld(i - 1, j, k)) +
@@ -284,10 +325,10 @@ __device__ R tv_fy(const Dom<R>& D, int i, int j, int k) {
   const int o = ord_mass(j, D.ny, D.spec_y);
   if (o == 2) {
     if (j <= 1) {
-      const R vb = (D.spec_y && D.v2.ld(i, j, k) < R(0)) ? D.v2.ld(i, j, k) : D.v2.ld(i, j - 1, k);
+      const R vb = (D.sy && D.v2.ld(i, j, k) < R(0)) ? D.v2.ld(i, j, k) : D.v2.ld(i, j - 1, k);
       return R(0.25) * (D.rv.ld(i, j, k) + D.rv.ld(i, j - 1, k)) * (D.v2.ld(i, j, k) + vb);
     }
-    const R vb = (D.spec_y && D.v2.ld(i, j - 1, k) > R(0)) ? D.v2.ld(i, j - 1, k) : D.v2.ld(i, j, k);
+    const R vb = (D.sy && D.v2.ld(i, j - 1, k) > R(0)) ? D.v2.ld(i, j - 1, k) : D.v2.ld(i, j, k);
     return R(0.25) * (D.rv.ld(i, j, k) + D.rv.ld(i, j - 1, k)) * (vb + D.v2.ld(i, j - 1, k));
   }
   const R vel = R(0.5) * (D.rv.ld(i, j, k) + D.rv.ld(i, j - 1, k));
@@ -302,13 +343,55 @@ __device__ R tv_fz(const Dom<R>& D, int i, int j, int k) {
   if (k == 1 || k == D.nz - 1) return vel * (R(D.fnm[k]) * D.v2.ld(i, j, k) + R(D.fnp[k]) * D.v2.ld(i, j, k - 1));
   return vel * flux3(D.v2.ld(i, j, k - 2), D.v2.ld(i, j, k - 1), D.v2.ld(i, j, k), D.v2.ld(i, j, k + 1), -vel, R(D.vup));
 }
+// advect_v open_xs / open_xe (KTendV::open_x_term, :307-323): the u-flux terms of the outermost columns
 template <class R>
+__device__ R tv_open_x(const Dom<R>& D, int i, int j, int k) {
+  const int jmin = 0, jmax = D.ny - 1;
+  const int jp = j < jmax ? j : jmax, jm = j - 1 > jmin ? j - 1 : jmin;
+  if (i == 0) {
+    const R mrdx = D.msfvy(0, j) * R(D.rdx);
+    const R uw = R(0.5) * (D.ru.ld(0, jp, k) + D.ru.ld(0, jm, k));
+    const R ub = uw < R(0) ? uw : R(0);
+    const R dup = D.ru.ld(1, jp, k) - D.ru.ld(0, jp, k), dum = D.ru.ld(1, jm, k) - D.ru.ld(0, jm, k);
+    return mrdx * (ub * (D.v2.ld(1, j, k) - D.v2.ld(0, j, k)) + R(0.5) * D.v2.ld(0, j, k) * (dup + dum));
+  }
+  const int ie = D.nx;
+  const R mrdx = D.msfvy(ie - 1, j) * R(D.rdx);
+  const R uw = R(0.5) * (D.ru.ld(ie, jp, k) + D.ru.ld(ie, jm, k));
+  const R ub = uw > R(0) ? uw : R(0);
+  const R dup = D.ru.ld(ie, jp, k) - D.ru.ld(ie - 1, jp, k), dum = D.ru.ld(ie, jm, k) - D.ru.ld(ie - 1, jm, k);
+  return mrdx * (ub * (D.v2.ld(ie - 1, j, k) - D.v2.ld(ie - 2, j, k)) + R(0.5) * D.v2.ld(ie - 1, j, k) * (dup + dum));
+}
+// an open y boundary face of v (:327-340): the radiation condition only, and the held tendency
+template <class R>
+__device__ R tend_v_open_face(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
+  const R rdy = R(D.rdy), c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
+  R t;
+  if (j == 0) {
+    R vb = D.rv.ld(i, 0, k) - R(k::cb) * (c1h * D.mut.ld(i, 0, 0) + c2h);
+    vb = vb < R(0) ? vb : R(0);
+    t = R(0) - rdy * vb * (D.v2.ld(i, 1, k) - D.v2.ld(i, 0, k));
+  } else {
+    R vb = D.rv.ld(i, j, k) + R(k::cb) * (c1h * D.mut.ld(i, j - 1, 0) + c2h);
+    vb = vb > R(0) ? vb : R(0);
+    t = R(0) - rdy * vb * (D.v2.ld(i, j, k) - D.v2.ld(i, j - 1, k));
+  }
+  if (use_tendf) t += D.rv_tendf.ld(i, j, k) * D.msfvx_inv(i, j);
+  return t;
+}
+template <bool OP, class R>
 __device__ R tend_v(const Dom<R>& D, int i, int j, int k, bool use_tendf, R fx0, R fx1, R fy0, R fy1) {
   const R rdx = R(D.rdx), rdy = R(D.rdy);
   const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
   const R rm = D.msfvy(i, j) / D.msfvx(i, j);
-  R t = -(D.msfvy(i, j) * rdx) * (fx1 - fx0);
-  t -= (D.msfvy(i, j) * rdy) * (fy1 - fy0);
+  R t;
+  if (OP && D.open_x && (i == 0 || i == D.nx - 1)) {  // open x: the y flux, then the open term instead of the x flux
+    t = -(D.msfvy(i, j) * rdy) * (fy1 - fy0);
+    t -= tv_open_x(D, i, j, k);
+  } else {
+    t = -(D.msfvy(i, j) * rdx) * (fx1 - fx0);
+    t -= (D.msfvy(i, j) * rdy) * (fy1 - fy0);
+  }
   t -= rm * R(D.rdnw[k]) * (tv_fz(D, i, j, k + 1) - tv_fz(D, i, j, k));
   R dpy = rm * R(0.5) * rdy * (c1h * D.muv.ld(i, j, 0) + c2h) *
           ((D.ph2.ld(i, j, k + 1) - D.ph2.ld(i, j - 1, k + 1) + D.ph2.ld(i, j, k) - D.ph2.ld(i, j - 1, k)) +
@@ -362,12 +445,50 @@ __device__ R tw_fz(const Dom<R>& D, int i, int j, int m) {
   const R vel = R(0.5) * (D.ww.ld(i, j, m + 1) + D.ww.ld(i, j, m));
   return vel * flux3(D.w2.ld(i, j, m - 1), D.w2.ld(i, j, m), D.w2.ld(i, j, m + 1), D.w2.ld(i, j, m + 2), -vel, R(D.vup));
 }
-template <class R>
+// advect_w open_xs/xe (open_ys/ye) terms of the outermost columns (rows) (KTendW::open_x_term / open_y_term,
+// :416-453): DI = 1 for x, 0 for y; the normal mass flux fnm/fnp-interpolated to the w level, extrapolated at the lid
+template <class R, int DI>
+__device__ R tw_open(const Dom<R>& D, int i, int j, int k) {
+  const int nz = D.nz;
+  const int c = DI ? i : j, n = DI ? D.nx : D.ny;
+  const int a = c == 0 ? 0 : n - 1, b = c == 0 ? 1 : n;  // faces: outer side a, inner side b
+  const V3<R>& rf = DI ? D.ru : D.rv;
+  auto RF = [&](int f, int kk) { return DI ? rf.ld(f, j, kk) : rf.ld(i, f, kk); };
+  auto Wv = [&](int f) { return DI ? D.w2.ld(f, j, k) : D.w2.ld(i, f, k); };
+  R uw, dru;
+  if (k < nz) {
+    const R fnm = R(D.fnm[k]), fnp = R(D.fnp[k]);
+    uw = R(0.5) * (fnm * (RF(a, k) + RF(b, k)) + fnp * (RF(a, k - 1) + RF(b, k - 1)));
+    dru = fnm * (RF(b, k) - RF(a, k)) + fnp * (RF(b, k - 1) - RF(a, k - 1));
+  } else {
+    const R fm = R(2) - R(D.fnm[nz - 1]), fp = R(D.fnp[nz - 1]);
+    uw = R(0.5) * (fm * (RF(a, nz - 1) + RF(b, nz - 1)) - fp * (RF(a, nz - 2) + RF(b, nz - 2)));
+    dru = fm * (RF(b, nz - 1) - RF(a, nz - 1)) - fp * (RF(b, nz - 2) - RF(a, nz - 2));
+  }
+  const R rd = DI ? R(D.rdx) : R(D.rdy);
+  if (c == 0) {
+    const R ub = uw < R(0) ? uw : R(0);
+    return rd * (ub * (Wv(1) - Wv(0)) + Wv(0) * dru);
+  }
+  const R ub = uw > R(0) ? uw : R(0);
+  return rd * (ub * (Wv(c) - Wv(c - 1)) + Wv(c) * dru);
+}
+template <bool OP, class R>
 __device__ R tend_w(const Dom<R>& D, int i, int j, int k, bool use_tendf, R fx0, R fx1, R fy0, R fy1) {
   const int nz = D.nz;
   const R rdx = R(D.rdx), rdy = R(D.rdy);
-  R t = -(D.msftx(i, j) * rdx) * (fx1 - fx0);
-  if (D.do_y) t -= (D.msftx(i, j) * rdy) * (fy1 - fy0);
+  R t;
+  const bool ocol = OP && D.open_x && (i == 0 || i == D.nx - 1), orow = OP && D.open_y && (j == 0 || j == D.ny - 1);
+  if (ocol || orow) {  // the reference's order: y flux, x flux, open x terms, open y terms
+    t = R(0);
+    if (D.do_y && !orow) t = t - (D.msftx(i, j) * rdy) * (fy1 - fy0);
+    if (!ocol) t = t - (D.msftx(i, j) * rdx) * (fx1 - fx0);
+    if (ocol) t = t - tw_open<R, 1>(D, i, j, k);
+    if (orow) t = t - tw_open<R, 0>(D, i, j, k);
+  } else {
+    t = -(D.msftx(i, j) * rdx) * (fx1 - fx0);
+    if (D.do_y) t -= (D.msftx(i, j) * rdy) * (fy1 - fy0);
+  }
   const R rmsft = R(1) / D.msfty(i, j);
   if (k < nz) {
     t -= R(D.rdn[k]) * (tw_fz(D, i, j, k) - tw_fz(D, i, j, k - 1));
@@ -435,10 +556,38 @@ __device__ R sc_fz(const Dom<R>& D, const V3<R>& q, const V3<R>& wwf, int i, int
   if (pd) return vel * flux3_pd(q.ld(i, j, k - 2), q.ld(i, j, k - 1), q.ld(i, j, k), q.ld(i, j, k + 1), -vel, R(D.vup));
   return vel * flux3(q.ld(i, j, k - 2), q.ld(i, j, k - 1), q.ld(i, j, k), q.ld(i, j, k + 1), -vel, R(D.vup));
 }
-template <class R>
+// open boundaries of advect_scalar / advect_scalar_pd (kern::open_x_scalar / open_y_scalar, kernels_common.hpp:61-84):
+// the outermost column (row) takes rd (ub (qo(inner) - qo(outer)) + q (f(b) - f(a))) with the inflow mean normal
+// mass flux ub of the cell (returned without sign); DI = 1 for x, 0 for y
+template <class R, int DI>
+__device__ R open_scalar(const Dom<R>& D, const V3<R>& q, const V3<R>& qo, const V3<R>& mf, int i, int j, int k) {
+  auto M = [&](int f) { return DI ? mf.ld(f, j, k) : mf.ld(i, f, k); };
+  auto Q = [&](const V3<R>& a, int f) { return DI ? a.ld(f, j, k) : a.ld(i, f, k); };
+  const int c = DI ? i : j, n = DI ? D.nx : D.ny;
+  const R rd = DI ? R(D.rdx) : R(D.rdy);
+  if (c == 0) {
+    R ub = R(0.5) * (M(0) + M(1));
+    ub = ub < R(0) ? ub : R(0);
+    return rd * (ub * (Q(qo, 1) - Q(qo, 0)) + Q(q, 0) * (M(1) - M(0)));
+  }
+  R ub = R(0.5) * (M(n - 1) + M(n));
+  ub = ub > R(0) ? ub : R(0);
+  return rd * (ub * (Q(qo, n - 1) - Q(qo, n - 2)) + Q(q, n - 1) * (M(n) - M(n - 1)));
+}
+template <bool OP, class R>
 __device__ R tend_t(const Dom<R>& D, int i, int j, int k, bool use_tendf, bool use_hd, R fx0, R fx1, R fy0, R fy1) {
-  R r = -(D.msftx(i, j) * R(D.rdx)) * (fx1 - fx0);
-  if (D.do_y) r -= (D.msftx(i, j) * R(D.rdy)) * (fy1 - fy0);
+  R r;
+  const bool ocol = OP && D.open_x && (i == 0 || i == D.nx - 1), orow = OP && D.open_y && (j == 0 || j == D.ny - 1);
+  if (ocol || orow) {  // open boundary (:535-541): y flux, x flux, open x terms, open y terms, then the vertical
+    r = R(0);
+    if (D.do_y && !orow) r = r - (D.msftx(i, j) * R(D.rdy)) * (fy1 - fy0);
+    if (!ocol) r = r - (D.msftx(i, j) * R(D.rdx)) * (fx1 - fx0);
+    if (ocol) r = r - open_scalar<R, 1>(D, D.t2, D.t2, D.ru, i, j, k);
+    if (orow) r = r - open_scalar<R, 0>(D, D.t2, D.t2, D.rv, i, j, k);
+  } else {
+    r = -(D.msftx(i, j) * R(D.rdx)) * (fx1 - fx0);
+    if (D.do_y) r -= (D.msftx(i, j) * R(D.rdy)) * (fy1 - fy0);
+  }
   r -= R(D.rdnw[k]) * (sc_fz(D, D.t2, D.ww, i, j, k + 1, false) - sc_fz(D, D.t2, D.ww, i, j, k, false));
   if (use_tendf) r += D.t_tendf.ld(i, j, k) / D.msfty(i, j);
   if (use_hd) r += (R(D.c1h[k]) * D.mut.ld(i, j, 0) + R(D.c2h[k])) * D.hd.ld(i, j, k) / D.msfty(i, j);
@@ -471,14 +620,14 @@ template <class R, int DI, int DJ>
 __device__ __forceinline__ R dfwd(const Dom<R>& D, int i, int j, int k) {
   return D.phb(i + DI, j + DJ, k) - D.phb(i, j, k) + D.ph2.ld(i + DI, j + DJ, k) - D.ph2.ld(i, j, k);
 }
-__device__ __forceinline__ int ph_horder(int i, int n, int on, int is_x) {
+__device__ __forceinline__ int ph_horder(int i, int n, int on, int is_x, int open_x) {
   if (!on) return 6;
   if (i <= 0 || i >= n - 1) return 0;
   if (i == 1 || i == n - 2) return 2;
-  if (i == 2 || i == n - 3) return is_x ? 0 : 4;
+  if (i == 2 || i == n - 3) return (is_x && !open_x) ? 0 : 4;  // open x: 4th order (open_xs/xe only)
   return 6;
 }
-template <class R>
+template <bool OP, class R>
 __device__ R tend_ph(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
   const int nz = D.nz;
   const R c1f = R(D.c1f[k]), c2f = R(D.c2f[k]);
@@ -491,7 +640,7 @@ __device__ R tend_ph(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
     const R vp = k < nz ? D.v2.ld(i, j + 1, k) + D.v2.ld(i, j + 1, k - 1) : R(D.cfn) * D.v2.ld(i, j + 1, nz - 1) + R(D.cfn1) * D.v2.ld(i, j + 1, nz - 2);
     const R vm = k < nz ? D.v2.ld(i, j, k) + D.v2.ld(i, j, k - 1) : R(D.cfn) * D.v2.ld(i, j, nz - 1) + R(D.cfn1) * D.v2.ld(i, j, nz - 2);
     const R cy = (k < nz ? R(0.25) : R(0.5)) * R(D.rdy) / D.msfty(i, j);
-    const int o = ph_horder(j, D.ny, D.spec_y, 0);
+    const int o = ph_horder(j, D.ny, D.spec_y, 0, OP && D.open_x);
     if (o == 6) t = t - cy * ((mvp * vp * D.msfvy(i, j + 1) + mvm * vm * D.msfvy(i, j)) * r60 * grad6<R, 0, 1>(D, i, j, k));
     else if (o == 4) t = t - cy * ((mvp * vp * D.msfvy(i, j + 1) + mvm * vm * D.msfvy(i, j)) * r12 * grad4<R, 0, 1>(D, i, j, k));
     else if (o == 2)
@@ -501,11 +650,41 @@ __device__ R tend_ph(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
   const R up = k < nz ? D.u2.ld(i + 1, j, k) + D.u2.ld(i + 1, j, k - 1) : R(D.cfn) * D.u2.ld(i + 1, j, nz - 1) + R(D.cfn1) * D.u2.ld(i + 1, j, nz - 2);
   const R um = k < nz ? D.u2.ld(i, j, k) + D.u2.ld(i, j, k - 1) : R(D.cfn) * D.u2.ld(i, j, nz - 1) + R(D.cfn1) * D.u2.ld(i, j, nz - 2);
   const R cx = (k < nz ? R(0.25) : R(0.5)) * R(D.rdx) / D.msfty(i, j);
-  const int o = ph_horder(i, D.nx, D.spec_x, 1);
+  const int o = ph_horder(i, D.nx, D.spec_x, 1, OP && D.open_x);
   if (o == 6) t = t - cx * ((mup * up * D.msfux(i + 1, j) + mum * um * D.msfux(i, j)) * r60 * grad6<R, 1, 0>(D, i, j, k));
   else if (o == 2)
     t = t - cx * (mup * up * D.msfux(i + 1, j) * dfwd<R, 1, 0>(D, i, j, k) + mum * um * D.msfux(i, j) * dfwd<R, 1, 0>(D, i - 1, j, k));
   else if (o == 4) t = t - cx * ((mup * up * D.msfux(i + 1, j) + mum * um * D.msfux(i, j)) * r12 * grad4<R, 1, 0>(D, i, j, k));
+  // open boundaries (:636-663, after the advection, south/north then west/east): inflow advection of ph by the
+  // normal wind interpolated to the w level (top: level nz - 1, except the west lid level, which adds nothing)
+  if (OP && D.open_y && (j == 0 || j == D.ny - 1)) {
+    const int kz = k < nz - 1 ? k : nz - 1;
+    const int a = j == 0 ? 0 : D.ny - 1, b = j == 0 ? 1 : D.ny;
+    const R vb = R(0.5) * (R(D.fnm[kz]) * (D.v2.ld(i, b, kz) + D.v2.ld(i, a, kz)) +
+                           R(D.fnp[kz]) * (D.v2.ld(i, b, kz - 1) + D.v2.ld(i, a, kz - 1)));
+    const R muf = c1f * D.mut.ld(i, j, 0) + c2f;
+    if (j == 0) {
+      const R vl = vb < R(0) ? vb : R(0);
+      t = t - R(D.rdy) * muf * (vl * (D.ph2.ld(i, 1, k) - D.ph2.ld(i, 0, k)));
+    } else {
+      const R vr = vb > R(0) ? vb : R(0);
+      t = t - R(D.rdy) * muf * (vr * (D.ph2.ld(i, j, k) - D.ph2.ld(i, j - 1, k)));
+    }
+  }
+  if (OP && D.open_x && (i == 0 || i == D.nx - 1) && !(i == 0 && k == nz)) {
+    const int kz = k < nz ? k : nz - 1;
+    const int a = i == 0 ? 0 : D.nx - 1, b = i == 0 ? 1 : D.nx;
+    const R ub = R(0.5) * (R(D.fnm[kz]) * (D.u2.ld(b, j, kz) + D.u2.ld(a, j, kz)) +
+                           R(D.fnp[kz]) * (D.u2.ld(b, j, kz - 1) + D.u2.ld(a, j, kz - 1)));
+    const R muf = c1f * D.mut.ld(i, j, 0) + c2f;
+    if (i == 0) {
+      const R ul = ub < R(0) ? ub : R(0);
+      t = t - (D.msftx(i, j) / D.msfty(i, j)) * R(D.rdx) * muf * (ul * (D.ph2.ld(1, j, k) - D.ph2.ld(0, j, k)));
+    } else {
+      const R ur = ub > R(0) ? ub : R(0);
+      t = t - (D.msftx(i, j) / D.msfty(i, j)) * R(D.rdx) * muf * (ur * (D.ph2.ld(i, j, k) - D.ph2.ld(i - 1, j, k)));
+    }
+  }
   if (use_tendf) t = t + D.ph_tendf.ld(i, j, k) / D.msfty(i, j);
   return t;
 }
@@ -610,7 +789,7 @@ __device__ __forceinline__ bool spec_at(Ring r, int i, int j, int& sl, int& pos)
 // its own range: ru (u_i0 .. u_i1), rv (v_j0 .. v_j1, 3-D), rw and ph (levels 1..nz), theta (mass cells).
 // Also mu_tend = 0 (zero_tend of a run with lateral boundaries) at rk 2 and 3, and with lateral
 // boundaries the spec zone's tendencies from the boundary slabs.
-template <class R, int NM, int SH>
+template <class R, int NM, int SH, bool OP>
 __global__ void __launch_bounds__(PX) k_tend(const __grid_constant__ Pack<R, NM> P, int rk) {
   constexpr int SX = shape_x(SH), SY = shape_y(SH);
   // the horizontal face fluxes of the block's tile, each evaluated once (u, v, w, theta): x faces i0 .. i0 + SX
@@ -670,17 +849,21 @@ __global__ void __launch_bounds__(PX) k_tend(const __grid_constant__ Pack<R, NM>
   R tu = 0, tv = 0;
   if (lbc && k < nz && spec_at(ring_for(nx, ny, 'u'), i, j, sl, pos)) {
     tu = slab_at(D.lbc_var[0], 1, sl, pos, k, 0);
+  } else if (OP && D.open_x && (i == 0 || i == nx) && j < ny && k < nz) {  // open boundaries: the faces are advanced too
+    tu = tend_u_open_face(D, i, j, k, use_tendf);
   } else if (i >= ui0 && i < nx && j < ny && k < nz) {
     F(0, fx0, fx1, fy0, fy1);
-    tu = tend_u(D, i, j, k, use_tendf, fx0, fx1, fy0, fy1);
+    tu = tend_u<OP>(D, i, j, k, use_tendf, fx0, fx1, fy0, fy1);
   } else {
     has_u = false;
   }
   if (lbc && k < nz && spec_at(ring_for(nx, ny, 'v'), i, j, sl, pos)) {
     tv = slab_at(D.lbc_var[1], 1, sl, pos, k, 0);
+  } else if (OP && dy && D.open_y && (j == 0 || j == ny) && i < nx && k < nz) {
+    tv = tend_v_open_face(D, i, j, k, use_tendf);
   } else if (dy && i < nx && j >= vj0 && j < ny && k < nz) {
     F(1, fx0, fx1, fy0, fy1);
-    tv = tend_v(D, i, j, k, use_tendf, fx0, fx1, fy0, fy1);
+    tv = tend_v<OP>(D, i, j, k, use_tendf, fx0, fx1, fy0, fy1);
   } else {
     has_v = false;
   }
@@ -691,13 +874,13 @@ __global__ void __launch_bounds__(PX) k_tend(const __grid_constant__ Pack<R, NM>
   if (mass) {
     if (k >= 1) {
       F(2, fx0, fx1, fy0, fy1);
-      tw = tend_w(D, i, j, k, use_tendf, fx0, fx1, fy0, fy1);
+      tw = tend_w<OP>(D, i, j, k, use_tendf, fx0, fx1, fy0, fy1);
     }
     if (spec) {
       tp = slab_at(D.lbc_var[3], 1, sl, pos, k, 0);
       has_p = true;
     } else if (k >= 1) {
-      tp = tend_ph(D, i, j, k, lbc);
+      tp = tend_ph<OP>(D, i, j, k, lbc);
       has_p = true;
     }
     if (k < nz) {
@@ -705,7 +888,7 @@ __global__ void __launch_bounds__(PX) k_tend(const __grid_constant__ Pack<R, NM>
         tt = slab_at(D.lbc_var[2], 1, sl, pos, k, 0);
       } else {
         F(3, fx0, fx1, fy0, fy1);
-        tt = tend_t(D, i, j, k, use_tendf, D.n_moist > 0, fx0, fx1, fy0, fy1);
+        tt = tend_t<OP>(D, i, j, k, use_tendf, D.n_moist > 0, fx0, fx1, fy0, fy1);
       }
     }
     if (k == 0 && lbc) {
@@ -875,19 +1058,27 @@ __device__ __forceinline__ R d6(const V3<R>& f, int i, int j, int k, int opt) {
   if (opt == 2 && d * (F(0) - F(-1)) <= R(0)) d = R(0);
   return d;
 }
-// the filter's index ranges (sixth_order.hpp:151-180): kind 'u', 'v', or 'm' (also w's levels 1..nz-1)
-__device__ __forceinline__ bool d6_in(char kind, int nx, int ny, bool sp, bool px, int i, int j) {
+// the filter's index ranges (sixth_order.hpp:174-205): kind 'u', 'v', or 'm' (also w's levels 1..nz-1); open
+// sides start 3 rows in and end 3 (u, v along their stagger) or 4 rows in, 'v' with open x takes the specified
+// limits on all four sides
+__device__ __forceinline__ bool d6_in(char kind, int nx, int ny, bool sp, bool px, bool ox, bool oy, int i, int j) {
   int is = 0, js = 0, ie, je;
   if (kind == 'u') {
     ie = nx + 1; je = ny;
+    if (ox) { is = 3; ie = nx - 2; }
+    if (oy) { js = 3; je = ny - 3; }
     if (sp) { is = 3; ie = nx - 2; js = 3; je = ny - 3; }
     if (px) { is = 0; ie = nx + 1; }
   } else if (kind == 'v') {
     ie = nx; je = ny + 1;
-    if (sp) { is = 3; ie = nx - 3; js = 3; je = ny - 2; }
+    if (ox) { is = 3; ie = nx - 3; }
+    if (oy) { js = 3; je = ny - 2; }
+    if (ox || sp) { is = 3; ie = nx - 3; js = 3; je = ny - 2; }
     if (px) { is = 0; ie = nx; }
   } else {
     ie = nx; je = ny;
+    if (ox) { is = 3; ie = nx - 3; }
+    if (oy) { js = 3; je = ny - 3; }
     if (sp) { is = 3; ie = nx - 3; js = 3; je = ny - 3; }
     if (px) { is = 0; ie = nx; }
   }
@@ -1022,8 +1213,11 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
   const Dom<R>& D = *Dp;
   const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
   const bool dd = D.diff_on;
-  const bool sp = D.lbc;  // specified boundaries (the diffusion's index ranges)
-  const bool px = D.bc_x == CW_BC_PERIODIC;
+  const bool sp = D.lbc;  // specified boundaries (relaxation; the diffusion's index ranges)
+  const bool px = D.bc_x == CW_BC_PERIODIC, ox = D.open_x, oy = D.open_y;
+  // horizontal_diffusion / vertical_diffusion_u, _v loop limits (big_step_diffusion.hpp:359-398, :459-500): one row
+  // in on the open sides, and on every side when any side is specified
+  const bool bx = sp || ox, by = sp || oy;
   const R khdif = R(D.khdif), kvdif = R(D.kvdif);
   const R khh = R(D.khdif / D.prandtl);
   const bool d6on = D.diff_6th_opt != 0 && D.diff_6th_factor != 0.0;  // sixth_order_diffusion (diffusion_driver.cpp:266-280)
@@ -1031,15 +1225,15 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
   if (j < ny && k < nz) {  // ru_tendf: U points [0, nx] x [0, ny) x [0, nz)
     R t = 0;
     if (dd) {
-      int is = sp ? 1 : 0, ie = sp ? nx : nx + 1;
-      const int js = sp ? 1 : 0, je = sp ? ny - 1 : ny;
+      int is = bx ? 1 : 0, ie = bx ? nx : nx + 1;
+      const int js = by ? 1 : 0, je = by ? ny - 1 : ny;
       if (px) { is = 0; ie = nx + 1; }
       if (i >= is && i < ie && j >= js && j < je) t += hdiff_u(D, D.u2, D.mut, khdif, i, j, k);
-      int vis = sp ? 1 : 0, vie = sp ? nx : nx + 1;
+      int vis = bx ? 1 : 0, vie = bx ? nx : nx + 1;
       if (px) { vis = 0; vie = nx + 1; }
       if (i >= vis && i < vie && k < nz - 1) t += vdiff_uv<R, 1, 0>(D, D.u2, D.u_base, D.muu, kvdif, i, j, k);
     }
-    if (d6on && d6_in('u', nx, ny, sp, px, i, j)) {
+    if (d6on && d6_in('u', nx, ny, sp, px, ox, oy, i, j)) {
       R tx, ty;
       d6_tend(D, 'u', D.u2, D.mut, D.c1h, D.c2h, c6, i, j, k, tx, ty);
       t = t + tx + ty;
@@ -1054,14 +1248,14 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
   if (i < nx && j < nyv && k < nz) {  // rv_tendf
     R t = 0;
     if (dd && D.do_y) {
-      int is = sp ? 1 : 0, ie = sp ? nx - 1 : nx;
-      const int js = sp ? 1 : 0, je = sp ? ny : ny + 1;
+      int is = bx ? 1 : 0, ie = bx ? nx - 1 : nx;
+      const int js = by ? 1 : 0, je = by ? ny : ny + 1;
       if (px) { is = 0; ie = nx; }
       if (i >= is && i < ie && j >= js && j < je) t += hdiff_v(D, D.v2, D.mut, khdif, i, j, k);
-      const int vjs = sp ? 1 : 0, vje = sp ? ny : ny + 1;
+      const int vjs = by ? 1 : 0, vje = by ? ny : ny + 1;
       if (j >= vjs && j < vje && k < nz - 1) t += vdiff_uv<R, 0, 1>(D, D.v2, D.v_base, D.muv, kvdif, i, j, k);
     }
-    if (d6on && D.do_y && d6_in('v', nx, ny, sp, px, i, j)) {
+    if (d6on && D.do_y && d6_in('v', nx, ny, sp, px, ox, oy, i, j)) {
       R tx, ty;
       d6_tend(D, 'v', D.v2, D.mut, D.c1h, D.c2h, c6, i, j, k, tx, ty);
       t = t + tx + ty;
@@ -1079,13 +1273,13 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
   if (i < nx && j < ny) {
     R tw = 0;
     if (dd && k >= 1 && k < nz) {
-      int is = sp ? 1 : 0, ie = sp ? nx - 1 : nx;
-      const int js = sp ? 1 : 0, je = sp ? ny - 1 : ny;
+      int is = bx ? 1 : 0, ie = bx ? nx - 1 : nx;
+      const int js = by ? 1 : 0, je = by ? ny - 1 : ny;
       if (px) { is = 0; ie = nx; }
       if (i >= is && i < ie && j >= js && j < je) tw += hdiff_w(D, D.w2, D.mut, khdif, i, j, k);
       tw += vdiff_w(D, D.w2, D.mut, kvdif, i, j, k);
     }
-    if (d6on && k >= 1 && k < nz && d6_in('m', nx, ny, sp, px, i, j)) {
+    if (d6on && k >= 1 && k < nz && d6_in('m', nx, ny, sp, px, ox, oy, i, j)) {
       R tx, ty;
       d6_tend(D, 'w', D.w2, D.mut, D.c1f, D.c2f, c6, i, j, k, tx, ty);
       tw = tw + tx + ty;
@@ -1100,13 +1294,13 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
     if (k < nz) {
       R tt = 0;
       if (dd) {
-        int is = sp ? 1 : 0, ie = sp ? nx - 1 : nx;
-        const int js = sp ? 1 : 0, je = sp ? ny - 1 : ny;
+        int is = bx ? 1 : 0, ie = bx ? nx - 1 : nx;
+        const int js = by ? 1 : 0, je = by ? ny - 1 : ny;
         if (px) { is = 0; ie = nx; }
         if (i >= is && i < ie && j >= js && j < je) tt += hdiff_m(D, D.t2, &D.t_init, D.mut, khh, i, j, k);
         tt += vdiff_m(D, D.t2, &D.t_init, D.mut, R(3.) * kvdif, i, j, k);
       }
-      if (d6on && d6_in('m', nx, ny, sp, px, i, j)) {
+      if (d6on && d6_in('m', nx, ny, sp, px, ox, oy, i, j)) {
         R tx, ty;
         d6_tend(D, 'm', D.t2, D.mut, D.c1h, D.c2h, c6, i, j, k, tx, ty);
         tt = tt + tx + ty;

@@ -7,18 +7,19 @@
 
 namespace cw {
 
-// Edge (small_step.cpp:39-45): the spec zone of specified boundaries
+// Edge (small_step.cpp:36-45): the spec zone of specified boundaries (open boundaries have none: every cell is
+// advanced)
 template <class R>
 __device__ __forceinline__ bool edge_mass(const Dom<R>& D, int i, int j) {
-  return (D.spec_x && (i == 0 || i == D.nx - 1)) || (D.spec_y && (j == 0 || j == D.ny - 1));
+  return (D.sx && (i == 0 || i == D.nx - 1)) || (D.sy && (j == 0 || j == D.ny - 1));
 }
 template <class R>
 __device__ __forceinline__ bool edge_uface(const Dom<R>& D, int i, int j) {
-  return (D.spec_x && (i <= 0 || i >= D.nx)) || (D.spec_y && (j == 0 || j == D.ny - 1));
+  return (D.sx && (i <= 0 || i >= D.nx)) || (D.sy && (j == 0 || j == D.ny - 1));
 }
 template <class R>
 __device__ __forceinline__ bool edge_vface(const Dom<R>& D, int i, int j) {
-  return (D.spec_x && (i == 0 || i == D.nx - 1)) || (D.spec_y && (j <= 0 || j >= D.ny));
+  return (D.sx && (i == 0 || i == D.nx - 1)) || (D.sy && (j <= 0 || j >= D.ny));
 }
 template <class R>
 __device__ __forceinline__ R mh_(const Dom<R>& D, int k, R m) { return R(D.c1h[k]) * m + R(D.c2h[k]); }
@@ -79,7 +80,8 @@ __device__ __forceinline__ R uv_dp(const Dom<R>& D, int i, int j, int k, R mface
   return d;
 }
 // over the staggered index range; with lateral boundaries the spec zone's faces take
-// u += dts ru_tend (LateralBC::update_uv, lateral_bc.cpp:353-361) instead
+// u += dts ru_tend (LateralBC::update_uv, lateral_bc.cpp:353-361) instead, and so do the faces of open boundaries
+// (no pressure gradient or divergence damping on them, :175-184)
 template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_uv(const __grid_constant__ Pack<R, NM> P, int rk) {
   const Dom<R>* Dp;
@@ -101,6 +103,14 @@ __global__ void __launch_bounds__(PX) k_uv(const __grid_constant__ Pack<R, NM> P
       vn = D.v2(i, j, k) + dts * D.rv_tend.ld(i, j, k);
       sv = true;
     }
+  }
+  if (D.open_x && (i == 0 || i == D.nx) && j < D.ny) {
+    un = D.u2(i, j, k) + dts * D.ru_tend.ld(i, j, k);
+    su = true;
+  }
+  if (D.do_y && D.open_y && (j == 0 || j == D.ny) && i < D.nx) {
+    vn = D.v2(i, j, k) + dts * D.rv_tend.ld(i, j, k);
+    sv = true;
   }
   if (i < D.nx && j < D.ny) {
     const int ui0 = D.bc_x != CW_BC_PERIODIC ? 1 : 0, ui1 = D.nx;
@@ -186,7 +196,7 @@ __device__ __forceinline__ bool q_is_pd(const Dom<R>& D, int n, int rk) {
 }
 template <class R>
 __device__ __forceinline__ bool spec_cell(const Dom<R>& D, int i, int j) {
-  return (D.spec_x && (i == 0 || i == D.nx - 1)) || (D.spec_y && (j == 0 || j == D.ny - 1));
+  return (D.sx && (i == 0 || i == D.nx - 1)) || (D.sy && (j == 0 || j == D.ny - 1));
 }
 template <class R>
 __device__ __forceinline__ R m_full(const Dom<R>& D, int k, R mub, R mu) { return R(D.c1h[k]) * (mub + mu) + R(D.c2h[k]); }
@@ -201,9 +211,9 @@ __global__ void __launch_bounds__(PX) k_q_tendf_rk1(const __grid_constant__ Pack
   int i, j, k;
   if (!thread_index<SH>(P, RG_MASS, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
-  const bool sp = D.lbc, px = D.bc_x == CW_BC_PERIODIC;
-  int is = sp ? 1 : 0, ie = sp ? D.nx - 1 : D.nx;
-  const int js = sp ? 1 : 0, je = sp ? D.ny - 1 : D.ny;
+  const bool sp = D.lbc, px = D.bc_x == CW_BC_PERIODIC, bx = sp || D.open_x, by = sp || D.open_y;
+  int is = bx ? 1 : 0, ie = bx ? D.nx - 1 : D.nx;
+  const int js = by ? 1 : 0, je = by ? D.ny - 1 : D.ny;
   if (px) { is = 0; ie = D.nx; }
   const R khh = R(D.khdif / D.prandtl), kvdq = R(D.kvdif / D.prandtl);
   const Ring rq = ring_for(D.nx, D.ny, 'q');
@@ -215,7 +225,7 @@ __global__ void __launch_bounds__(PX) k_q_tendf_rk1(const __grid_constant__ Pack
     const bool qv = n == 0 && D.n_moist > 0;
     t += vdiff_m(D, D.q2[n], qv ? &D.qv_base : (const VB<R>*)nullptr, D.muts, kvdq, i, j, k);
   }
-  if (D.diff_6th_opt != 0 && D.diff_6th_factor != 0.0 && d6_in('m', D.nx, D.ny, sp, px, i, j)) {
+  if (D.diff_6th_opt != 0 && D.diff_6th_factor != 0.0 && d6_in('m', D.nx, D.ny, sp, px, D.open_x, D.open_y, i, j)) {
     R tx, ty;  // DiffusionDriver::scalar (diffusion_driver.cpp:323-326): muts and the stage's dt / 3
     d6_tend(D, 'm', D.q2[n], D.muts, D.c1h, D.c2h, d6_coef(D, R(D.dt / 3.0)), i, j, k, tx, ty);
     t = t + tx + ty;
@@ -233,8 +243,18 @@ __global__ void __launch_bounds__(PX) k_q_tendf_rk1(const __grid_constant__ Pack
 template <class R>
 __device__ R q_adv(const Dom<R>& D, const V3<R>& q, int i, int j, int k, R fx0, R fx1, R fy0, R fy1) {
   if (spec_cell(D, i, j)) return 0;
-  R r = -(D.msftx(i, j) * R(D.rdx)) * (fx1 - fx0);
-  if (D.do_y) r -= (D.msftx(i, j) * R(D.rdy)) * (fy1 - fy0);
+  R r;
+  const bool ocol = D.open_x && (i == 0 || i == D.nx - 1), orow = D.open_y && (j == 0 || j == D.ny - 1);
+  if (ocol || orow) {  // open boundary (:129-134): y flux, x flux, open x, open y (field_old = the scalar), vertical
+    r = R(0);
+    if (D.do_y && !orow) r = r - (D.msftx(i, j) * R(D.rdy)) * (fy1 - fy0);
+    if (!ocol) r = r - (D.msftx(i, j) * R(D.rdx)) * (fx1 - fx0);
+    if (ocol) r = r - open_scalar<R, 1>(D, q, q, D.ru_m, i, j, k);
+    if (orow) r = r - open_scalar<R, 0>(D, q, q, D.rv_m, i, j, k);
+  } else {
+    r = -(D.msftx(i, j) * R(D.rdx)) * (fx1 - fx0);
+    if (D.do_y) r -= (D.msftx(i, j) * R(D.rdy)) * (fy1 - fy0);
+  }
   return r - R(D.rdnw[k]) * (sc_fz(D, q, D.ww_m, i, j, k + 1, false) - sc_fz(D, q, D.ww_m, i, j, k, false));
 }
 // KUpdate (:145-156) for the non-PD species of this stage; the horizontal face fluxes of the block's tile
@@ -419,9 +439,42 @@ __global__ void __launch_bounds__(PX) k_q_scale_pd(const __grid_constant__ Pack<
   }
   D.qscale[n](i, j, k) = sc;
 }
-// KUpdatePD (:244-291) from the stored face fluxes
+// KUpdatePD in an outermost cell of an open boundary (:275-281): the open terms (Fluxes::open_terms :110-116,
+// field_old = scalar_old), the vertical term, the x term (not in the outer columns), the y term (not in the outer
+// rows). Out of line: it runs on the boundary ring only.
+template <class R>
+__device__ __noinline__ void q_update_pd_open(const Dom<R>& D, int n, R dt, int i, int j, int k) {
+  const R mub = D.mub(i, j), mu1 = D.mu1(i, j, 0), mu2 = D.mu2(i, j, 0);
+  const V3<R>& qo = D.q1[n];
+  const V3<R>& sc = D.qscale[n];
+  const bool ocol = D.open_x && (i == 0 || i == D.nx - 1), orow = D.open_y && (j == 0 || j == D.ny - 1);
+  const V3<R>* f = D.qpd + 6 * n;
+  const R s0 = sc(i, j, k);
+  auto lim = [](R d, R s_up, R s_dn) { return d * (d > 0 ? s_up : (d < 0 ? s_dn : R(1))); };
+  const R dhz0 = f[4](i, j, k), loz0 = f[5](i, j, k), dhz1 = f[4](i, j, k + 1), loz1 = f[5](i, j, k + 1);
+  const R szm = k == 0 ? R(0) : sc(i, j, k - 1), szp = (k + 1 == D.nz) ? R(0) : sc(i, j, k + 1);
+  const R dz0 = (k == 0) ? R(0) : lim(dhz0, s0, szm);
+  const R dz1 = (k + 1 == D.nz) ? R(0) : lim(dhz1, szp, s0);
+  R tend = R(0);
+  if (ocol) tend = tend - open_scalar<R, 1>(D, D.q2[n], qo, D.ru_m, i, j, k);
+  if (orow) tend = tend - open_scalar<R, 0>(D, D.q2[n], qo, D.rv_m, i, j, k);
+  tend = tend - R(D.rdnw[k]) * (dz1 - dz0 + loz1 - loz0);
+  if (!ocol) {
+    const R dhx0 = f[0](i, j, k), lox0 = f[1](i, j, k), dhx1 = f[0](i + 1, j, k), lox1 = f[1](i + 1, j, k);
+    const R dx0 = lim(dhx0, sc(i - 1, j, k), s0), dx1 = lim(dhx1, s0, sc(i + 1, j, k));
+    tend -= D.msftx(i, j) * (R(D.rdx) * (dx1 - dx0 + lox1 - lox0));
+  }
+  if (D.do_y && !orow) {
+    const R dhy0 = f[2](i, j, k), loy0 = f[3](i, j, k), dhy1 = f[2](i, j + 1, k), loy1 = f[3](i, j + 1, k);
+    const R dy0 = lim(dhy0, sc(i, j - 1, k), s0), dy1 = lim(dhy1, s0, sc(i, j + 1, k));
+    tend -= D.msftx(i, j) * (R(D.rdy) * (dy1 - dy0 + loy1 - loy0));
+  }
+  D.qn[n](i, j, k) = (m_full(D, k, mub, mu1) * qo(i, j, k) + dt * (tend * D.msfty(i, j))) / m_full(D, k, mub, mu2);
+}
+// KUpdatePD (:244-291) from the stored face fluxes; the launch bound keeps the interior path at 40 registers (the
+// boundary ring's out-of-line update spills instead)
 template <class R, int NM, int SH>
-__global__ void __launch_bounds__(PX) k_q_update_pd(const __grid_constant__ Pack<R, NM> P, int rk) {
+__global__ void __launch_bounds__(PX, 12) k_q_update_pd(const __grid_constant__ Pack<R, NM> P, int rk) {
   const Dom<R>* Dp;
   int i, j, k;
   if (!thread_index<SH>(P, RG_MASS, Dp, i, j, k)) return;
@@ -435,6 +488,10 @@ __global__ void __launch_bounds__(PX) k_q_update_pd(const __grid_constant__ Pack
   const V3<R>& sc = D.qscale[n];
   if (spec_cell(D, i, j)) {
     D.qn[n](i, j, k) = m_full(D, k, mub, mu1) * qo(i, j, k) / m_full(D, k, mub, mu2);
+    return;
+  }
+  if ((D.open_x && (i == 0 || i == D.nx - 1)) || (D.open_y && (j == 0 || j == D.ny - 1))) {
+    q_update_pd_open(D, n, dt, i, j, k);
     return;
   }
   const V3<R>* f = D.qpd + 6 * n;

@@ -293,13 +293,13 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
   double* sc = cb_array(3, nz);  // per-column scalars: sc[n * CX + lane]
   double* s_t2s = cb_array(4, nz);  // theta'' before the substep's update (t_2save), phase 1 to phase 2
   if (phase & 1) {
-    if (col && D.spec_x && i == nx && j < ny)  // KSumEdge, east face
+    if (col && D.spec_x && i == nx && j < ny)  // KSumEdge, east face (specified or open x)
       CB_LOOP(k, nz) {
         const R su = (first ? R(0) : D.ru_m(i, j, k)) + D.u2.ld(i, j, k);
         const R cpl = (R(D.c1h[k]) * D.muu.ld(i, j, 0) + R(D.c2h[k])) * D.u_save.ld(i, j, k);
         D.ru_m(i, j, k) = last ? su / rn + cpl / D.msfuy(i, j) : su;
       }
-    if (col && D.spec_y && j == ny && i < nx)  // KSumEdge, north face
+    if (col && D.spec_y && j == ny && i < nx)  // KSumEdge, north face (specified or open y)
       CB_LOOP(k, nz) {
         const R su = (first ? R(0) : D.rv_m(i, j, k)) + D.v2.ld(i, j, k);
         const R cpl = (R(D.c1h[k]) * D.muv.ld(i, j, 0) + R(D.c2h[k])) * D.v_save.ld(i, j, k);

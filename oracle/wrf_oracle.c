@@ -7,12 +7,12 @@
  * compile with -ffp-contract=off), so a difference in a single bit is a real difference.
  *
  * Scope: the options of the dynamics step that the benchmark cases use -- 2-D (ny = 1) and 3-D,
- * periodic / symmetric / specified lateral boundaries, flat or terrain base state, any hybrid
+ * periodic / symmetric / specified / open lateral boundaries, flat or terrain base state, any hybrid
  * coefficients, moist species (calc_cq, positive-definite scalar advection at rk 3), passive
  * tracers, constant-K diffusion (diff_opt 1, km_opt 1), specified lateral boundaries (width 5),
  * top_lid, w_damping, h/v_adv_order 5/6, 3/4, damp_opt 2 and 3 (sin by the pow mode: glibc's or cw_sin), the
  * sixth-order filter, hypsometric_opt 1 and 2 (log by the pow mode), Kessler microphysics. Not restated (rejected
- * by or_create): open boundaries, map factors other than 1, Coriolis, damp_opt 1.
+ * by or_create): map factors other than 1, Coriolis, damp_opt 1.
  */
 #include "wrf_oracle.h"
 
@@ -42,6 +42,7 @@ extern __m128d _ZGVbN2v_log(__m128d);
 #define H 0.5
 #define Q 0.25
 #define RERADIUS (1. / 6370.0e03)
+#define CB 25.0 /* phase speed of the open (radiative) lateral boundaries, cst::cb */
 
 /* ------------------------------------------------------------------ storage */
 typedef struct {
@@ -274,12 +275,17 @@ static double flux_upwind(double qm1, double q0, double cr) {
   return 0.5 * (lo < 1.0 ? lo : 1.0) * qm1 + 0.5 * (hi > -1.0 ? hi : -1.0) * q0;
 }
 
-/* kern::Spec (kernels_common.hpp:46-56); no open boundaries here, so sx = x, sy = y */
+/* kern::Spec (kernels_common.hpp:33-45): x / y = degraded orders (specified or open), ox / oy = open (the boundary
+ * cells are advected with the open terms), sx / sy = specified only (the outermost row is set from boundary data) */
 typedef struct {
-  int x, y, nx, ny;
+  int x, y, nx, ny, ox, oy, sx, sy;
 } spec_t;
+static int open_x(const cw_grid* g) { return g->bc_x == CW_BC_OPEN; }
+static int open_y(const cw_grid* g) { return g->bc_y == CW_BC_OPEN && !two_d(g); }
 static spec_t spec_of(const cw_grid* g) {
-  spec_t s = {flat_x(g), flat_y(g) && !two_d(g), g->nx, g->ny};
+  spec_t s = {flat_x(g), flat_y(g) && !two_d(g), g->nx, g->ny, open_x(g), open_y(g), 0, 0};
+  s.sx = s.x && !s.ox;
+  s.sy = s.y && !s.oy;
   return s;
 }
 
@@ -428,10 +434,10 @@ static double tu_fx(const tctx* c, int i, int j, int k) {
   const int o = ord_mass(i, c->sp.nx, c->sp.x);
   if (o == 2) {
     if (i <= 1) {
-      const double ub = (c->sp.x && AT(u, i, j, k) < 0.0) ? AT(u, i, j, k) : AT(u, i - 1, j, k);
+      const double ub = (c->sp.sx && AT(u, i, j, k) < 0.0) ? AT(u, i, j, k) : AT(u, i - 1, j, k);
       return Q * (AT(ru, i, j, k) + AT(ru, i - 1, j, k)) * (AT(u, i, j, k) + ub);
     }
-    const double ub = (c->sp.x && AT(u, i - 1, j, k) > 0.0) ? AT(u, i - 1, j, k) : AT(u, i, j, k);
+    const double ub = (c->sp.sx && AT(u, i - 1, j, k) > 0.0) ? AT(u, i - 1, j, k) : AT(u, i, j, k);
     return Q * (AT(ru, i, j, k) + AT(ru, i - 1, j, k)) * (AT(u, i - 1, j, k) + ub);
   }
   const double vel = H * (AT(ru, i, j, k) + AT(ru, i - 1, j, k));
@@ -465,15 +471,55 @@ static double tu_dpn(const tctx* c, int i, int j, int k) {
   if (k == nz) return c->top_lid ? H * (d->cfn * pu_(d, i, j, nz - 1) + d->cfn1 * pu_(d, i, j, nz - 2)) : 0.0;
   return H * (d->fnm[k] * pu_(d, i, j, k) + d->fnp[k] * pu_(d, i, j, k - 1));
 }
+/* advect_u open_ys / open_ye: the v-flux terms of the outermost rows (KTendU::open_y_term, :193-208) */
+static double tu_open_y(const tctx* c, int i, int j, int k) {
+  or_dom* d = c->d;
+  fld *u = F_(CW_U_2), *rv = F_(CW_RV);
+  const int imin = 0, imax = c->sp.nx - 1;
+  const int ip = i < imax ? i : imax, im = i - 1 > imin ? i - 1 : imin;
+  const double mrdy = AT(F_(CW_MSFUX), i, j, 0) * d->rdy;
+  if (j == 0) {
+    const double vw = H * (AT(rv, ip, 0, k) + AT(rv, im, 0, k));
+    const double vb = vw < 0.0 ? vw : 0.0;
+    const double dvm = AT(rv, ip, 1, k) - AT(rv, ip, 0, k), dvp = AT(rv, im, 1, k) - AT(rv, im, 0, k);
+    return mrdy * (vb * (AT(u, i, 1, k) - AT(u, i, 0, k)) + H * AT(u, i, 0, k) * (dvm + dvp));
+  }
+  const int je = c->sp.ny;
+  const double vw = H * (AT(rv, ip, je, k) + AT(rv, im, je, k));
+  const double vb = vw > 0.0 ? vw : 0.0;
+  const double dvm = AT(rv, ip, je, k) - AT(rv, ip, je - 1, k), dvp = AT(rv, im, je, k) - AT(rv, im, je - 1, k);
+  return mrdy * (vb * (AT(u, i, je - 1, k) - AT(u, i, je - 2, k)) + H * AT(u, i, je - 1, k) * (dvm + dvp));
+}
 static double tend_u(const tctx* c, int i, int j, int k, int use_tendf) {
   or_dom* d = c->d;
   fld *msfux = F_(CW_MSFUX), *msfuy = F_(CW_MSFUY), *muu = F_(CW_MUU), *mu = F_(CW_MU_2);
   fld *ph = F_(CW_PH_2), *alt = F_(CW_ALT), *p = F_(CW_P), *al = F_(CW_AL), *pb = F_(CW_PB), *php = F_(CW_PHP);
-  fld *rv = F_(CW_RV), *rw = F_(CW_RW), *u = F_(CW_U_2);
+  fld *rv = F_(CW_RV), *rw = F_(CW_RW), *u = F_(CW_U_2), *ru = F_(CW_RU), *mut = F_(CW_MUT);
   const double rdx = d->rdx, rdy = d->rdy;
+  if (c->sp.ox && (i == 0 || i == c->sp.nx)) {
+    /* open x boundary face (:210-227): the radiation condition with phase speed cb, the vertical advection unless
+     * y is open too, and the held tendency */
+    double t;
+    if (i == 0) {
+      double ub = AT(ru, 0, j, k) - CB * (d->c1h[k] * AT(mut, 0, j, 0) + d->c2h[k]);
+      ub = ub < 0.0 ? ub : 0.0;
+      t = 0.0 - rdx * ub * (AT(u, 1, j, k) - AT(u, 0, j, k));
+    } else {
+      double ub = AT(ru, i, j, k) + CB * (d->c1h[k] * AT(mut, i - 1, j, 0) + d->c2h[k]);
+      ub = ub > 0.0 ? ub : 0.0;
+      t = 0.0 - rdx * ub * (AT(u, i, j, k) - AT(u, i - 1, j, k));
+    }
+    if (!c->sp.oy) t -= d->rdnw[k] * (tu_fz(c, i, j, k + 1) - tu_fz(c, i, j, k));
+    if (use_tendf) t += AT(F_(CW_RU_TENDF), i, j, k) / AT(msfuy, i, j, 0);
+    return t;
+  }
   double t = -(AT(msfux, i, j, 0) * rdx) * (tu_fx(c, i + 1, j, k) - tu_fx(c, i, j, k));
-  if (c->do_y) t -= (AT(msfux, i, j, 0) * rdy) * (tu_fy(c, i, j + 1, k) - tu_fy(c, i, j, k));
-  t -= d->rdnw[k] * (tu_fz(c, i, j, k + 1) - tu_fz(c, i, j, k));
+  if (c->do_y) {
+    const int orow = c->sp.oy && (j == 0 || j == c->sp.ny - 1);
+    if (!orow) t -= (AT(msfux, i, j, 0) * rdy) * (tu_fy(c, i, j + 1, k) - tu_fy(c, i, j, k));
+    else t -= tu_open_y(c, i, j, k);
+  }
+  if (!(c->sp.oy && c->sp.x && (i == 0 || i == c->sp.nx))) t -= d->rdnw[k] * (tu_fz(c, i, j, k + 1) - tu_fz(c, i, j, k));
   const double rm = AT(msfux, i, j, 0) / AT(msfuy, i, j, 0);
   double dpx = rm * H * rdx * (d->c1h[k] * AT(muu, i, j, 0) + d->c2h[k]) *
                ((AT(ph, i, j, k + 1) - AT(ph, i - 1, j, k + 1) + AT(ph, i, j, k) - AT(ph, i - 1, j, k)) +
@@ -507,10 +553,10 @@ static double tv_fy(const tctx* c, int i, int j, int k) {
   const int o = ord_mass(j, c->sp.ny, c->sp.y);
   if (o == 2) {
     if (j <= 1) {
-      const double vb = (c->sp.y && AT(v, i, j, k) < 0.0) ? AT(v, i, j, k) : AT(v, i, j - 1, k);
+      const double vb = (c->sp.sy && AT(v, i, j, k) < 0.0) ? AT(v, i, j, k) : AT(v, i, j - 1, k);
       return Q * (AT(rv, i, j, k) + AT(rv, i, j - 1, k)) * (AT(v, i, j, k) + vb);
     }
-    const double vb = (c->sp.y && AT(v, i, j - 1, k) > 0.0) ? AT(v, i, j - 1, k) : AT(v, i, j, k);
+    const double vb = (c->sp.sy && AT(v, i, j - 1, k) > 0.0) ? AT(v, i, j - 1, k) : AT(v, i, j, k);
     return Q * (AT(rv, i, j, k) + AT(rv, i, j - 1, k)) * (vb + AT(v, i, j - 1, k));
   }
   const double vel = H * (AT(rv, i, j, k) + AT(rv, i, j - 1, k));
@@ -534,15 +580,55 @@ static double tv_dpn(const tctx* c, int i, int j, int k) {
   if (k == nz) return c->top_lid ? H * (d->cfn * pv_(d, i, j, nz - 1) + d->cfn1 * pv_(d, i, j, nz - 2)) : 0.0;
   return H * (d->fnm[k] * pv_(d, i, j, k) + d->fnp[k] * pv_(d, i, j, k - 1));
 }
+/* advect_v open_xs / open_xe: the u-flux terms of the outermost columns (KTendV::open_x_term, :307-323) */
+static double tv_open_x(const tctx* c, int i, int j, int k) {
+  or_dom* d = c->d;
+  fld *v = F_(CW_V_2), *ru = F_(CW_RU), *msfvy = F_(CW_MSFVY);
+  const int jmin = 0, jmax = c->sp.ny - 1;
+  const int jp = j < jmax ? j : jmax, jm = j - 1 > jmin ? j - 1 : jmin;
+  if (i == 0) {
+    const double mrdx = AT(msfvy, 0, j, 0) * d->rdx;
+    const double uw = H * (AT(ru, 0, jp, k) + AT(ru, 0, jm, k));
+    const double ub = uw < 0.0 ? uw : 0.0;
+    const double dup = AT(ru, 1, jp, k) - AT(ru, 0, jp, k), dum = AT(ru, 1, jm, k) - AT(ru, 0, jm, k);
+    return mrdx * (ub * (AT(v, 1, j, k) - AT(v, 0, j, k)) + H * AT(v, 0, j, k) * (dup + dum));
+  }
+  const int ie = c->sp.nx;
+  const double mrdx = AT(msfvy, ie - 1, j, 0) * d->rdx;
+  const double uw = H * (AT(ru, ie, jp, k) + AT(ru, ie, jm, k));
+  const double ub = uw > 0.0 ? uw : 0.0;
+  const double dup = AT(ru, ie, jp, k) - AT(ru, ie - 1, jp, k), dum = AT(ru, ie, jm, k) - AT(ru, ie - 1, jm, k);
+  return mrdx * (ub * (AT(v, ie - 1, j, k) - AT(v, ie - 2, j, k)) + H * AT(v, ie - 1, j, k) * (dup + dum));
+}
 static double tend_v(const tctx* c, int i, int j, int k, int use_tendf) {
   or_dom* d = c->d;
   fld *msfvx = F_(CW_MSFVX), *msfvy = F_(CW_MSFVY), *mvi = F_(CW_MSFVX_INV), *muv = F_(CW_MUV), *mu = F_(CW_MU_2);
   fld *ph = F_(CW_PH_2), *alt = F_(CW_ALT), *p = F_(CW_P), *al = F_(CW_AL), *pb = F_(CW_PB), *php = F_(CW_PHP);
-  fld *rw = F_(CW_RW), *v = F_(CW_V_2);
+  fld *rw = F_(CW_RW), *v = F_(CW_V_2), *rv = F_(CW_RV), *mut = F_(CW_MUT);
   const double rdx = d->rdx, rdy = d->rdy;
+  if (c->sp.oy && (j == 0 || j == c->sp.ny)) { /* open y boundary face (:327-340): radiation only */
+    double t;
+    if (j == 0) {
+      double vb = AT(rv, i, 0, k) - CB * (d->c1h[k] * AT(mut, i, 0, 0) + d->c2h[k]);
+      vb = vb < 0.0 ? vb : 0.0;
+      t = 0.0 - rdy * vb * (AT(v, i, 1, k) - AT(v, i, 0, k));
+    } else {
+      double vb = AT(rv, i, j, k) + CB * (d->c1h[k] * AT(mut, i, j - 1, 0) + d->c2h[k]);
+      vb = vb > 0.0 ? vb : 0.0;
+      t = 0.0 - rdy * vb * (AT(v, i, j, k) - AT(v, i, j - 1, k));
+    }
+    if (use_tendf) t += AT(F_(CW_RV_TENDF), i, j, k) * AT(mvi, i, j, 0);
+    return t;
+  }
   const double rm = AT(msfvy, i, j, 0) / AT(msfvx, i, j, 0);
-  double t = -(AT(msfvy, i, j, 0) * rdx) * (tv_fx(c, i + 1, j, k) - tv_fx(c, i, j, k));
-  t -= (AT(msfvy, i, j, 0) * rdy) * (tv_fy(c, i, j + 1, k) - tv_fy(c, i, j, k));
+  double t;
+  if (c->sp.ox && (i == 0 || i == c->sp.nx - 1)) { /* open x: the y flux, then the open term instead of the x flux */
+    t = -(AT(msfvy, i, j, 0) * rdy) * (tv_fy(c, i, j + 1, k) - tv_fy(c, i, j, k));
+    t -= tv_open_x(c, i, j, k);
+  } else {
+    t = -(AT(msfvy, i, j, 0) * rdx) * (tv_fx(c, i + 1, j, k) - tv_fx(c, i, j, k));
+    t -= (AT(msfvy, i, j, 0) * rdy) * (tv_fy(c, i, j + 1, k) - tv_fy(c, i, j, k));
+  }
   t -= rm * d->rdnw[k] * (tv_fz(c, i, j, k + 1) - tv_fz(c, i, j, k));
   double dpy = rm * H * rdy * (d->c1h[k] * AT(muv, i, j, 0) + d->c2h[k]) *
                ((AT(ph, i, j, k + 1) - AT(ph, i, j - 1, k + 1) + AT(ph, i, j, k) - AT(ph, i, j - 1, k)) +
@@ -601,6 +687,50 @@ static double tw_fz(const tctx* c, int i, int j, int m) { /* vertical flux at ma
   const double vel = H * (AT(ww, i, j, m + 1) + AT(ww, i, j, m));
   return vel * flux3(AT(w, i, j, m - 1), AT(w, i, j, m), AT(w, i, j, m + 1), AT(w, i, j, m + 2), -vel, c->vup);
 }
+/* advect_w open_xs/xe (open_ys/ye) terms of the outermost columns (rows) (KTendW::open_x_term / open_y_term,
+ * :416-453): fnm/fnp-interpolated ru (rv) at the w level, extrapolated at the lid */
+static double tw_open_x(const tctx* c, int i, int j, int k) {
+  or_dom* d = c->d;
+  fld *ru = F_(CW_RU), *w = F_(CW_W_2);
+  const int nz = c->nz;
+  const int a = i == 0 ? 0 : c->sp.nx - 1, b = i == 0 ? 1 : c->sp.nx;
+  double uw, dru;
+  if (k < nz) {
+    uw = H * (d->fnm[k] * (AT(ru, a, j, k) + AT(ru, b, j, k)) + d->fnp[k] * (AT(ru, a, j, k - 1) + AT(ru, b, j, k - 1)));
+    dru = d->fnm[k] * (AT(ru, b, j, k) - AT(ru, a, j, k)) + d->fnp[k] * (AT(ru, b, j, k - 1) - AT(ru, a, j, k - 1));
+  } else {
+    const double fm = 2.0 - d->fnm[nz - 1], fp = d->fnp[nz - 1];
+    uw = H * (fm * (AT(ru, a, j, nz - 1) + AT(ru, b, j, nz - 1)) - fp * (AT(ru, a, j, nz - 2) + AT(ru, b, j, nz - 2)));
+    dru = fm * (AT(ru, b, j, nz - 1) - AT(ru, a, j, nz - 1)) - fp * (AT(ru, b, j, nz - 2) - AT(ru, a, j, nz - 2));
+  }
+  if (i == 0) {
+    const double ub = uw < 0.0 ? uw : 0.0;
+    return d->rdx * (ub * (AT(w, 1, j, k) - AT(w, 0, j, k)) + AT(w, 0, j, k) * dru);
+  }
+  const double ub = uw > 0.0 ? uw : 0.0;
+  return d->rdx * (ub * (AT(w, i, j, k) - AT(w, i - 1, j, k)) + AT(w, i, j, k) * dru);
+}
+static double tw_open_y(const tctx* c, int i, int j, int k) {
+  or_dom* d = c->d;
+  fld *rv = F_(CW_RV), *w = F_(CW_W_2);
+  const int nz = c->nz;
+  const int a = j == 0 ? 0 : c->sp.ny - 1, b = j == 0 ? 1 : c->sp.ny;
+  double vw, drv;
+  if (k < nz) {
+    vw = H * (d->fnm[k] * (AT(rv, i, a, k) + AT(rv, i, b, k)) + d->fnp[k] * (AT(rv, i, a, k - 1) + AT(rv, i, b, k - 1)));
+    drv = d->fnm[k] * (AT(rv, i, b, k) - AT(rv, i, a, k)) + d->fnp[k] * (AT(rv, i, b, k - 1) - AT(rv, i, a, k - 1));
+  } else {
+    const double fm = 2.0 - d->fnm[nz - 1], fp = d->fnp[nz - 1];
+    vw = H * (fm * (AT(rv, i, a, nz - 1) + AT(rv, i, b, nz - 1)) - fp * (AT(rv, i, a, nz - 2) + AT(rv, i, b, nz - 2)));
+    drv = fm * (AT(rv, i, b, nz - 1) - AT(rv, i, a, nz - 1)) - fp * (AT(rv, i, b, nz - 2) - AT(rv, i, a, nz - 2));
+  }
+  if (j == 0) {
+    const double vb = vw < 0.0 ? vw : 0.0;
+    return d->rdy * (vb * (AT(w, i, 1, k) - AT(w, i, 0, k)) + AT(w, i, 0, k) * drv);
+  }
+  const double vb = vw > 0.0 ? vw : 0.0;
+  return d->rdy * (vb * (AT(w, i, j, k) - AT(w, i, j - 1, k)) + AT(w, i, j, k) * drv);
+}
 static double tend_w(const tctx* c, int i, int j, int k, int use_tendf, double wd_dt, double w_crit) {
   or_dom* d = c->d;
   fld *msftx = F_(CW_MSFTX), *msfty = F_(CW_MSFTY), *p = F_(CW_P), *mu = F_(CW_MU_2), *mub = F_(CW_MUB);
@@ -608,8 +738,18 @@ static double tend_w(const tctx* c, int i, int j, int k, int use_tendf, double w
       *mut = F_(CW_MUT);
   const int nz = c->nz;
   const double rdx = d->rdx, rdy = d->rdy;
-  double t = -(AT(msftx, i, j, 0) * rdx) * (tw_fx(c, i + 1, j, k) - tw_fx(c, i, j, k));
-  if (c->do_y) t -= (AT(msftx, i, j, 0) * rdy) * (tw_fy(c, i, j + 1, k) - tw_fy(c, i, j, k));
+  double t;
+  const int ocol = c->sp.ox && (i == 0 || i == c->sp.nx - 1), orow = c->sp.oy && (j == 0 || j == c->sp.ny - 1);
+  if (ocol || orow) { /* WRF order: y flux, x flux, open x terms, open y terms */
+    t = 0.0;
+    if (c->do_y && !orow) t = t - (AT(msftx, i, j, 0) * rdy) * (tw_fy(c, i, j + 1, k) - tw_fy(c, i, j, k));
+    if (!ocol) t = t - (AT(msftx, i, j, 0) * rdx) * (tw_fx(c, i + 1, j, k) - tw_fx(c, i, j, k));
+    if (ocol) t = t - tw_open_x(c, i, j, k);
+    if (orow) t = t - tw_open_y(c, i, j, k);
+  } else {
+    t = -(AT(msftx, i, j, 0) * rdx) * (tw_fx(c, i + 1, j, k) - tw_fx(c, i, j, k));
+    if (c->do_y) t -= (AT(msftx, i, j, 0) * rdy) * (tw_fy(c, i, j + 1, k) - tw_fy(c, i, j, k));
+  }
   const double rmsft = 1.0 / AT(msfty, i, j, 0);
   if (k < nz) {
     t -= d->rdn[k] * (tw_fz(c, i, j, k) - tw_fz(c, i, j, k - 1));
@@ -673,11 +813,46 @@ static double tt_fz(const tctx* c, fld* t, int i, int j, int k) {
   if (k == 1 || k == c->nz - 1) return vel * (d->fnm[k] * AT(t, i, j, k) + d->fnp[k] * AT(t, i, j, k - 1));
   return vel * flux3(AT(t, i, j, k - 2), AT(t, i, j, k - 1), AT(t, i, j, k), AT(t, i, j, k + 1), -vel, c->vup);
 }
+/* open boundaries of advect_scalar / advect_scalar_pd (kern::open_x_scalar / open_y_scalar, kernels_common.hpp:61-84):
+ * the outermost column (row) takes rdx (ub (qo(inner) - qo(outer)) + q (ru(b) - ru(a))) with the inflow mean normal
+ * mass flux ub of the cell; returned without sign */
+static double open_x_scalar(const fld* q, const fld* qo, const fld* ru, double rdx, int i, int j, int k, int nx) {
+  if (i == 0) {
+    double ub = 0.5 * (AT(ru, 0, j, k) + AT(ru, 1, j, k));
+    ub = ub < 0.0 ? ub : 0.0;
+    return rdx * (ub * (AT(qo, 1, j, k) - AT(qo, 0, j, k)) + AT(q, 0, j, k) * (AT(ru, 1, j, k) - AT(ru, 0, j, k)));
+  }
+  double ub = 0.5 * (AT(ru, nx - 1, j, k) + AT(ru, nx, j, k));
+  ub = ub > 0.0 ? ub : 0.0;
+  return rdx * (ub * (AT(qo, nx - 1, j, k) - AT(qo, nx - 2, j, k)) +
+                AT(q, nx - 1, j, k) * (AT(ru, nx, j, k) - AT(ru, nx - 1, j, k)));
+}
+static double open_y_scalar(const fld* q, const fld* qo, const fld* rv, double rdy, int i, int j, int k, int ny) {
+  if (j == 0) {
+    double vb = 0.5 * (AT(rv, i, 0, k) + AT(rv, i, 1, k));
+    vb = vb < 0.0 ? vb : 0.0;
+    return rdy * (vb * (AT(qo, i, 1, k) - AT(qo, i, 0, k)) + AT(q, i, 0, k) * (AT(rv, i, 1, k) - AT(rv, i, 0, k)));
+  }
+  double vb = 0.5 * (AT(rv, i, ny - 1, k) + AT(rv, i, ny, k));
+  vb = vb > 0.0 ? vb : 0.0;
+  return rdy * (vb * (AT(qo, i, ny - 1, k) - AT(qo, i, ny - 2, k)) +
+                AT(q, i, ny - 1, k) * (AT(rv, i, ny, k) - AT(rv, i, ny - 1, k)));
+}
 static double tend_t(const tctx* c, int i, int j, int k, int use_tendf, int use_hd) {
   or_dom* d = c->d;
   fld *t = F_(CW_T_2), *msftx = F_(CW_MSFTX), *msfty = F_(CW_MSFTY);
-  double r = -(AT(msftx, i, j, 0) * d->rdx) * (tt_fx(c, t, i + 1, j, k) - tt_fx(c, t, i, j, k));
-  if (c->do_y) r -= (AT(msftx, i, j, 0) * d->rdy) * (tt_fy(c, t, i, j + 1, k) - tt_fy(c, t, i, j, k));
+  double r;
+  const int ocol = c->sp.ox && (i == 0 || i == c->sp.nx - 1), orow = c->sp.oy && (j == 0 || j == c->sp.ny - 1);
+  if (ocol || orow) { /* open boundary (:535-541): y flux, x flux, open x terms, open y terms, then the vertical */
+    r = 0.0;
+    if (c->do_y && !orow) r = r - (AT(msftx, i, j, 0) * d->rdy) * (tt_fy(c, t, i, j + 1, k) - tt_fy(c, t, i, j, k));
+    if (!ocol) r = r - (AT(msftx, i, j, 0) * d->rdx) * (tt_fx(c, t, i + 1, j, k) - tt_fx(c, t, i, j, k));
+    if (ocol) r = r - open_x_scalar(t, t, F_(CW_RU), d->rdx, i, j, k, c->sp.nx);
+    if (orow) r = r - open_y_scalar(t, t, F_(CW_RV), d->rdy, i, j, k, c->sp.ny);
+  } else {
+    r = -(AT(msftx, i, j, 0) * d->rdx) * (tt_fx(c, t, i + 1, j, k) - tt_fx(c, t, i, j, k));
+    if (c->do_y) r -= (AT(msftx, i, j, 0) * d->rdy) * (tt_fy(c, t, i, j + 1, k) - tt_fy(c, t, i, j, k));
+  }
   r -= d->rdnw[k] * (tt_fz(c, t, i, j, k + 1) - tt_fz(c, t, i, j, k));
   if (use_tendf) r += AT(F_(CW_T_TENDF), i, j, k) / AT(msfty, i, j, 0);
   if (use_hd)
@@ -711,11 +886,11 @@ static double dfwd(or_dom* d, int DI, int DJ, int i, int j, int k) {
   fld *ph = F_(CW_PH_2), *phb = F_(CW_PHB);
   return AT(phb, i + DI, j + DJ, k) - AT(phb, i, j, k) + AT(ph, i + DI, j + DJ, k) - AT(ph, i, j, k);
 }
-static int ph_horder(int i, int n, int on, int is_x) {
+static int ph_horder(int i, int n, int on, int is_x, int open_x) {
   if (!on) return 6;
   if (i <= 0 || i >= n - 1) return 0;
   if (i == 1 || i == n - 2) return 2;
-  if (i == 2 || i == n - 3) return is_x ? 0 : 4;
+  if (i == 2 || i == n - 3) return (is_x && !open_x) ? 0 : 4; /* open x: 4th order (open_xs/xe only) */
   return 6;
 }
 static double tend_ph(const tctx* c, int i, int j, int k, int use_tendf) {
@@ -734,7 +909,7 @@ static double tend_ph(const tctx* c, int i, int j, int k, int use_tendf) {
     const double vm = k < nz ? AT(v, i, j, k) + AT(v, i, j, k - 1)
                              : d->cfn * AT(v, i, j, nz - 1) + d->cfn1 * AT(v, i, j, nz - 2);
     const double cy = (k < nz ? 0.25 : H) * d->rdy / AT(msfty, i, j, 0);
-    const int o = ph_horder(j, c->sp.ny, c->sp.y, 0);
+    const int o = ph_horder(j, c->sp.ny, c->sp.y, 0, c->sp.ox);
     if (o == 6)
       t = t - cy * ((mvp * vp * AT(msfvy, i, j + 1, 0) + mvm * vm * AT(msfvy, i, j, 0)) * r60 * grad6(d, 0, 1, i, j, k));
     else if (o == 4)
@@ -749,7 +924,7 @@ static double tend_ph(const tctx* c, int i, int j, int k, int use_tendf) {
   const double um =
       k < nz ? AT(u, i, j, k) + AT(u, i, j, k - 1) : d->cfn * AT(u, i, j, nz - 1) + d->cfn1 * AT(u, i, j, nz - 2);
   const double cx = (k < nz ? 0.25 : H) * d->rdx / AT(msfty, i, j, 0);
-  const int o = ph_horder(i, c->sp.nx, c->sp.x, 1);
+  const int o = ph_horder(i, c->sp.nx, c->sp.x, 1, c->sp.ox);
   if (o == 6)
     t = t - cx * ((mup * up * AT(msfux, i + 1, j, 0) + mum * um * AT(msfux, i, j, 0)) * r60 * grad6(d, 1, 0, i, j, k));
   else if (o == 2)
@@ -757,6 +932,36 @@ static double tend_ph(const tctx* c, int i, int j, int k, int use_tendf) {
                   mum * um * AT(msfux, i, j, 0) * dfwd(d, 1, 0, i - 1, j, k));
   else if (o == 4)
     t = t - cx * ((mup * up * AT(msfux, i + 1, j, 0) + mum * um * AT(msfux, i, j, 0)) * r12 * grad4(d, 1, 0, i, j, k));
+  /* open boundaries (:636-663, after the advection, south/north then west/east): inflow advection of ph by the normal
+   * wind interpolated to the w level (top: level nz - 1, except the west lid level, which adds nothing) */
+  fld* ph = F_(CW_PH_2);
+  if (c->sp.oy && (j == 0 || j == c->sp.ny - 1)) {
+    const int kz = k < nz - 1 ? k : nz - 1;
+    const int a = j == 0 ? 0 : c->sp.ny - 1, b = j == 0 ? 1 : c->sp.ny;
+    const double vb = H * (d->fnm[kz] * (AT(v, i, b, kz) + AT(v, i, a, kz)) + d->fnp[kz] * (AT(v, i, b, kz - 1) + AT(v, i, a, kz - 1)));
+    const double muf = d->c1f[k] * AT(mut, i, j, 0) + d->c2f[k];
+    if (j == 0) {
+      const double vl = vb < 0.0 ? vb : 0.0;
+      t = t - d->rdy * muf * (vl * (AT(ph, i, 1, k) - AT(ph, i, 0, k)));
+    } else {
+      const double vr = vb > 0.0 ? vb : 0.0;
+      t = t - d->rdy * muf * (vr * (AT(ph, i, j, k) - AT(ph, i, j - 1, k)));
+    }
+  }
+  if (c->sp.ox && (i == 0 || i == c->sp.nx - 1) && !(i == 0 && k == nz)) {
+    const int kz = k < nz ? k : nz - 1;
+    const int a = i == 0 ? 0 : c->sp.nx - 1, b = i == 0 ? 1 : c->sp.nx;
+    const double ub = H * (d->fnm[kz] * (AT(u, b, j, kz) + AT(u, a, j, kz)) + d->fnp[kz] * (AT(u, b, j, kz - 1) + AT(u, a, j, kz - 1)));
+    const double muf = d->c1f[k] * AT(mut, i, j, 0) + d->c2f[k];
+    fld* msftx = F_(CW_MSFTX);
+    if (i == 0) {
+      const double ul = ub < 0.0 ? ub : 0.0;
+      t = t - (AT(msftx, i, j, 0) / AT(msfty, i, j, 0)) * d->rdx * muf * (ul * (AT(ph, 1, j, k) - AT(ph, 0, j, k)));
+    } else {
+      const double ur = ub > 0.0 ? ub : 0.0;
+      t = t - (AT(msftx, i, j, 0) / AT(msfty, i, j, 0)) * d->rdx * muf * (ur * (AT(ph, i, j, k) - AT(ph, i - 1, j, k)));
+    }
+  }
   if (use_tendf) t = t + AT(F_(CW_PH_TENDF), i, j, k) / AT(msfty, i, j, 0);
   return t;
 }
@@ -874,22 +1079,25 @@ static double hdiff_m(or_dom* d, fld* field, fld* base, fld* mut, fld* xk, const
 }
 
 /* horizontal_diffusion's index ranges (big_step_diffusion.hpp:359-395); no open boundaries */
+/* horizontal_diffusion's loop limits (big_step_diffusion.hpp:359-398): one row in on the sides that are open or
+ * when any side is specified */
 static void hdiff_range(or_dom* d, char name, int* is, int* ie, int* js, int* je) {
   const cw_grid* g = &d->g;
   const int sp = specified(g), nx = g->nx, ny = g->ny;
-  *is = sp ? 1 : 0;
-  *js = sp ? 1 : 0;
+  const int bx = sp || open_x(g), by = sp || open_y(g);
+  *is = bx ? 1 : 0;
+  *js = by ? 1 : 0;
   if (name == 'u') {
-    *ie = sp ? nx : nx + 1;
-    *je = sp ? ny - 1 : ny;
+    *ie = bx ? nx : nx + 1;
+    *je = by ? ny - 1 : ny;
     if (g->bc_x == CW_BC_PERIODIC) { *is = 0; *ie = nx + 1; }
   } else if (name == 'v') {
-    *ie = sp ? nx - 1 : nx;
-    *je = sp ? ny : ny + 1;
+    *ie = bx ? nx - 1 : nx;
+    *je = by ? ny : ny + 1;
     if (g->bc_x == CW_BC_PERIODIC) { *is = 0; *ie = nx; }
   } else {
-    *ie = sp ? nx - 1 : nx;
-    *je = sp ? ny - 1 : ny;
+    *ie = bx ? nx - 1 : nx;
+    *je = by ? ny - 1 : ny;
     if (g->bc_x == CW_BC_PERIODIC) { *is = 0; *ie = nx; }
   }
 }
@@ -965,18 +1173,26 @@ static void sixth_order(or_dom* d, char kind, fld* f, fld* tend, fld* mut, doubl
   const int nx = g->nx, ny = g->ny, nz = g->nz, opt = d->o.diff_6th_opt;
   if (opt == 0 || d->o.diff_6th_factor == 0) return;
   const double coef = d->o.diff_6th_factor * 0.015625 / (2.0 * dt);
-  const int sp = specified(g), px = g->bc_x == CW_BC_PERIODIC;
+  const int sp = specified(g), px = g->bc_x == CW_BC_PERIODIC, ox = open_x(g), oy = open_y(g);
+  /* loop limits (sixth_order.hpp:174-205): open sides start 3 rows in and end 3 (u, v along their stagger) or 4
+   * rows in; 'v' with open x takes the specified limits on all four sides */
   int is = 0, js = 0, ie, je, k0 = 0;
   if (kind == 'u') {
     ie = nx + 1; je = ny;
+    if (ox) { is = 3; ie = nx - 2; }
+    if (oy) { js = 3; je = ny - 3; }
     if (sp) { is = 3; ie = nx - 2; js = 3; je = ny - 3; }
     if (px) { is = 0; ie = nx + 1; }
   } else if (kind == 'v') {
     ie = nx; je = ny + 1;
-    if (sp) { is = 3; ie = nx - 3; js = 3; je = ny - 2; }
+    if (ox) { is = 3; ie = nx - 3; }
+    if (oy) { js = 3; je = ny - 2; }
+    if (ox || sp) { is = 3; ie = nx - 3; js = 3; je = ny - 2; }
     if (px) { is = 0; ie = nx; }
   } else {
     ie = nx; je = ny;
+    if (ox) { is = 3; ie = nx - 3; }
+    if (oy) { js = 3; je = ny - 3; }
     if (sp) { is = 3; ie = nx - 3; js = 3; je = ny - 3; }
     if (px) { is = 0; ie = nx; }
     if (kind == 'w') k0 = 1;
@@ -1158,16 +1374,16 @@ static void diffusion_dynamics(or_dom* d) {
         for (int i = is; i < ie; ++i)
           AT(F_(CW_T_TENDF), i, j, k) += hdiff_m(d, F_(CW_T_2), F_(CW_T_INIT), mut, &d->xkhh, d->c1h, d->c2h, i, j, k);
     { /* vertical_diffusion_u (big_step_diffusion.hpp:459-479) */
-      const int sp = specified(g);
-      int vis = sp ? 1 : 0, vie = sp ? nx : nx + 1;
+      const int bx = specified(g) || open_x(g);
+      int vis = bx ? 1 : 0, vie = bx ? nx : nx + 1;
       if (g->bc_x == CW_BC_PERIODIC) { vis = 0; vie = nx + 1; }
       for (int j = 0; j < ny; ++j)
         for (int i = vis; i < vie; ++i)
           vdiff_uv(d, F_(CW_U_2), d->u_base, F_(CW_MUU), F_(CW_RU_TENDF), d->o.kvdif, 1, 0, i, j);
     }
     if (do_y) { /* vertical_diffusion_v (:481-500) */
-      const int sp = specified(g);
-      const int vjs = sp ? 1 : 0, vje = sp ? ny : ny + 1;
+      const int by = specified(g) || open_y(g);
+      const int vjs = by ? 1 : 0, vje = by ? ny : ny + 1;
       for (int j = vjs; j < vje; ++j)
         for (int i = 0; i < nx; ++i)
           vdiff_uv(d, F_(CW_V_2), d->v_base, F_(CW_MUV), F_(CW_RV_TENDF), d->o.kvdif, 0, 1, i, j);
@@ -1570,21 +1786,26 @@ static void small_run_stage(or_dom* d, double dts, int n_small, int rk_step) {
   }
   const int ui0 = g->bc_x != CW_BC_PERIODIC ? 1 : 0, ui1 = nx;
   const int vj0 = (g->bc_y != CW_BC_PERIODIC && do_y) ? 1 : 0, vj1 = ny;
+  const int ox = open_x(g), oy = open_y(g);
   const double emdx = d->o.emdiv * (1. / d->rdx), emdy = do_y ? d->o.emdiv * (1. / d->rdy) : 0.0;
   fld *mudf = &d->mudf, *ru_tend = F_(CW_RU_TEND), *rv_tend = F_(CW_RV_TEND);
   for (int it = 1; it <= n_small; ++it) {
-    /* KUV (:151-190) */
+    /* KUV (:151-190); open boundaries: the boundary faces take only the large-step tendency */
     for (int k = 0; k < nz; ++k)
-      for (int j = 0; j < ny; ++j)
-        for (int i = 0; i < nx; ++i) {
-          if (i >= ui0 && i < ui1 && !edge_uface(&ed, i, j) && j < ed.ny) {
+      for (int j = 0; j < ny + oy; ++j)
+        for (int i = 0; i < nx + ox; ++i) {
+          if (ox && (i == 0 || i == nx) && j < ny) {
+            AT(u, i, j, k) = AT(u, i, j, k) + dts * AT(ru_tend, i, j, k);
+          } else if (i >= ui0 && i < ui1 && !edge_uface(&ed, i, j) && j < ed.ny) {
             const double mudf_x = -emdx * (AT(mudf, i, j, 0) - AT(mudf, i - 1, j, 0)) / AT(msfuy, i, j, 0);
             AT(u, i, j, k) = AT(u, i, j, k) + dts * AT(ru_tend, i, j, k) -
                              dts * cqu_(d, i, j, k) *
                                  uv_dp(d, 1, 0, i, j, k, AT(muu, i, j, 0), d->rdx, AT(msfux, i, j, 0) / AT(msfuy, i, j, 0)) +
                              d->c1h[k] * mudf_x;
           }
-          if (do_y && j >= vj0 && j < vj1 && !edge_vface(&ed, i, j) && i < ed.nx) {
+          if (do_y && oy && (j == 0 || j == ny) && i < nx) {
+            AT(v, i, j, k) = AT(v, i, j, k) + dts * AT(rv_tend, i, j, k);
+          } else if (do_y && j >= vj0 && j < vj1 && !edge_vface(&ed, i, j) && i < ed.nx) {
             const double mudf_y = -emdy * (AT(mudf, i, j, 0) - AT(mudf, i, j - 1, 0)) * AT(mvi, i, j, 0);
             AT(v, i, j, k) = AT(v, i, j, k) + dts * AT(rv_tend, i, j, k) -
                              dts * cqv_(d, i, j, k) *
@@ -1679,8 +1900,8 @@ static void small_run_stage(or_dom* d, double dts, int n_small, int rk_step) {
           AT(t, i, j, k) = tn - dts * AT(msfty, i, j, 0) * (AT(msftx, i, j, 0) * hflux + d->rdnw[k] * (WDTN(k + 1) - WDTN(k)));
 #undef WDTN
         }
-    /* KSumEdge (:281-290): east / north faces of specified boundaries */
-    if (ed.x) {
+    /* KSumEdge (:281-290): east / north faces of specified and open boundaries */
+    if (ed.x || ox) {
       for (int k = 0; k < nz; ++k)
         for (int jj = 0; jj < ny; ++jj) {
           const int i = nx, j = jj;
@@ -1689,7 +1910,7 @@ static void small_run_stage(or_dom* d, double dts, int n_small, int rk_step) {
           AT(ru_m, i, j, k) = last ? su / rn + cpl / AT(msfuy, i, j, 0) : su;
         }
     }
-    if (ed.y) {
+    if (ed.y || oy) {
       for (int k = 0; k < nz; ++k)
         for (int ii = 0; ii < nx; ++ii) {
           const int i = ii, j = ny;
@@ -1960,15 +2181,33 @@ static double sf_fzl(const sflux* f, int i, int j, int k) {
   const double cr = vel * f->dt / dz / mu;
   return mu * (dz / f->dt) * flux_upwind(AT(f->qo, i, j, k - 1), AT(f->qo, i, j, k), cr);
 }
+/* spec zone of a specified boundary (not advected); the outermost cells of an open boundary are */
 static int sf_spec_cell(const sflux* f, int i, int j) {
-  return (f->sp.x && (i == 0 || i == f->sp.nx - 1)) || (f->sp.y && (j == 0 || j == f->sp.ny - 1));
+  return (f->sp.sx && (i == 0 || i == f->sp.nx - 1)) || (f->sp.sy && (j == 0 || j == f->sp.ny - 1));
+}
+static int sf_open_col(const sflux* f, int i) { return f->sp.ox && (i == 0 || i == f->sp.nx - 1); }
+static int sf_open_row(const sflux* f, int j) { return f->sp.oy && (j == 0 || j == f->sp.ny - 1); }
+/* Fluxes::open_terms (:110-116): x, then y; fo = the scalar itself (advect_scalar) or scalar_old (advect_scalar_pd) */
+static double sf_open_terms(const sflux* f, double r, int i, int j, int k, const fld* fo) {
+  or_dom* d = f->d;
+  if (sf_open_col(f, i)) r = r - open_x_scalar(f->q, fo, F_(CW_RU_M), d->rdx, i, j, k, f->sp.nx);
+  if (sf_open_row(f, j)) r = r - open_y_scalar(f->q, fo, F_(CW_RV_M), d->rdy, i, j, k, f->sp.ny);
+  return r;
 }
 static double sf_adv(const sflux* f, int i, int j, int k) {
   or_dom* d = f->d;
   fld* msftx = F_(CW_MSFTX);
   if (sf_spec_cell(f, i, j)) return 0;
-  double r = -(AT(msftx, i, j, 0) * d->rdx) * (sf_fx(f, i + 1, j, k) - sf_fx(f, i, j, k));
-  if (f->do_y) r -= (AT(msftx, i, j, 0) * d->rdy) * (sf_fy(f, i, j + 1, k) - sf_fy(f, i, j, k));
+  double r;
+  if (sf_open_col(f, i) || sf_open_row(f, j)) { /* y flux, x flux, open x, open y, vertical */
+    r = 0.0;
+    if (f->do_y && !sf_open_row(f, j)) r = r - (AT(msftx, i, j, 0) * d->rdy) * (sf_fy(f, i, j + 1, k) - sf_fy(f, i, j, k));
+    if (!sf_open_col(f, i)) r = r - (AT(msftx, i, j, 0) * d->rdx) * (sf_fx(f, i + 1, j, k) - sf_fx(f, i, j, k));
+    r = sf_open_terms(f, r, i, j, k, f->q);
+  } else {
+    r = -(AT(msftx, i, j, 0) * d->rdx) * (sf_fx(f, i + 1, j, k) - sf_fx(f, i, j, k));
+    if (f->do_y) r -= (AT(msftx, i, j, 0) * d->rdy) * (sf_fy(f, i, j + 1, k) - sf_fy(f, i, j, k));
+  }
   return r - d->rdnw[k] * (sf_fz(f, i, j, k + 1) - sf_fz(f, i, j, k));
 }
 static double m_full(or_dom* d, int k, double mub, double mu) { return d->c1h[k] * (mub + mu) + d->c2h[k]; }
@@ -2062,10 +2301,20 @@ static void scalar_update(or_dom* d, int n, int pd, double dt_rk) {
                               m_full(d, k, AT(mub, i, j, 0), AT(mu2, i, j, 0));
             continue;
           }
-          double tend = -d->rdnw[k] * (DZL(i, j, k + 1) - DZL(i, j, k) + AT(loz, i, j, k + 1) - AT(loz, i, j, k));
-          tend -= AT(msftx, i, j, 0) * (d->rdx * (DXL(i + 1, j, k) - DXL(i, j, k) + AT(lox, i + 1, j, k) - AT(lox, i, j, k)));
-          if (do_y)
-            tend -= AT(msftx, i, j, 0) * (d->rdy * (DYL(i, j + 1, k) - DYL(i, j, k) + AT(loy, i, j + 1, k) - AT(loy, i, j, k)));
+          double tend;
+          if (sf_open_col(&f, i) || sf_open_row(&f, j)) { /* open terms, vertical, x (not outer columns), y */
+            tend = sf_open_terms(&f, 0.0, i, j, k, f.qo);
+            tend = tend - d->rdnw[k] * (DZL(i, j, k + 1) - DZL(i, j, k) + AT(loz, i, j, k + 1) - AT(loz, i, j, k));
+            if (!sf_open_col(&f, i))
+              tend -= AT(msftx, i, j, 0) * (d->rdx * (DXL(i + 1, j, k) - DXL(i, j, k) + AT(lox, i + 1, j, k) - AT(lox, i, j, k)));
+            if (do_y && !sf_open_row(&f, j))
+              tend -= AT(msftx, i, j, 0) * (d->rdy * (DYL(i, j + 1, k) - DYL(i, j, k) + AT(loy, i, j + 1, k) - AT(loy, i, j, k)));
+          } else {
+            tend = -d->rdnw[k] * (DZL(i, j, k + 1) - DZL(i, j, k) + AT(loz, i, j, k + 1) - AT(loz, i, j, k));
+            tend -= AT(msftx, i, j, 0) * (d->rdx * (DXL(i + 1, j, k) - DXL(i, j, k) + AT(lox, i + 1, j, k) - AT(lox, i, j, k)));
+            if (do_y)
+              tend -= AT(msftx, i, j, 0) * (d->rdy * (DYL(i, j + 1, k) - DYL(i, j, k) + AT(loy, i, j + 1, k) - AT(loy, i, j, k)));
+          }
           AT(qn, i, j, k) = (m_full(d, k, AT(mub, i, j, 0), AT(mu1, i, j, 0)) * AT(q1, i, j, k) +
                              dt_rk * (tend * AT(msfty, i, j, 0))) /
                             m_full(d, k, AT(mub, i, j, 0), AT(mu2, i, j, 0));
@@ -2157,8 +2406,9 @@ static void tendencies(or_dom* d, int rk) {
   if (dd_on && rk == 1) diffusion_dynamics(d);
   if (d->o.lbc && rk == 1) lbc_relax_dry(d);
   const int use_tendf = d->o.lbc || dd_on;
-  const int ui0 = g->bc_x != CW_BC_PERIODIC ? 1 : 0, ui1 = nx;
-  const int vj0 = (g->bc_y != CW_BC_PERIODIC && do_y) ? 1 : 0, vj1 = ny;
+  /* open boundaries: the boundary faces are advanced too (radiation condition) */
+  const int ui0 = (g->bc_x != CW_BC_PERIODIC && !open_x(g)) ? 1 : 0, ui1 = open_x(g) ? nx + 1 : nx;
+  const int vj0 = (g->bc_y != CW_BC_PERIODIC && do_y && !open_y(g)) ? 1 : 0, vj1 = open_y(g) ? ny + 1 : ny;
   const double wd_dt = d->o.w_damping == 1 ? g->dt : 0.0;
   for (int k = 0; k < nz; ++k)
     for (int j = 0; j < ny; ++j)
@@ -2406,7 +2656,7 @@ or_dom* or_create(const cw_grid* g, const cw_options* o) {
   or_dom* d = (or_dom*)calloc(1, sizeof(or_dom));
   d->g = *g;
   d->o = *o;
-  if (g->bc_x == CW_BC_OPEN || g->bc_y == CW_BC_OPEN || (o->damp_opt != 0 && o->damp_opt != 2 && o->damp_opt != 3) || (o->hypsometric_opt != 1 && o->hypsometric_opt != 2) ||
+  if ((o->damp_opt != 0 && o->damp_opt != 2 && o->damp_opt != 3) || (o->hypsometric_opt != 1 && o->hypsometric_opt != 2) ||
       o->diff_6th_opt < 0 || o->diff_6th_opt > 2 ||
       (o->mp_physics != 0 && (o->mp_physics != 1 || o->n_moist < 3 || g->nz > KS_LEVELS)) ||
       (o->diff_opt != 0 && (o->diff_opt != 1 || o->km_opt != 1))) {

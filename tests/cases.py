@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = json.load(open(os.path.join(HERE, "golden", "reference_snapshots.json")))
 KINDS = {"straka": capi.STRAKA, "warm_bubble": capi.WARM_BUBBLE, "igw": capi.IGW, "rest_state": capi.REST_STATE,
          "squall2d": capi.SQUALL2D}
-BCS = {"periodic": capi.PERIODIC, "symmetric": capi.SYMMETRIC}
+BCS = {"periodic": capi.PERIODIC, "symmetric": capi.SYMMETRIC, "open": capi.OPEN}
 
 
 def ideal_case(cfg, lib=None, u0=None, **opt):
@@ -31,11 +31,13 @@ def golden_config(name):
     return dict(GOLDEN["cases"][name]["config"])
 
 
-def lam_case(nx=24, ny=20, nz=14, seed=3, n_moist=5, n_scalars=5, diff=False, hybrid_opt=2, precision=capi.FP64):
-    """A limited-area case (terrain, hybrid coordinate, moist species, specified boundaries) from a seed."""
-    g = capi.grid(nx, ny, nz, 15000.0, 90.0, 0.0, dy=15000.0, p_top=5000.0, bc_x=capi.SPECIFIED, bc_y=capi.SPECIFIED)
-    o = capi.default_options(None, flat=0, n_moist=n_moist, n_scalars=n_scalars, lbc=1, time_step_sound=4,
-                             precision=precision)
+def lam_case(nx=24, ny=20, nz=14, seed=3, n_moist=5, n_scalars=5, diff=False, hybrid_opt=2, precision=capi.FP64,
+             bc=(capi.SPECIFIED, capi.SPECIFIED)):
+    """A limited-area case (terrain, hybrid coordinate, moist species, specified boundaries) from a seed; bc = the
+    (x, y) boundary kinds (open or periodic sides take no boundary data)."""
+    g = capi.grid(nx, ny, nz, 15000.0, 90.0, 0.0, dy=15000.0, p_top=5000.0, bc_x=bc[0], bc_y=bc[1])
+    o = capi.default_options(None, flat=0, n_moist=n_moist, n_scalars=n_scalars,
+                             lbc=int(capi.SPECIFIED in bc), time_step_sound=4, precision=precision)
     if diff:
         o.diff_opt, o.khdif, o.kvdif, o.pr_inv = 1, 3000.0, 1.0, 3.0
     return capi.Case(g, o).gen_lam(seed=seed, hybrid_opt=hybrid_opt)

@@ -17,11 +17,13 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-@pytest.mark.parametrize("hypso", [1, 2], ids=["linear", "log_pressure"])
-def test_mixed_close_to_fp64(hypso):
-    """hypsometric_opt 1 and 2 (the log-linear form's inverse density computed in double in both forms)."""
-    c64 = lam_case(nx=40, ny=32, nz=20, seed=11)
-    c32 = lam_case(nx=40, ny=32, nz=20, seed=11, precision=capi.MIXED)
+@pytest.mark.parametrize("hypso,bc", [(1, capi.SPECIFIED), (2, capi.SPECIFIED), (1, capi.OPEN)],
+                         ids=["linear", "log_pressure", "open_boundaries"])
+def test_mixed_close_to_fp64(hypso, bc):
+    """hypsometric_opt 1 and 2 (the log-linear form's inverse density computed in double in both forms); specified
+    and open lateral boundaries."""
+    c64 = lam_case(nx=40, ny=32, nz=20, seed=11, bc=(bc, bc))
+    c32 = lam_case(nx=40, ny=32, nz=20, seed=11, precision=capi.MIXED, bc=(bc, bc))
     c64.o.hypsometric_opt = c32.o.hypsometric_opt = hypso
     d64 = Domain(c64.g, c64.o).upload_case(c64)
     d32 = Domain(c32.g, c32.o).upload_case(c32)

@@ -159,3 +159,30 @@ def test_oracle_equals_reference_hypsometric_log_pressure_2d():
     ref = _refdump.run(case, 3, own_pow=False)
     bad = compare(orc, ref, case)
     assert not bad, "\n".join(bad)
+
+
+@pytest.mark.parametrize("bc,kw", [((capi.OPEN, capi.OPEN), dict()), ((capi.OPEN, capi.OPEN), dict(diff=True)),
+                                   ((capi.OPEN, capi.PERIODIC), dict(n_moist=2, n_scalars=3)),
+                                   ((capi.PERIODIC, capi.OPEN), dict(hybrid_opt=0))],
+                         ids=["open", "open_diffusion", "open_x_periodic_y", "periodic_x_open_y"])
+def test_oracle_equals_reference_open_boundaries(bc, kw):
+    """Open lateral boundaries (WRF open_xs/xe/ys/ye): the radiation condition on the boundary faces of u and v, the
+    open terms of the outermost cells' advection (u, v, w, theta, geopotential, every scalar, PD at rk 3), the
+    boundary faces' acoustic update and time sums, the diffusion's loop limits; corners where both are open."""
+    case = lam_case(seed=17, bc=bc, **kw)
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_OWN)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=True)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)
+
+
+def test_oracle_equals_reference_open_sixth_order_2d():
+    """2-D x-z with open x (squall-line style) and the sixth-order filter's open-side limits."""
+    cfg = dict(cases.SMALL["warm_bubble_small"], bc_x="open")
+    case = cases.ideal_case(cfg, diff_6th_opt=2, diff_6th_factor=0.12)
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_GLIBC)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=False)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)

@@ -141,6 +141,27 @@ def test_2d_hypsometric_log_pressure_bit_exact():
     assert not bad, "\n".join(bad)
 
 
+@pytest.mark.parametrize("bc,kw", [((capi.OPEN, capi.OPEN), dict()), ((capi.OPEN, capi.OPEN), dict(diff=True)),
+                                   ((capi.OPEN, capi.PERIODIC), dict(n_moist=2, n_scalars=3)),
+                                   ((capi.PERIODIC, capi.OPEN), dict(hybrid_opt=0))],
+                         ids=["open", "open_diffusion", "open_x_periodic_y", "periodic_x_open_y"])
+def test_lam_open_boundaries_bit_exact(bc, kw):
+    """Open lateral boundaries: radiation on the boundary faces of u and v, the open terms of the outermost cells
+    (u, v, w, theta, geopotential, every scalar incl. PD at rk 3), the faces' acoustic update and time sums, the
+    diffusion's loop limits; 4 steps."""
+    case = lam_case(seed=17, bc=bc, **kw)
+    dom, orc = run_pair(case, 4)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
+def test_2d_open_x_sixth_order_bit_exact():
+    case = cases.ideal_case(dict(cases.SMALL["warm_bubble_small"], bc_x="open"), diff_6th_opt=2, diff_6th_factor=0.12)
+    dom, orc = run_pair(case, 3)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
 def test_cfl_maxima_equal_oracle():
     """LargeStep::cfl_max of every RK stage (the adaptive time step's input): the device maxima equal the oracle's,
     and recording them changes no field."""
