@@ -129,6 +129,9 @@ __device__ __forceinline__ void halo_cell(const HaloField& f, unsigned c, int pa
     const int j = int(r % unsigned(f.lny)), k = int(r / unsigned(f.lny));
     const int i = halo_pos(a, f.gnx, f.face_x);
     if (i < f.wi0 || i >= f.wi1) return;
+    // the last face row of a periodic y-staggered field is a y-pass slot (a copy of row 0): its x halo is the y
+    // pass's value (the reference fills x, then y); writing the stale row here too would race with that pass
+    if (f.face_y && f.periodic_y && !f.two_d && j == f.gny) return;
     const int src = halo_src(i, f.gnx, f.face_x, f.periodic_x, f.flat_x);
     if (!f.periodic_x && !f.flat_x && src == i) {  // wall face: kept, or flipped by pass 1 (OddFace)
       if (pass == 1 && f.oddface_x) p[i + j * f.sj + k * f.sk] = -p[i + j * f.sj + k * f.sk];
