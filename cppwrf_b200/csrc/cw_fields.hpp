@@ -120,8 +120,8 @@ inline const char* unsupported(const cw_grid& g, const cw_options& o) {
     return "specified boundaries: both directions of a 3-D grid";
   if (specified(g) && !o.lbc) return "specified boundaries need lbc = 1";
   if (o.lbc && !specified(g)) return "lbc = 1 needs specified boundaries";
-  if (o.damp_opt != 0 && o.damp_opt != 2 && o.damp_opt != 3) return "damp_opt must be 0, 2 or 3 (Rayleigh damping)";
-  if (o.damp_opt != 0 && !(o.zdamp > 0)) return "damp_opt 2 and 3 need zdamp > 0";
+  if (o.damp_opt < 0 || o.damp_opt > 3) return "damp_opt must be 0, 1, 2 or 3";
+  if (o.damp_opt != 0 && !(o.zdamp > 0)) return "damp_opt 1, 2 and 3 need zdamp > 0";
   if (o.damp_opt == 2 && g.nz > 127) return "damp_opt 2: nz <= 127";
   if (o.hypsometric_opt != 1 && o.hypsometric_opt != 2) return "hypsometric_opt must be 1 or 2";
   if (o.diff_opt != 0 && !(o.diff_opt == 1 && o.km_opt == 1)) return "diffusion: diff_opt 0, or 1 with km_opt 1";

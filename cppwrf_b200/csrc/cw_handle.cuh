@@ -37,7 +37,9 @@ inline size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 
 // the work fields of one domain beyond State / Tendencies / BaseState (SmallStep's fields)
 enum Work { W_U_SAVE, W_V_SAVE, W_W_SAVE, W_T_SAVE, W_PH_SAVE, W_WW1, W_C2A, W_PM1, W_T_2SAVE, W_A, W_ALPHA, W_GAMMA,
-            W_MU_SAVE, W_MUDF, W_MUAVE, W_W_RHS, W_T2A, W_N };
+            W_MU_SAVE, W_MUDF, W_MUAVE, W_W_RHS, W_T2A, W_XKMH, W_XKHH, W_N };
+// W_XKMH, W_XKHH (damp_opt 1 only; no storage otherwise)
+inline bool work_used(int w, const cw_options& o) { return (w != W_XKMH && w != W_XKHH) || o.damp_opt == 1; }
 inline FieldKind work_kind(int w) {
   switch (w) {
     case W_U_SAVE: return {'U', 3, false};
@@ -118,7 +120,7 @@ struct cw_handle {
   size_t cb_level_bytes = 0;  // one shared level array of a column block: (nz + 2) x CX doubles
   // halo sets of the fill points
   enum { H_MU1, H_PREP0, H_PREP1, H_SS0, H_UV, H_AC, H_POST, H_FIN, H_Q1PD, H_SCPD, H_Q2, H_END_P, H_WS0, H_WS1, H_MP,
-         H_MP_P, H_N };
+         H_MP_P, H_XK, H_N };
   HaloSetHost hs[H_N];
   std::vector<CopyDesc> copies;
   CopyDesc* copies_d = nullptr;

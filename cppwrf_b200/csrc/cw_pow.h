@@ -19,7 +19,7 @@
  * glibc pow and against a 60-digit decimal evaluation in tests/test_pow.py.
  *
  * cw_exp(x) is the same exponential on a double argument, cw_log(x) the same logarithm rounded to double;
- * cw_sin(x) a double-double Taylor series for |x| <= 2.
+ * cw_sin(x) and cw_cos(x) double-double Taylor series for |x| <= 2.
  *
  * Domain: any double x, y; special values follow C99 Annex F for the cases the dycore can meet
  * (x > 0 finite; NaN, 0, infinities and negative x are handled for robustness).
@@ -263,10 +263,7 @@ CW_HD double cw_log(double x) {
  * (below 2.5e-3 of the sum) in double and the first four in double-double, the last kept term 4^14 / 29! < 2^-75
  * (advance_w's Rayleigh damping of w, damp_opt 3: sin of arguments in [0, pi/2]; the reference's CPU build takes
  * glibc's sin there) */
-CW_HD double cw_sin(double x) {
-  if (x != x) return CW_ADD(x, x);
-  if (x == 0.0) return x;
-  if (!(x <= 2.0 && x >= -2.0)) return CW_DIV(0.0, 0.0);
+CW_HD void cw_sin_dd(double x, double* sh, double* sl) { /* sin(x) in double-double, |x| <= 2, x != 0 */
   double zh, zl;
   cw_two_prod(x, x, &zh, &zl);
   const double z = zh;
@@ -289,9 +286,59 @@ CW_HD double cw_sin(double x) {
   cw_dd_add(-0x1.5555555555555p-3, -0x1.5555555555555p-57, ah, al, &ah, &al); /* -1/3! + z A */
   cw_dd_mul(zh, zl, ah, al, &ah, &al);
   cw_dd_add(1.0, 0.0, ah, al, &ah, &al); /* 1 + z A */
+  cw_dd_mul(x, 0.0, ah, al, sh, sl);
+}
+CW_HD double cw_sin(double x) {
+  if (x != x) return CW_ADD(x, x);
+  if (x == 0.0) return x;
+  if (!(x <= 2.0 && x >= -2.0)) return CW_DIV(0.0, 0.0);
   double sh, sl;
-  cw_dd_mul(x, 0.0, ah, al, &sh, &sl);
+  cw_sin_dd(x, &sh, &sl);
   return CW_ADD(sh, sl);
+}
+
+/* cos(x) for |x| <= 2 (NaN outside): for |x| <= pi/4 the Taylor series cos x = sum_n (-1)^n x^(2n) / (2n)!, its terms
+ * n >= 4 (below 4.1e-4 of the sum) in double and the first four in double-double, the last kept term
+ * (pi/4)^26 / 26! < 2^-95; above pi/4, cos x = sin(pi/2 - x) with pi/2 - x in double-double from the exact
+ * difference pio2_hi - x (Sterbenz) and the two lower parts of pi/2, so that the result keeps its relative accuracy
+ * near pi/2 (the eddy-viscosity damping of damp_opt 1: cos of arguments in [0, pi/2]; the
+ * reference's CPU build takes glibc's cos there, libmvec's on the lanes of its vectorised column loop) */
+CW_HD double cw_cos(double x) {
+  if (x != x) return CW_ADD(x, x);
+  if (x < 0.0) x = -x;
+  if (!(x <= 2.0)) return CW_DIV(0.0, 0.0);
+  if (x > 0x1.921fb54442d18p-1) {
+    /* u = pi/2 - x in double-double from a three-part pi/2; sin(uh + ul) = sin(uh) + ul cos(uh) to the last bit */
+    double uh, ul;
+    cw_dd_add(CW_SUB(0x1.921fb54442d18p+0, x), 0.0, 0x1.1a62633145c07p-54, -0x1.f1976b7ed8fbcp-110, &uh, &ul);
+    double sh = 0.0, sl = 0.0;
+    if (uh != 0.0) cw_sin_dd(uh, &sh, &sl);
+    const double u2 = CW_MUL(uh, uh);
+    const double c = CW_ADD(1.0, CW_MUL(u2, CW_ADD(-0.5, CW_MUL(u2, 0x1.5555555555555p-5)))); /* cos uh to its size here */
+    return CW_ADD(sh, CW_ADD(sl, CW_MUL(ul, c)));
+  }
+  double zh, zl;
+  cw_two_prod(x, x, &zh, &zl);
+  const double z = zh;
+  double t = -0x1.88e85fc6a4e5ap-89;               /* -1/26! */
+  t = CW_ADD(0x1.f2cf01972f578p-80, CW_MUL(z, t));  /* 1/24! */
+  t = CW_ADD(-0x1.0ce396db7f853p-70, CW_MUL(z, t)); /* -1/22! */
+  t = CW_ADD(0x1.e542ba4020225p-62, CW_MUL(z, t));  /* 1/20! */
+  t = CW_ADD(-0x1.6827863b97d97p-53, CW_MUL(z, t)); /* -1/18! */
+  t = CW_ADD(0x1.ae7f3e733b81fp-45, CW_MUL(z, t));  /* 1/16! */
+  t = CW_ADD(-0x1.93974a8c07c9dp-37, CW_MUL(z, t)); /* -1/14! */
+  t = CW_ADD(0x1.1eed8eff8d898p-29, CW_MUL(z, t));  /* 1/12! */
+  t = CW_ADD(-0x1.27e4fb7789f5cp-22, CW_MUL(z, t)); /* -1/10! */
+  t = CW_ADD(0x1.a01a01a01a01ap-16, CW_MUL(z, t));  /* 1/8! */
+  double ah, al;
+  cw_dd_add(-0x1.6c16c16c16c17p-10, 0x1.f49f49f49f49fp-65, CW_MUL(z, t), 0.0, &ah, &al); /* -1/6! + z t */
+  cw_dd_mul(zh, zl, ah, al, &ah, &al);
+  cw_dd_add(0x1.5555555555555p-5, 0x1.5555555555555p-59, ah, al, &ah, &al); /* 1/4! + z A */
+  cw_dd_mul(zh, zl, ah, al, &ah, &al);
+  cw_dd_add(-0.5, 0.0, ah, al, &ah, &al); /* -1/2! + z A */
+  cw_dd_mul(zh, zl, ah, al, &ah, &al);
+  cw_dd_add(1.0, 0.0, ah, al, &ah, &al); /* 1 + z A */
+  return CW_ADD(ah, al);
 }
 
 #endif /* CW_POW_H */

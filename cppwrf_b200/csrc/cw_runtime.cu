@@ -66,7 +66,7 @@ Plan plan_member(Member& M) {
   for (int w = 0; w < W_N; ++w) {
     const FieldKind k = work_kind(w);
     M.LW[w] = layout_make(M.g, k.stagger, k.rank, false);
-    P.w.push_back(take(field_bytes(M.LW[w], M.esz)));
+    P.w.push_back(take(work_used(w, M.o) ? field_bytes(M.LW[w], M.esz) : 0));
   }
   M.Lq = layout_make(M.g, 'M', 3, false);
   for (int n = 0; n < M.o.n_scalars; ++n) {
@@ -174,7 +174,7 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.damp_opt = o.damp_opt; D.zdamp = o.zdamp; D.dampcoef = o.dampcoef;
   D.diff_6th_opt = o.diff_6th_opt; D.diff_6th_factor = o.diff_6th_factor;
   D.dd_on = o.diff_opt == 1 || o.diff_6th_opt != 0 || o.damp_opt == 2;  // DiffusionConfig::on
-  D.dt = g.dt; D.epssm = o.epssm; D.smdiv = o.smdiv; D.emdiv = o.emdiv; D.khdif = o.khdif; D.kvdif = o.kvdif;
+  D.dt = g.dt; D.dx = g.dx; D.dy = g.dy; D.epssm = o.epssm; D.smdiv = o.smdiv; D.emdiv = o.emdiv; D.khdif = o.khdif; D.kvdif = o.kvdif;
   D.prandtl = 1.0 / o.pr_inv;
   D.hup = o.h_adv_order == 5 ? 1.0 : 0.0;
   D.vup = o.v_adv_order == 3 ? 1.0 : 0.0;
@@ -210,6 +210,7 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.ph_save = w3(W_PH_SAVE); D.ww1 = w3(W_WW1); D.c2a = w3(W_C2A); D.pm1 = w3(W_PM1); D.t_2save = w3(W_T_2SAVE);
   D.a = w3(W_A); D.alpha = w3(W_ALPHA); D.gamma = w3(W_GAMMA); D.mu_save = w3(W_MU_SAVE); D.mudf = w3(W_MUDF);
   D.muave = w3(W_MUAVE); D.w_rhs = w3(W_W_RHS); D.t2a = w3(W_T2A);
+  if (o.damp_opt == 1) { D.xkmh = w3(W_XKMH); D.xkhh = w3(W_XKHH); }
   const int ns = o.n_scalars;
   D.q1 = qtab_d; D.q2 = qtab_d + ns; D.qn = qtab_d + 2 * ns; D.qtf = qtab_d + 3 * ns; D.qscale = qtab_d + 4 * ns;
   D.qpd = qtab_d + 5 * ns;
@@ -381,6 +382,7 @@ void build_halosets_t(cw_handle* h, DevTables<R>& T) {
     };
     const bool spec = specified(M.g);
     add(cw_handle::H_MU1, {F(CW_MU_1)});
+    if (M.o.damp_opt == 1) add(cw_handle::H_XK, {W(W_XKMH), W(W_XKHH)});  // DiffusionDriver::prepare's fill
     add(cw_handle::H_PREP0, {F(CW_U_2), F(CW_V_2), F(CW_W_2), F(CW_T_2), F(CW_PH_2), F(CW_P), F(CW_AL)});
     if (!spec) add(cw_handle::H_PREP0, {F(CW_MU_2)});
     add(cw_handle::H_PREP1, {F(CW_MUT), F(CW_RU), F(CW_RV), F(CW_RW), F(CW_ALT), F(CW_PHP), F(CW_MUU, HP_ODDFACE_X),

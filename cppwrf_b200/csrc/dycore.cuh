@@ -55,11 +55,12 @@ struct Dom {
   int dd_on;     // a DiffusionDriver is attached (diff_opt 1 or the sixth-order filter): the tendf enter the tendencies
   int diff_6th_opt;
   double diff_6th_factor;
-  int damp_opt;  // 3: implicit Rayleigh damping of w in the upper zdamp metres (advance_w)
+  int damp_opt;  // 1: eddy viscosities raised near the top (xkmh, xkhh); 2: Rayleigh toward the base state; 3: implicit w
   double zdamp, dampcoef;
   int mp_physics;  // 1: Kessler after the RK3 loop (species 0, 1, 2 = qv, qc, qr)
   double mp_tend_lim;
   double dt, epssm, smdiv, emdiv, khdif, kvdif, prandtl, hup, vup, w_crit_cfl;
+  double dx, dy;  // grid spacing (cal_dampkm's horizontal limit)
   double* dtbc;  // device scalar: time since the boundary data (LateralBC::dtbc), advanced on the device
   unsigned long long* cfl;  // per RK stage: the vertical and horizontal CFL maxima (bits of positive doubles)
   double rdx, rdy, cf1, cf2, cf3, cfn, cfn1;
@@ -80,6 +81,7 @@ struct Dom {
   // acoustic-step work fields (SmallStep, src/dyn/small_step.hpp:45-49)
   V3<T> u_save, v_save, w_save, t_save, ph_save, ww1, c2a, pm1, t_2save, a, alpha, gamma, mu_save, mudf, muave,
       w_rhs, t2a;
+  V3<T> xkmh, xkhh;  // damp_opt 1: the horizontal eddy viscosities of momentum and heat per mass point (level 0..nz-1)
   // scalars: device tables of views (q2 and q_new swap roles after each update)
   V3<T>* q1;
   V3<T>* q2;

@@ -922,71 +922,83 @@ template <class R>
 __device__ __forceinline__ R mk(const double* c1, const double* c2, const V3<R>& mut, int i, int j, int k) {
   return R(c1[k]) * mut.ld(i, j, 0) + R(c2[k]);
 }
+// the horizontal eddy viscosity at a mass point: the constant of km_opt 1 (KIsotropicKm, km_kh.hpp:35-45), or the
+// per-point field that cal_dampkm raised near the top (damp_opt 1)
 template <class R>
-__device__ R hdiff_u(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, R xk, int i, int j, int k) {
+struct XkConst {
+  R v;
+  __device__ __forceinline__ R operator()(int, int, int) const { return v; }
+};
+template <class R>
+struct XkField {
+  V3<R> a;
+  __device__ __forceinline__ R operator()(int i, int j, int k) const { return a.ld(i, j, k); }
+};
+template <class R, class XK>
+__device__ R hdiff_u(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, XK X, int i, int j, int k) {
   const double *c1 = D.c1h, *c2 = D.c2h;
   const R rdx = R(D.rdx), rdy = R(D.rdy);
-  const R mkrdxm = (D.msftx(i - 1, j) / D.msfty(i - 1, j)) * mk(c1, c2, mut, i - 1, j, k) * xk * rdx;
-  const R mkrdxp = (D.msftx(i, j) / D.msfty(i, j)) * mk(c1, c2, mut, i, j, k) * xk * rdx;
+  const R mkrdxm = (D.msftx(i - 1, j) / D.msfty(i - 1, j)) * mk(c1, c2, mut, i - 1, j, k) * X(i - 1, j, k) * rdx;
+  const R mkrdxp = (D.msftx(i, j) / D.msfty(i, j)) * mk(c1, c2, mut, i, j, k) * X(i, j, k) * rdx;
   const R mrdx = D.msfux(i, j) * D.msfuy(i, j) * rdx;
   const R mkrdym = ((D.msfuy(i, j) + D.msfuy(i, j - 1)) / (D.msfux(i, j) + D.msfux(i, j - 1))) * R(0.25) *
                    (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k) + mk(c1, c2, mut, i - 1, j - 1, k) + mk(c1, c2, mut, i - 1, j, k)) *
-                   R(0.25) * (xk + xk + xk + xk) * rdy;
+                   R(0.25) * (X(i, j, k) + X(i, j - 1, k) + X(i - 1, j - 1, k) + X(i - 1, j, k)) * rdy;
   const R mkrdyp = ((D.msfuy(i, j) + D.msfuy(i, j + 1)) / (D.msfux(i, j) + D.msfux(i, j + 1))) * R(0.25) *
                    (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j + 1, k) + mk(c1, c2, mut, i - 1, j + 1, k) + mk(c1, c2, mut, i - 1, j, k)) *
-                   R(0.25) * (xk + xk + xk + xk) * rdy;
+                   R(0.25) * (X(i, j, k) + X(i, j + 1, k) + X(i - 1, j + 1, k) + X(i - 1, j, k)) * rdy;
   const R mrdy = D.msfux(i, j) * D.msfuy(i, j) * rdy;
   return mrdx * (mkrdxp * (f.ld(i + 1, j, k) - f.ld(i, j, k)) - mkrdxm * (f.ld(i, j, k) - f.ld(i - 1, j, k))) +
          mrdy * (mkrdyp * (f.ld(i, j + 1, k) - f.ld(i, j, k)) - mkrdym * (f.ld(i, j, k) - f.ld(i, j - 1, k)));
 }
-template <class R>
-__device__ R hdiff_v(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, R xk, int i, int j, int k) {
+template <class R, class XK>
+__device__ R hdiff_v(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, XK X, int i, int j, int k) {
   const double *c1 = D.c1h, *c2 = D.c2h;
   const R rdx = R(D.rdx), rdy = R(D.rdy);
   const R mkrdxm = ((D.msfvx(i, j) + D.msfvx(i - 1, j)) / (D.msfvy(i, j) + D.msfvy(i - 1, j))) * R(0.25) *
                    (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k) + mk(c1, c2, mut, i - 1, j - 1, k) + mk(c1, c2, mut, i - 1, j, k)) *
-                   R(0.25) * (xk + xk + xk + xk) * rdx;
+                   R(0.25) * (X(i, j, k) + X(i, j - 1, k) + X(i - 1, j - 1, k) + X(i - 1, j, k)) * rdx;
   const R mkrdxp = ((D.msfvx(i, j) + D.msfvx(i + 1, j)) / (D.msfvy(i, j) + D.msfvy(i + 1, j))) * R(0.25) *
                    (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k) + mk(c1, c2, mut, i + 1, j - 1, k) + mk(c1, c2, mut, i + 1, j, k)) *
-                   R(0.25) * (xk + xk + xk + xk) * rdx;
+                   R(0.25) * (X(i, j, k) + X(i, j - 1, k) + X(i + 1, j - 1, k) + X(i + 1, j, k)) * rdx;
   const R mrdx = D.msfvx(i, j) * D.msfvy(i, j) * rdx;
-  const R mkrdym = (D.msfty(i, j - 1) / D.msftx(i, j - 1)) * xk * rdy;
-  const R mkrdyp = (D.msfty(i, j) / D.msftx(i, j)) * xk * rdy;
+  const R mkrdym = (D.msfty(i, j - 1) / D.msftx(i, j - 1)) * X(i, j - 1, k) * rdy;
+  const R mkrdyp = (D.msfty(i, j) / D.msftx(i, j)) * X(i, j, k) * rdy;
   const R mrdy = D.msfvx(i, j) * D.msfvy(i, j) * rdy;
   return mrdx * (mkrdxp * (f.ld(i + 1, j, k) - f.ld(i, j, k)) - mkrdxm * (f.ld(i, j, k) - f.ld(i - 1, j, k))) +
          mrdy * (mkrdyp * (f.ld(i, j + 1, k) - f.ld(i, j, k)) - mkrdym * (f.ld(i, j, k) - f.ld(i, j - 1, k)));
 }
-template <class R>
-__device__ R hdiff_w(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, R xk, int i, int j, int k) {
+template <class R, class XK>
+__device__ R hdiff_w(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, XK X, int i, int j, int k) {
   const double *c1 = D.c1f, *c2 = D.c2f;
   const R rdx = R(D.rdx), rdy = R(D.rdy);
   const R mkrdxm = (D.msfux(i, j) / D.msfuy(i, j)) * R(0.25) *
                    (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i - 1, j, k) + mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i - 1, j, k)) *
-                   R(0.25) * (xk + xk + xk + xk) * rdx;
+                   R(0.25) * (X(i, j, k) + X(i - 1, j, k) + X(i, j, k - 1) + X(i - 1, j, k - 1)) * rdx;
   const R mkrdxp = (D.msfux(i + 1, j) / D.msfuy(i + 1, j)) * R(0.25) *
                    (mk(c1, c2, mut, i + 1, j, k) + mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i + 1, j, k) + mk(c1, c2, mut, i, j, k)) *
-                   R(0.25) * (xk + xk + xk + xk) * rdx;
+                   R(0.25) * (X(i + 1, j, k) + X(i, j, k) + X(i + 1, j, k - 1) + X(i, j, k - 1)) * rdx;
   const R mrdx = D.msftx(i, j) * D.msfty(i, j) * rdx;
   const R mkrdym = (D.msfvy(i, j) * D.msfvx_inv(i, j)) * R(0.25) *
                    (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k) + mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k)) *
-                   R(0.25) * (xk + xk + xk + xk) * rdy;
+                   R(0.25) * (X(i, j, k) + X(i, j - 1, k) + X(i, j, k - 1) + X(i, j - 1, k - 1)) * rdy;
   const R mkrdyp = (D.msfvy(i, j + 1) * D.msfvx_inv(i, j + 1)) * R(0.25) *
                    (mk(c1, c2, mut, i, j + 1, k) + mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j + 1, k) + mk(c1, c2, mut, i, j, k)) *
-                   R(0.25) * (xk + xk + xk + xk) * rdy;
+                   R(0.25) * (X(i, j + 1, k) + X(i, j, k) + X(i, j + 1, k - 1) + X(i, j, k - 1)) * rdy;
   const R mrdy = D.msftx(i, j) * D.msfty(i, j) * rdy;
   return mrdx * (mkrdxp * (f.ld(i + 1, j, k) - f.ld(i, j, k)) - mkrdxm * (f.ld(i, j, k) - f.ld(i - 1, j, k))) +
          mrdy * (mkrdyp * (f.ld(i, j + 1, k) - f.ld(i, j, k)) - mkrdym * (f.ld(i, j, k) - f.ld(i, j - 1, k)));
 }
 // KHorizDiffM1 (with_base = false) / KHorizDiff3DMP (base = t_init or qv_base)
-template <class R>
-__device__ R hdiff_m(const Dom<R>& D, const V3<R>& f, const VB<R>* base, const V3<R>& mut, R xk, int i, int j, int k) {
+template <class R, class XK>
+__device__ R hdiff_m(const Dom<R>& D, const V3<R>& f, const VB<R>* base, const V3<R>& mut, XK X, int i, int j, int k) {
   const double *c1 = D.c1h, *c2 = D.c2h;
   const R rdx = R(D.rdx), rdy = R(D.rdy);
-  const R mkrdxm = (D.msfux(i, j) / D.msfuy(i, j)) * R(0.5) * (xk + xk) * R(0.5) * (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i - 1, j, k)) * rdx;
-  const R mkrdxp = (D.msfux(i + 1, j) / D.msfuy(i + 1, j)) * R(0.5) * (xk + xk) * R(0.5) * (mk(c1, c2, mut, i + 1, j, k) + mk(c1, c2, mut, i, j, k)) * rdx;
+  const R mkrdxm = (D.msfux(i, j) / D.msfuy(i, j)) * R(0.5) * (X(i, j, k) + X(i - 1, j, k)) * R(0.5) * (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i - 1, j, k)) * rdx;
+  const R mkrdxp = (D.msfux(i + 1, j) / D.msfuy(i + 1, j)) * R(0.5) * (X(i + 1, j, k) + X(i, j, k)) * R(0.5) * (mk(c1, c2, mut, i + 1, j, k) + mk(c1, c2, mut, i, j, k)) * rdx;
   const R mrdx = D.msftx(i, j) * D.msfty(i, j) * rdx;
-  const R mkrdym = (D.msfvy(i, j) * D.msfvx_inv(i, j)) * R(0.5) * (xk + xk) * R(0.5) * (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k)) * rdy;
-  const R mkrdyp = (D.msfvy(i, j + 1) * D.msfvx_inv(i, j + 1)) * R(0.5) * (xk + xk) * R(0.5) * (mk(c1, c2, mut, i, j + 1, k) + mk(c1, c2, mut, i, j, k)) * rdy;
+  const R mkrdym = (D.msfvy(i, j) * D.msfvx_inv(i, j)) * R(0.5) * (X(i, j, k) + X(i, j - 1, k)) * R(0.5) * (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k)) * rdy;
+  const R mkrdyp = (D.msfvy(i, j + 1) * D.msfvx_inv(i, j + 1)) * R(0.5) * (X(i, j + 1, k) + X(i, j, k)) * R(0.5) * (mk(c1, c2, mut, i, j + 1, k) + mk(c1, c2, mut, i, j, k)) * rdy;
   const R mrdy = D.msftx(i, j) * D.msfty(i, j) * rdy;
   if (!base)
     return mrdx * (mkrdxp * (f.ld(i + 1, j, k) - f.ld(i, j, k)) - mkrdxm * (f.ld(i, j, k) - f.ld(i - 1, j, k))) +
@@ -1231,7 +1243,10 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
       int is = bx ? 1 : 0, ie = bx ? nx : nx + 1;
       const int js = by ? 1 : 0, je = by ? ny - 1 : ny;
       if (px) { is = 0; ie = nx + 1; }
-      if (i >= is && i < ie && j >= js && j < je) t += hdiff_u(D, D.u2, D.mut, khdif, i, j, k);
+      if (i >= is && i < ie && j >= js && j < je) {
+        if (D.damp_opt == 1) t += hdiff_u(D, D.u2, D.mut, XkField<R>{D.xkmh}, i, j, k);
+        else t += hdiff_u(D, D.u2, D.mut, XkConst<R>{khdif}, i, j, k);
+      }
       int vis = bx ? 1 : 0, vie = bx ? nx : nx + 1;
       if (px) { vis = 0; vie = nx + 1; }
       if (i >= vis && i < vie && k < nz - 1) t += vdiff_uv<R, 1, 0>(D, D.u2, D.u_base, D.muu, kvdif, i, j, k);
@@ -1254,7 +1269,10 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
       int is = bx ? 1 : 0, ie = bx ? nx - 1 : nx;
       const int js = by ? 1 : 0, je = by ? ny : ny + 1;
       if (px) { is = 0; ie = nx; }
-      if (i >= is && i < ie && j >= js && j < je) t += hdiff_v(D, D.v2, D.mut, khdif, i, j, k);
+      if (i >= is && i < ie && j >= js && j < je) {
+        if (D.damp_opt == 1) t += hdiff_v(D, D.v2, D.mut, XkField<R>{D.xkmh}, i, j, k);
+        else t += hdiff_v(D, D.v2, D.mut, XkConst<R>{khdif}, i, j, k);
+      }
       const int vjs = by ? 1 : 0, vje = by ? ny : ny + 1;
       if (j >= vjs && j < vje && k < nz - 1) t += vdiff_uv<R, 0, 1>(D, D.v2, D.v_base, D.muv, kvdif, i, j, k);
     }
@@ -1279,7 +1297,10 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
       int is = bx ? 1 : 0, ie = bx ? nx - 1 : nx;
       const int js = by ? 1 : 0, je = by ? ny - 1 : ny;
       if (px) { is = 0; ie = nx; }
-      if (i >= is && i < ie && j >= js && j < je) tw += hdiff_w(D, D.w2, D.mut, khdif, i, j, k);
+      if (i >= is && i < ie && j >= js && j < je) {
+        if (D.damp_opt == 1) tw += hdiff_w(D, D.w2, D.mut, XkField<R>{D.xkmh}, i, j, k);
+        else tw += hdiff_w(D, D.w2, D.mut, XkConst<R>{khdif}, i, j, k);
+      }
       tw += vdiff_w(D, D.w2, D.mut, kvdif, i, j, k);
     }
     if (d6on && k >= 1 && k < nz && d6_in('m', nx, ny, sp, px, ox, oy, i, j)) {
@@ -1300,7 +1321,10 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
         int is = bx ? 1 : 0, ie = bx ? nx - 1 : nx;
         const int js = by ? 1 : 0, je = by ? ny - 1 : ny;
         if (px) { is = 0; ie = nx; }
-        if (i >= is && i < ie && j >= js && j < je) tt += hdiff_m(D, D.t2, &D.t_init, D.mut, khh, i, j, k);
+        if (i >= is && i < ie && j >= js && j < je) {
+          if (D.damp_opt == 1) tt += hdiff_m(D, D.t2, &D.t_init, D.mut, XkField<R>{D.xkhh}, i, j, k);
+          else tt += hdiff_m(D, D.t2, &D.t_init, D.mut, XkConst<R>{khh}, i, j, k);
+        }
         tt += vdiff_m(D, D.t2, &D.t_init, D.mut, R(3.) * kvdif, i, j, k);
       }
       if (d6on && d6_in('m', nx, ny, sp, px, ox, oy, i, j)) {

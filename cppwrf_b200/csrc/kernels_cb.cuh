@@ -659,6 +659,67 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_finish(const __grid_constant__ 
   if (mass) CB_LOOP(k, nz) p_rho_phi_point(D, i, j, k);
 }
 
+// DiffusionDriver::prepare with damp_opt 1 (diffusion_driver.cpp:114-130): the horizontal eddy viscosities start at
+// khdif and khdif / prandtl (KIsotropicKm, km_kh.hpp:35-45); cal_dampkm (km_kh.hpp:485-567) raises them in the columns
+// inside spec_bdy_width - 1 rows of specified boundaries to dampcoef cos^2(pi/2 min(depth / zdamp, 1)) ds^2 / dt,
+// the depth below the top summed from the diffusion metrics 1 / rdz and 1 / rdzw of ph_2 + phb
+// (compute_diff_metrics, diff_metrics.hpp:11-33), level by level from the top. The vertical viscosities it also
+// raises are not read by constant-K diffusion. One thread per column (warp 0); cos: cw_cos in the FP64 form (the
+// reference's CPU build takes glibc's cos, libmvec's on the lanes of its column loop), CUDA's in the mixed form.
+template <class R>
+__device__ __forceinline__ double damp_cos(double x) {
+  if constexpr (sizeof(R) == 4) return ::cos(x);
+  else return cw_cos(x);
+}
+template <class R, int NM>
+__global__ void __launch_bounds__(CX * CNW) k_dampkm(const __grid_constant__ Pack<R, NM> P) {
+  int i, j;
+  const Dom<R>& D = cb_member(P, RG_COLS_MASS, i, j);
+  if (D.damp_opt != 1 || !D.diff_on) return;  // uniform over the block
+  const int nx = D.nx, ny = D.ny, nz = D.nz;
+  if (threadIdx.y != 0 || i >= nx || j >= ny) return;
+  const R khm = R(D.khdif), khh = R(D.khdif / D.prandtl);
+  int i0 = 0, i1 = nx, j0 = 0, j1 = ny;
+  if (D.lbc) {  // specified boundaries: spec_bdy_width (5) - 1 rows keep the constants
+    const int w = 5;
+    i0 = i0 > w - 1 ? i0 : w - 1;
+    i1 = i1 < nx - w + 1 ? i1 : nx - w + 1;
+    j0 = j0 > w - 1 ? j0 : w - 1;
+    j1 = j1 < ny - w + 1 ? j1 : ny - w + 1;
+  }
+  if (!(i >= i0 && i < i1 && j >= j0 && j < j1)) {
+    for (int k = 0; k < nz; ++k) {
+      D.xkmh(i, j, k) = khm;
+      D.xkhh(i, j, k) = khh;
+    }
+    return;
+  }
+  const double piconst = 3.1415926535897932384626433, degrad = piconst / 180.0, degrad90 = degrad * 90.0;
+  auto zw = [&](int k) { return (double(D.ph2.ld(i, j, k)) + double(D.phb(i, j, k))) / k::g; };
+  const double dx_m = D.dx / double(D.msftx(i, j)), dy_m = D.dy / double(D.msfty(i, j));
+  const double ds = dx_m < dy_m ? dx_m : dy_m;
+  const double kmmax = ds * ds / D.dt;
+  double zkp = zw(nz), zk = zw(nz - 1), deltaz = 0.0;  // zw at levels k + 1 and k
+  for (int k = nz - 1; k >= 0; --k) {
+    const double zkm = k > 0 ? zw(k - 1) : 0.0;
+    const double rdzw = 1.0 / (zkp - zk);
+    if (k == nz - 1) {
+      deltaz = 0.5 * (1.0 / rdzw);
+    } else {
+      const double rdz = k == 0 ? 2.0 / (zkp - zk) : 2.0 / (zkp - zkm);
+      deltaz = deltaz + 1.0 / rdz;
+    }
+    const double ratio = deltaz / D.zdamp;
+    const double tmp = ratio < 1.0 ? ratio : 1.0;
+    const double c = damp_cos<R>(degrad90 * tmp);
+    const R dampk = R(c * c * kmmax * D.dampcoef);
+    D.xkmh(i, j, k) = dampk > khm ? dampk : khm;
+    D.xkhh(i, j, k) = dampk > khh ? dampk : khh;
+    zkp = zk;
+    zk = zkm;
+  }
+}
+
 // set_w_surface (KSetWSurface, rk3.cpp:173-200), fill = false
 template <class R, int NM>
 __global__ void __launch_bounds__(CX * CNW) k_w_surface(const __grid_constant__ Pack<R, NM> P) {

@@ -4,7 +4,8 @@
  * 2-lane _ZGVbN2vv_pow, src/core/backend.hpp:118, :169-175) to cw_pow, the pow of the GPU path, and the
  * scalar and libmvec 2-lane sin of the Rayleigh dampings (damp_opt 3, src/dyn/small_step.cpp:400; damp_opt 2,
  * src/dyn/diffusion/rayleigh_damp.hpp:16-25, :136) to cw_sin, and the scalar and libmvec 2-lane log of
- * calc_p_rho_phi's hypsometric_opt 2 (src/dyn/small_step.cpp:467, src/core/backend.hpp:176-184) to cw_log. The
+ * calc_p_rho_phi's hypsometric_opt 2 (src/dyn/small_step.cpp:467, src/core/backend.hpp:176-184) to cw_log, and the
+ * scalar and libmvec 2-lane cos of cal_dampkm (damp_opt 1, src/dyn/diffusion/km_kh.hpp:24-33) to cw_cos. The
  * reference's every other operation is unchanged, so bit-identity with this build is a fair test of them. */
 #include <emmintrin.h>
 
@@ -33,4 +34,12 @@ __m128d _ZGVbN2v_log(__m128d x) {
   double a[2];
   _mm_storeu_pd(a, x);
   return _mm_set_pd(cw_log(a[1]), cw_log(a[0]));
+}
+
+double cos(double x) { return cw_cos(x); }
+
+__m128d _ZGVbN2v_cos(__m128d x) {
+  double a[2];
+  _mm_storeu_pd(a, x);
+  return _mm_set_pd(cw_cos(a[1]), cw_cos(a[0]));
 }

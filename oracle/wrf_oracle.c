@@ -11,8 +11,8 @@
  * coefficients, moist species (calc_cq, positive-definite scalar advection at rk 3), passive
  * tracers, constant-K diffusion (diff_opt 1, km_opt 1), specified lateral boundaries (width 5),
  * top_lid, w_damping, h/v_adv_order 5/6, 3/4, damp_opt 2 and 3 (sin by the pow mode: glibc's or cw_sin), the
- * sixth-order filter, hypsometric_opt 1 and 2 (log by the pow mode), Kessler microphysics. Not restated (rejected
- * by or_create): map factors other than 1, Coriolis, damp_opt 1.
+ * sixth-order filter, hypsometric_opt 1 and 2 (log by the pow mode), damp_opt 1 (cos by the pow mode), Kessler
+ * microphysics. Not restated (rejected by or_create): map factors other than 1, Coriolis.
  */
 #include "wrf_oracle.h"
 
@@ -29,6 +29,7 @@
 extern __m128d _ZGVbN2vv_pow(__m128d, __m128d);
 extern __m128d _ZGVbN2v_exp(__m128d);
 extern __m128d _ZGVbN2v_log(__m128d);
+extern __m128d _ZGVbN2v_cos(__m128d);
 
 /* ------------------------------------------------------------------ constants
  * src/core/constants.hpp:4-18 (WRF module_model_constants) */
@@ -1328,6 +1329,70 @@ static void rayleigh_damp(or_dom* d) {
     }
 }
 
+/* cal_dampkm (km_kh.hpp:485-567, damp_opt 1): near the model top the eddy viscosities rise to
+ * dampcoef cos^2(pi/2 min(depth / zdamp, 1)) times ds^2 / dt (horizontal) and dz^2 / dt (vertical), depth below the
+ * top accumulated from the diffusion metrics' rdzw / rdz (compute_diff_metrics, diff_metrics.hpp:11-33) of
+ * ph_2 + phb; the columns exclude spec_bdy_width - 1 rows of specified boundaries. cos by the pow mode: glibc's
+ * (libmvec's 2-lane cos on the lanes of the column loop, vm::lane) or cw_cos. */
+#define DK_LEVELS 128
+static double damp_cos(const or_dom* d, double x, int lane_i, int ni) {
+  if (d->pow_mode != OR_POW_GLIBC) return cw_cos(x);
+  if (ni > 1 && !((ni & 1) && lane_i == ni - 1)) return _mm_cvtsd_f64(_ZGVbN2v_cos(_mm_set1_pd(x)));
+  return cos(x);
+}
+static void cal_dampkm(or_dom* d) {
+  const cw_grid* g = &d->g;
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  int i0 = 0, i1 = nx, j0 = 0, j1 = ny;
+  if (specified(g)) {
+    const int w = 5; /* spec_bdy_width */
+    i0 = i0 > w - 1 ? i0 : w - 1;
+    i1 = i1 < nx - w + 1 ? i1 : nx - w + 1;
+    j0 = j0 > w - 1 ? j0 : w - 1;
+    j1 = j1 < ny - w + 1 ? j1 : ny - w + 1;
+  }
+  const int ni = i1 - i0;
+  const double piconst = 3.1415926535897932384626433, degrad = piconst / 180.0, degrad90 = degrad * 90.0;
+  const double dx = g->dx, dy = g->dy, dt = g->dt, dampcoef = d->o.dampcoef, zdamp = d->o.zdamp;
+  fld *ph = F_(CW_PH_2), *phb = F_(CW_PHB), *msftx = F_(CW_MSFTX), *msfty = F_(CW_MSFTY);
+  double zw[DK_LEVELS + 1], rdz[DK_LEVELS], rdzw[DK_LEVELS], dampk[DK_LEVELS], dampkv[DK_LEVELS];
+  for (int j = j0; j < j1; ++j)
+    for (int i = i0; i < i1; ++i) {
+      const int lane_i = i - i0;
+      for (int k = 0; k <= nz; ++k) zw[k] = (AT(ph, i, j, k) + AT(phb, i, j, k)) / G_;
+      for (int k = 0; k < nz; ++k) rdzw[k] = 1.0 / (zw[k + 1] - zw[k]);
+      rdz[0] = 2.0 / (zw[1] - zw[0]);
+      for (int k = 1; k < nz; ++k) rdz[k] = 2.0 / (zw[k + 1] - zw[k - 1]);
+      double deltaz = 0.0;
+      for (int k = nz - 1; k >= 0; --k) {
+        const double dx_m = dx / AT(msftx, i, j, 0), dy_m = dy / AT(msfty, i, j, 0);
+        const double ds = dx_m < dy_m ? dx_m : dy_m;
+        const double kmmax = ds * ds / dt;
+        double dz;
+        if (k == nz - 1) {
+          dz = 1.0 / rdzw[k];
+          deltaz = 0.5 * dz;
+        } else {
+          dz = 1.0 / rdz[k];
+          deltaz = deltaz + dz;
+          dz = 1.0 / rdzw[k];
+        }
+        const double kmmvmax = dz * dz / dt;
+        const double ratio = deltaz / zdamp;
+        const double tmp = ratio < 1.0 ? ratio : 1.0;
+        const double c = damp_cos(d, degrad90 * tmp, lane_i, ni);
+        dampk[k] = c * c * kmmax * dampcoef;
+        dampkv[k] = c * c * kmmvmax * dampcoef;
+        if (dampk[k] < dampkv[k]) dampkv[k] = dampk[k];
+      }
+      for (int k = 0; k < nz; ++k) {
+        if (dampk[k] > AT(&d->xkmh, i, j, k)) AT(&d->xkmh, i, j, k) = dampk[k];
+        if (dampk[k] > AT(&d->xkhh, i, j, k)) AT(&d->xkhh, i, j, k) = dampk[k];
+        if (dampkv[k] > AT(&d->xkmv, i, j, k)) AT(&d->xkmv, i, j, k) = dampkv[k];
+        if (dampkv[k] > AT(&d->xkhv, i, j, k)) AT(&d->xkhv, i, j, k) = dampkv[k];
+      }
+    }
+}
 static void diffusion_prepare(or_dom* d) {
   const cw_grid* g = &d->g;
   const double pr = prandtl(d);
@@ -1339,6 +1404,7 @@ static void diffusion_prepare(or_dom* d) {
         AT(&d->xkhh, i, j, k) = d->o.khdif / pr;
         AT(&d->xkhv, i, j, k) = d->o.kvdif / pr;
       }
+  if (d->o.damp_opt == 1) cal_dampkm(d);
   fill_halo(d, &d->xkmh);
   fill_halo(d, &d->xkmv);
   fill_halo(d, &d->xkhh);
@@ -2656,7 +2722,7 @@ or_dom* or_create(const cw_grid* g, const cw_options* o) {
   or_dom* d = (or_dom*)calloc(1, sizeof(or_dom));
   d->g = *g;
   d->o = *o;
-  if ((o->damp_opt != 0 && o->damp_opt != 2 && o->damp_opt != 3) || (o->hypsometric_opt != 1 && o->hypsometric_opt != 2) ||
+  if ((o->damp_opt < 0 || o->damp_opt > 3) || (o->hypsometric_opt != 1 && o->hypsometric_opt != 2) ||
       o->diff_6th_opt < 0 || o->diff_6th_opt > 2 ||
       (o->mp_physics != 0 && (o->mp_physics != 1 || o->n_moist < 3 || g->nz > KS_LEVELS)) ||
       (o->diff_opt != 0 && (o->diff_opt != 1 || o->km_opt != 1))) {

@@ -186,3 +186,31 @@ def test_oracle_equals_reference_open_sixth_order_2d():
     ref = _refdump.run(case, 3, own_pow=False)
     bad = compare(orc, ref, case)
     assert not bad, "\n".join(bad)
+
+
+@pytest.mark.parametrize("own", [True, False], ids=["cw_cos", "glibc"])
+def test_oracle_equals_reference_eddy_viscosity_damping(own):
+    """damp_opt 1 (cal_dampkm): the horizontal eddy viscosities of constant-K diffusion raised toward ds^2/dt in the
+    upper 8 km of the columns inside the boundary zone (libmvec's cos on the lanes of the reference's column loop
+    in the glibc build)."""
+    case = lam_case(seed=19, diff=True)
+    case.o.damp_opt, case.o.zdamp, case.o.dampcoef = 1, 8000.0, 0.2
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_OWN if own else _oracle.POW_GLIBC)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=own)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)
+    plain = lam_case(seed=19, diff=True)
+    undamped = _oracle.Oracle(plain, pow_mode=_oracle.POW_OWN if own else _oracle.POW_GLIBC)
+    undamped.step(3)
+    assert not np.array_equal(orc.array("U_2"), undamped.array("U_2"))  # the damping acted
+
+
+def test_oracle_equals_reference_eddy_viscosity_damping_2d():
+    cfg = dict(cases.SMALL["straka_small"])
+    case = cases.ideal_case(cfg, damp_opt=1, zdamp=1500.0, dampcoef=0.2)
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_GLIBC)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=False)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)

@@ -162,6 +162,23 @@ def test_2d_open_x_sixth_order_bit_exact():
     assert not bad, "\n".join(bad)
 
 
+def test_lam_eddy_viscosity_damping_bit_exact():
+    """damp_opt 1: cal_dampkm's horizontal eddy viscosities near the top (cos = cw_cos on both sides) in the
+    constant-K diffusion of the first stage, dynamics and scalars."""
+    case = lam_case(seed=19, diff=True)
+    case.o.damp_opt, case.o.zdamp, case.o.dampcoef = 1, 8000.0, 0.2
+    dom, orc = run_pair(case, 4)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
+def test_2d_eddy_viscosity_damping_bit_exact():
+    case = cases.ideal_case(dict(cases.SMALL["straka_small"]), damp_opt=1, zdamp=1500.0, dampcoef=0.2)
+    dom, orc = run_pair(case, 3)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
 def test_cfl_maxima_equal_oracle():
     """LargeStep::cfl_max of every RK stage (the adaptive time step's input): the device maxima equal the oracle's,
     and recording them changes no field."""

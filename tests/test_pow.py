@@ -1,5 +1,5 @@
 # SPDX-License-Identifier: GPL-3.0-or-later
-"""Accuracy of the dycore's own pow, exp, log and sin (cw_pow.h): against glibc's and against 60-digit decimal evaluations."""
+"""Accuracy of the dycore's own pow, exp, log, sin and cos (cw_pow.h): against glibc's and against 60-digit decimal evaluations."""
 import ctypes as C
 import math
 import os
@@ -17,6 +17,7 @@ double cwp(double x, double y) { return cw_pow(x, y); }
 double cwe(double x) { return cw_exp(x); }
 double cws(double x) { return cw_sin(x); }
 double cwl(double x) { return cw_log(x); }
+double cwc(double x) { return cw_cos(x); }
 """
 
 
@@ -29,7 +30,7 @@ def _lib(tmp_path):
     lib = C.CDLL(str(so))
     lib.cwp.restype = C.c_double
     lib.cwp.argtypes = [C.c_double, C.c_double]
-    for f in (lib.cwe, lib.cws, lib.cwl):
+    for f in (lib.cwe, lib.cws, lib.cwl, lib.cwc):
         f.restype = C.c_double
         f.argtypes = [C.c_double]
     return lib
@@ -138,4 +139,38 @@ def test_log_agrees_with_glibc_to_one_ulp(tmp_path):
     lib = _lib(tmp_path)
     for x in np.random.default_rng(7).uniform(1.0, 1.5, 5000):
         a, b = lib.cwl(float(x)), math.log(float(x))
+        assert abs(a - b) <= math.ulp(b), (x, a, b)
+
+
+def _dec_cos(x):
+    getcontext().prec = 60
+    x = Decimal(x)
+    s, term, n = Decimal(0), Decimal(1), 0
+    while term != 0 and (s == 0 or abs(term) > abs(s) * Decimal(10) ** -58):
+        s += term
+        term = -term * x * x / ((n + 1) * (n + 2))
+        n += 2
+    return s
+
+
+def test_cos_within_half_ulp_plus(tmp_path):
+    """cw_cos on damp_opt 1's range [0, pi/2] (and to |x| <= 2), near pi/2 too: within 0.5001 ulp of the exact value."""
+    lib = _lib(tmp_path)
+    rng = np.random.default_rng(8)
+    xs = list(rng.uniform(0.0, 2.0, 400)) + list(math.pi / 2 - rng.uniform(0.0, 1e-3, 100)) + \
+        [0.0, 1e-8, math.pi / 4, math.nextafter(math.pi / 4, 1.0), math.pi / 2, math.nextafter(math.pi / 2, 2.0)]
+    worst = Decimal(0)
+    for x in xs:
+        got = lib.cwc(float(x))
+        exact = _dec_cos(float(x))
+        worst = max(worst, abs(Decimal(got) - exact) / Decimal(math.ulp(float(exact))))
+    assert worst < Decimal("0.5001"), worst
+    assert lib.cwc(-1.0) == lib.cwc(1.0) and lib.cwc(0.0) == 1.0
+    assert math.isnan(lib.cwc(2.5)) and math.isnan(lib.cwc(math.nan))
+
+
+def test_cos_agrees_with_glibc_to_one_ulp(tmp_path):
+    lib = _lib(tmp_path)
+    for x in np.random.default_rng(9).uniform(0.0, math.pi / 2, 5000):
+        a, b = lib.cwc(float(x)), math.cos(float(x))
         assert abs(a - b) <= math.ulp(b), (x, a, b)
