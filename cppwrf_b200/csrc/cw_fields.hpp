@@ -124,7 +124,8 @@ inline const char* unsupported(const cw_grid& g, const cw_options& o) {
   if (o.damp_opt != 0 && !(o.zdamp > 0)) return "damp_opt 1, 2 and 3 need zdamp > 0";
   if (o.damp_opt == 2 && g.nz > 127) return "damp_opt 2: nz <= 127";
   if (o.hypsometric_opt != 1 && o.hypsometric_opt != 2) return "hypsometric_opt must be 1 or 2";
-  if (o.diff_opt != 0 && !(o.diff_opt == 1 && o.km_opt == 1)) return "diffusion: diff_opt 0, or 1 with km_opt 1";
+  if (o.diff_opt != 0 && !(o.diff_opt == 1 && (o.km_opt == 1 || o.km_opt == 4)))
+    return "diffusion: diff_opt 0, or 1 with km_opt 1 or 4";
   if (o.h_adv_order != 5 && o.h_adv_order != 6) return "h_adv_order must be 5 or 6";
   if (o.v_adv_order != 3 && o.v_adv_order != 4) return "v_adv_order must be 3 or 4";
   if (o.n_moist < 0 || o.n_scalars < o.n_moist || o.n_scalars > 64) return "scalars: 0 <= n_moist <= n_scalars <= 64";

@@ -38,8 +38,9 @@ inline size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 // the work fields of one domain beyond State / Tendencies / BaseState (SmallStep's fields)
 enum Work { W_U_SAVE, W_V_SAVE, W_W_SAVE, W_T_SAVE, W_PH_SAVE, W_WW1, W_C2A, W_PM1, W_T_2SAVE, W_A, W_ALPHA, W_GAMMA,
             W_MU_SAVE, W_MUDF, W_MUAVE, W_W_RHS, W_T2A, W_XKMH, W_XKHH, W_N };
-// W_XKMH, W_XKHH (damp_opt 1 only; no storage otherwise)
-inline bool work_used(int w, const cw_options& o) { return (w != W_XKMH && w != W_XKHH) || o.damp_opt == 1; }
+// W_XKMH, W_XKHH: per-point horizontal eddy viscosities (damp_opt 1 or km_opt 4 only; no storage otherwise)
+inline bool xk_fields(const cw_options& o) { return o.damp_opt == 1 || o.km_opt == 4; }
+inline bool work_used(int w, const cw_options& o) { return (w != W_XKMH && w != W_XKHH) || xk_fields(o); }
 inline FieldKind work_kind(int w) {
   switch (w) {
     case W_U_SAVE: return {'U', 3, false};

@@ -210,7 +210,8 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.ph_save = w3(W_PH_SAVE); D.ww1 = w3(W_WW1); D.c2a = w3(W_C2A); D.pm1 = w3(W_PM1); D.t_2save = w3(W_T_2SAVE);
   D.a = w3(W_A); D.alpha = w3(W_ALPHA); D.gamma = w3(W_GAMMA); D.mu_save = w3(W_MU_SAVE); D.mudf = w3(W_MUDF);
   D.muave = w3(W_MUAVE); D.w_rhs = w3(W_W_RHS); D.t2a = w3(W_T2A);
-  if (o.damp_opt == 1) { D.xkmh = w3(W_XKMH); D.xkhh = w3(W_XKHH); }
+  if (xk_fields(o)) { D.xkmh = w3(W_XKMH); D.xkhh = w3(W_XKHH); }
+  D.km_opt = o.km_opt; D.xk_field = xk_fields(o) && o.diff_opt == 1;
   const int ns = o.n_scalars;
   D.q1 = qtab_d; D.q2 = qtab_d + ns; D.qn = qtab_d + 2 * ns; D.qtf = qtab_d + 3 * ns; D.qscale = qtab_d + 4 * ns;
   D.qpd = qtab_d + 5 * ns;
@@ -382,7 +383,7 @@ void build_halosets_t(cw_handle* h, DevTables<R>& T) {
     };
     const bool spec = specified(M.g);
     add(cw_handle::H_MU1, {F(CW_MU_1)});
-    if (M.o.damp_opt == 1) add(cw_handle::H_XK, {W(W_XKMH), W(W_XKHH)});  // DiffusionDriver::prepare's fill
+    if (xk_fields(M.o)) add(cw_handle::H_XK, {W(W_XKMH), W(W_XKHH)});  // DiffusionDriver::prepare's fill
     add(cw_handle::H_PREP0, {F(CW_U_2), F(CW_V_2), F(CW_W_2), F(CW_T_2), F(CW_PH_2), F(CW_P), F(CW_AL)});
     if (!spec) add(cw_handle::H_PREP0, {F(CW_MU_2)});
     add(cw_handle::H_PREP1, {F(CW_MUT), F(CW_RU), F(CW_RV), F(CW_RW), F(CW_ALT), F(CW_PHP), F(CW_MUU, HP_ODDFACE_X),

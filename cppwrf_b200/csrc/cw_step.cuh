@@ -152,7 +152,8 @@ struct Launcher {
 template <class R, int NM>
 void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
   const Member& M0 = h->m[0];
-  bool lbc = false, terrain = false, scalars = false, any_pd = false, mp = false, open = false, dampkm = false;
+  bool lbc = false, terrain = false, scalars = false, any_pd = false, mp = false, open = false, dampkm = false,
+       smag = false;
   // every member specified on all four sides: the acoustic substeps read no halo cell of the fields the
   // per-substep fills (H_SS0, H_UV, H_AC) would refresh (the faces next to the boundary are the spec
   // zone's, updated from the boundary data), and the fills after the substeps (H_POST, H_FIN) refresh them
@@ -166,6 +167,7 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
     lbc |= M.o.lbc != 0;
     open |= M.g.bc_x == CW_BC_OPEN || M.g.bc_y == CW_BC_OPEN;
     dampkm |= M.o.damp_opt == 1 && M.o.diff_opt == 1;
+    smag |= M.o.km_opt == 4 && M.o.diff_opt == 1;
     mp |= M.o.mp_physics != 0;
     terrain |= !M.o.flat;
     scalars |= M.o.n_scalars > 0;
@@ -184,8 +186,9 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
     L.halo(cw_handle::H_PREP0);
     L.run_cb("k_ls_prep", RG_COLS_STAG, 1, k_ls_prep<R, NM>, d);
     L.halo(cw_handle::H_PREP1);
-    if (rk == 1 && dampkm) {  // DiffusionDriver::prepare: the eddy viscosities of damp_opt 1, then their halos
-      L.run_cb("k_dampkm", RG_COLS_MASS, 0, k_dampkm<R, NM>, d);
+    if (rk == 1 && (dampkm || smag)) {  // DiffusionDriver::prepare: km_opt 4's and damp_opt 1's eddy viscosities
+      if (smag) L.run_t("k_smag", RG_MASS, 1, KV(k_smag), d);
+      if (dampkm) L.run_cb("k_dampkm", RG_COLS_MASS, 0, k_dampkm<R, NM>, d);
       L.halo(cw_handle::H_XK);
     }
     if (rk == 1) L.run_t("k_tendf_rk1", RG_STAG, 1, KV(k_tendf_rk1), d);

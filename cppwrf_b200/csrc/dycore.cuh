@@ -81,7 +81,9 @@ struct Dom {
   // acoustic-step work fields (SmallStep, src/dyn/small_step.hpp:45-49)
   V3<T> u_save, v_save, w_save, t_save, ph_save, ww1, c2a, pm1, t_2save, a, alpha, gamma, mu_save, mudf, muave,
       w_rhs, t2a;
-  V3<T> xkmh, xkhh;  // damp_opt 1: the horizontal eddy viscosities of momentum and heat per mass point (level 0..nz-1)
+  V3<T> xkmh, xkhh;  // damp_opt 1 / km_opt 4: the horizontal eddy viscosities of momentum and heat per mass point
+  int km_opt;        // 1: constant K; 4: 2-D Smagorinsky (horizontal)
+  int xk_field;      // the horizontal diffusion reads xkmh / xkhh (else the constants)
   // scalars: device tables of views (q2 and q_new swap roles after each update)
   V3<T>* q1;
   V3<T>* q2;

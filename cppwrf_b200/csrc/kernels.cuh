@@ -1220,6 +1220,150 @@ __device__ bool ray_w(const Dom<R>& D, int i, int j, int k, R& term) {
   return true;
 }
 
+// ------------------------------------------------------------------ km_opt 4 (diff_opt 1)
+// DiffusionDriver::prepare with km_opt 4: the 2-D Smagorinsky eddy viscosities (KSmag2dKm, km_kh.hpp:47-97) from the
+// deformation defor11, defor22 (KDeformDiagAndDiv, deform_div.hpp:20-84) and defor12 (KDeform12 :86-156, with the
+// edge copies of cal_deform_and_div :271-318) with their terrain terms from compute_diff_metrics' rdzw, zx, zy
+// (diff_metrics.hpp:11-133, with set_physical_bc3d). Every one of them depends only on its neighbours' u, v, ph:
+// they are evaluated where they are needed, in the reference's expressions, one thread per mass point.
+template <class R>
+__device__ __forceinline__ R dm_zw(const Dom<R>& D, int i, int j, int k) {
+  return (D.ph2.ld(i, j, k) + D.phb(i, j, k)) / R(k::g);
+}
+template <class R>
+__device__ __forceinline__ R dm_rdzw(const Dom<R>& D, int i, int j, int k) {
+  return R(1.0) / (dm_zw(D, i, j, k + 1) - dm_zw(D, i, j, k));
+}
+// zx at U points i = 0..nx (KDiffMetricsZX; the boundary faces of specified / open sides copy the last column)
+template <class R>
+__device__ R dm_zx(const Dom<R>& D, int i, int j, int k) {
+  const int nx = D.nx;
+  const bool px = D.bc_x == CW_BC_PERIODIC, copy = D.lbc || D.open_x;
+  if (px && k == D.nz && (i == 0 || i == nx)) return R(0);
+  if (!px && (i == 0 || (i == nx && !copy))) return R(0);
+  int i0 = i, im1 = i - 1;
+  if (!px && i == nx) {
+    i0 = nx - 1;
+    im1 = nx - 2;
+  } else {
+    if (i == nx) i0 = 0;
+    if (i == 0) im1 = nx - 1;
+  }
+  R v = R(D.rdx) * (D.phb(i0, j, k) - D.phb(im1, j, k)) / R(k::g);
+  v += R(D.rdx) * (D.ph2.ld(i0, j, k) - D.ph2.ld(im1, j, k)) / R(k::g);
+  return v;
+}
+// zy at V points j = 0..ny (KDiffMetricsZY)
+template <class R>
+__device__ R dm_zy(const Dom<R>& D, int i, int j, int k) {
+  const int ny = D.ny;
+  const bool py = D.bc_y == CW_BC_PERIODIC, copy = D.lbc || D.open_y;
+  if (py && k == D.nz && (j == 0 || j == ny)) return R(0);
+  if (!py && (j == 0 || (j == ny && !copy))) return R(0);
+  int j0 = j, jm1 = j - 1;
+  if (!py && j == ny) {
+    j0 = ny - 1;
+    jm1 = ny - 2;
+  } else {
+    if (j == ny) j0 = 0;
+    if (j == 0) jm1 = ny - 1;
+  }
+  R v = R(D.rdy) * (D.phb(i, j0, k) - D.phb(i, jm1, k)) / R(k::g);
+  v += R(D.rdy) * (D.ph2.ld(i, j0, k) - D.ph2.ld(i, jm1, k)) / R(k::g);
+  return v;
+}
+// the average of two columns a(0, .), a(1, .) at w level k (the hatavg arrays of cal_deform_and_div)
+template <class R, class A>
+__device__ __forceinline__ R dm_hatavg(const Dom<R>& D, const A& a, int k) {
+  const int nz = D.nz;
+  if (k == 0)
+    return R(0.5) * (R(D.cf1) * a(0, 0) + R(D.cf2) * a(0, 1) + R(D.cf3) * a(0, 2) + R(D.cf1) * a(1, 0) +
+                     R(D.cf2) * a(1, 1) + R(D.cf3) * a(1, 2));
+  if (k == nz) {
+    const R cft2 = -R(0.5) * R(D.dnw[nz - 1]) / R(D.dn[nz - 1]), cft1 = R(1.0) - cft2;
+    return R(0.5) * (cft1 * (a(0, nz - 1) + a(1, nz - 1)) + cft2 * (a(0, nz - 2) + a(1, nz - 2)));
+  }
+  return R(0.5) * (R(D.fnm[k]) * (a(0, k) + a(1, k)) + R(D.fnp[k]) * (a(0, k - 1) + a(1, k - 1)));
+}
+// defor12 at vorticity point (ci, cj), level k, after the edge copies: the point computed there
+template <class R>
+__device__ R dm_defor12(const Dom<R>& D, int ci, int cj, int k) {
+  const int nx = D.nx, ny = D.ny;
+  const bool px = D.bc_x == CW_BC_PERIODIC, py = D.bc_y == CW_BC_PERIODIC;
+  const bool bx = !px && (D.lbc || D.open_x), by = !py && (D.lbc || D.open_y);
+  int i = ci, j = cj;
+  if (px) {
+    if (i == nx) i = 0;
+  } else if (bx) {
+    if (i == 0) i = 1;
+    if (i == nx) i = nx - 1;
+  }
+  if (py) {
+    if (j == ny) j = 0;
+  } else if (by) {
+    if (j == 0) j = 1;
+    if (j == ny) j = ny - 1;
+  }
+  const int im1 = i == 0 ? (px ? nx - 1 : 0) : i - 1, i0 = i == nx ? (px ? 0 : nx - 1) : i;
+  const int jm1 = j == 0 ? (py ? ny - 1 : 0) : j - 1, j0 = j == ny ? (py ? 0 : ny - 1) : j;
+  const R mm = R(0.25) * (D.msfux(i, jm1) + D.msfux(i, j0)) * (D.msfvy(im1, j) + D.msfvy(i0, j));
+  auto hu = [&](int c, int kk) { const int m = c ? j0 : jm1; return D.u2.ld(i, m, kk) / D.msfux(i, m); };
+  auto hv = [&](int c, int kk) { const int m = c ? i0 : im1; return D.v2.ld(m, j, kk) / D.msfvy(m, j); };
+  const R tmpzy = R(0.25) * (dm_zy(D, im1, j, k) + dm_zy(D, i0, j, k) + dm_zy(D, im1, j, k + 1) + dm_zy(D, i0, j, k + 1));
+  const R r00 = dm_rdzw(D, i0, j0, k), r10 = dm_rdzw(D, im1, j0, k), r11 = dm_rdzw(D, im1, jm1, k),
+          r01 = dm_rdzw(D, i0, jm1, k);
+  const R tmp1_u = (dm_hatavg(D, hu, k + 1) - dm_hatavg(D, hu, k)) * R(0.25) * tmpzy * (r00 + r10 + r11 + r01);
+  const R term_u = mm * (R(D.rdy) * (hu(1, k) - hu(0, k)) - tmp1_u);
+  const R tmpzx = R(0.25) * (dm_zx(D, i, jm1, k) + dm_zx(D, i, j0, k) + dm_zx(D, i, jm1, k + 1) + dm_zx(D, i, j0, k + 1));
+  const R tmp1_v = (dm_hatavg(D, hv, k + 1) - dm_hatavg(D, hv, k)) * R(0.25) * tmpzx * (r00 + r01 + r11 + r10);
+  const R term_v = mm * (R(D.rdx) * (hv(1, k) - hv(0, k)) - tmp1_v);
+  return term_u + term_v;
+}
+// calculate_km_kh with km_opt 4 (km_kh.hpp:585-625): KSmag2dKm one row inside open and specified sides, 0 elsewhere
+// (the reference zeroes the outermost rows of specified boundaries and never writes those of open ones)
+template <class R, int NM, int SH>
+__global__ void __launch_bounds__(PX) k_smag(const __grid_constant__ Pack<R, NM> P) {
+  const Dom<R>* Dp;
+  int i, j, k;
+  if (!thread_index<SH>(P, RG_MASS, Dp, i, j, k)) return;
+  const Dom<R>& D = *Dp;
+  if (D.km_opt != 4 || !D.diff_on) return;
+  const int nx = D.nx, ny = D.ny;
+  const bool bx = D.lbc || D.open_x, by = D.lbc || D.open_y;
+  int is = bx ? 1 : 0, ie = bx ? nx - 1 : nx;
+  const int js = by ? 1 : 0, je = by ? ny - 1 : ny;
+  if (D.bc_x == CW_BC_PERIODIC) {
+    is = 0;
+    ie = nx;
+  }
+  if (!(i >= is && i < ie && j >= js && j < je)) {
+    D.xkmh(i, j, k) = R(0);
+    D.xkhh(i, j, k) = R(0);
+    return;
+  }
+  const R mm = D.msftx(i, j) * D.msfty(i, j);
+  auto au = [&](int c, int kk) { return D.u2.ld(i + c, j, kk) / D.msfuy(i + c, j); };
+  auto av = [&](int c, int kk) { return D.v2.ld(i, j + c, kk) / D.msfvx(i, j + c); };
+  const R rdzw = dm_rdzw(D, i, j, k);
+  const R tmpzx = R(0.25) * (dm_zx(D, i, j, k) + dm_zx(D, i + 1, j, k) + dm_zx(D, i, j, k + 1) + dm_zx(D, i + 1, j, k + 1));
+  const R tmp1_u = (dm_hatavg(D, au, k + 1) - dm_hatavg(D, au, k)) * tmpzx * rdzw;
+  const R d11 = R(2.0) * (mm * (R(D.rdx) * (au(1, k) - au(0, k)) - tmp1_u));
+  const R tmpzy = R(0.25) * (dm_zy(D, i, j, k) + dm_zy(D, i, j + 1, k) + dm_zy(D, i, j, k + 1) + dm_zy(D, i, j + 1, k + 1));
+  const R tmp1_v = (dm_hatavg(D, av, k + 1) - dm_hatavg(D, av, k)) * tmpzy * rdzw;
+  const R d22 = R(2.0) * (mm * (R(D.rdy) * (av(1, k) - av(0, k)) - tmp1_v));
+  const R dd = d11 - d22;
+  R def2 = R(0.25) * (dd * dd);
+  const R d12 = R(0.25) * (dm_defor12(D, i, j, k) + dm_defor12(D, i, j + 1, k) + dm_defor12(D, i + 1, j, k) +
+                           dm_defor12(D, i + 1, j + 1, k));
+  def2 += d12 * d12;
+  const R mlen_h = sqrt(R(D.dx) / D.msftx(i, j) * R(D.dy) / D.msfty(i, j));
+  const R tmp = sqrt(def2);
+  R kmh = R(0.25) * R(0.25) * mlen_h * mlen_h * tmp;
+  kmh = kmh < R(10.0) * mlen_h ? kmh : R(10.0) * mlen_h;
+  D.xkmh(i, j, k) = kmh;
+  D.xkhh(i, j, k) = kmh / R(D.prandtl);
+}
+
 template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R, NM> P) {
   const Dom<R>* Dp;
@@ -1244,7 +1388,7 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
       const int js = by ? 1 : 0, je = by ? ny - 1 : ny;
       if (px) { is = 0; ie = nx + 1; }
       if (i >= is && i < ie && j >= js && j < je) {
-        if (D.damp_opt == 1) t += hdiff_u(D, D.u2, D.mut, XkField<R>{D.xkmh}, i, j, k);
+        if (D.xk_field) t += hdiff_u(D, D.u2, D.mut, XkField<R>{D.xkmh}, i, j, k);
         else t += hdiff_u(D, D.u2, D.mut, XkConst<R>{khdif}, i, j, k);
       }
       int vis = bx ? 1 : 0, vie = bx ? nx : nx + 1;
@@ -1270,7 +1414,7 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
       const int js = by ? 1 : 0, je = by ? ny : ny + 1;
       if (px) { is = 0; ie = nx; }
       if (i >= is && i < ie && j >= js && j < je) {
-        if (D.damp_opt == 1) t += hdiff_v(D, D.v2, D.mut, XkField<R>{D.xkmh}, i, j, k);
+        if (D.xk_field) t += hdiff_v(D, D.v2, D.mut, XkField<R>{D.xkmh}, i, j, k);
         else t += hdiff_v(D, D.v2, D.mut, XkConst<R>{khdif}, i, j, k);
       }
       const int vjs = by ? 1 : 0, vje = by ? ny : ny + 1;
@@ -1298,7 +1442,7 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
       const int js = by ? 1 : 0, je = by ? ny - 1 : ny;
       if (px) { is = 0; ie = nx; }
       if (i >= is && i < ie && j >= js && j < je) {
-        if (D.damp_opt == 1) tw += hdiff_w(D, D.w2, D.mut, XkField<R>{D.xkmh}, i, j, k);
+        if (D.xk_field) tw += hdiff_w(D, D.w2, D.mut, XkField<R>{D.xkmh}, i, j, k);
         else tw += hdiff_w(D, D.w2, D.mut, XkConst<R>{khdif}, i, j, k);
       }
       tw += vdiff_w(D, D.w2, D.mut, kvdif, i, j, k);
@@ -1322,7 +1466,7 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
         const int js = by ? 1 : 0, je = by ? ny - 1 : ny;
         if (px) { is = 0; ie = nx; }
         if (i >= is && i < ie && j >= js && j < je) {
-          if (D.damp_opt == 1) tt += hdiff_m(D, D.t2, &D.t_init, D.mut, XkField<R>{D.xkhh}, i, j, k);
+          if (D.xk_field) tt += hdiff_m(D, D.t2, &D.t_init, D.mut, XkField<R>{D.xkhh}, i, j, k);
           else tt += hdiff_m(D, D.t2, &D.t_init, D.mut, XkConst<R>{khh}, i, j, k);
         }
         tt += vdiff_m(D, D.t2, &D.t_init, D.mut, R(3.) * kvdif, i, j, k);

@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(PX) k_q_tendf_rk1(const __grid_constant__ Pack
   R t = 0;
   if (D.diff_on) {
     if (i >= is && i < ie && j >= js && j < je) {
-      if (D.damp_opt == 1) t += hdiff_m(D, D.q2[n], (const VB<R>*)nullptr, D.muts, XkField<R>{D.xkhh}, i, j, k);
+      if (D.xk_field) t += hdiff_m(D, D.q2[n], (const VB<R>*)nullptr, D.muts, XkField<R>{D.xkhh}, i, j, k);
       else t += hdiff_m(D, D.q2[n], (const VB<R>*)nullptr, D.muts, XkConst<R>{khh}, i, j, k);
     }
     const bool qv = n == 0 && D.n_moist > 0;

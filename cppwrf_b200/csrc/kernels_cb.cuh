@@ -687,11 +687,13 @@ __global__ void __launch_bounds__(CX * CNW) k_dampkm(const __grid_constant__ Pac
     j0 = j0 > w - 1 ? j0 : w - 1;
     j1 = j1 < ny - w + 1 ? j1 : ny - w + 1;
   }
+  const bool km4 = D.km_opt == 4;  // raise k_smag's viscosities instead of the constants
   if (!(i >= i0 && i < i1 && j >= j0 && j < j1)) {
-    for (int k = 0; k < nz; ++k) {
-      D.xkmh(i, j, k) = khm;
-      D.xkhh(i, j, k) = khh;
-    }
+    if (!km4)
+      for (int k = 0; k < nz; ++k) {
+        D.xkmh(i, j, k) = khm;
+        D.xkhh(i, j, k) = khh;
+      }
     return;
   }
   const double piconst = 3.1415926535897932384626433, degrad = piconst / 180.0, degrad90 = degrad * 90.0;
@@ -713,8 +715,9 @@ __global__ void __launch_bounds__(CX * CNW) k_dampkm(const __grid_constant__ Pac
     const double tmp = ratio < 1.0 ? ratio : 1.0;
     const double c = damp_cos<R>(degrad90 * tmp);
     const R dampk = R(c * c * kmmax * D.dampcoef);
-    D.xkmh(i, j, k) = dampk > khm ? dampk : khm;
-    D.xkhh(i, j, k) = dampk > khh ? dampk : khh;
+    const R bm = km4 ? D.xkmh(i, j, k) : khm, bh = km4 ? D.xkhh(i, j, k) : khh;
+    D.xkmh(i, j, k) = dampk > bm ? dampk : bm;
+    D.xkhh(i, j, k) = dampk > bh ? dampk : bh;
     zkp = zk;
     zk = zkm;
   }

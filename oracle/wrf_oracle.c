@@ -1393,17 +1393,224 @@ static void cal_dampkm(or_dom* d) {
       }
     }
 }
+/* km_opt 4 with diff_opt 1: compute_diff_metrics' rdzw, zx, zy (diff_metrics.hpp:11-133, with set_physical_bc3d),
+ * cal_deform_and_div's defor11, defor22, defor12 (deform_div.hpp:20-156, :264-318, the outermost faces of specified /
+ * open sides copied from the next ones) and the 2-D Smagorinsky eddy viscosities (KSmag2dKm km_kh.hpp:47-97 over
+ * calculate_km_kh's range :585-625, zero on the outermost rows of specified boundaries) */
+static void smag2d_km(or_dom* d) {
+  const cw_grid* g = &d->g;
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  const int px = g->bc_x == CW_BC_PERIODIC, py = g->bc_y == CW_BC_PERIODIC, sp = specified(g);
+  const int ox = open_x(g), oy = open_y(g);
+  fld *ph = F_(CW_PH_2), *phb = F_(CW_PHB), *u = F_(CW_U_2), *v = F_(CW_V_2);
+  fld *msftx = F_(CW_MSFTX), *msfty = F_(CW_MSFTY), *msfuy = F_(CW_MSFUY), *msfvx = F_(CW_MSFVX), *msfux = F_(CW_MSFUX),
+      *msfvy = F_(CW_MSFVY);
+  const long nzp = nz + 1;
+  double* rdzw = (double*)calloc((size_t)nx * ny * nz, sizeof(double));
+  double* zx = (double*)calloc((size_t)(nx + 1) * ny * nzp, sizeof(double));
+  double* zy = (double*)calloc((size_t)nx * (ny + 1) * nzp, sizeof(double));
+  double* d11 = (double*)calloc((size_t)nx * ny * nz, sizeof(double));
+  double* d22 = (double*)calloc((size_t)nx * ny * nz, sizeof(double));
+  double* d12 = (double*)calloc((size_t)(nx + 1) * (ny + 1) * nz, sizeof(double));
+#define RDZW(i, j, k) rdzw[((size_t)(k) * ny + (j)) * nx + (i)]
+#define ZX(i, j, k) zx[((size_t)(k) * ny + (j)) * (nx + 1) + (i)]
+#define ZY(i, j, k) zy[((size_t)(k) * (ny + 1) + (j)) * nx + (i)]
+#define D11(i, j, k) d11[((size_t)(k) * ny + (j)) * nx + (i)]
+#define D22(i, j, k) d22[((size_t)(k) * ny + (j)) * nx + (i)]
+#define D12(i, j, k) d12[((size_t)(k) * (ny + 1) + (j)) * (nx + 1) + (i)]
+  /* metrics */
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i)
+      for (int k = 0; k < nz; ++k) {
+        const double z0 = (AT(ph, i, j, k) + AT(phb, i, j, k)) / G_, z1 = (AT(ph, i, j, k + 1) + AT(phb, i, j, k + 1)) / G_;
+        RDZW(i, j, k) = 1.0 / (z1 - z0);
+      }
+  const int ktop_x = px ? nz : -1, ktop_y = py ? nz : -1;
+  const int ocx = sp || ox, ocy = sp || oy;
+  for (int k = 0; k <= nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i <= nx; ++i) {
+        double val;
+        if (k == ktop_x && (i == 0 || i == nx)) val = 0.0;
+        else if (!px && (i == 0 || (i == nx && !ocx))) val = 0.0;
+        else if (!px && i == nx) {
+          const int ii = nx - 1;
+          val = d->rdx * (AT(phb, ii, j, k) - AT(phb, ii - 1, j, k)) / G_;
+          val += d->rdx * (AT(ph, ii, j, k) - AT(ph, ii - 1, j, k)) / G_;
+        } else {
+          const int i0 = i == nx ? 0 : i, im1 = i == 0 ? nx - 1 : i - 1;
+          val = d->rdx * (AT(phb, i0, j, k) - AT(phb, im1, j, k)) / G_;
+          val += d->rdx * (AT(ph, i0, j, k) - AT(ph, im1, j, k)) / G_;
+        }
+        ZX(i, j, k) = val;
+      }
+  for (int k = 0; k <= nz; ++k)
+    for (int j = 0; j <= ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        double val;
+        if (k == ktop_y && (j == 0 || j == ny)) val = 0.0;
+        else if (!py && (j == 0 || (j == ny && !ocy))) val = 0.0;
+        else if (!py && j == ny) {
+          const int jj = ny - 1;
+          val = d->rdy * (AT(phb, i, jj, k) - AT(phb, i, jj - 1, k)) / G_;
+          val += d->rdy * (AT(ph, i, jj, k) - AT(ph, i, jj - 1, k)) / G_;
+        } else {
+          const int j0 = j == ny ? 0 : j, jm1 = j == 0 ? ny - 1 : j - 1;
+          val = d->rdy * (AT(phb, i, j0, k) - AT(phb, i, jm1, k)) / G_;
+          val += d->rdy * (AT(ph, i, j0, k) - AT(ph, i, jm1, k)) / G_;
+        }
+        ZY(i, j, k) = val;
+      }
+  const double cf1 = d->cf1, cf2 = d->cf2, cf3 = d->cf3;
+  const double cft2 = -0.5 * d->dnw[nz - 1] / d->dn[nz - 1], cft1 = 1.0 - cft2;
+  double a0[DK_LEVELS], a1[DK_LEVELS], av[DK_LEVELS + 1];
+  /* hatavg of two columns a0, a1 at the w levels (KDeformDiagAndDiv / KDeform12) */
+#define HATAVG()                                                                                                   \
+  do {                                                                                                             \
+    for (int k = 1; k < nz; ++k) av[k] = 0.5 * (d->fnm[k] * (a0[k] + a1[k]) + d->fnp[k] * (a0[k - 1] + a1[k - 1])); \
+    av[0] = 0.5 * (cf1 * a0[0] + cf2 * a0[1] + cf3 * a0[2] + cf1 * a1[0] + cf2 * a1[1] + cf3 * a1[2]);            \
+    av[nz] = 0.5 * (cft1 * (a0[nz - 1] + a1[nz - 1]) + cft2 * (a0[nz - 2] + a1[nz - 2]));                         \
+  } while (0)
+  for (int j = 0; j < ny; ++j) /* KDeformDiagAndDiv: defor11, defor22 */
+    for (int i = 0; i < nx; ++i) {
+      const double mm = AT(msftx, i, j, 0) * AT(msfty, i, j, 0);
+      for (int k = 0; k < nz; ++k) {
+        a0[k] = AT(u, i, j, k) / AT(msfuy, i, j, 0);
+        a1[k] = AT(u, i + 1, j, k) / AT(msfuy, i + 1, j, 0);
+      }
+      HATAVG();
+      for (int k = 0; k < nz; ++k) {
+        const double tmpzx = 0.25 * (ZX(i, j, k) + ZX(i + 1, j, k) + ZX(i, j, k + 1) + ZX(i + 1, j, k + 1));
+        const double tmp1 = (av[k + 1] - av[k]) * tmpzx * RDZW(i, j, k);
+        D11(i, j, k) = 2.0 * (mm * (d->rdx * (a1[k] - a0[k]) - tmp1));
+      }
+      for (int k = 0; k < nz; ++k) {
+        a0[k] = AT(v, i, j, k) / AT(msfvx, i, j, 0);
+        a1[k] = AT(v, i, j + 1, k) / AT(msfvx, i, j + 1, 0);
+      }
+      HATAVG();
+      for (int k = 0; k < nz; ++k) {
+        const double tmpzy = 0.25 * (ZY(i, j, k) + ZY(i, j + 1, k) + ZY(i, j, k + 1) + ZY(i, j + 1, k + 1));
+        const double tmp1 = (av[k + 1] - av[k]) * tmpzy * RDZW(i, j, k);
+        D22(i, j, k) = 2.0 * (mm * (d->rdy * (a1[k] - a0[k]) - tmp1));
+      }
+    }
+  const int bxs = !px && (sp || ox), bxe = bxs, bys = !py && (sp || oy), bye = bys;
+  const int i12s = bxs ? 1 : 0, i12e = bxe ? nx : nx + 1, j12s = bys ? 1 : 0, j12e = bye ? ny : ny + 1;
+  double b0[DK_LEVELS], b1[DK_LEVELS], bv[DK_LEVELS + 1];
+  for (int j = j12s; j < j12e; ++j) /* KDeform12 */
+    for (int i = i12s; i < i12e; ++i) {
+      const int im1 = i == 0 ? (px ? nx - 1 : 0) : i - 1, i0 = i == nx ? (px ? 0 : nx - 1) : i;
+      const int jm1 = j == 0 ? (py ? ny - 1 : 0) : j - 1, j0 = j == ny ? (py ? 0 : ny - 1) : j;
+      const double mm = 0.25 * (AT(msfux, i, jm1, 0) + AT(msfux, i, j0, 0)) * (AT(msfvy, im1, j, 0) + AT(msfvy, i0, j, 0));
+      for (int k = 0; k < nz; ++k) {
+        a0[k] = AT(u, i, jm1, k) / AT(msfux, i, jm1, 0);
+        a1[k] = AT(u, i, j0, k) / AT(msfux, i, j0, 0);
+      }
+      HATAVG();
+      for (int k = 0; k <= nz; ++k) bv[k] = av[k];
+      for (int k = 0; k < nz; ++k) {
+        b0[k] = AT(v, im1, j, k) / AT(msfvy, im1, j, 0);
+        b1[k] = AT(v, i0, j, k) / AT(msfvy, i0, j, 0);
+      }
+      { /* hatavg of v into av (the same statement on b0, b1) */
+        for (int k = 1; k < nz; ++k) av[k] = 0.5 * (d->fnm[k] * (b0[k] + b1[k]) + d->fnp[k] * (b0[k - 1] + b1[k - 1]));
+        av[0] = 0.5 * (cf1 * b0[0] + cf2 * b0[1] + cf3 * b0[2] + cf1 * b1[0] + cf2 * b1[1] + cf3 * b1[2]);
+        av[nz] = 0.5 * (cft1 * (b0[nz - 1] + b1[nz - 1]) + cft2 * (b0[nz - 2] + b1[nz - 2]));
+      }
+      for (int k = 0; k < nz; ++k) {
+        const double tmpzy = 0.25 * (ZY(im1, j, k) + ZY(i0, j, k) + ZY(im1, j, k + 1) + ZY(i0, j, k + 1));
+        const double tmp1_u = (bv[k + 1] - bv[k]) * 0.25 * tmpzy *
+                              (RDZW(i0, j0, k) + RDZW(im1, j0, k) + RDZW(im1, jm1, k) + RDZW(i0, jm1, k));
+        const double term_u = mm * (d->rdy * (a1[k] - a0[k]) - tmp1_u);
+        const double tmpzx = 0.25 * (ZX(i, jm1, k) + ZX(i, j0, k) + ZX(i, jm1, k + 1) + ZX(i, j0, k + 1));
+        const double tmp1_v = (av[k + 1] - av[k]) * 0.25 * tmpzx *
+                              (RDZW(i0, j0, k) + RDZW(i0, jm1, k) + RDZW(im1, jm1, k) + RDZW(im1, j0, k));
+        const double term_v = mm * (d->rdx * (b1[k] - b0[k]) - tmp1_v);
+        D12(i, j, k) = term_u + term_v;
+      }
+    }
+#undef HATAVG
+  /* the edge copies, in the reference's order */
+  for (int j = 0; j <= ny; ++j)
+    for (int k = 0; k < nz; ++k) {
+      if (px) D12(nx, j, k) = D12(0, j, k);
+      else if (bxs) D12(0, j, k) = D12(1, j, k);
+    }
+  for (int i = 0; i <= nx; ++i)
+    for (int k = 0; k < nz; ++k) {
+      if (py) D12(i, ny, k) = D12(i, 0, k);
+      else if (bys) D12(i, 0, k) = D12(i, 1, k);
+    }
+  if (bxe)
+    for (int j = 0; j <= ny; ++j)
+      for (int k = 0; k < nz; ++k) D12(nx, j, k) = D12(nx - 1, j, k);
+  if (bye)
+    for (int i = 0; i <= nx; ++i)
+      for (int k = 0; k < nz; ++k) D12(i, ny, k) = D12(i, ny - 1, k);
+  /* KSmag2dKm */
+  int is = (ox || sp) ? 1 : 0, ie = (ox || sp) ? nx - 1 : nx;
+  const int js = (oy || sp) ? 1 : 0, je = (oy || sp) ? ny - 1 : ny;
+  if (px) { is = 0; ie = nx; }
+  const double c_s = 0.25, pr = prandtl(d), dx = g->dx, dy = g->dy;
+  for (int k = 0; k < nz; ++k)
+    for (int j = js; j < je; ++j)
+      for (int i = is; i < ie; ++i) {
+        const double dd = D11(i, j, k) - D22(i, j, k);
+        double def2 = 0.25 * (dd * dd);
+        const double d12a = 0.25 * (D12(i, j, k) + D12(i, j + 1, k) + D12(i + 1, j, k) + D12(i + 1, j + 1, k));
+        def2 += d12a * d12a;
+        const double mlen_h = sqrt(dx / AT(msftx, i, j, 0) * dy / AT(msfty, i, j, 0));
+        const double tmp = sqrt(def2);
+        double kmh = c_s * c_s * mlen_h * mlen_h * tmp;
+        kmh = kmh < 10.0 * mlen_h ? kmh : 10.0 * mlen_h;
+        AT(&d->xkmh, i, j, k) = kmh;
+        AT(&d->xkmv, i, j, k) = kmh;
+        AT(&d->xkhh, i, j, k) = kmh / pr;
+        AT(&d->xkhv, i, j, k) = 0.0;
+      }
+  if (sp) {
+    for (int side = 0; side < 2; ++side)
+      for (int j = 0; j < ny; ++j)
+        for (int k = 0; k < nz; ++k) {
+          const int ic = side == 0 ? 0 : nx - 1;
+          AT(&d->xkmh, ic, j, k) = AT(&d->xkmv, ic, j, k) = AT(&d->xkhh, ic, j, k) = AT(&d->xkhv, ic, j, k) = 0.0;
+        }
+    for (int side = 0; side < 2; ++side)
+      for (int i = 0; i < nx; ++i)
+        for (int k = 0; k < nz; ++k) {
+          const int jc = side == 0 ? 0 : ny - 1;
+          AT(&d->xkmh, i, jc, k) = AT(&d->xkmv, i, jc, k) = AT(&d->xkhh, i, jc, k) = AT(&d->xkhv, i, jc, k) = 0.0;
+        }
+  }
+#undef RDZW
+#undef ZX
+#undef ZY
+#undef D11
+#undef D22
+#undef D12
+  free(rdzw);
+  free(zx);
+  free(zy);
+  free(d11);
+  free(d22);
+  free(d12);
+}
 static void diffusion_prepare(or_dom* d) {
   const cw_grid* g = &d->g;
   const double pr = prandtl(d);
-  for (int k = 0; k < g->nz; ++k)
-    for (int j = 0; j < g->ny; ++j)
-      for (int i = 0; i < g->nx; ++i) {
-        AT(&d->xkmh, i, j, k) = d->o.khdif;
-        AT(&d->xkmv, i, j, k) = d->o.kvdif;
-        AT(&d->xkhh, i, j, k) = d->o.khdif / pr;
-        AT(&d->xkhv, i, j, k) = d->o.kvdif / pr;
-      }
+  if (d->o.km_opt == 4) {
+    smag2d_km(d);
+  } else {
+    for (int k = 0; k < g->nz; ++k)
+      for (int j = 0; j < g->ny; ++j)
+        for (int i = 0; i < g->nx; ++i) {
+          AT(&d->xkmh, i, j, k) = d->o.khdif;
+          AT(&d->xkmv, i, j, k) = d->o.kvdif;
+          AT(&d->xkhh, i, j, k) = d->o.khdif / pr;
+          AT(&d->xkhv, i, j, k) = d->o.kvdif / pr;
+        }
+  }
   if (d->o.damp_opt == 1) cal_dampkm(d);
   fill_halo(d, &d->xkmh);
   fill_halo(d, &d->xkmv);
@@ -2725,7 +2932,7 @@ or_dom* or_create(const cw_grid* g, const cw_options* o) {
   if ((o->damp_opt < 0 || o->damp_opt > 3) || (o->hypsometric_opt != 1 && o->hypsometric_opt != 2) ||
       o->diff_6th_opt < 0 || o->diff_6th_opt > 2 ||
       (o->mp_physics != 0 && (o->mp_physics != 1 || o->n_moist < 3 || g->nz > KS_LEVELS)) ||
-      (o->diff_opt != 0 && (o->diff_opt != 1 || o->km_opt != 1))) {
+      (o->diff_opt != 0 && (o->diff_opt != 1 || (o->km_opt != 1 && o->km_opt != 4)))) {
     free(d);
     return NULL;
   }

@@ -115,7 +115,7 @@ def test_serve_create_without_gpu_fails_cleanly():
 @pytest.mark.parametrize("change,needle", [
     (dict(damp_opt=4), "damp_opt"), (dict(hypsometric_opt=3), "hypsometric"),
     (dict(mp_physics=6), "mp_physics"),
-    (dict(nz=130), "nz"), (dict(diff_opt=2), "diff_opt")])
+    (dict(nz=130), "nz"), (dict(diff_opt=2), "diff_opt"), (dict(diff_opt=1, km_opt=2), "km_opt")])
 def test_unsupported_options_are_refused_with_a_reason(change, needle):
     """Options outside the path are refused at cw_create with a message naming them (before any device work,
     so this runs without a GPU)."""

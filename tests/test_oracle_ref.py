@@ -214,3 +214,30 @@ def test_oracle_equals_reference_eddy_viscosity_damping_2d():
     ref = _refdump.run(case, 3, own_pow=False)
     bad = compare(orc, ref, case)
     assert not bad, "\n".join(bad)
+
+
+@pytest.mark.parametrize("bc,damp", [((capi.SPECIFIED, capi.SPECIFIED), 0), ((capi.OPEN, capi.OPEN), 0),
+                                     ((capi.OPEN, capi.PERIODIC), 0), ((capi.SPECIFIED, capi.SPECIFIED), 1)],
+                         ids=["lam", "open", "open_x_periodic_y", "lam_dampkm"])
+def test_oracle_equals_reference_smagorinsky_2d(bc, damp):
+    """diff_opt 1 with km_opt 4: the horizontal eddy viscosities from the 2-D deformation (Smagorinsky, c_s 0.25) with
+    the terrain-following metric terms, the boundary faces' copies and the zero outermost rows of specified boundaries
+    (and with damp_opt 1 on top)."""
+    case = lam_case(seed=21, diff=True, bc=bc)
+    case.o.km_opt = 4
+    if damp:
+        case.o.damp_opt, case.o.zdamp, case.o.dampcoef = 1, 8000.0, 0.2
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_OWN)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=True)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)
+
+
+def test_oracle_equals_reference_smagorinsky_2d_xz():
+    case = cases.ideal_case(dict(cases.SMALL["straka_small"]), km_opt=4)
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_GLIBC)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=False)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)

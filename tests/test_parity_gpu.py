@@ -179,6 +179,28 @@ def test_2d_eddy_viscosity_damping_bit_exact():
     assert not bad, "\n".join(bad)
 
 
+@pytest.mark.parametrize("bc,damp", [((capi.SPECIFIED, capi.SPECIFIED), 0), ((capi.OPEN, capi.OPEN), 0),
+                                     ((capi.OPEN, capi.PERIODIC), 0), ((capi.SPECIFIED, capi.SPECIFIED), 1)],
+                         ids=["lam", "open", "open_x_periodic_y", "lam_dampkm"])
+def test_lam_smagorinsky_2d_bit_exact(bc, damp):
+    """diff_opt 1 with km_opt 4: the 2-D Smagorinsky eddy viscosities from the deformation (metric terms, edge copies,
+    zero outermost rows), with and without damp_opt 1 on top; 4 steps."""
+    case = lam_case(seed=21, diff=True, bc=bc)
+    case.o.km_opt = 4
+    if damp:
+        case.o.damp_opt, case.o.zdamp, case.o.dampcoef = 1, 8000.0, 0.2
+    dom, orc = run_pair(case, 4)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
+def test_2d_smagorinsky_bit_exact():
+    case = cases.ideal_case(dict(cases.SMALL["straka_small"]), km_opt=4)
+    dom, orc = run_pair(case, 3)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
 def test_cfl_maxima_equal_oracle():
     """LargeStep::cfl_max of every RK stage (the adaptive time step's input): the device maxima equal the oracle's,
     and recording them changes no field."""
