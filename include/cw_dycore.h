@@ -51,7 +51,8 @@ typedef struct cw_options {
   int time_step_sound; /* 0: RK3::auto_sound_steps (src/dyn/rk3.cpp:149-152) */
   /* ScalarParams (src/dyn/scalars.hpp:14-19) */
   int moist_adv_opt, scalar_adv_opt, tke_adv_opt;
-  /* DiffusionConfig (src/dyn/diffusion_driver.hpp:24-51): diff_opt 0 or 1 with km_opt 1 */
+  /* DiffusionConfig (src/dyn/diffusion_driver.hpp:24-51): diff_opt 0, or 1 with km_opt 1 (constant K) or 4 (2-D
+     Smagorinsky, c_s 0.25) */
   int diff_opt, km_opt;
   /* State / BaseState shape: flat = horizontally uniform base state (1-D storage, BaseState::flat) */
   int flat;
