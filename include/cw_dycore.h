@@ -68,6 +68,9 @@ typedef struct cw_options {
    * 0 off, 1 linear, 2 flux-limited (monotonic); its factor */
   int diff_6th_opt;
   double diff_6th_factor;
+  /* BaseState::coriolis (src/dyn/state.hpp:107, set with nonzero f0 / e0, src/cases/model.cpp:108-113): the Coriolis
+   * terms of the u, v, w tendencies from the uniform fields CW_F, CW_E, CW_SINA, CW_COSA */
+  int coriolis;
 } cw_options;
 
 /* Fills o with the reference defaults (the values Model::build takes when a key is absent). */

@@ -12,7 +12,8 @@
  * tracers, constant-K diffusion (diff_opt 1, km_opt 1), specified lateral boundaries (width 5),
  * top_lid, w_damping, h/v_adv_order 5/6, 3/4, damp_opt 2 and 3 (sin by the pow mode: glibc's or cw_sin), the
  * sixth-order filter, hypsometric_opt 1 and 2 (log by the pow mode), damp_opt 1 (cos by the pow mode), Kessler
- * microphysics. Not restated (rejected by or_create): map factors other than 1, Coriolis.
+ * microphysics, the Coriolis terms (uniform f, e, sina, cosa). Not restated: horizontally varying map factors and
+ * their curvature terms (BaseState::mapped).
  */
 #include "wrf_oracle.h"
 
@@ -531,7 +532,12 @@ static double tend_u(const tctx* c, int i, int j, int k, int use_tendf) {
           H * (d->c1h[k] * AT(mu, i - 1, j, 0) + d->c1h[k] * AT(mu, i, j, 0)));
   t -= cqu_(d, i, j, k) * dpx;
   const double rw4 = Q * (AT(rw, i - 1, j, k + 1) + AT(rw, i - 1, j, k) + AT(rw, i, j, k + 1) + AT(rw, i, j, k));
-  (void)rv;
+  if (d->o.coriolis) { /* Coriolis (:249-253) */
+    fld *f = F_(CW_F), *e = F_(CW_E), *cosa = F_(CW_COSA);
+    const double rv4 = Q * (AT(rv, i - 1, j + 1, k) + AT(rv, i, j + 1, k) + AT(rv, i - 1, j, k) + AT(rv, i, j, k));
+    t = t + rm * H * (AT(f, i, j, 0) + AT(f, i - 1, j, 0)) * rv4 -
+        H * (AT(e, i, j, 0) + AT(e, i - 1, j, 0)) * H * (AT(cosa, i, j, 0) + AT(cosa, i - 1, j, 0)) * rw4;
+  }
   t = t - AT(u, i, j, k) * RERADIUS * rw4;
   if (use_tendf) t += AT(F_(CW_RU_TENDF), i, j, k) / AT(msfuy, i, j, 0);
   return t;
@@ -640,6 +646,12 @@ static double tend_v(const tctx* c, int i, int j, int k, int use_tendf) {
           H * (d->c1h[k] * AT(mu, i, j - 1, 0) + d->c1h[k] * AT(mu, i, j, 0)));
   t -= cqv_(d, i, j, k) * dpy;
   const double rw4 = Q * (AT(rw, i, j - 1, k + 1) + AT(rw, i, j - 1, k) + AT(rw, i, j, k + 1) + AT(rw, i, j, k));
+  if (d->o.coriolis) { /* Coriolis (:362-365) */
+    fld *ru = F_(CW_RU), *f = F_(CW_F), *e = F_(CW_E), *sina = F_(CW_SINA);
+    const double ru4 = Q * (AT(ru, i, j, k) + AT(ru, i + 1, j, k) + AT(ru, i, j - 1, k) + AT(ru, i + 1, j - 1, k));
+    t = t - rm * H * (AT(f, i, j, 0) + AT(f, i, j - 1, 0)) * ru4 +
+        rm * H * (AT(e, i, j, 0) + AT(e, i, j - 1, 0)) * H * (AT(sina, i, j, 0) + AT(sina, i, j - 1, 0)) * rw4;
+  }
   t = t - rm * AT(v, i, j, k) * RERADIUS * rw4;
   if (use_tendf) t += AT(F_(CW_RV_TENDF), i, j, k) * AT(mvi, i, j, 0);
   return t;
@@ -769,6 +781,8 @@ static double tend_w(const tctx* c, int i, int j, int k, int use_tendf, double w
     const double rvw = H * (d->fnm[k] * (AT(rv, i, j, k) + AT(rv, i, j + 1, k)) +
                             d->fnp[k] * (AT(rv, i, j, k - 1) + AT(rv, i, j + 1, k - 1)));
     const double rmt = AT(msftx, i, j, 0) / AT(msfty, i, j, 0);
+    if (d->o.coriolis) /* Coriolis (:484) */
+      t = t + AT(F_(CW_E), i, j, 0) * (AT(F_(CW_COSA), i, j, 0) * ruw - rmt * AT(F_(CW_SINA), i, j, 0) * rvw);
     const double uw = H * (d->fnm[k] * (AT(u, i, j, k) + AT(u, i + 1, j, k)) +
                            d->fnp[k] * (AT(u, i, j, k - 1) + AT(u, i + 1, j, k - 1)));
     const double vw = H * (d->fnm[k] * (AT(v, i, j, k) + AT(v, i, j + 1, k)) +

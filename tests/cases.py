@@ -50,3 +50,12 @@ SMALL = {
     "igw_small": dict(golden_config("igw"), nx=60, run_time=18.0),
     "rest_state_small": dict(golden_config("rest_state"), nx=12, ny=10, nz=16, run_time=30.0),
 }
+
+
+def with_coriolis(case, f=1.0e-4, e=5.0e-5, sina=0.2, cosa=0.98):
+    """Turn on the Coriolis terms (BaseState::coriolis) with uniform f, e and a rotated grid (sina, cosa)."""
+    for name, value in (("F", f), ("E", e), ("SINA", sina), ("COSA", cosa)):
+        a, _ = case.field(name)
+        a[:] = value
+    case.o.coriolis = 1
+    return case

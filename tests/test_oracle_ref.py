@@ -241,3 +241,19 @@ def test_oracle_equals_reference_smagorinsky_2d_xz():
     ref = _refdump.run(case, 3, own_pow=False)
     bad = compare(orc, ref, case)
     assert not bad, "\n".join(bad)
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(bc=(capi.OPEN, capi.PERIODIC), n_moist=2, n_scalars=3)],
+                         ids=["lam", "open_x_periodic_y"])
+def test_oracle_equals_reference_coriolis(kw):
+    """BaseState::coriolis: the Coriolis terms of the u, v, w tendencies with uniform f, e and a rotated grid."""
+    case = cases.with_coriolis(lam_case(seed=23, **kw))
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_OWN)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=True)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)
+    plain = lam_case(seed=23, **kw)
+    still = _oracle.Oracle(plain, pow_mode=_oracle.POW_OWN)
+    still.step(3)
+    assert not np.array_equal(orc.array("V_2"), still.array("V_2"))  # the terms acted

@@ -201,6 +201,16 @@ def test_2d_smagorinsky_bit_exact():
     assert not bad, "\n".join(bad)
 
 
+@pytest.mark.parametrize("kw", [dict(), dict(bc=(capi.OPEN, capi.PERIODIC), n_moist=2, n_scalars=3)],
+                         ids=["lam", "open_x_periodic_y"])
+def test_lam_coriolis_bit_exact(kw):
+    """The Coriolis terms (uniform f, e, sina, cosa) of the u, v, w tendencies; 4 steps."""
+    case = cases.with_coriolis(lam_case(seed=23, **kw))
+    dom, orc = run_pair(case, 4)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
 def test_cfl_maxima_equal_oracle():
     """LargeStep::cfl_max of every RK stage (the adaptive time step's input): the device maxima equal the oracle's,
     and recording them changes no field."""
