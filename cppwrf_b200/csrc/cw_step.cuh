@@ -183,7 +183,10 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
   L.halo(cw_handle::H_MU1);
   for (int rk = 1; rk <= 3; ++rk) {
     const int ns = rk == 1 ? 1 : (rk == 2 ? n_sound / 2 : n_sound);
-    L.halo(cw_handle::H_PREP0);
+    // rk_step_prep's fill (LargeStep::prep): at stages 2 and 3 the previous stage's H_FIN left these halos as this
+    // fill would make them (only the scalars change in between), so only the first stage runs it (the fill merges
+    // with the scalars' H_Q2 into one launch: fewer cells, not fewer launches)
+    if (rk == 1) L.halo(cw_handle::H_PREP0);
     L.run_cb("k_ls_prep", RG_COLS_STAG, 1, k_ls_prep<R, NM>, d);
     L.halo(cw_handle::H_PREP1);
     if (rk == 1 && (dampkm || smag)) {  // DiffusionDriver::prepare: km_opt 4's and damp_opt 1's eddy viscosities
