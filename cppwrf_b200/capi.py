@@ -60,7 +60,8 @@ class Options(C.Structure):
                 ("scalar_adv_opt", C.c_int), ("tke_adv_opt", C.c_int), ("diff_opt", C.c_int), ("km_opt", C.c_int),
                 ("flat", C.c_int), ("n_moist", C.c_int), ("n_scalars", C.c_int), ("lbc", C.c_int),
                 ("precision", C.c_int), ("mp_physics", C.c_int), ("mp_tend_lim", C.c_double),
-                ("diff_6th_opt", C.c_int), ("diff_6th_factor", C.c_double), ("coriolis", C.c_int)]
+                ("diff_6th_opt", C.c_int), ("diff_6th_factor", C.c_double), ("coriolis", C.c_int),
+                ("mapped", C.c_int)]
 
 
 _DP = C.POINTER(C.c_double)

@@ -227,7 +227,7 @@ int cw_default_options(cw_options* o) {
   o->diff_opt = 0; o->km_opt = 1;
   o->flat = 1; o->n_moist = 0; o->n_scalars = 0; o->lbc = 0; o->precision = CW_FP64;
   o->mp_physics = 0; o->mp_tend_lim = 10.0;
-  o->diff_6th_opt = 0; o->diff_6th_factor = 0.12; o->coriolis = 0;
+  o->diff_6th_opt = 0; o->diff_6th_factor = 0.12; o->coriolis = 0; o->mapped = 0;
   return 0;
 }
 

@@ -78,9 +78,9 @@ inline FieldKind field_kind(const cw_options& o, int id) {
     case CW_MUB: case CW_HT: return {'M', 2, o.flat != 0};
     case CW_PB: case CW_ALB: case CW_T_INIT: case CW_QV_BASE: return {'M', 3, o.flat != 0};
     case CW_PHB: return {'W', 3, o.flat != 0};
-    case CW_MSFTX: case CW_MSFTY: case CW_F: case CW_E: case CW_SINA: case CW_COSA: return {'M', 2, true};
-    case CW_MSFUX: case CW_MSFUY: return {'U', 2, true};
-    case CW_MSFVX: case CW_MSFVY: case CW_MSFVX_INV: return {'V', 2, true};
+    case CW_MSFTX: case CW_MSFTY: case CW_F: case CW_E: case CW_SINA: case CW_COSA: return {'M', 2, o.mapped == 0};
+    case CW_MSFUX: case CW_MSFUY: return {'U', 2, o.mapped == 0};
+    case CW_MSFVX: case CW_MSFVY: case CW_MSFVX_INV: return {'V', 2, o.mapped == 0};
     default: return {'M', 3, false};  // t, p, al, alt, php, h_diabatic, t_tend(f), q
   }
 }

@@ -206,7 +206,8 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.mub = fb(CW_MUB); D.pb = fb(CW_PB); D.alb = fb(CW_ALB); D.t_init = fb(CW_T_INIT); D.qv_base = fb(CW_QV_BASE);
   D.phb = fb(CW_PHB); D.ht = fb(CW_HT); D.msftx = fb(CW_MSFTX); D.msfty = fb(CW_MSFTY); D.msfux = fb(CW_MSFUX);
   D.msfuy = fb(CW_MSFUY); D.msfvx = fb(CW_MSFVX); D.msfvy = fb(CW_MSFVY); D.msfvx_inv = fb(CW_MSFVX_INV);
-  D.f = fb(CW_F); D.e = fb(CW_E); D.sina = fb(CW_SINA); D.cosa = fb(CW_COSA); D.cor = o.coriolis != 0;
+  D.f = fb(CW_F); D.e = fb(CW_E); D.sina = fb(CW_SINA); D.cosa = fb(CW_COSA); D.cor = o.coriolis != 0 || o.mapped != 0;
+  D.mapped = o.mapped != 0;
   D.u_save = w3(W_U_SAVE); D.v_save = w3(W_V_SAVE); D.w_save = w3(W_W_SAVE); D.t_save = w3(W_T_SAVE);
   D.ph_save = w3(W_PH_SAVE); D.ww1 = w3(W_WW1); D.c2a = w3(W_C2A); D.pm1 = w3(W_PM1); D.t_2save = w3(W_T_2SAVE);
   D.a = w3(W_A); D.alpha = w3(W_ALPHA); D.gamma = w3(W_GAMMA); D.mu_save = w3(W_MU_SAVE); D.mudf = w3(W_MUDF);

@@ -78,8 +78,9 @@ struct Dom {
   V3<T> ru_tend, rv_tend, rw_tend, t_tend, ph_tend, mu_tend, ru_tendf, rv_tendf, rw_tendf, t_tendf, ph_tendf;
   // BaseState
   VB<T> mub, pb, alb, t_init, qv_base, phb, ht, msftx, msfty, msfux, msfuy, msfvx, msfvy, msfvx_inv;
-  VB<T> f, e, sina, cosa;  // Coriolis parameters and grid rotation (uniform)
-  int cor;                 // BaseState::coriolis: the Coriolis terms of the u, v, w tendencies
+  VB<T> f, e, sina, cosa;  // Coriolis parameters and grid rotation
+  int cor;                 // MapC::cor = BaseState::mapped || coriolis: the Coriolis terms of the u, v, w tendencies
+  int mapped;              // BaseState::mapped: map factors vary; the curvature terms of u, v use their gradients
   // acoustic-step work fields (SmallStep, src/dyn/small_step.hpp:45-49)
   V3<T> u_save, v_save, w_save, t_save, ph_save, ww1, c2a, pm1, t_2save, a, alpha, gamma, mu_save, mudf, muave,
       w_rhs, t2a;

@@ -209,7 +209,13 @@ __device__ __forceinline__ R cqw_(const Dom<R>& D, int i, int j, int k) { return
 // (cqu, cqv, cqw are written only by k_ls_prep, which does not read them). The tendency, flux and diffusion
 // functions below read only fields that no thread of their kernels writes: the read-only load path (.ld).
 
-// KTendU (large_step.cpp:152-264), unmapped (uniform map factors, no curvature terms of their gradients)
+// MapC::vxgm (large_step.cpp:121-124): the curvature factor at mass point (i, j, k) from u, v and the map factors
+template <class R>
+__device__ __forceinline__ R vxgm(const Dom<R>& D, int i, int j, int k) {
+  return R(0.5) * (D.u2.ld(i, j, k) + D.u2.ld(i + 1, j, k)) * (D.msfvx(i, j + 1) - D.msfvx(i, j)) * R(D.rdy) -
+         R(0.5) * (D.v2.ld(i, j, k) + D.v2.ld(i, j + 1, k)) * (D.msfuy(i + 1, j) - D.msfuy(i, j)) * R(D.rdx);
+}
+// KTendU (large_step.cpp:152-264)
 template <class R>
 __device__ R tu_fx(const Dom<R>& D, int i, int j, int k) {
   const int o = ord_mass(i, D.nx, D.spec_x);
@@ -308,12 +314,15 @@ __device__ R tend_u(const Dom<R>& D, int i, int j, int k, bool use_tendf, R fx0,
           R(0.5) * (c1h * D.mu2.ld(i - 1, j, 0) + c1h * D.mu2.ld(i, j, 0)));
   t -= cqu_(D, i, j, k) * dpx;
   const R rw4 = R(0.25) * (D.rw.ld(i - 1, j, k + 1) + D.rw.ld(i - 1, j, k) + D.rw.ld(i, j, k + 1) + D.rw.ld(i, j, k));
-  if (D.cor) {  // Coriolis (:249-253)
+  if (D.cor) {  // Coriolis (:249-253), and the curvature from the map factors' gradients (:255-257)
     const R rv4 = R(0.25) * (D.rv.ld(i - 1, j + 1, k) + D.rv.ld(i, j + 1, k) + D.rv.ld(i - 1, j, k) + D.rv.ld(i, j, k));
     t = t + rm * R(0.5) * (D.f(i, j) + D.f(i - 1, j)) * rv4 -
         R(0.5) * (D.e(i, j) + D.e(i - 1, j)) * R(0.5) * (D.cosa(i, j) + D.cosa(i - 1, j)) * rw4;
+    if (D.mapped) t = t + R(0.5) * (vxgm(D, i, j, k) + vxgm(D, i - 1, j, k)) * rv4 - D.u2.ld(i, j, k) * R(k::reradius) * rw4;
+    else t = t - D.u2.ld(i, j, k) * R(k::reradius) * rw4;
+  } else {
+    t = t - D.u2.ld(i, j, k) * R(k::reradius) * rw4;
   }
-  t = t - D.u2.ld(i, j, k) * R(k::reradius) * rw4;
   if (use_tendf) t += D.ru_tendf.ld(i, j, k) / D.msfuy(i, j);
   return t;
 }
@@ -410,12 +419,15 @@ __device__ R tend_v(const Dom<R>& D, int i, int j, int k, bool use_tendf, R fx0,
           R(0.5) * (c1h * D.mu2.ld(i, j - 1, 0) + c1h * D.mu2.ld(i, j, 0)));
   t -= cqv_(D, i, j, k) * dpy;
   const R rw4 = R(0.25) * (D.rw.ld(i, j - 1, k + 1) + D.rw.ld(i, j - 1, k) + D.rw.ld(i, j, k + 1) + D.rw.ld(i, j, k));
-  if (D.cor) {  // Coriolis (:362-365)
+  if (D.cor) {  // Coriolis (:362-365), and the curvature from the map factors' gradients (:367-369)
     const R ru4 = R(0.25) * (D.ru.ld(i, j, k) + D.ru.ld(i + 1, j, k) + D.ru.ld(i, j - 1, k) + D.ru.ld(i + 1, j - 1, k));
     t = t - rm * R(0.5) * (D.f(i, j) + D.f(i, j - 1)) * ru4 +
         rm * R(0.5) * (D.e(i, j) + D.e(i, j - 1)) * R(0.5) * (D.sina(i, j) + D.sina(i, j - 1)) * rw4;
+    if (D.mapped) t = t - R(0.5) * (vxgm(D, i, j, k) + vxgm(D, i, j - 1, k)) * ru4 - rm * D.v2.ld(i, j, k) * R(k::reradius) * rw4;
+    else t = t - rm * D.v2.ld(i, j, k) * R(k::reradius) * rw4;
+  } else {
+    t = t - rm * D.v2.ld(i, j, k) * R(k::reradius) * rw4;
   }
-  t = t - rm * D.v2.ld(i, j, k) * R(k::reradius) * rw4;
   if (use_tendf) t += D.rv_tendf.ld(i, j, k) * D.msfvx_inv(i, j);
   return t;
 }

@@ -69,8 +69,12 @@ typedef struct cw_options {
   int diff_6th_opt;
   double diff_6th_factor;
   /* BaseState::coriolis (src/dyn/state.hpp:107, set with nonzero f0 / e0, src/cases/model.cpp:108-113): the Coriolis
-   * terms of the u, v, w tendencies from the uniform fields CW_F, CW_E, CW_SINA, CW_COSA */
+   * terms of the u, v, w tendencies from the fields CW_F, CW_E, CW_SINA, CW_COSA */
   int coriolis;
+  /* BaseState::mapped (src/dyn/state.hpp:97, :67-73): the map factors and CW_F, CW_E, CW_SINA, CW_COSA vary in the
+   * horizontal (2-D storage instead of one value; a real-data projection); adds the curvature terms of u and v from
+   * the map factors' gradients, and the Coriolis terms */
+  int mapped;
 } cw_options;
 
 /* Fills o with the reference defaults (the values Model::build takes when a key is absent). */

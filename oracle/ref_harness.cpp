@@ -81,7 +81,7 @@ int main(int argc, char** argv) {
     g.nx = cg.nx; g.ny = cg.ny; g.nz = cg.nz; g.dx = cg.dx; g.dy = cg.dy; g.dt = cg.dt; g.ztop = cg.ztop; g.p_top = cg.p_top;
     g.bc_x = BC(cg.bc_x); g.bc_y = BC(cg.bc_y);
     const int nz = g.nz;
-    dyn::BaseState b(g, co.flat != 0, false);
+    dyn::BaseState b(g, co.flat != 0, co.mapped != 0);
     b.coriolis = co.coriolis != 0;
     // vertical arrays: znu dnw rdnw c1h c2h c3h c4h (nz), znw dn rdn fnm fnp c1f c2f c3f c4f (nz+1),
     // u_base v_base t_base qv_base_1d z_base (nz), then cf1 cf2 cf3 cfn cfn1 rdx rdy p_top t0

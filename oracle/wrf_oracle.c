@@ -12,8 +12,7 @@
  * tracers, constant-K diffusion (diff_opt 1, km_opt 1), specified lateral boundaries (width 5),
  * top_lid, w_damping, h/v_adv_order 5/6, 3/4, damp_opt 2 and 3 (sin by the pow mode: glibc's or cw_sin), the
  * sixth-order filter, hypsometric_opt 1 and 2 (log by the pow mode), damp_opt 1 (cos by the pow mode), Kessler
- * microphysics, the Coriolis terms (uniform f, e, sina, cosa). Not restated: horizontally varying map factors and
- * their curvature terms (BaseState::mapped).
+ * microphysics, the Coriolis terms, horizontally varying map factors with their curvature terms (BaseState::mapped).
  */
 #include "wrf_oracle.h"
 
@@ -173,9 +172,9 @@ static void field_kind(const cw_options* o, int id, char* s, int* rank, int* uni
     case CW_MUB: case CW_HT: *s = ST_M; *rank = 2; *uniform = o->flat; break;
     case CW_PB: case CW_ALB: case CW_T_INIT: case CW_QV_BASE: *s = ST_M; *uniform = o->flat; break;
     case CW_PHB: *s = ST_W; *uniform = o->flat; break;
-    case CW_MSFTX: case CW_MSFTY: case CW_F: case CW_E: case CW_SINA: case CW_COSA: *s = ST_M; *rank = 2; *uniform = 1; break;
-    case CW_MSFUX: case CW_MSFUY: *s = ST_U; *rank = 2; *uniform = 1; break;
-    case CW_MSFVX: case CW_MSFVY: case CW_MSFVX_INV: *s = ST_V; *rank = 2; *uniform = 1; break;
+    case CW_MSFTX: case CW_MSFTY: case CW_F: case CW_E: case CW_SINA: case CW_COSA: *s = ST_M; *rank = 2; *uniform = !o->mapped; break;
+    case CW_MSFUX: case CW_MSFUY: *s = ST_U; *rank = 2; *uniform = !o->mapped; break;
+    case CW_MSFVX: case CW_MSFVY: case CW_MSFVX_INV: *s = ST_V; *rank = 2; *uniform = !o->mapped; break;
     default: *s = ST_M; break; /* M 3-D: t, p, al, alt, php, h_diabatic, t_tend, t_tendf, q */
   }
 }
@@ -429,6 +428,13 @@ typedef struct {
   int nz, do_y, top_lid;
 } tctx;
 
+/* MapC::vxgm (:121-124): the curvature factor at mass point (i, j, k) from the uncoupled u, v and the map factors */
+static double vxgm(or_dom* d, int i, int j, int k) {
+  fld *u = F_(CW_U_2), *v = F_(CW_V_2), *msfvx = F_(CW_MSFVX), *msfuy = F_(CW_MSFUY);
+  return H * (AT(u, i, j, k) + AT(u, i + 1, j, k)) * (AT(msfvx, i, j + 1, 0) - AT(msfvx, i, j, 0)) * d->rdy -
+         H * (AT(v, i, j, k) + AT(v, i, j + 1, k)) * (AT(msfuy, i + 1, j, 0) - AT(msfuy, i, j, 0)) * d->rdx;
+}
+
 /* --- U --- */
 static double tu_fx(const tctx* c, int i, int j, int k) {
   or_dom* d = c->d;
@@ -532,13 +538,16 @@ static double tend_u(const tctx* c, int i, int j, int k, int use_tendf) {
           H * (d->c1h[k] * AT(mu, i - 1, j, 0) + d->c1h[k] * AT(mu, i, j, 0)));
   t -= cqu_(d, i, j, k) * dpx;
   const double rw4 = Q * (AT(rw, i - 1, j, k + 1) + AT(rw, i - 1, j, k) + AT(rw, i, j, k + 1) + AT(rw, i, j, k));
-  if (d->o.coriolis) { /* Coriolis (:249-253) */
+  const double rv4 = Q * (AT(rv, i - 1, j + 1, k) + AT(rv, i, j + 1, k) + AT(rv, i - 1, j, k) + AT(rv, i, j, k));
+  if (d->o.coriolis || d->o.mapped) { /* Coriolis (:249-253; MapC::cor = mapped || coriolis) */
     fld *f = F_(CW_F), *e = F_(CW_E), *cosa = F_(CW_COSA);
-    const double rv4 = Q * (AT(rv, i - 1, j + 1, k) + AT(rv, i, j + 1, k) + AT(rv, i - 1, j, k) + AT(rv, i, j, k));
     t = t + rm * H * (AT(f, i, j, 0) + AT(f, i - 1, j, 0)) * rv4 -
         H * (AT(e, i, j, 0) + AT(e, i - 1, j, 0)) * H * (AT(cosa, i, j, 0) + AT(cosa, i - 1, j, 0)) * rw4;
   }
-  t = t - AT(u, i, j, k) * RERADIUS * rw4;
+  if (d->o.mapped) /* curvature with the map factors' gradients (:255-257) */
+    t = t + H * (vxgm(d, i, j, k) + vxgm(d, i - 1, j, k)) * rv4 - AT(u, i, j, k) * RERADIUS * rw4;
+  else
+    t = t - AT(u, i, j, k) * RERADIUS * rw4;
   if (use_tendf) t += AT(F_(CW_RU_TENDF), i, j, k) / AT(msfuy, i, j, 0);
   return t;
 }
@@ -646,13 +655,17 @@ static double tend_v(const tctx* c, int i, int j, int k, int use_tendf) {
           H * (d->c1h[k] * AT(mu, i, j - 1, 0) + d->c1h[k] * AT(mu, i, j, 0)));
   t -= cqv_(d, i, j, k) * dpy;
   const double rw4 = Q * (AT(rw, i, j - 1, k + 1) + AT(rw, i, j - 1, k) + AT(rw, i, j, k + 1) + AT(rw, i, j, k));
-  if (d->o.coriolis) { /* Coriolis (:362-365) */
-    fld *ru = F_(CW_RU), *f = F_(CW_F), *e = F_(CW_E), *sina = F_(CW_SINA);
-    const double ru4 = Q * (AT(ru, i, j, k) + AT(ru, i + 1, j, k) + AT(ru, i, j - 1, k) + AT(ru, i + 1, j - 1, k));
+  fld* ru = F_(CW_RU);
+  const double ru4 = Q * (AT(ru, i, j, k) + AT(ru, i + 1, j, k) + AT(ru, i, j - 1, k) + AT(ru, i + 1, j - 1, k));
+  if (d->o.coriolis || d->o.mapped) { /* Coriolis (:362-365) */
+    fld *f = F_(CW_F), *e = F_(CW_E), *sina = F_(CW_SINA);
     t = t - rm * H * (AT(f, i, j, 0) + AT(f, i, j - 1, 0)) * ru4 +
         rm * H * (AT(e, i, j, 0) + AT(e, i, j - 1, 0)) * H * (AT(sina, i, j, 0) + AT(sina, i, j - 1, 0)) * rw4;
   }
-  t = t - rm * AT(v, i, j, k) * RERADIUS * rw4;
+  if (d->o.mapped) /* curvature (:367-369) */
+    t = t - H * (vxgm(d, i, j, k) + vxgm(d, i, j - 1, k)) * ru4 - rm * AT(v, i, j, k) * RERADIUS * rw4;
+  else
+    t = t - rm * AT(v, i, j, k) * RERADIUS * rw4;
   if (use_tendf) t += AT(F_(CW_RV_TENDF), i, j, k) * AT(mvi, i, j, 0);
   return t;
 }
@@ -781,7 +794,7 @@ static double tend_w(const tctx* c, int i, int j, int k, int use_tendf, double w
     const double rvw = H * (d->fnm[k] * (AT(rv, i, j, k) + AT(rv, i, j + 1, k)) +
                             d->fnp[k] * (AT(rv, i, j, k - 1) + AT(rv, i, j + 1, k - 1)));
     const double rmt = AT(msftx, i, j, 0) / AT(msfty, i, j, 0);
-    if (d->o.coriolis) /* Coriolis (:484) */
+    if (d->o.coriolis || d->o.mapped) /* Coriolis (:484) */
       t = t + AT(F_(CW_E), i, j, 0) * (AT(F_(CW_COSA), i, j, 0) * ruw - rmt * AT(F_(CW_SINA), i, j, 0) * rvw);
     const double uw = H * (d->fnm[k] * (AT(u, i, j, k) + AT(u, i + 1, j, k)) +
                            d->fnp[k] * (AT(u, i, j, k - 1) + AT(u, i + 1, j, k - 1)));

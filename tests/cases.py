@@ -32,12 +32,13 @@ def golden_config(name):
 
 
 def lam_case(nx=24, ny=20, nz=14, seed=3, n_moist=5, n_scalars=5, diff=False, hybrid_opt=2, precision=capi.FP64,
-             bc=(capi.SPECIFIED, capi.SPECIFIED)):
+             bc=(capi.SPECIFIED, capi.SPECIFIED), mapped=False):
     """A limited-area case (terrain, hybrid coordinate, moist species, specified boundaries) from a seed; bc = the
     (x, y) boundary kinds (open or periodic sides take no boundary data)."""
     g = capi.grid(nx, ny, nz, 15000.0, 90.0, 0.0, dy=15000.0, p_top=5000.0, bc_x=bc[0], bc_y=bc[1])
     o = capi.default_options(None, flat=0, n_moist=n_moist, n_scalars=n_scalars,
-                             lbc=int(capi.SPECIFIED in bc), time_step_sound=4, precision=precision)
+                             lbc=int(capi.SPECIFIED in bc), time_step_sound=4, precision=precision,
+                             mapped=int(mapped))
     if diff:
         o.diff_opt, o.khdif, o.kvdif, o.pr_inv = 1, 3000.0, 1.0, 3.0
     return capi.Case(g, o).gen_lam(seed=seed, hybrid_opt=hybrid_opt)
@@ -58,4 +59,20 @@ def with_coriolis(case, f=1.0e-4, e=5.0e-5, sina=0.2, cosa=0.98):
         a, _ = case.field(name)
         a[:] = value
     case.o.coriolis = 1
+    return case
+
+
+def with_map_factors(case, amp=0.02):
+    """Horizontally varying map factors, f, e and grid rotation (a case made with mapped=True): smooth seeded
+    patterns over every stored point, halos included; msfvx_inv = 1 / msfvx."""
+    import numpy as np
+    base = {"MSFTX": 1.0, "MSFTY": 1.01, "MSFUX": 1.0, "MSFUY": 1.01, "MSFVX": 1.0, "MSFVY": 1.01, "F": 1.0e-4,
+            "E": 5.0e-5, "SINA": 0.1, "COSA": 0.99}
+    for n, (name, b) in enumerate(base.items()):
+        a, _ = case.field(name)
+        x = np.arange(a.size, dtype=np.float64)
+        a[:] = b * (1.0 + amp * np.sin(0.013 * x + 0.7 * n))
+    inv, _ = case.field("MSFVX_INV")
+    vx, _ = case.field("MSFVX")
+    inv[:] = 1.0 / vx
     return case

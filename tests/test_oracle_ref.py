@@ -257,3 +257,15 @@ def test_oracle_equals_reference_coriolis(kw):
     still = _oracle.Oracle(plain, pow_mode=_oracle.POW_OWN)
     still.step(3)
     assert not np.array_equal(orc.array("V_2"), still.array("V_2"))  # the terms acted
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(diff=True)], ids=["lam", "lam_diffusion"])
+def test_oracle_equals_reference_mapped(kw):
+    """BaseState::mapped: horizontally varying map factors, f, e, sina, cosa (2-D storage), the Coriolis terms and the
+    curvature terms from the map factors' gradients, in every term that carries a map factor."""
+    case = cases.with_map_factors(lam_case(seed=25, mapped=True, **kw))
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_OWN)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=True)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)

@@ -211,6 +211,16 @@ def test_lam_coriolis_bit_exact(kw):
     assert not bad, "\n".join(bad)
 
 
+@pytest.mark.parametrize("kw", [dict(), dict(diff=True)], ids=["lam", "lam_diffusion"])
+def test_lam_mapped_bit_exact(kw):
+    """Horizontally varying map factors, f, e, sina, cosa: Coriolis and curvature terms and every map factor of the
+    step; 4 steps."""
+    case = cases.with_map_factors(lam_case(seed=25, mapped=True, **kw))
+    dom, orc = run_pair(case, 4)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
 def test_cfl_maxima_equal_oracle():
     """LargeStep::cfl_max of every RK stage (the adaptive time step's input): the device maxima equal the oracle's,
     and recording them changes no field."""
