@@ -470,16 +470,17 @@ def main():
     g0 = torch.cuda.Event(enable_timing=True)
     g1 = torch.cuda.Event(enable_timing=True)
     g0.record(stream)
+    # every field of the state in one cw_upload_fields / cw_download_fields call (one synchronisation per step)
+    tensors = list(host.values()) + qhost
+    nf = len(tensors)
+    fids = (C.c_int * nf)(*([capi.F[name] for name in host] + [capi.F["Q_2"]] * len(qhost)))
+    fns = (C.c_int * nf)(*([0] * len(host) + list(range(len(qhost)))))
+    fptr = (dp * nf)(*[C.cast(t.data_ptr(), dp) for t in tensors])
+    fcnt = (C.c_size_t * nf)(*[t.numel() for t in tensors])
     for _ in range(n_e2e):
-        for name, t in host.items():
-            lib.cw_upload(dom.h, capi.F[name], 0, C.cast(t.data_ptr(), dp), t.numel())
-        for n, t in enumerate(qhost):
-            lib.cw_upload(dom.h, capi.F["Q_2"], n, C.cast(t.data_ptr(), dp), t.numel())
+        lib.cw_upload_fields(dom.h, 0, nf, fids, fns, fptr, fcnt)
         lib.cw_step(dom.h, 1)
-        for name, t in host.items():
-            lib.cw_download(dom.h, capi.F[name], 0, C.cast(t.data_ptr(), dp), t.numel())
-        for n, t in enumerate(qhost):
-            lib.cw_download(dom.h, capi.F["Q_2"], n, C.cast(t.data_ptr(), dp), t.numel())
+        lib.cw_download_fields(dom.h, 0, nf, fids, fns, fptr, fcnt)
     g1.record(stream)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0

@@ -923,6 +923,67 @@ int cw_member_download(cw_handle* h, int mi, int field, int n, double* host, siz
 int cw_download(cw_handle* h, int field, int n, double* host, size_t count) {
   return cw_member_download(h, 0, field, n, host, count);
 }
+// several fields, one synchronisation: FP64 fields copy directly; FP32 (mixed) fields go through one staging region
+// per field (the staging buffer sized for all of them first, so that no reallocation happens between the copies)
+int cw_upload_fields(cw_handle* h, int mi, int nf, const int* fields, const int* ns, const double* const* host,
+                     const size_t* counts) {
+  return guarded(h, [&] {
+    if (!h || nf < 0 || (nf > 0 && (!fields || !ns || !host || !counts))) throw std::runtime_error("null argument");
+    std::vector<Loc> locs;
+    size_t staged = 0;
+    for (int f = 0; f < nf; ++f) {
+      if (!host[f]) throw std::runtime_error("null host buffer");
+      locs.push_back(locate(h, mi, fields[f], ns[f]));
+      if (counts[f] != size_t(locs.back().L.total)) throw std::runtime_error("count != layout.total");
+      if (counts[f] >= (size_t(1) << 32)) throw std::runtime_error("field too large");
+      if (locs.back().esz != 8) staged += counts[f];
+    }
+    double* st = staged ? staging(h, staged) : nullptr;
+    for (int f = 0; f < nf; ++f) {
+      const Loc& l = locs[size_t(f)];
+      if (l.esz == 8) {
+        CW_CUDA(cudaMemcpyAsync(l.base, host[f], counts[f] * 8, cudaMemcpyHostToDevice, h->stream));
+      } else {
+        CW_CUDA(cudaMemcpyAsync(st, host[f], counts[f] * 8, cudaMemcpyHostToDevice, h->stream));
+        const unsigned n = unsigned(counts[f]), blocks = std::min(4096u, (n + 255u) / 256u);
+        k_narrow<<<blocks, 256, 0, h->stream>>>(st, reinterpret_cast<float*>(l.base), n);
+        CW_CUDA(cudaGetLastError());
+        st += counts[f];
+      }
+    }
+    return 0;
+  });
+}
+int cw_download_fields(cw_handle* h, int mi, int nf, const int* fields, const int* ns, double* const* host,
+                       const size_t* counts) {
+  return guarded(h, [&] {
+    if (!h || nf < 0 || (nf > 0 && (!fields || !ns || !host || !counts))) throw std::runtime_error("null argument");
+    std::vector<Loc> locs;
+    size_t staged = 0;
+    for (int f = 0; f < nf; ++f) {
+      if (!host[f]) throw std::runtime_error("null host buffer");
+      locs.push_back(locate(h, mi, fields[f], ns[f]));
+      if (counts[f] != size_t(locs.back().L.total)) throw std::runtime_error("count != layout.total");
+      if (counts[f] >= (size_t(1) << 32)) throw std::runtime_error("field too large");
+      if (locs.back().esz != 8) staged += counts[f];
+    }
+    double* st = staged ? staging(h, staged) : nullptr;
+    for (int f = 0; f < nf; ++f) {
+      const Loc& l = locs[size_t(f)];
+      if (l.esz == 8) {
+        CW_CUDA(cudaMemcpyAsync(host[f], l.base, counts[f] * 8, cudaMemcpyDeviceToHost, h->stream));
+      } else {
+        const unsigned n = unsigned(counts[f]), blocks = std::min(4096u, (n + 255u) / 256u);
+        k_widen<<<blocks, 256, 0, h->stream>>>(reinterpret_cast<const float*>(l.base), st, n);
+        CW_CUDA(cudaGetLastError());
+        CW_CUDA(cudaMemcpyAsync(host[f], st, counts[f] * 8, cudaMemcpyDeviceToHost, h->stream));
+        st += counts[f];
+      }
+    }
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+  });
+}
 int cw_member_field_layout(cw_handle* h, int mi, int field, int n, cw_layout* out) {
   return guarded(h, [&] {
     if (!h || !out) throw std::runtime_error("null argument");

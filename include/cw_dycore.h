@@ -134,6 +134,15 @@ int cw_set_vertical(cw_handle* h, const cw_vertical* v);
  * (halo included, Layout order) from / to host memory; count = layout.total. */
 int cw_upload(cw_handle* h, int field, int n, const double* host, size_t count);
 int cw_download(cw_handle* h, int field, int n, double* host, size_t count);
+/* The same for several fields in one call (FieldT::fill_host / download of each of nf fields, src/core/field.hpp:
+ * 119-129): fields[i], ns[i] (species index for CW_Q_*), host[i], counts[i]. The copies are queued on the handle's
+ * stream with one synchronisation: cw_upload_fields returns before they finish, in order with the next cw_step, so
+ * its host buffers must not change before the next synchronising call (cw_download_fields, cw_download, cw_sync);
+ * cw_download_fields returns when every field has arrived. Pinned host memory makes the copies asynchronous. */
+int cw_upload_fields(cw_handle* h, int member, int nf, const int* fields, const int* ns, const double* const* host,
+                     const size_t* counts);
+int cw_download_fields(cw_handle* h, int member, int nf, const int* fields, const int* ns, double* const* host,
+                       const size_t* counts);
 /* The field's layout (FieldT::layout, src/core/field.hpp:107). */
 int cw_field_layout(cw_handle* h, int field, int n, cw_layout* out);
 /* The device address of element (0,0,0) of a field (FieldT::data, src/core/field.hpp:108). */
