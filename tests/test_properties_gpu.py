@@ -82,3 +82,36 @@ def test_repeated_runs_bit_identical():
     a, b = run(case, 4), run(case, 4)
     for name in capi.STATE_FIELDS:
         assert np.array_equal(a.field(name).view(np.uint64), b.field(name).view(np.uint64)), name
+
+
+def test_inertial_oscillation():
+    """Coriolis on an f-plane (the reference's dycore check 2, configs/inertial.ini): a uniform u0 = 10 m/s with
+    f = 1e-3 1/s and no pressure gradient turns as u = u0 cos(f t), v = -u0 sin(f t); within 1e-3 m/s over one
+    period, checked every quarter period."""
+    cfg = dict(cases.golden_config("rest_state"), nx=8, ny=8, nz=20, dx=2000.0, dy=2000.0, ztop=20000.0, dt=10.0,
+               khdif=0.0, kvdif=0.0)
+    case = cases.with_coriolis(cases.ideal_case(cfg, u0=10.0), f=1.0e-3, e=0.0, sina=0.0, cosa=1.0)
+    d = Domain(case.g, case.o).upload_case(case)
+    worst = 0.0
+    for n in range(1, 5):
+        d.step(157)
+        t = 1570.0 * n
+        u = capi.interior(d.field("U_2"), d.layout("U_2"))
+        v = capi.interior(d.field("V_2"), d.layout("V_2"))
+        worst = max(worst, float(np.abs(u - 10.0 * np.cos(1.0e-3 * t)).max()),
+                    float(np.abs(v + 10.0 * np.sin(1.0e-3 * t)).max()))
+    assert worst <= 1.0e-3, worst
+
+
+def test_map_factor_invariance_bit_exact():
+    """The map-factor form is invariant (the reference's dycore check 1): squall2d (moist, Kessler, PD advection)
+    with a constant map factor m = 2 and dx = 2000 m equals m = 1 and dx = 1000 m bit for bit -- every scaling by 2
+    is exact in floating point. emdiv = 0: the external-mode filter uses the grid dx."""
+    from test_oracle_properties import scaled_pair
+    a, b = scaled_pair()
+    da, db = run(a, 20), run(b, 20)
+    names = ["U_2", "V_2", "W_2", "T_2", "PH_2", "MU_2", "P", "AL", "RAINNC"]
+    for name in names:
+        assert np.array_equal(da.field(name).view(np.uint64), db.field(name).view(np.uint64)), name
+    for n in range(a.o.n_scalars):
+        assert np.array_equal(da.field("Q_2", n).view(np.uint64), db.field("Q_2", n).view(np.uint64)), n
