@@ -76,3 +76,12 @@ def with_map_factors(case, amp=0.02):
     vx, _ = case.field("MSFVX")
     inv[:] = 1.0 / vx
     return case
+
+
+def every_option_case():
+    """A LAM case with every option the path accepts on at once (their interactions): varying map factors with
+    Coriolis, km_opt 4 with damp_opt 1, the flux-limited sixth-order filter, hypsometric_opt 2, w_damping."""
+    case = with_map_factors(lam_case(seed=31, diff=True, mapped=True))
+    case.o.km_opt, case.o.damp_opt, case.o.zdamp, case.o.dampcoef = 4, 1, 8000.0, 0.2
+    case.o.diff_6th_opt, case.o.diff_6th_factor, case.o.hypsometric_opt, case.o.w_damping = 2, 0.12, 2, 1
+    return case

@@ -269,3 +269,13 @@ def test_oracle_equals_reference_mapped(kw):
     ref = _refdump.run(case, 3, own_pow=True)
     bad = compare(orc, ref, case)
     assert not bad, "\n".join(bad)
+
+
+def test_oracle_equals_reference_every_option():
+    """Every option the path accepts on at once (cases.every_option_case), for their interactions."""
+    case = cases.every_option_case()
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_OWN)
+    orc.step(3)
+    ref = _refdump.run(case, 3, own_pow=True)
+    bad = compare(orc, ref, case)
+    assert not bad, "\n".join(bad)

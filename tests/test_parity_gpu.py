@@ -221,6 +221,14 @@ def test_lam_mapped_bit_exact(kw):
     assert not bad, "\n".join(bad)
 
 
+def test_lam_every_option_bit_exact():
+    """Every option the path accepts on at once (cases.every_option_case), for their interactions."""
+    case = cases.every_option_case()
+    dom, orc = run_pair(case, 4)
+    bad = compare_all(dom, orc, case)
+    assert not bad, "\n".join(bad)
+
+
 def test_cfl_maxima_equal_oracle():
     """LargeStep::cfl_max of every RK stage (the adaptive time step's input): the device maxima equal the oracle's,
     and recording them changes no field."""
