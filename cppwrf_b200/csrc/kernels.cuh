@@ -1521,6 +1521,7 @@ __global__ void __launch_bounds__(PX) k_ring(const __grid_constant__ Pack<R, NM>
   int pos, k, side;
   if (!thread_index<0>(P, RG_RING, Dp, pos, k, side)) return;
   const Dom<R>& D = *Dp;
+  if (!D.lbc) return;  // a member without boundary data in a pack with some: LateralBC belongs to the others only
   (void)rk;
   const int nx = D.nx, ny = D.ny, nz = D.nz;
   switch (op) {

@@ -178,6 +178,7 @@ __global__ void __launch_bounds__(PX) k_p_rho_phi(const __grid_constant__ Pack<R
   if (!thread_index<SH>(P, RG_MASS, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
   if (mode == 2 && D.mp_physics == 0) return;
+  if (mode == 1 && !D.lbc) return;  // calc_p_rho_phi_interior follows spec_bdy_final: members with boundary data only
   if (mode == 1 || (mode == 2 && D.lbc)) {  // calc_p_rho_phi_interior (:622-633): spec_zone 1 off each non-periodic side
     const int sz = 1;
     if (D.bc_x != CW_BC_PERIODIC && (i < sz || i >= D.nx - sz)) return;

@@ -65,3 +65,28 @@ def test_batch_more_members_than_a_pack():
             assert np.array_equal(b.field(m, name).view(np.uint64), orc.array(name).view(np.uint64)), (m, name)
         for n in range(c.o.n_scalars):
             assert np.array_equal(b.field(m, "Q_2", n).view(np.uint64), orc.array("Q_2", n).view(np.uint64)), (m, n)
+
+
+def test_batch_members_with_different_options():
+    """Members whose options differ in one launch sequence (the pack runs the open-boundary variant of k_tend for
+    all; each member keeps its own boundaries, Coriolis, map factors, eddy viscosities and damping): each equals the
+    oracle bit for bit."""
+    import cases as cs
+    c1 = lam_case(nx=22, ny=18, nz=14, seed=41)
+    c2 = cs.with_coriolis(lam_case(nx=26, ny=20, nz=14, seed=42, bc=(capi.OPEN, capi.OPEN)))
+    c3 = cs.every_option_case()
+    c4 = lam_case(nx=20, ny=24, nz=14, seed=43, diff=True, bc=(capi.OPEN, capi.PERIODIC))
+    c4.o.damp_opt, c4.o.zdamp, c4.o.dampcoef = 3, 8000.0, 0.2
+    members = [c1, c2, c3, c4]
+    b = Batch([c.g for c in members], [c.o for c in members])
+    for m, c in enumerate(members):
+        b.upload_case(m, c)
+    b.step(3)
+    b.sync()
+    for m, c in enumerate(members):
+        orc = _oracle.Oracle(c, pow_mode=_oracle.POW_OWN)
+        orc.step(3)
+        for name in ("U_2", "V_2", "W_2", "T_2", "PH_2", "MU_2", "P", "AL", "WW_M"):
+            assert np.array_equal(b.field(m, name).view(np.uint64), orc.array(name).view(np.uint64)), (m, name)
+        for n in range(c.o.n_scalars):
+            assert np.array_equal(b.field(m, "Q_2", n).view(np.uint64), orc.array("Q_2", n).view(np.uint64)), (m, n)
