@@ -201,7 +201,7 @@ def run_reference(args, rank):
     return 0
 
 
-# ---------------------------------------------------------------- further workloads
+# ---------------------------------------------------------------- further workloads (precision, ensemble, served)
 def _timed_steps(torch, stream, fn, steps):
     """device ms of fn(steps) on stream (CUDA events)."""
     torch.cuda.synchronize()
@@ -382,7 +382,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default block shapes")
     ap.add_argument("--workload", choices=["lam", "precision", "ensemble", "served"], default="lam",
-                    help="lam: the headline 119x89x44 line; the others: BASELINE configs 3, 4 and 5 (1 GPU)")
+                    help="lam: the headline 119x89x44 line; precision: 400x400x60 mixed vs FP64 with 1 h / 6 h errors; "
+                         "ensemble: 64 uneven members; served: Poisson requests under an HBM budget (1 GPU)")
     ap.add_argument("--requests", type=int, default=24, help="served: number of requests")
     ap.add_argument("--rate", type=float, default=2.0, help="served: Poisson arrival rate per second")
     args = ap.parse_args()
