@@ -153,7 +153,7 @@ template <class R, int NM>
 void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
   const Member& M0 = h->m[0];
   bool lbc = false, terrain = false, scalars = false, any_pd = false, mp = false, open = false, dampkm = false,
-       smag = false;
+       smag = false, any_plain = false;
   // every member specified on all four sides: the acoustic substeps read no halo cell of the fields the
   // per-substep fills (H_SS0, H_UV, H_AC) would refresh (the faces next to the boundary are the spec
   // zone's, updated from the boundary data), and the fills after the substeps (H_POST, H_FIN) refresh them
@@ -171,8 +171,11 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
     mp |= M.o.mp_physics != 0;
     terrain |= !M.o.flat;
     scalars |= M.o.n_scalars > 0;
-    for (int n = 0; n < M.o.n_scalars; ++n)
-      any_pd |= (n < M.o.n_moist ? M.o.moist_adv_opt : M.o.scalar_adv_opt) == 1;
+    for (int n = 0; n < M.o.n_scalars; ++n) {
+      const bool pd = (n < M.o.n_moist ? M.o.moist_adv_opt : M.o.scalar_adv_opt) == 1;
+      any_pd |= pd;
+      any_plain |= !pd;
+    }
   }
   const int n_sound = M0.n_sound;
   if (lbc) {
@@ -213,7 +216,8 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
     L.halo(cw_handle::H_FIN);
     if (scalars) {
       if (rk == 1) L.run_t("k_q_tendf_rk1", RG_MASS, nq, KV(k_q_tendf_rk1), d);
-      L.run_t("k_q_update", RG_MASS, nq, KV(k_q_update), d, rk);
+      // at rk 3 the PD species take k_q_*_pd: the plain update runs only when some species is not PD
+      if (rk != 3 || any_plain || !any_pd) L.run_t("k_q_update", RG_MASS, nq, KV(k_q_update), d, rk);
       if (rk == 3 && any_pd) {
         L.run_t("k_q_pre_pd", RG_MASS, nq, KV(k_q_pre_pd), d, rk);
         L.halo(cw_handle::H_Q1PD);
