@@ -26,8 +26,8 @@ MIXED_FLAGS = [f for f in FLAGS if f != "--fmad=false"] + ["--fmad=true", "-ftz=
 
 def build(verbose=False):
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
-    objs = []
-    for src in SOURCES:
+    objs, procs = [], []
+    for src in SOURCES:  # the translation units compile in parallel
         obj = os.path.join(HERE, "lib", os.path.splitext(src)[0] + ".o")
         flags = MIXED_FLAGS if src == "cw_step_mixed.cu" else FLAGS
         cmd = [NVCC] + ARCH + flags + ["-c", os.path.join(CSRC, src), "-o", obj]
@@ -36,8 +36,11 @@ def build(verbose=False):
                    "-o", obj]
         if verbose:
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        procs.append((cmd, subprocess.Popen(cmd)))
         objs.append(obj)
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
     cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-Xcompiler", "-fopenmp", "-lgomp"]
     subprocess.run(cmd, check=True)
     return LIB

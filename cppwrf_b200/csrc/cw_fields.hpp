@@ -90,7 +90,7 @@ inline cw_layout field_layout(const cw_grid& g, const cw_options& o, int id) {
   return layout_make(g, k.stagger, k.rank, k.uniform);
 }
 
-// n_sound: RK3::auto_sound_steps (src/dyn/rk3.cpp:149-152) when time_step_sound == 0
+// n_sound: RK3::auto_sound_steps (src/dyn/rk3.cpp:69-72) when time_step_sound == 0
 inline int sound_steps(const cw_grid& g, const cw_options& o) {
   if (o.time_step_sound > 0) return o.time_step_sound;
   const double spacing = g.dx < g.dy ? g.dx : g.dy;

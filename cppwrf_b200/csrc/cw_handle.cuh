@@ -107,6 +107,7 @@ struct cw_handle {
   std::vector<Member> m;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  int device = -1;  // the CUDA device current at create (every allocation of the handle is on it)
   DevTables<double> t64;
   DevTables<float> t32;
   double* dtbc_d = nullptr;  // per member: time since the boundary data, advanced by the step on the device

@@ -3,7 +3,7 @@
 // tables, the halo refresh sets, the RK3 step as a sequence of batched launches (captured once into a
 // CUDA graph and replayed), and the C ABI of include/cw_dycore.h (with cw_diagnostics of include/cw_output.h).
 //
-// The step order is CPPWRF's RK3::step (src/dyn/rk3.cpp:166-250): copy of the time-t state, then per RK
+// The step order is CPPWRF's RK3::step (src/dyn/rk3.cpp:86-170): copy of the time-t state, then per RK
 // stage rk_step_prep, rk_tendency (+ stage-1 diffusion and boundary relaxation), the acoustic loop,
 // small_step_finish, scalar transport and calc_p_rho_phi; spec_bdy_final and set_w_surface at the end.
 // Halos are refreshed where the reference refreshes them; refreshes with no kernel in between that
@@ -416,7 +416,7 @@ void build_halosets_t(cw_handle* h, DevTables<R>& T) {
 }
 
 void build_copies(cw_handle* h) {
-  // step start: u_1 = u_2, ... (whole allocations, src/dyn/rk3.cpp:175-178); q_1 = q_2 read through the table
+  // step start: u_1 = u_2, ... (whole allocations, src/dyn/rk3.cpp:95-99); q_1 = q_2 read through the table
   size_t q0 = 0;
   for (Member& M : h->m) {
     const int pairs[6][2] = {{CW_U_1, CW_U_2}, {CW_V_1, CW_V_2}, {CW_W_1, CW_W_2}, {CW_T_1, CW_T_2}, {CW_PH_1, CW_PH_2}, {CW_MU_1, CW_MU_2}};
@@ -610,6 +610,7 @@ void rebuild(cw_handle* h) {
 }
 
 void setup(cw_handle* h) {
+  CW_CUDA(cudaGetDevice(&h->device));
   allocate(h);
   build_tables(h);
 }
@@ -1371,12 +1372,19 @@ extern "C" int cw_download_noalloc(cw_handle* h, int field, int n, double* host,
   if (count > kNoallocScratchDoubles) return CW_NOALLOC_ETOOBIG;
   int device = -1;
   if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kNoallocMaxDevices) return CW_NOALLOC_ECUDA;
+  if (device != h->device) return CW_NOALLOC_EBADARG;  // the scratch of another device than the handle's
   double* scratch = noalloc_scratch(device);
   if (!scratch) return CW_NOALLOC_ECUDA;
   const unsigned nel = unsigned(count);
   const unsigned blocks = std::min(4096u, (nel + 255u) / 256u);
+  // an error left by an earlier asynchronous launch belongs to its caller: it is reported here but not
+  // consumed (cudaPeekAtLastError); only the failure of this call's own launch is cleared
+  if (cudaPeekAtLastError() != cudaSuccess) return CW_NOALLOC_ECUDA;
   k_widen<<<blocks, 256, 0, h->stream>>>(reinterpret_cast<const float*>(l.base), scratch, nel);
-  if (cudaGetLastError() != cudaSuccess) return CW_NOALLOC_ECUDA;
+  if (cudaPeekAtLastError() != cudaSuccess) {
+    (void)cudaGetLastError();
+    return CW_NOALLOC_ECUDA;
+  }
   if (cudaMemcpyAsync(host, scratch, count * 8, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
       cudaStreamSynchronize(h->stream) != cudaSuccess)
     return CW_NOALLOC_ECUDA;

@@ -1,5 +1,5 @@
 // SPDX-License-Identifier: GPL-3.0-or-later
-// The RK3 step as a sequence of batched launches (CPPWRF's RK3::step, src/dyn/rk3.cpp:166-250): the launcher
+// The RK3 step as a sequence of batched launches (CPPWRF's RK3::step, src/dyn/rk3.cpp:86-170): the launcher
 // (deferred and merged halo fills, per-kernel profiling and block-shape selection) and the step's launch order.
 //
 // Included by the two translation units that instantiate the step's kernels, each for its own precision under
@@ -231,7 +231,7 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
       L.halo(cw_handle::H_Q2);
     }
   }
-  if (mp) {  // the microphysics after the RK loop (PhysicsCoupling::step), then calc_p_rho_phi (rk3.cpp:150-158)
+  if (mp) {  // the microphysics after the RK loop (PhysicsCoupling::step), then calc_p_rho_phi (rk3.cpp:146-158)
     L.run_cb("k_kessler", RG_COLS_MASS, kCbArrays, k_kessler<R, NM>, d);
     L.halo(cw_handle::H_MP);
     L.run_t("k_p_rho_phi", RG_MASS, 1, KV(k_p_rho_phi), d, 2);

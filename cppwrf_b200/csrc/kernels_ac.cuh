@@ -170,7 +170,7 @@ __device__ __forceinline__ void p_rho_phi_point(const Dom<R>& D, int i, int j, i
   D.p(i, j, k) = R(k::p1000mb * eos_pow<R>(base) - double(D.pb(i, j, k)));
 }
 // mode 0: every mass point; 1: calc_p_rho_phi_interior (after spec_bdy_final); 2: after the microphysics, only in
-// the members that have it, on the interior where the member has boundary data (rk3.cpp:150-158)
+// the members that have it, on the interior where the member has boundary data (rk3.cpp:146-158)
 template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX) k_p_rho_phi(const __grid_constant__ Pack<R, NM> P, int mode) {
   const Dom<R>* Dp;

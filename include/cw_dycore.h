@@ -48,7 +48,7 @@ typedef struct cw_options {
   double epssm, smdiv, emdiv;
   int damp_opt, hypsometric_opt;
   double zdamp, dampcoef;
-  int time_step_sound; /* 0: RK3::auto_sound_steps (src/dyn/rk3.cpp:149-152) */
+  int time_step_sound; /* 0: RK3::auto_sound_steps (src/dyn/rk3.cpp:69-72) */
   /* ScalarParams (src/dyn/scalars.hpp:14-19) */
   int moist_adv_opt, scalar_adv_opt, tke_adv_opt;
   /* DiffusionConfig (src/dyn/diffusion_driver.hpp:24-51): diff_opt 0, or 1 with km_opt 1 (constant K) or 4 (2-D
@@ -61,7 +61,7 @@ typedef struct cw_options {
   int lbc;       /* 1: a LateralBC is attached (RK3::set_lateral_bc, width 5 / spec 1 / relax 4) */
   int precision; /* enum cw_precision */
   /* PhysicsParams (src/dyn/physics_coupling.hpp:23-35): 0 none, 1 Kessler (species 0, 1, 2 are qv, qc, qr),
-   * run after the RK3 loop as solve_em does (src/dyn/rk3.cpp:150-158) */
+   * run after the RK3 loop as solve_em does (src/dyn/rk3.cpp:146-158) */
   int mp_physics;
   double mp_tend_lim; /* K/s, limit on the microphysics heating rate */
   /* DiffusionConfig (src/dyn/diffusion_driver.hpp:42-43): sixth-order horizontal filter at the first RK stage,
@@ -123,7 +123,7 @@ typedef struct cw_handle cw_handle;
 /* Layout of a field of a grid without a handle: Layout::make (src/core/halo.cpp:12-48). */
 int cw_layout_of(const cw_grid* g, const cw_options* o, int field, cw_layout* out);
 
-/* RK3 ctor (src/dyn/rk3.hpp:36-37, rk3.cpp:128-136) together with the State, Tendencies and BaseState
+/* RK3 ctor (src/dyn/rk3.hpp:36-37, rk3.cpp:48-56) together with the State, Tendencies and BaseState
  * allocation of cases::Model (src/cases/model.hpp:28-50): device-resident, zero-filled. */
 int cw_create(const cw_grid* g, const cw_options* o, cw_handle** out);
 /* ~RK3 and the Model's fields. */
@@ -153,9 +153,9 @@ int cw_set_lbc(cw_handle* h, int var, int side, const double* values, const doub
 int cw_set_lbc_scalar(cw_handle* h, int n, int side, const double* values, const double* tends, size_t count);
 /* LateralBC::dtbc (src/dyn/lateral_bc.hpp:57): seconds since the start of the boundary interval. */
 int cw_set_lbc_time(cw_handle* h, double dtbc);
-/* RK3::step (src/dyn/rk3.hpp:52, rk3.cpp:166-250), nsteps times in a row on the handle's stream. */
+/* RK3::step (src/dyn/rk3.hpp:52, rk3.cpp:86-170), nsteps times in a row on the handle's stream. */
 int cw_step(cw_handle* h, int nsteps);
-/* RK3::set_dt (src/dyn/rk3.hpp:45, rk3.cpp:159-164). */
+/* RK3::set_dt (src/dyn/rk3.hpp:45, rk3.cpp:79-84). */
 int cw_set_dt(cw_handle* h, double dt, int n_sound);
 /* RK3::n_sound (src/dyn/rk3.hpp:43). */
 int cw_n_sound(cw_handle* h, int* out);
@@ -286,16 +286,21 @@ int cw_gen_lam(cw_case* c, const cw_lam_params* p);
  * copies that to `host`. FP64 fields are copied directly and have no size limit.
  *
  * Same arguments and result as cw_download (member 0 of the handle, the whole allocation of the field,
- * count = its layout's total). Call it with the handle's device current. The first call on each device
- * looks up the scratch's device address (cudaGetSymbolAddress), which may load the library's device code
- * on that device: make one call early, before the period in which nothing may be set up. No part of the
- * scratch has to start at zero: each call writes the count elements it then copies.
+ * count = its layout's total). Call it with the handle's device current (another current device returns
+ * CW_NOALLOC_EBADARG). The first call on each device looks up the scratch's device address
+ * (cudaGetSymbolAddress), which may load the library's device code on that device: make one call early,
+ * before the period in which nothing may be set up. The looked-up address is kept for the life of the
+ * process and does not survive cudaDeviceReset (which unloads the library's device code): after a reset,
+ * handles are gone anyway, and this call must not be used again in that process. No part of the scratch
+ * has to start at zero: each call writes the count elements it then copies. An error left pending by an
+ * earlier asynchronous launch is reported as CW_NOALLOC_ECUDA and left in place for its owner.
  *
  * The scratch is shared by every handle on a device: two calls that overlap in time (from two threads, or
  * on two streams before the first has returned) race on it, so callers serialize them. The call returns
  * after the copy has completed (it synchronizes the handle's stream). Errors are returned, not stored in
  * cw_last_error (storing a message could allocate):
- *   CW_NOALLOC_EBADARG  null handle or buffer, unknown field, species out of range, count != layout total
+ *   CW_NOALLOC_EBADARG  null handle or buffer, unknown field, species out of range, count != layout total,
+ *                       or a current device other than the handle's
  *   CW_NOALLOC_ETOOBIG  an FP32 field of more than CW_NOALLOC_SCRATCH_DOUBLES elements (nothing is copied)
  *   CW_NOALLOC_ECUDA    a CUDA call failed */
 #define CW_NOALLOC_SCRATCH_DOUBLES 1048576

@@ -14,7 +14,8 @@ from cppwrf_b200 import capi
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
-REFERENCE_SRC = os.environ.get("CPPWRF_REFERENCE", "/root/reference")
+# a CPPWRF checkout: CPPWRF_REFERENCE, else the directory `reference` beside this repository
+REFERENCE_SRC = os.environ.get("CPPWRF_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
 
 
 def available():

@@ -1,7 +1,7 @@
 /* SPDX-License-Identifier: GPL-3.0-or-later
  *
  * TEST INFRASTRUCTURE ONLY. The oracle is a plain-C, single-threaded restatement of CPPWRF's
- * RK3 split-explicit dry dynamical core step (src/dyn/rk3.cpp:166-250 and the kernels it calls).
+ * RK3 split-explicit dry dynamical core step (src/dyn/rk3.cpp:86-170 and the kernels it calls).
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it, and only as
  * the checker or the timed CPU reference; the product library never links or calls it.
  *

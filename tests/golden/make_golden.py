@@ -10,7 +10,8 @@ the snapshot's JSON text and the diag.csv lines verbatim, together with the case
 (configs/<case>.ini). The oracle test recomputes the same variables and compares hashes, which is a
 bit-for-bit comparison without committing megabytes of binary data.
 
-Run from the repository root, with the reference checked out at /root/reference:
+Run from the repository root, with a CPPWRF checkout named by CPPWRF_REFERENCE (default: the directory
+`reference` beside this repository):
     python tests/golden/make_golden.py
 """
 import hashlib
@@ -20,8 +21,8 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("CPPWRF_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("CPPWRF_REFERENCE") or os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(HERE))), "reference")
 
 # configs/<case>.ini of the reference, with the quick-mode run_time of run.sh:146-150
 CASES = {

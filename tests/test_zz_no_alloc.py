@@ -54,3 +54,24 @@ def test_noalloc_rejects_fields_beyond_the_scratch():
     bad = np.zeros(3)
     assert _noalloc(lib, dom, "MU_2", 0, bad) == capi.NOALLOC_EBADARG  # wrong count
     assert _noalloc(lib, dom, "Q_2", 5, out2) == capi.NOALLOC_EBADARG  # species out of range
+
+
+def test_noalloc_rejects_another_current_device():
+    """The scratch is looked up on the current device: a handle of another device is refused, not misused
+    (checked only where this process sees more than one device)."""
+    import torch
+
+    if torch.cuda.device_count() < 2:
+        pytest.skip("one device visible: the device check has nothing to compare")
+    lib = capi.load()
+    case = lam_case(nx=24, ny=20, nz=12, seed=3, precision=capi.MIXED)
+    lib.cw_use_device(0)
+    dom = Domain(case.g, case.o).upload_case(case)
+    L = dom.layout("T_2")
+    out = np.full(L.total, np.nan)
+    lib.cw_use_device(1)
+    try:
+        assert _noalloc(lib, dom, "T_2", 0, out) == capi.NOALLOC_EBADARG
+    finally:
+        lib.cw_use_device(0)
+    assert _noalloc(lib, dom, "T_2", 0, out) == 0
