@@ -156,24 +156,46 @@ def ncu_traffic(kernel, workload_tag):
     return None
 
 
-def cpu_baseline(capi, seconds_target=15.0):
-    """The reference's own CPU FP64 build (oracle/_ref) on a bounded sample of the workload, all host threads;
-    falls back to the oracle port (one thread) when the reference build is absent."""
+def host_description():
+    """The host CPU model and glibc version (the reference's CPU results depend on both)."""
+    model = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        glibc = subprocess.run(["ldd", "--version"], capture_output=True, text=True).stdout.splitlines()[0].strip()
+    except (OSError, IndexError):
+        glibc = None
+    return {"cpu_model": model, "glibc": glibc}
+
+
+def cpu_baseline(seconds_target=15.0, capi=None):
+    """The reference's own CPU FP64 build (oracle/_ref/ref_harness: its sources compiled unmodified, glibc's math)
+    on a bounded sample of the workload, all host threads. The case is generated inside the harness process
+    (ref_harness --lam, the same seeded generator and bytes as make_case), so this leg loads no library of this
+    repository. Falls back to the oracle port (one thread) when the reference build is absent."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    case = make_case(capi, capi.FP64)
     pts = WORKLOAD["nx"] * WORKLOAD["ny"] * WORKLOAD["nz"]
     ncores = os.cpu_count() or 1
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
     if os.path.exists(exe):
         import refdump
-        t1 = refdump.time_steps(case, 1, threads=ncores)
+        t1 = refdump.time_lam(WORKLOAD, 1, 1, threads=ncores)
         n = max(2, min(200, int(seconds_target / max(t1, 1e-3))))
-        t = refdump.time_steps(case, n, threads=ncores)
-        return {"value": pts * n / t, "unit": UNIT, "cores": ncores, "kind": "reference",
-                "sample": f"{n} RK3 steps of the {WORKLOAD['nx']}x{WORKLOAD['ny']}x{WORKLOAD['nz']} workload, "
-                          f"reference CPU FP64 build (oracle/_ref, OpenMP {ncores} threads), step loop only"}
+        t = refdump.time_lam(WORKLOAD, 1, n, threads=ncores)
+        return {"value": pts * n / t, "unit": UNIT, "cores": ncores, "kind": "reference", **host_description(),
+                "sample": f"{n} RK3 steps of the {WORKLOAD['nx']}x{WORKLOAD['ny']}x{WORKLOAD['nz']} workload (seed 1), "
+                          f"reference CPU FP64 build (oracle/_ref/ref_harness, OpenMP {ncores} threads, "
+                          "OMP_WAIT_POLICY=passive), step loop only"}
+    if capi is None:
+        from cppwrf_b200 import capi
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import _oracle
+    case = make_case(capi, capi.FP64)
     orc = _oracle.Oracle(case)
     t0 = time.perf_counter()
     orc.step(1)
@@ -182,19 +204,28 @@ def cpu_baseline(capi, seconds_target=15.0):
     t0 = time.perf_counter()
     orc.step(n)
     t = time.perf_counter() - t0
-    return {"value": pts * n / t, "unit": UNIT, "cores": 1, "kind": "port",
+    return {"value": pts * n / t, "unit": UNIT, "cores": 1, "kind": "port", **host_description(),
             "sample": f"{n} RK3 steps of the workload, the oracle (C restatement, 1 thread)"}
 
 
+def lam_config(precision, world):
+    """The `config` of the headline line: the same dict in both arms."""
+    return {"workload": f"lam_119x89x44_{precision}", **WORKLOAD, "moist_species": "qv qc qr qi qs (PD at rk 3)",
+            "lbc": "specified, width 5", "seed": 1, "parallelism": f"one domain per GPU x{world}",
+            "l2": "inputs larger than L2: ~110 fields x 5.4 MB per step, no flush"}
+
+
 def run_reference(args, rank):
+    """The reference arm: the reference's own CPU implementation of the path on this host's cores, for the same
+    workload, metric and config as our arm (rank 0 only; other ranks exit without work)."""
     if rank != 0:
         return 0
-    from cppwrf_b200 import capi
-    cb = cpu_baseline(capi, seconds_target=20.0)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    cb = cpu_baseline(seconds_target=20.0)
     line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "lam_119x89x44_fp64", **WORKLOAD}, "impl": "reference", "cpu_baseline": cb,
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (cw_gen_lam, seeded)",
+            "config": lam_config("fp64", world), "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     line["ms_per_step"] = 1000.0 * WORKLOAD["nx"] * WORKLOAD["ny"] * WORKLOAD["nz"] / cb["value"]
     print(json.dumps(line), flush=True)
@@ -510,7 +541,9 @@ def main():
     tag = f"lam119x89x44_{args.precision}"
     traffic = ncu_traffic(dom_name, tag)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": dom_name, "algorithmic_bytes_per_launch": alg_bytes,
+                "traffic": traffic, "traffic_source": f"the committed ncu summary profiles/{dom_name}_{tag}.md (not measured in "
+                                                     "this run)" if traffic is not None else None,
+                "kernel": dom_name, "algorithmic_bytes_per_launch": alg_bytes,
                 "avg_launch_ms": dom_ms / dom_n, "peak_source": peak_src,
                 "kernel_share": {r[0]: round(r[1] / total_ms, 4) for r in table[:8]}}
     # the whole step against the per-grid-point traffic model (4 416 B FP64 / 2 208 B FP32 per point-step)
@@ -522,20 +555,17 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if prec == capi.FP64 else "f32+f64",
             "data": "synthetic (cw_gen_lam, seeded)",
-            "config": {"workload": f"lam_119x89x44_{args.precision}", **WORKLOAD,
-                       "moist_species": "qv qc qr qi qs (PD at rk 3)", "lbc": "specified, width 5",
-                       "parallelism": f"one domain per GPU x{world}",
-                       "l2": "inputs larger than L2: ~110 fields x 5.4 MB per step, no flush",
-                       "block_shapes": {k: ["128x1", "64x2", "32x4"][dom.autotune_choice(k)]
-                                        for k in ("k_tend", "k_tendf_rk1", "k_uv", "k_q_update", "k_q_face_pd",
-                                                  "k_q_scale_pd", "k_q_update_pd", "k_p_rho_phi")
-                                        if dom.autotune_choice(k) >= 0}},
+            "config": lam_config(args.precision, world),
+            "block_shapes": {k: ["128x1", "64x2", "32x4"][dom.autotune_choice(k)]
+                             for k in ("k_tend", "k_tendf_rk1", "k_uv", "k_q_update", "k_q_face_pd",
+                                       "k_q_scale_pd", "k_q_update_pd", "k_p_rho_phi")
+                             if dom.autotune_choice(k) >= 0},
             "clocks": clocks, "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": ebytes,
                                       "d2h_bytes_per_step": ebytes, "steps": n_e2e},
             "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roofline}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_baseline(capi)
+            line["cpu_baseline"] = cpu_baseline(capi=capi)
         except Exception as e:  # noqa: BLE001 - reported, not fatal
             line["cpu_baseline"] = {"value": None, "error": str(e)}
     dom.close()

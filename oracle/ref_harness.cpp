@@ -1,8 +1,16 @@
 // SPDX-License-Identifier: GPL-3.0-or-later
 // TEST INFRASTRUCTURE ONLY: drives CPPWRF's own CPU FP64 dynamics step (its sources compiled by
-// oracle/Makefile into _ref/) on inputs written by tests/_refdump.py, and writes every field back.
+// oracle/Makefile into _ref/) on inputs written by oracle/refdump.py, and writes every field back.
 //
-//   ref_harness <input.bin> <output.bin>
+//   ref_harness <input.bin> <output.bin | --time>
+//   ref_harness --lam nx ny nz dx dt n_sound n_moist p_top hybrid_opt etac seed nsteps <output.bin | --time>
+//
+// The second form (ref_harness only, built with CW_HARNESS_LAM) makes the input in this process: a limited-area
+// case (specified boundaries, terrain, every species moist) from the repository's seeded generator (cw_gen_lam of
+// cppwrf_b200/csrc/cw_case.cpp, compiled into this program), serialised exactly as refdump.write_input serialises
+// it. The timed step loop is the reference's own RK3::step either way; nothing of the repository's dycore takes
+// part. ref_harness_own has no such form: its pow, sin, cos and log are interposed for the whole program, so the
+// generator would not compute what the product library's generator computes with glibc's.
 //
 // Input: the cw_grid and cw_options structs (include/cw_dycore.h), the vertical arrays, the whole
 // allocation of every State / Tendencies / BaseState field in CPPWRF's Layout (the same layout as this
@@ -65,15 +73,110 @@ void save(const real* base_ptr, const Layout& L) {
   std::fwrite(&n, sizeof n, 1, out_f);
   std::fwrite(base_ptr, sizeof(double), size_t(n), out_f);
 }
+
+#ifdef CW_HARNESS_LAM
+// the input bytes of a limited-area case made by cw_gen_lam, in refdump.write_input's order
+struct Bytes {
+  std::vector<char> b;
+  template <class T>
+  void put(const T& v) {
+    const char* p = reinterpret_cast<const char*>(&v);
+    b.insert(b.end(), p, p + sizeof(T));
+  }
+  void put_n(const double* p, size_t n) {
+    const char* c = reinterpret_cast<const char*>(p);
+    b.insert(b.end(), c, c + n * sizeof(double));
+  }
+};
+void check_rc(int rc, const char* what) {
+  if (rc != 0) throw std::runtime_error(std::string(what) + " failed");
+}
+std::vector<char> lam_input(char** a) {
+  cw_grid g{};
+  g.nx = std::atoi(a[0]); g.ny = std::atoi(a[1]); g.nz = std::atoi(a[2]);
+  g.dx = g.dy = std::atof(a[3]); g.dt = std::atof(a[4]); g.ztop = 0.0; g.p_top = std::atof(a[7]);
+  g.bc_x = g.bc_y = CW_BC_SPECIFIED;
+  cw_options o{};
+  check_rc(cw_default_options(&o), "cw_default_options");
+  o.flat = 0; o.lbc = 1; o.precision = CW_FP64;
+  o.time_step_sound = std::atoi(a[5]);
+  o.n_moist = o.n_scalars = std::atoi(a[6]);
+  cw_lam_params p{};
+  check_rc(cw_default_lam_params(&p), "cw_default_lam_params");
+  p.hybrid_opt = std::atoi(a[8]); p.etac = std::atof(a[9]); p.seed = std::strtoull(a[10], nullptr, 10);
+  const int nsteps = std::atoi(a[11]);
+  cw_case* c = nullptr;
+  check_rc(cw_case_create(&g, &o, &c), "cw_case_create");
+  std::unique_ptr<cw_case, int (*)(cw_case*)> own(c, cw_case_destroy);
+  check_rc(cw_gen_lam(c, &p), "cw_gen_lam");
+  check_rc(cw_case_config(c, &g, &o), "cw_case_config");
+  cw_vertical v{};
+  check_rc(cw_case_vertical(c, &v), "cw_case_vertical");
+  g.p_top = v.p_top;  // the generator sets the model top
+  Bytes B;
+  B.put(g);
+  B.put(o);
+  const int nz = g.nz;
+  const std::vector<double> zeros(size_t(nz) + 1, 0.0);
+  auto arr = [&](const double* x, int n) { B.put_n(x ? x : zeros.data(), size_t(n)); };
+  for (const double* x : {v.znu, v.dnw, v.rdnw, v.c1h, v.c2h, v.c3h, v.c4h}) arr(x, nz);
+  for (const double* x : {v.znw, v.dn, v.rdn, v.fnm, v.fnp, v.c1f, v.c2f, v.c3f, v.c4f}) arr(x, nz + 1);
+  for (const double* x : {v.u_base, v.v_base, v.t_base, v.qv_base_1d, v.z_base}) arr(x, nz);
+  for (double x : {v.cf1, v.cf2, v.cf3, v.cfn, v.cfn1, v.rdx, v.rdy, v.p_top, v.t0}) B.put(x);
+  auto field = [&](int id, int n) {
+    double* d = nullptr;
+    cw_layout L{};
+    check_rc(cw_case_field(c, id, n, &d, &L), "cw_case_field");
+    B.put(int64_t(L.total));
+    B.put_n(d, size_t(L.total));
+  };
+  for (int id = 0; id < CW_Q_1; ++id) field(id, 0);
+  for (int n = 0; n < o.n_scalars; ++n)
+    for (int id : {CW_Q_1, CW_Q_2, CW_Q_TENDF}) field(id, n);
+  for (int scalar = 0; scalar < 2; ++scalar)
+    for (int var = 0; var < (scalar ? o.n_scalars : 5); ++var)
+      for (int side = 0; side < 4; ++side) {
+        double *vals = nullptr, *tends = nullptr;
+        size_t cnt = 0;
+        if (cw_case_lbc(c, scalar, var, side, &vals, &tends, &cnt) != 0) {
+          if (!scalar) throw std::runtime_error("cw_case_lbc failed");
+          B.put(int64_t(0));
+          continue;
+        }
+        B.put(int64_t(cnt));
+        B.put_n(vals, cnt);
+        B.put_n(tends, cnt);
+      }
+  double dtbc = 0;
+  check_rc(cw_case_lbc_time(c, &dtbc), "cw_case_lbc_time");
+  B.put(dtbc);
+  B.put(int32_t(nsteps));
+  return std::move(B.b);
+}
+#else
+std::vector<char> lam_input(char**) { throw std::runtime_error("--lam: built without the case generator"); }
+#endif
 }  // namespace
 
 int main(int argc, char** argv) {
-  if (argc != 3 && argc != 4) {
-    std::fprintf(stderr, "usage: ref_harness input.bin output.bin [--time]\n");
+  const bool gen = argc >= 2 && std::strcmp(argv[1], "--lam") == 0;
+  if (gen ? argc != 15 : (argc != 3 && argc != 4)) {
+    std::fprintf(stderr,
+                 "usage: ref_harness input.bin output.bin [--time]\n"
+                 "       ref_harness --lam nx ny nz dx dt n_sound n_moist p_top hybrid_opt etac seed nsteps <output.bin|--time>\n");
     return 2;
   }
+  // the output path, or timing only (the step loop's wall time, no output)
+  const char* out_path = gen ? argv[14] : argv[2];
+  const bool time_only = gen ? std::strcmp(argv[14], "--time") == 0 : argc == 4;
   try {
-    in_f = std::fopen(argv[1], "rb");
+    std::vector<char> generated;
+    if (gen) {
+      generated = lam_input(argv + 2);
+      in_f = fmemopen(generated.data(), generated.size(), "rb");
+    } else {
+      in_f = std::fopen(argv[1], "rb");
+    }
     if (!in_f) throw std::runtime_error("cannot open input");
     const cw_grid cg = rd<cw_grid>();
     const cw_options co = rd<cw_options>();
@@ -207,11 +310,11 @@ int main(int argc, char** argv) {
     const auto t0 = std::chrono::steady_clock::now();
     for (int n = 0; n < nsteps; ++n) rk.step(s, t, b);
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    if (argc == 4) {  // timing only: the step loop's wall time, no output
+    if (time_only) {
       std::printf("STEP_SECONDS %.9f\n", secs);
       return 0;
     }
-    out_f = std::fopen(argv[2], "wb");
+    out_f = std::fopen(out_path, "wb");
     if (!out_f) throw std::runtime_error("cannot open output");
     each_field([&](real* p, const Layout& L) { save(p, L); }, [&](const real* p, const Layout& L) { save(p, L); },
                [&] {

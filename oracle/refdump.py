@@ -100,22 +100,61 @@ def time_steps(case, nsteps, threads=None, own_pow=False):
     raise RuntimeError("ref_harness printed no STEP_SECONDS")
 
 
+def lam_args(w, seed, nsteps):
+    """ref_harness --lam arguments of a limited-area case of shape w (nx ny nz dx dt time_step_sound n_moist p_top
+    hybrid_opt etac) made by the repository's seeded generator inside the harness, and nsteps."""
+    return ["--lam", str(w["nx"]), str(w["ny"]), str(w["nz"]), repr(float(w["dx"])), repr(float(w["dt"])),
+            str(w["time_step_sound"]), str(w["n_moist"]), repr(float(w["p_top"])), str(w["hybrid_opt"]),
+            repr(float(w["etac"])), str(int(seed)), str(int(nsteps))]
+
+
+def time_lam(w, seed, nsteps, threads=None):
+    """Wall seconds of the reference's step loop (the unmodified build, glibc's math) on a limited-area case
+    generated inside the harness: no Python-side input and no library of this repository in the calling process."""
+    exe = os.path.join(REF_DIR, "ref_harness")
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+    env.setdefault("OMP_WAIT_POLICY", "passive")
+    r = subprocess.run([exe] + lam_args(w, seed, nsteps) + ["--time"], check=True, capture_output=True, text=True,
+                       env=env)
+    for line in r.stdout.splitlines():
+        if line.startswith("STEP_SECONDS"):
+            return float(line.split()[1])
+    raise RuntimeError("ref_harness printed no STEP_SECONDS")
+
+
+def _read_output(fout, n_scalars):
+    names = [n for n in capi.FIELDS if not n.startswith("Q_")]
+    out = {}
+    with open(fout, "rb") as f:
+        for name in names:
+            (n,) = struct.unpack("<q", f.read(8))
+            out[name] = np.frombuffer(f.read(8 * n), dtype="<f8").copy()
+        for q in range(n_scalars):
+            for name in ("Q_1", "Q_2", "Q_TENDF"):
+                (n,) = struct.unpack("<q", f.read(8))
+                out[f"{name}:{q}"] = np.frombuffer(f.read(8 * n), dtype="<f8").copy()
+    return out
+
+
+def run_lam(w, seed, nsteps):
+    """{field name: whole allocation} of the reference (the unmodified build) after nsteps on the case
+    ref_harness --lam generates."""
+    build()
+    exe = os.path.join(REF_DIR, "ref_harness")
+    with tempfile.TemporaryDirectory() as td:
+        fout = os.path.join(td, "out.bin")
+        subprocess.run([exe] + lam_args(w, seed, nsteps) + [fout], check=True)
+        return _read_output(fout, int(w["n_moist"]))
+
+
 def run(case, nsteps, own_pow=True):
     """{field name: whole allocation} of the reference after nsteps (Q_* keyed 'Q_2:n')."""
     build()
     exe = os.path.join(REF_DIR, "ref_harness_own" if own_pow else "ref_harness")
-    names = [n for n in capi.FIELDS if not n.startswith("Q_")]
     with tempfile.TemporaryDirectory() as td:
         fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
         write_input(case, nsteps, fin)
         subprocess.run([exe, fin, fout], check=True)
-        out = {}
-        with open(fout, "rb") as f:
-            for name in names:
-                (n,) = struct.unpack("<q", f.read(8))
-                out[name] = np.frombuffer(f.read(8 * n), dtype="<f8").copy()
-            for q in range(case.o.n_scalars):
-                for name in ("Q_1", "Q_2", "Q_TENDF"):
-                    (n,) = struct.unpack("<q", f.read(8))
-                    out[f"{name}:{q}"] = np.frombuffer(f.read(8 * n), dtype="<f8").copy()
-        return out
+        return _read_output(fout, case.o.n_scalars)

@@ -1,0 +1,94 @@
+# SPDX-License-Identifier: GPL-3.0-or-later
+"""Parity on the benchmark configurations as they are stated, through the C ABI:
+
+- the 2-D density current (Straka 256 x 1 x 64, dt 1 s, 6 acoustic substeps, K = 75 m^2/s) over its whole
+  900 s: every field of the GPU FP64 form bit-identical to the oracle (pow = cw_pow on both sides);
+- the 3-D limited-area workload (119 x 89 x 44, bench.py) for 20 steps: every field of the GPU FP64 form
+  bit-identical to the reference's own CPU FP64 build (oracle/_ref/ref_harness_own, pow interposed by cw_pow),
+  with no oracle in between;
+- the precision form on the same workload after 1 h (40 steps of 90 s): relative L2 <= 1e-4 against the FP64
+  form for u, v, w, theta, phi', mu' and qv on the interior points, max-abs reported."""
+import numpy as np
+import pytest
+
+import _oracle
+import _refpath  # noqa: F401
+import refdump as _refdump
+import cases
+from cppwrf_b200 import Domain, capi
+
+pytestmark = pytest.mark.gpu
+
+# relative L2 bound of the precision form against the FP64 form after 1 h, per prognostic
+MIXED_REL_L2_1H = 1e-4
+PROGNOSTICS = {"u": ("U_2", 0), "v": ("V_2", 0), "w": ("W_2", 0), "theta": ("T_2", 0), "phi'": ("PH_2", 0),
+               "mu'": ("MU_2", 0), "qv": ("Q_2", 0)}
+
+
+def _diff(name, a, b):
+    if np.array_equal(a.view(np.uint64), b.view(np.uint64)):
+        return None
+    d = np.nonzero(a.view(np.uint64) != b.view(np.uint64))[0]
+    return f"{name}: {d.size} differ, first at {d[0]}: gpu {a[d[0]]!r} other {b[d[0]]!r}"
+
+
+def test_density_current_900s_bit_exact_with_oracle():
+    cfg = dict(cases.golden_config("straka"), nx=256, run_time=900.0)
+    case = cases.ideal_case(cfg)
+    n = int(round(cfg["run_time"] / cfg["dt"]))
+    dom = Domain(case.g, case.o).upload_case(case)
+    assert dom.n_sound() == 6
+    dom.step(n)
+    dom.sync()
+    orc = _oracle.Oracle(case, pow_mode=_oracle.POW_OWN)
+    orc.step(n)
+    bad = [m for m in (_diff(x, dom.field(x), orc.array(x)) for x in capi.FIELDS if not x.startswith("Q_")) if m]
+    assert not bad, "\n".join(bad)
+    # the cold pool is still there after 900 s (mixed by K = 75 m^2/s from its initial -15 K)
+    t = capi.interior(dom.field("T_2"), dom.layout("T_2"))
+    assert -15.0 < t.min() < -5.0
+
+
+@pytest.mark.skipif(not _refdump.available(), reason="oracle/_ref (the reference's CPU build) not present")
+def test_benchmark_workload_20_steps_bit_exact_with_reference_build():
+    import bench
+    case = bench.make_case(capi, capi.FP64)
+    dom = Domain(case.g, case.o).upload_case(case)
+    dom.step(20)
+    dom.sync()
+    ref = _refdump.run(case, 20, own_pow=True)
+    bad = []
+    for name in [x for x in capi.FIELDS if not x.startswith("Q_")]:
+        if ref[name].size == 0:
+            continue
+        m = _diff(name, dom.field(name), ref[name])
+        if m:
+            bad.append(m)
+    for n in range(case.o.n_scalars):
+        for name in ("Q_1", "Q_2", "Q_TENDF"):
+            m = _diff(f"{name}[{n}]", dom.field(name, n), ref[f"{name}:{n}"])
+            if m:
+                bad.append(m)
+    assert not bad, "\n".join(bad)
+
+
+def test_precision_form_within_1e4_after_one_hour():
+    import bench
+    steps = int(round(3600.0 / bench.WORKLOAD["dt"]))
+    doms = {}
+    for prec in (capi.FP64, capi.MIXED):
+        case = bench.make_case(capi, prec)
+        doms[prec] = Domain(case.g, case.o).upload_case(case)
+        doms[prec].step(steps)
+        doms[prec].sync()
+    report, bad = {}, []
+    for key, (name, n) in PROGNOSTICS.items():
+        L = doms[capi.FP64].layout(name, n)
+        a = capi.interior(doms[capi.MIXED].field(name, n), L)
+        b = capi.interior(doms[capi.FP64].field(name, n), L)
+        rel = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        report[key] = (rel, float(np.max(np.abs(a - b))))
+        if not (np.all(np.isfinite(a)) and rel <= MIXED_REL_L2_1H):
+            bad.append(f"{key}: relative L2 {rel:.3e}, max abs {report[key][1]:.3e}")
+    print("mixed vs FP64 after 1 h (rel L2, max abs):", report)
+    assert not bad, "\n".join(bad)

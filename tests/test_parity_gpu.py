@@ -252,3 +252,20 @@ def test_benchmark_workload_bit_exact():
     dom, orc = run_pair(case, 2)
     bad = compare_all(dom, orc, case, names=capi.STATE_FIELDS)
     assert not bad, "\n".join(bad)
+
+
+def test_launch_count_gates_the_plain_scalar_update():
+    """At rk 3 the plain scalar update runs only when some species is not PD: a case whose species are all PD
+    takes one launch less per step than the same case with one plain tracer (the count of the step's launches,
+    the same graph or eager)."""
+    pd = lam_case(n_moist=2, n_scalars=2)
+    mixed = lam_case(n_moist=2, n_scalars=3)
+    pd.o.scalar_adv_opt = mixed.o.scalar_adv_opt = 0  # the third species of `mixed` is a plain tracer
+    assert pd.o.moist_adv_opt == 1 and mixed.o.moist_adv_opt == 1
+    counts = []
+    for case in (pd, mixed):
+        dom = Domain(case.g, case.o).upload_case(case)
+        dom.step(1)
+        dom.sync()
+        counts.append(dom.launches())
+    assert counts[1] == counts[0] + 1, counts
