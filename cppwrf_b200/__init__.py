@@ -210,12 +210,14 @@ class Server:
     """The served form (include/cw_serve.h): a C++ request loop on its own thread that admits requests by
     device-memory footprint, keeps them resident and advances them together in batched steps."""
 
-    def __init__(self, budget_bytes=150e9, max_resident=256, precision=MIXED, device=0, keep_results=True, lib=None):
+    def __init__(self, budget_bytes=150e9, max_resident=256, precision=MIXED, device=0, keep_results=True, lib=None,
+                 test_fail_creates=0):
         self.lib = lib or capi.load()
         cfg = capi.ServeConfig()
         self.lib.cw_serve_default_config(C.byref(cfg))
         cfg.hbm_budget_bytes, cfg.max_resident, cfg.precision = float(budget_bytes), int(max_resident), int(precision)
         cfg.device, cfg.keep_results = int(device), 1 if keep_results else 0
+        cfg.test_fail_creates = int(test_fail_creates)
         self.h = C.c_void_p()
         rc = self.lib.cw_serve_create(C.byref(cfg), C.byref(self.h))
         if rc != 0:

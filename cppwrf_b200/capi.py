@@ -94,7 +94,7 @@ class LamParams(C.Structure):
 
 class ServeConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_double), ("max_resident", C.c_int), ("precision", C.c_int),
-                ("device", C.c_int), ("keep_results", C.c_int)]
+                ("device", C.c_int), ("keep_results", C.c_int), ("test_fail_creates", C.c_int)]
 
 
 class ServeStats(C.Structure):
@@ -181,6 +181,8 @@ def load(path=None):
         "cw_batch_adopt": (i, [vp, vp, ip]),
         "cw_set_autotune": (i, [vp, i]),
         "cw_check_finite": (i, [vp, i, ip, ip, ip, ip, ip]),
+        "cw_batch_release": (i, [vp, i, C.POINTER(vp)]),
+        "cw_check_div_const": (i, [C.c_ulonglong, C.c_ulonglong, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]),
         "cw_autotune_choice": (i, [vp, C.c_char_p, ip]),
         "cw_footprint": (i, [C.POINTER(Grid), C.POINTER(Options), C.POINTER(sz)]),
         "cw_case_clone": (i, [vp, C.POINTER(vp)]),

@@ -12,6 +12,7 @@
 #include <utility>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -86,10 +87,22 @@ struct Packs {
 };
 template <class R>
 struct DevTables {  // the kernels' views of the members and the device scalar tables
-  Packs<R, 1> one;              // a single domain
-  Packs<R, kPackMembers> many;  // a batch, in packs of kPackMembers
+  Packs<R, 1> one;   // a single domain
+  Packs<R, 0> many;  // a batch: one pack over every member, its descriptors in device memory
   V3<R>* qtab = nullptr;  // per member: q1, q2, qn, qtf, qscale, 6 PD faces (kQTab x n_scalars)
   Slabs<R>* lbcq = nullptr;
+  Dom<R>* doms_d = nullptr;  // the batch's member descriptors
+  int* starts_d = nullptr;   // the batch's block starts [kind][shape][member]
+};
+
+// a fill point's fields (or the union of consecutive fill points') as a device table: one launch per pass
+// whatever the number of fields (the batch path)
+struct HaloTable {
+  HaloField* f = nullptr;
+  unsigned* start = nullptr;
+  int nf = 0;
+  unsigned total = 0;
+  int has_oddface = 0;
 };
 
 struct HaloSetHost {
@@ -124,6 +137,7 @@ struct cw_handle {
   enum { H_MU1, H_PREP0, H_PREP1, H_SS0, H_UV, H_AC, H_POST, H_FIN, H_Q1PD, H_SCPD, H_Q2, H_END_P, H_WS0, H_WS1, H_MP,
          H_MP_P, H_XK, H_N };
   HaloSetHost hs[H_N];
+  std::map<std::vector<int>, HaloTable> halo_tabs;  // batch: device tables of the fill points met while enqueuing
   std::vector<CopyDesc> copies;
   CopyDesc* copies_d = nullptr;
   long long* copies_start_d = nullptr;
@@ -175,7 +189,8 @@ void chunk_fields(const std::vector<HaloField>& f, std::vector<HaloChunk<NF>>& o
   }
 }
 
-// the mixed form's step (cw_step_mixed.cu): enqueues one step of h on its stream, returns the launches
-long long enqueue_mixed(cw_handle* h);
+// the mixed form's step (cw_step_mixed.cu): enqueues one step of h on its stream (plan: no launch, only the
+// tables the launches need), returns the launches
+long long enqueue_mixed(cw_handle* h, bool plan);
 
 }  // namespace cw

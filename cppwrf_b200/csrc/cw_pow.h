@@ -341,4 +341,21 @@ CW_HD double cw_cos(double x) {
   return CW_ADD(ah, al);
 }
 
+/* x / c correctly rounded (the IEEE quotient, bit for bit) for a positive constant c without a division, given
+ * r = RN(1/c) (Markstein, "Computation of elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+ * Dev. 34, 1990; Muller et al., Handbook of Floating-Point Arithmetic, 2nd ed., 2018, section 4.9): q = RN(x r) is
+ * within one ulp of x / c, so the remainder x - q c is a double and one fused multiply-add computes it exactly,
+ * and RN(q + rem r) is then the correctly rounded quotient. The theorem needs the remainder to stay normal and the
+ * operands finite; outside 2^-960 <= |x| <= 2^1020 (zeros, whose sign the correction would not keep; values whose
+ * remainder could underflow; infinities, NaN) the IEEE division is taken. The flux statement functions divide by
+ * 60 and 12 this way; tests/test_div_const.py compares it with the division bit for bit on the host (and the GPU
+ * self-check cw_check_div_const on the device). */
+CW_HD double cw_div_const(double x, double c, double r) {
+  const double ax = fabs(x);
+  if (!(ax >= 0x1p-960 && ax <= 0x1p+1020)) return CW_DIV(x, c);
+  const double q = CW_MUL(x, r);
+  const double rem = CW_FMA(-q, c, x);
+  return CW_FMA(rem, r, q);
+}
+
 #endif /* CW_POW_H */

@@ -231,32 +231,58 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   return D;
 }
 
-// the members in packs of NM (a single domain: NM = 1; a batch: kPackMembers, the last pack partial)
-template <class R, int NM>
-void build_packs(cw_handle* h, const std::vector<Dom<R>>& doms, Packs<R, NM>& ps) {
+// member m's first block of each index range and block shape, and each range's block total
+template <class SET>
+std::array<std::array<int, kNumShapes>, kNumKinds> block_starts(cw_handle* h, size_t m0, int n, SET set) {
+  std::array<std::array<int, kNumShapes>, kNumKinds> tot{};
+  for (int kind = 0; kind < kNumKinds; ++kind)
+    for (int sh = 0; sh < kNumShapes; ++sh) {
+      long long b = 0;
+      for (int m = 0; m < n; ++m) {
+        const Member& M = h->m[m0 + size_t(m)];
+        set(kind, sh, m, int(b));
+        b += blocks_of(kind, M.g.nx, M.g.ny, M.g.nz, nys(M.g, 'V'), sh);
+      }
+      if (b >= (1ll << 31)) throw std::runtime_error("a batch launch of more than 2^31 blocks");
+      set(kind, sh, n, int(b));
+      tot[size_t(kind)][size_t(sh)] = int(b);
+    }
+  return tot;
+}
+// a single domain: its descriptor in the launch parameter
+template <class R>
+void build_packs(cw_handle* h, const std::vector<Dom<R>>& doms, Packs<R, 1>& ps) {
+  ps.p.clear();
+  ps.blocks.clear();
+  if (doms.size() != 1) return;
+  Pack<R, 1> P{};
+  P.n = 1;
+  P.d[0] = doms[0];
+  ps.blocks.push_back(block_starts(h, 0, 1, [&](int kind, int sh, int m, int b) { P.start_[kind][sh][m] = b; }));
+  ps.p.push_back(P);
+}
+// a batch: every member's descriptor and block starts in device memory, one pack (one launch per kernel)
+template <class R>
+void build_packs(cw_handle* h, const std::vector<Dom<R>>& doms, DevTables<R>& T) {
+  Packs<R, 0>& ps = T.many;
   ps.p.clear();
   ps.blocks.clear();
   const size_t nm = doms.size();
-  if ((NM == 1) != (nm == 1)) return;
-  for (size_t m0 = 0; m0 < nm; m0 += NM) {
-    Pack<R, NM> P{};
-    P.n = int(std::min(nm - m0, size_t(NM)));
-    std::array<std::array<int, kNumShapes>, kNumKinds> tot{};
-    for (int kind = 0; kind < kNumKinds; ++kind)
-      for (int sh = 0; sh < kNumShapes; ++sh) {
-        int b = 0;
-        for (int m = 0; m < P.n; ++m) {
-          const Member& M = h->m[m0 + size_t(m)];
-          P.start[kind][sh][m] = b;
-          b += blocks_of(kind, M.g.nx, M.g.ny, M.g.nz, nys(M.g, 'V'), sh);
-        }
-        P.start[kind][sh][P.n] = b;
-        tot[size_t(kind)][size_t(sh)] = b;
-      }
-    for (int m = 0; m < P.n; ++m) P.d[m] = doms[m0 + size_t(m)];
-    ps.p.push_back(P);
-    ps.blocks.push_back(tot);
-  }
+  if (nm <= 1) return;
+  std::vector<int> st(size_t(kNumKinds * kNumShapes) * (nm + 1));
+  ps.blocks.push_back(block_starts(h, 0, int(nm), [&](int kind, int sh, int m, int b) {
+    st[size_t(kind * kNumShapes + sh) * (nm + 1) + size_t(m)] = b;
+  }));
+  CW_CUDA(cudaMalloc(&T.doms_d, nm * sizeof(Dom<R>)));
+  CW_CUDA(cudaMalloc(&T.starts_d, st.size() * sizeof(int)));
+  CW_CUDA(cudaMemcpyAsync(T.doms_d, doms.data(), nm * sizeof(Dom<R>), cudaMemcpyHostToDevice, h->stream));
+  CW_CUDA(cudaMemcpyAsync(T.starts_d, st.data(), st.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  CW_CUDA(cudaStreamSynchronize(h->stream));  // the host vectors go out of scope
+  Pack<R, 0> P{};
+  P.d = T.doms_d;
+  P.starts = T.starts_d;
+  P.n = int(nm);
+  ps.p.push_back(P);
 }
 
 template <class R>
@@ -302,7 +328,7 @@ void upload_tables(cw_handle* h, DevTables<R>& T) {
     q0 += size_t(ns);
   }
   build_packs(h, doms, T.one);
-  build_packs(h, doms, T.many);
+  build_packs(h, doms, T);
   std::vector<double> dtbc(nm);
   for (size_t mi = 0; mi < nm; ++mi) dtbc[mi] = h->m[mi].dtbc;
   CW_CUDA(cudaMemcpyAsync(h->dtbc_d, dtbc.data(), nm * sizeof(double), cudaMemcpyHostToDevice, h->stream));
@@ -453,7 +479,7 @@ void build_copies(cw_handle* h) {
 // cw_step_mixed.cu, compiled with its own floating-point options
 void enqueue(cw_handle* h, Launcher& L) {
   if (h->precision == CW_FP64) enqueue_t<double>(h, L, h->t64);
-  else L.count += enqueue_mixed(h);
+  else L.count += enqueue_mixed(h, L.plan);
 }
 
 void invalidate_graph(cw_handle* h) {
@@ -526,6 +552,11 @@ void run_steps(cw_handle* h, int nsteps) {
   }
   if (nsteps == 0) return;
   if (h->use_graph && !h->graph_ok) {
+    if (h->m.size() > 1) {  // a batch's halo tables are device allocations: made before the capture
+      Launcher P{h};
+      P.plan = true;
+      enqueue(h, P);
+    }
     Launcher L{h};
     CW_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     try {
@@ -572,6 +603,11 @@ Member make_member(const cw_grid& g, const cw_options& o) {
 // they are rebuilt for a new set of members
 void free_tables(cw_handle* h) {
   for (auto& hs : h->hs) hs = HaloSetHost{};
+  for (auto& kv : h->halo_tabs) {
+    cudaFree(kv.second.f);
+    cudaFree(kv.second.start);
+  }
+  h->halo_tabs.clear();
   cudaFree(h->copies_d);
   cudaFree(h->copies_start_d);
   cudaFree(h->zeros_d);
@@ -587,8 +623,12 @@ void free_tables(cw_handle* h) {
   h->cfl_d = nullptr;
   cudaFree(h->t64.qtab);
   cudaFree(h->t64.lbcq);
+  cudaFree(h->t64.doms_d);
+  cudaFree(h->t64.starts_d);
   cudaFree(h->t32.qtab);
   cudaFree(h->t32.lbcq);
+  cudaFree(h->t32.doms_d);
+  cudaFree(h->t32.starts_d);
   h->t64 = DevTables<double>{};
   h->t32 = DevTables<float>{};
 }
@@ -742,6 +782,46 @@ void diagnostics_t(cw_handle* h, int mi, DevTables<R>& T, cw_diag* out) {
 
 }  // namespace
 
+// cw_check_div_const: cw_div_const against __ddiv_rn for c = 60 and 12 on n operands each (the kinds of
+// tests/div_const_check.c); counts[0] = checked, counts[1] = mismatches
+__device__ __forceinline__ unsigned long long dc_mix(unsigned long long z) {  // splitmix64's output function
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__global__ void k_check_div_const(unsigned long long n, unsigned long long seed, unsigned long long* counts) {
+  unsigned long long bad = 0, done = 0;
+  const unsigned long long stride = static_cast<unsigned long long>(gridDim.x) * blockDim.x;
+  for (unsigned long long t = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; t < n; t += stride) {
+    const unsigned long long u = dc_mix(seed + 0x9E3779B97F4A7C15ull * (2 * t + 1));
+    const unsigned long long v = dc_mix(seed + 0x9E3779B97F4A7C15ull * (2 * t + 2));
+    for (int ci = 0; ci < 2; ++ci) {
+      const double c = ci == 0 ? 60.0 : 12.0, r = ci == 0 ? 1.0 / 60.0 : 1.0 / 12.0;
+      double x;
+      const int kind = int(t % 3);
+      if (kind == 0) {
+        x = __longlong_as_double((long long)u);
+      } else if (kind == 1) {
+        const unsigned long long e = 1023ull - 900ull + v % 1801ull;
+        const double q = __longlong_as_double((long long)((u & 0x800FFFFFFFFFFFFFull) | (e << 52)));
+        const double ulp = nextafter(fabs(q), __longlong_as_double(0x7FF0000000000000ll)) - fabs(q);
+        x = __fma_rn(c, q, copysign(__dmul_rn(__dmul_rn(c, ulp), 0.5), q));
+      } else {
+        const long long m = (long long)(v % 2000001ull) - 1000000ll;
+        x = (u & 1) ? double(m) : __dmul_rn(c, double(m));
+        const int steps = int((u >> 1) % 5) - 2;
+        for (int k = 0; k < (steps < 0 ? -steps : steps); ++k)
+          x = nextafter(x, steps < 0 ? -__longlong_as_double(0x7FF0000000000000ll) : __longlong_as_double(0x7FF0000000000000ll));
+      }
+      const double a = cw_div_const(x, c, r), b = __ddiv_rn(x, c);
+      ++done;
+      if (__double_as_longlong(a) != __double_as_longlong(b) && !(isnan(a) && isnan(b))) ++bad;
+    }
+  }
+  atomicAdd(counts, done);
+  if (bad) atomicAdd(counts + 1, bad);
+}
+
 // ------------------------------------------------------------------ C ABI
 extern "C" {
 
@@ -815,6 +895,26 @@ int cw_batch_adopt(cw_handle* h, cw_handle* single, int* member) {
     single->m.clear();
     rebuild(h);
     if (member) *member = int(h->m.size()) - 1;
+    return 0;
+  });
+}
+
+int cw_batch_release(cw_handle* h, int member, cw_handle** out) {
+  return guarded(h, [&] {
+    if (!h || !out || member < 0 || member >= int(h->m.size())) throw std::runtime_error("member index out of range");
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+    auto s = std::make_unique<cw_handle>();
+    s->precision = h->precision;
+    s->device = h->device;
+    CW_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    s->own_stream = true;
+    invalidate_graph(h);
+    free_tables(h);
+    s->m.push_back(std::move(h->m[size_t(member)]));  // the domain's allocation changes hands, its contents stay
+    h->m.erase(h->m.begin() + member);
+    build_tables(h);
+    build_tables(s.get());
+    *out = s.release();
     return 0;
   });
 }
@@ -1168,6 +1268,27 @@ int cw_profile_entry(cw_handle* h, int idx, char* name, int len, double* ms, lon
   if (launches) *launches = h->prof_n[idx];
   return 0;
 }
+int cw_check_div_const(unsigned long long n, unsigned long long seed, unsigned long long* checked,
+                       unsigned long long* mismatches) {
+  return guarded(nullptr, [&] {
+    if (!checked || !mismatches) throw std::runtime_error("null argument");
+    unsigned long long* d = nullptr;
+    CW_CUDA(cudaMalloc(&d, 2 * sizeof(unsigned long long)));
+    cudaError_t e = cudaMemset(d, 0, 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess) {
+      k_check_div_const<<<148 * 8, 256>>>(n, seed, d);
+      e = cudaGetLastError();
+    }
+    unsigned long long hc[2] = {0, 0};
+    if (e == cudaSuccess) e = cudaMemcpy(hc, d, sizeof hc, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    CW_CUDA(e);
+    *checked = hc[0];
+    *mismatches = hc[1];
+    return 0;
+  });
+}
+
 int cw_check_finite(cw_handle* h, int mi, int* field, int* n, int* i, int* j, int* k) {
   return guarded(h, [&] {
     if (!h || mi < 0 || mi >= int(h->m.size())) throw std::runtime_error("member index out of range");

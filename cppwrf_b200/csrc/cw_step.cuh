@@ -15,6 +15,8 @@ using namespace cw;
 
 struct Launcher {
   cw_handle* h;
+  // plan: enqueue without launching, to make the batch's halo tables (device allocations) before a graph capture
+  bool plan = false;
   long long count = 0;
   cudaEvent_t ev0 = nullptr;
   void begin(const char* name) {
@@ -33,6 +35,7 @@ struct Launcher {
   }
   template <int NF>
   void halo_chunks(const std::vector<HaloChunk<NF>>& chunks) {
+    if (plan) return;
     for (const HaloChunk<NF>& c : chunks) {
       const unsigned total = c.start[c.nf];
       if (total == 0) continue;
@@ -52,19 +55,62 @@ struct Launcher {
   // them) become one launch over the union of their fields
   std::vector<int> pend;
   void halo(int set) { pend.push_back(set); }
+  // the union of the pending fill points' fields (each field once, first occurrence order)
+  std::vector<HaloField> pending_fields() const {
+    std::vector<HaloField> f;
+    for (int set : pend)
+      for (const HaloField& x : h->hs[set].f) {
+        bool dup = false;
+        for (const HaloField& y : f) dup |= y.p == x.p && y.ind == x.ind;
+        if (!dup) f.push_back(x);
+      }
+    return f;
+  }
+  // a batch: the pending fill points as one device table (made on first use, kept with the handle's tables)
+  const HaloTable& halo_table() {
+    auto it = h->halo_tabs.find(pend);
+    if (it != h->halo_tabs.end()) return it->second;
+    const std::vector<HaloField> f = pending_fields();
+    std::vector<unsigned> st(f.size() + 1);
+    long long total = 0;
+    HaloTable t;
+    for (size_t n = 0; n < f.size(); ++n) {
+      st[n] = unsigned(total);
+      total += f[n].ncell;
+      t.has_oddface |= f[n].oddface_x;
+    }
+    if (total >= (1ll << 31)) throw std::runtime_error("a halo fill of more than 2^31 cells");
+    st[f.size()] = unsigned(total);
+    t.nf = int(f.size());
+    t.total = unsigned(total);
+    if (t.nf > 0) {
+      CW_CUDA(cudaMalloc(&t.f, f.size() * sizeof(HaloField)));
+      CW_CUDA(cudaMalloc(&t.start, st.size() * sizeof(unsigned)));
+      CW_CUDA(cudaMemcpy(t.f, f.data(), f.size() * sizeof(HaloField), cudaMemcpyHostToDevice));
+      CW_CUDA(cudaMemcpy(t.start, st.data(), st.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+    }
+    return h->halo_tabs.emplace(pend, t).first->second;
+  }
   void flush() {
     if (pend.empty()) return;
+    if (h->m.size() > 1) {
+      const HaloTable& t = halo_table();
+      if (t.total > 0 && !plan) {
+        const unsigned nb = (t.total + 255u) / 256u;
+        for (int pass = 0; pass < (t.has_oddface ? 2 : 1); ++pass) {
+          begin("k_halo");
+          k_halo_tab<<<nb, 256, 0, h->stream>>>(t.f, t.start, t.nf, pass);
+          check();
+        }
+      }
+      pend.clear();
+      return;
+    }
     if (pend.size() == 1) {
       halo_chunks(h->hs[pend[0]].small);
       halo_chunks(h->hs[pend[0]].large);
     } else {
-      std::vector<HaloField> f;
-      for (int set : pend)
-        for (const HaloField& x : h->hs[set].f) {
-          bool dup = false;
-          for (const HaloField& y : f) dup |= y.p == x.p && y.ind == x.ind;
-          if (!dup) f.push_back(x);
-        }
+      const std::vector<HaloField> f = pending_fields();
       if (f.size() <= size_t(kHaloSmall)) {
         std::vector<HaloChunk<kHaloSmall>> c;
         chunk_fields(f, c);
@@ -79,7 +125,7 @@ struct Launcher {
   }
   void copy_list(CopyDesc* d, long long* sd, size_t n, long long total) {
     flush();
-    if (!total) return;
+    if (!total || plan) return;
     const int bs = 256;
     begin("k_copy");
     k_copy<<<unsigned((total + bs - 1) / bs), bs, 0, h->stream>>>(d, int(n), sd);
@@ -96,6 +142,7 @@ struct Launcher {
   template <class R, int NM, class K, class... Args>
   void run(const char* name, int kind, K kern, const Packs<R, NM>& ps, Args... args) {
     flush();
+    if (plan) return;
     for (size_t c = 0; c < ps.p.size(); ++c) {
       const int nb = ps.blocks[c][size_t(kind)][0];
       if (nb == 0) continue;
@@ -109,6 +156,7 @@ struct Launcher {
   void run_t(const char* name, int kind, int nq, const std::array<K, kNumShapes>& kerns, const Packs<R, NM>& ps,
              Args... args) {
     flush();
+    if (plan) return;
     const int sh = shape_for(name);
     for (size_t c = 0; c < ps.p.size(); ++c) {
       const int nb = ps.blocks[c][size_t(kind)][size_t(sh)];
@@ -122,6 +170,7 @@ struct Launcher {
   template <class R, int NM, class K, class... Args>
   void run_cb(const char* name, int kind, int arrays, K kern, const Packs<R, NM>& ps, Args... args) {
     flush();
+    if (plan) return;
     static_assert(CX == 32, "a column block's lanes are one warp");
     const size_t smem = size_t(arrays) * h->cb_level_bytes;
     CW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
@@ -137,6 +186,7 @@ struct Launcher {
   template <class R, int NM, class K>
   void run_members(const char* name, int threads, K kern, const Packs<R, NM>& ps) {
     flush();
+    if (plan) return;
     for (size_t c = 0; c < ps.p.size(); ++c) {
       begin(name);
       kern<<<unsigned(ps.p[c].n), threads, 0, h->stream>>>(ps.p[c]);
@@ -181,7 +231,7 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
   if (lbc) {
     L.run_members("k_advance_time", 1, k_advance_time<R, NM>, d);
   }
-  if (h->cfl_on) CW_CUDA(cudaMemsetAsync(h->cfl_d, 0, 6 * h->m.size() * sizeof(unsigned long long), h->stream));
+  if (h->cfl_on && !L.plan) CW_CUDA(cudaMemsetAsync(h->cfl_d, 0, 6 * h->m.size() * sizeof(unsigned long long), h->stream));
   L.copy_list(h->copies_d, h->copies_start_d, h->copies.size(), h->copies_total);
   L.halo(cw_handle::H_MU1);
   for (int rk = 1; rk <= 3; ++rk) {
@@ -253,7 +303,7 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
 template <class R>
 void enqueue_t(cw_handle* h, Launcher& L, const DevTables<R>& T) {
   if (h->m.size() == 1) enqueue_step<R, 1>(h, L, T.one);
-  else enqueue_step<R, kPackMembers>(h, L, T.many);
+  else enqueue_step<R, 0>(h, L, T.many);
 }
 
 }  // namespace

@@ -7,8 +7,9 @@
 
 namespace cw {
 
-long long enqueue_mixed(cw_handle* h) {
+long long enqueue_mixed(cw_handle* h, bool plan) {
   Launcher L{h};
+  L.plan = plan;
   enqueue_t<float>(h, L, h->t32);
   return L.count;
 }

@@ -99,18 +99,28 @@ struct Dom {
   Slabs<T>* lbc_q;
 };
 
-// The kernels' view of up to NM members, passed by value as a __grid_constant__ parameter: the field
-// descriptors are read from the constant bank (operands of the address arithmetic for a single domain,
-// NM = 1) and no store of a kernel can alias them. start[kind][m] is member m's first block of a launch
-// over the index range `kind`; a batch of more members is launched in packs of kPackMembers.
+// The kernels' view of the members. A single domain (NM = 1): its descriptor passed by value as a
+// __grid_constant__ parameter, so the field descriptors are read from the constant bank (operands of the address
+// arithmetic) and no store of a kernel can alias them. A batch (NM = 0, any number of members): the members'
+// descriptors and block prefix sums in device memory, so one launch of each kernel covers the whole batch.
+// start(kind, shape, m) is member m's first block of a launch over the index range `kind` in block shape `shape`.
 constexpr int kNumKinds = 6;
 constexpr int kNumShapes = 3;  // point-kernel block shapes (autotuned per kernel): 128 x 1, 64 x 2, 32 x 4
-constexpr int kPackMembers = 12;
 template <class R, int NM>
 struct Pack {
   Dom<R> d[NM];
   int n;
-  int start[kNumKinds][kNumShapes][NM + 1];
+  int start_[kNumKinds][kNumShapes][NM + 1];
+  __device__ __forceinline__ int start(int kind, int shape, int m) const { return start_[kind][shape][m]; }
+};
+template <class R>
+struct Pack<R, 0> {
+  const Dom<R>* __restrict__ d;      // n descriptors (device memory, written before the launch)
+  const int* __restrict__ starts;    // [kNumKinds][kNumShapes][n + 1]
+  int n;
+  __device__ __forceinline__ int start(int kind, int shape, int m) const {
+    return __ldg(starts + (kind * kNumShapes + shape) * (n + 1) + m);
+  }
 };
 template <class R, int NM>
 __device__ __forceinline__ int member_of(const Pack<R, NM>& P, int kind, int shape, int b) {
@@ -120,7 +130,7 @@ __device__ __forceinline__ int member_of(const Pack<R, NM>& P, int kind, int sha
     int lo = 0, hi = P.n - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (P.start[kind][shape][mid] <= b) lo = mid;
+      if (P.start(kind, shape, mid) <= b) lo = mid;
       else hi = mid - 1;
     }
     return lo;
@@ -144,14 +154,25 @@ template <class R>
 __device__ __forceinline__ R sgn1(R a) {
   return a >= R(0) ? R(1) : R(-1);
 }
+// x / C for the statement functions' constants C = 60, 12: in the FP64 form the correctly rounded quotient without a
+// division (cw_div_const: one multiply and two FMAs, bit-identical to the IEEE division); in the mixed form the
+// IEEE float division
+template <int C>
+__device__ __forceinline__ double div_c(double x) {
+  return cw_div_const(x, double(C), 1.0 / double(C));
+}
+template <int C>
+__device__ __forceinline__ float div_c(float x) {
+  return x / float(C);
+}
 template <class R>
 __device__ __forceinline__ R flux5(R qm3, R qm2, R qm1, R q0, R qp1, R qp2, R ua, R up) {
-  return (R(37) * (q0 + qm1) - R(8) * (qp1 + qm2) + (qp2 + qm3)) / R(60) -
-         up * sgn1(ua) * ((qp2 - qm3) - R(5) * (qp1 - qm2) + R(10) * (q0 - qm1)) / R(60);
+  return div_c<60>(R(37) * (q0 + qm1) - R(8) * (qp1 + qm2) + (qp2 + qm3)) -
+         div_c<60>(up * sgn1(ua) * ((qp2 - qm3) - R(5) * (qp1 - qm2) + R(10) * (q0 - qm1)));
 }
 template <class R>
 __device__ __forceinline__ R flux3(R qm2, R qm1, R q0, R qp1, R ua, R up) {
-  return (R(7) * (q0 + qm1) - (qp1 + qm2)) / R(12) + up * sgn1(ua) * ((qp1 - qm2) - R(3) * (q0 - qm1)) / R(12);
+  return div_c<12>(R(7) * (q0 + qm1) - (qp1 + qm2)) + div_c<12>(up * sgn1(ua) * ((qp1 - qm2) - R(3) * (q0 - qm1)));
 }
 template <class R>
 __device__ __forceinline__ R flux5_pd(R qm3, R qm2, R qm1, R q0, R qp1, R qp2, R ua, R up) {

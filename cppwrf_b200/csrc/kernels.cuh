@@ -53,7 +53,7 @@ __device__ __forceinline__ bool thread_index(const Pack<R, NM>& P, int kind, con
   Dp = &D;
   const Range r = range_of(kind, D.nx, D.ny, D.nz, D.nyv);
   const int bx = cdiv(r.i1 - r.i0, sx), by = cdiv(r.j1 - r.j0, sy);
-  int local = b - P.start[kind][SH][m];
+  int local = b - P.start(kind, SH, m);
   const int bi = local % bx;
   local /= bx;
   const int bj = local % by;
@@ -173,6 +173,22 @@ __global__ void k_halo(const __grid_constant__ HaloChunk<NF> s, int pass) {
   }
   const HaloField& f = s.f[lo];
   const unsigned c = t - s.start[lo];
+  if (f.is_float) halo_cell<float>(f, c, pass);
+  else halo_cell<double>(f, c, pass);
+}
+
+// the same over a fill point's fields held in device memory (a batch: every member's fields in one launch)
+static __global__ void k_halo_tab(const HaloField* __restrict__ fs, const unsigned* __restrict__ start, int nf, int pass) {
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= __ldg(start + nf)) return;
+  int lo = 0, hi = nf - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(start + mid) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  const HaloField f = fs[lo];
+  const unsigned c = t - __ldg(start + lo);
   if (f.is_float) halo_cell<float>(f, c, pass);
   else halo_cell<double>(f, c, pass);
 }

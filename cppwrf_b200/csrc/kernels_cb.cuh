@@ -15,6 +15,12 @@ namespace cw {
 // issued before the stores of this one (shared stores cannot alias global loads)
 #define CB_LOOP_SH(k, n) _Pragma("unroll 2") for (int k = int(threadIdx.y); k < (n); k += CNW)
 
+
+// a hint that brings the line of a into L2 (no register, no wait): the column blocks' level loops then meet L2
+// instead of DRAM latency
+__device__ __forceinline__ void pf_l2(const void* a) { asm volatile("prefetch.global.L2 [%0];" ::"l"(a)); }
+// the levels of a loop split over warps 1 .. CNW - 1 (warp 0 runs a recurrence meanwhile)
+#define CB_LOOP_W1(k, n) for (int k = int(threadIdx.y) - 1; threadIdx.y > 0 && k < (n); k += CNW - 1)
 // block -> (member, column i of this lane, row j)
 template <class R, int NM>
 __device__ __forceinline__ const Dom<R>& cb_member(const Pack<R, NM>& P, int kind, int& i, int& j) {
@@ -23,7 +29,7 @@ __device__ __forceinline__ const Dom<R>& cb_member(const Pack<R, NM>& P, int kin
   const Dom<R>& D = P.d[m];
   const Range r = range_of(kind, D.nx, D.ny, D.nz, D.nyv);
   const int bx = cdiv(r.i1 - r.i0, CX);
-  const int local = b - P.start[kind][0][m];
+  const int local = b - P.start(kind, 0, m);
   i = r.i0 + (local % bx) * CX + int(threadIdx.x);
   j = r.j0 + local / bx;
   return D;
@@ -292,6 +298,33 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
   double* s2 = cb_array(2, nz);
   double* sc = cb_array(3, nz);  // per-column scalars: sc[n * CX + lane]
   double* s_t2s = cb_array(4, nz);  // theta'' before the substep's update (t_2save), phase 1 to phase 2
+
+  if (mass)  // phase 1's inputs of the block's columns into L2 (a level above nz takes level 0: inside the field)
+    CB_LOOP(k, nz + 1) {
+      const int kh = k < nz ? k : 0;
+      pf_l2(&D.u2(i, j, kh));
+      pf_l2(&D.u2(i + 1, j, kh));
+      pf_l2(&D.u_save(i, j, kh));
+      pf_l2(&D.ru_m(i, j, kh));
+      if (D.do_y) {
+        pf_l2(&D.v2(i, j, kh));
+        pf_l2(&D.v2(i, j + 1, kh));
+        pf_l2(&D.v_save(i, j, kh));
+        pf_l2(&D.v_save(i, j + 1, kh));
+        pf_l2(&D.rv_m(i, j, kh));
+      }
+      pf_l2(&D.ww1(i, j, k));
+      pf_l2(&D.ww_m(i, j, k));
+      if (k < nz) {
+        pf_l2(&D.t2(i, j, k));
+        pf_l2(&D.t_tend(i, j, k));
+        pf_l2(&D.t_save(i, j, k));
+        if (D.do_y) {
+          pf_l2(&D.t_save(i, j - 1, k));
+          pf_l2(&D.t_save(i, j + 1, k));
+        }
+      }
+    }
   if (phase & 1) {
     if (col && D.spec_x && i == nx && j < ny)  // KSumEdge, east face (specified or open x)
       CB_LOOP(k, nz) {
@@ -355,6 +388,24 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
         }
       }
     __syncthreads();
+    if (mass)  // while warp 0 sums the column: phase 2's inputs into L2
+      CB_LOOP_W1(k, nz + 1) {
+        pf_l2(&D.ph_tend(i, j, k));
+        pf_l2(&D.w2(i, j, k));
+        pf_l2(&D.ph_save(i, j, k));
+        pf_l2(&D.ph2(i, j, k));
+        pf_l2(&D.rw_tend(i, j, k));
+        pf_l2(&D.a(i, j, k));
+        pf_l2(&D.alpha(i, j, k));
+        pf_l2(&D.gamma(i, j, k));
+        if (!D.flat) pf_l2(D.phb.p + (i * D.phb.si + j * D.phb.sj + k * D.phb.sk));
+        if (k < nz) {
+          pf_l2(&D.c2a(i, j, k));
+          pf_l2(&D.alt(i, j, k));
+          pf_l2(&D.pm1(i, j, k));
+          if (D.n_moist) pf_l2(&D.cqw(i, j, k));
+        }
+      }
     if (dyn && w0) {  // the column mass tendency: sum over k in order
       A dmdt = 0;
 #pragma unroll 4
@@ -435,8 +486,14 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
     __syncthreads();
   }
   if (phase & 2) {
-    const R ope = R(1) + epssm, ome = R(1) - epssm;
-    R mut = 0, muts = 0, mav = 0, msfty = 1;
+    // advance_w in double in both forms (the mixed form's fields are float; the explicit phi'' and w'' right-hand
+    // sides are differences of nearly equal pressure-gradient and buoyancy terms, kept in double). For the FP64
+    // form every conversion below is the identity and the operations are the reference's, in its order.
+    const A dtsA = rk == 1 ? D.dt / 3.0 : D.dt / D.n_sound, eps = D.epssm;
+    const A ope = 1.0 + eps, ome = 1.0 - eps;
+    auto mhA = [&](int kk, A m) { return D.c1h[kk] * m + D.c2h[kk]; };
+    auto mfA = [&](int kk, A m) { return D.c1f[kk] * m + D.c2f[kk]; };
+    A mut = 0, muts = 0, mav = 0, msfty = 1;
     double* s_a = cb_array(3, nz);
     double* s_al = cb_array(4, nz);
     double* s_ga = cb_array(5, nz);
@@ -448,77 +505,81 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
       }
     }
     if (dyn) {
-      mut = D.mut.ld(i, j, 0);
-      muts = D.muts(i, j, 0);
-      mav = D.muave(i, j, 0);
-      msfty = D.msfty(i, j);
+      mut = A(D.mut.ld(i, j, 0));
+      muts = A(D.muts(i, j, 0));
+      mav = A(D.muave(i, j, 0));
+      msfty = A(D.msfty(i, j));
       CB_LOOP_SH(k, nz + 1) {  // KWRhs: R (explicit phi'') and t_2ave
-        R r;
+        A r;
         if (k == 0 || (D.top_lid && k == nz)) {
           r = 0;
         } else {
-          R rr = dts * (D.ph_tend.ld(i, j, k) + R(0.5) * R(k::g) * (R(1) - epssm) * D.w2(i, j, k));
+          A rr = dtsA * (A(D.ph_tend.ld(i, j, k)) + 0.5 * k::g * (1.0 - eps) * A(D.w2(i, j, k)));
           if (k < nz) {
             auto wdwn = [&](int mm) {
-              return R(0.5) * (D.ww(i, j, mm) + D.ww(i, j, mm - 1)) * R(D.rdnw[mm - 1]) *
-                     (D.ph_save.ld(i, j, mm) - D.ph_save.ld(i, j, mm - 1) + D.phb(i, j, mm) - D.phb(i, j, mm - 1));
+              return 0.5 * (A(D.ww(i, j, mm)) + A(D.ww(i, j, mm - 1))) * D.rdnw[mm - 1] *
+                     (A(D.ph_save.ld(i, j, mm)) - A(D.ph_save.ld(i, j, mm - 1)) + A(D.phb(i, j, mm)) - A(D.phb(i, j, mm - 1)));
             };
-            rr -= dts * (R(D.fnm[k]) * wdwn(k + 1) + R(D.fnp[k]) * wdwn(k));
+            rr -= dtsA * (D.fnm[k] * wdwn(k + 1) + D.fnp[k] * wdwn(k));
           }
-          r = D.ph2(i, j, k) + msfty * rr / mf_(D, k, mut);
+          r = A(D.ph2(i, j, k)) + msfty * rr / mfA(k, mut);
         }
-        s0[k * CX + lane] = A(r);
+        s0[k * CX + lane] = r;
         if (k < nz) {
-          const R tav = R(0.5) * ((R(1) + epssm) * D.t2(i, j, k) + (R(1) - epssm) * R(s_t2s[k * CX + lane]));
-          s1[k * CX + lane] = A((tav + R(D.c1h[k]) * mav * R(k::t0)) / (mh_(D, k, muts) * (R(k::t0) + D.t_save.ld(i, j, k))));
+          const A tav = 0.5 * ((1.0 + eps) * A(D.t2(i, j, k)) + (1.0 - eps) * s_t2s[k * CX + lane]);
+          s1[k * CX + lane] = (tav + D.c1h[k] * mav * k::t0) / (mhA(k, muts) * (k::t0 + A(D.t_save.ld(i, j, k))));
         }
       }
     }
     __syncthreads();
     if (dyn) {
-      const R msft_inv = R(1) / msfty;
+      const A msft_inv = 1.0 / msfty;
       CB_LOOP_SH(k, nz + 1) {  // KWExpl: explicit w''
-        R wn;
+        A wn;
         if (k == 0) {
           if (!D.flat) {
-            R ws = D.msftx(i, j) * R(0.5) * R(D.rdx) *
-                   ((D.ht(i + 1, j) - D.ht(i, j)) * (R(D.cf1) * D.u2.ld(i + 1, j, 0) + R(D.cf2) * D.u2.ld(i + 1, j, 1) + R(D.cf3) * D.u2.ld(i + 1, j, 2)) +
-                    (D.ht(i, j) - D.ht(i - 1, j)) * (R(D.cf1) * D.u2.ld(i, j, 0) + R(D.cf2) * D.u2.ld(i, j, 1) + R(D.cf3) * D.u2.ld(i, j, 2)));
+            const A cf1 = D.cf1, cf2 = D.cf2, cf3 = D.cf3;
+            auto U = [&](int ii, int kk) { return A(D.u2.ld(ii, j, kk)); };
+            auto V = [&](int jj, int kk) { return A(D.v2.ld(i, jj, kk)); };
+            auto H = [&](int ii, int jj) { return A(D.ht(ii, jj)); };
+            A ws = A(D.msftx(i, j)) * 0.5 * D.rdx *
+                   ((H(i + 1, j) - H(i, j)) * (cf1 * U(i + 1, 0) + cf2 * U(i + 1, 1) + cf3 * U(i + 1, 2)) +
+                    (H(i, j) - H(i - 1, j)) * (cf1 * U(i, 0) + cf2 * U(i, 1) + cf3 * U(i, 2)));
             if (D.do_y)
-              ws = msfty * R(0.5) * R(D.rdy) *
-                       ((D.ht(i, j + 1) - D.ht(i, j)) * (R(D.cf1) * D.v2.ld(i, j + 1, 0) + R(D.cf2) * D.v2.ld(i, j + 1, 1) + R(D.cf3) * D.v2.ld(i, j + 1, 2)) +
-                        (D.ht(i, j) - D.ht(i, j - 1)) * (R(D.cf1) * D.v2.ld(i, j, 0) + R(D.cf2) * D.v2.ld(i, j, 1) + R(D.cf3) * D.v2.ld(i, j, 2))) +
+              ws = msfty * 0.5 * D.rdy *
+                       ((H(i, j + 1) - H(i, j)) * (cf1 * V(j + 1, 0) + cf2 * V(j + 1, 1) + cf3 * V(j + 1, 2)) +
+                        (H(i, j) - H(i, j - 1)) * (cf1 * V(j, 0) + cf2 * V(j, 1) + cf3 * V(j, 2))) +
                    ws;
             wn = ws;
           } else {
             wn = 0;
           }
         } else {
-          const R r_k = R(s0[k * CX + lane]), r_km1 = R(s0[(k - 1) * CX + lane]);
-          const R ph_k = D.ph2(i, j, k), ph_km1 = D.ph2(i, j, k - 1);
+          const A r_k = s0[k * CX + lane], r_km1 = s0[(k - 1) * CX + lane];
+          const A ph_k = A(D.ph2(i, j, k)), ph_km1 = A(D.ph2(i, j, k - 1));
+          const A c2a_k1 = A(D.c2a.ld(i, j, k - 1)), alt_k1 = A(D.alt.ld(i, j, k - 1));
           if (k < nz) {
-            const R r_kp1 = R(s0[(k + 1) * CX + lane]), ph_kp1 = D.ph2(i, j, k + 1);
-            const R cq1 = R(1) / (R(1) + cqw_(D, i, j, k));
-            wn = D.w2(i, j, k) + dts * D.rw_tend.ld(i, j, k) +
+            const A r_kp1 = s0[(k + 1) * CX + lane], ph_kp1 = A(D.ph2(i, j, k + 1));
+            const A cq1 = 1.0 / (1.0 + A(cqw_(D, i, j, k)));
+            const A c2a_k = A(D.c2a.ld(i, j, k)), alt_k = A(D.alt.ld(i, j, k));
+            wn = A(D.w2(i, j, k)) + dtsA * A(D.rw_tend.ld(i, j, k)) +
                  msft_inv * cq1 *
-                     (R(0.5) * dts * R(k::g) * R(D.rdn[k]) *
-                      (D.c2a.ld(i, j, k) * R(D.rdnw[k]) / mh_(D, k, mut) * (ope * (r_kp1 - r_k) + ome * (ph_kp1 - ph_k)) -
-                       D.c2a.ld(i, j, k - 1) * R(D.rdnw[k - 1]) / mh_(D, k - 1, mut) * (ope * (r_k - r_km1) + ome * (ph_k - ph_km1)))) +
-                 dts * R(k::g) * msft_inv *
-                     (R(D.rdn[k]) * (D.c2a.ld(i, j, k) * D.alt.ld(i, j, k) * R(s1[k * CX + lane]) -
-                                     D.c2a.ld(i, j, k - 1) * D.alt.ld(i, j, k - 1) * R(s1[(k - 1) * CX + lane])) -
-                      R(D.c1f[k]) * mav);
+                     (0.5 * dtsA * k::g * D.rdn[k] *
+                      (c2a_k * D.rdnw[k] / mhA(k, mut) * (ope * (r_kp1 - r_k) + ome * (ph_kp1 - ph_k)) -
+                       c2a_k1 * D.rdnw[k - 1] / mhA(k - 1, mut) * (ope * (r_k - r_km1) + ome * (ph_k - ph_km1)))) +
+                 dtsA * k::g * msft_inv *
+                     (D.rdn[k] * (c2a_k * alt_k * s1[k * CX + lane] - c2a_k1 * alt_k1 * s1[(k - 1) * CX + lane]) -
+                      D.c1f[k] * mav);
           } else {
             const int km = nz - 1;
-            wn = D.w2(i, j, k) + dts * D.rw_tend.ld(i, j, k) +
-                 msft_inv * (-R(0.5) * dts * R(k::g) / mh_(D, km, mut) * (R(D.rdnw[km]) * R(D.rdnw[km])) * R(2) * D.c2a.ld(i, j, km) *
+            wn = A(D.w2(i, j, k)) + dtsA * A(D.rw_tend.ld(i, j, k)) +
+                 msft_inv * (-0.5 * dtsA * k::g / mhA(km, mut) * (D.rdnw[km] * D.rdnw[km]) * 2.0 * c2a_k1 *
                                  (ope * (r_k - r_km1) + ome * (ph_k - ph_km1)) -
-                             dts * R(k::g) * (R(2) * R(D.rdnw[km]) * D.c2a.ld(i, j, km) * D.alt.ld(i, j, km) * R(s1[km * CX + lane]) +
-                                              R(D.c1f[k]) * mav));
+                             dtsA * k::g * (2.0 * D.rdnw[km] * c2a_k1 * alt_k1 * s1[km * CX + lane] + D.c1f[k] * mav));
             if (D.top_lid) wn = 0;
           }
         }
-        s2[k * CX + lane] = A(wn);
+        s2[k * CX + lane] = wn;
         s_a[k * CX + lane] = A(D.a.ld(i, j, k));
         s_al[k * CX + lane] = A(D.alpha.ld(i, j, k));
         s_ga[k * CX + lane] = A(D.gamma.ld(i, j, k));
@@ -529,15 +590,13 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
       A wprev = s2[0 * CX + lane];
 #pragma unroll 4
       for (int k = 1; k <= nz; ++k) {
-        const A wk = (s2[k * CX + lane] - s_a[k * CX + lane] * wprev) * s_al[k * CX + lane];
-        wprev = A(R(wk));
+        wprev = (s2[k * CX + lane] - s_a[k * CX + lane] * wprev) * s_al[k * CX + lane];
         s2[k * CX + lane] = wprev;
       }
       A wnext = wprev;
 #pragma unroll 4
       for (int k = nz - 1; k >= 1; --k) {
-        const A wk = s2[k * CX + lane] - s_ga[k * CX + lane] * wnext;
-        wnext = A(R(wk));
+        wnext = s2[k * CX + lane] - s_ga[k * CX + lane] * wnext;
         s2[k * CX + lane] = wnext;
       }
     }
@@ -554,7 +613,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
               const R sn = R(cw_sin(double(R(0.5) * pi * (hk - hbot) / hdepth)));
               dampwt = dampmag * sn * sn;
             }
-            s2[k * CX + lane] = A(R((R(s2[k * CX + lane]) - dampwt * mf_(D, k, mut) * D.w_save.ld(i, j, k)) / (R(1) + dampwt)));
+            s2[k * CX + lane] = A(R((R(s2[k * CX + lane]) - dampwt * mf_(D, k, R(mut)) * D.w_save.ld(i, j, k)) / (R(1) + dampwt)));
           }
         }
       }
@@ -563,7 +622,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
     // w'' and phi'' (dyn columns), then calc_p_rho of the level (every mass column, phase 4) from the new
     // phi'' of levels k and k + 1: recomputed from the shared terms here (the same expression as the store),
     // read back for the spec zone (written before the last barriers) and for the unchanged level 0
-    auto ph_new = [&](int m) { return R(s0[m * CX + lane]) + msfty * R(0.5) * dts * R(k::g) * ope * R(s2[m * CX + lane]) / mf_(D, m, muts); };
+    auto ph_new = [&](int m) { return R(s0[m * CX + lane] + msfty * 0.5 * dtsA * k::g * ope * s2[m * CX + lane] / mfA(m, muts)); };
     if (mass)
       CB_LOOP(k, nz + 1) {
         R wk = 0, phk = 0, phkp = 0;

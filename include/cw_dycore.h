@@ -195,6 +195,12 @@ int cw_members(cw_handle* h, int* out);
  * when every value is finite (field = -1), 1 with the first non-finite value's field id, species n and point
  * (i, j, k) in that order of fields and then k, j, i, < 0 on error. It synchronizes the handle's stream. */
 int cw_check_finite(cw_handle* h, int member, int* field, int* n, int* i, int* j, int* k);
+/* Self-check of the device arithmetic the flux statement functions rely on (no counterpart in the reference: its
+ * CPU build divides): the division by the constants 60 and 12 without a divide instruction (cw_div_const) against the
+ * IEEE division __ddiv_rn on n operands per constant drawn from seed (random bit patterns over every exponent,
+ * quotients next to a rounding midpoint, exact quotients and their neighbours), on the current device. */
+int cw_check_div_const(unsigned long long n, unsigned long long seed, unsigned long long* checked,
+                       unsigned long long* mismatches);
 /* Block-shape autotuning of the point kernels (no reference counterpart). With on = 1 the next three
  * cw_step steps run every tunable kernel in one of its block shapes (0: 128 x 1, 1: 64 x 2, 2: 32 x 4
  * points along i x j), timed per launch; afterwards each kernel keeps its fastest shape and the step is
@@ -214,6 +220,11 @@ int cw_batch_remove(cw_handle* h, int member);
  * batch steps) into the batch as its last member, without copying its fields; `single` is left empty (destroy
  * it). Same precision and acoustic step count as the batch's members. */
 int cw_batch_adopt(cw_handle* h, cw_handle* single, int* member);
+/* The reverse of cw_batch_adopt: moves member `member` out of the batch into a new single-domain handle (*out,
+ * with its own stream) without copying its fields, so that it can be read back on another thread while the batch
+ * steps on; the members after it move down by one. Destroy *out with cw_destroy. (No counterpart in the
+ * reference, which runs one domain per RK3 object.) */
+int cw_batch_release(cw_handle* h, int member, cw_handle** out);
 /* Device bytes one domain takes in a handle (fields, work fields, scalars, slabs, vertical arrays): the
  * footprint the served form admits by. Needs no device. */
 int cw_footprint(const cw_grid* g, const cw_options* o, size_t* bytes);

@@ -9,8 +9,17 @@
  * after the other (src/cases/nest_driver.cpp:871). Each request's result is the same as the request run
  * alone through cw_step (the batched kernels compute every member independently, in the same order).
  *
- * Threading: the loop runs on its own host thread (started by cw_serve_create, on the configured device);
- * every call below may be made from any thread.
+ * Threading: three host threads started by cw_serve_create on the configured device, so that setting up and
+ * reading back requests overlaps with stepping: an admitter (FIFO admission by footprint, each admitted request
+ * set up in a single-domain handle of its own), a stepper (ready requests join their batch without a copy,
+ * cw_batch_adopt; every batch's step is launched before any is waited for; finished requests leave without a
+ * copy, cw_batch_release) and a reader (the finished request's state downloaded on its own stream, its device
+ * memory freed). A request holds its footprint of the budget from admission until its state is read back.
+ * Every call below may be made from any thread.
+ *
+ * Failures: a request whose set-up, step or read-back fails is marked failed (cw_serve_wait returns -2) and its
+ * memory is returned to the budget; a batch whose step fails is dropped with its requests, and the next request
+ * of that acoustic step count makes a new one.
  */
 #ifndef CW_SERVE_H
 #define CW_SERVE_H
@@ -31,6 +40,8 @@ typedef struct cw_serve_config {
   int precision;           /* enum cw_precision of every request (a case's own setting is overridden) */
   int device;              /* CUDA device of the loop */
   int keep_results;        /* 1: keep each finished request's prognostic fields for cw_serve_result */
+  int test_fail_creates;   /* test hook, 0 in use: the first n batch-handle creations fail with an injected
+                              error (the failure path is exercised without a device fault) */
 } cw_serve_config;
 
 typedef struct cw_serve_stats {
@@ -47,8 +58,8 @@ int cw_serve_default_config(cw_serve_config* c);
 int cw_serve_create(const cw_serve_config* c, cw_server** out);
 /* Ends the loop; requests still pending or running are dropped. */
 int cw_serve_destroy(cw_server* s);
-/* Queues a request: the case (copied) advanced by nsteps RK3 steps. id: its handle for the calls below.
- * A request whose footprint exceeds the whole budget is rejected (-2). */
+/* Queues a request: the case (copied) advanced by nsteps RK3 steps (nsteps >= 1; otherwise -1). id: its handle
+ * for the calls below. A request whose footprint exceeds the whole budget is rejected (-2). */
 int cw_serve_submit(cw_server* s, const cw_case* c, int nsteps, long long* id);
 /* 0 when the request has finished, 1 on timeout (seconds < 0: wait without limit), < 0 failed / unknown */
 int cw_serve_wait(cw_server* s, long long id, double seconds);

@@ -34,6 +34,15 @@
 #include "dyn/state.hpp"
 #include "phys/driver/phy_prep.hpp"
 #include "../include/cw_dycore.h"
+#ifdef CW_HARNESS_FACADE
+// ref_harness_facade: the same driver with the step replaced by the repository's drop-in (RK3B200 over the C ABI,
+// on the GPU); everything else -- the reference's State / Tendencies / BaseState / LateralBC / DiffusionDriver
+// objects, their set-up and the output -- is unchanged
+#include "../cppwrf_b200/facade/rk3_b200.hpp"
+using Stepper = cppwrf_b200::RK3B200;
+#else
+using Stepper = cppwrf::dyn::RK3;
+#endif
 
 // The dycore links three symbols of the physics coupling that the dynamics-only configurations never call.
 namespace cppwrf::dyn {
@@ -296,7 +305,7 @@ int main(int argc, char** argv) {
     dyn::ScalarParams sp;
     sp.moist_adv_opt = co.moist_adv_opt; sp.scalar_adv_opt = co.scalar_adv_opt; sp.tke_adv_opt = co.tke_adv_opt;
     sp.h_adv_order = co.h_adv_order; sp.v_adv_order = co.v_adv_order;
-    dyn::RK3 rk(g, lp, ap, co.time_step_sound, sp);
+    Stepper rk(g, lp, ap, co.time_step_sound, sp);
     std::unique_ptr<dyn::DiffusionDriver> dd;
     if (co.diff_opt == 1 || co.diff_6th_opt != 0 || co.damp_opt == 2) {  // DiffusionConfig::on (model.cpp:439)
       dyn::DiffusionConfig dc;

@@ -149,10 +149,11 @@ def run_lam(w, seed, nsteps):
         return _read_output(fout, int(w["n_moist"]))
 
 
-def run(case, nsteps, own_pow=True):
-    """{field name: whole allocation} of the reference after nsteps (Q_* keyed 'Q_2:n')."""
+def run(case, nsteps, own_pow=True, harness=None):
+    """{field name: whole allocation} of the reference after nsteps (Q_* keyed 'Q_2:n'); harness: another build of
+    the driver (ref_harness_facade: the step replaced by the repository's drop-in)."""
     build()
-    exe = os.path.join(REF_DIR, "ref_harness_own" if own_pow else "ref_harness")
+    exe = os.path.join(REF_DIR, harness or ("ref_harness_own" if own_pow else "ref_harness"))
     with tempfile.TemporaryDirectory() as td:
         fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
         write_input(case, nsteps, fin)

@@ -62,3 +62,31 @@ def test_served_rejects_a_request_larger_than_the_budget():
         srv.submit(c, 3)
     assert srv.stats()["rejected"] == 1
     srv.close()
+
+
+def test_served_failed_batch_creation_does_not_block_later_requests():
+    """A failure injected on the host into the first batch-handle creation (the test hook of cw_serve_config) fails
+    only the request that needed it: the batch is not left half-made, and later requests of the same acoustic step
+    count make a new one and complete, equal to the same requests alone."""
+    cases = [lam_case(nx=24, ny=20, nz=14, seed=s) for s in (51, 52, 53)]
+    srv = Server(budget_bytes=1e12, precision=capi.FP64, test_fail_creates=1)
+    first = srv.submit(cases[0], 3)
+    assert srv.wait(first) == -2  # failed: the injected creation error
+    later = [srv.submit(c, 4) for c in cases[1:]]
+    srv.drain()
+    st = srv.stats()
+    assert st["failed"] == 1 and st["completed"] == 2, st
+    assert st["used_bytes"] == 0 and st["resident"] == 0, st
+    for rid, c in zip(later, cases[1:]):
+        check_alone(srv, rid, c, 4)
+    srv.close()
+
+
+def test_served_rejects_requests_without_steps():
+    c = lam_case(nx=24, ny=20, nz=14, seed=3)
+    srv = Server(budget_bytes=1e12, precision=capi.FP64)
+    with pytest.raises(Exception):
+        srv.submit(c, 0)
+    st = srv.stats()
+    assert st["submitted"] == 0 and st["failed"] == 0, st
+    srv.close()
