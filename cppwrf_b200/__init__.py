@@ -19,7 +19,7 @@ from . import capi
 from .capi import (DEFAULT, FIELDS, FP64, IGW, MIXED, PERIODIC, REST_STATE, SPECIFIED, STRAKA, SYMMETRIC,
                    WARM_BUBBLE, Case, F, Grid, Layout, Options, default_options, grid, interior)
 
-__all__ = ["Domain", "Batch", "Server", "Case", "Grid", "Options", "Layout", "grid", "default_options", "interior", "capi",
+__all__ = ["Domain", "Decomp", "Batch", "Server", "Case", "Grid", "Options", "Layout", "grid", "default_options", "interior", "capi",
            "FIELDS", "F", "PERIODIC", "SYMMETRIC", "SPECIFIED", "FP64", "MIXED", "REST_STATE", "STRAKA",
            "WARM_BUBBLE", "IGW", "DEFAULT"]
 
@@ -133,6 +133,50 @@ class Domain:
         v = C.c_int()
         self.lib.cw_autotune_choice(self.h, kernel.encode(), C.byref(v))
         return v.value
+
+
+class Decomp:
+    """One domain decomposed into px x py patches on the device (cw_decomp_create): fields go in and out as
+    whole-domain arrays; the step is RK3::step of the undecomposed domain, bit for bit."""
+
+    def __init__(self, g, o, px, py, lib=None):
+        self.lib = lib or capi.load()
+        self.g, self.o = g, o
+        self.h = C.c_void_p()
+        _check(self.lib, None, self.lib.cw_decomp_create(C.byref(g), C.byref(o), int(px), int(py), C.byref(self.h)),
+               "cw_decomp_create")
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.lib.cw_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def upload_case(self, case):
+        _check(self.lib, self.h, self.lib.cw_decomp_upload_case(self.h, case.h), "cw_decomp_upload_case")
+        return self
+
+    def step(self, n=1):
+        _check(self.lib, self.h, self.lib.cw_step(self.h, n), "cw_step")
+
+    def sync(self):
+        _check(self.lib, self.h, self.lib.cw_sync(self.h), "cw_sync")
+
+    def launches(self):
+        v = C.c_longlong()
+        self.lib.cw_launch_count(self.h, C.byref(v))
+        return v.value
+
+    def field(self, name, n=0):
+        L = Layout()
+        if self.lib.cw_layout_of(C.byref(self.g), C.byref(self.o), F[name], C.byref(L)) != 0:
+            raise KeyError(name)
+        out = np.empty(L.total, dtype=np.float64)
+        rc = self.lib.cw_decomp_download(self.h, F[name], n, out.ctypes.data_as(C.POINTER(C.c_double)), out.size)
+        _check(self.lib, self.h, rc, "cw_decomp_download")
+        return out
 
 
 class Batch:

@@ -182,6 +182,11 @@ def load(path=None):
         "cw_set_autotune": (i, [vp, i]),
         "cw_check_finite": (i, [vp, i, ip, ip, ip, ip, ip]),
         "cw_batch_release": (i, [vp, i, C.POINTER(vp)]),
+        "cw_decomp_patch": (i, [C.POINTER(Grid), i, i, i, C.POINTER(C.c_int)]),
+        "cw_decomp_create": (i, [C.POINTER(Grid), C.POINTER(Options), i, i, C.POINTER(vp)]),
+        "cw_decomp_upload": (i, [vp, i, i, dp, sz]),
+        "cw_decomp_download": (i, [vp, i, i, dp, sz]),
+        "cw_decomp_upload_case": (i, [vp, vp]),
         "cw_check_div_const": (i, [C.c_ulonglong, C.c_ulonglong, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]),
         "cw_autotune_choice": (i, [vp, C.c_char_p, ip]),
         "cw_footprint": (i, [C.POINTER(Grid), C.POINTER(Options), C.POINTER(sz)]),

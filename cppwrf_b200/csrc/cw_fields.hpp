@@ -22,8 +22,14 @@ inline bool flat_x(const cw_grid& g) { return g.bc_x == CW_BC_SPECIFIED || g.bc_
 inline bool flat_y(const cw_grid& g) { return g.bc_y == CW_BC_SPECIFIED || g.bc_y == CW_BC_OPEN; }
 inline bool specified(const cw_grid& g) { return g.bc_x == CW_BC_SPECIFIED || g.bc_y == CW_BC_SPECIFIED; }
 
-// Layout::make for the whole domain; uniform = horizontally uniform base field (1-D storage).
-inline cw_layout layout_make(const cw_grid& g, char s, int rank, bool uniform) {
+// A patch of a decomposed domain: the mass points i0 <= i < i1, j0 <= j < j1 it owns (the domain's indices).
+struct Box {
+  int i0, i1, j0, j1;
+};
+// Layout::make for the whole domain, or (patch) for a patch and a halo of 3 around it, indexed with the domain's
+// indices (the window [wi0, wi1) x [wj0, wj1); the east / north edge patches also hold the faces nx / ny and the
+// lateral halos); uniform = horizontally uniform base field (1-D storage).
+inline cw_layout layout_make(const cw_grid& g, char s, int rank, bool uniform, const Box* patch = nullptr) {
   cw_layout L{};
   L.nx = nxs(g, s);
   L.ny = nys(g, s);
@@ -44,6 +50,14 @@ inline cw_layout layout_make(const cw_grid& g, char s, int rank, bool uniform) {
   L.wi1 = L.nx + 3;
   L.wj0 = -hy;
   L.wj1 = L.ny + hy;
+  if (patch) {
+    L.wi0 = patch->i0 - 3;
+    L.wi1 = (patch->i1 == g.nx ? L.nx : patch->i1) + 3;
+    if (!two_d(g)) {
+      L.wj0 = patch->j0 - 3;
+      L.wj1 = (patch->j1 == g.ny ? L.ny : patch->j1) + 3;
+    }
+  }
   const int64_t pitch = (8 + (L.wi1 - L.wi0 - 3) + 31) / 32 * 32;
   L.si = 1;
   L.sj = two_d(g) ? 0 : pitch;
@@ -85,9 +99,26 @@ inline FieldKind field_kind(const cw_options& o, int id) {
   }
 }
 
-inline cw_layout field_layout(const cw_grid& g, const cw_options& o, int id) {
+inline cw_layout field_layout(const cw_grid& g, const cw_options& o, int id, const Box* patch = nullptr) {
   const FieldKind k = field_kind(o, id);
-  return layout_make(g, k.stagger, k.rank, k.uniform);
+  return layout_make(g, k.stagger, k.rank, k.uniform, patch);
+}
+
+// Patch t = tx + px ty of a px x py decomposition (tile::set_domain, src/core/tiles.hpp:70-74): the mass points
+// [tx nx / px, (tx + 1) nx / px) x [ty ny / py, (ty + 1) ny / py)
+inline Box patch_box(const cw_grid& g, int px, int py, int t) {
+  const int tx = t % px, ty = t / px;
+  return Box{int(int64_t(tx) * g.nx / px), int(int64_t(tx + 1) * g.nx / px), int(int64_t(ty) * g.ny / py),
+             int(int64_t(ty + 1) * g.ny / py)};
+}
+// why a px x py decomposition of g is refused (0: accepted)
+inline const char* decomp_unsupported(const cw_grid& g, int px, int py) {
+  if (px < 1 || py < 1 || px * py > 256) return "decomposition: 1 <= px, py and px * py <= 256";
+  if (two_d(g) && py != 1) return "decomposition: a 2-D (x-z) domain is split along x only";
+  if (g.bc_x == CW_BC_PERIODIC && px > 1) return "decomposition: a periodic direction is not split";
+  if (g.bc_y == CW_BC_PERIODIC && py > 1) return "decomposition: a periodic direction is not split";
+  if (g.nx / px < 6 || (!two_d(g) && g.ny / py < 6)) return "decomposition: patches of at least 6 x 6 points";
+  return nullptr;
 }
 
 // n_sound: RK3::auto_sound_steps (src/dyn/rk3.cpp:69-72) when time_step_sound == 0

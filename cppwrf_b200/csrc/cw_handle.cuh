@@ -17,6 +17,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/cw_output.h"
@@ -55,6 +56,9 @@ inline FieldKind work_kind(int w) {
 struct Member {
   cw_grid g{};
   cw_options o{};
+  bool patched = false;  // a patch of a decomposed domain (cw_decomp_create): fields allocated for `patch` + halo
+  Box patch{};
+  const Box* pbox() const { return patched ? &patch : nullptr; }
   int n_sound = 0;
   int esz = 8;  // element size of the fields (8: FP64 form, 4: mixed form)
   std::vector<cw_layout> L;         // CW_U_1 .. CW_COSA
@@ -92,21 +96,25 @@ struct DevTables {  // the kernels' views of the members and the device scalar t
   V3<R>* qtab = nullptr;  // per member: q1, q2, qn, qtf, qscale, 6 PD faces (kQTab x n_scalars)
   Slabs<R>* lbcq = nullptr;
   Dom<R>* doms_d = nullptr;  // the batch's member descriptors
-  int* starts_d = nullptr;   // the batch's block starts [kind][shape][member]
 };
 
 // a fill point's fields (or the union of consecutive fill points') as a device table: one launch per pass
-// whatever the number of fields (the batch path)
+// whatever the number of fields (the batch path); for a decomposed domain also the exchange boxes, copied first
 struct HaloTable {
   HaloField* f = nullptr;
   unsigned* start = nullptr;
   int nf = 0;
   unsigned total = 0;
   int has_oddface = 0;
+  XchgBox* x = nullptr;
+  unsigned* xstart = nullptr;
+  int nx = 0;
+  unsigned xtotal = 0;
 };
 
 struct HaloSetHost {
   std::vector<HaloField> f;
+  std::vector<XchgBox> x;  // a decomposed domain: the points of other patches each patch receives first
   std::vector<HaloChunk<kHaloSmall>> small;  // the fields in one small chunk (most single domains), or
   std::vector<HaloChunk<kHaloLarge>> large;  // in large chunks
 };
@@ -118,6 +126,7 @@ using namespace cw;
 struct cw_handle {
   int precision = CW_FP64;
   std::vector<Member> m;
+  int decomp_px = 0, decomp_py = 0;  // a decomposed domain (cw_decomp_create): its members are the px x py patches
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int device = -1;  // the CUDA device current at create (every allocation of the handle is on it)

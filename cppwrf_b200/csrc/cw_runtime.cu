@@ -59,16 +59,16 @@ Plan plan_member(Member& M) {
   };
   M.L.resize(CW_Q_1);
   for (int id = 0; id < CW_Q_1; ++id) {
-    M.L[id] = field_layout(M.g, M.o, id);
+    M.L[id] = field_layout(M.g, M.o, id, M.pbox());
     P.f.push_back(take(field_bytes(M.L[id], M.esz)));
   }
   M.LW.resize(W_N);
   for (int w = 0; w < W_N; ++w) {
     const FieldKind k = work_kind(w);
-    M.LW[w] = layout_make(M.g, k.stagger, k.rank, false);
+    M.LW[w] = layout_make(M.g, k.stagger, k.rank, false, M.pbox());
     P.w.push_back(take(work_used(w, M.o) ? field_bytes(M.LW[w], M.esz) : 0));
   }
-  M.Lq = layout_make(M.g, 'M', 3, false);
+  M.Lq = layout_make(M.g, 'M', 3, false, M.pbox());
   for (int n = 0; n < M.o.n_scalars; ++n) {
     P.q1.push_back(take(field_bytes(M.Lq, M.esz)));
     P.qa.push_back(take(field_bytes(M.Lq, M.esz)));
@@ -77,9 +77,9 @@ Plan plan_member(Member& M) {
     P.qsc.push_back(take(field_bytes(M.Lq, M.esz)));
   }
   if (pd_any(M.o)) {
-    M.Lpd[0] = layout_make(M.g, 'U', 3, false);
-    M.Lpd[1] = layout_make(M.g, 'V', 3, false);
-    M.Lpd[2] = layout_make(M.g, 'W', 3, false);
+    M.Lpd[0] = layout_make(M.g, 'U', 3, false, M.pbox());
+    M.Lpd[1] = layout_make(M.g, 'V', 3, false, M.pbox());
+    M.Lpd[2] = layout_make(M.g, 'W', 3, false, M.pbox());
     for (int n = 0; n < M.o.n_scalars; ++n)
       for (int f = 0; f < 6; ++f) P.qpd.push_back(take(field_bytes(M.Lpd[f / 2], M.esz)));
   }
@@ -163,6 +163,8 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   const cw_grid& g = M.g;
   const cw_options& o = M.o;
   D.nx = g.nx; D.ny = g.ny; D.nz = g.nz; D.nyv = nys(g, 'V'); D.two_d = two_d(g); D.do_y = !two_d(g);
+  const Box pb = M.patched ? M.patch : Box{0, g.nx, 0, g.ny};
+  D.pi0 = pb.i0; D.pi1 = pb.i1; D.pj0 = pb.j0; D.pj1 = pb.j1;
   D.bc_x = g.bc_x; D.bc_y = g.bc_y;
   D.spec_x = flat_x(g); D.spec_y = flat_y(g) && !two_d(g);
   D.open_x = g.bc_x == CW_BC_OPEN; D.open_y = g.bc_y == CW_BC_OPEN && !two_d(g);
@@ -241,7 +243,8 @@ std::array<std::array<int, kNumShapes>, kNumKinds> block_starts(cw_handle* h, si
       for (int m = 0; m < n; ++m) {
         const Member& M = h->m[m0 + size_t(m)];
         set(kind, sh, m, int(b));
-        b += blocks_of(kind, M.g.nx, M.g.ny, M.g.nz, nys(M.g, 'V'), sh);
+        const Box pb = M.patched ? M.patch : Box{0, M.g.nx, 0, M.g.ny};
+        b += blocks_of(range_of(kind, M.g.nx, M.g.ny, M.g.nz, nys(M.g, 'V'), pb.i0, pb.i1, pb.j0, pb.j1), kind, sh);
       }
       if (b >= (1ll << 31)) throw std::runtime_error("a batch launch of more than 2^31 blocks");
       set(kind, sh, n, int(b));
@@ -261,7 +264,8 @@ void build_packs(cw_handle* h, const std::vector<Dom<R>>& doms, Packs<R, 1>& ps)
   ps.blocks.push_back(block_starts(h, 0, 1, [&](int kind, int sh, int m, int b) { P.start_[kind][sh][m] = b; }));
   ps.p.push_back(P);
 }
-// a batch: every member's descriptor and block starts in device memory, one pack (one launch per kernel)
+// a batch: every member's descriptor in device memory and the block starts in the launch parameter, one pack (one
+// launch per kernel)
 template <class R>
 void build_packs(cw_handle* h, const std::vector<Dom<R>>& doms, DevTables<R>& T) {
   Packs<R, 0>& ps = T.many;
@@ -269,20 +273,14 @@ void build_packs(cw_handle* h, const std::vector<Dom<R>>& doms, DevTables<R>& T)
   ps.blocks.clear();
   const size_t nm = doms.size();
   if (nm <= 1) return;
-  std::vector<int> st(size_t(kNumKinds * kNumShapes) * (nm + 1));
-  ps.blocks.push_back(block_starts(h, 0, int(nm), [&](int kind, int sh, int m, int b) {
-    st[size_t(kind * kNumShapes + sh) * (nm + 1) + size_t(m)] = b;
-  }));
+  auto P = std::make_unique<Pack<R, 0>>();
+  ps.blocks.push_back(block_starts(h, 0, int(nm), [&](int kind, int sh, int m, int b) { P->start_[kind][sh][m] = b; }));
   CW_CUDA(cudaMalloc(&T.doms_d, nm * sizeof(Dom<R>)));
-  CW_CUDA(cudaMalloc(&T.starts_d, st.size() * sizeof(int)));
   CW_CUDA(cudaMemcpyAsync(T.doms_d, doms.data(), nm * sizeof(Dom<R>), cudaMemcpyHostToDevice, h->stream));
-  CW_CUDA(cudaMemcpyAsync(T.starts_d, st.data(), st.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
-  CW_CUDA(cudaStreamSynchronize(h->stream));  // the host vectors go out of scope
-  Pack<R, 0> P{};
-  P.d = T.doms_d;
-  P.starts = T.starts_d;
-  P.n = int(nm);
-  ps.p.push_back(P);
+  CW_CUDA(cudaStreamSynchronize(h->stream));  // the host vector goes out of scope
+  P->d = T.doms_d;
+  P->n = int(nm);
+  ps.p.push_back(*P);
 }
 
 template <class R>
@@ -387,7 +385,9 @@ HaloField halo_field(const Member& M, const HaloItem& it) {
     default: break;
   }
   f.is_float = M.esz == 4;
-  f.ncell_x = (long long)(f.face_x ? 8 : 6) * L.ny * L.nz;
+  f.xj0 = L.wj0 > 0 ? L.wj0 : 0;
+  f.xj1 = L.wj1 < L.ny ? L.wj1 : L.ny;
+  f.ncell_x = (long long)(f.face_x ? 8 : 6) * (f.xj1 - f.xj0) * L.nz;
   f.ncell = f.ncell_x + (f.two_d ? 0 : (long long)(f.face_y ? 8 : 6) * (L.wi1 - L.wi0) * L.nz);
   return f;
 }
@@ -398,22 +398,69 @@ void finish_haloset(cw_handle*, HaloSetHost& s) {
   if (s.f.size() <= size_t(kHaloSmall)) chunk_fields(s.f, s.small);
   else chunk_fields(s.f, s.large);
 }
+// the points of a field of staggering s ('U', 'V', else mass / W) that a patch owns: its cells' (the faces nx / ny
+// at the domain's east / north edge)
+Box owned_box(const Member& M, char s) {
+  const Box& p = M.patch;
+  return Box{p.i0, (s == 'U' && p.i1 == M.g.nx) ? M.g.nx + 1 : p.i1, p.j0,
+             (s == 'V' && p.j1 == M.g.ny && !two_d(M.g)) ? M.g.ny + 1 : p.j1};
+}
+// a decomposed domain's exchange of one field: every point of member `me`'s allocation window that member `t` owns
+void exchange_boxes(const Member& me, const HaloItem& a, const Member& t, const HaloItem& b, std::vector<XchgBox>& out) {
+  const cw_layout& L = a.L;
+  if (L.uniform) return;
+  const Box o = owned_box(t, L.stagger);
+  XchgBox x{};
+  x.i0 = std::max(L.wi0, o.i0);
+  x.i1 = std::min(L.wi1, o.i1);
+  x.j0 = std::max(L.wj0, o.j0);
+  x.j1 = std::min(L.wj1, o.j1);
+  if (x.i0 >= x.i1 || x.j0 >= x.j1) return;
+  x.src = b.base ? b.base + size_t(b.L.offset) * t.esz : nullptr;
+  x.src_ind = b.ind;
+  x.dst = a.base ? a.base + size_t(L.offset) * me.esz : nullptr;
+  x.dst_ind = a.ind;
+  x.ssj = int(b.L.sj);
+  x.ssk = int(b.L.sk);
+  x.dsj = int(L.sj);
+  x.dsk = int(L.sk);
+  x.nk = L.nz;
+  x.is_float = me.esz == 4;
+  x.ncell = (long long)(x.i1 - x.i0) * (x.j1 - x.j0) * x.nk;
+  out.push_back(x);
+}
+
 template <class R>
 void build_halosets_t(cw_handle* h, DevTables<R>& T) {
   size_t q0 = 0;
+  // a decomposed domain: each member's items per fill point in the same order (the patches share their options),
+  // the exchange-only ones marked (neighbours' points refreshed without a boundary fill)
+  std::vector<std::vector<std::tuple<int, HaloItem, bool>>> items(h->m.size());
+  const bool dec = h->decomp_px > 0;
   for (size_t mi = 0; mi < h->m.size(); ++mi) {
     Member& M = h->m[mi];
     const int ns = M.o.n_scalars;
     auto F = [&](int id, int par = HP_DEFAULT) { return HaloItem{M.base[id], nullptr, M.L[id], par}; };
     auto W = [&](int w, int par = HP_DEFAULT) { return HaloItem{M.wbase[w], nullptr, M.LW[w], par}; };
-    auto add = [&](int set, std::initializer_list<HaloItem> items) {
-      for (const HaloItem& it : items) h->hs[set].f.push_back(halo_field(M, it));
+    auto add = [&](int set, std::initializer_list<HaloItem> its) {
+      for (const HaloItem& it : its) {
+        h->hs[set].f.push_back(halo_field(M, it));
+        if (dec) items[mi].emplace_back(set, it, false);
+      }
+    };
+    auto exchange_only = [&](int set, const HaloItem& it) {
+      if (dec) items[mi].emplace_back(set, it, true);
     };
     const bool spec = specified(M.g);
     add(cw_handle::H_MU1, {F(CW_MU_1)});
     if (xk_fields(M.o)) add(cw_handle::H_XK, {W(W_XKMH), W(W_XKHH)});  // DiffusionDriver::prepare's fill
     add(cw_handle::H_PREP0, {F(CW_U_2), F(CW_V_2), F(CW_W_2), F(CW_T_2), F(CW_PH_2), F(CW_P), F(CW_AL)});
     if (!spec) add(cw_handle::H_PREP0, {F(CW_MU_2)});
+    else {  // tiles: the neighbours' points that spec_bdy_final changed (large_step.cpp:705; the scalars' too)
+      exchange_only(cw_handle::H_PREP0, F(CW_MU_2));
+      for (int n = 0; n < ns; ++n)
+        exchange_only(cw_handle::H_PREP0, HaloItem{nullptr, T.qtab + kQTab * q0 + ns + n, M.Lq, HP_DEFAULT});
+    }
     add(cw_handle::H_PREP1, {F(CW_MUT), F(CW_RU), F(CW_RV), F(CW_RW), F(CW_ALT), F(CW_PHP), F(CW_MUU, HP_ODDFACE_X),
                              F(CW_MUV, HP_ODD_Y), F(CW_WW)});
     add(cw_handle::H_SS0, {F(CW_U_2), F(CW_V_2), F(CW_PH_2), W(W_T_SAVE), W(W_U_SAVE), W(W_V_SAVE), F(CW_MU_2),
@@ -438,6 +485,16 @@ void build_halosets_t(cw_handle* h, DevTables<R>& T) {
     add(cw_handle::H_WS1, {F(CW_W_2)});
     q0 += size_t(ns);
   }
+  if (dec)  // every patch receives, at each fill point, the points of its window that the others own
+    for (size_t me = 0; me < h->m.size(); ++me)
+      for (size_t t = 0; t < h->m.size(); ++t) {
+        if (t == me) continue;
+        if (items[me].size() != items[t].size()) throw std::runtime_error("decomposition: patches differ");
+        for (size_t k = 0; k < items[me].size(); ++k) {
+          const auto& [set, a, xo] = items[me][k];
+          exchange_boxes(h->m[me], a, h->m[t], std::get<1>(items[t][k]), h->hs[set].x);
+        }
+      }
   for (int s = 0; s < cw_handle::H_N; ++s) finish_haloset(h, h->hs[s]);
 }
 
@@ -606,6 +663,8 @@ void free_tables(cw_handle* h) {
   for (auto& kv : h->halo_tabs) {
     cudaFree(kv.second.f);
     cudaFree(kv.second.start);
+    cudaFree(kv.second.x);
+    cudaFree(kv.second.xstart);
   }
   h->halo_tabs.clear();
   cudaFree(h->copies_d);
@@ -624,11 +683,9 @@ void free_tables(cw_handle* h) {
   cudaFree(h->t64.qtab);
   cudaFree(h->t64.lbcq);
   cudaFree(h->t64.doms_d);
-  cudaFree(h->t64.starts_d);
   cudaFree(h->t32.qtab);
   cudaFree(h->t32.lbcq);
   cudaFree(h->t32.doms_d);
-  cudaFree(h->t32.starts_d);
   h->t64 = DevTables<double>{};
   h->t32 = DevTables<float>{};
 }
@@ -822,6 +879,54 @@ __global__ void k_check_div_const(unsigned long long n, unsigned long long seed,
   if (bad) atomicAdd(counts + 1, bad);
 }
 
+// ---- a decomposed domain's fields as whole-domain arrays (cw_decomp_upload / _download)
+// the layout of a field of member M in a run with one patch (tile::whole_layout, src/core/tiles.hpp:98)
+cw_layout whole_layout(const Member& M, int field) {
+  if (field >= CW_Q_1) return layout_make(M.g, 'M', 3, false);
+  return field_layout(M.g, M.o, field);
+}
+// a whole-domain array as member M's allocation: every point of its window (the others 0)
+std::vector<double> to_patch(const cw_layout& Lp, const cw_layout& Lw, const double* whole) {
+  std::vector<double> v(size_t(Lp.total), 0.0);
+  if (Lw.uniform) {
+    std::copy(whole, whole + std::min(Lp.total, Lw.total), v.begin());
+    return v;
+  }
+  for (int k = 0; k < Lp.nz; ++k)
+    for (int j = Lp.wj0; j < Lp.wj1; ++j)
+      for (int i = Lp.wi0; i < Lp.wi1; ++i)
+        v[size_t(Lp.offset + i + j * Lp.sj + k * Lp.sk)] = whole[Lw.offset + i + j * Lw.sj + k * Lw.sk];
+  return v;
+}
+// member M's points into the whole-domain array: the points it owns, with the domain's halo beyond its edges
+void from_patch(const Member& M, const cw_layout& Lp, const cw_layout& Lw, const double* part, double* whole) {
+  if (Lw.uniform) {
+    std::copy(part, part + std::min(Lp.total, Lw.total), whole);
+    return;
+  }
+  const Box o = owned_box(M, Lp.stagger);
+  const int i0 = M.patch.i0 == 0 ? Lp.wi0 : o.i0, i1 = M.patch.i1 == M.g.nx ? Lp.wi1 : o.i1;
+  const int j0 = (two_d(M.g) || M.patch.j0 == 0) ? Lp.wj0 : o.j0;
+  const int j1 = (two_d(M.g) || M.patch.j1 == M.g.ny) ? Lp.wj1 : o.j1;
+  for (int k = 0; k < Lp.nz; ++k)
+    for (int j = j0; j < j1; ++j)
+      for (int i = i0; i < i1; ++i)
+        whole[Lw.offset + i + j * Lw.sj + k * Lw.sk] = part[size_t(Lp.offset + i + j * Lp.sj + k * Lp.sk)];
+}
+// upload a whole-domain array to member mi (a patch: its window)
+void upload_whole(cw_handle* h, int mi, int field, int n, const double* host, size_t count) {
+  const Member& M = h->m.at(size_t(mi));
+  const Loc l = locate(h, mi, field, n);
+  if (!M.patched) {
+    copy_in(h, l, host, count);
+    return;
+  }
+  const cw_layout Lw = whole_layout(M, field);
+  if (count != size_t(Lw.total)) throw std::runtime_error("count != the field's whole-domain layout total");
+  const std::vector<double> v = to_patch(l.L, Lw, host);
+  copy_in(h, l, v.data(), v.size());
+}
+
 // ------------------------------------------------------------------ C ABI
 extern "C" {
 
@@ -857,9 +962,76 @@ int cw_batch_create(int n, const cw_grid* g, const cw_options* o, cw_handle** ou
   });
 }
 
+int cw_decomp_patch(const cw_grid* g, int px, int py, int t, int* box) {
+  return guarded(nullptr, [&] {
+    if (!g || !box || t < 0 || t >= px * py) throw std::runtime_error("bad decomposition arguments");
+    if (const char* why = decomp_unsupported(*g, px, py)) throw std::runtime_error(why);
+    const Box b = patch_box(*g, px, py, t);
+    box[0] = b.i0; box[1] = b.i1; box[2] = b.j0; box[3] = b.j1;
+    return 0;
+  });
+}
+
+int cw_decomp_create(const cw_grid* g, const cw_options* o, int px, int py, cw_handle** out) {
+  return guarded(nullptr, [&] {
+    if (!g || !o || !out) throw std::runtime_error("null argument");
+    if (const char* why = decomp_unsupported(*g, px, py)) throw std::runtime_error(why);
+    auto h = std::make_unique<cw_handle>();
+    h->precision = o->precision;
+    h->decomp_px = px;
+    h->decomp_py = py;
+    for (int t = 0; t < px * py; ++t) {
+      Member M = make_member(*g, *o);
+      M.patched = true;
+      M.patch = patch_box(*g, px, py, t);
+      h->m.push_back(std::move(M));
+    }
+    CW_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+    setup(h.get());
+    *out = h.release();
+    return 0;
+  });
+}
+
+int cw_decomp_upload(cw_handle* h, int field, int n, const double* host, size_t count) {
+  return guarded(h, [&] {
+    if (!h || !host || h->decomp_px == 0) throw std::runtime_error("not a decomposed domain");
+    for (int mi = 0; mi < int(h->m.size()); ++mi) upload_whole(h, mi, field, n, host, count);
+    CW_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+  });
+}
+
+int cw_decomp_download(cw_handle* h, int field, int n, double* host, size_t count) {
+  return guarded(h, [&] {
+    if (!h || !host || h->decomp_px == 0) throw std::runtime_error("not a decomposed domain");
+    const cw_layout Lw = whole_layout(h->m[0], field);
+    if (count != size_t(Lw.total)) throw std::runtime_error("count != the field's whole-domain layout total");
+    std::fill(host, host + count, 0.0);
+    for (int mi = 0; mi < int(h->m.size()); ++mi) {
+      const Loc l = locate(h, mi, field, n);
+      std::vector<double> part(size_t(l.L.total));
+      copy_out(h, l, part.data(), part.size());
+      from_patch(h->m[size_t(mi)], l.L, Lw, part.data(), host);
+    }
+    return 0;
+  });
+}
+
+int cw_decomp_upload_case(cw_handle* h, cw_case* c) {
+  if (!h || !c || h->decomp_px == 0) return -1;
+  for (int mi = 0; mi < int(h->m.size()); ++mi) {
+    const int rc = cw_member_upload_case(h, mi, c);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
 int cw_batch_add(cw_handle* h, const cw_grid* g, const cw_options* o, int* member) {
   return guarded(h, [&] {
     if (!h || !g || !o) throw std::runtime_error("null argument");
+    if (h->decomp_px) throw std::runtime_error("a decomposed domain's patches are fixed");
     if (int(h->m.size()) >= kMaxMembers) throw std::runtime_error("the batch is full");
     if (o->precision != h->precision) throw std::runtime_error("batch members must share the precision");
     Member M = make_member(*g, *o);
@@ -883,6 +1055,7 @@ int cw_batch_add(cw_handle* h, const cw_grid* g, const cw_options* o, int* membe
 int cw_batch_adopt(cw_handle* h, cw_handle* single, int* member) {
   return guarded(h, [&] {
     if (!h || !single || single == h) throw std::runtime_error("bad arguments");
+    if (h->decomp_px || single->decomp_px) throw std::runtime_error("a decomposed domain's patches are fixed");
     if (single->m.size() != 1) throw std::runtime_error("the adopted handle must hold one domain");
     if (single->precision != h->precision) throw std::runtime_error("batch members must share the precision");
     if (int(h->m.size()) >= kMaxMembers) throw std::runtime_error("the batch is full");
@@ -902,6 +1075,7 @@ int cw_batch_adopt(cw_handle* h, cw_handle* single, int* member) {
 int cw_batch_release(cw_handle* h, int member, cw_handle** out) {
   return guarded(h, [&] {
     if (!h || !out || member < 0 || member >= int(h->m.size())) throw std::runtime_error("member index out of range");
+    if (h->decomp_px) throw std::runtime_error("a decomposed domain's patches are fixed");
     CW_CUDA(cudaStreamSynchronize(h->stream));
     auto s = std::make_unique<cw_handle>();
     s->precision = h->precision;
@@ -922,6 +1096,7 @@ int cw_batch_release(cw_handle* h, int member, cw_handle** out) {
 int cw_batch_remove(cw_handle* h, int member) {
   return guarded(h, [&] {
     if (!h || member < 0 || member >= int(h->m.size())) throw std::runtime_error("member index out of range");
+    if (h->decomp_px) throw std::runtime_error("a decomposed domain's patches are fixed");
     CW_CUDA(cudaStreamSynchronize(h->stream));
     invalidate_graph(h);
     free_tables(h);
@@ -1403,11 +1578,19 @@ int cw_member_upload_case(cw_handle* h, int mi, cw_case* c) {
   int rc = cw_member_set_vertical(h, mi, &v);
   if (rc) return rc;
   const Member& M = h->m.at(size_t(mi));
+  // a patch of a decomposed domain takes its window of the case's whole-domain fields
+  auto up = [&](int id, int n, const double* data, size_t count) {
+    return guarded(h, [&] {
+      upload_whole(h, mi, id, n, data, count);
+      CW_CUDA(cudaStreamSynchronize(h->stream));
+      return 0;
+    });
+  };
   for (int id = 0; id < CW_Q_1; ++id) {
     double* data = nullptr;
     cw_layout L{};
     cw_case_field(c, id, 0, &data, &L);
-    rc = cw_member_upload(h, mi, id, 0, data, size_t(L.total));
+    rc = up(id, 0, data, size_t(L.total));
     if (rc) return rc;
   }
   for (int n = 0; n < M.o.n_scalars; ++n)
@@ -1415,7 +1598,7 @@ int cw_member_upload_case(cw_handle* h, int mi, cw_case* c) {
       double* data = nullptr;
       cw_layout L{};
       cw_case_field(c, id, n, &data, &L);
-      rc = cw_member_upload(h, mi, id, n, data, size_t(L.total));
+      rc = up(id, n, data, size_t(L.total));
       if (rc) return rc;
     }
   if (M.o.lbc) {

@@ -89,12 +89,43 @@ struct Launcher {
       CW_CUDA(cudaMemcpy(t.f, f.data(), f.size() * sizeof(HaloField), cudaMemcpyHostToDevice));
       CW_CUDA(cudaMemcpy(t.start, st.data(), st.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
     }
+    // a decomposed domain: the pending fill points' exchange boxes (each once)
+    std::vector<XchgBox> x;
+    for (int set : pend)
+      for (const XchgBox& b : h->hs[set].x) {
+        bool dup = false;
+        for (const XchgBox& y : x)
+          dup |= y.dst == b.dst && y.dst_ind == b.dst_ind && y.src == b.src && y.src_ind == b.src_ind && y.i0 == b.i0 &&
+                 y.j0 == b.j0;
+        if (!dup) x.push_back(b);
+      }
+    if (!x.empty()) {
+      std::vector<unsigned> xs(x.size() + 1);
+      long long xt = 0;
+      for (size_t n = 0; n < x.size(); ++n) {
+        xs[n] = unsigned(xt);
+        xt += x[n].ncell;
+      }
+      if (xt >= (1ll << 31)) throw std::runtime_error("an exchange of more than 2^31 points");
+      xs[x.size()] = unsigned(xt);
+      t.nx = int(x.size());
+      t.xtotal = unsigned(xt);
+      CW_CUDA(cudaMalloc(&t.x, x.size() * sizeof(XchgBox)));
+      CW_CUDA(cudaMalloc(&t.xstart, xs.size() * sizeof(unsigned)));
+      CW_CUDA(cudaMemcpy(t.x, x.data(), x.size() * sizeof(XchgBox), cudaMemcpyHostToDevice));
+      CW_CUDA(cudaMemcpy(t.xstart, xs.data(), xs.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+    }
     return h->halo_tabs.emplace(pend, t).first->second;
   }
   void flush() {
     if (pend.empty()) return;
     if (h->m.size() > 1) {
       const HaloTable& t = halo_table();
+      if (t.xtotal > 0 && !plan) {  // a decomposed domain: the exchange first, then the boundary fill
+        begin("k_exchange");
+        k_exchange<<<(t.xtotal + 255u) / 256u, 256, 0, h->stream>>>(t.x, t.xstart, t.nx);
+        check();
+      }
       if (t.total > 0 && !plan) {
         const unsigned nb = (t.total + 255u) / 256u;
         for (int pass = 0; pass < (t.has_oddface ? 2 : 1); ++pass) {
@@ -209,7 +240,7 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
   // zone's, updated from the boundary data), and the fills after the substeps (H_POST, H_FIN) refresh them
   // before anything reads them; those fills, and the spec zone's zero-gradient w of every substep but the
   // last (overwritten by the next one, read only after the substeps), are left out
-  bool spec_all = true;
+  bool spec_all = h->decomp_px * h->decomp_py <= 1;  // a decomposed domain takes every fill: its patches read each other's points
   int nq = 0;  // the most species of a member
   for (const Member& M : h->m) {
     spec_all &= M.o.lbc != 0 && flat_x(M.g) && flat_y(M.g) && !two_d(M.g);
@@ -271,7 +302,7 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
       if (rk == 3 && any_pd) {
         L.run_t("k_q_pre_pd", RG_MASS, nq, KV(k_q_pre_pd), d, rk);
         L.halo(cw_handle::H_Q1PD);
-        L.run_t("k_q_face_pd", RG_STAG, 1, KV(k_q_face_pd), d, rk);
+        L.run_t("k_q_face_pd", RG_FACES, 1, KV(k_q_face_pd), d, rk);
         L.run_t("k_q_scale_pd", RG_MASS, nq, KV(k_q_scale_pd), d, rk);
         L.halo(cw_handle::H_SCPD);
         L.run_t("k_q_update_pd", RG_MASS, nq, KV(k_q_update_pd), d, rk);

@@ -48,6 +48,10 @@ template <class T>
 struct Dom {
   // grid and options
   int nx, ny, nz, nyv, two_d, do_y;
+  // the mass points this member computes, pi0 <= i < pi1, pj0 <= j < pj1, in the domain's indices: the whole domain,
+  // or a patch of a domain decomposed over several members (cw_decomp_create), whose fields are allocated for the
+  // patch and a halo of 3 and indexed with the domain's indices; the edge patches also own the faces nx / ny
+  int pi0, pi1, pj0, pj1;
   int bc_x, bc_y, spec_x, spec_y;  // spec_*: specified or open in that direction (degraded orders)
   int sx, sy;                      // specified in that direction (spec zone, upstream boundary velocity)
   int open_x, open_y;              // open (radiation) in that direction; open_y is 0 in 2-D
@@ -104,7 +108,7 @@ struct Dom {
 // arithmetic) and no store of a kernel can alias them. A batch (NM = 0, any number of members): the members'
 // descriptors and block prefix sums in device memory, so one launch of each kernel covers the whole batch.
 // start(kind, shape, m) is member m's first block of a launch over the index range `kind` in block shape `shape`.
-constexpr int kNumKinds = 6;
+constexpr int kNumKinds = 7;
 constexpr int kNumShapes = 3;  // point-kernel block shapes (autotuned per kernel): 128 x 1, 64 x 2, 32 x 4
 template <class R, int NM>
 struct Pack {
@@ -115,12 +119,12 @@ struct Pack {
 };
 template <class R>
 struct Pack<R, 0> {
-  const Dom<R>* __restrict__ d;      // n descriptors (device memory, written before the launch)
-  const int* __restrict__ starts;    // [kNumKinds][kNumShapes][n + 1]
+  const Dom<R>* __restrict__ d;  // n descriptors (device memory, written before the launch)
   int n;
-  __device__ __forceinline__ int start(int kind, int shape, int m) const {
-    return __ldg(starts + (kind * kNumShapes + shape) * (n + 1) + m);
-  }
+  // the block starts in the parameter (the constant bank: a block's binary search over them is uniform and
+  // needs no global load), 18.5 KB for the largest batch, within the 32 KB parameter limit
+  int start_[kNumKinds][kNumShapes][kMaxMembers + 1];
+  __device__ __forceinline__ int start(int kind, int shape, int m) const { return start_[kind][shape][m]; }
 };
 template <class R, int NM>
 __device__ __forceinline__ int member_of(const Pack<R, NM>& P, int kind, int shape, int b) {
@@ -229,7 +233,22 @@ struct HaloField {
   int gnx, gny;      // the member's mass-point extents
   unsigned char periodic_x, periodic_y, flat_x, flat_y, two_d, face_x, face_y, odd_x, odd_y, oddface_x, is_float,
       pad;
+  int xj0, xj1;              // the x pass's rows: the window's rows inside the domain
   long long ncell_x, ncell;  // x-pass cells, all cells
+};
+// A decomposed domain's exchange (the halo exchange of core/halo.cpp:120-129 / tiles.hpp:6-12): the rectangle
+// i0 <= i < i1, j0 <= j < j1 (all nk levels) of a field that a patch holds in its halo and another patch owns,
+// copied from the owner's allocation into the patch's at the same domain indices. src / dst: element (0, 0, 0);
+// src_ind / dst_ind (scalars whose buffers swap): a device V3 whose .p is read at run time instead.
+struct XchgBox {
+  const void* src;
+  const void* src_ind;
+  void* dst;
+  const void* dst_ind;
+  int ssj, ssk, dsj, dsk;
+  int i0, i1, j0, j1, nk;
+  int is_float;
+  long long ncell;
 };
 // The fields of one launch, passed by value as a __grid_constant__ parameter (no descriptor is read from
 // global memory). Two capacities: a fill point of a single domain fits the small one; a batch's fill point

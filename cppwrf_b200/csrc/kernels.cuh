@@ -23,35 +23,49 @@ enum RangeKind {
   RG_COLS_MASS,   // columns [0, nx) x [0, ny)
   RG_RING,        // boundary ring b = 0: pos in [0, max(nx, ny)+1), k in [0, nz+1), 4 sides
   RG_MASS_W,      // [0, nx) x [0, ny) x [0, nz+1)
+  RG_FACES,       // as RG_STAG; in a patch, the faces of its cells up to the face after its last cell
 };
 struct Range {
   int i0, i1, j0, j1, k0, k1;
 };
-__host__ __device__ __forceinline__ Range range_of(int kind, int nx, int ny, int nz, int nyv) {
+// A member's points of an index range. The whole domain: the range as above. A patch (pi0 <= i < pi1,
+// pj0 <= j < pj1 of the domain's mass points): the points it owns -- its cells, the faces between them and, at the
+// domain's east / north edge, the faces nx / ny -- except RG_FACES, which also takes the face after its last cell
+// (owned by the next patch; a kernel of face fluxes computes it again from the values around it). The ring is not
+// clipped: its kernel keeps the points the member owns.
+__host__ __device__ __forceinline__ Range range_of(int kind, int nx, int ny, int nz, int nyv, int pi0, int pi1, int pj0,
+                                                   int pj1) {
+  const int iu = pi1 == nx ? nx + 1 : pi1, jv = pj1 == ny ? nyv : pj1;  // owned faces end
+  const int jf = nyv > ny ? pj1 + 1 : pj1;                               // RG_FACES: one face more (3-D)
   switch (kind) {
-    case RG_STAG: return {0, nx + 1, 0, nyv, 0, nz + 1};
-    case RG_MASS: return {0, nx, 0, ny, 0, nz};
-    case RG_COLS_STAG: return {0, nx + 1, 0, nyv, 0, 1};
-    case RG_COLS_MASS: return {0, nx, 0, ny, 0, 1};
+    case RG_STAG: return {pi0, iu, pj0, jv, 0, nz + 1};
+    case RG_MASS: return {pi0, pi1, pj0, pj1, 0, nz};
+    case RG_COLS_STAG: return {pi0, iu, pj0, jv, 0, 1};
+    case RG_COLS_MASS: return {pi0, pi1, pj0, pj1, 0, 1};
     case RG_RING: return {0, (nx > ny ? nx : ny) + 1, 0, nz + 1, 0, 4};
-    default: return {0, nx, 0, ny, 0, nz + 1};
+    case RG_FACES: return {pi0, pi1 + 1, pj0, jf, 0, nz + 1};
+    default: return {pi0, pi1, pj0, pj1, 0, nz + 1};
   }
 }
+template <class R>
+__host__ __device__ __forceinline__ Range range_of(int kind, const Dom<R>& D) {
+  return range_of(kind, D.nx, D.ny, D.nz, D.nyv, D.pi0, D.pi1, D.pj0, D.pj1);
+}
 __host__ __device__ __forceinline__ bool is_column(int kind) { return kind == RG_COLS_STAG || kind == RG_COLS_MASS; }
-__host__ __device__ __forceinline__ int blocks_of(int kind, int nx, int ny, int nz, int nyv, int shape = 0) {
-  const Range r = range_of(kind, nx, ny, nz, nyv);
+__host__ __device__ __forceinline__ int blocks_of(const Range& r, int kind, int shape = 0) {
   if (is_column(kind)) return cdiv(r.i1 - r.i0, CX) * (r.j1 - r.j0) * (r.k1 - r.k0);
   return cdiv(r.i1 - r.i0, shape_x(shape)) * cdiv(r.j1 - r.j0, shape_y(shape)) * (r.k1 - r.k0);
 }
-// thread -> (member, i, j, k) of a point kernel launched with block shape SH; false past the range
+// thread -> (member, i, j, k) of a point kernel launched with block shape SH; false past the range (the range in rg)
 template <int SH, class R, int NM>
-__device__ __forceinline__ bool thread_index(const Pack<R, NM>& P, int kind, const Dom<R>*& Dp, int& i, int& j, int& k) {
+__device__ __forceinline__ bool thread_index(const Pack<R, NM>& P, int kind, const Dom<R>*& Dp, int& i, int& j, int& k,
+                                             Range& r) {
   constexpr int sx = shape_x(SH), sy = shape_y(SH);
   const int b = blockIdx.x;
   const int m = member_of(P, kind, SH, b);
   const Dom<R>& D = P.d[m];
   Dp = &D;
-  const Range r = range_of(kind, D.nx, D.ny, D.nz, D.nyv);
+  r = range_of(kind, D);
   const int bx = cdiv(r.i1 - r.i0, sx), by = cdiv(r.j1 - r.j0, sy);
   int local = b - P.start(kind, SH, m);
   const int bi = local % bx;
@@ -61,6 +75,11 @@ __device__ __forceinline__ bool thread_index(const Pack<R, NM>& P, int kind, con
   i = r.i0 + bi * sx + int(threadIdx.x) % sx;
   j = r.j0 + bj * sy + int(threadIdx.x) / sx;
   return i < r.i1 && j < r.j1;
+}
+template <int SH, class R, int NM>
+__device__ __forceinline__ bool thread_index(const Pack<R, NM>& P, int kind, const Dom<R>*& Dp, int& i, int& j, int& k) {
+  Range r;
+  return thread_index<SH>(P, kind, Dp, i, j, k, r);
 }
 
 // ------------------------------------------------------------------ copies and halos
@@ -126,7 +145,8 @@ __device__ __forceinline__ void halo_cell(const HaloField& f, unsigned c, int pa
     const unsigned na = f.face_x ? 8 : 6;
     const int a = int(c % na);
     const unsigned r = c / na;
-    const int j = int(r % unsigned(f.lny)), k = int(r / unsigned(f.lny));
+    const unsigned nr = unsigned(f.xj1 - f.xj0);
+    const int j = f.xj0 + int(r % nr), k = int(r / nr);
     const int i = halo_pos(a, f.gnx, f.face_x);
     if (i < f.wi0 || i >= f.wi1) return;
     // the last face row of a periodic y-staggered field is a y-pass slot (a copy of row 0): its x halo is the y
@@ -191,6 +211,32 @@ static __global__ void k_halo_tab(const HaloField* __restrict__ fs, const unsign
   const unsigned c = t - __ldg(start + lo);
   if (f.is_float) halo_cell<float>(f, c, pass);
   else halo_cell<double>(f, c, pass);
+}
+
+// a decomposed domain's exchange: one thread per received point of every box of the table
+static __global__ void k_exchange(const XchgBox* __restrict__ bs, const unsigned* __restrict__ start, int nb) {
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= __ldg(start + nb)) return;
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(start + mid) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  const XchgBox b = bs[lo];
+  const unsigned c = t - __ldg(start + lo);
+  const unsigned wi = unsigned(b.i1 - b.i0), wj = unsigned(b.j1 - b.j0);
+  const int i = b.i0 + int(c % wi), j = b.j0 + int((c / wi) % wj), k = int(c / (wi * wj));
+  const long long s = i + (long long)j * b.ssj + (long long)k * b.ssk, d = i + (long long)j * b.dsj + (long long)k * b.dsk;
+  if (b.is_float) {
+    const float* src = b.src_ind ? static_cast<const V3<float>*>(b.src_ind)->p : static_cast<const float*>(b.src);
+    float* dst = b.dst_ind ? static_cast<const V3<float>*>(b.dst_ind)->p : static_cast<float*>(b.dst);
+    dst[d] = src[s];
+  } else {
+    const double* src = b.src_ind ? static_cast<const V3<double>*>(b.src_ind)->p : static_cast<const double*>(b.src);
+    double* dst = b.dst_ind ? static_cast<const V3<double>*>(b.dst_ind)->p : static_cast<double*>(b.dst);
+    dst[d] = src[s];
+  }
 }
 
 // ------------------------------------------------------------------ rk_step_prep
@@ -832,7 +878,7 @@ __device__ __forceinline__ bool spec_at(Ring r, int i, int j, int& sl, int& pos)
 // Also mu_tend = 0 (zero_tend of a run with lateral boundaries) at rk 2 and 3, and with lateral
 // boundaries the spec zone's tendencies from the boundary slabs.
 template <class R, int NM, int SH, bool OP>
-__global__ void __launch_bounds__(PX) k_tend(const __grid_constant__ Pack<R, NM> P, int rk) {
+__global__ void __launch_bounds__(PX, 10) k_tend(const __grid_constant__ Pack<R, NM> P, int rk) {
   constexpr int SX = shape_x(SH), SY = shape_y(SH);
   // the horizontal face fluxes of the block's tile, each evaluated once (u, v, w, theta): x faces i0 .. i0 + SX
   // of each row, y faces j0 .. j0 + SY of each column
@@ -840,7 +886,8 @@ __global__ void __launch_bounds__(PX) k_tend(const __grid_constant__ Pack<R, NM>
   __shared__ R sfy[4][SY + 1][SX];
   const Dom<R>* Dp;
   int i, j, k;
-  const bool in = thread_index<SH>(P, RG_STAG, Dp, i, j, k);
+  Range r;
+  const bool in = thread_index<SH>(P, RG_STAG, Dp, i, j, k, r);
   const Dom<R>& D = *Dp;
   const int tx = int(threadIdx.x) % SX, ty = int(threadIdx.x) / SX;
   const int nx = D.nx, ny = D.ny, nz = D.nz;
@@ -848,15 +895,17 @@ __global__ void __launch_bounds__(PX) k_tend(const __grid_constant__ Pack<R, NM>
   const int ui0 = D.bc_x != CW_BC_PERIODIC ? 1 : 0;
   const int vj0 = (D.bc_y != CW_BC_PERIODIC && D.do_y) ? 1 : 0;
   const bool dy = D.do_y;
-  // the faces a point of each tendency's range uses (x faces f of its row, y faces f of its column)
-  auto ux = [&](int f) { return j < ny && k < nz && f >= ui0 && f <= nx; };
-  auto uy = [&](int f) { return dy && i >= ui0 && i < nx && k < nz && f >= 0 && f <= ny; };
-  auto vx = [&](int f) { return dy && j >= vj0 && j < ny && k < nz && f >= 0 && f <= nx; };
-  auto vy = [&](int f) { return dy && i < nx && k < nz && f >= vj0 && f <= ny; };
-  auto wx = [&](int f) { return j < ny && k >= 1 && f >= 0 && f <= nx; };
-  auto wy = [&](int f) { return dy && i < nx && k >= 1 && f >= 0 && f <= ny; };
-  auto tx_ = [&](int f) { return j < ny && k < nz && f >= 0 && f <= nx; };
-  auto ty_ = [&](int f) { return dy && i < nx && k < nz && f >= 0 && f <= ny; };
+  // the faces a point of each tendency's range uses (x faces f of its row, y faces f of its column), within the
+  // member's range: up to the face after its last point, in its rows (x faces) / columns (y faces)
+  const bool rx = j < r.j1, ry = i < r.i1;
+  auto ux = [&](int f) { return rx && j < ny && k < nz && f >= ui0 && f <= nx && f <= r.i1; };
+  auto uy = [&](int f) { return ry && dy && i >= ui0 && i < nx && k < nz && f >= 0 && f <= ny && f <= r.j1; };
+  auto vx = [&](int f) { return rx && dy && j >= vj0 && j < ny && k < nz && f >= 0 && f <= nx && f <= r.i1; };
+  auto vy = [&](int f) { return ry && dy && i < nx && k < nz && f >= vj0 && f <= ny && f <= r.j1; };
+  auto wx = [&](int f) { return rx && j < ny && k >= 1 && f >= 0 && f <= nx && f <= r.i1; };
+  auto wy = [&](int f) { return ry && dy && i < nx && k >= 1 && f >= 0 && f <= ny && f <= r.j1; };
+  auto tx_ = [&](int f) { return rx && j < ny && k < nz && f >= 0 && f <= nx && f <= r.i1; };
+  auto ty_ = [&](int f) { return ry && dy && i < nx && k < nz && f >= 0 && f <= ny && f <= r.j1; };
   const bool xe = tx == SX - 1, ye = ty == SY - 1;  // the tile's last column / row also takes the next face
   if (ux(i)) sfx[0][ty][tx] = tu_fx(D, i, j, k);
   if (xe && ux(i + 1)) sfx[0][ty][SX] = tu_fx(D, i + 1, j, k);
@@ -1404,7 +1453,7 @@ __global__ void __launch_bounds__(PX) k_smag(const __grid_constant__ Pack<R, NM>
 }
 
 template <class R, int NM, int SH>
-__global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R, NM> P) {
+__global__ void __launch_bounds__(PX, 10) k_tendf_rk1(const __grid_constant__ Pack<R, NM> P) {
   const Dom<R>* Dp;
   int i, j, k;
   if (!thread_index<SH>(P, RG_STAG, Dp, i, j, k)) return;
@@ -1531,6 +1580,14 @@ __global__ void __launch_bounds__(PX) k_tendf_rk1(const __grid_constant__ Pack<R
 // flow_dep_bdy of the scalars without boundary data, zero_grad_bdy of w. The other boundary operations run
 // inside the kernels that compute the same points (k_tendf_rk1, k_tend, k_uv, k_ac, k_q_tendf_rk1).
 enum RingOp { RO_FINAL = 0, RO_FLOW_DEP, RO_ZERO_GRAD_W };
+// the member computes point (i, j) of a field of staggering s ('u': x faces, 'v': y faces, else mass points): its
+// patch's points (the whole domain's without a decomposition)
+template <class R>
+__device__ __forceinline__ bool owns(const Dom<R>& D, int i, int j, char s) {
+  const int iu = (s == 'u' && D.pi1 == D.nx) ? D.nx + 1 : D.pi1;
+  const int jv = (s == 'v' && D.pj1 == D.ny) ? D.nyv : D.pj1;
+  return i >= D.pi0 && i < iu && j >= D.pj0 && j < jv;
+}
 template <class R, int NM>
 __global__ void __launch_bounds__(PX) k_ring(const __grid_constant__ Pack<R, NM> P, int op, int rk) {
   const Dom<R>* Dp;
@@ -1544,7 +1601,7 @@ __global__ void __launch_bounds__(PX) k_ring(const __grid_constant__ Pack<R, NM>
     case RO_ZERO_GRAD_W: {  // zero_grad_bdy on w (KZeroGrad, lateral_bc.cpp:143-159)
       int i, j;
       const Ring r = ring_for(nx, ny, 'h');
-      if (!r.map(pos, side, 0, i, j)) return;
+      if (!r.map(pos, side, 0, i, j) || !owns(D, i, j, 'h')) return;
       const int ic = i < 1 ? 1 : (i > r.ibe - 1 ? r.ibe - 1 : i);
       const int jc = j < 1 ? 1 : (j > r.jbe - 1 ? r.jbe - 1 : j);
       switch (side) {
@@ -1559,15 +1616,15 @@ __global__ void __launch_bounds__(PX) k_ring(const __grid_constant__ Pack<R, NM>
       int i, j;
       const int sl = slab_of_side(side);
       const R dtbc = R(*D.dtbc);
-      if (k < nz && ring_for(nx, ny, 'u').map(pos, side, 0, i, j)) {
+      if (k < nz && ring_for(nx, ny, 'u').map(pos, side, 0, i, j) && owns(D, i, j, 'u')) {
         const R bval = slab_val(D.lbc_var[0], sl, pos, k, 0, dtbc);
         D.u2(i, j, k) = D.msfuy(i, j) * bval / (R(D.c1h[k]) * D.muus(i, j, 0) + R(D.c2h[k]));
       }
-      if (k < nz && ring_for(nx, ny, 'v').map(pos, side, 0, i, j)) {
+      if (k < nz && ring_for(nx, ny, 'v').map(pos, side, 0, i, j) && owns(D, i, j, 'v')) {
         const R bval = slab_val(D.lbc_var[1], sl, pos, k, 0, dtbc);
         D.v2(i, j, k) = D.msfvx(i, j) * bval / (R(D.c1h[k]) * D.muvs(i, j, 0) + R(D.c2h[k]));
       }
-      if (k < nz && ring_for(nx, ny, 't').map(pos, side, 0, i, j)) {
+      if (k < nz && ring_for(nx, ny, 't').map(pos, side, 0, i, j) && owns(D, i, j, 't')) {
         const R bval = slab_val(D.lbc_var[2], sl, pos, k, 0, dtbc);
         D.t2(i, j, k) = R(1) * bval / (R(D.c1h[k]) * D.muts(i, j, 0) + R(D.c2h[k]));
         for (int n = 0; n < D.n_scalars; ++n)
@@ -1576,11 +1633,11 @@ __global__ void __launch_bounds__(PX) k_ring(const __grid_constant__ Pack<R, NM>
             D.q2[n](i, j, k) = R(1) * qb / (R(D.c1h[k]) * D.muts(i, j, 0) + R(D.c2h[k]));
           }
       }
-      if (ring_for(nx, ny, 'h').map(pos, side, 0, i, j)) {
+      if (ring_for(nx, ny, 'h').map(pos, side, 0, i, j) && owns(D, i, j, 'h')) {
         const R bval = slab_val(D.lbc_var[3], sl, pos, k, 0, dtbc);
         D.ph2(i, j, k) = R(1) * bval / (R(D.c1f[k]) * D.muts(i, j, 0) + R(D.c2f[k]));
       }
-      if (k == 0 && ring_for(nx, ny, 'm').map(pos, side, 0, i, j)) {
+      if (k == 0 && ring_for(nx, ny, 'm').map(pos, side, 0, i, j) && owns(D, i, j, 'm')) {
         const R bval = slab_val(D.lbc_var[4], sl, pos, 0, 0, dtbc);
         D.mu2(i, j, 0) = R(1) * bval / R(1);
       }
@@ -1590,7 +1647,7 @@ __global__ void __launch_bounds__(PX) k_ring(const __grid_constant__ Pack<R, NM>
       if (k >= nz) return;
       int i, j;
       const Ring r = ring_for(nx, ny, 'q');
-      if (!r.map(pos, side, 0, i, j)) return;
+      if (!r.map(pos, side, 0, i, j) || !owns(D, i, j, 'q')) return;
       const int ic = i < 1 ? 1 : (i > r.ibe - 1 ? r.ibe - 1 : i);
       const int jc = j < 1 ? 1 : (j > r.jbe - 1 ? r.jbe - 1 : j);
       for (int n = 0; n < D.n_scalars; ++n) {

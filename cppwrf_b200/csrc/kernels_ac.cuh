@@ -83,7 +83,7 @@ __device__ __forceinline__ R uv_dp(const Dom<R>& D, int i, int j, int k, R mface
 // u += dts ru_tend (LateralBC::update_uv, lateral_bc.cpp:353-361) instead, and so do the faces of open boundaries
 // (no pressure gradient or divergence damping on them, :175-184)
 template <class R, int NM, int SH>
-__global__ void __launch_bounds__(PX) k_uv(const __grid_constant__ Pack<R, NM> P, int rk) {
+__global__ void __launch_bounds__(PX, 10) k_uv(const __grid_constant__ Pack<R, NM> P, int rk) {
   const Dom<R>* Dp;
   int i, j, k;
   if (!thread_index<SH>(P, RG_STAG, Dp, i, j, k)) return;
@@ -264,23 +264,26 @@ __device__ R q_adv(const Dom<R>& D, const V3<R>& q, int i, int j, int k, R fx0, 
 // KUpdate (:145-156) for the non-PD species of this stage; the horizontal face fluxes of the block's tile
 // once, in shared memory
 template <class R, int NM, int SH>
-__global__ void __launch_bounds__(PX) k_q_update(const __grid_constant__ Pack<R, NM> P, int rk) {
+__global__ void __launch_bounds__(PX, 12) k_q_update(const __grid_constant__ Pack<R, NM> P, int rk) {
   constexpr int SX = shape_x(SH), SY = shape_y(SH);
   __shared__ R sfx[SY][SX + 1];
   __shared__ R sfy[SY + 1][SX];
   const Dom<R>* Dp;
   int i, j, k;
-  const bool in = thread_index<SH>(P, RG_MASS, Dp, i, j, k);
+  Range r;
+  const bool in = thread_index<SH>(P, RG_MASS, Dp, i, j, k, r);
   const Dom<R>& D = *Dp;
   const int n = blockIdx.y;  // the species (uniform in the block)
   if (n >= D.n_scalars || q_is_pd(D, n, rk)) return;
   const int tx = int(threadIdx.x) % SX, ty = int(threadIdx.x) / SX;
   const int nx = D.nx, ny = D.ny;
   const V3<R> q = D.q2[n];
-  if (j < ny && i <= nx) sfx[ty][tx] = sc_fx(D, q, D.ru_m, i, j, k, false);
-  if (tx == SX - 1 && j < ny && i + 1 <= nx) sfx[ty][SX] = sc_fx(D, q, D.ru_m, i + 1, j, k, false);
-  if (D.do_y && i < nx && j <= ny) sfy[ty][tx] = sc_fy(D, q, D.rv_m, i, j, k, false);
-  if (D.do_y && ty == SY - 1 && i < nx && j + 1 <= ny) sfy[SY][tx] = sc_fy(D, q, D.rv_m, i, j + 1, k, false);
+  // the faces of the member's cells (up to the face after its last one), in its rows / columns
+  const bool rx = j < r.j1 && j < ny, ry = i < r.i1 && i < nx;
+  if (rx && i <= nx && i <= r.i1) sfx[ty][tx] = sc_fx(D, q, D.ru_m, i, j, k, false);
+  if (tx == SX - 1 && rx && i + 1 <= nx && i + 1 <= r.i1) sfx[ty][SX] = sc_fx(D, q, D.ru_m, i + 1, j, k, false);
+  if (D.do_y && ry && j <= ny && j <= r.j1) sfy[ty][tx] = sc_fy(D, q, D.rv_m, i, j, k, false);
+  if (D.do_y && ty == SY - 1 && ry && j + 1 <= ny && j + 1 <= r.j1) sfy[SY][tx] = sc_fy(D, q, D.rv_m, i, j + 1, k, false);
   __syncthreads();
   if (!in) return;
   const R dt_rk = R(rk == 1 ? D.dt / 3.0 : (rk == 2 ? 0.5 * D.dt : D.dt));
@@ -339,10 +342,11 @@ __device__ void pd_fz(const Dom<R>& D, const V3<R>& q, const V3<R>& qo, R dt, in
 // thread per face point for all species: the Courant number and the mass factor of a face (the expressions
 // of pd_fx / pd_fy / pd_fz) do not depend on the species and are evaluated once.
 template <class R, int NM, int SH>
-__global__ void __launch_bounds__(PX) k_q_face_pd(const __grid_constant__ Pack<R, NM> P, int rk) {
+__global__ void __launch_bounds__(PX, 10) k_q_face_pd(const __grid_constant__ Pack<R, NM> P, int rk) {
   const Dom<R>* Dp;
   int i, j, k;
-  if (!thread_index<SH>(P, RG_STAG, Dp, i, j, k)) return;
+  // RG_FACES: in a patch, the faces of its cells up to the face after its last one (the cells' updates read both)
+  if (!thread_index<SH>(P, RG_FACES, Dp, i, j, k)) return;
   const Dom<R>& D = *Dp;
   const int nx = D.nx, ny = D.ny, nz = D.nz;
   const R dt = R(rk == 1 ? D.dt / 3.0 : (rk == 2 ? 0.5 * D.dt : D.dt));

@@ -22,16 +22,18 @@ __device__ __forceinline__ void pf_l2(const void* a) { asm volatile("prefetch.gl
 // the levels of a loop split over warps 1 .. CNW - 1 (warp 0 runs a recurrence meanwhile)
 #define CB_LOOP_W1(k, n) for (int k = int(threadIdx.y) - 1; threadIdx.y > 0 && k < (n); k += CNW - 1)
 // block -> (member, column i of this lane, row j)
+// (ilim: the end of the member's column range along i; the lanes at or past it have no column)
 template <class R, int NM>
-__device__ __forceinline__ const Dom<R>& cb_member(const Pack<R, NM>& P, int kind, int& i, int& j) {
+__device__ __forceinline__ const Dom<R>& cb_member(const Pack<R, NM>& P, int kind, int& i, int& j, int& ilim) {
   const int b = blockIdx.x;
   const int m = member_of(P, kind, 0, b);
   const Dom<R>& D = P.d[m];
-  const Range r = range_of(kind, D.nx, D.ny, D.nz, D.nyv);
+  const Range r = range_of(kind, D);
   const int bx = cdiv(r.i1 - r.i0, CX);
   const int local = b - P.start(kind, 0, m);
   i = r.i0 + (local % bx) * CX + int(threadIdx.x);
   j = r.j0 + local / bx;
+  ilim = r.i1;
   return D;
 }
 // shared level array a of the block: a[k * CX + lane]
@@ -43,11 +45,11 @@ __device__ __forceinline__ double* cb_array(int a, int nz) {
 // rk_step_prep: KMu (large_step.cpp:49-66), KPrep3 (:68-81), KWW (:83-108), KCq (:127-148)
 template <class R, int NM>
 __global__ void __launch_bounds__(CX * CNW, 3) k_ls_prep(const __grid_constant__ Pack<R, NM> P) {
-  int i, j;
-  const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j);
+  int i, j, ilim;
+  const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j, ilim);
   const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
   const int lane = threadIdx.x;
-  const bool col = i < nx + 1;
+  const bool col = i < ilim;  // a column of the member (its faces' range)
   const bool w0 = threadIdx.y == 0;
   const int spx = D.spec_x, spy = D.spec_y;
   double* s_div = cb_array(0, nz);
@@ -139,11 +141,11 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ls_prep(const __grid_constant__
 // small_step_prep (KPrep small_step.cpp:50-93) + calc_p_rho (KPRho :114-119) + calc_coef_w (KCoefW :122-148)
 template <class R, int NM>
 __global__ void __launch_bounds__(CX * CNW, 3) k_ss_prep(const __grid_constant__ Pack<R, NM> P, int rk) {
-  int i, j;
-  const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j);
+  int i, j, ilim;
+  const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j, ilim);
   const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
   const int lane = threadIdx.x;
-  const bool col = i < nx + 1;
+  const bool col = i < ilim;  // a column of the member (its faces' range)
   const bool w0 = threadIdx.y == 0;
   const bool mass = col && i < nx && j < ny;
   const bool first = rk == 1;
@@ -279,13 +281,13 @@ template <class R, int NM>
 __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack<R, NM> P, int rk, int it,
                                                     int nsteps) {
   constexpr int phase = 7;
-  int i, j;
-  const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j);
+  int i, j, ilim;
+  const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j, ilim);
   using A = double;
   const int nx = D.nx, ny = D.ny, nz = D.nz;
   const int lane = threadIdx.x;
   const bool w0 = threadIdx.y == 0;
-  const bool col = i < nx + 1;
+  const bool col = i < ilim;  // a column of the member (its faces' range)
   const R dts = R(rk == 1 ? D.dt / 3.0 : D.dt / D.n_sound);
   const R epssm = R(D.epssm);
   const bool first = it == 1, last = it == nsteps;
@@ -646,10 +648,10 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
 // small_step_finish (KFinish :419-444, KFinishMu :446-453) + calc_p_rho_phi (KPRhoPhi :456-477)
 template <class R, int NM>
 __global__ void __launch_bounds__(CX * CNW, 3) k_finish(const __grid_constant__ Pack<R, NM> P, int rk, int nsmall) {
-  int i, j;
-  const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j);
+  int i, j, ilim;
+  const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j, ilim);
   const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
-  const bool col = i < nx + 1;
+  const bool col = i < ilim;  // a column of the member (its faces' range)
   const bool mass = col && i < nx && j < ny;
   const R dts = R(rk == 1 ? D.dt / 3.0 : D.dt / D.n_sound);
   const R hd_dt = (rk == 3 && D.n_moist > 0) ? dts * R(nsmall) : R(0);
@@ -732,11 +734,11 @@ __device__ __forceinline__ double damp_cos(double x) {
 }
 template <class R, int NM>
 __global__ void __launch_bounds__(CX * CNW) k_dampkm(const __grid_constant__ Pack<R, NM> P) {
-  int i, j;
-  const Dom<R>& D = cb_member(P, RG_COLS_MASS, i, j);
+  int i, j, ilim;
+  const Dom<R>& D = cb_member(P, RG_COLS_MASS, i, j, ilim);
   if (D.damp_opt != 1 || !D.diff_on) return;  // uniform over the block
   const int nx = D.nx, ny = D.ny, nz = D.nz;
-  if (threadIdx.y != 0 || i >= nx || j >= ny) return;
+  if (threadIdx.y != 0 || i >= ilim || j >= ny) return;
   const R khm = R(D.khdif), khh = R(D.khdif / D.prandtl);
   int i0 = 0, i1 = nx, j0 = 0, j1 = ny;
   if (D.lbc) {  // specified boundaries: spec_bdy_width (5) - 1 rows keep the constants
@@ -785,9 +787,9 @@ __global__ void __launch_bounds__(CX * CNW) k_dampkm(const __grid_constant__ Pac
 // set_w_surface (KSetWSurface, rk3.cpp:173-200), fill = false
 template <class R, int NM>
 __global__ void __launch_bounds__(CX * CNW) k_w_surface(const __grid_constant__ Pack<R, NM> P) {
-  int i, j;
-  const Dom<R>& D = cb_member(P, RG_COLS_MASS, i, j);
-  if (threadIdx.y != 0 || i >= D.nx) return;
+  int i, j, ilim;
+  const Dom<R>& D = cb_member(P, RG_COLS_MASS, i, j, ilim);
+  if (threadIdx.y != 0 || i >= ilim) return;
   const R cf1 = R(D.cf1), cf2 = R(D.cf2), cf3 = R(D.cf3);
   const R ws = D.msfty(i, j) * R(0.5) * R(D.rdy) *
                    ((D.ht(i, j + 1) - D.ht(i, j)) * (cf1 * D.v2(i, j + 1, 0) + cf2 * D.v2(i, j + 1, 1) + cf3 * D.v2(i, j + 1, 2)) +

@@ -44,11 +44,11 @@ __device__ __forceinline__ int mp_fall(double crmax) {
 
 template <class R, int NM>
 __global__ void __launch_bounds__(CX * CNW) k_kessler(const __grid_constant__ Pack<R, NM> P) {
-  int i, j;
-  const Dom<R>& D = cb_member(P, RG_COLS_MASS, i, j);
+  int i, j, ilim;
+  const Dom<R>& D = cb_member(P, RG_COLS_MASS, i, j, ilim);
   if (D.mp_physics != 1) return;  // uniform over the block
   const int nx = D.nx, ny = D.ny, nz = D.nz, lane = threadIdx.x;
-  const bool col = i < nx && j < ny;
+  const bool col = i < ilim && j < ny;
   const int sx = D.bc_x == CW_BC_SPECIFIED ? 1 : 0, sy = D.bc_y == CW_BC_SPECIFIED ? 1 : 0;
   const bool mp = col && i >= sx && i < nx - sx && j >= sy && j < ny - sy;
   constexpr double t0 = 300.0, g = 9.81, rvrd = 461.6 / 287.0, rcp = 287.0 / (7.0 * 287.0 / 2.0);

@@ -286,6 +286,24 @@ typedef struct cw_lam_params {
 int cw_default_lam_params(cw_lam_params* p);
 int cw_gen_lam(cw_case* c, const cw_lam_params* p);
 
+/* ---- one domain decomposed into px x py patches (tile::Options, src/core/tiles.hpp:22-120; docs/MPI.md §3) ----
+ * Patch t = tx + px ty owns the mass points [tx nx / px, (tx + 1) nx / px) x [ty ny / py, (ty + 1) ny / py) and the
+ * faces between them; the east / north edge patches also own the faces nx / ny and the lateral halos beyond the
+ * domain's edges (tile::set_domain, tiles.hpp:70-74). Each patch is a member of the handle whose fields are allocated
+ * for its patch and a halo of 3 and indexed with the domain's indices (Grid::dom, pi0 .. pj1); every launch covers
+ * every patch and is clipped to the points each owns, and at every halo fill point each patch first receives the
+ * points of its allocation that other patches own (the exchange), then fills the domain's halo where it touches the
+ * domain's edge, as core/halo.cpp:120-140 does. The result equals the undecomposed domain's bit for bit. Here the
+ * patches share the handle's device and stream. Refused: a periodic direction split over several patches, a split
+ * along y of a 2-D domain, patches under 6 x 6 points. */
+int cw_decomp_patch(const cw_grid* g, int px, int py, int t, int box[4]); /* i0, i1, j0, j1 of patch t (no device) */
+int cw_decomp_create(const cw_grid* g, const cw_options* o, int px, int py, cw_handle** out);
+/* A field as one whole-domain array (the layout of cw_layout_of): uploaded into every patch's allocation, or
+ * gathered from the points each patch owns (tile::download, tiles.hpp:84-97). */
+int cw_decomp_upload(cw_handle* h, int field, int n, const double* host, size_t count);
+int cw_decomp_download(cw_handle* h, int field, int n, double* host, size_t count);
+/* cw_upload_case into every patch (vertical arrays, each patch's window of the fields, the boundary slabs). */
+int cw_decomp_upload_case(cw_handle* h, cw_case* c);
 /* cw_download without any allocation (no counterpart in the reference; CPPWRF's FieldT::download always
  * stages through host memory).
  *
