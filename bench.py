@@ -72,6 +72,36 @@ def shard_seed(rank):
     return 1 + rank
 
 
+def place_by_footprint(footprints, world):
+    """Independent units (ensemble members, served requests) onto ranks by device footprint: each unit, largest
+    first, to the rank holding the fewest bytes so far (ties: the lower rank). The same on every rank (deterministic),
+    each unit on exactly one rank. Returns the unit indices of each rank, in unit order."""
+    load = [0] * world
+    ranks = [[] for _ in range(world)]
+    for u in sorted(range(len(footprints)), key=lambda u: (-footprints[u], u)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        load[r] += footprints[u]
+        ranks[r].append(u)
+    return [sorted(x) for x in ranks]
+
+
+def footprint_of(capi, case):
+    b = C.c_size_t()
+    if capi.load().cw_footprint(C.byref(case.g), C.byref(case.o), C.byref(b)) != 0:
+        raise RuntimeError("cw_footprint failed")
+    return b.value
+
+
+def gather_over_ranks(obj, world):
+    """Every rank's object on every rank (rank order)."""
+    if world <= 1:
+        return [obj]
+    import torch.distributed as dist
+    out = [None] * world
+    dist.all_gather_object(out, obj)
+    return out
+
+
 def max_over_ranks(value, world, device):
     """The maximum of a per-rank time over all ranks (the job's time): an all-reduce MAX of one number."""
     if world <= 1:
@@ -298,16 +328,21 @@ def ensemble_members(rng, n=64):
     return out
 
 
-def run_ensemble(args, torch, capi, Domain, Batch):
+def run_ensemble(args, torch, capi, Domain, Batch, rank=0, world=1):
     """64 members of uneven sizes (nx, ny in [60, 200], nz in {35, 44, 50, 60}, dx 15 km): the batched mixed
-    and FP64 forms against the members run one after the other as plain FP64 domains."""
+    and FP64 forms against the members run one after the other as plain FP64 domains. With several ranks the
+    members are placed on the ranks by device footprint (place_by_footprint; no data-path collective) and the job
+    time is the slowest rank's (strong scaling: the ensemble is fixed)."""
     lib = capi.load()
     rng = np.random.default_rng(2024)
-    spec = ensemble_members(rng)
+    spec_all = ensemble_members(rng)
+    cases_all = [make_case(capi, capi.FP64, seed=m["seed"], w=m, theta_pert=0.5, wind_pert=1.0) for m in spec_all]
+    mine = place_by_footprint([footprint_of(capi, c) for c in cases_all], world)[rank]
+    spec = [spec_all[u] for u in mine]
+    cases = [cases_all[u] for u in mine]
     stream = torch.cuda.Stream()
-    gp = sum(m["nx"] * m["ny"] * m["nz"] for m in spec)
+    gp_all = sum(m["nx"] * m["ny"] * m["nz"] for m in spec_all)
     out = {}
-    cases = [make_case(capi, capi.FP64, seed=m["seed"], w=m, theta_pert=0.5, wind_pert=1.0) for m in spec]
     for prec in (capi.MIXED, capi.FP64):
         opts = []
         for c in cases:
@@ -319,10 +354,12 @@ def run_ensemble(args, torch, capi, Domain, Batch):
             b.upload_case(k, c)
         lib.cw_set_stream(b.h, C.c_void_p(stream.cuda_stream))
         b.step(args.warmup)
-        ms = _timed_steps(torch, stream, b.step, args.steps)
-        out[prec] = (gp * args.steps / (ms / 1000.0), ms / args.steps, b.launches() // max(args.steps, 1))
+        if world > 1:
+            torch.distributed.barrier()
+        ms = max_over_ranks(_timed_steps(torch, stream, b.step, args.steps), world, "cuda")
+        out[prec] = (gp_all * args.steps / (ms / 1000.0), ms / args.steps, b.launches() // max(args.steps, 1))
         b.close()
-    # plain FP64: every member alone, one after the other
+    # plain FP64: every member alone, one after the other (each rank its own members)
     plain_ms = 0.0
     for c in cases:
         d = Domain(c.g, c.o).upload_case(c)
@@ -330,16 +367,21 @@ def run_ensemble(args, torch, capi, Domain, Batch):
         d.step(1)
         plain_ms += _timed_steps(torch, stream, d.step, args.steps)
         d.close()
-    plain = gp * args.steps / (plain_ms / 1000.0)
-    line = {"metric": METRIC, "value": out[capi.MIXED][0], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": out[capi.MIXED][1], "higher_is_better": True, "scaling": "weak",
+    plain_ms = max_over_ranks(plain_ms, world, "cuda")
+    plain = gp_all * args.steps / (plain_ms / 1000.0)
+    line = {"metric": METRIC, "value": out[capi.MIXED][0], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": out[capi.MIXED][1], "higher_is_better": True,
+            "scaling": "strong" if world > 1 else "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (cw_gen_lam, seeded; per-member theta and wind noise)",
-            "config": {"workload": "ensemble_64", "members": len(spec), "grid_points": gp, "dx": 15000.0, "dt": 90.0,
-                       "time_step_sound": 4, "sizes_seed": 2024},
+            "config": {"workload": "ensemble_64", "members": len(spec_all), "grid_points": gp_all, "dx": 15000.0,
+                       "dt": 90.0, "time_step_sound": 4, "sizes_seed": 2024,
+                       "placement": f"members on {world} rank(s) by device footprint"},
+            "members_per_rank": [len(x) for x in gather_over_ranks(mine, world)],
             "fp64_batched_value": out[capi.FP64][0], "fp64_plain_serial_value": plain,
             "mixed_batched_over_fp64_plain": out[capi.MIXED][0] / plain,
             "launches_per_step": out[capi.MIXED][2]}
-    print(json.dumps(line), flush=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     return 0
 
 
@@ -354,15 +396,21 @@ def served_requests(rng, n, rate):
     return out
 
 
-def run_served(args, torch, capi, Domain, Server):
+def run_served(args, torch, capi, Domain, Server, rank=0, world=1):
     """Poisson arrivals of forecast requests (40..300 squared, nz 35..60, 30..360 steps) into the served
     mixed-precision form under a 150 GB budget: p50 / p99 latency and aggregate gp-steps/s, beside the same
-    requests solved one after the other as plain FP64 domains."""
+    requests solved one after the other as plain FP64 domains. With several ranks each request goes to a rank by
+    device footprint (place_by_footprint over the stream; each rank serves its requests at their arrival times)."""
     lib = capi.load()
     rng = np.random.default_rng(77)
-    reqs = served_requests(rng, args.requests, args.rate)
-    cases = [make_case(capi, capi.MIXED, seed=r["seed"], w=r) for r in reqs]
+    reqs_all = served_requests(rng, args.requests, args.rate)
+    cases_all = [make_case(capi, capi.MIXED, seed=r["seed"], w=r) for r in reqs_all]
+    mine = place_by_footprint([footprint_of(capi, c) for c in cases_all], world)[rank]
+    reqs = [reqs_all[u] for u in mine]
+    cases = [cases_all[u] for u in mine]
     srv = Server(budget_bytes=150e9, precision=capi.MIXED, keep_results=False)
+    if world > 1:
+        torch.distributed.barrier()
     t0 = time.perf_counter()
     for r, c in zip(reqs, cases):
         dt = r["t"] - (time.perf_counter() - t0)
@@ -371,8 +419,20 @@ def run_served(args, torch, capi, Domain, Server):
         srv.submit(c, r["steps"])
     srv.drain()
     st = srv.stats()
+    lat = []
+    for rid in srv.cases:
+        try:
+            lat.append(srv.latency(rid))
+        except Exception:  # noqa: BLE001 - a failed request has no latency (counted in served_stats)
+            pass
+    wall = time.perf_counter() - t0
     srv.close()
     gps = sum(r["nx"] * r["ny"] * r["nz"] * r["steps"] for r in reqs)
+    if world > 1:  # the job: every rank's requests over the slowest rank's wall time, latencies of all requests
+        lat = [x for part in gather_over_ranks(lat, world) for x in part]
+        wall_job = max(gather_over_ranks(wall, world))
+        st = dict(st, p50_s=float(np.percentile(lat, 50)), p99_s=float(np.percentile(lat, 99)),
+                  mean_s=float(np.mean(lat)), gp_steps_per_s=sum(gather_over_ranks(gps, world)) / wall_job)
     # plain FP64, one request after the other: the device time of the steps alone, and the wall time of the
     # whole solve (domain set-up, upload, steps, read-back of the prognostic state), the served path's equal
     stream = torch.cuda.Stream()
@@ -387,10 +447,12 @@ def run_served(args, torch, capi, Domain, Server):
             d.field(name)
         d.close()
         plain_wall += time.perf_counter() - t0
-    plain = gps / (plain_ms / 1000.0)
-    plain_w = gps / plain_wall
-    line = {"metric": METRIC, "value": st["gp_steps_per_s"], "unit": UNIT, "n_gpus": 1, "steps": None,
-            "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+    gps_job = sum(gather_over_ranks(gps, world))
+    plain = gps_job / (max_over_ranks(plain_ms, world, "cuda") / 1000.0)
+    plain_w = gps_job / max(gather_over_ranks(plain_wall, world))
+    line = {"metric": METRIC, "value": st["gp_steps_per_s"], "unit": UNIT, "n_gpus": world, "steps": None,
+            "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "strong" if world > 1 else "weak",
+            "vs_baseline": None,
             "dtype": "f32+f64", "data": "synthetic (cw_gen_lam, seeded per request; Poisson arrivals)",
             "config": {"workload": "served_stream", "requests": len(reqs), "rate_per_s": args.rate,
                        "hbm_budget_bytes": 150e9, "sizes": "log-uniform 40..300, nz 35..60, 30..360 steps"},
@@ -399,7 +461,8 @@ def run_served(args, torch, capi, Domain, Server):
             "fp64_plain_serial_wall_value": plain_w, "served_over_fp64_plain_wall": st["gp_steps_per_s"] / plain_w,
             "note": "value = completed gp-steps / (last completion - first submission), host clock, arrival gaps "
                     "included; fp64_plain_serial_value: device time of the steps only; _wall_value: whole solves"}
-    print(json.dumps(line), flush=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     return 0
 
 
@@ -414,7 +477,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default block shapes")
     ap.add_argument("--workload", choices=["lam", "precision", "ensemble", "served"], default="lam",
                     help="lam: the headline 119x89x44 line; precision: 400x400x60 mixed vs FP64 with 1 h / 6 h errors; "
-                         "ensemble: 64 uneven members; served: Poisson requests under an HBM budget (1 GPU)")
+                         "ensemble: 64 uneven members; served: Poisson requests under an HBM budget (members and "
+                         "requests placed on the ranks by device footprint when N > 1)")
     ap.add_argument("--requests", type=int, default=24, help="served: number of requests")
     ap.add_argument("--rate", type=float, default=2.0, help="served: Poisson arrival rate per second")
     args = ap.parse_args()
@@ -436,13 +500,20 @@ def main():
     if args.workload != "lam":
         from cppwrf_b200 import Batch, Server
         capi.load().cw_use_device(local)
-        if rank != 0:
-            return 0
-        if args.workload == "precision":
-            return run_precision(args, torch, capi, Domain)
-        if args.workload == "ensemble":
-            return run_ensemble(args, torch, capi, Domain, Batch)
-        return run_served(args, torch, capi, Domain, Server)
+        if args.workload == "precision":  # one domain pair: rank 0 alone
+            return run_precision(args, torch, capi, Domain) if rank == 0 else 0
+        if world > 1:  # ensemble members / served requests placed on the ranks by footprint
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            import datetime
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        try:
+            if args.workload == "ensemble":
+                return run_ensemble(args, torch, capi, Domain, Batch, rank, world)
+            return run_served(args, torch, capi, Domain, Server, rank, world)
+        finally:
+            if world > 1:
+                dist.destroy_process_group()
     if world > 1:
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         import datetime

@@ -61,3 +61,45 @@ def test_reference_arm_runs_on_rank_zero_only(capsys):
     args = argparse.Namespace(gpus=2, steps=1, warmup=0)
     assert bench.run_reference(args, rank=1) == 0
     assert capsys.readouterr().out == ""
+
+
+def _place_rank(rank, world, port, q):
+    import datetime
+    import sys
+
+    import torch.distributed as dist
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    import numpy as np
+
+    import bench
+    rng = np.random.default_rng(5)
+    fp = [int(x) for x in rng.integers(1, 1000, size=37)]  # the units' footprints, the same on every rank
+    mine = bench.place_by_footprint(fp, world)[rank]
+    every = bench.gather_over_ranks(mine, world)
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, fp, every))
+
+
+def test_units_placed_on_ranks_by_footprint():
+    """Ensemble members and served requests go to ranks by device footprint: every rank computes the same
+    placement, each unit lands on exactly one rank, and the ranks' loads differ by at most one unit's footprint."""
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_place_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted(q.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    fp, every0 = out[0][1], out[0][2]
+    assert out[1][2] == every0  # the same placement on both ranks
+    units = sorted(u for part in every0 for u in part)
+    assert units == list(range(len(fp)))
+    loads = [sum(fp[u] for u in part) for part in every0]
+    assert max(loads) - min(loads) <= max(fp)
