@@ -60,7 +60,8 @@ ALG_ARRAYS = {
     "k_ac": 24 + 11,          # u2 v2 u_save v_save ww1 ww_m ru_m rv_m t2 t_save t_tend w2 ph2 rw_tend ph_tend
                               # ph_save phb c2a alt a alpha gamma cqw pm1 | ww ww_m ru_m rv_m t2 t_2save w2 ph2 al p pm1
     "k_finish": 15 + 8,       # u2 v2 w2 t2 ph2 ww 5 saves ww1 hd alb pb | u2 v2 w2 t2 ph2 ww al p
-    "k_q_update": 3 + 3 + 1,  # per species: q2 q1 qtf + ru_m rv_m ww_m | qn
+    "k_q_update": 3 + 3 + 1,  # per species: q2 q1 qtf + ru_m rv_m ww_m | qn (one thread updates every species: the
+                              # fluxes ru_m rv_m ww_m once, below)
     "k_q_update_pd": 4 + 3 + 1,
     "k_q_scale_pd": 2 + 3 + 1,
 }
@@ -605,6 +606,8 @@ def main():
     dom_name, dom_ms, dom_n = next((r for r in table if r[0] in ALG_ARRAYS), table[0])
     esz = 4 if prec == capi.MIXED else 8
     arrays = ALG_ARRAYS.get(dom_name, 0) * (WORKLOAD["n_moist"] if dom_name.startswith("k_q_") else 1)
+    if dom_name == "k_q_update":
+        arrays = 4 * WORKLOAD["n_moist"] + 3
     alg_bytes = arrays * pts * esz
     avg_s = dom_ms / 1000.0 / dom_n
     peak, peak_src = measured_peak()
@@ -631,6 +634,8 @@ def main():
                              for k in ("k_tend", "k_tendf_rk1", "k_uv", "k_q_update", "k_q_face_pd",
                                        "k_q_scale_pd", "k_q_update_pd", "k_p_rho_phi")
                              if dom.autotune_choice(k) >= 0},
+            "column_warps": {k: [8, 16, 4][dom.autotune_choice(k)]
+                             for k in ("k_ls_prep", "k_ss_prep", "k_ac", "k_finish") if dom.autotune_choice(k) >= 0},
             "clocks": clocks, "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": ebytes,
                                       "d2h_bytes_per_step": ebytes, "steps": n_e2e},
             "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roofline}

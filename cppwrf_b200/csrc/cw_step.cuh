@@ -203,13 +203,26 @@ struct Launcher {
     flush();
     if (plan) return;
     static_assert(CX == 32, "a column block's lanes are one warp");
+    launch_cb(name, kind, arrays, kern, CNW, ps, args...);
+  }
+  // the same with a tunable warp count (one instantiation per shape: cb_warps(shape) warps per column block)
+  template <class R, int NM, class K, class... Args>
+  void run_cbt(const char* name, int kind, int arrays, const std::array<K, kNumShapes>& kerns, const Packs<R, NM>& ps,
+               Args... args) {
+    flush();
+    if (plan) return;
+    const int sh = shape_for(name);
+    launch_cb(name, kind, arrays, kerns[size_t(sh)], cb_warps(sh), ps, args...);
+  }
+  template <class R, int NM, class K, class... Args>
+  void launch_cb(const char* name, int kind, int arrays, K kern, int nw, const Packs<R, NM>& ps, Args... args) {
     const size_t smem = size_t(arrays) * h->cb_level_bytes;
     CW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     for (size_t c = 0; c < ps.p.size(); ++c) {
       const int nb = ps.blocks[c][size_t(kind)][0];
       if (nb == 0) continue;
       begin(name);
-      kern<<<nb, dim3(CX, CNW), smem, h->stream>>>(ps.p[c], args...);
+      kern<<<nb, dim3(CX, nw), smem, h->stream>>>(ps.p[c], args...);
       check();
     }
   }
@@ -229,6 +242,8 @@ struct Launcher {
 // the three block-shape instantiations of a tunable point kernel
 #define KV(kern) std::array{kern<R, NM, 0>, kern<R, NM, 1>, kern<R, NM, 2>}
 #define KV_OP(kern, op) std::array{kern<R, NM, 0, op>, kern<R, NM, 1, op>, kern<R, NM, 2, op>}
+// the three warp-count instantiations of a tunable column kernel
+#define KC(kern) std::array{kern<R, NM, cb_warps(0)>, kern<R, NM, cb_warps(1)>, kern<R, NM, cb_warps(2)>}
 
 template <class R, int NM>
 void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
@@ -271,7 +286,7 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
     // fill would make them (only the scalars change in between), so only the first stage runs it (the fill merges
     // with the scalars' H_Q2 into one launch: fewer cells, not fewer launches)
     if (rk == 1) L.halo(cw_handle::H_PREP0);
-    L.run_cb("k_ls_prep", RG_COLS_STAG, 1, k_ls_prep<R, NM>, d);
+    L.run_cbt("k_ls_prep", RG_COLS_STAG, 1, KC(k_ls_prep), d);
     L.halo(cw_handle::H_PREP1);
     if (rk == 1 && (dampkm || smag)) {  // DiffusionDriver::prepare: km_opt 4's and damp_opt 1's eddy viscosities
       if (smag) L.run_t("k_smag", RG_MASS, 1, KV(k_smag), d);
@@ -283,22 +298,22 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
     else L.run_t("k_tend", RG_STAG, 1, KV_OP(k_tend, false), d, rk);
     if (h->cfl_on) L.run_t("k_cfl", RG_MASS, 1, KV(k_cfl), d, rk);
     if (rk == 1) L.copy_list(h->zeros_d, h->zeros_start_d, h->zeros.size(), h->zeros_total);
-    L.run_cb("k_ss_prep", RG_COLS_STAG, 3, k_ss_prep<R, NM>, d, rk);
+    L.run_cbt("k_ss_prep", RG_COLS_STAG, 3, KC(k_ss_prep), d, rk);
     if (!spec_all) L.halo(cw_handle::H_SS0);
     for (int it = 1; it <= ns; ++it) {
       L.run_t("k_uv", RG_STAG, 1, KV(k_uv), d, rk);
       if (!spec_all) L.halo(cw_handle::H_UV);
-      L.run_cb("k_ac", RG_COLS_STAG, kCbArrays, k_ac<R, NM>, d, rk, it, ns);
+      L.run_cbt("k_ac", RG_COLS_STAG, kCbArrays, KC(k_ac), d, rk, it, ns);
       if (lbc && (!spec_all || it == ns)) L.run("k_ring", RG_RING, k_ring<R, NM>, d, int(RO_ZERO_GRAD_W), rk);
       if (!spec_all) L.halo(cw_handle::H_AC);
     }
     L.halo(cw_handle::H_POST);
-    L.run_cb("k_finish", RG_COLS_STAG, 0, k_finish<R, NM>, d, rk, ns);
+    L.run_cbt("k_finish", RG_COLS_STAG, 0, KC(k_finish), d, rk, ns);
     L.halo(cw_handle::H_FIN);
     if (scalars) {
       if (rk == 1) L.run_t("k_q_tendf_rk1", RG_MASS, nq, KV(k_q_tendf_rk1), d);
       // at rk 3 the PD species take k_q_*_pd: the plain update runs only when some species is not PD
-      if (rk != 3 || any_plain || !any_pd) L.run_t("k_q_update", RG_MASS, nq, KV(k_q_update), d, rk);
+      if (rk != 3 || any_plain || !any_pd) L.run_t("k_q_update", RG_MASS, 1, KV(k_q_update), d, rk);
       if (rk == 3 && any_pd) {
         L.run_t("k_q_pre_pd", RG_MASS, nq, KV(k_q_pre_pd), d, rk);
         L.halo(cw_handle::H_Q1PD);

@@ -141,6 +141,13 @@ __device__ __forceinline__ int member_of(const Pack<R, NM>& P, int kind, int sha
   }
 }
 
+// x / m for a map factor m. In IEEE arithmetic x / 1 is x exactly, so the division is skipped when m == 1 with the
+// same bits as its result: an unmapped domain's map factors are all 1, and its divisions by them cost a compare.
+template <class X>
+__device__ __forceinline__ X div_msf(X x, X m) {
+  return m == X(1) ? x : x / m;
+}
+
 // Block geometry of the two launch shapes. Point kernels: PX threads along i, blockIdx over (i-tiles, j, k)
 // of a member. Column kernels ("column blocks"): CX columns along i (the lanes of a warp, coalesced) x CNW
 // warps; the pointwise work of the columns' levels is split over the warps, the vertical recurrences run
@@ -150,6 +157,10 @@ constexpr int PX = 128, PY = 1;
 __host__ __device__ constexpr int shape_x(int s) { return s == 0 ? PX : (s == 1 ? PX / 2 : PX / 4); }
 __host__ __device__ constexpr int shape_y(int s) { return PX / shape_x(s); }
 constexpr int CX = 32, CNW = 8;
+// the column kernels' warp counts the autotuner chooses from (shape s: cb_warps(s) warps; the fewest blocks per SM
+// their launch bound asks for keeps 3 x 256, 2 x 512 and 6 x 128 threads resident)
+__host__ __device__ constexpr int cb_warps(int s) { return s == 0 ? CNW : (s == 1 ? 2 * CNW : CNW / 2); }
+__host__ __device__ constexpr int cb_minblocks(int nw) { return nw == CNW ? 3 : (nw > CNW ? 2 : 6); }
 constexpr int kCbArrays = 6;  // shared-memory level arrays of the acoustic column block: kCbArrays x (nz + 2) x CX doubles
 __host__ __device__ __forceinline__ int cdiv(int a, int b) { return (a + b - 1) / b; }
 

@@ -256,7 +256,7 @@ template <class R>
 __device__ __forceinline__ R ww_divv(const Dom<R>& D, int i, int j, int k, R mu1, R mu0, R mv1, R mv0) {
   const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
   return D.msftx(i, j) * R(D.dnw[k]) *
-         (R(D.rdx) * ((c1h * mu1 + c2h) * D.u2.ld(i + 1, j, k) / D.msfuy(i + 1, j) - (c1h * mu0 + c2h) * D.u2.ld(i, j, k) / D.msfuy(i, j)) +
+         (R(D.rdx) * (div_msf((c1h * mu1 + c2h) * D.u2.ld(i + 1, j, k), D.msfuy(i + 1, j)) - div_msf((c1h * mu0 + c2h) * D.u2.ld(i, j, k), D.msfuy(i, j))) +
           R(D.rdy) * ((c1h * mv1 + c2h) * D.v2.ld(i, j + 1, k) * D.msfvx_inv(i, j + 1) -
                       (c1h * mv0 + c2h) * D.v2.ld(i, j, k) * D.msfvx_inv(i, j)));
 }
@@ -352,7 +352,7 @@ __device__ R tend_u_open_face(const Dom<R>& D, int i, int j, int k, bool use_ten
     t = R(0) - rdx * ub * (D.u2.ld(i, j, k) - D.u2.ld(i - 1, j, k));
   }
   if (!D.open_y) t -= R(D.rdnw[k]) * (tu_fz(D, i, j, k + 1) - tu_fz(D, i, j, k));
-  if (use_tendf) t += D.ru_tendf.ld(i, j, k) / D.msfuy(i, j);
+  if (use_tendf) t += div_msf(D.ru_tendf.ld(i, j, k), D.msfuy(i, j));
   return t;
 }
 // OP: the kernel variant for packs with an open boundary (the checks compile away in the other)
@@ -366,7 +366,7 @@ __device__ R tend_u(const Dom<R>& D, int i, int j, int k, bool use_tendf, R fx0,
     else t -= tu_open_y(D, i, j, k);
   }
   if (!(OP && D.open_y && D.spec_x && (i == 0 || i == D.nx))) t -= R(D.rdnw[k]) * (tu_fz(D, i, j, k + 1) - tu_fz(D, i, j, k));
-  const R rm = D.msfux(i, j) / D.msfuy(i, j);
+  const R rm = div_msf(D.msfux(i, j), D.msfuy(i, j));
   R dpx = rm * R(0.5) * rdx * (c1h * D.muu.ld(i, j, 0) + c2h) *
           ((D.ph2.ld(i, j, k + 1) - D.ph2.ld(i - 1, j, k + 1) + D.ph2.ld(i, j, k) - D.ph2.ld(i - 1, j, k)) +
            (D.alt.ld(i, j, k) + D.alt.ld(i - 1, j, k)) * (D.p.ld(i, j, k) - D.p.ld(i - 1, j, k)) +
@@ -385,7 +385,7 @@ __device__ R tend_u(const Dom<R>& D, int i, int j, int k, bool use_tendf, R fx0,
   } else {
     t = t - D.u2.ld(i, j, k) * R(k::reradius) * rw4;
   }
-  if (use_tendf) t += D.ru_tendf.ld(i, j, k) / D.msfuy(i, j);
+  if (use_tendf) t += div_msf(D.ru_tendf.ld(i, j, k), D.msfuy(i, j));
   return t;
 }
 
@@ -462,7 +462,7 @@ template <bool OP, class R>
 __device__ R tend_v(const Dom<R>& D, int i, int j, int k, bool use_tendf, R fx0, R fx1, R fy0, R fy1) {
   const R rdx = R(D.rdx), rdy = R(D.rdy);
   const R c1h = R(D.c1h[k]), c2h = R(D.c2h[k]);
-  const R rm = D.msfvy(i, j) / D.msfvx(i, j);
+  const R rm = div_msf(D.msfvy(i, j), D.msfvx(i, j));
   R t;
   if (OP && D.open_x && (i == 0 || i == D.nx - 1)) {  // open x: the y flux, then the open term instead of the x flux
     t = -(D.msfvy(i, j) * rdy) * (fy1 - fy0);
@@ -576,7 +576,7 @@ __device__ R tend_w(const Dom<R>& D, int i, int j, int k, bool use_tendf, R fx0,
     t = -(D.msftx(i, j) * rdx) * (fx1 - fx0);
     if (D.do_y) t -= (D.msftx(i, j) * rdy) * (fy1 - fy0);
   }
-  const R rmsft = R(1) / D.msfty(i, j);
+  const R rmsft = div_msf(R(1), D.msfty(i, j));
   if (k < nz) {
     t -= R(D.rdn[k]) * (tw_fz(D, i, j, k) - tw_fz(D, i, j, k - 1));
     const R cqw = cqw_(D, i, j, k), cq1 = R(1) / (R(1) + cqw), cq2 = cqw * cq1;
@@ -593,7 +593,7 @@ __device__ R tend_w(const Dom<R>& D, int i, int j, int k, bool use_tendf, R fx0,
     const R fnm = R(D.fnm[k]), fnp = R(D.fnp[k]);
     const R ruw = R(0.5) * (fnm * (D.ru.ld(i, j, k) + D.ru.ld(i + 1, j, k)) + fnp * (D.ru.ld(i, j, k - 1) + D.ru.ld(i + 1, j, k - 1)));
     const R rvw = R(0.5) * (fnm * (D.rv.ld(i, j, k) + D.rv.ld(i, j + 1, k)) + fnp * (D.rv.ld(i, j, k - 1) + D.rv.ld(i, j + 1, k - 1)));
-    const R rmt = D.msftx(i, j) / D.msfty(i, j);
+    const R rmt = div_msf(D.msftx(i, j), D.msfty(i, j));
     if (D.cor) t = t + D.e(i, j) * (D.cosa(i, j) * ruw - rmt * D.sina(i, j) * rvw);  // Coriolis (:484)
     const R uw = R(0.5) * (fnm * (D.u2.ld(i, j, k) + D.u2.ld(i + 1, j, k)) + fnp * (D.u2.ld(i, j, k - 1) + D.u2.ld(i + 1, j, k - 1)));
     const R vw = R(0.5) * (fnm * (D.v2.ld(i, j, k) + D.v2.ld(i, j + 1, k)) + fnp * (D.v2.ld(i, j, k - 1) + D.v2.ld(i, j + 1, k - 1)));
@@ -605,7 +605,7 @@ __device__ R tend_w(const Dom<R>& D, int i, int j, int k, bool use_tendf, R fx0,
          (cq1 * R(2) * R(D.rdnw[nz - 1]) * (-D.p.ld(i, j, nz - 1)) - R(D.c1f[nz]) * D.mu2.ld(i, j, 0) -
           cq2 * (R(D.c1f[nz]) * D.mub(i, j) + R(D.c2f[nz])));
   }
-  if (use_tendf) t += D.rw_tendf.ld(i, j, k) / D.msfty(i, j);
+  if (use_tendf) t += div_msf(D.rw_tendf.ld(i, j, k), D.msfty(i, j));
   return t;
 }
 
@@ -677,8 +677,8 @@ __device__ R tend_t(const Dom<R>& D, int i, int j, int k, bool use_tendf, bool u
     if (D.do_y) r -= (D.msftx(i, j) * R(D.rdy)) * (fy1 - fy0);
   }
   r -= R(D.rdnw[k]) * (sc_fz(D, D.t2, D.ww, i, j, k + 1, false) - sc_fz(D, D.t2, D.ww, i, j, k, false));
-  if (use_tendf) r += D.t_tendf.ld(i, j, k) / D.msfty(i, j);
-  if (use_hd) r += (R(D.c1h[k]) * D.mut.ld(i, j, 0) + R(D.c2h[k])) * D.hd.ld(i, j, k) / D.msfty(i, j);
+  if (use_tendf) r += div_msf(D.t_tendf.ld(i, j, k), D.msfty(i, j));
+  if (use_hd) r += div_msf((R(D.c1h[k]) * D.mut.ld(i, j, 0) + R(D.c2h[k])) * D.hd.ld(i, j, k), D.msfty(i, j));
   return r;
 }
 
@@ -721,13 +721,13 @@ __device__ R tend_ph(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
   const R c1f = R(D.c1f[k]), c2f = R(D.c2f[k]);
   R t = 0;
   if (k < nz) t = t - (R(D.fnm[k]) * tph_wdwn(D, i, j, k) + R(D.fnp[k]) * tph_wdwn(D, i, j, k - 1));
-  t = t + (c1f * D.mut.ld(i, j, 0) + c2f) * R(k::g) * D.w2.ld(i, j, k) / D.msfty(i, j);
+  t = t + div_msf((c1f * D.mut.ld(i, j, 0) + c2f) * R(k::g) * D.w2.ld(i, j, k), D.msfty(i, j));
   const R r60 = R(1) / R(60), r12 = R(1) / R(12);
   if (D.do_y) {
     const R mvp = c1f * D.muv.ld(i, j + 1, 0) + c2f, mvm = c1f * D.muv.ld(i, j, 0) + c2f;
     const R vp = k < nz ? D.v2.ld(i, j + 1, k) + D.v2.ld(i, j + 1, k - 1) : R(D.cfn) * D.v2.ld(i, j + 1, nz - 1) + R(D.cfn1) * D.v2.ld(i, j + 1, nz - 2);
     const R vm = k < nz ? D.v2.ld(i, j, k) + D.v2.ld(i, j, k - 1) : R(D.cfn) * D.v2.ld(i, j, nz - 1) + R(D.cfn1) * D.v2.ld(i, j, nz - 2);
-    const R cy = (k < nz ? R(0.25) : R(0.5)) * R(D.rdy) / D.msfty(i, j);
+    const R cy = div_msf((k < nz ? R(0.25) : R(0.5)) * R(D.rdy), D.msfty(i, j));
     const int o = ph_horder(j, D.ny, D.spec_y, 0, OP && D.open_x);
     if (o == 6) t = t - cy * ((mvp * vp * D.msfvy(i, j + 1) + mvm * vm * D.msfvy(i, j)) * r60 * grad6<R, 0, 1>(D, i, j, k));
     else if (o == 4) t = t - cy * ((mvp * vp * D.msfvy(i, j + 1) + mvm * vm * D.msfvy(i, j)) * r12 * grad4<R, 0, 1>(D, i, j, k));
@@ -737,7 +737,7 @@ __device__ R tend_ph(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
   const R mup = c1f * D.muu.ld(i + 1, j, 0) + c2f, mum = c1f * D.muu.ld(i, j, 0) + c2f;
   const R up = k < nz ? D.u2.ld(i + 1, j, k) + D.u2.ld(i + 1, j, k - 1) : R(D.cfn) * D.u2.ld(i + 1, j, nz - 1) + R(D.cfn1) * D.u2.ld(i + 1, j, nz - 2);
   const R um = k < nz ? D.u2.ld(i, j, k) + D.u2.ld(i, j, k - 1) : R(D.cfn) * D.u2.ld(i, j, nz - 1) + R(D.cfn1) * D.u2.ld(i, j, nz - 2);
-  const R cx = (k < nz ? R(0.25) : R(0.5)) * R(D.rdx) / D.msfty(i, j);
+  const R cx = div_msf((k < nz ? R(0.25) : R(0.5)) * R(D.rdx), D.msfty(i, j));
   const int o = ph_horder(i, D.nx, D.spec_x, 1, OP && D.open_x);
   if (o == 6) t = t - cx * ((mup * up * D.msfux(i + 1, j) + mum * um * D.msfux(i, j)) * r60 * grad6<R, 1, 0>(D, i, j, k));
   else if (o == 2)
@@ -767,13 +767,13 @@ __device__ R tend_ph(const Dom<R>& D, int i, int j, int k, bool use_tendf) {
     const R muf = c1f * D.mut.ld(i, j, 0) + c2f;
     if (i == 0) {
       const R ul = ub < R(0) ? ub : R(0);
-      t = t - (D.msftx(i, j) / D.msfty(i, j)) * R(D.rdx) * muf * (ul * (D.ph2.ld(1, j, k) - D.ph2.ld(0, j, k)));
+      t = t - (div_msf(D.msftx(i, j), D.msfty(i, j))) * R(D.rdx) * muf * (ul * (D.ph2.ld(1, j, k) - D.ph2.ld(0, j, k)));
     } else {
       const R ur = ub > R(0) ? ub : R(0);
-      t = t - (D.msftx(i, j) / D.msfty(i, j)) * R(D.rdx) * muf * (ur * (D.ph2.ld(i, j, k) - D.ph2.ld(i - 1, j, k)));
+      t = t - (div_msf(D.msftx(i, j), D.msfty(i, j))) * R(D.rdx) * muf * (ur * (D.ph2.ld(i, j, k) - D.ph2.ld(i - 1, j, k)));
     }
   }
-  if (use_tendf) t = t + D.ph_tendf.ld(i, j, k) / D.msfty(i, j);
+  if (use_tendf) t = t + div_msf(D.ph_tendf.ld(i, j, k), D.msfty(i, j));
   return t;
 }
 
@@ -1026,8 +1026,8 @@ template <class R, class XK>
 __device__ R hdiff_u(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, XK X, int i, int j, int k) {
   const double *c1 = D.c1h, *c2 = D.c2h;
   const R rdx = R(D.rdx), rdy = R(D.rdy);
-  const R mkrdxm = (D.msftx(i - 1, j) / D.msfty(i - 1, j)) * mk(c1, c2, mut, i - 1, j, k) * X(i - 1, j, k) * rdx;
-  const R mkrdxp = (D.msftx(i, j) / D.msfty(i, j)) * mk(c1, c2, mut, i, j, k) * X(i, j, k) * rdx;
+  const R mkrdxm = (div_msf(D.msftx(i - 1, j), D.msfty(i - 1, j))) * mk(c1, c2, mut, i - 1, j, k) * X(i - 1, j, k) * rdx;
+  const R mkrdxp = (div_msf(D.msftx(i, j), D.msfty(i, j))) * mk(c1, c2, mut, i, j, k) * X(i, j, k) * rdx;
   const R mrdx = D.msfux(i, j) * D.msfuy(i, j) * rdx;
   const R mkrdym = ((D.msfuy(i, j) + D.msfuy(i, j - 1)) / (D.msfux(i, j) + D.msfux(i, j - 1))) * R(0.25) *
                    (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k) + mk(c1, c2, mut, i - 1, j - 1, k) + mk(c1, c2, mut, i - 1, j, k)) *
@@ -1050,8 +1050,8 @@ __device__ R hdiff_v(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, XK X, in
                    (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k) + mk(c1, c2, mut, i + 1, j - 1, k) + mk(c1, c2, mut, i + 1, j, k)) *
                    R(0.25) * (X(i, j, k) + X(i, j - 1, k) + X(i + 1, j - 1, k) + X(i + 1, j, k)) * rdx;
   const R mrdx = D.msfvx(i, j) * D.msfvy(i, j) * rdx;
-  const R mkrdym = (D.msfty(i, j - 1) / D.msftx(i, j - 1)) * X(i, j - 1, k) * rdy;
-  const R mkrdyp = (D.msfty(i, j) / D.msftx(i, j)) * X(i, j, k) * rdy;
+  const R mkrdym = (div_msf(D.msfty(i, j - 1), D.msftx(i, j - 1))) * X(i, j - 1, k) * rdy;
+  const R mkrdyp = (div_msf(D.msfty(i, j), D.msftx(i, j))) * X(i, j, k) * rdy;
   const R mrdy = D.msfvx(i, j) * D.msfvy(i, j) * rdy;
   return mrdx * (mkrdxp * (f.ld(i + 1, j, k) - f.ld(i, j, k)) - mkrdxm * (f.ld(i, j, k) - f.ld(i - 1, j, k))) +
          mrdy * (mkrdyp * (f.ld(i, j + 1, k) - f.ld(i, j, k)) - mkrdym * (f.ld(i, j, k) - f.ld(i, j - 1, k)));
@@ -1060,10 +1060,10 @@ template <class R, class XK>
 __device__ R hdiff_w(const Dom<R>& D, const V3<R>& f, const V3<R>& mut, XK X, int i, int j, int k) {
   const double *c1 = D.c1f, *c2 = D.c2f;
   const R rdx = R(D.rdx), rdy = R(D.rdy);
-  const R mkrdxm = (D.msfux(i, j) / D.msfuy(i, j)) * R(0.25) *
+  const R mkrdxm = (div_msf(D.msfux(i, j), D.msfuy(i, j))) * R(0.25) *
                    (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i - 1, j, k) + mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i - 1, j, k)) *
                    R(0.25) * (X(i, j, k) + X(i - 1, j, k) + X(i, j, k - 1) + X(i - 1, j, k - 1)) * rdx;
-  const R mkrdxp = (D.msfux(i + 1, j) / D.msfuy(i + 1, j)) * R(0.25) *
+  const R mkrdxp = (div_msf(D.msfux(i + 1, j), D.msfuy(i + 1, j))) * R(0.25) *
                    (mk(c1, c2, mut, i + 1, j, k) + mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i + 1, j, k) + mk(c1, c2, mut, i, j, k)) *
                    R(0.25) * (X(i + 1, j, k) + X(i, j, k) + X(i + 1, j, k - 1) + X(i, j, k - 1)) * rdx;
   const R mrdx = D.msftx(i, j) * D.msfty(i, j) * rdx;
@@ -1082,8 +1082,8 @@ template <class R, class XK>
 __device__ R hdiff_m(const Dom<R>& D, const V3<R>& f, const VB<R>* base, const V3<R>& mut, XK X, int i, int j, int k) {
   const double *c1 = D.c1h, *c2 = D.c2h;
   const R rdx = R(D.rdx), rdy = R(D.rdy);
-  const R mkrdxm = (D.msfux(i, j) / D.msfuy(i, j)) * R(0.5) * (X(i, j, k) + X(i - 1, j, k)) * R(0.5) * (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i - 1, j, k)) * rdx;
-  const R mkrdxp = (D.msfux(i + 1, j) / D.msfuy(i + 1, j)) * R(0.5) * (X(i + 1, j, k) + X(i, j, k)) * R(0.5) * (mk(c1, c2, mut, i + 1, j, k) + mk(c1, c2, mut, i, j, k)) * rdx;
+  const R mkrdxm = (div_msf(D.msfux(i, j), D.msfuy(i, j))) * R(0.5) * (X(i, j, k) + X(i - 1, j, k)) * R(0.5) * (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i - 1, j, k)) * rdx;
+  const R mkrdxp = (div_msf(D.msfux(i + 1, j), D.msfuy(i + 1, j))) * R(0.5) * (X(i + 1, j, k) + X(i, j, k)) * R(0.5) * (mk(c1, c2, mut, i + 1, j, k) + mk(c1, c2, mut, i, j, k)) * rdx;
   const R mrdx = D.msftx(i, j) * D.msfty(i, j) * rdx;
   const R mkrdym = (D.msfvy(i, j) * D.msfvx_inv(i, j)) * R(0.5) * (X(i, j, k) + X(i, j - 1, k)) * R(0.5) * (mk(c1, c2, mut, i, j, k) + mk(c1, c2, mut, i, j - 1, k)) * rdy;
   const R mkrdyp = (D.msfvy(i, j + 1) * D.msfvx_inv(i, j + 1)) * R(0.5) * (X(i, j + 1, k) + X(i, j, k)) * R(0.5) * (mk(c1, c2, mut, i, j + 1, k) + mk(c1, c2, mut, i, j, k)) * rdy;
@@ -1395,8 +1395,8 @@ __device__ R dm_defor12(const Dom<R>& D, int ci, int cj, int k) {
   const int im1 = i == 0 ? (px ? nx - 1 : 0) : i - 1, i0 = i == nx ? (px ? 0 : nx - 1) : i;
   const int jm1 = j == 0 ? (py ? ny - 1 : 0) : j - 1, j0 = j == ny ? (py ? 0 : ny - 1) : j;
   const R mm = R(0.25) * (D.msfux(i, jm1) + D.msfux(i, j0)) * (D.msfvy(im1, j) + D.msfvy(i0, j));
-  auto hu = [&](int c, int kk) { const int m = c ? j0 : jm1; return D.u2.ld(i, m, kk) / D.msfux(i, m); };
-  auto hv = [&](int c, int kk) { const int m = c ? i0 : im1; return D.v2.ld(m, j, kk) / D.msfvy(m, j); };
+  auto hu = [&](int c, int kk) { const int m = c ? j0 : jm1; return div_msf(D.u2.ld(i, m, kk), D.msfux(i, m)); };
+  auto hv = [&](int c, int kk) { const int m = c ? i0 : im1; return div_msf(D.v2.ld(m, j, kk), D.msfvy(m, j)); };
   const R tmpzy = R(0.25) * (dm_zy(D, im1, j, k) + dm_zy(D, i0, j, k) + dm_zy(D, im1, j, k + 1) + dm_zy(D, i0, j, k + 1));
   const R r00 = dm_rdzw(D, i0, j0, k), r10 = dm_rdzw(D, im1, j0, k), r11 = dm_rdzw(D, im1, jm1, k),
           r01 = dm_rdzw(D, i0, jm1, k);
@@ -1430,8 +1430,8 @@ __global__ void __launch_bounds__(PX) k_smag(const __grid_constant__ Pack<R, NM>
     return;
   }
   const R mm = D.msftx(i, j) * D.msfty(i, j);
-  auto au = [&](int c, int kk) { return D.u2.ld(i + c, j, kk) / D.msfuy(i + c, j); };
-  auto av = [&](int c, int kk) { return D.v2.ld(i, j + c, kk) / D.msfvx(i, j + c); };
+  auto au = [&](int c, int kk) { return div_msf(D.u2.ld(i + c, j, kk), D.msfuy(i + c, j)); };
+  auto av = [&](int c, int kk) { return div_msf(D.v2.ld(i, j + c, kk), D.msfvx(i, j + c)); };
   const R rdzw = dm_rdzw(D, i, j, k);
   const R tmpzx = R(0.25) * (dm_zx(D, i, j, k) + dm_zx(D, i + 1, j, k) + dm_zx(D, i, j, k + 1) + dm_zx(D, i + 1, j, k + 1));
   const R tmp1_u = (dm_hatavg(D, au, k + 1) - dm_hatavg(D, au, k)) * tmpzx * rdzw;
@@ -1444,7 +1444,7 @@ __global__ void __launch_bounds__(PX) k_smag(const __grid_constant__ Pack<R, NM>
   const R d12 = R(0.25) * (dm_defor12(D, i, j, k) + dm_defor12(D, i, j + 1, k) + dm_defor12(D, i + 1, j, k) +
                            dm_defor12(D, i + 1, j + 1, k));
   def2 += d12 * d12;
-  const R mlen_h = sqrt(R(D.dx) / D.msftx(i, j) * R(D.dy) / D.msfty(i, j));
+  const R mlen_h = sqrt(div_msf(div_msf(R(D.dx), D.msftx(i, j)) * R(D.dy), D.msfty(i, j)));
   const R tmp = sqrt(def2);
   R kmh = R(0.25) * R(0.25) * mlen_h * mlen_h * tmp;
   kmh = kmh < R(10.0) * mlen_h ? kmh : R(10.0) * mlen_h;

@@ -118,16 +118,16 @@ __global__ void __launch_bounds__(PX, 10) k_uv(const __grid_constant__ Pack<R, N
     const R emdx = R(D.emdiv) * (R(1.) / R(D.rdx)), emdy = D.do_y ? R(D.emdiv) * (R(1.) / R(D.rdy)) : R(0);
     const R c1h = R(D.c1h[k]);
     if (i >= ui0 && i < ui1 && !edge_uface(D, i, j)) {
-      const R mudf_x = -emdx * (D.mudf.ld(i, j, 0) - D.mudf.ld(i - 1, j, 0)) / D.msfuy(i, j);
+      const R mudf_x = div_msf(-emdx * (D.mudf.ld(i, j, 0) - D.mudf.ld(i - 1, j, 0)), D.msfuy(i, j));
       un = D.u2(i, j, k) + dts * D.ru_tend.ld(i, j, k) -
-           dts * cqu_(D, i, j, k) * uv_dp<R, 1, 0>(D, i, j, k, D.muu.ld(i, j, 0), R(D.rdx), D.msfux(i, j) / D.msfuy(i, j)) +
+           dts * cqu_(D, i, j, k) * uv_dp<R, 1, 0>(D, i, j, k, D.muu.ld(i, j, 0), R(D.rdx), div_msf(D.msfux(i, j), D.msfuy(i, j))) +
            c1h * mudf_x;
       su = true;
     }
     if (D.do_y && j >= vj0 && j < vj1 && !edge_vface(D, i, j)) {
       const R mudf_y = -emdy * (D.mudf.ld(i, j, 0) - D.mudf.ld(i, j - 1, 0)) * D.msfvx_inv(i, j);
       vn = D.v2(i, j, k) + dts * D.rv_tend.ld(i, j, k) -
-           dts * cqv_(D, i, j, k) * uv_dp<R, 0, 1>(D, i, j, k, D.muv.ld(i, j, 0), R(D.rdy), D.msfvy(i, j) / D.msfvx(i, j)) +
+           dts * cqv_(D, i, j, k) * uv_dp<R, 0, 1>(D, i, j, k, D.muv.ld(i, j, 0), R(D.rdy), div_msf(D.msfvy(i, j), D.msfvx(i, j))) +
            c1h * mudf_y;
       sv = true;
     }
@@ -261,8 +261,9 @@ __device__ R q_adv(const Dom<R>& D, const V3<R>& q, int i, int j, int k, R fx0, 
   }
   return r - R(D.rdnw[k]) * (sc_fz(D, q, D.ww_m, i, j, k + 1, false) - sc_fz(D, q, D.ww_m, i, j, k, false));
 }
-// KUpdate (:145-156) for the non-PD species of this stage; the horizontal face fluxes of the block's tile
-// once, in shared memory
+// KUpdate (:145-156) for the non-PD species of this stage, every species of the point in one thread (the mass
+// fluxes, column masses and map factors loaded once for all of them); the horizontal face fluxes of the block's tile
+// once per species, in shared memory
 template <class R, int NM, int SH>
 __global__ void __launch_bounds__(PX, 12) k_q_update(const __grid_constant__ Pack<R, NM> P, int rk) {
   constexpr int SX = shape_x(SH), SY = shape_y(SH);
@@ -273,24 +274,35 @@ __global__ void __launch_bounds__(PX, 12) k_q_update(const __grid_constant__ Pac
   Range r;
   const bool in = thread_index<SH>(P, RG_MASS, Dp, i, j, k, r);
   const Dom<R>& D = *Dp;
-  const int n = blockIdx.y;  // the species (uniform in the block)
-  if (n >= D.n_scalars || q_is_pd(D, n, rk)) return;
   const int tx = int(threadIdx.x) % SX, ty = int(threadIdx.x) / SX;
   const int nx = D.nx, ny = D.ny;
-  const V3<R> q = D.q2[n];
   // the faces of the member's cells (up to the face after its last one), in its rows / columns
   const bool rx = j < r.j1 && j < ny, ry = i < r.i1 && i < nx;
-  if (rx && i <= nx && i <= r.i1) sfx[ty][tx] = sc_fx(D, q, D.ru_m, i, j, k, false);
-  if (tx == SX - 1 && rx && i + 1 <= nx && i + 1 <= r.i1) sfx[ty][SX] = sc_fx(D, q, D.ru_m, i + 1, j, k, false);
-  if (D.do_y && ry && j <= ny && j <= r.j1) sfy[ty][tx] = sc_fy(D, q, D.rv_m, i, j, k, false);
-  if (D.do_y && ty == SY - 1 && ry && j + 1 <= ny && j + 1 <= r.j1) sfy[SY][tx] = sc_fy(D, q, D.rv_m, i, j + 1, k, false);
-  __syncthreads();
-  if (!in) return;
+  const bool fx0 = rx && i <= nx && i <= r.i1, fx1 = tx == SX - 1 && rx && i + 1 <= nx && i + 1 <= r.i1;
+  const bool fy0 = D.do_y && ry && j <= ny && j <= r.j1, fy1 = D.do_y && ty == SY - 1 && ry && j + 1 <= ny && j + 1 <= r.j1;
   const R dt_rk = R(rk == 1 ? D.dt / 3.0 : (rk == 2 ? 0.5 * D.dt : D.dt));
-  const R mub = D.mub(i, j), mu1 = D.mu1.ld(i, j, 0), mu2 = D.mu2.ld(i, j, 0);
-  R tend = q_adv(D, q, i, j, k, sfx[ty][tx], sfx[ty][tx + 1], sfy[ty][tx], sfy[ty + 1][tx]) * D.msfty(i, j);
-  tend += D.qtf[n].ld(i, j, k);
-  D.qn[n](i, j, k) = (m_full(D, k, mub, mu1) * D.q1[n].ld(i, j, k) + dt_rk * tend) / m_full(D, k, mub, mu2);
+  R mub = 0, mu1 = 0, mu2 = 0, msfty = 0;
+  if (in) {
+    mub = D.mub(i, j);
+    mu1 = D.mu1.ld(i, j, 0);
+    mu2 = D.mu2.ld(i, j, 0);
+    msfty = D.msfty(i, j);
+  }
+  for (int n = 0; n < D.n_scalars; ++n) {  // uniform over the block
+    if (q_is_pd(D, n, rk)) continue;
+    const V3<R> q = D.q2[n];
+    if (fx0) sfx[ty][tx] = sc_fx(D, q, D.ru_m, i, j, k, false);
+    if (fx1) sfx[ty][SX] = sc_fx(D, q, D.ru_m, i + 1, j, k, false);
+    if (fy0) sfy[ty][tx] = sc_fy(D, q, D.rv_m, i, j, k, false);
+    if (fy1) sfy[SY][tx] = sc_fy(D, q, D.rv_m, i, j + 1, k, false);
+    __syncthreads();
+    if (in) {
+      R tend = q_adv(D, q, i, j, k, sfx[ty][tx], sfx[ty][tx + 1], sfy[ty][tx], sfy[ty + 1][tx]) * msfty;
+      tend += D.qtf[n].ld(i, j, k);
+      D.qn[n](i, j, k) = (m_full(D, k, mub, mu1) * D.q1[n].ld(i, j, k) + dt_rk * tend) / m_full(D, k, mub, mu2);
+    }
+    __syncthreads();  // the next species reuses the face arrays
+  }
 }
 // KPreUpdatePD (:174-180)
 template <class R, int NM, int SH>

@@ -10,17 +10,20 @@
 
 namespace cw {
 
-#define CB_LOOP(k, n) for (int k = int(threadIdx.y); k < (n); k += CNW)
+#define CB_LOOP(k, n) for (int k = int(threadIdx.y); k < (n); k += NW)
 // the same for a body whose only stores go to shared memory: unrolled, the loads of the next level can be
 // issued before the stores of this one (shared stores cannot alias global loads)
-#define CB_LOOP_SH(k, n) _Pragma("unroll 2") for (int k = int(threadIdx.y); k < (n); k += CNW)
+#define CB_LOOP_SH(k, n) _Pragma("unroll 2") for (int k = int(threadIdx.y); k < (n); k += NW)
+// unrolled by two where that measured faster although the body stores to global memory (its read-only loads of
+// the next level can still be issued early)
+#define CB_LOOP_U2(k, n) _Pragma("unroll 2") for (int k = int(threadIdx.y); k < (n); k += NW)
 
 
 // a hint that brings the line of a into L2 (no register, no wait): the column blocks' level loops then meet L2
 // instead of DRAM latency
 __device__ __forceinline__ void pf_l2(const void* a) { asm volatile("prefetch.global.L2 [%0];" ::"l"(a)); }
-// the levels of a loop split over warps 1 .. CNW - 1 (warp 0 runs a recurrence meanwhile)
-#define CB_LOOP_W1(k, n) for (int k = int(threadIdx.y) - 1; threadIdx.y > 0 && k < (n); k += CNW - 1)
+// the levels of a loop split over warps 1 .. NW - 1 (warp 0 runs a recurrence meanwhile)
+#define CB_LOOP_W1(k, n) for (int k = int(threadIdx.y) - 1; threadIdx.y > 0 && k < (n); k += NW - 1)
 // block -> (member, column i of this lane, row j)
 // (ilim: the end of the member's column range along i; the lanes at or past it have no column)
 template <class R, int NM>
@@ -43,8 +46,8 @@ __device__ __forceinline__ double* cb_array(int a, int nz) {
 }
 
 // rk_step_prep: KMu (large_step.cpp:49-66), KPrep3 (:68-81), KWW (:83-108), KCq (:127-148)
-template <class R, int NM>
-__global__ void __launch_bounds__(CX * CNW, 3) k_ls_prep(const __grid_constant__ Pack<R, NM> P) {
+template <class R, int NM, int NW = CNW>
+__global__ void __launch_bounds__(CX * NW, cb_minblocks(NW)) k_ls_prep(const __grid_constant__ Pack<R, NM> P) {
   int i, j, ilim;
   const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j, ilim);
   const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
@@ -88,9 +91,9 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ls_prep(const __grid_constant__
         ph0 = D.ph2.ld(i, j, k);
         ph1 = D.ph2.ld(i, j, k + 1);
       }
-      if (has_u) D.ru(i, j, k) = u2 * (R(D.c1h[k]) * muu + R(D.c2h[k])) / msfuy;
+      if (has_u) D.ru(i, j, k) = div_msf(u2 * (R(D.c1h[k]) * muu + R(D.c2h[k])), msfuy);
       if (has_v) D.rv(i, j, k) = v2 * (R(D.c1h[k]) * muv + R(D.c2h[k])) * mvxi;
-      if (has_w) D.rw(i, j, k) = w2 * (R(D.c1f[k]) * mut + R(D.c2f[k])) / msfty;
+      if (has_w) D.rw(i, j, k) = div_msf(w2 * (R(D.c1f[k]) * mut + R(D.c2f[k])), msfty);
       if (has_m) {
         D.alt(i, j, k) = al + alb;
         D.php(i, j, k) = R(0.5) * (phb0 + phb1 + ph0 + ph1);
@@ -139,8 +142,8 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ls_prep(const __grid_constant__
 }
 
 // small_step_prep (KPrep small_step.cpp:50-93) + calc_p_rho (KPRho :114-119) + calc_coef_w (KCoefW :122-148)
-template <class R, int NM>
-__global__ void __launch_bounds__(CX * CNW, 3) k_ss_prep(const __grid_constant__ Pack<R, NM> P, int rk) {
+template <class R, int NM, int NW = CNW>
+__global__ void __launch_bounds__(CX * NW, cb_minblocks(NW)) k_ss_prep(const __grid_constant__ Pack<R, NM> P, int rk) {
   int i, j, ilim;
   const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j, ilim);
   const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
@@ -164,7 +167,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ss_prep(const __grid_constant__
       if (j < ny) D.muus(i, j, 0) = mus_u;
       if (i < nx && j < nyv) D.muvs(i, j, 0) = mus_v;
     }
-    CB_LOOP(k, nz + 1) {  // KPrep (every load of a level before its first store)
+    CB_LOOP_U2(k, nz + 1) {  // KPrep (every load of a level before its first store)
       const R c1h = k < nz ? R(D.c1h[k]) : R(0), c2h = k < nz ? R(D.c2h[k]) : R(0);
       const bool has_u = j < ny && k < nz, has_v = i < nx && j < nyv && k < nz;
       R ui = 0, u1 = 0, muu = 0, msfuy = 1, vi = 0, v1 = 0, muv = 0, mvxi = 0;
@@ -198,7 +201,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ss_prep(const __grid_constant__
       }
       if (has_u) {
         D.u_save(i, j, k) = ui;
-        D.u2(i, j, k) = ((c1h * mus_u + c2h) * u1 - (c1h * muu + c2h) * ui) / msfuy;
+        D.u2(i, j, k) = div_msf(((c1h * mus_u + c2h) * u1 - (c1h * muu + c2h) * ui), msfuy);
       }
       if (has_v) {
         D.v_save(i, j, k) = vi;
@@ -211,7 +214,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ss_prep(const __grid_constant__
           D.c2a(i, j, k) = R(k::cpovcv) * (pb + pp) / alt;
         }
         D.w_save(i, j, k) = wi;
-        D.w2(i, j, k) = ((R(D.c1f[k]) * mts + R(D.c2f[k])) * w1 - (R(D.c1f[k]) * mut + R(D.c2f[k])) * wi) / msfty;
+        D.w2(i, j, k) = div_msf(((R(D.c1f[k]) * mts + R(D.c2f[k])) * w1 - (R(D.c1f[k]) * mut + R(D.c2f[k])) * wi), msfty);
         D.ph_save(i, j, k) = phi;
         D.ph2(i, j, k) = ph1 - phi;
         D.ww1(i, j, k) = ww;
@@ -277,8 +280,8 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ss_prep(const __grid_constant__
 // shared memory. With lateral boundaries the spec zone's columns take LateralBC::update_mu_t (phase 1) and
 // the phi'' part of update_ph_w (phase 2); the zero-gradient w of that zone needs the neighbours' new w and
 // follows in its own launch.
-template <class R, int NM>
-__global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack<R, NM> P, int rk, int it,
+template <class R, int NM, int NW = CNW>
+__global__ void __launch_bounds__(CX * NW, cb_minblocks(NW)) k_ac(const __grid_constant__ Pack<R, NM> P, int rk, int it,
                                                     int nsteps) {
   constexpr int phase = 7;
   int i, j, ilim;
@@ -332,7 +335,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
       CB_LOOP(k, nz) {
         const R su = (first ? R(0) : D.ru_m(i, j, k)) + D.u2.ld(i, j, k);
         const R cpl = (R(D.c1h[k]) * D.muu.ld(i, j, 0) + R(D.c2h[k])) * D.u_save.ld(i, j, k);
-        D.ru_m(i, j, k) = last ? su / rn + cpl / D.msfuy(i, j) : su;
+        D.ru_m(i, j, k) = last ? su / rn + div_msf(cpl, D.msfuy(i, j)) : su;
       }
     if (col && D.spec_y && j == ny && i < nx)  // KSumEdge, north face (specified or open y)
       CB_LOOP(k, nz) {
@@ -375,7 +378,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
           }
           if (k + 1 < nz) s2[(k + 1) * CX + lane] = A(D.ww1.ld(i, j, k + 1));
           // KMuTDiv (small_step.cpp:194-206), the expression of mut_dv
-          const R fx = (u_ip + (c1h * muu_ip + c2h) * usv_ip / msfuy_ip) - (u_k + (c1h * muu + c2h) * usv / msfuy);
+          const R fx = (u_ip + div_msf((c1h * muu_ip + c2h) * usv_ip, msfuy_ip)) - (u_k + div_msf((c1h * muu + c2h) * usv, msfuy));
           R d = R(D.rdx) * fx;
           if (D.do_y) d += R(D.rdy) * ((v_jp + (c1h * muv_jp + c2h) * vsv_jp * mvxi_jp) - (v_k + (c1h * muv + c2h) * vsv * mvxi));
           const A dv = A(D.msftx(i, j) * D.msfty(i, j) * d);
@@ -383,7 +386,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
           s1[k * CX + lane] = D.dnw[k] * dv;  // the term of the column sum, for the serial sum below
         }
         const R su = rum + u_k;
-        D.ru_m(i, j, k) = last ? su / rn + (c1h * muu + c2h) * usv / msfuy : su;
+        D.ru_m(i, j, k) = last ? su / rn + div_msf((c1h * muu + c2h) * usv, msfuy) : su;
         if (D.do_y) {
           const R sv = rvm + v_k;
           D.rv_m(i, j, k) = last ? sv / rn + (c1h * muv + c2h) * vsv * mvxi : sv;
@@ -426,7 +429,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
     if (dyn) {  // the decrement of the omega integral at each level
       const A dmdt = sc[0 * CX + lane], mtend = sc[1 * CX + lane];
       const A msfty = A(D.msfty(i, j));
-      CB_LOOP_SH(k, nz - 1) s1[k * CX + lane] = D.dnw[k] * (D.c1h[k] * dmdt + s0[k * CX + lane] + D.c1h[k] * mtend) / msfty;
+      CB_LOOP_SH(k, nz - 1) s1[k * CX + lane] = div_msf(D.dnw[k] * (D.c1h[k] * dmdt + s0[k * CX + lane] + D.c1h[k] * mtend), msfty);
     }
     __syncthreads();
     if (dyn && w0) {  // ww'' by the running integral (ww1 of level k + 1 staged in s2[k + 1])
@@ -535,7 +538,7 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
     }
     __syncthreads();
     if (dyn) {
-      const A msft_inv = 1.0 / msfty;
+      const A msft_inv = div_msf(1.0, msfty);
       CB_LOOP_SH(k, nz + 1) {  // KWExpl: explicit w''
         A wn;
         if (k == 0) {
@@ -646,8 +649,8 @@ __global__ void __launch_bounds__(CX * CNW, 3) k_ac(const __grid_constant__ Pack
 }
 
 // small_step_finish (KFinish :419-444, KFinishMu :446-453) + calc_p_rho_phi (KPRhoPhi :456-477)
-template <class R, int NM>
-__global__ void __launch_bounds__(CX * CNW, 3) k_finish(const __grid_constant__ Pack<R, NM> P, int rk, int nsmall) {
+template <class R, int NM, int NW = CNW>
+__global__ void __launch_bounds__(CX * NW, cb_minblocks(NW)) k_finish(const __grid_constant__ Pack<R, NM> P, int rk, int nsmall) {
   int i, j, ilim;
   const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j, ilim);
   const int nx = D.nx, ny = D.ny, nz = D.nz, nyv = D.nyv;
@@ -732,8 +735,8 @@ __device__ __forceinline__ double damp_cos(double x) {
   if constexpr (sizeof(R) == 4) return ::cos(x);
   else return cw_cos(x);
 }
-template <class R, int NM>
-__global__ void __launch_bounds__(CX * CNW) k_dampkm(const __grid_constant__ Pack<R, NM> P) {
+template <class R, int NM, int NW = CNW>
+__global__ void __launch_bounds__(CX * NW) k_dampkm(const __grid_constant__ Pack<R, NM> P) {
   int i, j, ilim;
   const Dom<R>& D = cb_member(P, RG_COLS_MASS, i, j, ilim);
   if (D.damp_opt != 1 || !D.diff_on) return;  // uniform over the block
@@ -785,8 +788,8 @@ __global__ void __launch_bounds__(CX * CNW) k_dampkm(const __grid_constant__ Pac
 }
 
 // set_w_surface (KSetWSurface, rk3.cpp:173-200), fill = false
-template <class R, int NM>
-__global__ void __launch_bounds__(CX * CNW) k_w_surface(const __grid_constant__ Pack<R, NM> P) {
+template <class R, int NM, int NW = CNW>
+__global__ void __launch_bounds__(CX * NW) k_w_surface(const __grid_constant__ Pack<R, NM> P) {
   int i, j, ilim;
   const Dom<R>& D = cb_member(P, RG_COLS_MASS, i, j, ilim);
   if (threadIdx.y != 0 || i >= ilim) return;

@@ -42,8 +42,8 @@ __device__ __forceinline__ int mp_fall(double crmax) {
   return 1 < n ? n : 1;
 }
 
-template <class R, int NM>
-__global__ void __launch_bounds__(CX * CNW) k_kessler(const __grid_constant__ Pack<R, NM> P) {
+template <class R, int NM, int NW = CNW>
+__global__ void __launch_bounds__(CX * NW) k_kessler(const __grid_constant__ Pack<R, NM> P) {
   int i, j, ilim;
   const Dom<R>& D = cb_member(P, RG_COLS_MASS, i, j, ilim);
   if (D.mp_physics != 1) return;  // uniform over the block

@@ -1,6 +1,7 @@
 # SPDX-License-Identifier: GPL-3.0-or-later
 """Block-shape autotuning: the tuning steps are ordinary steps and every shape computes the same values, so an
-autotuned run is bit-identical to a run with the default shapes; afterwards each tunable kernel has a choice."""
+autotuned run is bit-identical to a run with the default shapes; afterwards each tunable kernel has a choice. A
+column kernel's shape is its warps per column block (8, 16 or 4): only the parallel loops over levels change."""
 import numpy as np
 import pytest
 
@@ -9,7 +10,8 @@ from cases import lam_case
 
 pytestmark = pytest.mark.gpu
 
-TUNABLE = ["k_tend", "k_tendf_rk1", "k_uv", "k_q_update", "k_q_face_pd", "k_q_scale_pd", "k_q_update_pd"]
+TUNABLE = ["k_tend", "k_tendf_rk1", "k_uv", "k_q_update", "k_q_face_pd", "k_q_scale_pd", "k_q_update_pd",
+           "k_ls_prep", "k_ss_prep", "k_ac", "k_finish"]  # the last four: warps per column block
 
 
 @pytest.mark.parametrize("precision", [capi.FP64, capi.MIXED], ids=["fp64", "mixed"])
