@@ -135,16 +135,53 @@ class Domain:
         return v.value
 
 
-class Decomp:
-    """One domain decomposed into px x py patches on the device (cw_decomp_create): fields go in and out as
-    whole-domain arrays; the step is RK3::step of the undecomposed domain, bit for bit."""
+def nccl_unique_id(lib=None):
+    """The 128 bytes that every rank of a decomposed domain passes to Decomp (made on one rank, sent to the others)."""
+    lib = lib or capi.load()
+    buf = (C.c_ubyte * 128)()
+    _check(lib, None, lib.cw_nccl_unique_id(buf), "cw_nccl_unique_id")
+    return bytes(buf)
 
-    def __init__(self, g, o, px, py, lib=None):
+
+def decomp_plan(g, o, px, py, rank, nranks, sets, lib=None):
+    """cw_decomp_plan: the boxes crossing between `rank` and the other ranks at the fill point made of `sets`, one row
+    each: role (0 packed by this rank, 1 unpacked), peer, receiving patch, owning patch, field, i0, i1, j0, j1,
+    levels, offset in the send / receive region (no device)."""
+    lib = lib or capi.load()
+    s = (C.c_int * len(sets))(*sets)
+    n = C.c_int()
+    _check(lib, None, lib.cw_decomp_plan(C.byref(g), C.byref(o), px, py, rank, nranks, len(sets), s, None, 0,
+                                         C.byref(n)), "cw_decomp_plan")
+    out = np.zeros((max(n.value, 1), 11), dtype=np.int64)
+    _check(lib, None, lib.cw_decomp_plan(C.byref(g), C.byref(o), px, py, rank, nranks, len(sets), s,
+                                         out.ctypes.data_as(C.POINTER(C.c_longlong)), n.value, C.byref(n)),
+           "cw_decomp_plan")
+    return out[:n.value]
+
+
+class Decomp:
+    """One domain decomposed into px x py patches (cw_decomp_create): fields go in and out as whole-domain arrays;
+    the step is RK3::step of the undecomposed domain, bit for bit. With nranks > 1 the patches are spread over
+    processes (cw_decomp_create_ranked: patch t on rank t % nranks, halos over NCCL; nccl_id from nccl_unique_id on
+    one rank, the same on all), or with loopback=True all held here with the ranks' exchanges through the packed
+    buffers."""
+
+    def __init__(self, g, o, px, py, lib=None, rank=0, nranks=1, nccl_id=None, loopback=False):
         self.lib = lib or capi.load()
         self.g, self.o = g, o
         self.h = C.c_void_p()
-        _check(self.lib, None, self.lib.cw_decomp_create(C.byref(g), C.byref(o), int(px), int(py), C.byref(self.h)),
-               "cw_decomp_create")
+        if nranks == 1 and not loopback:
+            rc = self.lib.cw_decomp_create(C.byref(g), C.byref(o), int(px), int(py), C.byref(self.h))
+            _check(self.lib, None, rc, "cw_decomp_create")
+            return
+        idp = None
+        if not loopback:
+            if nccl_id is None or len(nccl_id) != 128:
+                raise ValueError("nccl_id: the 128 bytes of nccl_unique_id, the same on every rank")
+            idp = (C.c_ubyte * 128)(*nccl_id)
+        rc = self.lib.cw_decomp_create_ranked(C.byref(g), C.byref(o), int(px), int(py), int(rank), int(nranks), idp,
+                                              C.byref(self.h))
+        _check(self.lib, None, rc, "cw_decomp_create_ranked")
 
     def close(self):
         if getattr(self, "h", None) and self.h.value:

@@ -41,7 +41,7 @@ def build(verbose=False):
     failed = [cmd for cmd, p in procs if p.wait() != 0]
     if failed:
         raise subprocess.CalledProcessError(1, failed[0])
-    cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-Xcompiler", "-fopenmp", "-lgomp"]
+    cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-Xcompiler", "-fopenmp", "-lgomp", "-ldl"]
     subprocess.run(cmd, check=True)
     return LIB
 

@@ -40,6 +40,11 @@ XS, XE, YS, YE = range(4)
 # enum cw_ideal_kind
 REST_STATE, STRAKA, WARM_BUBBLE, IGW, SQUALL2D = range(5)
 DEFAULT = -1.0e300
+# the fill points of one step (cw_decomp_plan)
+(FILL_MU1, FILL_PREP0, FILL_PREP1, FILL_SS0, FILL_UV, FILL_AC, FILL_POST, FILL_FIN, FILL_Q1PD, FILL_SCPD, FILL_Q2,
+ FILL_END_P, FILL_WS0, FILL_WS1, FILL_MP, FILL_MP_P, FILL_XK) = range(17)
+# cw_decomp_plan's field numbers beyond the field ids
+FID_W, FID_Q2, FID_Q1, FID_QSC = 1000, 2000, 3000, 4000
 # cw_download_noalloc: scratch capacity (doubles) and return codes
 NOALLOC_SCRATCH_DOUBLES = 1048576
 NOALLOC_EBADARG, NOALLOC_ETOOBIG, NOALLOC_ECUDA = -1, -2, -3
@@ -187,6 +192,11 @@ def load(path=None):
         "cw_decomp_upload": (i, [vp, i, i, dp, sz]),
         "cw_decomp_download": (i, [vp, i, i, dp, sz]),
         "cw_decomp_upload_case": (i, [vp, vp]),
+        "cw_nccl_unique_id": (i, [C.POINTER(C.c_ubyte)]),
+        "cw_decomp_create_ranked": (i, [C.POINTER(Grid), C.POINTER(Options), i, i, i, i, C.POINTER(C.c_ubyte),
+                                        C.POINTER(vp)]),
+        "cw_decomp_plan": (i, [C.POINTER(Grid), C.POINTER(Options), i, i, i, i, i, ip, C.POINTER(C.c_longlong), i,
+                               ip]),
         "cw_check_div_const": (i, [C.c_ulonglong, C.c_ulonglong, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]),
         "cw_autotune_choice": (i, [vp, C.c_char_p, ip]),
         "cw_footprint": (i, [C.POINTER(Grid), C.POINTER(Options), C.POINTER(sz)]),

@@ -58,6 +58,7 @@ struct Member {
   cw_options o{};
   bool patched = false;  // a patch of a decomposed domain (cw_decomp_create): fields allocated for `patch` + halo
   Box patch{};
+  int tid = -1;  // its patch number t = tx + px ty
   const Box* pbox() const { return patched ? &patch : nullptr; }
   int n_sound = 0;
   int esz = 8;  // element size of the fields (8: FP64 form, 4: mixed form)
@@ -100,20 +101,43 @@ struct DevTables {  // the kernels' views of the members and the device scalar t
 
 // a fill point's fields (or the union of consecutive fill points') as a device table: one launch per pass
 // whatever the number of fields (the batch path); for a decomposed domain also the exchange boxes, copied first
+// A box of a decomposed domain's exchange whose two patches are on different ranks: patch `me` (on dst_rank)
+// receives the points of the rectangle that patch t (on src_rank) owns. send: t's field -> the packed send buffer
+// (when t is this process's); recv: the packed receive buffer -> me's field (when me is this process's).
+struct RBox {
+  int me, t, fid, src_rank, dst_rank;
+  bool has_send, has_recv;
+  XchgBox send, recv;
+};
+struct Xfer {  // a fill point's transfer with one rank: n elements at element offset off of the send / receive region
+  int peer;
+  size_t off, n;
+};
+struct XCopy {  // loopback transport: a send segment copied into its receive segment
+  size_t soff, roff, n;
+};
+
 struct HaloTable {
   HaloField* f = nullptr;
   unsigned* start = nullptr;
   int nf = 0;
   unsigned total = 0;
   int has_oddface = 0;
-  XchgBox* x = nullptr;
+  XchgBox* x = nullptr;  // the exchange between this process's patches, then the unpacking of received boxes
   unsigned* xstart = nullptr;
   int nx = 0;
   unsigned xtotal = 0;
+  XchgBox* pk = nullptr;  // the packing of the boxes other ranks receive
+  unsigned* pkstart = nullptr;
+  int npk = 0;
+  unsigned pktotal = 0;
+  std::vector<Xfer> sends, recvs;  // over NCCL, in this order inside one group
+  std::vector<XCopy> copies;       // loopback
 };
 
 struct HaloSetHost {
   std::vector<HaloField> f;
+  std::vector<RBox> r;     // a decomposed domain over ranks: the boxes crossing between ranks
   std::vector<XchgBox> x;  // a decomposed domain: the points of other patches each patch receives first
   std::vector<HaloChunk<kHaloSmall>> small;  // the fields in one small chunk (most single domains), or
   std::vector<HaloChunk<kHaloLarge>> large;  // in large chunks
@@ -127,6 +151,14 @@ struct cw_handle {
   int precision = CW_FP64;
   std::vector<Member> m;
   int decomp_px = 0, decomp_py = 0;  // a decomposed domain (cw_decomp_create): its members are the px x py patches
+  // a decomposed domain over ranks (cw_decomp_create_ranked): patch t is rank t % nranks's; this process holds the
+  // patches of `rank` (every patch in the loopback form, whose exchanges between ranks are device copies)
+  int rank = 0, nranks = 1;
+  bool loopback = false;
+  std::vector<Member> remote;  // the other ranks' patches: layouts only, for the exchange plan
+  void* comm = nullptr;        // the ranks' NCCL communicator
+  char* xbuf = nullptr;        // packed exchange buffers: send region (xsend_cap elements), then receive region
+  size_t xsend_cap = 0, xrecv_cap = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int device = -1;  // the CUDA device current at create (every allocation of the handle is on it)
@@ -201,5 +233,29 @@ void chunk_fields(const std::vector<HaloField>& f, std::vector<HaloChunk<NF>>& o
 // the mixed form's step (cw_step_mixed.cu): enqueues one step of h on its stream (plan: no launch, only the
 // tables the launches need), returns the launches
 long long enqueue_mixed(cw_handle* h, bool plan);
+
+// A decomposed domain over ranks: the boxes between ranks of a fill point (the union of the sets `pend`), each once,
+// grouped by (sending rank, receiving rank) in ascending order and in list order inside a group -- the order both
+// ranks of a pair derive -- packed into consecutive segments of the send region and unpacked from the same segments of
+// the receive region. pk: the boxes this process packs (destination: the send region, doff the element offset),
+// unpk: those it unpacks (source: the receive region, soff); the transfers per rank (or loopback copies); `role`
+// lists every box as (0: packed, 1: unpacked) with its peer rank and region offset, in that order.
+struct CrossPlan {
+  std::vector<XchgBox> pk, unpk;
+  std::vector<Xfer> sends, recvs;
+  std::vector<XCopy> copies;
+  struct Entry {
+    int role, peer;
+    const RBox* box;
+    size_t off;
+  };
+  std::vector<Entry> role;
+  size_t send_n = 0, recv_n = 0;
+};
+CrossPlan cross_plan(const cw_handle* h, const std::vector<int>& pend);
+
+// a fill point's transfers between ranks (a decomposed domain over ranks): the send segments to their ranks and the
+// receive segments from theirs, NCCL point-to-point in one group on the handle's stream (cw_runtime.cu)
+void nccl_exchange(cw_handle* h, const HaloTable& t, char* sbuf, char* rbuf, size_t esz);
 
 }  // namespace cw

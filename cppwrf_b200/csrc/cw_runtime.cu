@@ -8,6 +8,9 @@
 // small_step_finish, scalar transport and calc_p_rho_phi; spec_bdy_final and set_w_surface at the end.
 // Halos are refreshed where the reference refreshes them; refreshes with no kernel in between that
 // reads the refreshed cells are merged into one launch.
+#include <dlfcn.h>
+#include <nccl.h>
+
 #include "cw_step.cuh"
 
 namespace {
@@ -165,6 +168,8 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.nx = g.nx; D.ny = g.ny; D.nz = g.nz; D.nyv = nys(g, 'V'); D.two_d = two_d(g); D.do_y = !two_d(g);
   const Box pb = M.patched ? M.patch : Box{0, g.nx, 0, g.ny};
   D.pi0 = pb.i0; D.pi1 = pb.i1; D.pj0 = pb.j0; D.pj1 = pb.j1;
+  D.wi0 = M.L[CW_T_2].wi0; D.wi1m = M.L[CW_T_2].wi1; D.wi1u = M.L[CW_U_2].wi1;
+  D.wj0 = M.L[CW_T_2].wj0; D.wj1m = M.L[CW_T_2].wj1; D.wj1v = M.L[CW_V_2].wj1;
   D.bc_x = g.bc_x; D.bc_y = g.bc_y;
   D.spec_x = flat_x(g); D.spec_y = flat_y(g) && !two_d(g);
   D.open_x = g.bc_x == CW_BC_OPEN; D.open_y = g.bc_y == CW_BC_OPEN && !two_d(g);
@@ -355,7 +360,9 @@ struct HaloItem {
   void* ind;         // indirect view address
   cw_layout L;
   int parity;
+  int fid;           // the field: its id, or FID_W + work field, FID_Q2 / FID_Q1 / FID_QSC + species
 };
+enum : int { FID_W = 1000, FID_Q2 = 2000, FID_Q1 = 3000, FID_QSC = 4000 };
 
 HaloField halo_field(const Member& M, const HaloItem& it) {
   HaloField f{};
@@ -405,96 +412,171 @@ Box owned_box(const Member& M, char s) {
   return Box{p.i0, (s == 'U' && p.i1 == M.g.nx) ? M.g.nx + 1 : p.i1, p.j0,
              (s == 'V' && p.j1 == M.g.ny && !two_d(M.g)) ? M.g.ny + 1 : p.j1};
 }
-// a decomposed domain's exchange of one field: every point of member `me`'s allocation window that member `t` owns
-void exchange_boxes(const Member& me, const HaloItem& a, const Member& t, const HaloItem& b, std::vector<XchgBox>& out) {
-  const cw_layout& L = a.L;
-  if (L.uniform) return;
+// the rectangle of a field's window (layout L of some patch) that patch t owns, all levels
+bool exchange_rect(const cw_layout& L, const Member& t, XchgBox& x) {
+  if (L.uniform) return false;
   const Box o = owned_box(t, L.stagger);
-  XchgBox x{};
+  x = XchgBox{};
   x.i0 = std::max(L.wi0, o.i0);
   x.i1 = std::min(L.wi1, o.i1);
   x.j0 = std::max(L.wj0, o.j0);
   x.j1 = std::min(L.wj1, o.j1);
-  if (x.i0 >= x.i1 || x.j0 >= x.j1) return;
+  if (x.i0 >= x.i1 || x.j0 >= x.j1) return false;
+  x.nk = L.nz;
+  x.ncell = (long long)(x.i1 - x.i0) * (x.j1 - x.j0) * x.nk;
+  return true;
+}
+// the source side of a box: the owner's field (element (0, 0, 0) or its table entry)
+void box_source(XchgBox& x, const Member& t, const HaloItem& b) {
   x.src = b.base ? b.base + size_t(b.L.offset) * t.esz : nullptr;
   x.src_ind = b.ind;
-  x.dst = a.base ? a.base + size_t(L.offset) * me.esz : nullptr;
-  x.dst_ind = a.ind;
   x.ssj = int(b.L.sj);
   x.ssk = int(b.L.sk);
-  x.dsj = int(L.sj);
-  x.dsk = int(L.sk);
-  x.nk = L.nz;
+  x.is_float = t.esz == 4;
+}
+// the destination side: the receiving patch's field
+void box_dest(XchgBox& x, const Member& me, const HaloItem& a) {
+  x.dst = a.base ? a.base + size_t(a.L.offset) * me.esz : nullptr;
+  x.dst_ind = a.ind;
+  x.dsj = int(a.L.sj);
+  x.dsk = int(a.L.sk);
   x.is_float = me.esz == 4;
-  x.ncell = (long long)(x.i1 - x.i0) * (x.j1 - x.j0) * x.nk;
-  out.push_back(x);
 }
 
+// one field of a fill point: its set (the fill point), the field, and whether the fill only refreshes the points of
+// the neighbouring patches (no boundary fill)
+struct FillItem {
+  int set;
+  HaloItem it;
+  bool xonly;
+};
+// The fields of every fill point of member M, in one order (the same for every patch of a decomposed domain, whose
+// patches share their options). qt: the member's scalar table in device memory, null for a patch of another rank
+// (its items carry layouts only).
 template <class R>
-void build_halosets_t(cw_handle* h, DevTables<R>& T) {
-  size_t q0 = 0;
-  // a decomposed domain: each member's items per fill point in the same order (the patches share their options),
-  // the exchange-only ones marked (neighbours' points refreshed without a boundary fill)
-  std::vector<std::vector<std::tuple<int, HaloItem, bool>>> items(h->m.size());
+std::vector<FillItem> fill_items(const Member& M, V3<R>* qt) {
+  std::vector<FillItem> v;
+  const int ns = M.o.n_scalars;
+  auto at = [](const std::vector<char*>& b, size_t k) -> char* { return k < b.size() ? b[k] : nullptr; };
+  auto F = [&](int id, int par = HP_DEFAULT) { return HaloItem{at(M.base, size_t(id)), nullptr, M.L[id], par, id}; };
+  auto W = [&](int w, int par = HP_DEFAULT) {
+    return HaloItem{at(M.wbase, size_t(w)), nullptr, M.LW[w], par, FID_W + w};
+  };
+  auto Q2 = [&](int n) { return HaloItem{nullptr, qt ? qt + ns + n : nullptr, M.Lq, HP_DEFAULT, FID_Q2 + n}; };
+  auto add = [&](int set, std::initializer_list<HaloItem> its) {
+    for (const HaloItem& it : its) v.push_back(FillItem{set, it, false});
+  };
+  auto exchange_only = [&](int set, const HaloItem& it) { v.push_back(FillItem{set, it, true}); };
+  const bool spec = specified(M.g);
+  add(cw_handle::H_MU1, {F(CW_MU_1)});
+  if (xk_fields(M.o)) add(cw_handle::H_XK, {W(W_XKMH), W(W_XKHH)});  // DiffusionDriver::prepare's fill
+  add(cw_handle::H_PREP0, {F(CW_U_2), F(CW_V_2), F(CW_W_2), F(CW_T_2), F(CW_PH_2), F(CW_P), F(CW_AL)});
+  if (!spec) add(cw_handle::H_PREP0, {F(CW_MU_2)});
+  else {  // tiles: the neighbours' points that spec_bdy_final changed (large_step.cpp:705; the scalars' too)
+    exchange_only(cw_handle::H_PREP0, F(CW_MU_2));
+    for (int n = 0; n < ns; ++n) exchange_only(cw_handle::H_PREP0, Q2(n));
+  }
+  add(cw_handle::H_PREP1, {F(CW_MUT), F(CW_RU), F(CW_RV), F(CW_RW), F(CW_ALT), F(CW_PHP), F(CW_MUU, HP_ODDFACE_X),
+                           F(CW_MUV, HP_ODD_Y), F(CW_WW)});
+  add(cw_handle::H_SS0, {F(CW_U_2), F(CW_V_2), F(CW_PH_2), W(W_T_SAVE), W(W_U_SAVE), W(W_V_SAVE), F(CW_MU_2),
+                         F(CW_MUTS), F(CW_P), F(CW_AL)});
+  add(cw_handle::H_UV, {F(CW_U_2)});
+  if (!two_d(M.g)) add(cw_handle::H_UV, {F(CW_V_2)});
+  add(cw_handle::H_AC, {F(CW_MU_2), W(W_MUDF), F(CW_MUTS), F(CW_PH_2), F(CW_P), F(CW_AL)});
+  add(cw_handle::H_POST, {F(CW_MUTS), F(CW_RU_M), F(CW_RV_M), F(CW_WW_M)});
+  add(cw_handle::H_FIN, {F(CW_U_2), F(CW_V_2), F(CW_W_2), F(CW_T_2), F(CW_PH_2), F(CW_WW), F(CW_MU_2), F(CW_P), F(CW_AL)});
+  for (int n = 0; n < ns; ++n) {
+    add(cw_handle::H_Q1PD, {HaloItem{at(M.q1, size_t(n)), nullptr, M.Lq, HP_DEFAULT, FID_Q1 + n}});
+    add(cw_handle::H_SCPD, {HaloItem{at(M.qsc, size_t(n)), nullptr, M.Lq, HP_DEFAULT, FID_QSC + n}});
+    add(cw_handle::H_Q2, {Q2(n)});
+  }
+  add(cw_handle::H_END_P, {F(CW_P), F(CW_AL)});
+  if (M.o.mp_physics != 0) {  // PhysicsCoupling::step's halos (physics_coupling.cpp:452-456), then calc_p_rho_phi's
+    add(cw_handle::H_MP, {F(CW_T_2), F(CW_H_DIABATIC)});
+    for (int n = 0; n < M.o.n_moist; ++n) add(cw_handle::H_MP, {Q2(n)});
+    add(cw_handle::H_MP_P, {F(CW_P), F(CW_AL)});
+  }
+  add(cw_handle::H_WS0, {F(CW_U_2), F(CW_V_2)});
+  add(cw_handle::H_WS1, {F(CW_W_2)});
+  return v;
+}
+
+// patch t's rank in a decomposed domain over ranks
+inline int rank_of(const cw_handle* h, int t) { return t % h->nranks; }
+
+// (device: false for a plan made without a device, cw_decomp_plan: no exchange buffer)
+template <class R>
+void build_halosets_t(cw_handle* h, DevTables<R>& T, bool device = true) {
   const bool dec = h->decomp_px > 0;
+  const int np = dec ? h->decomp_px * h->decomp_py : 0;
+  std::vector<std::vector<FillItem>> items(dec ? size_t(np) : 0);  // a decomposed domain: by patch number
+  std::vector<const Member*> pat(items.size(), nullptr);
+  std::vector<char> local(items.size(), 0);
+  size_t q0 = 0;
   for (size_t mi = 0; mi < h->m.size(); ++mi) {
     Member& M = h->m[mi];
-    const int ns = M.o.n_scalars;
-    auto F = [&](int id, int par = HP_DEFAULT) { return HaloItem{M.base[id], nullptr, M.L[id], par}; };
-    auto W = [&](int w, int par = HP_DEFAULT) { return HaloItem{M.wbase[w], nullptr, M.LW[w], par}; };
-    auto add = [&](int set, std::initializer_list<HaloItem> its) {
-      for (const HaloItem& it : its) {
-        h->hs[set].f.push_back(halo_field(M, it));
-        if (dec) items[mi].emplace_back(set, it, false);
-      }
-    };
-    auto exchange_only = [&](int set, const HaloItem& it) {
-      if (dec) items[mi].emplace_back(set, it, true);
-    };
-    const bool spec = specified(M.g);
-    add(cw_handle::H_MU1, {F(CW_MU_1)});
-    if (xk_fields(M.o)) add(cw_handle::H_XK, {W(W_XKMH), W(W_XKHH)});  // DiffusionDriver::prepare's fill
-    add(cw_handle::H_PREP0, {F(CW_U_2), F(CW_V_2), F(CW_W_2), F(CW_T_2), F(CW_PH_2), F(CW_P), F(CW_AL)});
-    if (!spec) add(cw_handle::H_PREP0, {F(CW_MU_2)});
-    else {  // tiles: the neighbours' points that spec_bdy_final changed (large_step.cpp:705; the scalars' too)
-      exchange_only(cw_handle::H_PREP0, F(CW_MU_2));
-      for (int n = 0; n < ns; ++n)
-        exchange_only(cw_handle::H_PREP0, HaloItem{nullptr, T.qtab + kQTab * q0 + ns + n, M.Lq, HP_DEFAULT});
+    std::vector<FillItem> v = fill_items<R>(M, T.qtab ? T.qtab + kQTab * q0 : nullptr);
+    for (const FillItem& fi : v)
+      if (!fi.xonly) h->hs[fi.set].f.push_back(halo_field(M, fi.it));
+    if (dec) {
+      const size_t t = size_t(M.tid);
+      pat[t] = &M;
+      local[t] = 1;
+      items[t] = std::move(v);
     }
-    add(cw_handle::H_PREP1, {F(CW_MUT), F(CW_RU), F(CW_RV), F(CW_RW), F(CW_ALT), F(CW_PHP), F(CW_MUU, HP_ODDFACE_X),
-                             F(CW_MUV, HP_ODD_Y), F(CW_WW)});
-    add(cw_handle::H_SS0, {F(CW_U_2), F(CW_V_2), F(CW_PH_2), W(W_T_SAVE), W(W_U_SAVE), W(W_V_SAVE), F(CW_MU_2),
-                           F(CW_MUTS), F(CW_P), F(CW_AL)});
-    add(cw_handle::H_UV, {F(CW_U_2)});
-    if (!two_d(M.g)) add(cw_handle::H_UV, {F(CW_V_2)});
-    add(cw_handle::H_AC, {F(CW_MU_2), W(W_MUDF), F(CW_MUTS), F(CW_PH_2), F(CW_P), F(CW_AL)});
-    add(cw_handle::H_POST, {F(CW_MUTS), F(CW_RU_M), F(CW_RV_M), F(CW_WW_M)});
-    add(cw_handle::H_FIN, {F(CW_U_2), F(CW_V_2), F(CW_W_2), F(CW_T_2), F(CW_PH_2), F(CW_WW), F(CW_MU_2), F(CW_P), F(CW_AL)});
-    for (int n = 0; n < ns; ++n) {
-      add(cw_handle::H_Q1PD, {HaloItem{M.q1[n], nullptr, M.Lq, HP_DEFAULT}});
-      add(cw_handle::H_SCPD, {HaloItem{M.qsc[n], nullptr, M.Lq, HP_DEFAULT}});
-      add(cw_handle::H_Q2, {HaloItem{nullptr, T.qtab + kQTab * q0 + ns + n, M.Lq, HP_DEFAULT}});
-    }
-    add(cw_handle::H_END_P, {F(CW_P), F(CW_AL)});
-    if (M.o.mp_physics != 0) {  // PhysicsCoupling::step's halos (physics_coupling.cpp:452-456), then calc_p_rho_phi's
-      add(cw_handle::H_MP, {F(CW_T_2), F(CW_H_DIABATIC)});
-      for (int n = 0; n < M.o.n_moist; ++n) add(cw_handle::H_MP, {HaloItem{nullptr, T.qtab + kQTab * q0 + ns + n, M.Lq, HP_DEFAULT}});
-      add(cw_handle::H_MP_P, {F(CW_P), F(CW_AL)});
-    }
-    add(cw_handle::H_WS0, {F(CW_U_2), F(CW_V_2)});
-    add(cw_handle::H_WS1, {F(CW_W_2)});
-    q0 += size_t(ns);
+    q0 += size_t(M.o.n_scalars);
   }
-  if (dec)  // every patch receives, at each fill point, the points of its window that the others own
-    for (size_t me = 0; me < h->m.size(); ++me)
-      for (size_t t = 0; t < h->m.size(); ++t) {
-        if (t == me) continue;
-        if (items[me].size() != items[t].size()) throw std::runtime_error("decomposition: patches differ");
-        for (size_t k = 0; k < items[me].size(); ++k) {
-          const auto& [set, a, xo] = items[me][k];
-          exchange_boxes(h->m[me], a, h->m[t], std::get<1>(items[t][k]), h->hs[set].x);
+  for (const Member& M : h->remote) {
+    pat[size_t(M.tid)] = &M;
+    items[size_t(M.tid)] = fill_items<R>(M, nullptr);
+  }
+  // every patch receives, at each fill point, the points of its window that the others own: a box between two
+  // patches of one rank is copied directly, a box between ranks is packed by the owner's rank, transferred and
+  // unpacked by the receiver's (both ranks list it in the same order: receiving patch, owning patch, field)
+  size_t send_cap = 0, recv_cap = 0;
+  for (int me = 0; me < np; ++me)
+    for (int t = 0; t < np; ++t) {
+      if (t == me || (!local[size_t(me)] && !local[size_t(t)])) continue;
+      if (!pat[size_t(me)] || !pat[size_t(t)]) throw std::runtime_error("decomposition: a patch is missing");
+      const std::vector<FillItem>& A = items[size_t(me)];
+      const std::vector<FillItem>& B = items[size_t(t)];
+      if (A.size() != B.size()) throw std::runtime_error("decomposition: patches differ");
+      const bool cross = h->loopback ? rank_of(h, me) != rank_of(h, t) : !(local[size_t(me)] && local[size_t(t)]);
+      for (size_t k = 0; k < A.size(); ++k) {
+        XchgBox x;
+        if (!exchange_rect(A[k].it.L, *pat[size_t(t)], x)) continue;
+        if (!cross) {
+          box_source(x, *pat[size_t(t)], B[k].it);
+          box_dest(x, *pat[size_t(me)], A[k].it);
+          h->hs[A[k].set].x.push_back(x);
+          continue;
         }
+        RBox r{};
+        r.me = me;
+        r.t = t;
+        r.fid = A[k].it.fid;
+        r.src_rank = rank_of(h, t);
+        r.dst_rank = rank_of(h, me);
+        r.has_send = local[size_t(t)] != 0;
+        r.has_recv = local[size_t(me)] != 0;
+        r.send = r.recv = x;
+        if (r.has_send) {
+          box_source(r.send, *pat[size_t(t)], B[k].it);
+          send_cap += size_t(x.ncell);
+        }
+        if (r.has_recv) {
+          box_dest(r.recv, *pat[size_t(me)], A[k].it);
+          recv_cap += size_t(x.ncell);
+        }
+        h->hs[A[k].set].r.push_back(r);
       }
+    }
+  if (device && send_cap + recv_cap > 0) {  // every fill point's boxes fit (a fill point is a union of sets)
+    const size_t esz = h->m.empty() ? 8 : size_t(h->m[0].esz);
+    CW_CUDA(cudaMalloc(&h->xbuf, (send_cap + recv_cap) * esz));
+    h->xsend_cap = send_cap;
+    h->xrecv_cap = recv_cap;
+  }
   for (int s = 0; s < cw_handle::H_N; ++s) finish_haloset(h, h->hs[s]);
 }
 
@@ -609,7 +691,7 @@ void run_steps(cw_handle* h, int nsteps) {
   }
   if (nsteps == 0) return;
   if (h->use_graph && !h->graph_ok) {
-    if (h->m.size() > 1) {  // a batch's halo tables are device allocations: made before the capture
+    if (h->m.size() > 1 || h->decomp_px > 0) {  // a batch's halo tables are device allocations: made before the capture
       Launcher P{h};
       P.plan = true;
       enqueue(h, P);
@@ -665,8 +747,13 @@ void free_tables(cw_handle* h) {
     cudaFree(kv.second.start);
     cudaFree(kv.second.x);
     cudaFree(kv.second.xstart);
+    cudaFree(kv.second.pk);
+    cudaFree(kv.second.pkstart);
   }
   h->halo_tabs.clear();
+  cudaFree(h->xbuf);
+  h->xbuf = nullptr;
+  h->xsend_cap = h->xrecv_cap = 0;
   cudaFree(h->copies_d);
   cudaFree(h->copies_start_d);
   cudaFree(h->zeros_d);
@@ -837,7 +924,159 @@ void diagnostics_t(cw_handle* h, int mi, DevTables<R>& T, cw_diag* out) {
   out->max_abs_q = 0.0 < mq ? mq : 0.0;
 }
 
+// a decomposed domain's handle on this process: its patches (every patch when loopback or nranks == 1), the other
+// ranks' patches as layouts; no device work
+std::unique_ptr<cw_handle> decomp_handle(const cw_grid* g, const cw_options* o, int px, int py, int rank, int nranks,
+                                         bool loopback) {
+  if (!g || !o) throw std::runtime_error("null argument");
+  if (const char* why = decomp_unsupported(*g, px, py)) throw std::runtime_error(why);
+  if (nranks < 1 || nranks > px * py || rank < 0 || rank >= nranks)
+    throw std::runtime_error("decomposition: 0 <= rank < nranks <= px * py");
+  auto h = std::make_unique<cw_handle>();
+  h->precision = o->precision;
+  h->decomp_px = px;
+  h->decomp_py = py;
+  h->rank = rank;
+  h->nranks = nranks;
+  h->loopback = loopback && nranks > 1;
+  for (int t = 0; t < px * py; ++t) {
+    Member M = make_member(*g, *o);
+    M.patched = true;
+    M.patch = patch_box(*g, px, py, t);
+    M.tid = t;
+    if (h->loopback || t % nranks == rank) {
+      h->m.push_back(std::move(M));
+    } else {
+      plan_member(M);  // the layouts of its fields
+      h->remote.push_back(std::move(M));
+    }
+  }
+  return h;
+}
+
+// NCCL, loaded when the first decomposed domain over ranks is made (libnccl.so.2: the one the process has loaded
+// already, if any); nothing else needs it
+struct NcclApi {
+  bool ok = false;
+  std::string err;
+  decltype(&ncclGetUniqueId) GetUniqueId = nullptr;
+  decltype(&ncclCommInitRank) CommInitRank = nullptr;
+  decltype(&ncclCommDestroy) CommDestroy = nullptr;
+  decltype(&ncclSend) Send = nullptr;
+  decltype(&ncclRecv) Recv = nullptr;
+  decltype(&ncclGroupStart) GroupStart = nullptr;
+  decltype(&ncclGroupEnd) GroupEnd = nullptr;
+  decltype(&ncclGetErrorString) GetErrorString = nullptr;
+};
+const NcclApi& nccl_api() {
+  static const NcclApi api = [] {
+    NcclApi a;
+    void* lib = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+    if (!lib) {
+      const char* e = dlerror();
+      a.err = std::string("NCCL: ") + (e ? e : "libnccl.so.2 not found");
+      return a;
+    }
+    bool ok = true;
+    auto sym = [&](auto& f, const char* name) {
+      f = reinterpret_cast<std::remove_reference_t<decltype(f)>>(dlsym(lib, name));
+      ok &= f != nullptr;
+    };
+    sym(a.GetUniqueId, "ncclGetUniqueId");
+    sym(a.CommInitRank, "ncclCommInitRank");
+    sym(a.CommDestroy, "ncclCommDestroy");
+    sym(a.Send, "ncclSend");
+    sym(a.Recv, "ncclRecv");
+    sym(a.GroupStart, "ncclGroupStart");
+    sym(a.GroupEnd, "ncclGroupEnd");
+    sym(a.GetErrorString, "ncclGetErrorString");
+    a.ok = ok;
+    if (!ok) a.err = "NCCL: a symbol is missing from libnccl.so.2";
+    return a;
+  }();
+  return api;
+}
+void nccl_check(const NcclApi& N, ncclResult_t r, const char* what) {
+  if (r != ncclSuccess) throw std::runtime_error(std::string(what) + ": " + N.GetErrorString(r));
+}
+
 }  // namespace
+
+// the step's exchange between ranks (declared in cw_handle.cuh, called by the launcher of either form)
+namespace cw {
+
+CrossPlan cross_plan(const cw_handle* h, const std::vector<int>& pend) {
+  CrossPlan c;
+  std::vector<const RBox*> rb;
+  for (int set : pend)
+    for (const RBox& r : h->hs[set].r) {
+      bool dup = false;
+      for (const RBox* y : rb)
+        dup |= y->me == r.me && y->t == r.t && y->fid == r.fid && y->send.i0 == r.send.i0 && y->send.j0 == r.send.j0;
+      if (!dup) rb.push_back(&r);
+    }
+  std::stable_sort(rb.begin(), rb.end(), [](const RBox* a, const RBox* b) {
+    return a->src_rank != b->src_rank ? a->src_rank < b->src_rank : a->dst_rank < b->dst_rank;
+  });
+  size_t so = 0, ro = 0;
+  for (size_t g0 = 0; g0 < rb.size();) {
+    size_t g1 = g0;
+    while (g1 < rb.size() && rb[g1]->src_rank == rb[g0]->src_rank && rb[g1]->dst_rank == rb[g0]->dst_rank) ++g1;
+    const size_t seg_s = so, seg_r = ro;
+    for (size_t n = g0; n < g1; ++n) {
+      const RBox& r = *rb[n];
+      const long long wi = r.send.i1 - r.send.i0, wij = wi * (r.send.j1 - r.send.j0);
+      if (r.has_send) {  // element (i, j, k) of the box at so + (i - i0) + (j - j0) wi + k wi wj of the send region
+        XchgBox b = r.send;
+        b.dst = nullptr;
+        b.dst_ind = nullptr;
+        b.dsj = int(wi);
+        b.dsk = int(wij);
+        b.doff = (long long)so - r.send.i0 - (long long)r.send.j0 * wi;
+        c.pk.push_back(b);
+        c.role.push_back(CrossPlan::Entry{0, r.dst_rank, &r, so});
+        so += size_t(r.send.ncell);
+      }
+      if (r.has_recv) {
+        XchgBox b = r.recv;
+        b.src = nullptr;
+        b.src_ind = nullptr;
+        b.ssj = int(wi);
+        b.ssk = int(wij);
+        b.soff = (long long)ro - r.recv.i0 - (long long)r.recv.j0 * wi;
+        c.unpk.push_back(b);
+        c.role.push_back(CrossPlan::Entry{1, r.src_rank, &r, ro});
+        ro += size_t(r.recv.ncell);
+      }
+    }
+    const RBox& r0 = *rb[g0];
+    if (h->loopback) c.copies.push_back(XCopy{seg_s, seg_r, so - seg_s});
+    else if (r0.src_rank == h->rank) c.sends.push_back(Xfer{r0.dst_rank, seg_s, so - seg_s});
+    else c.recvs.push_back(Xfer{r0.src_rank, seg_r, ro - seg_r});
+    g0 = g1;
+  }
+  c.send_n = so;
+  c.recv_n = ro;
+  return c;
+}
+
+void nccl_exchange(cw_handle* h, const HaloTable& t, char* sbuf, char* rbuf, size_t esz) {
+  const NcclApi& N = nccl_api();
+  if (!N.ok || !h->comm) throw std::runtime_error("decomposition over ranks: no NCCL communicator");
+  auto comm = static_cast<ncclComm_t>(h->comm);
+  nccl_check(N, N.GroupStart(), "ncclGroupStart");
+  ncclResult_t r = ncclSuccess;
+  for (const Xfer& x : t.sends)
+    if (r == ncclSuccess) r = N.Send(sbuf + x.off * esz, x.n * esz, ncclInt8, x.peer, comm, h->stream);
+  for (const Xfer& x : t.recvs)
+    if (r == ncclSuccess) r = N.Recv(rbuf + x.off * esz, x.n * esz, ncclInt8, x.peer, comm, h->stream);
+  const ncclResult_t e = N.GroupEnd();
+  nccl_check(N, r, "ncclSend / ncclRecv");
+  nccl_check(N, e, "ncclGroupEnd");
+}
+
+
+}  // namespace cw
 
 // cw_check_div_const: cw_div_const against __ddiv_rn for c = 60 and 12 on n operands each (the kinds of
 // tests/div_const_check.c); counts[0] = checked, counts[1] = mismatches
@@ -974,22 +1213,82 @@ int cw_decomp_patch(const cw_grid* g, int px, int py, int t, int* box) {
 
 int cw_decomp_create(const cw_grid* g, const cw_options* o, int px, int py, cw_handle** out) {
   return guarded(nullptr, [&] {
-    if (!g || !o || !out) throw std::runtime_error("null argument");
-    if (const char* why = decomp_unsupported(*g, px, py)) throw std::runtime_error(why);
-    auto h = std::make_unique<cw_handle>();
-    h->precision = o->precision;
-    h->decomp_px = px;
-    h->decomp_py = py;
-    for (int t = 0; t < px * py; ++t) {
-      Member M = make_member(*g, *o);
-      M.patched = true;
-      M.patch = patch_box(*g, px, py, t);
-      h->m.push_back(std::move(M));
-    }
+    if (!out) throw std::runtime_error("null argument");
+    auto h = decomp_handle(g, o, px, py, 0, 1, false);
     CW_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->own_stream = true;
     setup(h.get());
     *out = h.release();
+    return 0;
+  });
+}
+
+int cw_nccl_unique_id(unsigned char* id) {
+  return guarded(nullptr, [&] {
+    if (!id) throw std::runtime_error("null argument");
+    const NcclApi& N = nccl_api();
+    if (!N.ok) throw std::runtime_error(N.err);
+    ncclUniqueId u;
+    nccl_check(N, N.GetUniqueId(&u), "ncclGetUniqueId");
+    static_assert(sizeof(u) == 128, "ncclUniqueId is 128 bytes");
+    std::memcpy(id, &u, sizeof(u));
+    return 0;
+  });
+}
+
+int cw_decomp_create_ranked(const cw_grid* g, const cw_options* o, int px, int py, int rank, int nranks,
+                            const unsigned char* nccl_id, cw_handle** out) {
+  return guarded(nullptr, [&] {
+    if (!out) throw std::runtime_error("null argument");
+    auto h = decomp_handle(g, o, px, py, rank, nranks, nccl_id == nullptr);
+    CW_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+    if (nranks > 1 && !h->loopback) {  // every rank calls this with the same id: ncclCommInitRank waits for all
+      const NcclApi& N = nccl_api();
+      if (!N.ok) throw std::runtime_error(N.err);
+      ncclUniqueId u;
+      std::memcpy(&u, nccl_id, sizeof(u));
+      ncclComm_t comm = nullptr;
+      nccl_check(N, N.CommInitRank(&comm, nranks, u, rank), "ncclCommInitRank");
+      h->comm = comm;
+    }
+    try {
+      setup(h.get());
+    } catch (...) {
+      if (h->comm) nccl_api().CommDestroy(static_cast<ncclComm_t>(h->comm));
+      throw;
+    }
+    *out = h.release();
+    return 0;
+  });
+}
+
+static_assert(CW_FILL_MU1 == cw_handle::H_MU1 && CW_FILL_PREP0 == cw_handle::H_PREP0 && CW_FILL_FIN == cw_handle::H_FIN &&
+                  CW_FILL_Q2 == cw_handle::H_Q2 && CW_FILL_WS1 == cw_handle::H_WS1 && CW_FILL_XK == cw_handle::H_XK &&
+                  CW_FILL_XK + 1 == cw_handle::H_N,
+              "the fill point indices of cw_decomp_plan are the handle's");
+int cw_decomp_plan(const cw_grid* g, const cw_options* o, int px, int py, int rank, int nranks, int nsets,
+                   const int* sets, long long* out, int cap, int* n) {
+  return guarded(nullptr, [&] {
+    if (!n || nsets < 1 || !sets || (cap > 0 && !out)) throw std::runtime_error("bad arguments");
+    auto h = decomp_handle(g, o, px, py, rank, nranks, false);
+    for (Member& M : h->m) plan_member(M);
+    DevTables<double> T;  // no device tables: the items carry layouts only
+    build_halosets_t<double>(h.get(), T, false);
+    std::vector<int> pend;
+    for (int k = 0; k < nsets; ++k) {
+      if (sets[k] < 0 || sets[k] >= cw_handle::H_N) throw std::runtime_error("no such fill point");
+      pend.push_back(sets[k]);
+    }
+    const CrossPlan c = cross_plan(h.get(), pend);
+    *n = int(c.role.size());
+    for (size_t k = 0; k < c.role.size() && int(k) < cap; ++k) {
+      const CrossPlan::Entry& e = c.role[k];
+      const RBox& r = *e.box;
+      const long long v[11] = {e.role, e.peer, r.me, r.t, r.fid, r.send.i0, r.send.i1, r.send.j0, r.send.j1,
+                               r.send.nk, (long long)e.off};
+      std::copy(v, v + 11, out + 11 * k);
+    }
     return 0;
   });
 }
@@ -1119,8 +1418,9 @@ int cw_footprint(const cw_grid* g, const cw_options* o, size_t* bytes) {
 int cw_destroy(cw_handle* h) {
   if (!h) return 0;
   cudaStreamSynchronize(h->stream);
-  invalidate_graph(h);
+  invalidate_graph(h);  // the captured step holds the NCCL operations: released before the communicator
   free_tables(h);
+  if (h->comm) nccl_api().CommDestroy(static_cast<ncclComm_t>(h->comm));
   cudaFree(h->staging);
   cudaFree(h->diag);
   cudaFree(h->diag_part);

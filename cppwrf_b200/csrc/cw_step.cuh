@@ -66,6 +66,46 @@ struct Launcher {
       }
     return f;
   }
+  // a decomposed domain over ranks: the pending fill points' boxes between ranks (cross_plan): the packing boxes
+  // into t.pk, the unpacking ones appended to x, the transfers into t
+  void cross_ranks(HaloTable& t, std::vector<XchgBox>& x) {
+    CrossPlan c = cross_plan(h, pend);
+    const size_t esz = h->m.empty() ? 8 : size_t(h->m[0].esz);
+    if (c.send_n > h->xsend_cap || c.recv_n > h->xrecv_cap) throw std::runtime_error("decomposition: exchange buffer too small");
+    for (XchgBox& b : c.pk) b.dst = h->xbuf;
+    for (XchgBox& b : c.unpk) {
+      b.src = h->xbuf + h->xsend_cap * esz;
+      x.push_back(b);
+    }
+    t.sends = std::move(c.sends);
+    t.recvs = std::move(c.recvs);
+    t.copies = std::move(c.copies);
+    if (c.pk.empty()) return;
+    std::vector<unsigned> st(c.pk.size() + 1);
+    long long tot = 0;
+    for (size_t n = 0; n < c.pk.size(); ++n) {
+      st[n] = unsigned(tot);
+      tot += c.pk[n].ncell;
+    }
+    if (tot >= (1ll << 31)) throw std::runtime_error("an exchange of more than 2^31 points");
+    st[c.pk.size()] = unsigned(tot);
+    t.npk = int(c.pk.size());
+    t.pktotal = unsigned(tot);
+    CW_CUDA(cudaMalloc(&t.pk, c.pk.size() * sizeof(XchgBox)));
+    CW_CUDA(cudaMalloc(&t.pkstart, st.size() * sizeof(unsigned)));
+    CW_CUDA(cudaMemcpy(t.pk, c.pk.data(), c.pk.size() * sizeof(XchgBox), cudaMemcpyHostToDevice));
+    CW_CUDA(cudaMemcpy(t.pkstart, st.data(), st.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+  }
+  // the transfers of a fill point between ranks: NCCL point-to-point in one group on the handle's stream (captured
+  // into the step's graph like the kernels), or device copies in the loopback form
+  void transfer(const HaloTable& t) {
+    const size_t esz = h->m.empty() ? 8 : size_t(h->m[0].esz);
+    char* sbuf = h->xbuf;
+    char* rbuf = h->xbuf + h->xsend_cap * esz;
+    for (const XCopy& c : t.copies)
+      if (c.n) CW_CUDA(cudaMemcpyAsync(rbuf + c.roff * esz, sbuf + c.soff * esz, c.n * esz, cudaMemcpyDeviceToDevice, h->stream));
+    if (!t.sends.empty() || !t.recvs.empty()) nccl_exchange(h, t, sbuf, rbuf, esz);
+  }
   // a batch: the pending fill points as one device table (made on first use, kept with the handle's tables)
   const HaloTable& halo_table() {
     auto it = h->halo_tabs.find(pend);
@@ -99,6 +139,7 @@ struct Launcher {
                  y.j0 == b.j0;
         if (!dup) x.push_back(b);
       }
+    cross_ranks(t, x);
     if (!x.empty()) {
       std::vector<unsigned> xs(x.size() + 1);
       long long xt = 0;
@@ -119,8 +160,14 @@ struct Launcher {
   }
   void flush() {
     if (pend.empty()) return;
-    if (h->m.size() > 1) {
+    if (h->m.size() > 1 || h->decomp_px > 0) {
       const HaloTable& t = halo_table();
+      if (t.pktotal > 0 && !plan) {  // a decomposed domain over ranks: the boxes other ranks receive, packed
+        begin("k_exchange");
+        k_exchange<<<(t.pktotal + 255u) / 256u, 256, 0, h->stream>>>(t.pk, t.pkstart, t.npk);
+        check();
+      }
+      if (!plan) transfer(t);
       if (t.xtotal > 0 && !plan) {  // a decomposed domain: the exchange first, then the boundary fill
         begin("k_exchange");
         k_exchange<<<(t.xtotal + 255u) / 256u, 256, 0, h->stream>>>(t.x, t.xstart, t.nx);

@@ -52,6 +52,9 @@ struct Dom {
   // or a patch of a domain decomposed over several members (cw_decomp_create), whose fields are allocated for the
   // patch and a halo of 3 and indexed with the domain's indices; the edge patches also own the faces nx / ny
   int pi0, pi1, pj0, pj1;
+  // the allocation window of its fields: i in [wi0, wi1m) (mass and w points; u: [wi0, wi1u)), j in [wj0, wj1m)
+  // (v: [wj0, wj1v))
+  int wi0, wi1m, wi1u, wj0, wj1m, wj1v;
   int bc_x, bc_y, spec_x, spec_y;  // spec_*: specified or open in that direction (degraded orders)
   int sx, sy;                      // specified in that direction (spec zone, upstream boundary velocity)
   int open_x, open_y;              // open (radiation) in that direction; open_y is 0 in 2-D
@@ -249,14 +252,16 @@ struct HaloField {
 };
 // A decomposed domain's exchange (the halo exchange of core/halo.cpp:120-129 / tiles.hpp:6-12): the rectangle
 // i0 <= i < i1, j0 <= j < j1 (all nk levels) of a field that a patch holds in its halo and another patch owns,
-// copied from the owner's allocation into the patch's at the same domain indices. src / dst: element (0, 0, 0);
-// src_ind / dst_ind (scalars whose buffers swap): a device V3 whose .p is read at run time instead.
+// copied from the owner's allocation into the patch's at the same domain indices. src / dst: element (0, 0, 0),
+// or the start of a packed buffer with soff / doff the index of element (0, 0, 0) in it; src_ind / dst_ind (scalars
+// whose buffers swap): a device V3 whose .p is read at run time instead.
 struct XchgBox {
   const void* src;
   const void* src_ind;
   void* dst;
   const void* dst_ind;
   int ssj, ssk, dsj, dsk;
+  long long soff, doff;  // element offsets added to the source / destination index (a packed buffer's box)
   int i0, i1, j0, j1, nk;
   int is_float;
   long long ncell;

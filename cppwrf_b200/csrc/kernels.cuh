@@ -213,7 +213,8 @@ static __global__ void k_halo_tab(const HaloField* __restrict__ fs, const unsign
   else halo_cell<double>(f, c, pass);
 }
 
-// a decomposed domain's exchange: one thread per received point of every box of the table
+// a decomposed domain's exchange: one thread per received point of every box of the table (a box between two patches
+// of this process, or between a patch and the packed buffer of an exchange with another rank)
 static __global__ void k_exchange(const XchgBox* __restrict__ bs, const unsigned* __restrict__ start, int nb) {
   const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= __ldg(start + nb)) return;
@@ -227,7 +228,8 @@ static __global__ void k_exchange(const XchgBox* __restrict__ bs, const unsigned
   const unsigned c = t - __ldg(start + lo);
   const unsigned wi = unsigned(b.i1 - b.i0), wj = unsigned(b.j1 - b.j0);
   const int i = b.i0 + int(c % wi), j = b.j0 + int((c / wi) % wj), k = int(c / (wi * wj));
-  const long long s = i + (long long)j * b.ssj + (long long)k * b.ssk, d = i + (long long)j * b.dsj + (long long)k * b.dsk;
+  const long long s = b.soff + i + (long long)j * b.ssj + (long long)k * b.ssk;
+  const long long d = b.doff + i + (long long)j * b.dsj + (long long)k * b.dsk;
   if (b.is_float) {
     const float* src = b.src_ind ? static_cast<const V3<float>*>(b.src_ind)->p : static_cast<const float*>(b.src);
     float* dst = b.dst_ind ? static_cast<const V3<float>*>(b.dst_ind)->p : static_cast<float*>(b.dst);

@@ -304,6 +304,37 @@ int cw_decomp_upload(cw_handle* h, int field, int n, const double* host, size_t 
 int cw_decomp_download(cw_handle* h, int field, int n, double* host, size_t count);
 /* cw_upload_case into every patch (vertical arrays, each patch's window of the fields, the boundary slabs). */
 int cw_decomp_upload_case(cw_handle* h, cw_case* c);
+
+/* ---- the patches of one domain over several processes, one GPU each (tiles_mpi.cpp:35-64: the ranks of
+ * docs/MPI.md §3 with NCCL in place of MPI) ----
+ * Patch t belongs to rank t % nranks (one patch per rank when nranks = px py, the reference's layout). Each rank's
+ * handle holds its patches; at every fill point each rank packs the points that other ranks' patches receive into
+ * one send buffer on its GPU (one segment per receiving rank), the segments cross as NCCL point-to-point transfers
+ * grouped on the handle's stream (captured into the step's CUDA graph with the kernels), and each rank unpacks its
+ * receive buffer into its patches' halos, then exchanges between its own patches and fills the domain's halo, as
+ * cw_decomp_create does on one device. The boxes of a pair of ranks are listed in one order by both (receiving
+ * patch, owning patch, field) and no device reads another's memory. Every rank makes the same calls in the same
+ * order: cw_decomp_create_ranked (collective: NCCL's communicator), cw_step, cw_destroy.
+ * cw_decomp_upload / _upload_case take the whole-domain arrays on every rank (each keeps its patches' windows);
+ * cw_decomp_download gives the points this rank's patches own (the others 0: the ranks' arrays sum to the domain).
+ * nccl_id: 128 bytes from cw_nccl_unique_id on one rank, passed to all (e.g. by torch.distributed). nccl_id = NULL
+ * is the loopback form: this process holds every patch and the exchanges between patches of different ranks go
+ * through the packed buffers with a device copy in place of the transfer (the whole path on one GPU but NCCL). */
+int cw_nccl_unique_id(unsigned char id[128]);
+int cw_decomp_create_ranked(const cw_grid* g, const cw_options* o, int px, int py, int rank, int nranks,
+                            const unsigned char* nccl_id, cw_handle** out);
+/* The fill point indices of cw_decomp_plan (the halo refreshes of one RK3 step, src/dyn/rk3.cpp:86-170). */
+enum { CW_FILL_MU1, CW_FILL_PREP0, CW_FILL_PREP1, CW_FILL_SS0, CW_FILL_UV, CW_FILL_AC, CW_FILL_POST, CW_FILL_FIN,
+       CW_FILL_Q1PD, CW_FILL_SCPD, CW_FILL_Q2, CW_FILL_END_P, CW_FILL_WS0, CW_FILL_WS1, CW_FILL_MP, CW_FILL_MP_P,
+       CW_FILL_XK };
+/* The boxes that cross between rank `rank` and the others at the fill point made of the nsets fill points `sets`,
+ * as that rank packs and unpacks them (no device): n boxes, 11 values each into out (up to cap boxes): role (0: this
+ * rank packs it, 1: unpacks it), peer rank, receiving patch, owning patch, field (its id; 1000 + a work field,
+ * 2000 + n: q_2 of species n, 3000 + n: q_1, 4000 + n: the PD scale), i0, i1, j0, j1, levels, element offset in the
+ * send (role 0) or receive (role 1) region. The segment of a peer is its boxes' points in list order, each box's
+ * points i fastest, then j, then k. For a transport of the caller's own, and for tests. */
+int cw_decomp_plan(const cw_grid* g, const cw_options* o, int px, int py, int rank, int nranks, int nsets,
+                   const int* sets, long long* out, int cap, int* n);
 /* cw_download without any allocation (no counterpart in the reference; CPPWRF's FieldT::download always
  * stages through host memory).
  *

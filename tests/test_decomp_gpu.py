@@ -44,9 +44,9 @@ def compare(dec, dom, case):
     return bad
 
 
-def run_both(case, px, py, nsteps):
+def run_both(case, px, py, nsteps, **ranks):
     dom = Domain(case.g, case.o).upload_case(case)
-    dec = Decomp(case.g, case.o, px, py).upload_case(case)
+    dec = Decomp(case.g, case.o, px, py, **ranks).upload_case(case)
     dom.step(nsteps)
     dec.step(nsteps)
     dom.sync()
@@ -96,3 +96,30 @@ def test_benchmark_workload_on_six_patches_mixed_and_fp64():
         dec, dom = run_both(case, 3, 2, 2)
         bad = compare(dec, dom, case)
         assert not bad, "\n".join(bad)
+
+
+@pytest.mark.parametrize("px,py,nranks", [(2, 1, 2), (2, 2, 4), (3, 2, 2), (3, 2, 6)])
+def test_patches_over_ranks_loopback_equal_whole_domain(px, py, nranks):
+    """cw_decomp_create_ranked in its loopback form: this process holds every patch, and the exchanges between patches
+    of different ranks (t % nranks) go through the packing kernel, the packed send and receive buffers (a device copy
+    in place of the NCCL transfer) and the unpacking kernel -- the ranks' path on one GPU but NCCL itself."""
+    case = lam_case(nx=40, ny=34, nz=14, seed=71)
+    dec, dom = run_both(case, px, py, 4, nranks=nranks, loopback=True)
+    bad = compare(dec, dom, case)
+    assert not bad, "\n".join(bad)
+
+
+def test_benchmark_workload_over_three_ranks_loopback_mixed_and_fp64():
+    import bench
+    for prec in (capi.FP64, capi.MIXED):
+        case = bench.make_case(capi, prec)
+        dec, dom = run_both(case, 3, 2, 2, nranks=3, loopback=True)
+        bad = compare(dec, dom, case)
+        assert not bad, "\n".join(bad)
+
+
+def test_every_option_over_ranks_loopback():
+    case = cases.every_option_case()
+    dec, dom = run_both(case, 2, 2, 3, nranks=2, loopback=True)
+    bad = compare(dec, dom, case)
+    assert not bad, "\n".join(bad)
