@@ -168,8 +168,6 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.nx = g.nx; D.ny = g.ny; D.nz = g.nz; D.nyv = nys(g, 'V'); D.two_d = two_d(g); D.do_y = !two_d(g);
   const Box pb = M.patched ? M.patch : Box{0, g.nx, 0, g.ny};
   D.pi0 = pb.i0; D.pi1 = pb.i1; D.pj0 = pb.j0; D.pj1 = pb.j1;
-  D.wi0 = M.L[CW_T_2].wi0; D.wi1m = M.L[CW_T_2].wi1; D.wi1u = M.L[CW_U_2].wi1;
-  D.wj0 = M.L[CW_T_2].wj0; D.wj1m = M.L[CW_T_2].wj1; D.wj1v = M.L[CW_V_2].wj1;
   D.bc_x = g.bc_x; D.bc_y = g.bc_y;
   D.spec_x = flat_x(g); D.spec_y = flat_y(g) && !two_d(g);
   D.open_x = g.bc_x == CW_BC_OPEN; D.open_y = g.bc_y == CW_BC_OPEN && !two_d(g);

@@ -52,9 +52,6 @@ struct Dom {
   // or a patch of a domain decomposed over several members (cw_decomp_create), whose fields are allocated for the
   // patch and a halo of 3 and indexed with the domain's indices; the edge patches also own the faces nx / ny
   int pi0, pi1, pj0, pj1;
-  // the allocation window of its fields: i in [wi0, wi1m) (mass and w points; u: [wi0, wi1u)), j in [wj0, wj1m)
-  // (v: [wj0, wj1v))
-  int wi0, wi1m, wi1u, wj0, wj1m, wj1v;
   int bc_x, bc_y, spec_x, spec_y;  // spec_*: specified or open in that direction (degraded orders)
   int sx, sy;                      // specified in that direction (spec zone, upstream boundary velocity)
   int open_x, open_y;              // open (radiation) in that direction; open_y is 0 in 2-D
