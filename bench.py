@@ -12,7 +12,7 @@ synthetic (cw_gen_lam, seeded). The step's working set (~110 fields of 5.4 MB) i
 
 One JSON line on rank 0: value = all ranks' grid points x steps / max over ranks of the device time of the
 K timed steps (CUDA events on the handle's stream), e2e = the same through the C ABI with the prognostic
-state copied from / to pinned host memory every step, roofline of the dominant kernel (per-kernel CUDA
+state (every point of each field's window: domain and halo) copied from / to pinned host memory every step, roofline of the dominant kernel (per-kernel CUDA
 events, algorithmic bytes below), and the reference CPU build timed on this host.
 """
 import argparse
@@ -565,7 +565,13 @@ def main():
         t = torch.empty(L.total, dtype=torch.float64).pin_memory()
         t.copy_(torch.from_numpy(dom.field("Q_2", n)))
         qhost.append(t)
-    ebytes = sum(t.numel() * 8 for t in host.values()) + sum(t.numel() * 8 for t in qhost)
+    # the window points of each field (domain and halo; the allocations' row padding is not copied)
+    def window_points(L):
+        if L.uniform:
+            return L.total
+        return (L.wi1 - L.wi0) * (L.wj1 - L.wj0) * (L.nz if L.rank == 3 else 1)
+    ebytes = sum(window_points(dom.layout(n)) * 8 for n in host) + \
+        sum(window_points(dom.layout("Q_2", q)) * 8 for q in range(len(qhost)))
     dp = C.POINTER(C.c_double)
     n_e2e = max(3, min(args.steps, 20))
     barrier()
@@ -574,7 +580,7 @@ def main():
     g0 = torch.cuda.Event(enable_timing=True)
     g1 = torch.cuda.Event(enable_timing=True)
     g0.record(stream)
-    # every field of the state in one cw_upload_fields / cw_download_fields call (one synchronisation per step)
+    # every field of the state in one cw_upload_windows / cw_download_windows call (one synchronisation per step)
     tensors = list(host.values()) + qhost
     nf = len(tensors)
     fids = (C.c_int * nf)(*([capi.F[name] for name in host] + [capi.F["Q_2"]] * len(qhost)))
@@ -582,9 +588,9 @@ def main():
     fptr = (dp * nf)(*[C.cast(t.data_ptr(), dp) for t in tensors])
     fcnt = (C.c_size_t * nf)(*[t.numel() for t in tensors])
     for _ in range(n_e2e):
-        lib.cw_upload_fields(dom.h, 0, nf, fids, fns, fptr, fcnt)
+        lib.cw_upload_windows(dom.h, 0, nf, fids, fns, fptr, fcnt)
         lib.cw_step(dom.h, 1)
-        lib.cw_download_fields(dom.h, 0, nf, fids, fns, fptr, fcnt)
+        lib.cw_download_windows(dom.h, 0, nf, fids, fns, fptr, fcnt)
     g1.record(stream)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0

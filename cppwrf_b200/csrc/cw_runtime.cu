@@ -998,6 +998,91 @@ void nccl_check(const NcclApi& N, ncclResult_t r, const char* what) {
   if (r != ncclSuccess) throw std::runtime_error(std::string(what) + ": " + N.GetErrorString(r));
 }
 
+// ---- several fields in one call (cw_upload_fields / cw_upload_windows and the downloads)
+// The rows of a field's window: `rows` rows of `width` points at stride `pitch`, the first at element `first` of the
+// allocation (the levels' windows follow each other at the same stride: sk = sj (wj1 - wj0), or sj = 0 in 2-D with
+// sk the row stride). Otherwise (horizontally uniform storage) the whole allocation as one row.
+struct WinRows {
+  size_t first, width, pitch, rows;
+};
+WinRows window_rows(const cw_layout& L) {
+  const size_t w = size_t(L.wi1 - L.wi0), nj = size_t(L.wj1 - L.wj0), nk = size_t(L.rank == 3 ? L.nz : 1);
+  if (!L.uniform && L.sj > 0 && (L.rank != 3 || size_t(L.sk) == size_t(L.sj) * nj))
+    return WinRows{size_t(L.offset + L.wi0 + int64_t(L.wj0) * L.sj), w, size_t(L.sj), nj * nk};
+  if (!L.uniform && L.sj == 0 && L.rank == 3 && nj == 1 && L.sk > 0)
+    return WinRows{size_t(L.offset + L.wi0 + int64_t(L.wj0) * L.sj), w, size_t(L.sk), nk};
+  return WinRows{0, size_t(L.total), size_t(L.total), 1};
+}
+// one field's copy: the whole allocation, or its window's rows (window)
+void copy_rows(cw_handle* h, char* dst, const char* src, const cw_layout& L, bool window, cudaMemcpyKind kind) {
+  if (!window) {
+    CW_CUDA(cudaMemcpyAsync(dst, src, size_t(L.total) * 8, kind, h->stream));
+    return;
+  }
+  const WinRows r = window_rows(L);
+  CW_CUDA(cudaMemcpy2DAsync(dst + r.first * 8, r.pitch * 8, src + r.first * 8, r.pitch * 8, r.width * 8, r.rows, kind,
+                            h->stream));
+}
+std::vector<Loc> locate_all(cw_handle* h, int mi, int nf, const int* fields, const int* ns, const void* const* host,
+                            const size_t* counts, size_t& staged) {
+  if (!h || nf < 0 || (nf > 0 && (!fields || !ns || !host || !counts))) throw std::runtime_error("null argument");
+  std::vector<Loc> locs;
+  staged = 0;
+  for (int f = 0; f < nf; ++f) {
+    if (!host[f]) throw std::runtime_error("null host buffer");
+    locs.push_back(locate(h, mi, fields[f], ns[f]));
+    if (counts[f] != size_t(locs.back().L.total)) throw std::runtime_error("count != layout.total");
+    if (counts[f] >= (size_t(1) << 32)) throw std::runtime_error("field too large");
+    if (locs.back().esz != 8) staged += counts[f];
+  }
+  return locs;
+}
+// FP64 fields copy directly; FP32 (mixed) fields go through one staging region per field (the staging buffer sized
+// for all of them first, so that no reallocation happens between the copies; with window copies it is zeroed first,
+// so that the narrowed row padding holds zeros)
+void upload_fields(cw_handle* h, int mi, int nf, const int* fields, const int* ns, const double* const* host,
+                   const size_t* counts, bool window) {
+  size_t staged = 0;
+  const std::vector<Loc> locs =
+      locate_all(h, mi, nf, fields, ns, reinterpret_cast<const void* const*>(host), counts, staged);
+  double* st = staged ? staging(h, staged) : nullptr;
+  if (st && window) CW_CUDA(cudaMemsetAsync(st, 0, staged * sizeof(double), h->stream));
+  for (int f = 0; f < nf; ++f) {
+    const Loc& l = locs[size_t(f)];
+    if (l.esz == 8) {
+      copy_rows(h, l.base, reinterpret_cast<const char*>(host[f]), l.L, window, cudaMemcpyHostToDevice);
+    } else {
+      copy_rows(h, reinterpret_cast<char*>(st), reinterpret_cast<const char*>(host[f]), l.L, window,
+                cudaMemcpyHostToDevice);
+      const unsigned n = unsigned(counts[f]), blocks = std::min(4096u, (n + 255u) / 256u);
+      k_narrow<<<blocks, 256, 0, h->stream>>>(st, reinterpret_cast<float*>(l.base), n);
+      CW_CUDA(cudaGetLastError());
+      st += counts[f];
+    }
+  }
+}
+void download_fields(cw_handle* h, int mi, int nf, const int* fields, const int* ns, double* const* host,
+                     const size_t* counts, bool window) {
+  size_t staged = 0;
+  const std::vector<Loc> locs =
+      locate_all(h, mi, nf, fields, ns, reinterpret_cast<const void* const*>(host), counts, staged);
+  double* st = staged ? staging(h, staged) : nullptr;
+  for (int f = 0; f < nf; ++f) {
+    const Loc& l = locs[size_t(f)];
+    if (l.esz == 8) {
+      copy_rows(h, reinterpret_cast<char*>(host[f]), l.base, l.L, window, cudaMemcpyDeviceToHost);
+    } else {
+      const unsigned n = unsigned(counts[f]), blocks = std::min(4096u, (n + 255u) / 256u);
+      k_widen<<<blocks, 256, 0, h->stream>>>(reinterpret_cast<const float*>(l.base), st, n);
+      CW_CUDA(cudaGetLastError());
+      copy_rows(h, reinterpret_cast<char*>(host[f]), reinterpret_cast<const char*>(st), l.L, window,
+                cudaMemcpyDeviceToHost);
+      st += counts[f];
+    }
+  }
+  CW_CUDA(cudaStreamSynchronize(h->stream));
+}
+
 }  // namespace
 
 // the step's exchange between ranks (declared in cw_handle.cuh, called by the launcher of either form)
@@ -1502,59 +1587,28 @@ int cw_download(cw_handle* h, int field, int n, double* host, size_t count) {
 int cw_upload_fields(cw_handle* h, int mi, int nf, const int* fields, const int* ns, const double* const* host,
                      const size_t* counts) {
   return guarded(h, [&] {
-    if (!h || nf < 0 || (nf > 0 && (!fields || !ns || !host || !counts))) throw std::runtime_error("null argument");
-    std::vector<Loc> locs;
-    size_t staged = 0;
-    for (int f = 0; f < nf; ++f) {
-      if (!host[f]) throw std::runtime_error("null host buffer");
-      locs.push_back(locate(h, mi, fields[f], ns[f]));
-      if (counts[f] != size_t(locs.back().L.total)) throw std::runtime_error("count != layout.total");
-      if (counts[f] >= (size_t(1) << 32)) throw std::runtime_error("field too large");
-      if (locs.back().esz != 8) staged += counts[f];
-    }
-    double* st = staged ? staging(h, staged) : nullptr;
-    for (int f = 0; f < nf; ++f) {
-      const Loc& l = locs[size_t(f)];
-      if (l.esz == 8) {
-        CW_CUDA(cudaMemcpyAsync(l.base, host[f], counts[f] * 8, cudaMemcpyHostToDevice, h->stream));
-      } else {
-        CW_CUDA(cudaMemcpyAsync(st, host[f], counts[f] * 8, cudaMemcpyHostToDevice, h->stream));
-        const unsigned n = unsigned(counts[f]), blocks = std::min(4096u, (n + 255u) / 256u);
-        k_narrow<<<blocks, 256, 0, h->stream>>>(st, reinterpret_cast<float*>(l.base), n);
-        CW_CUDA(cudaGetLastError());
-        st += counts[f];
-      }
-    }
+    upload_fields(h, mi, nf, fields, ns, host, counts, false);
     return 0;
   });
 }
 int cw_download_fields(cw_handle* h, int mi, int nf, const int* fields, const int* ns, double* const* host,
                        const size_t* counts) {
   return guarded(h, [&] {
-    if (!h || nf < 0 || (nf > 0 && (!fields || !ns || !host || !counts))) throw std::runtime_error("null argument");
-    std::vector<Loc> locs;
-    size_t staged = 0;
-    for (int f = 0; f < nf; ++f) {
-      if (!host[f]) throw std::runtime_error("null host buffer");
-      locs.push_back(locate(h, mi, fields[f], ns[f]));
-      if (counts[f] != size_t(locs.back().L.total)) throw std::runtime_error("count != layout.total");
-      if (counts[f] >= (size_t(1) << 32)) throw std::runtime_error("field too large");
-      if (locs.back().esz != 8) staged += counts[f];
-    }
-    double* st = staged ? staging(h, staged) : nullptr;
-    for (int f = 0; f < nf; ++f) {
-      const Loc& l = locs[size_t(f)];
-      if (l.esz == 8) {
-        CW_CUDA(cudaMemcpyAsync(host[f], l.base, counts[f] * 8, cudaMemcpyDeviceToHost, h->stream));
-      } else {
-        const unsigned n = unsigned(counts[f]), blocks = std::min(4096u, (n + 255u) / 256u);
-        k_widen<<<blocks, 256, 0, h->stream>>>(reinterpret_cast<const float*>(l.base), st, n);
-        CW_CUDA(cudaGetLastError());
-        CW_CUDA(cudaMemcpyAsync(host[f], st, counts[f] * 8, cudaMemcpyDeviceToHost, h->stream));
-        st += counts[f];
-      }
-    }
-    CW_CUDA(cudaStreamSynchronize(h->stream));
+    download_fields(h, mi, nf, fields, ns, host, counts, false);
+    return 0;
+  });
+}
+int cw_upload_windows(cw_handle* h, int mi, int nf, const int* fields, const int* ns, const double* const* host,
+                      const size_t* counts) {
+  return guarded(h, [&] {
+    upload_fields(h, mi, nf, fields, ns, host, counts, true);
+    return 0;
+  });
+}
+int cw_download_windows(cw_handle* h, int mi, int nf, const int* fields, const int* ns, double* const* host,
+                        const size_t* counts) {
+  return guarded(h, [&] {
+    download_fields(h, mi, nf, fields, ns, host, counts, true);
     return 0;
   });
 }

@@ -143,6 +143,14 @@ int cw_upload_fields(cw_handle* h, int member, int nf, const int* fields, const 
                      const size_t* counts);
 int cw_download_fields(cw_handle* h, int member, int nf, const int* fields, const int* ns, double* const* host,
                        const size_t* counts);
+/* The same for the points of each field's window only (its domain and halo, the points a step reads and writes;
+ * FieldT's allocation also holds row padding, which no computation reads): one strided copy per field, about a
+ * fifth fewer bytes than the whole allocations. The host arrays keep the layout; their padding is neither read nor
+ * written (the device's padding holds zeros after an upload in the mixed form, and is left as it was in FP64). */
+int cw_upload_windows(cw_handle* h, int member, int nf, const int* fields, const int* ns, const double* const* host,
+                      const size_t* counts);
+int cw_download_windows(cw_handle* h, int member, int nf, const int* fields, const int* ns, double* const* host,
+                        const size_t* counts);
 /* The field's layout (FieldT::layout, src/core/field.hpp:107). */
 int cw_field_layout(cw_handle* h, int field, int n, cw_layout* out);
 /* The device address of element (0,0,0) of a field (FieldT::data, src/core/field.hpp:108). */
