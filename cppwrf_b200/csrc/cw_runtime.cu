@@ -1346,9 +1346,10 @@ int cw_decomp_create_ranked(const cw_grid* g, const cw_options* o, int px, int p
   });
 }
 
-static_assert(CW_FILL_MU1 == cw_handle::H_MU1 && CW_FILL_PREP0 == cw_handle::H_PREP0 && CW_FILL_FIN == cw_handle::H_FIN &&
-                  CW_FILL_Q2 == cw_handle::H_Q2 && CW_FILL_WS1 == cw_handle::H_WS1 && CW_FILL_XK == cw_handle::H_XK &&
-                  CW_FILL_XK + 1 == cw_handle::H_N,
+static_assert(int(CW_FILL_MU1) == int(cw_handle::H_MU1) && int(CW_FILL_PREP0) == int(cw_handle::H_PREP0) &&
+                  int(CW_FILL_FIN) == int(cw_handle::H_FIN) && int(CW_FILL_Q2) == int(cw_handle::H_Q2) &&
+                  int(CW_FILL_WS1) == int(cw_handle::H_WS1) && int(CW_FILL_XK) == int(cw_handle::H_XK) &&
+                  int(CW_FILL_XK) + 1 == int(cw_handle::H_N),
               "the fill point indices of cw_decomp_plan are the handle's");
 int cw_decomp_plan(const cw_grid* g, const cw_options* o, int px, int py, int rank, int nranks, int nsets,
                    const int* sets, long long* out, int cap, int* n) {
