@@ -24,7 +24,15 @@ SETS = {"prep0+q2": [capi.FILL_PREP0, capi.FILL_Q2], "prep1": [capi.FILL_PREP1],
         "post": [capi.FILL_POST], "fin": [capi.FILL_FIN], "ws": [capi.FILL_WS0, capi.FILL_WS1]}
 
 
-def setup(nx=30, ny=24, nz=4):
+def setup(nx=30, ny=24, nz=4, kind="lam"):
+    if kind == "2d":  # an x-z slice with symmetric walls (no y exchange; rows of stride 0)
+        g = capi.grid(nx, 1, nz, 1000.0, 5.0, 6000.0, bc_x=capi.SYMMETRIC, bc_y=capi.PERIODIC)
+        o = capi.default_options(None, n_moist=1, n_scalars=1, time_step_sound=4)
+        return g, o
+    if kind == "open":
+        g = capi.grid(nx, ny, nz, 15000.0, 90.0, 0.0, dy=15000.0, p_top=5000.0, bc_x=capi.OPEN, bc_y=capi.SYMMETRIC)
+        o = capi.default_options(None, flat=0, n_moist=2, n_scalars=2, lbc=0, time_step_sound=4)
+        return g, o
     g = capi.grid(nx, ny, nz, 15000.0, 90.0, 0.0, dy=15000.0, p_top=5000.0, bc_x=capi.SPECIFIED, bc_y=capi.SPECIFIED)
     o = capi.default_options(None, flat=0, n_moist=2, n_scalars=2, lbc=1, time_step_sound=4)
     return g, o
@@ -58,9 +66,9 @@ def value(fid, i, j, k):
     return fid * 1.0e6 + k * 1.0e4 + (j + 5) * 100.0 + (i + 5)
 
 
-def exchange(rank, world, px, py, sets, send, recv):
+def exchange(rank, world, px, py, sets, send, recv, kind="lam"):
     """The fill point on this rank; send(peer, array) / recv(peer, n) the transport. Returns the points left wrong."""
-    g, o = setup()
+    g, o = setup(kind=kind)
     plan = decomp_plan(g, o, px, py, rank, world, sets)
     fids = sorted({int(f) for r in range(world) for f in decomp_plan(g, o, px, py, r, world, sets)[:, 4]})
     assert fids, "no box crosses between ranks"
@@ -143,7 +151,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _rank(rank, world, port, px, py, q):
+def _rank(rank, world, port, px, py, q, kind="lam"):
     import torch
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
@@ -159,18 +167,19 @@ def _rank(rank, world, port, px, py, q):
 
     out = {}
     for name, sets in SETS.items():
-        out[name] = exchange(rank, world, px, py, sets, send, recv)
+        out[name] = exchange(rank, world, px, py, sets, send, recv, kind)
     dist.barrier()
     dist.destroy_process_group()
     q.put((rank, out))
 
 
-@pytest.mark.parametrize("px,py,world", [(2, 1, 2), (2, 2, 2), (3, 2, 3)])
-def test_exchange_between_ranks_fills_every_halo_point(px, py, world):
+@pytest.mark.parametrize("px,py,world,kind", [(2, 1, 2, "lam"), (2, 2, 2, "lam"), (3, 2, 3, "lam"), (3, 1, 3, "2d"),
+                                              (2, 2, 4, "open")])
+def test_exchange_between_ranks_fills_every_halo_point(px, py, world, kind):
     port = _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_rank, args=(r, world, port, px, py, q)) for r in range(world)]
+    procs = [ctx.Process(target=_rank, args=(r, world, port, px, py, q, kind)) for r in range(world)]
     for p in procs:
         p.start()
     res = dict(q.get(timeout=300) for _ in range(world))
