@@ -48,9 +48,9 @@ def test_batch_mixed_nz_and_ideal():
             assert np.array_equal(b.field(m, name).view(np.uint64), orc.array(name).view(np.uint64)), (m, name)
 
 
-def test_batch_more_members_than_a_pack():
-    """A batch larger than one kernel parameter pack (12 members) is launched pack by pack; every member
-    still matches the oracle bit for bit, the species count differing between members."""
+def test_batch_of_fourteen_members():
+    """Fourteen members of uneven sizes and species counts in one launch per kernel (the members' descriptors in
+    device memory): every member matches the oracle bit for bit."""
     cases = [lam_case(nx=14 + (m % 5), ny=12 + (m % 3), nz=10, seed=20 + m, n_moist=2 + (m % 2),
                       n_scalars=2 + (m % 2) + (m % 3)) for m in range(14)]
     b = Batch([c.g for c in cases], [c.o for c in cases])
