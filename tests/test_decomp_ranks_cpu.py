@@ -213,3 +213,11 @@ def test_both_ranks_of_a_pair_list_the_same_boxes():
 def test_one_rank_has_no_boxes_between_ranks():
     g, o = setup()
     assert len(decomp_plan(g, o, 3, 2, 0, 1, [capi.FILL_FIN])) == 0
+
+
+def test_plan_refuses_bad_ranks_and_fill_points():
+    g, o = setup()
+    for rank, world, sets in ((2, 2, [capi.FILL_FIN]), (0, 5, [capi.FILL_FIN]), (-1, 2, [capi.FILL_FIN]),
+                              (0, 2, [99])):
+        with pytest.raises(RuntimeError):
+            decomp_plan(g, o, 2, 2, rank, world, sets)
