@@ -908,23 +908,25 @@ __global__ void __launch_bounds__(PX, 10) k_tend(const __grid_constant__ Pack<R,
   auto wy = [&](int f) { return ry && dy && i < nx && k >= 1 && f >= 0 && f <= ny && f <= r.j1; };
   auto tx_ = [&](int f) { return rx && j < ny && k < nz && f >= 0 && f <= nx && f <= r.i1; };
   auto ty_ = [&](int f) { return ry && dy && i < nx && k < nz && f >= 0 && f <= ny && f <= r.j1; };
-  const bool xe = tx == SX - 1, ye = ty == SY - 1;  // the tile's last column / row also takes the next face
-  if (ux(i)) sfx[0][ty][tx] = tu_fx(D, i, j, k);
-  if (xe && ux(i + 1)) sfx[0][ty][SX] = tu_fx(D, i + 1, j, k);
-  if (uy(j)) sfy[0][ty][tx] = tu_fy(D, i, j, k);
-  if (ye && uy(j + 1)) sfy[0][SY][tx] = tu_fy(D, i, j + 1, k);
-  if (vx(i)) sfx[1][ty][tx] = tv_fx(D, i, j, k);
-  if (xe && vx(i + 1)) sfx[1][ty][SX] = tv_fx(D, i + 1, j, k);
-  if (vy(j)) sfy[1][ty][tx] = tv_fy(D, i, j, k);
-  if (ye && vy(j + 1)) sfy[1][SY][tx] = tv_fy(D, i, j + 1, k);
-  if (wx(i)) sfx[2][ty][tx] = tw_fx(D, i, j, k);
-  if (xe && wx(i + 1)) sfx[2][ty][SX] = tw_fx(D, i + 1, j, k);
-  if (wy(j)) sfy[2][ty][tx] = tw_fy(D, i, j, k);
-  if (ye && wy(j + 1)) sfy[2][SY][tx] = tw_fy(D, i, j + 1, k);
-  if (tx_(i)) sfx[3][ty][tx] = sc_fx(D, D.t2, D.ru, i, j, k, false);
-  if (xe && tx_(i + 1)) sfx[3][ty][SX] = sc_fx(D, D.t2, D.ru, i + 1, j, k, false);
-  if (ty_(j)) sfy[3][ty][tx] = sc_fy(D, D.t2, D.rv, i, j, k, false);
-  if (ye && ty_(j + 1)) sfy[3][SY][tx] = sc_fy(D, D.t2, D.rv, i, j + 1, k, false);
+  // the tile's last column / row also takes the next face, in a loop: one call site per flux function, so that each
+  // flux body is inlined once (the kernel's size is what its instruction-cache misses follow)
+  const bool xe = tx == SX - 1, ye = ty == SY - 1;
+#pragma unroll 1
+  for (int e = 0; e <= int(xe); ++e) {
+    const int f = i + e;
+    if (ux(f)) sfx[0][ty][tx + e] = tu_fx(D, f, j, k);
+    if (vx(f)) sfx[1][ty][tx + e] = tv_fx(D, f, j, k);
+    if (wx(f)) sfx[2][ty][tx + e] = tw_fx(D, f, j, k);
+    if (tx_(f)) sfx[3][ty][tx + e] = sc_fx(D, D.t2, D.ru, f, j, k, false);
+  }
+#pragma unroll 1
+  for (int e = 0; e <= int(ye); ++e) {
+    const int f = j + e;
+    if (uy(f)) sfy[0][ty + e][tx] = tu_fy(D, i, f, k);
+    if (vy(f)) sfy[1][ty + e][tx] = tv_fy(D, i, f, k);
+    if (wy(f)) sfy[2][ty + e][tx] = tw_fy(D, i, f, k);
+    if (ty_(f)) sfy[3][ty + e][tx] = sc_fy(D, D.t2, D.rv, i, f, k, false);
+  }
   __syncthreads();
   if (!in) return;
   auto F = [&](int v, R& fx0, R& fx1, R& fy0, R& fy1) {
