@@ -485,7 +485,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if not args.no_autotune:
-        args.warmup = max(args.warmup, 5)  # 3 tuning steps, the graph capture, one replay
+        args.warmup = max(args.warmup, 8)  # 6 tuning steps, the graph capture, one replay
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

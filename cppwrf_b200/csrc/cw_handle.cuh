@@ -147,6 +147,8 @@ struct HaloSetHost {
 
 using namespace cw;
 
+constexpr int kTuneRounds = 2;  // autotuning: steps per block shape (one per round)
+
 struct cw_handle {
   int precision = CW_FP64;
   std::vector<Member> m;
@@ -198,7 +200,7 @@ struct cw_handle {
   // per-kernel timing of eager steps (cw_profile): events around each launch
   // block-shape autotuning of the point kernels: the first kNumShapes steps each run every tunable kernel
   // with one shape (eager, timed per launch); then each kernel keeps its fastest shape
-  bool autotune = false, tuned = false;
+  bool autotune = false, tuned = false;  // (kTuneRounds steps per shape)
   int tuning_shape = -1, tune_steps_done = 0;
   std::vector<std::pair<std::string, int>> shape_choice;
   std::vector<std::pair<std::string, std::array<double, kNumShapes>>> tune_ms;

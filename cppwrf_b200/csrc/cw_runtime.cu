@@ -661,7 +661,7 @@ void tune_step(cw_handle* h, int shape) {
   h->launches_last += L.count;
 }
 
-// after one tuning step per shape: every kernel keeps its fastest shape (the lowest on a tie)
+// after the tuning steps: every kernel keeps its fastest shape (the lowest on a tie)
 void finish_tuning(cw_handle* h) {
   h->shape_choice.clear();
   for (const auto& [name, ms] : h->tune_ms) {
@@ -677,15 +677,17 @@ void finish_tuning(cw_handle* h) {
 void run_steps(cw_handle* h, int nsteps) {
   h->launches_last = 0;
   if (h->m.empty()) return;
-  while (h->autotune && !h->tuned && nsteps > 0) {  // tuning steps advance the state like any other step
-    const int sh = int(h->tune_ms.empty() ? 0 : h->tune_steps_done);
-    tune_step(h, sh);
+  // tuning steps advance the state like any other step: kTuneRounds rounds of one step per shape, the order reversed
+  // in every other round (a drift over the steps weighs on every shape alike); each kernel's times summed over them
+  while (h->autotune && !h->tuned && nsteps > 0) {
+    const int s = h->tune_steps_done, idx = s % kNumShapes;
+    tune_step(h, (s / kNumShapes) % 2 == 0 ? idx : kNumShapes - 1 - idx);
     for (Member& M : h->m) {
       if (M.o.lbc) M.dtbc += M.g.dt;
       if (M.o.n_scalars > 0) M.q_parity ^= 1;
     }
     --nsteps;
-    if (++h->tune_steps_done == kNumShapes) finish_tuning(h);
+    if (++h->tune_steps_done == kNumShapes * kTuneRounds) finish_tuning(h);
   }
   if (nsteps == 0) return;
   if (h->use_graph && !h->graph_ok) {

@@ -209,10 +209,10 @@ int cw_check_finite(cw_handle* h, int member, int* field, int* n, int* i, int* j
  * quotients next to a rounding midpoint, exact quotients and their neighbours), on the current device. */
 int cw_check_div_const(unsigned long long n, unsigned long long seed, unsigned long long* checked,
                        unsigned long long* mismatches);
-/* Block-shape autotuning of the point kernels (no reference counterpart). With on = 1 the next three
- * cw_step steps run every tunable kernel in one of its block shapes (0: 128 x 1, 1: 64 x 2, 2: 32 x 4
- * points along i x j), timed per launch; afterwards each kernel keeps its fastest shape and the step is
- * captured again. The tuning steps are ordinary steps: every shape computes the same values. Calling it
+/* Block-shape autotuning (no reference counterpart). With on = 1 the next six cw_step steps run every tunable kernel
+ * in one of its shapes -- a point kernel's block of 0: 128 x 1, 1: 64 x 2, 2: 32 x 4 points along i x j, a column
+ * kernel's 0: 8, 1: 16, 2: 4 warps per column block -- two steps per shape (orders 0 1 2, then 2 1 0), timed per
+ * launch; afterwards each kernel keeps its fastest shape and the step is captured again. The tuning steps are ordinary steps: every shape computes the same values. Calling it
  * again re-tunes. cw_autotune_choice gives a kernel's chosen shape (-1 before the tuning has finished). */
 int cw_set_autotune(cw_handle* h, int on);
 /* LargeStep::cfl_max (src/dyn/large_step.cpp:865-877), the maxima behind RK3::on_cfl (rk3.hpp) that the reference's

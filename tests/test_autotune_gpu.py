@@ -20,9 +20,9 @@ def test_autotuned_equals_default(precision):
     a = Domain(case.g, case.o).upload_case(case).set_autotune(True)
     b = Domain(case.g, case.o).upload_case(case)
     assert a.autotune_choice("k_tend") == -1
-    a.step(2)  # two of the three tuning steps
-    a.step(3)  # the third, then two graph-replayed steps with the chosen shapes
-    b.step(5)
+    a.step(4)  # four of the six tuning steps
+    a.step(4)  # the last two, then two graph-replayed steps with the chosen shapes
+    b.step(8)
     for name in capi.STATE_FIELDS:
         assert np.array_equal(a.field(name).view(np.uint64), b.field(name).view(np.uint64)), name
     for n in range(case.o.n_scalars):
