@@ -354,18 +354,24 @@ def run_ensemble(args, torch, capi, Domain, Batch, rank=0, world=1):
         for k, c in enumerate(cases):
             b.upload_case(k, c)
         lib.cw_set_stream(b.h, C.c_void_p(stream.cuda_stream))
+        if not args.no_autotune:
+            b.set_autotune(True)  # the warm-up steps pick the batch's block shapes and warps per column block
         b.step(args.warmup)
         if world > 1:
             torch.distributed.barrier()
         ms = max_over_ranks(_timed_steps(torch, stream, b.step, args.steps), world, "cuda")
         out[prec] = (gp_all * args.steps / (ms / 1000.0), ms / args.steps, b.launches() // max(args.steps, 1))
         b.close()
-    # plain FP64: every member alone, one after the other (each rank its own members)
+    # plain FP64: every member alone, one after the other (each rank its own members), each tuned for itself
     plain_ms = 0.0
     for c in cases:
         d = Domain(c.g, c.o).upload_case(c)
         lib.cw_set_stream(d.h, C.c_void_p(stream.cuda_stream))
-        d.step(1)
+        if not args.no_autotune:
+            d.set_autotune(True)
+            d.step(args.warmup)
+        else:
+            d.step(1)
         plain_ms += _timed_steps(torch, stream, d.step, args.steps)
         d.close()
     plain_ms = max_over_ranks(plain_ms, world, "cuda")

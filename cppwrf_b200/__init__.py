@@ -125,7 +125,8 @@ class Domain:
         return self
 
     def set_autotune(self, on=True):
-        """The next three steps time the point kernels' block shapes; each kernel then keeps its fastest."""
+        """The next six steps time the kernels' block shapes (two steps per shape); each kernel then keeps its
+        fastest."""
         self.lib.cw_set_autotune(self.h, 1 if on else 0)
         return self
 
@@ -244,6 +245,7 @@ class Batch:
         return self
 
     def set_autotune(self, on=True):
+        """The next six steps time the kernels' block shapes over all members; each kernel then keeps its fastest."""
         self.lib.cw_set_autotune(self.h, 1 if on else 0)
         return self
 
