@@ -171,6 +171,11 @@ void cw_server::step_loop() {
         }
         if (inject) e = "injected batch creation failure";
         else if (cw_batch_create(0, nullptr, &r->o, &h) != 0) e = last_error(nullptr);
+        else if (cw_set_autotune(h, 1) != 0) e = last_error(h);  // its first steps pick the kernels' shapes
+        if (!e.empty() && h) {
+          cw_destroy(h);
+          h = nullptr;
+        }
         if (e.empty()) {
           groups.push_back(Group{r->n_sound, h, {}});
           G = &groups.back();

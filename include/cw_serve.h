@@ -12,8 +12,9 @@
  * Threading: three host threads started by cw_serve_create on the configured device, so that setting up and
  * reading back requests overlaps with stepping: an admitter (FIFO admission by footprint, each admitted request
  * set up in a single-domain handle of its own), a stepper (ready requests join their batch without a copy,
- * cw_batch_adopt; every batch's step is launched before any is waited for; finished requests leave without a
- * copy, cw_batch_release) and a reader (the finished request's state downloaded on its own stream, its device
+ * cw_batch_adopt; every batch's step is launched before any is waited for, and each batch tunes its kernels' block
+ * shapes over its first six steps, cw_set_autotune; finished requests leave without a copy, cw_batch_release) and a
+ * reader (the finished request's state downloaded on its own stream, its device
  * memory freed). A request holds its footprint of the budget from admission until its state is read back.
  * Every call below may be made from any thread.
  *
