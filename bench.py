@@ -645,7 +645,7 @@ def main():
             "data": "synthetic (cw_gen_lam, seeded)",
             "config": lam_config(args.precision, world),
             "block_shapes": {k: ["128x1", "64x2", "32x4"][dom.autotune_choice(k)]
-                             for k in ("k_tend", "k_tendf_rk1", "k_uv", "k_q_update", "k_q_face_pd",
+                             for k in ("k_tend", "k_tend_b", "k_tendf_rk1", "k_uv", "k_q_update", "k_q_face_pd",
                                        "k_q_scale_pd", "k_q_update_pd", "k_p_rho_phi")
                              if dom.autotune_choice(k) >= 0},
             "column_warps": {k: [8, 16, 4][dom.autotune_choice(k)]

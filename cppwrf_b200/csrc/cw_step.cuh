@@ -289,6 +289,8 @@ struct Launcher {
 // the three block-shape instantiations of a tunable point kernel
 #define KV(kern) std::array{kern<R, NM, 0>, kern<R, NM, 1>, kern<R, NM, 2>}
 #define KV_OP(kern, op) std::array{kern<R, NM, 0, op>, kern<R, NM, 1, op>, kern<R, NM, 2, op>}
+// the same with the kernel's part (its fifth template argument)
+#define KV_OP2(kern, op, x) std::array{kern<R, NM, 0, op, x>, kern<R, NM, 1, op, x>, kern<R, NM, 2, op, x>}
 // the three warp-count instantiations of a tunable column kernel
 #define KC(kern) std::array{kern<R, NM, cb_warps(0)>, kern<R, NM, cb_warps(1)>, kern<R, NM, cb_warps(2)>}
 
@@ -341,8 +343,18 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
       L.halo(cw_handle::H_XK);
     }
     if (rk == 1) L.run_t("k_tendf_rk1", RG_STAG, 1, KV(k_tendf_rk1), d);
-    if (open) L.run_t("k_tend", RG_STAG, 1, KV_OP(k_tend, true), d, rk);
-    else L.run_t("k_tend", RG_STAG, 1, KV_OP(k_tend, false), d, rk);
+    if constexpr (sizeof(R) == 8) {  // FP64: the tendencies in two launches (-1.4 % per step); mixed: one (faster)
+      if (open) {
+        L.run_t("k_tend", RG_STAG, 1, KV_OP2(k_tend, true, 3), d, rk);
+        L.run_t("k_tend_b", RG_STAG, 1, KV_OP2(k_tend, true, 12), d, rk);
+      } else {
+        L.run_t("k_tend", RG_STAG, 1, KV_OP2(k_tend, false, 3), d, rk);
+        L.run_t("k_tend_b", RG_STAG, 1, KV_OP2(k_tend, false, 12), d, rk);
+      }
+    } else {
+      if (open) L.run_t("k_tend", RG_STAG, 1, KV_OP(k_tend, true), d, rk);
+      else L.run_t("k_tend", RG_STAG, 1, KV_OP(k_tend, false), d, rk);
+    }
     if (h->cfl_on) L.run_t("k_cfl", RG_MASS, 1, KV(k_cfl), d, rk);
     if (rk == 1) L.copy_list(h->zeros_d, h->zeros_start_d, h->zeros.size(), h->zeros_total);
     L.run_cbt("k_ss_prep", RG_COLS_STAG, 3, KC(k_ss_prep), d, rk);

@@ -879,8 +879,11 @@ __device__ __forceinline__ bool spec_at(Ring r, int i, int j, int& sl, int& pos)
 // its own range: ru (u_i0 .. u_i1), rv (v_j0 .. v_j1, 3-D), rw and ph (levels 1..nz), theta (mass cells).
 // Also mu_tend = 0 (zero_tend of a run with lateral boundaries) at rk 2 and 3, and with lateral
 // boundaries the spec zone's tendencies from the boundary slabs.
-template <class R, int NM, int SH, bool OP>
+// PART: the tendencies a launch computes (1 u, 2 v, 4 w and phi, 8 theta and mu): the FP64 form runs the kernel as two
+// launches, (u, v) and (w, phi, theta, mu), whose smaller code misses the instruction cache less (the same values)
+template <class R, int NM, int SH, bool OP, int PART = 15>
 __global__ void __launch_bounds__(PX, 10) k_tend(const __grid_constant__ Pack<R, NM> P, int rk) {
+  constexpr bool PU = PART & 1, PV = PART & 2, PW = PART & 4, PT = PART & 8;
   constexpr int SX = shape_x(SH), SY = shape_y(SH);
   // the horizontal face fluxes of the block's tile, each evaluated once (u, v, w, theta): x faces i0 .. i0 + SX
   // of each row, y faces j0 .. j0 + SY of each column
@@ -914,18 +917,18 @@ __global__ void __launch_bounds__(PX, 10) k_tend(const __grid_constant__ Pack<R,
 #pragma unroll 1
   for (int e = 0; e <= int(xe); ++e) {
     const int f = i + e;
-    if (ux(f)) sfx[0][ty][tx + e] = tu_fx(D, f, j, k);
-    if (vx(f)) sfx[1][ty][tx + e] = tv_fx(D, f, j, k);
-    if (wx(f)) sfx[2][ty][tx + e] = tw_fx(D, f, j, k);
-    if (tx_(f)) sfx[3][ty][tx + e] = sc_fx(D, D.t2, D.ru, f, j, k, false);
+    if (PU && ux(f)) sfx[0][ty][tx + e] = tu_fx(D, f, j, k);
+    if (PV && vx(f)) sfx[1][ty][tx + e] = tv_fx(D, f, j, k);
+    if (PW && wx(f)) sfx[2][ty][tx + e] = tw_fx(D, f, j, k);
+    if (PT && tx_(f)) sfx[3][ty][tx + e] = sc_fx(D, D.t2, D.ru, f, j, k, false);
   }
 #pragma unroll 1
   for (int e = 0; e <= int(ye); ++e) {
     const int f = j + e;
-    if (uy(f)) sfy[0][ty + e][tx] = tu_fy(D, i, f, k);
-    if (vy(f)) sfy[1][ty + e][tx] = tv_fy(D, i, f, k);
-    if (wy(f)) sfy[2][ty + e][tx] = tw_fy(D, i, f, k);
-    if (ty_(f)) sfy[3][ty + e][tx] = sc_fy(D, D.t2, D.rv, i, f, k, false);
+    if (PU && uy(f)) sfy[0][ty + e][tx] = tu_fy(D, i, f, k);
+    if (PV && vy(f)) sfy[1][ty + e][tx] = tv_fy(D, i, f, k);
+    if (PW && wy(f)) sfy[2][ty + e][tx] = tw_fy(D, i, f, k);
+    if (PT && ty_(f)) sfy[3][ty + e][tx] = sc_fy(D, D.t2, D.rv, i, f, k, false);
   }
   __syncthreads();
   if (!in) return;
@@ -940,9 +943,10 @@ __global__ void __launch_bounds__(PX, 10) k_tend(const __grid_constant__ Pack<R,
   int sl, pos;
   // every tendency is computed before the first store (the stores cannot alias the loads then)
   // LateralBC::spec_dry (lateral_bc.cpp:337-351): the spec zone (row 0) takes the boundary tendency
-  bool has_u = true, has_v = true;
+  bool has_u = PU, has_v = PV;
   R tu = 0, tv = 0;
-  if (lbc && k < nz && spec_at(ring_for(nx, ny, 'u'), i, j, sl, pos)) {
+  if (!PU) {
+  } else if (lbc && k < nz && spec_at(ring_for(nx, ny, 'u'), i, j, sl, pos)) {
     tu = slab_at(D.lbc_var[0], 1, sl, pos, k, 0);
   } else if (OP && D.open_x && (i == 0 || i == nx) && j < ny && k < nz) {  // open boundaries: the faces are advanced too
     tu = tend_u_open_face(D, i, j, k, use_tendf);
@@ -952,7 +956,8 @@ __global__ void __launch_bounds__(PX, 10) k_tend(const __grid_constant__ Pack<R,
   } else {
     has_u = false;
   }
-  if (lbc && k < nz && spec_at(ring_for(nx, ny, 'v'), i, j, sl, pos)) {
+  if (!PV) {
+  } else if (lbc && k < nz && spec_at(ring_for(nx, ny, 'v'), i, j, sl, pos)) {
     tv = slab_at(D.lbc_var[1], 1, sl, pos, k, 0);
   } else if (OP && dy && D.open_y && (j == 0 || j == ny) && i < nx && k < nz) {
     tv = tend_v_open_face(D, i, j, k, use_tendf);
@@ -962,23 +967,24 @@ __global__ void __launch_bounds__(PX, 10) k_tend(const __grid_constant__ Pack<R,
   } else {
     has_v = false;
   }
-  const bool mass = i < nx && j < ny;
+  const bool mass = (PW || PT) && i < nx && j < ny;
   const bool spec = mass && lbc && spec_at(ring_for(nx, ny, 'h'), i, j, sl, pos);
   R tw = 0, tp = 0, tt = 0, tm = 0;
   bool has_p = false, has_m = false;
   if (mass) {
-    if (k >= 1) {
+    if (PW && k >= 1) {
       F(2, fx0, fx1, fy0, fy1);
       tw = tend_w<OP>(D, i, j, k, use_tendf, fx0, fx1, fy0, fy1);
     }
-    if (spec) {
+    if (!PW) {
+    } else if (spec) {
       tp = slab_at(D.lbc_var[3], 1, sl, pos, k, 0);
       has_p = true;
     } else if (k >= 1) {
       tp = tend_ph<OP>(D, i, j, k, lbc);
       has_p = true;
     }
-    if (k < nz) {
+    if (PT && k < nz) {
       if (spec) {
         tt = slab_at(D.lbc_var[2], 1, sl, pos, k, 0);
       } else {
@@ -986,7 +992,7 @@ __global__ void __launch_bounds__(PX, 10) k_tend(const __grid_constant__ Pack<R,
         tt = tend_t<OP>(D, i, j, k, use_tendf, D.n_moist > 0, fx0, fx1, fy0, fy1);
       }
     }
-    if (k == 0 && lbc) {
+    if (PT && k == 0 && lbc) {
       if (spec) {
         tm = slab_at(D.lbc_var[4], 1, sl, pos, 0, 0);
         has_m = true;
@@ -998,9 +1004,9 @@ __global__ void __launch_bounds__(PX, 10) k_tend(const __grid_constant__ Pack<R,
   if (has_u) D.ru_tend(i, j, k) = tu;
   if (has_v) D.rv_tend(i, j, k) = tv;
   if (mass) {
-    if (k >= 1) D.rw_tend(i, j, k) = tw;
+    if (PW && k >= 1) D.rw_tend(i, j, k) = tw;
     if (has_p) D.ph_tend(i, j, k) = tp;
-    if (k < nz) D.t_tend(i, j, k) = tt;
+    if (PT && k < nz) D.t_tend(i, j, k) = tt;
     if (has_m) D.mu_tend(i, j, 0) = tm;
   }
 }
