@@ -131,6 +131,7 @@ class RK3B200 {
     o.mp_physics = mp_physics_;
     o.mp_tend_lim = mp_tend_lim_;
     check(cw_create(&cg, &o, &h_), "cw_create");
+    check_h(cw_set_autotune(h_, 1), "cw_set_autotune");  // the first six steps pick the kernels' shapes (same values)
     if (on_cfl) check_h(cw_set_cfl_diagnostics(h_, 1), "cw_set_cfl_diagnostics");
   }
 
