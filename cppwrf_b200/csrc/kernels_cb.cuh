@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(CX * NW, cb_minblocks(NW)) k_ss_prep(const __g
 
 // One acoustic substep of a column block: advance_mu_t + sumflux (KMuTCol :208-249, KMuTPoint :251-277,
 // KSumEdge :281-290) (phase 1), advance_w (KWRhs / KWExpl / KWSolve :295-408) (phase 2), calc_p_rho with
-// divergence damping (KWPRho :411-416) (phase 4). The column mass sum, the running
+// divergence damping (KWPRho :411-416) (phase 3). The column mass sum, the running
 // omega integral and the tridiagonal sweeps are evaluated in double in both forms, on terms staged in
 // shared memory. With lateral boundaries the spec zone's columns take LateralBC::update_mu_t (phase 1) and
 // the phi'' part of update_ph_w (phase 2); the zero-gradient w of that zone needs the neighbours' new w and
@@ -283,7 +283,6 @@ __global__ void __launch_bounds__(CX * NW, cb_minblocks(NW)) k_ss_prep(const __g
 template <class R, int NM, int NW = CNW>
 __global__ void __launch_bounds__(CX * NW, cb_minblocks(NW)) k_ac(const __grid_constant__ Pack<R, NM> P, int rk, int it,
                                                     int nsteps) {
-  constexpr int phase = 7;
   int i, j, ilim;
   const Dom<R>& D = cb_member(P, RG_COLS_STAG, i, j, ilim);
   using A = double;
@@ -330,7 +329,7 @@ __global__ void __launch_bounds__(CX * NW, cb_minblocks(NW)) k_ac(const __grid_c
         }
       }
     }
-  if (phase & 1) {
+  {  // phase 1
     if (col && D.spec_x && i == nx && j < ny)  // KSumEdge, east face (specified or open x)
       CB_LOOP(k, nz) {
         const R su = (first ? R(0) : D.ru_m(i, j, k)) + D.u2.ld(i, j, k);
@@ -490,7 +489,7 @@ __global__ void __launch_bounds__(CX * NW, cb_minblocks(NW)) k_ac(const __grid_c
     }
     __syncthreads();
   }
-  if (phase & 2) {
+  {  // phase 2
     // advance_w in double in both forms (the mixed form's fields are float; the explicit phi'' and w'' right-hand
     // sides are differences of nearly equal pressure-gradient and buoyancy terms, kept in double). For the FP64
     // form every conversion below is the identity and the operations are the reference's, in its order.
@@ -624,7 +623,7 @@ __global__ void __launch_bounds__(CX * NW, cb_minblocks(NW)) k_ac(const __grid_c
       }
       __syncthreads();  // the member's option: uniform over the block
     }
-    // w'' and phi'' (dyn columns), then calc_p_rho of the level (every mass column, phase 4) from the new
+    // w'' and phi'' (dyn columns), then calc_p_rho of the level (every mass column, phase 3) from the new
     // phi'' of levels k and k + 1: recomputed from the shared terms here (the same expression as the store),
     // read back for the spec zone (written before the last barriers) and for the unchanged level 0
     auto ph_new = [&](int m) { return R(s0[m * CX + lane] + msfty * 0.5 * dtsA * k::g * ope * s2[m * CX + lane] / mfA(m, muts)); };
@@ -643,7 +642,7 @@ __global__ void __launch_bounds__(CX * NW, cb_minblocks(NW)) k_ac(const __grid_c
           D.w2(i, j, k) = wk;
           if (k >= 1) D.ph2(i, j, k) = phk;
         }
-        if ((phase & 4) && k < nz) p_rho_point_ph<true>(D, i, j, k, true, phk, phkp);
+        if (k < nz) p_rho_point_ph<true>(D, i, j, k, true, phk, phkp);
       }
   }
 }
