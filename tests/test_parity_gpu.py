@@ -269,3 +269,16 @@ def test_launch_count_gates_the_plain_scalar_update():
         dom.sync()
         counts.append(dom.launches())
     assert counts[1] == counts[0] + 1, counts
+
+
+def test_launches_per_step_of_the_lam_workload():
+    """One step of the 119 x 89 x 44 workload in one CUDA graph: 72 launches in FP64 (the large-step tendencies as
+    two launches, (u, v) and (w, phi, theta, mu)), 69 in the mixed form (one)."""
+    import bench
+    for prec, want in ((capi.FP64, 72), (capi.MIXED, 69)):
+        case = bench.make_case(capi, prec)
+        dom = Domain(case.g, case.o).upload_case(case)
+        dom.step(1)  # the captured step
+        dom.step(1)  # a replay: the count of the last call
+        dom.sync()
+        assert dom.launches() == want, (prec, dom.launches())
