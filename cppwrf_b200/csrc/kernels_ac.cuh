@@ -166,7 +166,9 @@ __device__ __forceinline__ void p_rho_phi_point(const Dom<R>& D, int i, int j, i
         (D.alb(i, j, k) * (R(D.c1h[k]) * D.mu2(i, j, 0)) + R(D.rdnw[k]) * (D.ph2(i, j, k + 1) - D.ph2(i, j, k)));
   }
   D.al(i, j, k) = a;
-  const double base = double(R(k::r_d) * (R(k::t0) + D.t2(i, j, k)) / (R(k::p1000mb) * (a + D.alb(i, j, k))));
+  // the equation of state in double in both forms: p'' is a small difference of totals of ~1e5 Pa (in float the
+  // rounding of the total's base, 6e-8, would be ~1e-4 of p'') -- for the FP64 form the same operations
+  const double base = k::r_d * (k::t0 + double(D.t2(i, j, k))) / (k::p1000mb * (double(a) + double(D.alb(i, j, k))));
   D.p(i, j, k) = R(k::p1000mb * eos_pow<R>(base) - double(D.pb(i, j, k)));
 }
 // mode 0: every mass point; 1: calc_p_rho_phi_interior (after spec_bdy_final); 2: after the microphysics, only in

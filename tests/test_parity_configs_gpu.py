@@ -7,7 +7,7 @@
   bit-identical to the reference's own CPU FP64 build (oracle/_ref/ref_harness_own, pow interposed by cw_pow),
   with no oracle in between;
 - the precision form on the same workload after 1 h (40 steps of 90 s): relative L2 <= 1e-4 against the FP64
-  form for u, v, theta, phi', mu' and qv, <= 1e-3 for w, on the interior points, max-abs reported."""
+  form for u, v, w, theta, phi', mu' and qv, on the interior points, max-abs reported."""
 import numpy as np
 import pytest
 
@@ -19,12 +19,11 @@ from cppwrf_b200 import Domain, capi
 
 pytestmark = pytest.mark.gpu
 
-# relative L2 bound of the precision form against the FP64 form after 1 h, per prognostic: 1e-4, except w at 1e-3.
-# w is a small residual field (|w| ~ 0.1 m/s here) fed by the horizontal divergence; the float roundings of u and v
-# (max abs ~7e-4 m/s after 1 h) put its relative L2 at 4.4e-4 (measured), with w's own equation, the column sums,
-# the tridiagonal solve and p'' in double; rounding the inputs or the base state to float changes it by < 1 %.
+# relative L2 bound of the precision form against the FP64 form after 1 h, per prognostic: 1e-4 for every one.
+# w is the tightest (|w| ~ 0.1 m/s here; 8.7e-5 measured): it follows p'', whose equation of state is evaluated in
+# double -- in float the rounding of the total's argument (6e-8 of ~1e5 Pa) made w's error 4.4e-4.
 # (The reference's own all-FP32 build reaches 3.7e-3 for W at 1 h on its 119 x 89 x 44 case, docs/FP32_ACCURACY.md.)
-MIXED_REL_L2_1H = {"u": 1e-4, "v": 1e-4, "w": 1e-3, "theta": 1e-4, "phi'": 1e-4, "mu'": 1e-4, "qv": 1e-4}
+MIXED_REL_L2_1H = {"u": 1e-4, "v": 1e-4, "w": 1e-4, "theta": 1e-4, "phi'": 1e-4, "mu'": 1e-4, "qv": 1e-4}
 PROGNOSTICS = {"u": ("U_2", 0), "v": ("V_2", 0), "w": ("W_2", 0), "theta": ("T_2", 0), "phi'": ("PH_2", 0),
                "mu'": ("MU_2", 0), "qv": ("Q_2", 0)}
 
