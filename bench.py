@@ -62,6 +62,7 @@ ALG_ARRAYS = {
     "k_finish": 15 + 8,       # u2 v2 w2 t2 ph2 ww 5 saves ww1 hd alb pb | u2 v2 w2 t2 ph2 ww al p
     "k_q_update": 3 + 3 + 1,  # per species: q2 q1 qtf + ru_m rv_m ww_m | qn (one thread updates every species: the
                               # fluxes ru_m rv_m ww_m once, below)
+    "k_q_march": 3 + 3 + 1,   # the same update with the species' planes staged by TMA (3-D domains)
     "k_q_update_pd": 4 + 3 + 1,
     "k_q_scale_pd": 2 + 3 + 1,
 }
@@ -620,7 +621,7 @@ def main():
     dom_name, dom_ms, dom_n = next((r for r in table if r[0] in ALG_ARRAYS), table[0])
     esz = 4 if prec == capi.MIXED else 8
     arrays = ALG_ARRAYS.get(dom_name, 0) * (WORKLOAD["n_moist"] if dom_name.startswith("k_q_") else 1)
-    if dom_name == "k_q_update":
+    if dom_name in ("k_q_update", "k_q_march"):
         arrays = 4 * WORKLOAD["n_moist"] + 3
     alg_bytes = arrays * pts * esz
     avg_s = dom_ms / 1000.0 / dom_n
@@ -648,6 +649,7 @@ def main():
                              for k in ("k_tend", "k_tend_b", "k_tendf_rk1", "k_uv", "k_q_update", "k_q_face_pd",
                                        "k_q_scale_pd", "k_q_update_pd", "k_p_rho_phi")
                              if dom.autotune_choice(k) >= 0},
+            "level_chunks": {k: [4, 2, 8][dom.autotune_choice(k)] for k in ("k_q_march",) if dom.autotune_choice(k) >= 0},
             "column_warps": {k: [8, 16, 4][dom.autotune_choice(k)]
                              for k in ("k_ls_prep", "k_ss_prep", "k_ac", "k_finish") if dom.autotune_choice(k) >= 0},
             "clocks": clocks, "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": ebytes,

@@ -167,6 +167,7 @@ def load(path=None):
         "cw_n_sound": (i, [vp, ip]),
         "cw_set_stream": (i, [vp, vp]),
         "cw_sync": (i, [vp]),
+        "cw_selftest_wait": (i, [vp, C.c_longlong]),
         "cw_last_error": (C.c_char_p, [vp]),
         "cw_launch_count": (i, [vp, C.POINTER(C.c_longlong)]),
         "cw_upload_case": (i, [vp, vp]),

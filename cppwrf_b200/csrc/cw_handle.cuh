@@ -36,6 +36,13 @@ namespace cw {
 
 constexpr size_t kAlign = 256;
 inline size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
+// the base-state fields the mixed form also keeps in double (Member::b64)
+constexpr int kB64Fields[3] = {CW_PB, CW_ALB, CW_PHB};
+inline int b64_slot(int field) {
+  for (int x = 0; x < 3; ++x)
+    if (kB64Fields[x] == field) return x;
+  return -1;
+}
 
 // the work fields of one domain beyond State / Tendencies / BaseState (SmallStep's fields)
 enum Work { W_U_SAVE, W_V_SAVE, W_W_SAVE, W_T_SAVE, W_PH_SAVE, W_WW1, W_C2A, W_PM1, W_T_2SAVE, W_A, W_ALPHA, W_GAMMA,
@@ -79,6 +86,9 @@ struct Member {
   std::vector<char> q_have;
   double dtbc = 0;
   int q_parity = 0;
+  // the mixed form: double copies of PB, ALB, PHB (kB64Fields), written with every upload of those fields and read
+  // by the double parts of the step (the equation of state, the hydrostatic integrations); nullptr in FP64
+  char* b64[3] = {nullptr, nullptr, nullptr};
   char* arena = nullptr;  // the member's device allocation (every pointer above points into it)
   size_t arena_bytes = 0;
   double cf1 = 0, cf2 = 0, cf3 = 0, cfn = 0, cfn1 = 0, rdx = 0, rdy = 0;
@@ -97,6 +107,7 @@ struct DevTables {  // the kernels' views of the members and the device scalar t
   V3<R>* qtab = nullptr;  // per member: q1, q2, qn, qtf, qscale, 6 PD faces (kQTab x n_scalars)
   Slabs<R>* lbcq = nullptr;
   Dom<R>* doms_d = nullptr;  // the batch's member descriptors
+  QMap* qmap = nullptr;       // per member and species: the tensor maps of the TMA-staged scalar update
 };
 
 // a fill point's fields (or the union of consecutive fill points') as a device table: one launch per pass
@@ -168,6 +179,9 @@ struct cw_handle {
   DevTables<float> t32;
   double* dtbc_d = nullptr;  // per member: time since the boundary data, advanced by the step on the device
   unsigned long long* cfl_d = nullptr;  // per member: 3 stages x (vertical, horizontal) CFL maxima of the last step
+  unsigned* status_d = nullptr;  // bit 0: a kernel's bounded wait for its copies gave up; bit 1: an unaligned copy refused
+  bool q_tma = false;            // every member has the tensor maps: the TMA-staged k_q_march can run
+  bool q_march = false;          // the autotuner chose k_q_march over the point kernel k_q_update
   bool cfl_on = false;                  // cw_set_cfl_diagnostics
   unsigned long long* diag = nullptr;  // cw_check_finite's result
   double* diag_part = nullptr;         // cw_diagnostics' per-level partials

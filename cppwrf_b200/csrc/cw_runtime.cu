@@ -49,6 +49,7 @@ bool pd_any(const cw_options& o) {
 // one member's allocation plan: byte offsets of every field, work field, scalar, vertical array and slab
 struct Plan {
   std::vector<size_t> f, w, q1, qa, qb, qtf, qsc, qslab, qpd;
+  size_t b64[3]{};
   size_t vert = 0;
   size_t slab[5]{};
   size_t total = 0;
@@ -65,6 +66,8 @@ Plan plan_member(Member& M) {
     M.L[id] = field_layout(M.g, M.o, id, M.pbox());
     P.f.push_back(take(field_bytes(M.L[id], M.esz)));
   }
+  if (M.esz == 4)
+    for (int x = 0; x < 3; ++x) P.b64[x] = take(field_bytes(M.L[kB64Fields[x]], 8));
   M.LW.resize(W_N);
   for (int w = 0; w < W_N; ++w) {
     const FieldKind k = work_kind(w);
@@ -124,6 +127,7 @@ void allocate_member(cw_handle* h, Member& M) {
   M.q1.clear(); M.qa.clear(); M.qb.clear(); M.qtf.clear(); M.qsc.clear(); M.qslab.clear(); M.qpd.clear();
   for (size_t off : P.qpd) M.qpd.push_back(A + off);
   for (int id = 0; id < CW_Q_1; ++id) M.base.push_back(A + P.f[id]);
+  for (int x = 0; x < 3; ++x) M.b64[x] = M.esz == 4 ? A + P.b64[x] : nullptr;
   for (int w = 0; w < W_N; ++w) M.wbase.push_back(A + P.w[w]);
   for (int n = 0; n < M.o.n_scalars; ++n) {
     M.q1.push_back(A + P.q1[n]);
@@ -186,6 +190,7 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.w_crit_cfl = o.w_crit_cfl;
   D.dtbc = h->dtbc_d + mi;
   D.cfl = h->cfl_d + 6 * mi;
+  D.status = h->status_d;
   D.cf1 = M.cf1; D.cf2 = M.cf2; D.cf3 = M.cf3; D.cfn = M.cfn; D.cfn1 = M.cfn1; D.rdx = M.rdx; D.rdy = M.rdy;
   const double* v = M.vert;
   auto va = [&](int a) { return v + M.vert_off[a]; };
@@ -212,6 +217,8 @@ Dom<R> make_dom(cw_handle* h, size_t mi, V3<R>* qtab_d, Slabs<R>* lbcq_d) {
   D.phb = fb(CW_PHB); D.ht = fb(CW_HT); D.msftx = fb(CW_MSFTX); D.msfty = fb(CW_MSFTY); D.msfux = fb(CW_MSFUX);
   D.msfuy = fb(CW_MSFUY); D.msfvx = fb(CW_MSFVX); D.msfvy = fb(CW_MSFVY); D.msfvx_inv = fb(CW_MSFVX_INV);
   D.f = fb(CW_F); D.e = fb(CW_E); D.sina = fb(CW_SINA); D.cosa = fb(CW_COSA); D.cor = o.coriolis != 0 || o.mapped != 0;
+  auto f64 = [&](int x) { return viewb<double>(M.esz == 8 ? M.base[kB64Fields[x]] : M.b64[x], M.L[kB64Fields[x]]); };
+  D.pb64 = f64(0); D.alb64 = f64(1); D.phb64 = f64(2);
   D.mapped = o.mapped != 0;
   D.u_save = w3(W_U_SAVE); D.v_save = w3(W_V_SAVE); D.w_save = w3(W_W_SAVE); D.t_save = w3(W_T_SAVE);
   D.ph_save = w3(W_PH_SAVE); D.ww1 = w3(W_WW1); D.c2a = w3(W_C2A); D.pm1 = w3(W_PM1); D.t_2save = w3(W_T_2SAVE);
@@ -286,6 +293,62 @@ void build_packs(cw_handle* h, const std::vector<Dom<R>>& doms, DevTables<R>& T)
   ps.p.push_back(*P);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against the driver library)
+using EncodeTiled = decltype(&cuTensorMapEncodeTiled);
+EncodeTiled encode_tiled() {
+  static EncodeTiled fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return EncodeTiled(nullptr);
+    return reinterpret_cast<EncodeTiled>(p);
+  }();
+  return fn;
+}
+// the tensor map of one scalar buffer for k_q_march: the allocation as (pitch, rows, levels), a box of one plane of
+// a tile with its halo; false where the layout does not allow it (2-D, narrower than the box, unaligned)
+template <class R>
+bool encode_q_map(CUtensorMap* out, const char* base, const cw_layout& L) {
+  const EncodeTiled enc = encode_tiled();
+  constexpr int W = QPlanes<R>::W, H = QPlanes<R>::H;
+  const int64_t rows = L.wj1 - L.wj0;
+  if (!enc || L.sj <= 0 || L.sj < W || rows < H || L.nz < 1) return false;
+  if ((reinterpret_cast<uintptr_t>(base) % 16) != 0 || (L.sj * int64_t(sizeof(R))) % 16 != 0 ||
+      (L.sk * int64_t(sizeof(R))) % 16 != 0 || L.sk != L.sj * rows)
+    return false;
+  const cuuint64_t dims[3] = {cuuint64_t(L.sj), cuuint64_t(rows), cuuint64_t(L.nz)};
+  const cuuint64_t strides[2] = {cuuint64_t(L.sj) * sizeof(R), cuuint64_t(L.sk) * sizeof(R)};
+  const cuuint32_t box[3] = {cuuint32_t(W), cuuint32_t(H), 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(out, sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                         const_cast<char*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+// member M's maps (one per species) for k_q_march, false if any cannot be made. Element (i, j, k) of a scalar
+// buffer is at offset + i + j sj + k sk with offset = x0 + y0 sj, x0 = 5 - wi0 (a row's 8-element lead before its
+// halo of 3), y0 = -wj0: the map coordinates of i = 0, j = 0. The tiles start at i = pi0 + 32 b, so the x of a
+// tile's first staged column, x0 + pi0 - 4 + 32 b = 4 + 32 b, is 16-byte aligned.
+template <class R>
+bool make_q_maps(const Member& M, std::vector<QMap>& out) {
+  if (two_d(M.g) || M.o.n_scalars == 0) return false;
+  const cw_layout& L = M.Lq;
+  const int x0 = 5 - L.wi0, y0 = -L.wj0;
+  const int pi0 = M.patched ? M.patch.i0 : 0;
+  if (L.offset != int64_t(x0) + int64_t(y0) * L.sj) return false;  // the layout's lead as assumed above
+  if ((int64_t(x0 + pi0 - 4) * int64_t(sizeof(R))) % 16 != 0) return false;
+  for (int n = 0; n < M.o.n_scalars; ++n) {
+    QMap q{};
+    if (!encode_q_map<R>(&q.a, M.qa[size_t(n)], L) || !encode_q_map<R>(&q.b, M.qb[size_t(n)], L)) return false;
+    q.pa = view3<R>(M.qa[size_t(n)], L).p;
+    q.x0 = x0;
+    q.y0 = y0;
+    out.push_back(q);
+  }
+  return true;
+}
+
 template <class R>
 void upload_tables(cw_handle* h, DevTables<R>& T) {
   const size_t nm = h->m.size();
@@ -299,6 +362,17 @@ void upload_tables(cw_handle* h, DevTables<R>& T) {
   for (const Member& M : h->m) nq += size_t(M.o.n_scalars);
   if (!T.qtab && nq) CW_CUDA(cudaMalloc(&T.qtab, kQTab * nq * sizeof(V3<R>)));
   if (!T.lbcq && nq) CW_CUDA(cudaMalloc(&T.lbcq, nq * sizeof(Slabs<R>)));
+  if (!h->status_d) {
+    CW_CUDA(cudaMalloc(&h->status_d, sizeof(unsigned)));
+    CW_CUDA(cudaMemsetAsync(h->status_d, 0, sizeof(unsigned), h->stream));
+  }
+  // the TMA-staged scalar update where every member allows it (3-D, wide enough for a tile's planes)
+  std::vector<QMap> qmaps;
+  bool q_tma = nq > 0;
+  for (const Member& M : h->m)
+    if (q_tma && M.o.n_scalars > 0) q_tma = make_q_maps<R>(M, qmaps);
+  h->q_tma = q_tma;
+  if (q_tma && !T.qmap) CW_CUDA(cudaMalloc(&T.qmap, qmaps.size() * sizeof(QMap)));
   std::vector<Dom<R>> doms(nm);
   std::vector<V3<R>> qtab(kQTab * nq);
   std::vector<Slabs<R>> lbcq(nq);
@@ -307,6 +381,7 @@ void upload_tables(cw_handle* h, DevTables<R>& T) {
     Member& M = h->m[mi];
     const int ns = M.o.n_scalars;
     doms[mi] = make_dom<R>(h, mi, T.qtab ? T.qtab + kQTab * q0 : nullptr, T.lbcq ? T.lbcq + q0 : nullptr);
+    doms[mi].qmap = q_tma ? T.qmap + q0 : nullptr;
     for (int n = 0; n < ns; ++n) {
       char* q2 = M.q_parity ? M.qb[n] : M.qa[n];
       char* qn = M.q_parity ? M.qa[n] : M.qb[n];
@@ -337,6 +412,7 @@ void upload_tables(cw_handle* h, DevTables<R>& T) {
     CW_CUDA(cudaMemcpyAsync(T.qtab, qtab.data(), qtab.size() * sizeof(V3<R>), cudaMemcpyHostToDevice, h->stream));
     CW_CUDA(cudaMemcpyAsync(T.lbcq, lbcq.data(), lbcq.size() * sizeof(Slabs<R>), cudaMemcpyHostToDevice, h->stream));
   }
+  if (q_tma) CW_CUDA(cudaMemcpyAsync(T.qmap, qmaps.data(), qmaps.size() * sizeof(QMap), cudaMemcpyHostToDevice, h->stream));
   CW_CUDA(cudaStreamSynchronize(h->stream));
 }
 
@@ -661,15 +737,21 @@ void tune_step(cw_handle* h, int shape) {
   h->launches_last += L.count;
 }
 
-// after the tuning steps: every kernel keeps its fastest shape (the lowest on a tie)
+// after the tuning steps: every kernel keeps its fastest shape (the lowest on a tie); the scalar update is the
+// faster of the point kernel k_q_update and the TMA-staged k_q_march, each in its fastest shape (each was timed in
+// one round of steps, in every shape)
 void finish_tuning(cw_handle* h) {
   h->shape_choice.clear();
+  float best_update = -1, best_march = -1;
   for (const auto& [name, ms] : h->tune_ms) {
     int best = 0;
     for (int sh = 1; sh < kNumShapes; ++sh)
       if (ms[size_t(sh)] < ms[size_t(best)]) best = sh;
     h->shape_choice.push_back({name, best});
+    if (name == "k_q_update") best_update = ms[size_t(best)];
+    if (name == "k_q_march") best_march = ms[size_t(best)];
   }
+  h->q_march = best_march >= 0 && best_update >= 0 && best_march < best_update;
   h->tuned = true;
   invalidate_graph(h);
 }
@@ -770,9 +852,12 @@ void free_tables(cw_handle* h) {
   cudaFree(h->t64.qtab);
   cudaFree(h->t64.lbcq);
   cudaFree(h->t64.doms_d);
+  cudaFree(h->t64.qmap);
   cudaFree(h->t32.qtab);
   cudaFree(h->t32.lbcq);
   cudaFree(h->t32.doms_d);
+  cudaFree(h->t32.qmap);
+  h->q_tma = false;
   h->t64 = DevTables<double>{};
   h->t32 = DevTables<float>{};
 }
@@ -804,11 +889,15 @@ struct Loc {
   char* base;
   cw_layout L;
   int esz;
+  char* b64 = nullptr;  // the mixed form's double copy of the field (PB, ALB, PHB), written with it
 };
 Loc locate(cw_handle* h, int mi, int field, int n) {
   if (mi < 0 || mi >= int(h->m.size())) throw std::runtime_error("member index out of range");
   Member& M = h->m[mi];
-  if (field >= 0 && field < CW_Q_1) return Loc{M.base[field], M.L[field], M.esz};
+  if (field >= 0 && field < CW_Q_1) {
+    const int x = b64_slot(field);
+    return Loc{M.base[field], M.L[field], M.esz, x >= 0 ? M.b64[x] : nullptr};
+  }
   if (n < 0 || n >= M.o.n_scalars) throw std::runtime_error("scalar index out of range");
   if (field == CW_Q_1) return Loc{M.q1[n], M.Lq, M.esz};
   if (field == CW_Q_2) return Loc{M.q_parity ? M.qb[n] : M.qa[n], M.Lq, M.esz};
@@ -847,6 +936,7 @@ void copy_in(cw_handle* h, const Loc& l, const double* host, size_t count) {
     const unsigned n = unsigned(count), blocks = std::min(4096u, (n + 255u) / 256u);
     k_narrow<<<blocks, 256, 0, h->stream>>>(st, reinterpret_cast<float*>(l.base), n);
     CW_CUDA(cudaGetLastError());
+    if (l.b64) CW_CUDA(cudaMemcpyAsync(l.b64, st, count * 8, cudaMemcpyDeviceToDevice, h->stream));
   }
 }
 void copy_out(cw_handle* h, const Loc& l, double* host, size_t count) {
@@ -1059,6 +1149,7 @@ void upload_fields(cw_handle* h, int mi, int nf, const int* fields, const int* n
       const unsigned n = unsigned(counts[f]), blocks = std::min(4096u, (n + 255u) / 256u);
       k_narrow<<<blocks, 256, 0, h->stream>>>(st, reinterpret_cast<float*>(l.base), n);
       CW_CUDA(cudaGetLastError());
+      if (l.b64) CW_CUDA(cudaMemcpyAsync(l.b64, st, counts[f] * 8, cudaMemcpyDeviceToDevice, h->stream));
       st += counts[f];
     }
   }
@@ -1510,6 +1601,7 @@ int cw_destroy(cw_handle* h) {
   cudaFree(h->staging);
   cudaFree(h->diag);
   cudaFree(h->diag_part);
+  cudaFree(h->status_d);
   for (Member& M : h->m) cudaFree(M.arena);
   if (h->own_stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -1734,9 +1826,40 @@ int cw_set_stream(cw_handle* h, void* stream) {
     return 0;
   });
 }
+// a barrier that nothing completes, waited on with the kernels' bounded wait (cw_selftest_wait)
+static __global__ void k_selftest_wait(unsigned* status, long long cycles) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const bool ok = cycles > 0 ? mbar_wait(&bar, 0, cycles) : mbar_wait(&bar, 0);
+  if (!ok && threadIdx.x == 0) atomicOr(status, 1u);
+}
+// the device status word: a kernel that gave up a bounded wait, or refused an unaligned copy, left work undone
+static void check_status(cw_handle* h) {
+  if (!h->status_d) return;
+  unsigned st = 0;
+  CW_CUDA(cudaMemcpyAsync(&st, h->status_d, sizeof st, cudaMemcpyDeviceToHost, h->stream));
+  CW_CUDA(cudaStreamSynchronize(h->stream));
+  if (st == 0) return;
+  CW_CUDA(cudaMemsetAsync(h->status_d, 0, sizeof st, h->stream));
+  throw std::runtime_error((st & 1u) ? "a kernel's wait for its tensor copies timed out: the step is incomplete"
+                                     : "a kernel refused an unaligned tensor copy: the step is incomplete");
+}
 int cw_sync(cw_handle* h) {
   return guarded(h, [&] {
     CW_CUDA(cudaStreamSynchronize(h->stream));
+    CW_CUDA(cudaGetLastError());
+    check_status(h);
+    return 0;
+  });
+}
+int cw_selftest_wait(cw_handle* h, long long cycles) {
+  return guarded(h, [&] {
+    if (!h || !h->status_d) throw std::runtime_error("no handle");
+    k_selftest_wait<<<1, 32, 0, h->stream>>>(h->status_d, cycles);
     CW_CUDA(cudaGetLastError());
     return 0;
   });
@@ -1900,6 +2023,7 @@ int cw_set_autotune(cw_handle* h, int on) {
   h->tune_steps_done = 0;
   h->tune_ms.clear();
   h->shape_choice.clear();
+  h->q_march = false;
   invalidate_graph(h);
   return 0;
 }

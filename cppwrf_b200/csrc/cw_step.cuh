@@ -244,6 +244,23 @@ struct Launcher {
       check();
     }
   }
+  // the TMA-staged scalar update over RG_TILES: the shape is the chunk of levels a block takes (q_chunk), the planes
+  // and face fluxes in dynamic shared memory
+  template <class R, int NM, class K, class... Args>
+  void run_q(const char* name, const std::array<K, kNumShapes>& kerns, const Packs<R, NM>& ps, Args... args) {
+    flush();
+    if (plan) return;
+    const int sh = shape_for(name);
+    const size_t smem = q_march_smem<R>(sh);
+    CW_CUDA(cudaFuncSetAttribute(kerns[size_t(sh)], cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    for (size_t c = 0; c < ps.p.size(); ++c) {
+      const int nb = ps.blocks[c][size_t(RG_TILES)][size_t(sh)];
+      if (nb == 0) continue;
+      begin(name);
+      kerns[size_t(sh)]<<<nb, kQTx * kQTy, smem, h->stream>>>(ps.p[c], args...);
+      check();
+    }
+  }
   // a column-block kernel using `arrays` shared level arrays
   template <class R, int NM, class K, class... Args>
   void run_cb(const char* name, int kind, int arrays, K kern, const Packs<R, NM>& ps, Args... args) {
@@ -372,7 +389,13 @@ void enqueue_step(cw_handle* h, Launcher& L, const Packs<R, NM>& d) {
     if (scalars) {
       if (rk == 1) L.run_t("k_q_tendf_rk1", RG_MASS, nq, KV(k_q_tendf_rk1), d);
       // at rk 3 the PD species take k_q_*_pd: the plain update runs only when some species is not PD
-      if (rk != 3 || any_plain || !any_pd) L.run_t("k_q_update", RG_MASS, 1, KV(k_q_update), d, rk);
+      if (rk != 3 || any_plain || !any_pd) {
+        // the TMA-staged update where the tuner chose it; while tuning, the point kernel in the first round of
+        // steps and the staged one in the second
+        const bool march = h->q_tma && (h->tuning_shape >= 0 ? h->tune_steps_done / kNumShapes == 1 : h->q_march);
+        if (march) L.run_q("k_q_march", KV(k_q_march), d, rk);
+        else L.run_t("k_q_update", RG_MASS, 1, KV(k_q_update), d, rk);
+      }
       if (rk == 3 && any_pd) {
         L.run_t("k_q_pre_pd", RG_MASS, nq, KV(k_q_pre_pd), d, rk);
         L.halo(cw_handle::H_Q1PD);

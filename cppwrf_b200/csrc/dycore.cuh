@@ -10,6 +10,7 @@
 #include <cstdint>
 
 #include "cw_pow.h"
+#include "tma.cuh"
 
 namespace cw {
 
@@ -83,6 +84,9 @@ struct Dom {
   // BaseState
   VB<T> mub, pb, alb, t_init, qv_base, phb, ht, msftx, msfty, msfux, msfuy, msfvx, msfvy, msfvx_inv;
   VB<T> f, e, sina, cosa;  // Coriolis parameters and grid rotation
+  // pb, alb, phb in double for the double parts of both forms (the FP64 form: the same arrays; the mixed form:
+  // double copies, so that the equation of state's p'' = p(alpha, theta) - pb does not carry pb's float rounding)
+  VB<double> pb64, alb64, phb64;
   int cor;                 // MapC::cor = BaseState::mapped || coriolis: the Coriolis terms of the u, v, w tendencies
   int mapped;              // BaseState::mapped: map factors vary; the curvature terms of u, v use their gradients
   // acoustic-step work fields (SmallStep, src/dyn/small_step.hpp:45-49)
@@ -101,6 +105,9 @@ struct Dom {
   // boundary slabs: U V T PH MU, then scalars (n_scalars entries)
   Slabs<T> lbc_var[5];
   Slabs<T>* lbc_q;
+  // the TMA-staged scalar update: each species' tensor maps (device memory; nullptr where it does not run)
+  const QMap* qmap;
+  unsigned* status;  // device word of the handle: bit 0 set when a kernel's bounded wait gave up (cw_sync reports it)
 };
 
 // The kernels' view of the members. A single domain (NM = 1): its descriptor passed by value as a
@@ -108,7 +115,7 @@ struct Dom {
 // arithmetic) and no store of a kernel can alias them. A batch (NM = 0, any number of members): the members'
 // descriptors and block prefix sums in device memory, so one launch of each kernel covers the whole batch.
 // start(kind, shape, m) is member m's first block of a launch over the index range `kind` in block shape `shape`.
-constexpr int kNumKinds = 7;
+constexpr int kNumKinds = 8;
 constexpr int kNumShapes = 3;  // point-kernel block shapes (autotuned per kernel): 128 x 1, 64 x 2, 32 x 4
 template <class R, int NM>
 struct Pack {
@@ -122,7 +129,7 @@ struct Pack<R, 0> {
   const Dom<R>* __restrict__ d;  // n descriptors (device memory, written before the launch)
   int n;
   // the block starts in the parameter (the constant bank: a block's binary search over them is uniform and
-  // needs no global load), 18.5 KB for the largest batch, within the 32 KB parameter limit
+  // needs no global load), 24.1 KB for the largest batch, within the 32 KB parameter limit
   int start_[kNumKinds][kNumShapes][kMaxMembers + 1];
   __device__ __forceinline__ int start(int kind, int shape, int m) const { return start_[kind][shape][m]; }
 };

@@ -24,7 +24,11 @@ enum RangeKind {
   RG_RING,        // boundary ring b = 0: pos in [0, max(nx, ny)+1), k in [0, nz+1), 4 sides
   RG_MASS_W,      // [0, nx) x [0, ny) x [0, nz+1)
   RG_FACES,       // as RG_STAG; in a patch, the faces of its cells up to the face after its last cell
+  RG_TILES,       // as RG_MASS, in blocks of kQTx x kQTy columns and q_chunk(shape) levels (the TMA-staged scalars)
 };
+// The TMA-staged scalar update's block: a tile of kQTx x kQTy columns (one thread each) and a chunk of levels
+constexpr int kQTx = 32, kQTy = 4;
+__host__ __device__ constexpr int q_chunk(int shape) { return shape == 0 ? 4 : (shape == 1 ? 2 : 8); }
 struct Range {
   int i0, i1, j0, j1, k0, k1;
 };
@@ -44,6 +48,7 @@ __host__ __device__ __forceinline__ Range range_of(int kind, int nx, int ny, int
     case RG_COLS_MASS: return {pi0, pi1, pj0, pj1, 0, 1};
     case RG_RING: return {0, (nx > ny ? nx : ny) + 1, 0, nz + 1, 0, 4};
     case RG_FACES: return {pi0, pi1 + 1, pj0, jf, 0, nz + 1};
+    case RG_TILES: return {pi0, pi1, pj0, pj1, 0, nz};
     default: return {pi0, pi1, pj0, pj1, 0, nz + 1};
   }
 }
@@ -54,6 +59,7 @@ __host__ __device__ __forceinline__ Range range_of(int kind, const Dom<R>& D) {
 __host__ __device__ __forceinline__ bool is_column(int kind) { return kind == RG_COLS_STAG || kind == RG_COLS_MASS; }
 __host__ __device__ __forceinline__ int blocks_of(const Range& r, int kind, int shape = 0) {
   if (is_column(kind)) return cdiv(r.i1 - r.i0, CX) * (r.j1 - r.j0) * (r.k1 - r.k0);
+  if (kind == RG_TILES) return cdiv(r.i1 - r.i0, kQTx) * cdiv(r.j1 - r.j0, kQTy) * cdiv(r.k1 - r.k0, q_chunk(shape));
   return cdiv(r.i1 - r.i0, shape_x(shape)) * cdiv(r.j1 - r.j0, shape_y(shape)) * (r.k1 - r.k0);
 }
 // thread -> (member, i, j, k) of a point kernel launched with block shape SH; false past the range (the range in rg)
@@ -611,9 +617,10 @@ __device__ R tend_w(const Dom<R>& D, int i, int j, int k, bool use_tendf, R fx0,
   return t;
 }
 
-// KTendT (:502-565) / advect_scalar face fluxes of any mass field q with mass fluxes (ufx, vfy, wfz)
-template <class R>
-__device__ R sc_fx(const Dom<R>& D, const V3<R>& q, const V3<R>& ruf, int i, int j, int k, bool pd) {
+// KTendT (:502-565) / advect_scalar face fluxes of any mass field q with mass fluxes (ufx, vfy, wfz); q is a view of
+// the field in global memory (V3) or of a tile of its planes in shared memory (QPlanes), read with the domain's indices
+template <class R, class QV>
+__device__ R sc_fx(const Dom<R>& D, const QV& q, const V3<R>& ruf, int i, int j, int k, bool pd) {
   const R vel = ruf.ld(i, j, k);
   const int o = ord_face(i, D.nx, D.spec_x);
   if (o == 2) return R(0.5) * vel * (q.ld(i, j, k) + q.ld(i - 1, j, k));
@@ -625,8 +632,8 @@ __device__ R sc_fx(const Dom<R>& D, const V3<R>& q, const V3<R>& ruf, int i, int
     return vel * flux5_pd(q.ld(i - 3, j, k), q.ld(i - 2, j, k), q.ld(i - 1, j, k), q.ld(i, j, k), q.ld(i + 1, j, k), q.ld(i + 2, j, k), vel, R(D.hup));
   return vel * flux5(q.ld(i - 3, j, k), q.ld(i - 2, j, k), q.ld(i - 1, j, k), q.ld(i, j, k), q.ld(i + 1, j, k), q.ld(i + 2, j, k), vel, R(D.hup));
 }
-template <class R>
-__device__ R sc_fy(const Dom<R>& D, const V3<R>& q, const V3<R>& rvf, int i, int j, int k, bool pd) {
+template <class R, class QV>
+__device__ R sc_fy(const Dom<R>& D, const QV& q, const V3<R>& rvf, int i, int j, int k, bool pd) {
   const R vel = rvf.ld(i, j, k);
   const int o = ord_face(j, D.ny, D.spec_y);
   if (o == 2) return R(0.5) * vel * (q.ld(i, j, k) + q.ld(i, j - 1, k));
@@ -638,8 +645,8 @@ __device__ R sc_fy(const Dom<R>& D, const V3<R>& q, const V3<R>& rvf, int i, int
     return vel * flux5_pd(q.ld(i, j - 3, k), q.ld(i, j - 2, k), q.ld(i, j - 1, k), q.ld(i, j, k), q.ld(i, j + 1, k), q.ld(i, j + 2, k), vel, R(D.hup));
   return vel * flux5(q.ld(i, j - 3, k), q.ld(i, j - 2, k), q.ld(i, j - 1, k), q.ld(i, j, k), q.ld(i, j + 1, k), q.ld(i, j + 2, k), vel, R(D.hup));
 }
-template <class R>
-__device__ R sc_fz(const Dom<R>& D, const V3<R>& q, const V3<R>& wwf, int i, int j, int k, bool pd) {
+template <class R, class QV>
+__device__ R sc_fz(const Dom<R>& D, const QV& q, const V3<R>& wwf, int i, int j, int k, bool pd) {
   if (k == 0 || k == D.nz) return 0;
   const R vel = wwf.ld(i, j, k);
   if (k == 1 || k == D.nz - 1) return vel * (R(D.fnm[k]) * q.ld(i, j, k) + R(D.fnp[k]) * q.ld(i, j, k - 1));

@@ -158,9 +158,9 @@ __device__ __forceinline__ void p_rho_phi_point(const Dom<R>& D, int i, int j, i
     const double m = double(D.muts(i, j, 0)), ptop = D.p_top;
     const double pfu = D.c3f[k + 1] * m + D.c4f[k + 1] + ptop, pfd = D.c3f[k] * m + D.c4f[k] + ptop;
     const double phm = D.c3h[k] * m + D.c4h[k] + ptop;
-    a = R((double(D.ph2(i, j, k + 1)) - double(D.ph2(i, j, k)) + double(D.phb(i, j, k + 1)) - double(D.phb(i, j, k))) /
+    a = R((double(D.ph2(i, j, k + 1)) - double(D.ph2(i, j, k)) + D.phb64(i, j, k + 1) - D.phb64(i, j, k)) /
               phm / hypso_log<R>(pfd / pfu) -
-          double(D.alb(i, j, k)));
+          D.alb64(i, j, k));
   } else {
     a = R(-1) / (R(D.c1h[k]) * D.muts(i, j, 0) + R(D.c2h[k])) *
         (D.alb(i, j, k) * (R(D.c1h[k]) * D.mu2(i, j, 0)) + R(D.rdnw[k]) * (D.ph2(i, j, k + 1) - D.ph2(i, j, k)));
@@ -168,8 +168,8 @@ __device__ __forceinline__ void p_rho_phi_point(const Dom<R>& D, int i, int j, i
   D.al(i, j, k) = a;
   // the equation of state in double in both forms: p'' is a small difference of totals of ~1e5 Pa (in float the
   // rounding of the total's base, 6e-8, would be ~1e-4 of p'') -- for the FP64 form the same operations
-  const double base = k::r_d * (k::t0 + double(D.t2(i, j, k))) / (k::p1000mb * (double(a) + double(D.alb(i, j, k))));
-  D.p(i, j, k) = R(k::p1000mb * eos_pow<R>(base) - double(D.pb(i, j, k)));
+  const double base = k::r_d * (k::t0 + double(D.t2(i, j, k))) / (k::p1000mb * (double(a) + D.alb64(i, j, k)));
+  D.p(i, j, k) = R(k::p1000mb * eos_pow<R>(base) - D.pb64(i, j, k));
 }
 // mode 0: every mass point; 1: calc_p_rho_phi_interior (after spec_bdy_final); 2: after the microphysics, only in
 // the members that have it, on the interior where the member has boundary data (rk3.cpp:146-158)
@@ -245,10 +245,10 @@ __global__ void __launch_bounds__(PX) k_q_tendf_rk1(const __grid_constant__ Pack
   D.qtf[n](i, j, k) = t;
 }
 
-// advect_scalar (Fluxes::adv :126-139) of species n at a cell, from its horizontal face fluxes
+// advect_scalar (Fluxes::adv :126-139) of species n at a cell outside the spec zone, from its horizontal face
+// fluxes: the horizontal part (the vertical flux divergence follows in q_adv)
 template <class R>
-__device__ R q_adv(const Dom<R>& D, const V3<R>& q, int i, int j, int k, R fx0, R fx1, R fy0, R fy1) {
-  if (spec_cell(D, i, j)) return 0;
+__device__ R q_adv_h(const Dom<R>& D, const V3<R>& q, int i, int j, int k, R fx0, R fx1, R fy0, R fy1) {
   R r;
   const bool ocol = D.open_x && (i == 0 || i == D.nx - 1), orow = D.open_y && (j == 0 || j == D.ny - 1);
   if (ocol || orow) {  // open boundary (:129-134): y flux, x flux, open x, open y (field_old = the scalar), vertical
@@ -261,6 +261,12 @@ __device__ R q_adv(const Dom<R>& D, const V3<R>& q, int i, int j, int k, R fx0, 
     r = -(D.msftx(i, j) * R(D.rdx)) * (fx1 - fx0);
     if (D.do_y) r -= (D.msftx(i, j) * R(D.rdy)) * (fy1 - fy0);
   }
+  return r;
+}
+template <class R>
+__device__ R q_adv(const Dom<R>& D, const V3<R>& q, int i, int j, int k, R fx0, R fx1, R fy0, R fy1) {
+  if (spec_cell(D, i, j)) return 0;
+  const R r = q_adv_h(D, q, i, j, k, fx0, fx1, fy0, fy1);
   return r - R(D.rdnw[k]) * (sc_fz(D, q, D.ww_m, i, j, k + 1, false) - sc_fz(D, q, D.ww_m, i, j, k, false));
 }
 // KUpdate (:145-156) for the non-PD species of this stage, every species of the point in one thread (the mass
@@ -304,6 +310,133 @@ __global__ void __launch_bounds__(PX, 12) k_q_update(const __grid_constant__ Pac
       D.qn[n](i, j, k) = (m_full(D, k, mub, mu1) * D.q1[n].ld(i, j, k) + dt_rk * tend) / m_full(D, k, mub, mu2);
     }
     __syncthreads();  // the next species reuses the face arrays
+  }
+}
+// The same update with the species' planes staged in shared memory by the tensor-memory accelerator: a block takes
+// a tile of kQTx x kQTy columns (one thread each) over a chunk of q_chunk(SH) levels; for each species one copy per
+// plane brings the tile's planes k0 - 2 .. k1 + 1 with a halo of 4 columns (the copy's x start stays 16-byte
+// aligned) and 3 rows into a plane slot of its own (slots 128-byte aligned, as a tensor copy's destination must be),
+// the next species' planes copied into the other buffer while this one is computed. Per level
+// the block's x and y face fluxes are formed once (shared arrays); each thread then marches up its column, the
+// vertical face flux of the level below carried over from the step before. Statement for statement the arithmetic
+// of k_q_update (the same values are read, from shared memory instead of global memory).
+template <class R>
+struct QPlanes {  // a species' planes of one tile in shared memory, read with the domain's indices
+  const R* s;
+  int i0, j0, k0;  // the indices of s[0]
+  static constexpr int W = kQTx + 8, H = kQTy + 6;
+  static constexpr int PS = int((W * H * sizeof(R) + 127) / 128 * 128 / sizeof(R));  // plane slot, 128-byte multiple
+  __device__ __forceinline__ R ld(int i, int j, int k) const { return s[(i - i0) + W * (j - j0) + PS * (k - k0)]; }
+};
+template <class R>
+__host__ __device__ constexpr size_t q_march_smem(int shape) {
+  // two plane buffers, then the x and y face fluxes of every level of the chunk, and 128 bytes to align the start
+  return 2 * size_t(q_chunk(shape) + 4) * QPlanes<R>::PS * sizeof(R) +
+         size_t(q_chunk(shape)) * (kQTy * (kQTx + 1) + (kQTy + 1) * kQTx) * sizeof(R) + 128;
+}
+template <class R, int NM, int SH>
+__global__ void __launch_bounds__(kQTx * kQTy) k_q_march(const __grid_constant__ Pack<R, NM> P, int rk) {
+  constexpr int KC = q_chunk(SH), NP = KC + 4, PL = QPlanes<R>::W * QPlanes<R>::H, PS = QPlanes<R>::PS;
+  extern __shared__ __align__(128) unsigned char q_smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  // the plane slots from the first 128-byte boundary of the dynamic shared memory (its size has 128 bytes to spare)
+  R* const pbuf = reinterpret_cast<R*>(q_smem + ((128u - (smem_u32(q_smem) & 127u)) & 127u));
+  R (*const sfx)[kQTy][kQTx + 1] = reinterpret_cast<R (*)[kQTy][kQTx + 1]>(pbuf + 2 * NP * PS);
+  R (*const sfy)[kQTy + 1][kQTx] = reinterpret_cast<R (*)[kQTy + 1][kQTx]>(pbuf + 2 * NP * PS + KC * kQTy * (kQTx + 1));
+  const int b = blockIdx.x;
+  const int m = member_of(P, RG_TILES, SH, b);
+  const Dom<R>& D = P.d[m];
+  const Range r = range_of(RG_TILES, D);
+  const int bx = cdiv(r.i1 - r.i0, kQTx), by = cdiv(r.j1 - r.j0, kQTy);
+  int local = b - P.start(RG_TILES, SH, m);
+  const int bi = local % bx;
+  local /= bx;
+  const int bj = local % by;
+  const int c0 = (local / by) * KC, c1 = min(c0 + KC, D.nz);
+  const int tx = int(threadIdx.x) % kQTx, ty = int(threadIdx.x) / kQTx;
+  const int ti0 = r.i0 + bi * kQTx, tj0 = r.j0 + bj * kQTy;
+  const int i = ti0 + tx, j = tj0 + ty;
+  const int nx = D.nx, ny = D.ny;
+  const bool in = i < r.i1 && j < r.j1;
+  const bool rx = j < r.j1 && j < ny, ry = i < r.i1 && i < nx;
+  const bool fx0 = rx && i <= nx && i <= r.i1, fx1 = tx == kQTx - 1 && rx && i + 1 <= nx && i + 1 <= r.i1;
+  const bool fy0 = D.do_y && ry && j <= ny && j <= r.j1, fy1 = D.do_y && ty == kQTy - 1 && ry && j + 1 <= ny && j + 1 <= r.j1;
+  const R dt_rk = R(rk == 1 ? D.dt / 3.0 : (rk == 2 ? 0.5 * D.dt : D.dt));
+  R mub = 0, mu1 = 0, mu2 = 0, msfty = 0;
+  if (in) {
+    mub = D.mub(i, j);
+    mu1 = D.mu1.ld(i, j, 0);
+    mu2 = D.mu2.ld(i, j, 0);
+    msfty = D.msfty(i, j);
+  }
+  auto next = [&](int n) {  // the next species updated here (not PD at this stage), from n on
+    while (n < D.n_scalars && q_is_pd(D, n, rk)) ++n;
+    return n;
+  };
+  int n = next(0);
+  if (n >= D.n_scalars) return;  // uniform over the block
+  const QMap* const qm = D.qmap;
+  // the map coordinates of the tile's first staged element (ti0 - 4, tj0 - 3, c0 - 2); x * sizeof(R) is a
+  // multiple of 16 bytes: ti0 - r.i0 is a multiple of kQTx, and the map's x0 puts the domain's i = r.i0 - 4 at
+  // a multiple of 4 elements
+  const int xs = qm[0].x0 + ti0 - 4, ys = qm[0].y0 + tj0 - 3;
+  if ((xs * int(sizeof(R))) % 16 != 0 || (smem_u32(pbuf) & 127u) != 0) {  // never (maps of cw_create, slots above):
+    // an unaligned copy would fault
+    if (threadIdx.x == 0) atomicOr(D.status, 2u);
+    return;
+  }
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  auto issue = [&](int s, int u) {  // thread 0: species s's planes into buffer u
+    const CUtensorMap* map = D.q2[s].p == qm[s].pa ? &qm[s].a : &qm[s].b;
+    mbar_expect_tx(&bar[u], unsigned(NP * PL * sizeof(R)));
+    for (int p = 0; p < NP; ++p) tma_load_3d(pbuf + (u * NP + p) * PS, map, xs, ys, c0 - 2 + p, &bar[u]);
+  };
+  if (threadIdx.x == 0) issue(n, 0);
+  unsigned phase[2] = {0u, 0u};
+  for (int u = 0; n < D.n_scalars; u ^= 1) {
+    const int nn = next(n + 1);
+    const bool ok = mbar_wait(&bar[u], phase[u]);
+    phase[u] ^= 1u;
+    if (__syncthreads_or(!ok)) {  // the copies did not arrive: report, leave the species untouched
+      if (threadIdx.x == 0) atomicOr(D.status, 1u);
+      return;
+    }
+    // buffer u ^ 1 is free: its last reads (the species before) ended before the barrier above
+    if (nn < D.n_scalars && threadIdx.x == 0) issue(nn, u ^ 1);
+    const QPlanes<R> T{pbuf + u * NP * PS, ti0 - 4, tj0 - 3, c0 - 2};
+    for (int k = c0; k < c1; ++k) {
+      const int l = k - c0;
+      if (fx0) sfx[l][ty][tx] = sc_fx(D, T, D.ru_m, i, j, k, false);
+      if (fx1) sfx[l][ty][kQTx] = sc_fx(D, T, D.ru_m, i + 1, j, k, false);
+      if (fy0) sfy[l][ty][tx] = sc_fy(D, T, D.rv_m, i, j, k, false);
+      if (fy1) sfy[l][kQTy][tx] = sc_fy(D, T, D.rv_m, i, j + 1, k, false);
+    }
+    __syncthreads();
+    if (in) {
+      const bool spec = spec_cell(D, i, j);
+      const V3<R> q2 = D.q2[n], q1 = D.q1[n], qtf = D.qtf[n], qn = D.qn[n];
+      R fz0 = sc_fz(D, T, D.ww_m, i, j, c0, false);
+      for (int k = c0; k < c1; ++k) {
+        const int l = k - c0;
+        const R fz1 = sc_fz(D, T, D.ww_m, i, j, k + 1, false);
+        R a = 0;
+        if (!spec) {
+          const R h = q_adv_h(D, q2, i, j, k, sfx[l][ty][tx], sfx[l][ty][tx + 1], sfy[l][ty][tx], sfy[l][ty + 1][tx]);
+          a = h - R(D.rdnw[k]) * (fz1 - fz0);
+        }
+        R tend = a * msfty;
+        tend += qtf.ld(i, j, k);
+        qn(i, j, k) = (m_full(D, k, mub, mu1) * q1.ld(i, j, k) + dt_rk * tend) / m_full(D, k, mub, mu2);
+        fz0 = fz1;
+      }
+    }
+    __syncthreads();  // the face arrays are rewritten by the next species
+    n = nn;
   }
 }
 // KPreUpdatePD (:174-180)

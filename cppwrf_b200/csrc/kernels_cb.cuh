@@ -522,7 +522,7 @@ __global__ void __launch_bounds__(CX * NW, cb_minblocks(NW)) k_ac(const __grid_c
           if (k < nz) {
             auto wdwn = [&](int mm) {
               return 0.5 * (A(D.ww(i, j, mm)) + A(D.ww(i, j, mm - 1))) * D.rdnw[mm - 1] *
-                     (A(D.ph_save.ld(i, j, mm)) - A(D.ph_save.ld(i, j, mm - 1)) + A(D.phb(i, j, mm)) - A(D.phb(i, j, mm - 1)));
+                     (A(D.ph_save.ld(i, j, mm)) - A(D.ph_save.ld(i, j, mm - 1)) + A(D.phb64(i, j, mm)) - A(D.phb64(i, j, mm - 1)));
             };
             rr -= dtsA * (D.fnm[k] * wdwn(k + 1) + D.fnp[k] * wdwn(k));
           }
@@ -760,7 +760,7 @@ __global__ void __launch_bounds__(CX * NW) k_dampkm(const __grid_constant__ Pack
     return;
   }
   const double piconst = 3.1415926535897932384626433, degrad = piconst / 180.0, degrad90 = degrad * 90.0;
-  auto zw = [&](int k) { return (double(D.ph2.ld(i, j, k)) + double(D.phb(i, j, k))) / k::g; };
+  auto zw = [&](int k) { return (double(D.ph2.ld(i, j, k)) + D.phb64(i, j, k)) / k::g; };
   const double dx_m = D.dx / double(D.msftx(i, j)), dy_m = D.dy / double(D.msfty(i, j));
   const double ds = dx_m < dy_m ? dx_m : dy_m;
   const double kmmax = ds * ds / D.dt;

@@ -50,9 +50,9 @@ __device__ __forceinline__ double dg_energy(const Dom<R>& D, const DiagConst& c,
   const double uc = 0.5 * (double(D.u2.ld(i, j, k)) + double(D.u2.ld(i + 1, j, k)));
   const double vc = 0.5 * (double(D.v2.ld(i, j, k)) + double(D.v2.ld(i, j + 1, k)));
   const double wc = 0.5 * (double(D.w2.ld(i, j, k)) + double(D.w2.ld(i, j, k + 1)));
-  const double T = (double(D.t2.ld(i, j, k)) + 300.0) * cw_pow((double(D.p.ld(i, j, k)) + double(D.pb(i, j, k))) / 100000.0, c.rcp);
-  const double phm = 0.5 * (double(D.ph2.ld(i, j, k)) + double(D.ph2.ld(i, j, k + 1)) + double(D.phb(i, j, k)) +
-                            double(D.phb(i, j, k + 1)));
+  const double T = (double(D.t2.ld(i, j, k)) + 300.0) * cw_pow((double(D.p.ld(i, j, k)) + D.pb64(i, j, k)) / 100000.0, c.rcp);
+  const double phm = 0.5 * (double(D.ph2.ld(i, j, k)) + double(D.ph2.ld(i, j, k + 1)) + D.phb64(i, j, k) +
+                            D.phb64(i, j, k + 1));
   return -D.dnw[k] * m * (0.5 * (uc * uc + vc * vc + wc * wc) + c.cv * T + phm);
 }
 

@@ -62,8 +62,8 @@ __global__ void __launch_bounds__(CX * NW) k_kessler(const __grid_constant__ Pac
   double* s_vtden = cb_array(3, nz);
   double* s_rdzw = cb_array(4, nz);
   double* s_rdzk = cb_array(5, nz);
-  auto zw = [&](int k) { return (double(D.ph2(i, j, k)) + double(D.phb(i, j, k))) / g; };
-  auto rho_at = [&](int k) { return 1.0 / (double(D.al(i, j, k)) + double(D.alb(i, j, k))); };
+  auto zw = [&](int k) { return (double(D.ph2(i, j, k)) + D.phb64(i, j, k)) / g; };
+  auto rho_at = [&](int k) { return 1.0 / (double(D.al(i, j, k)) + D.alb64(i, j, k)); };
   if (mp) {
     const double rho0 = rho_at(0);
     CB_LOOP(k, nz) {  // kessler.hpp:103-117
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(CX * NW) k_kessler(const __grid_constant__ Pac
     double th = th_old, q = q_old;
     if (mp) {  // production of rain, condensation, evaporation (kessler.hpp:168-197)
       const double c1 = 0.001, c2 = 0.001, c3 = 2.2, c4 = 0.875;
-      const double pii = mp_pow<R>((double(D.p(i, j, k)) + double(D.pb(i, j, k))) / 100000.0, rcp);
+      const double pii = mp_pow<R>((double(D.p(i, j, k)) + D.pb64(i, j, k)) / 100000.0, rcp);
       double qck = double(qc(i, j, k)), qrk = double(qr(i, j, k));
       const double prodk = s_prodk[k * CX + lane];
       const double factorn = 1.0 / (1.0 + c3 * dt * mp_pow<R>(mp_max(0.0, qrk), c4));

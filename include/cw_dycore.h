@@ -170,8 +170,13 @@ int cw_n_sound(cw_handle* h, int* out);
 /* The stream the handle launches on (cuda_stream_raw, src/core/backend.cpp:73-81); NULL = its own. */
 int cw_set_stream(cw_handle* h, void* cuda_stream);
 /* dev_sync + fatal_check (src/core/backend.hpp:745-769): waits for the handle's work and reports a
- * device-side error status. */
+ * device-side error status: a CUDA error, or the handle's status word (a kernel whose bounded wait for its
+ * tensor-memory copies ran out, about a second, left its part of the step undone; the word is cleared). */
 int cw_sync(cw_handle* h);
+/* Self-test of the kernels' bounded waits (no reference counterpart): one block waits on a shared-memory barrier
+ * that nothing completes, gives up after `cycles` SM clock cycles (<= 0: the kernels' own limit, about a second) and
+ * sets the status word, so that the next cw_sync fails with its message and clears it; the handle stays usable. */
+int cw_selftest_wait(cw_handle* h, long long cycles);
 /* The last error message of h (or of the last failed cw_create when h is NULL). */
 const char* cw_last_error(cw_handle* h);
 /* Kernel launches of the last cw_step call (the count this library issued). */

@@ -10,8 +10,9 @@ from cases import lam_case
 
 pytestmark = pytest.mark.gpu
 
-TUNABLE = ["k_tend", "k_tendf_rk1", "k_uv", "k_q_update", "k_q_face_pd", "k_q_scale_pd", "k_q_update_pd",
-           "k_ls_prep", "k_ss_prep", "k_ac", "k_finish"]  # the last four: warps per column block
+TUNABLE = ["k_tend", "k_tendf_rk1", "k_uv", "k_q_march", "k_q_face_pd", "k_q_scale_pd", "k_q_update_pd",
+           "k_ls_prep", "k_ss_prep", "k_ac", "k_finish"]  # k_q_march: levels per block; the last four: warps per
+#                                                             column block
 
 
 @pytest.mark.parametrize("precision", [capi.FP64, capi.MIXED], ids=["fp64", "mixed"])
