@@ -652,7 +652,7 @@ def main():
                              for k in ("k_tend", "k_tend_b", "k_tendf_rk1", "k_uv", "k_q_update", "k_q_face_pd",
                                        "k_q_scale_pd", "k_q_update_pd", "k_p_rho_phi")
                              if dom.autotune_choice(k) >= 0},
-            "level_chunks": {k: [4, 2, 8][dom.autotune_choice(k)] for k in ("k_q_march",) if dom.autotune_choice(k) >= 0},
+            "level_chunks": {k: [2, 1, 4][dom.autotune_choice(k)] for k in ("k_q_march",) if dom.autotune_choice(k) >= 0},
             "column_warps": {k: [8, 16, 4][dom.autotune_choice(k)]
                              for k in ("k_ls_prep", "k_ss_prep", "k_ac", "k_finish") if dom.autotune_choice(k) >= 0},
             "clocks": clocks, "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": ebytes,

@@ -257,7 +257,7 @@ struct Launcher {
       const int nb = ps.blocks[c][size_t(RG_TILES)][size_t(sh)];
       if (nb == 0) continue;
       begin(name);
-      kerns[size_t(sh)]<<<nb, kQTx * kQTy, smem, h->stream>>>(ps.p[c], args...);
+      kerns[size_t(sh)]<<<nb, q_march_threads(sh), smem, h->stream>>>(ps.p[c], args...);
       check();
     }
   }

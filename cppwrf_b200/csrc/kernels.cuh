@@ -26,9 +26,9 @@ enum RangeKind {
   RG_FACES,       // as RG_STAG; in a patch, the faces of its cells up to the face after its last cell
   RG_TILES,       // as RG_MASS, in blocks of kQTx x kQTy columns and q_chunk(shape) levels (the TMA-staged scalars)
 };
-// The TMA-staged scalar update's block: a tile of kQTx x kQTy columns (one thread each) and a chunk of levels
+// The TMA-staged scalar update's block: a tile of kQTx x kQTy columns and a chunk of levels, one thread per point
 constexpr int kQTx = 32, kQTy = 4;
-__host__ __device__ constexpr int q_chunk(int shape) { return shape == 0 ? 4 : (shape == 1 ? 2 : 8); }
+__host__ __device__ constexpr int q_chunk(int shape) { return shape == 0 ? 2 : (shape == 1 ? 1 : 4); }
 struct Range {
   int i0, i1, j0, j1, k0, k1;
 };

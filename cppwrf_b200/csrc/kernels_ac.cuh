@@ -313,13 +313,12 @@ __global__ void __launch_bounds__(PX, 12) k_q_update(const __grid_constant__ Pac
   }
 }
 // The same update with the species' planes staged in shared memory by the tensor-memory accelerator: a block takes
-// a tile of kQTx x kQTy columns (one thread each) over a chunk of q_chunk(SH) levels; for each species one copy per
-// plane brings the tile's planes k0 - 2 .. k1 + 1 with a halo of 4 columns (the copy's x start stays 16-byte
-// aligned) and 3 rows into a plane slot of its own (slots 128-byte aligned, as a tensor copy's destination must be),
-// the next species' planes copied into the other buffer while this one is computed. Per level
-// the block's x and y face fluxes are formed once (shared arrays); each thread then marches up its column, the
-// vertical face flux of the level below carried over from the step before. Statement for statement the arithmetic
-// of k_q_update (the same values are read, from shared memory instead of global memory).
+// a tile of kQTx x kQTy columns over a chunk of q_chunk(SH) levels, one thread per point of it; for each species one
+// copy per plane brings the tile's planes k0 - 2 .. k1 + 1 with a halo of 4 columns (the copy's x start stays
+// 16-byte aligned) and 3 rows into a plane slot of its own (slots 128-byte aligned, as a tensor copy's destination
+// must be), the next species' planes copied into the other buffer while this one is computed. The block forms every
+// x, y and z face flux of the chunk once (shared arrays), then every point its update. Statement for statement the
+// arithmetic of k_q_update (the same values are read, from shared memory instead of global memory).
 template <class R>
 struct QPlanes {  // a species' planes of one tile in shared memory, read with the domain's indices
   const R* s;
@@ -330,12 +329,17 @@ struct QPlanes {  // a species' planes of one tile in shared memory, read with t
 };
 template <class R>
 __host__ __device__ constexpr size_t q_march_smem(int shape) {
-  // two plane buffers, then the x and y face fluxes of every level of the chunk, and 128 bytes to align the start
+  // two plane buffers, then the x, y and z face fluxes of the chunk, and 128 bytes to align the start
   return 2 * size_t(q_chunk(shape) + 4) * QPlanes<R>::PS * sizeof(R) +
-         size_t(q_chunk(shape)) * (kQTy * (kQTx + 1) + (kQTy + 1) * kQTx) * sizeof(R) + 128;
+         (size_t(q_chunk(shape)) * (kQTy * (kQTx + 1) + (kQTy + 1) * kQTx) + size_t(q_chunk(shape) + 1) * kQTy * kQTx) *
+             sizeof(R) +
+         128;
 }
+__host__ __device__ constexpr int q_march_threads(int shape) { return kQTx * kQTy * q_chunk(shape); }
 template <class R, int NM, int SH>
-__global__ void __launch_bounds__(kQTx * kQTy) k_q_march(const __grid_constant__ Pack<R, NM> P, int rk) {
+// (1024 threads per SM by the launch bound: at most 64 registers a thread, 32 warps per SM where shared memory allows)
+__global__ void __launch_bounds__(q_march_threads(SH), 1024 / q_march_threads(SH))
+    k_q_march(const __grid_constant__ Pack<R, NM> P, int rk) {
   constexpr int KC = q_chunk(SH), NP = KC + 4, PL = QPlanes<R>::W * QPlanes<R>::H, PS = QPlanes<R>::PS;
   extern __shared__ __align__(128) unsigned char q_smem[];
   __shared__ __align__(8) uint64_t bar[2];
@@ -343,6 +347,8 @@ __global__ void __launch_bounds__(kQTx * kQTy) k_q_march(const __grid_constant__
   R* const pbuf = reinterpret_cast<R*>(q_smem + ((128u - (smem_u32(q_smem) & 127u)) & 127u));
   R (*const sfx)[kQTy][kQTx + 1] = reinterpret_cast<R (*)[kQTy][kQTx + 1]>(pbuf + 2 * NP * PS);
   R (*const sfy)[kQTy + 1][kQTx] = reinterpret_cast<R (*)[kQTy + 1][kQTx]>(pbuf + 2 * NP * PS + KC * kQTy * (kQTx + 1));
+  R (*const sfz)[kQTy][kQTx] =
+      reinterpret_cast<R (*)[kQTy][kQTx]>(pbuf + 2 * NP * PS + KC * (kQTy * (kQTx + 1) + (kQTy + 1) * kQTx));
   const int b = blockIdx.x;
   const int m = member_of(P, RG_TILES, SH, b);
   const Dom<R>& D = P.d[m];
@@ -353,14 +359,16 @@ __global__ void __launch_bounds__(kQTx * kQTy) k_q_march(const __grid_constant__
   local /= bx;
   const int bj = local % by;
   const int c0 = (local / by) * KC, c1 = min(c0 + KC, D.nz);
-  const int tx = int(threadIdx.x) % kQTx, ty = int(threadIdx.x) / kQTx;
+  const int tx = int(threadIdx.x) % kQTx, ty = (int(threadIdx.x) / kQTx) % kQTy, tk = int(threadIdx.x) / (kQTx * kQTy);
   const int ti0 = r.i0 + bi * kQTx, tj0 = r.j0 + bj * kQTy;
-  const int i = ti0 + tx, j = tj0 + ty;
+  const int i = ti0 + tx, j = tj0 + ty, k = c0 + tk;
   const int nx = D.nx, ny = D.ny;
-  const bool in = i < r.i1 && j < r.j1;
-  const bool rx = j < r.j1 && j < ny, ry = i < r.i1 && i < nx;
+  const bool lev = k < c1;
+  const bool col = i < r.i1 && j < r.j1, in = col && lev;
+  const bool rx = lev && j < r.j1 && j < ny, ry = lev && i < r.i1 && i < nx;
   const bool fx0 = rx && i <= nx && i <= r.i1, fx1 = tx == kQTx - 1 && rx && i + 1 <= nx && i + 1 <= r.i1;
   const bool fy0 = D.do_y && ry && j <= ny && j <= r.j1, fy1 = D.do_y && ty == kQTy - 1 && ry && j + 1 <= ny && j + 1 <= r.j1;
+  const bool fz1 = in && k + 1 == c1;  // the top face of the chunk's last level
   const R dt_rk = R(rk == 1 ? D.dt / 3.0 : (rk == 2 ? 0.5 * D.dt : D.dt));
   R mub = 0, mu1 = 0, mu2 = 0, msfty = 0;
   if (in) {
@@ -409,31 +417,22 @@ __global__ void __launch_bounds__(kQTx * kQTy) k_q_march(const __grid_constant__
     // buffer u ^ 1 is free: its last reads (the species before) ended before the barrier above
     if (nn < D.n_scalars && threadIdx.x == 0) issue(nn, u ^ 1);
     const QPlanes<R> T{pbuf + u * NP * PS, ti0 - 4, tj0 - 3, c0 - 2};
-    for (int k = c0; k < c1; ++k) {
-      const int l = k - c0;
-      if (fx0) sfx[l][ty][tx] = sc_fx(D, T, D.ru_m, i, j, k, false);
-      if (fx1) sfx[l][ty][kQTx] = sc_fx(D, T, D.ru_m, i + 1, j, k, false);
-      if (fy0) sfy[l][ty][tx] = sc_fy(D, T, D.rv_m, i, j, k, false);
-      if (fy1) sfy[l][kQTy][tx] = sc_fy(D, T, D.rv_m, i, j + 1, k, false);
-    }
+    if (fx0) sfx[tk][ty][tx] = sc_fx(D, T, D.ru_m, i, j, k, false);
+    if (fx1) sfx[tk][ty][kQTx] = sc_fx(D, T, D.ru_m, i + 1, j, k, false);
+    if (fy0) sfy[tk][ty][tx] = sc_fy(D, T, D.rv_m, i, j, k, false);
+    if (fy1) sfy[tk][kQTy][tx] = sc_fy(D, T, D.rv_m, i, j + 1, k, false);
+    if (in) sfz[tk][ty][tx] = sc_fz(D, T, D.ww_m, i, j, k, false);
+    if (fz1) sfz[tk + 1][ty][tx] = sc_fz(D, T, D.ww_m, i, j, k + 1, false);
     __syncthreads();
     if (in) {
-      const bool spec = spec_cell(D, i, j);
-      const V3<R> q2 = D.q2[n], q1 = D.q1[n], qtf = D.qtf[n], qn = D.qn[n];
-      R fz0 = sc_fz(D, T, D.ww_m, i, j, c0, false);
-      for (int k = c0; k < c1; ++k) {
-        const int l = k - c0;
-        const R fz1 = sc_fz(D, T, D.ww_m, i, j, k + 1, false);
-        R a = 0;
-        if (!spec) {
-          const R h = q_adv_h(D, q2, i, j, k, sfx[l][ty][tx], sfx[l][ty][tx + 1], sfy[l][ty][tx], sfy[l][ty + 1][tx]);
-          a = h - R(D.rdnw[k]) * (fz1 - fz0);
-        }
-        R tend = a * msfty;
-        tend += qtf.ld(i, j, k);
-        qn(i, j, k) = (m_full(D, k, mub, mu1) * q1.ld(i, j, k) + dt_rk * tend) / m_full(D, k, mub, mu2);
-        fz0 = fz1;
+      R a = 0;
+      if (!spec_cell(D, i, j)) {
+        const R h = q_adv_h(D, D.q2[n], i, j, k, sfx[tk][ty][tx], sfx[tk][ty][tx + 1], sfy[tk][ty][tx], sfy[tk][ty + 1][tx]);
+        a = h - R(D.rdnw[k]) * (sfz[tk + 1][ty][tx] - sfz[tk][ty][tx]);
       }
+      R tend = a * msfty;
+      tend += D.qtf[n].ld(i, j, k);
+      D.qn[n](i, j, k) = (m_full(D, k, mub, mu1) * D.q1[n].ld(i, j, k) + dt_rk * tend) / m_full(D, k, mub, mu2);
     }
     __syncthreads();  // the face arrays are rewritten by the next species
     n = nn;
