@@ -327,13 +327,14 @@ struct QPlanes {  // a species' planes of one tile in shared memory, read with t
   static constexpr int PS = int((W * H * sizeof(R) + 127) / 128 * 128 / sizeof(R));  // plane slot, 128-byte multiple
   __device__ __forceinline__ R ld(int i, int j, int k) const { return s[(i - i0) + W * (j - j0) + PS * (k - k0)]; }
 };
+// the x, y and z face fluxes of a chunk
+__host__ __device__ constexpr size_t q_face_elems(int shape) {
+  return size_t(q_chunk(shape)) * (kQTy * (kQTx + 1) + (kQTy + 1) * kQTx) + size_t(q_chunk(shape) + 1) * kQTy * kQTx;
+}
 template <class R>
 __host__ __device__ constexpr size_t q_march_smem(int shape) {
   // two plane buffers, then the x, y and z face fluxes of the chunk, and 128 bytes to align the start
-  return 2 * size_t(q_chunk(shape) + 4) * QPlanes<R>::PS * sizeof(R) +
-         (size_t(q_chunk(shape)) * (kQTy * (kQTx + 1) + (kQTy + 1) * kQTx) + size_t(q_chunk(shape) + 1) * kQTy * kQTx) *
-             sizeof(R) +
-         128;
+  return 2 * size_t(q_chunk(shape) + 4) * QPlanes<R>::PS * sizeof(R) + q_face_elems(shape) * sizeof(R) + 128;
 }
 __host__ __device__ constexpr int q_march_threads(int shape) { return kQTx * kQTy * q_chunk(shape); }
 template <class R, int NM, int SH>
@@ -414,7 +415,8 @@ __global__ void __launch_bounds__(q_march_threads(SH), 1024 / q_march_threads(SH
       if (threadIdx.x == 0) atomicOr(D.status, 1u);
       return;
     }
-    // buffer u ^ 1 is free: its last reads (the species before) ended before the barrier above
+    // every thread has passed the barrier above after the species before: its reads of plane buffer u ^ 1 (the face
+    // phase) and of the face arrays (the update phase) are over, so both may be written again
     if (nn < D.n_scalars && threadIdx.x == 0) issue(nn, u ^ 1);
     const QPlanes<R> T{pbuf + u * NP * PS, ti0 - 4, tj0 - 3, c0 - 2};
     if (fx0) sfx[tk][ty][tx] = sc_fx(D, T, D.ru_m, i, j, k, false);
@@ -434,8 +436,7 @@ __global__ void __launch_bounds__(q_march_threads(SH), 1024 / q_march_threads(SH
       tend += D.qtf[n].ld(i, j, k);
       D.qn[n](i, j, k) = (m_full(D, k, mub, mu1) * D.q1[n].ld(i, j, k) + dt_rk * tend) / m_full(D, k, mub, mu2);
     }
-    __syncthreads();  // the face arrays are rewritten by the next species
-    n = nn;
+    n = nn;  // no barrier here: the one after the next species' wait orders these reads before its writes
   }
 }
 // KPreUpdatePD (:174-180)
