@@ -342,6 +342,7 @@ template <class R, int NM, int SH>
 __global__ void __launch_bounds__(q_march_threads(SH), 1024 / q_march_threads(SH))
     k_q_march(const __grid_constant__ Pack<R, NM> P, int rk) {
   constexpr int KC = q_chunk(SH), NP = KC + 4, PL = QPlanes<R>::W * QPlanes<R>::H, PS = QPlanes<R>::PS;
+  constexpr int kNX = KC * kQTy * (kQTx + 1), kNY = KC * (kQTy + 1) * kQTx, kNZ = (KC + 1) * kQTy * kQTx;
   extern __shared__ __align__(128) unsigned char q_smem[];
   __shared__ __align__(8) uint64_t bar[2];
   // the plane slots from the first 128-byte boundary of the dynamic shared memory (its size has 128 bytes to spare)
@@ -364,12 +365,8 @@ __global__ void __launch_bounds__(q_march_threads(SH), 1024 / q_march_threads(SH
   const int ti0 = r.i0 + bi * kQTx, tj0 = r.j0 + bj * kQTy;
   const int i = ti0 + tx, j = tj0 + ty, k = c0 + tk;
   const int nx = D.nx, ny = D.ny;
-  const bool lev = k < c1;
+  const bool lev = k < c1;  // this thread's point: its update
   const bool col = i < r.i1 && j < r.j1, in = col && lev;
-  const bool rx = lev && j < r.j1 && j < ny, ry = lev && i < r.i1 && i < nx;
-  const bool fx0 = rx && i <= nx && i <= r.i1, fx1 = tx == kQTx - 1 && rx && i + 1 <= nx && i + 1 <= r.i1;
-  const bool fy0 = D.do_y && ry && j <= ny && j <= r.j1, fy1 = D.do_y && ty == kQTy - 1 && ry && j + 1 <= ny && j + 1 <= r.j1;
-  const bool fz1 = in && k + 1 == c1;  // the top face of the chunk's last level
   const R dt_rk = R(rk == 1 ? D.dt / 3.0 : (rk == 2 ? 0.5 * D.dt : D.dt));
   R mub = 0, mu1 = 0, mu2 = 0, msfty = 0;
   if (in) {
@@ -419,12 +416,29 @@ __global__ void __launch_bounds__(q_march_threads(SH), 1024 / q_march_threads(SH
     // phase) and of the face arrays (the update phase) are over, so both may be written again
     if (nn < D.n_scalars && threadIdx.x == 0) issue(nn, u ^ 1);
     const QPlanes<R> T{pbuf + u * NP * PS, ti0 - 4, tj0 - 3, c0 - 2};
-    if (fx0) sfx[tk][ty][tx] = sc_fx(D, T, D.ru_m, i, j, k, false);
-    if (fx1) sfx[tk][ty][kQTx] = sc_fx(D, T, D.ru_m, i + 1, j, k, false);
-    if (fy0) sfy[tk][ty][tx] = sc_fy(D, T, D.rv_m, i, j, k, false);
-    if (fy1) sfy[tk][kQTy][tx] = sc_fy(D, T, D.rv_m, i, j + 1, k, false);
-    if (in) sfz[tk][ty][tx] = sc_fz(D, T, D.ww_m, i, j, k, false);
-    if (fz1) sfz[tk + 1][ty][tx] = sc_fz(D, T, D.ww_m, i, j, k + 1, false);
+    // the chunk's faces in one flat list over the block's threads (consecutive threads take neighbouring faces of one
+    // kind, so a warp's lanes seldom diverge): the x faces ti0 .. ti0 + 32 of rows in range, the y faces tj0 ..
+    // tj0 + 4 of columns in range, the z faces c0 .. c1 of the columns in range; the faces up to nx (ny) and r.i1
+    // (r.j1), as k_q_update forms them
+    for (int f = int(threadIdx.x); f < kNX + kNY + kNZ; f += q_march_threads(SH)) {
+      if (f < kNX) {
+        const int fi = f % (kQTx + 1), fj = (f / (kQTx + 1)) % kQTy, fk = f / ((kQTx + 1) * kQTy);
+        const int fi_ = ti0 + fi, fj_ = tj0 + fj, fk_ = c0 + fk;
+        if (fk_ < c1 && fj_ < r.j1 && fj_ < ny && fi_ <= nx && fi_ <= r.i1)
+          sfx[fk][fj][fi] = sc_fx(D, T, D.ru_m, fi_, fj_, fk_, false);
+      } else if (f < kNX + kNY) {
+        const int g = f - kNX;
+        const int fi = g % kQTx, fj = (g / kQTx) % (kQTy + 1), fk = g / (kQTx * (kQTy + 1));
+        const int fi_ = ti0 + fi, fj_ = tj0 + fj, fk_ = c0 + fk;
+        if (D.do_y && fk_ < c1 && fi_ < r.i1 && fi_ < nx && fj_ <= ny && fj_ <= r.j1)
+          sfy[fk][fj][fi] = sc_fy(D, T, D.rv_m, fi_, fj_, fk_, false);
+      } else {
+        const int g = f - kNX - kNY;
+        const int fi = g % kQTx, fj = (g / kQTx) % kQTy, fk = g / (kQTx * kQTy);
+        const int fi_ = ti0 + fi, fj_ = tj0 + fj, fk_ = c0 + fk;
+        if (fk_ <= c1 && fi_ < r.i1 && fj_ < r.j1) sfz[fk][fj][fi] = sc_fz(D, T, D.ww_m, fi_, fj_, fk_, false);
+      }
+    }
     __syncthreads();
     if (in) {
       R a = 0;
